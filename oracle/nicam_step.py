@@ -1,0 +1,1600 @@
+"""CPU oracle: float64 numpy restatement of the NICAM-DC dynamics step.
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker the CUDA path is compared
+against; it is imported by ``tests/``, by ``__graft_entry__.smoke()`` and by the
+``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` and by nothing else.
+The product path never calls it.
+
+It restates, operator by operator and in the same floating-point association
+order, the reference's numpy backend of ``Dyn.dynamics_step``
+(pynicamdc/nhm/dynamics/mod_dynamics.py:1725-2741) for the configuration the
+reference runs in its JW baroclinic-wave case: RK3 HEVI, DIRECT lap_order-2
+hyperdiffusion and divergence damping, NOBASE reference state, MIURA2004
+tracer advection with the Thuburn limiters, TEM/TEM thermal and FREE/RIGID
+momentum boundaries, one rank holding all regions and both poles.
+
+Array layout is the reference's: regional ``(i, j, k, l)`` (+ trailing
+component axis), pole ``(g, k, l)`` with g = 0 the pole point and 1..5 its
+neighbours.  ``geo`` is the flat setup dict written by the fixture generator
+(keys are the reference's attribute names, e.g. ``VMTR_RGAM``).
+
+Pinned against the reference: ``tests/test_oracle_golden.py`` replays the
+committed golden states produced by the reference itself
+(``tests/golden/make_golden.py``).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+I_RHOG, I_RHOGVX, I_RHOGVY, I_RHOGVZ, I_RHOGW, I_RHOGE = 0, 1, 2, 3, 4, 5
+I_pre, I_tem, I_vx, I_vy, I_vz, I_w = 0, 1, 2, 3, 4, 5
+XDIR, YDIR, ZDIR = 0, 1, 2
+TI, TJ = 0, 1
+AI, AIJ, AJ = 0, 1, 2
+W1, W2, W3 = 2, 3, 4            # GMTR_t column indices
+P_RAREA = 1                      # GMTR_p column index
+HNX, HNY, HNZ = 0, 1, 2          # GMTR_a column indices (regional and pole)
+
+
+class Geo:
+    """Run constants of one grid: a thin attribute view of the setup dict."""
+
+    def __init__(self, d):
+        self.d = d
+        c = lambda k: d[k].item() if np.ndim(d[k]) == 0 else d[k]
+        self.kall = int(c("kall"))
+        self.kmin = int(c("kmin"))
+        self.kmax = int(c("kmax"))
+        self.gall_1d = int(c("gall_1d"))
+        self.gmin = int(c("gmin"))
+        self.gmax = int(c("gmax"))
+        self.lall = int(c("lall"))
+        self.have_sgp = np.asarray(d["have_sgp"], bool)
+        self.pntmask = np.asarray(d["pntmask"])
+        self.nq = int(c("nq"))
+        for k in ("GRAV", "Rdry", "CVdry", "CPdry", "Rvap", "OHM", "RADIUS",
+                  "EPS", "HUGE", "PRE00", "rscale", "alpha", "dtl", "dts",
+                  "Kh_coef", "divdamp_coef", "hdiff_fact_rho"):
+            setattr(self, k, float(c(k)))
+        self.sstep = [int(x) for x in np.asarray(d["sstep"])]
+        self.CVW = np.asarray(d["CVW"], np.float64)
+
+    def __getattr__(self, k):
+        d = self.__dict__.get("d")
+        if d is not None and k in d:
+            return d[k]
+        raise AttributeError(k)
+
+
+# --------------------------------------------------------------------------
+# halo exchange  (share/mod_comm.py:1563-1644, single rank: local copies only)
+# --------------------------------------------------------------------------
+def comm(g, var, var_pl):
+    """In-place region-edge / pole / singular-point copy of ``var (i,j,k,l,v)``
+    and ``var_pl (g,k,l,v)``; copy order and read-before-write semantics follow
+    mod_comm.py:1613-1641."""
+    c = g.copy_r2r
+    if c.shape[1]:
+        var[c[3], c[4], :, c[5], :] = var[c[0], c[1], :, c[2], :]
+    c = g.copy_p2r
+    if c.shape[1]:
+        var[c[3], c[4], :, c[5], :] = var_pl[c[0], :, c[2], :]
+    c = g.copy_r2p
+    if c.shape[1]:
+        var_pl[c[3], :, c[5], :] = var[c[0], c[1], :, c[2], :]
+    c = g.copy_sgp
+    if c.shape[1]:
+        var[c[3], c[4], :, c[5], :] = var[c[0], c[1], :, c[2], :].copy()
+
+
+def comm1(g, a, a_pl):
+    """COMM of a single (i,j,k,l) field."""
+    v = a[..., None].copy()
+    vp = a_pl[..., None].copy()
+    comm(g, v, vp)
+    a[...] = v[..., 0]
+    a_pl[...] = vp[..., 0]
+
+
+# --------------------------------------------------------------------------
+# Pre_Post: diagnostics, boundary conditions, deviations
+# --------------------------------------------------------------------------
+def diagnostics(g, PROG, PROGq, DIAG, PROG_pl, PROGq_pl, DIAG_pl):
+    """kernels/diag.py:53-143 (regional) and mod_dynamics.py:1163-1196 (pole).
+    Returns rho, ein, q (+pole) and writes DIAG/DIAG_pl in place."""
+    kmin, kmax = g.kmin, g.kmax
+    out = []
+    for P, Pq, D, GS, C2W in ((PROG, PROGq, DIAG, g.VMTR_GSGAM2, g.VMTR_C2Wfact),
+                              (PROG_pl, PROGq_pl, DIAG_pl, g.VMTR_GSGAM2_pl, g.VMTR_C2Wfact_pl)):
+        RHOG = P[..., I_RHOG]
+        rho = RHOG / GS
+        D[..., I_vx] = P[..., I_RHOGVX] / RHOG
+        D[..., I_vy] = P[..., I_RHOGVY] / RHOG
+        D[..., I_vz] = P[..., I_RHOGVZ] / RHOG
+        ein = P[..., I_RHOGE] / RHOG
+        q = Pq / RHOG[..., None]
+        qd = 1.0 - q[..., 0]
+        cv = q[..., 0] * g.CVW[0] + qd * g.CVdry
+        tem = ein / cv
+        D[..., I_tem] = tem
+        D[..., I_pre] = rho * tem * (qd * g.Rdry + q[..., 0] * g.Rvap)
+        ks = [slice(None)] * (P.ndim - 1)
+        kin, kdn = list(ks), list(ks)
+        kax = P.ndim - 3
+        kin[kax] = slice(kmin + 1, kmax + 1)
+        kdn[kax] = slice(kmin, kmax)
+        kin, kdn = tuple(kin), tuple(kdn)
+        D[kin + (I_w,)] = P[kin + (I_RHOGW,)] / (C2W[kin + (0,)] * RHOG[kin] + C2W[kin + (1,)] * RHOG[kdn])
+        out += [rho, ein, q]
+    return out
+
+
+def _kidx(a, k):
+    """index k on the level axis of a regional (i,j,k,l) or pole (g,k,l) array"""
+    return a[:, :, k, :] if a.ndim == 4 else a[:, k, :]
+
+
+def _kset(a, k, v):
+    if a.ndim == 4:
+        a[:, :, k, :] = v
+    else:
+        a[:, k, :] = v
+
+
+def bndcnd_all(g, DIAG, PROG, rho, ein, pole=False):
+    """share/mod_bndcnd.py:182-264 with kernels/bndcnd.py (TEM/TEM, FREE top,
+    RIGID bottom); in place."""
+    kmin, kmax = g.kmin, g.kmax
+    sfx = "_pl" if pole else ""
+    GS = getattr(g, "VMTR_GSGAM2" + sfx)
+    C2W = getattr(g, "VMTR_C2Wfact" + sfx)
+    C2WGz = getattr(g, "VMTR_C2WfactGz" + sfx)
+    PHI = getattr(g, "VMTR_PHI" + sfx)
+    tem = DIAG[..., I_tem]
+    pre = DIAG[..., I_pre]
+    K = lambda a, k: _kidx(a, k)
+    tem_top = K(tem, kmax).copy()
+    tem_btm = K(tem, kmin).copy()
+    pre_top = K(pre, kmax - 1) - K(rho, kmax) * (K(PHI, kmax + 1) - K(PHI, kmax - 1))
+    pre_btm = K(pre, kmin + 1) - K(rho, kmin) * (K(PHI, kmin - 1) - K(PHI, kmin + 1))
+    rho_top = pre_top / (g.Rdry * tem_top)
+    rho_btm = pre_btm / (g.Rdry * tem_btm)
+    _kset(tem, kmax + 1, tem_top); _kset(tem, kmin - 1, tem_btm)
+    _kset(pre, kmax + 1, pre_top); _kset(pre, kmin - 1, pre_btm)
+    _kset(rho, kmax + 1, rho_top); _kset(rho, kmin - 1, rho_btm)
+    rhog = PROG[..., I_RHOG]
+    _kset(rhog, kmax + 1, K(rho, kmax + 1) * K(GS, kmax + 1))
+    _kset(rhog, kmin - 1, K(rho, kmin - 1) * K(GS, kmin - 1))
+    _kset(ein, kmax + 1, g.CVdry * K(tem, kmax + 1))
+    _kset(ein, kmin - 1, g.CVdry * K(tem, kmin - 1))
+    _kset(PROG[..., I_RHOGE], kmax + 1, K(rhog, kmax + 1) * K(ein, kmax + 1))
+    _kset(PROG[..., I_RHOGE], kmin - 1, K(rhog, kmin - 1) * K(ein, kmin - 1))
+    # momentum: FREE top (sgn +1), RIGID bottom (sgn -1)
+    for iv in (I_RHOGVX, I_RHOGVY, I_RHOGVZ):
+        v = PROG[..., iv]
+        top = 1.0 * (K(v, kmax) / K(rhog, kmax)) * K(rhog, kmax + 1)
+        btm = -1.0 * (K(v, kmin) / K(rhog, kmin)) * K(rhog, kmin - 1)
+        _kset(v, kmax + 1, top)
+        _kset(v, kmin - 1, btm)
+    for kk in (kmax + 1, kmin - 1):
+        for iv, idg in ((I_RHOGVX, I_vx), (I_RHOGVY, I_vy), (I_RHOGVZ, I_vz)):
+            _kset(DIAG[..., idg], kk, K(PROG[..., iv], kk) / K(rhog, kk))
+    rw = PROG[..., I_RHOGW]
+    vx, vy, vz = PROG[..., I_RHOGVX], PROG[..., I_RHOGVY], PROG[..., I_RHOGVZ]
+    cz = lambda k, c: K(C2WGz[..., c], k)
+    rw_top = -(cz(kmax + 1, 0) * K(vx, kmax + 1) + cz(kmax + 1, 1) * K(vx, kmax)
+               + cz(kmax + 1, 2) * K(vy, kmax + 1) + cz(kmax + 1, 3) * K(vy, kmax)
+               + cz(kmax + 1, 4) * K(vz, kmax + 1) + cz(kmax + 1, 5) * K(vz, kmax))
+    _kset(rw, kmax + 1, rw_top)
+    _kset(rw, kmin, np.zeros_like(K(rw, kmin)))
+    _kset(rw, kmin - 1, 0.0)
+    w = DIAG[..., I_w]
+    _kset(w, kmax + 1, K(rw, kmax + 1) / (K(C2W[..., 0], kmax + 1) * K(rhog, kmax + 1)
+                                          + K(C2W[..., 1], kmax + 1) * K(rhog, kmax)))
+    _kset(w, kmin, K(rw, kmin) / (K(C2W[..., 0], kmin) * K(rhog, kmin)
+                                  + K(C2W[..., 1], kmin) * K(rhog, kmin - 1)))
+    _kset(w, kmin - 1, 0.0)
+
+
+# --------------------------------------------------------------------------
+# horizontal operators (kernels/oprt*.py)
+# --------------------------------------------------------------------------
+def _pad2(inner, i, j, lo=1):
+    out = np.zeros((i, j) + inner.shape[2:], inner.dtype)
+    out[lo:lo + inner.shape[0], lo:lo + inner.shape[1]] = inner
+    return out
+
+
+def divergence(g, vx, vy, vz):
+    """kernels/fluxconv.py:52-78 (coef_div 7-point, zero border)."""
+    i, j = vx.shape[:2]
+    c = g.OPRT_coef_div[1:i - 1, 1:j - 1]
+
+    def st(v, d):
+        return (c[..., d, 0] * v[1:i - 1, 1:j - 1] + c[..., d, 1] * v[2:i, 1:j - 1]
+                + c[..., d, 2] * v[2:i, 2:j] + c[..., d, 3] * v[1:i - 1, 2:j]
+                + c[..., d, 4] * v[0:i - 2, 1:j - 1] + c[..., d, 5] * v[0:i - 2, 0:j - 2]
+                + c[..., d, 6] * v[1:i - 1, 0:j - 2])
+    return _pad2(st(vx, XDIR) + st(vy, YDIR) + st(vz, ZDIR), i, j)
+
+
+def divergence_pl(g, vx, vy, vz):
+    """kernels/fluxconv.py:81-108: only the pole row, summed over v = 0..5."""
+    c = g.OPRT_coef_div_pl
+    per_v = (c[:, 0, :, XDIR][:, None, :] * vx + c[:, 0, :, YDIR][:, None, :] * vy
+             + c[:, 0, :, ZDIR][:, None, :] * vz)
+    out = np.zeros_like(vx)
+    out[0] = per_v.sum(axis=0)
+    return out
+
+
+def gradient(g, s):
+    """kernels/oprtgradient.py:45-70 (and presgrad.py:64-97), returns (i,j,k,l,3)."""
+    i, j = s.shape[:2]
+    stk = np.stack([s[1:i - 1, 1:j - 1], s[2:i, 1:j - 1], s[2:i, 2:j], s[1:i - 1, 2:j],
+                    s[0:i - 2, 1:j - 1], s[0:i - 2, 0:j - 2], s[1:i - 1, 0:j - 2]], axis=4)
+    cg = g.OPRT_coef_grad[1:i - 1, 1:j - 1]
+    comps = [np.sum(cg[..., d, :] * stk, axis=4) for d in (XDIR, YDIR, ZDIR)]
+    return _pad2(np.stack(comps, axis=4), i, j)
+
+
+def gradient_pl(g, s_pl):
+    """kernels/oprtgradient.py:73-88: pole row, per-direction sequential sum."""
+    cg = g.OPRT_coef_grad_pl[:, 0]                       # (6, l, 3)
+    row = (cg[:, None, :, :] * s_pl[..., None]).sum(axis=0)
+    out = np.zeros(s_pl.shape + (3,))
+    out[0] = row
+    return out
+
+
+def laplacian(g, s):
+    """kernels/oprtlaplacian.py:41-55."""
+    i, j = s.shape[:2]
+    c = g.OPRT_coef_lap[1:i - 1, 1:j - 1]
+    inner = (c[..., 0] * s[1:i - 1, 1:j - 1] + c[..., 1] * s[2:i, 1:j - 1]
+             + c[..., 2] * s[2:i, 2:j] + c[..., 3] * s[1:i - 1, 2:j]
+             + c[..., 4] * s[0:i - 2, 1:j - 1] + c[..., 5] * s[0:i - 2, 0:j - 2]
+             + c[..., 6] * s[1:i - 1, 0:j - 2])
+    return _pad2(inner, i, j)
+
+
+def laplacian_pl(g, s_pl):
+    """kernels/oprtlaplacian.py:58-70."""
+    out = np.zeros_like(s_pl)
+    out[0] = (g.OPRT_coef_lap_pl * s_pl).sum(axis=0)
+    return out
+
+
+def _sgp_corner(g, tTI, tTJ):
+    """singular-point fix at the (0,0) vertex (kernels/oprtdiffusion.py:91-96)."""
+    fdt = tTI.dtype
+    m0 = g.pntmask[0, :, 0].astype(fdt)
+    m1 = g.pntmask[0, :, 1].astype(fdt)
+    m0 = m0.reshape((1, 1, 1, -1) + (1,) * (tTI.ndim - 4))
+    m1 = m1.reshape((1, 1, 1, -1) + (1,) * (tTI.ndim - 4))
+    tTI = tTI.copy()
+    tTI[0:1, 0:1] = tTI[0:1, 0:1] * m0 + tTJ[1:2, 0:1] * m1
+    return tTI
+
+
+def diffusion(g, s, kh):
+    """kernels/oprtdiffusion.py:59-134."""
+    i, j = s.shape[:2]
+    gmin, gmax = g.gmin, g.gmax
+    bi, bj, bip, bjp = slice(0, i - 1), slice(0, j - 1), slice(1, i), slice(1, j)
+    s0 = s[bi, bj][..., None]
+    s_ip = s[bip, bj][..., None]
+    s_d = s[bip, bjp][..., None]
+    s_jp = s[bi, bjp][..., None]
+    cti = g.OPRT_coef_intp[bi, bj, :, :, :, :, TI]
+    ctj = g.OPRT_coef_intp[bi, bj, :, :, :, :, TJ]
+    c1i, c2i, c3i = cti[..., 0], cti[..., 1], cti[..., 2]
+    c1j, c2j, c3j = ctj[..., 0], ctj[..., 1], ctj[..., 2]
+    tTI = ((2.0 * c1i - c2i - c3i) * s0 + (-c1i + 2.0 * c2i - c3i) * s_ip
+           + (-c1i - c2i + 2.0 * c3i) * s_d) / 3.0
+    tTJ = ((2.0 * c1j - c2j - c3j) * s0 + (-c1j + 2.0 * c2j - c3j) * s_d
+           + (-c1j - c2j + 2.0 * c3j) * s_jp) / 3.0
+    tTI = _sgp_corner(g, tTI, tTJ)
+    sl, slp, slm = slice(gmin, gmax + 1), slice(gmin + 1, gmax + 2), slice(gmin - 1, gmax)
+    kh0 = kh[sl, sl]
+    kf = [0.5 * (kh0 + kh[slp, slp]), 0.5 * (kh0 + kh[sl, slp]), 0.5 * (kh0 + kh[slm, sl]),
+          0.5 * (kh0 + kh[slm, slm]), 0.5 * (kh0 + kh[sl, slm]), 0.5 * (kh0 + kh[slp, sl])]
+    II, IIm = slice(gmin, gmax + 1), slice(gmin - 1, gmax)
+    a_ti, a_tj = tTI[II, II], tTJ[II, II]
+    b_ti = tTI[IIm, II]
+    c_tj, c_ti = tTJ[IIm, IIm], tTI[IIm, IIm]
+    d_tj = tTJ[II, IIm]
+    inner = None
+    for d in range(3):
+        cd = g.OPRT_coef_diff[II, II, :, :, d, :]
+        blk = (kf[0] * cd[..., 0] * (a_ti[..., d] + a_tj[..., d])
+               + kf[1] * cd[..., 1] * (a_tj[..., d] + b_ti[..., d])
+               + kf[2] * cd[..., 2] * (b_ti[..., d] + c_tj[..., d])
+               + kf[3] * cd[..., 3] * (c_tj[..., d] + c_ti[..., d])
+               + kf[4] * cd[..., 4] * (c_ti[..., d] + d_tj[..., d])
+               + kf[5] * cd[..., 5] * (d_tj[..., d] + a_ti[..., d]))
+        inner = blk if inner is None else inner + blk
+    return _pad2(inner, i, j, lo=gmin)
+
+
+def diffusion_pl(g, s_pl, kh_pl):
+    """kernels/oprtdiffusion.py:137-177."""
+    sv = s_pl[1:6]
+    svp1 = np.roll(sv, -1, axis=0)
+    cI = g.OPRT_coef_intp_pl[1:6, 0]                     # (5, l, 3, 3)
+    c0 = cI[..., 0][:, None]
+    c1 = cI[..., 1][:, None]
+    c2 = cI[..., 2][:, None]
+    vt = ((2.0 * c0 - c1 - c2) * s_pl[0][None, :, :, None] + (-c0 + 2.0 * c1 - c2) * sv[..., None]
+          + (-c0 - c1 + 2.0 * c2) * svp1[..., None]) / 3.0
+    vsum = np.roll(vt, 1, axis=0) + vt
+    kh_avg = 0.5 * (kh_pl[0][None] + kh_pl[1:6])
+    cd = g.OPRT_coef_diff_pl[1:6, 0][:, None]
+    contrib = kh_avg * (cd * vsum).sum(axis=-1)
+    out = np.zeros_like(s_pl)
+    out[0] = contrib.sum(axis=0)
+    return out
+
+
+def horizontalize(g, vx, vy, vz):
+    """kernels/horizontalizevec.py:34-55; interior only, border kept (in place)."""
+    i, j = vx.shape[:2]
+    gv = g.GRD_x[1:i - 1, 1:j - 1, 0]
+    gx, gy, gz = (gv[..., d][:, :, None, :] for d in (XDIR, YDIR, ZDIR))
+    r = g.rscale
+    sx, sy, sz = vx[1:i - 1, 1:j - 1], vy[1:i - 1, 1:j - 1], vz[1:i - 1, 1:j - 1]
+    prd = (sx * gx + sy * gy + sz * gz) / r
+    nx = sx - prd * gx / r
+    ny = sy - prd * gy / r
+    nz = sz - prd * gz / r
+    vx[1:i - 1, 1:j - 1] = nx
+    vy[1:i - 1, 1:j - 1] = ny
+    vz[1:i - 1, 1:j - 1] = nz
+
+
+def horizontalize_pl(g, vx, vy, vz):
+    """kernels/horizontalizevec.py:58-71 (in place)."""
+    gx, gy, gz = (g.GRD_x_pl[:, 0, :, d][:, None, :] for d in (XDIR, YDIR, ZDIR))
+    r = g.rscale
+    prd = vx * gx / r + vy * gy / r + vz * gz / r
+    nx = vx - prd * gx / r
+    ny = vy - prd * gy / r
+    nz = vz - prd * gz / r
+    vx[...] = nx
+    vy[...] = ny
+    vz[...] = nz
+
+
+def _sclt(g, c, vx, vy, vz, R, Rp1):
+    """sclt_TI / sclt_TJ of kernels/oprtdivdamp.py:73-94."""
+    ti = (c[..., XDIR, 0, TI] * vx[R, R] + c[..., XDIR, 1, TI] * vx[Rp1, R] + c[..., XDIR, 2, TI] * vx[Rp1, Rp1]
+          + c[..., YDIR, 0, TI] * vy[R, R] + c[..., YDIR, 1, TI] * vy[Rp1, R] + c[..., YDIR, 2, TI] * vy[Rp1, Rp1]
+          + c[..., ZDIR, 0, TI] * vz[R, R] + c[..., ZDIR, 1, TI] * vz[Rp1, R] + c[..., ZDIR, 2, TI] * vz[Rp1, Rp1])
+    tj = (c[..., XDIR, 0, TJ] * vx[R, R] + c[..., XDIR, 1, TJ] * vx[Rp1, Rp1] + c[..., XDIR, 2, TJ] * vx[R, Rp1]
+          + c[..., YDIR, 0, TJ] * vy[R, R] + c[..., YDIR, 1, TJ] * vy[Rp1, Rp1] + c[..., YDIR, 2, TJ] * vy[R, Rp1]
+          + c[..., ZDIR, 0, TJ] * vz[R, R] + c[..., ZDIR, 1, TJ] * vz[Rp1, Rp1] + c[..., ZDIR, 2, TJ] * vz[R, Rp1])
+    return ti, tj
+
+
+def _ddivd(g, sTI, sTJ, d):
+    G = g.gmax + 1
+    II, IIm = slice(1, G), slice(0, G - 1)
+    a_ti, a_tj = sTI[II, II], sTJ[II, II]
+    b_ti = sTI[IIm, II]
+    c_tj, c_ti = sTJ[IIm, IIm], sTI[IIm, IIm]
+    d_tj = sTJ[II, IIm]
+    cd = g.OPRT_coef_diff[II, II, :, :, d, :]
+    return (cd[..., 0] * (a_ti + a_tj) + cd[..., 1] * (a_tj + b_ti) + cd[..., 2] * (b_ti + c_tj)
+            + cd[..., 3] * (c_tj + c_ti) + cd[..., 4] * (c_ti + d_tj) + cd[..., 5] * (d_tj + a_ti))
+
+
+def divdamp(g, vx, vy, vz):
+    """kernels/oprtdivdamp.py:54-122 -> (dx, dy, dz)."""
+    i, j = vx.shape[:2]
+    G = g.gmax + 1
+    R, Rp1 = slice(0, G), slice(1, G + 1)
+    c = g.OPRT_coef_intp[R, R]
+    sTI, sTJ = _sclt(g, c, vx, vy, vz, R, Rp1)
+    return [_pad2(_ddivd(g, sTI, sTJ, d), i, j) for d in (XDIR, YDIR, ZDIR)]
+
+
+def divdamp_pl(g, vx, vy, vz):
+    """kernels/oprtdivdamp.py:125-173."""
+    sx, sy, sz = vx[0], vy[0], vz[0]
+    ijx, ijy, ijz = vx[1:6], vy[1:6], vz[1:6]
+    px, py, pz = np.roll(ijx, -1, 0), np.roll(ijy, -1, 0), np.roll(ijz, -1, 0)
+    cI = g.OPRT_coef_intp_pl[1:6, 0]
+    b = lambda a: a[:, None, :]
+    sclt = (b(cI[:, :, XDIR, 0]) * sx + b(cI[:, :, XDIR, 1]) * ijx + b(cI[:, :, XDIR, 2]) * px
+            + b(cI[:, :, YDIR, 0]) * sy + b(cI[:, :, YDIR, 1]) * ijy + b(cI[:, :, YDIR, 2]) * py
+            + b(cI[:, :, ZDIR, 0]) * sz + b(cI[:, :, ZDIR, 1]) * ijz + b(cI[:, :, ZDIR, 2]) * pz)
+    pair = np.roll(sclt, 1, 0) + sclt
+    cd = g.OPRT_coef_diff_pl[1:6, 0]
+    outs = []
+    for d in (XDIR, YDIR, ZDIR):
+        o = np.zeros_like(vx)
+        o[0] = (b(cd[:, :, d]) * pair).sum(axis=0)
+        outs.append(o)
+    return outs
+
+
+def _rhogw_vm(g, vx, vy, vz, w, pole=False):
+    """kernels/oprt3ddivdamp.py:50-82 (== fluxconv rhogw_vmh with vflag 1)."""
+    sfx = "_pl" if pole else ""
+    kmin, kmax = g.kmin, g.kmax
+    cz = getattr(g, "VMTR_C2WfactGz" + sfx)
+    RGAMH = getattr(g, "VMTR_RGAMH" + sfx)
+    RGSQRTH = getattr(g, "VMTR_RGSQRTH" + sfx)
+    ks, km = slice(kmin + 1, kmax + 1), slice(kmin, kmax)
+    K = (lambda a, s: a[:, :, s]) if not pole else (lambda a, s: a[:, s])
+    horiz = (K(cz, ks)[..., 0] * K(vx, ks) + K(cz, ks)[..., 1] * K(vx, km)
+             + K(cz, ks)[..., 2] * K(vy, ks) + K(cz, ks)[..., 3] * K(vy, km)
+             + K(cz, ks)[..., 4] * K(vz, ks) + K(cz, ks)[..., 5] * K(vz, km))
+    out = np.zeros_like(w)
+    if pole:
+        out[:, ks] = horiz * RGAMH[:, ks] + w[:, ks] * RGSQRTH[:, ks]
+    else:
+        out[:, :, ks] = horiz * RGAMH[:, :, ks] + w[:, :, ks] * RGSQRTH[:, :, ks]
+    return out
+
+
+def divdamp3d(g, rvx, rvy, rvz, rw):
+    """kernels/oprt3ddivdamp.py:85-173."""
+    i, j, kall = rvx.shape[:3]
+    kmin, kmax = g.kmin, g.kmax
+    G = g.gmax + 1
+    rwv = _rhogw_vm(g, rvx, rvy, rvz, rw)
+    K = slice(kmin, kmax + 1)
+    RG = g.VMTR_RGAM[:, :, K]
+    vmx, vmy, vmz = rvx[:, :, K] * RG, rvy[:, :, K] * RG, rvz[:, :, K] * RG
+    R, Rp1 = slice(0, G), slice(1, G + 1)
+    UP, DN = slice(kmin + 1, kmax + 2), slice(kmin, kmax + 1)
+    rdz = g.GRD_rdgz[K][None, None, :, None]
+    wTI = ((rwv[R, R, UP] + rwv[Rp1, R, UP] + rwv[Rp1, Rp1, UP])
+           - (rwv[R, R, DN] + rwv[Rp1, R, DN] + rwv[Rp1, Rp1, DN])) / 3.0 * rdz
+    wTJ = ((rwv[R, R, UP] + rwv[Rp1, Rp1, UP] + rwv[R, Rp1, UP])
+           - (rwv[R, R, DN] + rwv[Rp1, Rp1, DN] + rwv[R, Rp1, DN])) / 3.0 * rdz
+    c = g.OPRT_coef_intp[R, R]
+    sTI, sTJ = _sclt(g, c, vmx, vmy, vmz, R, Rp1)
+    sTI = sTI + wTI
+    sTJ = sTJ + wTJ
+    sTI = _sgp_corner(g, sTI, sTJ)
+    outs = []
+    for d in (XDIR, YDIR, ZDIR):
+        o = np.zeros(rvx.shape)
+        o[1:G, 1:G, K] = _ddivd(g, sTI, sTJ, d)
+        outs.append(o)
+    return outs
+
+
+def divdamp3d_pl(g, rvx, rvy, rvz, rw):
+    """kernels/oprt3ddivdamp.py:176-237."""
+    kmin, kmax = g.kmin, g.kmax
+    rwv = _rhogw_vm(g, rvx, rvy, rvz, rw, pole=True)
+    K = slice(kmin, kmax + 1)
+    RG = g.VMTR_RGAM_pl[:, K]
+    vmx, vmy, vmz = rvx[:, K] * RG, rvy[:, K] * RG, rvz[:, K] * RG
+    sx, sy, sz = vmx[0], vmy[0], vmz[0]
+    ijx, ijy, ijz = vmx[1:6], vmy[1:6], vmz[1:6]
+    px, py, pz = np.roll(ijx, -1, 0), np.roll(ijy, -1, 0), np.roll(ijz, -1, 0)
+    UP, DN = slice(kmin + 1, kmax + 2), slice(kmin, kmax + 1)
+    r_n_up, r_n_dn = rwv[0, UP], rwv[0, DN]
+    r_ij_up, r_ij_dn = rwv[1:6, UP], rwv[1:6, DN]
+    sclt_w = ((r_n_up + r_ij_up + np.roll(r_ij_up, -1, 0))
+              - (r_n_dn + r_ij_dn + np.roll(r_ij_dn, -1, 0))) / 3.0 * g.GRD_rdgz[K][None, :, None]
+    cI = g.OPRT_coef_intp_pl[1:6, 0]
+    b = lambda a: a[:, None, :]
+    sclt = (b(cI[:, :, XDIR, 0]) * sx + b(cI[:, :, XDIR, 1]) * ijx + b(cI[:, :, XDIR, 2]) * px
+            + b(cI[:, :, YDIR, 0]) * sy + b(cI[:, :, YDIR, 1]) * ijy + b(cI[:, :, YDIR, 2]) * py
+            + b(cI[:, :, ZDIR, 0]) * sz + b(cI[:, :, ZDIR, 1]) * ijz + b(cI[:, :, ZDIR, 2]) * pz
+            + sclt_w)
+    pair = np.roll(sclt, 1, 0) + sclt
+    cd = g.OPRT_coef_diff_pl[1:6, 0]
+    outs = []
+    for d in (XDIR, YDIR, ZDIR):
+        o = np.zeros_like(rvx)
+        o[0, K] = (b(cd[:, :, d]) * pair).sum(axis=0)
+        outs.append(o)
+    return outs
+
+
+# --------------------------------------------------------------------------
+# source terms (kernels/advconv.py, fluxconv.py, presgrad.py, buoyancy.py)
+# --------------------------------------------------------------------------
+def flux_convergence(g, rvx, rvy, rvz, rw, vertical=True, pole=False):
+    """kernels/fluxconv.py:111-208 (fluxtype default / horizontal)."""
+    sfx = "_pl" if pole else ""
+    kmin, kmax = g.kmin, g.kmax
+    RGAM = getattr(g, "VMTR_RGAM" + sfx)
+    RGAMH = getattr(g, "VMTR_RGAMH" + sfx)
+    RGSQRTH = getattr(g, "VMTR_RGSQRTH" + sfx)
+    cz_all = getattr(g, "VMTR_C2WfactGz" + sfx)
+    vflag = 1.0 if vertical else 0.0
+    ks, km = slice(kmin + 1, kmax + 1), slice(kmin, kmax)
+    K = (lambda a, s: a[:, :, s]) if not pole else (lambda a, s: a[:, s])
+    vxm, vym, vzm = rvx * RGAM, rvy * RGAM, rvz * RGAM
+    cz = K(cz_all, ks)
+    horiz = (cz[..., 0] * K(rvx, ks) + cz[..., 1] * K(rvx, km) + cz[..., 2] * K(rvy, ks)
+             + cz[..., 3] * K(rvy, km) + cz[..., 4] * K(rvz, ks) + cz[..., 5] * K(rvz, km))
+    horiz = horiz * K(RGAMH, ks)
+    vert = vflag * K(rw, ks) * K(RGSQRTH, ks)
+    vmh = np.zeros_like(rw)
+    if pole:
+        vmh[:, ks] = horiz + vert
+        div = divergence_pl(g, vxm, vym, vzm)
+    else:
+        vmh[:, :, ks] = horiz + vert
+        div = divergence(g, vxm, vym, vzm)
+    kc, kcp = slice(kmin, kmax + 1), slice(kmin + 1, kmax + 2)
+    out = np.zeros_like(rw)
+    if pole:
+        rdz = g.GRD_rdgz[kc][None, :, None]
+        out[:, kc] = -div[:, kc] - (vmh[:, kcp] - vmh[:, kc]) * rdz
+    else:
+        rdz = g.GRD_rdgz[kc][None, None, :, None]
+        out[:, :, kc] = -div[:, :, kc] - (vmh[:, :, kcp] - vmh[:, :, kc]) * rdz
+    return out
+
+
+def scaled_fluxes(g, rvx, rvy, rvz, rw, scl, vertical=True, pole=False):
+    """kernels/advconv.py:42-108."""
+    kmin, kmax = g.kmin, g.kmax
+    sx, sy, sz = rvx * scl, rvy * scl, rvz * scl
+    sw = np.zeros_like(rw)
+    if vertical:
+        af = g.GRD_afact[kmin:kmax + 2]
+        bf = g.GRD_bfact[kmin:kmax + 2]
+        if pole:
+            sw[:, kmin:kmax + 2] = rw[:, kmin:kmax + 2] * (af[None, :, None] * scl[:, kmin:kmax + 2]
+                                                           + bf[None, :, None] * scl[:, kmin - 1:kmax + 1])
+        else:
+            sw[:, :, kmin:kmax + 2] = rw[:, :, kmin:kmax + 2] * (
+                af[None, None, :, None] * scl[:, :, kmin:kmax + 2]
+                + bf[None, None, :, None] * scl[:, :, kmin - 1:kmax + 1])
+    return sx, sy, sz, sw
+
+
+def advection_convergence(g, rvx, rvy, rvz, rw, scl, vertical=True, pole=False):
+    """mod_src.py:499-623 = scaled fluxes then flux convergence."""
+    sx, sy, sz, sw = scaled_fluxes(g, rvx, rvy, rvz, rw, scl, vertical, pole)
+    return flux_convergence(g, sx, sy, sz, sw, vertical, pole)
+
+
+def pres_gradient(g, P, P_pl, vertical=True):
+    """kernels/presgrad.py:126-265 with first_layer_remedy and horizontalize."""
+    kmin, kmax = g.kmin, g.kmax
+    i, j, kall, l = P.shape
+    out = []
+    for pole in (False, True):
+        sfx = "_pl" if pole else ""
+        PP = P_pl if pole else P
+        RGAM = getattr(g, "VMTR_RGAM" + sfx)
+        RGAMH = getattr(g, "VMTR_RGAMH" + sfx)
+        czall = getattr(g, "VMTR_C2WfactGz" + sfx)
+        if pole:
+            Pvm = PP * RGAM * 1.0      # * plmask (== 1 here)
+            gh = gradient_pl(g, Pvm)
+            K = lambda a, s: a[:, s]
+        else:
+            Pvm = PP * RGAM
+            gh = gradient(g, Pvm)
+            K = lambda a, s: a[:, :, s]
+        cz = K(czall, slice(kmin, kmax + 2))
+        rgh = K(RGAMH, slice(kmin, kmax + 2))
+        Pk = K(PP, slice(kmin, kmax + 2))
+        Pkm1 = K(PP, slice(kmin - 1, kmax + 1))
+        pvmh = np.stack([(cz[..., 0] * Pk + cz[..., 1] * Pkm1) * rgh,
+                         (cz[..., 2] * Pk + cz[..., 3] * Pkm1) * rgh,
+                         (cz[..., 4] * Pk + cz[..., 5] * Pkm1) * rgh], axis=-1)
+        if pole:
+            rdz = g.GRD_rdgz[kmin:kmax + 1][None, :, None, None]
+            vterm = (pvmh[:, 1:] - pvmh[:, :-1]) * rdz
+            gf = gh[:, kmin:kmax + 1] + vterm
+            Pg = gh.copy()
+            Pg[:, kmin - 1] = 0.0
+            Pg[:, kmin] = gf[:, 1]
+            Pg[:, kmin + 1:kmax + 1] = gf[:, 1:]
+            Pg[:, kmax + 1] = 0.0
+            horizontalize_pl(g, Pg[..., 0], Pg[..., 1], Pg[..., 2])
+        else:
+            rdz = g.GRD_rdgz[kmin:kmax + 1][None, None, :, None, None]
+            vterm = (pvmh[:, :, 1:] - pvmh[:, :, :-1]) * rdz
+            gf = gh[:, :, kmin:kmax + 1] + vterm
+            Pg = gh.copy()
+            Pg[:, :, kmin - 1] = 0.0
+            Pg[:, :, kmin] = gf[:, :, 1]
+            Pg[:, :, kmin + 1:kmax + 1] = gf[:, :, 1:]
+            Pg[:, :, kmax + 1] = 0.0
+            Pgx, Pgy, Pgz = Pg[..., 0].copy(), Pg[..., 1].copy(), Pg[..., 2].copy()
+            horizontalize(g, Pgx, Pgy, Pgz)
+            Pg = np.stack([Pgx, Pgy, Pgz], axis=-1)
+        Pgw = np.zeros_like(PP)
+        if vertical:
+            GAM2H = getattr(g, "VMTR_GAM2H" + sfx)
+            RGSGAM2 = getattr(g, "VMTR_RGSGAM2" + sfx)
+            ks, km = slice(kmin + 1, kmax + 1), slice(kmin, kmax)
+            if pole:
+                rdh = g.GRD_rdgzh[ks][None, :, None]
+                Pgw[:, ks] = GAM2H[:, ks] * (PP[:, ks] * RGSGAM2[:, ks] - PP[:, km] * RGSGAM2[:, km]) * rdh
+            else:
+                rdh = g.GRD_rdgzh[ks][None, None, :, None]
+                Pgw[:, :, ks] = GAM2H[:, :, ks] * (PP[:, :, ks] * RGSGAM2[:, :, ks]
+                                                   - PP[:, :, km] * RGSGAM2[:, :, km]) * rdh
+        out += [Pg, Pgw]
+    return out            # Pgrad, Pgradw, Pgrad_pl, Pgradw_pl
+
+
+def buoyancy(g, rhog, pole=False):
+    """kernels/buoyancy.py:40-81."""
+    sfx = "_pl" if pole else ""
+    C2W = getattr(g, "VMTR_C2Wfact" + sfx)
+    kmin, kmax = g.kmin, g.kmax
+    out = np.zeros_like(rhog)
+    ks, km = slice(kmin + 1, kmax + 1), slice(kmin, kmax)
+    if pole:
+        out[:, ks] = -g.GRAV * (C2W[:, ks, :, 0] * rhog[:, ks] + C2W[:, ks, :, 1] * rhog[:, km])
+    else:
+        out[:, :, ks] = -g.GRAV * (C2W[:, :, ks, :, 0] * rhog[:, :, ks] + C2W[:, :, ks, :, 1] * rhog[:, :, km])
+    return out
+
+
+def advection_momentum(g, DIAG, PROG, DIAG_pl, PROG_pl):
+    """mod_src.py:96-497 with kernels/advconvmom.py (sphere).  Returns
+    (gvx, gvy, gvz, gw) regional and pole."""
+    kmin, kmax = g.kmin, g.kmax
+    res = []
+    for pole in (False, True):
+        D = DIAG_pl if pole else DIAG
+        P = PROG_pl if pole else PROG
+        gx = (g.GRD_x_pl[:, 0] if pole else g.GRD_x[:, :, 0])
+        gxs = [gx[..., d] for d in (XDIR, YDIR, ZDIR)]
+        kc, kp = slice(kmin, kmax + 1), slice(kmin + 1, kmax + 2)
+        cf, df = g.GRD_cfact[kc], g.GRD_dfact[kc]
+        w = D[..., I_w]
+        if pole:
+            wc = cf[None, :, None] * w[:, kp] + df[None, :, None] * w[:, kc]
+            gb = [a[:, None, :] for a in gxs]
+        else:
+            wc = cf[None, None, :, None] * w[:, :, kp] + df[None, None, :, None] * w[:, :, kc]
+            gb = [a[:, :, None, :] for a in gxs]
+        vv = []
+        for idg, gd in zip((I_vx, I_vy, I_vz), gb):
+            a = np.zeros_like(w)
+            if pole:
+                a[:, kc] = D[:, kc, :, idg] + (wc * gd / g.rscale)
+            else:
+                a[:, :, kc] = D[:, :, kc, :, idg] + wc * gd / g.rscale
+            vv.append(a)
+        rvx, rvy, rvz, rw = P[..., I_RHOGVX], P[..., I_RHOGVY], P[..., I_RHOGVZ], P[..., I_RHOGW]
+        dv = [advection_convergence(g, rvx, rvy, rvz, rw, s, True, pole) for s in vv]
+        Kc = (lambda a: a[:, kc]) if pole else (lambda a: a[:, :, kc])
+        rh = Kc(P[..., I_RHOG])
+        dvx = Kc(dv[0]) - (-2.0 * rh * (g.OHM * Kc(vv[1])))
+        dvy = Kc(dv[1]) - (2.0 * rh * (g.OHM * Kc(vv[0])))
+        dvz = Kc(dv[2])
+        gg = [a / g.rscale for a in gb]
+        prd = dvx * gg[0] + dvy * gg[1] + dvz * gg[2]
+        outs = [np.zeros_like(w) for _ in range(4)]
+        gwc = prd * g.alpha
+        C2W = g.VMTR_C2Wfact_pl if pole else g.VMTR_C2Wfact
+        ks = slice(kmin + 1, kmax + 1)
+        if pole:
+            outs[0][:, kc] = dvx - prd * gg[0]
+            outs[1][:, kc] = dvy - prd * gg[1]
+            outs[2][:, kc] = dvz - prd * gg[2]
+            outs[3][:, ks] = C2W[:, ks, :, 0] * gwc[:, 1:] + C2W[:, ks, :, 1] * gwc[:, :-1]
+        else:
+            outs[0][:, :, kc] = dvx - prd * gg[0]
+            outs[1][:, :, kc] = dvy - prd * gg[1]
+            outs[2][:, :, kc] = dvz - prd * gg[2]
+            outs[3][:, :, ks] = C2W[:, :, ks, :, 0] * gwc[:, :, 1:] + C2W[:, :, ks, :, 1] * gwc[:, :, :-1]
+        res.append(outs)
+    return res
+
+
+# --------------------------------------------------------------------------
+# numerical filters (mod_numfilter.py)
+# --------------------------------------------------------------------------
+def hdiffusion(g, rhog, rho, DIAG, rhog_pl, rho_pl, DIAG_pl):
+    """mod_numfilter.py:845-1469 (DIRECT, lap_order 2, tracer part off) with
+    _hdiff_tendency_host :1519-1578 and the final horizontalize.  Returns
+    f_TEND (i,j,k,l,6) and f_TEND_pl."""
+    kmin, kmax = g.kmin, g.kmax
+    Kh = g.Kh_coef
+    rhog_h = np.zeros_like(rhog)
+    rhog_h[:, :, kmin:kmax + 2] = (g.VMTR_C2Wfact[:, :, kmin:kmax + 2, :, 0] * rhog[:, :, kmin:kmax + 2]
+                                   + g.VMTR_C2Wfact[:, :, kmin:kmax + 2, :, 1] * rhog[:, :, kmin - 1:kmax + 1])
+    rhog_h[:, :, kmin - 1] = 0.0
+    rhog_h_pl = np.zeros_like(rhog_pl)
+    rhog_h_pl[:, kmin:kmax + 2] = (g.VMTR_C2Wfact_pl[:, kmin:kmax + 2, :, 0] * rhog_pl[:, kmin:kmax + 2]
+                                   + g.VMTR_C2Wfact_pl[:, kmin:kmax + 2, :, 1] * rhog_pl[:, kmin - 1:kmax + 1])
+    rhog_h_pl[:, kmin - 1] = 0.0
+    vt = np.stack([DIAG[..., I_vx], DIAG[..., I_vy], DIAG[..., I_vz], DIAG[..., I_w],
+                   DIAG[..., I_tem] - g.tem_bs, rho - g.rho_bs], axis=-1)
+    vtp = np.stack([DIAG_pl[..., I_vx], DIAG_pl[..., I_vy], DIAG_pl[..., I_vz], DIAG_pl[..., I_w],
+                    DIAG_pl[..., I_tem] - g.tem_bs_pl, rho_pl - g.rho_bs_pl], axis=-1)
+    KhA = np.full(rhog.shape, Kh)
+    KhA_pl = np.full(rhog_pl.shape, Kh)
+    for p in range(2):
+        v2 = np.zeros_like(vt)
+        v2p = np.zeros_like(vtp)
+        for n in range(4):
+            v2[..., n] = laplacian(g, vt[..., n])
+            v2p[..., n] = laplacian_pl(g, vtp[..., n])
+        if p == 1:
+            wk = rhog * g.CVdry * KhA
+            wkp = rhog_pl * g.CVdry * KhA_pl
+            v2[..., 4] = diffusion(g, vt[..., 4], wk)
+            v2p[..., 4] = diffusion_pl(g, vtp[..., 4], wkp)
+            wk = rhog * g.hdiff_fact_rho * KhA
+            wkp = rhog_pl * g.hdiff_fact_rho * KhA_pl
+            v2[..., 5] = diffusion(g, vt[..., 5], wk)
+            v2p[..., 5] = diffusion_pl(g, vtp[..., 5], wkp)
+        else:
+            v2[..., 4] = laplacian(g, vt[..., 4])
+            v2p[..., 4] = laplacian_pl(g, vtp[..., 4])
+            v2[..., 5] = laplacian(g, vt[..., 5])
+            v2p[..., 5] = laplacian_pl(g, vtp[..., 5])
+        vt = -v2
+        vtp = -v2p
+        comm(g, vt, vtp)
+    f = np.zeros(rhog.shape + (6,))
+    fp = np.zeros(rhog_pl.shape + (6,))
+    zero = 0.0 * 0.0
+    for (F, V, RG, RGH, KA) in ((f, vt, rhog, rhog_h, KhA), (fp, vtp, rhog_pl, rhog_h_pl, KhA_pl)):
+        F[..., I_RHOGVX] = -(V[..., 0] * KA + zero) * RG
+        F[..., I_RHOGVY] = -(V[..., 1] * KA + zero) * RG
+        F[..., I_RHOGVZ] = -(V[..., 2] * KA + zero) * RG
+        F[..., I_RHOGW] = -(V[..., 3] * KA + zero) * RGH
+        F[..., I_RHOGE] = -(V[..., 4] + zero)
+        F[..., I_RHOG] = -(V[..., 5] + zero)
+    a, b, c = f[..., I_RHOGVX].copy(), f[..., I_RHOGVY].copy(), f[..., I_RHOGVZ].copy()
+    horizontalize(g, a, b, c)
+    f[..., I_RHOGVX], f[..., I_RHOGVY], f[..., I_RHOGVZ] = a, b, c
+    a, b, c = fp[..., I_RHOGVX].copy(), fp[..., I_RHOGVY].copy(), fp[..., I_RHOGVZ].copy()
+    horizontalize_pl(g, a, b, c)
+    fp[..., I_RHOGVX], fp[..., I_RHOGVY], fp[..., I_RHOGVZ] = a, b, c
+    return f, fp
+
+
+def numfilter_divdamp(g, rvx, rvy, rvz, rw, rvx_pl, rvy_pl, rvz_pl, rw_pl):
+    """mod_numfilter.py:2032-2268 (lap_order 2: 3-D divdamp, COMM, post-COMM
+    island kernels/divdamppostcomm.py:29-81).  Returns gd(x,y,z) and pole."""
+    d = divdamp3d(g, rvx, rvy, rvz, rw)
+    dp = divdamp3d_pl(g, rvx_pl, rvy_pl, rvz_pl, rw_pl)
+    v2 = np.stack(d, axis=-1)
+    v2p = np.stack(dp, axis=-1)
+    comm(g, v2, v2p)
+    o = divdamp(g, -v2[..., 0], -v2[..., 1], -v2[..., 2])
+    op = divdamp_pl(g, -v2p[..., 0], -v2p[..., 1], -v2p[..., 2])
+    gd = [g.divdamp_coef * a for a in o]
+    gdp = [g.divdamp_coef * a for a in op]
+    horizontalize(g, gd[0], gd[1], gd[2])
+    horizontalize_pl(g, gdp[0], gdp[1], gdp[2])
+    return gd, gdp
+
+
+# --------------------------------------------------------------------------
+# HEVI vertical implicit (mod_vi.py, kernels/vimatrix.py, virhowsolver.py,
+# rhogkin.py, vimain.py, vipath1.py)
+# --------------------------------------------------------------------------
+def rhow_matrix(g, eth_h, gz, dt, pole=False):
+    """kernels/vimatrix.py:67-164 (pre-combined coefficients)."""
+    sfx = "_pl" if pole else ""
+    kmin, kmax = g.kmin, g.kmax
+    ks, ksp, ksm = slice(kmin + 1, kmax + 1), slice(kmin + 2, kmax + 2), slice(kmin, kmax)
+    RGSGAM2 = getattr(g, "VMTR_RGSGAM2" + sfx)
+    GAM2H = getattr(g, "VMTR_GAM2H" + sfx)
+    RGAMH = getattr(g, "VMTR_RGAMH" + sfx)
+    RGSQRTH = getattr(g, "VMTR_RGSQRTH" + sfx)
+    GCVovR = g.GRAV * g.CVdry / g.Rdry
+    ACVovRt2 = g.alpha * g.CVdry / g.Rdry / (dt * dt)
+    if pole:
+        K = lambda a, s: a[:, s]
+        b1 = lambda v: v[None, :, None]
+    else:
+        K = lambda a, s: a[:, :, s]
+        b1 = lambda v: v[None, None, :, None]
+    rg, rgm = b1(g.GRD_rdgz[ks]), b1(g.GRD_rdgz[ksm])
+    Ca = (K(RGSGAM2, ks) * rg + K(RGSGAM2, ksm) * rgm) * K(GAM2H, ks)
+    Cb = b1(g.GRD_dfact[ks] - g.GRD_cfact[ksm])
+    Cu1 = K(RGSGAM2, ks) * rg * K(GAM2H, ksp)
+    Cu2 = K(GAM2H, ksp) * K(RGAMH, ks) ** 2 * GCVovR
+    Cl1 = K(RGSGAM2, ks) * rg * K(GAM2H, ksm)
+    Cl2 = K(GAM2H, ksm) * K(RGAMH, ks) ** 2 * GCVovR
+    rgh = b1(g.GRD_rdgzh[ks])
+    cf = b1(g.GRD_cfact[ks])
+    dfm = b1(g.GRD_dfact[ksm])
+    Mc = ACVovRt2 / K(RGSQRTH, ks) + rgh * (Ca * K(eth_h, ks) - Cb * (K(gz, ks) + GCVovR))
+    Mu = -rgh * (Cu1 * K(eth_h, ksp) + cf * (K(gz, ksp) + Cu2))
+    Ml = -rgh * (Cl1 * K(eth_h, ksm) - dfm * (K(gz, ksm) + Cl2))
+    return Mc, Mu, Ml            # interior k = kmin+1..kmax
+
+
+def rhow_solver(g, rhogw, rhogw0, preg0, rhog0, Srho, Sw, Spre, Mc, Mu, Ml, dt, pole=False):
+    """kernels/virhowsolver.py:42-172 (Thomas solve on k = kmin+1..kmax)."""
+    sfx = "_pl" if pole else ""
+    kmin, kmax = g.kmin, g.kmax
+    ks, ksm = slice(kmin + 1, kmax + 1), slice(kmin, kmax)
+    RGAMH = getattr(g, "VMTR_RGAMH" + sfx)
+    RGSGAM2 = getattr(g, "VMTR_RGSGAM2" + sfx)
+    RGAM = getattr(g, "VMTR_RGAM" + sfx)
+    RGSGAM2H = getattr(g, "VMTR_RGSGAM2H" + sfx)
+    GSGAM2H = getattr(g, "VMTR_GSGAM2H" + sfx)
+    CVovRt2 = g.CVdry / g.Rdry / (dt * dt)
+    if pole:
+        K = lambda a, s: a[:, s]
+        b1 = lambda v: v[None, :, None]
+    else:
+        K = lambda a, s: a[:, :, s]
+        b1 = lambda v: v[None, None, :, None]
+    rgh, af, bf = b1(g.GRD_rdgzh[ks]), b1(g.GRD_afact[ks]), b1(g.GRD_bfact[ks])
+    Sall = ((K(rhogw0, ks) * g.alpha + dt * K(Sw, ks)) * K(RGAMH, ks) ** 2
+            - ((K(preg0, ks) + dt * K(Spre, ks)) * K(RGSGAM2, ks)
+               - (K(preg0, ksm) + dt * K(Spre, ksm)) * K(RGSGAM2, ksm)) * dt * rgh
+            - ((K(rhog0, ks) + dt * K(Srho, ks)) * K(RGAM, ks) ** 2 * af
+               + (K(rhog0, ksm) + dt * K(Srho, ksm)) * K(RGAM, ksm) ** 2 * bf) * dt * g.GRAV
+            ) * CVovRt2
+    rw_kmin = _kidx(rhogw, kmin) * _kidx(RGSGAM2H, kmin)
+    rw_kmaxp1 = _kidx(rhogw, kmax + 1) * _kidx(RGSGAM2H, kmax + 1)
+    N = kmax - kmin
+    S = [_kidx(Sall, n) for n in range(N)]
+    C = [_kidx(Mc, n) for n in range(N)]
+    U = [_kidx(Mu, n) for n in range(N)]
+    L = [_kidx(Ml, n) for n in range(N)]
+    S[0] = S[0] - L[0] * rw_kmin
+    S[N - 1] = S[N - 1] - U[N - 1] * rw_kmaxp1
+    beta = C[0]
+    u = [S[0] / beta]
+    gam = [None] * N
+    for n in range(1, N):
+        gg = U[n - 1] / beta
+        beta = C[n] - L[n] * gg
+        u.append((S[n] - L[n] * u[n - 1]) / beta)
+        gam[n] = gg
+    x = [None] * N
+    x[N - 1] = u[N - 1]
+    for n in range(N - 2, -1, -1):
+        x[n] = u[n] - gam[n + 1] * x[n + 1]
+    out = rhogw.copy()
+    for n in range(N):
+        _kset(out, kmin + 1 + n, x[n] * _kidx(GSGAM2H, kmin + 1 + n))
+    _kset(out, kmin, rw_kmin * _kidx(GSGAM2H, kmin))
+    _kset(out, kmax + 1, rw_kmaxp1 * _kidx(GSGAM2H, kmax + 1))
+    return out
+
+
+def rhogkin(g, rhog, rvx, rvy, rvz, rw, pole=False):
+    """kernels/rhogkin.py:38-119."""
+    sfx = "_pl" if pole else ""
+    kmin, kmax = g.kmin, g.kmax
+    C2W = getattr(g, "VMTR_C2Wfact" + sfx)
+    W2C = getattr(g, "VMTR_W2Cfact" + sfx)
+    kc, kvi, kcm = slice(kmin, kmax + 1), slice(kmin + 1, kmax + 1), slice(kmin, kmax)
+    K = (lambda a, s: a[:, s]) if pole else (lambda a, s: a[:, :, s])
+    kh = 0.5 * (K(rvx, kc) ** 2 + K(rvy, kc) ** 2 + K(rvz, kc) ** 2) / K(rhog, kc)
+    denom = K(C2W, kvi)[..., 0] * K(rhog, kvi) + K(C2W, kvi)[..., 1] * K(rhog, kcm)
+    v_int = 0.5 * K(rw, kvi) ** 2 / denom
+    kax = 1 if pole else 2
+    z = np.zeros_like(np.take(v_int, [0], axis=kax))
+    vb = np.concatenate([z, v_int, z], axis=kax)
+    vup = np.take(vb, range(1, vb.shape[kax]), axis=kax)
+    vdn = np.take(vb, range(0, vb.shape[kax] - 1), axis=kax)
+    tot = kh + K(W2C, kc)[..., 0] * vup + K(W2C, kc)[..., 1] * vdn
+    out = np.zeros_like(rhog)
+    if pole:
+        out[:, kc] = tot
+    else:
+        out[:, :, kc] = tot
+    return out
+
+
+def vi_main(g, P, dt, pole):
+    """kernels/vimain.py:127-262 (TIME_split) for one of regional / pole.
+    ``P`` holds the arrays named as in the reference's P dict."""
+    sfx = "_pl" if pole else ""
+    PHI = getattr(g, "VMTR_PHI" + sfx)
+    C2WGz = getattr(g, "VMTR_C2WfactGz" + sfx)
+    kmin, kmax = g.kmin, g.kmax
+    drhog = flux_convergence(g, P["rhogvx_s1"], P["rhogvy_s1"], P["rhogvz_s1"], P["rhogw_s0"], False, pole)
+    drhoge = advection_convergence(g, P["rhogvx_s1"], P["rhogvy_s1"], P["rhogvz_s1"], P["rhogw_s0"],
+                                   P["eth0"], False, pole)
+    grhog1 = P["grhog"] + drhog
+    grhoge1 = P["grhoge"] + drhoge
+    gpre = grhoge1 * g.Rdry / g.CVdry
+    vx, vy, vz = P["rhogvx_s1"], P["rhogvy_s1"], P["rhogvz_s1"]
+    K = lambda a, k: _kidx(a, k)
+    cz = lambda c: K(C2WGz[..., c], kmax + 1)
+    rw_top = -(cz(0) * K(vx, kmax + 1) + cz(1) * K(vx, kmax) + cz(2) * K(vy, kmax + 1)
+               + cz(3) * K(vy, kmax) + cz(4) * K(vz, kmax + 1) + cz(5) * K(vz, kmax))
+    rhogw_s1 = np.zeros_like(vx)
+    _kset(rhogw_s1, kmin, np.zeros_like(K(vx, kmin)))
+    _kset(rhogw_s1, kmax + 1, rw_top)
+    Mc, Mu, Ml = P["Mc"], P["Mu"], P["Ml"]
+    rhogw_s1 = rhow_solver(g, rhogw_s1, P["rhogw_s0"], P["preg_s0"], P["rhog_s0"], grhog1, P["grhogw"],
+                           gpre, Mc, Mu, Ml, dt, pole)
+    drhog2 = flux_convergence(g, vx, vy, vz, rhogw_s1, True, pole)
+    rhog_s1 = P["rhog_s0"] + (P["grhog"] + drhog2) * dt
+    kin0 = rhogkin(g, P["rhog0"], P["rhogvx0"], P["rhogvy0"], P["rhogvz0"], P["rhogw0"], pole)
+    kin10 = rhogkin(g, P["rhog0"] + P["rhog_s0"], P["rhogvx0"] + P["rhogvx_s0"], P["rhogvy0"] + P["rhogvy_s0"],
+                    P["rhogvz0"] + P["rhogvz_s0"], P["rhogw0"] + P["rhogw_s0"], pole)
+    rhogvx1b = P["rhogvx0"] + vx
+    rhogvy1b = P["rhogvy0"] + vy
+    rhogvz1b = P["rhogvz0"] + vz
+    rhogw1b = P["rhogw0"] + rhogw_s1
+    kin11 = rhogkin(g, P["rhog0"] + rhog_s1, rhogvx1b, rhogvy1b, rhogvz1b, rhogw1b, pole)
+    ethtot0 = P["eth0"] + kin0 / P["rhog0"] + PHI
+    drhogetot = advection_convergence(g, rhogvx1b, rhogvy1b, rhogvz1b, rhogw1b, ethtot0, True, pole)
+    rhoge_s1 = (P["rhoge_s0"] + (P["grhogetot"] + drhogetot) * dt + (kin10 - kin11)
+                + (P["rhog_s0"] - rhog_s1) * PHI)
+    return rhog_s1, rhogw_s1, rhoge_s1
+
+
+def vi_small_step(g, PROG, PROG_pl, DIAG, DIAG_pl, eth, eth_pl, rhogd, rhogd_pl, pregd, pregd_pl,
+                  g_TEND0, g_TEND0_pl, PROG_split, PROG_split_pl, nitr, dt):
+    """mod_vi.py:104-1590 numpy path.  Updates PROG/PROG_pl in place and
+    returns PROG_mean, PROG_mean_pl (post-COMM)."""
+    kmin, kmax = g.kmin, g.kmax
+    RovCV = g.Rdry / g.CVdry
+    alpha = g.alpha
+    res = {}
+    for pole in (False, True):
+        sfx = "_pl" if pole else ""
+        P = PROG_pl if pole else PROG
+        eth_ = eth_pl if pole else eth
+        C2W = getattr(g, "VMTR_C2Wfact" + sfx)
+        K = (lambda a, s: a[:, s]) if pole else (lambda a, s: a[:, :, s])
+        ks_, ksm_ = slice(kmin, kmax + 2), slice(kmin - 1, kmax + 1)
+        rhog_h = np.zeros_like(P[..., 0])
+        eth_h = np.zeros_like(P[..., 0])
+        if pole:
+            rhog_h[:, ks_] = C2W[:, ks_, :, 0] * P[:, ks_, :, I_RHOG] + C2W[:, ks_, :, 1] * P[:, ksm_, :, I_RHOG]
+            eth_h[:, ks_] = (g.GRD_afact[ks_][None, :, None] * eth_[:, ks_]
+                             + g.GRD_bfact[ks_][None, :, None] * eth_[:, ksm_])
+            eth_h[:, kmin - 1] = eth_h[:, kmin]
+            rhog_h[:, kmin - 1] = rhog_h[:, kmin]
+        else:
+            rhog_h[:, :, ks_] = (C2W[:, :, ks_, :, 0] * P[:, :, ks_, :, I_RHOG]
+                                 + C2W[:, :, ks_, :, 1] * P[:, :, ksm_, :, I_RHOG])
+            eth_h[:, :, ks_] = (g.GRD_afact[ks_][None, None, :, None] * eth_[:, :, ks_]
+                                + g.GRD_bfact[ks_][None, None, :, None] * eth_[:, :, ksm_])
+            rhog_h[:, :, kmin - 1] = rhog_h[:, :, kmin]
+            eth_h[:, :, kmin - 1] = eth_h[:, :, kmin]
+        res["rhog_h" + sfx] = rhog_h
+        res["eth_h" + sfx] = eth_h
+        res["drhog" + sfx] = flux_convergence(g, P[..., I_RHOGVX], P[..., I_RHOGVY], P[..., I_RHOGVZ],
+                                              P[..., I_RHOGW], True, pole)
+    gd, gdp = numfilter_divdamp(g, PROG[..., I_RHOGVX], PROG[..., I_RHOGVY], PROG[..., I_RHOGVZ],
+                                PROG[..., I_RHOGW], PROG_pl[..., I_RHOGVX], PROG_pl[..., I_RHOGVY],
+                                PROG_pl[..., I_RHOGVZ], PROG_pl[..., I_RHOGW])
+    dpg, dpgw, dpg_pl, dpgw_pl = pres_gradient(g, pregd, pregd_pl, True)
+    g_TEND, g_TEND_pl = {}, {}
+    gz = {}
+    for pole in (False, True):
+        sfx = "_pl" if pole else ""
+        P = PROG_pl if pole else PROG
+        D = DIAG_pl if pole else DIAG
+        G0 = g_TEND0_pl if pole else g_TEND0
+        dbuo = buoyancy(g, rhogd_pl if pole else rhogd, pole)
+        drhoge = advection_convergence(g, P[..., I_RHOGVX], P[..., I_RHOGVY], P[..., I_RHOGVZ], P[..., I_RHOGW],
+                                       eth_pl if pole else eth, True, pole)
+        dg, dgw = (dpg_pl, dpgw_pl) if pole else (dpg, dpgw)
+        gzt = g.GRAV - (dgw - dbuo) / res["rhog_h" + sfx]
+        pwh = -gzt * P[..., I_RHOGW]
+        W2C = getattr(g, "VMTR_W2Cfact" + sfx)
+        kc, kp = slice(kmin, kmax + 1), slice(kmin + 1, kmax + 2)
+        pw = np.zeros_like(pwh)
+        if pole:
+            pw[:, kc] = (D[:, kc, :, I_vx] * dg[:, kc, :, XDIR] + D[:, kc, :, I_vy] * dg[:, kc, :, YDIR]
+                         + D[:, kc, :, I_vz] * dg[:, kc, :, ZDIR] + W2C[:, kc, :, 0] * pwh[:, kp]
+                         + W2C[:, kc, :, 1] * pwh[:, kc])
+        else:
+            pw[:, :, kc] = (D[:, :, kc, :, I_vx] * dg[:, :, kc, :, XDIR] + D[:, :, kc, :, I_vy] * dg[:, :, kc, :, YDIR]
+                            + D[:, :, kc, :, I_vz] * dg[:, :, kc, :, ZDIR] + W2C[:, :, kc, :, 0] * pwh[:, :, kp]
+                            + W2C[:, :, kc, :, 1] * pwh[:, :, kc])
+        dd = gdp if pole else gd
+        zero = np.zeros_like(pw)
+        T = np.zeros(pw.shape + (6,))
+        T[..., I_RHOG] = G0[..., I_RHOG] + res["drhog" + sfx]
+        T[..., I_RHOGVX] = G0[..., I_RHOGVX] - dg[..., XDIR] + dd[0] + zero
+        T[..., I_RHOGVY] = G0[..., I_RHOGVY] - dg[..., YDIR] + dd[1] + zero
+        T[..., I_RHOGVZ] = G0[..., I_RHOGVZ] - dg[..., ZDIR] + dd[2] + zero
+        T[..., I_RHOGW] = G0[..., I_RHOGW] + zero * alpha - dgw + dbuo
+        T[..., I_RHOGE] = G0[..., I_RHOGE] + drhoge + pw
+        if pole:
+            g_TEND_pl = T
+        else:
+            g_TEND = T
+        gz[sfx] = gzt
+    rweight = 1.0 / float(nitr)
+    PROG_mean = PROG[..., 0:5].copy()
+    PROG_mean_pl = PROG_pl[..., 0:5].copy()
+    Mats = {}
+    for pole in (False, True):
+        sfx = "_pl" if pole else ""
+        Mats[sfx] = rhow_matrix(g, res["eth_h" + sfx], gz[sfx], dt, pole)
+    PS, PSp = PROG_split, PROG_split_pl
+    for ns in range(nitr):
+        preg_s = PS[..., I_RHOGE] * RovCV
+        _kset(preg_s, kmin - 1, _kidx(preg_s, kmin)); _kset(preg_s, kmax + 1, _kidx(preg_s, kmax))
+        _kset(PS[..., I_RHOGE], kmin - 1, _kidx(PS[..., I_RHOGE], kmin))
+        _kset(PS[..., I_RHOGE], kmax + 1, _kidx(PS[..., I_RHOGE], kmax))
+        preg_sp = PSp[..., I_RHOGE] * RovCV
+        _kset(preg_sp, kmin - 1, _kidx(preg_sp, kmin)); _kset(preg_sp, kmax + 1, _kidx(preg_sp, kmax))
+        _kset(PSp[..., I_RHOGE], kmin - 1, _kidx(PSp[..., I_RHOGE], kmin))
+        _kset(PSp[..., I_RHOGE], kmax + 1, _kidx(PSp[..., I_RHOGE], kmax))
+        dd, ddp = numfilter_divdamp(g, PS[..., I_RHOGVX], PS[..., I_RHOGVY], PS[..., I_RHOGVZ], PS[..., I_RHOGW],
+                                    PSp[..., I_RHOGVX], PSp[..., I_RHOGVY], PSp[..., I_RHOGVZ], PSp[..., I_RHOGW])
+        # _vi_path1_fused (kernels/vipath1.py:68-160), gradtype horizontal
+        Pg, _, Pg_pl, _ = pres_gradient(g, preg_s, preg_sp, False)
+        dvh, dvhp = [], []
+        drw = {}
+        for pole in (False, True):
+            T = g_TEND_pl if pole else g_TEND
+            pg = Pg_pl if pole else Pg
+            ddd = ddp if pole else dd
+            S = PSp if pole else PS
+            P = PROG_pl if pole else PROG
+            zero = np.zeros_like(T[..., 0])
+            dx = T[..., I_RHOGVX] - pg[..., XDIR] + ddd[0] + zero
+            dy = T[..., I_RHOGVY] - pg[..., YDIR] + ddd[1] + zero
+            dz = T[..., I_RHOGVZ] - pg[..., ZDIR] + ddd[2] + zero
+            drw["_pl" if pole else ""] = T[..., I_RHOGW] + zero * alpha
+            vx_ = S[..., I_RHOGVX] + dx * dt
+            vy_ = S[..., I_RHOGVY] + dy * dt
+            vz_ = S[..., I_RHOGVZ] + dz * dt
+            rg = P[..., I_RHOG]
+            for v in (vx_, vy_, vz_):
+                top = 1.0 * (_kidx(v, kmax) / _kidx(rg, kmax)) * _kidx(rg, kmax + 1)
+                btm = -1.0 * (_kidx(v, kmin) / _kidx(rg, kmin)) * _kidx(rg, kmin - 1)
+                _kset(v, kmax + 1, top)
+                _kset(v, kmin - 1, btm)
+            arr = np.stack([vx_, vy_, vz_], axis=-1)
+            (dvhp if pole else dvh).append(arr)
+        dvh, dvhp = dvh[0], dvhp[0]
+        comm(g, dvh, dvhp)
+        dwe = np.zeros(PS.shape[:-1] + (3,))
+        dwep = np.zeros(PSp.shape[:-1] + (3,))
+        for pole in (False, True):
+            sfx = "_pl" if pole else ""
+            S = PSp if pole else PS
+            P = PROG_pl if pole else PROG
+            T = g_TEND_pl if pole else g_TEND
+            G0 = g_TEND0_pl if pole else g_TEND0
+            V = dvhp if pole else dvh
+            Mc, Mu, Ml = Mats[sfx]
+            Pd = {
+                "rhogvx_s1": V[..., 0], "rhogvy_s1": V[..., 1], "rhogvz_s1": V[..., 2],
+                "rhog_s0": S[..., I_RHOG], "rhogvx_s0": S[..., I_RHOGVX], "rhogvy_s0": S[..., I_RHOGVY],
+                "rhogvz_s0": S[..., I_RHOGVZ], "rhogw_s0": S[..., I_RHOGW], "rhoge_s0": S[..., I_RHOGE],
+                "preg_s0": preg_sp if pole else preg_s,
+                "rhog0": P[..., I_RHOG], "rhogvx0": P[..., I_RHOGVX], "rhogvy0": P[..., I_RHOGVY],
+                "rhogvz0": P[..., I_RHOGVZ], "rhogw0": P[..., I_RHOGW], "eth0": eth_pl if pole else eth,
+                "grhog": T[..., I_RHOG], "grhogw": drw[sfx], "grhoge": T[..., I_RHOGE],
+                "grhogetot": G0[..., I_RHOGE], "Mc": Mc, "Mu": Mu, "Ml": Ml,
+            }
+            r1, rw1, re1 = vi_main(g, Pd, dt, pole)
+            W = dwep if pole else dwe
+            W[..., 0], W[..., 1], W[..., 2] = r1, rw1, re1
+        comm(g, dwe, dwep)
+        for (S, V, W, PM) in ((PS, dvh, dwe, PROG_mean), (PSp, dvhp, dwep, PROG_mean_pl)):
+            S[..., I_RHOGVX] = V[..., 0]
+            S[..., I_RHOGVY] = V[..., 1]
+            S[..., I_RHOGVZ] = V[..., 2]
+            S[..., I_RHOG] = W[..., 0]
+            S[..., I_RHOGW] = W[..., 1]
+            S[..., I_RHOGE] = W[..., 2]
+            PM += S[..., 0:5] * rweight
+    PROG[..., 0:6] += PS[..., 0:6]
+    PROG_pl[...] += PSp
+    a, b, c = PROG[..., I_RHOGVX].copy(), PROG[..., I_RHOGVY].copy(), PROG[..., I_RHOGVZ].copy()
+    horizontalize(g, a, b, c)
+    PROG[..., I_RHOGVX], PROG[..., I_RHOGVY], PROG[..., I_RHOGVZ] = a, b, c
+    a, b, c = PROG_pl[..., I_RHOGVX].copy(), PROG_pl[..., I_RHOGVY].copy(), PROG_pl[..., I_RHOGVZ].copy()
+    horizontalize_pl(g, a, b, c)
+    PROG_pl[..., I_RHOGVX], PROG_pl[..., I_RHOGVY], PROG_pl[..., I_RHOGVZ] = a, b, c
+    comm(g, PROG_mean, PROG_mean_pl)
+    return PROG_mean, PROG_mean_pl
+
+
+
+# --------------------------------------------------------------------------
+# tracer advection (mod_src_tracer.py, MIURA2004 + Thuburn limiters)
+# --------------------------------------------------------------------------
+def _tracer_vert_flux(g, rvx, rvy, rvz, rw, rhog_in, frhog, dt, pole):
+    """kernels/tracervertflux.py:44-167 -> flx_v, ck(...,2), rhog (b1 = 0)."""
+    sfx = "_pl" if pole else ""
+    kmin, kmax = g.kmin, g.kmax
+    C2WGz = getattr(g, "VMTR_C2WfactGz" + sfx)
+    RGAMH = getattr(g, "VMTR_RGAMH" + sfx)
+    RGSQRTH = getattr(g, "VMTR_RGSQRTH" + sfx)
+    ks, km = slice(kmin + 1, kmax + 1), slice(kmin, kmax)
+    kc, kcp = slice(kmin, kmax + 1), slice(kmin + 1, kmax + 2)
+    K = (lambda a, s: a[:, s]) if pole else (lambda a, s: a[:, :, s])
+    c2w = K(C2WGz, ks)
+    horiz = (c2w[..., 0] * K(rvx, ks) + c2w[..., 1] * K(rvx, km) + c2w[..., 2] * K(rvy, ks)
+             + c2w[..., 3] * K(rvy, km) + c2w[..., 4] * K(rvz, ks) + c2w[..., 5] * K(rvz, km)) * K(RGAMH, ks)
+    vert = K(rw, ks) * K(RGSQRTH, ks)
+    flx = np.zeros_like(rhog_in)
+    ck = np.zeros(rhog_in.shape + (2,))
+    rhog = np.zeros_like(rhog_in)
+    b1 = 0.0
+    if pole:
+        flx[:, ks] = (horiz + vert) * 0.5 * dt
+        rdz = g.GRD_rdgz[kc][None, :, None]
+        ck[:, kc, :, 0] = -flx[:, kc] / rhog_in[:, kc] * rdz
+        ck[:, kc, :, 1] = flx[:, kcp] / rhog_in[:, kc] * rdz
+        rhog[:, kc] = rhog_in[:, kc] - (flx[:, kcp] - flx[:, kc]) * rdz + b1 * frhog[:, kc] * dt
+        rhog[:, kmin - 1] = rhog_in[:, kmin]
+        rhog[:, kmax + 1] = rhog_in[:, kmax]
+    else:
+        flx[:, :, ks] = (horiz + vert) * 0.5 * dt
+        rdz = g.GRD_rdgz[kc][None, None, :, None]
+        ck[:, :, kc, :, 0] = -flx[:, :, kc] / rhog_in[:, :, kc] * rdz
+        ck[:, :, kc, :, 1] = flx[:, :, kcp] / rhog_in[:, :, kc] * rdz
+        rhog[:, :, kc] = rhog_in[:, :, kc] - (flx[:, :, kcp] - flx[:, :, kc]) * rdz + b1 * frhog[:, :, kc] * dt
+        rhog[:, :, kmin - 1] = rhog_in[:, :, kmin]
+        rhog[:, :, kmax + 1] = rhog_in[:, :, kmax]
+    return flx, ck, rhog
+
+
+def vertical_limiter(g, q_h, q, d, ck):
+    """mod_src_tracer.py:1909-2074 (host loop; regional and pole alike):
+    clips q_h on k = kmin+1..kmax, in place.  Works on (..., k, l) arrays whose
+    level axis is -2 (regional (i,j,k,l) and pole (g,k,l))."""
+    kmin, kmax = g.kmin, g.kmax
+    BIG, EPS = g.HUGE, g.EPS
+    ax = q.ndim - 2
+    T = lambda a, k: np.take(a, k, axis=ax)
+    ck0, ck1 = ck[..., 0], ck[..., 1]
+    qmin_prev = qmax_prev = None
+    for k in range(kmin, kmax + 1):
+        inL = 0.5 - np.copysign(0.5, T(ck0, k))
+        inU = 0.5 + np.copysign(0.5, T(ck0, k + 1))
+        qc, qb, qa = T(q, k), T(q, k - 1), T(q, k + 1)
+        QminL = np.where(inL == 1.0, np.minimum(qc, qb), BIG)
+        QminU = np.where(inU == 1.0, np.minimum(qc, qa), BIG)
+        QmaxL = np.where(inL == 1.0, np.maximum(qc, qb), -BIG)
+        QmaxU = np.where(inU == 1.0, np.maximum(qc, qa), -BIG)
+        qnmin = np.minimum(np.minimum(QminL, QminU), qc)
+        qnmax = np.maximum(np.maximum(QmaxL, QmaxU), qc)
+        c1, c2 = T(ck0, k), T(ck1, k)
+        Cin = inL * c1 + inU * c2
+        Cout = (1.0 - inL) * c1 + (1.0 - inU) * c2
+        CQmin = inL * c1 * QminL + inU * c2 * QminU
+        CQmax = inL * c1 * QmaxL + inU * c2 * QmaxU
+        zsw = 0.5 - np.copysign(0.5, np.abs(Cout) - EPS)
+        dk = T(d, k)
+        qomin = ((qc - qnmax) + qnmax * (Cin + Cout - dk) - CQmax) / (Cout + zsw) * (1.0 - zsw) + qc * zsw
+        qomax = ((qc - qnmin) + qnmin * (Cin + Cout - dk) - CQmin) / (Cout + zsw) * (1.0 - zsw) + qc * zsw
+        if k > kmin:
+            qh = T(q_h, k)
+            new = (inL * np.minimum(np.maximum(qh, qmin_prev), qmax_prev)
+                   + (1.0 - inL) * np.minimum(np.maximum(qh, qomin), qomax))
+            if ax == 2:
+                q_h[:, :, k] = new
+            else:
+                q_h[:, k] = new
+        qmin_prev, qmax_prev = qomin, qomax
+
+
+def _vertical_advection(g, rhogq, q_den, flx, ck, d, pole, clamp):
+    """one vertical fractional step for one tracer (mod_src_tracer.py:389-533,
+    1036-1204), in place on rhogq."""
+    kmin, kmax = g.kmin, g.kmax
+    af, bf = g.GRD_afact, g.GRD_bfact
+    q = rhogq / q_den
+    q_h = np.zeros_like(q)
+    if pole:
+        q_h[:, kmin:kmax + 2] = af[kmin:kmax + 2][None, :, None] * q[:, kmin:kmax + 2] \
+            + bf[kmin:kmax + 2][None, :, None] * q[:, kmin - 1:kmax + 1]
+    else:
+        for k in range(kmin, kmax + 2):
+            q_h[:, :, k] = af[k] * q[:, :, k] + bf[k] * q[:, :, k - 1]
+    vertical_limiter(g, q_h, q, d, ck)
+    _kset(q_h, kmin, 0.0)
+    _kset(q_h, kmax + 1, 0.0)
+    for k in range(kmin, kmax + 1):
+        upd = (_kidx(flx, k + 1) * _kidx(q_h, k + 1) - _kidx(flx, k) * _kidx(q_h, k)) * g.GRD_rdgz[k]
+        _kset(rhogq, k, _kidx(rhogq, k) - upd)
+    _kset(rhogq, kmin - 1, 0.0)
+    _kset(rhogq, kmax + 1, 0.0)
+    if clamp:
+        if pole:
+            m = (rhogq > -1.0e-10) & (rhogq < 0.0)
+            rhogq[m] = 0.0
+        else:
+            sub = rhogq[:, :, kmin:kmax + 1]
+            m = (sub > -1.0e-10) & (sub < 0.0)
+            sub[m] = 0.0
+
+
+def horizontal_flux(g, rho, rvx, rvy, rvz, rho_pl, rvx_pl, rvy_pl, rvz_pl, dt):
+    """mod_src_tracer.py:1376-1531 -> flx_h (i,j,k,l,6), grd_xc (i,j,k,l,3,3),
+    flx_h_pl (g,k,l), grd_xc_pl (g,k,l,3)."""
+    i, j, kall, lall = rho.shape
+    EPS = g.EPS
+    gt = g.GMTR_t[:, :, 0]                      # (i,j,l,2,5)
+    ga = g.GMTR_a[:, :, 0]                      # (i,j,l,3,12)
+    gp = g.GMTR_p[:, :, 0]                      # (i,j,l,8)
+    xr = g.GRD_xr[:, :, 0]                      # (i,j,l,3,3)
+    flx_h = np.zeros(rho.shape + (6,))
+    grd_xc = np.zeros(rho.shape + (3, 3))
+    isl, jsl = slice(0, i - 1), slice(0, j - 1)
+    isp, jsp = slice(1, i), slice(1, j)
+    W = lambda t, w: gt[isl, jsl, :, t, w][:, :, None, :]
+    fields = [rho, rvx, rvy, rvz]
+    TIv, TJv = [], []
+    for f in fields:
+        ti = f[isl, jsl] * W(TI, W1) + f[isp, jsl] * W(TI, W2)
+        tj = f[isl, jsl] * W(TJ, W1)
+        ti = ti + f[isp, jsp] * W(TI, W3)
+        tj = tj + (f[isp, jsp] * W(TJ, W2) + f[isl, jsp] * W(TJ, W3))
+        m0 = g.pntmask[0, :, 0][None, :]
+        m1 = g.pntmask[0, :, 1][None, :]
+        ti[0, 0] = ti[0, 0] * m0 + tj[1, 0] * m1
+        TIv.append(ti)
+        TJv.append(tj)
+    rT, xT, yT, zT = TIv
+    rJ, xJ, yJ, zJ = TJv
+    PR = lambda a, b: gp[a, b, :, P_RAREA][:, :, None, :]
+
+    def edge(a_sl, b_sl, rr, vx2, vy2, vz2, face):
+        rr2 = 1.0 / np.maximum(rr, EPS)
+        A = lambda c: ga[a_sl, b_sl, :, face, c][:, :, None, :]
+        flux = 0.5 * (vx2 * A(HNX) + vy2 * A(HNY) + vz2 * A(HNZ))
+        xc = [xr[a_sl, b_sl, :, face, d][:, :, None, :] - v2 * rr2 * dt * 0.5
+              for d, v2 in ((XDIR, vx2), (YDIR, vy2), (ZDIR, vz2))]
+        return flux, xc
+    # AI face: isl, jsl = 0..i-2, 1..j-2
+    a_, b_ = slice(0, i - 1), slice(1, j - 1)
+    bm = slice(0, j - 2)
+    flux, xc = edge(a_, b_, rJ[:, bm] + rT[:, b_], xJ[:, bm] + xT[:, b_], yJ[:, bm] + yT[:, b_],
+                    zJ[:, bm] + zT[:, b_], AI)
+    flx_h[a_, b_, :, :, 0] = flux * PR(a_, b_) * dt
+    flx_h[1:i, b_, :, :, 3] = -flux * PR(slice(1, i), b_) * dt
+    for d in range(3):
+        grd_xc[a_, b_, :, :, AI, d] = xc[d]
+    # AIJ face: 0..i-2, 0..j-2
+    a_, b_ = slice(0, i - 1), slice(0, j - 1)
+    flux, xc = edge(a_, b_, rT + rJ, xT + xJ, yT + yJ, zT + zJ, AIJ)
+    flx_h[a_, b_, :, :, 1] = flux * PR(a_, b_) * dt
+    flx_h[1:i, 1:j, :, :, 4] = -flux * PR(slice(1, i), slice(1, j)) * dt
+    for d in range(3):
+        grd_xc[a_, b_, :, :, AIJ, d] = xc[d]
+    # AJ face: 1..i-2, 0..j-2
+    a_, b_ = slice(1, i - 1), slice(0, j - 1)
+    am = slice(0, i - 2)
+    flux, xc = edge(a_, b_, rJ[a_] + rT[am], xJ[a_] + xT[am], yJ[a_] + yT[am], zJ[a_] + zT[am], AJ)
+    flx_h[a_, b_, :, :, 2] = flux * PR(a_, b_) * dt
+    flx_h[a_, 1:j, :, :, 5] = -flux * PR(a_, slice(1, j)) * dt
+    for d in range(3):
+        grd_xc[a_, b_, :, :, AJ, d] = xc[d]
+    flx_h[1, 1, :, :, 5] *= g.pntmask[0, :, 0].astype(np.float64)[None, :]
+    # pole
+    gtp = g.GMTR_t_pl[:, 0]                     # (6, l, 5)
+    gap = g.GMTR_a_pl[:, 0]                     # (6, l, 18)
+    gpp = g.GMTR_p_pl[:, 0]
+    flx_pl = np.zeros_like(rho_pl)
+    xc_pl = np.zeros(rho_pl.shape + (3,))
+    for l in range(rho_pl.shape[2]):
+        tv = {}
+        for v in range(1, 6):
+            vp1 = 1 if v + 1 == 6 else v + 1
+            tv[v] = [f[0, :, l] * gtp[v, l, W1] + f[v, :, l] * gtp[v, l, W2] + f[vp1, :, l] * gtp[v, l, W3]
+                     for f in (rho_pl, rvx_pl, rvy_pl, rvz_pl)]
+        for v in range(1, 6):
+            vm1 = 5 if v - 1 == 0 else v - 1
+            rr2 = 1.0 / np.maximum(tv[vm1][0] + tv[v][0], EPS)
+            v2 = [tv[vm1][n] + tv[v][n] for n in (1, 2, 3)]
+            flux = 0.5 * (v2[0] * gap[v, l, HNX] + v2[1] * gap[v, l, HNY] + v2[2] * gap[v, l, HNZ])
+            flx_pl[v, :, l] = flux * gpp[0, l, P_RAREA] * dt
+            for d in range(3):
+                xc_pl[v, :, l, d] = g.GRD_xr_pl[v, 0, l, d] - v2[d] * rr2 * dt * 0.5
+    return flx_h, grd_xc, flx_pl, xc_pl
+
+
+def horizontal_remap(g, q, q_pl, cmask, cmask_pl, grd_xc, grd_xc_pl):
+    """mod_src_tracer.py:1535-1847 (numpy loops) -> q_a (i,j,k,l,6), q_a_pl."""
+    i, j = q.shape[:2]
+    gq = gradient(g, q)
+    gq_pl = gradient_pl(g, q_pl)
+    comm(g, gq, gq_pl)
+    X = g.GRD_x[:, :, 0]                        # (i,j,l,3)
+
+    def rec(qs, gqs, xcs, xs):
+        out = qs
+        for d in (XDIR, YDIR, ZDIR):
+            out = out + gqs[..., d] * (xcs[..., d] - xs[..., d][:, :, None, :])
+        return out
+    isl, jsl, isp, jsp = slice(0, i - 1), slice(0, j - 1), slice(1, i), slice(1, j)
+    ins, jns, inm, jnm = slice(1, i - 1), slice(1, j - 1), slice(0, i - 2), slice(0, j - 2)
+    qap = [np.zeros(q.shape) for _ in range(6)]
+    qam = [np.zeros(q.shape) for _ in range(6)]
+    xc = lambda a, b, f: grd_xc[a, b, :, :, f, :]
+    qap[0][isl, jsl] = rec(q[isl, jsl], gq[isl, jsl], xc(isl, jsl, AI), X[isl, jsl])
+    qam[0][isl, jsl] = rec(q[isp, jsl], gq[isp, jsl], xc(isl, jsl, AI), X[isp, jsl])
+    qap[1][isl, jsl] = rec(q[isl, jsl], gq[isl, jsl], xc(isl, jsl, AIJ), X[isl, jsl])
+    qam[1][isl, jsl] = rec(q[isp, jsp], gq[isp, jsp], xc(isl, jsl, AIJ), X[isp, jsp])
+    qap[2][isl, jsl] = rec(q[isl, jsl], gq[isl, jsl], xc(isl, jsl, AJ), X[isl, jsl])
+    qam[2][isl, jsl] = rec(q[isl, jsp], gq[isl, jsp], xc(isl, jsl, AJ), X[isl, jsp])
+    qap[3][ins, jns] = rec(q[inm, jns], gq[inm, jns], xc(inm, jns, AI), X[inm, jns])
+    qam[3][ins, jns] = rec(q[ins, jns], gq[ins, jns], xc(inm, jns, AI), X[ins, jns])
+    qap[4][ins, jns] = rec(q[inm, jnm], gq[inm, jnm], xc(inm, jnm, AIJ), X[inm, jnm])
+    qam[4][ins, jns] = rec(q[ins, jns], gq[ins, jns], xc(inm, jnm, AIJ), X[ins, jns])
+    qap[5][ins, jns] = rec(q[ins, jnm], gq[ins, jnm], xc(ins, jnm, AJ), X[ins, jnm])
+    qam[5][ins, jns] = rec(q[ins, jns], gq[ins, jns], xc(ins, jnm, AJ), X[ins, jns])
+    q_a = np.full(q.shape + (6,), np.nan)
+    for f in range(6):
+        q_a[isl, jsl, :, :, f] = cmask[isl, jsl, :, :, f] * qam[f][isl, jsl] \
+            + (1.0 - cmask[isl, jsl, :, :, f]) * qap[f][isl, jsl]
+    q_a_pl = np.full(q_pl.shape, np.nan)
+    Xp = g.GRD_x_pl[:, 0]                       # (6,l,3)
+    for v in range(1, 6):
+        ap = q_pl[0]
+        am = q_pl[v]
+        for d in (XDIR, YDIR, ZDIR):
+            ap = ap + gq_pl[0, :, :, d] * (grd_xc_pl[v, :, :, d] - Xp[0, :, d][None, :])
+        for d in (XDIR, YDIR, ZDIR):
+            am = am + gq_pl[v, :, :, d] * (grd_xc_pl[v, :, :, d] - Xp[v, :, d][None, :])
+        q_a_pl[v] = cmask_pl[v] * am + (1.0 - cmask_pl[v]) * ap
+    return q_a, q_a_pl
+
+
+def horizontal_limiter(g, q_a, q_a_pl, q, q_pl, d, d_pl, ch, ch_pl, cmask, cmask_pl):
+    """mod_src_tracer.py:2115-2664 (numpy branch), in place on q_a / q_a_pl."""
+    i, j = q.shape[:2]
+    BIG, EPS = g.HUGE, g.EPS
+    Qin = np.full(q.shape + (2, 6), np.nan)
+    mn = lambda *a: _reduce(np.minimum, a)
+    mx = lambda *a: _reduce(np.maximum, a)
+    I0, J0 = slice(0, i - 1), slice(0, j - 1)
+    q0 = q[I0, J0]
+    q1 = np.empty_like(q0)
+    q1[:, 1:] = q[I0, 0:j - 2]
+    q1[:, 0] = q[0, 0]
+    q2 = q[1:i, J0]
+    q3 = q[1:i, 1:j]
+    qjp = q[I0, 1:j]
+    q4 = np.empty_like(q0)
+    q4[1:, :] = q[0:i - 2, J0]
+    q4[0, :] = q[0, 0]
+    qmin = [mn(q0, q1, q2, q3), mn(q0, q2, q3, qjp), mn(q0, q3, qjp, q4)]
+    qmax = [mx(q0, q1, q2, q3), mx(q0, q2, q3, qjp), mx(q0, q3, qjp, q4)]
+    cm = cmask[I0, J0]
+    for m in range(3):
+        Qin[I0, J0, :, :, 0, m] = cm[..., m] * qmin[m] + (1.0 - cm[..., m]) * BIG
+        Qin[I0, J0, :, :, 1, m] = cm[..., m] * qmax[m] + (1.0 - cm[..., m]) * (-BIG)
+    Qin[1:i, J0, :, :, 0, 3] = cm[..., 0] * BIG + (1.0 - cm[..., 0]) * qmin[0]
+    Qin[1:i, J0, :, :, 1, 3] = cm[..., 0] * (-BIG) + (1.0 - cm[..., 0]) * qmax[0]
+    Qin[1:i, 1:j, :, :, 0, 4] = cm[..., 1] * BIG + (1.0 - cm[..., 1]) * qmin[1]
+    Qin[1:i, 1:j, :, :, 1, 4] = cm[..., 1] * (-BIG) + (1.0 - cm[..., 1]) * qmax[1]
+    Qin[I0, 1:j, :, :, 0, 5] = cm[..., 2] * BIG + (1.0 - cm[..., 2]) * qmin[2]
+    Qin[I0, 1:j, :, :, 1, 5] = cm[..., 2] * (-BIG) + (1.0 - cm[..., 2]) * qmax[2]
+    for l in range(q.shape[3]):
+        if g.have_sgp[l]:
+            vals = np.stack([q[0, 0, :, l], q[1, 1, :, l], q[2, 1, :, l], q[0, 1, :, l]])
+            qn, qx = vals.min(axis=0), vals.max(axis=0)
+            c1 = cmask[0, 0, :, l, 1]
+            Qin[0, 0, :, l, 0, 1] = np.where(c1 == 1.0, qn, BIG)
+            Qin[1, 1, :, l, 0, 4] = np.where(c1 == 1.0, BIG, qn)
+            Qin[0, 0, :, l, 1, 1] = np.where(c1 == 1.0, qx, -BIG)
+            Qin[1, 1, :, l, 1, 4] = np.where(c1 == 1.0, -BIG, qx)
+    Qout = np.full(q.shape + (2,), np.nan)
+    In, Jn = slice(1, i - 1), slice(1, j - 1)
+    qi = q[In, Jn]
+    Qi = Qin[In, Jn]
+    qnmin = mn(qi, *[Qi[..., 0, m] for m in range(6)])
+    qnmax = mx(qi, *[Qi[..., 1, m] for m in range(6)])
+    chi = ch[In, Jn]
+    chm = np.minimum(chi, 0.0)
+    Cin = np.sum(chm, axis=-1)
+    Cout = np.sum(chi - chm, axis=-1)
+    CQmin = np.sum(chm * Qi[..., 0, :], axis=-1)
+    CQmax = np.sum(chm * Qi[..., 1, :], axis=-1)
+    zsw = 0.5 - np.copysign(0.5, np.abs(Cout) - EPS)
+    di = d[In, Jn]
+    Qout[In, Jn, :, :, 0] = (qi - CQmax - qnmax * (1.0 - Cin - Cout + di)) / (Cout + zsw) * (1.0 - zsw) + qi * zsw
+    Qout[In, Jn, :, :, 1] = (qi - CQmin - qnmin * (1.0 - Cin - Cout + di)) / (Cout + zsw) * (1.0 - zsw) + qi * zsw
+    for b in (0, 1):
+        Qout[:, 0, :, :, b] = q[:, 0]
+        Qout[:, j - 1, :, :, b] = q[:, j - 1]
+        Qout[0, 1:j - 1, :, :, b] = q[0, 1:j - 1]
+        Qout[i - 1, 1:j - 1, :, :, b] = q[i - 1, 1:j - 1]
+    # pole Qin / Qout (mod_src_tracer.py:2437-2495)
+    Qin_pl = np.full(q_pl.shape + (2, 2), np.nan)
+    Qout_pl = np.full(q_pl.shape + (2,), np.nan)
+    for v in range(1, 6):
+        vp1 = 1 if v + 1 > 5 else v + 1
+        vm1 = 5 if v - 1 < 1 else v - 1
+        qn = mn(q_pl[0], q_pl[v], q_pl[vm1], q_pl[vp1])
+        qx = mx(q_pl[0], q_pl[v], q_pl[vm1], q_pl[vp1])
+        c = cmask_pl[v]
+        Qin_pl[v, ..., 0, 0] = np.where(c == 1.0, qn, BIG)
+        Qin_pl[v, ..., 0, 1] = np.where(c == 1.0, BIG, qn)
+        Qin_pl[v, ..., 1, 0] = np.where(c == 1.0, qx, -BIG)
+        Qin_pl[v, ..., 1, 1] = np.where(c == 1.0, -BIG, qx)
+    qnm = q_pl[0].copy()
+    qnx = q_pl[0].copy()
+    for v in range(1, 6):
+        qnm = np.minimum(qnm, Qin_pl[v, ..., 0, 0])
+        qnx = np.maximum(qnx, Qin_pl[v, ..., 1, 0])
+    Ci = np.zeros_like(q_pl[0]); Co = np.zeros_like(q_pl[0])
+    CQn = np.zeros_like(q_pl[0]); CQx = np.zeros_like(q_pl[0])
+    for v in range(1, 6):
+        chm_ = cmask_pl[v] * ch_pl[v]
+        Ci = Ci + chm_
+        Co = Co + (ch_pl[v] - chm_)
+        CQn = CQn + chm_ * Qin_pl[v, ..., 0, 0]
+        CQx = CQx + chm_ * Qin_pl[v, ..., 1, 0]
+    zs = 0.5 - np.copysign(0.5, np.abs(Co) - EPS)
+    den = Co + zs
+    fac = 1.0 - zs
+    q0p = q_pl[0]
+    dv = d_pl[0]
+    Qout_pl[0, ..., 0] = (q0p - CQx - qnx * (1.0 - Ci - Co + dv)) / den * fac + q0p * zs
+    Qout_pl[0, ..., 1] = (q0p - CQn - qnm * (1.0 - Ci - Co + dv)) / den * fac + q0p * zs
+    comm(g, Qout, Qout_pl)
+    # apply (mod_src_tracer.py:2536-2605)
+    Ip, Jp = slice(1, i), slice(1, j)
+    c = cmask[I0, J0]
+
+    def clampin(x, lo, hi):
+        return np.minimum(np.maximum(x, lo), hi)
+
+    def clampout(x, hi, lo):
+        return np.maximum(np.minimum(x, hi), lo)
+    for f, (A, B), m2 in ((0, (Ip, J0), 3), (1, (Ip, Jp), 4), (2, (I0, Jp), 5)):
+        cf = c[..., f]
+        qa = q_a[I0, J0, :, :, f]
+        qa = cf * clampin(qa, Qin[I0, J0, :, :, 0, f], Qin[I0, J0, :, :, 1, f]) \
+            + (1.0 - cf) * clampin(qa, Qin[A, B, :, :, 0, m2], Qin[A, B, :, :, 1, m2])
+        qa = cf * clampout(qa, Qout[A, B, :, :, 1], Qout[A, B, :, :, 0]) \
+            + (1.0 - cf) * clampout(qa, Qout[I0, J0, :, :, 1], Qout[I0, J0, :, :, 0])
+        q_a[I0, J0, :, :, f] = qa
+        q_a[A, B, :, :, m2] = qa
+    for v in range(1, 6):
+        cmv = cmask_pl[v]
+        a0 = clampin(q_a_pl[v], Qin_pl[v, ..., 0, 0], Qin_pl[v, ..., 1, 0])
+        a1 = clampin(q_a_pl[v], Qin_pl[v, ..., 0, 1], Qin_pl[v, ..., 1, 1])
+        q_a_pl[v] = cmv * a0 + (1.0 - cmv) * a1
+        a2 = clampout(q_a_pl[v], Qout_pl[v, ..., 1], Qout_pl[v, ..., 0])
+        a3 = clampout(q_a_pl[v], Qout_pl[0, ..., 1], Qout_pl[0, ..., 0])
+        q_a_pl[v] = cmv * a2 + (1.0 - cmv) * a3
+
+
+def _reduce(fn, arrs):
+    out = arrs[0]
+    for a in arrs[1:]:
+        out = fn(out, a)
+    return out
+
+
+def tracer_advection(g, rhogq, rhogq_pl, rhog_in, rhog_in_pl, PM, PM_pl, frhog, frhog_pl, dt):
+    """mod_src_tracer.py:83-1228 numpy path (Strang V/H/V, b1=0, b2=1, b3=0);
+    updates rhogq (i,j,k,l,nq) / rhogq_pl in place."""
+    kmin, kmax = g.kmin, g.kmax
+    rvx_m, rvy_m, rvz_m, rw_m = (PM[..., I_RHOGVX], PM[..., I_RHOGVY], PM[..., I_RHOGVZ], PM[..., I_RHOGW])
+    rvx_mp, rvy_mp, rvz_mp, rw_mp = (PM_pl[..., I_RHOGVX], PM_pl[..., I_RHOGVY], PM_pl[..., I_RHOGVZ],
+                                     PM_pl[..., I_RHOGW])
+    flx, ck, rhog = _tracer_vert_flux(g, rvx_m, rvy_m, rvz_m, rw_m, rhog_in, frhog, dt, False)
+    flxp, ckp, rhogp = _tracer_vert_flux(g, rvx_mp, rvy_mp, rvz_mp, rw_mp, rhog_in_pl, frhog_pl, dt, True)
+    b1, b2, b3 = 0.0, 1.0, 1.0 - (0.0 + 1.0)
+    d = b1 * frhog / rhog_in * dt
+    dp = b1 * frhog_pl / rhog_in_pl * dt
+    for iq in range(rhogq.shape[-1]):
+        _vertical_advection(g, rhogq[..., iq], rhog_in, flx, ck, d, False, False)
+        _vertical_advection(g, rhogq_pl[..., iq], rhog_in_pl, flxp, ckp, dp, True, False)
+    # horizontal step
+    d = b2 * frhog / rhog * dt
+    rvx = rvx_m * g.VMTR_RGAM
+    rvy = rvy_m * g.VMTR_RGAM
+    rvz = rvz_m * g.VMTR_RGAM
+    rvxp = rvx_mp * g.VMTR_RGAM_pl
+    rvyp = rvy_mp * g.VMTR_RGAM_pl
+    rvzp = rvz_mp * g.VMTR_RGAM_pl
+    flx_h, grd_xc, flx_hp, grd_xcp = horizontal_flux(g, PM[..., I_RHOG], rvx, rvy, rvz,
+                                                      PM_pl[..., I_RHOG], rvxp, rvyp, rvzp, dt)
+    ch = flx_h / rhog[..., None]
+    cmask = 0.5 - np.copysign(0.5, ch - g.EPS)
+    ch_pl = np.full_like(flx_hp, np.nan)
+    cmask_pl = np.full_like(flx_hp, np.nan)
+    ch_pl[1:6] = flx_hp[1:6] / rhogp[0]
+    cmask_pl[1:6] = 0.5 - np.copysign(0.5, ch_pl[1:6] - g.EPS)
+    dp = b2 * frhog_pl / rhogp * dt
+    i, j = rhog.shape[:2]
+    isl, jsl = slice(1, i - 1), slice(1, j - 1)
+    for iq in range(rhogq.shape[-1]):
+        q = rhogq[..., iq] / rhog
+        q_pl = rhogq_pl[..., iq] / rhogp
+        q_a, q_a_pl = horizontal_remap(g, q, q_pl, cmask, cmask_pl, grd_xc, grd_xcp)
+        horizontal_limiter(g, q_a, q_a_pl, q, q_pl, d, dp, ch, ch_pl, cmask, cmask_pl)
+        rhogq[isl, jsl, :, :, iq] -= (flx_h[isl, jsl, :, :, 0] * q_a[isl, jsl, :, :, 0]
+                                      + flx_h[isl, jsl, :, :, 1] * q_a[isl, jsl, :, :, 1]
+                                      + flx_h[isl, jsl, :, :, 2] * q_a[isl, jsl, :, :, 2]
+                                      + flx_h[isl, jsl, :, :, 3] * q_a[isl, jsl, :, :, 3]
+                                      + flx_h[isl, jsl, :, :, 4] * q_a[isl, jsl, :, :, 4]
+                                      + flx_h[isl, jsl, :, :, 5] * q_a[isl, jsl, :, :, 5])
+        for v in range(1, 6):
+            rhogq_pl[0, :, :, iq] -= flx_hp[v] * q_a_pl[v]
+    rhog[isl, jsl] -= (flx_h[isl, jsl, :, :, 0] + flx_h[isl, jsl, :, :, 1] + flx_h[isl, jsl, :, :, 2]
+                       + flx_h[isl, jsl, :, :, 3] + flx_h[isl, jsl, :, :, 4]
+                       + flx_h[isl, jsl, :, :, 5]) - (b2 * frhog[isl, jsl] * dt)
+    for v in range(1, 6):
+        rhogp[0] -= flx_hp[v]
+    rhogp[0] += b2 * frhog_pl[0] * dt
+    # second vertical step
+    d = b3 * frhog / rhog * dt
+    ck = np.zeros_like(ck)
+    kc = slice(kmin, kmax + 1)
+    rdz = g.GRD_rdgz[kc][:, None]
+    ck[:, :, kc, :, 0] = -flx[:, :, kc] / rhog[:, :, kc] * rdz
+    ck[:, :, kc, :, 1] = flx[:, :, kmin + 1:kmax + 2] / rhog[:, :, kc] * rdz
+    dp = b3 * frhog_pl / rhogp * dt
+    ckp = np.zeros_like(ckp)
+    for k in range(kmin, kmax + 1):
+        ckp[:, k, :, 0] = -flxp[:, k] / rhogp[:, k] * g.GRD_rdgz[k]
+        ckp[:, k, :, 1] = flxp[:, k + 1] / rhogp[:, k] * g.GRD_rdgz[k]
+    for iq in range(rhogq.shape[-1]):
+        _vertical_advection(g, rhogq[..., iq], rhog, flx, ck, d, False, True)
+        _vertical_advection(g, rhogq_pl[..., iq], rhogp, flxp, ckp, dp, True, True)
+
+
+# --------------------------------------------------------------------------
+# the large step
+# --------------------------------------------------------------------------
+def dynamics_step(g, prg, prg_pl):
+    """mod_dynamics.py:1725-2741 numpy path: one RK3-HEVI large step.
+    ``prg (i,j,k,l,6+nq)`` / ``prg_pl (g,k,l,6+nq)`` are not modified; the new
+    state is returned (after the final halo exchange)."""
+    PROG = prg[..., 0:6].copy()
+    PROG_pl = prg_pl[..., 0:6].copy()
+    PROGq = prg[..., 6:].copy()
+    PROGq_pl = prg_pl[..., 6:].copy()
+    PROG0 = PROG.copy()
+    PROG0_pl = PROG_pl.copy()
+    PROG00_rhog = PROG[..., I_RHOG].copy()
+    PROG00_rhog_pl = PROG_pl[..., I_RHOG].copy()
+    DIAG = np.zeros(PROG.shape)
+    DIAG_pl = np.zeros(PROG_pl.shape)
+    nstage = len(g.sstep)
+    large_dt = g.dtl
+    for nl in range(nstage):
+        rho, ein, q, rho_pl, ein_pl, q_pl = diagnostics(g, PROG, PROGq, DIAG, PROG_pl, PROGq_pl, DIAG_pl)
+        bndcnd_all(g, DIAG, PROG, rho, ein)
+        bndcnd_all(g, DIAG_pl, PROG_pl, rho_pl, ein_pl, pole=True)
+        eth = ein + DIAG[..., I_pre] / rho
+        eth_pl = ein_pl + DIAG_pl[..., I_pre] / rho_pl
+        pregd = (DIAG[..., I_pre] - g.pre_bs) * g.VMTR_GSGAM2
+        rhogd = (rho - g.rho_bs) * g.VMTR_GSGAM2
+        pregd_pl = (DIAG_pl[..., I_pre] - g.pre_bs_pl) * g.VMTR_GSGAM2_pl
+        rhogd_pl = (rho_pl - g.rho_bs_pl) * g.VMTR_GSGAM2_pl
+        adv, adv_pl = advection_momentum(g, DIAG, PROG, DIAG_pl, PROG_pl)
+        g_TEND = np.zeros(PROG.shape)
+        g_TEND_pl = np.zeros(PROG_pl.shape)
+        for n, iv in enumerate((I_RHOGVX, I_RHOGVY, I_RHOGVZ, I_RHOGW)):
+            g_TEND[..., iv] = adv[n]
+            g_TEND_pl[..., iv] = adv_pl[n]
+        f_TEND, f_TEND_pl = hdiffusion(g, PROG[..., I_RHOG], rho, DIAG, PROG_pl[..., I_RHOG], rho_pl, DIAG_pl)
+        g_TEND = g_TEND + f_TEND
+        g_TEND_pl = g_TEND_pl + f_TEND_pl
+        if nl == 0:
+            PROG_split = np.zeros(PROG.shape)
+            PROG_split_pl = np.zeros(PROG_pl.shape)
+        else:
+            PROG_split = PROG0 - PROG
+            PROG_split_pl = PROG0_pl - PROG_pl
+        PM, PM_pl = vi_small_step(g, PROG, PROG_pl, DIAG, DIAG_pl, eth, eth_pl, rhogd, rhogd_pl,
+                                  pregd, pregd_pl, g_TEND, g_TEND_pl, PROG_split, PROG_split_pl,
+                                  g.sstep[nl], g.dts)
+        if nl != nstage - 1:
+            comm(g, PROG, PROG_pl)
+        else:
+            tracer_advection(g, PROGq, PROGq_pl, PROG00_rhog, PROG00_rhog_pl, PM, PM_pl,
+                             f_TEND[..., I_RHOG], f_TEND_pl[..., I_RHOG], large_dt)
+            PROGq += large_dt * np.zeros_like(PROGq)
+            PROGq_pl += large_dt * np.zeros_like(PROGq_pl)
+    out = np.concatenate([PROG, PROGq], axis=-1)
+    out_pl = np.concatenate([PROG_pl, PROGq_pl], axis=-1)
+    comm(g, out, out_pl)
+    return out, out_pl
