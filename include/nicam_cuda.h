@@ -1,0 +1,112 @@
+/* C ABI of the B200 NICAM-DC dynamics step (libnicamcuda.so).
+ *
+ * The reference drives its time step through the Python object
+ * Dyn (pynicamdc/nhm/dynamics/mod_dynamics.py): dynamics_step(msc) at
+ * mod_dynamics.py:1725, called once per step from pyNICAM.run
+ * (pynicamdc/api.py:724), with the prognostic state in
+ * prgv.PRG_var (gall_1d, gall_1d, kall, lall, 6+nq) and prgv.PRG_var_pl
+ * (6, kall, 2, 6+nq) (pynicamdc/nhm/share/mod_prgvar.py:51), drained to the
+ * host with Dyn.sync_prgvar_to_host (mod_dynamics.py:429).  These entry points
+ * are what a "cuda" backend binds in place of that Python step: the host
+ * keeps the reference's arrays and layouts; the library owns the device copy.
+ *
+ * Every function returns 0 on success and a non-zero status otherwise;
+ * nc_last_error() returns the message.  No function aborts the process.
+ * A handle is not re-entrant: one host thread drives one handle.
+ */
+#ifndef NICAM_CUDA_H
+#define NICAM_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  NC_OK = 0,
+  NC_ERR_ARG = 1,      /* bad argument, missing or mis-shaped setup array */
+  NC_ERR_CUDA = 2,     /* a CUDA runtime call failed */
+  NC_ERR_STATE = 3,    /* call out of order (e.g. step before upload) */
+  NC_ERR_NONFINITE = 4 /* non-finite value detected in the state */
+};
+
+enum { NC_F64 = 0, NC_I32 = 1, NC_I64 = 2, NC_BOOL = 3 };
+
+/* One named host array of the setup.  Names and shapes follow the
+ * reference's attributes: VMTR_* of share/mod_vmtr.py:30, OPRT_coef_* of
+ * share/mod_oprt.py:65, GRD_* of share/mod_grd.py:64, GMTR_* of
+ * share/mod_gmtr.py:65, bsstate rho_bs/pre_bs/tem_bs of
+ * nhm/share/mod_bsstate.py:20, ppm.pntmask and adm.ADM_have_sgp, run
+ * constants as 0-d arrays, and the halo plan (halo_r_dst, halo_r_src,
+ * halo_p_dst, halo_p_src) composed from comm.Copy_list_* and
+ * comm.Singular_list (share/mod_comm.py:1400-1561). */
+typedef struct nc_array {
+  const char* name;
+  const void* data;
+  int32_t dtype;
+  int32_t ndim;
+  int64_t shape[8];
+} nc_array;
+
+typedef struct nc_handle nc_handle;
+
+/* Replaces Dyn.dynamics_setup (mod_dynamics.py:164) for the device: uploads
+ * geometry, metrics and the halo plan, allocates all device work arrays. */
+int nc_create(const nc_array* arrays, int32_t narrays, nc_handle** out);
+
+/* Marshal-in of the prognostic state (mod_dynamics.py:1876-1880) from host
+ * memory in the reference layout: prg (gall_1d, gall_1d, kall, lall, 6+nq),
+ * prg_pl (6, kall, 2, 6+nq), both C-order float64.  Pinned host memory gives
+ * the fastest copy. */
+int nc_upload_state(nc_handle* h, const double* prg, const double* prg_pl);
+
+/* Marshal-out (Dyn.sync_prgvar_to_host, mod_dynamics.py:429-440) into host
+ * memory in the same layout. */
+int nc_download_state(nc_handle* h, double* prg, double* prg_pl);
+
+/* nsteps large steps of Dyn.dynamics_step (mod_dynamics.py:1725-2741) on the
+ * device-resident state.  Asynchronous on the handle's stream. */
+int nc_step(nc_handle* h, int32_t nsteps);
+
+/* Capture one large step as a CUDA graph and replay it (default on). */
+int nc_set_graph(nc_handle* h, int32_t enable);
+
+/* Debugging aid: run only the first nphases phases of one large step
+ * (phase boundaries sit after each halo exchange / kernel group, in the order
+ * of Dyn.dynamics_step), without graph capture, then synchronize. */
+int nc_run_phases(nc_handle* h, int32_t nphases);
+
+/* Wait for the handle's stream. */
+int nc_sync(nc_handle* h);
+
+/* Global sums of the embudget monitor (nhm/share/mod_embudget.py:74-80,
+ * _gsum = sum of var * VMTR_VOLUME over the interior): out[0] total air mass
+ * sum(rho*VOLUME), out[1 + n] tracer n mass sum(rho*q_n*VOLUME), n < nq.
+ * Float64 with compensated (Neumaier) summation on the device. */
+int nc_mass_sums(nc_handle* h, double* out, int32_t nout);
+
+/* Copy a named device work field to host in the reference layout
+ * (regional (i,j,k,l), pole (g,k,l)).  Names are those registered by
+ * nc_create: the state ("RHOG", "RHOGVX", .., "RHOGQ.<n>") and the work
+ * fields of the step (e.g. "rho", "pre", "eth", "gT0.<n>", "Mc").  Returns
+ * NC_ERR_ARG for an unknown name.  Debugging and parity tests only. */
+int nc_get_field(nc_handle* h, const char* name, double* host_reg, double* host_pl);
+
+/* Device pointers of the resident state, for callers that keep the state in
+ * their own device memory pipeline: field v (0..5 PROG, 6.. tracers) regional
+ * [l][k][j][i] and pole (g,k,l).  Pointers stay valid until nc_destroy. */
+int nc_state_pointers(nc_handle* h, int32_t v, double** reg, double** pl);
+
+/* Number of kernels the library launched since the handle was created. */
+int64_t nc_kernel_launches(nc_handle* h);
+
+const char* nc_last_error(void);
+
+void nc_destroy(nc_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NICAM_CUDA_H */

@@ -1407,8 +1407,9 @@ def horizontal_limiter(g, q_a, q_a_pl, q, q_pl, d, d_pl, ch, ch_pl, cmask, cmask
     for v in range(1, 6):
         vp1 = 1 if v + 1 > 5 else v + 1
         vm1 = 5 if v - 1 < 1 else v - 1
-        qn = mn(q_pl[0], q_pl[v], q_pl[vm1], q_pl[vp1])
-        qx = mx(q_pl[0], q_pl[v], q_pl[vm1], q_pl[vp1])
+        # Python builtin min/max (mod_src_tracer.py:2446-2447): ties keep the first
+        qn = _reduce(_pymin, (q_pl[0], q_pl[v], q_pl[vm1], q_pl[vp1]))
+        qx = _reduce(_pymax, (q_pl[0], q_pl[v], q_pl[vm1], q_pl[vp1]))
         c = cmask_pl[v]
         Qin_pl[v, ..., 0, 0] = np.where(c == 1.0, qn, BIG)
         Qin_pl[v, ..., 0, 1] = np.where(c == 1.0, BIG, qn)
@@ -1417,8 +1418,8 @@ def horizontal_limiter(g, q_a, q_a_pl, q, q_pl, d, d_pl, ch, ch_pl, cmask, cmask
     qnm = q_pl[0].copy()
     qnx = q_pl[0].copy()
     for v in range(1, 6):
-        qnm = np.minimum(qnm, Qin_pl[v, ..., 0, 0])
-        qnx = np.maximum(qnx, Qin_pl[v, ..., 1, 0])
+        qnm = _pymin(qnm, Qin_pl[v, ..., 0, 0])
+        qnx = _pymax(qnx, Qin_pl[v, ..., 1, 0])
     Ci = np.zeros_like(q_pl[0]); Co = np.zeros_like(q_pl[0])
     CQn = np.zeros_like(q_pl[0]); CQx = np.zeros_like(q_pl[0])
     for v in range(1, 6):
@@ -1461,6 +1462,14 @@ def horizontal_limiter(g, q_a, q_a_pl, q, q_pl, d, d_pl, ch, ch_pl, cmask, cmask
         a2 = clampout(q_a_pl[v], Qout_pl[v, ..., 1], Qout_pl[v, ..., 0])
         a3 = clampout(q_a_pl[v], Qout_pl[0, ..., 1], Qout_pl[0, ..., 0])
         q_a_pl[v] = cmv * a2 + (1.0 - cmv) * a3
+
+
+def _pymin(a, b):
+    return np.where(b < a, b, a)
+
+
+def _pymax(a, b):
+    return np.where(b > a, b, a)
 
 
 def _reduce(fn, arrs):

@@ -1,0 +1,135 @@
+"""The ``cuda`` backend object that stands in for the reference's ``Dyn``.
+
+pyNICAM-DC's driver calls, per step, ``dyn.dynamics_step(msc)`` and
+``dyn.forcing_step(msc)`` (pynicamdc/api.py:724-730), or
+``dyn.run_timeloop_chunk(msc, K)`` for fused chunks (api.py:697-699), and
+drains the device state with ``dyn.sync_prgvar_to_host(prgv, msc)`` before
+output and budgets (api.py:800, nhm/share/mod_embudget.py:68).  ``CudaDyn``
+offers the same methods with the same meaning:
+
+* ``dynamics_step(msc)`` -- one large step of ``Dyn.dynamics_step``
+  (nhm/dynamics/mod_dynamics.py:1725-2741) on the device; the host
+  ``prgv.PRG_var`` becomes stale (the reference's "drain only at output"
+  invariant, mod_dynamics.py:2693-2697);
+* ``run_timeloop_chunk(msc, K)`` -- K such steps (mod_dynamics.py:784);
+* ``sync_prgvar_to_host(prgv, msc)`` -- copy the device state into
+  ``prgv.PRG_var`` / ``prgv.PRG_var_pl`` in place (mod_dynamics.py:429-440);
+* ``assert_host_prgvar_synced(who)`` -- ``AssertionError`` on a stale host read
+  (mod_dynamics.py:460-468);
+* ``forcing_step(msc)`` -- a no-op for ``AF_TYPE = NONE`` like the reference
+  (mod_dynamics.py:597); other forcings are not part of this backend and raise.
+
+Geometry, metrics and operator coefficients are read once from the
+reference's setup services on ``msc`` (grd, gmtr, oprt, vmtr, bsst, comm, ...)
+and uploaded; the device keeps them for the run.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .runtime import NicamCuda
+
+
+def geo_from_msc(msc) -> dict:
+    """Collect the setup arrays of the reference's services into the flat
+    dict that ``NicamCuda`` uploads (attribute names kept)."""
+    m = msc
+    a = m.adm
+    g = dict(kall=a.ADM_kall, kmin=a.ADM_kmin, kmax=a.ADM_kmax, gall_1d=a.ADM_gall_1d, gmin=a.ADM_gmin,
+             gmax=a.ADM_gmax, lall=a.ADM_lall, have_sgp=np.asarray(a.ADM_have_sgp),
+             nq=m.prgv.PRG_var.shape[-1] - 6)
+    g["pntmask"] = np.asarray(m.ppm.pntmask)
+    c = m.cnst
+    g.update(GRAV=c.CONST_GRAV, Rdry=c.CONST_Rdry, CVdry=c.CONST_CVdry, CPdry=c.CONST_CPdry, Rvap=c.CONST_Rvap,
+             OHM=c.CONST_OHM, RADIUS=c.CONST_RADIUS, EPS=c.CONST_EPS, HUGE=c.CONST_HUGE, PRE00=c.CONST_PRE00)
+    g.update(rscale=m.grd.GRD_rscale, alpha=float(m.rcnf.NON_HYDRO_ALPHA), dtl=m.tim.TIME_dtl,
+             dts=m.tim.TIME_dts, hdiff_fact_rho=m.numf.hdiff_fact_rho)
+    Kh, dd = np.asarray(m.numf.Kh_coef), np.asarray(m.numf.divdamp_coef)
+    if not (np.all(Kh == Kh.flat[0]) and np.all(dd == dd.flat[0])):
+        raise NotImplementedError("cuda backend: only spatially uniform (DIRECT) diffusion coefficients")
+    g["Kh_coef"], g["divdamp_coef"] = float(Kh.flat[0]), float(dd.flat[0])
+    g["sstep"] = np.asarray(m.dyn.num_of_iteration_sstep[:m.dyn.num_of_iteration_lstep])
+    g["CVW"] = np.asarray(m.rcnf.CVW)
+    co = m.comm
+    g["copy_r2r"] = co.Copy_list_r2r[:, :int(co.Copy_info_r2r[co.I_size])].astype(np.int64)
+    g["copy_p2r"] = co.Copy_list_p2r[:, :int(co.Copy_info_p2r[co.I_size])].astype(np.int64)
+    g["copy_r2p"] = co.Copy_list_r2p[:, :int(co.Copy_info_r2p[co.I_size])].astype(np.int64)
+    g["copy_sgp"] = co.Singular_list[:, :int(co.Singular_info[co.I_size])].astype(np.int64)
+    for k, v in vars(m.vmtr).items():
+        if k.startswith("VMTR_") and isinstance(v, np.ndarray):
+            g[k] = v
+    for k in ("GRD_x", "GRD_x_pl", "GRD_xr", "GRD_xr_pl", "GRD_afact", "GRD_bfact", "GRD_cfact", "GRD_dfact",
+              "GRD_rdgz", "GRD_rdgzh"):
+        g[k] = getattr(m.grd, k)
+    for k in ("OPRT_coef_div", "OPRT_coef_grad", "OPRT_coef_lap", "OPRT_coef_intp", "OPRT_coef_diff"):
+        g[k] = getattr(m.oprt, k)
+        g[k + "_pl"] = getattr(m.oprt, k + "_pl")
+    for k in ("GMTR_t", "GMTR_a", "GMTR_p"):
+        g[k] = getattr(m.gmtr, k)
+        g[k + "_pl"] = getattr(m.gmtr, k + "_pl")
+    for k in ("rho_bs", "pre_bs", "tem_bs"):
+        g[k] = getattr(m.bsst, k)
+        g[k + "_pl"] = getattr(m.bsst, k + "_pl")
+    return {k: np.asarray(v) for k, v in g.items()}
+
+
+class CudaDyn:
+    """Device-resident replacement of the reference's ``Dyn`` step API."""
+
+    def __init__(self, msc=None, geo: dict = None, graph: bool = True):
+        if geo is None:
+            if msc is None:
+                raise ValueError("CudaDyn needs the reference services (msc) or a setup dict (geo)")
+            self._check_config(msc)
+            geo = geo_from_msc(msc)
+        self.core = NicamCuda(geo, graph=graph)
+        self._host_stale = False
+        self._device_valid = False
+
+    @staticmethod
+    def _check_config(msc):
+        r = msc.rcnf
+        if msc.tim.TIME_integ_type != "RK3":
+            raise NotImplementedError("cuda backend: RK3 time integration only")
+        if r.TRC_ADV_TYPE != "MIURA2004" or not r.THUBURN_LIM:
+            raise NotImplementedError("cuda backend: MIURA2004 tracer advection with Thuburn limiters only")
+        nf = msc.numf
+        if nf.lap_order_hdiff != 2 or nf.lap_order_divdamp != 2 or nf.NUMFILTER_DOrayleigh or \
+                nf.NUMFILTER_DOdivdamp_2d or nf.NUMFILTER_DOdivdamp_v or nf.NUMFILTER_DOhorizontaldiff_lap1 \
+                or nf.hdiff_nonlinear:
+            raise NotImplementedError("cuda backend: lap_order 2 hyperdiffusion/divdamp without Rayleigh, "
+                                      "2-D/vertical divdamp, lap1 or nonlinear diffusion")
+        if r.DYN_DIV_NUM != 1:
+            raise NotImplementedError("cuda backend: DYN_DIV_NUM = 1 only")
+
+    # -- the reference's step API -------------------------------------------
+    def dynamics_step(self, msc):
+        self._ensure_device(msc)
+        self.core.step(1)
+        self._host_stale = True
+
+    def run_timeloop_chunk(self, msc, K: int):
+        self._ensure_device(msc)
+        self.core.step(int(K))
+        self._host_stale = True
+
+    def forcing_step(self, msc):
+        if getattr(msc.rcnf, "AF_TYPE", "NONE") not in ("NONE", None):
+            raise NotImplementedError("cuda backend: artificial forcing is not on the device")
+
+    def sync_prgvar_to_host(self, prgv, msc=None):
+        if not self._device_valid:
+            return
+        self.core.download(prgv.PRG_var, prgv.PRG_var_pl)
+        self._host_stale = False
+
+    def assert_host_prgvar_synced(self, who: str = ""):
+        if self._host_stale:
+            raise AssertionError(f"host PRG_var read while the device state is newer ({who}); "
+                                 "call sync_prgvar_to_host first")
+
+    def _ensure_device(self, msc):
+        if not self._device_valid:
+            pv, pvp = msc.prgv.PRG_var, msc.prgv.PRG_var_pl
+            self.core.upload(np.ascontiguousarray(pv), np.ascontiguousarray(pvp))
+            self._device_valid = True

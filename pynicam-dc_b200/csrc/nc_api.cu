@@ -1,0 +1,1056 @@
+// C ABI, device memory, halo exchange and the orchestration of one NICAM-DC
+// large step (RK3 HEVI, pynicamdc/nhm/dynamics/mod_dynamics.py:1725-2741).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/nicam_cuda.h"
+#include "nc_tracer.cuh"
+
+using namespace nc;
+
+static thread_local std::string g_err;
+static int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+#define CU(call)                                                                                       \
+  do {                                                                                                 \
+    cudaError_t e_ = (call);                                                                           \
+    if (e_ != cudaSuccess) return fail(NC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define NC_MAXCOMM 8
+
+// ---------------------------------------------------------------------------
+// halo exchange: one gather from interior / pole sources into every halo cell
+// and the pole neighbour points (share/mod_comm.py:1563-1644 with the r2r,
+// p2r, r2p and singular lists composed on the host, so the copy is a single
+// race-free pass: no source is also a destination).
+// ---------------------------------------------------------------------------
+struct CommFields {
+  double* r[NC_MAXCOMM];
+  double* p[NC_MAXCOMM];
+  int n;
+};
+
+__global__ void k_comm(CommFields f, const long long* r_dst, const long long* r_src, int nr, const long long* p_dst,
+                       const long long* p_src, int np) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long ne = (long long)(nr + np) * cD.KA;
+  if (t >= ne) return;
+  int k = (int)(t % cD.KA);
+  int e = (int)(t / cD.KA);
+  const long long pl = cD.plane;
+  if (e < nr) {
+    long long d = r_dst[e];
+    long long di = ((d / pl) * cD.KA + k) * pl + d % pl;
+    long long s = r_src[e];
+    if (s >= 0) {
+      long long si = ((s / pl) * cD.KA + k) * pl + s % pl;
+      for (int n = 0; n < f.n; ++n) f.r[n][di] = f.r[n][si];
+    } else {
+      long long gp = -s - 1;   // g*LP + lp
+      int g = (int)(gp / cD.LP), lp = (int)(gp % cD.LP);
+      int pi = ipl(g, k, lp);
+      for (int n = 0; n < f.n; ++n) f.r[n][di] = f.p[n][pi];
+    }
+  } else {
+    e -= nr;
+    long long gp = p_dst[e];
+    int g = (int)(gp / cD.LP), lp = (int)(gp % cD.LP);
+    int pi = ipl(g, k, lp);
+    long long s = p_src[e];
+    long long si = ((s / pl) * cD.KA + k) * pl + s % pl;
+    for (int n = 0; n < f.n; ++n) f.p[n][pi] = f.r[n][si];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// marshal kernels: host layout (i,j,k,l,v) <-> per-variable [l][k][j][i]
+// ---------------------------------------------------------------------------
+struct VarPtrs {
+  double* v[NC_MAXNQ + 6];
+};
+
+__global__ void k_unpack(const double* st, const double* st_pl, VarPtrs reg, VarPtrs pol, int nv) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < cD.npt) {
+    int i = (int)(t % cD.G);
+    long long r = t / cD.G;
+    int j = (int)(r % cD.G);
+    r /= cD.G;
+    int k = (int)(r % cD.KA);
+    int l = (int)(r / cD.KA);
+    long long src = ((((long long)i * cD.G + j) * cD.KA + k) * cD.L + l) * nv;
+    for (int v = 0; v < nv; ++v) reg.v[v][t] = st[src + v];
+  } else if (t < cD.npt + cD.npl) {
+    int q = (int)(t - cD.npt);
+    for (int v = 0; v < nv; ++v) pol.v[v][q] = st_pl[(long long)q * nv + v];
+  }
+}
+
+__global__ void k_pack(double* st, double* st_pl, VarPtrs reg, VarPtrs pol, int nv) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < cD.npt) {
+    int i = (int)(t % cD.G);
+    long long r = t / cD.G;
+    int j = (int)(r % cD.G);
+    r /= cD.G;
+    int k = (int)(r % cD.KA);
+    int l = (int)(r / cD.KA);
+    long long dst = ((((long long)i * cD.G + j) * cD.KA + k) * cD.L + l) * nv;
+    for (int v = 0; v < nv; ++v) st[dst + v] = reg.v[v][t];
+  } else if (t < cD.npt + cD.npl) {
+    int q = (int)(t - cD.npt);
+    for (int v = 0; v < nv; ++v) st_pl[(long long)q * nv + v] = pol.v[v][q];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// global sums with Neumaier compensation (nhm/share/mod_embudget.py:74-80)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void neu_add(double& s, double& c, double x) {
+  double t = s + x;
+  if (fabs(s) >= fabs(x)) c += (s - t) + x;
+  else c += (x - t) + s;
+  s = t;
+}
+
+__global__ void k_mass(const double* rhog, const double* rhogq, const double* vol, const double* rhog_pl,
+                       const double* rhogq_pl, const double* vol_pl, double* part) {
+  // part[block*2 + {0,1}] = (sum, compensation) of rho*VOLUME (rhogq given: rho*q*VOLUME)
+  __shared__ double ss[256], sc[256];
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double s = 0.0, c = 0.0;
+  int i, j, l;
+  const double* num = rhogq ? rhogq : rhog;
+  if (col_of(t, i, j, l)) {
+    if (interior(i, j)) {
+      for (int k = cD.kmin; k <= cD.kmax; ++k) {
+        long long p = ix(i, j, k, l);
+        neu_add(s, c, num[p] / cG.GSGAM2[p] * vol[p]);
+      }
+    }
+  } else if (t - cD.npt2 < cD.LP) {
+    int lp = (int)(t - cD.npt2);
+    const double* nump = rhogq_pl ? rhogq_pl : rhog_pl;
+    for (int k = cD.kmin; k <= cD.kmax; ++k) {
+      int p = ipl(0, k, lp);
+      neu_add(s, c, nump[p] / cG.GSGAM2_pl[p] * vol_pl[p]);
+    }
+  }
+  ss[threadIdx.x] = s;
+  sc[threadIdx.x] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double S = 0.0, C = 0.0;
+    for (int n = 0; n < (int)blockDim.x; ++n) {
+      neu_add(S, C, ss[n]);
+      C += sc[n];
+    }
+    part[blockIdx.x * 2 + 0] = S;
+    part[blockIdx.x * 2 + 1] = C;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------
+struct FieldPair {
+  double* r = nullptr;
+  double* p = nullptr;
+};
+
+struct nc_handle {
+  Dims D{};
+  Consts C{};
+  Geom Gm{};
+  std::vector<void*> allocs;          // everything cudaMalloc'd
+  std::map<std::string, FieldPair> fields;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  bool use_graph = true;
+  bool have_state = false;
+  int sstep[4] = {0, 0, 0, 0};
+  int nstage = 0;
+  double dtl = 0, dts = 0;
+  // halo plan
+  long long *r_dst = nullptr, *r_src = nullptr, *p_dst = nullptr, *p_src = nullptr;
+  int nr = 0, np = 0;
+  // marshal staging
+  double *stage = nullptr, *stage_pl = nullptr;
+  double* mass_part = nullptr;
+  int mass_blocks = 0;
+  double* vol = nullptr;
+  double* vol_pl = nullptr;
+  long long launches = 0;
+  long long graph_kernels = 0;
+  int stop_phase = 0;   // debugging: end run_step after this many phases (0 = full step)
+  int phase = 0;
+  // state + work fields
+  FieldPair P[6], Pq[NC_MAXNQ], P0[6];
+  FieldPair pre, tem, vx, vy, vz, w, rho, ein, eth, pregd, rhogd, vv[3];
+  FieldPair gadv[4], vt[6], vt2[6], gT0[6], frhog;
+  FieldPair PSa[6], PSb[6], PM[5], vtmp2[3], gT[6], Mc, Mu, Ml, ethtot0, hdiv[3];
+  FieldPair flx_v, rhog_t, flx[6], xc[9], ch[6], cm[6], q, gq[3], qa[3], Qmin, Qmax;
+};
+
+static nc_handle* g_current = nullptr;   // handle whose constants are loaded
+
+static int dev_alloc(nc_handle* h, double** p, size_t n) {
+  CU(cudaMalloc((void**)p, n * sizeof(double)));
+  h->allocs.push_back(*p);
+  CU(cudaMemset(*p, 0, n * sizeof(double)));
+  return 0;
+}
+
+static int field(nc_handle* h, FieldPair& f, const char* name) {
+  int rc = dev_alloc(h, &f.r, (size_t)h->D.npt);
+  if (rc) return rc;
+  rc = dev_alloc(h, &f.p, (size_t)h->D.npl);
+  if (rc) return rc;
+  h->fields[name] = f;
+  return 0;
+}
+
+// ---- setup array lookup / layout conversion -------------------------------
+struct ArrTab {
+  std::map<std::string, const nc_array*> m;
+  const nc_array* get(const char* n) const {
+    auto it = m.find(n);
+    return it == m.end() ? nullptr : it->second;
+  }
+};
+
+static int64_t numel(const nc_array* a) {
+  int64_t n = 1;
+  for (int d = 0; d < a->ndim; ++d) n *= a->shape[d];
+  return n;
+}
+
+static int scalar(const ArrTab& T, const char* name, double& out) {
+  const nc_array* a = T.get(name);
+  if (!a || numel(a) < 1) return fail(NC_ERR_ARG, std::string("missing scalar ") + name);
+  if (a->dtype == NC_F64) out = ((const double*)a->data)[0];
+  else if (a->dtype == NC_I32) out = ((const int32_t*)a->data)[0];
+  else if (a->dtype == NC_I64) out = (double)((const int64_t*)a->data)[0];
+  else out = ((const uint8_t*)a->data)[0];
+  return 0;
+}
+
+// regional array (i, j, kk, l, trailing...) -> device [c][l][kk][j][i]
+static int up_reg(nc_handle* h, const ArrTab& T, const char* name, int kk, int ncomp, const double** out) {
+  const nc_array* a = T.get(name);
+  const Dims& D = h->D;
+  if (!a || a->dtype != NC_F64) return fail(NC_ERR_ARG, std::string("missing float64 array ") + name);
+  if (a->ndim < 4 || a->shape[0] != D.G || a->shape[1] != D.G || a->shape[2] != kk || a->shape[3] != D.L ||
+      numel(a) != (int64_t)D.G * D.G * kk * D.L * ncomp)
+    return fail(NC_ERR_ARG, std::string("bad shape of ") + name);
+  const double* src = (const double*)a->data;
+  size_t n = (size_t)numel(a);
+  std::vector<double> tmp(n);
+  for (int i = 0; i < D.G; ++i)
+    for (int j = 0; j < D.G; ++j)
+      for (int k = 0; k < kk; ++k)
+        for (int l = 0; l < D.L; ++l)
+          for (int c = 0; c < ncomp; ++c) {
+            size_t s = ((((size_t)i * D.G + j) * kk + k) * D.L + l) * ncomp + c;
+            size_t d = ((((size_t)c * D.L + l) * kk + k) * D.G + j) * D.G + i;
+            tmp[d] = src[s];
+          }
+  double* dp;
+  int rc = dev_alloc(h, &dp, n);
+  if (rc) return rc;
+  CU(cudaMemcpy(dp, tmp.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  *out = dp;
+  return 0;
+}
+
+// pole array uploaded in its own (reference) layout
+static int up_pl(nc_handle* h, const ArrTab& T, const char* name, int64_t expect, const double** out) {
+  const nc_array* a = T.get(name);
+  if (!a || a->dtype != NC_F64) return fail(NC_ERR_ARG, std::string("missing float64 array ") + name);
+  if (numel(a) != expect) return fail(NC_ERR_ARG, std::string("bad size of ") + name);
+  double* dp;
+  int rc = dev_alloc(h, &dp, (size_t)expect);
+  if (rc) return rc;
+  CU(cudaMemcpy(dp, a->data, (size_t)expect * sizeof(double), cudaMemcpyHostToDevice));
+  *out = dp;
+  return 0;
+}
+
+static int up_vec(const ArrTab& T, const char* name, int n, double* dst) {
+  const nc_array* a = T.get(name);
+  if (!a || a->dtype != NC_F64 || numel(a) != n) return fail(NC_ERR_ARG, std::string("bad 1-d array ") + name);
+  std::memcpy(dst, a->data, n * sizeof(double));
+  return 0;
+}
+
+static int load_consts(nc_handle* h) {
+  if (g_current == h) return 0;
+  CU(cudaMemcpyToSymbol(cD, &h->D, sizeof(Dims)));
+  CU(cudaMemcpyToSymbol(cC, &h->C, sizeof(Consts)));
+  CU(cudaMemcpyToSymbol(cG, &h->Gm, sizeof(Geom)));
+  g_current = h;
+  return 0;
+}
+
+#define TRY(x)            \
+  do {                    \
+    int rc_ = (x);        \
+    if (rc_) return rc_;  \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+static const int kBlock = 128;
+static unsigned grid_cols_kl(const nc_handle* h) {   // regional columns + (k, lp) pole threads
+  long long n = h->D.npt2 + (long long)h->D.KA * h->D.LP;
+  return (unsigned)((n + kBlock - 1) / kBlock);
+}
+
+static int check_launch(nc_handle* h, const char* what) {
+  h->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(NC_ERR_CUDA, std::string("launch ") + what + ": " + cudaGetErrorString(e));
+  return 0;
+}
+
+static int comm(nc_handle* h, std::initializer_list<FieldPair> fl) {
+  CommFields f{};
+  f.n = 0;
+  for (const FieldPair& p : fl) {
+    f.r[f.n] = p.r;
+    f.p[f.n] = p.p;
+    f.n++;
+  }
+  long long ne = (long long)(h->nr + h->np) * h->D.KA;
+  unsigned g = (unsigned)((ne + 255) / 256);
+  k_comm<<<g, 256, 0, h->stream>>>(f, h->r_dst, h->r_src, h->nr, h->p_dst, h->p_src, h->np);
+  return check_launch(h, "comm");
+}
+
+static Prog prog_reg(nc_handle* h) {
+  Prog p;
+  for (int v = 0; v < 6; ++v) p.v[v] = h->P[v].r;
+  return p;
+}
+static Prog prog_pl(nc_handle* h) {
+  Prog p;
+  for (int v = 0; v < 6; ++v) p.v[v] = h->P[v].p;
+  return p;
+}
+
+// ---------------------------------------------------------------------------
+// one large step (mod_dynamics.py:1725-2741, numpy path)
+// ---------------------------------------------------------------------------
+#define PHASE()                                                     \
+  do {                                                              \
+    if (h->stop_phase > 0 && ++h->phase >= h->stop_phase) return 0; \
+  } while (0)
+
+static int run_step(nc_handle* h) {
+  cudaStream_t s = h->stream;
+  h->phase = 0;
+  const Dims& D = h->D;
+  const unsigned gkl = grid_cols_kl(h);
+  const unsigned greg = (unsigned)((D.npt2 + kBlock - 1) / kBlock);
+  const unsigned plk = (unsigned)(((D.KA * D.LP) + 31) / 32 * 32);
+  const unsigned npt_blocks = (unsigned)((D.npt + kBlock - 1) / kBlock);
+  const unsigned npl_blocks = (unsigned)((D.npl + kBlock - 1) / kBlock);
+  // PROG0 = PROG at the start of the step (mod_dynamics.py:1939-1968)
+  for (int v = 0; v < 6; ++v) {
+    CU(cudaMemcpyAsync(h->P0[v].r, h->P[v].r, D.npt * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CU(cudaMemcpyAsync(h->P0[v].p, h->P[v].p, D.npl * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  }
+  for (int nl = 0; nl < h->nstage; ++nl) {
+    const bool last = (nl == h->nstage - 1);
+    // ---- Pre_Post
+    auto diag_args = [&](bool pole) {
+      DiagArgs a;
+      a.P = pole ? prog_pl(h) : prog_reg(h);
+      a.Pq0 = pole ? h->Pq[0].p : h->Pq[0].r;
+      auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
+      a.pre = F(h->pre); a.tem = F(h->tem); a.vx = F(h->vx); a.vy = F(h->vy); a.vz = F(h->vz); a.w = F(h->w);
+      a.rho = F(h->rho); a.ein = F(h->ein); a.eth = F(h->eth); a.pregd = F(h->pregd); a.rhogd = F(h->rhogd);
+      a.vvx = F(h->vv[0]); a.vvy = F(h->vv[1]); a.vvz = F(h->vv[2]);
+      return a;
+    };
+    // regional and pole columns: same kernel, launched with the matching pointers
+    k_diag<<<greg, kBlock, 0, s>>>(diag_args(false), 0);
+    TRY(check_launch(h, "diag"));
+    k_diag<<<1, 32, 0, s>>>(diag_args(true), 1);
+    TRY(check_launch(h, "diag_pl"));
+    PHASE();
+    // ---- momentum advection
+    AdvMomArgs am;
+    am.rg = h->P[0].r; am.rvx = h->P[1].r; am.rvy = h->P[2].r; am.rvz = h->P[3].r; am.rw = h->P[4].r;
+    am.vvx = h->vv[0].r; am.vvy = h->vv[1].r; am.vvz = h->vv[2].r;
+    am.gvx = h->gadv[0].r; am.gvy = h->gadv[1].r; am.gvz = h->gadv[2].r; am.gw = h->gadv[3].r;
+    k_advmom<<<greg, kBlock, 0, s>>>(am);
+    TRY(check_launch(h, "advmom"));
+    AdvMomArgs amp;
+    amp.rg = h->P[0].p; amp.rvx = h->P[1].p; amp.rvy = h->P[2].p; amp.rvz = h->P[3].p; amp.rw = h->P[4].p;
+    amp.vvx = h->vv[0].p; amp.vvy = h->vv[1].p; amp.vvz = h->vv[2].p;
+    amp.gvx = h->gadv[0].p; amp.gvy = h->gadv[1].p; amp.gvz = h->gadv[2].p; amp.gw = h->gadv[3].p;
+    k_advmom_pl<<<1, 32, 0, s>>>(amp);
+    TRY(check_launch(h, "advmom_pl"));
+    PHASE();
+    // ---- hyperdiffusion
+    Six src, srcp;
+    SixOut o1, o1p;
+    const FieldPair* sf[6] = {&h->vx, &h->vy, &h->vz, &h->w, &h->tem, &h->rho};
+    for (int n = 0; n < 6; ++n) {
+      src.f[n] = sf[n]->r; srcp.f[n] = sf[n]->p;
+      o1.f[n] = h->vt[n].r; o1p.f[n] = h->vt[n].p;
+    }
+    k_hdiff1<<<greg, kBlock, 0, s>>>(src, o1);
+    TRY(check_launch(h, "hdiff1"));
+    k_hdiff1_pl<<<1, plk, 0, s>>>(srcp, o1p);
+    TRY(check_launch(h, "hdiff1_pl"));
+    TRY(comm(h, {h->vt[0], h->vt[1], h->vt[2], h->vt[3], h->vt[4], h->vt[5]}));
+    PHASE();
+    Six vin, vinp;
+    SixOut o2, o2p;
+    for (int n = 0; n < 6; ++n) {
+      vin.f[n] = h->vt[n].r; vinp.f[n] = h->vt[n].p;
+      o2.f[n] = h->vt2[n].r; o2p.f[n] = h->vt2[n].p;
+    }
+    k_hdiff2<<<greg, kBlock, 0, s>>>(vin, h->P[0].r, o2);
+    TRY(check_launch(h, "hdiff2"));
+    k_hdiff2_pl<<<1, plk, 0, s>>>(vinp, h->P[0].p, o2p);
+    TRY(check_launch(h, "hdiff2_pl"));
+    TRY(comm(h, {h->vt2[0], h->vt2[1], h->vt2[2], h->vt2[3], h->vt2[4], h->vt2[5]}));
+    PHASE();
+    // ---- large-step tendency
+    for (int pole = 0; pole < 2; ++pole) {
+      GtendArgs ga;
+      auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
+      for (int n = 0; n < 6; ++n) { ga.vt2.f[n] = F(h->vt2[n]); ga.gT0[n] = F(h->gT0[n]); }
+      ga.rhog = F(h->P[0]); ga.gvx = F(h->gadv[0]); ga.gvy = F(h->gadv[1]); ga.gvz = F(h->gadv[2]);
+      ga.gw = F(h->gadv[3]); ga.frhog = F(h->frhog);
+      if (!pole) k_gtend<<<greg, kBlock, 0, s>>>(ga, 0);
+      else k_gtend<<<1, 32, 0, s>>>(ga, 1);
+      TRY(check_launch(h, "gtend"));
+    }
+    PHASE();
+    // ---- vi_small_step (mod_vi.py:104-1590)
+    k_split_init<<<npt_blocks, kBlock, 0, s>>>(h->P0[0].r, h->P0[1].r, h->P0[2].r, h->P0[3].r, h->P0[4].r,
+                                                h->P0[5].r, prog_reg(h), h->PSa[0].r, h->PSa[1].r, h->PSa[2].r,
+                                                h->PSa[3].r, h->PSa[4].r, h->PSa[5].r, h->PM[0].r, h->PM[1].r,
+                                                h->PM[2].r, h->PM[3].r, h->PM[4].r, D.npt, nl == 0);
+    TRY(check_launch(h, "split_init"));
+    k_split_init<<<npl_blocks, kBlock, 0, s>>>(h->P0[0].p, h->P0[1].p, h->P0[2].p, h->P0[3].p, h->P0[4].p,
+                                                h->P0[5].p, prog_pl(h), h->PSa[0].p, h->PSa[1].p, h->PSa[2].p,
+                                                h->PSa[3].p, h->PSa[4].p, h->PSa[5].p, h->PM[0].p, h->PM[1].p,
+                                                h->PM[2].p, h->PM[3].p, h->PM[4].p, D.npl, nl == 0);
+    TRY(check_launch(h, "split_init_pl"));
+    auto dd3d = [&](FieldPair* v4) -> int {
+      Four v, vp;
+      Three o, op;
+      for (int n = 0; n < 4; ++n) { v.f[n] = v4[n].r; vp.f[n] = v4[n].p; }
+      for (int d = 0; d < 3; ++d) { o.f[d] = h->vtmp2[d].r; op.f[d] = h->vtmp2[d].p; }
+      k_dd3d<<<greg, kBlock, 0, s>>>(v, o);
+      TRY(check_launch(h, "dd3d"));
+      k_dd3d_pl<<<1, plk, 0, s>>>(vp, op);
+      TRY(check_launch(h, "dd3d_pl"));
+      return comm(h, {h->vtmp2[0], h->vtmp2[1], h->vtmp2[2]});
+    };
+    {
+      FieldPair v4[4] = {h->P[1], h->P[2], h->P[3], h->P[4]};
+      TRY(dd3d(v4));
+    }
+    PHASE();
+    for (int pole = 0; pole < 2; ++pole) {
+      Vp0Args va;
+      auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
+      va.P = pole ? prog_pl(h) : prog_reg(h);
+      va.vx = F(h->vx); va.vy = F(h->vy); va.vz = F(h->vz); va.eth = F(h->eth); va.pregd = F(h->pregd);
+      va.rhogd = F(h->rhogd);
+      for (int d = 0; d < 3; ++d) va.vt.f[d] = F(h->vtmp2[d]);
+      for (int n = 0; n < 6; ++n) { va.gT0[n] = F(h->gT0[n]); va.gT[n] = F(h->gT[n]); }
+      va.Mc = F(h->Mc); va.Mu = F(h->Mu); va.Ml = F(h->Ml); va.ethtot0 = F(h->ethtot0);
+      va.dt = h->dts;
+      if (!pole) k_vp0<<<greg, kBlock, 0, s>>>(va, 0);
+      else k_vp0<<<1, 32, 0, s>>>(va, 1);
+      TRY(check_launch(h, "vp0"));
+    }
+    PHASE();
+    const int nitr = h->sstep[nl];
+    const double rweight = 1.0 / (double)nitr;
+    const double RovCV = h->C.Rdry / h->C.CVdry;
+    for (int ns = 0; ns < nitr; ++ns) {
+      FieldPair* PS = (ns % 2 == 0) ? h->PSa : h->PSb;     // current split values
+      FieldPair* PN = (ns % 2 == 0) ? h->PSb : h->PSa;     // next split values
+      {
+        FieldPair v4[4] = {PS[1], PS[2], PS[3], PS[4]};
+        TRY(dd3d(v4));
+      }
+      PHASE();
+      for (int pole = 0; pole < 2; ++pole) {
+        Path1Args pa;
+        auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
+        for (int n = 0; n < 6; ++n) { pa.PS[n] = F(PS[n]); pa.gT[n] = F(h->gT[n]); }
+        pa.rhog = F(h->P[0]);
+        for (int d = 0; d < 3; ++d) { pa.vt.f[d] = F(h->vtmp2[d]); pa.dvh[d] = F(PN[1 + d]); }
+        for (int n = 0; n < 5; ++n) pa.PM[n] = F(h->PM[n]);
+        pa.dt = h->dts; pa.rweight = rweight; pa.RovCV = RovCV;
+        if (!pole) k_path1<<<greg, kBlock, 0, s>>>(pa, 0);
+        else k_path1<<<1, 32, 0, s>>>(pa, 1);
+        TRY(check_launch(h, "path1"));
+      }
+      TRY(comm(h, {PN[1], PN[2], PN[3]}));
+      PHASE();
+      for (int pole = 0; pole < 2; ++pole) {
+        VimainArgs va;
+        auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
+        for (int n = 0; n < 6; ++n) { va.PS[n] = F(PS[n]); va.P[n] = F(h->P[n]); va.gT[n] = F(h->gT[n]); }
+        va.eth = F(h->eth); va.ethtot0 = F(h->ethtot0); va.gT0e = F(h->gT0[5]);
+        va.Mc = F(h->Mc); va.Mu = F(h->Mu); va.Ml = F(h->Ml);
+        for (int d = 0; d < 3; ++d) { va.dvh.f[d] = F(PN[1 + d]); va.hdiv[d] = F(h->hdiv[d]); }
+        va.dwe[0] = F(PN[0]); va.dwe[1] = F(PN[4]); va.dwe[2] = F(PN[5]);
+        va.PM0 = F(h->PM[0]); va.PM4 = F(h->PM[4]);
+        va.dt = h->dts; va.rweight = rweight; va.RovCV = RovCV;
+        if (!pole) {
+          k_vimain_a<<<greg, kBlock, 0, s>>>(va, 0);
+          TRY(check_launch(h, "vimain_a"));
+          k_vimain_b<<<greg, kBlock, 0, s>>>(va, 0);
+          TRY(check_launch(h, "vimain_b"));
+        } else {
+          k_vimain_a<<<1, plk, 0, s>>>(va, 1);
+          TRY(check_launch(h, "vimain_a_pl"));
+          k_vimain_b<<<1, 32, 0, s>>>(va, 1);
+          TRY(check_launch(h, "vimain_b_pl"));
+        }
+      }
+      TRY(comm(h, {PN[0], PN[4], PN[5]}));
+      PHASE();
+    }
+    FieldPair* PSf = (nitr % 2 == 0) ? h->PSa : h->PSb;
+    k_post<<<greg, kBlock, 0, s>>>(prog_reg(h), PSf[0].r, PSf[1].r, PSf[2].r, PSf[3].r, PSf[4].r, PSf[5].r, 0);
+    TRY(check_launch(h, "post"));
+    k_post<<<1, 32, 0, s>>>(prog_pl(h), PSf[0].p, PSf[1].p, PSf[2].p, PSf[3].p, PSf[4].p, PSf[5].p, 1);
+    TRY(check_launch(h, "post_pl"));
+    TRY(comm(h, {h->PM[0], h->PM[1], h->PM[2], h->PM[3], h->PM[4]}));
+    PHASE();
+    if (!last) {
+      TRY(comm(h, {h->P[0], h->P[1], h->P[2], h->P[3], h->P[4], h->P[5]}));
+      PHASE();
+      continue;
+    }
+    // ---- tracer advection (mod_src_tracer.py:83-1228)
+    const double dt = h->dtl;
+    for (int pole = 0; pole < 2; ++pole) {
+      TrcFluxArgs ta;
+      auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
+      ta.rvx = F(h->PM[1]); ta.rvy = F(h->PM[2]); ta.rvz = F(h->PM[3]); ta.rw = F(h->PM[4]);
+      ta.rhog_in = F(h->P0[0]); ta.frhog = F(h->frhog); ta.flx_v = F(h->flx_v); ta.rhog_t = F(h->rhog_t);
+      ta.dt = dt;
+      if (!pole) k_trc_vflux<<<greg, kBlock, 0, s>>>(ta, 0);
+      else k_trc_vflux<<<1, 32, 0, s>>>(ta, 1);
+      TRY(check_launch(h, "trc_vflux"));
+    }
+    auto vadv = [&](int iq, bool second) -> int {
+      for (int pole = 0; pole < 2; ++pole) {
+        TrcVadvArgs va;
+        auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
+        va.rhogq = F(h->Pq[iq]);
+        va.den = second ? F(h->rhog_t) : F(h->P0[0]);
+        va.flx_v = F(h->flx_v); va.frhog = F(h->frhog);
+        va.dt = dt; va.bcoef = 0.0; va.clamp = second ? 1 : 0; va.dtl = dt;
+        if (!pole) k_trc_vadv<<<greg, kBlock, 0, s>>>(va, 0);
+        else k_trc_vadv<<<1, 32, 0, s>>>(va, 1);
+        TRY(check_launch(h, "trc_vadv"));
+      }
+      return 0;
+    };
+    // first vertical step uses the density at the start of the step; the
+    // Courant numbers of the first step are those of rhog_in
+    for (int iq = 0; iq < D.nq; ++iq) TRY(vadv(iq, false));
+    PHASE();
+    {
+      TrcHfluxArgs ha;
+      ha.rho = h->PM[0].r; ha.rvx = h->PM[1].r; ha.rvy = h->PM[2].r; ha.rvz = h->PM[3].r; ha.rhog_t = h->rhog_t.r;
+      for (int f = 0; f < 6; ++f) { ha.flx[f] = h->flx[f].r; ha.ch[f] = h->ch[f].r; ha.cm[f] = h->cm[f].r; }
+      for (int f = 0; f < 9; ++f) ha.xc[f] = h->xc[f].r;
+      ha.dt = dt;
+      k_trc_hflux<<<greg, kBlock, 0, s>>>(ha);
+      TRY(check_launch(h, "trc_hflux"));
+      TrcHfluxPlArgs hp;
+      hp.rho = h->PM[0].p; hp.rvx = h->PM[1].p; hp.rvy = h->PM[2].p; hp.rvz = h->PM[3].p; hp.rhog_t = h->rhog_t.p;
+      hp.flx = h->flx[0].p; hp.xc = h->xc[0].p; hp.ch = h->ch[0].p; hp.cm = h->cm[0].p; hp.dt = dt;
+      k_trc_hflux_pl<<<1, plk, 0, s>>>(hp);
+      TRY(check_launch(h, "trc_hflux_pl"));
+    }
+    PHASE();
+    for (int iq = 0; iq < D.nq; ++iq) {
+      k_trc_grad<<<greg, kBlock, 0, s>>>(h->Pq[iq].r, h->rhog_t.r, h->q.r,
+                                                                               h->gq[0].r, h->gq[1].r, h->gq[2].r);
+      TRY(check_launch(h, "trc_grad"));
+      k_trc_grad_pl<<<1, plk, 0, s>>>(h->Pq[iq].p, h->rhog_t.p, h->q.p, h->gq[0].p, h->gq[1].p, h->gq[2].p);
+      TRY(check_launch(h, "trc_grad_pl"));
+      TRY(comm(h, {h->gq[0], h->gq[1], h->gq[2]}));
+      TrcRemapArgs ra;
+      ra.q = h->q.r; ra.gq0 = h->gq[0].r; ra.gq1 = h->gq[1].r; ra.gq2 = h->gq[2].r;
+      for (int f = 0; f < 9; ++f) ra.xc[f] = h->xc[f].r;
+      for (int f = 0; f < 6; ++f) ra.cm[f] = h->cm[f].r;
+      for (int f = 0; f < 3; ++f) ra.qa[f] = h->qa[f].r;
+      k_trc_remap<<<greg, kBlock, 0, s>>>(ra);
+      TRY(check_launch(h, "trc_remap"));
+      TrcRemapPlArgs rp;
+      rp.q = h->q.p; rp.gq0 = h->gq[0].p; rp.gq1 = h->gq[1].p; rp.gq2 = h->gq[2].p; rp.xc = h->xc[0].p;
+      rp.cm = h->cm[0].p; rp.qa = h->qa[0].p;
+      k_trc_remap_pl<<<1, plk, 0, s>>>(rp);
+      TRY(check_launch(h, "trc_remap_pl"));
+      TrcLimArgs la;
+      la.q = h->q.r; la.rhog_t = h->rhog_t.r; la.frhog = h->frhog.r;
+      for (int f = 0; f < 6; ++f) { la.ch[f] = h->ch[f].r; la.cm[f] = h->cm[f].r; la.flx[f] = h->flx[f].r; }
+      for (int f = 0; f < 3; ++f) la.qa[f] = h->qa[f].r;
+      la.qout_min = h->Qmin.r; la.qout_max = h->Qmax.r; la.Qmin = h->Qmin.r; la.Qmax = h->Qmax.r;
+      la.rhogq = h->Pq[iq].r; la.dt = dt;
+      TrcLimPlArgs lp;
+      lp.q = h->q.p; lp.ch = h->ch[0].p; lp.cm = h->cm[0].p; lp.rhog_t = h->rhog_t.p; lp.frhog = h->frhog.p;
+      lp.qa = h->qa[0].p; lp.flx = h->flx[0].p; lp.Qmin = h->Qmin.p; lp.Qmax = h->Qmax.p;
+      lp.qout_min = h->Qmin.p; lp.qout_max = h->Qmax.p; lp.rhogq = h->Pq[iq].p; lp.dt = dt;
+      k_trc_qout<<<greg, kBlock, 0, s>>>(la);
+      TRY(check_launch(h, "trc_qout"));
+      k_trc_qout_pl<<<1, plk, 0, s>>>(lp);
+      TRY(check_launch(h, "trc_qout_pl"));
+      TRY(comm(h, {h->Qmin, h->Qmax}));
+      k_trc_apply<<<greg, kBlock, 0, s>>>(la);
+      TRY(check_launch(h, "trc_apply"));
+      k_trc_apply_pl<<<1, plk, 0, s>>>(lp);
+      TRY(check_launch(h, "trc_apply_pl"));
+    }
+    PHASE();
+    k_trc_rhog<<<gkl, kBlock, 0, s>>>(h->rhog_t.r, h->flx[0].r, h->flx[1].r, h->flx[2].r, h->flx[3].r, h->flx[4].r,
+                                       h->flx[5].r, h->frhog.r, dt, h->flx[0].p, h->rhog_t.p, h->frhog.p);
+    TRY(check_launch(h, "trc_rhog"));
+    for (int iq = 0; iq < D.nq; ++iq) TRY(vadv(iq, true));
+    PHASE();
+  }
+  // marshal-out halo exchange of PRG_var (mod_dynamics.py:2726-2727)
+  {
+    CommFields f{};
+    int n = 0;
+    for (int v = 0; v < 6; ++v) { f.r[n] = h->P[v].r; f.p[n] = h->P[v].p; n++; }
+    for (int iq = 0; iq < D.nq && n < NC_MAXCOMM; ++iq) { f.r[n] = h->Pq[iq].r; f.p[n] = h->Pq[iq].p; n++; }
+    f.n = n;
+    long long ne = (long long)(h->nr + h->np) * D.KA;
+    k_comm<<<(unsigned)((ne + 255) / 256), 256, 0, s>>>(f, h->r_dst, h->r_src, h->nr, h->p_dst, h->p_src, h->np);
+    TRY(check_launch(h, "comm_final"));
+    for (int iq = NC_MAXCOMM - 6; iq < D.nq; ++iq) TRY(comm(h, {h->Pq[iq]}));
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* nc_last_error(void) { return g_err.c_str(); }
+
+int64_t nc_kernel_launches(nc_handle* h) { return h ? h->launches : 0; }
+
+static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
+  ArrTab T;
+  for (int n = 0; n < narrays; ++n) {
+    if (!arrays[n].name || !arrays[n].data) return fail(NC_ERR_ARG, "null array entry");
+    T.m[arrays[n].name] = &arrays[n];
+  }
+  double v;
+  Dims& D = h->D;
+  TRY(scalar(T, "gall_1d", v)); D.G = (int)v;
+  TRY(scalar(T, "kall", v)); D.KA = (int)v;
+  TRY(scalar(T, "lall", v)); D.L = (int)v;
+  TRY(scalar(T, "kmin", v)); D.kmin = (int)v;
+  TRY(scalar(T, "kmax", v)); D.kmax = (int)v;
+  TRY(scalar(T, "gmin", v)); D.gmin = (int)v;
+  TRY(scalar(T, "gmax", v)); D.gmax = (int)v;
+  TRY(scalar(T, "nq", v)); D.nq = (int)v;
+  D.LP = 2;
+  if (D.G < 4 || D.KA < 4 || D.KA > NC_MAXK || D.L < 1 || D.kmin != 1 || D.kmax != D.KA - 2 || D.gmin != 1 ||
+      D.gmax != D.G - 2 || D.nq < 1 || D.nq > NC_MAXNQ)
+    return fail(NC_ERR_ARG, "unsupported grid dimensions (need kmin=1, kmax=kall-2, 1<=nq<=32, kall<=128)");
+  D.plane = (long long)D.G * D.G;
+  D.npt = D.plane * D.KA * D.L;
+  D.npt2 = D.plane * D.L;
+  D.npl = 6 * D.KA * D.LP;
+  Consts& C = h->C;
+  TRY(scalar(T, "GRAV", C.GRAV)); TRY(scalar(T, "Rdry", C.Rdry)); TRY(scalar(T, "CVdry", C.CVdry));
+  TRY(scalar(T, "CPdry", C.CPdry)); TRY(scalar(T, "Rvap", C.Rvap)); TRY(scalar(T, "OHM", C.OHM));
+  TRY(scalar(T, "EPS", C.EPS)); TRY(scalar(T, "HUGE", C.HUGE_)); TRY(scalar(T, "rscale", C.rscale));
+  TRY(scalar(T, "alpha", C.alpha)); TRY(scalar(T, "Kh_coef", C.Kh)); TRY(scalar(T, "divdamp_coef", C.divdamp_coef));
+  TRY(scalar(T, "hdiff_fact_rho", C.hdiff_fact_rho));
+  TRY(scalar(T, "dtl", h->dtl)); TRY(scalar(T, "dts", h->dts));
+  {
+    const nc_array* cvw = T.get("CVW");
+    if (!cvw || cvw->dtype != NC_F64 || numel(cvw) < 1) return fail(NC_ERR_ARG, "missing CVW");
+    C.CVW0 = ((const double*)cvw->data)[0];
+    const nc_array* ss = T.get("sstep");
+    if (!ss || numel(ss) < 1 || numel(ss) > 4) return fail(NC_ERR_ARG, "missing sstep");
+    h->nstage = (int)numel(ss);
+    for (int n = 0; n < h->nstage; ++n) {
+      h->sstep[n] = (ss->dtype == NC_I64) ? (int)((const int64_t*)ss->data)[n] : (int)((const int32_t*)ss->data)[n];
+      if (h->sstep[n] < 1) return fail(NC_ERR_ARG, "sstep entries must be >= 1");
+    }
+  }
+  TRY(up_vec(T, "GRD_afact", D.KA, C.afact)); TRY(up_vec(T, "GRD_bfact", D.KA, C.bfact));
+  TRY(up_vec(T, "GRD_cfact", D.KA, C.cfact)); TRY(up_vec(T, "GRD_dfact", D.KA, C.dfact));
+  TRY(up_vec(T, "GRD_rdgz", D.KA, C.rdgz)); TRY(up_vec(T, "GRD_rdgzh", D.KA, C.rdgzh));
+  Geom& Gm = h->Gm;
+  const int KA = D.KA;
+  TRY(up_reg(h, T, "VMTR_GSGAM2", KA, 1, &Gm.GSGAM2));
+  TRY(up_reg(h, T, "VMTR_GSGAM2H", KA, 1, &Gm.GSGAM2H));
+  TRY(up_reg(h, T, "VMTR_RGSGAM2", KA, 1, &Gm.RGSGAM2));
+  TRY(up_reg(h, T, "VMTR_RGSGAM2H", KA, 1, &Gm.RGSGAM2H));
+  TRY(up_reg(h, T, "VMTR_RGSQRTH", KA, 1, &Gm.RGSQRTH));
+  TRY(up_reg(h, T, "VMTR_RGAM", KA, 1, &Gm.RGAM));
+  TRY(up_reg(h, T, "VMTR_RGAMH", KA, 1, &Gm.RGAMH));
+  TRY(up_reg(h, T, "VMTR_GAM2H", KA, 1, &Gm.GAM2H));
+  TRY(up_reg(h, T, "VMTR_PHI", KA, 1, &Gm.PHI));
+  TRY(up_reg(h, T, "VMTR_C2Wfact", KA, 2, &Gm.C2W));
+  TRY(up_reg(h, T, "VMTR_W2Cfact", KA, 2, &Gm.W2C));
+  TRY(up_reg(h, T, "VMTR_C2WfactGz", KA, 6, &Gm.C2WGz));
+  TRY(up_reg(h, T, "rho_bs", KA, 1, &Gm.rho_bs));
+  TRY(up_reg(h, T, "pre_bs", KA, 1, &Gm.pre_bs));
+  TRY(up_reg(h, T, "tem_bs", KA, 1, &Gm.tem_bs));
+  {
+    const double* vol;
+    TRY(up_reg(h, T, "VMTR_VOLUME", KA, 1, &vol));
+    h->vol = const_cast<double*>(vol);
+  }
+  TRY(up_reg(h, T, "OPRT_coef_div", 1, 21, &Gm.coef_div));
+  TRY(up_reg(h, T, "OPRT_coef_grad", 1, 21, &Gm.coef_grad));
+  TRY(up_reg(h, T, "OPRT_coef_lap", 1, 7, &Gm.coef_lap));
+  TRY(up_reg(h, T, "OPRT_coef_intp", 1, 18, &Gm.coef_intp));
+  TRY(up_reg(h, T, "OPRT_coef_diff", 1, 18, &Gm.coef_diff));
+  TRY(up_reg(h, T, "GRD_x", 1, 3, &Gm.GRD_x));
+  TRY(up_reg(h, T, "GRD_xr", 1, 9, &Gm.GRD_xr));
+  TRY(up_reg(h, T, "GMTR_t_W", 1, 6, &Gm.GMTR_t));
+  TRY(up_reg(h, T, "GMTR_a_HN", 1, 9, &Gm.GMTR_a));
+  TRY(up_reg(h, T, "GMTR_p_RAREA", 1, 1, &Gm.GMTR_p));
+  const int64_t npl = D.npl;
+  TRY(up_pl(h, T, "VMTR_GSGAM2_pl", npl, &Gm.GSGAM2_pl));
+  TRY(up_pl(h, T, "VMTR_GSGAM2H_pl", npl, &Gm.GSGAM2H_pl));
+  TRY(up_pl(h, T, "VMTR_RGSGAM2_pl", npl, &Gm.RGSGAM2_pl));
+  TRY(up_pl(h, T, "VMTR_RGSGAM2H_pl", npl, &Gm.RGSGAM2H_pl));
+  TRY(up_pl(h, T, "VMTR_RGSQRTH_pl", npl, &Gm.RGSQRTH_pl));
+  TRY(up_pl(h, T, "VMTR_RGAM_pl", npl, &Gm.RGAM_pl));
+  TRY(up_pl(h, T, "VMTR_RGAMH_pl", npl, &Gm.RGAMH_pl));
+  TRY(up_pl(h, T, "VMTR_GAM2H_pl", npl, &Gm.GAM2H_pl));
+  TRY(up_pl(h, T, "VMTR_PHI_pl", npl, &Gm.PHI_pl));
+  TRY(up_pl(h, T, "VMTR_C2Wfact_pl", npl * 2, &Gm.C2W_pl));
+  TRY(up_pl(h, T, "VMTR_W2Cfact_pl", npl * 2, &Gm.W2C_pl));
+  TRY(up_pl(h, T, "VMTR_C2WfactGz_pl", npl * 6, &Gm.C2WGz_pl));
+  TRY(up_pl(h, T, "rho_bs_pl", npl, &Gm.rho_bs_pl));
+  TRY(up_pl(h, T, "pre_bs_pl", npl, &Gm.pre_bs_pl));
+  TRY(up_pl(h, T, "tem_bs_pl", npl, &Gm.tem_bs_pl));
+  {
+    const double* vp;
+    TRY(up_pl(h, T, "VMTR_VOLUME_pl", npl, &vp));
+    h->vol_pl = const_cast<double*>(vp);
+  }
+  const int64_t gl = 6 * D.LP;
+  TRY(up_pl(h, T, "OPRT_coef_div_pl", gl * 3, &Gm.coef_div_pl));
+  TRY(up_pl(h, T, "OPRT_coef_grad_pl", gl * 3, &Gm.coef_grad_pl));
+  TRY(up_pl(h, T, "OPRT_coef_lap_pl", gl, &Gm.coef_lap_pl));
+  TRY(up_pl(h, T, "OPRT_coef_intp_pl", gl * 9, &Gm.coef_intp_pl));
+  TRY(up_pl(h, T, "OPRT_coef_diff_pl", gl * 3, &Gm.coef_diff_pl));
+  TRY(up_pl(h, T, "GRD_x_pl", gl * 3, &Gm.GRD_x_pl));
+  TRY(up_pl(h, T, "GRD_xr_pl", gl * 3, &Gm.GRD_xr_pl));
+  TRY(up_pl(h, T, "GMTR_t_pl", gl * 5, &Gm.GMTR_t_pl));
+  TRY(up_pl(h, T, "GMTR_a_pl", gl * 18, &Gm.GMTR_a_pl));
+  TRY(up_pl(h, T, "GMTR_p_pl", gl * 8, &Gm.GMTR_p_pl));
+  // integer tables
+  {
+    const nc_array* pm = T.get("pntmask");
+    if (!pm || numel(pm) != 2LL * D.L || (pm->dtype != NC_I32 && pm->dtype != NC_I64))
+      return fail(NC_ERR_ARG, "bad pntmask");
+    std::vector<int> tmp(2 * D.L);
+    for (int n = 0; n < 2 * D.L; ++n)
+      tmp[n] = pm->dtype == NC_I32 ? ((const int32_t*)pm->data)[n] : (int)((const int64_t*)pm->data)[n];
+    int* dp;
+    CU(cudaMalloc((void**)&dp, tmp.size() * sizeof(int)));
+    h->allocs.push_back(dp);
+    CU(cudaMemcpy(dp, tmp.data(), tmp.size() * sizeof(int), cudaMemcpyHostToDevice));
+    Gm.pntmask = dp;
+    const nc_array* sg = T.get("have_sgp");
+    if (!sg || numel(sg) != D.L) return fail(NC_ERR_ARG, "bad have_sgp");
+    std::vector<int> t2(D.L);
+    for (int n = 0; n < D.L; ++n)
+      t2[n] = sg->dtype == NC_BOOL ? ((const uint8_t*)sg->data)[n]
+                                   : (sg->dtype == NC_I32 ? ((const int32_t*)sg->data)[n] : (int)((const int64_t*)sg->data)[n]);
+    CU(cudaMalloc((void**)&dp, t2.size() * sizeof(int)));
+    h->allocs.push_back(dp);
+    CU(cudaMemcpy(dp, t2.data(), t2.size() * sizeof(int), cudaMemcpyHostToDevice));
+    Gm.have_sgp = dp;
+  }
+  // halo plan
+  {
+    const nc_array* a = T.get("halo_r_dst");
+    const nc_array* b = T.get("halo_r_src");
+    const nc_array* c = T.get("halo_p_dst");
+    const nc_array* d = T.get("halo_p_src");
+    if (!a || !b || !c || !d || a->dtype != NC_I64 || b->dtype != NC_I64 || c->dtype != NC_I64 || d->dtype != NC_I64 ||
+        numel(a) != numel(b) || numel(c) != numel(d))
+      return fail(NC_ERR_ARG, "bad halo plan");
+    h->nr = (int)numel(a);
+    h->np = (int)numel(c);
+    const nc_array* src[4] = {a, b, c, d};
+    long long** dst[4] = {&h->r_dst, &h->r_src, &h->p_dst, &h->p_src};
+    for (int n = 0; n < 4; ++n) {
+      size_t bytes = (size_t)std::max<int64_t>(numel(src[n]), 1) * sizeof(long long);
+      CU(cudaMalloc((void**)dst[n], bytes));
+      h->allocs.push_back(*dst[n]);
+      if (numel(src[n])) CU(cudaMemcpy(*dst[n], src[n]->data, numel(src[n]) * sizeof(long long), cudaMemcpyHostToDevice));
+    }
+  }
+  // state and work fields
+  char nm[32];
+  const char* pn[6] = {"RHOG", "RHOGVX", "RHOGVY", "RHOGVZ", "RHOGW", "RHOGE"};
+  for (int v = 0; v < 6; ++v) TRY(field(h, h->P[v], pn[v]));
+  for (int v = 0; v < D.nq; ++v) { snprintf(nm, sizeof nm, "RHOGQ.%d", v); TRY(field(h, h->Pq[v], nm)); }
+  for (int v = 0; v < 6; ++v) { snprintf(nm, sizeof nm, "PROG0.%d", v); TRY(field(h, h->P0[v], nm)); }
+  TRY(field(h, h->pre, "pre")); TRY(field(h, h->tem, "tem")); TRY(field(h, h->vx, "vx")); TRY(field(h, h->vy, "vy"));
+  TRY(field(h, h->vz, "vz")); TRY(field(h, h->w, "w")); TRY(field(h, h->rho, "rho")); TRY(field(h, h->ein, "ein"));
+  TRY(field(h, h->eth, "eth")); TRY(field(h, h->pregd, "pregd")); TRY(field(h, h->rhogd, "rhogd"));
+  for (int d = 0; d < 3; ++d) { snprintf(nm, sizeof nm, "vv.%d", d); TRY(field(h, h->vv[d], nm)); }
+  for (int d = 0; d < 4; ++d) { snprintf(nm, sizeof nm, "gadv.%d", d); TRY(field(h, h->gadv[d], nm)); }
+  for (int n = 0; n < 6; ++n) {
+    snprintf(nm, sizeof nm, "vt.%d", n); TRY(field(h, h->vt[n], nm));
+    snprintf(nm, sizeof nm, "vt2.%d", n); TRY(field(h, h->vt2[n], nm));
+    snprintf(nm, sizeof nm, "gT0.%d", n); TRY(field(h, h->gT0[n], nm));
+    snprintf(nm, sizeof nm, "gT.%d", n); TRY(field(h, h->gT[n], nm));
+    snprintf(nm, sizeof nm, "PSa.%d", n); TRY(field(h, h->PSa[n], nm));
+    snprintf(nm, sizeof nm, "PSb.%d", n); TRY(field(h, h->PSb[n], nm));
+  }
+  TRY(field(h, h->frhog, "frhog"));
+  for (int n = 0; n < 5; ++n) { snprintf(nm, sizeof nm, "PM.%d", n); TRY(field(h, h->PM[n], nm)); }
+  for (int d = 0; d < 3; ++d) {
+    snprintf(nm, sizeof nm, "vtmp2.%d", d); TRY(field(h, h->vtmp2[d], nm));
+    snprintf(nm, sizeof nm, "hdiv.%d", d); TRY(field(h, h->hdiv[d], nm));
+    snprintf(nm, sizeof nm, "gq.%d", d); TRY(field(h, h->gq[d], nm));
+    snprintf(nm, sizeof nm, "qa.%d", d); TRY(field(h, h->qa[d], nm));
+  }
+  TRY(field(h, h->Mc, "Mc")); TRY(field(h, h->Mu, "Mu")); TRY(field(h, h->Ml, "Ml"));
+  TRY(field(h, h->ethtot0, "ethtot0"));
+  TRY(field(h, h->flx_v, "flx_v")); TRY(field(h, h->rhog_t, "rhog_t")); TRY(field(h, h->q, "q"));
+  TRY(field(h, h->Qmin, "Qmin")); TRY(field(h, h->Qmax, "Qmax"));
+  for (int f = 0; f < 6; ++f) {
+    snprintf(nm, sizeof nm, "flx.%d", f); TRY(field(h, h->flx[f], nm));
+    snprintf(nm, sizeof nm, "ch.%d", f); TRY(field(h, h->ch[f], nm));
+    snprintf(nm, sizeof nm, "cm.%d", f); TRY(field(h, h->cm[f], nm));
+  }
+  for (int f = 0; f < 9; ++f) { snprintf(nm, sizeof nm, "xc.%d", f); TRY(field(h, h->xc[f], nm)); }
+  // the pole arrays of flx/ch/cm/xc/qa are single (g,k,l[,3]) arrays: make the
+  // first pole buffer of each family large enough for its (g,k,l,3) use
+  {
+    double* big;
+    TRY(dev_alloc(h, &big, (size_t)D.npl * 3));
+    h->xc[0].p = big;
+    h->fields["xc.0"] = h->xc[0];
+  }
+  TRY(dev_alloc(h, &h->stage, (size_t)D.npt * (6 + D.nq)));
+  TRY(dev_alloc(h, &h->stage_pl, (size_t)D.npl * (6 + D.nq)));
+  h->mass_blocks = (int)((D.npt2 + D.LP + 255) / 256);
+  TRY(dev_alloc(h, &h->mass_part, (size_t)h->mass_blocks * 2));
+  CU(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  return 0;
+}
+
+int nc_create(const nc_array* arrays, int32_t narrays, nc_handle** out) {
+  if (!out || !arrays || narrays <= 0) return fail(NC_ERR_ARG, "nc_create: null argument");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return fail(NC_ERR_CUDA, "no CUDA device");
+  nc_handle* h = new nc_handle();
+  int rc = create_impl(arrays, narrays, h);
+  if (rc) {
+    std::string keep = g_err;
+    nc_destroy(h);
+    g_err = keep;
+    return rc;
+  }
+  *out = h;
+  return 0;
+}
+
+void nc_destroy(nc_handle* h) {
+  if (!h) return;
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (void* p : h->allocs) cudaFree(p);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  if (g_current == h) g_current = nullptr;
+  delete h;
+}
+
+static VarPtrs state_ptrs(nc_handle* h, bool pole) {
+  VarPtrs v{};
+  for (int n = 0; n < 6; ++n) v.v[n] = pole ? h->P[n].p : h->P[n].r;
+  for (int n = 0; n < h->D.nq; ++n) v.v[6 + n] = pole ? h->Pq[n].p : h->Pq[n].r;
+  return v;
+}
+
+int nc_upload_state(nc_handle* h, const double* prg, const double* prg_pl) {
+  if (!h || !prg || !prg_pl) return fail(NC_ERR_ARG, "nc_upload_state: null argument");
+  TRY(load_consts(h));
+  const Dims& D = h->D;
+  const int nv = 6 + D.nq;
+  CU(cudaMemcpyAsync(h->stage, prg, (size_t)D.npt * nv * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CU(cudaMemcpyAsync(h->stage_pl, prg_pl, (size_t)D.npl * nv * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  long long n = D.npt + D.npl;
+  k_unpack<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->stage, h->stage_pl, state_ptrs(h, false),
+                                                                 state_ptrs(h, true), nv);
+  TRY(check_launch(h, "unpack"));
+  h->have_state = true;
+  return 0;
+}
+
+int nc_download_state(nc_handle* h, double* prg, double* prg_pl) {
+  if (!h || !prg || !prg_pl) return fail(NC_ERR_ARG, "nc_download_state: null argument");
+  if (!h->have_state) return fail(NC_ERR_STATE, "nc_download_state: no state uploaded");
+  TRY(load_consts(h));
+  const Dims& D = h->D;
+  const int nv = 6 + D.nq;
+  long long n = D.npt + D.npl;
+  k_pack<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->stage, h->stage_pl, state_ptrs(h, false),
+                                                               state_ptrs(h, true), nv);
+  TRY(check_launch(h, "pack"));
+  CU(cudaMemcpyAsync(prg, h->stage, (size_t)D.npt * nv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaMemcpyAsync(prg_pl, h->stage_pl, (size_t)D.npl * nv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int nc_set_graph(nc_handle* h, int32_t enable) {
+  if (!h) return fail(NC_ERR_ARG, "nc_set_graph: null handle");
+  h->use_graph = enable != 0;
+  return 0;
+}
+
+int nc_step(nc_handle* h, int32_t nsteps) {
+  if (!h || nsteps < 0) return fail(NC_ERR_ARG, "nc_step: bad argument");
+  if (!h->have_state) return fail(NC_ERR_STATE, "nc_step: no state uploaded");
+  TRY(load_consts(h));
+  if (!h->use_graph) {
+    for (int n = 0; n < nsteps; ++n) TRY(run_step(h));
+    return 0;
+  }
+  if (!h->gexec) {
+    long long before = h->launches;
+    CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = run_step(h);
+    cudaGraph_t g = nullptr;
+    cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ec != cudaSuccess) return fail(NC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+    h->graph = g;
+    CU(cudaGraphInstantiate(&h->gexec, h->graph, 0));
+    h->launches = before;
+    h->graph_kernels = 0;
+    {
+      size_t nn = 0;
+      CU(cudaGraphGetNodes(h->graph, nullptr, &nn));
+      std::vector<cudaGraphNode_t> nodes(nn);
+      CU(cudaGraphGetNodes(h->graph, nodes.data(), &nn));
+      for (auto& node : nodes) {
+        cudaGraphNodeType t;
+        CU(cudaGraphNodeGetType(node, &t));
+        if (t == cudaGraphNodeTypeKernel) h->graph_kernels++;
+      }
+    }
+  }
+  for (int n = 0; n < nsteps; ++n) {
+    CU(cudaGraphLaunch(h->gexec, h->stream));
+    h->launches += h->graph_kernels;
+  }
+  return 0;
+}
+
+int nc_run_phases(nc_handle* h, int32_t nphases) {
+  if (!h || nphases < 1) return fail(NC_ERR_ARG, "nc_run_phases: bad argument");
+  if (!h->have_state) return fail(NC_ERR_STATE, "nc_run_phases: no state uploaded");
+  TRY(load_consts(h));
+  h->stop_phase = nphases;
+  int rc = run_step(h);
+  h->stop_phase = 0;
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int nc_sync(nc_handle* h) {
+  if (!h) return fail(NC_ERR_ARG, "nc_sync: null handle");
+  CU(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int nc_mass_sums(nc_handle* h, double* out, int32_t nout) {
+  if (!h || !out || nout < 1) return fail(NC_ERR_ARG, "nc_mass_sums: bad argument");
+  if (!h->have_state) return fail(NC_ERR_STATE, "nc_mass_sums: no state uploaded");
+  TRY(load_consts(h));
+  std::vector<double> part((size_t)h->mass_blocks * 2);
+  for (int n = 0; n < nout && n <= h->D.nq; ++n) {
+    const double* num = n == 0 ? nullptr : h->Pq[n - 1].r;
+    const double* nump = n == 0 ? nullptr : h->Pq[n - 1].p;
+    k_mass<<<h->mass_blocks, 256, 0, h->stream>>>(h->P[0].r, num, h->vol, h->P[0].p, nump, h->vol_pl, h->mass_part);
+    TRY(check_launch(h, "mass"));
+    CU(cudaMemcpyAsync(part.data(), h->mass_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    double S = 0.0, Cc = 0.0;
+    for (int b = 0; b < h->mass_blocks; ++b) {
+      double x = part[b * 2];
+      double t = S + x;
+      if (std::fabs(S) >= std::fabs(x)) Cc += (S - t) + x;
+      else Cc += (x - t) + S;
+      S = t;
+      Cc += part[b * 2 + 1];
+    }
+    out[n] = S + Cc;
+  }
+  return 0;
+}
+
+int nc_get_field(nc_handle* h, const char* name, double* host_reg, double* host_pl) {
+  if (!h || !name) return fail(NC_ERR_ARG, "nc_get_field: null argument");
+  auto it = h->fields.find(name);
+  if (it == h->fields.end()) return fail(NC_ERR_ARG, std::string("unknown field ") + name);
+  TRY(load_consts(h));
+  const Dims& D = h->D;
+  CU(cudaStreamSynchronize(h->stream));
+  if (host_reg) {
+    std::vector<double> tmp((size_t)D.npt);
+    CU(cudaMemcpy(tmp.data(), it->second.r, D.npt * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int l = 0; l < D.L; ++l)
+      for (int k = 0; k < D.KA; ++k)
+        for (int j = 0; j < D.G; ++j)
+          for (int i = 0; i < D.G; ++i)
+            host_reg[(((size_t)i * D.G + j) * D.KA + k) * D.L + l] = tmp[(((size_t)l * D.KA + k) * D.G + j) * D.G + i];
+  }
+  if (host_pl) CU(cudaMemcpy(host_pl, it->second.p, D.npl * sizeof(double), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int nc_state_pointers(nc_handle* h, int32_t v, double** reg, double** pl) {
+  if (!h || v < 0 || v >= 6 + h->D.nq || !reg || !pl) return fail(NC_ERR_ARG, "nc_state_pointers: bad argument");
+  FieldPair f = v < 6 ? h->P[v] : h->Pq[v - 6];
+  *reg = f.r;
+  *pl = f.p;
+  return 0;
+}
+
+}  // extern "C"

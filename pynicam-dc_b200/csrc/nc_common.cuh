@@ -1,0 +1,133 @@
+// Device data model of the NICAM-DC dynamics step on one B200.
+//
+// Regional fields: one float64 array per variable, layout [l][k][j][i] with i
+// fastest (the Fortran/fio (gall, kall, lall) order, ij = j*gall_1d + i), so a
+// warp of threads on consecutive i issues coalesced 128-byte loads and the
+// 7-point hexagonal stencil touches rows j-1, j, j+1 of the same k-plane.
+// Horizontal (k-independent) coefficients: [c][l][j][i].  Pole fields keep the
+// reference's (g, k, l) C-order (g = 0 pole point, 1..5 its neighbours).
+//
+// Every kernel is a "column" kernel: one thread owns one (i, j, l) column and
+// walks k, so k-independent coefficients are loaded once into registers and
+// the vertical recurrences (Thomas solve, limiter) stay in registers.
+//
+// All arithmetic follows the float64 numpy reference op-for-op (same
+// association order, no FMA contraction: the library is built -fmad=false),
+// which is what makes the CUDA step bit-identical to the reference.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define NC_MAXK 128
+#define NC_MAXNQ 32
+
+namespace nc {
+
+struct Dims {
+  int G;      // gall_1d (region tile edge incl. 1-cell halo)
+  int KA;     // kall
+  int L;      // regions on this device
+  int LP;     // pole regions (2)
+  int kmin, kmax, gmin, gmax;
+  int nq;
+  long long plane;   // G*G
+  long long npt;     // L*KA*G*G
+  long long npt2;    // L*G*G
+  int npl;           // 6*KA*LP
+};
+
+// Physical / run constants (identical names to the reference's CONST_*).
+struct Consts {
+  double GRAV, Rdry, CVdry, CPdry, Rvap, OHM, EPS, HUGE_, rscale, alpha;
+  double Kh, divdamp_coef, hdiff_fact_rho, CVW0;
+  double afact[NC_MAXK], bfact[NC_MAXK], cfact[NC_MAXK], dfact[NC_MAXK];
+  double rdgz[NC_MAXK], rdgzh[NC_MAXK];
+};
+
+// Geometry on the device (all float64).  Regional 3-D metrics [l][k][j][i];
+// 2-D coefficient planes [c][l][j][i].  Pole arrays in reference layout.
+struct Geom {
+  // 3-D vertical metrics
+  const double *GSGAM2, *GSGAM2H, *RGSGAM2, *RGSGAM2H, *RGSQRTH, *RGAM, *RGAMH, *GAM2H, *PHI;
+  const double *C2W;     // 2 comps
+  const double *W2C;     // 2 comps
+  const double *C2WGz;   // 6 comps
+  const double *rho_bs, *pre_bs, *tem_bs;
+  // 2-D horizontal coefficients
+  const double *coef_div;   // 21 planes (d*7+m)
+  const double *coef_grad;  // 21 planes
+  const double *coef_lap;   // 7
+  const double *coef_intp;  // 18 planes ((d*3+p)*2+t)
+  const double *coef_diff;  // 18 planes (d*6+m)
+  const double *GRD_x;      // 3
+  const double *GRD_xr;     // 9 (face*3+d)
+  const double *GMTR_t;     // 6 (t*3 + (W-2))
+  const double *GMTR_a;     // 9 (face*3 + HN)
+  const double *GMTR_p;     // 1 (P_RAREA)
+  const int *pntmask;       // [l][2]
+  const int *have_sgp;      // [l]
+  // pole (reference layouts)
+  const double *GSGAM2_pl, *GSGAM2H_pl, *RGSGAM2_pl, *RGSGAM2H_pl, *RGSQRTH_pl, *RGAM_pl, *RGAMH_pl,
+      *GAM2H_pl, *PHI_pl;
+  const double *C2W_pl, *W2C_pl, *C2WGz_pl;   // (g,k,l,c)
+  const double *rho_bs_pl, *pre_bs_pl, *tem_bs_pl;
+  const double *coef_div_pl;   // (g,l,3)
+  const double *coef_grad_pl;  // (g,l,3)
+  const double *coef_lap_pl;   // (g,l)
+  const double *coef_intp_pl;  // (g,l,3,3)
+  const double *coef_diff_pl;  // (g,l,3)
+  const double *GRD_x_pl;      // (g,l,3)
+  const double *GRD_xr_pl;     // (g,l,3)
+  const double *GMTR_t_pl;     // (g,l,5)
+  const double *GMTR_a_pl;     // (g,l,18)
+  const double *GMTR_p_pl;     // (g,l,8)
+};
+
+// The library is one translation unit (nc_api.cu includes every kernel
+// header), so the constant-memory symbols are defined here.
+__constant__ Dims cD;
+__constant__ Consts cC;
+__constant__ Geom cG;
+
+// ---- indexing -------------------------------------------------------------
+__device__ __forceinline__ long long ix(int i, int j, int k, int l) {
+  return (((long long)l * cD.KA + k) * cD.G + j) * cD.G + i;
+}
+__device__ __forceinline__ long long ix2(int c, int i, int j, int l) {
+  return (((long long)c * cD.L + l) * cD.G + j) * cD.G + i;
+}
+// pole (g, k, l)
+__device__ __forceinline__ int ipl(int g, int k, int lp) { return (g * cD.KA + k) * cD.LP + lp; }
+// pole (g, k, l, c) with nc comps
+__device__ __forceinline__ int iplc(int g, int k, int lp, int c, int ncomp) {
+  return ((g * cD.KA + k) * cD.LP + lp) * ncomp + c;
+}
+// 3-D metric component c of a multi-component regional metric
+__device__ __forceinline__ double M3(const double* a, int c, int i, int j, int k, int l) {
+  return a[(long long)c * cD.npt + ix(i, j, k, l)];
+}
+__device__ __forceinline__ double P2(const double* a, int c, int i, int j, int l) { return a[ix2(c, i, j, l)]; }
+
+// 7-point neighbour offsets in the reference's coefficient order:
+// (i,j) (i+1,j) (i+1,j+1) (i,j+1) (i-1,j) (i-1,j-1) (i,j-1)
+__device__ __constant__ static const int kNbI[7] = {0, 1, 1, 0, -1, -1, 0};
+__device__ __constant__ static const int kNbJ[7] = {0, 0, 1, 1, 0, -1, -1};
+
+__device__ __forceinline__ bool interior(int i, int j) {
+  return i >= 1 && i <= cD.G - 2 && j >= 1 && j <= cD.G - 2;
+}
+
+// Column thread mapping: thread -> (i, j, l).  Returns false for surplus threads.
+__device__ __forceinline__ bool col_of(long long t, int& i, int& j, int& l) {
+  if (t >= cD.npt2) return false;
+  i = (int)(t % cD.G);
+  long long r = t / cD.G;
+  j = (int)(r % cD.G);
+  l = (int)(r / cD.G);
+  return true;
+}
+
+__device__ __forceinline__ double dmin(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ double dmax(double a, double b) { return fmax(a, b); }
+
+}  // namespace nc

@@ -1,0 +1,501 @@
+// Large-step kernels of one RK stage: diagnostics + boundary conditions,
+// momentum advection, hyperdiffusion and the large-step tendency.
+#pragma once
+#include "nc_ops.cuh"
+
+namespace nc {
+
+// Field bundles (device pointers, one array per variable)
+struct Prog { double* v[6]; };   // RHOG, RHOGVX, RHOGVY, RHOGVZ, RHOGW, RHOGE
+
+// ---------------------------------------------------------------------------
+// Pre_Post: diagnostics (kernels/diag.py:53-143), BNDCND_all
+// (share/mod_bndcnd.py:182-264 with kernels/bndcnd.py), th/eth and the
+// deviations (mod_dynamics.py:1043-1057), then the merged velocity of the
+// momentum advection (kernels/advconvmom.py:54-78).  One thread per column,
+// regional and pole columns alike.
+// ---------------------------------------------------------------------------
+struct DiagArgs {
+  Prog P;               // in/out (ghost rows written)
+  const double* Pq0;    // first tracer (water vapour)
+  double *pre, *tem, *vx, *vy, *vz, *w, *rho, *ein, *eth, *pregd, *rhogd;
+  double *vvx, *vvy, *vvz;
+};
+
+__device__ void diag_column(const Col c, const Met m, const DiagArgs& a, double gx, double gy, double gz) {
+  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
+  double** P = const_cast<double**>(a.P.v);
+  for (int k = 0; k < KA; ++k) {
+    long long p = c.at(k);
+    double RHOG = P[0][p];
+    double rho = RHOG / m.GSGAM2[p];
+    a.vx[p] = P[1][p] / RHOG;
+    a.vy[p] = P[2][p] / RHOG;
+    a.vz[p] = P[3][p] / RHOG;
+    double ein = P[5][p] / RHOG;
+    double q0 = a.Pq0[p] / RHOG;
+    double qd = 1.0 - q0;
+    double cv = q0 * cC.CVW0 + qd * cC.CVdry;
+    double tem = ein / cv;
+    a.tem[p] = tem;
+    a.pre[p] = rho * tem * (qd * cC.Rdry + q0 * cC.Rvap);
+    a.rho[p] = rho;
+    a.ein[p] = ein;
+    if (k >= kmin + 1 && k <= kmax) {
+      long long pm = c.at(k - 1);
+      a.w[p] = P[4][p] / (mc(m.C2W, c, 0, 2, k) * RHOG + mc(m.C2W, c, 1, 2, k) * P[0][pm]);
+    }
+  }
+  // ---- boundary conditions: TEM top/bottom, FREE top, RIGID bottom
+  const long long pT = c.at(kmax + 1), pK = c.at(kmax), pKm = c.at(kmax - 1);
+  const long long pB = c.at(kmin - 1), pN = c.at(kmin), pNp = c.at(kmin + 1);
+  double tem_top = a.tem[pK];
+  double tem_btm = a.tem[pN];
+  double pre_top = a.pre[pKm] - a.rho[pK] * (m.PHI[pT] - m.PHI[pKm]);
+  double pre_btm = a.pre[pNp] - a.rho[pN] * (m.PHI[pB] - m.PHI[pNp]);
+  double rho_top = pre_top / (cC.Rdry * tem_top);
+  double rho_btm = pre_btm / (cC.Rdry * tem_btm);
+  a.tem[pT] = tem_top; a.tem[pB] = tem_btm;
+  a.pre[pT] = pre_top; a.pre[pB] = pre_btm;
+  a.rho[pT] = rho_top; a.rho[pB] = rho_btm;
+  double rgT = rho_top * m.GSGAM2[pT];
+  double rgB = rho_btm * m.GSGAM2[pB];
+  P[0][pT] = rgT; P[0][pB] = rgB;
+  double einT = cC.CVdry * tem_top, einB = cC.CVdry * tem_btm;
+  a.ein[pT] = einT; a.ein[pB] = einB;
+  P[5][pT] = rgT * einT; P[5][pB] = rgB * einB;
+  double rgK = P[0][pK], rgN = P[0][pN];
+  double vT[3], vB[3];
+  for (int d = 0; d < 3; ++d) {
+    vT[d] = 1.0 * (P[1 + d][pK] / rgK) * rgT;
+    vB[d] = -1.0 * (P[1 + d][pN] / rgN) * rgB;
+    P[1 + d][pT] = vT[d];
+    P[1 + d][pB] = vB[d];
+  }
+  double* dv[3] = {a.vx, a.vy, a.vz};
+  for (int d = 0; d < 3; ++d) {
+    dv[d][pT] = P[1 + d][pT] / P[0][pT];
+    dv[d][pB] = P[1 + d][pB] / P[0][pB];
+  }
+  const int kT = kmax + 1;
+  double rwT = -(mc(m.C2WGz, c, 0, 6, kT) * vT[0] + mc(m.C2WGz, c, 1, 6, kT) * P[1][pK] +
+                 mc(m.C2WGz, c, 2, 6, kT) * vT[1] + mc(m.C2WGz, c, 3, 6, kT) * P[2][pK] +
+                 mc(m.C2WGz, c, 4, 6, kT) * vT[2] + mc(m.C2WGz, c, 5, 6, kT) * P[3][pK]);
+  P[4][pT] = rwT;
+  P[4][pN] = 0.0;
+  P[4][pB] = 0.0;
+  a.w[pT] = rwT / (mc(m.C2W, c, 0, 2, kT) * rgT + mc(m.C2W, c, 1, 2, kT) * rgK);
+  a.w[pN] = P[4][pN] / (mc(m.C2W, c, 0, 2, kmin) * rgN + mc(m.C2W, c, 1, 2, kmin) * rgB);
+  a.w[pB] = 0.0;
+  // ---- eth, deviations, merged velocity
+  for (int k = 0; k < KA; ++k) {
+    long long p = c.at(k);
+    double pre = a.pre[p], rho = a.rho[p];
+    a.eth[p] = a.ein[p] + pre / rho;
+    a.pregd[p] = (pre - m.pre_bs[p]) * m.GSGAM2[p];
+    a.rhogd[p] = (rho - m.rho_bs[p]) * m.GSGAM2[p];
+    if (k >= kmin && k <= kmax) {
+      double wc = cC.cfact[k] * a.w[c.at(k + 1)] + cC.dfact[k] * a.w[p];
+      a.vvx[p] = a.vx[p] + wc * gx / cC.rscale;
+      a.vvy[p] = a.vy[p] + wc * gy / cC.rscale;
+      a.vvz[p] = a.vz[p] + wc * gz / cC.rscale;
+    } else {
+      a.vvx[p] = 0.0; a.vvy[p] = 0.0; a.vvz[p] = 0.0;
+    }
+  }
+}
+
+__global__ void k_diag(DiagArgs a, int pole) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l, g, lp;
+  if (!map_col(pole, t, i, j, l, g, lp)) return;
+  if (!pole) {
+    diag_column(col_reg(i, j, l), met_of(false), a, P2(cG.GRD_x, 0, i, j, l), P2(cG.GRD_x, 1, i, j, l),
+                P2(cG.GRD_x, 2, i, j, l));
+  } else {
+    const double* X = cG.GRD_x_pl;
+    diag_column(col_pl(g, lp), met_of(true), a, X[(g * cD.LP + lp) * 3 + 0], X[(g * cD.LP + lp) * 3 + 1],
+                X[(g * cD.LP + lp) * 3 + 2]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Momentum advection convergence + Coriolis + horizontalize
+// (mod_src.py:96-497, kernels/advconv.py:42-108, fluxconv.py:111-208,
+// advconvmom.py:111-194).  Outputs grhogv{x,y,z}, grhogw.
+// ---------------------------------------------------------------------------
+struct AdvMomArgs {
+  const double *rg, *rvx, *rvy, *rvz, *rw;    // PROG (post BNDCND)
+  const double *vvx, *vvy, *vvz;              // merged velocity
+  double *gvx, *gvy, *gvz, *gw;               // out
+};
+
+// regional: flux convergence of the scaled fluxes rhogv*scl at level k
+template <class SCL>
+__device__ __forceinline__ double advconv_reg(int i, int j, int k, int l, const Col& c, const Met& m,
+                                              const double* rvx, const double* rvy, const double* rvz,
+                                              const double* rw, SCL scl) {
+  double div = 0.0;
+  if (interior(i, j)) {
+    div = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) -> double {
+      long long q = ix(ii, jj, kk, l);
+      const double* rv = (d == 0) ? rvx : ((d == 1) ? rvy : rvz);
+      return (rv[q] * scl(q, kk)) * cG.RGAM[q];
+    });
+  }
+  auto vmh = [&](int kk) -> double {
+    if (kk <= cD.kmin || kk > cD.kmax) return 0.0;
+    double h = vmh_horiz(c, m, kk, [&](int k2, int d) -> double {
+      long long q = c.at(k2);
+      const double* rv = (d == 0) ? rvx : ((d == 1) ? rvy : rvz);
+      return rv[q] * scl(q, k2);
+    });
+    long long q = c.at(kk);
+    double sw = rw[q] * (cC.afact[kk] * scl(q, kk) + cC.bfact[kk] * scl(c.at(kk - 1), kk - 1));
+    return h + 1.0 * sw * m.RGSQRTH[q];
+  };
+  return -div - (vmh(k + 1) - vmh(k)) * cC.rdgz[k];
+}
+
+__global__ void k_advmom(AdvMomArgs a) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (!col_of(t, i, j, l)) return;
+  const Col c = col_reg(i, j, l);
+  const Met m = met_of(false);
+  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
+  const double r = cC.rscale;
+  const double gx = P2(cG.GRD_x, 0, i, j, l) / r, gy = P2(cG.GRD_x, 1, i, j, l) / r, gz = P2(cG.GRD_x, 2, i, j, l) / r;
+  double gwc_prev = 0.0;
+  for (int k = 0; k < KA; ++k) {
+    long long p = c.at(k);
+    if (k < kmin || k > kmax) {
+      a.gvx[p] = 0.0; a.gvy[p] = 0.0; a.gvz[p] = 0.0; a.gw[p] = 0.0;
+      continue;
+    }
+    double dv[3];
+    const double* vv[3] = {a.vvx, a.vvy, a.vvz};
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+      const double* sc = vv[s];
+      dv[s] = advconv_reg(i, j, k, l, c, m, a.rvx, a.rvy, a.rvz, a.rw,
+                          [&](long long q, int) -> double { return sc[q]; });
+    }
+    double rh = a.rg[p];
+    double dvx = dv[0] - (-2.0 * rh * (cC.OHM * a.vvy[p]));
+    double dvy = dv[1] - (2.0 * rh * (cC.OHM * a.vvx[p]));
+    double dvz = dv[2];
+    double prd = dvx * gx + dvy * gy + dvz * gz;
+    a.gvx[p] = dvx - prd * gx;
+    a.gvy[p] = dvy - prd * gy;
+    a.gvz[p] = dvz - prd * gz;
+    double gwc = prd * cC.alpha;
+    a.gw[p] = (k >= kmin + 1) ? (mc(m.C2W, c, 0, 2, k) * gwc + mc(m.C2W, c, 1, 2, k) * gwc_prev) : 0.0;
+    gwc_prev = gwc;
+  }
+}
+
+// pole part of the momentum advection (one thread per pole column (g, lp))
+__device__ double advconv_pl_at(int g, int lp, int k, const Col& c, const Met& m, const double* rvx,
+                                const double* rvy, const double* rvz, const double* rw, const double* scl) {
+  double div = 0.0;
+  if (g == 0) {
+    const double* cd = cG.coef_div_pl;
+    double row = 0.0;
+    for (int v = 0; v < 6; ++v) {
+      int q = ipl(v, k, lp);
+      double vx = (rvx[q] * scl[q]) * cG.RGAM_pl[q];
+      double vy = (rvy[q] * scl[q]) * cG.RGAM_pl[q];
+      double vz = (rvz[q] * scl[q]) * cG.RGAM_pl[q];
+      double pv = cd[(v * cD.LP + lp) * 3 + 0] * vx + cd[(v * cD.LP + lp) * 3 + 1] * vy +
+                  cd[(v * cD.LP + lp) * 3 + 2] * vz;
+      row = (v == 0) ? pv : row + pv;
+    }
+    div = row;
+  }
+  auto vmh = [&](int kk) -> double {
+    if (kk <= cD.kmin || kk > cD.kmax) return 0.0;
+    double h = vmh_horiz(c, m, kk, [&](int k2, int d) -> double {
+      long long q = c.at(k2);
+      const double* rv = (d == 0) ? rvx : ((d == 1) ? rvy : rvz);
+      return rv[q] * scl[q];
+    });
+    long long q = c.at(kk);
+    double sw = rw[q] * (cC.afact[kk] * scl[q] + cC.bfact[kk] * scl[c.at(kk - 1)]);
+    return h + 1.0 * sw * m.RGSQRTH[q];
+  };
+  return -div - (vmh(k + 1) - vmh(k)) * cC.rdgz[k];
+}
+
+__global__ void k_advmom_pl(AdvMomArgs a) {
+  int t = threadIdx.x;
+  if (t >= 6 * cD.LP) return;
+  int g = t / cD.LP, lp = t % cD.LP;
+  const Col c = col_pl(g, lp);
+  const Met m = met_of(true);
+  const double r = cC.rscale;
+  const double* X = cG.GRD_x_pl;
+  const double gx = X[(g * cD.LP + lp) * 3 + 0] / r, gy = X[(g * cD.LP + lp) * 3 + 1] / r,
+               gz = X[(g * cD.LP + lp) * 3 + 2] / r;
+  double gwc_prev = 0.0;
+  for (int k = 0; k < cD.KA; ++k) {
+    long long p = c.at(k);
+    if (k < cD.kmin || k > cD.kmax) {
+      a.gvx[p] = 0.0; a.gvy[p] = 0.0; a.gvz[p] = 0.0; a.gw[p] = 0.0;
+      continue;
+    }
+    double dv[3];
+    const double* vv[3] = {a.vvx, a.vvy, a.vvz};
+    for (int s = 0; s < 3; ++s) dv[s] = advconv_pl_at(g, lp, k, c, m, a.rvx, a.rvy, a.rvz, a.rw, vv[s]);
+    double rh = a.rg[p];
+    double dvx = dv[0] - (-2.0 * rh * (cC.OHM * a.vvy[p]));
+    double dvy = dv[1] - (2.0 * rh * (cC.OHM * a.vvx[p]));
+    double dvz = dv[2];
+    double prd = dvx * gx + dvy * gy + dvz * gz;
+    a.gvx[p] = dvx - prd * gx;
+    a.gvy[p] = dvy - prd * gy;
+    a.gvz[p] = dvz - prd * gz;
+    double gwc = prd * cC.alpha;
+    a.gw[p] = (k >= cD.kmin + 1) ? (mc(m.C2W, c, 0, 2, k) * gwc + mc(m.C2W, c, 1, 2, k) * gwc_prev) : 0.0;
+    gwc_prev = gwc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Hyperdiffusion (mod_numfilter.py:845-1469, lap_order 2, DIRECT).
+// Pass 1: vt = -lap(src), src = (vx, vy, vz, w, tem - tem_bs, rho - rho_bs).
+// Pass 2: vt2 = -(lap of comps 0..3, kh-weighted diffusion of comps 4, 5).
+// ---------------------------------------------------------------------------
+struct Six { const double* f[6]; };
+struct SixOut { double* f[6]; };
+
+__global__ void k_hdiff1(Six src, SixOut out) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (!col_of(t, i, j, l)) return;
+  const bool in = interior(i, j);
+  for (int k = 0; k < cD.KA; ++k) {
+    long long p = ix(i, j, k, l);
+#pragma unroll
+    for (int n = 0; n < 6; ++n) {
+      double v = 0.0;
+      if (in) {
+        const double* s = src.f[n];
+        if (n == 4) {
+          v = lap7(i, j, k, l, [&](int ii, int jj, int kk) {
+            long long q = ix(ii, jj, kk, l);
+            return s[q] - cG.tem_bs[q];
+          });
+        } else if (n == 5) {
+          v = lap7(i, j, k, l, [&](int ii, int jj, int kk) {
+            long long q = ix(ii, jj, kk, l);
+            return s[q] - cG.rho_bs[q];
+          });
+        } else {
+          v = lap7(i, j, k, l, [&](int ii, int jj, int kk) { return s[ix(ii, jj, kk, l)]; });
+        }
+      }
+      out.f[n][p] = -v;
+    }
+  }
+}
+
+__global__ void k_hdiff1_pl(Six src, SixOut out) {
+  int t = threadIdx.x;
+  if (t >= cD.KA * cD.LP) return;
+  int k = t / cD.LP, lp = t % cD.LP;
+  for (int n = 0; n < 6; ++n) {
+    double row = 0.0;
+    for (int v = 0; v < 6; ++v) {
+      int q = ipl(v, k, lp);
+      double s = src.f[n][q];
+      if (n == 4) s = s - cG.tem_bs_pl[q];
+      if (n == 5) s = s - cG.rho_bs_pl[q];
+      double tv = cG.coef_lap_pl[v * cD.LP + lp] * s;
+      row = (v == 0) ? tv : row + tv;
+    }
+    out.f[n][ipl(0, k, lp)] = -row;
+    for (int g = 1; g < 6; ++g) out.f[n][ipl(g, k, lp)] = -0.0;
+  }
+}
+
+// kh-weighted diffusion at one interior point (kernels/oprtdiffusion.py:59-134)
+// KH(ii,jj) returns the diffusion coefficient field at (ii,jj,k).
+template <class S, class KH>
+__device__ double diffusion_at(int i, int j, int k, int l, S scl, KH kh) {
+  // vertex values tTI/tTJ at (ii,jj) for the three directions
+  auto tvert = [&](int ii, int jj, double tti[3], double ttj[3]) {
+    double s0 = scl(ii, jj), sip = scl(ii + 1, jj), sd = scl(ii + 1, jj + 1), sjp = scl(ii, jj + 1);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      double c1i = P2(cG.coef_intp, (d * 3 + 0) * 2 + 0, ii, jj, l);
+      double c2i = P2(cG.coef_intp, (d * 3 + 1) * 2 + 0, ii, jj, l);
+      double c3i = P2(cG.coef_intp, (d * 3 + 2) * 2 + 0, ii, jj, l);
+      double c1j = P2(cG.coef_intp, (d * 3 + 0) * 2 + 1, ii, jj, l);
+      double c2j = P2(cG.coef_intp, (d * 3 + 1) * 2 + 1, ii, jj, l);
+      double c3j = P2(cG.coef_intp, (d * 3 + 2) * 2 + 1, ii, jj, l);
+      tti[d] = ((2.0 * c1i - c2i - c3i) * s0 + (-c1i + 2.0 * c2i - c3i) * sip + (-c1i - c2i + 2.0 * c3i) * sd) / 3.0;
+      ttj[d] = ((2.0 * c1j - c2j - c3j) * s0 + (-c1j + 2.0 * c2j - c3j) * sd + (-c1j - c2j + 2.0 * c3j) * sjp) / 3.0;
+    }
+    if (ii == 0 && jj == 0) {  // singular-point fix (kernels/oprtdiffusion.py:91-96)
+      double m0 = (double)cG.pntmask[l * 2 + 0], m1 = (double)cG.pntmask[l * 2 + 1];
+      double s0b = scl(1, 0), sipb = scl(2, 0), sdb = scl(2, 1), sjpb = scl(1, 1);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double c1j = P2(cG.coef_intp, (d * 3 + 0) * 2 + 1, 1, 0, l);
+        double c2j = P2(cG.coef_intp, (d * 3 + 1) * 2 + 1, 1, 0, l);
+        double c3j = P2(cG.coef_intp, (d * 3 + 2) * 2 + 1, 1, 0, l);
+        double tj10 = ((2.0 * c1j - c2j - c3j) * s0b + (-c1j + 2.0 * c2j - c3j) * sdb + (-c1j - c2j + 2.0 * c3j) * sjpb) / 3.0;
+        (void)sipb;
+        tti[d] = tti[d] * m0 + tj10 * m1;
+      }
+    }
+  };
+  double aTI[3], aTJ[3], bTI[3], bTJ[3], cTI[3], cTJ[3], dTI[3], dTJ[3];
+  tvert(i, j, aTI, aTJ);
+  tvert(i - 1, j, bTI, bTJ);
+  tvert(i - 1, j - 1, cTI, cTJ);
+  tvert(i, j - 1, dTI, dTJ);
+  double kh0 = kh(i, j);
+  double kf1 = 0.5 * (kh0 + kh(i + 1, j + 1));
+  double kf2 = 0.5 * (kh0 + kh(i, j + 1));
+  double kf3 = 0.5 * (kh0 + kh(i - 1, j));
+  double kf4 = 0.5 * (kh0 + kh(i - 1, j - 1));
+  double kf5 = 0.5 * (kh0 + kh(i, j - 1));
+  double kf6 = 0.5 * (kh0 + kh(i + 1, j));
+  double inner = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double cd0 = P2(cG.coef_diff, d * 6 + 0, i, j, l), cd1 = P2(cG.coef_diff, d * 6 + 1, i, j, l),
+           cd2 = P2(cG.coef_diff, d * 6 + 2, i, j, l), cd3 = P2(cG.coef_diff, d * 6 + 3, i, j, l),
+           cd4 = P2(cG.coef_diff, d * 6 + 4, i, j, l), cd5 = P2(cG.coef_diff, d * 6 + 5, i, j, l);
+    double blk = kf1 * cd0 * (aTI[d] + aTJ[d]) + kf2 * cd1 * (aTJ[d] + bTI[d]) + kf3 * cd2 * (bTI[d] + cTJ[d]) +
+                 kf4 * cd3 * (cTJ[d] + cTI[d]) + kf5 * cd4 * (cTI[d] + dTJ[d]) + kf6 * cd5 * (dTJ[d] + aTI[d]);
+    inner = (d == 0) ? blk : inner + blk;
+  }
+  return inner;
+}
+
+__global__ void k_hdiff2(Six vt, const double* rhog, SixOut out) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (!col_of(t, i, j, l)) return;
+  const bool in = interior(i, j);
+  const double Kh = cC.Kh;
+  for (int k = 0; k < cD.KA; ++k) {
+    long long p = ix(i, j, k, l);
+    for (int n = 0; n < 6; ++n) {
+      double v = 0.0;
+      if (in) {
+        const double* s = vt.f[n];
+        auto S = [&](int ii, int jj) { return s[ix(ii, jj, k, l)]; };
+        if (n < 4) {
+          v = lap7(i, j, k, l, [&](int ii, int jj, int kk) { return s[ix(ii, jj, kk, l)]; });
+        } else if (n == 4) {
+          v = diffusion_at(i, j, k, l, S, [&](int ii, int jj) { return rhog[ix(ii, jj, k, l)] * cC.CVdry * Kh; });
+        } else {
+          v = diffusion_at(i, j, k, l, S,
+                           [&](int ii, int jj) { return rhog[ix(ii, jj, k, l)] * cC.hdiff_fact_rho * Kh; });
+        }
+      }
+      out.f[n][p] = -v;
+    }
+  }
+}
+
+__global__ void k_hdiff2_pl(Six vt, const double* rhog, SixOut out) {
+  int t = threadIdx.x;
+  if (t >= cD.KA * cD.LP) return;
+  int k = t / cD.LP, lp = t % cD.LP;
+  const double Kh = cC.Kh;
+  for (int n = 0; n < 6; ++n) {
+    const double* s = vt.f[n];
+    double row = 0.0;
+    if (n < 4) {
+      for (int v = 0; v < 6; ++v) {
+        double tv = cG.coef_lap_pl[v * cD.LP + lp] * s[ipl(v, k, lp)];
+        row = (v == 0) ? tv : row + tv;
+      }
+    } else {
+      // kernels/oprtdiffusion.py:137-177
+      const double fac = (n == 4) ? cC.CVdry : cC.hdiff_fact_rho;
+      double sn = s[ipl(0, k, lp)];
+      double vt_[5][3];
+      for (int v = 1; v <= 5; ++v) {
+        int vp1 = (v == 5) ? 1 : v + 1;
+        double sij = s[ipl(v, k, lp)], sp1 = s[ipl(vp1, k, lp)];
+        for (int d = 0; d < 3; ++d) {
+          const double* cI = cG.coef_intp_pl + ((v * cD.LP + lp) * 3 + d) * 3;
+          double c0 = cI[0], c1 = cI[1], c2 = cI[2];
+          vt_[v - 1][d] = ((2.0 * c0 - c1 - c2) * sn + (-c0 + 2.0 * c1 - c2) * sij + (-c0 - c1 + 2.0 * c2) * sp1) / 3.0;
+        }
+      }
+      double khn = rhog[ipl(0, k, lp)] * fac * Kh;
+      for (int v = 1; v <= 5; ++v) {
+        int vm1 = (v == 1) ? 5 : v - 1;
+        double khv = rhog[ipl(v, k, lp)] * fac * Kh;
+        double kavg = 0.5 * (khn + khv);
+        double sd = 0.0;
+        for (int d = 0; d < 3; ++d) {
+          double cdv = cG.coef_diff_pl[(v * cD.LP + lp) * 3 + d];
+          double tv = cdv * (vt_[vm1 - 1][d] + vt_[v - 1][d]);
+          sd = (d == 0) ? tv : sd + tv;
+        }
+        double contrib = kavg * sd;
+        row = (v == 1) ? contrib : row + contrib;
+      }
+    }
+    out.f[n][ipl(0, k, lp)] = -row;
+    for (int g = 1; g < 6; ++g) out.f[n][ipl(g, k, lp)] = -0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Large-step tendency: hyperdiffusion tendency (mod_numfilter.py:1519-1578)
+// + horizontalize (mod_numfilter.py:1364-1369) + g_TEND = adv + f
+// (mod_dynamics.py:1340-1464).  All columns; projection on interior points.
+// ---------------------------------------------------------------------------
+struct GtendArgs {
+  Six vt2;                       // post-COMM hyperdiffusion Laplacians
+  const double *rhog, *gvx, *gvy, *gvz, *gw;
+  double* gT0[6];
+  double* frhog;                 // f_TEND[RHOG] (tracer input)
+};
+
+__device__ void gtend_column(const Col c, const Met m, const GtendArgs& a, int i, int j, int l, int g, int lp) {
+  const double Kh = cC.Kh;
+  for (int k = 0; k < cD.KA; ++k) {
+    long long p = c.at(k);
+    double rg = a.rhog[p];
+    double rgh = 0.0;
+    if (k >= cD.kmin) rgh = mc(m.C2W, c, 0, 2, k) * rg + mc(m.C2W, c, 1, 2, k) * a.rhog[c.at(k - 1)];
+    double fx = -(a.vt2.f[0][p] * Kh + 0.0) * rg;
+    double fy = -(a.vt2.f[1][p] * Kh + 0.0) * rg;
+    double fz = -(a.vt2.f[2][p] * Kh + 0.0) * rg;
+    double fw = -(a.vt2.f[3][p] * Kh + 0.0) * rgh;
+    double fe = -(a.vt2.f[4][p] + 0.0);
+    double fr = -(a.vt2.f[5][p] + 0.0);
+    if (!c.pole) {
+      if (interior(i, j)) horiz_reg(i, j, l, fx, fy, fz);
+    } else {
+      horiz_pl(g, lp, fx, fy, fz);
+    }
+    a.gT0[0][p] = 0.0 + fr;
+    a.gT0[1][p] = a.gvx[p] + fx;
+    a.gT0[2][p] = a.gvy[p] + fy;
+    a.gT0[3][p] = a.gvz[p] + fz;
+    a.gT0[4][p] = a.gw[p] + fw;
+    a.gT0[5][p] = 0.0 + fe;
+    a.frhog[p] = fr;
+  }
+}
+
+__global__ void k_gtend(GtendArgs a, int pole) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l, g, lp;
+  if (!map_col(pole, t, i, j, l, g, lp)) return;
+  if (!pole) gtend_column(col_reg(i, j, l), met_of(false), a, i, j, l, 0, 0);
+  else gtend_column(col_pl(g, lp), met_of(true), a, 0, 0, 0, g, lp);
+}
+
+}  // namespace nc

@@ -1,0 +1,178 @@
+// Point/column building blocks shared by the dynamics kernels.  Each function
+// restates one reference expression with the reference's association order
+// (pynicamdc/nhm/dynamics/kernels/*.py); comments cite the file:line.
+#pragma once
+#include "nc_common.cuh"
+
+namespace nc {
+
+// numpy elementwise minimum/maximum: on ties the second operand is returned
+__device__ __forceinline__ double npmin(double a, double b) { return (a < b) ? a : b; }
+__device__ __forceinline__ double npmax(double a, double b) { return (a > b) ? a : b; }
+// Python builtin min/max: on ties the first operand is kept
+__device__ __forceinline__ double pymin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double pymax(double a, double b) { return (b > a) ? b : a; }
+
+// Column accessor: value index = base + k*ks.  Regional columns use
+// base = ix(i,j,0,l), ks = G*G; pole columns base = g*KA*LP + lp, ks = LP.
+// Multi-component metrics: regional comp c lives at c*npt + idx, pole comps are
+// interleaved (idx*nc + c).
+struct Col {
+  long long base, ks;
+  bool pole;
+  __device__ __forceinline__ long long at(int k) const { return base + (long long)k * ks; }
+};
+
+__device__ __forceinline__ Col col_reg(int i, int j, int l) {
+  Col c;
+  c.base = ix(i, j, 0, l);
+  c.ks = cD.plane;
+  c.pole = false;
+  return c;
+}
+__device__ __forceinline__ Col col_pl(int g, int lp) {
+  Col c;
+  c.base = (long long)g * cD.KA * cD.LP + lp;
+  c.ks = cD.LP;
+  c.pole = true;
+  return c;
+}
+
+// Thread -> column for a launch over regional columns (pole == 0) or over the
+// 6*LP pole columns (pole != 0).  The caller passes pointers of the matching kind.
+__device__ __forceinline__ bool map_col(int pole, long long t, int& i, int& j, int& l, int& g, int& lp) {
+  if (!pole) {
+    g = lp = 0;
+    return col_of(t, i, j, l);
+  }
+  if (t >= 6 * cD.LP) return false;
+  g = (int)(t / cD.LP);
+  lp = (int)(t % cD.LP);
+  i = j = l = 0;
+  return true;
+}
+
+// Metric selection by column kind
+struct Met {
+  const double *GSGAM2, *GSGAM2H, *RGSGAM2, *RGSGAM2H, *RGSQRTH, *RGAM, *RGAMH, *GAM2H, *PHI;
+  const double *C2W, *W2C, *C2WGz, *rho_bs, *pre_bs, *tem_bs;
+};
+__device__ __forceinline__ Met met_of(bool pole) {
+  Met m;
+  if (!pole) {
+    m.GSGAM2 = cG.GSGAM2; m.GSGAM2H = cG.GSGAM2H; m.RGSGAM2 = cG.RGSGAM2; m.RGSGAM2H = cG.RGSGAM2H;
+    m.RGSQRTH = cG.RGSQRTH; m.RGAM = cG.RGAM; m.RGAMH = cG.RGAMH; m.GAM2H = cG.GAM2H; m.PHI = cG.PHI;
+    m.C2W = cG.C2W; m.W2C = cG.W2C; m.C2WGz = cG.C2WGz;
+    m.rho_bs = cG.rho_bs; m.pre_bs = cG.pre_bs; m.tem_bs = cG.tem_bs;
+  } else {
+    m.GSGAM2 = cG.GSGAM2_pl; m.GSGAM2H = cG.GSGAM2H_pl; m.RGSGAM2 = cG.RGSGAM2_pl;
+    m.RGSGAM2H = cG.RGSGAM2H_pl; m.RGSQRTH = cG.RGSQRTH_pl; m.RGAM = cG.RGAM_pl; m.RGAMH = cG.RGAMH_pl;
+    m.GAM2H = cG.GAM2H_pl; m.PHI = cG.PHI_pl; m.C2W = cG.C2W_pl; m.W2C = cG.W2C_pl; m.C2WGz = cG.C2WGz_pl;
+    m.rho_bs = cG.rho_bs_pl; m.pre_bs = cG.pre_bs_pl; m.tem_bs = cG.tem_bs_pl;
+  }
+  return m;
+}
+// component c (of nc) of a multi-component metric at column level k
+__device__ __forceinline__ double mc(const double* a, const Col& c, int comp, int ncomp, int k) {
+  return c.pole ? a[c.at(k) * ncomp + comp] : a[(long long)comp * cD.npt + c.at(k)];
+}
+
+// ---- horizontal 7-point operators (regional, interior (i,j) only) ---------
+
+// divergence of (vx,vy,vz) at (i,j,k,l) given a functor returning the three
+// components at a neighbour: kernels/fluxconv.py:52-78
+template <class F>
+__device__ __forceinline__ double div7(int i, int j, int k, int l, F vel) {
+  double acc[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double s = 0.0;
+#pragma unroll
+    for (int m = 0; m < 7; ++m) {
+      double v = vel(i + kNbI[m], j + kNbJ[m], k, d);
+      double t = P2(cG.coef_div, d * 7 + m, i, j, l) * v;
+      s = (m == 0) ? t : s + t;
+    }
+    acc[d] = s;
+  }
+  return acc[0] + acc[1] + acc[2];
+}
+
+// gradient components (kernels/oprtgradient.py:45-70): np.sum over the 7
+// stencil points, left to right
+template <class F>
+__device__ __forceinline__ void grad7(int i, int j, int k, int l, F scl, double out[3]) {
+  double s[7];
+#pragma unroll
+  for (int m = 0; m < 7; ++m) s[m] = scl(i + kNbI[m], j + kNbJ[m], k);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double a = P2(cG.coef_grad, d * 7 + 0, i, j, l) * s[0];
+#pragma unroll
+    for (int m = 1; m < 7; ++m) a = a + P2(cG.coef_grad, d * 7 + m, i, j, l) * s[m];
+    out[d] = a;
+  }
+}
+
+// laplacian (kernels/oprtlaplacian.py:41-55)
+template <class F>
+__device__ __forceinline__ double lap7(int i, int j, int k, int l, F scl) {
+  double a = P2(cG.coef_lap, 0, i, j, l) * scl(i, j, k);
+#pragma unroll
+  for (int m = 1; m < 7; ++m) a = a + P2(cG.coef_lap, m, i, j, l) * scl(i + kNbI[m], j + kNbJ[m], k);
+  return a;
+}
+
+// tangent-plane projection of one vector at an interior point
+// (kernels/horizontalizevec.py:51-54)
+__device__ __forceinline__ void horiz_reg(int i, int j, int l, double& vx, double& vy, double& vz) {
+  const double r = cC.rscale;
+  double gx = P2(cG.GRD_x, 0, i, j, l), gy = P2(cG.GRD_x, 1, i, j, l), gz = P2(cG.GRD_x, 2, i, j, l);
+  double prd = (vx * gx + vy * gy + vz * gz) / r;
+  double nx = vx - prd * gx / r;
+  double ny = vy - prd * gy / r;
+  double nz = vz - prd * gz / r;
+  vx = nx; vy = ny; vz = nz;
+}
+// pole projection (kernels/horizontalizevec.py:67-71)
+__device__ __forceinline__ void horiz_pl(int g, int lp, double& vx, double& vy, double& vz) {
+  const double r = cC.rscale;
+  const double* X = cG.GRD_x_pl;
+  double gx = X[(g * cD.LP + lp) * 3 + 0], gy = X[(g * cD.LP + lp) * 3 + 1], gz = X[(g * cD.LP + lp) * 3 + 2];
+  double prd = vx * gx / r + vy * gy / r + vz * gz / r;
+  double nx = vx - prd * gx / r;
+  double ny = vy - prd * gy / r;
+  double nz = vz - prd * gz / r;
+  vx = nx; vy = ny; vz = nz;
+}
+
+// ---- vertical pieces ------------------------------------------------------
+
+// horizontal part of the half-level mass flux (kernels/fluxconv.py:142-151):
+// (sum of C2WfactGz * fluxes at k, k-1) * RGAMH(k)
+template <class F>
+__device__ __forceinline__ double vmh_horiz(const Col& c, const Met& m, int k, F flux) {
+  double h = mc(m.C2WGz, c, 0, 6, k) * flux(k, 0) + mc(m.C2WGz, c, 1, 6, k) * flux(k - 1, 0) +
+             mc(m.C2WGz, c, 2, 6, k) * flux(k, 1) + mc(m.C2WGz, c, 3, 6, k) * flux(k - 1, 1) +
+             mc(m.C2WGz, c, 4, 6, k) * flux(k, 2) + mc(m.C2WGz, c, 5, 6, k) * flux(k - 1, 2);
+  return h * m.RGAMH[c.at(k)];
+}
+
+// total kinetic energy rhogkin at level k of one column (kernels/rhogkin.py:38-79)
+template <class F>
+__device__ __forceinline__ double rhogkin_at(const Col& c, const Met& m, int k, F st) {
+  // st(k, comp): comp 0 rhog, 1..3 rhogv{x,y,z}, 4 rhogw
+  const int kmin = cD.kmin, kmax = cD.kmax;
+  if (k < kmin || k > kmax) return 0.0;
+  double rg = st(k, 0), vx = st(k, 1), vy = st(k, 2), vz = st(k, 3);
+  double kh = 0.5 * (vx * vx + vy * vy + vz * vz) / rg;
+  auto vint = [&](int kk) -> double {  // defined for kk in kmin+1..kmax, zero at kmin and kmax+1
+    if (kk <= kmin || kk > kmax) return 0.0;
+    double den = mc(m.C2W, c, 0, 2, kk) * st(kk, 0) + mc(m.C2W, c, 1, 2, kk) * st(kk - 1, 0);
+    double w = st(kk, 4);
+    return 0.5 * (w * w) / den;
+  };
+  return kh + mc(m.W2C, c, 0, 2, k) * vint(k + 1) + mc(m.W2C, c, 1, 2, k) * vint(k);
+}
+
+}  // namespace nc

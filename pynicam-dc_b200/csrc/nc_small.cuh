@@ -1,0 +1,676 @@
+// HEVI small-step kernels: 3-D/2-D divergence damping, pressure gradient,
+// vp0 source terms + tridiagonal matrix, the acoustic-loop path1 update and
+// vi_main (flux convergences + Thomas solve + energy update).
+#pragma once
+#include "nc_large.cuh"
+
+namespace nc {
+
+// ---------------------------------------------------------------------------
+// 3-D divergence damping operator (kernels/oprt3ddivdamp.py:85-173)
+// ---------------------------------------------------------------------------
+struct Four { const double* f[4]; };   // rhogvx, rhogvy, rhogvz, rhogw
+struct Three { double* f[3]; };
+struct CThree { const double* f[3]; };
+
+// half-level vertical mass flux rhogw_vm at (ii,jj,k) (kernels/oprt3ddivdamp.py:50-82)
+__device__ __forceinline__ double rwv_at(const Four& v, int ii, int jj, int k, int l) {
+  if (k <= cD.kmin || k > cD.kmax) return 0.0;
+  long long q = ix(ii, jj, k, l), qm = ix(ii, jj, k - 1, l);
+  const long long n = cD.npt;
+  const double* cz = cG.C2WGz;
+  double h = cz[q] * v.f[0][q] + cz[n + q] * v.f[0][qm] + cz[2 * n + q] * v.f[1][q] + cz[3 * n + q] * v.f[1][qm] +
+             cz[4 * n + q] * v.f[2][q] + cz[5 * n + q] * v.f[2][qm];
+  return h * cG.RGAMH[q] + v.f[3][q] * cG.RGSQRTH[q];
+}
+
+// sclt_TI / sclt_TJ at vertex (ii,jj) and level k (interior-k only)
+__device__ void sclt3d(const Four& v, int ii, int jj, int k, int l, double& sTI, double& sTJ) {
+  long long a = ix(ii, jj, k, l), b = ix(ii + 1, jj, k, l), c = ix(ii + 1, jj + 1, k, l), d = ix(ii, jj + 1, k, l);
+  double vx[4], vy[4], vz[4];
+  long long pts[4] = {a, b, c, d};
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    double rg = cG.RGAM[pts[n]];
+    vx[n] = v.f[0][pts[n]] * rg;
+    vy[n] = v.f[1][pts[n]] * rg;
+    vz[n] = v.f[2][pts[n]] * rg;
+  }
+  auto C = [&](int dir, int p, int t) { return P2(cG.coef_intp, (dir * 3 + p) * 2 + t, ii, jj, l); };
+  double rdz = cC.rdgz[k];
+  double wTI = ((rwv_at(v, ii, jj, k + 1, l) + rwv_at(v, ii + 1, jj, k + 1, l) + rwv_at(v, ii + 1, jj + 1, k + 1, l)) -
+                (rwv_at(v, ii, jj, k, l) + rwv_at(v, ii + 1, jj, k, l) + rwv_at(v, ii + 1, jj + 1, k, l))) / 3.0 * rdz;
+  double wTJ = ((rwv_at(v, ii, jj, k + 1, l) + rwv_at(v, ii + 1, jj + 1, k + 1, l) + rwv_at(v, ii, jj + 1, k + 1, l)) -
+                (rwv_at(v, ii, jj, k, l) + rwv_at(v, ii + 1, jj + 1, k, l) + rwv_at(v, ii, jj + 1, k, l))) / 3.0 * rdz;
+  sTI = C(0, 0, 0) * vx[0] + C(0, 1, 0) * vx[1] + C(0, 2, 0) * vx[2] + C(1, 0, 0) * vy[0] + C(1, 1, 0) * vy[1] +
+        C(1, 2, 0) * vy[2] + C(2, 0, 0) * vz[0] + C(2, 1, 0) * vz[1] + C(2, 2, 0) * vz[2] + wTI;
+  sTJ = C(0, 0, 1) * vx[0] + C(0, 1, 1) * vx[2] + C(0, 2, 1) * vx[3] + C(1, 0, 1) * vy[0] + C(1, 1, 1) * vy[2] +
+        C(1, 2, 1) * vy[3] + C(2, 0, 1) * vz[0] + C(2, 1, 1) * vz[2] + C(2, 2, 1) * vz[3] + wTJ;
+}
+
+// sclt pair at a vertex including the singular-point fix at (0,0)
+template <class SC>
+__device__ __forceinline__ void sclt_fixed(SC sc, int ii, int jj, int l, double& sTI, double& sTJ) {
+  sc(ii, jj, sTI, sTJ);
+  if (ii == 0 && jj == 0) {
+    double tI10, tJ10;
+    sc(1, 0, tI10, tJ10);
+    sTI = sTI * (double)cG.pntmask[l * 2 + 0] + tJ10 * (double)cG.pntmask[l * 2 + 1];
+  }
+}
+
+// the six-edge divergence-damping combination for direction d at (i,j)
+// (kernels/oprtdivdamp.py:110-120)
+__device__ __forceinline__ double ddivd(int i, int j, int l, int d, const double aTI, const double aTJ,
+                                        const double bTI, const double cTJ, const double cTI, const double dTJ) {
+  return P2(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) + P2(cG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
+         P2(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) + P2(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
+         P2(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) + P2(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI);
+}
+
+__global__ void k_dd3d(Four v, Three out) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (!col_of(t, i, j, l)) return;
+  const bool in = interior(i, j);   // output rows 1..gmax == interior
+  for (int k = 0; k < cD.KA; ++k) {
+    long long p = ix(i, j, k, l);
+    if (!in || k < cD.kmin || k > cD.kmax) {
+      out.f[0][p] = 0.0; out.f[1][p] = 0.0; out.f[2][p] = 0.0;
+      continue;
+    }
+    auto sc = [&](int ii, int jj, double& a, double& b) { sclt3d(v, ii, jj, k, l, a, b); };
+    double aTI, aTJ, bTI, bTJ, cTI, cTJ, dTI, dTJ;
+    sclt_fixed(sc, i, j, l, aTI, aTJ);
+    sclt_fixed(sc, i - 1, j, l, bTI, bTJ);
+    sclt_fixed(sc, i - 1, j - 1, l, cTI, cTJ);
+    sclt_fixed(sc, i, j - 1, l, dTI, dTJ);
+    for (int d = 0; d < 3; ++d) out.f[d][p] = ddivd(i, j, l, d, aTI, aTJ, bTI, cTJ, cTI, dTJ);
+  }
+}
+
+// pole 3-D divergence damping (kernels/oprt3ddivdamp.py:176-237)
+__global__ void k_dd3d_pl(Four v, Three out) {
+  int t = threadIdx.x;
+  if (t >= cD.KA * cD.LP) return;
+  int k = t / cD.LP, lp = t % cD.LP;
+  for (int g = 0; g < 6; ++g)
+    for (int d = 0; d < 3; ++d) out.f[d][ipl(g, k, lp)] = 0.0;
+  if (k < cD.kmin || k > cD.kmax) return;
+  auto rw = [&](int g, int kk) -> double {
+    if (kk <= cD.kmin || kk > cD.kmax) return 0.0;
+    int q = ipl(g, kk, lp), qm = ipl(g, kk - 1, lp);
+    const double* cz = cG.C2WGz_pl;
+    double h = cz[q * 6 + 0] * v.f[0][q] + cz[q * 6 + 1] * v.f[0][qm] + cz[q * 6 + 2] * v.f[1][q] +
+               cz[q * 6 + 3] * v.f[1][qm] + cz[q * 6 + 4] * v.f[2][q] + cz[q * 6 + 5] * v.f[2][qm];
+    return h * cG.RGAMH_pl[q] + v.f[3][q] * cG.RGSQRTH_pl[q];
+  };
+  double vm[6][3];
+  for (int g = 0; g < 6; ++g) {
+    int q = ipl(g, k, lp);
+    for (int d = 0; d < 3; ++d) vm[g][d] = v.f[d][q] * cG.RGAM_pl[q];
+  }
+  double sclt[5];
+  for (int v_ = 1; v_ <= 5; ++v_) {
+    int vp1 = (v_ == 5) ? 1 : v_ + 1;
+    double sw = ((rw(0, k + 1) + rw(v_, k + 1) + rw(vp1, k + 1)) - (rw(0, k) + rw(v_, k) + rw(vp1, k))) / 3.0 * cC.rdgz[k];
+    const double* cI = cG.coef_intp_pl + (v_ * cD.LP + lp) * 9;
+    sclt[v_ - 1] = cI[0] * vm[0][0] + cI[1] * vm[v_][0] + cI[2] * vm[vp1][0] + cI[3] * vm[0][1] + cI[4] * vm[v_][1] +
+                   cI[5] * vm[vp1][1] + cI[6] * vm[0][2] + cI[7] * vm[v_][2] + cI[8] * vm[vp1][2] + sw;
+  }
+  for (int d = 0; d < 3; ++d) {
+    double row = 0.0;
+    for (int v_ = 1; v_ <= 5; ++v_) {
+      int vm1 = (v_ == 1) ? 5 : v_ - 1;
+      double pair = sclt[vm1 - 1] + sclt[v_ - 1];
+      double tv = cG.coef_diff_pl[(v_ * cD.LP + lp) * 3 + d] * pair;
+      row = (v_ == 1) ? tv : row + tv;
+    }
+    out.f[d][ipl(0, k, lp)] = row;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// post-COMM 2-D divergence damping (kernels/divdamppostcomm.py:29-81):
+// gd = coef * OPRT_divdamp(-vtmp2), then horizontalize (interior).
+// ---------------------------------------------------------------------------
+__device__ void divdamp2d_at(const CThree& vt, int i, int j, int k, int l, double gd[3]) {
+  if (!interior(i, j)) {
+    for (int d = 0; d < 3; ++d) gd[d] = cC.divdamp_coef * 0.0;
+    return;
+  }
+  auto sc = [&](int ii, int jj, double& sTI, double& sTJ) {
+    long long a = ix(ii, jj, k, l), b = ix(ii + 1, jj, k, l), c = ix(ii + 1, jj + 1, k, l), d = ix(ii, jj + 1, k, l);
+    auto C = [&](int dir, int p, int t) { return P2(cG.coef_intp, (dir * 3 + p) * 2 + t, ii, jj, l); };
+    double x0 = -vt.f[0][a], x1 = -vt.f[0][b], x2 = -vt.f[0][c], x3 = -vt.f[0][d];
+    double y0 = -vt.f[1][a], y1 = -vt.f[1][b], y2 = -vt.f[1][c], y3 = -vt.f[1][d];
+    double z0 = -vt.f[2][a], z1 = -vt.f[2][b], z2 = -vt.f[2][c], z3 = -vt.f[2][d];
+    sTI = C(0, 0, 0) * x0 + C(0, 1, 0) * x1 + C(0, 2, 0) * x2 + C(1, 0, 0) * y0 + C(1, 1, 0) * y1 + C(1, 2, 0) * y2 +
+          C(2, 0, 0) * z0 + C(2, 1, 0) * z1 + C(2, 2, 0) * z2;
+    sTJ = C(0, 0, 1) * x0 + C(0, 1, 1) * x2 + C(0, 2, 1) * x3 + C(1, 0, 1) * y0 + C(1, 1, 1) * y2 + C(1, 2, 1) * y3 +
+          C(2, 0, 1) * z0 + C(2, 1, 1) * z2 + C(2, 2, 1) * z3;
+  };
+  double aTI, aTJ, bTI, bTJ, cTI, cTJ, dTI, dTJ;
+  sc(i, j, aTI, aTJ);
+  sc(i - 1, j, bTI, bTJ);
+  sc(i - 1, j - 1, cTI, cTJ);
+  sc(i, j - 1, dTI, dTJ);
+  double o[3];
+  for (int d = 0; d < 3; ++d) o[d] = cC.divdamp_coef * ddivd(i, j, l, d, aTI, aTJ, bTI, cTJ, cTI, dTJ);
+  horiz_reg(i, j, l, o[0], o[1], o[2]);
+  gd[0] = o[0]; gd[1] = o[1]; gd[2] = o[2];
+}
+
+// pole 2-D divergence damping of -vtmp2 at (g,k,lp) (kernels/oprtdivdamp.py:125-173
+// then horizontalize over all g)
+__device__ void divdamp2d_pl_at(const CThree& vt, int g, int k, int lp, double gd[3]) {
+  double o[3] = {0.0, 0.0, 0.0};
+  if (g == 0) {
+    double vv[6][3];
+    for (int q = 0; q < 6; ++q)
+      for (int d = 0; d < 3; ++d) vv[q][d] = -vt.f[d][ipl(q, k, lp)];
+    double sclt[5];
+    for (int v_ = 1; v_ <= 5; ++v_) {
+      int vp1 = (v_ == 5) ? 1 : v_ + 1;
+      const double* cI = cG.coef_intp_pl + (v_ * cD.LP + lp) * 9;
+      sclt[v_ - 1] = cI[0] * vv[0][0] + cI[1] * vv[v_][0] + cI[2] * vv[vp1][0] + cI[3] * vv[0][1] +
+                     cI[4] * vv[v_][1] + cI[5] * vv[vp1][1] + cI[6] * vv[0][2] + cI[7] * vv[v_][2] +
+                     cI[8] * vv[vp1][2];
+    }
+    for (int d = 0; d < 3; ++d) {
+      double row = 0.0;
+      for (int v_ = 1; v_ <= 5; ++v_) {
+        int vm1 = (v_ == 1) ? 5 : v_ - 1;
+        double tv = cG.coef_diff_pl[(v_ * cD.LP + lp) * 3 + d] * (sclt[vm1 - 1] + sclt[v_ - 1]);
+        row = (v_ == 1) ? tv : row + tv;
+      }
+      o[d] = row;
+    }
+  }
+  for (int d = 0; d < 3; ++d) o[d] = cC.divdamp_coef * o[d];
+  horiz_pl(g, lp, o[0], o[1], o[2]);
+  gd[0] = o[0]; gd[1] = o[1]; gd[2] = o[2];
+}
+
+// ---------------------------------------------------------------------------
+// pressure gradient (kernels/presgrad.py:126-265): horizontal part at level
+// k with the first-layer remedy and the tangent-plane projection.
+// P(ii,jj,kk) gives the pressure; returns Pgrad (3 comps).
+// ---------------------------------------------------------------------------
+template <class PF>
+__device__ void presgrad_reg(int i, int j, int k, int l, const Col& c, const Met& m, PF P, double out[3]) {
+  const int kmin = cD.kmin, kmax = cD.kmax;
+  out[0] = out[1] = out[2] = 0.0;
+  if (k >= kmin && k <= kmax) {
+    const int kk = (k == kmin) ? kmin + 1 : k;
+    double gh[3] = {0.0, 0.0, 0.0};
+    if (interior(i, j)) grad7(i, j, kk, l, [&](int ii, int jj, int k2) { return P(ii, jj, k2) * cG.RGAM[ix(ii, jj, k2, l)]; }, gh);
+    auto pvmh = [&](int k2, int d) {
+      return (mc(m.C2WGz, c, 2 * d, 6, k2) * P(i, j, k2) + mc(m.C2WGz, c, 2 * d + 1, 6, k2) * P(i, j, k2 - 1)) *
+             m.RGAMH[c.at(k2)];
+    };
+    for (int d = 0; d < 3; ++d) out[d] = gh[d] + (pvmh(kk + 1, d) - pvmh(kk, d)) * cC.rdgz[kk];
+  }
+  if (interior(i, j)) horiz_reg(i, j, l, out[0], out[1], out[2]);
+}
+
+template <class PF>
+__device__ void presgrad_pl(int g, int k, int lp, const Col& c, const Met& m, PF P, double out[3]) {
+  const int kmin = cD.kmin, kmax = cD.kmax;
+  out[0] = out[1] = out[2] = 0.0;
+  if (k >= kmin && k <= kmax) {
+    const int kk = (k == kmin) ? kmin + 1 : k;
+    double gh[3] = {0.0, 0.0, 0.0};
+    if (g == 0) {
+      for (int d = 0; d < 3; ++d) {
+        double row = 0.0;
+        for (int v_ = 0; v_ < 6; ++v_) {
+          double pvm = P(v_, kk) * cG.RGAM_pl[ipl(v_, kk, lp)] * 1.0;
+          double tv = cG.coef_grad_pl[(v_ * cD.LP + lp) * 3 + d] * pvm;
+          row = (v_ == 0) ? tv : row + tv;
+        }
+        gh[d] = row;
+      }
+    }
+    auto pvmh = [&](int k2, int d) {
+      return (mc(m.C2WGz, c, 2 * d, 6, k2) * P(g, k2) + mc(m.C2WGz, c, 2 * d + 1, 6, k2) * P(g, k2 - 1)) *
+             m.RGAMH[c.at(k2)];
+    };
+    for (int d = 0; d < 3; ++d) out[d] = gh[d] + (pvmh(kk + 1, d) - pvmh(kk, d)) * cC.rdgz[kk];
+  }
+  horiz_pl(g, lp, out[0], out[1], out[2]);
+}
+
+// vertical pressure gradient (kernels/presgrad.py:196-204)
+template <class PF>
+__device__ __forceinline__ double presgradw(const Col& c, const Met& m, int k, PF Pk) {
+  if (k < cD.kmin + 1 || k > cD.kmax) return 0.0;
+  long long p = c.at(k), pm = c.at(k - 1);
+  return m.GAM2H[p] * (Pk(k) * m.RGSGAM2[p] - Pk(k - 1) * m.RGSGAM2[pm]) * cC.rdgzh[k];
+}
+
+// flux convergence at level k of a regional or pole column given the
+// horizontal divergence value (zero on the halo) and the flux accessors
+// (kernels/fluxconv.py:111-208, vflag 1 or 0)
+template <class FH, class FW>
+__device__ __forceinline__ double fluxconv_col(const Col& c, const Met& m, int k, double div, double vflag, FH fh, FW fw) {
+  if (k < cD.kmin || k > cD.kmax) return 0.0;
+  auto vmh = [&](int kk) -> double {
+    if (kk <= cD.kmin || kk > cD.kmax) return 0.0;
+    double h = vmh_horiz(c, m, kk, fh);
+    return h + vflag * fw(kk) * m.RGSQRTH[c.at(kk)];
+  };
+  return -div - (vmh(k + 1) - vmh(k)) * cC.rdgz[k];
+}
+
+// pole divergence row of (fx,fy,fz)*RGAM at level k (kernels/fluxconv.py:81-108)
+template <class F>
+__device__ __forceinline__ double div_pl(int lp, int k, F f) {
+  double row = 0.0;
+  for (int v_ = 0; v_ < 6; ++v_) {
+    int q = ipl(v_, k, lp);
+    double rg = cG.RGAM_pl[q];
+    double vx = f(q, 0) * rg, vy = f(q, 1) * rg, vz = f(q, 2) * rg;
+    const double* cd = cG.coef_div_pl + (v_ * cD.LP + lp) * 3;
+    double pv = cd[0] * vx + cd[1] * vy + cd[2] * vz;
+    row = (v_ == 0) ? pv : row + pv;
+  }
+  return row;
+}
+
+// ---------------------------------------------------------------------------
+// vp0: small-step source terms, g_TEND of the small step, the vertical
+// implicit matrix and ethtot0 (mod_vi.py:295-878 numpy path,
+// kernels/vimatrix.py:67-136, kernels/vimain.py:195-239)
+// ---------------------------------------------------------------------------
+struct Vp0Args {
+  Prog P;                       // PROG (post BNDCND)
+  const double *vx, *vy, *vz, *eth, *pregd, *rhogd;
+  CThree vt;                    // post-COMM 3-D divdamp of PROG
+  const double* gT0[6];         // large-step tendency
+  double* gT[6];                // out: small-step tendency
+  double *Mc, *Mu, *Ml, *ethtot0;
+  double dt;                    // small-step dt
+};
+
+template <bool POLE>
+__device__ void vp0_column(const Vp0Args& a, int i, int j, int l, int g, int lp) {
+  const Col c = POLE ? col_pl(g, lp) : col_reg(i, j, l);
+  const Met m = met_of(POLE);
+  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
+  const double* const* P = a.P.v;
+  double dt = a.dt;
+  // column-local half-level values
+  auto rhog_h = [&](int k) -> double {
+    int kk = (k < kmin) ? kmin : k;
+    return mc(m.C2W, c, 0, 2, kk) * P[0][c.at(kk)] + mc(m.C2W, c, 1, 2, kk) * P[0][c.at(kk - 1)];
+  };
+  auto eth_h = [&](int k) -> double {
+    int kk = (k < kmin) ? kmin : k;
+    return cC.afact[kk] * a.eth[c.at(kk)] + cC.bfact[kk] * a.eth[c.at(kk - 1)];
+  };
+  auto dbuo = [&](int k) -> double {
+    if (k < kmin + 1 || k > kmax) return 0.0;
+    return -cC.GRAV * (mc(m.C2W, c, 0, 2, k) * a.rhogd[c.at(k)] + mc(m.C2W, c, 1, 2, k) * a.rhogd[c.at(k - 1)]);
+  };
+  auto dpgw = [&](int k) -> double { return presgradw(c, m, k, [&](int kk) { return a.pregd[c.at(kk)]; }); };
+  auto gz = [&](int k) -> double { return cC.GRAV - (dpgw(k) - dbuo(k)) / rhog_h(k); };
+  auto pwh = [&](int k) -> double { return -gz(k) * P[4][c.at(k)]; };
+  auto PF = [&](int k, int d) -> double { return P[1 + d][c.at(k)]; };
+  auto PEF = [&](int k, int d) -> double { return P[1 + d][c.at(k)] * a.eth[c.at(k)]; };
+  for (int k = 0; k < KA; ++k) {
+    long long p = c.at(k);
+    // horizontal divergences
+    double div1 = 0.0, div2 = 0.0;
+    if (!POLE) {
+      if (interior(i, j)) {
+        div1 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
+          long long q = ix(ii, jj, kk, l);
+          return P[1 + d][q] * cG.RGAM[q];
+        });
+        div2 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
+          long long q = ix(ii, jj, kk, l);
+          return (P[1 + d][q] * a.eth[q]) * cG.RGAM[q];
+        });
+      }
+    } else if (g == 0) {
+      div1 = div_pl(lp, k, [&](int q, int d) { return P[1 + d][q]; });
+      div2 = div_pl(lp, k, [&](int q, int d) { return P[1 + d][q] * a.eth[q]; });
+    }
+    double drhog = fluxconv_col(c, m, k, div1, 1.0, PF, [&](int kk) { return P[4][c.at(kk)]; });
+    double drhoge = fluxconv_col(c, m, k, div2, 1.0, PEF, [&](int kk) {
+      long long q = c.at(kk);
+      return P[4][q] * (cC.afact[kk] * a.eth[q] + cC.bfact[kk] * a.eth[c.at(kk - 1)]);
+    });
+    double dd[3], dpg[3];
+    if (!POLE) {
+      divdamp2d_at(a.vt, i, j, k, l, dd);
+      presgrad_reg(i, j, k, l, c, m, [&](int ii, int jj, int kk) { return a.pregd[ix(ii, jj, kk, l)]; }, dpg);
+    } else {
+      divdamp2d_pl_at(a.vt, g, k, lp, dd);
+      presgrad_pl(g, k, lp, c, m, [&](int gg, int kk) { return a.pregd[ipl(gg, kk, lp)]; }, dpg);
+    }
+    double pw = 0.0;
+    if (k >= kmin && k <= kmax)
+      pw = a.vx[p] * dpg[0] + a.vy[p] * dpg[1] + a.vz[p] * dpg[2] + mc(m.W2C, c, 0, 2, k) * pwh(k + 1) +
+           mc(m.W2C, c, 1, 2, k) * pwh(k);
+    a.gT[0][p] = a.gT0[0][p] + drhog;
+    a.gT[1][p] = a.gT0[1][p] - dpg[0] + dd[0] + 0.0;
+    a.gT[2][p] = a.gT0[2][p] - dpg[1] + dd[1] + 0.0;
+    a.gT[3][p] = a.gT0[3][p] - dpg[2] + dd[2] + 0.0;
+    a.gT[4][p] = a.gT0[4][p] + 0.0 * cC.alpha - dpgw(k) + dbuo(k);
+    a.gT[5][p] = a.gT0[5][p] + drhoge + pw;
+    // vertical implicit matrix on k = kmin+1..kmax
+    if (k >= kmin + 1 && k <= kmax) {
+      const double GCVovR = cC.GRAV * cC.CVdry / cC.Rdry;
+      const double ACVovRt2 = cC.alpha * cC.CVdry / cC.Rdry / (dt * dt);
+      long long pm = c.at(k - 1), pp = c.at(k + 1);
+      double rg = cC.rdgz[k], rgm = cC.rdgz[k - 1];
+      double Ca = (m.RGSGAM2[p] * rg + m.RGSGAM2[pm] * rgm) * m.GAM2H[p];
+      double Cb = cC.dfact[k] - cC.cfact[k - 1];
+      double Cu1 = m.RGSGAM2[p] * rg * m.GAM2H[pp];
+      double rgh2 = m.RGAMH[p] * m.RGAMH[p];
+      double Cu2 = m.GAM2H[pp] * rgh2 * GCVovR;
+      double Cl1 = m.RGSGAM2[p] * rg * m.GAM2H[pm];
+      double Cl2 = m.GAM2H[pm] * rgh2 * GCVovR;
+      double rgh = cC.rdgzh[k];
+      a.Mc[p] = ACVovRt2 / m.RGSQRTH[p] + rgh * (Ca * eth_h(k) - Cb * (gz(k) + GCVovR));
+      a.Mu[p] = -rgh * (Cu1 * eth_h(k + 1) + cC.cfact[k] * (gz(k + 1) + Cu2));
+      a.Ml[p] = -rgh * (Cl1 * eth_h(k - 1) - cC.dfact[k - 1] * (gz(k - 1) + Cl2));
+    }
+    // total energy at the start of the small steps
+    double kin0 = rhogkin_at(c, m, k, [&](int kk, int comp) { return P[comp][c.at(kk)]; });
+    a.ethtot0[p] = a.eth[p] + kin0 / P[0][p] + m.PHI[p];
+  }
+}
+
+__global__ void k_vp0(Vp0Args a, int pole) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l, g, lp;
+  if (!map_col(pole, t, i, j, l, g, lp)) return;
+  if (!pole) vp0_column<false>(a, i, j, l, 0, 0);
+  else vp0_column<true>(a, 0, 0, 0, g, lp);
+}
+
+// ---------------------------------------------------------------------------
+// acoustic loop, path1 (kernels/vipath1.py:68-160): diff_vh with BNDCND and
+// the running mean of the horizontal momentum.
+// ---------------------------------------------------------------------------
+struct Path1Args {
+  const double* PS[6];     // PROG_split (RHOGE boundary rows read clamped)
+  const double* rhog;      // PROG rhog
+  const double* gT[6];
+  CThree vt;               // post-COMM 3-D divdamp of PROG_split
+  double* dvh[3];          // out
+  double* PM[5];           // running mean (in/out)
+  double dt, rweight, RovCV;
+};
+
+template <bool POLE>
+__device__ void path1_column(const Path1Args& a, int i, int j, int l, int g, int lp) {
+  const Col c = POLE ? col_pl(g, lp) : col_reg(i, j, l);
+  const Met m = met_of(POLE);
+  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
+  const double dt = a.dt;
+  auto pregs = [&](long long base_q, int kk) -> double {  // preg_prim_split with clamped boundary rows
+    int k2 = kk < kmin ? kmin : (kk > kmax ? kmax : kk);
+    return a.PS[5][base_q + (long long)k2 * c.ks] * a.RovCV;
+  };
+  double vals[3][2];  // values at kmin and kmax for the boundary rows
+  double* const* out = a.dvh;
+  for (int k = 0; k < KA; ++k) {
+    long long p = c.at(k);
+    double dd[3], pg[3];
+    if (!POLE) {
+      divdamp2d_at(a.vt, i, j, k, l, dd);
+      presgrad_reg(i, j, k, l, c, m, [&](int ii, int jj, int kk) { return pregs(ix(ii, jj, 0, l), kk); }, pg);
+    } else {
+      divdamp2d_pl_at(a.vt, g, k, lp, dd);
+      presgrad_pl(g, k, lp, c, m, [&](int gg, int kk) { return pregs((long long)gg * cD.KA * cD.LP + lp, kk); }, pg);
+    }
+    for (int d = 0; d < 3; ++d) {
+      double drv = a.gT[1 + d][p] - pg[d] + dd[d] + 0.0;
+      double v = a.PS[1 + d][p] + drv * dt;
+      out[d][p] = v;
+      if (k == kmin) vals[d][0] = v;
+      if (k == kmax) vals[d][1] = v;
+    }
+  }
+  const long long pT = c.at(kmax + 1), pK = c.at(kmax), pB = c.at(kmin - 1), pN = c.at(kmin);
+  for (int d = 0; d < 3; ++d) {
+    out[d][pT] = 1.0 * (vals[d][1] / a.rhog[pK]) * a.rhog[pT];
+    out[d][pB] = -1.0 * (vals[d][0] / a.rhog[pN]) * a.rhog[pB];
+  }
+  for (int k = 0; k < KA; ++k) {
+    long long p = c.at(k);
+    for (int d = 0; d < 3; ++d) a.PM[1 + d][p] = a.PM[1 + d][p] + out[d][p] * a.rweight;
+  }
+}
+
+__global__ void k_path1(Path1Args a, int pole) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l, g, lp;
+  if (!map_col(pole, t, i, j, l, g, lp)) return;
+  if (!pole) path1_column<false>(a, i, j, l, 0, 0);
+  else path1_column<true>(a, 0, 0, 0, g, lp);
+}
+
+// ---------------------------------------------------------------------------
+// vi_main (kernels/vimain.py:127-262): horizontal divergences (kernel A),
+// then per column the flux convergences, the tridiagonal Thomas solve
+// (kernels/virhowsolver.py:42-120), kinetic energies and the energy update.
+// ---------------------------------------------------------------------------
+struct VimainArgs {
+  const double* PS[6];
+  const double* P[6];          // PROG
+  const double *eth, *ethtot0;
+  const double* gT[6];         // small-step tendency
+  const double* gT0e;          // large-step tendency of RHOGE (grhogetot)
+  const double *Mc, *Mu, *Ml;
+  CThree dvh;                  // post-COMM diff_vh
+  double* hdiv[3];             // kernel A output
+  double* dwe[3];              // out: rhog_s1, rhogw_s1, rhoge_s1
+  double* PM0;                 // running mean of RHOG (in/out)
+  double* PM4;                 // running mean of RHOGW (in/out)
+  double dt, rweight, RovCV;
+};
+
+__global__ void k_vimain_a(VimainArgs a, int pole) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (!pole) {
+    if (!col_of(t, i, j, l)) return;
+    const bool in = interior(i, j);
+    for (int k = 0; k < cD.KA; ++k) {
+      long long p = ix(i, j, k, l);
+      double h1 = 0.0, h2 = 0.0, h3 = 0.0;
+      if (in && k >= cD.kmin && k <= cD.kmax) {
+        h1 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
+          long long q = ix(ii, jj, kk, l);
+          return a.dvh.f[d][q] * cG.RGAM[q];
+        });
+        h2 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
+          long long q = ix(ii, jj, kk, l);
+          return (a.dvh.f[d][q] * a.eth[q]) * cG.RGAM[q];
+        });
+        h3 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
+          long long q = ix(ii, jj, kk, l);
+          return ((a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q]) * cG.RGAM[q];
+        });
+      }
+      a.hdiv[0][p] = h1; a.hdiv[1][p] = h2; a.hdiv[2][p] = h3;
+    }
+  } else {
+    long long tp = t;
+    if (tp < cD.KA * cD.LP) {
+      int k = (int)(tp / cD.LP), lp = (int)(tp % cD.LP);
+      for (int g = 0; g < 6; ++g) {
+        int p = ipl(g, k, lp);
+        double h1 = 0.0, h2 = 0.0, h3 = 0.0;
+        if (g == 0 && k >= cD.kmin && k <= cD.kmax) {
+          h1 = div_pl(lp, k, [&](int q, int d) { return a.dvh.f[d][q]; });
+          h2 = div_pl(lp, k, [&](int q, int d) { return a.dvh.f[d][q] * a.eth[q]; });
+          h3 = div_pl(lp, k, [&](int q, int d) { return (a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q]; });
+        }
+        a.hdiv[0][p] = h1; a.hdiv[1][p] = h2; a.hdiv[2][p] = h3;
+      }
+    }
+  }
+}
+
+template <bool POLE>
+__device__ void vimain_column(const VimainArgs& a, const Col c) {
+  const Met m = met_of(POLE);
+  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
+  const double dt = a.dt;
+  const double Rdry = cC.Rdry, CVdry = cC.CVdry;
+  auto PSk = [&](int comp, int k) -> double {  // PROG_split with clamped RHOGE boundary rows
+    if (comp == 5) k = k < kmin ? kmin : (k > kmax ? kmax : k);
+    return a.PS[comp][c.at(k)];
+  };
+  auto preg0 = [&](int k) -> double { return PSk(5, k) * a.RovCV; };
+  auto DV = [&](int k, int d) -> double { return a.dvh.f[d][c.at(k)]; };
+  auto DVE = [&](int k, int d) -> double { return a.dvh.f[d][c.at(k)] * a.eth[c.at(k)]; };
+  // grhog1 and gpre on every level
+  double grhog1[NC_MAXK], gpre[NC_MAXK];
+  for (int k = 0; k < KA; ++k) {
+    long long p = c.at(k);
+    double drhog = fluxconv_col(c, m, k, a.hdiv[0][p], 0.0, DV, [&](int kk) { return PSk(4, kk); });
+    double drhoge = fluxconv_col(c, m, k, a.hdiv[1][p], 0.0, DVE, [&](int kk) { return 0.0; });
+    grhog1[k] = a.gT[0][p] + drhog;
+    double grhoge1 = a.gT[5][p] + drhoge;
+    gpre[k] = grhoge1 * Rdry / CVdry;
+  }
+  // Thomas solve (kernels/virhowsolver.py:67-120)
+  const int kT = kmax + 1;
+  double rw_top = -(mc(m.C2WGz, c, 0, 6, kT) * DV(kT, 0) + mc(m.C2WGz, c, 1, 6, kT) * DV(kmax, 0) +
+                    mc(m.C2WGz, c, 2, 6, kT) * DV(kT, 1) + mc(m.C2WGz, c, 3, 6, kT) * DV(kmax, 1) +
+                    mc(m.C2WGz, c, 4, 6, kT) * DV(kT, 2) + mc(m.C2WGz, c, 5, 6, kT) * DV(kmax, 2));
+  const double CVovRt2 = CVdry / Rdry / (dt * dt);
+  const double rw_kmin = 0.0 * m.RGSGAM2H[c.at(kmin)];
+  const double rw_kmaxp1 = rw_top * m.RGSGAM2H[c.at(kT)];
+  const int N = kmax - kmin;
+  double u[NC_MAXK], gam[NC_MAXK];
+  double beta = 0.0;
+  for (int n = 0; n < N; ++n) {
+    int k = kmin + 1 + n;
+    long long p = c.at(k), pm = c.at(k - 1);
+    double rg2 = m.RGAMH[p] * m.RGAMH[p];
+    double rgam2 = m.RGAM[p] * m.RGAM[p], rgam2m = m.RGAM[pm] * m.RGAM[pm];
+    double Sw = a.gT[4][p] + 0.0 * cC.alpha;
+    double S = ((PSk(4, k) * cC.alpha + dt * Sw) * rg2 -
+                ((preg0(k) + dt * gpre[k]) * m.RGSGAM2[p] - (preg0(k - 1) + dt * gpre[k - 1]) * m.RGSGAM2[pm]) * dt *
+                    cC.rdgzh[k] -
+                ((PSk(0, k) + dt * grhog1[k]) * rgam2 * cC.afact[k] + (PSk(0, k - 1) + dt * grhog1[k - 1]) * rgam2m * cC.bfact[k]) *
+                    dt * cC.GRAV) *
+               CVovRt2;
+    if (n == 0) S = S - a.Ml[c.at(kmin + 1)] * rw_kmin;
+    if (n == N - 1) S = S - a.Mu[c.at(kmax)] * rw_kmaxp1;
+    double Mc = a.Mc[p], Ml = a.Ml[p];
+    if (n == 0) {
+      beta = Mc;
+      u[0] = S / beta;
+    } else {
+      double gg = a.Mu[pm] / beta;
+      beta = Mc - Ml * gg;
+      u[n] = (S - Ml * u[n - 1]) / beta;
+      gam[n] = gg;
+    }
+  }
+  double rws1[NC_MAXK];
+  for (int k = 0; k < KA; ++k) rws1[k] = 0.0;
+  {
+    double x = u[N - 1];
+    rws1[kmin + N] = x * m.GSGAM2H[c.at(kmin + N)];
+    for (int n = N - 2; n >= 0; --n) {
+      x = u[n] - gam[n + 1] * x;
+      rws1[kmin + 1 + n] = x * m.GSGAM2H[c.at(kmin + 1 + n)];
+    }
+    rws1[kmin] = rw_kmin * m.GSGAM2H[c.at(kmin)];
+    rws1[kT] = rw_kmaxp1 * m.GSGAM2H[c.at(kT)];
+  }
+  // rhog_split1, kinetic energies, total-energy advection, rhoge_split1
+  double rs1[NC_MAXK];
+  for (int k = 0; k < KA; ++k) {
+    long long p = c.at(k);
+    double drhog2 = fluxconv_col(c, m, k, a.hdiv[0][p], 1.0, DV, [&](int kk) { return rws1[kk]; });
+    rs1[k] = PSk(0, k) + (a.gT[0][p] + drhog2) * dt;
+  }
+  for (int k = 0; k < KA; ++k) {
+    long long p = c.at(k);
+    auto st10 = [&](int kk, int comp) -> double {
+      long long q = c.at(kk);
+      return a.P[comp][q] + PSk(comp, kk);
+    };
+    auto st11 = [&](int kk, int comp) -> double {
+      long long q = c.at(kk);
+      if (comp == 0) return a.P[0][q] + rs1[kk];
+      if (comp == 4) return a.P[4][q] + rws1[kk];
+      return a.P[comp][q] + a.dvh.f[comp - 1][q];
+    };
+    double kin10 = rhogkin_at(c, m, k, st10);
+    double kin11 = rhogkin_at(c, m, k, st11);
+    double drhogetot = fluxconv_col(
+        c, m, k, a.hdiv[2][p], 1.0,
+        [&](int kk, int d) {
+          long long q = c.at(kk);
+          return (a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q];
+        },
+        [&](int kk) {
+          long long q = c.at(kk), qm = c.at(kk - 1);
+          return (a.P[4][q] + rws1[kk]) * (cC.afact[kk] * a.ethtot0[q] + cC.bfact[kk] * a.ethtot0[qm]);
+        });
+    double re = PSk(5, k) + (a.gT0e[p] + drhogetot) * dt + (kin10 - kin11) + (PSk(0, k) - rs1[k]) * m.PHI[p];
+    a.dwe[0][p] = rs1[k];
+    a.dwe[1][p] = rws1[k];
+    a.dwe[2][p] = re;
+    a.PM0[p] = a.PM0[p] + rs1[k] * a.rweight;
+    a.PM4[p] = a.PM4[p] + rws1[k] * a.rweight;
+  }
+}
+
+__global__ void k_vimain_b(VimainArgs a, int pole) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l, g, lp;
+  if (!map_col(pole, t, i, j, l, g, lp)) return;
+  if (!pole) vimain_column<false>(a, col_reg(i, j, l));
+  else vimain_column<true>(a, col_pl(g, lp));
+}
+
+// ---------------------------------------------------------------------------
+// elementwise helpers of the small step
+// ---------------------------------------------------------------------------
+// PROG_split = 0 (first stage) or PROG0 - PROG; PROG_mean = PROG[0:5]
+__global__ void k_split_init(const double* P0a, const double* P0b, const double* P0c, const double* P0d,
+                             const double* P0e, const double* P0f, Prog P, double* PS0, double* PS1, double* PS2,
+                             double* PS3, double* PS4, double* PS5, double* PM0, double* PM1, double* PM2,
+                             double* PM3, double* PM4, long long n, int first) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double* P0[6] = {P0a, P0b, P0c, P0d, P0e, P0f};
+  double* PS[6] = {PS0, PS1, PS2, PS3, PS4, PS5};
+  double* PM[5] = {PM0, PM1, PM2, PM3, PM4};
+  for (int v = 0; v < 6; ++v) PS[v][t] = first ? 0.0 : (P0[v][t] - P.v[v][t]);
+  for (int v = 0; v < 5; ++v) PM[v][t] = P.v[v][t];
+}
+
+// PROG += PROG_split, then horizontalize the momentum (mod_vi.py:1572-1583)
+__global__ void k_post(Prog P, const double* PS0, const double* PS1, const double* PS2, const double* PS3,
+                       const double* PS4, const double* PS5, int pole) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const double* PS[6] = {PS0, PS1, PS2, PS3, PS4, PS5};
+  int i, j, l, g, lp;
+  if (!map_col(pole, t, i, j, l, g, lp)) return;
+  const Col c = pole ? col_pl(g, lp) : col_reg(i, j, l);
+  const bool in = !pole && interior(i, j);
+  for (int k = 0; k < cD.KA; ++k) {
+    long long p = c.at(k);
+    double v[6];
+    for (int n = 0; n < 6; ++n) v[n] = P.v[n][p] + PS[n][p];
+    if (pole) horiz_pl(g, lp, v[1], v[2], v[3]);
+    else if (in) horiz_reg(i, j, l, v[1], v[2], v[3]);
+    for (int n = 0; n < 6; ++n) P.v[n][p] = v[n];
+  }
+}
+
+}  // namespace nc

@@ -1,0 +1,660 @@
+// Tracer advection of the last RK stage: MIURA2004 horizontal scheme with
+// the Thuburn horizontal and vertical flux limiters, Strang-split V/H/V
+// (pynicamdc/nhm/dynamics/mod_src_tracer.py:83-1228).
+#pragma once
+#include "nc_small.cuh"
+
+namespace nc {
+
+// ---------------------------------------------------------------------------
+// tracer-independent part of the first vertical step (kernels/tracervertflux.py)
+// flx_v and the updated density rhog_t, on every column.
+// ---------------------------------------------------------------------------
+struct TrcFluxArgs {
+  const double *rvx, *rvy, *rvz, *rw;    // time-mean momentum (PROG_mean)
+  const double* rhog_in;                 // density at the start of the step
+  const double* frhog;
+  double *flx_v, *rhog_t;
+  double dt;
+};
+
+__device__ void trc_vflux_column(const Col c, const Met m, const TrcFluxArgs& a) {
+  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
+  for (int k = 0; k < KA; ++k) {
+    long long p = c.at(k);
+    double f = 0.0;
+    if (k >= kmin + 1 && k <= kmax) {
+      long long pm = c.at(k - 1);
+      double horiz = (mc(m.C2WGz, c, 0, 6, k) * a.rvx[p] + mc(m.C2WGz, c, 1, 6, k) * a.rvx[pm] +
+                      mc(m.C2WGz, c, 2, 6, k) * a.rvy[p] + mc(m.C2WGz, c, 3, 6, k) * a.rvy[pm] +
+                      mc(m.C2WGz, c, 4, 6, k) * a.rvz[p] + mc(m.C2WGz, c, 5, 6, k) * a.rvz[pm]) * m.RGAMH[p];
+      double vert = a.rw[p] * m.RGSQRTH[p];
+      f = (horiz + vert) * 0.5 * a.dt;
+    }
+    a.flx_v[p] = f;
+  }
+  for (int k = 0; k < KA; ++k) {
+    long long p = c.at(k);
+    double r = 0.0;
+    if (k >= kmin && k <= kmax) {
+      r = a.rhog_in[p] - (a.flx_v[c.at(k + 1)] - a.flx_v[p]) * cC.rdgz[k] + 0.0 * a.frhog[p] * a.dt;
+    } else if (k == kmin - 1) {
+      r = a.rhog_in[c.at(kmin)];
+    } else if (k == kmax + 1) {
+      r = a.rhog_in[c.at(kmax)];
+    }
+    a.rhog_t[p] = r;
+  }
+}
+
+__global__ void k_trc_vflux(TrcFluxArgs a, int pole) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l, g, lp;
+  if (!map_col(pole, t, i, j, l, g, lp)) return;
+  if (!pole) trc_vflux_column(col_reg(i, j, l), met_of(false), a);
+  else trc_vflux_column(col_pl(g, lp), met_of(true), a);
+}
+
+// ---------------------------------------------------------------------------
+// one vertical fractional step of one tracer with the vertical Thuburn
+// limiter (mod_src_tracer.py:389-533 and 1036-1204, limiter :1909-2074)
+// ---------------------------------------------------------------------------
+struct TrcVadvArgs {
+  double* rhogq;
+  const double *den, *flx_v, *frhog;
+  double dt, bcoef;      // d = bcoef*frhog/den*dt
+  int clamp;             // second step: zero tiny negatives, then add dt*0
+  double dtl;
+};
+
+__device__ void trc_vadv_column(const Col c, const TrcVadvArgs& a) {
+  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
+  const double BIG = cC.HUGE_, EPS = cC.EPS;
+  double q[NC_MAXK], qh[NC_MAXK], ck0[NC_MAXK], ck1[NC_MAXK];
+  for (int k = 0; k < KA; ++k) {
+    long long p = c.at(k);
+    q[k] = a.rhogq[p] / a.den[p];
+  }
+  for (int k = 0; k < KA; ++k) {
+    if (k >= kmin && k <= kmax + 1) qh[k] = cC.afact[k] * q[k] + cC.bfact[k] * q[k - 1];
+    else qh[k] = 0.0;
+    if (k >= kmin && k <= kmax) {
+      long long p = c.at(k);
+      ck0[k] = -a.flx_v[p] / a.den[p] * cC.rdgz[k];
+      ck1[k] = a.flx_v[c.at(k + 1)] / a.den[p] * cC.rdgz[k];
+    } else {
+      ck0[k] = 0.0;
+      ck1[k] = 0.0;
+    }
+  }
+  double qmin_prev = 0.0, qmax_prev = 0.0;
+  for (int k = kmin; k <= kmax; ++k) {
+    long long p = c.at(k);
+    double inL = 0.5 - copysign(0.5, ck0[k]);
+    double inU = 0.5 + copysign(0.5, ck0[k + 1]);
+    double qc = q[k], qb = q[k - 1], qa = q[k + 1];
+    double QminL = (inL == 1.0) ? npmin(qc, qb) : BIG;
+    double QminU = (inU == 1.0) ? npmin(qc, qa) : BIG;
+    double QmaxL = (inL == 1.0) ? npmax(qc, qb) : -BIG;
+    double QmaxU = (inU == 1.0) ? npmax(qc, qa) : -BIG;
+    double qnmin = npmin(npmin(QminL, QminU), qc);
+    double qnmax = npmax(npmax(QmaxL, QmaxU), qc);
+    double c1 = ck0[k], c2 = ck1[k];
+    double Cin = inL * c1 + inU * c2;
+    double Cout = (1.0 - inL) * c1 + (1.0 - inU) * c2;
+    double CQmin = inL * c1 * QminL + inU * c2 * QminU;
+    double CQmax = inL * c1 * QmaxL + inU * c2 * QmaxU;
+    double zsw = 0.5 - copysign(0.5, fabs(Cout) - EPS);
+    double dk = a.bcoef * a.frhog[p] / a.den[p] * a.dt;
+    double qomin = ((qc - qnmax) + qnmax * (Cin + Cout - dk) - CQmax) / (Cout + zsw) * (1.0 - zsw) + qc * zsw;
+    double qomax = ((qc - qnmin) + qnmin * (Cin + Cout - dk) - CQmin) / (Cout + zsw) * (1.0 - zsw) + qc * zsw;
+    if (k > kmin) {
+      double h = qh[k];
+      qh[k] = inL * npmin(npmax(h, qmin_prev), qmax_prev) + (1.0 - inL) * npmin(npmax(h, qomin), qomax);
+    }
+    qmin_prev = qomin;
+    qmax_prev = qomax;
+  }
+  qh[kmin] = 0.0;
+  qh[kmax + 1] = 0.0;
+  for (int k = 0; k < KA; ++k) {
+    long long p = c.at(k);
+    double x;
+    if (k >= kmin && k <= kmax) {
+      x = a.rhogq[p] - (a.flx_v[c.at(k + 1)] * qh[k + 1] - a.flx_v[p] * qh[k]) * cC.rdgz[k];
+      if (a.clamp && x > -1.0e-10 && x < 0.0) x = 0.0;
+    } else {
+      x = 0.0;
+    }
+    if (a.clamp) x = x + a.dtl * 0.0;
+    a.rhogq[p] = x;
+  }
+}
+
+__global__ void k_trc_vadv(TrcVadvArgs a, int pole) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l, g, lp;
+  if (!map_col(pole, t, i, j, l, g, lp)) return;
+  if (!pole) trc_vadv_column(col_reg(i, j, l), a);
+  else trc_vadv_column(col_pl(g, lp), a);
+}
+
+// ---------------------------------------------------------------------------
+// horizontal mass flux through the six hexagon edges and the upwind mass
+// centroids (mod_src_tracer.py:1376-1484), Courant numbers and the upwind
+// mask (mod_src_tracer.py:716-718)
+// ---------------------------------------------------------------------------
+struct TrcHfluxArgs {
+  const double *rho, *rvx, *rvy, *rvz;   // PROG_mean rhog and momentum (times RGAM on the fly)
+  const double* rhog_t;
+  double* flx[6];
+  double* xc[9];                          // face*3 + dir (AI, AIJ, AJ)
+  double* ch[6];
+  double* cm[6];
+  double dt;
+};
+
+// rho/rho*v at the two triangle vertices of cell (ii,jj): TI and TJ (4 fields),
+// before the singular-point fix
+__device__ void trc_vertex_raw(const TrcHfluxArgs& a, int ii, int jj, int k, int l, double TI[4], double TJ[4]) {
+  long long q0 = ix(ii, jj, k, l), qi = ix(ii + 1, jj, k, l), qd = ix(ii + 1, jj + 1, k, l), qj = ix(ii, jj + 1, k, l);
+  double w1i = P2(cG.GMTR_t, 0, ii, jj, l), w2i = P2(cG.GMTR_t, 1, ii, jj, l), w3i = P2(cG.GMTR_t, 2, ii, jj, l);
+  double w1j = P2(cG.GMTR_t, 3, ii, jj, l), w2j = P2(cG.GMTR_t, 4, ii, jj, l), w3j = P2(cG.GMTR_t, 5, ii, jj, l);
+  auto F = [&](int n, long long q) -> double {
+    if (n == 0) return a.rho[q];
+    const double* r = (n == 1) ? a.rvx : ((n == 2) ? a.rvy : a.rvz);
+    return r[q] * cG.RGAM[q];
+  };
+  for (int n = 0; n < 4; ++n) {
+    double f0 = F(n, q0), fi = F(n, qi), fd = F(n, qd), fj = F(n, qj);
+    double ti = f0 * w1i + fi * w2i;
+    ti = ti + fd * w3i;
+    double tj = f0 * w1j;
+    tj = tj + (fd * w2j + fj * w3j);
+    TI[n] = ti;
+    TJ[n] = tj;
+  }
+}
+
+// vertex values with the singular-point fix at (0,0) (mod_src_tracer.py:1409-1412)
+__device__ void trc_vertex(const TrcHfluxArgs& a, int ii, int jj, int k, int l, double TI[4], double TJ[4]) {
+  trc_vertex_raw(a, ii, jj, k, l, TI, TJ);
+  if (ii == 0 && jj == 0) {
+    double TI1[4], TJ1[4];
+    trc_vertex_raw(a, 1, 0, k, l, TI1, TJ1);
+    double m0 = (double)cG.pntmask[l * 2 + 0], m1 = (double)cG.pntmask[l * 2 + 1];
+    for (int n = 0; n < 4; ++n) TI[n] = TI[n] * m0 + TJ1[n] * m1;
+  }
+}
+
+// flux and centroid of face f of cell (ii,jj) given the summed vertex values
+__device__ __forceinline__ double trc_face(const TrcHfluxArgs& a, int ii, int jj, int l, int f, const double s[4],
+                                           double xc[3]) {
+  double rr2 = 1.0 / npmax(s[0], cC.EPS);
+  double flux = 0.5 * (s[1] * P2(cG.GMTR_a, f * 3 + 0, ii, jj, l) + s[2] * P2(cG.GMTR_a, f * 3 + 1, ii, jj, l) +
+                       s[3] * P2(cG.GMTR_a, f * 3 + 2, ii, jj, l));
+  for (int d = 0; d < 3; ++d) xc[d] = P2(cG.GRD_xr, f * 3 + d, ii, jj, l) - s[1 + d] * rr2 * a.dt * 0.5;
+  return flux;
+}
+
+// face f in {0,1,2} of cell (ii,jj): returns false if the reference leaves it zero
+__device__ bool trc_face_flux(const TrcHfluxArgs& a, int ii, int jj, int k, int l, int f, double& flux, double xc[3]) {
+  const int G = cD.G;
+  double s[4];
+  if (f == 0) {
+    if (!(ii >= 0 && ii <= G - 2 && jj >= 1 && jj <= G - 2)) return false;
+    double TIa[4], TJa[4], TIb[4], TJb[4];
+    trc_vertex(a, ii, jj - 1, k, l, TIb, TJb);
+    trc_vertex(a, ii, jj, k, l, TIa, TJa);
+    for (int n = 0; n < 4; ++n) s[n] = TJb[n] + TIa[n];
+  } else if (f == 1) {
+    if (!(ii >= 0 && ii <= G - 2 && jj >= 0 && jj <= G - 2)) return false;
+    double TIa[4], TJa[4];
+    trc_vertex(a, ii, jj, k, l, TIa, TJa);
+    for (int n = 0; n < 4; ++n) s[n] = TIa[n] + TJa[n];
+  } else {
+    if (!(ii >= 1 && ii <= G - 2 && jj >= 0 && jj <= G - 2)) return false;
+    double TIa[4], TJa[4], TIb[4], TJb[4];
+    trc_vertex(a, ii, jj, k, l, TIa, TJa);
+    trc_vertex(a, ii - 1, jj, k, l, TIb, TJb);
+    for (int n = 0; n < 4; ++n) s[n] = TJa[n] + TIb[n];
+  }
+  flux = trc_face(a, ii, jj, l, f, s, xc);
+  return true;
+}
+
+__global__ void k_trc_hflux(TrcHfluxArgs a) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (!col_of(t, i, j, l)) return;
+  const double dt = a.dt;
+  const double PR = P2(cG.GMTR_p, 0, i, j, l);
+  for (int k = 0; k < cD.KA; ++k) {
+    long long p = ix(i, j, k, l);
+    double fl[6];
+    double xc[3];
+    for (int f = 0; f < 3; ++f) {
+      double flux;
+      if (trc_face_flux(a, i, j, k, l, f, flux, xc)) {
+        fl[f] = flux * PR * dt;
+        for (int d = 0; d < 3; ++d) a.xc[f * 3 + d][p] = xc[d];
+      } else {
+        fl[f] = 0.0;
+        for (int d = 0; d < 3; ++d) a.xc[f * 3 + d][p] = 0.0;
+      }
+    }
+    // edges 3..5 are the opposite sides of the neighbours' edges 0..2
+    const int nbI[3] = {-1, -1, 0}, nbJ[3] = {0, -1, -1};
+    for (int f = 0; f < 3; ++f) {
+      double flux;
+      double xcn[3];
+      if (trc_face_flux(a, i + nbI[f], j + nbJ[f], k, l, f, flux, xcn)) fl[3 + f] = -flux * PR * dt;
+      else fl[3 + f] = 0.0;
+    }
+    if (i == 1 && j == 1) fl[5] *= (double)cG.pntmask[l * 2 + 0];
+    double rg = a.rhog_t[p];
+    for (int f = 0; f < 6; ++f) {
+      a.flx[f][p] = fl[f];
+      double chv = fl[f] / rg;
+      a.ch[f][p] = chv;
+      a.cm[f][p] = 0.5 - copysign(0.5, chv - cC.EPS);
+    }
+  }
+}
+
+// pole edges (mod_src_tracer.py:1487-1531) and Courant numbers
+struct TrcHfluxPlArgs {
+  const double *rho, *rvx, *rvy, *rvz, *rhog_t;
+  double *flx, *xc, *ch, *cm;   // flx/ch/cm (g,k,l); xc (g,k,l,3)
+  double dt;
+};
+
+__global__ void k_trc_hflux_pl(TrcHfluxPlArgs a) {
+  int t = threadIdx.x;
+  if (t >= cD.KA * cD.LP) return;
+  int k = t / cD.LP, lp = t % cD.LP;
+  const double* gt = cG.GMTR_t_pl;
+  const double* ga = cG.GMTR_a_pl;
+  const double* gp = cG.GMTR_p_pl;
+  double tv[6][4];
+  auto F = [&](int n, int q) -> double {
+    if (n == 0) return a.rho[q];
+    const double* r = (n == 1) ? a.rvx : ((n == 2) ? a.rvy : a.rvz);
+    return r[q] * cG.RGAM_pl[q];
+  };
+  for (int v = 1; v <= 5; ++v) {
+    int vp1 = (v + 1 == 6) ? 1 : v + 1;
+    const double* g5 = gt + (v * cD.LP + lp) * 5;
+    for (int n = 0; n < 4; ++n)
+      tv[v][n] = F(n, ipl(0, k, lp)) * g5[2] + F(n, ipl(v, k, lp)) * g5[3] + F(n, ipl(vp1, k, lp)) * g5[4];
+  }
+  double rc = a.rhog_t[ipl(0, k, lp)];
+  for (int v = 1; v <= 5; ++v) {
+    int vm1 = (v - 1 == 0) ? 5 : v - 1;
+    double rr2 = 1.0 / npmax(tv[vm1][0] + tv[v][0], cC.EPS);
+    double v2[3];
+    for (int n = 0; n < 3; ++n) v2[n] = tv[vm1][n + 1] + tv[v][n + 1];
+    const double* g18 = ga + (v * cD.LP + lp) * 18;
+    double flux = 0.5 * (v2[0] * g18[0] + v2[1] * g18[1] + v2[2] * g18[2]);
+    int q = ipl(v, k, lp);
+    double fl = flux * gp[(0 * cD.LP + lp) * 8 + 1] * a.dt;
+    a.flx[q] = fl;
+    for (int d = 0; d < 3; ++d) a.xc[q * 3 + d] = cG.GRD_xr_pl[(v * cD.LP + lp) * 3 + d] - v2[d] * rr2 * a.dt * 0.5;
+    double chv = fl / rc;
+    a.ch[q] = chv;
+    a.cm[q] = 0.5 - copysign(0.5, chv - cC.EPS);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// per tracer: q and its gradient (mod_src_tracer.py:758-771, 1634-1640)
+// ---------------------------------------------------------------------------
+__global__ void k_trc_grad(const double* rhogq, const double* rhog_t, double* q, double* gq0, double* gq1,
+                           double* gq2) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (col_of(t, i, j, l)) {
+    const bool in = interior(i, j);
+    for (int k = 0; k < cD.KA; ++k) {
+      long long p = ix(i, j, k, l);
+      q[p] = rhogq[p] / rhog_t[p];
+      double g[3] = {0.0, 0.0, 0.0};
+      if (in) grad7(i, j, k, l, [&](int ii, int jj, int kk) { long long qq = ix(ii, jj, kk, l); return rhogq[qq] / rhog_t[qq]; }, g);
+      gq0[p] = g[0]; gq1[p] = g[1]; gq2[p] = g[2];
+    }
+  }
+}
+
+__global__ void k_trc_grad_pl(const double* rhogq, const double* rhog_t, double* q, double* gq0, double* gq1,
+                              double* gq2) {
+  int t = threadIdx.x;
+  if (t >= cD.KA * cD.LP) return;
+  int k = t / cD.LP, lp = t % cD.LP;
+  double qv[6];
+  for (int v = 0; v < 6; ++v) {
+    int p = ipl(v, k, lp);
+    qv[v] = rhogq[p] / rhog_t[p];
+    q[p] = qv[v];
+  }
+  double* gq[3] = {gq0, gq1, gq2};
+  for (int d = 0; d < 3; ++d) {
+    double row = 0.0;
+    for (int v = 0; v < 6; ++v) {
+      double tv = cG.coef_grad_pl[(v * cD.LP + lp) * 3 + d] * qv[v];
+      row = (v == 0) ? tv : row + tv;
+    }
+    gq[d][ipl(0, k, lp)] = row;
+    for (int v = 1; v < 6; ++v) gq[d][ipl(v, k, lp)] = 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// MIURA2004 face values of edges 0..2 (mod_src_tracer.py:1696-1787)
+// ---------------------------------------------------------------------------
+struct TrcRemapArgs {
+  const double *q, *gq0, *gq1, *gq2;
+  const double* xc[9];
+  const double* cm[6];
+  double* qa[3];
+};
+
+__device__ __forceinline__ double trc_rec(const TrcRemapArgs& a, int ii, int jj, int k, int l, long long pxc, int f) {
+  long long q = ix(ii, jj, k, l);
+  double r = a.q[q];
+  r = r + a.gq0[q] * (a.xc[f * 3 + 0][pxc] - P2(cG.GRD_x, 0, ii, jj, l));
+  r = r + a.gq1[q] * (a.xc[f * 3 + 1][pxc] - P2(cG.GRD_x, 1, ii, jj, l));
+  r = r + a.gq2[q] * (a.xc[f * 3 + 2][pxc] - P2(cG.GRD_x, 2, ii, jj, l));
+  return r;
+}
+
+__global__ void k_trc_remap(TrcRemapArgs a) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (!col_of(t, i, j, l)) return;
+  const int G = cD.G;
+  const bool ok = (i <= G - 2 && j <= G - 2);
+  for (int k = 0; k < cD.KA; ++k) {
+    long long p = ix(i, j, k, l);
+    if (!ok) {
+      a.qa[0][p] = 0.0; a.qa[1][p] = 0.0; a.qa[2][p] = 0.0;
+      continue;
+    }
+    const int mi[3] = {1, 1, 0}, mj[3] = {0, 1, 1};
+    for (int f = 0; f < 3; ++f) {
+      double ap = trc_rec(a, i, j, k, l, p, f);
+      double am = trc_rec(a, i + mi[f], j + mj[f], k, l, p, f);
+      double c = a.cm[f][p];
+      a.qa[f][p] = c * am + (1.0 - c) * ap;
+    }
+  }
+}
+
+struct TrcRemapPlArgs {
+  const double *q, *gq0, *gq1, *gq2, *xc, *cm;
+  double* qa;
+};
+
+__global__ void k_trc_remap_pl(TrcRemapPlArgs a) {
+  int t = threadIdx.x;
+  if (t >= cD.KA * cD.LP) return;
+  int k = t / cD.LP, lp = t % cD.LP;
+  const double* X = cG.GRD_x_pl;
+  const double* gq[3] = {a.gq0, a.gq1, a.gq2};
+  int p0 = ipl(0, k, lp);
+  for (int v = 1; v <= 5; ++v) {
+    int pv = ipl(v, k, lp);
+    double ap = a.q[p0];
+    for (int d = 0; d < 3; ++d) ap = ap + gq[d][p0] * (a.xc[pv * 3 + d] - X[(0 * cD.LP + lp) * 3 + d]);
+    double am = a.q[pv];
+    for (int d = 0; d < 3; ++d) am = am + gq[d][pv] * (a.xc[pv * 3 + d] - X[(v * cD.LP + lp) * 3 + d]);
+    double c = a.cm[pv];
+    a.qa[pv] = c * am + (1.0 - c) * ap;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// horizontal Thuburn limiter (mod_src_tracer.py:2190-2605, numpy branch)
+// ---------------------------------------------------------------------------
+struct TrcLimArgs {
+  const double *q, *rhog_t, *frhog;
+  const double* ch[6];
+  const double* cm[6];
+  const double* qa[3];
+  const double *qout_min, *qout_max;
+  double *Qmin, *Qmax;          // Qout (output of the Qout kernel)
+  const double* flx[6];
+  double* rhogq;
+  double dt;
+};
+
+// q_min / q_max over the stencil of edge f of cell (a,b) (mod_src_tracer.py:2191-2217)
+__device__ void trc_face_minmax(const double* q, int a, int b, int k, int l, int f, double& qn, double& qx) {
+  auto Q = [&](int ii, int jj) { return q[ix(ii, jj, k, l)]; };
+  double q0 = Q(a, b);
+  double q2 = Q(a + 1, b), q3 = Q(a + 1, b + 1), qj = Q(a, b + 1);
+  double v1, v2, v3;
+  if (f == 0) {
+    double q1 = (b > 0) ? Q(a, b - 1) : Q(0, 0);
+    v1 = q1; v2 = q2; v3 = q3;
+  } else if (f == 1) {
+    v1 = q2; v2 = q3; v3 = qj;
+  } else {
+    double q4 = (a > 0) ? Q(a - 1, b) : Q(0, 0);
+    v1 = q3; v2 = qj; v3 = q4;
+  }
+  qn = npmin(npmin(npmin(q0, v1), v2), v3);
+  qx = npmax(npmax(npmax(q0, v1), v2), v3);
+}
+
+// Qin of slot m (0..5) of cell (i,j): slots 0..2 from the cell's own edges,
+// slots 3..5 from the neighbours' edges 0..2 (mod_src_tracer.py:2220-2234 and
+// the singular-point override :2298-2323)
+__device__ void trc_qin(const TrcLimArgs& a, int i, int j, int k, int l, int m, double& qin_min, double& qin_max) {
+  const double BIG = cC.HUGE_;
+  int ai = i, bj = j, f = m;
+  if (m >= 3) {
+    const int nbI[3] = {-1, -1, 0}, nbJ[3] = {0, -1, -1};
+    ai = i + nbI[m - 3];
+    bj = j + nbJ[m - 3];
+    f = m - 3;
+  }
+  double cmv = a.cm[f][ix(ai, bj, k, l)];
+  double qn, qx;
+  const bool sgp = cG.have_sgp[l] && ai == 0 && bj == 0 && f == 1;
+  if (sgp) {
+    auto Q = [&](int ii, int jj) { return a.q[ix(ii, jj, k, l)]; };
+    // np.min over [q(0,0), q(1,1), q(2,1), q(0,1)]
+    qn = npmin(npmin(npmin(Q(0, 0), Q(1, 1)), Q(2, 1)), Q(0, 1));
+    qx = npmax(npmax(npmax(Q(0, 0), Q(1, 1)), Q(2, 1)), Q(0, 1));
+    if (m < 3) {
+      qin_min = (cmv == 1.0) ? qn : BIG;
+      qin_max = (cmv == 1.0) ? qx : -BIG;
+    } else {
+      qin_min = (cmv == 1.0) ? BIG : qn;
+      qin_max = (cmv == 1.0) ? -BIG : qx;
+    }
+    return;
+  }
+  trc_face_minmax(a.q, ai, bj, k, l, f, qn, qx);
+  if (m < 3) {
+    qin_min = cmv * qn + (1.0 - cmv) * BIG;
+    qin_max = cmv * qx + (1.0 - cmv) * (-BIG);
+  } else {
+    qin_min = cmv * BIG + (1.0 - cmv) * qn;
+    qin_max = cmv * (-BIG) + (1.0 - cmv) * qx;
+  }
+}
+
+__global__ void k_trc_qout(TrcLimArgs a) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (!col_of(t, i, j, l)) return;
+  const bool in = interior(i, j);
+  const double EPS = cC.EPS;
+  for (int k = 0; k < cD.KA; ++k) {
+    long long p = ix(i, j, k, l);
+    double qc = a.q[p];
+    if (!in) {
+      a.Qmin[p] = qc;
+      a.Qmax[p] = qc;
+      continue;
+    }
+    double qnmin = qc, qnmax = qc;
+    double Cin = 0.0, Cout = 0.0, CQmin = 0.0, CQmax = 0.0;
+    for (int m = 0; m < 6; ++m) {
+      double qi, qx;
+      trc_qin(a, i, j, k, l, m, qi, qx);
+      qnmin = npmin(qnmin, qi);
+      qnmax = npmax(qnmax, qx);
+      double chv = a.ch[m][p];
+      double chm = npmin(chv, 0.0);
+      if (m == 0) {
+        Cin = chm; Cout = chv - chm; CQmin = chm * qi; CQmax = chm * qx;
+      } else {
+        Cin = Cin + chm; Cout = Cout + (chv - chm); CQmin = CQmin + chm * qi; CQmax = CQmax + chm * qx;
+      }
+    }
+    double zsw = 0.5 - copysign(0.5, fabs(Cout) - EPS);
+    double d = 1.0 * a.frhog[p] / a.rhog_t[p] * a.dt;
+    a.Qmin[p] = (qc - CQmax - qnmax * (1.0 - Cin - Cout + d)) / (Cout + zsw) * (1.0 - zsw) + qc * zsw;
+    a.Qmax[p] = (qc - CQmin - qnmin * (1.0 - Cin - Cout + d)) / (Cout + zsw) * (1.0 - zsw) + qc * zsw;
+  }
+}
+
+// limited value of edge f in {0,1,2} of cell (ai,bj) (mod_src_tracer.py:2545-2605)
+__device__ double trc_limited_face(const TrcLimArgs& a, int ai, int bj, int k, int l, int f) {
+  const int mi[3] = {1, 1, 0}, mj[3] = {0, 1, 1};
+  int ni = ai + mi[f], nj = bj + mj[f];
+  long long p = ix(ai, bj, k, l), pn = ix(ni, nj, k, l);
+  double c = a.cm[f][p];
+  double qa = a.qa[f][p];
+  double qi0, qx0, qi1, qx1;
+  trc_qin(a, ai, bj, k, l, f, qi0, qx0);
+  trc_qin(a, ni, nj, k, l, 3 + f, qi1, qx1);
+  qa = c * npmin(npmax(qa, qi0), qx0) + (1.0 - c) * npmin(npmax(qa, qi1), qx1);
+  qa = c * npmax(npmin(qa, a.qout_max[pn]), a.qout_min[pn]) + (1.0 - c) * npmax(npmin(qa, a.qout_max[p]), a.qout_min[p]);
+  return qa;
+}
+
+__global__ void k_trc_apply(TrcLimArgs a) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (!col_of(t, i, j, l)) return;
+  if (!interior(i, j)) return;
+  for (int k = 0; k < cD.KA; ++k) {
+    long long p = ix(i, j, k, l);
+    double q0 = trc_limited_face(a, i, j, k, l, 0);
+    double q1 = trc_limited_face(a, i, j, k, l, 1);
+    double q2 = trc_limited_face(a, i, j, k, l, 2);
+    double q3 = trc_limited_face(a, i - 1, j, k, l, 0);
+    double q4 = trc_limited_face(a, i - 1, j - 1, k, l, 1);
+    double q5 = trc_limited_face(a, i, j - 1, k, l, 2);
+    double upd = a.flx[0][p] * q0 + a.flx[1][p] * q1 + a.flx[2][p] * q2 + a.flx[3][p] * q3 + a.flx[4][p] * q4 +
+                 a.flx[5][p] * q5;
+    a.rhogq[p] = a.rhogq[p] - upd;
+  }
+}
+
+// pole Qout (mod_src_tracer.py:2437-2495) at g = 0
+struct TrcLimPlArgs {
+  const double *q, *ch, *cm, *rhog_t, *frhog, *qa, *flx;
+  double *Qmin, *Qmax;
+  const double *qout_min, *qout_max;
+  double* rhogq;
+  double dt;
+};
+
+__device__ void trc_qin_pl(const TrcLimPlArgs& a, int v, int k, int lp, double& in0n, double& in1n, double& in0x,
+                           double& in1x) {
+  const double BIG = cC.HUGE_;
+  int vp1 = (v + 1 > 5) ? 1 : v + 1, vm1 = (v - 1 < 1) ? 5 : v - 1;
+  double q0 = a.q[ipl(0, k, lp)], qv = a.q[ipl(v, k, lp)], qm = a.q[ipl(vm1, k, lp)], qp = a.q[ipl(vp1, k, lp)];
+  double qn = pymin(pymin(pymin(q0, qv), qm), qp);
+  double qx = pymax(pymax(pymax(q0, qv), qm), qp);
+  double c = a.cm[ipl(v, k, lp)];
+  in0n = (c == 1.0) ? qn : BIG;
+  in1n = (c == 1.0) ? BIG : qn;
+  in0x = (c == 1.0) ? qx : -BIG;
+  in1x = (c == 1.0) ? -BIG : qx;
+}
+
+__global__ void k_trc_qout_pl(TrcLimPlArgs a) {
+  int t = threadIdx.x;
+  if (t >= cD.KA * cD.LP) return;
+  int k = t / cD.LP, lp = t % cD.LP;
+  int p0 = ipl(0, k, lp);
+  double qnm = a.q[p0], qnx = a.q[p0];
+  double in0n[6], in0x[6], d1, d2;
+  for (int v = 1; v <= 5; ++v) {
+    trc_qin_pl(a, v, k, lp, in0n[v], d1, in0x[v], d2);
+    qnm = pymin(qnm, in0n[v]);
+    qnx = pymax(qnx, in0x[v]);
+  }
+  double Ci = 0.0, Co = 0.0, CQn = 0.0, CQx = 0.0;
+  for (int v = 1; v <= 5; ++v) {
+    int pv = ipl(v, k, lp);
+    double chm = a.cm[pv] * a.ch[pv];
+    Ci = Ci + chm;
+    Co = Co + (a.ch[pv] - chm);
+    CQn = CQn + chm * in0n[v];
+    CQx = CQx + chm * in0x[v];
+  }
+  double zs = 0.5 - copysign(0.5, fabs(Co) - cC.EPS);
+  double den = Co + zs;
+  double fac = 1.0 - zs;
+  double q0 = a.q[p0];
+  double dv = 1.0 * a.frhog[p0] / a.rhog_t[p0] * a.dt;
+  a.Qmin[p0] = (q0 - CQx - qnx * (1.0 - Ci - Co + dv)) / den * fac + q0 * zs;
+  a.Qmax[p0] = (q0 - CQn - qnm * (1.0 - Ci - Co + dv)) / den * fac + q0 * zs;
+}
+
+__global__ void k_trc_apply_pl(TrcLimPlArgs a) {
+  int t = threadIdx.x;
+  if (t >= cD.KA * cD.LP) return;
+  int k = t / cD.LP, lp = t % cD.LP;
+  int p0 = ipl(0, k, lp);
+  double acc = a.rhogq[p0];
+  for (int v = 1; v <= 5; ++v) {
+    int pv = ipl(v, k, lp);
+    double in0n, in1n, in0x, in1x;
+    trc_qin_pl(a, v, k, lp, in0n, in1n, in0x, in1x);
+    double c = a.cm[pv];
+    double x = a.qa[pv];
+    double a0 = npmin(npmax(x, in0n), in0x);
+    double a1 = npmin(npmax(x, in1n), in1x);
+    x = c * a0 + (1.0 - c) * a1;
+    double a2 = npmax(npmin(x, a.qout_max[pv]), a.qout_min[pv]);
+    double a3 = npmax(npmin(x, a.qout_max[p0]), a.qout_min[p0]);
+    x = c * a2 + (1.0 - c) * a3;
+    acc = acc - a.flx[pv] * x;
+  }
+  a.rhogq[p0] = acc;
+}
+
+// density after the horizontal step (mod_src_tracer.py:890-916)
+__global__ void k_trc_rhog(double* rhog_t, const double* f0, const double* f1, const double* f2, const double* f3,
+                           const double* f4, const double* f5, const double* frhog, double dt, const double* flx_pl,
+                           double* rhog_t_pl, const double* frhog_pl) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (col_of(t, i, j, l)) {
+    if (!interior(i, j)) return;
+    for (int k = 0; k < cD.KA; ++k) {
+      long long p = ix(i, j, k, l);
+      double s = f0[p] + f1[p] + f2[p] + f3[p] + f4[p] + f5[p];
+      rhog_t[p] = rhog_t[p] - (s - (1.0 * frhog[p] * dt));
+    }
+  } else {
+    long long tp = t - cD.npt2;
+    if (tp < cD.KA * cD.LP) {
+      int k = (int)(tp / cD.LP), lp = (int)(tp % cD.LP);
+      int p0 = ipl(0, k, lp);
+      double r = rhog_t_pl[p0];
+      for (int v = 1; v <= 5; ++v) r = r - flx_pl[ipl(v, k, lp)];
+      r = r + 1.0 * frhog_pl[p0] * dt;
+      rhog_t_pl[p0] = r;
+    }
+  }
+}
+
+}  // namespace nc

@@ -1,0 +1,220 @@
+"""ctypes binding of libnicamcuda.so and the device-resident dynamics object.
+
+``NicamCuda`` owns one C-ABI handle: it turns a setup dict (the reference's
+geometry/metric/operator arrays under their attribute names) into the
+``nc_array`` table of ``nc_create``, and exposes the step, marshal and budget
+calls.  The library is loaded from this package directory only; if it is
+missing or cannot be loaded, construction raises -- there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import halo
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_NAME = "libnicamcuda.so"
+LIB_PATH = os.path.join(_HERE, LIB_NAME)
+
+NC_F64, NC_I32, NC_I64, NC_BOOL = 0, 1, 2, 3
+
+
+class NcArray(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char_p), ("data", ctypes.c_void_p), ("dtype", ctypes.c_int32),
+                ("ndim", ctypes.c_int32), ("shape", ctypes.c_int64 * 8)]
+
+
+_lib = None
+
+# every entry point declared in include/nicam_cuda.h
+EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync",
+           "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_last_error",
+           "nc_destroy")
+
+
+def load_library(path: str = LIB_PATH):
+    """Load (once) and type the C ABI.  Raises OSError if the library is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError(f"{LIB_NAME} not built: run __graft_entry__.build() (expected at {path})")
+    lib = ctypes.CDLL(path)
+    vp, i32, i64, dp = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p
+    lib.nc_create.argtypes = [ctypes.POINTER(NcArray), i32, ctypes.POINTER(vp)]
+    lib.nc_upload_state.argtypes = [vp, dp, dp]
+    lib.nc_download_state.argtypes = [vp, dp, dp]
+    lib.nc_step.argtypes = [vp, i32]
+    lib.nc_set_graph.argtypes = [vp, i32]
+    lib.nc_run_phases.argtypes = [vp, i32]
+    lib.nc_sync.argtypes = [vp]
+    lib.nc_mass_sums.argtypes = [vp, dp, i32]
+    lib.nc_get_field.argtypes = [vp, ctypes.c_char_p, dp, dp]
+    lib.nc_state_pointers.argtypes = [vp, i32, ctypes.POINTER(vp), ctypes.POINTER(vp)]
+    lib.nc_kernel_launches.argtypes = [vp]
+    lib.nc_kernel_launches.restype = i64
+    lib.nc_last_error.restype = ctypes.c_char_p
+    lib.nc_destroy.argtypes = [vp]
+    lib.nc_destroy.restype = None
+    for f in ("nc_create", "nc_upload_state", "nc_download_state", "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync",
+              "nc_mass_sums", "nc_get_field", "nc_state_pointers"):
+        getattr(lib, f).restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+class NicamError(RuntimeError):
+    pass
+
+
+def _check(rc: int):
+    if rc != 0:
+        msg = _lib.nc_last_error().decode(errors="replace")
+        raise NicamError(f"libnicamcuda status {rc}: {msg}")
+
+
+def _dtype_code(a: np.ndarray) -> int:
+    if a.dtype == np.float64:
+        return NC_F64
+    if a.dtype == np.int32:
+        return NC_I32
+    if a.dtype == np.int64:
+        return NC_I64
+    if a.dtype == np.bool_:
+        return NC_BOOL
+    raise TypeError(f"unsupported dtype {a.dtype}")
+
+
+def setup_table(geo: dict) -> dict:
+    """Host arrays handed to ``nc_create`` (names as in include/nicam_cuda.h).
+
+    ``geo`` holds the reference's arrays under their attribute names (the
+    layout of ``tests/golden`` fixtures).  Column subsets the device needs are
+    cut here: GMTR_t weights W1..W3, GMTR_a outward normals HNX..HNZ of the
+    three edges, GMTR_p inverse area.
+    """
+    t = {}
+    for k in ("kall", "kmin", "kmax", "gall_1d", "gmin", "gmax", "lall", "nq"):
+        t[k] = np.asarray(int(np.asarray(geo[k])), np.int64)
+    for k in ("GRAV", "Rdry", "CVdry", "CPdry", "Rvap", "OHM", "EPS", "HUGE", "rscale", "alpha", "dtl", "dts",
+              "Kh_coef", "divdamp_coef", "hdiff_fact_rho"):
+        t[k] = np.asarray(float(np.asarray(geo[k])), np.float64)
+    t["CVW"] = np.ascontiguousarray(geo["CVW"], np.float64)
+    t["sstep"] = np.ascontiguousarray(geo["sstep"], np.int64)
+    for k in ("GRD_afact", "GRD_bfact", "GRD_cfact", "GRD_dfact", "GRD_rdgz", "GRD_rdgzh"):
+        t[k] = np.ascontiguousarray(geo[k], np.float64)
+    for k in ("VMTR_GSGAM2", "VMTR_GSGAM2H", "VMTR_RGSGAM2", "VMTR_RGSGAM2H", "VMTR_RGSQRTH", "VMTR_RGAM",
+              "VMTR_RGAMH", "VMTR_GAM2H", "VMTR_PHI", "VMTR_C2Wfact", "VMTR_W2Cfact", "VMTR_C2WfactGz",
+              "VMTR_VOLUME", "rho_bs", "pre_bs", "tem_bs",
+              "OPRT_coef_div", "OPRT_coef_grad", "OPRT_coef_lap", "OPRT_coef_intp", "OPRT_coef_diff",
+              "GRD_x", "GRD_xr"):
+        t[k] = np.ascontiguousarray(geo[k], np.float64)
+        pk = k + "_pl"
+        if pk in geo:
+            t[pk] = np.ascontiguousarray(geo[pk], np.float64)
+    for k in ("GMTR_t_pl", "GMTR_a_pl", "GMTR_p_pl"):
+        t[k] = np.ascontiguousarray(geo[k], np.float64)
+    t["GMTR_t_W"] = np.ascontiguousarray(np.asarray(geo["GMTR_t"])[..., 2:5], np.float64)
+    t["GMTR_a_HN"] = np.ascontiguousarray(np.asarray(geo["GMTR_a"])[..., 0:3], np.float64)
+    t["GMTR_p_RAREA"] = np.ascontiguousarray(np.asarray(geo["GMTR_p"])[..., 1:2], np.float64)
+    t["pntmask"] = np.ascontiguousarray(geo["pntmask"], np.int32)
+    t["have_sgp"] = np.ascontiguousarray(geo["have_sgp"], np.bool_)
+    plan = halo.compose(geo["copy_r2r"], geo["copy_p2r"], geo["copy_r2p"], geo["copy_sgp"],
+                        int(np.asarray(geo["gall_1d"])), int(np.asarray(geo["lall"])))
+    for k, v in zip(("halo_r_dst", "halo_r_src", "halo_p_dst", "halo_p_src"), plan):
+        t[k] = np.ascontiguousarray(v, np.int64)
+    return t
+
+
+class NicamCuda:
+    """One device-resident NICAM-DC dynamical core (one C-ABI handle)."""
+
+    def __init__(self, geo: dict, graph: bool = True):
+        lib = load_library()
+        self._lib = lib
+        self._tab = setup_table(geo)
+        names, arrs = [], []
+        entries = (NcArray * len(self._tab))()
+        for n, (k, a) in enumerate(self._tab.items()):
+            a = np.ascontiguousarray(a)
+            self._tab[k] = a
+            names.append(k.encode())
+            e = entries[n]
+            e.name = names[-1]
+            e.data = a.ctypes.data
+            e.dtype = _dtype_code(a)
+            e.ndim = a.ndim
+            for d in range(a.ndim):
+                e.shape[d] = a.shape[d]
+        self._names = names
+        h = ctypes.c_void_p()
+        _check(lib.nc_create(entries, len(self._tab), ctypes.byref(h)))
+        self._h = h
+        _check(lib.nc_set_graph(h, 1 if graph else 0))
+        G = int(self._tab["gall_1d"])
+        self.shape = (G, G, int(self._tab["kall"]), int(self._tab["lall"]), 6 + int(self._tab["nq"]))
+        self.shape_pl = (6, int(self._tab["kall"]), 2, 6 + int(self._tab["nq"]))
+
+    # ---- state marshal (host arrays in the reference layout)
+    def upload(self, prg: np.ndarray, prg_pl: np.ndarray):
+        if prg.shape != self.shape or prg_pl.shape != self.shape_pl:
+            raise ValueError(f"state shape {prg.shape}/{prg_pl.shape}, expected {self.shape}/{self.shape_pl}")
+        prg = np.ascontiguousarray(prg, np.float64)
+        prg_pl = np.ascontiguousarray(prg_pl, np.float64)
+        self._keep = (prg, prg_pl)
+        _check(self._lib.nc_upload_state(self._h, prg.ctypes.data, prg_pl.ctypes.data))
+
+    def upload_ptr(self, prg_ptr: int, prg_pl_ptr: int):
+        """upload from raw host pointers (e.g. pinned torch tensors)"""
+        _check(self._lib.nc_upload_state(self._h, prg_ptr, prg_pl_ptr))
+
+    def download(self, prg: np.ndarray = None, prg_pl: np.ndarray = None):
+        if prg is None:
+            prg = np.empty(self.shape)
+        if prg_pl is None:
+            prg_pl = np.empty(self.shape_pl)
+        _check(self._lib.nc_download_state(self._h, prg.ctypes.data, prg_pl.ctypes.data))
+        return prg, prg_pl
+
+    def download_ptr(self, prg_ptr: int, prg_pl_ptr: int):
+        _check(self._lib.nc_download_state(self._h, prg_ptr, prg_pl_ptr))
+
+    def step(self, nsteps: int = 1):
+        _check(self._lib.nc_step(self._h, int(nsteps)))
+
+    def run_phases(self, nphases: int):
+        """debugging: run the first ``nphases`` phases of one step"""
+        _check(self._lib.nc_run_phases(self._h, int(nphases)))
+
+    def sync(self):
+        _check(self._lib.nc_sync(self._h))
+
+    def mass_sums(self):
+        n = 1 + int(self._tab["nq"])
+        out = np.zeros(n)
+        _check(self._lib.nc_mass_sums(self._h, out.ctypes.data, n))
+        return out
+
+    def field(self, name: str):
+        """a named device work field in the reference layout (debug / parity)"""
+        reg = np.empty(self.shape[:4])
+        pl = np.empty(self.shape_pl[:3])
+        _check(self._lib.nc_get_field(self._h, name.encode(), reg.ctypes.data, pl.ctypes.data))
+        return reg, pl
+
+    def kernel_launches(self) -> int:
+        return int(self._lib.nc_kernel_launches(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.nc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

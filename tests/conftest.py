@@ -1,0 +1,28 @@
+import importlib
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+if GOLDEN not in sys.path:
+    sys.path.insert(0, GOLDEN)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+
+
+@pytest.fixture(scope="session")
+def pkg():
+    """the product package (its directory name is not a Python identifier)"""
+    return importlib.import_module("pynicam-dc_b200")
+
+
+@pytest.fixture(scope="session")
+def golden():
+    from make_golden import load
+    return load(os.path.join(GOLDEN, "gl03_z10_trc.npz"))
