@@ -101,6 +101,19 @@ int nc_state_pointers(nc_handle* h, int32_t v, double** reg, double** pl);
 /* Number of kernels the library launched since the handle was created. */
 int64_t nc_kernel_launches(nc_handle* h);
 
+/* Grid generation helper (no counterpart in the reference's step interface;
+ * restates the spring-dynamics smoothing of prep/hgrid/mod_mkgrd.py:204-320).
+ * x (lall, gall_1d, gall_1d, 3) region-major unit vectors with halos filled,
+ * x_pl (2, 6, 3) pole points, both updated in place; the halo plan arrays are
+ * those of nc_create (halo_r_dst, halo_r_src, halo_p_dst, halo_p_src).  Runs
+ * until max |F|/lambda < criterion (NC_ERR_STATE after max_iter iterations);
+ * the iteration count is written to *iterations.  Synchronous; allocates and
+ * frees its own device memory. */
+int nc_grid_spring(int32_t lall, int32_t gall_1d, double* x, double* x_pl, const unsigned char* have_sgp,
+                   const int64_t* r_dst, const int64_t* r_src, int32_t nr, const int64_t* p_dst,
+                   const int64_t* p_src, int32_t np, double lambda, double dbar, double dt, double criterion,
+                   int64_t max_iter, int64_t* iterations);
+
 const char* nc_last_error(void);
 
 void nc_destroy(nc_handle* h);

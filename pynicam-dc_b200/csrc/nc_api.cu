@@ -10,6 +10,7 @@
 
 #include "../../include/nicam_cuda.h"
 #include "nc_tracer.cuh"
+#include "nc_grid.cuh"
 
 using namespace nc;
 
@@ -1051,6 +1052,106 @@ int nc_state_pointers(nc_handle* h, int32_t v, double** reg, double** pl) {
   *reg = f.r;
   *pl = f.p;
   return 0;
+}
+
+// grid generation helper: spring-dynamics relaxation (see nc_grid.cuh)
+static int spring_impl(int32_t L, int32_t G, double* x, double* x_pl, const unsigned char* have_sgp,
+                       const int64_t* r_dst, const int64_t* r_src, int32_t nr, const int64_t* p_dst,
+                       const int64_t* p_src, int32_t np, double lam, double dbar, double dt, double crit,
+                       int64_t max_iter, int64_t* iters_out, std::vector<void*>& mem, cudaStream_t& st,
+                       cudaGraph_t& graph, cudaGraphExec_t& gexec) {
+  const size_t plane = (size_t)L * G * G;
+  auto alloc = [&](void** p, size_t bytes) -> int {
+    CU(cudaMalloc(p, bytes));
+    mem.push_back(*p);
+    return 0;
+  };
+  SpringDev s{};
+  std::vector<double> h(plane);
+  for (int b = 0; b < 2; ++b)
+    for (int d = 0; d < 3; ++d) {
+      TRY(alloc((void**)&s.R[b][d], plane * sizeof(double)));
+      for (size_t q = 0; q < plane; ++q) h[q] = x[q * 3 + d];
+      CU(cudaMemcpy(s.R[b][d], h.data(), plane * sizeof(double), cudaMemcpyHostToDevice));
+    }
+  for (int d = 0; d < 3; ++d) {
+    TRY(alloc((void**)&s.W[d], plane * sizeof(double)));
+    CU(cudaMemset(s.W[d], 0, plane * sizeof(double)));
+    double pl[12];
+    for (int g = 0; g < 6; ++g)
+      for (int lp = 0; lp < 2; ++lp) pl[g * 2 + lp] = x_pl[(lp * 6 + g) * 3 + d];
+    TRY(alloc((void**)&s.Rpl[d], sizeof(pl)));
+    CU(cudaMemcpy(s.Rpl[d], pl, sizeof(pl), cudaMemcpyHostToDevice));
+  }
+  const void* src[4] = {r_dst, r_src, p_dst, p_src};
+  const long long** dst[4] = {&s.r_dst, &s.r_src, &s.p_dst, &s.p_src};
+  const int cnt[4] = {nr, nr, np, np};
+  for (int n = 0; n < 4; ++n) {
+    TRY(alloc((void**)dst[n], (size_t)std::max(cnt[n], 1) * sizeof(long long)));
+    if (cnt[n]) CU(cudaMemcpy((void*)*dst[n], src[n], cnt[n] * sizeof(long long), cudaMemcpyHostToDevice));
+  }
+  TRY(alloc((void**)&s.sgp, L));
+  CU(cudaMemcpy((void*)s.sgp, have_sgp, L, cudaMemcpyHostToDevice));
+  TRY(alloc((void**)&s.fmax, sizeof(unsigned long long)));
+  TRY(alloc((void**)&s.done, sizeof(int)));
+  TRY(alloc((void**)&s.iters, sizeof(long long)));
+  CU(cudaMemset(s.fmax, 0, sizeof(unsigned long long)));
+  CU(cudaMemset(s.done, 0, sizeof(int)));
+  CU(cudaMemset(s.iters, 0, sizeof(long long)));
+  s.nr = nr; s.np = np; s.G = G; s.L = L; s.lam = lam; s.dbar = dbar; s.dt = dt; s.crit = crit;
+  CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  const int n = G - 2;
+  const unsigned bstep = (unsigned)(((long long)L * n * n + 255) / 256);
+  const unsigned bcomm = (unsigned)((nr + np + 255) / 256);
+  const int chunk = 256;   // even: buffer roles repeat every chunk
+  CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  for (int it = 0; it < chunk; ++it) {
+    const int sb = it & 1;
+    k_spring_step<<<bstep, 256, 0, st>>>(s, sb);
+    k_spring_comm<<<bcomm, 256, 0, st>>>(s, 1 - sb);
+    k_spring_check<<<1, 1, 0, st>>>(s);
+  }
+  CU(cudaStreamEndCapture(st, &graph));
+  CU(cudaGraphInstantiate(&gexec, graph, 0));
+  long long iters = 0;
+  int done = 0;
+  while (!done && iters < max_iter) {
+    CU(cudaGraphLaunch(gexec, st));
+    CU(cudaStreamSynchronize(st));
+    CU(cudaMemcpy(&done, s.done, sizeof(int), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(&iters, s.iters, sizeof(long long), cudaMemcpyDeviceToHost));
+  }
+  const int fb = (int)(iters & 1);
+  for (int d = 0; d < 3; ++d) {
+    CU(cudaMemcpy(h.data(), s.R[fb][d], plane * sizeof(double), cudaMemcpyDeviceToHost));
+    for (size_t q = 0; q < plane; ++q) x[q * 3 + d] = h[q];
+    double pl[12];
+    CU(cudaMemcpy(pl, s.Rpl[d], sizeof(pl), cudaMemcpyDeviceToHost));
+    for (int g = 0; g < 6; ++g)
+      for (int lp = 0; lp < 2; ++lp) x_pl[(lp * 6 + g) * 3 + d] = pl[g * 2 + lp];
+  }
+  *iters_out = iters;
+  return done ? 0 : fail(NC_ERR_STATE, "spring relaxation did not converge within max_iter");
+}
+
+int nc_grid_spring(int32_t lall, int32_t gall_1d, double* x, double* x_pl, const unsigned char* have_sgp,
+                   const int64_t* r_dst, const int64_t* r_src, int32_t nr, const int64_t* p_dst,
+                   const int64_t* p_src, int32_t np, double lambda, double dbar, double dt, double criterion,
+                   int64_t max_iter, int64_t* iterations) {
+  if (!x || !x_pl || !have_sgp || !iterations || lall <= 0 || gall_1d < 4 || nr < 0 || np < 0)
+    return fail(NC_ERR_ARG, "nc_grid_spring: bad argument");
+  std::vector<void*> mem;
+  cudaStream_t st = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int rc = spring_impl(lall, gall_1d, x, x_pl, have_sgp, r_dst, r_src, nr, p_dst, p_src, np, lambda, dbar, dt,
+                       criterion, max_iter, iterations, mem, st, graph, gexec);
+  if (gexec) cudaGraphExecDestroy(gexec);
+  if (graph) cudaGraphDestroy(graph);
+  if (st) cudaStreamSynchronize(st);
+  for (void* p : mem) cudaFree(p);
+  if (st) cudaStreamDestroy(st);
+  return rc;
 }
 
 }  // extern "C"

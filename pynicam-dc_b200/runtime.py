@@ -31,8 +31,8 @@ _lib = None
 
 # every entry point declared in include/nicam_cuda.h
 EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync",
-           "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_last_error",
-           "nc_destroy")
+           "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_grid_spring",
+           "nc_last_error", "nc_destroy")
 
 
 def load_library(path: str = LIB_PATH):
@@ -57,6 +57,9 @@ def load_library(path: str = LIB_PATH):
     lib.nc_kernel_launches.argtypes = [vp]
     lib.nc_kernel_launches.restype = i64
     lib.nc_last_error.restype = ctypes.c_char_p
+    lib.nc_grid_spring.argtypes = [i32, i32, dp, dp, dp, dp, dp, i32, dp, dp, i32, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_double, i64, ctypes.POINTER(i64)]
+    lib.nc_grid_spring.restype = ctypes.c_int
     lib.nc_destroy.argtypes = [vp]
     lib.nc_destroy.restype = None
     for f in ("nc_create", "nc_upload_state", "nc_download_state", "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync",
@@ -68,6 +71,23 @@ def load_library(path: str = LIB_PATH):
 
 class NicamError(RuntimeError):
     pass
+
+
+def grid_spring(x, x_pl, have_sgp, plan, lam, dbar, dt, crit, max_iter):
+    """Spring relaxation on the device (nc_grid_spring); x (L,G,G,3) and
+    x_pl (2,6,3) are updated in place.  Returns the iteration count."""
+    lib = load_library()
+    x = np.ascontiguousarray(x, np.float64)
+    x_pl = np.ascontiguousarray(x_pl, np.float64)
+    sg = np.ascontiguousarray(have_sgp, np.uint8)
+    r_dst, r_src, p_dst, p_src = (np.ascontiguousarray(a, np.int64) for a in plan)
+    it = ctypes.c_int64(0)
+    rc = lib.nc_grid_spring(x.shape[0], x.shape[1], x.ctypes.data, x_pl.ctypes.data, sg.ctypes.data,
+                            r_dst.ctypes.data, r_src.ctypes.data, len(r_dst), p_dst.ctypes.data, p_src.ctypes.data,
+                            len(p_dst), lam, dbar, dt, crit, int(max_iter), ctypes.byref(it))
+    if rc != 0:
+        raise NicamError(f"nc_grid_spring status {rc}: {lib.nc_last_error().decode(errors='replace')}")
+    return x, x_pl, int(it.value)
 
 
 def _check(rc: int):
