@@ -101,6 +101,22 @@ int nc_state_pointers(nc_handle* h, int32_t v, double** reg, double** pl);
 /* Number of kernels the library launched since the handle was created. */
 int64_t nc_kernel_launches(nc_handle* h);
 
+/* The CUDA stream (cudaStream_t) every call of this handle is ordered on, for
+ * callers that time or order their own work against it. */
+int nc_stream(nc_handle* h, void** stream);
+
+/* Per-kernel device timing (measurement aid, no counterpart in the reference):
+ * while enabled, nc_step launches eagerly and records an event after every
+ * kernel; a kernel's time is the gap to the preceding event on the stream.
+ * Enabling or disabling clears the totals. */
+int nc_profile(nc_handle* h, int32_t enable);
+
+/* Totals of the profiled steps: up to max_kernels entries of kernel name
+ * (48-byte slots in names), summed milliseconds and launch count.  Returns the
+ * number of distinct kernels (which may exceed max_kernels), or a negative
+ * status on a bad argument. */
+int nc_kernel_stats(nc_handle* h, int32_t max_kernels, char* names, double* total_ms, int64_t* launches);
+
 /* Grid generation helper (no counterpart in the reference's step interface;
  * restates the spring-dynamics smoothing of prep/hgrid/mod_mkgrd.py:204-320).
  * x (lall, gall_1d, gall_1d, 3) region-major unit vectors with halos filled,

@@ -26,6 +26,7 @@ static int fail(int code, const std::string& msg) {
   } while (0)
 
 #define NC_MAXCOMM 8
+#define NC_KNAME 48
 
 // ---------------------------------------------------------------------------
 // halo exchange: one gather from interior / pole sources into every halo cell
@@ -200,6 +201,13 @@ struct nc_handle {
   FieldPair gadv[4], vt[6], vt2[6], gT0[6], frhog;
   FieldPair PSa[6], PSb[6], PM[5], vtmp2[3], gT[6], Mc, Mu, Ml, ethtot0, hdiv[3];
   FieldPair flx_v, rhog_t, flx[6], xc[9], ch[6], cm[6], q, gq[3], qa[3], Qmin, Qmax;
+  // per-kernel timing (opt-in, eager launches only): an event after every
+  // launch; a kernel's time is the gap to the previous event on the stream
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<const char*> ev_name;
+  size_t ev_used = 0;
+  std::map<std::string, std::pair<double, long long>> kstats;
 };
 
 static nc_handle* g_current = nullptr;   // handle whose constants are loaded
@@ -317,10 +325,39 @@ static unsigned grid_cols_kl(const nc_handle* h) {   // regional columns + (k, l
   return (unsigned)((n + kBlock - 1) / kBlock);
 }
 
+static int mark(nc_handle* h, const char* what) {
+  if (h->ev_used == h->ev_pool.size()) {
+    cudaEvent_t e;
+    CU(cudaEventCreate(&e));
+    h->ev_pool.push_back(e);
+    h->ev_name.push_back(nullptr);
+  }
+  CU(cudaEventRecord(h->ev_pool[h->ev_used], h->stream));
+  h->ev_name[h->ev_used] = what;
+  h->ev_used++;
+  return 0;
+}
+
 static int check_launch(nc_handle* h, const char* what) {
   h->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(NC_ERR_CUDA, std::string("launch ") + what + ": " + cudaGetErrorString(e));
+  if (h->prof) return mark(h, what);
+  return 0;
+}
+
+// fold the events of one profiled step into the per-kernel totals
+static int collect_profile(nc_handle* h) {
+  CU(cudaStreamSynchronize(h->stream));
+  for (size_t n = 1; n < h->ev_used; ++n) {
+    if (!h->ev_name[n]) continue;
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, h->ev_pool[n - 1], h->ev_pool[n]));
+    auto& st = h->kstats[h->ev_name[n]];
+    st.first += ms;
+    st.second += 1;
+  }
+  h->ev_used = 0;
   return 0;
 }
 
@@ -371,6 +408,7 @@ static int run_step(nc_handle* h) {
     CU(cudaMemcpyAsync(h->P0[v].r, h->P[v].r, D.npt * sizeof(double), cudaMemcpyDeviceToDevice, s));
     CU(cudaMemcpyAsync(h->P0[v].p, h->P[v].p, D.npl * sizeof(double), cudaMemcpyDeviceToDevice, s));
   }
+  if (h->prof) TRY(mark(h, nullptr));
   for (int nl = 0; nl < h->nstage; ++nl) {
     const bool last = (nl == h->nstage - 1);
     // ---- Pre_Post
@@ -890,6 +928,7 @@ void nc_destroy(nc_handle* h) {
   if (h->gexec) cudaGraphExecDestroy(h->gexec);
   if (h->graph) cudaGraphDestroy(h->graph);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   for (void* p : h->allocs) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
   if (g_current == h) g_current = nullptr;
@@ -944,8 +983,12 @@ int nc_step(nc_handle* h, int32_t nsteps) {
   if (!h || nsteps < 0) return fail(NC_ERR_ARG, "nc_step: bad argument");
   if (!h->have_state) return fail(NC_ERR_STATE, "nc_step: no state uploaded");
   TRY(load_consts(h));
-  if (!h->use_graph) {
-    for (int n = 0; n < nsteps; ++n) TRY(run_step(h));
+  if (!h->use_graph || h->prof) {
+    for (int n = 0; n < nsteps; ++n) {
+      if (h->prof) h->ev_used = 0;
+      TRY(run_step(h));
+      if (h->prof) TRY(collect_profile(h));
+    }
     return 0;
   }
   if (!h->gexec) {
@@ -1052,6 +1095,36 @@ int nc_state_pointers(nc_handle* h, int32_t v, double** reg, double** pl) {
   *reg = f.r;
   *pl = f.p;
   return 0;
+}
+
+int nc_stream(nc_handle* h, void** stream) {
+  if (!h || !stream) return fail(NC_ERR_ARG, "nc_stream: null argument");
+  *stream = (void*)h->stream;
+  return 0;
+}
+
+int nc_profile(nc_handle* h, int32_t enable) {
+  if (!h) return fail(NC_ERR_ARG, "nc_profile: null handle");
+  CU(cudaStreamSynchronize(h->stream));
+  h->prof = enable != 0;
+  h->kstats.clear();
+  h->ev_used = 0;
+  return 0;
+}
+
+int nc_kernel_stats(nc_handle* h, int32_t max_kernels, char* names, double* total_ms, int64_t* launches) {
+  if (!h || max_kernels < 0 || (max_kernels > 0 && (!names || !total_ms || !launches)))
+    return -fail(NC_ERR_ARG, "nc_kernel_stats: bad argument");
+  int n = 0;
+  for (const auto& kv : h->kstats) {
+    if (n < max_kernels) {
+      snprintf(names + (size_t)n * NC_KNAME, NC_KNAME, "%s", kv.first.c_str());
+      total_ms[n] = kv.second.first;
+      launches[n] = kv.second.second;
+    }
+    ++n;
+  }
+  return n;
 }
 
 // grid generation helper: spring-dynamics relaxation (see nc_grid.cuh)

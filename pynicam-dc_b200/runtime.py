@@ -31,8 +31,8 @@ _lib = None
 
 # every entry point declared in include/nicam_cuda.h
 EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync",
-           "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_grid_spring",
-           "nc_last_error", "nc_destroy")
+           "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",
+           "nc_kernel_stats", "nc_grid_spring", "nc_last_error", "nc_destroy")
 
 
 def load_library(path: str = LIB_PATH):
@@ -57,13 +57,17 @@ def load_library(path: str = LIB_PATH):
     lib.nc_kernel_launches.argtypes = [vp]
     lib.nc_kernel_launches.restype = i64
     lib.nc_last_error.restype = ctypes.c_char_p
+    lib.nc_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    lib.nc_profile.argtypes = [vp, i32]
+    lib.nc_kernel_stats.argtypes = [vp, i32, ctypes.c_char_p, dp, dp]
+    lib.nc_kernel_stats.restype = ctypes.c_int
     lib.nc_grid_spring.argtypes = [i32, i32, dp, dp, dp, dp, dp, i32, dp, dp, i32, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_double, i64, ctypes.POINTER(i64)]
     lib.nc_grid_spring.restype = ctypes.c_int
     lib.nc_destroy.argtypes = [vp]
     lib.nc_destroy.restype = None
     for f in ("nc_create", "nc_upload_state", "nc_download_state", "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync",
-              "nc_mass_sums", "nc_get_field", "nc_state_pointers"):
+              "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_stream", "nc_profile"):
         getattr(lib, f).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -227,6 +231,30 @@ class NicamCuda:
 
     def kernel_launches(self) -> int:
         return int(self._lib.nc_kernel_launches(self._h))
+
+    def stream_ptr(self) -> int:
+        """cudaStream_t of the handle (for CUDA events on the same stream)"""
+        p = ctypes.c_void_p()
+        _check(self._lib.nc_stream(self._h, ctypes.byref(p)))
+        return int(p.value or 0)
+
+    def profile(self, enable: bool):
+        _check(self._lib.nc_profile(self._h, 1 if enable else 0))
+
+    def kernel_stats(self) -> dict:
+        """{kernel name: (total ms, launches)} of the profiled steps"""
+        n = self._lib.nc_kernel_stats(self._h, 0, None, None, None)
+        if n < 0:
+            _check(-n)
+        names = ctypes.create_string_buffer(48 * max(n, 1))
+        ms = np.zeros(max(n, 1))
+        cnt = np.zeros(max(n, 1), np.int64)
+        self._lib.nc_kernel_stats(self._h, n, names, ms.ctypes.data, cnt.ctypes.data)
+        out = {}
+        for k in range(n):
+            nm = names.raw[48 * k:48 * (k + 1)].split(b"\0", 1)[0].decode()
+            out[nm] = (float(ms[k]), int(cnt[k]))
+        return out
 
     def close(self):
         if getattr(self, "_h", None):
