@@ -496,7 +496,10 @@ static int run_step(nc_handle* h) {
       Three o, op;
       for (int n = 0; n < 4; ++n) { v.f[n] = v4[n].r; vp.f[n] = v4[n].p; }
       for (int d = 0; d < 3; ++d) { o.f[d] = h->vtmp2[d].r; op.f[d] = h->vtmp2[d].p; }
-      k_dd3d<<<greg, kBlock, 0, s>>>(v, o);
+      // interior cells only: halo rows are filled by the exchange below and the
+      // boundary levels of vtmp2 stay zero from allocation
+      const dim3 gt((unsigned)((D.G - 2 + DD_DX - 1) / DD_DX), (unsigned)((D.G - 2 + DD_DY - 1) / DD_DY), (unsigned)D.L);
+      k_dd3d_t<<<gt, DD_DX * DD_DY, 0, s>>>(v, o);
       TRY(check_launch(h, "dd3d"));
       k_dd3d_pl<<<1, plk, 0, s>>>(vp, op);
       TRY(check_launch(h, "dd3d_pl"));

@@ -90,6 +90,106 @@ __global__ void k_dd3d(Four v, Three out) {
 }
 
 // pole 3-D divergence damping (kernels/oprt3ddivdamp.py:176-237)
+// Tiled 3-D divergence damping: one block per DD_DX x DD_DY tile of output
+// cells of one region, marching upward in k.  Per level the block stages the
+// haloed tile of RGAM-scaled momentum and the vertical mass flux rwv(k+1) in
+// shared memory (rwv(k) is kept from the level below), evaluates every
+// triangle value once, applies the singular-point fix, then each thread forms
+// its cell's three components.  Arithmetic and association order are those of
+// k_dd3d (the untiled form kept for reference and the pole-adjacent checks).
+#define DD_DX 32
+#define DD_DY 8
+__global__ void __launch_bounds__(DD_DX * DD_DY) k_dd3d_t(Four v, Three out) {
+  constexpr int PX = DD_DX + 2, PY = DD_DY + 2;   // points i0-1 .. i0+DX, j0-1 .. j0+DY
+  constexpr int TX = DD_DX + 1, TY = DD_DY + 1;   // triangles i0-1 .. i0+DX-1, j0-1 .. j0+DY-1
+  __shared__ double s_vm[3][PY * PX];
+  __shared__ double s_rw[2][PY * PX];
+  __shared__ double s_ti[TY * TX], s_tj[TY * TX];
+  const int l = blockIdx.z;
+  const int i0 = 1 + blockIdx.x * DD_DX, j0 = 1 + blockIdx.y * DD_DY;
+  const int G = cD.G, gmax = cD.G - 2;
+  const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool own = (i <= gmax) && (j <= gmax);
+  const long long n = cD.npt;
+  const double* cz = cG.C2WGz;
+  double cd[3][6];
+  if (own) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int m = 0; m < 6; ++m) cd[d][m] = P2(cG.coef_diff, d * 6 + m, i, j, l);
+  }
+  for (int p = tid; p < PX * PY; p += blockDim.x) s_rw[0][p] = 0.0;   // rwv(kmin) = 0
+  int cur = 0;
+  for (int k = cD.kmin; k <= cD.kmax; ++k) {
+    const bool up = (k + 1 <= cD.kmax);   // rwv(k+1) = 0 above kmax
+    for (int p = tid; p < PX * PY; p += blockDim.x) {
+      const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
+      double a = 0.0, b = 0.0, c = 0.0, r = 0.0;
+      if (ii < G && jj < G) {
+        const long long q = ix(ii, jj, k, l);
+        const double f0 = v.f[0][q], f1 = v.f[1][q], f2 = v.f[2][q];
+        const double rg = cG.RGAM[q];
+        a = f0 * rg;
+        b = f1 * rg;
+        c = f2 * rg;
+        if (up) {
+          const long long qp = q + cD.plane;   // level k+1
+          const double h = cz[qp] * v.f[0][qp] + cz[n + qp] * f0 + cz[2 * n + qp] * v.f[1][qp] +
+                           cz[3 * n + qp] * f1 + cz[4 * n + qp] * v.f[2][qp] + cz[5 * n + qp] * f2;
+          r = h * cG.RGAMH[qp] + v.f[3][qp] * cG.RGSQRTH[qp];
+        }
+      }
+      s_vm[0][p] = a;
+      s_vm[1][p] = b;
+      s_vm[2][p] = c;
+      s_rw[cur ^ 1][p] = r;
+    }
+    __syncthreads();
+    const double rdz = cC.rdgz[k];
+    const double* rU = s_rw[cur ^ 1];
+    const double* rD = s_rw[cur];
+    for (int p = tid; p < TX * TY; p += blockDim.x) {
+      const int px = p % TX, py = p / TX;
+      const int ii = i0 - 1 + px, jj = j0 - 1 + py;
+      double sTI = 0.0, sTJ = 0.0;
+      if (ii <= G - 2 && jj <= G - 2) {
+        const int a = py * PX + px, b = a + 1, c = a + PX + 1, d = a + PX;
+        auto C = [&](int dir, int pt, int t) { return P2(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
+        const double wTI = ((rU[a] + rU[b] + rU[c]) - (rD[a] + rD[b] + rD[c])) / 3.0 * rdz;
+        const double wTJ = ((rU[a] + rU[c] + rU[d]) - (rD[a] + rD[c] + rD[d])) / 3.0 * rdz;
+        sTI = C(0, 0, 0) * s_vm[0][a] + C(0, 1, 0) * s_vm[0][b] + C(0, 2, 0) * s_vm[0][c] +
+              C(1, 0, 0) * s_vm[1][a] + C(1, 1, 0) * s_vm[1][b] + C(1, 2, 0) * s_vm[1][c] +
+              C(2, 0, 0) * s_vm[2][a] + C(2, 1, 0) * s_vm[2][b] + C(2, 2, 0) * s_vm[2][c] + wTI;
+        sTJ = C(0, 0, 1) * s_vm[0][a] + C(0, 1, 1) * s_vm[0][c] + C(0, 2, 1) * s_vm[0][d] +
+              C(1, 0, 1) * s_vm[1][a] + C(1, 1, 1) * s_vm[1][c] + C(1, 2, 1) * s_vm[1][d] +
+              C(2, 0, 1) * s_vm[2][a] + C(2, 1, 1) * s_vm[2][c] + C(2, 2, 1) * s_vm[2][d] + wTJ;
+      }
+      s_ti[p] = sTI;
+      s_tj[p] = sTJ;
+    }
+    __syncthreads();
+    if (tid == 0 && i0 == 1 && j0 == 1)   // singular-point fix at the (0,0) triangle
+      s_ti[0] = s_ti[0] * (double)cG.pntmask[l * 2 + 0] + s_tj[1] * (double)cG.pntmask[l * 2 + 1];
+    __syncthreads();
+    if (own) {
+      const int ta = (ty + 1) * TX + (tx + 1);   // triangle (i, j)
+      const double aTI = s_ti[ta], aTJ = s_tj[ta];
+      const double bTI = s_ti[ta - 1];            // (i-1, j)
+      const double cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1];   // (i-1, j-1)
+      const double dTJ = s_tj[ta - TX];           // (i, j-1)
+      const long long q = ix(i, j, k, l);
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        out.f[d][q] = cd[d][0] * (aTI + aTJ) + cd[d][1] * (aTJ + bTI) + cd[d][2] * (bTI + cTJ) +
+                      cd[d][3] * (cTJ + cTI) + cd[d][4] * (cTI + dTJ) + cd[d][5] * (dTJ + aTI);
+    }
+    __syncthreads();
+    cur ^= 1;
+  }
+}
+
 __global__ void k_dd3d_pl(Four v, Three out) {
   int t = threadIdx.x;
   if (t >= cD.KA * cD.LP) return;

@@ -920,6 +920,20 @@ class Grid:
         vzz = vzz + nzv * np.zeros_like(pw)
         return pp, tmp, vx, vy, vzz
 
+    def _jw_chunked(self, z, lat, lon):
+        """the column solve over chunks of the leading axis on host threads
+        (every operation is per column, so chunking does not change results)"""
+        n = z.shape[0]
+        workers = min(n, os.cpu_count() or 1, 16)
+        if workers <= 1 or z.size < 1_000_000:
+            return self._jw_columns(z, lat, lon)
+        from concurrent.futures import ThreadPoolExecutor
+        bounds = np.linspace(0, n, workers + 1).astype(int)
+        with ThreadPoolExecutor(workers) as ex:
+            parts = list(ex.map(lambda b: self._jw_columns(z[b[0]:b[1]], lat[b[0]:b[1]], lon[b[0]:b[1]]),
+                                zip(bounds[:-1], bounds[1:])))
+        return tuple(np.concatenate([p[v] for p in parts], axis=0) for v in range(5))
+
     def jw_state(self, nq: int = 1):
         """JW balanced jet + perturbation as PRG_var (G, G, kall, L, 6+nq) and
         PRG_var_pl (6, kall, 2, 6+nq) in the reference layout."""
@@ -932,7 +946,7 @@ class Grid:
             z = np.zeros(z3.shape[:-1])
             z[..., kmin - 1] = z3[..., kmin, 1]
             z[..., kmin:kmax + 2] = z3[..., kmin:kmax + 2, 0]
-            out.append(self._jw_columns(z, lat, lon))
+            out.append(self._jw_chunked(z, lat, lon))
         diag = np.stack(out[0] + (np.zeros_like(out[0][0]),), axis=-1)        # (L,G,G,K,6) pre,tem,vx,vy,vz,w
         diag_pl = np.stack(out[1] + (np.zeros_like(out[1][0]),), axis=-1)
         self.exch(diag, diag_pl)

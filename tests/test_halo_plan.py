@@ -31,3 +31,18 @@ def test_plan_covers_every_halo_cell_once(pkg, golden):
     si, sj = src % Gl, (src // Gl) % Gl
     assert np.all((si > 0) & (sj > 0) & (si < Gl - 1) & (sj < Gl - 1)), "sources must be interior"
     assert sorted((p_dst % 2).tolist()).count(0) == 5 and len(p_dst) == 10
+
+
+def test_every_halo_cell_is_written_at_all_levels(pkg):
+    """kernels that compute interior cells only rely on the exchange to write
+    every halo cell (and the five pole neighbours) at every grid level"""
+    import os
+    import numpy as np
+    z = np.load(os.path.join(os.path.dirname(pkg.__file__), "data", "halo_rl01.npz"))
+    for gl in range(3, 9):
+        G = 2 ** (gl - 1) + 2
+        k = f"gl{gl:02d}_"
+        r_dst, r_src, p_dst, p_src = pkg.halo.compose(*(z[k + n].astype(np.int64) for n in ("r2r", "p2r", "r2p", "sgp")),
+                                                      G, 40)
+        assert len(set(r_dst.tolist())) == len(r_dst) == 40 * (4 * G - 4), gl
+        assert sorted(p_dst.tolist()) == sorted(g * 2 + lp for g in range(1, 6) for lp in range(2)), gl
