@@ -477,7 +477,7 @@ static int run_step(nc_handle* h) {
       ga.gw = F(h->gadv[3]); ga.frhog = F(h->frhog);
       if (!pole) k_gtend<<<greg, kBlock, 0, s>>>(ga, 0);
       else k_gtend<<<1, 32, 0, s>>>(ga, 1);
-      TRY(check_launch(h, "gtend"));
+      TRY(check_launch(h, pole ? "gtend_pl" : "gtend"));
     }
     PHASE();
     // ---- vi_small_step (mod_vi.py:104-1590)
@@ -522,7 +522,7 @@ static int run_step(nc_handle* h) {
       va.dt = h->dts;
       if (!pole) k_vp0<<<greg, kBlock, 0, s>>>(va, 0);
       else k_vp0<<<1, 32, 0, s>>>(va, 1);
-      TRY(check_launch(h, "vp0"));
+      TRY(check_launch(h, pole ? "vp0_pl" : "vp0"));
     }
     PHASE();
     const int nitr = h->sstep[nl];
@@ -544,9 +544,15 @@ static int run_step(nc_handle* h) {
         for (int d = 0; d < 3; ++d) { pa.vt.f[d] = F(h->vtmp2[d]); pa.dvh[d] = F(PN[1 + d]); }
         for (int n = 0; n < 5; ++n) pa.PM[n] = F(h->PM[n]);
         pa.dt = h->dts; pa.rweight = rweight; pa.RovCV = RovCV;
-        if (!pole) k_path1<<<greg, kBlock, 0, s>>>(pa, 0);
-        else k_path1<<<1, 32, 0, s>>>(pa, 1);
-        TRY(check_launch(h, "path1"));
+        if (!pole) {
+          const dim3 gt((unsigned)((D.G - 2 + DD_DX - 1) / DD_DX), (unsigned)((D.G - 2 + DD_DY - 1) / DD_DY),
+                        (unsigned)D.L);
+          k_path1_t<<<gt, DD_DX * DD_DY, 0, s>>>(pa);
+          TRY(check_launch(h, "path1"));
+        } else {
+          k_path1<<<1, 32, 0, s>>>(pa, 1);
+          TRY(check_launch(h, "path1_pl"));
+        }
       }
       TRY(comm(h, {PN[1], PN[2], PN[3]}));
       PHASE();
@@ -597,7 +603,7 @@ static int run_step(nc_handle* h) {
       ta.dt = dt;
       if (!pole) k_trc_vflux<<<greg, kBlock, 0, s>>>(ta, 0);
       else k_trc_vflux<<<1, 32, 0, s>>>(ta, 1);
-      TRY(check_launch(h, "trc_vflux"));
+      TRY(check_launch(h, pole ? "trc_vflux_pl" : "trc_vflux"));
     }
     auto vadv = [&](int iq, bool second) -> int {
       for (int pole = 0; pole < 2; ++pole) {
@@ -609,7 +615,7 @@ static int run_step(nc_handle* h) {
         va.dt = dt; va.bcoef = 0.0; va.clamp = second ? 1 : 0; va.dtl = dt;
         if (!pole) k_trc_vadv<<<greg, kBlock, 0, s>>>(va, 0);
         else k_trc_vadv<<<1, 32, 0, s>>>(va, 1);
-        TRY(check_launch(h, "trc_vadv"));
+        TRY(check_launch(h, pole ? "trc_vadv_pl" : "trc_vadv"));
       }
       return 0;
     };

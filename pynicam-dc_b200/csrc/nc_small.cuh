@@ -89,7 +89,6 @@ __global__ void k_dd3d(Four v, Three out) {
   }
 }
 
-// pole 3-D divergence damping (kernels/oprt3ddivdamp.py:176-237)
 // Tiled 3-D divergence damping: one block per DD_DX x DD_DY tile of output
 // cells of one region, marching upward in k.  Per level the block stages the
 // haloed tile of RGAM-scaled momentum and the vertical mass flux rwv(k+1) in
@@ -190,6 +189,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY) k_dd3d_t(Four v, Three out) {
   }
 }
 
+// pole 3-D divergence damping (kernels/oprt3ddivdamp.py:176-237)
 __global__ void k_dd3d_pl(Four v, Three out) {
   int t = threadIdx.x;
   if (t >= cD.KA * cD.LP) return;
@@ -544,6 +544,146 @@ __device__ void path1_column(const Path1Args& a, int i, int j, int l, int g, int
   for (int k = 0; k < KA; ++k) {
     long long p = c.at(k);
     for (int d = 0; d < 3; ++d) a.PM[1 + d][p] = a.PM[1 + d][p] + out[d][p] * a.rweight;
+  }
+}
+
+// Tiled regional path 1: one block per DD_DX x DD_DY tile of interior cells,
+// marching over k.  Per level the haloed tile of -vtmp2 (2-D divergence
+// damping) and of the RGAM-weighted split pressure at the gradient level kk
+// are staged in shared memory and every triangle value is formed once.  Halo
+// cells are not computed: diff_vh is exchanged right after this kernel and
+// the running means are exchanged before they are read off the interior.
+// Arithmetic and association order are those of path1_column.
+__global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_path1_t(Path1Args a) {
+  constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
+  __shared__ double s_v[3][PY * PX];
+  __shared__ double s_p[PY * PX];
+  __shared__ double s_ti[TY * TX], s_tj[TY * TX];
+  const int l = blockIdx.z;
+  const int i0 = 1 + blockIdx.x * DD_DX, j0 = 1 + blockIdx.y * DD_DY;
+  const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin, kmax = cD.kmax;
+  const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool own = (i <= gmax) && (j <= gmax);
+  const double dt = a.dt, RovCV = a.RovCV, rweight = a.rweight, ddc = cC.divdamp_coef, r = cC.rscale;
+  const long long n = cD.npt;
+  const double* cz = cG.C2WGz;
+  double cd[3][6], gxyz[3] = {0.0, 0.0, 0.0};
+  long long q0 = 0;
+  if (own) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      gxyz[d] = P2(cG.GRD_x, d, i, j, l);
+#pragma unroll
+      for (int m = 0; m < 6; ++m) cd[d][m] = P2(cG.coef_diff, d * 6 + m, i, j, l);
+    }
+    q0 = ix(i, j, 0, l);
+  }
+  auto Pown = [&](int kk) {   // split pressure of the own column, boundary rows clamped
+    const int k2 = kk < kmin ? kmin : (kk > kmax ? kmax : kk);
+    return a.PS[5][q0 + (long long)k2 * cD.plane] * RovCV;
+  };
+  double vals[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+  for (int k = kmin; k <= kmax; ++k) {
+    const int kk = (k == kmin) ? kmin + 1 : k;
+    for (int p = tid; p < PX * PY; p += blockDim.x) {
+      const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
+      double x = 0.0, y = 0.0, z = 0.0, pp = 0.0;
+      if (ii < G && jj < G) {
+        const long long q = ix(ii, jj, k, l);
+        x = -a.vt.f[0][q];
+        y = -a.vt.f[1][q];
+        z = -a.vt.f[2][q];
+        const long long qk = ix(ii, jj, kk, l);
+        pp = a.PS[5][qk] * RovCV * cG.RGAM[qk];
+      }
+      s_v[0][p] = x;
+      s_v[1][p] = y;
+      s_v[2][p] = z;
+      s_p[p] = pp;
+    }
+    __syncthreads();
+    for (int p = tid; p < TX * TY; p += blockDim.x) {
+      const int px = p % TX, py = p / TX;
+      const int ii = i0 - 1 + px, jj = j0 - 1 + py;
+      double sTI = 0.0, sTJ = 0.0;
+      if (ii <= G - 2 && jj <= G - 2) {
+        const int ia = py * PX + px, ib = ia + 1, ic = ia + PX + 1, id = ia + PX;
+        auto C = [&](int dir, int pt, int t) { return P2(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
+        sTI = C(0, 0, 0) * s_v[0][ia] + C(0, 1, 0) * s_v[0][ib] + C(0, 2, 0) * s_v[0][ic] +
+              C(1, 0, 0) * s_v[1][ia] + C(1, 1, 0) * s_v[1][ib] + C(1, 2, 0) * s_v[1][ic] +
+              C(2, 0, 0) * s_v[2][ia] + C(2, 1, 0) * s_v[2][ib] + C(2, 2, 0) * s_v[2][ic];
+        sTJ = C(0, 0, 1) * s_v[0][ia] + C(0, 1, 1) * s_v[0][ic] + C(0, 2, 1) * s_v[0][id] +
+              C(1, 0, 1) * s_v[1][ia] + C(1, 1, 1) * s_v[1][ic] + C(1, 2, 1) * s_v[1][id] +
+              C(2, 0, 1) * s_v[2][ia] + C(2, 1, 1) * s_v[2][ic] + C(2, 2, 1) * s_v[2][id];
+      }
+      s_ti[p] = sTI;
+      s_tj[p] = sTJ;
+    }
+    __syncthreads();
+    if (own) {
+      const int ta = (ty + 1) * TX + (tx + 1);
+      const double aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
+      const double cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1], dTJ = s_tj[ta - TX];
+      double dd[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        dd[d] = ddc * (cd[d][0] * (aTI + aTJ) + cd[d][1] * (aTJ + bTI) + cd[d][2] * (bTI + cTJ) +
+                       cd[d][3] * (cTJ + cTI) + cd[d][4] * (cTI + dTJ) + cd[d][5] * (dTJ + aTI));
+      {
+        const double prd = (dd[0] * gxyz[0] + dd[1] * gxyz[1] + dd[2] * gxyz[2]) / r;
+        dd[0] = dd[0] - prd * gxyz[0] / r;
+        dd[1] = dd[1] - prd * gxyz[1] / r;
+        dd[2] = dd[2] - prd * gxyz[2] / r;
+      }
+      // pressure gradient at level kk: 7-point horizontal part + vertical part
+      const int c0 = (ty + 1) * PX + (tx + 1);
+      const double s7[7] = {s_p[c0], s_p[c0 + 1], s_p[c0 + PX + 1], s_p[c0 + PX], s_p[c0 - 1], s_p[c0 - PX - 1],
+                            s_p[c0 - PX]};
+      double pg[3];
+      const long long qkk = q0 + (long long)kk * cD.plane, qk1 = qkk + cD.plane;
+      const double P_k1 = Pown(kk + 1), P_k = Pown(kk), P_km = Pown(kk - 1);
+      const double rgh1 = cG.RGAMH[qk1], rgh0 = cG.RGAMH[qkk];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double g = P2(cG.coef_grad, d * 7 + 0, i, j, l) * s7[0];
+#pragma unroll
+        for (int m = 1; m < 7; ++m) g = g + P2(cG.coef_grad, d * 7 + m, i, j, l) * s7[m];
+        const double up = (cz[(2 * d) * n + qk1] * P_k1 + cz[(2 * d + 1) * n + qk1] * P_k) * rgh1;
+        const double dn = (cz[(2 * d) * n + qkk] * P_k + cz[(2 * d + 1) * n + qkk] * P_km) * rgh0;
+        pg[d] = g + (up - dn) * cC.rdgz[kk];
+      }
+      {
+        const double prd = (pg[0] * gxyz[0] + pg[1] * gxyz[1] + pg[2] * gxyz[2]) / r;
+        pg[0] = pg[0] - prd * gxyz[0] / r;
+        pg[1] = pg[1] - prd * gxyz[1] / r;
+        pg[2] = pg[2] - prd * gxyz[2] / r;
+      }
+      const long long q = q0 + (long long)k * cD.plane;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double drv = a.gT[1 + d][q] - pg[d] + dd[d] + 0.0;
+        const double v = a.PS[1 + d][q] + drv * dt;
+        a.dvh[d][q] = v;
+        a.PM[1 + d][q] = a.PM[1 + d][q] + v * rweight;
+        if (k == kmin) vals[d][0] = v;
+        if (k == kmax) vals[d][1] = v;
+      }
+    }
+    __syncthreads();
+  }
+  if (own) {
+    const long long pT = q0 + (long long)(kmax + 1) * cD.plane, pK = q0 + (long long)kmax * cD.plane;
+    const long long pB = q0 + (long long)(kmin - 1) * cD.plane, pN = q0 + (long long)kmin * cD.plane;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double vT = 1.0 * (vals[d][1] / a.rhog[pK]) * a.rhog[pT];
+      const double vB = -1.0 * (vals[d][0] / a.rhog[pN]) * a.rhog[pB];
+      a.dvh[d][pT] = vT;
+      a.dvh[d][pB] = vB;
+      a.PM[1 + d][pT] = a.PM[1 + d][pT] + vT * rweight;
+      a.PM[1 + d][pB] = a.PM[1 + d][pB] + vB * rweight;
+    }
   }
 }
 
