@@ -201,6 +201,7 @@ struct nc_handle {
   FieldPair gadv[4], vt[6], vt2[6], gT0[6], frhog;
   FieldPair PSa[6], PSb[6], PM[5], vtmp2[3], gT[6], Mc, Mu, Ml, ethtot0, hdiv[3];
   FieldPair flx_v, rhog_t, flx[6], xc[9], ch[6], cm[6], q, gq[3], qa[3], Qmin, Qmax;
+  FieldPair vph[8];             // horizontal terms of vp0 (div1, div2, dd, dpg)
   // per-kernel timing (opt-in, eager launches only): an event after every
   // launch; a kernel's time is the gap to the previous event on the stream
   bool prof = false;
@@ -462,8 +463,13 @@ static int run_step(nc_handle* h) {
       vin.f[n] = h->vt[n].r; vinp.f[n] = h->vt[n].p;
       o2.f[n] = h->vt2[n].r; o2p.f[n] = h->vt2[n].p;
     }
-    k_hdiff2<<<greg, kBlock, 0, s>>>(vin, h->P[0].r, o2);
-    TRY(check_launch(h, "hdiff2"));
+    {
+      // interior cells; the exchange below fills the halo rows
+      const dim3 gt((unsigned)((D.G - 2 + HD_DX - 1) / HD_DX), (unsigned)((D.G - 2 + HD_DY - 1) / HD_DY),
+                    (unsigned)D.L);
+      k_hdiff2_t<<<gt, HD_DX * HD_DY, 0, s>>>(vin, h->P[0].r, o2);
+      TRY(check_launch(h, "hdiff2"));
+    }
     k_hdiff2_pl<<<1, plk, 0, s>>>(vinp, h->P[0].p, o2p);
     TRY(check_launch(h, "hdiff2_pl"));
     TRY(comm(h, {h->vt2[0], h->vt2[1], h->vt2[2], h->vt2[3], h->vt2[4], h->vt2[5]}));
@@ -520,9 +526,19 @@ static int run_step(nc_handle* h) {
       for (int n = 0; n < 6; ++n) { va.gT0[n] = F(h->gT0[n]); va.gT[n] = F(h->gT[n]); }
       va.Mc = F(h->Mc); va.Mu = F(h->Mu); va.Ml = F(h->Ml); va.ethtot0 = F(h->ethtot0);
       va.dt = h->dts;
-      if (!pole) k_vp0<<<greg, kBlock, 0, s>>>(va, 0);
-      else k_vp0<<<1, 32, 0, s>>>(va, 1);
-      TRY(check_launch(h, pole ? "vp0_pl" : "vp0"));
+      if (!pole) {
+        Vp0H vh;
+        for (int n = 0; n < 8; ++n) vh.out[n] = h->vph[n].r;
+        const dim3 gt((unsigned)((D.G - 2 + DD_DX - 1) / DD_DX), (unsigned)((D.G - 2 + DD_DY - 1) / DD_DY),
+                      (unsigned)D.L);
+        k_vp0_h<<<gt, DD_DX * DD_DY, 0, s>>>(va, vh);
+        TRY(check_launch(h, "vp0_h"));
+        k_vp0_c<<<greg, kBlock, 0, s>>>(va, vh);
+        TRY(check_launch(h, "vp0_c"));
+      } else {
+        k_vp0<<<1, 32, 0, s>>>(va, 1);
+        TRY(check_launch(h, "vp0_pl"));
+      }
     }
     PHASE();
     const int nitr = h->sstep[nl];
@@ -893,6 +909,7 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   TRY(field(h, h->ethtot0, "ethtot0"));
   TRY(field(h, h->flx_v, "flx_v")); TRY(field(h, h->rhog_t, "rhog_t")); TRY(field(h, h->q, "q"));
   TRY(field(h, h->Qmin, "Qmin")); TRY(field(h, h->Qmax, "Qmax"));
+  for (int n = 0; n < 8; ++n) { snprintf(nm, sizeof nm, "vph.%d", n); TRY(field(h, h->vph[n], nm)); }
   for (int f = 0; f < 6; ++f) {
     snprintf(nm, sizeof nm, "flx.%d", f); TRY(field(h, h->flx[f], nm));
     snprintf(nm, sizeof nm, "ch.%d", f); TRY(field(h, h->ch[f], nm));

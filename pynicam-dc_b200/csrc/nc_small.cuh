@@ -484,6 +484,232 @@ __device__ void vp0_column(const Vp0Args& a, int i, int j, int l, int g, int lp)
   }
 }
 
+// Horizontal terms of vp0, tiled like k_path1_t: for interior cells and
+// levels kmin..kmax, the divergences of RGAM*rhogv and RGAM*rhogv*eth
+// (div1, div2), the 2-D divergence damping of -vtmp2 (dd) and the pressure
+// gradient of pregd (dpg), written to eight work fields for the column kernel.
+struct Vp0H {
+  double* out[8];               // div1, div2, dd x/y/z, dpg x/y/z
+};
+
+__global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_vp0_h(Vp0Args a, Vp0H h) {
+  constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
+  __shared__ double s_m[3][PY * PX];    // RGAM * rhogv
+  __shared__ double s_e[3][PY * PX];    // RGAM * rhogv * eth
+  __shared__ double s_v[3][PY * PX];    // -vtmp2
+  __shared__ double s_p[PY * PX];       // RGAM * pregd at the gradient level
+  __shared__ double s_ti[TY * TX], s_tj[TY * TX];
+  const int l = blockIdx.z;
+  const int i0 = 1 + blockIdx.x * DD_DX, j0 = 1 + blockIdx.y * DD_DY;
+  const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin, kmax = cD.kmax;
+  const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool own = (i <= gmax) && (j <= gmax);
+  const double ddc = cC.divdamp_coef, r = cC.rscale;
+  const long long n = cD.npt;
+  const double* cz = cG.C2WGz;
+  const double* const* P = a.P.v;
+  double gxyz[3] = {0.0, 0.0, 0.0};
+  long long q0 = 0;
+  if (own) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) gxyz[d] = P2(cG.GRD_x, d, i, j, l);
+    q0 = ix(i, j, 0, l);
+  }
+  for (int k = kmin; k <= kmax; ++k) {
+    const int kk = (k == kmin) ? kmin + 1 : k;
+    for (int p = tid; p < PX * PY; p += blockDim.x) {
+      const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
+      double mv[3] = {0.0, 0.0, 0.0}, ev[3] = {0.0, 0.0, 0.0}, vv[3] = {0.0, 0.0, 0.0}, pp = 0.0;
+      if (ii < G && jj < G) {
+        const long long q = ix(ii, jj, k, l);
+        const double rg = cG.RGAM[q], e = a.eth[q];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double pv = P[1 + d][q];
+          mv[d] = pv * rg;
+          ev[d] = (pv * e) * rg;
+          vv[d] = -a.vt.f[d][q];
+        }
+        const long long qk = ix(ii, jj, kk, l);
+        pp = a.pregd[qk] * cG.RGAM[qk];
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        s_m[d][p] = mv[d];
+        s_e[d][p] = ev[d];
+        s_v[d][p] = vv[d];
+      }
+      s_p[p] = pp;
+    }
+    __syncthreads();
+    for (int p = tid; p < TX * TY; p += blockDim.x) {
+      const int px = p % TX, py = p / TX;
+      const int ii = i0 - 1 + px, jj = j0 - 1 + py;
+      double sTI = 0.0, sTJ = 0.0;
+      if (ii <= G - 2 && jj <= G - 2) {
+        const int ia = py * PX + px, ib = ia + 1, ic = ia + PX + 1, id = ia + PX;
+        auto C = [&](int dir, int pt, int t) { return P2(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
+        sTI = C(0, 0, 0) * s_v[0][ia] + C(0, 1, 0) * s_v[0][ib] + C(0, 2, 0) * s_v[0][ic] +
+              C(1, 0, 0) * s_v[1][ia] + C(1, 1, 0) * s_v[1][ib] + C(1, 2, 0) * s_v[1][ic] +
+              C(2, 0, 0) * s_v[2][ia] + C(2, 1, 0) * s_v[2][ib] + C(2, 2, 0) * s_v[2][ic];
+        sTJ = C(0, 0, 1) * s_v[0][ia] + C(0, 1, 1) * s_v[0][ic] + C(0, 2, 1) * s_v[0][id] +
+              C(1, 0, 1) * s_v[1][ia] + C(1, 1, 1) * s_v[1][ic] + C(1, 2, 1) * s_v[1][id] +
+              C(2, 0, 1) * s_v[2][ia] + C(2, 1, 1) * s_v[2][ic] + C(2, 2, 1) * s_v[2][id];
+      }
+      s_ti[p] = sTI;
+      s_tj[p] = sTJ;
+    }
+    __syncthreads();
+    if (own) {
+      const int c0 = (ty + 1) * PX + (tx + 1);
+      const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
+      const long long q = q0 + (long long)k * cD.plane;
+      // divergences (div7: per direction left to right, then x + y + z)
+      double acc1[3], acc2[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+        for (int m = 0; m < 7; ++m) {
+          const double cdv = P2(cG.coef_div, d * 7 + m, i, j, l);
+          const double t1 = cdv * s_m[d][nb[m]], t2 = cdv * s_e[d][nb[m]];
+          s1 = (m == 0) ? t1 : s1 + t1;
+          s2 = (m == 0) ? t2 : s2 + t2;
+        }
+        acc1[d] = s1;
+        acc2[d] = s2;
+      }
+      h.out[0][q] = acc1[0] + acc1[1] + acc1[2];
+      h.out[1][q] = acc2[0] + acc2[1] + acc2[2];
+      // 2-D divergence damping, projected
+      const int ta = (ty + 1) * TX + (tx + 1);
+      const double aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
+      const double cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1], dTJ = s_tj[ta - TX];
+      double dd[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        dd[d] = ddc * (P2(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) +
+                       P2(cG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
+                       P2(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) +
+                       P2(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
+                       P2(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) +
+                       P2(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI));
+      {
+        const double prd = (dd[0] * gxyz[0] + dd[1] * gxyz[1] + dd[2] * gxyz[2]) / r;
+        dd[0] = dd[0] - prd * gxyz[0] / r;
+        dd[1] = dd[1] - prd * gxyz[1] / r;
+        dd[2] = dd[2] - prd * gxyz[2] / r;
+      }
+      // pressure gradient of pregd at level kk
+      const long long qkk = q0 + (long long)kk * cD.plane, qk1 = qkk + cD.plane, qkm = qkk - cD.plane;
+      const double P_k1 = a.pregd[qk1], P_k = a.pregd[qkk], P_km = a.pregd[qkm];
+      const double rgh1 = cG.RGAMH[qk1], rgh0 = cG.RGAMH[qkk];
+      double pg[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double g = P2(cG.coef_grad, d * 7 + 0, i, j, l) * s_p[nb[0]];
+#pragma unroll
+        for (int m = 1; m < 7; ++m) g = g + P2(cG.coef_grad, d * 7 + m, i, j, l) * s_p[nb[m]];
+        const double up = (cz[(2 * d) * n + qk1] * P_k1 + cz[(2 * d + 1) * n + qk1] * P_k) * rgh1;
+        const double dn = (cz[(2 * d) * n + qkk] * P_k + cz[(2 * d + 1) * n + qkk] * P_km) * rgh0;
+        pg[d] = g + (up - dn) * cC.rdgz[kk];
+      }
+      {
+        const double prd = (pg[0] * gxyz[0] + pg[1] * gxyz[1] + pg[2] * gxyz[2]) / r;
+        pg[0] = pg[0] - prd * gxyz[0] / r;
+        pg[1] = pg[1] - prd * gxyz[1] / r;
+        pg[2] = pg[2] - prd * gxyz[2] / r;
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        h.out[2 + d][q] = dd[d];
+        h.out[5 + d][q] = pg[d];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Column part of vp0 for every regional column: vertical flux convergences,
+// small-step tendencies, the implicit matrix and ethtot0, with the horizontal
+// terms read from k_vp0_h (zero on halo columns and outside kmin..kmax, where
+// the values that depend on them are replaced by the halo exchanges or the
+// boundary rows before they are read).
+__global__ void __launch_bounds__(128) k_vp0_c(Vp0Args a, Vp0H h) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (!col_of(t, i, j, l)) return;
+  const Col c = col_reg(i, j, l);
+  const Met m = met_of(false);
+  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
+  const bool in = interior(i, j);
+  const double* const* P = a.P.v;
+  const double dt = a.dt;
+  auto rhog_h = [&](int k) -> double {
+    int kk = (k < kmin) ? kmin : k;
+    return mc(m.C2W, c, 0, 2, kk) * P[0][c.at(kk)] + mc(m.C2W, c, 1, 2, kk) * P[0][c.at(kk - 1)];
+  };
+  auto eth_h = [&](int k) -> double {
+    int kk = (k < kmin) ? kmin : k;
+    return cC.afact[kk] * a.eth[c.at(kk)] + cC.bfact[kk] * a.eth[c.at(kk - 1)];
+  };
+  auto dbuo = [&](int k) -> double {
+    if (k < kmin + 1 || k > kmax) return 0.0;
+    return -cC.GRAV * (mc(m.C2W, c, 0, 2, k) * a.rhogd[c.at(k)] + mc(m.C2W, c, 1, 2, k) * a.rhogd[c.at(k - 1)]);
+  };
+  auto dpgw = [&](int k) -> double { return presgradw(c, m, k, [&](int kk) { return a.pregd[c.at(kk)]; }); };
+  auto gz = [&](int k) -> double { return cC.GRAV - (dpgw(k) - dbuo(k)) / rhog_h(k); };
+  auto pwh = [&](int k) -> double { return -gz(k) * P[4][c.at(k)]; };
+  auto PF = [&](int k, int d) -> double { return P[1 + d][c.at(k)]; };
+  auto PEF = [&](int k, int d) -> double { return P[1 + d][c.at(k)] * a.eth[c.at(k)]; };
+  for (int k = 0; k < KA; ++k) {
+    const long long p = c.at(k);
+    const bool hk = in && k >= kmin && k <= kmax;
+    const double div1 = hk ? h.out[0][p] : 0.0, div2 = hk ? h.out[1][p] : 0.0;
+    const double drhog = fluxconv_col(c, m, k, div1, 1.0, PF, [&](int kk) { return P[4][c.at(kk)]; });
+    const double drhoge = fluxconv_col(c, m, k, div2, 1.0, PEF, [&](int kk) {
+      long long q = c.at(kk);
+      return P[4][q] * (cC.afact[kk] * a.eth[q] + cC.bfact[kk] * a.eth[c.at(kk - 1)]);
+    });
+    double dd[3], dpg[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      dd[d] = hk ? h.out[2 + d][p] : 0.0;
+      dpg[d] = hk ? h.out[5 + d][p] : 0.0;
+    }
+    double pw = 0.0;
+    if (k >= kmin && k <= kmax)
+      pw = a.vx[p] * dpg[0] + a.vy[p] * dpg[1] + a.vz[p] * dpg[2] + mc(m.W2C, c, 0, 2, k) * pwh(k + 1) +
+           mc(m.W2C, c, 1, 2, k) * pwh(k);
+    a.gT[0][p] = a.gT0[0][p] + drhog;
+    a.gT[1][p] = a.gT0[1][p] - dpg[0] + dd[0] + 0.0;
+    a.gT[2][p] = a.gT0[2][p] - dpg[1] + dd[1] + 0.0;
+    a.gT[3][p] = a.gT0[3][p] - dpg[2] + dd[2] + 0.0;
+    a.gT[4][p] = a.gT0[4][p] + 0.0 * cC.alpha - dpgw(k) + dbuo(k);
+    a.gT[5][p] = a.gT0[5][p] + drhoge + pw;
+    if (k >= kmin + 1 && k <= kmax) {
+      const double GCVovR = cC.GRAV * cC.CVdry / cC.Rdry;
+      const double ACVovRt2 = cC.alpha * cC.CVdry / cC.Rdry / (dt * dt);
+      long long pm = c.at(k - 1), pp = c.at(k + 1);
+      double rg = cC.rdgz[k], rgm = cC.rdgz[k - 1];
+      double Ca = (m.RGSGAM2[p] * rg + m.RGSGAM2[pm] * rgm) * m.GAM2H[p];
+      double Cb = cC.dfact[k] - cC.cfact[k - 1];
+      double Cu1 = m.RGSGAM2[p] * rg * m.GAM2H[pp];
+      double rgh2 = m.RGAMH[p] * m.RGAMH[p];
+      double Cu2 = m.GAM2H[pp] * rgh2 * GCVovR;
+      double Cl1 = m.RGSGAM2[p] * rg * m.GAM2H[pm];
+      double Cl2 = m.GAM2H[pm] * rgh2 * GCVovR;
+      double rgh = cC.rdgzh[k];
+      a.Mc[p] = ACVovRt2 / m.RGSQRTH[p] + rgh * (Ca * eth_h(k) - Cb * (gz(k) + GCVovR));
+      a.Mu[p] = -rgh * (Cu1 * eth_h(k + 1) + cC.cfact[k] * (gz(k + 1) + Cu2));
+      a.Ml[p] = -rgh * (Cl1 * eth_h(k - 1) - cC.dfact[k - 1] * (gz(k - 1) + Cl2));
+    }
+    double kin0 = rhogkin_at(c, m, k, [&](int kk, int comp) { return P[comp][c.at(kk)]; });
+    a.ethtot0[p] = a.eth[p] + kin0 / P[0][p] + m.PHI[p];
+  }
+}
+
 __global__ void k_vp0(Vp0Args a, int pole) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
