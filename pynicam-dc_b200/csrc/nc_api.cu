@@ -583,10 +583,14 @@ static int run_step(nc_handle* h) {
         va.PM0 = F(h->PM[0]); va.PM4 = F(h->PM[4]);
         va.dt = h->dts; va.rweight = rweight; va.RovCV = RovCV;
         if (!pole) {
-          k_vimain_a<<<greg, kBlock, 0, s>>>(va, 0);
+          const dim3 gt((unsigned)((D.G - 2 + DD_DX - 1) / DD_DX), (unsigned)((D.G - 2 + DD_DY - 1) / DD_DY),
+                        (unsigned)D.L);
+          k_vimain_a_t<<<gt, DD_DX * DD_DY, 0, s>>>(va);
           TRY(check_launch(h, "vimain_a"));
-          k_vimain_b<<<greg, kBlock, 0, s>>>(va, 0);
-          TRY(check_launch(h, "vimain_b"));
+          k_vi_solve<<<greg, kBlock, 0, s>>>(va);
+          TRY(check_launch(h, "vi_solve"));
+          k_vi_energy<<<greg, kBlock, 0, s>>>(va);
+          TRY(check_launch(h, "vi_energy"));
         } else {
           k_vimain_a<<<1, plk, 0, s>>>(va, 1);
           TRY(check_launch(h, "vimain_a_pl"));

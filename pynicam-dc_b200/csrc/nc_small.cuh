@@ -984,6 +984,68 @@ __global__ void k_vimain_a(VimainArgs a, int pole) {
   }
 }
 
+// Tiled kernel A of vi_main for interior cells and levels kmin..kmax: the
+// haloed tiles of RGAM*diff_vh, RGAM*diff_vh*eth and RGAM*(rhogv+diff_vh)*ethtot0
+// are staged per level and the three 7-point divergences formed from shared
+// memory.  Halo cells and boundary levels of hdiv stay zero from allocation
+// (the column kernel reads zero divergence there, as with k_vimain_a).
+__global__ void __launch_bounds__(DD_DX * DD_DY) k_vimain_a_t(VimainArgs a) {
+  constexpr int PX = DD_DX + 2, PY = DD_DY + 2;
+  __shared__ double s_h[3][3][PY * PX];
+  const int l = blockIdx.z;
+  const int i0 = 1 + blockIdx.x * DD_DX, j0 = 1 + blockIdx.y * DD_DY;
+  const int G = cD.G, gmax = cD.G - 2;
+  const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool own = (i <= gmax) && (j <= gmax);
+  for (int k = cD.kmin; k <= cD.kmax; ++k) {
+    for (int p = tid; p < PX * PY; p += blockDim.x) {
+      const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
+      if (ii < G && jj < G) {
+        const long long q = ix(ii, jj, k, l);
+        const double rg = cG.RGAM[q], e = a.eth[q], et = a.ethtot0[q];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double dv = a.dvh.f[d][q];
+          s_h[0][d][p] = dv * rg;
+          s_h[1][d][p] = (dv * e) * rg;
+          s_h[2][d][p] = ((a.P[1 + d][q] + dv) * et) * rg;
+        }
+      } else {
+#pragma unroll
+        for (int f = 0; f < 3; ++f)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) s_h[f][d][p] = 0.0;
+      }
+    }
+    __syncthreads();
+    if (own) {
+      const int c0 = (ty + 1) * PX + (tx + 1);
+      const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
+      const long long q = ix(i, j, k, l);
+      double acc[3][3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double s[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int m = 0; m < 7; ++m) {
+          const double cdv = P2(cG.coef_div, d * 7 + m, i, j, l);
+#pragma unroll
+          for (int f = 0; f < 3; ++f) {
+            const double t = cdv * s_h[f][d][nb[m]];
+            s[f] = (m == 0) ? t : s[f] + t;
+          }
+        }
+#pragma unroll
+        for (int f = 0; f < 3; ++f) acc[f][d] = s[f];
+      }
+#pragma unroll
+      for (int f = 0; f < 3; ++f) a.hdiv[f][q] = acc[f][0] + acc[f][1] + acc[f][2];
+    }
+    __syncthreads();
+  }
+}
+
 template <bool POLE>
 __device__ void vimain_column(const VimainArgs& a, const Col c) {
   const Met m = met_of(POLE);
@@ -1092,6 +1154,164 @@ __device__ void vimain_column(const VimainArgs& a, const Col c) {
     a.dwe[2][p] = re;
     a.PM0[p] = a.PM0[p] + rs1[k] * a.rweight;
     a.PM4[p] = a.PM4[p] + rws1[k] * a.rweight;
+  }
+}
+
+// Regional vi_main in two column kernels (interior columns; the halo columns
+// of the outputs are replaced by the exchange that follows).
+// k_vi_solve: flux convergences of diff_vh (rolling half-level fluxes), the
+// Thomas forward sweep, then the back substitution fused with rhog_split1 on
+// the way down; writes rhog_s1, rhogw_s1 and their running means.
+__global__ void __launch_bounds__(128) k_vi_solve(VimainArgs a) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (!col_of(t, i, j, l) || !interior(i, j)) return;
+  const Col c = col_reg(i, j, l);
+  const Met m = met_of(false);
+  const int kmin = cD.kmin, kmax = cD.kmax, kT = kmax + 1;
+  const double dt = a.dt, Rdry = cC.Rdry, CVdry = cC.CVdry, RovCV = a.RovCV;
+  const long long n = cD.npt;
+  const double* cz = cG.C2WGz;
+  const double* const* DVp = a.dvh.f;
+  auto preg0 = [&](int k) -> double {
+    const int k2 = k < kmin ? kmin : (k > kmax ? kmax : k);
+    return a.PS[5][c.at(k2)] * RovCV;
+  };
+  // horizontal part of the half-level flux of diff_vh (and of diff_vh*eth) at kk
+  auto hflux = [&](int kk, bool withe) -> double {
+    const long long q = c.at(kk), qm = c.at(kk - 1);
+    const double e = withe ? a.eth[q] : 1.0, em = withe ? a.eth[qm] : 1.0;
+    double f0 = DVp[0][q], f0m = DVp[0][qm], f1 = DVp[1][q], f1m = DVp[1][qm], f2 = DVp[2][q], f2m = DVp[2][qm];
+    if (withe) {
+      f0 = f0 * e; f0m = f0m * em; f1 = f1 * e; f1m = f1m * em; f2 = f2 * e; f2m = f2m * em;
+    }
+    const double h = cz[q] * f0 + cz[n + q] * f0m + cz[2 * n + q] * f1 + cz[3 * n + q] * f1m + cz[4 * n + q] * f2 +
+                     cz[5 * n + q] * f2m;
+    return h * m.RGAMH[q];
+  };
+  double hD[NC_MAXK];
+  const long long pT = c.at(kT), pK = c.at(kmax);
+  const double rw_top = -(cz[pT] * DVp[0][pT] + cz[n + pT] * DVp[0][pK] + cz[2 * n + pT] * DVp[1][pT] +
+                          cz[3 * n + pT] * DVp[1][pK] + cz[4 * n + pT] * DVp[2][pT] + cz[5 * n + pT] * DVp[2][pK]);
+  const double CVovRt2 = CVdry / Rdry / (dt * dt);
+  const double rw_kmin = 0.0 * m.RGSGAM2H[c.at(kmin)];
+  const double rw_kmaxp1 = rw_top * m.RGSGAM2H[pT];
+  const int N = kmax - kmin;
+  double u[NC_MAXK], gam[NC_MAXK];
+  double vD_lo = 0.0, vE_lo = 0.0, g1_prev = 0.0, gp_prev = 0.0, beta = 0.0;
+  for (int k = kmin; k <= kmax; ++k) {
+    const long long p = c.at(k);
+    const int kk = k + 1;
+    double vD_hi = 0.0, vE_hi = 0.0;
+    if (kk <= kmax) {
+      const double hd = hflux(kk, false);
+      hD[kk] = hd;
+      const double rq = m.RGSQRTH[c.at(kk)];
+      vD_hi = hd + 0.0 * a.PS[4][c.at(kk)] * rq;
+      vE_hi = hflux(kk, true) + 0.0 * 0.0 * rq;
+    }
+    const double drhog = -a.hdiv[0][p] - (vD_hi - vD_lo) * cC.rdgz[k];
+    const double drhoge = -a.hdiv[1][p] - (vE_hi - vE_lo) * cC.rdgz[k];
+    const double g1 = a.gT[0][p] + drhog;
+    const double gp = (a.gT[5][p] + drhoge) * Rdry / CVdry;
+    if (k >= kmin + 1) {
+      const int nn = k - kmin - 1;
+      const long long pm = c.at(k - 1);
+      const double rg2 = m.RGAMH[p] * m.RGAMH[p];
+      const double rgam2 = m.RGAM[p] * m.RGAM[p], rgam2m = m.RGAM[pm] * m.RGAM[pm];
+      const double Sw = a.gT[4][p] + 0.0 * cC.alpha;
+      double S = ((a.PS[4][p] * cC.alpha + dt * Sw) * rg2 -
+                  ((preg0(k) + dt * gp) * m.RGSGAM2[p] - (preg0(k - 1) + dt * gp_prev) * m.RGSGAM2[pm]) * dt *
+                      cC.rdgzh[k] -
+                  ((a.PS[0][p] + dt * g1) * rgam2 * cC.afact[k] + (a.PS[0][pm] + dt * g1_prev) * rgam2m * cC.bfact[k]) *
+                      dt * cC.GRAV) *
+                 CVovRt2;
+      if (nn == 0) S = S - a.Ml[c.at(kmin + 1)] * rw_kmin;
+      if (nn == N - 1) S = S - a.Mu[c.at(kmax)] * rw_kmaxp1;
+      const double Mc = a.Mc[p], Ml = a.Ml[p];
+      if (nn == 0) {
+        beta = Mc;
+        u[0] = S / beta;
+      } else {
+        const double gg = a.Mu[pm] / beta;
+        beta = Mc - Ml * gg;
+        u[nn] = (S - Ml * u[nn - 1]) / beta;
+        gam[nn] = gg;
+      }
+    }
+    g1_prev = g1;
+    gp_prev = gp;
+    vD_lo = vD_hi;
+    vE_lo = vE_hi;
+  }
+  // back substitution (downward) fused with rhog_split1
+  double x = 0.0, rws_hi = 0.0, v2_hi = 0.0;
+  for (int k = kT; k >= 0; --k) {
+    const long long p = c.at(k);
+    double rws;
+    if (k == kT) {
+      rws = rw_kmaxp1 * m.GSGAM2H[p];
+    } else if (k >= kmin + 1) {
+      const int nn = k - kmin - 1;
+      x = (nn == N - 1) ? u[N - 1] : u[nn] - gam[nn + 1] * x;
+      rws = x * m.GSGAM2H[p];
+    } else if (k == kmin) {
+      rws = rw_kmin * m.GSGAM2H[p];
+    } else {
+      rws = 0.0;
+    }
+    const double v2 = (k > kmin && k <= kmax) ? hD[k] + 1.0 * rws * m.RGSQRTH[p] : 0.0;
+    double drhog2 = 0.0;
+    if (k >= kmin && k <= kmax) drhog2 = -a.hdiv[0][p] - (v2_hi - v2) * cC.rdgz[k];
+    const double rs = a.PS[0][p] + (a.gT[0][p] + drhog2) * dt;
+    a.dwe[0][p] = rs;
+    a.dwe[1][p] = rws;
+    a.PM0[p] = a.PM0[p] + rs * a.rweight;
+    a.PM4[p] = a.PM4[p] + rws * a.rweight;
+    rws_hi = rws;
+    v2_hi = v2;
+  }
+  (void)rws_hi;
+}
+
+// k_vi_energy: kinetic energies, total-energy advection and rhoge_split1 from
+// the rhog_s1 / rhogw_s1 written by k_vi_solve.
+__global__ void __launch_bounds__(128) k_vi_energy(VimainArgs a) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (!col_of(t, i, j, l) || !interior(i, j)) return;
+  const Col c = col_reg(i, j, l);
+  const Met m = met_of(false);
+  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
+  const double dt = a.dt;
+  const double* rs1 = a.dwe[0];
+  const double* rws1 = a.dwe[1];
+  auto PSk = [&](int comp, int k) -> double {
+    if (comp == 5) k = k < kmin ? kmin : (k > kmax ? kmax : k);
+    return a.PS[comp][c.at(k)];
+  };
+  for (int k = 0; k < KA; ++k) {
+    const long long p = c.at(k);
+    auto st10 = [&](int kk, int comp) -> double { return a.P[comp][c.at(kk)] + PSk(comp, kk); };
+    auto st11 = [&](int kk, int comp) -> double {
+      const long long q = c.at(kk);
+      if (comp == 0) return a.P[0][q] + rs1[q];
+      if (comp == 4) return a.P[4][q] + rws1[q];
+      return a.P[comp][q] + a.dvh.f[comp - 1][q];
+    };
+    const double kin10 = rhogkin_at(c, m, k, st10);
+    const double kin11 = rhogkin_at(c, m, k, st11);
+    const double drhogetot = fluxconv_col(
+        c, m, k, a.hdiv[2][p], 1.0,
+        [&](int kk, int d) {
+          const long long q = c.at(kk);
+          return (a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q];
+        },
+        [&](int kk) {
+          const long long q = c.at(kk), qm = c.at(kk - 1);
+          return (a.P[4][q] + rws1[q]) * (cC.afact[kk] * a.ethtot0[q] + cC.bfact[kk] * a.ethtot0[qm]);
+        });
+    a.dwe[2][p] = PSk(5, k) + (a.gT0e[p] + drhogetot) * dt + (kin10 - kin11) + (PSk(0, k) - rs1[p]) * m.PHI[p];
   }
 }
 
