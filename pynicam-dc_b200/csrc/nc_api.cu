@@ -404,6 +404,9 @@ static int run_step(nc_handle* h) {
   const unsigned plk = (unsigned)(((D.KA * D.LP) + 31) / 32 * 32);
   const unsigned npt_blocks = (unsigned)((D.npt + kBlock - 1) / kBlock);
   const unsigned npl_blocks = (unsigned)((D.npl + kBlock - 1) / kBlock);
+  // per-level tiled kernels: (levels kmin..kmax, tiles, regions)
+  const dim3 lvgrid((unsigned)(D.kmax - D.kmin + 1),
+                    (unsigned)(((D.G - 2 + DD_DX - 1) / DD_DX) * ((D.G - 2 + DD_DY - 1) / DD_DY)), (unsigned)D.L);
   // PROG0 = PROG at the start of the step (mod_dynamics.py:1939-1968)
   for (int v = 0; v < 6; ++v) {
     CU(cudaMemcpyAsync(h->P0[v].r, h->P[v].r, D.npt * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -504,8 +507,7 @@ static int run_step(nc_handle* h) {
       for (int d = 0; d < 3; ++d) { o.f[d] = h->vtmp2[d].r; op.f[d] = h->vtmp2[d].p; }
       // interior cells only: halo rows are filled by the exchange below and the
       // boundary levels of vtmp2 stay zero from allocation
-      const dim3 gt((unsigned)((D.G - 2 + DD_DX - 1) / DD_DX), (unsigned)((D.G - 2 + DD_DY - 1) / DD_DY), (unsigned)D.L);
-      k_dd3d_t<<<gt, DD_DX * DD_DY, 0, s>>>(v, o);
+      k_dd3d_l<<<lvgrid, DD_DX * DD_DY, 0, s>>>(v, o);
       TRY(check_launch(h, "dd3d"));
       k_dd3d_pl<<<1, plk, 0, s>>>(vp, op);
       TRY(check_launch(h, "dd3d_pl"));
@@ -561,9 +563,7 @@ static int run_step(nc_handle* h) {
         for (int n = 0; n < 5; ++n) pa.PM[n] = F(h->PM[n]);
         pa.dt = h->dts; pa.rweight = rweight; pa.RovCV = RovCV;
         if (!pole) {
-          const dim3 gt((unsigned)((D.G - 2 + DD_DX - 1) / DD_DX), (unsigned)((D.G - 2 + DD_DY - 1) / DD_DY),
-                        (unsigned)D.L);
-          k_path1_t<<<gt, DD_DX * DD_DY, 0, s>>>(pa);
+          k_path1_l<<<lvgrid, DD_DX * DD_DY, 0, s>>>(pa);
           TRY(check_launch(h, "path1"));
         } else {
           k_path1<<<1, 32, 0, s>>>(pa, 1);
@@ -589,7 +589,7 @@ static int run_step(nc_handle* h) {
           TRY(check_launch(h, "vimain_a"));
           k_vi_solve<<<greg, kBlock, 0, s>>>(va);
           TRY(check_launch(h, "vi_solve"));
-          k_vi_energy<<<greg, kBlock, 0, s>>>(va);
+          k_vi_energy_p<<<npt_blocks, kBlock, 0, s>>>(va);
           TRY(check_launch(h, "vi_energy"));
         } else {
           k_vimain_a<<<1, plk, 0, s>>>(va, 1);

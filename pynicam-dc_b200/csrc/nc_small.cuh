@@ -189,6 +189,102 @@ __global__ void __launch_bounds__(DD_DX * DD_DY) k_dd3d_t(Four v, Three out) {
   }
 }
 
+// Block -> (level, tile, region) of the per-level tiled kernels: the level
+// is the fastest block index so that blocks sharing a tile's haloed data at
+// neighbouring levels run together and meet in L2.
+struct TileLv {
+  int k, l, i0, j0;
+};
+__device__ __forceinline__ TileLv tile_level(int kbase) {
+  const int ntx = (cD.G - 2 + DD_DX - 1) / DD_DX;
+  TileLv t;
+  t.k = kbase + (int)blockIdx.x;
+  t.l = (int)blockIdx.z;
+  t.i0 = 1 + ((int)blockIdx.y % ntx) * DD_DX;
+  t.j0 = 1 + ((int)blockIdx.y / ntx) * DD_DY;
+  return t;
+}
+
+// 3-D divergence damping, one block per (level, tile): the haloed tile of
+// RGAM-scaled momentum and of the vertical mass flux at k and k+1 is staged,
+// every triangle value formed once (singular-point fix at the (0,0) vertex),
+// then each thread writes its cell.  Same arithmetic as k_dd3d.
+__global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_dd3d_l(Four v, Three out) {
+  constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
+  __shared__ double s_vm[3][PY * PX];
+  __shared__ double s_rd[PY * PX], s_ru[PY * PX];
+  __shared__ double s_ti[TY * TX], s_tj[TY * TX];
+  const TileLv tl = tile_level(cD.kmin);
+  const int k = tl.k, l = tl.l, i0 = tl.i0, j0 = tl.j0;
+  const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin, kmax = cD.kmax;
+  const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
+  const long long n = cD.npt;
+  const double* cz = cG.C2WGz;
+  auto rwv = [&](long long q, long long qm) {
+    const double h = cz[q] * v.f[0][q] + cz[n + q] * v.f[0][qm] + cz[2 * n + q] * v.f[1][q] +
+                     cz[3 * n + q] * v.f[1][qm] + cz[4 * n + q] * v.f[2][q] + cz[5 * n + q] * v.f[2][qm];
+    return h * cG.RGAMH[q] + v.f[3][q] * cG.RGSQRTH[q];
+  };
+  for (int p = tid; p < PX * PY; p += blockDim.x) {
+    const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
+    double a = 0.0, b = 0.0, c = 0.0, rd = 0.0, ru = 0.0;
+    if (ii < G && jj < G) {
+      const long long q = ix(ii, jj, k, l);
+      const double rg = cG.RGAM[q];
+      a = v.f[0][q] * rg;
+      b = v.f[1][q] * rg;
+      c = v.f[2][q] * rg;
+      if (k > kmin) rd = rwv(q, q - cD.plane);
+      if (k + 1 <= kmax) ru = rwv(q + cD.plane, q);
+    }
+    s_vm[0][p] = a;
+    s_vm[1][p] = b;
+    s_vm[2][p] = c;
+    s_rd[p] = rd;
+    s_ru[p] = ru;
+  }
+  __syncthreads();
+  const double rdz = cC.rdgz[k];
+  for (int p = tid; p < TX * TY; p += blockDim.x) {
+    const int px = p % TX, py = p / TX;
+    const int ii = i0 - 1 + px, jj = j0 - 1 + py;
+    double sTI = 0.0, sTJ = 0.0;
+    if (ii <= G - 2 && jj <= G - 2) {
+      const int a = py * PX + px, b = a + 1, c = a + PX + 1, d = a + PX;
+      auto C = [&](int dir, int pt, int t) { return P2(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
+      const double wTI = ((s_ru[a] + s_ru[b] + s_ru[c]) - (s_rd[a] + s_rd[b] + s_rd[c])) / 3.0 * rdz;
+      const double wTJ = ((s_ru[a] + s_ru[c] + s_ru[d]) - (s_rd[a] + s_rd[c] + s_rd[d])) / 3.0 * rdz;
+      sTI = C(0, 0, 0) * s_vm[0][a] + C(0, 1, 0) * s_vm[0][b] + C(0, 2, 0) * s_vm[0][c] +
+            C(1, 0, 0) * s_vm[1][a] + C(1, 1, 0) * s_vm[1][b] + C(1, 2, 0) * s_vm[1][c] +
+            C(2, 0, 0) * s_vm[2][a] + C(2, 1, 0) * s_vm[2][b] + C(2, 2, 0) * s_vm[2][c] + wTI;
+      sTJ = C(0, 0, 1) * s_vm[0][a] + C(0, 1, 1) * s_vm[0][c] + C(0, 2, 1) * s_vm[0][d] +
+            C(1, 0, 1) * s_vm[1][a] + C(1, 1, 1) * s_vm[1][c] + C(1, 2, 1) * s_vm[1][d] +
+            C(2, 0, 1) * s_vm[2][a] + C(2, 1, 1) * s_vm[2][c] + C(2, 2, 1) * s_vm[2][d] + wTJ;
+    }
+    s_ti[p] = sTI;
+    s_tj[p] = sTJ;
+  }
+  __syncthreads();
+  if (tid == 0 && i0 == 1 && j0 == 1)
+    s_ti[0] = s_ti[0] * (double)cG.pntmask[l * 2 + 0] + s_tj[1] * (double)cG.pntmask[l * 2 + 1];
+  __syncthreads();
+  const int i = i0 + tx, j = j0 + ty;
+  if (i <= gmax && j <= gmax) {
+    const int ta = (ty + 1) * TX + (tx + 1);
+    const double aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
+    const double cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1], dTJ = s_tj[ta - TX];
+    const long long q = ix(i, j, k, l);
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      out.f[d][q] = P2(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) +
+                    P2(cG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
+                    P2(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) +
+                    P2(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
+                    P2(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) +
+                    P2(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI);
+  }
+}
+
 // pole 3-D divergence damping (kernels/oprt3ddivdamp.py:176-237)
 __global__ void k_dd3d_pl(Four v, Three out) {
   int t = threadIdx.x;
@@ -913,6 +1009,131 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_path1_t(Path1Args a) {
   }
 }
 
+// Regional path 1, one block per (level, tile): same stencils and
+// arithmetic as path1_column.  The blocks at kmin and kmax also write the
+// boundary rows kmin-1 and kmax+1 from the values they computed.
+__global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_path1_l(Path1Args a) {
+  constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
+  __shared__ double s_v[3][PY * PX];
+  __shared__ double s_p[PY * PX];
+  __shared__ double s_ti[TY * TX], s_tj[TY * TX];
+  const TileLv tl = tile_level(cD.kmin);
+  const int k = tl.k, l = tl.l, i0 = tl.i0, j0 = tl.j0;
+  const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin, kmax = cD.kmax;
+  const int kk = (k == kmin) ? kmin + 1 : k;
+  const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
+  const double RovCV = a.RovCV;
+  for (int p = tid; p < PX * PY; p += blockDim.x) {
+    const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
+    double x = 0.0, y = 0.0, z = 0.0, pp = 0.0;
+    if (ii < G && jj < G) {
+      const long long q = ix(ii, jj, k, l);
+      x = -a.vt.f[0][q];
+      y = -a.vt.f[1][q];
+      z = -a.vt.f[2][q];
+      const long long qk = ix(ii, jj, kk, l);
+      pp = a.PS[5][qk] * RovCV * cG.RGAM[qk];
+    }
+    s_v[0][p] = x;
+    s_v[1][p] = y;
+    s_v[2][p] = z;
+    s_p[p] = pp;
+  }
+  __syncthreads();
+  for (int p = tid; p < TX * TY; p += blockDim.x) {
+    const int px = p % TX, py = p / TX;
+    const int ii = i0 - 1 + px, jj = j0 - 1 + py;
+    double sTI = 0.0, sTJ = 0.0;
+    if (ii <= G - 2 && jj <= G - 2) {
+      const int ia = py * PX + px, ib = ia + 1, ic = ia + PX + 1, id = ia + PX;
+      auto C = [&](int dir, int pt, int t) { return P2(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
+      sTI = C(0, 0, 0) * s_v[0][ia] + C(0, 1, 0) * s_v[0][ib] + C(0, 2, 0) * s_v[0][ic] +
+            C(1, 0, 0) * s_v[1][ia] + C(1, 1, 0) * s_v[1][ib] + C(1, 2, 0) * s_v[1][ic] +
+            C(2, 0, 0) * s_v[2][ia] + C(2, 1, 0) * s_v[2][ib] + C(2, 2, 0) * s_v[2][ic];
+      sTJ = C(0, 0, 1) * s_v[0][ia] + C(0, 1, 1) * s_v[0][ic] + C(0, 2, 1) * s_v[0][id] +
+            C(1, 0, 1) * s_v[1][ia] + C(1, 1, 1) * s_v[1][ic] + C(1, 2, 1) * s_v[1][id] +
+            C(2, 0, 1) * s_v[2][ia] + C(2, 1, 1) * s_v[2][ic] + C(2, 2, 1) * s_v[2][id];
+    }
+    s_ti[p] = sTI;
+    s_tj[p] = sTJ;
+  }
+  __syncthreads();
+  const int i = i0 + tx, j = j0 + ty;
+  if (i > gmax || j > gmax) return;
+  const double r = cC.rscale, ddc = cC.divdamp_coef, dt = a.dt, rweight = a.rweight;
+  const long long n = cD.npt;
+  const double* cz = cG.C2WGz;
+  const double gx = P2(cG.GRD_x, 0, i, j, l), gy = P2(cG.GRD_x, 1, i, j, l), gz = P2(cG.GRD_x, 2, i, j, l);
+  const long long q0 = ix(i, j, 0, l);
+  auto Pown = [&](int k2) {
+    const int kc = k2 < kmin ? kmin : (k2 > kmax ? kmax : k2);
+    return a.PS[5][q0 + (long long)kc * cD.plane] * RovCV;
+  };
+  const int ta = (ty + 1) * TX + (tx + 1);
+  const double aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
+  const double cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1], dTJ = s_tj[ta - TX];
+  double dd[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    dd[d] = ddc * (P2(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) + P2(cG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
+                   P2(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) + P2(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
+                   P2(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) + P2(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI));
+  {
+    const double prd = (dd[0] * gx + dd[1] * gy + dd[2] * gz) / r;
+    dd[0] = dd[0] - prd * gx / r;
+    dd[1] = dd[1] - prd * gy / r;
+    dd[2] = dd[2] - prd * gz / r;
+  }
+  const int c0 = (ty + 1) * PX + (tx + 1);
+  const double s7[7] = {s_p[c0], s_p[c0 + 1], s_p[c0 + PX + 1], s_p[c0 + PX], s_p[c0 - 1], s_p[c0 - PX - 1], s_p[c0 - PX]};
+  const long long qkk = q0 + (long long)kk * cD.plane, qk1 = qkk + cD.plane;
+  const double P_k1 = Pown(kk + 1), P_k = Pown(kk), P_km = Pown(kk - 1);
+  const double rgh1 = cG.RGAMH[qk1], rgh0 = cG.RGAMH[qkk];
+  double pg[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double g = P2(cG.coef_grad, d * 7 + 0, i, j, l) * s7[0];
+#pragma unroll
+    for (int m = 1; m < 7; ++m) g = g + P2(cG.coef_grad, d * 7 + m, i, j, l) * s7[m];
+    const double up = (cz[(2 * d) * n + qk1] * P_k1 + cz[(2 * d + 1) * n + qk1] * P_k) * rgh1;
+    const double dn = (cz[(2 * d) * n + qkk] * P_k + cz[(2 * d + 1) * n + qkk] * P_km) * rgh0;
+    pg[d] = g + (up - dn) * cC.rdgz[kk];
+  }
+  {
+    const double prd = (pg[0] * gx + pg[1] * gy + pg[2] * gz) / r;
+    pg[0] = pg[0] - prd * gx / r;
+    pg[1] = pg[1] - prd * gy / r;
+    pg[2] = pg[2] - prd * gz / r;
+  }
+  const long long q = q0 + (long long)k * cD.plane;
+  double v[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double drv = a.gT[1 + d][q] - pg[d] + dd[d] + 0.0;
+    v[d] = a.PS[1 + d][q] + drv * dt;
+    a.dvh[d][q] = v[d];
+    a.PM[1 + d][q] = a.PM[1 + d][q] + v[d] * rweight;
+  }
+  if (k == kmin) {
+    const long long pB = q - cD.plane;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double vB = -1.0 * (v[d] / a.rhog[q]) * a.rhog[pB];
+      a.dvh[d][pB] = vB;
+      a.PM[1 + d][pB] = a.PM[1 + d][pB] + vB * rweight;
+    }
+  }
+  if (k == kmax) {
+    const long long pT = q + cD.plane;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double vT = 1.0 * (v[d] / a.rhog[q]) * a.rhog[pT];
+      a.dvh[d][pT] = vT;
+      a.PM[1 + d][pT] = a.PM[1 + d][pT] + vT * rweight;
+    }
+  }
+}
+
 __global__ void k_path1(Path1Args a, int pole) {
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
@@ -1313,6 +1534,47 @@ __global__ void __launch_bounds__(128) k_vi_energy(VimainArgs a) {
         });
     a.dwe[2][p] = PSk(5, k) + (a.gT0e[p] + drhogetot) * dt + (kin10 - kin11) + (PSk(0, k) - rs1[p]) * m.PHI[p];
   }
+}
+
+// k_vi_energy with one thread per interior grid point (the energy update has
+// no vertical recurrence; neighbouring levels are read through the cache).
+__global__ void __launch_bounds__(128) k_vi_energy_p(VimainArgs a) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cD.npt) return;
+  const int G = cD.G, KA = cD.KA;
+  const int i = (int)(t % G), j = (int)((t / G) % G), k = (int)((t / ((long long)G * G)) % KA);
+  const int l = (int)(t / ((long long)G * G * KA));
+  if (!interior(i, j)) return;
+  const Col c = col_reg(i, j, l);
+  const Met m = met_of(false);
+  const int kmin = cD.kmin, kmax = cD.kmax;
+  const double* rs1 = a.dwe[0];
+  const double* rws1 = a.dwe[1];
+  auto PSk = [&](int comp, int kk) -> double {
+    if (comp == 5) kk = kk < kmin ? kmin : (kk > kmax ? kmax : kk);
+    return a.PS[comp][c.at(kk)];
+  };
+  const long long p = c.at(k);
+  auto st10 = [&](int kk, int comp) -> double { return a.P[comp][c.at(kk)] + PSk(comp, kk); };
+  auto st11 = [&](int kk, int comp) -> double {
+    const long long q = c.at(kk);
+    if (comp == 0) return a.P[0][q] + rs1[q];
+    if (comp == 4) return a.P[4][q] + rws1[q];
+    return a.P[comp][q] + a.dvh.f[comp - 1][q];
+  };
+  const double kin10 = rhogkin_at(c, m, k, st10);
+  const double kin11 = rhogkin_at(c, m, k, st11);
+  const double drhogetot = fluxconv_col(
+      c, m, k, a.hdiv[2][p], 1.0,
+      [&](int kk, int d) {
+        const long long q = c.at(kk);
+        return (a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q];
+      },
+      [&](int kk) {
+        const long long q = c.at(kk), qm = c.at(kk - 1);
+        return (a.P[4][q] + rws1[q]) * (cC.afact[kk] * a.ethtot0[q] + cC.bfact[kk] * a.ethtot0[qm]);
+      });
+  a.dwe[2][p] = PSk(5, k) + (a.gT0e[p] + drhogetot) * a.dt + (kin10 - kin11) + (PSk(0, k) - rs1[p]) * m.PHI[p];
 }
 
 __global__ void k_vimain_b(VimainArgs a, int pole) {
