@@ -507,7 +507,8 @@ static int run_step(nc_handle* h) {
       for (int d = 0; d < 3; ++d) { o.f[d] = h->vtmp2[d].r; op.f[d] = h->vtmp2[d].p; }
       // interior cells only: halo rows are filled by the exchange below and the
       // boundary levels of vtmp2 stay zero from allocation
-      k_dd3d_l<<<lvgrid, DD_DX * DD_DY, 0, s>>>(v, o);
+      const dim3 gt((unsigned)((D.G - 2 + DD_DX - 1) / DD_DX), (unsigned)((D.G - 2 + DD_DY - 1) / DD_DY), (unsigned)D.L);
+      k_dd3d_t<<<gt, DD_DX * DD_DY, 0, s>>>(v, o);
       TRY(check_launch(h, "dd3d"));
       k_dd3d_pl<<<1, plk, 0, s>>>(vp, op);
       TRY(check_launch(h, "dd3d_pl"));
