@@ -130,6 +130,34 @@ int nc_grid_spring(int32_t lall, int32_t gall_1d, double* x, double* x_pl, const
                    const int64_t* p_src, int32_t np, double lambda, double dbar, double dt, double criterion,
                    int64_t max_iter, int64_t* iterations);
 
+/* Allocation-free air or tracer mass sum.  No counterpart in the reference.
+ * For callers that may not call cudaMalloc: code that runs inside another
+ * framework's memory manager (a caching allocator that owns the device memory,
+ * an XLA/JAX custom call) or on a stream that is being captured, where a new
+ * allocation either fails, is forbidden or would break the capture.  Creating
+ * a handle (nc_create) allocates, so this entry point takes no handle: the
+ * caller passes its own device arrays in the library's device layout --
+ * regional (lall, kall, gall_1d, gall_1d) C-order, pole (6, kall, 2) -- and a
+ * device output of one double, and the call is ordered on `stream` (a
+ * cudaStream_t; NULL for the legacy default stream).  out[0] = sum over
+ * interior cells and the two pole points, levels kmin..kmax, of
+ * num / gsgam2 * volume with num = rhogq if given, else rhog: the same
+ * compensated sum, in the same order, as nc_mass_sums.
+ * Limit: lall * gall_1d^2 + 2 <= 1,048,576 columns (grid level 8 at rlevel 1
+ * uses 676,002); larger grids get NC_ERR_ARG.  The block partial sums live in
+ * one fixed 64 KiB device array that every GPU loading the library keeps
+ * until the process exits; every call overwrites the slots it reads, so no
+ * state needs clearing between calls, but calls that run concurrently on the
+ * GPU (different streams, overlapping) race on it and must be serialized by
+ * the caller.  The first call on each device looks up that array's device
+ * address (cudaGetSymbolAddress) with the device current; make that first
+ * call before any stream capture.  Asynchronous: read out after the stream
+ * is synchronized. */
+int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* gsgam2, const double* volume,
+                        const double* rhog_pl, const double* rhogq_pl, const double* gsgam2_pl,
+                        const double* volume_pl, int32_t gall_1d, int32_t lall, int32_t kall, int32_t kmin,
+                        int32_t kmax, double* out, void* stream);
+
 const char* nc_last_error(void);
 
 void nc_destroy(nc_handle* h);

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -721,6 +722,90 @@ static int run_step(nc_handle* h) {
 }
 
 // ---------------------------------------------------------------------------
+// Allocation-free air/tracer mass sum (nc_mass_sum_noalloc).  Same per-block
+// compensated partial sums and the same fold order as k_mass + the host fold
+// of nc_mass_sums, but with all sizes passed as arguments (no handle, no
+// constant memory) and the block partials kept in a file-scope device array,
+// so a call allocates nothing.  Every call on a device shares this array.
+// ---------------------------------------------------------------------------
+#define NC_NOALLOC_MASS_MAX_BLOCKS 4096   // 4096 blocks x 256 columns = 1,048,576 columns
+static __device__ __align__(256) double g_mass_scratch[NC_NOALLOC_MASS_MAX_BLOCKS * 2];
+
+__global__ void k_mass_noalloc(const double* rhog, const double* rhogq, const double* gsgam2, const double* vol,
+                               const double* rhog_pl, const double* rhogq_pl, const double* gsgam2_pl,
+                               const double* vol_pl, int G, int L, int KA, int kmin, int kmax, double* part) {
+  __shared__ double ss[256], sc[256];
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long ncol = (long long)L * G * G;
+  double s = 0.0, c = 0.0;
+  const double* num = rhogq ? rhogq : rhog;
+  if (t < ncol) {
+    const int i = (int)(t % G), j = (int)((t / G) % G), l = (int)(t / ((long long)G * G));
+    if (i >= 1 && i <= G - 2 && j >= 1 && j <= G - 2) {
+      for (int k = kmin; k <= kmax; ++k) {
+        const long long p = (((long long)l * KA + k) * G + j) * G + i;
+        neu_add(s, c, num[p] / gsgam2[p] * vol[p]);
+      }
+    }
+  } else if (t - ncol < 2) {
+    const int lp = (int)(t - ncol);
+    const double* nump = rhogq_pl ? rhogq_pl : rhog_pl;
+    for (int k = kmin; k <= kmax; ++k) {
+      const int p = k * 2 + lp;   // pole point g = 0 of (g, k, lp)
+      neu_add(s, c, nump[p] / gsgam2_pl[p] * vol_pl[p]);
+    }
+  }
+  ss[threadIdx.x] = s;
+  sc[threadIdx.x] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double S = 0.0, C = 0.0;
+    for (int n = 0; n < (int)blockDim.x; ++n) {
+      neu_add(S, C, ss[n]);
+      C += sc[n];
+    }
+    part[blockIdx.x * 2 + 0] = S;
+    part[blockIdx.x * 2 + 1] = C;
+  }
+}
+
+// one thread folds the block partials in block order (the order of the host
+// fold in nc_mass_sums) and writes the sum
+__global__ void k_mass_noalloc_fold(const double* part, int nblocks, double* out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  double S = 0.0, Cc = 0.0;
+  for (int b = 0; b < nblocks; ++b) {
+    const double x = part[b * 2];
+    const double t = S + x;
+    if (fabs(S) >= fabs(x)) Cc += (S - t) + x;
+    else Cc += (x - t) + S;
+    S = t;
+    Cc += part[b * 2 + 1];
+  }
+  out[0] = S + Cc;
+}
+
+// device address of g_mass_scratch, looked up once per device
+static std::mutex g_scratch_mu;
+static std::map<int, double*> g_scratch_addr;
+
+static int mass_scratch_ptr(double** out) {
+  int dev = -1;
+  CU(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  auto it = g_scratch_addr.find(dev);
+  if (it != g_scratch_addr.end()) {
+    *out = it->second;
+    return 0;
+  }
+  double* ptr = nullptr;
+  CU(cudaGetSymbolAddress((void**)&ptr, g_mass_scratch));
+  g_scratch_addr[dev] = ptr;
+  *out = ptr;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
 extern "C" {
@@ -1256,6 +1341,34 @@ int nc_grid_spring(int32_t lall, int32_t gall_1d, double* x, double* x_pl, const
   for (void* p : mem) cudaFree(p);
   if (st) cudaStreamDestroy(st);
   return rc;
+}
+
+int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* gsgam2, const double* volume,
+                        const double* rhog_pl, const double* rhogq_pl, const double* gsgam2_pl,
+                        const double* volume_pl, int32_t gall_1d, int32_t lall, int32_t kall, int32_t kmin,
+                        int32_t kmax, double* out, void* stream) {
+  if (!rhog || !gsgam2 || !volume || !rhog_pl || !gsgam2_pl || !volume_pl || !out)
+    return fail(NC_ERR_ARG, "nc_mass_sum_noalloc: null pointer");
+  if ((rhogq == nullptr) != (rhogq_pl == nullptr))
+    return fail(NC_ERR_ARG, "nc_mass_sum_noalloc: rhogq and rhogq_pl must both be given or both be null");
+  if (gall_1d < 3 || lall < 1 || kmin < 0 || kmax < kmin || kmax >= kall)
+    return fail(NC_ERR_ARG, "nc_mass_sum_noalloc: bad sizes");
+  const long long cols = (long long)lall * gall_1d * gall_1d + 2;
+  const long long blocks = (cols + 255) / 256;
+  if (blocks > NC_NOALLOC_MASS_MAX_BLOCKS)
+    return fail(NC_ERR_ARG, "nc_mass_sum_noalloc: " + std::to_string(cols) +
+                                " columns exceed the fixed scratch limit of " +
+                                std::to_string((long long)NC_NOALLOC_MASS_MAX_BLOCKS * 256 - 2) +
+                                " (lall * gall_1d^2); use nc_mass_sums");
+  double* part = nullptr;
+  TRY(mass_scratch_ptr(&part));
+  cudaStream_t st = (cudaStream_t)stream;
+  k_mass_noalloc<<<(unsigned)blocks, 256, 0, st>>>(rhog, rhogq, gsgam2, volume, rhog_pl, rhogq_pl, gsgam2_pl,
+                                                   volume_pl, gall_1d, lall, kall, kmin, kmax, part);
+  CU(cudaGetLastError());
+  k_mass_noalloc_fold<<<1, 1, 0, st>>>(part, (int)blocks, out);
+  CU(cudaGetLastError());
+  return 0;
 }
 
 }  // extern "C"

@@ -32,7 +32,7 @@ _lib = None
 # every entry point declared in include/nicam_cuda.h
 EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync",
            "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",
-           "nc_kernel_stats", "nc_grid_spring", "nc_last_error", "nc_destroy")
+           "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_last_error", "nc_destroy")
 
 
 def load_library(path: str = LIB_PATH):
@@ -61,6 +61,8 @@ def load_library(path: str = LIB_PATH):
     lib.nc_profile.argtypes = [vp, i32]
     lib.nc_kernel_stats.argtypes = [vp, i32, ctypes.c_char_p, dp, dp]
     lib.nc_kernel_stats.restype = ctypes.c_int
+    lib.nc_mass_sum_noalloc.argtypes = [dp] * 8 + [i32] * 5 + [dp, vp]
+    lib.nc_mass_sum_noalloc.restype = ctypes.c_int
     lib.nc_grid_spring.argtypes = [i32, i32, dp, dp, dp, dp, dp, i32, dp, dp, i32, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_double, i64, ctypes.POINTER(i64)]
     lib.nc_grid_spring.restype = ctypes.c_int
