@@ -203,6 +203,10 @@ struct nc_handle {
   FieldPair PSa[6], PSb[6], PM[5], vtmp2[3], gT[6], Mc, Mu, Ml, ethtot0, hdiv[3];
   FieldPair flx_v, rhog_t, flx[6], xc[9], ch[6], cm[6], q, gq[3], qa[3], Qmin, Qmax;
   FieldPair vph[8];             // horizontal terms of vp0 (div1, div2, dd, dpg)
+  // the pole columns run on a second stream between the operations that mix
+  // regional and pole data (halo exchanges, tracer density update)
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // per-kernel timing (opt-in, eager launches only): an event after every
   // launch; a kernel's time is the gap to the previous event on the stream
   bool prof = false;
@@ -363,6 +367,26 @@ static int collect_profile(nc_handle* h) {
   return 0;
 }
 
+#define TRY_(x)           \
+  do {                    \
+    int rc_ = (x);        \
+    if (rc_) return rc_;  \
+  } while (0)
+
+static int fork_pl(nc_handle* h) {
+  if (h->prof || !h->stream2) return 0;
+  CU(cudaEventRecord(h->ev_fork, h->stream));
+  CU(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0));
+  return 0;
+}
+static int join_pl(nc_handle* h) {
+  if (h->prof || !h->stream2) return 0;
+  CU(cudaEventRecord(h->ev_join, h->stream2));
+  CU(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+  return 0;
+}
+static cudaStream_t pole_stream(nc_handle* h) { return (h->prof || !h->stream2) ? h->stream : h->stream2; }
+
 static int comm(nc_handle* h, std::initializer_list<FieldPair> fl) {
   CommFields f{};
   f.n = 0;
@@ -373,8 +397,10 @@ static int comm(nc_handle* h, std::initializer_list<FieldPair> fl) {
   }
   long long ne = (long long)(h->nr + h->np) * h->D.KA;
   unsigned g = (unsigned)((ne + 255) / 256);
+  TRY_(join_pl(h));
   k_comm<<<g, 256, 0, h->stream>>>(f, h->r_dst, h->r_src, h->nr, h->p_dst, h->p_src, h->np);
-  return check_launch(h, "comm");
+  TRY_(check_launch(h, "comm"));
+  return fork_pl(h);
 }
 
 static Prog prog_reg(nc_handle* h) {
@@ -391,13 +417,14 @@ static Prog prog_pl(nc_handle* h) {
 // ---------------------------------------------------------------------------
 // one large step (mod_dynamics.py:1725-2741, numpy path)
 // ---------------------------------------------------------------------------
-#define PHASE()                                                     \
-  do {                                                              \
-    if (h->stop_phase > 0 && ++h->phase >= h->stop_phase) return 0; \
+#define PHASE()                                                                   \
+  do {                                                                            \
+    if (h->stop_phase > 0 && ++h->phase >= h->stop_phase) return join_pl(h);      \
   } while (0)
 
 static int run_step(nc_handle* h) {
   cudaStream_t s = h->stream;
+  const cudaStream_t ps = pole_stream(h);
   h->phase = 0;
   const Dims& D = h->D;
   const unsigned gkl = grid_cols_kl(h);
@@ -414,6 +441,7 @@ static int run_step(nc_handle* h) {
     CU(cudaMemcpyAsync(h->P0[v].p, h->P[v].p, D.npl * sizeof(double), cudaMemcpyDeviceToDevice, s));
   }
   if (h->prof) TRY(mark(h, nullptr));
+  TRY(fork_pl(h));
   for (int nl = 0; nl < h->nstage; ++nl) {
     const bool last = (nl == h->nstage - 1);
     // ---- Pre_Post
@@ -430,7 +458,7 @@ static int run_step(nc_handle* h) {
     // regional and pole columns: same kernel, launched with the matching pointers
     k_diag<<<greg, kBlock, 0, s>>>(diag_args(false), 0);
     TRY(check_launch(h, "diag"));
-    k_diag<<<1, 32, 0, s>>>(diag_args(true), 1);
+    k_diag<<<1, 32, 0, ps>>>(diag_args(true), 1);
     TRY(check_launch(h, "diag_pl"));
     PHASE();
     // ---- momentum advection
@@ -444,7 +472,7 @@ static int run_step(nc_handle* h) {
     amp.rg = h->P[0].p; amp.rvx = h->P[1].p; amp.rvy = h->P[2].p; amp.rvz = h->P[3].p; amp.rw = h->P[4].p;
     amp.vvx = h->vv[0].p; amp.vvy = h->vv[1].p; amp.vvz = h->vv[2].p;
     amp.gvx = h->gadv[0].p; amp.gvy = h->gadv[1].p; amp.gvz = h->gadv[2].p; amp.gw = h->gadv[3].p;
-    k_advmom_pl<<<1, 32, 0, s>>>(amp);
+    k_advmom_pl<<<1, 32, 0, ps>>>(amp);
     TRY(check_launch(h, "advmom_pl"));
     PHASE();
     // ---- hyperdiffusion
@@ -457,7 +485,7 @@ static int run_step(nc_handle* h) {
     }
     k_hdiff1<<<greg, kBlock, 0, s>>>(src, o1);
     TRY(check_launch(h, "hdiff1"));
-    k_hdiff1_pl<<<1, plk, 0, s>>>(srcp, o1p);
+    k_hdiff1_pl<<<1, plk, 0, ps>>>(srcp, o1p);
     TRY(check_launch(h, "hdiff1_pl"));
     TRY(comm(h, {h->vt[0], h->vt[1], h->vt[2], h->vt[3], h->vt[4], h->vt[5]}));
     PHASE();
@@ -471,10 +499,11 @@ static int run_step(nc_handle* h) {
       // interior cells; the exchange below fills the halo rows
       const dim3 gt((unsigned)((D.G - 2 + HD_DX - 1) / HD_DX), (unsigned)((D.G - 2 + HD_DY - 1) / HD_DY),
                     (unsigned)D.L);
-      k_hdiff2_t<<<gt, HD_DX * HD_DY, 0, s>>>(vin, h->P[0].r, o2);
+      const dim3 gl2((unsigned)D.KA, gt.x * gt.y, gt.z);
+      k_hdiff2_l<<<gl2, HD_DX * HD_DY, 0, s>>>(vin, h->P[0].r, o2);
       TRY(check_launch(h, "hdiff2"));
     }
-    k_hdiff2_pl<<<1, plk, 0, s>>>(vinp, h->P[0].p, o2p);
+    k_hdiff2_pl<<<1, plk, 0, ps>>>(vinp, h->P[0].p, o2p);
     TRY(check_launch(h, "hdiff2_pl"));
     TRY(comm(h, {h->vt2[0], h->vt2[1], h->vt2[2], h->vt2[3], h->vt2[4], h->vt2[5]}));
     PHASE();
@@ -486,7 +515,7 @@ static int run_step(nc_handle* h) {
       ga.rhog = F(h->P[0]); ga.gvx = F(h->gadv[0]); ga.gvy = F(h->gadv[1]); ga.gvz = F(h->gadv[2]);
       ga.gw = F(h->gadv[3]); ga.frhog = F(h->frhog);
       if (!pole) k_gtend<<<greg, kBlock, 0, s>>>(ga, 0);
-      else k_gtend<<<1, 32, 0, s>>>(ga, 1);
+      else k_gtend<<<1, 32, 0, ps>>>(ga, 1);
       TRY(check_launch(h, pole ? "gtend_pl" : "gtend"));
     }
     PHASE();
@@ -496,7 +525,7 @@ static int run_step(nc_handle* h) {
                                                 h->PSa[3].r, h->PSa[4].r, h->PSa[5].r, h->PM[0].r, h->PM[1].r,
                                                 h->PM[2].r, h->PM[3].r, h->PM[4].r, D.npt, nl == 0);
     TRY(check_launch(h, "split_init"));
-    k_split_init<<<npl_blocks, kBlock, 0, s>>>(h->P0[0].p, h->P0[1].p, h->P0[2].p, h->P0[3].p, h->P0[4].p,
+    k_split_init<<<npl_blocks, kBlock, 0, ps>>>(h->P0[0].p, h->P0[1].p, h->P0[2].p, h->P0[3].p, h->P0[4].p,
                                                 h->P0[5].p, prog_pl(h), h->PSa[0].p, h->PSa[1].p, h->PSa[2].p,
                                                 h->PSa[3].p, h->PSa[4].p, h->PSa[5].p, h->PM[0].p, h->PM[1].p,
                                                 h->PM[2].p, h->PM[3].p, h->PM[4].p, D.npl, nl == 0);
@@ -511,7 +540,7 @@ static int run_step(nc_handle* h) {
       const dim3 gt((unsigned)((D.G - 2 + DD_DX - 1) / DD_DX), (unsigned)((D.G - 2 + DD_DY - 1) / DD_DY), (unsigned)D.L);
       k_dd3d_t<<<gt, DD_DX * DD_DY, 0, s>>>(v, o);
       TRY(check_launch(h, "dd3d"));
-      k_dd3d_pl<<<1, plk, 0, s>>>(vp, op);
+      k_dd3d_pl<<<1, plk, 0, ps>>>(vp, op);
       TRY(check_launch(h, "dd3d_pl"));
       return comm(h, {h->vtmp2[0], h->vtmp2[1], h->vtmp2[2]});
     };
@@ -535,12 +564,13 @@ static int run_step(nc_handle* h) {
         for (int n = 0; n < 8; ++n) vh.out[n] = h->vph[n].r;
         const dim3 gt((unsigned)((D.G - 2 + DD_DX - 1) / DD_DX), (unsigned)((D.G - 2 + DD_DY - 1) / DD_DY),
                       (unsigned)D.L);
-        k_vp0_h<<<gt, DD_DX * DD_DY, 0, s>>>(va, vh);
+        (void)gt;
+        k_vp0_hl<<<lvgrid, DD_DX * DD_DY, 0, s>>>(va, vh);
         TRY(check_launch(h, "vp0_h"));
         k_vp0_c<<<greg, kBlock, 0, s>>>(va, vh);
         TRY(check_launch(h, "vp0_c"));
       } else {
-        k_vp0<<<1, 32, 0, s>>>(va, 1);
+        k_vp0<<<1, 32, 0, ps>>>(va, 1);
         TRY(check_launch(h, "vp0_pl"));
       }
     }
@@ -568,7 +598,7 @@ static int run_step(nc_handle* h) {
           k_path1_l<<<lvgrid, DD_DX * DD_DY, 0, s>>>(pa);
           TRY(check_launch(h, "path1"));
         } else {
-          k_path1<<<1, 32, 0, s>>>(pa, 1);
+          k_path1<<<1, 32, 0, ps>>>(pa, 1);
           TRY(check_launch(h, "path1_pl"));
         }
       }
@@ -587,16 +617,17 @@ static int run_step(nc_handle* h) {
         if (!pole) {
           const dim3 gt((unsigned)((D.G - 2 + DD_DX - 1) / DD_DX), (unsigned)((D.G - 2 + DD_DY - 1) / DD_DY),
                         (unsigned)D.L);
-          k_vimain_a_t<<<gt, DD_DX * DD_DY, 0, s>>>(va);
+          (void)gt;
+          k_vimain_a_l<<<lvgrid, DD_DX * DD_DY, 0, s>>>(va);
           TRY(check_launch(h, "vimain_a"));
           k_vi_solve<<<greg, kBlock, 0, s>>>(va);
           TRY(check_launch(h, "vi_solve"));
           k_vi_energy_p<<<npt_blocks, kBlock, 0, s>>>(va);
           TRY(check_launch(h, "vi_energy"));
         } else {
-          k_vimain_a<<<1, plk, 0, s>>>(va, 1);
+          k_vimain_a<<<1, plk, 0, ps>>>(va, 1);
           TRY(check_launch(h, "vimain_a_pl"));
-          k_vimain_b<<<1, 32, 0, s>>>(va, 1);
+          k_vimain_b<<<1, 32, 0, ps>>>(va, 1);
           TRY(check_launch(h, "vimain_b_pl"));
         }
       }
@@ -606,7 +637,7 @@ static int run_step(nc_handle* h) {
     FieldPair* PSf = (nitr % 2 == 0) ? h->PSa : h->PSb;
     k_post<<<greg, kBlock, 0, s>>>(prog_reg(h), PSf[0].r, PSf[1].r, PSf[2].r, PSf[3].r, PSf[4].r, PSf[5].r, 0);
     TRY(check_launch(h, "post"));
-    k_post<<<1, 32, 0, s>>>(prog_pl(h), PSf[0].p, PSf[1].p, PSf[2].p, PSf[3].p, PSf[4].p, PSf[5].p, 1);
+    k_post<<<1, 32, 0, ps>>>(prog_pl(h), PSf[0].p, PSf[1].p, PSf[2].p, PSf[3].p, PSf[4].p, PSf[5].p, 1);
     TRY(check_launch(h, "post_pl"));
     TRY(comm(h, {h->PM[0], h->PM[1], h->PM[2], h->PM[3], h->PM[4]}));
     PHASE();
@@ -624,7 +655,7 @@ static int run_step(nc_handle* h) {
       ta.rhog_in = F(h->P0[0]); ta.frhog = F(h->frhog); ta.flx_v = F(h->flx_v); ta.rhog_t = F(h->rhog_t);
       ta.dt = dt;
       if (!pole) k_trc_vflux<<<greg, kBlock, 0, s>>>(ta, 0);
-      else k_trc_vflux<<<1, 32, 0, s>>>(ta, 1);
+      else k_trc_vflux<<<1, 32, 0, ps>>>(ta, 1);
       TRY(check_launch(h, pole ? "trc_vflux_pl" : "trc_vflux"));
     }
     auto vadv = [&](int iq, bool second) -> int {
@@ -636,7 +667,7 @@ static int run_step(nc_handle* h) {
         va.flx_v = F(h->flx_v); va.frhog = F(h->frhog);
         va.dt = dt; va.bcoef = 0.0; va.clamp = second ? 1 : 0; va.dtl = dt;
         if (!pole) k_trc_vadv<<<greg, kBlock, 0, s>>>(va, 0);
-        else k_trc_vadv<<<1, 32, 0, s>>>(va, 1);
+        else k_trc_vadv<<<1, 32, 0, ps>>>(va, 1);
         TRY(check_launch(h, pole ? "trc_vadv_pl" : "trc_vadv"));
       }
       return 0;
@@ -656,7 +687,7 @@ static int run_step(nc_handle* h) {
       TrcHfluxPlArgs hp;
       hp.rho = h->PM[0].p; hp.rvx = h->PM[1].p; hp.rvy = h->PM[2].p; hp.rvz = h->PM[3].p; hp.rhog_t = h->rhog_t.p;
       hp.flx = h->flx[0].p; hp.xc = h->xc[0].p; hp.ch = h->ch[0].p; hp.cm = h->cm[0].p; hp.dt = dt;
-      k_trc_hflux_pl<<<1, plk, 0, s>>>(hp);
+      k_trc_hflux_pl<<<1, plk, 0, ps>>>(hp);
       TRY(check_launch(h, "trc_hflux_pl"));
     }
     PHASE();
@@ -664,7 +695,7 @@ static int run_step(nc_handle* h) {
       k_trc_grad<<<greg, kBlock, 0, s>>>(h->Pq[iq].r, h->rhog_t.r, h->q.r,
                                                                                h->gq[0].r, h->gq[1].r, h->gq[2].r);
       TRY(check_launch(h, "trc_grad"));
-      k_trc_grad_pl<<<1, plk, 0, s>>>(h->Pq[iq].p, h->rhog_t.p, h->q.p, h->gq[0].p, h->gq[1].p, h->gq[2].p);
+      k_trc_grad_pl<<<1, plk, 0, ps>>>(h->Pq[iq].p, h->rhog_t.p, h->q.p, h->gq[0].p, h->gq[1].p, h->gq[2].p);
       TRY(check_launch(h, "trc_grad_pl"));
       TRY(comm(h, {h->gq[0], h->gq[1], h->gq[2]}));
       TrcRemapArgs ra;
@@ -677,7 +708,7 @@ static int run_step(nc_handle* h) {
       TrcRemapPlArgs rp;
       rp.q = h->q.p; rp.gq0 = h->gq[0].p; rp.gq1 = h->gq[1].p; rp.gq2 = h->gq[2].p; rp.xc = h->xc[0].p;
       rp.cm = h->cm[0].p; rp.qa = h->qa[0].p;
-      k_trc_remap_pl<<<1, plk, 0, s>>>(rp);
+      k_trc_remap_pl<<<1, plk, 0, ps>>>(rp);
       TRY(check_launch(h, "trc_remap_pl"));
       TrcLimArgs la;
       la.q = h->q.r; la.rhog_t = h->rhog_t.r; la.frhog = h->frhog.r;
@@ -691,18 +722,20 @@ static int run_step(nc_handle* h) {
       lp.qout_min = h->Qmin.p; lp.qout_max = h->Qmax.p; lp.rhogq = h->Pq[iq].p; lp.dt = dt;
       k_trc_qout<<<greg, kBlock, 0, s>>>(la);
       TRY(check_launch(h, "trc_qout"));
-      k_trc_qout_pl<<<1, plk, 0, s>>>(lp);
+      k_trc_qout_pl<<<1, plk, 0, ps>>>(lp);
       TRY(check_launch(h, "trc_qout_pl"));
       TRY(comm(h, {h->Qmin, h->Qmax}));
       k_trc_apply<<<greg, kBlock, 0, s>>>(la);
       TRY(check_launch(h, "trc_apply"));
-      k_trc_apply_pl<<<1, plk, 0, s>>>(lp);
+      k_trc_apply_pl<<<1, plk, 0, ps>>>(lp);
       TRY(check_launch(h, "trc_apply_pl"));
     }
     PHASE();
+    TRY(join_pl(h));
     k_trc_rhog<<<gkl, kBlock, 0, s>>>(h->rhog_t.r, h->flx[0].r, h->flx[1].r, h->flx[2].r, h->flx[3].r, h->flx[4].r,
                                        h->flx[5].r, h->frhog.r, dt, h->flx[0].p, h->rhog_t.p, h->frhog.p);
     TRY(check_launch(h, "trc_rhog"));
+    TRY(fork_pl(h));
     for (int iq = 0; iq < D.nq; ++iq) TRY(vadv(iq, true));
     PHASE();
   }
@@ -714,10 +747,12 @@ static int run_step(nc_handle* h) {
     for (int iq = 0; iq < D.nq && n < NC_MAXCOMM; ++iq) { f.r[n] = h->Pq[iq].r; f.p[n] = h->Pq[iq].p; n++; }
     f.n = n;
     long long ne = (long long)(h->nr + h->np) * D.KA;
+    TRY(join_pl(h));
     k_comm<<<(unsigned)((ne + 255) / 256), 256, 0, s>>>(f, h->r_dst, h->r_src, h->nr, h->p_dst, h->p_src, h->np);
     TRY(check_launch(h, "comm_final"));
     for (int iq = NC_MAXCOMM - 6; iq < D.nq; ++iq) TRY(comm(h, {h->Pq[iq]}));
   }
+  TRY(join_pl(h));
   return 0;
 }
 
@@ -1019,6 +1054,9 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   h->mass_blocks = (int)((D.npt2 + D.LP + 255) / 256);
   TRY(dev_alloc(h, &h->mass_part, (size_t)h->mass_blocks * 2));
   CU(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  CU(cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking));
+  CU(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+  CU(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
   return 0;
 }
 
@@ -1046,6 +1084,10 @@ void nc_destroy(nc_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   for (void* p : h->allocs) cudaFree(p);
+  if (h->stream2) cudaStreamSynchronize(h->stream2);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
+  if (h->stream2) cudaStreamDestroy(h->stream2);
   if (h->stream) cudaStreamDestroy(h->stream);
   if (g_current == h) g_current = nullptr;
   delete h;

@@ -506,6 +506,104 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, 2) k_hdiff2_t(Six vt, const dou
   }
 }
 
+// Second hyperdiffusion pass, one block per (level, tile): same staging,
+// triangle gradients and arithmetic as k_hdiff2_t, without the level loop.
+__global__ void __launch_bounds__(HD_DX * HD_DY, 3) k_hdiff2_l(Six vt, const double* rhog, SixOut out) {
+  constexpr int PX = HD_DX + 2, PY = HD_DY + 2, TX = HD_DX + 1, TY = HD_DY + 1;
+  __shared__ double s_f[6][PY * PX];
+  __shared__ double s_r[PY * PX];
+  __shared__ double s_t[2][6][TY * TX];   // field 4/5: tti x,y,z then ttj x,y,z
+  const int kb = (int)blockIdx.x, l = (int)blockIdx.z;
+  const int ntx = (cD.G - 2 + HD_DX - 1) / HD_DX;
+  const int i0 = 1 + ((int)blockIdx.y % ntx) * HD_DX, j0 = 1 + ((int)blockIdx.y / ntx) * HD_DY;
+  const int G = cD.G, gmax = cD.G - 2;
+  const int tid = threadIdx.x, tx = tid % HD_DX, ty = tid / HD_DX;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool own = (i <= gmax) && (j <= gmax);
+  const double Kh = cC.Kh;
+  const double kfac[2] = {cC.CVdry, cC.hdiff_fact_rho};
+  {
+    const int k = kb;
+    for (int p = tid; p < PX * PY; p += blockDim.x) {
+      const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
+      const bool ok = ii < G && jj < G;
+      const long long q = ok ? ix(ii, jj, k, l) : 0;
+#pragma unroll
+      for (int n = 0; n < 6; ++n) s_f[n][p] = ok ? vt.f[n][q] : 0.0;
+      s_r[p] = ok ? rhog[q] : 0.0;
+    }
+    __syncthreads();
+    for (int p = tid; p < TX * TY; p += blockDim.x) {
+      const int px = p % TX, py = p / TX;
+      const int ii = i0 - 1 + px, jj = j0 - 1 + py;
+      const bool ok = ii <= G - 2 && jj <= G - 2;
+      const int ia = py * PX + px, ib = ia + 1, ic = ia + PX + 1, id = ia + PX;
+#pragma unroll
+      for (int f = 0; f < 2; ++f) {
+        const double* s = s_f[4 + f];
+        const double s0 = s[ia], sip = s[ib], sd = s[ic], sjp = s[id];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          double ti = 0.0, tj = 0.0;
+          if (ok) {
+            const double c1i = P2(cG.coef_intp, (d * 3 + 0) * 2 + 0, ii, jj, l);
+            const double c2i = P2(cG.coef_intp, (d * 3 + 1) * 2 + 0, ii, jj, l);
+            const double c3i = P2(cG.coef_intp, (d * 3 + 2) * 2 + 0, ii, jj, l);
+            const double c1j = P2(cG.coef_intp, (d * 3 + 0) * 2 + 1, ii, jj, l);
+            const double c2j = P2(cG.coef_intp, (d * 3 + 1) * 2 + 1, ii, jj, l);
+            const double c3j = P2(cG.coef_intp, (d * 3 + 2) * 2 + 1, ii, jj, l);
+            ti = ((2.0 * c1i - c2i - c3i) * s0 + (-c1i + 2.0 * c2i - c3i) * sip + (-c1i - c2i + 2.0 * c3i) * sd) / 3.0;
+            tj = ((2.0 * c1j - c2j - c3j) * s0 + (-c1j + 2.0 * c2j - c3j) * sd + (-c1j - c2j + 2.0 * c3j) * sjp) / 3.0;
+          }
+          s_t[f][d][p] = ti;
+          s_t[f][3 + d][p] = tj;
+        }
+      }
+    }
+    __syncthreads();
+    if (i0 == 1 && j0 == 1 && tid < 6) {   // singular-point fix of the (0,0) triangle, fields 4 and 5
+      const int f = tid / 3, d = tid % 3;
+      const double m0 = (double)cG.pntmask[l * 2 + 0], m1 = (double)cG.pntmask[l * 2 + 1];
+      s_t[f][d][0] = s_t[f][d][0] * m0 + s_t[f][3 + d][1] * m1;
+    }
+    __syncthreads();
+    if (own) {
+      const long long q = ix(i, j, k, l);
+      const int c0 = (ty + 1) * PX + (tx + 1);
+      const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        double v = P2(cG.coef_lap, 0, i, j, l) * s_f[n][nb[0]];
+#pragma unroll
+        for (int m = 1; m < 7; ++m) v = v + P2(cG.coef_lap, m, i, j, l) * s_f[n][nb[m]];
+        out.f[n][q] = -v;
+      }
+      const int ta = (ty + 1) * TX + (tx + 1), tb = ta - 1, tc = ta - TX - 1, td = ta - TX;
+#pragma unroll
+      for (int f = 0; f < 2; ++f) {
+        auto kh = [&](int pt) { return s_r[pt] * kfac[f] * Kh; };
+        const double kh0 = kh(nb[0]);
+        const double kf1 = 0.5 * (kh0 + kh(nb[2])), kf2 = 0.5 * (kh0 + kh(nb[3])), kf3 = 0.5 * (kh0 + kh(nb[4]));
+        const double kf4 = 0.5 * (kh0 + kh(nb[5])), kf5 = 0.5 * (kh0 + kh(nb[6])), kf6 = 0.5 * (kh0 + kh(nb[1]));
+        double inner = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double aTI = s_t[f][d][ta], aTJ = s_t[f][3 + d][ta], bTI = s_t[f][d][tb];
+          const double cTI = s_t[f][d][tc], cTJ = s_t[f][3 + d][tc], dTJ = s_t[f][3 + d][td];
+          const double cd0 = P2(cG.coef_diff, d * 6 + 0, i, j, l), cd1 = P2(cG.coef_diff, d * 6 + 1, i, j, l),
+                       cd2 = P2(cG.coef_diff, d * 6 + 2, i, j, l), cd3 = P2(cG.coef_diff, d * 6 + 3, i, j, l),
+                       cd4 = P2(cG.coef_diff, d * 6 + 4, i, j, l), cd5 = P2(cG.coef_diff, d * 6 + 5, i, j, l);
+          const double blk = kf1 * cd0 * (aTI + aTJ) + kf2 * cd1 * (aTJ + bTI) + kf3 * cd2 * (bTI + cTJ) +
+                             kf4 * cd3 * (cTJ + cTI) + kf5 * cd4 * (cTI + dTJ) + kf6 * cd5 * (dTJ + aTI);
+          inner = (d == 0) ? blk : inner + blk;
+        }
+        out.f[4 + f][q] = -inner;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 __global__ void k_hdiff2_pl(Six vt, const double* rhog, SixOut out) {
   int t = threadIdx.x;
   if (t >= cD.KA * cD.LP) return;

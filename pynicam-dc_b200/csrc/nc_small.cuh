@@ -727,6 +727,147 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_vp0_h(Vp0Args a, Vp0H h) {
   }
 }
 
+// vp0 horizontal terms, one block per (level, tile) (body of k_vp0_h).
+__global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_vp0_hl(Vp0Args a, Vp0H h) {
+  constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
+  __shared__ double s_m[3][PY * PX];    // RGAM * rhogv
+  __shared__ double s_e[3][PY * PX];    // RGAM * rhogv * eth
+  __shared__ double s_v[3][PY * PX];    // -vtmp2
+  __shared__ double s_p[PY * PX];       // RGAM * pregd at the gradient level
+  __shared__ double s_ti[TY * TX], s_tj[TY * TX];
+  const TileLv tl = tile_level(cD.kmin);
+  const int l = tl.l, i0 = tl.i0, j0 = tl.j0;
+  const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin, kmax = cD.kmax;
+  const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool own = (i <= gmax) && (j <= gmax);
+  const double ddc = cC.divdamp_coef, r = cC.rscale;
+  const long long n = cD.npt;
+  const double* cz = cG.C2WGz;
+  const double* const* P = a.P.v;
+  double gxyz[3] = {0.0, 0.0, 0.0};
+  long long q0 = 0;
+  if (own) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) gxyz[d] = P2(cG.GRD_x, d, i, j, l);
+    q0 = ix(i, j, 0, l);
+  }
+  {
+    const int k = tl.k;
+    const int kk = (k == kmin) ? kmin + 1 : k;
+    for (int p = tid; p < PX * PY; p += blockDim.x) {
+      const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
+      double mv[3] = {0.0, 0.0, 0.0}, ev[3] = {0.0, 0.0, 0.0}, vv[3] = {0.0, 0.0, 0.0}, pp = 0.0;
+      if (ii < G && jj < G) {
+        const long long q = ix(ii, jj, k, l);
+        const double rg = cG.RGAM[q], e = a.eth[q];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double pv = P[1 + d][q];
+          mv[d] = pv * rg;
+          ev[d] = (pv * e) * rg;
+          vv[d] = -a.vt.f[d][q];
+        }
+        const long long qk = ix(ii, jj, kk, l);
+        pp = a.pregd[qk] * cG.RGAM[qk];
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        s_m[d][p] = mv[d];
+        s_e[d][p] = ev[d];
+        s_v[d][p] = vv[d];
+      }
+      s_p[p] = pp;
+    }
+    __syncthreads();
+    for (int p = tid; p < TX * TY; p += blockDim.x) {
+      const int px = p % TX, py = p / TX;
+      const int ii = i0 - 1 + px, jj = j0 - 1 + py;
+      double sTI = 0.0, sTJ = 0.0;
+      if (ii <= G - 2 && jj <= G - 2) {
+        const int ia = py * PX + px, ib = ia + 1, ic = ia + PX + 1, id = ia + PX;
+        auto C = [&](int dir, int pt, int t) { return P2(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
+        sTI = C(0, 0, 0) * s_v[0][ia] + C(0, 1, 0) * s_v[0][ib] + C(0, 2, 0) * s_v[0][ic] +
+              C(1, 0, 0) * s_v[1][ia] + C(1, 1, 0) * s_v[1][ib] + C(1, 2, 0) * s_v[1][ic] +
+              C(2, 0, 0) * s_v[2][ia] + C(2, 1, 0) * s_v[2][ib] + C(2, 2, 0) * s_v[2][ic];
+        sTJ = C(0, 0, 1) * s_v[0][ia] + C(0, 1, 1) * s_v[0][ic] + C(0, 2, 1) * s_v[0][id] +
+              C(1, 0, 1) * s_v[1][ia] + C(1, 1, 1) * s_v[1][ic] + C(1, 2, 1) * s_v[1][id] +
+              C(2, 0, 1) * s_v[2][ia] + C(2, 1, 1) * s_v[2][ic] + C(2, 2, 1) * s_v[2][id];
+      }
+      s_ti[p] = sTI;
+      s_tj[p] = sTJ;
+    }
+    __syncthreads();
+    if (own) {
+      const int c0 = (ty + 1) * PX + (tx + 1);
+      const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
+      const long long q = q0 + (long long)k * cD.plane;
+      // divergences (div7: per direction left to right, then x + y + z)
+      double acc1[3], acc2[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+        for (int m = 0; m < 7; ++m) {
+          const double cdv = P2(cG.coef_div, d * 7 + m, i, j, l);
+          const double t1 = cdv * s_m[d][nb[m]], t2 = cdv * s_e[d][nb[m]];
+          s1 = (m == 0) ? t1 : s1 + t1;
+          s2 = (m == 0) ? t2 : s2 + t2;
+        }
+        acc1[d] = s1;
+        acc2[d] = s2;
+      }
+      h.out[0][q] = acc1[0] + acc1[1] + acc1[2];
+      h.out[1][q] = acc2[0] + acc2[1] + acc2[2];
+      // 2-D divergence damping, projected
+      const int ta = (ty + 1) * TX + (tx + 1);
+      const double aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
+      const double cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1], dTJ = s_tj[ta - TX];
+      double dd[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        dd[d] = ddc * (P2(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) +
+                       P2(cG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
+                       P2(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) +
+                       P2(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
+                       P2(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) +
+                       P2(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI));
+      {
+        const double prd = (dd[0] * gxyz[0] + dd[1] * gxyz[1] + dd[2] * gxyz[2]) / r;
+        dd[0] = dd[0] - prd * gxyz[0] / r;
+        dd[1] = dd[1] - prd * gxyz[1] / r;
+        dd[2] = dd[2] - prd * gxyz[2] / r;
+      }
+      // pressure gradient of pregd at level kk
+      const long long qkk = q0 + (long long)kk * cD.plane, qk1 = qkk + cD.plane, qkm = qkk - cD.plane;
+      const double P_k1 = a.pregd[qk1], P_k = a.pregd[qkk], P_km = a.pregd[qkm];
+      const double rgh1 = cG.RGAMH[qk1], rgh0 = cG.RGAMH[qkk];
+      double pg[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double g = P2(cG.coef_grad, d * 7 + 0, i, j, l) * s_p[nb[0]];
+#pragma unroll
+        for (int m = 1; m < 7; ++m) g = g + P2(cG.coef_grad, d * 7 + m, i, j, l) * s_p[nb[m]];
+        const double up = (cz[(2 * d) * n + qk1] * P_k1 + cz[(2 * d + 1) * n + qk1] * P_k) * rgh1;
+        const double dn = (cz[(2 * d) * n + qkk] * P_k + cz[(2 * d + 1) * n + qkk] * P_km) * rgh0;
+        pg[d] = g + (up - dn) * cC.rdgz[kk];
+      }
+      {
+        const double prd = (pg[0] * gxyz[0] + pg[1] * gxyz[1] + pg[2] * gxyz[2]) / r;
+        pg[0] = pg[0] - prd * gxyz[0] / r;
+        pg[1] = pg[1] - prd * gxyz[1] / r;
+        pg[2] = pg[2] - prd * gxyz[2] / r;
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        h.out[2 + d][q] = dd[d];
+        h.out[5 + d][q] = pg[d];
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Column part of vp0 for every regional column: vertical flux convergences,
 // small-step tendencies, the implicit matrix and ethtot0, with the horizontal
 // terms read from k_vp0_h (zero on halo columns and outside kmin..kmax, where
@@ -1220,6 +1361,65 @@ __global__ void __launch_bounds__(DD_DX * DD_DY) k_vimain_a_t(VimainArgs a) {
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= gmax) && (j <= gmax);
   for (int k = cD.kmin; k <= cD.kmax; ++k) {
+    for (int p = tid; p < PX * PY; p += blockDim.x) {
+      const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
+      if (ii < G && jj < G) {
+        const long long q = ix(ii, jj, k, l);
+        const double rg = cG.RGAM[q], e = a.eth[q], et = a.ethtot0[q];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double dv = a.dvh.f[d][q];
+          s_h[0][d][p] = dv * rg;
+          s_h[1][d][p] = (dv * e) * rg;
+          s_h[2][d][p] = ((a.P[1 + d][q] + dv) * et) * rg;
+        }
+      } else {
+#pragma unroll
+        for (int f = 0; f < 3; ++f)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) s_h[f][d][p] = 0.0;
+      }
+    }
+    __syncthreads();
+    if (own) {
+      const int c0 = (ty + 1) * PX + (tx + 1);
+      const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
+      const long long q = ix(i, j, k, l);
+      double acc[3][3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double s[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int m = 0; m < 7; ++m) {
+          const double cdv = P2(cG.coef_div, d * 7 + m, i, j, l);
+#pragma unroll
+          for (int f = 0; f < 3; ++f) {
+            const double t = cdv * s_h[f][d][nb[m]];
+            s[f] = (m == 0) ? t : s[f] + t;
+          }
+        }
+#pragma unroll
+        for (int f = 0; f < 3; ++f) acc[f][d] = s[f];
+      }
+#pragma unroll
+      for (int f = 0; f < 3; ++f) a.hdiv[f][q] = acc[f][0] + acc[f][1] + acc[f][2];
+    }
+    __syncthreads();
+  }
+}
+
+// vi_main kernel A, one block per (level, tile) (body of k_vimain_a_t).
+__global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_vimain_a_l(VimainArgs a) {
+  constexpr int PX = DD_DX + 2, PY = DD_DY + 2;
+  __shared__ double s_h[3][3][PY * PX];
+  const TileLv tl = tile_level(cD.kmin);
+  const int l = tl.l, i0 = tl.i0, j0 = tl.j0;
+  const int G = cD.G, gmax = cD.G - 2;
+  const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool own = (i <= gmax) && (j <= gmax);
+  {
+    const int k = tl.k;
     for (int p = tid; p < PX * PY; p += blockDim.x) {
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
       if (ii < G && jj < G) {
