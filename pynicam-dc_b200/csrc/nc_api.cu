@@ -873,6 +873,11 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   D.npt = D.plane * D.KA * D.L;
   D.npt2 = D.plane * D.L;
   D.npl = 6 * D.KA * D.LP;
+  if (D.npt * 6 > 2147483647LL)
+    return fail(NC_ERR_ARG, "grid too large for 32-bit device indexing (6 * lall * kall * gall_1d^2 >= 2^31)");
+  D.planei = (int)D.plane;
+  D.npti = (int)D.npt;
+  D.npt2i = (int)D.npt2;
   Consts& C = h->C;
   TRY(scalar(T, "GRAV", C.GRAV)); TRY(scalar(T, "Rdry", C.Rdry)); TRY(scalar(T, "CVdry", C.CVdry));
   TRY(scalar(T, "CPdry", C.CPdry)); TRY(scalar(T, "Rvap", C.Rvap)); TRY(scalar(T, "OHM", C.OHM));

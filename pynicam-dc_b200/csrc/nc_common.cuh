@@ -34,6 +34,9 @@ struct Dims {
   long long npt;     // L*KA*G*G
   long long npt2;    // L*G*G
   int npl;           // 6*KA*LP
+  // the same sizes as 32-bit ints: device index arithmetic is 32-bit (the
+  // host rejects grids where 6*npt would not fit)
+  int planei, npti, npt2i;
 };
 
 // Physical / run constants (identical names to the reference's CONST_*).
@@ -90,11 +93,13 @@ __constant__ Consts cC;
 __constant__ Geom cG;
 
 // ---- indexing -------------------------------------------------------------
-__device__ __forceinline__ long long ix(int i, int j, int k, int l) {
-  return (((long long)l * cD.KA + k) * cD.G + j) * cD.G + i;
+__device__ __forceinline__ int ix(int i, int j, int k, int l) {
+  return ((l * cD.KA + k) * cD.G + j) * cD.G + i;
 }
-__device__ __forceinline__ long long ix2(int c, int i, int j, int l) {
-  return (((long long)c * cD.L + l) * cD.G + j) * cD.G + i;
+// plane c of a 2-D coefficient array: c * (L*G*G) + cell offset, written so
+// that the cell offset is shared between the planes of one cell
+__device__ __forceinline__ int ix2(int c, int i, int j, int l) {
+  return c * cD.npt2i + ((l * cD.G + j) * cD.G + i);
 }
 // pole (g, k, l)
 __device__ __forceinline__ int ipl(int g, int k, int lp) { return (g * cD.KA + k) * cD.LP + lp; }
@@ -104,7 +109,7 @@ __device__ __forceinline__ int iplc(int g, int k, int lp, int c, int ncomp) {
 }
 // 3-D metric component c of a multi-component regional metric
 __device__ __forceinline__ double M3(const double* a, int c, int i, int j, int k, int l) {
-  return a[(long long)c * cD.npt + ix(i, j, k, l)];
+  return a[c * cD.npti + ix(i, j, k, l)];
 }
 __device__ __forceinline__ double P2(const double* a, int c, int i, int j, int l) { return a[ix2(c, i, j, l)]; }
 
@@ -118,10 +123,10 @@ __device__ __forceinline__ bool interior(int i, int j) {
 }
 
 // Column thread mapping: thread -> (i, j, l).  Returns false for surplus threads.
-__device__ __forceinline__ bool col_of(long long t, int& i, int& j, int& l) {
-  if (t >= cD.npt2) return false;
-  i = (int)(t % cD.G);
-  long long r = t / cD.G;
+__device__ __forceinline__ bool col_of(int t, int& i, int& j, int& l) {
+  if (t >= cD.npt2i) return false;
+  i = t % cD.G;
+  int r = t / cD.G;
   j = (int)(r % cD.G);
   l = (int)(r / cD.G);
   return true;

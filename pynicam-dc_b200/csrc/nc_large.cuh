@@ -26,7 +26,7 @@ __device__ void diag_column(const Col c, const Met m, const DiagArgs& a, double 
   const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
   double** P = const_cast<double**>(a.P.v);
   for (int k = 0; k < KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     double RHOG = P[0][p];
     double rho = RHOG / m.GSGAM2[p];
     a.vx[p] = P[1][p] / RHOG;
@@ -42,13 +42,13 @@ __device__ void diag_column(const Col c, const Met m, const DiagArgs& a, double 
     a.rho[p] = rho;
     a.ein[p] = ein;
     if (k >= kmin + 1 && k <= kmax) {
-      long long pm = c.at(k - 1);
+      int pm = c.at(k - 1);
       a.w[p] = P[4][p] / (mc(m.C2W, c, 0, 2, k) * RHOG + mc(m.C2W, c, 1, 2, k) * P[0][pm]);
     }
   }
   // ---- boundary conditions: TEM top/bottom, FREE top, RIGID bottom
-  const long long pT = c.at(kmax + 1), pK = c.at(kmax), pKm = c.at(kmax - 1);
-  const long long pB = c.at(kmin - 1), pN = c.at(kmin), pNp = c.at(kmin + 1);
+  const int pT = c.at(kmax + 1), pK = c.at(kmax), pKm = c.at(kmax - 1);
+  const int pB = c.at(kmin - 1), pN = c.at(kmin), pNp = c.at(kmin + 1);
   double tem_top = a.tem[pK];
   double tem_btm = a.tem[pN];
   double pre_top = a.pre[pKm] - a.rho[pK] * (m.PHI[pT] - m.PHI[pKm]);
@@ -89,7 +89,7 @@ __device__ void diag_column(const Col c, const Met m, const DiagArgs& a, double 
   a.w[pB] = 0.0;
   // ---- eth, deviations, merged velocity
   for (int k = 0; k < KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     double pre = a.pre[p], rho = a.rho[p];
     a.eth[p] = a.ein[p] + pre / rho;
     a.pregd[p] = (pre - m.pre_bs[p]) * m.GSGAM2[p];
@@ -106,7 +106,7 @@ __device__ void diag_column(const Col c, const Met m, const DiagArgs& a, double 
 }
 
 __global__ void k_diag(DiagArgs a, int pole) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
   if (!pole) {
@@ -138,7 +138,7 @@ __device__ __forceinline__ double advconv_reg(int i, int j, int k, int l, const 
   double div = 0.0;
   if (interior(i, j)) {
     div = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) -> double {
-      long long q = ix(ii, jj, kk, l);
+      int q = ix(ii, jj, kk, l);
       const double* rv = (d == 0) ? rvx : ((d == 1) ? rvy : rvz);
       return (rv[q] * scl(q, kk)) * cG.RGAM[q];
     });
@@ -146,11 +146,11 @@ __device__ __forceinline__ double advconv_reg(int i, int j, int k, int l, const 
   auto vmh = [&](int kk) -> double {
     if (kk <= cD.kmin || kk > cD.kmax) return 0.0;
     double h = vmh_horiz(c, m, kk, [&](int k2, int d) -> double {
-      long long q = c.at(k2);
+      int q = c.at(k2);
       const double* rv = (d == 0) ? rvx : ((d == 1) ? rvy : rvz);
       return rv[q] * scl(q, k2);
     });
-    long long q = c.at(kk);
+    int q = c.at(kk);
     double sw = rw[q] * (cC.afact[kk] * scl(q, kk) + cC.bfact[kk] * scl(c.at(kk - 1), kk - 1));
     return h + 1.0 * sw * m.RGSQRTH[q];
   };
@@ -158,7 +158,7 @@ __device__ __forceinline__ double advconv_reg(int i, int j, int k, int l, const 
 }
 
 __global__ void k_advmom(AdvMomArgs a) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
   const Col c = col_reg(i, j, l);
@@ -168,7 +168,7 @@ __global__ void k_advmom(AdvMomArgs a) {
   const double gx = P2(cG.GRD_x, 0, i, j, l) / r, gy = P2(cG.GRD_x, 1, i, j, l) / r, gz = P2(cG.GRD_x, 2, i, j, l) / r;
   double gwc_prev = 0.0;
   for (int k = 0; k < KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     if (k < kmin || k > kmax) {
       a.gvx[p] = 0.0; a.gvy[p] = 0.0; a.gvz[p] = 0.0; a.gw[p] = 0.0;
       continue;
@@ -179,7 +179,7 @@ __global__ void k_advmom(AdvMomArgs a) {
     for (int s = 0; s < 3; ++s) {
       const double* sc = vv[s];
       dv[s] = advconv_reg(i, j, k, l, c, m, a.rvx, a.rvy, a.rvz, a.rw,
-                          [&](long long q, int) -> double { return sc[q]; });
+                          [&](int q, int) -> double { return sc[q]; });
     }
     double rh = a.rg[p];
     double dvx = dv[0] - (-2.0 * rh * (cC.OHM * a.vvy[p]));
@@ -216,11 +216,11 @@ __device__ double advconv_pl_at(int g, int lp, int k, const Col& c, const Met& m
   auto vmh = [&](int kk) -> double {
     if (kk <= cD.kmin || kk > cD.kmax) return 0.0;
     double h = vmh_horiz(c, m, kk, [&](int k2, int d) -> double {
-      long long q = c.at(k2);
+      int q = c.at(k2);
       const double* rv = (d == 0) ? rvx : ((d == 1) ? rvy : rvz);
       return rv[q] * scl[q];
     });
-    long long q = c.at(kk);
+    int q = c.at(kk);
     double sw = rw[q] * (cC.afact[kk] * scl[q] + cC.bfact[kk] * scl[c.at(kk - 1)]);
     return h + 1.0 * sw * m.RGSQRTH[q];
   };
@@ -239,7 +239,7 @@ __global__ void k_advmom_pl(AdvMomArgs a) {
                gz = X[(g * cD.LP + lp) * 3 + 2] / r;
   double gwc_prev = 0.0;
   for (int k = 0; k < cD.KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     if (k < cD.kmin || k > cD.kmax) {
       a.gvx[p] = 0.0; a.gvy[p] = 0.0; a.gvz[p] = 0.0; a.gw[p] = 0.0;
       continue;
@@ -270,12 +270,12 @@ struct Six { const double* f[6]; };
 struct SixOut { double* f[6]; };
 
 __global__ void k_hdiff1(Six src, SixOut out) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
   const bool in = interior(i, j);
   for (int k = 0; k < cD.KA; ++k) {
-    long long p = ix(i, j, k, l);
+    int p = ix(i, j, k, l);
 #pragma unroll
     for (int n = 0; n < 6; ++n) {
       double v = 0.0;
@@ -283,12 +283,12 @@ __global__ void k_hdiff1(Six src, SixOut out) {
         const double* s = src.f[n];
         if (n == 4) {
           v = lap7(i, j, k, l, [&](int ii, int jj, int kk) {
-            long long q = ix(ii, jj, kk, l);
+            int q = ix(ii, jj, kk, l);
             return s[q] - cG.tem_bs[q];
           });
         } else if (n == 5) {
           v = lap7(i, j, k, l, [&](int ii, int jj, int kk) {
-            long long q = ix(ii, jj, kk, l);
+            int q = ix(ii, jj, kk, l);
             return s[q] - cG.rho_bs[q];
           });
         } else {
@@ -377,13 +377,13 @@ __device__ double diffusion_at(int i, int j, int k, int l, S scl, KH kh) {
 }
 
 __global__ void k_hdiff2(Six vt, const double* rhog, SixOut out) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
   const bool in = interior(i, j);
   const double Kh = cC.Kh;
   for (int k = 0; k < cD.KA; ++k) {
-    long long p = ix(i, j, k, l);
+    int p = ix(i, j, k, l);
     for (int n = 0; n < 6; ++n) {
       double v = 0.0;
       if (in) {
@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, 2) k_hdiff2_t(Six vt, const dou
     for (int p = tid; p < PX * PY; p += blockDim.x) {
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
       const bool ok = ii < G && jj < G;
-      const long long q = ok ? ix(ii, jj, k, l) : 0;
+      const int q = ok ? ix(ii, jj, k, l) : 0;
 #pragma unroll
       for (int n = 0; n < 6; ++n) s_f[n][p] = ok ? vt.f[n][q] : 0.0;
       s_r[p] = ok ? rhog[q] : 0.0;
@@ -470,7 +470,7 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, 2) k_hdiff2_t(Six vt, const dou
     }
     __syncthreads();
     if (own) {
-      const long long q = ix(i, j, k, l);
+      const int q = ix(i, j, k, l);
       const int c0 = (ty + 1) * PX + (tx + 1);
       const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
 #pragma unroll
@@ -527,7 +527,7 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, 3) k_hdiff2_l(Six vt, const dou
     for (int p = tid; p < PX * PY; p += blockDim.x) {
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
       const bool ok = ii < G && jj < G;
-      const long long q = ok ? ix(ii, jj, k, l) : 0;
+      const int q = ok ? ix(ii, jj, k, l) : 0;
 #pragma unroll
       for (int n = 0; n < 6; ++n) s_f[n][p] = ok ? vt.f[n][q] : 0.0;
       s_r[p] = ok ? rhog[q] : 0.0;
@@ -568,7 +568,7 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, 3) k_hdiff2_l(Six vt, const dou
     }
     __syncthreads();
     if (own) {
-      const long long q = ix(i, j, k, l);
+      const int q = ix(i, j, k, l);
       const int c0 = (ty + 1) * PX + (tx + 1);
       const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
 #pragma unroll
@@ -666,7 +666,7 @@ struct GtendArgs {
 __device__ void gtend_column(const Col c, const Met m, const GtendArgs& a, int i, int j, int l, int g, int lp) {
   const double Kh = cC.Kh;
   for (int k = 0; k < cD.KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     double rg = a.rhog[p];
     double rgh = 0.0;
     if (k >= cD.kmin) rgh = mc(m.C2W, c, 0, 2, k) * rg + mc(m.C2W, c, 1, 2, k) * a.rhog[c.at(k - 1)];
@@ -692,7 +692,7 @@ __device__ void gtend_column(const Col c, const Met m, const GtendArgs& a, int i
 }
 
 __global__ void k_gtend(GtendArgs a, int pole) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
   if (!pole) gtend_column(col_reg(i, j, l), met_of(false), a, i, j, l, 0, 0);

@@ -18,21 +18,21 @@ __device__ __forceinline__ double pymax(double a, double b) { return (b > a) ? b
 // Multi-component metrics: regional comp c lives at c*npt + idx, pole comps are
 // interleaved (idx*nc + c).
 struct Col {
-  long long base, ks;
+  int base, ks;
   bool pole;
-  __device__ __forceinline__ long long at(int k) const { return base + (long long)k * ks; }
+  __device__ __forceinline__ int at(int k) const { return base + k * ks; }
 };
 
 __device__ __forceinline__ Col col_reg(int i, int j, int l) {
   Col c;
   c.base = ix(i, j, 0, l);
-  c.ks = cD.plane;
+  c.ks = cD.planei;
   c.pole = false;
   return c;
 }
 __device__ __forceinline__ Col col_pl(int g, int lp) {
   Col c;
-  c.base = (long long)g * cD.KA * cD.LP + lp;
+  c.base = g * cD.KA * cD.LP + lp;
   c.ks = cD.LP;
   c.pole = true;
   return c;
@@ -40,7 +40,7 @@ __device__ __forceinline__ Col col_pl(int g, int lp) {
 
 // Thread -> column for a launch over regional columns (pole == 0) or over the
 // 6*LP pole columns (pole != 0).  The caller passes pointers of the matching kind.
-__device__ __forceinline__ bool map_col(int pole, long long t, int& i, int& j, int& l, int& g, int& lp) {
+__device__ __forceinline__ bool map_col(int pole, int t, int& i, int& j, int& l, int& g, int& lp) {
   if (!pole) {
     g = lp = 0;
     return col_of(t, i, j, l);
@@ -74,7 +74,7 @@ __device__ __forceinline__ Met met_of(bool pole) {
 }
 // component c (of nc) of a multi-component metric at column level k
 __device__ __forceinline__ double mc(const double* a, const Col& c, int comp, int ncomp, int k) {
-  return c.pole ? a[c.at(k) * ncomp + comp] : a[(long long)comp * cD.npt + c.at(k)];
+  return c.pole ? a[c.at(k) * ncomp + comp] : a[comp * cD.npti + c.at(k)];
 }
 
 // ---- horizontal 7-point operators (regional, interior (i,j) only) ---------

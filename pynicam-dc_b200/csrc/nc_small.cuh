@@ -16,8 +16,8 @@ struct CThree { const double* f[3]; };
 // half-level vertical mass flux rhogw_vm at (ii,jj,k) (kernels/oprt3ddivdamp.py:50-82)
 __device__ __forceinline__ double rwv_at(const Four& v, int ii, int jj, int k, int l) {
   if (k <= cD.kmin || k > cD.kmax) return 0.0;
-  long long q = ix(ii, jj, k, l), qm = ix(ii, jj, k - 1, l);
-  const long long n = cD.npt;
+  int q = ix(ii, jj, k, l), qm = ix(ii, jj, k - 1, l);
+  const int n = cD.npti;
   const double* cz = cG.C2WGz;
   double h = cz[q] * v.f[0][q] + cz[n + q] * v.f[0][qm] + cz[2 * n + q] * v.f[1][q] + cz[3 * n + q] * v.f[1][qm] +
              cz[4 * n + q] * v.f[2][q] + cz[5 * n + q] * v.f[2][qm];
@@ -26,9 +26,9 @@ __device__ __forceinline__ double rwv_at(const Four& v, int ii, int jj, int k, i
 
 // sclt_TI / sclt_TJ at vertex (ii,jj) and level k (interior-k only)
 __device__ void sclt3d(const Four& v, int ii, int jj, int k, int l, double& sTI, double& sTJ) {
-  long long a = ix(ii, jj, k, l), b = ix(ii + 1, jj, k, l), c = ix(ii + 1, jj + 1, k, l), d = ix(ii, jj + 1, k, l);
+  int a = ix(ii, jj, k, l), b = ix(ii + 1, jj, k, l), c = ix(ii + 1, jj + 1, k, l), d = ix(ii, jj + 1, k, l);
   double vx[4], vy[4], vz[4];
-  long long pts[4] = {a, b, c, d};
+  int pts[4] = {a, b, c, d};
 #pragma unroll
   for (int n = 0; n < 4; ++n) {
     double rg = cG.RGAM[pts[n]];
@@ -69,12 +69,12 @@ __device__ __forceinline__ double ddivd(int i, int j, int l, int d, const double
 }
 
 __global__ void k_dd3d(Four v, Three out) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
   const bool in = interior(i, j);   // output rows 1..gmax == interior
   for (int k = 0; k < cD.KA; ++k) {
-    long long p = ix(i, j, k, l);
+    int p = ix(i, j, k, l);
     if (!in || k < cD.kmin || k > cD.kmax) {
       out.f[0][p] = 0.0; out.f[1][p] = 0.0; out.f[2][p] = 0.0;
       continue;
@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY) k_dd3d_t(Four v, Three out) {
   const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= gmax) && (j <= gmax);
-  const long long n = cD.npt;
+  const int n = cD.npti;
   const double* cz = cG.C2WGz;
   double cd[3][6];
   if (own) {
@@ -127,14 +127,14 @@ __global__ void __launch_bounds__(DD_DX * DD_DY) k_dd3d_t(Four v, Three out) {
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
       double a = 0.0, b = 0.0, c = 0.0, r = 0.0;
       if (ii < G && jj < G) {
-        const long long q = ix(ii, jj, k, l);
+        const int q = ix(ii, jj, k, l);
         const double f0 = v.f[0][q], f1 = v.f[1][q], f2 = v.f[2][q];
         const double rg = cG.RGAM[q];
         a = f0 * rg;
         b = f1 * rg;
         c = f2 * rg;
         if (up) {
-          const long long qp = q + cD.plane;   // level k+1
+          const int qp = q + cD.planei;   // level k+1
           const double h = cz[qp] * v.f[0][qp] + cz[n + qp] * f0 + cz[2 * n + qp] * v.f[1][qp] +
                            cz[3 * n + qp] * f1 + cz[4 * n + qp] * v.f[2][qp] + cz[5 * n + qp] * f2;
           r = h * cG.RGAMH[qp] + v.f[3][qp] * cG.RGSQRTH[qp];
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY) k_dd3d_t(Four v, Three out) {
       const double bTI = s_ti[ta - 1];            // (i-1, j)
       const double cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1];   // (i-1, j-1)
       const double dTJ = s_tj[ta - TX];           // (i, j-1)
-      const long long q = ix(i, j, k, l);
+      const int q = ix(i, j, k, l);
 #pragma unroll
       for (int d = 0; d < 3; ++d)
         out.f[d][q] = cd[d][0] * (aTI + aTJ) + cd[d][1] * (aTJ + bTI) + cd[d][2] * (bTI + cTJ) +
@@ -218,9 +218,9 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_dd3d_l(Four v, Three out) 
   const int k = tl.k, l = tl.l, i0 = tl.i0, j0 = tl.j0;
   const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin, kmax = cD.kmax;
   const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
-  const long long n = cD.npt;
+  const int n = cD.npti;
   const double* cz = cG.C2WGz;
-  auto rwv = [&](long long q, long long qm) {
+  auto rwv = [&](int q, int qm) {
     const double h = cz[q] * v.f[0][q] + cz[n + q] * v.f[0][qm] + cz[2 * n + q] * v.f[1][q] +
                      cz[3 * n + q] * v.f[1][qm] + cz[4 * n + q] * v.f[2][q] + cz[5 * n + q] * v.f[2][qm];
     return h * cG.RGAMH[q] + v.f[3][q] * cG.RGSQRTH[q];
@@ -229,13 +229,13 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_dd3d_l(Four v, Three out) 
     const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
     double a = 0.0, b = 0.0, c = 0.0, rd = 0.0, ru = 0.0;
     if (ii < G && jj < G) {
-      const long long q = ix(ii, jj, k, l);
+      const int q = ix(ii, jj, k, l);
       const double rg = cG.RGAM[q];
       a = v.f[0][q] * rg;
       b = v.f[1][q] * rg;
       c = v.f[2][q] * rg;
-      if (k > kmin) rd = rwv(q, q - cD.plane);
-      if (k + 1 <= kmax) ru = rwv(q + cD.plane, q);
+      if (k > kmin) rd = rwv(q, q - cD.planei);
+      if (k + 1 <= kmax) ru = rwv(q + cD.planei, q);
     }
     s_vm[0][p] = a;
     s_vm[1][p] = b;
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_dd3d_l(Four v, Three out) 
     const int ta = (ty + 1) * TX + (tx + 1);
     const double aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
     const double cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1], dTJ = s_tj[ta - TX];
-    const long long q = ix(i, j, k, l);
+    const int q = ix(i, j, k, l);
 #pragma unroll
     for (int d = 0; d < 3; ++d)
       out.f[d][q] = P2(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) +
@@ -336,7 +336,7 @@ __device__ void divdamp2d_at(const CThree& vt, int i, int j, int k, int l, doubl
     return;
   }
   auto sc = [&](int ii, int jj, double& sTI, double& sTJ) {
-    long long a = ix(ii, jj, k, l), b = ix(ii + 1, jj, k, l), c = ix(ii + 1, jj + 1, k, l), d = ix(ii, jj + 1, k, l);
+    int a = ix(ii, jj, k, l), b = ix(ii + 1, jj, k, l), c = ix(ii + 1, jj + 1, k, l), d = ix(ii, jj + 1, k, l);
     auto C = [&](int dir, int p, int t) { return P2(cG.coef_intp, (dir * 3 + p) * 2 + t, ii, jj, l); };
     double x0 = -vt.f[0][a], x1 = -vt.f[0][b], x2 = -vt.f[0][c], x3 = -vt.f[0][d];
     double y0 = -vt.f[1][a], y1 = -vt.f[1][b], y2 = -vt.f[1][c], y3 = -vt.f[1][d];
@@ -441,7 +441,7 @@ __device__ void presgrad_pl(int g, int k, int lp, const Col& c, const Met& m, PF
 template <class PF>
 __device__ __forceinline__ double presgradw(const Col& c, const Met& m, int k, PF Pk) {
   if (k < cD.kmin + 1 || k > cD.kmax) return 0.0;
-  long long p = c.at(k), pm = c.at(k - 1);
+  int p = c.at(k), pm = c.at(k - 1);
   return m.GAM2H[p] * (Pk(k) * m.RGSGAM2[p] - Pk(k - 1) * m.RGSGAM2[pm]) * cC.rdgzh[k];
 }
 
@@ -515,17 +515,17 @@ __device__ void vp0_column(const Vp0Args& a, int i, int j, int l, int g, int lp)
   auto PF = [&](int k, int d) -> double { return P[1 + d][c.at(k)]; };
   auto PEF = [&](int k, int d) -> double { return P[1 + d][c.at(k)] * a.eth[c.at(k)]; };
   for (int k = 0; k < KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     // horizontal divergences
     double div1 = 0.0, div2 = 0.0;
     if (!POLE) {
       if (interior(i, j)) {
         div1 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
-          long long q = ix(ii, jj, kk, l);
+          int q = ix(ii, jj, kk, l);
           return P[1 + d][q] * cG.RGAM[q];
         });
         div2 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
-          long long q = ix(ii, jj, kk, l);
+          int q = ix(ii, jj, kk, l);
           return (P[1 + d][q] * a.eth[q]) * cG.RGAM[q];
         });
       }
@@ -535,7 +535,7 @@ __device__ void vp0_column(const Vp0Args& a, int i, int j, int l, int g, int lp)
     }
     double drhog = fluxconv_col(c, m, k, div1, 1.0, PF, [&](int kk) { return P[4][c.at(kk)]; });
     double drhoge = fluxconv_col(c, m, k, div2, 1.0, PEF, [&](int kk) {
-      long long q = c.at(kk);
+      int q = c.at(kk);
       return P[4][q] * (cC.afact[kk] * a.eth[q] + cC.bfact[kk] * a.eth[c.at(kk - 1)]);
     });
     double dd[3], dpg[3];
@@ -560,7 +560,7 @@ __device__ void vp0_column(const Vp0Args& a, int i, int j, int l, int g, int lp)
     if (k >= kmin + 1 && k <= kmax) {
       const double GCVovR = cC.GRAV * cC.CVdry / cC.Rdry;
       const double ACVovRt2 = cC.alpha * cC.CVdry / cC.Rdry / (dt * dt);
-      long long pm = c.at(k - 1), pp = c.at(k + 1);
+      int pm = c.at(k - 1), pp = c.at(k + 1);
       double rg = cC.rdgz[k], rgm = cC.rdgz[k - 1];
       double Ca = (m.RGSGAM2[p] * rg + m.RGSGAM2[pm] * rgm) * m.GAM2H[p];
       double Cb = cC.dfact[k] - cC.cfact[k - 1];
@@ -602,11 +602,11 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_vp0_h(Vp0Args a, Vp0H h) {
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= gmax) && (j <= gmax);
   const double ddc = cC.divdamp_coef, r = cC.rscale;
-  const long long n = cD.npt;
+  const int n = cD.npti;
   const double* cz = cG.C2WGz;
   const double* const* P = a.P.v;
   double gxyz[3] = {0.0, 0.0, 0.0};
-  long long q0 = 0;
+  int q0 = 0;
   if (own) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) gxyz[d] = P2(cG.GRD_x, d, i, j, l);
@@ -618,7 +618,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_vp0_h(Vp0Args a, Vp0H h) {
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
       double mv[3] = {0.0, 0.0, 0.0}, ev[3] = {0.0, 0.0, 0.0}, vv[3] = {0.0, 0.0, 0.0}, pp = 0.0;
       if (ii < G && jj < G) {
-        const long long q = ix(ii, jj, k, l);
+        const int q = ix(ii, jj, k, l);
         const double rg = cG.RGAM[q], e = a.eth[q];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -627,7 +627,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_vp0_h(Vp0Args a, Vp0H h) {
           ev[d] = (pv * e) * rg;
           vv[d] = -a.vt.f[d][q];
         }
-        const long long qk = ix(ii, jj, kk, l);
+        const int qk = ix(ii, jj, kk, l);
         pp = a.pregd[qk] * cG.RGAM[qk];
       }
 #pragma unroll
@@ -660,7 +660,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_vp0_h(Vp0Args a, Vp0H h) {
     if (own) {
       const int c0 = (ty + 1) * PX + (tx + 1);
       const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
-      const long long q = q0 + (long long)k * cD.plane;
+      const int q = q0 + (int)k * cD.planei;
       // divergences (div7: per direction left to right, then x + y + z)
       double acc1[3], acc2[3];
 #pragma unroll
@@ -698,7 +698,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_vp0_h(Vp0Args a, Vp0H h) {
         dd[2] = dd[2] - prd * gxyz[2] / r;
       }
       // pressure gradient of pregd at level kk
-      const long long qkk = q0 + (long long)kk * cD.plane, qk1 = qkk + cD.plane, qkm = qkk - cD.plane;
+      const int qkk = q0 + (int)kk * cD.planei, qk1 = qkk + cD.planei, qkm = qkk - cD.planei;
       const double P_k1 = a.pregd[qk1], P_k = a.pregd[qkk], P_km = a.pregd[qkm];
       const double rgh1 = cG.RGAMH[qk1], rgh0 = cG.RGAMH[qkk];
       double pg[3];
@@ -742,11 +742,11 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_vp0_hl(Vp0Args a, Vp0H h) 
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= gmax) && (j <= gmax);
   const double ddc = cC.divdamp_coef, r = cC.rscale;
-  const long long n = cD.npt;
+  const int n = cD.npti;
   const double* cz = cG.C2WGz;
   const double* const* P = a.P.v;
   double gxyz[3] = {0.0, 0.0, 0.0};
-  long long q0 = 0;
+  int q0 = 0;
   if (own) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) gxyz[d] = P2(cG.GRD_x, d, i, j, l);
@@ -759,7 +759,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_vp0_hl(Vp0Args a, Vp0H h) 
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
       double mv[3] = {0.0, 0.0, 0.0}, ev[3] = {0.0, 0.0, 0.0}, vv[3] = {0.0, 0.0, 0.0}, pp = 0.0;
       if (ii < G && jj < G) {
-        const long long q = ix(ii, jj, k, l);
+        const int q = ix(ii, jj, k, l);
         const double rg = cG.RGAM[q], e = a.eth[q];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -768,7 +768,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_vp0_hl(Vp0Args a, Vp0H h) 
           ev[d] = (pv * e) * rg;
           vv[d] = -a.vt.f[d][q];
         }
-        const long long qk = ix(ii, jj, kk, l);
+        const int qk = ix(ii, jj, kk, l);
         pp = a.pregd[qk] * cG.RGAM[qk];
       }
 #pragma unroll
@@ -801,7 +801,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_vp0_hl(Vp0Args a, Vp0H h) 
     if (own) {
       const int c0 = (ty + 1) * PX + (tx + 1);
       const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
-      const long long q = q0 + (long long)k * cD.plane;
+      const int q = q0 + (int)k * cD.planei;
       // divergences (div7: per direction left to right, then x + y + z)
       double acc1[3], acc2[3];
 #pragma unroll
@@ -839,7 +839,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_vp0_hl(Vp0Args a, Vp0H h) 
         dd[2] = dd[2] - prd * gxyz[2] / r;
       }
       // pressure gradient of pregd at level kk
-      const long long qkk = q0 + (long long)kk * cD.plane, qk1 = qkk + cD.plane, qkm = qkk - cD.plane;
+      const int qkk = q0 + (int)kk * cD.planei, qk1 = qkk + cD.planei, qkm = qkk - cD.planei;
       const double P_k1 = a.pregd[qk1], P_k = a.pregd[qkk], P_km = a.pregd[qkm];
       const double rgh1 = cG.RGAMH[qk1], rgh0 = cG.RGAMH[qkk];
       double pg[3];
@@ -874,7 +874,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_vp0_hl(Vp0Args a, Vp0H h) 
 // the values that depend on them are replaced by the halo exchanges or the
 // boundary rows before they are read).
 __global__ void __launch_bounds__(128) k_vp0_c(Vp0Args a, Vp0H h) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
   const Col c = col_reg(i, j, l);
@@ -901,12 +901,12 @@ __global__ void __launch_bounds__(128) k_vp0_c(Vp0Args a, Vp0H h) {
   auto PF = [&](int k, int d) -> double { return P[1 + d][c.at(k)]; };
   auto PEF = [&](int k, int d) -> double { return P[1 + d][c.at(k)] * a.eth[c.at(k)]; };
   for (int k = 0; k < KA; ++k) {
-    const long long p = c.at(k);
+    const int p = c.at(k);
     const bool hk = in && k >= kmin && k <= kmax;
     const double div1 = hk ? h.out[0][p] : 0.0, div2 = hk ? h.out[1][p] : 0.0;
     const double drhog = fluxconv_col(c, m, k, div1, 1.0, PF, [&](int kk) { return P[4][c.at(kk)]; });
     const double drhoge = fluxconv_col(c, m, k, div2, 1.0, PEF, [&](int kk) {
-      long long q = c.at(kk);
+      int q = c.at(kk);
       return P[4][q] * (cC.afact[kk] * a.eth[q] + cC.bfact[kk] * a.eth[c.at(kk - 1)]);
     });
     double dd[3], dpg[3];
@@ -928,7 +928,7 @@ __global__ void __launch_bounds__(128) k_vp0_c(Vp0Args a, Vp0H h) {
     if (k >= kmin + 1 && k <= kmax) {
       const double GCVovR = cC.GRAV * cC.CVdry / cC.Rdry;
       const double ACVovRt2 = cC.alpha * cC.CVdry / cC.Rdry / (dt * dt);
-      long long pm = c.at(k - 1), pp = c.at(k + 1);
+      int pm = c.at(k - 1), pp = c.at(k + 1);
       double rg = cC.rdgz[k], rgm = cC.rdgz[k - 1];
       double Ca = (m.RGSGAM2[p] * rg + m.RGSGAM2[pm] * rgm) * m.GAM2H[p];
       double Cb = cC.dfact[k] - cC.cfact[k - 1];
@@ -948,7 +948,7 @@ __global__ void __launch_bounds__(128) k_vp0_c(Vp0Args a, Vp0H h) {
 }
 
 __global__ void k_vp0(Vp0Args a, int pole) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
   if (!pole) vp0_column<false>(a, i, j, l, 0, 0);
@@ -975,21 +975,21 @@ __device__ void path1_column(const Path1Args& a, int i, int j, int l, int g, int
   const Met m = met_of(POLE);
   const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
   const double dt = a.dt;
-  auto pregs = [&](long long base_q, int kk) -> double {  // preg_prim_split with clamped boundary rows
+  auto pregs = [&](int base_q, int kk) -> double {  // preg_prim_split with clamped boundary rows
     int k2 = kk < kmin ? kmin : (kk > kmax ? kmax : kk);
-    return a.PS[5][base_q + (long long)k2 * c.ks] * a.RovCV;
+    return a.PS[5][base_q + (int)k2 * c.ks] * a.RovCV;
   };
   double vals[3][2];  // values at kmin and kmax for the boundary rows
   double* const* out = a.dvh;
   for (int k = 0; k < KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     double dd[3], pg[3];
     if (!POLE) {
       divdamp2d_at(a.vt, i, j, k, l, dd);
       presgrad_reg(i, j, k, l, c, m, [&](int ii, int jj, int kk) { return pregs(ix(ii, jj, 0, l), kk); }, pg);
     } else {
       divdamp2d_pl_at(a.vt, g, k, lp, dd);
-      presgrad_pl(g, k, lp, c, m, [&](int gg, int kk) { return pregs((long long)gg * cD.KA * cD.LP + lp, kk); }, pg);
+      presgrad_pl(g, k, lp, c, m, [&](int gg, int kk) { return pregs((int)gg * cD.KA * cD.LP + lp, kk); }, pg);
     }
     for (int d = 0; d < 3; ++d) {
       double drv = a.gT[1 + d][p] - pg[d] + dd[d] + 0.0;
@@ -999,13 +999,13 @@ __device__ void path1_column(const Path1Args& a, int i, int j, int l, int g, int
       if (k == kmax) vals[d][1] = v;
     }
   }
-  const long long pT = c.at(kmax + 1), pK = c.at(kmax), pB = c.at(kmin - 1), pN = c.at(kmin);
+  const int pT = c.at(kmax + 1), pK = c.at(kmax), pB = c.at(kmin - 1), pN = c.at(kmin);
   for (int d = 0; d < 3; ++d) {
     out[d][pT] = 1.0 * (vals[d][1] / a.rhog[pK]) * a.rhog[pT];
     out[d][pB] = -1.0 * (vals[d][0] / a.rhog[pN]) * a.rhog[pB];
   }
   for (int k = 0; k < KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     for (int d = 0; d < 3; ++d) a.PM[1 + d][p] = a.PM[1 + d][p] + out[d][p] * a.rweight;
   }
 }
@@ -1029,10 +1029,10 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_path1_t(Path1Args a) {
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= gmax) && (j <= gmax);
   const double dt = a.dt, RovCV = a.RovCV, rweight = a.rweight, ddc = cC.divdamp_coef, r = cC.rscale;
-  const long long n = cD.npt;
+  const int n = cD.npti;
   const double* cz = cG.C2WGz;
   double cd[3][6], gxyz[3] = {0.0, 0.0, 0.0};
-  long long q0 = 0;
+  int q0 = 0;
   if (own) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -1044,7 +1044,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_path1_t(Path1Args a) {
   }
   auto Pown = [&](int kk) {   // split pressure of the own column, boundary rows clamped
     const int k2 = kk < kmin ? kmin : (kk > kmax ? kmax : kk);
-    return a.PS[5][q0 + (long long)k2 * cD.plane] * RovCV;
+    return a.PS[5][q0 + (int)k2 * cD.planei] * RovCV;
   };
   double vals[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
   for (int k = kmin; k <= kmax; ++k) {
@@ -1053,11 +1053,11 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_path1_t(Path1Args a) {
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
       double x = 0.0, y = 0.0, z = 0.0, pp = 0.0;
       if (ii < G && jj < G) {
-        const long long q = ix(ii, jj, k, l);
+        const int q = ix(ii, jj, k, l);
         x = -a.vt.f[0][q];
         y = -a.vt.f[1][q];
         z = -a.vt.f[2][q];
-        const long long qk = ix(ii, jj, kk, l);
+        const int qk = ix(ii, jj, kk, l);
         pp = a.PS[5][qk] * RovCV * cG.RGAM[qk];
       }
       s_v[0][p] = x;
@@ -1104,7 +1104,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_path1_t(Path1Args a) {
       const double s7[7] = {s_p[c0], s_p[c0 + 1], s_p[c0 + PX + 1], s_p[c0 + PX], s_p[c0 - 1], s_p[c0 - PX - 1],
                             s_p[c0 - PX]};
       double pg[3];
-      const long long qkk = q0 + (long long)kk * cD.plane, qk1 = qkk + cD.plane;
+      const int qkk = q0 + (int)kk * cD.planei, qk1 = qkk + cD.planei;
       const double P_k1 = Pown(kk + 1), P_k = Pown(kk), P_km = Pown(kk - 1);
       const double rgh1 = cG.RGAMH[qk1], rgh0 = cG.RGAMH[qkk];
 #pragma unroll
@@ -1122,7 +1122,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_path1_t(Path1Args a) {
         pg[1] = pg[1] - prd * gxyz[1] / r;
         pg[2] = pg[2] - prd * gxyz[2] / r;
       }
-      const long long q = q0 + (long long)k * cD.plane;
+      const int q = q0 + (int)k * cD.planei;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         const double drv = a.gT[1 + d][q] - pg[d] + dd[d] + 0.0;
@@ -1136,8 +1136,8 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_path1_t(Path1Args a) {
     __syncthreads();
   }
   if (own) {
-    const long long pT = q0 + (long long)(kmax + 1) * cD.plane, pK = q0 + (long long)kmax * cD.plane;
-    const long long pB = q0 + (long long)(kmin - 1) * cD.plane, pN = q0 + (long long)kmin * cD.plane;
+    const int pT = q0 + (int)(kmax + 1) * cD.planei, pK = q0 + (int)kmax * cD.planei;
+    const int pB = q0 + (int)(kmin - 1) * cD.planei, pN = q0 + (int)kmin * cD.planei;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const double vT = 1.0 * (vals[d][1] / a.rhog[pK]) * a.rhog[pT];
@@ -1168,11 +1168,11 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_path1_l(Path1Args a) {
     const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
     double x = 0.0, y = 0.0, z = 0.0, pp = 0.0;
     if (ii < G && jj < G) {
-      const long long q = ix(ii, jj, k, l);
+      const int q = ix(ii, jj, k, l);
       x = -a.vt.f[0][q];
       y = -a.vt.f[1][q];
       z = -a.vt.f[2][q];
-      const long long qk = ix(ii, jj, kk, l);
+      const int qk = ix(ii, jj, kk, l);
       pp = a.PS[5][qk] * RovCV * cG.RGAM[qk];
     }
     s_v[0][p] = x;
@@ -1202,13 +1202,13 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_path1_l(Path1Args a) {
   const int i = i0 + tx, j = j0 + ty;
   if (i > gmax || j > gmax) return;
   const double r = cC.rscale, ddc = cC.divdamp_coef, dt = a.dt, rweight = a.rweight;
-  const long long n = cD.npt;
+  const int n = cD.npti;
   const double* cz = cG.C2WGz;
   const double gx = P2(cG.GRD_x, 0, i, j, l), gy = P2(cG.GRD_x, 1, i, j, l), gz = P2(cG.GRD_x, 2, i, j, l);
-  const long long q0 = ix(i, j, 0, l);
+  const int q0 = ix(i, j, 0, l);
   auto Pown = [&](int k2) {
     const int kc = k2 < kmin ? kmin : (k2 > kmax ? kmax : k2);
-    return a.PS[5][q0 + (long long)kc * cD.plane] * RovCV;
+    return a.PS[5][q0 + (int)kc * cD.planei] * RovCV;
   };
   const int ta = (ty + 1) * TX + (tx + 1);
   const double aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
@@ -1227,7 +1227,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_path1_l(Path1Args a) {
   }
   const int c0 = (ty + 1) * PX + (tx + 1);
   const double s7[7] = {s_p[c0], s_p[c0 + 1], s_p[c0 + PX + 1], s_p[c0 + PX], s_p[c0 - 1], s_p[c0 - PX - 1], s_p[c0 - PX]};
-  const long long qkk = q0 + (long long)kk * cD.plane, qk1 = qkk + cD.plane;
+  const int qkk = q0 + (int)kk * cD.planei, qk1 = qkk + cD.planei;
   const double P_k1 = Pown(kk + 1), P_k = Pown(kk), P_km = Pown(kk - 1);
   const double rgh1 = cG.RGAMH[qk1], rgh0 = cG.RGAMH[qkk];
   double pg[3];
@@ -1246,7 +1246,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_path1_l(Path1Args a) {
     pg[1] = pg[1] - prd * gy / r;
     pg[2] = pg[2] - prd * gz / r;
   }
-  const long long q = q0 + (long long)k * cD.plane;
+  const int q = q0 + (int)k * cD.planei;
   double v[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -1256,7 +1256,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_path1_l(Path1Args a) {
     a.PM[1 + d][q] = a.PM[1 + d][q] + v[d] * rweight;
   }
   if (k == kmin) {
-    const long long pB = q - cD.plane;
+    const int pB = q - cD.planei;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const double vB = -1.0 * (v[d] / a.rhog[q]) * a.rhog[pB];
@@ -1265,7 +1265,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_path1_l(Path1Args a) {
     }
   }
   if (k == kmax) {
-    const long long pT = q + cD.plane;
+    const int pT = q + cD.planei;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const double vT = 1.0 * (v[d] / a.rhog[q]) * a.rhog[pT];
@@ -1276,7 +1276,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_path1_l(Path1Args a) {
 }
 
 __global__ void k_path1(Path1Args a, int pole) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
   if (!pole) path1_column<false>(a, i, j, l, 0, 0);
@@ -1304,32 +1304,32 @@ struct VimainArgs {
 };
 
 __global__ void k_vimain_a(VimainArgs a, int pole) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!pole) {
     if (!col_of(t, i, j, l)) return;
     const bool in = interior(i, j);
     for (int k = 0; k < cD.KA; ++k) {
-      long long p = ix(i, j, k, l);
+      int p = ix(i, j, k, l);
       double h1 = 0.0, h2 = 0.0, h3 = 0.0;
       if (in && k >= cD.kmin && k <= cD.kmax) {
         h1 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
-          long long q = ix(ii, jj, kk, l);
+          int q = ix(ii, jj, kk, l);
           return a.dvh.f[d][q] * cG.RGAM[q];
         });
         h2 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
-          long long q = ix(ii, jj, kk, l);
+          int q = ix(ii, jj, kk, l);
           return (a.dvh.f[d][q] * a.eth[q]) * cG.RGAM[q];
         });
         h3 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
-          long long q = ix(ii, jj, kk, l);
+          int q = ix(ii, jj, kk, l);
           return ((a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q]) * cG.RGAM[q];
         });
       }
       a.hdiv[0][p] = h1; a.hdiv[1][p] = h2; a.hdiv[2][p] = h3;
     }
   } else {
-    long long tp = t;
+    int tp = t;
     if (tp < cD.KA * cD.LP) {
       int k = (int)(tp / cD.LP), lp = (int)(tp % cD.LP);
       for (int g = 0; g < 6; ++g) {
@@ -1364,7 +1364,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY) k_vimain_a_t(VimainArgs a) {
     for (int p = tid; p < PX * PY; p += blockDim.x) {
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
       if (ii < G && jj < G) {
-        const long long q = ix(ii, jj, k, l);
+        const int q = ix(ii, jj, k, l);
         const double rg = cG.RGAM[q], e = a.eth[q], et = a.ethtot0[q];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -1384,7 +1384,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY) k_vimain_a_t(VimainArgs a) {
     if (own) {
       const int c0 = (ty + 1) * PX + (tx + 1);
       const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
-      const long long q = ix(i, j, k, l);
+      const int q = ix(i, j, k, l);
       double acc[3][3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
@@ -1423,7 +1423,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_vimain_a_l(VimainArgs a) {
     for (int p = tid; p < PX * PY; p += blockDim.x) {
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
       if (ii < G && jj < G) {
-        const long long q = ix(ii, jj, k, l);
+        const int q = ix(ii, jj, k, l);
         const double rg = cG.RGAM[q], e = a.eth[q], et = a.ethtot0[q];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -1443,7 +1443,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_vimain_a_l(VimainArgs a) {
     if (own) {
       const int c0 = (ty + 1) * PX + (tx + 1);
       const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
-      const long long q = ix(i, j, k, l);
+      const int q = ix(i, j, k, l);
       double acc[3][3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
@@ -1483,7 +1483,7 @@ __device__ void vimain_column(const VimainArgs& a, const Col c) {
   // grhog1 and gpre on every level
   double grhog1[NC_MAXK], gpre[NC_MAXK];
   for (int k = 0; k < KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     double drhog = fluxconv_col(c, m, k, a.hdiv[0][p], 0.0, DV, [&](int kk) { return PSk(4, kk); });
     double drhoge = fluxconv_col(c, m, k, a.hdiv[1][p], 0.0, DVE, [&](int kk) { return 0.0; });
     grhog1[k] = a.gT[0][p] + drhog;
@@ -1503,7 +1503,7 @@ __device__ void vimain_column(const VimainArgs& a, const Col c) {
   double beta = 0.0;
   for (int n = 0; n < N; ++n) {
     int k = kmin + 1 + n;
-    long long p = c.at(k), pm = c.at(k - 1);
+    int p = c.at(k), pm = c.at(k - 1);
     double rg2 = m.RGAMH[p] * m.RGAMH[p];
     double rgam2 = m.RGAM[p] * m.RGAM[p], rgam2m = m.RGAM[pm] * m.RGAM[pm];
     double Sw = a.gT[4][p] + 0.0 * cC.alpha;
@@ -1541,18 +1541,18 @@ __device__ void vimain_column(const VimainArgs& a, const Col c) {
   // rhog_split1, kinetic energies, total-energy advection, rhoge_split1
   double rs1[NC_MAXK];
   for (int k = 0; k < KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     double drhog2 = fluxconv_col(c, m, k, a.hdiv[0][p], 1.0, DV, [&](int kk) { return rws1[kk]; });
     rs1[k] = PSk(0, k) + (a.gT[0][p] + drhog2) * dt;
   }
   for (int k = 0; k < KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     auto st10 = [&](int kk, int comp) -> double {
-      long long q = c.at(kk);
+      int q = c.at(kk);
       return a.P[comp][q] + PSk(comp, kk);
     };
     auto st11 = [&](int kk, int comp) -> double {
-      long long q = c.at(kk);
+      int q = c.at(kk);
       if (comp == 0) return a.P[0][q] + rs1[kk];
       if (comp == 4) return a.P[4][q] + rws1[kk];
       return a.P[comp][q] + a.dvh.f[comp - 1][q];
@@ -1562,11 +1562,11 @@ __device__ void vimain_column(const VimainArgs& a, const Col c) {
     double drhogetot = fluxconv_col(
         c, m, k, a.hdiv[2][p], 1.0,
         [&](int kk, int d) {
-          long long q = c.at(kk);
+          int q = c.at(kk);
           return (a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q];
         },
         [&](int kk) {
-          long long q = c.at(kk), qm = c.at(kk - 1);
+          int q = c.at(kk), qm = c.at(kk - 1);
           return (a.P[4][q] + rws1[kk]) * (cC.afact[kk] * a.ethtot0[q] + cC.bfact[kk] * a.ethtot0[qm]);
         });
     double re = PSk(5, k) + (a.gT0e[p] + drhogetot) * dt + (kin10 - kin11) + (PSk(0, k) - rs1[k]) * m.PHI[p];
@@ -1584,14 +1584,14 @@ __device__ void vimain_column(const VimainArgs& a, const Col c) {
 // Thomas forward sweep, then the back substitution fused with rhog_split1 on
 // the way down; writes rhog_s1, rhogw_s1 and their running means.
 __global__ void __launch_bounds__(128) k_vi_solve(VimainArgs a) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l) || !interior(i, j)) return;
   const Col c = col_reg(i, j, l);
   const Met m = met_of(false);
   const int kmin = cD.kmin, kmax = cD.kmax, kT = kmax + 1;
   const double dt = a.dt, Rdry = cC.Rdry, CVdry = cC.CVdry, RovCV = a.RovCV;
-  const long long n = cD.npt;
+  const int n = cD.npti;
   const double* cz = cG.C2WGz;
   const double* const* DVp = a.dvh.f;
   auto preg0 = [&](int k) -> double {
@@ -1600,7 +1600,7 @@ __global__ void __launch_bounds__(128) k_vi_solve(VimainArgs a) {
   };
   // horizontal part of the half-level flux of diff_vh (and of diff_vh*eth) at kk
   auto hflux = [&](int kk, bool withe) -> double {
-    const long long q = c.at(kk), qm = c.at(kk - 1);
+    const int q = c.at(kk), qm = c.at(kk - 1);
     const double e = withe ? a.eth[q] : 1.0, em = withe ? a.eth[qm] : 1.0;
     double f0 = DVp[0][q], f0m = DVp[0][qm], f1 = DVp[1][q], f1m = DVp[1][qm], f2 = DVp[2][q], f2m = DVp[2][qm];
     if (withe) {
@@ -1611,7 +1611,7 @@ __global__ void __launch_bounds__(128) k_vi_solve(VimainArgs a) {
     return h * m.RGAMH[q];
   };
   double hD[NC_MAXK];
-  const long long pT = c.at(kT), pK = c.at(kmax);
+  const int pT = c.at(kT), pK = c.at(kmax);
   const double rw_top = -(cz[pT] * DVp[0][pT] + cz[n + pT] * DVp[0][pK] + cz[2 * n + pT] * DVp[1][pT] +
                           cz[3 * n + pT] * DVp[1][pK] + cz[4 * n + pT] * DVp[2][pT] + cz[5 * n + pT] * DVp[2][pK]);
   const double CVovRt2 = CVdry / Rdry / (dt * dt);
@@ -1621,7 +1621,7 @@ __global__ void __launch_bounds__(128) k_vi_solve(VimainArgs a) {
   double u[NC_MAXK], gam[NC_MAXK];
   double vD_lo = 0.0, vE_lo = 0.0, g1_prev = 0.0, gp_prev = 0.0, beta = 0.0;
   for (int k = kmin; k <= kmax; ++k) {
-    const long long p = c.at(k);
+    const int p = c.at(k);
     const int kk = k + 1;
     double vD_hi = 0.0, vE_hi = 0.0;
     if (kk <= kmax) {
@@ -1637,7 +1637,7 @@ __global__ void __launch_bounds__(128) k_vi_solve(VimainArgs a) {
     const double gp = (a.gT[5][p] + drhoge) * Rdry / CVdry;
     if (k >= kmin + 1) {
       const int nn = k - kmin - 1;
-      const long long pm = c.at(k - 1);
+      const int pm = c.at(k - 1);
       const double rg2 = m.RGAMH[p] * m.RGAMH[p];
       const double rgam2 = m.RGAM[p] * m.RGAM[p], rgam2m = m.RGAM[pm] * m.RGAM[pm];
       const double Sw = a.gT[4][p] + 0.0 * cC.alpha;
@@ -1668,7 +1668,7 @@ __global__ void __launch_bounds__(128) k_vi_solve(VimainArgs a) {
   // back substitution (downward) fused with rhog_split1
   double x = 0.0, rws_hi = 0.0, v2_hi = 0.0;
   for (int k = kT; k >= 0; --k) {
-    const long long p = c.at(k);
+    const int p = c.at(k);
     double rws;
     if (k == kT) {
       rws = rw_kmaxp1 * m.GSGAM2H[p];
@@ -1698,7 +1698,7 @@ __global__ void __launch_bounds__(128) k_vi_solve(VimainArgs a) {
 // k_vi_energy: kinetic energies, total-energy advection and rhoge_split1 from
 // the rhog_s1 / rhogw_s1 written by k_vi_solve.
 __global__ void __launch_bounds__(128) k_vi_energy(VimainArgs a) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l) || !interior(i, j)) return;
   const Col c = col_reg(i, j, l);
@@ -1712,10 +1712,10 @@ __global__ void __launch_bounds__(128) k_vi_energy(VimainArgs a) {
     return a.PS[comp][c.at(k)];
   };
   for (int k = 0; k < KA; ++k) {
-    const long long p = c.at(k);
+    const int p = c.at(k);
     auto st10 = [&](int kk, int comp) -> double { return a.P[comp][c.at(kk)] + PSk(comp, kk); };
     auto st11 = [&](int kk, int comp) -> double {
-      const long long q = c.at(kk);
+      const int q = c.at(kk);
       if (comp == 0) return a.P[0][q] + rs1[q];
       if (comp == 4) return a.P[4][q] + rws1[q];
       return a.P[comp][q] + a.dvh.f[comp - 1][q];
@@ -1725,11 +1725,11 @@ __global__ void __launch_bounds__(128) k_vi_energy(VimainArgs a) {
     const double drhogetot = fluxconv_col(
         c, m, k, a.hdiv[2][p], 1.0,
         [&](int kk, int d) {
-          const long long q = c.at(kk);
+          const int q = c.at(kk);
           return (a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q];
         },
         [&](int kk) {
-          const long long q = c.at(kk), qm = c.at(kk - 1);
+          const int q = c.at(kk), qm = c.at(kk - 1);
           return (a.P[4][q] + rws1[q]) * (cC.afact[kk] * a.ethtot0[q] + cC.bfact[kk] * a.ethtot0[qm]);
         });
     a.dwe[2][p] = PSk(5, k) + (a.gT0e[p] + drhogetot) * dt + (kin10 - kin11) + (PSk(0, k) - rs1[p]) * m.PHI[p];
@@ -1739,11 +1739,11 @@ __global__ void __launch_bounds__(128) k_vi_energy(VimainArgs a) {
 // k_vi_energy with one thread per interior grid point (the energy update has
 // no vertical recurrence; neighbouring levels are read through the cache).
 __global__ void __launch_bounds__(128) k_vi_energy_p(VimainArgs a) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= cD.npt) return;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= cD.npti) return;
   const int G = cD.G, KA = cD.KA;
-  const int i = (int)(t % G), j = (int)((t / G) % G), k = (int)((t / ((long long)G * G)) % KA);
-  const int l = (int)(t / ((long long)G * G * KA));
+  const int i = (int)(t % G), j = (int)((t / G) % G), k = (int)((t / ((int)G * G)) % KA);
+  const int l = (int)(t / ((int)G * G * KA));
   if (!interior(i, j)) return;
   const Col c = col_reg(i, j, l);
   const Met m = met_of(false);
@@ -1754,10 +1754,10 @@ __global__ void __launch_bounds__(128) k_vi_energy_p(VimainArgs a) {
     if (comp == 5) kk = kk < kmin ? kmin : (kk > kmax ? kmax : kk);
     return a.PS[comp][c.at(kk)];
   };
-  const long long p = c.at(k);
+  const int p = c.at(k);
   auto st10 = [&](int kk, int comp) -> double { return a.P[comp][c.at(kk)] + PSk(comp, kk); };
   auto st11 = [&](int kk, int comp) -> double {
-    const long long q = c.at(kk);
+    const int q = c.at(kk);
     if (comp == 0) return a.P[0][q] + rs1[q];
     if (comp == 4) return a.P[4][q] + rws1[q];
     return a.P[comp][q] + a.dvh.f[comp - 1][q];
@@ -1767,18 +1767,18 @@ __global__ void __launch_bounds__(128) k_vi_energy_p(VimainArgs a) {
   const double drhogetot = fluxconv_col(
       c, m, k, a.hdiv[2][p], 1.0,
       [&](int kk, int d) {
-        const long long q = c.at(kk);
+        const int q = c.at(kk);
         return (a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q];
       },
       [&](int kk) {
-        const long long q = c.at(kk), qm = c.at(kk - 1);
+        const int q = c.at(kk), qm = c.at(kk - 1);
         return (a.P[4][q] + rws1[q]) * (cC.afact[kk] * a.ethtot0[q] + cC.bfact[kk] * a.ethtot0[qm]);
       });
   a.dwe[2][p] = PSk(5, k) + (a.gT0e[p] + drhogetot) * a.dt + (kin10 - kin11) + (PSk(0, k) - rs1[p]) * m.PHI[p];
 }
 
 __global__ void k_vimain_b(VimainArgs a, int pole) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
   if (!pole) vimain_column<false>(a, col_reg(i, j, l));
@@ -1792,8 +1792,8 @@ __global__ void k_vimain_b(VimainArgs a, int pole) {
 __global__ void k_split_init(const double* P0a, const double* P0b, const double* P0c, const double* P0d,
                              const double* P0e, const double* P0f, Prog P, double* PS0, double* PS1, double* PS2,
                              double* PS3, double* PS4, double* PS5, double* PM0, double* PM1, double* PM2,
-                             double* PM3, double* PM4, long long n, int first) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+                             double* PM3, double* PM4, int n, int first) {
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const double* P0[6] = {P0a, P0b, P0c, P0d, P0e, P0f};
   double* PS[6] = {PS0, PS1, PS2, PS3, PS4, PS5};
@@ -1805,14 +1805,14 @@ __global__ void k_split_init(const double* P0a, const double* P0b, const double*
 // PROG += PROG_split, then horizontalize the momentum (mod_vi.py:1572-1583)
 __global__ void k_post(Prog P, const double* PS0, const double* PS1, const double* PS2, const double* PS3,
                        const double* PS4, const double* PS5, int pole) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   const double* PS[6] = {PS0, PS1, PS2, PS3, PS4, PS5};
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
   const Col c = pole ? col_pl(g, lp) : col_reg(i, j, l);
   const bool in = !pole && interior(i, j);
   for (int k = 0; k < cD.KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     double v[6];
     for (int n = 0; n < 6; ++n) v[n] = P.v[n][p] + PS[n][p];
     if (pole) horiz_pl(g, lp, v[1], v[2], v[3]);

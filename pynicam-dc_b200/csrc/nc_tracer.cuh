@@ -21,10 +21,10 @@ struct TrcFluxArgs {
 __device__ void trc_vflux_column(const Col c, const Met m, const TrcFluxArgs& a) {
   const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
   for (int k = 0; k < KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     double f = 0.0;
     if (k >= kmin + 1 && k <= kmax) {
-      long long pm = c.at(k - 1);
+      int pm = c.at(k - 1);
       double horiz = (mc(m.C2WGz, c, 0, 6, k) * a.rvx[p] + mc(m.C2WGz, c, 1, 6, k) * a.rvx[pm] +
                       mc(m.C2WGz, c, 2, 6, k) * a.rvy[p] + mc(m.C2WGz, c, 3, 6, k) * a.rvy[pm] +
                       mc(m.C2WGz, c, 4, 6, k) * a.rvz[p] + mc(m.C2WGz, c, 5, 6, k) * a.rvz[pm]) * m.RGAMH[p];
@@ -34,7 +34,7 @@ __device__ void trc_vflux_column(const Col c, const Met m, const TrcFluxArgs& a)
     a.flx_v[p] = f;
   }
   for (int k = 0; k < KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     double r = 0.0;
     if (k >= kmin && k <= kmax) {
       r = a.rhog_in[p] - (a.flx_v[c.at(k + 1)] - a.flx_v[p]) * cC.rdgz[k] + 0.0 * a.frhog[p] * a.dt;
@@ -48,7 +48,7 @@ __device__ void trc_vflux_column(const Col c, const Met m, const TrcFluxArgs& a)
 }
 
 __global__ void k_trc_vflux(TrcFluxArgs a, int pole) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
   if (!pole) trc_vflux_column(col_reg(i, j, l), met_of(false), a);
@@ -72,14 +72,14 @@ __device__ void trc_vadv_column(const Col c, const TrcVadvArgs& a) {
   const double BIG = cC.HUGE_, EPS = cC.EPS;
   double q[NC_MAXK], qh[NC_MAXK], ck0[NC_MAXK], ck1[NC_MAXK];
   for (int k = 0; k < KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     q[k] = a.rhogq[p] / a.den[p];
   }
   for (int k = 0; k < KA; ++k) {
     if (k >= kmin && k <= kmax + 1) qh[k] = cC.afact[k] * q[k] + cC.bfact[k] * q[k - 1];
     else qh[k] = 0.0;
     if (k >= kmin && k <= kmax) {
-      long long p = c.at(k);
+      int p = c.at(k);
       ck0[k] = -a.flx_v[p] / a.den[p] * cC.rdgz[k];
       ck1[k] = a.flx_v[c.at(k + 1)] / a.den[p] * cC.rdgz[k];
     } else {
@@ -89,7 +89,7 @@ __device__ void trc_vadv_column(const Col c, const TrcVadvArgs& a) {
   }
   double qmin_prev = 0.0, qmax_prev = 0.0;
   for (int k = kmin; k <= kmax; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     double inL = 0.5 - copysign(0.5, ck0[k]);
     double inU = 0.5 + copysign(0.5, ck0[k + 1]);
     double qc = q[k], qb = q[k - 1], qa = q[k + 1];
@@ -118,7 +118,7 @@ __device__ void trc_vadv_column(const Col c, const TrcVadvArgs& a) {
   qh[kmin] = 0.0;
   qh[kmax + 1] = 0.0;
   for (int k = 0; k < KA; ++k) {
-    long long p = c.at(k);
+    int p = c.at(k);
     double x;
     if (k >= kmin && k <= kmax) {
       x = a.rhogq[p] - (a.flx_v[c.at(k + 1)] * qh[k + 1] - a.flx_v[p] * qh[k]) * cC.rdgz[k];
@@ -132,7 +132,7 @@ __device__ void trc_vadv_column(const Col c, const TrcVadvArgs& a) {
 }
 
 __global__ void k_trc_vadv(TrcVadvArgs a, int pole) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
   if (!pole) trc_vadv_column(col_reg(i, j, l), a);
@@ -157,10 +157,10 @@ struct TrcHfluxArgs {
 // rho/rho*v at the two triangle vertices of cell (ii,jj): TI and TJ (4 fields),
 // before the singular-point fix
 __device__ void trc_vertex_raw(const TrcHfluxArgs& a, int ii, int jj, int k, int l, double TI[4], double TJ[4]) {
-  long long q0 = ix(ii, jj, k, l), qi = ix(ii + 1, jj, k, l), qd = ix(ii + 1, jj + 1, k, l), qj = ix(ii, jj + 1, k, l);
+  int q0 = ix(ii, jj, k, l), qi = ix(ii + 1, jj, k, l), qd = ix(ii + 1, jj + 1, k, l), qj = ix(ii, jj + 1, k, l);
   double w1i = P2(cG.GMTR_t, 0, ii, jj, l), w2i = P2(cG.GMTR_t, 1, ii, jj, l), w3i = P2(cG.GMTR_t, 2, ii, jj, l);
   double w1j = P2(cG.GMTR_t, 3, ii, jj, l), w2j = P2(cG.GMTR_t, 4, ii, jj, l), w3j = P2(cG.GMTR_t, 5, ii, jj, l);
-  auto F = [&](int n, long long q) -> double {
+  auto F = [&](int n, int q) -> double {
     if (n == 0) return a.rho[q];
     const double* r = (n == 1) ? a.rvx : ((n == 2) ? a.rvy : a.rvz);
     return r[q] * cG.RGAM[q];
@@ -224,13 +224,13 @@ __device__ bool trc_face_flux(const TrcHfluxArgs& a, int ii, int jj, int k, int 
 }
 
 __global__ void k_trc_hflux(TrcHfluxArgs a) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
   const double dt = a.dt;
   const double PR = P2(cG.GMTR_p, 0, i, j, l);
   for (int k = 0; k < cD.KA; ++k) {
-    long long p = ix(i, j, k, l);
+    int p = ix(i, j, k, l);
     double fl[6];
     double xc[3];
     for (int f = 0; f < 3; ++f) {
@@ -311,15 +311,15 @@ __global__ void k_trc_hflux_pl(TrcHfluxPlArgs a) {
 // ---------------------------------------------------------------------------
 __global__ void k_trc_grad(const double* rhogq, const double* rhog_t, double* q, double* gq0, double* gq1,
                            double* gq2) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (col_of(t, i, j, l)) {
     const bool in = interior(i, j);
     for (int k = 0; k < cD.KA; ++k) {
-      long long p = ix(i, j, k, l);
+      int p = ix(i, j, k, l);
       q[p] = rhogq[p] / rhog_t[p];
       double g[3] = {0.0, 0.0, 0.0};
-      if (in) grad7(i, j, k, l, [&](int ii, int jj, int kk) { long long qq = ix(ii, jj, kk, l); return rhogq[qq] / rhog_t[qq]; }, g);
+      if (in) grad7(i, j, k, l, [&](int ii, int jj, int kk) { int qq = ix(ii, jj, kk, l); return rhogq[qq] / rhog_t[qq]; }, g);
       gq0[p] = g[0]; gq1[p] = g[1]; gq2[p] = g[2];
     }
   }
@@ -358,8 +358,8 @@ struct TrcRemapArgs {
   double* qa[3];
 };
 
-__device__ __forceinline__ double trc_rec(const TrcRemapArgs& a, int ii, int jj, int k, int l, long long pxc, int f) {
-  long long q = ix(ii, jj, k, l);
+__device__ __forceinline__ double trc_rec(const TrcRemapArgs& a, int ii, int jj, int k, int l, int pxc, int f) {
+  int q = ix(ii, jj, k, l);
   double r = a.q[q];
   r = r + a.gq0[q] * (a.xc[f * 3 + 0][pxc] - P2(cG.GRD_x, 0, ii, jj, l));
   r = r + a.gq1[q] * (a.xc[f * 3 + 1][pxc] - P2(cG.GRD_x, 1, ii, jj, l));
@@ -368,13 +368,13 @@ __device__ __forceinline__ double trc_rec(const TrcRemapArgs& a, int ii, int jj,
 }
 
 __global__ void k_trc_remap(TrcRemapArgs a) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
   const int G = cD.G;
   const bool ok = (i <= G - 2 && j <= G - 2);
   for (int k = 0; k < cD.KA; ++k) {
-    long long p = ix(i, j, k, l);
+    int p = ix(i, j, k, l);
     if (!ok) {
       a.qa[0][p] = 0.0; a.qa[1][p] = 0.0; a.qa[2][p] = 0.0;
       continue;
@@ -486,13 +486,13 @@ __device__ void trc_qin(const TrcLimArgs& a, int i, int j, int k, int l, int m, 
 }
 
 __global__ void k_trc_qout(TrcLimArgs a) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
   const bool in = interior(i, j);
   const double EPS = cC.EPS;
   for (int k = 0; k < cD.KA; ++k) {
-    long long p = ix(i, j, k, l);
+    int p = ix(i, j, k, l);
     double qc = a.q[p];
     if (!in) {
       a.Qmin[p] = qc;
@@ -525,7 +525,7 @@ __global__ void k_trc_qout(TrcLimArgs a) {
 __device__ double trc_limited_face(const TrcLimArgs& a, int ai, int bj, int k, int l, int f) {
   const int mi[3] = {1, 1, 0}, mj[3] = {0, 1, 1};
   int ni = ai + mi[f], nj = bj + mj[f];
-  long long p = ix(ai, bj, k, l), pn = ix(ni, nj, k, l);
+  int p = ix(ai, bj, k, l), pn = ix(ni, nj, k, l);
   double c = a.cm[f][p];
   double qa = a.qa[f][p];
   double qi0, qx0, qi1, qx1;
@@ -537,12 +537,12 @@ __device__ double trc_limited_face(const TrcLimArgs& a, int ai, int bj, int k, i
 }
 
 __global__ void k_trc_apply(TrcLimArgs a) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
   if (!interior(i, j)) return;
   for (int k = 0; k < cD.KA; ++k) {
-    long long p = ix(i, j, k, l);
+    int p = ix(i, j, k, l);
     double q0 = trc_limited_face(a, i, j, k, l, 0);
     double q1 = trc_limited_face(a, i, j, k, l, 1);
     double q2 = trc_limited_face(a, i, j, k, l, 2);
@@ -635,17 +635,17 @@ __global__ void k_trc_apply_pl(TrcLimPlArgs a) {
 __global__ void k_trc_rhog(double* rhog_t, const double* f0, const double* f1, const double* f2, const double* f3,
                            const double* f4, const double* f5, const double* frhog, double dt, const double* flx_pl,
                            double* rhog_t_pl, const double* frhog_pl) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (col_of(t, i, j, l)) {
     if (!interior(i, j)) return;
     for (int k = 0; k < cD.KA; ++k) {
-      long long p = ix(i, j, k, l);
+      int p = ix(i, j, k, l);
       double s = f0[p] + f1[p] + f2[p] + f3[p] + f4[p] + f5[p];
       rhog_t[p] = rhog_t[p] - (s - (1.0 * frhog[p] * dt));
     }
   } else {
-    long long tp = t - cD.npt2;
+    int tp = t - cD.npt2i;
     if (tp < cD.KA * cD.LP) {
       int k = (int)(tp / cD.LP), lp = (int)(tp % cD.LP);
       int p0 = ipl(0, k, lp);
