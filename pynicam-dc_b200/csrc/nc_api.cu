@@ -466,7 +466,11 @@ static int run_step(nc_handle* h) {
     am.rg = h->P[0].r; am.rvx = h->P[1].r; am.rvy = h->P[2].r; am.rvz = h->P[3].r; am.rw = h->P[4].r;
     am.vvx = h->vv[0].r; am.vvy = h->vv[1].r; am.vvz = h->vv[2].r;
     am.gvx = h->gadv[0].r; am.gvy = h->gadv[1].r; am.gvz = h->gadv[2].r; am.gw = h->gadv[3].r;
-    k_advmom<<<greg, kBlock, 0, s>>>(am);
+    {
+      // interior cells, levels kmin..kmax (see k_advmom_t)
+      const dim3 gt((unsigned)(((D.G - 2 + 31) / 32) * ((D.G - 2 + 7) / 8)), 1, (unsigned)D.L);
+      k_advmom_t<<<gt, 256, 0, s>>>(am);
+    }
     TRY(check_launch(h, "advmom"));
     AdvMomArgs amp;
     amp.rg = h->P[0].p; amp.rvx = h->P[1].p; amp.rvy = h->P[2].p; amp.rvz = h->P[3].p; amp.rw = h->P[4].p;

@@ -157,6 +157,104 @@ __device__ __forceinline__ double advconv_reg(int i, int j, int k, int l, const 
   return -div - (vmh(k + 1) - vmh(k)) * cC.rdgz[k];
 }
 
+// Tiled momentum advection for interior cells: one block per 32x8 tile of a
+// region, marching upward over kmin..kmax (the vertical-momentum tendency at k
+// needs the projection at k-1, and the half-level flux at k is reused from the
+// level below).  Per level the haloed tile of rhogv, the merged velocity and
+// RGAM is staged in shared memory for the three 7-point divergences.  Halo
+// cells and boundary levels are not written (their values are never read:
+// the large-step tendencies derived from them are replaced by the exchanges).
+// Arithmetic and association order are those of k_advmom.
+__global__ void __launch_bounds__(256, 2) k_advmom_t(AdvMomArgs a) {
+  constexpr int TXD = 32, TYD = 8;
+  constexpr int PX = TXD + 2, PY = TYD + 2;
+  __shared__ double s_rv[3][PY * PX], s_vv[3][PY * PX], s_rg[PY * PX];
+  const int ntx = (cD.G - 2 + TXD - 1) / TXD;
+  const int l = (int)blockIdx.z;
+  const int i0 = 1 + ((int)blockIdx.x % ntx) * TXD, j0 = 1 + ((int)blockIdx.x / ntx) * TYD;
+  const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin, kmax = cD.kmax;
+  const int tid = threadIdx.x, tx = tid % TXD, ty = tid / TXD;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool own = (i <= gmax) && (j <= gmax);
+  const double r = cC.rscale;
+  const double* rv[3] = {a.rvx, a.rvy, a.rvz};
+  const double* vv[3] = {a.vvx, a.vvy, a.vvz};
+  const double* cz = cG.C2WGz;
+  const int n = cD.npti;
+  double gx = 0.0, gy = 0.0, gz = 0.0;
+  int q0 = 0;
+  if (own) {
+    gx = P2(cG.GRD_x, 0, i, j, l) / r;
+    gy = P2(cG.GRD_x, 1, i, j, l) / r;
+    gz = P2(cG.GRD_x, 2, i, j, l) / r;
+    q0 = ix(i, j, 0, l);
+  }
+  double vmh_lo[3] = {0.0, 0.0, 0.0};
+  double gwc_prev = 0.0;
+  for (int k = kmin; k <= kmax; ++k) {
+    for (int p = tid; p < PX * PY; p += blockDim.x) {
+      const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
+      const bool ok = ii < G && jj < G;
+      const int q = ok ? ix(ii, jj, k, l) : 0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        s_rv[d][p] = ok ? rv[d][q] : 0.0;
+        s_vv[d][p] = ok ? vv[d][q] : 0.0;
+      }
+      s_rg[p] = ok ? cG.RGAM[q] : 0.0;
+    }
+    __syncthreads();
+    if (own) {
+      const int c0 = (ty + 1) * PX + (tx + 1);
+      const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
+      const int p = q0 + k * cD.planei;
+      const int kk = k + 1;
+      const bool hv = (kk > kmin && kk <= kmax);
+      const int qh = p + cD.planei;   // level k+1 of the own column
+      double dv[3];
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        double acc[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          double sm = 0.0;
+#pragma unroll
+          for (int m = 0; m < 7; ++m) {
+            const double v = (s_rv[d][nb[m]] * s_vv[s][nb[m]]) * s_rg[nb[m]];
+            const double t = P2(cG.coef_div, d * 7 + m, i, j, l) * v;
+            sm = (m == 0) ? t : sm + t;
+          }
+          acc[d] = sm;
+        }
+        const double div = acc[0] + acc[1] + acc[2];
+        double vmh_hi = 0.0;
+        if (hv) {
+          const double sh = vv[s][qh], sl = s_vv[s][c0];
+          const double h = cz[qh] * (rv[0][qh] * sh) + cz[n + qh] * (s_rv[0][c0] * sl) +
+                           cz[2 * n + qh] * (rv[1][qh] * sh) + cz[3 * n + qh] * (s_rv[1][c0] * sl) +
+                           cz[4 * n + qh] * (rv[2][qh] * sh) + cz[5 * n + qh] * (s_rv[2][c0] * sl);
+          const double sw = a.rw[qh] * (cC.afact[kk] * sh + cC.bfact[kk] * sl);
+          vmh_hi = h * cG.RGAMH[qh] + 1.0 * sw * cG.RGSQRTH[qh];
+        }
+        dv[s] = -div - (vmh_hi - vmh_lo[s]) * cC.rdgz[k];
+        vmh_lo[s] = vmh_hi;
+      }
+      const double rh = a.rg[p];
+      const double dvx = dv[0] - (-2.0 * rh * (cC.OHM * s_vv[1][c0]));
+      const double dvy = dv[1] - (2.0 * rh * (cC.OHM * s_vv[0][c0]));
+      const double dvz = dv[2];
+      const double prd = dvx * gx + dvy * gy + dvz * gz;
+      a.gvx[p] = dvx - prd * gx;
+      a.gvy[p] = dvy - prd * gy;
+      a.gvz[p] = dvz - prd * gz;
+      const double gwc = prd * cC.alpha;
+      a.gw[p] = (k >= kmin + 1) ? (cG.C2W[p] * gwc + cG.C2W[n + p] * gwc_prev) : 0.0;
+      gwc_prev = gwc;
+    }
+    __syncthreads();
+  }
+}
+
 __global__ void k_advmom(AdvMomArgs a) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;

@@ -98,7 +98,7 @@ __global__ void k_dd3d(Four v, Three out) {
 // k_dd3d (the untiled form kept for reference and the pole-adjacent checks).
 #define DD_DX 32
 #define DD_DY 8
-__global__ void __launch_bounds__(DD_DX * DD_DY) k_dd3d_t(Four v, Three out) {
+__global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_dd3d_t(Four v, Three out) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2;   // points i0-1 .. i0+DX, j0-1 .. j0+DY
   constexpr int TX = DD_DX + 1, TY = DD_DY + 1;   // triangles i0-1 .. i0+DX-1, j0-1 .. j0+DY-1
   __shared__ double s_vm[3][PY * PX];
@@ -1153,7 +1153,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_path1_t(Path1Args a) {
 // Regional path 1, one block per (level, tile): same stencils and
 // arithmetic as path1_column.  The blocks at kmin and kmax also write the
 // boundary rows kmin-1 and kmax+1 from the values they computed.
-__global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_path1_l(Path1Args a) {
+__global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_path1_l(Path1Args a) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
   __shared__ double s_v[3][PY * PX];
   __shared__ double s_p[PY * PX];
