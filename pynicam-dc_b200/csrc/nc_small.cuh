@@ -1147,7 +1147,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_path1_t(Path1Args a) {
 // Regional path 1, one block per (level, tile): same stencils and
 // arithmetic as path1_column.  The blocks at kmin and kmax also write the
 // boundary rows kmin-1 and kmax+1 from the values they computed.
-__global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_path1_l(Path1Args a) {
+__global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_path1_l(Path1Args a) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
   __shared__ double s_v[3][PY * PX];
   __shared__ double s_p[PY * PX];
@@ -1158,37 +1158,6 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_path1_l(Path1Args a) {
   const int kk = (k == kmin) ? kmin + 1 : k;
   const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
   const double RovCV = a.RovCV;
-  // the cell's own-column loads do not depend on the staged tile: issue them
-  // before the first barrier so that their latency overlaps the staging
-  const int i = i0 + tx, j = j0 + ty;
-  const bool own = (i <= gmax) && (j <= gmax);
-  const int q0 = own ? ix(i, j, 0, l) : 0;
-  const int n = cD.npti;
-  const int qk = q0 + k * cD.planei, qkk = q0 + kk * cD.planei, qk1 = qkk + cD.planei;
-  double gTv[3] = {0.0, 0.0, 0.0}, PSv[3] = {0.0, 0.0, 0.0}, PMv[3] = {0.0, 0.0, 0.0};
-  double czu[6], czd[6], P_k1 = 0.0, P_k = 0.0, P_km = 0.0, rgh1 = 0.0, rgh0 = 0.0;
-  if (own) {
-    auto Pown = [&](int k2) {
-      const int kc = k2 < kmin ? kmin : (k2 > kmax ? kmax : k2);
-      return a.PS[5][q0 + kc * cD.planei] * RovCV;
-    };
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      gTv[d] = a.gT[1 + d][qk];
-      PSv[d] = a.PS[1 + d][qk];
-      PMv[d] = a.PM[1 + d][qk];
-    }
-    P_k1 = Pown(kk + 1);
-    P_k = Pown(kk);
-    P_km = Pown(kk - 1);
-    rgh1 = cG.RGAMH[qk1];
-    rgh0 = cG.RGAMH[qkk];
-#pragma unroll
-    for (int c6 = 0; c6 < 6; ++c6) {
-      czu[c6] = cG.C2WGz[c6 * n + qk1];
-      czd[c6] = cG.C2WGz[c6 * n + qkk];
-    }
-  }
   for (int p = tid; p < PX * PY; p += blockDim.x) {
     const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
     double x = 0.0, y = 0.0, z = 0.0, pp = 0.0;
@@ -1224,9 +1193,17 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_path1_l(Path1Args a) {
     s_tj[p] = sTJ;
   }
   __syncthreads();
-  if (!own) return;
+  const int i = i0 + tx, j = j0 + ty;
+  if (i > gmax || j > gmax) return;
   const double r = cC.rscale, ddc = cC.divdamp_coef, dt = a.dt, rweight = a.rweight;
+  const int n = cD.npti;
+  const double* cz = cG.C2WGz;
   const double gx = P2(cG.GRD_x, 0, i, j, l), gy = P2(cG.GRD_x, 1, i, j, l), gz = P2(cG.GRD_x, 2, i, j, l);
+  const int q0 = ix(i, j, 0, l);
+  auto Pown = [&](int k2) {
+    const int kc = k2 < kmin ? kmin : (k2 > kmax ? kmax : k2);
+    return a.PS[5][q0 + (int)kc * cD.planei] * RovCV;
+  };
   const int ta = (ty + 1) * TX + (tx + 1);
   const double aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
   const double cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1], dTJ = s_tj[ta - TX];
@@ -1244,14 +1221,17 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_path1_l(Path1Args a) {
   }
   const int c0 = (ty + 1) * PX + (tx + 1);
   const double s7[7] = {s_p[c0], s_p[c0 + 1], s_p[c0 + PX + 1], s_p[c0 + PX], s_p[c0 - 1], s_p[c0 - PX - 1], s_p[c0 - PX]};
+  const int qkk = q0 + (int)kk * cD.planei, qk1 = qkk + cD.planei;
+  const double P_k1 = Pown(kk + 1), P_k = Pown(kk), P_km = Pown(kk - 1);
+  const double rgh1 = cG.RGAMH[qk1], rgh0 = cG.RGAMH[qkk];
   double pg[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     double g = P2(cG.coef_grad, d * 7 + 0, i, j, l) * s7[0];
 #pragma unroll
     for (int m = 1; m < 7; ++m) g = g + P2(cG.coef_grad, d * 7 + m, i, j, l) * s7[m];
-    const double up = (czu[2 * d] * P_k1 + czu[2 * d + 1] * P_k) * rgh1;
-    const double dn = (czd[2 * d] * P_k + czd[2 * d + 1] * P_km) * rgh0;
+    const double up = (cz[(2 * d) * n + qk1] * P_k1 + cz[(2 * d + 1) * n + qk1] * P_k) * rgh1;
+    const double dn = (cz[(2 * d) * n + qkk] * P_k + cz[(2 * d + 1) * n + qkk] * P_km) * rgh0;
     pg[d] = g + (up - dn) * cC.rdgz[kk];
   }
   {
@@ -1260,14 +1240,14 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_path1_l(Path1Args a) {
     pg[1] = pg[1] - prd * gy / r;
     pg[2] = pg[2] - prd * gz / r;
   }
-  const int q = qk;
+  const int q = q0 + (int)k * cD.planei;
   double v[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    const double drv = gTv[d] - pg[d] + dd[d] + 0.0;
-    v[d] = PSv[d] + drv * dt;
+    const double drv = a.gT[1 + d][q] - pg[d] + dd[d] + 0.0;
+    v[d] = a.PS[1 + d][q] + drv * dt;
     a.dvh[d][q] = v[d];
-    a.PM[1 + d][q] = PMv[d] + v[d] * rweight;
+    a.PM[1 + d][q] = a.PM[1 + d][q] + v[d] * rweight;
   }
   if (k == kmin) {
     const int pB = q - cD.planei;
