@@ -571,7 +571,7 @@ static int run_step(nc_handle* h) {
         (void)gt;
         k_vp0_hl<<<lvgrid, DD_DX * DD_DY, 0, s>>>(va, vh);
         TRY(check_launch(h, "vp0_h"));
-        k_vp0_c<<<greg, kBlock, 0, s>>>(va, vh);
+        k_vp0_cr<<<greg, kBlock, 0, s>>>(va, vh);
         TRY(check_launch(h, "vp0_c"));
       } else {
         k_vp0<<<1, 32, 0, ps>>>(va, 1);

@@ -112,6 +112,12 @@ __device__ __forceinline__ double M3(const double* a, int c, int i, int j, int k
   return a[c * cD.npti + ix(i, j, k, l)];
 }
 __device__ __forceinline__ double P2(const double* a, int c, int i, int j, int l) { return a[ix2(c, i, j, l)]; }
+// the same through the read-only (non-coherent) path: the planes are constant
+// after set-up, and the compiler may batch these loads ahead of shared-memory
+// stores.  Used where that measured faster (path 1, 3-D divergence damping,
+// tracer horizontal flux); where it raised register pressure into spills
+// (momentum advection, vp0 horizontal terms) the plain load is kept.
+__device__ __forceinline__ double P2c(const double* a, int c, int i, int j, int l) { return __ldg(a + ix2(c, i, j, l)); }
 
 // 7-point neighbour offsets in the reference's coefficient order:
 // (i,j) (i+1,j) (i+1,j+1) (i,j+1) (i-1,j) (i-1,j-1) (i,j-1)

@@ -105,13 +105,116 @@ __device__ void diag_column(const Col c, const Met m, const DiagArgs& a, double 
   }
 }
 
+// diag_column with the second pass (eth, deviations, merged velocity) fused
+// into the first for the levels kmin+1..kmax-1, whose inputs do not depend on
+// the boundary rows: level k-1 is finished while level k is diagnosed, from
+// values carried in registers.  The four levels next to and on the boundary
+// rows are finished after the boundary conditions, as in diag_column.  Same
+// expressions, same results.
+__device__ void diag_column_fused(const Col c, const Met m, const DiagArgs& a, double gx, double gy, double gz) {
+  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
+  double** P = const_cast<double**>(a.P.v);
+  auto finish = [&](int k, int p, double pre, double rho, double ein, double vxk, double vyk, double vzk,
+                    double wk, double wk1) {
+    a.eth[p] = ein + pre / rho;
+    a.pregd[p] = (pre - m.pre_bs[p]) * m.GSGAM2[p];
+    a.rhogd[p] = (rho - m.rho_bs[p]) * m.GSGAM2[p];
+    if (k >= kmin && k <= kmax) {
+      double wc = cC.cfact[k] * wk1 + cC.dfact[k] * wk;
+      a.vvx[p] = vxk + wc * gx / cC.rscale;
+      a.vvy[p] = vyk + wc * gy / cC.rscale;
+      a.vvz[p] = vzk + wc * gz / cC.rscale;
+    } else {
+      a.vvx[p] = 0.0; a.vvy[p] = 0.0; a.vvz[p] = 0.0;
+    }
+  };
+  double pp = 0.0, pr = 0.0, pe = 0.0, px = 0.0, py = 0.0, pz = 0.0, pw = 0.0;   // level k-1
+  double rg_prev = 0.0;
+  for (int k = 0; k < KA; ++k) {
+    int p = c.at(k);
+    double RHOG = P[0][p];
+    double rho = RHOG / m.GSGAM2[p];
+    const double vx = P[1][p] / RHOG, vy = P[2][p] / RHOG, vz = P[3][p] / RHOG;
+    a.vx[p] = vx;
+    a.vy[p] = vy;
+    a.vz[p] = vz;
+    double ein = P[5][p] / RHOG;
+    double q0 = a.Pq0[p] / RHOG;
+    double qd = 1.0 - q0;
+    double cv = q0 * cC.CVW0 + qd * cC.CVdry;
+    double tem = ein / cv;
+    const double pre = rho * tem * (qd * cC.Rdry + q0 * cC.Rvap);
+    a.tem[p] = tem;
+    a.pre[p] = pre;
+    a.rho[p] = rho;
+    a.ein[p] = ein;
+    double w = 0.0;
+    if (k >= kmin + 1 && k <= kmax) {
+      w = P[4][p] / (mc(m.C2W, c, 0, 2, k) * RHOG + mc(m.C2W, c, 1, 2, k) * rg_prev);
+      a.w[p] = w;
+    }
+    if (k - 1 >= kmin + 1 && k - 1 <= kmax - 1) finish(k - 1, c.at(k - 1), pp, pr, pe, px, py, pz, pw, w);
+    pp = pre; pr = rho; pe = ein; px = vx; py = vy; pz = vz; pw = w;
+    rg_prev = RHOG;
+  }
+  // ---- boundary conditions: TEM top/bottom, FREE top, RIGID bottom
+  const int pT = c.at(kmax + 1), pK = c.at(kmax), pKm = c.at(kmax - 1);
+  const int pB = c.at(kmin - 1), pN = c.at(kmin), pNp = c.at(kmin + 1);
+  double tem_top = a.tem[pK];
+  double tem_btm = a.tem[pN];
+  double pre_top = a.pre[pKm] - a.rho[pK] * (m.PHI[pT] - m.PHI[pKm]);
+  double pre_btm = a.pre[pNp] - a.rho[pN] * (m.PHI[pB] - m.PHI[pNp]);
+  double rho_top = pre_top / (cC.Rdry * tem_top);
+  double rho_btm = pre_btm / (cC.Rdry * tem_btm);
+  a.tem[pT] = tem_top; a.tem[pB] = tem_btm;
+  a.pre[pT] = pre_top; a.pre[pB] = pre_btm;
+  a.rho[pT] = rho_top; a.rho[pB] = rho_btm;
+  double rgT = rho_top * m.GSGAM2[pT];
+  double rgB = rho_btm * m.GSGAM2[pB];
+  P[0][pT] = rgT; P[0][pB] = rgB;
+  double einT = cC.CVdry * tem_top, einB = cC.CVdry * tem_btm;
+  a.ein[pT] = einT; a.ein[pB] = einB;
+  P[5][pT] = rgT * einT; P[5][pB] = rgB * einB;
+  double rgK = P[0][pK], rgN = P[0][pN];
+  double vT[3], vB[3];
+  for (int d = 0; d < 3; ++d) {
+    vT[d] = 1.0 * (P[1 + d][pK] / rgK) * rgT;
+    vB[d] = -1.0 * (P[1 + d][pN] / rgN) * rgB;
+    P[1 + d][pT] = vT[d];
+    P[1 + d][pB] = vB[d];
+  }
+  double* dv[3] = {a.vx, a.vy, a.vz};
+  for (int d = 0; d < 3; ++d) {
+    dv[d][pT] = P[1 + d][pT] / P[0][pT];
+    dv[d][pB] = P[1 + d][pB] / P[0][pB];
+  }
+  const int kT = kmax + 1;
+  double rwT = -(mc(m.C2WGz, c, 0, 6, kT) * vT[0] + mc(m.C2WGz, c, 1, 6, kT) * P[1][pK] +
+                 mc(m.C2WGz, c, 2, 6, kT) * vT[1] + mc(m.C2WGz, c, 3, 6, kT) * P[2][pK] +
+                 mc(m.C2WGz, c, 4, 6, kT) * vT[2] + mc(m.C2WGz, c, 5, 6, kT) * P[3][pK]);
+  P[4][pT] = rwT;
+  P[4][pN] = 0.0;
+  P[4][pB] = 0.0;
+  a.w[pT] = rwT / (mc(m.C2W, c, 0, 2, kT) * rgT + mc(m.C2W, c, 1, 2, kT) * rgK);
+  a.w[pN] = P[4][pN] / (mc(m.C2W, c, 0, 2, kmin) * rgN + mc(m.C2W, c, 1, 2, kmin) * rgB);
+  a.w[pB] = 0.0;
+  // ---- the levels next to the boundary rows
+  const int rest[4] = {kmin - 1, kmin, kmax, kmax + 1};
+  for (int r = 0; r < 4; ++r) {
+    const int k = rest[r];
+    const int p = c.at(k);
+    const double wk1 = (k >= kmin && k <= kmax) ? a.w[c.at(k + 1)] : 0.0;
+    finish(k, p, a.pre[p], a.rho[p], a.ein[p], a.vx[p], a.vy[p], a.vz[p], a.w[p], wk1);
+  }
+}
+
 __global__ void k_diag(DiagArgs a, int pole) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
   if (!pole) {
-    diag_column(col_reg(i, j, l), met_of(false), a, P2(cG.GRD_x, 0, i, j, l), P2(cG.GRD_x, 1, i, j, l),
-                P2(cG.GRD_x, 2, i, j, l));
+    diag_column_fused(col_reg(i, j, l), met_of(false), a, P2(cG.GRD_x, 0, i, j, l), P2(cG.GRD_x, 1, i, j, l),
+                      P2(cG.GRD_x, 2, i, j, l));
   } else {
     const double* X = cG.GRD_x_pl;
     diag_column(col_pl(g, lp), met_of(true), a, X[(g * cD.LP + lp) * 3 + 0], X[(g * cD.LP + lp) * 3 + 1],
@@ -372,6 +475,10 @@ __global__ void k_hdiff1(Six src, SixOut out) {
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
   const bool in = interior(i, j);
+  // the column's seven laplacian coefficients, loaded once for all levels
+  double cl[7];
+#pragma unroll
+  for (int m = 0; m < 7; ++m) cl[m] = in ? P2(cG.coef_lap, m, i, j, l) : 0.0;
   for (int k = 0; k < cD.KA; ++k) {
     int p = ix(i, j, k, l);
 #pragma unroll
@@ -379,19 +486,16 @@ __global__ void k_hdiff1(Six src, SixOut out) {
       double v = 0.0;
       if (in) {
         const double* s = src.f[n];
-        if (n == 4) {
-          v = lap7(i, j, k, l, [&](int ii, int jj, int kk) {
-            int q = ix(ii, jj, kk, l);
-            return s[q] - cG.tem_bs[q];
-          });
-        } else if (n == 5) {
-          v = lap7(i, j, k, l, [&](int ii, int jj, int kk) {
-            int q = ix(ii, jj, kk, l);
-            return s[q] - cG.rho_bs[q];
-          });
-        } else {
-          v = lap7(i, j, k, l, [&](int ii, int jj, int kk) { return s[ix(ii, jj, kk, l)]; });
-        }
+        const double* bs = (n == 4) ? cG.tem_bs : cG.rho_bs;
+        // lap7 (kernels/oprtlaplacian.py:41-55) with the reference-state
+        // deviation for TEM and RHO
+        auto scl = [&](int m) {
+          const int q = ix(i + kNbI[m], j + kNbJ[m], k, l);
+          return (n >= 4) ? s[q] - bs[q] : s[q];
+        };
+        v = cl[0] * scl(0);
+#pragma unroll
+        for (int m = 1; m < 7; ++m) v = v + cl[m] * scl(m);
       }
       out.f[n][p] = -v;
     }
@@ -606,7 +710,7 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, 2) k_hdiff2_t(Six vt, const dou
 
 // Second hyperdiffusion pass, one block per (level, tile): same staging,
 // triangle gradients and arithmetic as k_hdiff2_t, without the level loop.
-__global__ void __launch_bounds__(HD_DX * HD_DY, 3) k_hdiff2_l(Six vt, const double* rhog, SixOut out) {
+__global__ void __launch_bounds__(HD_DX * HD_DY, 4) k_hdiff2_l(Six vt, const double* rhog, SixOut out) {
   constexpr int PX = HD_DX + 2, PY = HD_DY + 2, TX = HD_DX + 1, TY = HD_DY + 1;
   __shared__ double s_f[6][PY * PX];
   __shared__ double s_r[PY * PX];

@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_dd3d_t(Four v, Three out) 
       double sTI = 0.0, sTJ = 0.0;
       if (ii <= G - 2 && jj <= G - 2) {
         const int a = py * PX + px, b = a + 1, c = a + PX + 1, d = a + PX;
-        auto C = [&](int dir, int pt, int t) { return P2(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
+        auto C = [&](int dir, int pt, int t) { return P2c(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
         const double wTI = ((rU[a] + rU[b] + rU[c]) - (rD[a] + rD[b] + rD[c])) / 3.0 * rdz;
         const double wTJ = ((rU[a] + rU[c] + rU[d]) - (rD[a] + rD[c] + rD[d])) / 3.0 * rdz;
         sTI = C(0, 0, 0) * s_vm[0][a] + C(0, 1, 0) * s_vm[0][b] + C(0, 2, 0) * s_vm[0][c] +
@@ -174,9 +174,9 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_dd3d_t(Four v, Three out) 
       const int q = ix(i, j, k, l);
 #pragma unroll
       for (int d = 0; d < 3; ++d)
-        out.f[d][q] = P2(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) + P2(cG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
-                      P2(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) + P2(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
-                      P2(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) + P2(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI);
+        out.f[d][q] = P2c(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) + P2c(cG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
+                      P2c(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) + P2c(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
+                      P2c(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) + P2c(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI);
     }
     __syncthreads();
     cur ^= 1;
@@ -722,7 +722,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_vp0_h(Vp0Args a, Vp0H h) {
 }
 
 // vp0 horizontal terms, one block per (level, tile) (body of k_vp0_h).
-__global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_vp0_hl(Vp0Args a, Vp0H h) {
+__global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
   __shared__ double s_m[3][PY * PX];    // RGAM * rhogv
   __shared__ double s_e[3][PY * PX];    // RGAM * rhogv * eth
@@ -938,6 +938,116 @@ __global__ void __launch_bounds__(128) k_vp0_c(Vp0Args a, Vp0H h) {
     }
     double kin0 = rhogkin_at(c, m, k, [&](int kk, int comp) { return P[comp][c.at(kk)]; });
     a.ethtot0[p] = a.eth[p] + kin0 / P[0][p] + m.PHI[p];
+  }
+}
+
+// k_vp0_c marching upward with every half-level quantity evaluated once per
+// column: at level k the values at k+1 (vertical mass and energy fluxes,
+// buoyancy, vertical pressure gradient, gz, pwh, half-level eth, the vertical
+// kinetic-energy term) are formed and the ones at k and k-1 are carried in
+// registers.  Each value is the same expression as in k_vp0_c, so the results
+// are identical.
+__global__ void __launch_bounds__(128) k_vp0_cr(Vp0Args a, Vp0H h) {
+  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (!col_of(t, i, j, l)) return;
+  const Col c = col_reg(i, j, l);
+  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
+  const int n = cD.npti;
+  const bool in = interior(i, j);
+  const double* const* P = a.P.v;
+  const double dt = a.dt;
+  const double GRAV = cC.GRAV;
+  const double* cz = cG.C2WGz;
+  const double* c2w = cG.C2W;
+  const double* w2c = cG.W2C;
+  const double GCVovR = cC.GRAV * cC.CVdry / cC.Rdry;
+  const double ACVovRt2 = cC.alpha * cC.CVdry / cC.Rdry / (dt * dt);
+  // values at level k (index 0) and k-1 (index m), carried upward
+  double vA0 = 0.0, vE0 = 0.0;            // vertical fluxes of rhog / rhoge at half level k
+  double gz0 = 0.0, gzm = 0.0;            // gz at k and k-1
+  double eh0 = 0.0, ehm = 0.0;            // half-level eth at k and k-1
+  double pwh0 = 0.0, dpgw0 = 0.0, dbuo0 = 0.0, vint0 = 0.0;
+  for (int k = 0; k < KA; ++k) {
+    const int p = c.at(k);
+    const int kn = k + 1;
+    // ---- half-level values at kn = k+1
+    double vA1 = 0.0, vE1 = 0.0, gz1 = 0.0, eh1 = 0.0, pwh1 = 0.0, dpgw1 = 0.0, dbuo1 = 0.0, vint1 = 0.0;
+    if (kn < KA) {
+      const int q = c.at(kn), qm = c.at(kn - 1);
+      if (kn > kmin && kn <= kmax) {
+        const double rgh = cG.RGAMH[q], rsq = cG.RGSQRTH[q];
+        const double z0 = cz[q], z1 = cz[n + q], z2 = cz[2 * n + q], z3 = cz[3 * n + q], z4 = cz[4 * n + q],
+                     z5 = cz[5 * n + q];
+        const double px = P[1][q], pxm = P[1][qm], py = P[2][q], pym = P[2][qm], pz = P[3][q], pzm = P[3][qm];
+        const double e = a.eth[q], em = a.eth[qm], w = P[4][q];
+        const double hA = z0 * px + z1 * pxm + z2 * py + z3 * pym + z4 * pz + z5 * pzm;
+        vA1 = hA * rgh + 1.0 * w * rsq;
+        const double hE = z0 * (px * e) + z1 * (pxm * em) + z2 * (py * e) + z3 * (pym * em) + z4 * (pz * e) +
+                          z5 * (pzm * em);
+        vE1 = hE * rgh + 1.0 * (w * (cC.afact[kn] * e + cC.bfact[kn] * em)) * rsq;
+        // vertical kinetic-energy term of rhogkin
+        const double den = c2w[q] * P[0][q] + c2w[n + q] * P[0][qm];
+        vint1 = 0.5 * (w * w) / den;
+        // buoyancy and vertical pressure gradient
+        dbuo1 = -GRAV * (c2w[q] * a.rhogd[q] + c2w[n + q] * a.rhogd[qm]);
+        dpgw1 = cG.GAM2H[q] * (a.pregd[q] * cG.RGSGAM2[q] - a.pregd[qm] * cG.RGSGAM2[qm]) * cC.rdgzh[kn];
+      }
+      if (kn >= kmin && kn <= kmax + 1) {
+        const int kk = kn;   // kn >= kmin here, so the clamp of rhog_h / eth_h is inactive
+        const double rh = c2w[q] * P[0][q] + c2w[n + q] * P[0][c.at(kk - 1)];
+        gz1 = GRAV - (dpgw1 - dbuo1) / rh;
+        pwh1 = -gz1 * P[4][q];
+        eh1 = cC.afact[kk] * a.eth[q] + cC.bfact[kk] * a.eth[c.at(kk - 1)];
+      }
+    }
+    // ---- level k
+    const bool hk = in && k >= kmin && k <= kmax;
+    const bool kin = k >= kmin && k <= kmax;
+    const double div1 = hk ? h.out[0][p] : 0.0, div2 = hk ? h.out[1][p] : 0.0;
+    const double drhog = kin ? -div1 - (vA1 - vA0) * cC.rdgz[k] : 0.0;
+    const double drhoge = kin ? -div2 - (vE1 - vE0) * cC.rdgz[k] : 0.0;
+    double dd[3], dpg[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      dd[d] = hk ? h.out[2 + d][p] : 0.0;
+      dpg[d] = hk ? h.out[5 + d][p] : 0.0;
+    }
+    double pw = 0.0;
+    if (kin)
+      pw = a.vx[p] * dpg[0] + a.vy[p] * dpg[1] + a.vz[p] * dpg[2] + w2c[p] * pwh1 + w2c[n + p] * pwh0;
+    a.gT[0][p] = a.gT0[0][p] + drhog;
+    a.gT[1][p] = a.gT0[1][p] - dpg[0] + dd[0] + 0.0;
+    a.gT[2][p] = a.gT0[2][p] - dpg[1] + dd[1] + 0.0;
+    a.gT[3][p] = a.gT0[3][p] - dpg[2] + dd[2] + 0.0;
+    a.gT[4][p] = a.gT0[4][p] + 0.0 * cC.alpha - dpgw0 + dbuo0;
+    a.gT[5][p] = a.gT0[5][p] + drhoge + pw;
+    if (k >= kmin + 1 && k <= kmax) {
+      const int pm = c.at(k - 1), pp = c.at(k + 1);
+      const double rg = cC.rdgz[k], rgm = cC.rdgz[k - 1];
+      const double Ca = (cG.RGSGAM2[p] * rg + cG.RGSGAM2[pm] * rgm) * cG.GAM2H[p];
+      const double Cb = cC.dfact[k] - cC.cfact[k - 1];
+      const double Cu1 = cG.RGSGAM2[p] * rg * cG.GAM2H[pp];
+      const double rgh2 = cG.RGAMH[p] * cG.RGAMH[p];
+      const double Cu2 = cG.GAM2H[pp] * rgh2 * GCVovR;
+      const double Cl1 = cG.RGSGAM2[p] * rg * cG.GAM2H[pm];
+      const double Cl2 = cG.GAM2H[pm] * rgh2 * GCVovR;
+      const double rgh = cC.rdgzh[k];
+      a.Mc[p] = ACVovRt2 / cG.RGSQRTH[p] + rgh * (Ca * eh0 - Cb * (gz0 + GCVovR));
+      a.Mu[p] = -rgh * (Cu1 * eh1 + cC.cfact[k] * (gz1 + Cu2));
+      a.Ml[p] = -rgh * (Cl1 * ehm - cC.dfact[k - 1] * (gzm + Cl2));
+    }
+    double kin0 = 0.0;
+    if (kin) {
+      const double rg = P[0][p], vx = P[1][p], vy = P[2][p], vz = P[3][p];
+      const double kh = 0.5 * (vx * vx + vy * vy + vz * vz) / rg;
+      kin0 = kh + w2c[p] * vint1 + w2c[n + p] * vint0;
+    }
+    a.ethtot0[p] = a.eth[p] + kin0 / P[0][p] + cG.PHI[p];
+    vA0 = vA1; vE0 = vE1;
+    gzm = gz0; gz0 = gz1;
+    ehm = eh0; eh0 = eh1;
+    pwh0 = pwh1; dpgw0 = dpgw1; dbuo0 = dbuo1; vint0 = vint1;
   }
 }
 
@@ -1163,11 +1273,11 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_path1_l(Path1Args a) {
     double x = 0.0, y = 0.0, z = 0.0, pp = 0.0;
     if (ii < G && jj < G) {
       const int q = ix(ii, jj, k, l);
-      x = -a.vt.f[0][q];
-      y = -a.vt.f[1][q];
-      z = -a.vt.f[2][q];
+      x = -__ldg(&a.vt.f[0][q]);
+      y = -__ldg(&a.vt.f[1][q]);
+      z = -__ldg(&a.vt.f[2][q]);
       const int qk = ix(ii, jj, kk, l);
-      pp = a.PS[5][qk] * RovCV * cG.RGAM[qk];
+      pp = __ldg(&a.PS[5][qk]) * RovCV * __ldg(&cG.RGAM[qk]);
     }
     s_v[0][p] = x;
     s_v[1][p] = y;
@@ -1181,7 +1291,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_path1_l(Path1Args a) {
     double sTI = 0.0, sTJ = 0.0;
     if (ii <= G - 2 && jj <= G - 2) {
       const int ia = py * PX + px, ib = ia + 1, ic = ia + PX + 1, id = ia + PX;
-      auto C = [&](int dir, int pt, int t) { return P2(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
+      auto C = [&](int dir, int pt, int t) { return P2c(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
       sTI = C(0, 0, 0) * s_v[0][ia] + C(0, 1, 0) * s_v[0][ib] + C(0, 2, 0) * s_v[0][ic] +
             C(1, 0, 0) * s_v[1][ia] + C(1, 1, 0) * s_v[1][ib] + C(1, 2, 0) * s_v[1][ic] +
             C(2, 0, 0) * s_v[2][ia] + C(2, 1, 0) * s_v[2][ib] + C(2, 2, 0) * s_v[2][ic];
@@ -1198,11 +1308,11 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_path1_l(Path1Args a) {
   const double r = cC.rscale, ddc = cC.divdamp_coef, dt = a.dt, rweight = a.rweight;
   const int n = cD.npti;
   const double* cz = cG.C2WGz;
-  const double gx = P2(cG.GRD_x, 0, i, j, l), gy = P2(cG.GRD_x, 1, i, j, l), gz = P2(cG.GRD_x, 2, i, j, l);
+  const double gx = P2c(cG.GRD_x, 0, i, j, l), gy = P2c(cG.GRD_x, 1, i, j, l), gz = P2c(cG.GRD_x, 2, i, j, l);
   const int q0 = ix(i, j, 0, l);
   auto Pown = [&](int k2) {
     const int kc = k2 < kmin ? kmin : (k2 > kmax ? kmax : k2);
-    return a.PS[5][q0 + (int)kc * cD.planei] * RovCV;
+    return __ldg(&a.PS[5][q0 + (int)kc * cD.planei]) * RovCV;
   };
   const int ta = (ty + 1) * TX + (tx + 1);
   const double aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
@@ -1210,9 +1320,9 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_path1_l(Path1Args a) {
   double dd[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d)
-    dd[d] = ddc * (P2(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) + P2(cG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
-                   P2(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) + P2(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
-                   P2(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) + P2(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI));
+    dd[d] = ddc * (P2c(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) + P2c(cG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
+                   P2c(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) + P2c(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
+                   P2c(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) + P2c(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI));
   {
     const double prd = (dd[0] * gx + dd[1] * gy + dd[2] * gz) / r;
     dd[0] = dd[0] - prd * gx / r;
@@ -1223,15 +1333,15 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_path1_l(Path1Args a) {
   const double s7[7] = {s_p[c0], s_p[c0 + 1], s_p[c0 + PX + 1], s_p[c0 + PX], s_p[c0 - 1], s_p[c0 - PX - 1], s_p[c0 - PX]};
   const int qkk = q0 + (int)kk * cD.planei, qk1 = qkk + cD.planei;
   const double P_k1 = Pown(kk + 1), P_k = Pown(kk), P_km = Pown(kk - 1);
-  const double rgh1 = cG.RGAMH[qk1], rgh0 = cG.RGAMH[qkk];
+  const double rgh1 = __ldg(&cG.RGAMH[qk1]), rgh0 = __ldg(&cG.RGAMH[qkk]);
   double pg[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    double g = P2(cG.coef_grad, d * 7 + 0, i, j, l) * s7[0];
+    double g = P2c(cG.coef_grad, d * 7 + 0, i, j, l) * s7[0];
 #pragma unroll
-    for (int m = 1; m < 7; ++m) g = g + P2(cG.coef_grad, d * 7 + m, i, j, l) * s7[m];
-    const double up = (cz[(2 * d) * n + qk1] * P_k1 + cz[(2 * d + 1) * n + qk1] * P_k) * rgh1;
-    const double dn = (cz[(2 * d) * n + qkk] * P_k + cz[(2 * d + 1) * n + qkk] * P_km) * rgh0;
+    for (int m = 1; m < 7; ++m) g = g + P2c(cG.coef_grad, d * 7 + m, i, j, l) * s7[m];
+    const double up = (__ldg(&cz[(2 * d) * n + qk1]) * P_k1 + __ldg(&cz[(2 * d + 1) * n + qk1]) * P_k) * rgh1;
+    const double dn = (__ldg(&cz[(2 * d) * n + qkk]) * P_k + __ldg(&cz[(2 * d + 1) * n + qkk]) * P_km) * rgh0;
     pg[d] = g + (up - dn) * cC.rdgz[kk];
   }
   {
@@ -1244,8 +1354,8 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_path1_l(Path1Args a) {
   double v[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    const double drv = a.gT[1 + d][q] - pg[d] + dd[d] + 0.0;
-    v[d] = a.PS[1 + d][q] + drv * dt;
+    const double drv = __ldg(&a.gT[1 + d][q]) - pg[d] + dd[d] + 0.0;
+    v[d] = __ldg(&a.PS[1 + d][q]) + drv * dt;
     a.dvh[d][q] = v[d];
     a.PM[1 + d][q] = a.PM[1 + d][q] + v[d] * rweight;
   }
@@ -1253,7 +1363,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_path1_l(Path1Args a) {
     const int pB = q - cD.planei;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const double vB = -1.0 * (v[d] / a.rhog[q]) * a.rhog[pB];
+      const double vB = -1.0 * (v[d] / __ldg(&a.rhog[q])) * __ldg(&a.rhog[pB]);
       a.dvh[d][pB] = vB;
       a.PM[1 + d][pB] = a.PM[1 + d][pB] + vB * rweight;
     }
@@ -1262,7 +1372,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_path1_l(Path1Args a) {
     const int pT = q + cD.planei;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const double vT = 1.0 * (v[d] / a.rhog[q]) * a.rhog[pT];
+      const double vT = 1.0 * (v[d] / __ldg(&a.rhog[q])) * __ldg(&a.rhog[pT]);
       a.dvh[d][pT] = vT;
       a.PM[1 + d][pT] = a.PM[1 + d][pT] + vT * rweight;
     }
@@ -1418,13 +1528,13 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_vimain_a_l(VimainArgs a) {
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
       if (ii < G && jj < G) {
         const int q = ix(ii, jj, k, l);
-        const double rg = cG.RGAM[q], e = a.eth[q], et = a.ethtot0[q];
+        const double rg = __ldg(&cG.RGAM[q]), e = __ldg(&a.eth[q]), et = __ldg(&a.ethtot0[q]);
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          const double dv = a.dvh.f[d][q];
+          const double dv = __ldg(&a.dvh.f[d][q]);
           s_h[0][d][p] = dv * rg;
           s_h[1][d][p] = (dv * e) * rg;
-          s_h[2][d][p] = ((a.P[1 + d][q] + dv) * et) * rg;
+          s_h[2][d][p] = ((__ldg(&a.P[1 + d][q]) + dv) * et) * rg;
         }
       } else {
 #pragma unroll
@@ -1444,7 +1554,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_vimain_a_l(VimainArgs a) {
         double s[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int m = 0; m < 7; ++m) {
-          const double cdv = P2(cG.coef_div, d * 7 + m, i, j, l);
+          const double cdv = P2c(cG.coef_div, d * 7 + m, i, j, l);
 #pragma unroll
           for (int f = 0; f < 3; ++f) {
             const double t = cdv * s_h[f][d][nb[m]];

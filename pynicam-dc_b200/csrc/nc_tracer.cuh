@@ -158,8 +158,8 @@ struct TrcHfluxArgs {
 // before the singular-point fix
 __device__ void trc_vertex_raw(const TrcHfluxArgs& a, int ii, int jj, int k, int l, double TI[4], double TJ[4]) {
   int q0 = ix(ii, jj, k, l), qi = ix(ii + 1, jj, k, l), qd = ix(ii + 1, jj + 1, k, l), qj = ix(ii, jj + 1, k, l);
-  double w1i = P2(cG.GMTR_t, 0, ii, jj, l), w2i = P2(cG.GMTR_t, 1, ii, jj, l), w3i = P2(cG.GMTR_t, 2, ii, jj, l);
-  double w1j = P2(cG.GMTR_t, 3, ii, jj, l), w2j = P2(cG.GMTR_t, 4, ii, jj, l), w3j = P2(cG.GMTR_t, 5, ii, jj, l);
+  double w1i = P2c(cG.GMTR_t, 0, ii, jj, l), w2i = P2c(cG.GMTR_t, 1, ii, jj, l), w3i = P2c(cG.GMTR_t, 2, ii, jj, l);
+  double w1j = P2c(cG.GMTR_t, 3, ii, jj, l), w2j = P2c(cG.GMTR_t, 4, ii, jj, l), w3j = P2c(cG.GMTR_t, 5, ii, jj, l);
   auto F = [&](int n, int q) -> double {
     if (n == 0) return a.rho[q];
     const double* r = (n == 1) ? a.rvx : ((n == 2) ? a.rvy : a.rvz);
@@ -191,9 +191,9 @@ __device__ void trc_vertex(const TrcHfluxArgs& a, int ii, int jj, int k, int l, 
 __device__ __forceinline__ double trc_face(const TrcHfluxArgs& a, int ii, int jj, int l, int f, const double s[4],
                                            double xc[3]) {
   double rr2 = 1.0 / npmax(s[0], cC.EPS);
-  double flux = 0.5 * (s[1] * P2(cG.GMTR_a, f * 3 + 0, ii, jj, l) + s[2] * P2(cG.GMTR_a, f * 3 + 1, ii, jj, l) +
-                       s[3] * P2(cG.GMTR_a, f * 3 + 2, ii, jj, l));
-  for (int d = 0; d < 3; ++d) xc[d] = P2(cG.GRD_xr, f * 3 + d, ii, jj, l) - s[1 + d] * rr2 * a.dt * 0.5;
+  double flux = 0.5 * (s[1] * P2c(cG.GMTR_a, f * 3 + 0, ii, jj, l) + s[2] * P2c(cG.GMTR_a, f * 3 + 1, ii, jj, l) +
+                       s[3] * P2c(cG.GMTR_a, f * 3 + 2, ii, jj, l));
+  for (int d = 0; d < 3; ++d) xc[d] = P2c(cG.GRD_xr, f * 3 + d, ii, jj, l) - s[1 + d] * rr2 * a.dt * 0.5;
   return flux;
 }
 
@@ -228,7 +228,7 @@ __global__ void k_trc_hflux(TrcHfluxArgs a) {
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
   const double dt = a.dt;
-  const double PR = P2(cG.GMTR_p, 0, i, j, l);
+  const double PR = P2c(cG.GMTR_p, 0, i, j, l);
   for (int k = 0; k < cD.KA; ++k) {
     int p = ix(i, j, k, l);
     double fl[6];
