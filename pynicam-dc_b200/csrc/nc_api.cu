@@ -435,6 +435,8 @@ static int run_step(nc_handle* h) {
   // per-level tiled kernels: (levels kmin..kmax, tiles, regions)
   const dim3 lvgrid((unsigned)(D.kmax - D.kmin + 1),
                     (unsigned)(((D.G - 2 + DD_DX - 1) / DD_DX) * ((D.G - 2 + DD_DY - 1) / DD_DY)), (unsigned)D.L);
+  const dim3 lvgrid_vp((unsigned)(D.kmax - D.kmin + 1),
+                       (unsigned)(((D.G - 2 + VP_DX - 1) / VP_DX) * ((D.G - 2 + VP_DY - 1) / VP_DY)), (unsigned)D.L);
   // PROG0 = PROG at the start of the step (mod_dynamics.py:1939-1968)
   for (int v = 0; v < 6; ++v) {
     CU(cudaMemcpyAsync(h->P0[v].r, h->P[v].r, D.npt * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -566,10 +568,7 @@ static int run_step(nc_handle* h) {
       if (!pole) {
         Vp0H vh;
         for (int n = 0; n < 8; ++n) vh.out[n] = h->vph[n].r;
-        const dim3 gt((unsigned)((D.G - 2 + DD_DX - 1) / DD_DX), (unsigned)((D.G - 2 + DD_DY - 1) / DD_DY),
-                      (unsigned)D.L);
-        (void)gt;
-        k_vp0_hl<<<lvgrid, DD_DX * DD_DY, 0, s>>>(va, vh);
+        k_vp0_hl<<<lvgrid_vp, VP_DX * VP_DY, 0, s>>>(va, vh);
         TRY(check_launch(h, "vp0_h"));
         k_vp0_cr<<<greg, kBlock, 0, s>>>(va, vh);
         TRY(check_launch(h, "vp0_c"));
@@ -619,9 +618,6 @@ static int run_step(nc_handle* h) {
         va.PM0 = F(h->PM[0]); va.PM4 = F(h->PM[4]);
         va.dt = h->dts; va.rweight = rweight; va.RovCV = RovCV;
         if (!pole) {
-          const dim3 gt((unsigned)((D.G - 2 + DD_DX - 1) / DD_DX), (unsigned)((D.G - 2 + DD_DY - 1) / DD_DY),
-                        (unsigned)D.L);
-          (void)gt;
           k_vimain_a_l<<<lvgrid, DD_DX * DD_DY, 0, s>>>(va);
           TRY(check_launch(h, "vimain_a"));
           k_vi_solve<<<greg, kBlock, 0, s>>>(va);

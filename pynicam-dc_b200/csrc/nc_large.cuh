@@ -267,7 +267,8 @@ __device__ __forceinline__ double advconv_reg(int i, int j, int k, int l, const 
 // RGAM is staged in shared memory for the three 7-point divergences.  Halo
 // cells and boundary levels are not written (their values are never read:
 // the large-step tendencies derived from them are replaced by the exchanges).
-// Arithmetic and association order are those of k_advmom.
+// Arithmetic and association order are those of the reference's expressions
+// (kernels/advconv.py, kernels/advconvmom.py), as in the pole kernel.
 __global__ void __launch_bounds__(256, 2) k_advmom_t(AdvMomArgs a) {
   constexpr int TXD = 32, TYD = 8;
   constexpr int PX = TXD + 2, PY = TYD + 2;
@@ -355,44 +356,6 @@ __global__ void __launch_bounds__(256, 2) k_advmom_t(AdvMomArgs a) {
       gwc_prev = gwc;
     }
     __syncthreads();
-  }
-}
-
-__global__ void k_advmom(AdvMomArgs a) {
-  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
-  int i, j, l;
-  if (!col_of(t, i, j, l)) return;
-  const Col c = col_reg(i, j, l);
-  const Met m = met_of(false);
-  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
-  const double r = cC.rscale;
-  const double gx = P2(cG.GRD_x, 0, i, j, l) / r, gy = P2(cG.GRD_x, 1, i, j, l) / r, gz = P2(cG.GRD_x, 2, i, j, l) / r;
-  double gwc_prev = 0.0;
-  for (int k = 0; k < KA; ++k) {
-    int p = c.at(k);
-    if (k < kmin || k > kmax) {
-      a.gvx[p] = 0.0; a.gvy[p] = 0.0; a.gvz[p] = 0.0; a.gw[p] = 0.0;
-      continue;
-    }
-    double dv[3];
-    const double* vv[3] = {a.vvx, a.vvy, a.vvz};
-#pragma unroll
-    for (int s = 0; s < 3; ++s) {
-      const double* sc = vv[s];
-      dv[s] = advconv_reg(i, j, k, l, c, m, a.rvx, a.rvy, a.rvz, a.rw,
-                          [&](int q, int) -> double { return sc[q]; });
-    }
-    double rh = a.rg[p];
-    double dvx = dv[0] - (-2.0 * rh * (cC.OHM * a.vvy[p]));
-    double dvy = dv[1] - (2.0 * rh * (cC.OHM * a.vvx[p]));
-    double dvz = dv[2];
-    double prd = dvx * gx + dvy * gy + dvz * gz;
-    a.gvx[p] = dvx - prd * gx;
-    a.gvy[p] = dvy - prd * gy;
-    a.gvz[p] = dvz - prd * gz;
-    double gwc = prd * cC.alpha;
-    a.gw[p] = (k >= kmin + 1) ? (mc(m.C2W, c, 0, 2, k) * gwc + mc(m.C2W, c, 1, 2, k) * gwc_prev) : 0.0;
-    gwc_prev = gwc;
   }
 }
 
@@ -578,138 +541,15 @@ __device__ double diffusion_at(int i, int j, int k, int l, S scl, KH kh) {
   return inner;
 }
 
-__global__ void k_hdiff2(Six vt, const double* rhog, SixOut out) {
-  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
-  int i, j, l;
-  if (!col_of(t, i, j, l)) return;
-  const bool in = interior(i, j);
-  const double Kh = cC.Kh;
-  for (int k = 0; k < cD.KA; ++k) {
-    int p = ix(i, j, k, l);
-    for (int n = 0; n < 6; ++n) {
-      double v = 0.0;
-      if (in) {
-        const double* s = vt.f[n];
-        auto S = [&](int ii, int jj) { return s[ix(ii, jj, k, l)]; };
-        if (n < 4) {
-          v = lap7(i, j, k, l, [&](int ii, int jj, int kk) { return s[ix(ii, jj, kk, l)]; });
-        } else if (n == 4) {
-          v = diffusion_at(i, j, k, l, S, [&](int ii, int jj) { return rhog[ix(ii, jj, k, l)] * cC.CVdry * Kh; });
-        } else {
-          v = diffusion_at(i, j, k, l, S,
-                           [&](int ii, int jj) { return rhog[ix(ii, jj, k, l)] * cC.hdiff_fact_rho * Kh; });
-        }
-      }
-      out.f[n][p] = -v;
-    }
-  }
-}
-
-// Tiled second hyperdiffusion pass: one block per HD_DX x HD_DY tile of
-// interior cells, all levels.  Per level the haloed tile of the six
-// Laplacians and of rhog is staged in shared memory, the triangle gradients of
-// the temperature and density Laplacians are formed once (with the
-// singular-point fix at the (0,0) vertex), then each thread writes its cell's
-// four Laplacians and two Kh-weighted diffusions.  Halo cells are left to the
-// exchange that follows.  Arithmetic order is that of k_hdiff2.
+// Second hyperdiffusion pass, one block per (level, HD_DX x HD_DY tile) of
+// interior cells: the haloed tile of the six Laplacians and of rhog is staged
+// in shared memory, the triangle gradients of the temperature and density
+// Laplacians are formed once (with the singular-point fix at the (0,0)
+// vertex), then each thread writes its cell's four Laplacians and two
+// Kh-weighted diffusions (kernels/oprtlaplacian.py:41-55,
+// kernels/oprtdiffusion.py).  Halo cells are left to the exchange that follows.
 #define HD_DX 32
 #define HD_DY 8
-__global__ void __launch_bounds__(HD_DX * HD_DY, 2) k_hdiff2_t(Six vt, const double* rhog, SixOut out) {
-  constexpr int PX = HD_DX + 2, PY = HD_DY + 2, TX = HD_DX + 1, TY = HD_DY + 1;
-  __shared__ double s_f[6][PY * PX];
-  __shared__ double s_r[PY * PX];
-  __shared__ double s_t[2][6][TY * TX];   // field 4/5: tti x,y,z then ttj x,y,z
-  const int l = blockIdx.z;
-  const int i0 = 1 + blockIdx.x * HD_DX, j0 = 1 + blockIdx.y * HD_DY;
-  const int G = cD.G, gmax = cD.G - 2;
-  const int tid = threadIdx.x, tx = tid % HD_DX, ty = tid / HD_DX;
-  const int i = i0 + tx, j = j0 + ty;
-  const bool own = (i <= gmax) && (j <= gmax);
-  const double Kh = cC.Kh;
-  const double kfac[2] = {cC.CVdry, cC.hdiff_fact_rho};
-  for (int k = 0; k < cD.KA; ++k) {
-    for (int p = tid; p < PX * PY; p += blockDim.x) {
-      const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
-      const bool ok = ii < G && jj < G;
-      const int q = ok ? ix(ii, jj, k, l) : 0;
-#pragma unroll
-      for (int n = 0; n < 6; ++n) s_f[n][p] = ok ? vt.f[n][q] : 0.0;
-      s_r[p] = ok ? rhog[q] : 0.0;
-    }
-    __syncthreads();
-    for (int p = tid; p < TX * TY; p += blockDim.x) {
-      const int px = p % TX, py = p / TX;
-      const int ii = i0 - 1 + px, jj = j0 - 1 + py;
-      const bool ok = ii <= G - 2 && jj <= G - 2;
-      const int ia = py * PX + px, ib = ia + 1, ic = ia + PX + 1, id = ia + PX;
-#pragma unroll
-      for (int f = 0; f < 2; ++f) {
-        const double* s = s_f[4 + f];
-        const double s0 = s[ia], sip = s[ib], sd = s[ic], sjp = s[id];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          double ti = 0.0, tj = 0.0;
-          if (ok) {
-            const double c1i = P2(cG.coef_intp, (d * 3 + 0) * 2 + 0, ii, jj, l);
-            const double c2i = P2(cG.coef_intp, (d * 3 + 1) * 2 + 0, ii, jj, l);
-            const double c3i = P2(cG.coef_intp, (d * 3 + 2) * 2 + 0, ii, jj, l);
-            const double c1j = P2(cG.coef_intp, (d * 3 + 0) * 2 + 1, ii, jj, l);
-            const double c2j = P2(cG.coef_intp, (d * 3 + 1) * 2 + 1, ii, jj, l);
-            const double c3j = P2(cG.coef_intp, (d * 3 + 2) * 2 + 1, ii, jj, l);
-            ti = ((2.0 * c1i - c2i - c3i) * s0 + (-c1i + 2.0 * c2i - c3i) * sip + (-c1i - c2i + 2.0 * c3i) * sd) / 3.0;
-            tj = ((2.0 * c1j - c2j - c3j) * s0 + (-c1j + 2.0 * c2j - c3j) * sd + (-c1j - c2j + 2.0 * c3j) * sjp) / 3.0;
-          }
-          s_t[f][d][p] = ti;
-          s_t[f][3 + d][p] = tj;
-        }
-      }
-    }
-    __syncthreads();
-    if (i0 == 1 && j0 == 1 && tid < 6) {   // singular-point fix of the (0,0) triangle, fields 4 and 5
-      const int f = tid / 3, d = tid % 3;
-      const double m0 = (double)cG.pntmask[l * 2 + 0], m1 = (double)cG.pntmask[l * 2 + 1];
-      s_t[f][d][0] = s_t[f][d][0] * m0 + s_t[f][3 + d][1] * m1;
-    }
-    __syncthreads();
-    if (own) {
-      const int q = ix(i, j, k, l);
-      const int c0 = (ty + 1) * PX + (tx + 1);
-      const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
-#pragma unroll
-      for (int n = 0; n < 4; ++n) {
-        double v = P2(cG.coef_lap, 0, i, j, l) * s_f[n][nb[0]];
-#pragma unroll
-        for (int m = 1; m < 7; ++m) v = v + P2(cG.coef_lap, m, i, j, l) * s_f[n][nb[m]];
-        out.f[n][q] = -v;
-      }
-      const int ta = (ty + 1) * TX + (tx + 1), tb = ta - 1, tc = ta - TX - 1, td = ta - TX;
-#pragma unroll
-      for (int f = 0; f < 2; ++f) {
-        auto kh = [&](int pt) { return s_r[pt] * kfac[f] * Kh; };
-        const double kh0 = kh(nb[0]);
-        const double kf1 = 0.5 * (kh0 + kh(nb[2])), kf2 = 0.5 * (kh0 + kh(nb[3])), kf3 = 0.5 * (kh0 + kh(nb[4]));
-        const double kf4 = 0.5 * (kh0 + kh(nb[5])), kf5 = 0.5 * (kh0 + kh(nb[6])), kf6 = 0.5 * (kh0 + kh(nb[1]));
-        double inner = 0.0;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const double aTI = s_t[f][d][ta], aTJ = s_t[f][3 + d][ta], bTI = s_t[f][d][tb];
-          const double cTI = s_t[f][d][tc], cTJ = s_t[f][3 + d][tc], dTJ = s_t[f][3 + d][td];
-          const double cd0 = P2(cG.coef_diff, d * 6 + 0, i, j, l), cd1 = P2(cG.coef_diff, d * 6 + 1, i, j, l),
-                       cd2 = P2(cG.coef_diff, d * 6 + 2, i, j, l), cd3 = P2(cG.coef_diff, d * 6 + 3, i, j, l),
-                       cd4 = P2(cG.coef_diff, d * 6 + 4, i, j, l), cd5 = P2(cG.coef_diff, d * 6 + 5, i, j, l);
-          const double blk = kf1 * cd0 * (aTI + aTJ) + kf2 * cd1 * (aTJ + bTI) + kf3 * cd2 * (bTI + cTJ) +
-                             kf4 * cd3 * (cTJ + cTI) + kf5 * cd4 * (cTI + dTJ) + kf6 * cd5 * (dTJ + aTI);
-          inner = (d == 0) ? blk : inner + blk;
-        }
-        out.f[4 + f][q] = -inner;
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// Second hyperdiffusion pass, one block per (level, tile): same staging,
-// triangle gradients and arithmetic as k_hdiff2_t, without the level loop.
 __global__ void __launch_bounds__(HD_DX * HD_DY, 4) k_hdiff2_l(Six vt, const double* rhog, SixOut out) {
   constexpr int PX = HD_DX + 2, PY = HD_DY + 2, TX = HD_DX + 1, TY = HD_DY + 1;
   __shared__ double s_f[6][PY * PX];

@@ -13,52 +13,6 @@ struct Four { const double* f[4]; };   // rhogvx, rhogvy, rhogvz, rhogw
 struct Three { double* f[3]; };
 struct CThree { const double* f[3]; };
 
-// half-level vertical mass flux rhogw_vm at (ii,jj,k) (kernels/oprt3ddivdamp.py:50-82)
-__device__ __forceinline__ double rwv_at(const Four& v, int ii, int jj, int k, int l) {
-  if (k <= cD.kmin || k > cD.kmax) return 0.0;
-  int q = ix(ii, jj, k, l), qm = ix(ii, jj, k - 1, l);
-  const int n = cD.npti;
-  const double* cz = cG.C2WGz;
-  double h = cz[q] * v.f[0][q] + cz[n + q] * v.f[0][qm] + cz[2 * n + q] * v.f[1][q] + cz[3 * n + q] * v.f[1][qm] +
-             cz[4 * n + q] * v.f[2][q] + cz[5 * n + q] * v.f[2][qm];
-  return h * cG.RGAMH[q] + v.f[3][q] * cG.RGSQRTH[q];
-}
-
-// sclt_TI / sclt_TJ at vertex (ii,jj) and level k (interior-k only)
-__device__ void sclt3d(const Four& v, int ii, int jj, int k, int l, double& sTI, double& sTJ) {
-  int a = ix(ii, jj, k, l), b = ix(ii + 1, jj, k, l), c = ix(ii + 1, jj + 1, k, l), d = ix(ii, jj + 1, k, l);
-  double vx[4], vy[4], vz[4];
-  int pts[4] = {a, b, c, d};
-#pragma unroll
-  for (int n = 0; n < 4; ++n) {
-    double rg = cG.RGAM[pts[n]];
-    vx[n] = v.f[0][pts[n]] * rg;
-    vy[n] = v.f[1][pts[n]] * rg;
-    vz[n] = v.f[2][pts[n]] * rg;
-  }
-  auto C = [&](int dir, int p, int t) { return P2(cG.coef_intp, (dir * 3 + p) * 2 + t, ii, jj, l); };
-  double rdz = cC.rdgz[k];
-  double wTI = ((rwv_at(v, ii, jj, k + 1, l) + rwv_at(v, ii + 1, jj, k + 1, l) + rwv_at(v, ii + 1, jj + 1, k + 1, l)) -
-                (rwv_at(v, ii, jj, k, l) + rwv_at(v, ii + 1, jj, k, l) + rwv_at(v, ii + 1, jj + 1, k, l))) / 3.0 * rdz;
-  double wTJ = ((rwv_at(v, ii, jj, k + 1, l) + rwv_at(v, ii + 1, jj + 1, k + 1, l) + rwv_at(v, ii, jj + 1, k + 1, l)) -
-                (rwv_at(v, ii, jj, k, l) + rwv_at(v, ii + 1, jj + 1, k, l) + rwv_at(v, ii, jj + 1, k, l))) / 3.0 * rdz;
-  sTI = C(0, 0, 0) * vx[0] + C(0, 1, 0) * vx[1] + C(0, 2, 0) * vx[2] + C(1, 0, 0) * vy[0] + C(1, 1, 0) * vy[1] +
-        C(1, 2, 0) * vy[2] + C(2, 0, 0) * vz[0] + C(2, 1, 0) * vz[1] + C(2, 2, 0) * vz[2] + wTI;
-  sTJ = C(0, 0, 1) * vx[0] + C(0, 1, 1) * vx[2] + C(0, 2, 1) * vx[3] + C(1, 0, 1) * vy[0] + C(1, 1, 1) * vy[2] +
-        C(1, 2, 1) * vy[3] + C(2, 0, 1) * vz[0] + C(2, 1, 1) * vz[2] + C(2, 2, 1) * vz[3] + wTJ;
-}
-
-// sclt pair at a vertex including the singular-point fix at (0,0)
-template <class SC>
-__device__ __forceinline__ void sclt_fixed(SC sc, int ii, int jj, int l, double& sTI, double& sTJ) {
-  sc(ii, jj, sTI, sTJ);
-  if (ii == 0 && jj == 0) {
-    double tI10, tJ10;
-    sc(1, 0, tI10, tJ10);
-    sTI = sTI * (double)cG.pntmask[l * 2 + 0] + tJ10 * (double)cG.pntmask[l * 2 + 1];
-  }
-}
-
 // the six-edge divergence-damping combination for direction d at (i,j)
 // (kernels/oprtdivdamp.py:110-120)
 __device__ __forceinline__ double ddivd(int i, int j, int l, int d, const double aTI, const double aTJ,
@@ -68,37 +22,25 @@ __device__ __forceinline__ double ddivd(int i, int j, int l, int d, const double
          P2(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) + P2(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI);
 }
 
-__global__ void k_dd3d(Four v, Three out) {
-  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
-  int i, j, l;
-  if (!col_of(t, i, j, l)) return;
-  const bool in = interior(i, j);   // output rows 1..gmax == interior
-  for (int k = 0; k < cD.KA; ++k) {
-    int p = ix(i, j, k, l);
-    if (!in || k < cD.kmin || k > cD.kmax) {
-      out.f[0][p] = 0.0; out.f[1][p] = 0.0; out.f[2][p] = 0.0;
-      continue;
-    }
-    auto sc = [&](int ii, int jj, double& a, double& b) { sclt3d(v, ii, jj, k, l, a, b); };
-    double aTI, aTJ, bTI, bTJ, cTI, cTJ, dTI, dTJ;
-    sclt_fixed(sc, i, j, l, aTI, aTJ);
-    sclt_fixed(sc, i - 1, j, l, bTI, bTJ);
-    sclt_fixed(sc, i - 1, j - 1, l, cTI, cTJ);
-    sclt_fixed(sc, i, j - 1, l, dTI, dTJ);
-    for (int d = 0; d < 3; ++d) out.f[d][p] = ddivd(i, j, l, d, aTI, aTJ, bTI, cTJ, cTI, dTJ);
-  }
-}
-
 // Tiled 3-D divergence damping: one block per DD_DX x DD_DY tile of output
 // cells of one region, marching upward in k.  Per level the block stages the
 // haloed tile of RGAM-scaled momentum and the vertical mass flux rwv(k+1) in
 // shared memory (rwv(k) is kept from the level below), evaluates every
 // triangle value once, applies the singular-point fix, then each thread forms
-// its cell's three components.  Arithmetic and association order are those of
-// k_dd3d (the untiled form kept for reference and the pole-adjacent checks).
+// its cell's three components.  Per triangle: the RGAM-weighted momenta at
+// its three vertices against coef_intp plus the vertical flux difference
+// ((rwv(k+1) summed over the vertices) - (rwv(k) summed)) / 3 * rdgz(k)
+// (kernels/oprt3ddivdamp.py:50-173); the rwv sums and coefficient products
+// are added left to right in the reference's order.
+#ifndef DD_DX
 #define DD_DX 32
+#endif
+#ifndef DD_DY
 #define DD_DY 8
-__global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_dd3d_t(Four v, Three out) {
+#endif
+// resident blocks per SM for a register budget of n blocks of 256 threads
+#define DD_MINB(n) ((n) * 256 / (DD_DX * DD_DY) > 0 ? (n) * 256 / (DD_DX * DD_DY) : 1)
+__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(4)) k_dd3d_t(Four v, Three out) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2;   // points i0-1 .. i0+DX, j0-1 .. j0+DY
   constexpr int TX = DD_DX + 1, TY = DD_DY + 1;   // triangles i0-1 .. i0+DX-1, j0-1 .. j0+DY-1
   __shared__ double s_vm[3][PY * PX];
@@ -189,94 +131,15 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_dd3d_t(Four v, Three out) 
 struct TileLv {
   int k, l, i0, j0;
 };
+template <int TDX, int TDY>
 __device__ __forceinline__ TileLv tile_level(int kbase) {
-  const int ntx = (cD.G - 2 + DD_DX - 1) / DD_DX;
+  const int ntx = (cD.G - 2 + TDX - 1) / TDX;
   TileLv t;
   t.k = kbase + (int)blockIdx.x;
   t.l = (int)blockIdx.z;
-  t.i0 = 1 + ((int)blockIdx.y % ntx) * DD_DX;
-  t.j0 = 1 + ((int)blockIdx.y / ntx) * DD_DY;
+  t.i0 = 1 + ((int)blockIdx.y % ntx) * TDX;
+  t.j0 = 1 + ((int)blockIdx.y / ntx) * TDY;
   return t;
-}
-
-// 3-D divergence damping, one block per (level, tile): the haloed tile of
-// RGAM-scaled momentum and of the vertical mass flux at k and k+1 is staged,
-// every triangle value formed once (singular-point fix at the (0,0) vertex),
-// then each thread writes its cell.  Same arithmetic as k_dd3d.
-__global__ void __launch_bounds__(DD_DX * DD_DY, 3) k_dd3d_l(Four v, Three out) {
-  constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
-  __shared__ double s_vm[3][PY * PX];
-  __shared__ double s_rd[PY * PX], s_ru[PY * PX];
-  __shared__ double s_ti[TY * TX], s_tj[TY * TX];
-  const TileLv tl = tile_level(cD.kmin);
-  const int k = tl.k, l = tl.l, i0 = tl.i0, j0 = tl.j0;
-  const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin, kmax = cD.kmax;
-  const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
-  const int n = cD.npti;
-  const double* cz = cG.C2WGz;
-  auto rwv = [&](int q, int qm) {
-    const double h = cz[q] * v.f[0][q] + cz[n + q] * v.f[0][qm] + cz[2 * n + q] * v.f[1][q] +
-                     cz[3 * n + q] * v.f[1][qm] + cz[4 * n + q] * v.f[2][q] + cz[5 * n + q] * v.f[2][qm];
-    return h * cG.RGAMH[q] + v.f[3][q] * cG.RGSQRTH[q];
-  };
-  for (int p = tid; p < PX * PY; p += blockDim.x) {
-    const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
-    double a = 0.0, b = 0.0, c = 0.0, rd = 0.0, ru = 0.0;
-    if (ii < G && jj < G) {
-      const int q = ix(ii, jj, k, l);
-      const double rg = cG.RGAM[q];
-      a = v.f[0][q] * rg;
-      b = v.f[1][q] * rg;
-      c = v.f[2][q] * rg;
-      if (k > kmin) rd = rwv(q, q - cD.planei);
-      if (k + 1 <= kmax) ru = rwv(q + cD.planei, q);
-    }
-    s_vm[0][p] = a;
-    s_vm[1][p] = b;
-    s_vm[2][p] = c;
-    s_rd[p] = rd;
-    s_ru[p] = ru;
-  }
-  __syncthreads();
-  const double rdz = cC.rdgz[k];
-  for (int p = tid; p < TX * TY; p += blockDim.x) {
-    const int px = p % TX, py = p / TX;
-    const int ii = i0 - 1 + px, jj = j0 - 1 + py;
-    double sTI = 0.0, sTJ = 0.0;
-    if (ii <= G - 2 && jj <= G - 2) {
-      const int a = py * PX + px, b = a + 1, c = a + PX + 1, d = a + PX;
-      auto C = [&](int dir, int pt, int t) { return P2(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
-      const double wTI = ((s_ru[a] + s_ru[b] + s_ru[c]) - (s_rd[a] + s_rd[b] + s_rd[c])) / 3.0 * rdz;
-      const double wTJ = ((s_ru[a] + s_ru[c] + s_ru[d]) - (s_rd[a] + s_rd[c] + s_rd[d])) / 3.0 * rdz;
-      sTI = C(0, 0, 0) * s_vm[0][a] + C(0, 1, 0) * s_vm[0][b] + C(0, 2, 0) * s_vm[0][c] +
-            C(1, 0, 0) * s_vm[1][a] + C(1, 1, 0) * s_vm[1][b] + C(1, 2, 0) * s_vm[1][c] +
-            C(2, 0, 0) * s_vm[2][a] + C(2, 1, 0) * s_vm[2][b] + C(2, 2, 0) * s_vm[2][c] + wTI;
-      sTJ = C(0, 0, 1) * s_vm[0][a] + C(0, 1, 1) * s_vm[0][c] + C(0, 2, 1) * s_vm[0][d] +
-            C(1, 0, 1) * s_vm[1][a] + C(1, 1, 1) * s_vm[1][c] + C(1, 2, 1) * s_vm[1][d] +
-            C(2, 0, 1) * s_vm[2][a] + C(2, 1, 1) * s_vm[2][c] + C(2, 2, 1) * s_vm[2][d] + wTJ;
-    }
-    s_ti[p] = sTI;
-    s_tj[p] = sTJ;
-  }
-  __syncthreads();
-  if (tid == 0 && i0 == 1 && j0 == 1)
-    s_ti[0] = s_ti[0] * (double)cG.pntmask[l * 2 + 0] + s_tj[1] * (double)cG.pntmask[l * 2 + 1];
-  __syncthreads();
-  const int i = i0 + tx, j = j0 + ty;
-  if (i <= gmax && j <= gmax) {
-    const int ta = (ty + 1) * TX + (tx + 1);
-    const double aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
-    const double cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1], dTJ = s_tj[ta - TX];
-    const int q = ix(i, j, k, l);
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-      out.f[d][q] = P2(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) +
-                    P2(cG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
-                    P2(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) +
-                    P2(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
-                    P2(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) +
-                    P2(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI);
-  }
 }
 
 // pole 3-D divergence damping (kernels/oprt3ddivdamp.py:176-237)
@@ -574,7 +437,7 @@ __device__ void vp0_column(const Vp0Args& a, int i, int j, int l, int g, int lp)
   }
 }
 
-// Horizontal terms of vp0, tiled like k_path1_t: for interior cells and
+// Horizontal terms of vp0, tiled like k_path1_l: for interior cells and
 // levels kmin..kmax, the divergences of RGAM*rhogv and RGAM*rhogv*eth
 // (div1, div2), the 2-D divergence damping of -vtmp2 (dd) and the pressure
 // gradient of pregd (dpg), written to eight work fields for the column kernel.
@@ -582,157 +445,22 @@ struct Vp0H {
   double* out[8];               // div1, div2, dd x/y/z, dpg x/y/z
 };
 
-__global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_vp0_h(Vp0Args a, Vp0H h) {
-  constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
+// vp0 horizontal terms, one block per (level, tile).
+// vp0 keeps a 32x8 tile: its staged fields need more than the 48 KB of
+// static shared memory at larger tiles
+#define VP_DX 32
+#define VP_DY 8
+__global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) {
+  constexpr int PX = VP_DX + 2, PY = VP_DY + 2, TX = VP_DX + 1, TY = VP_DY + 1;
   __shared__ double s_m[3][PY * PX];    // RGAM * rhogv
   __shared__ double s_e[3][PY * PX];    // RGAM * rhogv * eth
   __shared__ double s_v[3][PY * PX];    // -vtmp2
   __shared__ double s_p[PY * PX];       // RGAM * pregd at the gradient level
   __shared__ double s_ti[TY * TX], s_tj[TY * TX];
-  const int l = blockIdx.z;
-  const int i0 = 1 + blockIdx.x * DD_DX, j0 = 1 + blockIdx.y * DD_DY;
-  const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin, kmax = cD.kmax;
-  const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
-  const int i = i0 + tx, j = j0 + ty;
-  const bool own = (i <= gmax) && (j <= gmax);
-  const double ddc = cC.divdamp_coef, r = cC.rscale;
-  const int n = cD.npti;
-  const double* cz = cG.C2WGz;
-  const double* const* P = a.P.v;
-  double gxyz[3] = {0.0, 0.0, 0.0};
-  int q0 = 0;
-  if (own) {
-#pragma unroll
-    for (int d = 0; d < 3; ++d) gxyz[d] = P2(cG.GRD_x, d, i, j, l);
-    q0 = ix(i, j, 0, l);
-  }
-  for (int k = kmin; k <= kmax; ++k) {
-    const int kk = (k == kmin) ? kmin + 1 : k;
-    for (int p = tid; p < PX * PY; p += blockDim.x) {
-      const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
-      double mv[3] = {0.0, 0.0, 0.0}, ev[3] = {0.0, 0.0, 0.0}, vv[3] = {0.0, 0.0, 0.0}, pp = 0.0;
-      if (ii < G && jj < G) {
-        const int q = ix(ii, jj, k, l);
-        const double rg = cG.RGAM[q], e = a.eth[q];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const double pv = P[1 + d][q];
-          mv[d] = pv * rg;
-          ev[d] = (pv * e) * rg;
-          vv[d] = -a.vt.f[d][q];
-        }
-        const int qk = ix(ii, jj, kk, l);
-        pp = a.pregd[qk] * cG.RGAM[qk];
-      }
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        s_m[d][p] = mv[d];
-        s_e[d][p] = ev[d];
-        s_v[d][p] = vv[d];
-      }
-      s_p[p] = pp;
-    }
-    __syncthreads();
-    for (int p = tid; p < TX * TY; p += blockDim.x) {
-      const int px = p % TX, py = p / TX;
-      const int ii = i0 - 1 + px, jj = j0 - 1 + py;
-      double sTI = 0.0, sTJ = 0.0;
-      if (ii <= G - 2 && jj <= G - 2) {
-        const int ia = py * PX + px, ib = ia + 1, ic = ia + PX + 1, id = ia + PX;
-        auto C = [&](int dir, int pt, int t) { return P2(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
-        sTI = C(0, 0, 0) * s_v[0][ia] + C(0, 1, 0) * s_v[0][ib] + C(0, 2, 0) * s_v[0][ic] +
-              C(1, 0, 0) * s_v[1][ia] + C(1, 1, 0) * s_v[1][ib] + C(1, 2, 0) * s_v[1][ic] +
-              C(2, 0, 0) * s_v[2][ia] + C(2, 1, 0) * s_v[2][ib] + C(2, 2, 0) * s_v[2][ic];
-        sTJ = C(0, 0, 1) * s_v[0][ia] + C(0, 1, 1) * s_v[0][ic] + C(0, 2, 1) * s_v[0][id] +
-              C(1, 0, 1) * s_v[1][ia] + C(1, 1, 1) * s_v[1][ic] + C(1, 2, 1) * s_v[1][id] +
-              C(2, 0, 1) * s_v[2][ia] + C(2, 1, 1) * s_v[2][ic] + C(2, 2, 1) * s_v[2][id];
-      }
-      s_ti[p] = sTI;
-      s_tj[p] = sTJ;
-    }
-    __syncthreads();
-    if (own) {
-      const int c0 = (ty + 1) * PX + (tx + 1);
-      const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
-      const int q = q0 + (int)k * cD.planei;
-      // divergences (div7: per direction left to right, then x + y + z)
-      double acc1[3], acc2[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        double s1 = 0.0, s2 = 0.0;
-#pragma unroll
-        for (int m = 0; m < 7; ++m) {
-          const double cdv = P2(cG.coef_div, d * 7 + m, i, j, l);
-          const double t1 = cdv * s_m[d][nb[m]], t2 = cdv * s_e[d][nb[m]];
-          s1 = (m == 0) ? t1 : s1 + t1;
-          s2 = (m == 0) ? t2 : s2 + t2;
-        }
-        acc1[d] = s1;
-        acc2[d] = s2;
-      }
-      h.out[0][q] = acc1[0] + acc1[1] + acc1[2];
-      h.out[1][q] = acc2[0] + acc2[1] + acc2[2];
-      // 2-D divergence damping, projected
-      const int ta = (ty + 1) * TX + (tx + 1);
-      const double aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
-      const double cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1], dTJ = s_tj[ta - TX];
-      double dd[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d)
-        dd[d] = ddc * (P2(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) +
-                       P2(cG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
-                       P2(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) +
-                       P2(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
-                       P2(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) +
-                       P2(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI));
-      {
-        const double prd = (dd[0] * gxyz[0] + dd[1] * gxyz[1] + dd[2] * gxyz[2]) / r;
-        dd[0] = dd[0] - prd * gxyz[0] / r;
-        dd[1] = dd[1] - prd * gxyz[1] / r;
-        dd[2] = dd[2] - prd * gxyz[2] / r;
-      }
-      // pressure gradient of pregd at level kk
-      const int qkk = q0 + (int)kk * cD.planei, qk1 = qkk + cD.planei, qkm = qkk - cD.planei;
-      const double P_k1 = a.pregd[qk1], P_k = a.pregd[qkk], P_km = a.pregd[qkm];
-      const double rgh1 = cG.RGAMH[qk1], rgh0 = cG.RGAMH[qkk];
-      double pg[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        double g = P2(cG.coef_grad, d * 7 + 0, i, j, l) * s_p[nb[0]];
-#pragma unroll
-        for (int m = 1; m < 7; ++m) g = g + P2(cG.coef_grad, d * 7 + m, i, j, l) * s_p[nb[m]];
-        const double up = (cz[(2 * d) * n + qk1] * P_k1 + cz[(2 * d + 1) * n + qk1] * P_k) * rgh1;
-        const double dn = (cz[(2 * d) * n + qkk] * P_k + cz[(2 * d + 1) * n + qkk] * P_km) * rgh0;
-        pg[d] = g + (up - dn) * cC.rdgz[kk];
-      }
-      {
-        const double prd = (pg[0] * gxyz[0] + pg[1] * gxyz[1] + pg[2] * gxyz[2]) / r;
-        pg[0] = pg[0] - prd * gxyz[0] / r;
-        pg[1] = pg[1] - prd * gxyz[1] / r;
-        pg[2] = pg[2] - prd * gxyz[2] / r;
-      }
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        h.out[2 + d][q] = dd[d];
-        h.out[5 + d][q] = pg[d];
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// vp0 horizontal terms, one block per (level, tile) (body of k_vp0_h).
-__global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) {
-  constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
-  __shared__ double s_m[3][PY * PX];    // RGAM * rhogv
-  __shared__ double s_e[3][PY * PX];    // RGAM * rhogv * eth
-  __shared__ double s_v[3][PY * PX];    // -vtmp2
-  __shared__ double s_p[PY * PX];       // RGAM * pregd at the gradient level
-  __shared__ double s_ti[TY * TX], s_tj[TY * TX];
-  const TileLv tl = tile_level(cD.kmin);
+  const TileLv tl = tile_level<VP_DX, VP_DY>(cD.kmin);
   const int l = tl.l, i0 = tl.i0, j0 = tl.j0;
   const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin, kmax = cD.kmax;
-  const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
+  const int tid = threadIdx.x, tx = tid % VP_DX, ty = tid / VP_DX;
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= gmax) && (j <= gmax);
   const double ddc = cC.divdamp_coef, r = cC.rscale;
@@ -864,89 +592,14 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) 
 
 // Column part of vp0 for every regional column: vertical flux convergences,
 // small-step tendencies, the implicit matrix and ethtot0, with the horizontal
-// terms read from k_vp0_h (zero on halo columns and outside kmin..kmax, where
+// terms read from k_vp0_hl (zero on halo columns and outside kmin..kmax, where
 // the values that depend on them are replaced by the halo exchanges or the
-// boundary rows before they are read).
-__global__ void __launch_bounds__(128) k_vp0_c(Vp0Args a, Vp0H h) {
-  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
-  int i, j, l;
-  if (!col_of(t, i, j, l)) return;
-  const Col c = col_reg(i, j, l);
-  const Met m = met_of(false);
-  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
-  const bool in = interior(i, j);
-  const double* const* P = a.P.v;
-  const double dt = a.dt;
-  auto rhog_h = [&](int k) -> double {
-    int kk = (k < kmin) ? kmin : k;
-    return mc(m.C2W, c, 0, 2, kk) * P[0][c.at(kk)] + mc(m.C2W, c, 1, 2, kk) * P[0][c.at(kk - 1)];
-  };
-  auto eth_h = [&](int k) -> double {
-    int kk = (k < kmin) ? kmin : k;
-    return cC.afact[kk] * a.eth[c.at(kk)] + cC.bfact[kk] * a.eth[c.at(kk - 1)];
-  };
-  auto dbuo = [&](int k) -> double {
-    if (k < kmin + 1 || k > kmax) return 0.0;
-    return -cC.GRAV * (mc(m.C2W, c, 0, 2, k) * a.rhogd[c.at(k)] + mc(m.C2W, c, 1, 2, k) * a.rhogd[c.at(k - 1)]);
-  };
-  auto dpgw = [&](int k) -> double { return presgradw(c, m, k, [&](int kk) { return a.pregd[c.at(kk)]; }); };
-  auto gz = [&](int k) -> double { return cC.GRAV - (dpgw(k) - dbuo(k)) / rhog_h(k); };
-  auto pwh = [&](int k) -> double { return -gz(k) * P[4][c.at(k)]; };
-  auto PF = [&](int k, int d) -> double { return P[1 + d][c.at(k)]; };
-  auto PEF = [&](int k, int d) -> double { return P[1 + d][c.at(k)] * a.eth[c.at(k)]; };
-  for (int k = 0; k < KA; ++k) {
-    const int p = c.at(k);
-    const bool hk = in && k >= kmin && k <= kmax;
-    const double div1 = hk ? h.out[0][p] : 0.0, div2 = hk ? h.out[1][p] : 0.0;
-    const double drhog = fluxconv_col(c, m, k, div1, 1.0, PF, [&](int kk) { return P[4][c.at(kk)]; });
-    const double drhoge = fluxconv_col(c, m, k, div2, 1.0, PEF, [&](int kk) {
-      int q = c.at(kk);
-      return P[4][q] * (cC.afact[kk] * a.eth[q] + cC.bfact[kk] * a.eth[c.at(kk - 1)]);
-    });
-    double dd[3], dpg[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      dd[d] = hk ? h.out[2 + d][p] : 0.0;
-      dpg[d] = hk ? h.out[5 + d][p] : 0.0;
-    }
-    double pw = 0.0;
-    if (k >= kmin && k <= kmax)
-      pw = a.vx[p] * dpg[0] + a.vy[p] * dpg[1] + a.vz[p] * dpg[2] + mc(m.W2C, c, 0, 2, k) * pwh(k + 1) +
-           mc(m.W2C, c, 1, 2, k) * pwh(k);
-    a.gT[0][p] = a.gT0[0][p] + drhog;
-    a.gT[1][p] = a.gT0[1][p] - dpg[0] + dd[0] + 0.0;
-    a.gT[2][p] = a.gT0[2][p] - dpg[1] + dd[1] + 0.0;
-    a.gT[3][p] = a.gT0[3][p] - dpg[2] + dd[2] + 0.0;
-    a.gT[4][p] = a.gT0[4][p] + 0.0 * cC.alpha - dpgw(k) + dbuo(k);
-    a.gT[5][p] = a.gT0[5][p] + drhoge + pw;
-    if (k >= kmin + 1 && k <= kmax) {
-      const double GCVovR = cC.GRAV * cC.CVdry / cC.Rdry;
-      const double ACVovRt2 = cC.alpha * cC.CVdry / cC.Rdry / (dt * dt);
-      int pm = c.at(k - 1), pp = c.at(k + 1);
-      double rg = cC.rdgz[k], rgm = cC.rdgz[k - 1];
-      double Ca = (m.RGSGAM2[p] * rg + m.RGSGAM2[pm] * rgm) * m.GAM2H[p];
-      double Cb = cC.dfact[k] - cC.cfact[k - 1];
-      double Cu1 = m.RGSGAM2[p] * rg * m.GAM2H[pp];
-      double rgh2 = m.RGAMH[p] * m.RGAMH[p];
-      double Cu2 = m.GAM2H[pp] * rgh2 * GCVovR;
-      double Cl1 = m.RGSGAM2[p] * rg * m.GAM2H[pm];
-      double Cl2 = m.GAM2H[pm] * rgh2 * GCVovR;
-      double rgh = cC.rdgzh[k];
-      a.Mc[p] = ACVovRt2 / m.RGSQRTH[p] + rgh * (Ca * eth_h(k) - Cb * (gz(k) + GCVovR));
-      a.Mu[p] = -rgh * (Cu1 * eth_h(k + 1) + cC.cfact[k] * (gz(k + 1) + Cu2));
-      a.Ml[p] = -rgh * (Cl1 * eth_h(k - 1) - cC.dfact[k - 1] * (gz(k - 1) + Cl2));
-    }
-    double kin0 = rhogkin_at(c, m, k, [&](int kk, int comp) { return P[comp][c.at(kk)]; });
-    a.ethtot0[p] = a.eth[p] + kin0 / P[0][p] + m.PHI[p];
-  }
-}
-
-// k_vp0_c marching upward with every half-level quantity evaluated once per
-// column: at level k the values at k+1 (vertical mass and energy fluxes,
-// buoyancy, vertical pressure gradient, gz, pwh, half-level eth, the vertical
-// kinetic-energy term) are formed and the ones at k and k-1 are carried in
-// registers.  Each value is the same expression as in k_vp0_c, so the results
-// are identical.
+// boundary rows before they are read).  The column marches upward with every
+// half-level quantity evaluated once: at level k the values at k+1 (vertical
+// mass and energy fluxes, buoyancy, vertical pressure gradient, gz, pwh,
+// half-level eth, the vertical kinetic-energy term) are formed and the ones at
+// k and k-1 are carried in registers.  Each value is the expression of
+// vp0_column (the pole form), so regional and pole columns round alike.
 __global__ void __launch_bounds__(128) k_vp0_cr(Vp0Args a, Vp0H h) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
@@ -1114,155 +767,15 @@ __device__ void path1_column(const Path1Args& a, int i, int j, int l, int g, int
   }
 }
 
-// Tiled regional path 1: one block per DD_DX x DD_DY tile of interior cells,
-// marching over k.  Per level the haloed tile of -vtmp2 (2-D divergence
-// damping) and of the RGAM-weighted split pressure at the gradient level kk
-// are staged in shared memory and every triangle value is formed once.  Halo
-// cells are not computed: diff_vh is exchanged right after this kernel and
-// the running means are exchanged before they are read off the interior.
-// Arithmetic and association order are those of path1_column.
-__global__ void __launch_bounds__(DD_DX * DD_DY, 2) k_path1_t(Path1Args a) {
-  constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
-  __shared__ double s_v[3][PY * PX];
-  __shared__ double s_p[PY * PX];
-  __shared__ double s_ti[TY * TX], s_tj[TY * TX];
-  const int l = blockIdx.z;
-  const int i0 = 1 + blockIdx.x * DD_DX, j0 = 1 + blockIdx.y * DD_DY;
-  const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin, kmax = cD.kmax;
-  const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
-  const int i = i0 + tx, j = j0 + ty;
-  const bool own = (i <= gmax) && (j <= gmax);
-  const double dt = a.dt, RovCV = a.RovCV, rweight = a.rweight, ddc = cC.divdamp_coef, r = cC.rscale;
-  const int n = cD.npti;
-  const double* cz = cG.C2WGz;
-  double cd[3][6], gxyz[3] = {0.0, 0.0, 0.0};
-  int q0 = 0;
-  if (own) {
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      gxyz[d] = P2(cG.GRD_x, d, i, j, l);
-#pragma unroll
-      for (int m = 0; m < 6; ++m) cd[d][m] = P2(cG.coef_diff, d * 6 + m, i, j, l);
-    }
-    q0 = ix(i, j, 0, l);
-  }
-  auto Pown = [&](int kk) {   // split pressure of the own column, boundary rows clamped
-    const int k2 = kk < kmin ? kmin : (kk > kmax ? kmax : kk);
-    return a.PS[5][q0 + (int)k2 * cD.planei] * RovCV;
-  };
-  double vals[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
-  for (int k = kmin; k <= kmax; ++k) {
-    const int kk = (k == kmin) ? kmin + 1 : k;
-    for (int p = tid; p < PX * PY; p += blockDim.x) {
-      const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
-      double x = 0.0, y = 0.0, z = 0.0, pp = 0.0;
-      if (ii < G && jj < G) {
-        const int q = ix(ii, jj, k, l);
-        x = -a.vt.f[0][q];
-        y = -a.vt.f[1][q];
-        z = -a.vt.f[2][q];
-        const int qk = ix(ii, jj, kk, l);
-        pp = a.PS[5][qk] * RovCV * cG.RGAM[qk];
-      }
-      s_v[0][p] = x;
-      s_v[1][p] = y;
-      s_v[2][p] = z;
-      s_p[p] = pp;
-    }
-    __syncthreads();
-    for (int p = tid; p < TX * TY; p += blockDim.x) {
-      const int px = p % TX, py = p / TX;
-      const int ii = i0 - 1 + px, jj = j0 - 1 + py;
-      double sTI = 0.0, sTJ = 0.0;
-      if (ii <= G - 2 && jj <= G - 2) {
-        const int ia = py * PX + px, ib = ia + 1, ic = ia + PX + 1, id = ia + PX;
-        auto C = [&](int dir, int pt, int t) { return P2(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
-        sTI = C(0, 0, 0) * s_v[0][ia] + C(0, 1, 0) * s_v[0][ib] + C(0, 2, 0) * s_v[0][ic] +
-              C(1, 0, 0) * s_v[1][ia] + C(1, 1, 0) * s_v[1][ib] + C(1, 2, 0) * s_v[1][ic] +
-              C(2, 0, 0) * s_v[2][ia] + C(2, 1, 0) * s_v[2][ib] + C(2, 2, 0) * s_v[2][ic];
-        sTJ = C(0, 0, 1) * s_v[0][ia] + C(0, 1, 1) * s_v[0][ic] + C(0, 2, 1) * s_v[0][id] +
-              C(1, 0, 1) * s_v[1][ia] + C(1, 1, 1) * s_v[1][ic] + C(1, 2, 1) * s_v[1][id] +
-              C(2, 0, 1) * s_v[2][ia] + C(2, 1, 1) * s_v[2][ic] + C(2, 2, 1) * s_v[2][id];
-      }
-      s_ti[p] = sTI;
-      s_tj[p] = sTJ;
-    }
-    __syncthreads();
-    if (own) {
-      const int ta = (ty + 1) * TX + (tx + 1);
-      const double aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
-      const double cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1], dTJ = s_tj[ta - TX];
-      double dd[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d)
-        dd[d] = ddc * (cd[d][0] * (aTI + aTJ) + cd[d][1] * (aTJ + bTI) + cd[d][2] * (bTI + cTJ) +
-                       cd[d][3] * (cTJ + cTI) + cd[d][4] * (cTI + dTJ) + cd[d][5] * (dTJ + aTI));
-      {
-        const double prd = (dd[0] * gxyz[0] + dd[1] * gxyz[1] + dd[2] * gxyz[2]) / r;
-        dd[0] = dd[0] - prd * gxyz[0] / r;
-        dd[1] = dd[1] - prd * gxyz[1] / r;
-        dd[2] = dd[2] - prd * gxyz[2] / r;
-      }
-      // pressure gradient at level kk: 7-point horizontal part + vertical part
-      const int c0 = (ty + 1) * PX + (tx + 1);
-      const double s7[7] = {s_p[c0], s_p[c0 + 1], s_p[c0 + PX + 1], s_p[c0 + PX], s_p[c0 - 1], s_p[c0 - PX - 1],
-                            s_p[c0 - PX]};
-      double pg[3];
-      const int qkk = q0 + (int)kk * cD.planei, qk1 = qkk + cD.planei;
-      const double P_k1 = Pown(kk + 1), P_k = Pown(kk), P_km = Pown(kk - 1);
-      const double rgh1 = cG.RGAMH[qk1], rgh0 = cG.RGAMH[qkk];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        double g = P2(cG.coef_grad, d * 7 + 0, i, j, l) * s7[0];
-#pragma unroll
-        for (int m = 1; m < 7; ++m) g = g + P2(cG.coef_grad, d * 7 + m, i, j, l) * s7[m];
-        const double up = (cz[(2 * d) * n + qk1] * P_k1 + cz[(2 * d + 1) * n + qk1] * P_k) * rgh1;
-        const double dn = (cz[(2 * d) * n + qkk] * P_k + cz[(2 * d + 1) * n + qkk] * P_km) * rgh0;
-        pg[d] = g + (up - dn) * cC.rdgz[kk];
-      }
-      {
-        const double prd = (pg[0] * gxyz[0] + pg[1] * gxyz[1] + pg[2] * gxyz[2]) / r;
-        pg[0] = pg[0] - prd * gxyz[0] / r;
-        pg[1] = pg[1] - prd * gxyz[1] / r;
-        pg[2] = pg[2] - prd * gxyz[2] / r;
-      }
-      const int q = q0 + (int)k * cD.planei;
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const double drv = a.gT[1 + d][q] - pg[d] + dd[d] + 0.0;
-        const double v = a.PS[1 + d][q] + drv * dt;
-        a.dvh[d][q] = v;
-        a.PM[1 + d][q] = a.PM[1 + d][q] + v * rweight;
-        if (k == kmin) vals[d][0] = v;
-        if (k == kmax) vals[d][1] = v;
-      }
-    }
-    __syncthreads();
-  }
-  if (own) {
-    const int pT = q0 + (int)(kmax + 1) * cD.planei, pK = q0 + (int)kmax * cD.planei;
-    const int pB = q0 + (int)(kmin - 1) * cD.planei, pN = q0 + (int)kmin * cD.planei;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const double vT = 1.0 * (vals[d][1] / a.rhog[pK]) * a.rhog[pT];
-      const double vB = -1.0 * (vals[d][0] / a.rhog[pN]) * a.rhog[pB];
-      a.dvh[d][pT] = vT;
-      a.dvh[d][pB] = vB;
-      a.PM[1 + d][pT] = a.PM[1 + d][pT] + vT * rweight;
-      a.PM[1 + d][pB] = a.PM[1 + d][pB] + vB * rweight;
-    }
-  }
-}
-
 // Regional path 1, one block per (level, tile): same stencils and
 // arithmetic as path1_column.  The blocks at kmin and kmax also write the
 // boundary rows kmin-1 and kmax+1 from the values they computed.
-__global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_path1_l(Path1Args a) {
+__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(4)) k_path1_l(Path1Args a) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
   __shared__ double s_v[3][PY * PX];
   __shared__ double s_p[PY * PX];
   __shared__ double s_ti[TY * TX], s_tj[TY * TX];
-  const TileLv tl = tile_level(cD.kmin);
+  const TileLv tl = tile_level<DD_DX, DD_DY>(cD.kmin);
   const int k = tl.k, l = tl.l, i0 = tl.i0, j0 = tl.j0;
   const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin, kmax = cD.kmax;
   const int kk = (k == kmin) ? kmin + 1 : k;
@@ -1450,73 +963,12 @@ __global__ void k_vimain_a(VimainArgs a, int pole) {
   }
 }
 
-// Tiled kernel A of vi_main for interior cells and levels kmin..kmax: the
-// haloed tiles of RGAM*diff_vh, RGAM*diff_vh*eth and RGAM*(rhogv+diff_vh)*ethtot0
-// are staged per level and the three 7-point divergences formed from shared
-// memory.  Halo cells and boundary levels of hdiv stay zero from allocation
-// (the column kernel reads zero divergence there, as with k_vimain_a).
-__global__ void __launch_bounds__(DD_DX * DD_DY) k_vimain_a_t(VimainArgs a) {
+// vi_main kernel A, one block per (level, tile): the horizontal divergences
+// of RGAM*diff_vh, RGAM*diff_vh*eth and RGAM*(rhogv + diff_vh)*ethtot0.
+__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(4)) k_vimain_a_l(VimainArgs a) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2;
   __shared__ double s_h[3][3][PY * PX];
-  const int l = blockIdx.z;
-  const int i0 = 1 + blockIdx.x * DD_DX, j0 = 1 + blockIdx.y * DD_DY;
-  const int G = cD.G, gmax = cD.G - 2;
-  const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
-  const int i = i0 + tx, j = j0 + ty;
-  const bool own = (i <= gmax) && (j <= gmax);
-  for (int k = cD.kmin; k <= cD.kmax; ++k) {
-    for (int p = tid; p < PX * PY; p += blockDim.x) {
-      const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
-      if (ii < G && jj < G) {
-        const int q = ix(ii, jj, k, l);
-        const double rg = cG.RGAM[q], e = a.eth[q], et = a.ethtot0[q];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const double dv = a.dvh.f[d][q];
-          s_h[0][d][p] = dv * rg;
-          s_h[1][d][p] = (dv * e) * rg;
-          s_h[2][d][p] = ((a.P[1 + d][q] + dv) * et) * rg;
-        }
-      } else {
-#pragma unroll
-        for (int f = 0; f < 3; ++f)
-#pragma unroll
-          for (int d = 0; d < 3; ++d) s_h[f][d][p] = 0.0;
-      }
-    }
-    __syncthreads();
-    if (own) {
-      const int c0 = (ty + 1) * PX + (tx + 1);
-      const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
-      const int q = ix(i, j, k, l);
-      double acc[3][3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        double s[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-        for (int m = 0; m < 7; ++m) {
-          const double cdv = P2(cG.coef_div, d * 7 + m, i, j, l);
-#pragma unroll
-          for (int f = 0; f < 3; ++f) {
-            const double t = cdv * s_h[f][d][nb[m]];
-            s[f] = (m == 0) ? t : s[f] + t;
-          }
-        }
-#pragma unroll
-        for (int f = 0; f < 3; ++f) acc[f][d] = s[f];
-      }
-#pragma unroll
-      for (int f = 0; f < 3; ++f) a.hdiv[f][q] = acc[f][0] + acc[f][1] + acc[f][2];
-    }
-    __syncthreads();
-  }
-}
-
-// vi_main kernel A, one block per (level, tile) (body of k_vimain_a_t).
-__global__ void __launch_bounds__(DD_DX * DD_DY, 4) k_vimain_a_l(VimainArgs a) {
-  constexpr int PX = DD_DX + 2, PY = DD_DY + 2;
-  __shared__ double s_h[3][3][PY * PX];
-  const TileLv tl = tile_level(cD.kmin);
+  const TileLv tl = tile_level<DD_DX, DD_DY>(cD.kmin);
   const int l = tl.l, i0 = tl.i0, j0 = tl.j0;
   const int G = cD.G, gmax = cD.G - 2;
   const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
@@ -1799,49 +1251,10 @@ __global__ void __launch_bounds__(128) k_vi_solve(VimainArgs a) {
   (void)rws_hi;
 }
 
-// k_vi_energy: kinetic energies, total-energy advection and rhoge_split1 from
-// the rhog_s1 / rhogw_s1 written by k_vi_solve.
-__global__ void __launch_bounds__(128) k_vi_energy(VimainArgs a) {
-  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
-  int i, j, l;
-  if (!col_of(t, i, j, l) || !interior(i, j)) return;
-  const Col c = col_reg(i, j, l);
-  const Met m = met_of(false);
-  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
-  const double dt = a.dt;
-  const double* rs1 = a.dwe[0];
-  const double* rws1 = a.dwe[1];
-  auto PSk = [&](int comp, int k) -> double {
-    if (comp == 5) k = k < kmin ? kmin : (k > kmax ? kmax : k);
-    return a.PS[comp][c.at(k)];
-  };
-  for (int k = 0; k < KA; ++k) {
-    const int p = c.at(k);
-    auto st10 = [&](int kk, int comp) -> double { return a.P[comp][c.at(kk)] + PSk(comp, kk); };
-    auto st11 = [&](int kk, int comp) -> double {
-      const int q = c.at(kk);
-      if (comp == 0) return a.P[0][q] + rs1[q];
-      if (comp == 4) return a.P[4][q] + rws1[q];
-      return a.P[comp][q] + a.dvh.f[comp - 1][q];
-    };
-    const double kin10 = rhogkin_at(c, m, k, st10);
-    const double kin11 = rhogkin_at(c, m, k, st11);
-    const double drhogetot = fluxconv_col(
-        c, m, k, a.hdiv[2][p], 1.0,
-        [&](int kk, int d) {
-          const int q = c.at(kk);
-          return (a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q];
-        },
-        [&](int kk) {
-          const int q = c.at(kk), qm = c.at(kk - 1);
-          return (a.P[4][q] + rws1[q]) * (cC.afact[kk] * a.ethtot0[q] + cC.bfact[kk] * a.ethtot0[qm]);
-        });
-    a.dwe[2][p] = PSk(5, k) + (a.gT0e[p] + drhogetot) * dt + (kin10 - kin11) + (PSk(0, k) - rs1[p]) * m.PHI[p];
-  }
-}
-
-// k_vi_energy with one thread per interior grid point (the energy update has
-// no vertical recurrence; neighbouring levels are read through the cache).
+// vi_main energy update with one thread per interior grid point: kinetic
+// energies, total-energy advection and rhoge_split1 from the rhog_s1 /
+// rhogw_s1 written by k_vi_solve (no vertical recurrence; neighbouring levels
+// are read through the cache).
 __global__ void __launch_bounds__(128) k_vi_energy_p(VimainArgs a) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= cD.npti) return;
