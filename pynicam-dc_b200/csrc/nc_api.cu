@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/nicam_cuda.h"
+
 #include "nc_tracer.cuh"
 #include "nc_grid.cuh"
 
@@ -570,7 +571,7 @@ static int run_step(nc_handle* h) {
         for (int n = 0; n < 8; ++n) vh.out[n] = h->vph[n].r;
         k_vp0_hl<<<lvgrid_vp, VP_DX * VP_DY, 0, s>>>(va, vh);
         TRY(check_launch(h, "vp0_h"));
-        k_vp0_cr<<<greg, kBlock, 0, s>>>(va, vh);
+        k_vp0_cr<<<(unsigned)((D.npt2 + NC_VP0C_BLOCK - 1) / NC_VP0C_BLOCK), NC_VP0C_BLOCK, 0, s>>>(va, vh);
         TRY(check_launch(h, "vp0_c"));
       } else {
         k_vp0<<<1, 32, 0, ps>>>(va, 1);

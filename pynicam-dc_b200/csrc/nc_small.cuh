@@ -459,7 +459,7 @@ __global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) 
   __shared__ double s_ti[TY * TX], s_tj[TY * TX];
   const TileLv tl = tile_level<VP_DX, VP_DY>(cD.kmin);
   const int l = tl.l, i0 = tl.i0, j0 = tl.j0;
-  const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin, kmax = cD.kmax;
+  const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin;
   const int tid = threadIdx.x, tx = tid % VP_DX, ty = tid / VP_DX;
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= gmax) && (j <= gmax);
@@ -600,7 +600,10 @@ __global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) 
 // half-level eth, the vertical kinetic-energy term) are formed and the ones at
 // k and k-1 are carried in registers.  Each value is the expression of
 // vp0_column (the pole form), so regional and pole columns round alike.
-__global__ void __launch_bounds__(128) k_vp0_cr(Vp0Args a, Vp0H h) {
+// 256-thread blocks: at 72 registers three blocks fit an SM, and the
+// 676,000 columns of gl08 then fill 5.95 waves of the 148 SMs
+#define NC_VP0C_BLOCK 256
+__global__ void __launch_bounds__(NC_VP0C_BLOCK) k_vp0_cr(Vp0Args a, Vp0H h) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
@@ -1139,7 +1142,9 @@ __device__ void vimain_column(const VimainArgs& a, const Col c) {
 // k_vi_solve: flux convergences of diff_vh (rolling half-level fluxes), the
 // Thomas forward sweep, then the back substitution fused with rhog_split1 on
 // the way down; writes rhog_s1, rhogw_s1 and their running means.
-__global__ void __launch_bounds__(128) k_vi_solve(VimainArgs a) {
+// nine 128-thread blocks per SM (56 registers): the 655,360 interior columns
+// of gl08 fill 3.84 waves of the 148 SMs instead of 4.32 at eight
+__global__ void __launch_bounds__(128, 9) k_vi_solve(VimainArgs a) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l) || !interior(i, j)) return;
@@ -1222,7 +1227,7 @@ __global__ void __launch_bounds__(128) k_vi_solve(VimainArgs a) {
     vE_lo = vE_hi;
   }
   // back substitution (downward) fused with rhog_split1
-  double x = 0.0, rws_hi = 0.0, v2_hi = 0.0;
+  double x = 0.0, v2_hi = 0.0;
   for (int k = kT; k >= 0; --k) {
     const int p = c.at(k);
     double rws;
@@ -1245,10 +1250,8 @@ __global__ void __launch_bounds__(128) k_vi_solve(VimainArgs a) {
     a.dwe[1][p] = rws;
     a.PM0[p] = a.PM0[p] + rs * a.rweight;
     a.PM4[p] = a.PM4[p] + rws * a.rweight;
-    rws_hi = rws;
     v2_hi = v2;
   }
-  (void)rws_hi;
 }
 
 // vi_main energy update with one thread per interior grid point: kinetic
