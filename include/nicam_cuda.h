@@ -158,6 +158,18 @@ int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* g
                         const double* volume_pl, int32_t gall_1d, int32_t lall, int32_t kall, int32_t kmin,
                         int32_t kmax, double* out, void* stream);
 
+/* Dyn.forcing_step (pynicamdc/nhm/dynamics/mod_dynamics.py:597-735) for
+ * AF_TYPE 'HELD-SUAREZ' (nhm/forcing/mod_af_heldsuarez.py, dry case, applied as
+ * in nhm/forcing/mod_forcing.py:14-28 / :323-349): diagnostics of the current
+ * prognostic, Rayleigh friction and Newtonian temperature relaxation applied
+ * to RHOGV{X,Y,Z} and RHOGE over kmin..kmax with the large time step, then
+ * the halo exchange of PRG_var.  The poles are not forced, as in the
+ * reference's host path.  Needs the handle to have been created with the
+ * setup entries "AF_hs_lat_terms" ((gall_1d, gall_1d, 1, lall, 3): |sin lat|^2,
+ * |cos lat|^2, |cos lat|^4 of GRD_LAT[:, :, K0, :]) and "PRE00"; otherwise
+ * NC_ERR_STATE.  Asynchronous on the handle's stream, like nc_step. */
+int nc_forcing_step(nc_handle* h);
+
 const char* nc_last_error(void);
 
 void nc_destroy(nc_handle* h);

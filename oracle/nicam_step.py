@@ -1607,3 +1607,73 @@ def dynamics_step(g, prg, prg_pl):
     out_pl = np.concatenate([PROG_pl, PROGq_pl], axis=-1)
     comm(g, out, out_pl)
     return out, out_pl
+
+
+# --------------------------------------------------------------------------
+# Held-Suarez artificial forcing  (Dyn.forcing_step, AF_TYPE 'HELD-SUAREZ')
+# --------------------------------------------------------------------------
+HS_SIGMA_B = 0.7                        # forcing/mod_af_heldsuarez.py:19-24 (dry case, :31-36)
+HS_KF = 1.0 / (1.0 * 86400.0)
+HS_DTH_Z = 10.0
+HS_KA = 1.0 / (40.0 * 86400.0)
+HS_KS = 1.0 / (4.0 * 86400.0)
+HS_T_EQ0 = 315.0
+HS_DT_Y = 60.0
+
+
+def hs_latitude_terms(lat):
+    """|sin(lat)|**2, |cos(lat)|**2 and |cos(lat)|**4 of the column latitudes,
+    with the reference's numpy expressions (mod_af_heldsuarez.py:61-63)."""
+    sinlat = np.abs(np.sin(lat))
+    coslat = np.abs(np.cos(lat))
+    return sinlat ** 2, coslat ** 2, coslat ** 4
+
+
+def held_suarez(g, lat, pre, tem, vx, vy, vz):
+    """forcing/mod_af_heldsuarez.py:38-88 AF_heldsuarez: tendencies
+    (fvx, fvy, fvz, fe) on regional (i,j,k,l) fields, zero outside kmin..kmax."""
+    kmin, kmax = g.kmin, g.kmax
+    sin2, cos2, cos4 = (t[:, :, None, :] for t in hs_latitude_terms(lat))
+    psref = (0.5 * (pre[:, :, kmin, :] + pre[:, :, kmin - 1, :]))[:, :, None, :]
+    sigma = pre / psref
+    factor = np.maximum((sigma - HS_SIGMA_B) / (1.0 - HS_SIGMA_B), 0.0)
+    fvx = -HS_KF * factor * vx
+    fvy = -HS_KF * factor * vy
+    fvz = -HS_KF * factor * vz
+    ap0 = np.abs(pre / g.PRE00)
+    Kt = HS_KA + (HS_KS - HS_KA) * factor * cos4
+    T_eq = np.maximum(200.0, (HS_T_EQ0 - HS_DT_Y * sin2
+                              - HS_DTH_Z * np.log(np.maximum(ap0, 1e-30)) * cos2) * ap0 ** (g.Rdry / g.CPdry))
+    fe = -Kt * (tem - T_eq) * g.CVdry
+    kk = np.arange(pre.shape[2]).reshape(1, 1, -1, 1)
+    valid = (kk >= kmin) & (kk <= kmax)
+    return tuple(np.where(valid, f, 0.0) for f in (fvx, fvy, fvz, fe))
+
+
+def forcing_step_hs(g, prg, prg_pl, lat):
+    """Dyn.forcing_step for AF_TYPE 'HELD-SUAREZ' on the host path
+    (nhm/dynamics/mod_dynamics.py:597-735): diagnostics of the regional
+    prognostic, the Held-Suarez tendencies applied as
+    PROG + dt * f * rho * GSGAM2 (nhm/forcing/mod_forcing.py:14-28
+    hs_apply_core, :323-349 forcing_step_hs; no forcing of RHOG, RHOGW, the
+    tracers or the poles), then the halo exchange of the whole PRG_var.
+    ``lat`` is GRD_LAT[:, :, K0, :] (i, j, l).  Returns new arrays."""
+    out = prg.copy()
+    out_pl = prg_pl.copy()
+    PROG = out[..., 0:6]
+    PROGq = out[..., 6:]
+    DIAG = np.zeros(PROG.shape)
+    rho, _ein, _q, _, _, _ = diagnostics(g, PROG, PROGq, DIAG, prg_pl[..., 0:6].copy(), prg_pl[..., 6:].copy(),
+                                          np.zeros(prg_pl[..., 0:6].shape))
+    fvx, fvy, fvz, fe = held_suarez(g, lat, DIAG[..., I_pre], DIAG[..., I_tem], DIAG[..., I_vx], DIAG[..., I_vy],
+                                    DIAG[..., I_vz])
+    dt = g.dtl
+    z = np.zeros_like(fvx)
+    comps = [z] * 6
+    comps[I_RHOGVX] = dt * fvx * rho * g.VMTR_GSGAM2
+    comps[I_RHOGVY] = dt * fvy * rho * g.VMTR_GSGAM2
+    comps[I_RHOGVZ] = dt * fvz * rho * g.VMTR_GSGAM2
+    comps[I_RHOGE] = dt * fe * rho * g.VMTR_GSGAM2
+    out[..., 0:6] = PROG + np.stack(comps, axis=-1)
+    comm(g, out, out_pl)
+    return out, out_pl

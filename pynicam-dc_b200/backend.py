@@ -17,7 +17,9 @@ offers the same methods with the same meaning:
 * ``assert_host_prgvar_synced(who)`` -- ``AssertionError`` on a stale host read
   (mod_dynamics.py:460-468);
 * ``forcing_step(msc)`` -- a no-op for ``AF_TYPE = NONE`` like the reference
-  (mod_dynamics.py:597); other forcings are not part of this backend and raise.
+  (mod_dynamics.py:597); the Held-Suarez forcing (``AF_TYPE = HELD-SUAREZ``)
+  on the device through ``nc_forcing_step``; DCMIP forcing is not part of
+  this backend and raises at set-up.
 
 Geometry, metrics and operator coefficients are read once from the
 reference's setup services on ``msc`` (grd, gmtr, oprt, vmtr, bsst, comm, ...)
@@ -70,6 +72,9 @@ def geo_from_msc(msc) -> dict:
     for k in ("rho_bs", "pre_bs", "tem_bs"):
         g[k] = getattr(m.bsst, k)
         g[k + "_pl"] = getattr(m.bsst, k + "_pl")
+    if getattr(m.rcnf, "AF_TYPE", "NONE") == "HELD-SUAREZ":
+        # the column latitudes the forcing reads (mod_dynamics.py: GRD_LAT[:, :, K0, :])
+        g["GRD_LAT"] = np.ascontiguousarray(m.grd.GRD_LAT[:, :, m.adm.ADM_K0, :])
     return {k: np.asarray(v) for k, v in g.items()}
 
 
@@ -83,6 +88,7 @@ class CudaDyn:
             self._check_config(msc)
             geo = geo_from_msc(msc)
         self.core = NicamCuda(geo, graph=graph)
+        self._forced = "GRD_LAT" in geo
         self._host_stale = False
         self._device_valid = False
 
@@ -101,6 +107,8 @@ class CudaDyn:
                                       "2-D/vertical divdamp, lap1 or nonlinear diffusion")
         if r.DYN_DIV_NUM != 1:
             raise NotImplementedError("cuda backend: DYN_DIV_NUM = 1 only")
+        if getattr(r, "AF_TYPE", "NONE") not in ("NONE", "HELD-SUAREZ"):
+            raise NotImplementedError("cuda backend: artificial forcing NONE or HELD-SUAREZ only")
 
     # -- the reference's step API -------------------------------------------
     def dynamics_step(self, msc):
@@ -109,13 +117,28 @@ class CudaDyn:
         self._host_stale = True
 
     def run_timeloop_chunk(self, msc, K: int):
+        """K large steps; with the Held-Suarez forcing active each step is
+        followed by the forcing step, as in the reference's per-step loop
+        (pynicamdc/api.py:724-730)"""
         self._ensure_device(msc)
-        self.core.step(int(K))
+        if self._forced:
+            for _ in range(int(K)):
+                self.core.step(1)
+                self.core.forcing_step()
+        else:
+            self.core.step(int(K))
         self._host_stale = True
 
     def forcing_step(self, msc):
-        if getattr(msc.rcnf, "AF_TYPE", "NONE") not in ("NONE", None):
-            raise NotImplementedError("cuda backend: artificial forcing is not on the device")
+        af = getattr(msc.rcnf, "AF_TYPE", "NONE")
+        if af in ("NONE", None):
+            return None
+        if af != "HELD-SUAREZ" or not self._forced:
+            raise NotImplementedError(f"cuda backend: artificial forcing {af!r} is not configured on the device")
+        self._ensure_device(msc)
+        self.core.forcing_step()
+        self._host_stale = True
+        return None
 
     def sync_prgvar_to_host(self, prgv, msc=None):
         if not self._device_valid:

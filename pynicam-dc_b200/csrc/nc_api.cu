@@ -11,6 +11,7 @@
 
 #include "../../include/nicam_cuda.h"
 
+#include "nc_forcing.cuh"
 #include "nc_tracer.cuh"
 #include "nc_grid.cuh"
 
@@ -204,6 +205,7 @@ struct nc_handle {
   FieldPair PSa[6], PSb[6], PM[5], vtmp2[3], gT[6], Mc, Mu, Ml, ethtot0, hdiv[3];
   FieldPair flx_v, rhog_t, flx[6], xc[9], ch[6], cm[6], q, gq[3], qa[3], Qmin, Qmax;
   FieldPair vph[8];             // horizontal terms of vp0 (div1, div2, dd, dpg)
+  const double* hs_lat = nullptr;   // Held-Suarez latitude planes (optional)
   // the pole columns run on a second stream between the operations that mix
   // regional and pole data (halo exchanges, tracer density update)
   cudaStream_t stream2 = nullptr;
@@ -422,6 +424,22 @@ static Prog prog_pl(nc_handle* h) {
   do {                                                                            \
     if (h->stop_phase > 0 && ++h->phase >= h->stop_phase) return join_pl(h);      \
   } while (0)
+
+// halo exchange of the whole PRG_var: PROG and every tracer
+static int comm_prg(nc_handle* h) {
+  const Dims& D = h->D;
+  CommFields f{};
+  int n = 0;
+  for (int v = 0; v < 6; ++v) { f.r[n] = h->P[v].r; f.p[n] = h->P[v].p; n++; }
+  for (int iq = 0; iq < D.nq && n < NC_MAXCOMM; ++iq) { f.r[n] = h->Pq[iq].r; f.p[n] = h->Pq[iq].p; n++; }
+  f.n = n;
+  long long ne = (long long)(h->nr + h->np) * D.KA;
+  TRY(join_pl(h));
+  k_comm<<<(unsigned)((ne + 255) / 256), 256, 0, h->stream>>>(f, h->r_dst, h->r_src, h->nr, h->p_dst, h->p_src, h->np);
+  TRY(check_launch(h, "comm_final"));
+  for (int iq = NC_MAXCOMM - 6; iq < D.nq; ++iq) TRY(comm(h, {h->Pq[iq]}));
+  return 0;
+}
 
 static int run_step(nc_handle* h) {
   cudaStream_t s = h->stream;
@@ -741,18 +759,7 @@ static int run_step(nc_handle* h) {
     PHASE();
   }
   // marshal-out halo exchange of PRG_var (mod_dynamics.py:2726-2727)
-  {
-    CommFields f{};
-    int n = 0;
-    for (int v = 0; v < 6; ++v) { f.r[n] = h->P[v].r; f.p[n] = h->P[v].p; n++; }
-    for (int iq = 0; iq < D.nq && n < NC_MAXCOMM; ++iq) { f.r[n] = h->Pq[iq].r; f.p[n] = h->Pq[iq].p; n++; }
-    f.n = n;
-    long long ne = (long long)(h->nr + h->np) * D.KA;
-    TRY(join_pl(h));
-    k_comm<<<(unsigned)((ne + 255) / 256), 256, 0, s>>>(f, h->r_dst, h->r_src, h->nr, h->p_dst, h->p_src, h->np);
-    TRY(check_launch(h, "comm_final"));
-    for (int iq = NC_MAXCOMM - 6; iq < D.nq; ++iq) TRY(comm(h, {h->Pq[iq]}));
-  }
+  TRY(comm_prg(h));
   TRY(join_pl(h));
   return 0;
 }
@@ -846,6 +853,35 @@ static int mass_scratch_ptr(double** out) {
 // ---------------------------------------------------------------------------
 extern "C" {
 
+int nc_forcing_step(nc_handle* h) {
+  if (!h) return fail(NC_ERR_ARG, "nc_forcing_step: null handle");
+  if (!h->have_state) return fail(NC_ERR_STATE, "nc_forcing_step: no state uploaded");
+  if (!h->hs_lat)
+    return fail(NC_ERR_STATE, "nc_forcing_step: the handle was created without AF_hs_lat_terms "
+                              "(Held-Suarez forcing not configured)");
+  TRY(load_consts(h));
+  const Dims& D = h->D;
+  HsArgs a;
+  for (int v = 0; v < 6; ++v) a.P.v[v] = h->P[v].r;
+  a.Pq0 = h->Pq[0].r;
+  a.lat3 = h->hs_lat;
+  a.dt = h->dtl;
+  a.RdCp = h->C.Rdry / h->C.CPdry;
+  a.sigma_b = 0.7;
+  a.Kf = 1.0 / (1.0 * 86400.0);
+  a.Dth_z = 10.0;
+  a.Ka = 1.0 / (40.0 * 86400.0);
+  a.Ks = 1.0 / (4.0 * 86400.0);
+  a.T_eq0 = 315.0;
+  a.DT_y = 60.0;
+  a.PRE00 = h->C.PRE00;
+  k_forcing_hs<<<(unsigned)((D.npt2 + kBlock - 1) / kBlock), kBlock, 0, h->stream>>>(a);
+  TRY(check_launch(h, "forcing_hs"));
+  TRY(comm_prg(h));
+  TRY(join_pl(h));
+  return 0;
+}
+
 const char* nc_last_error(void) { return g_err.c_str(); }
 
 int64_t nc_kernel_launches(nc_handle* h) { return h ? h->launches : 0; }
@@ -933,6 +969,11 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   TRY(up_reg(h, T, "GMTR_t_W", 1, 6, &Gm.GMTR_t));
   TRY(up_reg(h, T, "GMTR_a_HN", 1, 9, &Gm.GMTR_a));
   TRY(up_reg(h, T, "GMTR_p_RAREA", 1, 1, &Gm.GMTR_p));
+  if (T.get("AF_hs_lat_terms")) {   // Held-Suarez forcing configured (nc_forcing_step)
+    if (!T.get("PRE00")) return fail(NC_ERR_ARG, "AF_hs_lat_terms given without PRE00");
+    TRY(scalar(T, "PRE00", C.PRE00));
+    TRY(up_reg(h, T, "AF_hs_lat_terms", 1, 3, &h->hs_lat));
+  }
   const int64_t npl = D.npl;
   TRY(up_pl(h, T, "VMTR_GSGAM2_pl", npl, &Gm.GSGAM2_pl));
   TRY(up_pl(h, T, "VMTR_GSGAM2H_pl", npl, &Gm.GSGAM2H_pl));

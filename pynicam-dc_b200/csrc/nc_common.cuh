@@ -42,7 +42,7 @@ struct Dims {
 // Physical / run constants (identical names to the reference's CONST_*).
 struct Consts {
   double GRAV, Rdry, CVdry, CPdry, Rvap, OHM, EPS, HUGE_, rscale, alpha;
-  double Kh, divdamp_coef, hdiff_fact_rho, CVW0;
+  double Kh, divdamp_coef, hdiff_fact_rho, CVW0, PRE00;
   double afact[NC_MAXK], bfact[NC_MAXK], cfact[NC_MAXK], dfact[NC_MAXK];
   double rdgz[NC_MAXK], rdgzh[NC_MAXK];
 };

@@ -32,7 +32,8 @@ _lib = None
 # every entry point declared in include/nicam_cuda.h
 EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync",
            "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",
-           "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_last_error", "nc_destroy")
+           "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_forcing_step", "nc_last_error",
+           "nc_destroy")
 
 
 def load_library(path: str = LIB_PATH):
@@ -66,6 +67,8 @@ def load_library(path: str = LIB_PATH):
     lib.nc_grid_spring.argtypes = [i32, i32, dp, dp, dp, dp, dp, i32, dp, dp, i32, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_double, i64, ctypes.POINTER(i64)]
     lib.nc_grid_spring.restype = ctypes.c_int
+    lib.nc_forcing_step.argtypes = [vp]
+    lib.nc_forcing_step.restype = ctypes.c_int
     lib.nc_destroy.argtypes = [vp]
     lib.nc_destroy.restype = None
     for f in ("nc_create", "nc_upload_state", "nc_download_state", "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync",
@@ -114,6 +117,11 @@ def _dtype_code(a: np.ndarray) -> int:
     raise TypeError(f"unsupported dtype {a.dtype}")
 
 
+def _scalar(a):
+    """the single value of a 0-d or one-element array (or a Python number)"""
+    return np.asarray(a).reshape(-1)[0].item()
+
+
 def setup_table(geo: dict) -> dict:
     """Host arrays handed to ``nc_create`` (names as in include/nicam_cuda.h).
 
@@ -124,10 +132,10 @@ def setup_table(geo: dict) -> dict:
     """
     t = {}
     for k in ("kall", "kmin", "kmax", "gall_1d", "gmin", "gmax", "lall", "nq"):
-        t[k] = np.asarray(int(np.asarray(geo[k])), np.int64)
+        t[k] = np.asarray(int(_scalar(geo[k])), np.int64)
     for k in ("GRAV", "Rdry", "CVdry", "CPdry", "Rvap", "OHM", "EPS", "HUGE", "rscale", "alpha", "dtl", "dts",
               "Kh_coef", "divdamp_coef", "hdiff_fact_rho"):
-        t[k] = np.asarray(float(np.asarray(geo[k])), np.float64)
+        t[k] = np.asarray(float(_scalar(geo[k])), np.float64)
     t["CVW"] = np.ascontiguousarray(geo["CVW"], np.float64)
     t["sstep"] = np.ascontiguousarray(geo["sstep"], np.int64)
     for k in ("GRD_afact", "GRD_bfact", "GRD_cfact", "GRD_dfact", "GRD_rdgz", "GRD_rdgzh"):
@@ -146,10 +154,16 @@ def setup_table(geo: dict) -> dict:
     t["GMTR_t_W"] = np.ascontiguousarray(np.asarray(geo["GMTR_t"])[..., 2:5], np.float64)
     t["GMTR_a_HN"] = np.ascontiguousarray(np.asarray(geo["GMTR_a"])[..., 0:3], np.float64)
     t["GMTR_p_RAREA"] = np.ascontiguousarray(np.asarray(geo["GMTR_p"])[..., 1:2], np.float64)
+    if "GRD_LAT" in geo:   # Held-Suarez forcing: latitude terms with the reference's numpy expressions
+        lat = np.asarray(geo["GRD_LAT"], np.float64)
+        lat = lat.reshape(lat.shape[0], lat.shape[1], 1, lat.shape[-1])
+        sinlat, coslat = np.abs(np.sin(lat)), np.abs(np.cos(lat))
+        t["AF_hs_lat_terms"] = np.ascontiguousarray(np.stack([sinlat ** 2, coslat ** 2, coslat ** 4], axis=-1))
+        t["PRE00"] = np.asarray(float(_scalar(geo["PRE00"])), np.float64)
     t["pntmask"] = np.ascontiguousarray(geo["pntmask"], np.int32)
     t["have_sgp"] = np.ascontiguousarray(geo["have_sgp"], np.bool_)
     plan = halo.compose(geo["copy_r2r"], geo["copy_p2r"], geo["copy_r2p"], geo["copy_sgp"],
-                        int(np.asarray(geo["gall_1d"])), int(np.asarray(geo["lall"])))
+                        int(_scalar(geo["gall_1d"])), int(_scalar(geo["lall"])))
     for k, v in zip(("halo_r_dst", "halo_r_src", "halo_p_dst", "halo_p_src"), plan):
         t[k] = np.ascontiguousarray(v, np.int64)
     return t
@@ -180,9 +194,9 @@ class NicamCuda:
         _check(lib.nc_create(entries, len(self._tab), ctypes.byref(h)))
         self._h = h
         _check(lib.nc_set_graph(h, 1 if graph else 0))
-        G = int(self._tab["gall_1d"])
-        self.shape = (G, G, int(self._tab["kall"]), int(self._tab["lall"]), 6 + int(self._tab["nq"]))
-        self.shape_pl = (6, int(self._tab["kall"]), 2, 6 + int(self._tab["nq"]))
+        G, K, L, nq = (int(_scalar(self._tab[k])) for k in ("gall_1d", "kall", "lall", "nq"))
+        self.shape = (G, G, K, L, 6 + nq)
+        self.shape_pl = (6, K, 2, 6 + nq)
 
     # ---- state marshal (host arrays in the reference layout)
     def upload(self, prg: np.ndarray, prg_pl: np.ndarray):
@@ -211,6 +225,11 @@ class NicamCuda:
     def step(self, nsteps: int = 1):
         _check(self._lib.nc_step(self._h, int(nsteps)))
 
+    def forcing_step(self):
+        """Dyn.forcing_step for AF_TYPE 'HELD-SUAREZ' (nc_forcing_step); the
+        handle must have been built from a setup with GRD_LAT"""
+        _check(self._lib.nc_forcing_step(self._h))
+
     def run_phases(self, nphases: int):
         """debugging: run the first ``nphases`` phases of one step"""
         _check(self._lib.nc_run_phases(self._h, int(nphases)))
@@ -219,7 +238,7 @@ class NicamCuda:
         _check(self._lib.nc_sync(self._h))
 
     def mass_sums(self):
-        n = 1 + int(self._tab["nq"])
+        n = 1 + int(_scalar(self._tab["nq"]))
         out = np.zeros(n)
         _check(self._lib.nc_mass_sums(self._h, out.ctypes.data, n))
         return out

@@ -26,3 +26,13 @@ def pkg():
 def golden():
     from make_golden import load
     return load(os.path.join(GOLDEN, "gl03_z10_trc.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_hs():
+    """gl03 z10 with the reference's Held-Suarez forcing (make_hs.py): setup
+    arrays (plus GRD_LAT at K0), the column latitudes and three states"""
+    from make_golden import load
+    geo, st = load(os.path.join(GOLDEN, "gl03_z10_hs.npz"))
+    lat = geo.pop("GRD_LAT")
+    return geo, lat, st

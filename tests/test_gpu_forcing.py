@@ -1,0 +1,73 @@
+"""Held-Suarez forcing step on the device (nc_forcing_step) against the
+reference run with AF_TYPE 'HELD-SUAREZ' (tests/golden/make_hs.py) and
+against the oracle.
+
+The forcing's T_eq uses log and pow, which CUDA and numpy may round
+differently in the last bit, so these comparisons use a tolerance: relative
+L2 per prognostic <= 1e-12 after each forced step (the north star's one-step
+tolerance) and <= 1e-14 for the forcing alone."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ("RHOG", "RHOGVX", "RHOGVY", "RHOGVZ", "RHOGW", "RHOGE", "RHOGQ1")
+
+
+def _rel_l2(a, b):
+    out = {}
+    for v, nm in enumerate(NAMES[:a.shape[-1]]):
+        x, y = a[..., v], b[..., v]
+        den = np.sqrt(np.sum(y * y))
+        out[nm] = float(np.sqrt(np.sum((x - y) ** 2)) / den) if den > 0 else float(np.abs(x - y).max())
+    return out
+
+
+@pytest.fixture(scope="module")
+def core_hs(pkg, golden_hs):
+    geo, lat, _ = golden_hs
+    g = dict(geo)
+    g["GRD_LAT"] = lat
+    c = pkg.NicamCuda(g, graph=True)
+    yield c
+    c.close()
+
+
+def test_held_suarez_two_steps_vs_reference(core_hs, golden_hs):
+    _, _, st = golden_hs
+    core_hs.upload(st["state0"], st["state0_pl"])
+    for s in (1, 2):
+        core_hs.step(1)
+        core_hs.forcing_step()
+        out, out_pl = core_hs.download()
+        err = _rel_l2(out, st[f"state{s}"])
+        err_pl = _rel_l2(out_pl, st[f"state{s}_pl"])
+        assert max(err.values()) <= 1e-12, (s, err)
+        assert max(err_pl.values()) <= 1e-12, (s, err_pl)
+
+
+def test_forcing_alone_vs_oracle(core_hs, golden_hs):
+    from oracle import nicam_step as O
+    geo, lat, st = golden_hs
+    s, sp = st["state1"], st["state1_pl"]
+    want, want_pl = O.forcing_step_hs(O.Geo(geo), s, sp, lat)
+    core_hs.upload(s, sp)
+    core_hs.forcing_step()
+    out, out_pl = core_hs.download()
+    assert max(_rel_l2(out, want).values()) <= 1e-14
+    assert np.array_equal(out_pl, want_pl)
+    # the forcing changed the momentum and the energy, and nothing else
+    for v in (0, 4, 6):
+        assert np.array_equal(out[..., v], want[..., v])
+    assert np.abs(want[..., 1:4] - s[..., 1:4]).max() > 0.0
+
+
+def test_forcing_needs_its_setup(pkg, golden):
+    geo, st = golden
+    c = pkg.NicamCuda(geo, graph=False)
+    try:
+        c.upload(st["state0"], st["state0_pl"])
+        with pytest.raises(pkg.NicamError, match="Held-Suarez"):
+            c.forcing_step()
+    finally:
+        c.close()

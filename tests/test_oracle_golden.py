@@ -18,3 +18,24 @@ def test_golden_tracer_is_nontrivial(golden):
     _, st = golden
     q = st["state0"][..., 6]
     assert q.max() > 1e-3 and (q > 0).mean() > 0.5
+
+
+def test_oracle_held_suarez_matches_reference_two_steps(golden_hs):
+    """dynamics step + Held-Suarez forcing step, against the reference run
+    with AF_TYPE 'HELD-SUAREZ' (tests/golden/make_hs.py)"""
+    geo, lat, st = golden_hs
+    G = O.Geo(geo)
+    for s in (0, 1):
+        out, out_pl = O.dynamics_step(G, st[f"state{s}"], st[f"state{s}_pl"])
+        out, out_pl = O.forcing_step_hs(G, out, out_pl, lat)
+        assert np.array_equal(out, st[f"state{s + 1}"]), f"step {s + 1} regional"
+        assert np.array_equal(out_pl, st[f"state{s + 1}_pl"]), f"step {s + 1} pole"
+
+
+def test_held_suarez_fixture_is_forced(golden, golden_hs):
+    """the forced states differ from the unforced reference run of the same case"""
+    _, _, st = golden_hs
+    _, st0 = golden
+    assert np.array_equal(st["state0"], st0["state0"])
+    d = np.abs(st["state1"][..., 1:4] - st0["state1"][..., 1:4]).max()
+    assert d > 0.0
