@@ -1677,3 +1677,69 @@ def forcing_step_hs(g, prg, prg_pl, lat):
     out[..., 0:6] = PROG + np.stack(comps, axis=-1)
     comm(g, out, out_pl)
     return out, out_pl
+
+
+# --------------------------------------------------------------------------
+# offline tracer advection  (integ_type TRCADV, DCMIP2012 test 1-1)
+# --------------------------------------------------------------------------
+TRC_A, TRC_RD, TRC_G, TRC_PI = 6371220.0, 287.0, 9.80616, 3.141592653589793238   # mod_af_trcadv.py:14-19
+
+
+def trcadv_winds(time, lon, lat, zf, zh):
+    """nhm/forcing/mod_af_trcadv.py:22-97 test11_velocity with
+    Sp_Unit_East / Sp_Unit_North (:151-171): winds (vx, vy, vz) at full levels
+    and w at half levels at model time ``time``; ``lon``/``lat`` broadcast
+    against the heights."""
+    tau = 12.0 * 86400.0
+    u0 = 2.0 * TRC_PI * TRC_A / tau
+    k0 = 10.0 * TRC_A / tau
+    omega0 = 23000.0 * TRC_PI / tau
+    T0 = 300.0
+    H = TRC_RD * T0 / TRC_G
+    p0 = 1000.E2
+    dlon = 2.0 * TRC_PI * time / tau
+    lonp = lon - dlon
+    bs = 0.2
+    p = p0 * np.exp(-zf / H)
+    ptop = p0 * np.exp(-12000.0 / H)
+    ud = (omega0 * TRC_A) / (bs * ptop) * np.cos(lonp) * np.cos(lat) ** 2 * np.cos(dlon) * (
+        -np.exp((p - p0) / (bs * ptop)) + np.exp((ptop - p) / (bs * ptop)))
+    u = k0 * np.sin(2.0 * lat) * np.sin(lonp) ** 2 * np.cos(0.5 * dlon) + u0 * np.cos(lat) + ud
+    v = k0 * np.sin(2.0 * lonp) * np.cos(lat) * np.cos(0.5 * dlon)
+    e0, e1, e2 = -np.sin(lon), np.cos(lon), np.zeros_like(lon)
+    n0, n1, n2 = -np.sin(lat) * np.cos(lon), -np.sin(lat) * np.sin(lon), np.cos(lat)
+    vx = e0 * u + n0 * v
+    vy = e1 * u + n1 * v
+    vz = e2 * u + n2 * v
+    p = p0 * np.exp(-zh / H)
+    s = (1.0 + np.exp((ptop - p0) / (bs * ptop)) - np.exp((p - p0) / (bs * ptop)) - np.exp((ptop - p) / (bs * ptop)))
+    w = -(TRC_RD * T0) / (TRC_G * p) * omega0 * np.sin(lonp) * np.cos(lat) * np.cos(dlon) * s
+    return vx, vy, vz, w
+
+
+def trcadv_step(g, prg, prg_pl, time, lon, lat, zf, zh, lon_pl, lat_pl, zf_pl, zh_pl):
+    """Dyn.dynamics_step for integ_type TRCADV (mod_dynamics.py:2030-2085 and
+    the marshal-out :2690-2727): the tracers are advected with the current
+    PROG as the mean state (rhog_in = PROG0 rhog, no density tendency), then
+    the prescribed winds of model time ``time`` are set as wind * RHOG
+    (nhm/forcing/mod_forcing.py:113-210 forcing_update), then PRG_var is
+    exchanged.  ``lon``/``lat`` are GRD_LON/GRD_LAT[:, :, K0, :] (i,j,l),
+    ``zf``/``zh`` the full/half-level heights (i,j,k,l); the pole arrays are
+    (g,l) and (g,k,l).  Returns new arrays."""
+    out = prg.copy()
+    out_pl = prg_pl.copy()
+    PROG, PROGq = out[..., 0:6], out[..., 6:]
+    PROG_pl, PROGq_pl = out_pl[..., 0:6], out_pl[..., 6:]
+    rhog_in = PROG[..., I_RHOG].copy()
+    rhog_in_pl = PROG_pl[..., I_RHOG].copy()
+    tracer_advection(g, PROGq, PROGq_pl, rhog_in, rhog_in_pl, PROG[..., 0:5].copy(), PROG_pl[..., 0:5].copy(),
+                     np.zeros_like(rhog_in), np.zeros_like(rhog_in_pl), g.dtl)
+    for P, lo, la, z, zhh in ((PROG, lon[:, :, None, :], lat[:, :, None, :], zf, zh),
+                              (PROG_pl, lon_pl[:, None, :], lat_pl[:, None, :], zf_pl, zh_pl)):
+        vx, vy, vz, w = trcadv_winds(time, lo, la, z, zhh)
+        P[..., I_RHOGVX] = vx * P[..., I_RHOG]
+        P[..., I_RHOGVY] = vy * P[..., I_RHOG]
+        P[..., I_RHOGVZ] = vz * P[..., I_RHOG]
+        P[..., I_RHOGW] = w * P[..., I_RHOG]
+    comm(g, out, out_pl)
+    return out, out_pl

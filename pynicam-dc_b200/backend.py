@@ -72,7 +72,20 @@ def geo_from_msc(msc) -> dict:
     for k in ("rho_bs", "pre_bs", "tem_bs"):
         g[k] = getattr(m.bsst, k)
         g[k + "_pl"] = getattr(m.bsst, k + "_pl")
-    if getattr(m.rcnf, "AF_TYPE", "NONE") == "HELD-SUAREZ":
+    if m.tim.TIME_integ_type == "TRCADV":
+        # the coordinates of the prescribed winds (mod_forcing.py forcing_update)
+        K0 = m.adm.ADM_K0
+        grd = m.grd
+        g["integ_type"] = "TRCADV"
+        g["GRD_LON"] = np.ascontiguousarray(grd.GRD_LON[:, :, K0, :])
+        g["GRD_LAT"] = np.ascontiguousarray(grd.GRD_LAT[:, :, K0, :])
+        g["GRD_LON_pl"] = np.ascontiguousarray(grd.GRD_LON_pl[:, K0, :])
+        g["GRD_LAT_pl"] = np.ascontiguousarray(grd.GRD_LAT_pl[:, K0, :])
+        g["GRD_Z"] = np.ascontiguousarray(grd.GRD_vz[:, :, :, :, grd.GRD_Z])
+        g["GRD_ZH"] = np.ascontiguousarray(grd.GRD_vz[:, :, :, :, grd.GRD_ZH])
+        g["GRD_Z_pl"] = np.ascontiguousarray(grd.GRD_vz_pl[:, :, :, grd.GRD_Z])
+        g["GRD_ZH_pl"] = np.ascontiguousarray(grd.GRD_vz_pl[:, :, :, grd.GRD_ZH])
+    elif getattr(m.rcnf, "AF_TYPE", "NONE") == "HELD-SUAREZ":
         # the column latitudes the forcing reads (mod_dynamics.py: GRD_LAT[:, :, K0, :])
         g["GRD_LAT"] = np.ascontiguousarray(m.grd.GRD_LAT[:, :, m.adm.ADM_K0, :])
     return {k: np.asarray(v) for k, v in g.items()}
@@ -88,15 +101,18 @@ class CudaDyn:
             self._check_config(msc)
             geo = geo_from_msc(msc)
         self.core = NicamCuda(geo, graph=graph)
-        self._forced = "GRD_LAT" in geo
+        self._forced = "GRD_LAT" in geo and str(np.asarray(geo.get("integ_type", "RK3"))) != "TRCADV"
         self._host_stale = False
         self._device_valid = False
 
     @staticmethod
     def _check_config(msc):
         r = msc.rcnf
-        if msc.tim.TIME_integ_type != "RK3":
-            raise NotImplementedError("cuda backend: RK3 time integration only")
+        if msc.tim.TIME_integ_type == "TRCADV":
+            if (getattr(r, "DCTEST_type", "") != "Traceradvection" or getattr(r, "DCTEST_case", "") != "1-1"):
+                raise NotImplementedError("cuda backend: offline tracer advection with the DCMIP 1-1 winds only")
+        elif msc.tim.TIME_integ_type != "RK3":
+            raise NotImplementedError("cuda backend: RK3 time integration or TRCADV only")
         if r.TRC_ADV_TYPE != "MIURA2004" or not r.THUBURN_LIM:
             raise NotImplementedError("cuda backend: MIURA2004 tracer advection with Thuburn limiters only")
         nf = msc.numf

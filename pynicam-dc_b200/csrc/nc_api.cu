@@ -206,6 +206,11 @@ struct nc_handle {
   FieldPair flx_v, rhog_t, flx[6], xc[9], ch[6], cm[6], q, gq[3], qa[3], Qmin, Qmax;
   FieldPair vph[8];             // horizontal terms of vp0 (div1, div2, dd, dpg)
   const double* hs_lat = nullptr;   // Held-Suarez latitude planes (optional)
+  // offline tracer advection (integ_type TRCADV, DCMIP2012 test 1-1 winds)
+  bool trcadv = false;
+  double* trc_time = nullptr;       // model time of the prescribed winds (device scalar)
+  const double *trc_lon = nullptr, *trc_lat = nullptr, *trc_zf = nullptr, *trc_zh = nullptr;
+  const double *trc_lon_pl = nullptr, *trc_lat_pl = nullptr, *trc_zf_pl = nullptr, *trc_zh_pl = nullptr;
   // the pole columns run on a second stream between the operations that mix
   // regional and pole data (halo exchanges, tracer density update)
   cudaStream_t stream2 = nullptr;
@@ -665,98 +670,127 @@ static int run_step(nc_handle* h) {
       PHASE();
       continue;
     }
-    // ---- tracer advection (mod_src_tracer.py:83-1228)
-    const double dt = h->dtl;
-    for (int pole = 0; pole < 2; ++pole) {
-      TrcFluxArgs ta;
-      auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
-      ta.rvx = F(h->PM[1]); ta.rvy = F(h->PM[2]); ta.rvz = F(h->PM[3]); ta.rw = F(h->PM[4]);
-      ta.rhog_in = F(h->P0[0]); ta.frhog = F(h->frhog); ta.flx_v = F(h->flx_v); ta.rhog_t = F(h->rhog_t);
-      ta.dt = dt;
-      if (!pole) k_trc_vflux<<<greg, kBlock, 0, s>>>(ta, 0);
-      else k_trc_vflux<<<1, 32, 0, ps>>>(ta, 1);
-      TRY(check_launch(h, pole ? "trc_vflux_pl" : "trc_vflux"));
+  }
+  if (h->trcadv) {
+    // offline tracer advection (integ_type TRCADV, mod_dynamics.py:2030-2085): the
+    // tracers move with the current PROG (as the mean state, rhog_in = PROG0) and
+    // no density tendency
+    for (int v = 0; v < 5; ++v) {
+      CU(cudaMemcpyAsync(h->PM[v].r, h->P[v].r, D.npt * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      CU(cudaMemcpyAsync(h->PM[v].p, h->P[v].p, D.npl * sizeof(double), cudaMemcpyDeviceToDevice, s));
     }
-    auto vadv = [&](int iq, bool second) -> int {
-      for (int pole = 0; pole < 2; ++pole) {
-        TrcVadvArgs va;
-        auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
-        va.rhogq = F(h->Pq[iq]);
-        va.den = second ? F(h->rhog_t) : F(h->P0[0]);
-        va.flx_v = F(h->flx_v); va.frhog = F(h->frhog);
-        va.dt = dt; va.bcoef = 0.0; va.clamp = second ? 1 : 0; va.dtl = dt;
-        if (!pole) k_trc_vadv<<<greg, kBlock, 0, s>>>(va, 0);
-        else k_trc_vadv<<<1, 32, 0, ps>>>(va, 1);
-        TRY(check_launch(h, pole ? "trc_vadv_pl" : "trc_vadv"));
-      }
-      return 0;
-    };
-    // first vertical step uses the density at the start of the step; the
-    // Courant numbers of the first step are those of rhog_in
-    for (int iq = 0; iq < D.nq; ++iq) TRY(vadv(iq, false));
-    PHASE();
-    {
-      TrcHfluxArgs ha;
-      ha.rho = h->PM[0].r; ha.rvx = h->PM[1].r; ha.rvy = h->PM[2].r; ha.rvz = h->PM[3].r; ha.rhog_t = h->rhog_t.r;
-      for (int f = 0; f < 6; ++f) { ha.flx[f] = h->flx[f].r; ha.ch[f] = h->ch[f].r; ha.cm[f] = h->cm[f].r; }
-      for (int f = 0; f < 9; ++f) ha.xc[f] = h->xc[f].r;
-      ha.dt = dt;
-      k_trc_hflux<<<greg, kBlock, 0, s>>>(ha);
-      TRY(check_launch(h, "trc_hflux"));
-      TrcHfluxPlArgs hp;
-      hp.rho = h->PM[0].p; hp.rvx = h->PM[1].p; hp.rvy = h->PM[2].p; hp.rvz = h->PM[3].p; hp.rhog_t = h->rhog_t.p;
-      hp.flx = h->flx[0].p; hp.xc = h->xc[0].p; hp.ch = h->ch[0].p; hp.cm = h->cm[0].p; hp.dt = dt;
-      k_trc_hflux_pl<<<1, plk, 0, ps>>>(hp);
-      TRY(check_launch(h, "trc_hflux_pl"));
-    }
-    PHASE();
-    for (int iq = 0; iq < D.nq; ++iq) {
-      k_trc_grad<<<greg, kBlock, 0, s>>>(h->Pq[iq].r, h->rhog_t.r, h->q.r,
-                                                                               h->gq[0].r, h->gq[1].r, h->gq[2].r);
-      TRY(check_launch(h, "trc_grad"));
-      k_trc_grad_pl<<<1, plk, 0, ps>>>(h->Pq[iq].p, h->rhog_t.p, h->q.p, h->gq[0].p, h->gq[1].p, h->gq[2].p);
-      TRY(check_launch(h, "trc_grad_pl"));
-      TRY(comm(h, {h->gq[0], h->gq[1], h->gq[2]}));
-      TrcRemapArgs ra;
-      ra.q = h->q.r; ra.gq0 = h->gq[0].r; ra.gq1 = h->gq[1].r; ra.gq2 = h->gq[2].r;
-      for (int f = 0; f < 9; ++f) ra.xc[f] = h->xc[f].r;
-      for (int f = 0; f < 6; ++f) ra.cm[f] = h->cm[f].r;
-      for (int f = 0; f < 3; ++f) ra.qa[f] = h->qa[f].r;
-      k_trc_remap<<<greg, kBlock, 0, s>>>(ra);
-      TRY(check_launch(h, "trc_remap"));
-      TrcRemapPlArgs rp;
-      rp.q = h->q.p; rp.gq0 = h->gq[0].p; rp.gq1 = h->gq[1].p; rp.gq2 = h->gq[2].p; rp.xc = h->xc[0].p;
-      rp.cm = h->cm[0].p; rp.qa = h->qa[0].p;
-      k_trc_remap_pl<<<1, plk, 0, ps>>>(rp);
-      TRY(check_launch(h, "trc_remap_pl"));
-      TrcLimArgs la;
-      la.q = h->q.r; la.rhog_t = h->rhog_t.r; la.frhog = h->frhog.r;
-      for (int f = 0; f < 6; ++f) { la.ch[f] = h->ch[f].r; la.cm[f] = h->cm[f].r; la.flx[f] = h->flx[f].r; }
-      for (int f = 0; f < 3; ++f) la.qa[f] = h->qa[f].r;
-      la.qout_min = h->Qmin.r; la.qout_max = h->Qmax.r; la.Qmin = h->Qmin.r; la.Qmax = h->Qmax.r;
-      la.rhogq = h->Pq[iq].r; la.dt = dt;
-      TrcLimPlArgs lp;
-      lp.q = h->q.p; lp.ch = h->ch[0].p; lp.cm = h->cm[0].p; lp.rhog_t = h->rhog_t.p; lp.frhog = h->frhog.p;
-      lp.qa = h->qa[0].p; lp.flx = h->flx[0].p; lp.Qmin = h->Qmin.p; lp.Qmax = h->Qmax.p;
-      lp.qout_min = h->Qmin.p; lp.qout_max = h->Qmax.p; lp.rhogq = h->Pq[iq].p; lp.dt = dt;
-      k_trc_qout<<<greg, kBlock, 0, s>>>(la);
-      TRY(check_launch(h, "trc_qout"));
-      k_trc_qout_pl<<<1, plk, 0, ps>>>(lp);
-      TRY(check_launch(h, "trc_qout_pl"));
-      TRY(comm(h, {h->Qmin, h->Qmax}));
-      k_trc_apply<<<greg, kBlock, 0, s>>>(la);
-      TRY(check_launch(h, "trc_apply"));
-      k_trc_apply_pl<<<1, plk, 0, ps>>>(lp);
-      TRY(check_launch(h, "trc_apply_pl"));
-    }
-    PHASE();
+    CU(cudaMemsetAsync(h->frhog.r, 0, D.npt * sizeof(double), s));
+    CU(cudaMemsetAsync(h->frhog.p, 0, D.npl * sizeof(double), s));
     TRY(join_pl(h));
-    k_trc_rhog<<<gkl, kBlock, 0, s>>>(h->rhog_t.r, h->flx[0].r, h->flx[1].r, h->flx[2].r, h->flx[3].r, h->flx[4].r,
-                                       h->flx[5].r, h->frhog.r, dt, h->flx[0].p, h->rhog_t.p, h->frhog.p);
-    TRY(check_launch(h, "trc_rhog"));
     TRY(fork_pl(h));
-    for (int iq = 0; iq < D.nq; ++iq) TRY(vadv(iq, true));
-    PHASE();
+  }
+  // ---- tracer advection (mod_src_tracer.py:83-1228), after the last RK stage
+  const double dt = h->dtl;
+  for (int pole = 0; pole < 2; ++pole) {
+    TrcFluxArgs ta;
+    auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
+    ta.rvx = F(h->PM[1]); ta.rvy = F(h->PM[2]); ta.rvz = F(h->PM[3]); ta.rw = F(h->PM[4]);
+    ta.rhog_in = F(h->P0[0]); ta.frhog = F(h->frhog); ta.flx_v = F(h->flx_v); ta.rhog_t = F(h->rhog_t);
+    ta.dt = dt;
+    if (!pole) k_trc_vflux<<<greg, kBlock, 0, s>>>(ta, 0);
+    else k_trc_vflux<<<1, 32, 0, ps>>>(ta, 1);
+    TRY(check_launch(h, pole ? "trc_vflux_pl" : "trc_vflux"));
+  }
+  auto vadv = [&](int iq, bool second) -> int {
+    for (int pole = 0; pole < 2; ++pole) {
+      TrcVadvArgs va;
+      auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
+      va.rhogq = F(h->Pq[iq]);
+      va.den = second ? F(h->rhog_t) : F(h->P0[0]);
+      va.flx_v = F(h->flx_v); va.frhog = F(h->frhog);
+      va.dt = dt; va.bcoef = 0.0; va.clamp = second ? 1 : 0; va.dtl = dt;
+      if (!pole) k_trc_vadv<<<greg, kBlock, 0, s>>>(va, 0);
+      else k_trc_vadv<<<1, 32, 0, ps>>>(va, 1);
+      TRY(check_launch(h, pole ? "trc_vadv_pl" : "trc_vadv"));
+    }
+    return 0;
+  };
+  // first vertical step uses the density at the start of the step; the
+  // Courant numbers of the first step are those of rhog_in
+  for (int iq = 0; iq < D.nq; ++iq) TRY(vadv(iq, false));
+  PHASE();
+  {
+    TrcHfluxArgs ha;
+    ha.rho = h->PM[0].r; ha.rvx = h->PM[1].r; ha.rvy = h->PM[2].r; ha.rvz = h->PM[3].r; ha.rhog_t = h->rhog_t.r;
+    for (int f = 0; f < 6; ++f) { ha.flx[f] = h->flx[f].r; ha.ch[f] = h->ch[f].r; ha.cm[f] = h->cm[f].r; }
+    for (int f = 0; f < 9; ++f) ha.xc[f] = h->xc[f].r;
+    ha.dt = dt;
+    k_trc_hflux<<<greg, kBlock, 0, s>>>(ha);
+    TRY(check_launch(h, "trc_hflux"));
+    TrcHfluxPlArgs hp;
+    hp.rho = h->PM[0].p; hp.rvx = h->PM[1].p; hp.rvy = h->PM[2].p; hp.rvz = h->PM[3].p; hp.rhog_t = h->rhog_t.p;
+    hp.flx = h->flx[0].p; hp.xc = h->xc[0].p; hp.ch = h->ch[0].p; hp.cm = h->cm[0].p; hp.dt = dt;
+    k_trc_hflux_pl<<<1, plk, 0, ps>>>(hp);
+    TRY(check_launch(h, "trc_hflux_pl"));
+  }
+  PHASE();
+  for (int iq = 0; iq < D.nq; ++iq) {
+    k_trc_grad<<<greg, kBlock, 0, s>>>(h->Pq[iq].r, h->rhog_t.r, h->q.r,
+                                                                             h->gq[0].r, h->gq[1].r, h->gq[2].r);
+    TRY(check_launch(h, "trc_grad"));
+    k_trc_grad_pl<<<1, plk, 0, ps>>>(h->Pq[iq].p, h->rhog_t.p, h->q.p, h->gq[0].p, h->gq[1].p, h->gq[2].p);
+    TRY(check_launch(h, "trc_grad_pl"));
+    TRY(comm(h, {h->gq[0], h->gq[1], h->gq[2]}));
+    TrcRemapArgs ra;
+    ra.q = h->q.r; ra.gq0 = h->gq[0].r; ra.gq1 = h->gq[1].r; ra.gq2 = h->gq[2].r;
+    for (int f = 0; f < 9; ++f) ra.xc[f] = h->xc[f].r;
+    for (int f = 0; f < 6; ++f) ra.cm[f] = h->cm[f].r;
+    for (int f = 0; f < 3; ++f) ra.qa[f] = h->qa[f].r;
+    k_trc_remap<<<greg, kBlock, 0, s>>>(ra);
+    TRY(check_launch(h, "trc_remap"));
+    TrcRemapPlArgs rp;
+    rp.q = h->q.p; rp.gq0 = h->gq[0].p; rp.gq1 = h->gq[1].p; rp.gq2 = h->gq[2].p; rp.xc = h->xc[0].p;
+    rp.cm = h->cm[0].p; rp.qa = h->qa[0].p;
+    k_trc_remap_pl<<<1, plk, 0, ps>>>(rp);
+    TRY(check_launch(h, "trc_remap_pl"));
+    TrcLimArgs la;
+    la.q = h->q.r; la.rhog_t = h->rhog_t.r; la.frhog = h->frhog.r;
+    for (int f = 0; f < 6; ++f) { la.ch[f] = h->ch[f].r; la.cm[f] = h->cm[f].r; la.flx[f] = h->flx[f].r; }
+    for (int f = 0; f < 3; ++f) la.qa[f] = h->qa[f].r;
+    la.qout_min = h->Qmin.r; la.qout_max = h->Qmax.r; la.Qmin = h->Qmin.r; la.Qmax = h->Qmax.r;
+    la.rhogq = h->Pq[iq].r; la.dt = dt;
+    TrcLimPlArgs lp;
+    lp.q = h->q.p; lp.ch = h->ch[0].p; lp.cm = h->cm[0].p; lp.rhog_t = h->rhog_t.p; lp.frhog = h->frhog.p;
+    lp.qa = h->qa[0].p; lp.flx = h->flx[0].p; lp.Qmin = h->Qmin.p; lp.Qmax = h->Qmax.p;
+    lp.qout_min = h->Qmin.p; lp.qout_max = h->Qmax.p; lp.rhogq = h->Pq[iq].p; lp.dt = dt;
+    k_trc_qout<<<greg, kBlock, 0, s>>>(la);
+    TRY(check_launch(h, "trc_qout"));
+    k_trc_qout_pl<<<1, plk, 0, ps>>>(lp);
+    TRY(check_launch(h, "trc_qout_pl"));
+    TRY(comm(h, {h->Qmin, h->Qmax}));
+    k_trc_apply<<<greg, kBlock, 0, s>>>(la);
+    TRY(check_launch(h, "trc_apply"));
+    k_trc_apply_pl<<<1, plk, 0, ps>>>(lp);
+    TRY(check_launch(h, "trc_apply_pl"));
+  }
+  PHASE();
+  TRY(join_pl(h));
+  k_trc_rhog<<<gkl, kBlock, 0, s>>>(h->rhog_t.r, h->flx[0].r, h->flx[1].r, h->flx[2].r, h->flx[3].r, h->flx[4].r,
+                                     h->flx[5].r, h->frhog.r, dt, h->flx[0].p, h->rhog_t.p, h->frhog.p);
+  TRY(check_launch(h, "trc_rhog"));
+  TRY(fork_pl(h));
+  for (int iq = 0; iq < D.nq; ++iq) TRY(vadv(iq, true));
+  PHASE();
+  if (h->trcadv) {
+    // the prescribed winds of the next time (mod_forcing.py forcing_update)
+    TRY(join_pl(h));
+    k_trcadv_time<<<1, 1, 0, s>>>(h->trc_time, h->dtl);
+    TRY(check_launch(h, "trcadv_time"));
+    TrcWindArgs w;
+    for (int v = 0; v < 6; ++v) w.P.v[v] = h->P[v].r;
+    w.lon = h->trc_lon; w.lat = h->trc_lat; w.zf = h->trc_zf; w.zh = h->trc_zh; w.time = h->trc_time;
+    w.a = 6371220.0; w.Rd = 287.0; w.g = 9.80616; w.pi = 3.141592653589793238;
+    k_trcadv_winds<<<npt_blocks, kBlock, 0, s>>>(w, 0);
+    TRY(check_launch(h, "trcadv_winds"));
+    for (int v = 0; v < 6; ++v) w.P.v[v] = h->P[v].p;
+    w.lon = h->trc_lon_pl; w.lat = h->trc_lat_pl; w.zf = h->trc_zf_pl; w.zh = h->trc_zh_pl;
+    k_trcadv_winds<<<npl_blocks, kBlock, 0, s>>>(w, 1);
+    TRY(check_launch(h, "trcadv_winds_pl"));
   }
   // marshal-out halo exchange of PRG_var (mod_dynamics.py:2726-2727)
   TRY(comm_prg(h));
@@ -926,8 +960,13 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
     const nc_array* cvw = T.get("CVW");
     if (!cvw || cvw->dtype != NC_F64 || numel(cvw) < 1) return fail(NC_ERR_ARG, "missing CVW");
     C.CVW0 = ((const double*)cvw->data)[0];
+    if (T.get("trcadv")) {
+      double f;
+      TRY(scalar(T, "trcadv", f));
+      h->trcadv = (f != 0.0);
+    }
     const nc_array* ss = T.get("sstep");
-    if (!ss || numel(ss) < 1 || numel(ss) > 4) return fail(NC_ERR_ARG, "missing sstep");
+    if (!ss || numel(ss) > 4 || (numel(ss) < 1 && !h->trcadv)) return fail(NC_ERR_ARG, "missing sstep");
     h->nstage = (int)numel(ss);
     for (int n = 0; n < h->nstage; ++n) {
       h->sstep[n] = (ss->dtype == NC_I64) ? (int)((const int64_t*)ss->data)[n] : (int)((const int32_t*)ss->data)[n];
@@ -969,6 +1008,18 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   TRY(up_reg(h, T, "GMTR_t_W", 1, 6, &Gm.GMTR_t));
   TRY(up_reg(h, T, "GMTR_a_HN", 1, 9, &Gm.GMTR_a));
   TRY(up_reg(h, T, "GMTR_p_RAREA", 1, 1, &Gm.GMTR_p));
+  if (h->trcadv) {   // the coordinates the prescribed winds are computed from
+    TRY(up_reg(h, T, "GRD_LON", 1, 1, &h->trc_lon));
+    TRY(up_reg(h, T, "GRD_LAT", 1, 1, &h->trc_lat));
+    TRY(up_reg(h, T, "GRD_Z", KA, 1, &h->trc_zf));
+    TRY(up_reg(h, T, "GRD_ZH", KA, 1, &h->trc_zh));
+    TRY(up_pl(h, T, "GRD_LON_pl", 6LL * D.LP, &h->trc_lon_pl));
+    TRY(up_pl(h, T, "GRD_LAT_pl", 6LL * D.LP, &h->trc_lat_pl));
+    TRY(up_pl(h, T, "GRD_Z_pl", D.npl, &h->trc_zf_pl));
+    TRY(up_pl(h, T, "GRD_ZH_pl", D.npl, &h->trc_zh_pl));
+    TRY(dev_alloc(h, &h->trc_time, 1));
+    CU(cudaMemset(h->trc_time, 0, sizeof(double)));
+  }
   if (T.get("AF_hs_lat_terms")) {   // Held-Suarez forcing configured (nc_forcing_step)
     if (!T.get("PRE00")) return fail(NC_ERR_ARG, "AF_hs_lat_terms given without PRE00");
     TRY(scalar(T, "PRE00", C.PRE00));

@@ -80,3 +80,78 @@ __global__ void k_forcing_hs(HsArgs a) {
 }
 
 }  // namespace nc
+
+namespace nc {
+
+// ---------------------------------------------------------------------------
+// Offline tracer advection (integ_type TRCADV): the prescribed winds of
+// DCMIP2012 test 1-1 set after each step (nhm/forcing/mod_forcing.py
+// forcing_update; nhm/forcing/mod_af_trcadv.py test11_velocity,
+// Sp_Unit_East / Sp_Unit_North).  exp, sin and cos are CUDA's, so the winds
+// can differ from numpy's in the last bits.
+// ---------------------------------------------------------------------------
+struct TrcWindArgs {
+  Prog P;                     // RHOGV{X,Y,Z}, RHOGW set to wind * RHOG
+  const double *lon, *lat;    // column longitude / latitude: regional [l][j][i], pole [g][l]
+  const double *zf, *zh;      // full / half-level height: regional [l][k][j][i], pole [g][k][l]
+  const double* time;         // model time of the winds (device scalar)
+  double a, Rd, g, pi;        // the test's constants (mod_af_trcadv.py:14-19)
+};
+
+__global__ void k_trcadv_time(double* time, double dt) { *time = *time + dt; }
+
+// one thread per point of the regional (pole == 0) or pole (pole != 0) grid
+__global__ void k_trcadv_winds(TrcWindArgs w, int pole) {
+  const int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
+  const int KA = cD.KA;
+  int p, c2;   // point index and column index of lon/lat
+  if (!pole) {
+    if (t >= cD.npti) return;
+    const int G = cD.G;
+    const int i = t % G, j = (t / G) % G, l = t / (G * G * KA);
+    p = t;
+    c2 = (l * G + j) * G + i;
+  } else {
+    if (t >= 6 * KA * cD.LP) return;
+    const int g = t / (KA * cD.LP), lp = t % cD.LP;
+    p = t;
+    c2 = g * cD.LP + lp;
+  }
+  const double time = *w.time;
+  const double a = w.a, pi = w.pi;
+  const double tau = 12.0 * 86400.0;
+  const double u0 = 2.0 * pi * a / tau;
+  const double k0 = 10.0 * a / tau;
+  const double omega0 = 23000.0 * pi / tau;
+  const double T0 = 300.0;
+  const double H = w.Rd * T0 / w.g;
+  const double p0 = 1000.E2;
+  const double dlon = 2.0 * pi * time / tau;
+  const double lon = w.lon[c2], lat = w.lat[c2];
+  const double lonp = lon - dlon;
+  const double bs = 0.2;
+  const double ptop = p0 * exp(-12000.0 / H);
+  // full level
+  double pf = p0 * exp(-w.zf[p] / H);
+  const double cl = cos(lat);
+  const double ud = (omega0 * a) / (bs * ptop) * cos(lonp) * (cl * cl) * cos(dlon) *
+                    (-exp((pf - p0) / (bs * ptop)) + exp((ptop - pf) / (bs * ptop)));
+  const double sl = sin(lonp);
+  const double u = k0 * sin(2.0 * lat) * (sl * sl) * cos(0.5 * dlon) + u0 * cl + ud;
+  const double v = k0 * sin(2.0 * lonp) * cl * cos(0.5 * dlon);
+  const double e0 = -sin(lon), e1 = cos(lon), e2 = 0.0;
+  const double n0 = -sin(lat) * cos(lon), n1 = -sin(lat) * sin(lon), n2 = cl;
+  const double vx = e0 * u + n0 * v, vy = e1 * u + n1 * v, vz = e2 * u + n2 * v;
+  // half level
+  const double ph = p0 * exp(-w.zh[p] / H);
+  const double s = (1.0 + exp((ptop - p0) / (bs * ptop)) - exp((ph - p0) / (bs * ptop)) -
+                    exp((ptop - ph) / (bs * ptop)));
+  const double ww = -(w.Rd * T0) / (w.g * ph) * omega0 * sl * cl * cos(dlon) * s;
+  const double rg = w.P.v[0][p];
+  w.P.v[1][p] = vx * rg;
+  w.P.v[2][p] = vy * rg;
+  w.P.v[3][p] = vz * rg;
+  w.P.v[4][p] = ww * rg;
+}
+
+}  // namespace nc

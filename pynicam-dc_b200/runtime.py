@@ -154,7 +154,15 @@ def setup_table(geo: dict) -> dict:
     t["GMTR_t_W"] = np.ascontiguousarray(np.asarray(geo["GMTR_t"])[..., 2:5], np.float64)
     t["GMTR_a_HN"] = np.ascontiguousarray(np.asarray(geo["GMTR_a"])[..., 0:3], np.float64)
     t["GMTR_p_RAREA"] = np.ascontiguousarray(np.asarray(geo["GMTR_p"])[..., 1:2], np.float64)
-    if "GRD_LAT" in geo:   # Held-Suarez forcing: latitude terms with the reference's numpy expressions
+    trcadv = str(np.asarray(geo.get("integ_type", "RK3"))) == "TRCADV"
+    if trcadv:   # offline tracer advection: the coordinates the prescribed winds are computed from
+        t["trcadv"] = np.asarray(1.0, np.float64)
+        G, L = int(_scalar(geo["gall_1d"])), int(_scalar(geo["lall"]))
+        for k in ("GRD_LON", "GRD_LAT"):
+            t[k] = np.ascontiguousarray(np.asarray(geo[k], np.float64).reshape(G, G, 1, L))
+        for k in ("GRD_Z", "GRD_ZH", "GRD_LON_pl", "GRD_LAT_pl", "GRD_Z_pl", "GRD_ZH_pl"):
+            t[k] = np.ascontiguousarray(geo[k], np.float64)
+    if "GRD_LAT" in geo and not trcadv:   # Held-Suarez forcing: latitude terms with the reference's numpy expressions
         lat = np.asarray(geo["GRD_LAT"], np.float64)
         lat = lat.reshape(lat.shape[0], lat.shape[1], 1, lat.shape[-1])
         sinlat, coslat = np.abs(np.sin(lat)), np.abs(np.cos(lat))

@@ -36,3 +36,15 @@ def golden_hs():
     geo, st = load(os.path.join(GOLDEN, "gl03_z10_hs.npz"))
     lat = geo.pop("GRD_LAT")
     return geo, lat, st
+
+
+TRC_COORDS = ("GRD_LON", "GRD_LAT", "GRD_Z", "GRD_ZH", "GRD_LON_pl", "GRD_LAT_pl", "GRD_Z_pl", "GRD_ZH_pl")
+
+
+@pytest.fixture(scope="session")
+def golden_trcadv():
+    """gl03 z10 DCMIP 1-1 offline tracer advection run by the reference
+    (make_trcadv.py): setup arrays (including integ_type and the coordinates
+    the prescribed winds read) and four states"""
+    from make_golden import load
+    return load(os.path.join(GOLDEN, "gl03_z10_trcadv.npz"))

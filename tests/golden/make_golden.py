@@ -83,7 +83,7 @@ RGNMNG_out_fname='tempout'
 """
 
 
-def prep(ref: str, case_dir: str, gl: int, vl: int, ztop: float):
+def prep(ref: str, case_dir: str, gl: int, vl: int, ztop: float, layer_type: str = "ULLRICH14"):
     os.makedirs(os.path.join(case_dir, "case", "config"), exist_ok=True)
     os.makedirs(os.path.join(case_dir, "case", "prepdata"), exist_ok=True)
     work = os.path.join(case_dir, "a", "b")
@@ -94,7 +94,7 @@ def prep(ref: str, case_dir: str, gl: int, vl: int, ztop: float):
     with open(os.path.join(cfg, "mkrawgrid.toml"), "w") as f:
         f.write(MKRAWGRID_TOML.format(gl=gl))
     with open(os.path.join(cfg, "mkvlayer.toml"), "w") as f:
-        f.write(f"[mkvlayer]\nnum_of_layer = {vl}\nlayer_type = 'ULLRICH14'\nztop = {ztop}\n"
+        f.write(f"[mkvlayer]\nnum_of_layer = {vl}\nlayer_type = '{layer_type}'\nztop = {ztop}\n"
                 "outfname = '../../case/prepdata/vgrid.json'\n")
     P = os.path.join(ref, "pynicamdc", "prep")
     run = lambda *a: subprocess.run([sys.executable, *a], cwd=work, check=True, capture_output=True)

@@ -39,3 +39,22 @@ def test_held_suarez_fixture_is_forced(golden, golden_hs):
     assert np.array_equal(st["state0"], st0["state0"])
     d = np.abs(st["state1"][..., 1:4] - st0["state1"][..., 1:4]).max()
     assert d > 0.0
+
+
+def test_oracle_trcadv_matches_reference_three_steps(golden_trcadv):
+    """offline tracer advection (integ_type TRCADV, DCMIP 1-1 winds) against
+    the reference's own run (tests/golden/make_trcadv.py)"""
+    from conftest import TRC_COORDS
+    geo, st = golden_trcadv
+    geo = dict(geo)
+    co = [geo.pop(k) for k in TRC_COORDS]
+    assert str(geo.pop("integ_type")) == "TRCADV"
+    G = O.Geo(geo)
+    s, sp = st["state0"], st["state0_pl"]
+    for n in (1, 2, 3):
+        s, sp = O.trcadv_step(G, s, sp, n * G.dtl, *co)
+        assert np.array_equal(s, st[f"state{n}"]), f"step {n} regional"
+        assert np.array_equal(sp, st[f"state{n}_pl"]), f"step {n} pole"
+    # four passive tracers were advected and the winds were reset every step
+    assert np.abs(st["state3"][..., 7:11] - st["state0"][..., 7:11]).max() > 0.0
+    assert np.abs(st["state2"][..., 1:5] - st["state1"][..., 1:5]).max() > 0.0
