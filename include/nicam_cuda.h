@@ -57,13 +57,26 @@ int nc_create(const nc_array* arrays, int32_t narrays, nc_handle** out);
 
 /* Marshal-in of the prognostic state (mod_dynamics.py:1876-1880) from host
  * memory in the reference layout: prg (gall_1d, gall_1d, kall, lall, 6+nq),
- * prg_pl (6, kall, 2, 6+nq), both C-order float64.  Pinned host memory gives
- * the fastest copy. */
+ * prg_pl (6, kall, 2, 6+nq), both C-order float64.  The copy runs on the
+ * handle's upload stream and the steps queued after this call wait for it;
+ * from pinned host memory it is asynchronous (keep the host buffer unchanged
+ * until nc_sync), from pageable memory the call returns after the copy. */
 int nc_upload_state(nc_handle* h, const double* prg, const double* prg_pl);
 
 /* Marshal-out (Dyn.sync_prgvar_to_host, mod_dynamics.py:429-440) into host
- * memory in the same layout. */
+ * memory in the same layout, after every step queued before the call;
+ * returns when the host arrays hold the state. */
 int nc_download_state(nc_handle* h, double* prg, double* prg_pl);
+
+/* nc_download_state without the wait: the copy runs on the handle's download
+ * stream, overlapping the steps queued after this call (into pinned host
+ * memory); the host arrays hold the state after nc_sync.  No counterpart in
+ * the reference (its drain to host is synchronous). */
+int nc_download_state_async(nc_handle* h, double* prg, double* prg_pl);
+
+/* Make the handle's stream wait for the last upload and download copies, so
+ * that work or an event queued on it afterwards follows them. */
+int nc_join_copies(nc_handle* h);
 
 /* nsteps large steps of Dyn.dynamics_step (mod_dynamics.py:1725-2741) on the
  * device-resident state.  Asynchronous on the handle's stream. */
@@ -77,7 +90,7 @@ int nc_set_graph(nc_handle* h, int32_t enable);
  * of Dyn.dynamics_step), without graph capture, then synchronize. */
 int nc_run_phases(nc_handle* h, int32_t nphases);
 
-/* Wait for the handle's stream. */
+/* Wait for the handle's streams (steps, uploads and downloads). */
 int nc_sync(nc_handle* h);
 
 /* Global sums of the embudget monitor (nhm/share/mod_embudget.py:74-80,

@@ -215,6 +215,12 @@ struct nc_handle {
   // regional and pole data (halo exchanges, tracer density update)
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // host<->device copies on their own streams (one per direction), so that a
+  // state upload or download overlaps the steps on the library stream; the
+  // download stages through its own buffer
+  cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
+  cudaEvent_t ev_in_ready = nullptr, ev_in_free = nullptr, ev_out_ready = nullptr, ev_out_done = nullptr;
+  double *stage_out = nullptr, *stage_out_pl = nullptr;
   // per-kernel timing (opt-in, eager launches only): an event after every
   // launch; a kernel's time is the gap to the previous event on the stream
   bool prof = false;
@@ -1149,12 +1155,18 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   }
   TRY(dev_alloc(h, &h->stage, (size_t)D.npt * (6 + D.nq)));
   TRY(dev_alloc(h, &h->stage_pl, (size_t)D.npl * (6 + D.nq)));
+  TRY(dev_alloc(h, &h->stage_out, (size_t)D.npt * (6 + D.nq)));
+  TRY(dev_alloc(h, &h->stage_out_pl, (size_t)D.npl * (6 + D.nq)));
   h->mass_blocks = (int)((D.npt2 + D.LP + 255) / 256);
   TRY(dev_alloc(h, &h->mass_part, (size_t)h->mass_blocks * 2));
   CU(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   CU(cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking));
   CU(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
   CU(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+  CU(cudaStreamCreateWithFlags(&h->s_h2d, cudaStreamNonBlocking));
+  CU(cudaStreamCreateWithFlags(&h->s_d2h, cudaStreamNonBlocking));
+  for (cudaEvent_t* e : {&h->ev_in_ready, &h->ev_in_free, &h->ev_out_ready, &h->ev_out_done})
+    CU(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   return 0;
 }
 
@@ -1183,6 +1195,12 @@ void nc_destroy(nc_handle* h) {
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   for (void* p : h->allocs) cudaFree(p);
   if (h->stream2) cudaStreamSynchronize(h->stream2);
+  for (cudaStream_t st : {h->s_h2d, h->s_d2h})
+    if (st) cudaStreamSynchronize(st);
+  for (cudaEvent_t e : {h->ev_in_ready, h->ev_in_free, h->ev_out_ready, h->ev_out_done})
+    if (e) cudaEventDestroy(e);
+  for (cudaStream_t st : {h->s_h2d, h->s_d2h})
+    if (st) cudaStreamDestroy(st);
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
   if (h->ev_join) cudaEventDestroy(h->ev_join);
   if (h->stream2) cudaStreamDestroy(h->stream2);
@@ -1203,13 +1221,38 @@ int nc_upload_state(nc_handle* h, const double* prg, const double* prg_pl) {
   TRY(load_consts(h));
   const Dims& D = h->D;
   const int nv = 6 + D.nq;
-  CU(cudaMemcpyAsync(h->stage, prg, (size_t)D.npt * nv * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-  CU(cudaMemcpyAsync(h->stage_pl, prg_pl, (size_t)D.npl * nv * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  // copy on the upload stream once the staging buffer's last unpack is done,
+  // then unpack on the library stream behind everything already queued there
+  CU(cudaStreamWaitEvent(h->s_h2d, h->ev_in_free, 0));
+  CU(cudaMemcpyAsync(h->stage, prg, (size_t)D.npt * nv * sizeof(double), cudaMemcpyHostToDevice, h->s_h2d));
+  CU(cudaMemcpyAsync(h->stage_pl, prg_pl, (size_t)D.npl * nv * sizeof(double), cudaMemcpyHostToDevice, h->s_h2d));
+  CU(cudaEventRecord(h->ev_in_ready, h->s_h2d));
+  CU(cudaStreamWaitEvent(h->stream, h->ev_in_ready, 0));
   long long n = D.npt + D.npl;
   k_unpack<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->stage, h->stage_pl, state_ptrs(h, false),
                                                                  state_ptrs(h, true), nv);
   TRY(check_launch(h, "unpack"));
+  CU(cudaEventRecord(h->ev_in_free, h->stream));
   h->have_state = true;
+  return 0;
+}
+
+// pack the state into the download staging buffer on the library stream and
+// copy it out on the download stream
+static int download_issue(nc_handle* h, double* prg, double* prg_pl) {
+  const Dims& D = h->D;
+  const int nv = 6 + D.nq;
+  long long n = D.npt + D.npl;
+  CU(cudaStreamWaitEvent(h->stream, h->ev_out_done, 0));   // the previous download has left the buffer
+  k_pack<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->stage_out, h->stage_out_pl, state_ptrs(h, false),
+                                                               state_ptrs(h, true), nv);
+  TRY(check_launch(h, "pack"));
+  CU(cudaEventRecord(h->ev_out_ready, h->stream));
+  CU(cudaStreamWaitEvent(h->s_d2h, h->ev_out_ready, 0));
+  CU(cudaMemcpyAsync(prg, h->stage_out, (size_t)D.npt * nv * sizeof(double), cudaMemcpyDeviceToHost, h->s_d2h));
+  CU(cudaMemcpyAsync(prg_pl, h->stage_out_pl, (size_t)D.npl * nv * sizeof(double), cudaMemcpyDeviceToHost,
+                     h->s_d2h));
+  CU(cudaEventRecord(h->ev_out_done, h->s_d2h));
   return 0;
 }
 
@@ -1217,15 +1260,22 @@ int nc_download_state(nc_handle* h, double* prg, double* prg_pl) {
   if (!h || !prg || !prg_pl) return fail(NC_ERR_ARG, "nc_download_state: null argument");
   if (!h->have_state) return fail(NC_ERR_STATE, "nc_download_state: no state uploaded");
   TRY(load_consts(h));
-  const Dims& D = h->D;
-  const int nv = 6 + D.nq;
-  long long n = D.npt + D.npl;
-  k_pack<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->stage, h->stage_pl, state_ptrs(h, false),
-                                                               state_ptrs(h, true), nv);
-  TRY(check_launch(h, "pack"));
-  CU(cudaMemcpyAsync(prg, h->stage, (size_t)D.npt * nv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaMemcpyAsync(prg_pl, h->stage_pl, (size_t)D.npl * nv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaStreamSynchronize(h->stream));
+  TRY(download_issue(h, prg, prg_pl));
+  CU(cudaEventSynchronize(h->ev_out_done));
+  return 0;
+}
+
+int nc_download_state_async(nc_handle* h, double* prg, double* prg_pl) {
+  if (!h || !prg || !prg_pl) return fail(NC_ERR_ARG, "nc_download_state_async: null argument");
+  if (!h->have_state) return fail(NC_ERR_STATE, "nc_download_state_async: no state uploaded");
+  TRY(load_consts(h));
+  return download_issue(h, prg, prg_pl);
+}
+
+int nc_join_copies(nc_handle* h) {
+  if (!h) return fail(NC_ERR_ARG, "nc_join_copies: null handle");
+  CU(cudaStreamWaitEvent(h->stream, h->ev_in_ready, 0));
+  CU(cudaStreamWaitEvent(h->stream, h->ev_out_done, 0));
   return 0;
 }
 
@@ -1296,6 +1346,8 @@ int nc_run_phases(nc_handle* h, int32_t nphases) {
 int nc_sync(nc_handle* h) {
   if (!h) return fail(NC_ERR_ARG, "nc_sync: null handle");
   CU(cudaStreamSynchronize(h->stream));
+  CU(cudaStreamSynchronize(h->s_h2d));
+  CU(cudaStreamSynchronize(h->s_d2h));
   return 0;
 }
 

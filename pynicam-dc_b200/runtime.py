@@ -30,8 +30,8 @@ class NcArray(ctypes.Structure):
 _lib = None
 
 # every entry point declared in include/nicam_cuda.h
-EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync",
-           "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",
+EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_state_async", "nc_join_copies",
+           "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",
            "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_forcing_step", "nc_last_error",
            "nc_destroy")
 
@@ -48,6 +48,8 @@ def load_library(path: str = LIB_PATH):
     lib.nc_create.argtypes = [ctypes.POINTER(NcArray), i32, ctypes.POINTER(vp)]
     lib.nc_upload_state.argtypes = [vp, dp, dp]
     lib.nc_download_state.argtypes = [vp, dp, dp]
+    lib.nc_download_state_async.argtypes = [vp, dp, dp]
+    lib.nc_join_copies.argtypes = [vp]
     lib.nc_step.argtypes = [vp, i32]
     lib.nc_set_graph.argtypes = [vp, i32]
     lib.nc_run_phases.argtypes = [vp, i32]
@@ -71,8 +73,8 @@ def load_library(path: str = LIB_PATH):
     lib.nc_forcing_step.restype = ctypes.c_int
     lib.nc_destroy.argtypes = [vp]
     lib.nc_destroy.restype = None
-    for f in ("nc_create", "nc_upload_state", "nc_download_state", "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync",
-              "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_stream", "nc_profile"):
+    for f in ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_state_async", "nc_join_copies",
+              "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_stream", "nc_profile"):
         getattr(lib, f).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -229,6 +231,15 @@ class NicamCuda:
 
     def download_ptr(self, prg_ptr: int, prg_pl_ptr: int):
         _check(self._lib.nc_download_state(self._h, prg_ptr, prg_pl_ptr))
+
+    def download_ptr_async(self, prg_ptr: int, prg_pl_ptr: int):
+        """download into raw (pinned) host pointers without waiting; the data
+        are there after sync()"""
+        _check(self._lib.nc_download_state_async(self._h, prg_ptr, prg_pl_ptr))
+
+    def join_copies(self):
+        """order the library stream after the last upload / download copies"""
+        _check(self._lib.nc_join_copies(self._h))
 
     def step(self, nsteps: int = 1):
         _check(self._lib.nc_step(self._h, int(nsteps)))
