@@ -82,38 +82,68 @@ struct VarPtrs {
   double* v[NC_MAXNQ + 6];
 };
 
-__global__ void k_unpack(const double* st, const double* st_pl, VarPtrs reg, VarPtrs pol, int nv) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < cD.npt) {
-    int i = (int)(t % cD.G);
-    long long r = t / cD.G;
-    int j = (int)(r % cD.G);
-    r /= cD.G;
-    int k = (int)(r % cD.KA);
-    int l = (int)(r / cD.KA);
-    long long src = ((((long long)i * cD.G + j) * cD.KA + k) * cD.L + l) * nv;
-    for (int v = 0; v < nv; ++v) reg.v[v][t] = st[src + v];
-  } else if (t < cD.npt + cD.npl) {
-    int q = (int)(t - cD.npt);
-    for (int v = 0; v < nv; ++v) pol.v[v][q] = st_pl[(long long)q * nv + v];
+// Tiled layout conversion of the regional state between the reference layout
+// (i, j, k, l, v) and the device fields [v][l][k][j][i].  For one (j, k), the
+// reference layout holds for every i a contiguous run over (l, v); the device
+// layout holds for every (v, l) a contiguous run over i.  A block moves an
+// UI x UC tile (UI values of i, UC consecutive (l, v) pairs) through shared
+// memory so that both sides are read and written in contiguous runs.
+#define UI 32
+#define UC 128
+__global__ void __launch_bounds__(256) k_unpack_t(const double* st, VarPtrs reg, int nv) {
+  __shared__ double tile[UI][UC + 1];
+  const int G = cD.G, KA = cD.KA, L = cD.L;
+  const int i0 = (int)blockIdx.x * UI, c0 = (int)blockIdx.y * UC;
+  const int jk = (int)blockIdx.z, k = jk % KA, j = jk / KA;
+  const int ncl = L * nv;
+  for (int t = threadIdx.x; t < UI * UC; t += blockDim.x) {
+    const int ii = t / UC, cc = t % UC;
+    const int i = i0 + ii, c = c0 + cc;
+    if (i < G && c < ncl) tile[ii][cc] = st[(((long long)i * G + j) * KA + k) * ncl + c];
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < UI * UC; t += blockDim.x) {
+    const int cc = t / UI, ii = t % UI;
+    const int i = i0 + ii, c = c0 + cc;
+    if (i < G && c < ncl) {
+      const int l = c / nv, v = c % nv;
+      reg.v[v][((l * KA + k) * G + j) * G + i] = tile[ii][cc];
+    }
   }
 }
 
-__global__ void k_pack(double* st, double* st_pl, VarPtrs reg, VarPtrs pol, int nv) {
-  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < cD.npt) {
-    int i = (int)(t % cD.G);
-    long long r = t / cD.G;
-    int j = (int)(r % cD.G);
-    r /= cD.G;
-    int k = (int)(r % cD.KA);
-    int l = (int)(r / cD.KA);
-    long long dst = ((((long long)i * cD.G + j) * cD.KA + k) * cD.L + l) * nv;
-    for (int v = 0; v < nv; ++v) st[dst + v] = reg.v[v][t];
-  } else if (t < cD.npt + cD.npl) {
-    int q = (int)(t - cD.npt);
-    for (int v = 0; v < nv; ++v) st_pl[(long long)q * nv + v] = pol.v[v][q];
+__global__ void __launch_bounds__(256) k_pack_t(double* st, VarPtrs reg, int nv) {
+  __shared__ double tile[UI][UC + 1];
+  const int G = cD.G, KA = cD.KA, L = cD.L;
+  const int i0 = (int)blockIdx.x * UI, c0 = (int)blockIdx.y * UC;
+  const int jk = (int)blockIdx.z, k = jk % KA, j = jk / KA;
+  const int ncl = L * nv;
+  for (int t = threadIdx.x; t < UI * UC; t += blockDim.x) {
+    const int cc = t / UI, ii = t % UI;
+    const int i = i0 + ii, c = c0 + cc;
+    if (i < G && c < ncl) {
+      const int l = c / nv, v = c % nv;
+      tile[ii][cc] = reg.v[v][((l * KA + k) * G + j) * G + i];
+    }
   }
+  __syncthreads();
+  for (int t = threadIdx.x; t < UI * UC; t += blockDim.x) {
+    const int ii = t / UC, cc = t % UC;
+    const int i = i0 + ii, c = c0 + cc;
+    if (i < G && c < ncl) st[(((long long)i * G + j) * KA + k) * ncl + c] = tile[ii][cc];
+  }
+}
+
+// the pole part of the layout conversion: (g, k, l, v) <-> fields [v][g][k][l]
+__global__ void k_unpack_pl(const double* st_pl, VarPtrs pol, int nv) {
+  const int q = (int)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= cD.npl) return;
+  for (int v = 0; v < nv; ++v) pol.v[v][q] = st_pl[(long long)q * nv + v];
+}
+__global__ void k_pack_pl(double* st_pl, VarPtrs pol, int nv) {
+  const int q = (int)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= cD.npl) return;
+  for (int v = 0; v < nv; ++v) st_pl[(long long)q * nv + v] = pol.v[v][q];
 }
 
 // ---------------------------------------------------------------------------
@@ -1228,10 +1258,11 @@ int nc_upload_state(nc_handle* h, const double* prg, const double* prg_pl) {
   CU(cudaMemcpyAsync(h->stage_pl, prg_pl, (size_t)D.npl * nv * sizeof(double), cudaMemcpyHostToDevice, h->s_h2d));
   CU(cudaEventRecord(h->ev_in_ready, h->s_h2d));
   CU(cudaStreamWaitEvent(h->stream, h->ev_in_ready, 0));
-  long long n = D.npt + D.npl;
-  k_unpack<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->stage, h->stage_pl, state_ptrs(h, false),
-                                                                 state_ptrs(h, true), nv);
+  const dim3 gt((unsigned)((D.G + UI - 1) / UI), (unsigned)((D.L * nv + UC - 1) / UC), (unsigned)(D.G * D.KA));
+  k_unpack_t<<<gt, 256, 0, h->stream>>>(h->stage, state_ptrs(h, false), nv);
   TRY(check_launch(h, "unpack"));
+  k_unpack_pl<<<(unsigned)((D.npl + 127) / 128), 128, 0, h->stream>>>(h->stage_pl, state_ptrs(h, true), nv);
+  TRY(check_launch(h, "unpack_pl"));
   CU(cudaEventRecord(h->ev_in_free, h->stream));
   h->have_state = true;
   return 0;
@@ -1242,11 +1273,12 @@ int nc_upload_state(nc_handle* h, const double* prg, const double* prg_pl) {
 static int download_issue(nc_handle* h, double* prg, double* prg_pl) {
   const Dims& D = h->D;
   const int nv = 6 + D.nq;
-  long long n = D.npt + D.npl;
   CU(cudaStreamWaitEvent(h->stream, h->ev_out_done, 0));   // the previous download has left the buffer
-  k_pack<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->stage_out, h->stage_out_pl, state_ptrs(h, false),
-                                                               state_ptrs(h, true), nv);
+  const dim3 gt((unsigned)((D.G + UI - 1) / UI), (unsigned)((D.L * nv + UC - 1) / UC), (unsigned)(D.G * D.KA));
+  k_pack_t<<<gt, 256, 0, h->stream>>>(h->stage_out, state_ptrs(h, false), nv);
   TRY(check_launch(h, "pack"));
+  k_pack_pl<<<(unsigned)((D.npl + 127) / 128), 128, 0, h->stream>>>(h->stage_out_pl, state_ptrs(h, true), nv);
+  TRY(check_launch(h, "pack_pl"));
   CU(cudaEventRecord(h->ev_out_ready, h->stream));
   CU(cudaStreamWaitEvent(h->s_d2h, h->ev_out_ready, 0));
   CU(cudaMemcpyAsync(prg, h->stage_out, (size_t)D.npt * nv * sizeof(double), cudaMemcpyDeviceToHost, h->s_d2h));
