@@ -773,7 +773,7 @@ __device__ void path1_column(const Path1Args& a, int i, int j, int l, int g, int
 // Regional path 1, one block per (level, tile): same stencils and
 // arithmetic as path1_column.  The blocks at kmin and kmax also write the
 // boundary rows kmin-1 and kmax+1 from the values they computed.
-__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(4)) k_path1_l(Path1Args a) {
+__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_path1_l(Path1Args a) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
   __shared__ double s_v[3][PY * PX];
   __shared__ double s_p[PY * PX];
@@ -968,7 +968,7 @@ __global__ void k_vimain_a(VimainArgs a, int pole) {
 
 // vi_main kernel A, one block per (level, tile): the horizontal divergences
 // of RGAM*diff_vh, RGAM*diff_vh*eth and RGAM*(rhogv + diff_vh)*ethtot0.
-__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(4)) k_vimain_a_l(VimainArgs a) {
+__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_vimain_a_l(VimainArgs a) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2;
   __shared__ double s_h[3][3][PY * PX];
   const TileLv tl = tile_level<DD_DX, DD_DY>(cD.kmin);
