@@ -600,10 +600,10 @@ __global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) 
 // half-level eth, the vertical kinetic-energy term) are formed and the ones at
 // k and k-1 are carried in registers.  Each value is the expression of
 // vp0_column (the pole form), so regional and pole columns round alike.
-// 256-thread blocks: at 72 registers three blocks fit an SM, and the
-// 676,000 columns of gl08 then fill 5.95 waves of the 148 SMs
+// 256-thread blocks capped at 64 registers (four per SM; measured faster
+// than three at 74 registers)
 #define NC_VP0C_BLOCK 256
-__global__ void __launch_bounds__(NC_VP0C_BLOCK) k_vp0_cr(Vp0Args a, Vp0H h) {
+__global__ void __launch_bounds__(NC_VP0C_BLOCK, 4) k_vp0_cr(Vp0Args a, Vp0H h) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l)) return;

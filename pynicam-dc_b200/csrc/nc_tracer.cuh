@@ -309,7 +309,7 @@ __global__ void k_trc_hflux_pl(TrcHfluxPlArgs a) {
 // ---------------------------------------------------------------------------
 // per tracer: q and its gradient (mod_src_tracer.py:758-771, 1634-1640)
 // ---------------------------------------------------------------------------
-__global__ void k_trc_grad(const double* rhogq, const double* rhog_t, double* q, double* gq0, double* gq1,
+__global__ void __launch_bounds__(128, 8) k_trc_grad(const double* rhogq, const double* rhog_t, double* q, double* gq0, double* gq1,
                            double* gq2) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
