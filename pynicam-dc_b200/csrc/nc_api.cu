@@ -1044,6 +1044,17 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   TRY(up_reg(h, T, "GMTR_t_W", 1, 6, &Gm.GMTR_t));
   TRY(up_reg(h, T, "GMTR_a_HN", 1, 9, &Gm.GMTR_a));
   TRY(up_reg(h, T, "GMTR_p_RAREA", 1, 1, &Gm.GMTR_p));
+  {
+    // shallow atmosphere: every gamma factor exactly 1 (checked element by element)
+    bool unit = true;
+    for (const char* nm : {"VMTR_RGAM", "VMTR_RGAMH", "VMTR_GAM2H", "VMTR_RGAM_pl", "VMTR_RGAMH_pl", "VMTR_GAM2H_pl"}) {
+      const nc_array* a = T.get(nm);
+      if (!a || a->dtype != NC_F64) { unit = false; break; }
+      const double* d = (const double*)a->data;
+      for (int64_t n = 0, e = numel(a); n < e && unit; ++n) unit = (d[n] == 1.0);
+    }
+    C.gam_unit = unit ? 1 : 0;
+  }
   if (h->trcadv) {   // the coordinates the prescribed winds are computed from
     TRY(up_reg(h, T, "GRD_LON", 1, 1, &h->trc_lon));
     TRY(up_reg(h, T, "GRD_LAT", 1, 1, &h->trc_lat));

@@ -43,6 +43,7 @@ struct Dims {
 struct Consts {
   double GRAV, Rdry, CVdry, CPdry, Rvap, OHM, EPS, HUGE_, rscale, alpha;
   double Kh, divdamp_coef, hdiff_fact_rho, CVW0, PRE00;
+  int gam_unit;   // RGAM, RGAMH and GAM2H are 1 everywhere (shallow atmosphere)
   double afact[NC_MAXK], bfact[NC_MAXK], cfact[NC_MAXK], dfact[NC_MAXK];
   double rdgz[NC_MAXK], rdgzh[NC_MAXK];
 };
@@ -91,6 +92,13 @@ struct Geom {
 __constant__ Dims cD;
 __constant__ Consts cC;
 __constant__ Geom cG;
+
+// The gamma factors of the vertical metrics: RGAM, RGAMH, GAM2H (regional or
+// pole) at index p.  With a shallow atmosphere every value is exactly 1 (the
+// host checks each element at set-up and sets gam_unit); the factor is then
+// not loaded, and x * 1.0 == x leaves every product bit-for-bit unchanged.
+__device__ __forceinline__ double gam_at(const double* a, int p) { return cC.gam_unit ? 1.0 : a[p]; }
+__device__ __forceinline__ double gam_at_ldg(const double* a, int p) { return cC.gam_unit ? 1.0 : __ldg(a + p); }
 
 // ---- indexing -------------------------------------------------------------
 __device__ __forceinline__ int ix(int i, int j, int k, int l) {

@@ -245,7 +245,7 @@ __device__ __forceinline__ double advconv_reg(int i, int j, int k, int l, const 
     div = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) -> double {
       int q = ix(ii, jj, kk, l);
       const double* rv = (d == 0) ? rvx : ((d == 1) ? rvy : rvz);
-      return (rv[q] * scl(q, kk)) * cG.RGAM[q];
+      return (rv[q] * scl(q, kk)) * gam_at(cG.RGAM, q);
     });
   }
   auto vmh = [&](int kk) -> double {
@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(256, 2) k_advmom_t(AdvMomArgs a) {
         s_rv[d][p] = ok ? rv[d][q] : 0.0;
         s_vv[d][p] = ok ? vv[d][q] : 0.0;
       }
-      s_rg[p] = ok ? cG.RGAM[q] : 0.0;
+      s_rg[p] = ok ? gam_at(cG.RGAM, q) : 0.0;
     }
     __syncthreads();
     if (own) {
@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(256, 2) k_advmom_t(AdvMomArgs a) {
                            cz[2 * n + qh] * (rv[1][qh] * sh) + cz[3 * n + qh] * (s_rv[1][c0] * sl) +
                            cz[4 * n + qh] * (rv[2][qh] * sh) + cz[5 * n + qh] * (s_rv[2][c0] * sl);
           const double sw = a.rw[qh] * (cC.afact[kk] * sh + cC.bfact[kk] * sl);
-          vmh_hi = h * cG.RGAMH[qh] + 1.0 * sw * cG.RGSQRTH[qh];
+          vmh_hi = h * gam_at(cG.RGAMH, qh) + 1.0 * sw * cG.RGSQRTH[qh];
         }
         dv[s] = -div - (vmh_hi - vmh_lo[s]) * cC.rdgz[k];
         vmh_lo[s] = vmh_hi;
@@ -370,9 +370,9 @@ __device__ double advconv_pl_at(int g, int lp, int k, const Col& c, const Met& m
     double row = 0.0;
     for (int v = 0; v < 6; ++v) {
       int q = ipl(v, k, lp);
-      double vx = (rvx[q] * scl[q]) * cG.RGAM_pl[q];
-      double vy = (rvy[q] * scl[q]) * cG.RGAM_pl[q];
-      double vz = (rvz[q] * scl[q]) * cG.RGAM_pl[q];
+      double vx = (rvx[q] * scl[q]) * gam_at(cG.RGAM_pl, q);
+      double vy = (rvy[q] * scl[q]) * gam_at(cG.RGAM_pl, q);
+      double vz = (rvz[q] * scl[q]) * gam_at(cG.RGAM_pl, q);
       double pv = cd[(v * cD.LP + lp) * 3 + 0] * vx + cd[(v * cD.LP + lp) * 3 + 1] * vy +
                   cd[(v * cD.LP + lp) * 3 + 2] * vz;
       row = (v == 0) ? pv : row + pv;

@@ -155,7 +155,7 @@ __device__ __forceinline__ double vmh_horiz(const Col& c, const Met& m, int k, F
   double h = mc(m.C2WGz, c, 0, 6, k) * flux(k, 0) + mc(m.C2WGz, c, 1, 6, k) * flux(k - 1, 0) +
              mc(m.C2WGz, c, 2, 6, k) * flux(k, 1) + mc(m.C2WGz, c, 3, 6, k) * flux(k - 1, 1) +
              mc(m.C2WGz, c, 4, 6, k) * flux(k, 2) + mc(m.C2WGz, c, 5, 6, k) * flux(k - 1, 2);
-  return h * m.RGAMH[c.at(k)];
+  return h * gam_at(m.RGAMH, c.at(k));
 }
 
 // total kinetic energy rhogkin at level k of one column (kernels/rhogkin.py:38-79)

@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(4)) k_dd3d_t(Four v, Th
       if (ii < G && jj < G) {
         const int q = ix(ii, jj, k, l);
         const double f0 = v.f[0][q], f1 = v.f[1][q], f2 = v.f[2][q];
-        const double rg = cG.RGAM[q];
+        const double rg = gam_at(cG.RGAM, q);
         a = f0 * rg;
         b = f1 * rg;
         c = f2 * rg;
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(4)) k_dd3d_t(Four v, Th
           const int qp = q + cD.planei;   // level k+1
           const double h = cz[qp] * v.f[0][qp] + cz[n + qp] * f0 + cz[2 * n + qp] * v.f[1][qp] +
                            cz[3 * n + qp] * f1 + cz[4 * n + qp] * v.f[2][qp] + cz[5 * n + qp] * f2;
-          r = h * cG.RGAMH[qp] + v.f[3][qp] * cG.RGSQRTH[qp];
+          r = h * gam_at(cG.RGAMH, qp) + v.f[3][qp] * cG.RGSQRTH[qp];
         }
       }
       s_vm[0][p] = a;
@@ -156,12 +156,12 @@ __global__ void k_dd3d_pl(Four v, Three out) {
     const double* cz = cG.C2WGz_pl;
     double h = cz[q * 6 + 0] * v.f[0][q] + cz[q * 6 + 1] * v.f[0][qm] + cz[q * 6 + 2] * v.f[1][q] +
                cz[q * 6 + 3] * v.f[1][qm] + cz[q * 6 + 4] * v.f[2][q] + cz[q * 6 + 5] * v.f[2][qm];
-    return h * cG.RGAMH_pl[q] + v.f[3][q] * cG.RGSQRTH_pl[q];
+    return h * gam_at(cG.RGAMH_pl, q) + v.f[3][q] * cG.RGSQRTH_pl[q];
   };
   double vm[6][3];
   for (int g = 0; g < 6; ++g) {
     int q = ipl(g, k, lp);
-    for (int d = 0; d < 3; ++d) vm[g][d] = v.f[d][q] * cG.RGAM_pl[q];
+    for (int d = 0; d < 3; ++d) vm[g][d] = v.f[d][q] * gam_at(cG.RGAM_pl, q);
   }
   double sclt[5];
   for (int v_ = 1; v_ <= 5; ++v_) {
@@ -257,10 +257,10 @@ __device__ void presgrad_reg(int i, int j, int k, int l, const Col& c, const Met
   if (k >= kmin && k <= kmax) {
     const int kk = (k == kmin) ? kmin + 1 : k;
     double gh[3] = {0.0, 0.0, 0.0};
-    if (interior(i, j)) grad7(i, j, kk, l, [&](int ii, int jj, int k2) { return P(ii, jj, k2) * cG.RGAM[ix(ii, jj, k2, l)]; }, gh);
+    if (interior(i, j)) grad7(i, j, kk, l, [&](int ii, int jj, int k2) { return P(ii, jj, k2) * gam_at(cG.RGAM, ix(ii, jj, k2, l)); }, gh);
     auto pvmh = [&](int k2, int d) {
       return (mc(m.C2WGz, c, 2 * d, 6, k2) * P(i, j, k2) + mc(m.C2WGz, c, 2 * d + 1, 6, k2) * P(i, j, k2 - 1)) *
-             m.RGAMH[c.at(k2)];
+             gam_at(m.RGAMH, c.at(k2));
     };
     for (int d = 0; d < 3; ++d) out[d] = gh[d] + (pvmh(kk + 1, d) - pvmh(kk, d)) * cC.rdgz[kk];
   }
@@ -278,7 +278,7 @@ __device__ void presgrad_pl(int g, int k, int lp, const Col& c, const Met& m, PF
       for (int d = 0; d < 3; ++d) {
         double row = 0.0;
         for (int v_ = 0; v_ < 6; ++v_) {
-          double pvm = P(v_, kk) * cG.RGAM_pl[ipl(v_, kk, lp)] * 1.0;
+          double pvm = P(v_, kk) * gam_at(cG.RGAM_pl, ipl(v_, kk, lp)) * 1.0;
           double tv = cG.coef_grad_pl[(v_ * cD.LP + lp) * 3 + d] * pvm;
           row = (v_ == 0) ? tv : row + tv;
         }
@@ -287,7 +287,7 @@ __device__ void presgrad_pl(int g, int k, int lp, const Col& c, const Met& m, PF
     }
     auto pvmh = [&](int k2, int d) {
       return (mc(m.C2WGz, c, 2 * d, 6, k2) * P(g, k2) + mc(m.C2WGz, c, 2 * d + 1, 6, k2) * P(g, k2 - 1)) *
-             m.RGAMH[c.at(k2)];
+             gam_at(m.RGAMH, c.at(k2));
     };
     for (int d = 0; d < 3; ++d) out[d] = gh[d] + (pvmh(kk + 1, d) - pvmh(kk, d)) * cC.rdgz[kk];
   }
@@ -299,7 +299,7 @@ template <class PF>
 __device__ __forceinline__ double presgradw(const Col& c, const Met& m, int k, PF Pk) {
   if (k < cD.kmin + 1 || k > cD.kmax) return 0.0;
   int p = c.at(k), pm = c.at(k - 1);
-  return m.GAM2H[p] * (Pk(k) * m.RGSGAM2[p] - Pk(k - 1) * m.RGSGAM2[pm]) * cC.rdgzh[k];
+  return gam_at(m.GAM2H, p) * (Pk(k) * m.RGSGAM2[p] - Pk(k - 1) * m.RGSGAM2[pm]) * cC.rdgzh[k];
 }
 
 // flux convergence at level k of a regional or pole column given the
@@ -322,7 +322,7 @@ __device__ __forceinline__ double div_pl(int lp, int k, F f) {
   double row = 0.0;
   for (int v_ = 0; v_ < 6; ++v_) {
     int q = ipl(v_, k, lp);
-    double rg = cG.RGAM_pl[q];
+    double rg = gam_at(cG.RGAM_pl, q);
     double vx = f(q, 0) * rg, vy = f(q, 1) * rg, vz = f(q, 2) * rg;
     const double* cd = cG.coef_div_pl + (v_ * cD.LP + lp) * 3;
     double pv = cd[0] * vx + cd[1] * vy + cd[2] * vz;
@@ -379,11 +379,11 @@ __device__ void vp0_column(const Vp0Args& a, int i, int j, int l, int g, int lp)
       if (interior(i, j)) {
         div1 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
           int q = ix(ii, jj, kk, l);
-          return P[1 + d][q] * cG.RGAM[q];
+          return P[1 + d][q] * gam_at(cG.RGAM, q);
         });
         div2 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
           int q = ix(ii, jj, kk, l);
-          return (P[1 + d][q] * a.eth[q]) * cG.RGAM[q];
+          return (P[1 + d][q] * a.eth[q]) * gam_at(cG.RGAM, q);
         });
       }
     } else if (g == 0) {
@@ -419,13 +419,13 @@ __device__ void vp0_column(const Vp0Args& a, int i, int j, int l, int g, int lp)
       const double ACVovRt2 = cC.alpha * cC.CVdry / cC.Rdry / (dt * dt);
       int pm = c.at(k - 1), pp = c.at(k + 1);
       double rg = cC.rdgz[k], rgm = cC.rdgz[k - 1];
-      double Ca = (m.RGSGAM2[p] * rg + m.RGSGAM2[pm] * rgm) * m.GAM2H[p];
+      double Ca = (m.RGSGAM2[p] * rg + m.RGSGAM2[pm] * rgm) * gam_at(m.GAM2H, p);
       double Cb = cC.dfact[k] - cC.cfact[k - 1];
-      double Cu1 = m.RGSGAM2[p] * rg * m.GAM2H[pp];
-      double rgh2 = m.RGAMH[p] * m.RGAMH[p];
-      double Cu2 = m.GAM2H[pp] * rgh2 * GCVovR;
-      double Cl1 = m.RGSGAM2[p] * rg * m.GAM2H[pm];
-      double Cl2 = m.GAM2H[pm] * rgh2 * GCVovR;
+      double Cu1 = m.RGSGAM2[p] * rg * gam_at(m.GAM2H, pp);
+      double rgh2 = gam_at(m.RGAMH, p) * gam_at(m.RGAMH, p);
+      double Cu2 = gam_at(m.GAM2H, pp) * rgh2 * GCVovR;
+      double Cl1 = m.RGSGAM2[p] * rg * gam_at(m.GAM2H, pm);
+      double Cl2 = gam_at(m.GAM2H, pm) * rgh2 * GCVovR;
       double rgh = cC.rdgzh[k];
       a.Mc[p] = ACVovRt2 / m.RGSQRTH[p] + rgh * (Ca * eth_h(k) - Cb * (gz(k) + GCVovR));
       a.Mu[p] = -rgh * (Cu1 * eth_h(k + 1) + cC.cfact[k] * (gz(k + 1) + Cu2));
@@ -632,7 +632,7 @@ __global__ void __launch_bounds__(NC_VP0C_BLOCK, 4) k_vp0_cr(Vp0Args a, Vp0H h) 
     if (kn < KA) {
       const int q = c.at(kn), qm = c.at(kn - 1);
       if (kn > kmin && kn <= kmax) {
-        const double rgh = cG.RGAMH[q], rsq = cG.RGSQRTH[q];
+        const double rgh = gam_at(cG.RGAMH, q), rsq = cG.RGSQRTH[q];
         const double z0 = cz[q], z1 = cz[n + q], z2 = cz[2 * n + q], z3 = cz[3 * n + q], z4 = cz[4 * n + q],
                      z5 = cz[5 * n + q];
         const double px = P[1][q], pxm = P[1][qm], py = P[2][q], pym = P[2][qm], pz = P[3][q], pzm = P[3][qm];
@@ -647,7 +647,7 @@ __global__ void __launch_bounds__(NC_VP0C_BLOCK, 4) k_vp0_cr(Vp0Args a, Vp0H h) 
         vint1 = 0.5 * (w * w) / den;
         // buoyancy and vertical pressure gradient
         dbuo1 = -GRAV * (c2w[q] * a.rhogd[q] + c2w[n + q] * a.rhogd[qm]);
-        dpgw1 = cG.GAM2H[q] * (a.pregd[q] * cG.RGSGAM2[q] - a.pregd[qm] * cG.RGSGAM2[qm]) * cC.rdgzh[kn];
+        dpgw1 = gam_at(cG.GAM2H, q) * (a.pregd[q] * cG.RGSGAM2[q] - a.pregd[qm] * cG.RGSGAM2[qm]) * cC.rdgzh[kn];
       }
       if (kn >= kmin && kn <= kmax + 1) {
         const int kk = kn;   // kn >= kmin here, so the clamp of rhog_h / eth_h is inactive
@@ -681,13 +681,13 @@ __global__ void __launch_bounds__(NC_VP0C_BLOCK, 4) k_vp0_cr(Vp0Args a, Vp0H h) 
     if (k >= kmin + 1 && k <= kmax) {
       const int pm = c.at(k - 1), pp = c.at(k + 1);
       const double rg = cC.rdgz[k], rgm = cC.rdgz[k - 1];
-      const double Ca = (cG.RGSGAM2[p] * rg + cG.RGSGAM2[pm] * rgm) * cG.GAM2H[p];
+      const double Ca = (cG.RGSGAM2[p] * rg + cG.RGSGAM2[pm] * rgm) * gam_at(cG.GAM2H, p);
       const double Cb = cC.dfact[k] - cC.cfact[k - 1];
-      const double Cu1 = cG.RGSGAM2[p] * rg * cG.GAM2H[pp];
-      const double rgh2 = cG.RGAMH[p] * cG.RGAMH[p];
-      const double Cu2 = cG.GAM2H[pp] * rgh2 * GCVovR;
-      const double Cl1 = cG.RGSGAM2[p] * rg * cG.GAM2H[pm];
-      const double Cl2 = cG.GAM2H[pm] * rgh2 * GCVovR;
+      const double Cu1 = cG.RGSGAM2[p] * rg * gam_at(cG.GAM2H, pp);
+      const double rgh2 = gam_at(cG.RGAMH, p) * gam_at(cG.RGAMH, p);
+      const double Cu2 = gam_at(cG.GAM2H, pp) * rgh2 * GCVovR;
+      const double Cl1 = cG.RGSGAM2[p] * rg * gam_at(cG.GAM2H, pm);
+      const double Cl2 = gam_at(cG.GAM2H, pm) * rgh2 * GCVovR;
       const double rgh = cC.rdgzh[k];
       a.Mc[p] = ACVovRt2 / cG.RGSQRTH[p] + rgh * (Ca * eh0 - Cb * (gz0 + GCVovR));
       a.Mu[p] = -rgh * (Cu1 * eh1 + cC.cfact[k] * (gz1 + Cu2));
@@ -935,15 +935,15 @@ __global__ void k_vimain_a(VimainArgs a, int pole) {
       if (in && k >= cD.kmin && k <= cD.kmax) {
         h1 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
           int q = ix(ii, jj, kk, l);
-          return a.dvh.f[d][q] * cG.RGAM[q];
+          return a.dvh.f[d][q] * gam_at(cG.RGAM, q);
         });
         h2 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
           int q = ix(ii, jj, kk, l);
-          return (a.dvh.f[d][q] * a.eth[q]) * cG.RGAM[q];
+          return (a.dvh.f[d][q] * a.eth[q]) * gam_at(cG.RGAM, q);
         });
         h3 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
           int q = ix(ii, jj, kk, l);
-          return ((a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q]) * cG.RGAM[q];
+          return ((a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q]) * gam_at(cG.RGAM, q);
         });
       }
       a.hdiv[0][p] = h1; a.hdiv[1][p] = h2; a.hdiv[2][p] = h3;
@@ -983,7 +983,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_vimain_a_l(Vimain
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
       if (ii < G && jj < G) {
         const int q = ix(ii, jj, k, l);
-        const double rg = __ldg(&cG.RGAM[q]), e = __ldg(&a.eth[q]), et = __ldg(&a.ethtot0[q]);
+        const double rg = gam_at_ldg(cG.RGAM, q), e = __ldg(&a.eth[q]), et = __ldg(&a.ethtot0[q]);
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
           const double dv = __ldg(&a.dvh.f[d][q]);
@@ -1063,8 +1063,8 @@ __device__ void vimain_column(const VimainArgs& a, const Col c) {
   for (int n = 0; n < N; ++n) {
     int k = kmin + 1 + n;
     int p = c.at(k), pm = c.at(k - 1);
-    double rg2 = m.RGAMH[p] * m.RGAMH[p];
-    double rgam2 = m.RGAM[p] * m.RGAM[p], rgam2m = m.RGAM[pm] * m.RGAM[pm];
+    double rg2 = gam_at(m.RGAMH, p) * gam_at(m.RGAMH, p);
+    double rgam2 = gam_at(m.RGAM, p) * gam_at(m.RGAM, p), rgam2m = gam_at(m.RGAM, pm) * gam_at(m.RGAM, pm);
     double Sw = a.gT[4][p] + 0.0 * cC.alpha;
     double S = ((PSk(4, k) * cC.alpha + dt * Sw) * rg2 -
                 ((preg0(k) + dt * gpre[k]) * m.RGSGAM2[p] - (preg0(k - 1) + dt * gpre[k - 1]) * m.RGSGAM2[pm]) * dt *

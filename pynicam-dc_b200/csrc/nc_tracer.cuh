@@ -27,7 +27,7 @@ __device__ void trc_vflux_column(const Col c, const Met m, const TrcFluxArgs& a)
       int pm = c.at(k - 1);
       double horiz = (mc(m.C2WGz, c, 0, 6, k) * a.rvx[p] + mc(m.C2WGz, c, 1, 6, k) * a.rvx[pm] +
                       mc(m.C2WGz, c, 2, 6, k) * a.rvy[p] + mc(m.C2WGz, c, 3, 6, k) * a.rvy[pm] +
-                      mc(m.C2WGz, c, 4, 6, k) * a.rvz[p] + mc(m.C2WGz, c, 5, 6, k) * a.rvz[pm]) * m.RGAMH[p];
+                      mc(m.C2WGz, c, 4, 6, k) * a.rvz[p] + mc(m.C2WGz, c, 5, 6, k) * a.rvz[pm]) * gam_at(m.RGAMH, p);
       double vert = a.rw[p] * m.RGSQRTH[p];
       f = (horiz + vert) * 0.5 * a.dt;
     }
@@ -280,7 +280,7 @@ __global__ void k_trc_hflux_pl(TrcHfluxPlArgs a) {
   auto F = [&](int n, int q) -> double {
     if (n == 0) return a.rho[q];
     const double* r = (n == 1) ? a.rvx : ((n == 2) ? a.rvy : a.rvz);
-    return r[q] * cG.RGAM_pl[q];
+    return r[q] * gam_at(cG.RGAM_pl, q);
   };
   for (int v = 1; v <= 5; ++v) {
     int vp1 = (v + 1 == 6) ? 1 : v + 1;
