@@ -81,3 +81,24 @@ def test_mass_sums_match_host(core, golden):
     qp = sp[0, ks, :, 6] / sp[0, ks, :, 0]
     wq = np.sum(rho * q * vol) + np.sum(rho_p * qp * vol_p)
     assert abs(m[1] - wq) <= 1e-12 * abs(wq)
+
+
+def test_non_unit_gamma_factors_vs_oracle(pkg, golden):
+    """a deep-atmosphere-like setup (gamma factors not all 1) takes the loaded
+    path of the gamma factors; device and oracle agree bit for bit"""
+    from oracle import nicam_step as O
+    geo, st = golden
+    g = dict(geo)
+    rng = np.random.default_rng(5)
+    for k in ("VMTR_RGAM", "VMTR_RGAMH", "VMTR_GAM2H"):
+        g[k] = geo[k] * (1.0 + 1e-6 * rng.random(geo[k].shape))
+    s, sp = st["state0"], st["state0_pl"]
+    want, want_pl = O.dynamics_step(O.Geo(g), s, sp)
+    c = pkg.NicamCuda(g, graph=False)
+    try:
+        c.upload(s, sp)
+        c.step(1)
+        out, out_pl = c.download()
+    finally:
+        c.close()
+    assert np.array_equal(out, want) and np.array_equal(out_pl, want_pl)
