@@ -680,7 +680,8 @@ static int run_step(nc_handle* h) {
         if (!pole) {
           k_vimain_a_l<<<lvgrid, DD_DX * DD_DY, 0, s>>>(va);
           TRY(check_launch(h, "vimain_a"));
-          k_vi_solve<<<greg, kBlock, 0, s>>>(va);
+          if (h->C.gam_unit) k_vi_solve<true><<<greg, kBlock, 0, s>>>(va);
+          else k_vi_solve<false><<<greg, kBlock, 0, s>>>(va);
           TRY(check_launch(h, "vi_solve"));
           k_vi_energy_p<<<npt_blocks, kBlock, 0, s>>>(va);
           TRY(check_launch(h, "vi_energy"));

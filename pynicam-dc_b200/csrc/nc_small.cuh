@@ -1144,6 +1144,8 @@ __device__ void vimain_column(const VimainArgs& a, const Col c) {
 // the way down; writes rhog_s1, rhogw_s1 and their running means.
 // nine 128-thread blocks per SM (56 registers): the 655,360 interior columns
 // of gl08 fill 3.84 waves of the 148 SMs instead of 4.32 at eight
+// GU: the gamma factors are all 1 and are not loaded; the other instance loads them
+template <bool GU>
 __global__ void __launch_bounds__(128, 9) k_vi_solve(VimainArgs a) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
@@ -1169,7 +1171,7 @@ __global__ void __launch_bounds__(128, 9) k_vi_solve(VimainArgs a) {
     }
     const double h = cz[q] * f0 + cz[n + q] * f0m + cz[2 * n + q] * f1 + cz[3 * n + q] * f1m + cz[4 * n + q] * f2 +
                      cz[5 * n + q] * f2m;
-    return h * m.RGAMH[q];
+    return h * (GU ? 1.0 : m.RGAMH[q]);
   };
   double hD[NC_MAXK];
   const int pT = c.at(kT), pK = c.at(kmax);
@@ -1199,8 +1201,9 @@ __global__ void __launch_bounds__(128, 9) k_vi_solve(VimainArgs a) {
     if (k >= kmin + 1) {
       const int nn = k - kmin - 1;
       const int pm = c.at(k - 1);
-      const double rg2 = m.RGAMH[p] * m.RGAMH[p];
-      const double rgam2 = m.RGAM[p] * m.RGAM[p], rgam2m = m.RGAM[pm] * m.RGAM[pm];
+      const double rgh = GU ? 1.0 : m.RGAMH[p], rgm = GU ? 1.0 : m.RGAM[p], rgmm = GU ? 1.0 : m.RGAM[pm];
+      const double rg2 = rgh * rgh;
+      const double rgam2 = rgm * rgm, rgam2m = rgmm * rgmm;
       const double Sw = a.gT[4][p] + 0.0 * cC.alpha;
       double S = ((a.PS[4][p] * cC.alpha + dt * Sw) * rg2 -
                   ((preg0(k) + dt * gp) * m.RGSGAM2[p] - (preg0(k - 1) + dt * gp_prev) * m.RGSGAM2[pm]) * dt *
