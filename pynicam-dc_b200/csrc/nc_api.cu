@@ -18,6 +18,19 @@
 using namespace nc;
 
 static thread_local std::string g_err;
+// RN(1/b) and the tail RN(1/b - RN(1/b)) for div_by: the residual 1 - b*RN(1/b)
+// is exactly representable, so one fused multiply-add gives it exactly and a
+// division of it by b rounds the tail correctly.
+static void recip_pair(double b, double& h, double& l) {
+  h = 1.0 / b;
+  l = std::fma(-h, b, 1.0) / b;
+}
+
+__global__ void k_divide_known(const double* x, double* q, int n, double b, double bh, double bl) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t < n) q[t] = nc::div_by(x[t], b, bh, bl);
+}
+
 static int fail(int code, const std::string& msg) {
   g_err = msg;
   return code;
@@ -992,6 +1005,9 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   TRY(scalar(T, "EPS", C.EPS)); TRY(scalar(T, "HUGE", C.HUGE_)); TRY(scalar(T, "rscale", C.rscale));
   TRY(scalar(T, "alpha", C.alpha)); TRY(scalar(T, "Kh_coef", C.Kh)); TRY(scalar(T, "divdamp_coef", C.divdamp_coef));
   TRY(scalar(T, "hdiff_fact_rho", C.hdiff_fact_rho));
+  if (!(C.rscale != 0.0 && std::isfinite(C.rscale))) return fail(NC_ERR_ARG, "rscale must be finite and nonzero");
+  recip_pair(C.rscale, C.rsc_h, C.rsc_l);
+  recip_pair(3.0, C.third_h, C.third_l);
   TRY(scalar(T, "dtl", h->dtl)); TRY(scalar(T, "dts", h->dts));
   {
     const nc_array* cvw = T.get("CVW");
@@ -1604,6 +1620,26 @@ int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* g
   CU(cudaGetLastError());
   k_mass_noalloc_fold<<<1, 1, 0, st>>>(part, (int)blocks, out);
   CU(cudaGetLastError());
+  return 0;
+}
+
+int nc_divide_known(const double* x, double* q, int64_t n, double b) {
+  if (!x || !q || n < 0 || n > (int64_t)1 << 28) return fail(NC_ERR_ARG, "nc_divide_known: bad argument");
+  if (!(b != 0.0 && std::isfinite(b))) return fail(NC_ERR_ARG, "nc_divide_known: divisor must be finite and nonzero");
+  if (n == 0) return 0;
+  double bh, bl;
+  recip_pair(b, bh, bl);
+  double* d = nullptr;
+  const size_t bytes = (size_t)n * sizeof(double);
+  CU(cudaMalloc(&d, 2 * bytes));
+  cudaError_t e = cudaMemcpy(d, x, bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_divide_known<<<(unsigned)((n + 255) / 256), 256>>>(d, d + n, (int)n, b, bh, bl);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(q, d + n, bytes, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(NC_ERR_CUDA, std::string("nc_divide_known: ") + cudaGetErrorString(e));
   return 0;
 }
 

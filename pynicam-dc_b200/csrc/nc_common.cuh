@@ -44,6 +44,9 @@ struct Consts {
   double GRAV, Rdry, CVdry, CPdry, Rvap, OHM, EPS, HUGE_, rscale, alpha;
   double Kh, divdamp_coef, hdiff_fact_rho, CVW0, PRE00;
   int gam_unit;   // RGAM, RGAMH and GAM2H are 1 everywhere (shallow atmosphere)
+  // rounded reciprocals and their tails, RN(1/b) and RN(1/b - RN(1/b)), of the
+  // divisors rscale and 3 (see div_by)
+  double rsc_h, rsc_l, third_h, third_l;
   double afact[NC_MAXK], bfact[NC_MAXK], cfact[NC_MAXK], dfact[NC_MAXK];
   double rdgz[NC_MAXK], rdgzh[NC_MAXK];
 };
@@ -99,6 +102,27 @@ __constant__ Geom cG;
 // not loaded, and x * 1.0 == x leaves every product bit-for-bit unchanged.
 __device__ __forceinline__ double gam_at(const double* a, int p) { return cC.gam_unit ? 1.0 : a[p]; }
 __device__ __forceinline__ double gam_at_ldg(const double* a, int p) { return cC.gam_unit ? 1.0 : __ldg(a + p); }
+
+// x / b for a divisor fixed before the launch, with the same bits as the IEEE
+// division x / b for finite x whose quotient is in the normal range.  From
+// bh = RN(1/b) and bl = RN(1/b - bh), q0 = RN(x*bh + x*bl) is within one ulp
+// of x/b (the double-word reciprocal of Brisebarre, Muller and Raina,
+// "Accelerating correctly rounded floating-point division when the divisor is
+// known in advance", IEEE Trans. Computers 53(8), 2004); the remainder
+// x - b*q0 is then exact, and one correction RN(q0 + r*bh) gives the correctly
+// rounded quotient (Markstein, "Computation of elementary functions on the IBM
+// RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990).  A zero x takes
+// its quotient's sign from x*bh.  Three FMAs and a multiply instead of a
+// general division.
+__device__ __forceinline__ double div_by(double x, double b, double bh, double bl) {
+  const double q0 = __fma_rn(x, bh, __dmul_rn(x, bl));
+  const double r = __fma_rn(-q0, b, x);
+  const double q = __fma_rn(r, bh, q0);
+  return (x == 0.0) ? __dmul_rn(x, bh) : q;
+}
+// x / rscale and x / 3.0
+__device__ __forceinline__ double div_r(double x) { return div_by(x, cC.rscale, cC.rsc_h, cC.rsc_l); }
+__device__ __forceinline__ double div3(double x) { return div_by(x, 3.0, cC.third_h, cC.third_l); }
 
 // ---- indexing -------------------------------------------------------------
 __device__ __forceinline__ int ix(int i, int j, int k, int l) {

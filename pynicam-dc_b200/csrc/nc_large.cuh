@@ -96,9 +96,9 @@ __device__ void diag_column(const Col c, const Met m, const DiagArgs& a, double 
     a.rhogd[p] = (rho - m.rho_bs[p]) * m.GSGAM2[p];
     if (k >= kmin && k <= kmax) {
       double wc = cC.cfact[k] * a.w[c.at(k + 1)] + cC.dfact[k] * a.w[p];
-      a.vvx[p] = a.vx[p] + wc * gx / cC.rscale;
-      a.vvy[p] = a.vy[p] + wc * gy / cC.rscale;
-      a.vvz[p] = a.vz[p] + wc * gz / cC.rscale;
+      a.vvx[p] = a.vx[p] + div_r(wc * gx);
+      a.vvy[p] = a.vy[p] + div_r(wc * gy);
+      a.vvz[p] = a.vz[p] + div_r(wc * gz);
     } else {
       a.vvx[p] = 0.0; a.vvy[p] = 0.0; a.vvz[p] = 0.0;
     }
@@ -121,9 +121,9 @@ __device__ void diag_column_fused(const Col c, const Met m, const DiagArgs& a, d
     a.rhogd[p] = (rho - m.rho_bs[p]) * m.GSGAM2[p];
     if (k >= kmin && k <= kmax) {
       double wc = cC.cfact[k] * wk1 + cC.dfact[k] * wk;
-      a.vvx[p] = vxk + wc * gx / cC.rscale;
-      a.vvy[p] = vyk + wc * gy / cC.rscale;
-      a.vvz[p] = vzk + wc * gz / cC.rscale;
+      a.vvx[p] = vxk + div_r(wc * gx);
+      a.vvy[p] = vyk + div_r(wc * gy);
+      a.vvz[p] = vzk + div_r(wc * gz);
     } else {
       a.vvx[p] = 0.0; a.vvy[p] = 0.0; a.vvz[p] = 0.0;
     }
@@ -282,7 +282,6 @@ __global__ void __launch_bounds__(256, 2) k_advmom_t(AdvMomArgs a) {
   const int tid = threadIdx.x, tx = tid % TXD, ty = tid / TXD;
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= gmax) && (j <= gmax);
-  const double r = cC.rscale;
   const double* rv[3] = {a.rvx, a.rvy, a.rvz};
   const double* vv[3] = {a.vvx, a.vvy, a.vvz};
   const double* cz = cG.C2WGz;
@@ -290,9 +289,9 @@ __global__ void __launch_bounds__(256, 2) k_advmom_t(AdvMomArgs a) {
   double gx = 0.0, gy = 0.0, gz = 0.0;
   int q0 = 0;
   if (own) {
-    gx = P2(cG.GRD_x, 0, i, j, l) / r;
-    gy = P2(cG.GRD_x, 1, i, j, l) / r;
-    gz = P2(cG.GRD_x, 2, i, j, l) / r;
+    gx = div_r(P2(cG.GRD_x, 0, i, j, l));
+    gy = div_r(P2(cG.GRD_x, 1, i, j, l));
+    gz = div_r(P2(cG.GRD_x, 2, i, j, l));
     q0 = ix(i, j, 0, l);
   }
   double vmh_lo[3] = {0.0, 0.0, 0.0};
@@ -399,10 +398,9 @@ __global__ void k_advmom_pl(AdvMomArgs a) {
   int g = t / cD.LP, lp = t % cD.LP;
   const Col c = col_pl(g, lp);
   const Met m = met_of(true);
-  const double r = cC.rscale;
   const double* X = cG.GRD_x_pl;
-  const double gx = X[(g * cD.LP + lp) * 3 + 0] / r, gy = X[(g * cD.LP + lp) * 3 + 1] / r,
-               gz = X[(g * cD.LP + lp) * 3 + 2] / r;
+  const double gx = div_r(X[(g * cD.LP + lp) * 3 + 0]), gy = div_r(X[(g * cD.LP + lp) * 3 + 1]),
+               gz = div_r(X[(g * cD.LP + lp) * 3 + 2]);
   double gwc_prev = 0.0;
   for (int k = 0; k < cD.KA; ++k) {
     int p = c.at(k);
@@ -501,8 +499,8 @@ __device__ double diffusion_at(int i, int j, int k, int l, S scl, KH kh) {
       double c1j = P2(cG.coef_intp, (d * 3 + 0) * 2 + 1, ii, jj, l);
       double c2j = P2(cG.coef_intp, (d * 3 + 1) * 2 + 1, ii, jj, l);
       double c3j = P2(cG.coef_intp, (d * 3 + 2) * 2 + 1, ii, jj, l);
-      tti[d] = ((2.0 * c1i - c2i - c3i) * s0 + (-c1i + 2.0 * c2i - c3i) * sip + (-c1i - c2i + 2.0 * c3i) * sd) / 3.0;
-      ttj[d] = ((2.0 * c1j - c2j - c3j) * s0 + (-c1j + 2.0 * c2j - c3j) * sd + (-c1j - c2j + 2.0 * c3j) * sjp) / 3.0;
+      tti[d] = div3((2.0 * c1i - c2i - c3i) * s0 + (-c1i + 2.0 * c2i - c3i) * sip + (-c1i - c2i + 2.0 * c3i) * sd);
+      ttj[d] = div3((2.0 * c1j - c2j - c3j) * s0 + (-c1j + 2.0 * c2j - c3j) * sd + (-c1j - c2j + 2.0 * c3j) * sjp);
     }
     if (ii == 0 && jj == 0) {  // singular-point fix (kernels/oprtdiffusion.py:91-96)
       double m0 = (double)cG.pntmask[l * 2 + 0], m1 = (double)cG.pntmask[l * 2 + 1];
@@ -512,7 +510,7 @@ __device__ double diffusion_at(int i, int j, int k, int l, S scl, KH kh) {
         double c1j = P2(cG.coef_intp, (d * 3 + 0) * 2 + 1, 1, 0, l);
         double c2j = P2(cG.coef_intp, (d * 3 + 1) * 2 + 1, 1, 0, l);
         double c3j = P2(cG.coef_intp, (d * 3 + 2) * 2 + 1, 1, 0, l);
-        double tj10 = ((2.0 * c1j - c2j - c3j) * s0b + (-c1j + 2.0 * c2j - c3j) * sdb + (-c1j - c2j + 2.0 * c3j) * sjpb) / 3.0;
+        double tj10 = div3((2.0 * c1j - c2j - c3j) * s0b + (-c1j + 2.0 * c2j - c3j) * sdb + (-c1j - c2j + 2.0 * c3j) * sjpb);
         (void)sipb;
         tti[d] = tti[d] * m0 + tj10 * m1;
       }
@@ -596,8 +594,8 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, 4) k_hdiff2_l(Six vt, const dou
             const double c1j = P2(cG.coef_intp, (d * 3 + 0) * 2 + 1, ii, jj, l);
             const double c2j = P2(cG.coef_intp, (d * 3 + 1) * 2 + 1, ii, jj, l);
             const double c3j = P2(cG.coef_intp, (d * 3 + 2) * 2 + 1, ii, jj, l);
-            ti = ((2.0 * c1i - c2i - c3i) * s0 + (-c1i + 2.0 * c2i - c3i) * sip + (-c1i - c2i + 2.0 * c3i) * sd) / 3.0;
-            tj = ((2.0 * c1j - c2j - c3j) * s0 + (-c1j + 2.0 * c2j - c3j) * sd + (-c1j - c2j + 2.0 * c3j) * sjp) / 3.0;
+            ti = div3((2.0 * c1i - c2i - c3i) * s0 + (-c1i + 2.0 * c2i - c3i) * sip + (-c1i - c2i + 2.0 * c3i) * sd);
+            tj = div3((2.0 * c1j - c2j - c3j) * s0 + (-c1j + 2.0 * c2j - c3j) * sd + (-c1j - c2j + 2.0 * c3j) * sjp);
           }
           s_t[f][d][p] = ti;
           s_t[f][3 + d][p] = tj;
@@ -672,7 +670,7 @@ __global__ void k_hdiff2_pl(Six vt, const double* rhog, SixOut out) {
         for (int d = 0; d < 3; ++d) {
           const double* cI = cG.coef_intp_pl + ((v * cD.LP + lp) * 3 + d) * 3;
           double c0 = cI[0], c1 = cI[1], c2 = cI[2];
-          vt_[v - 1][d] = ((2.0 * c0 - c1 - c2) * sn + (-c0 + 2.0 * c1 - c2) * sij + (-c0 - c1 + 2.0 * c2) * sp1) / 3.0;
+          vt_[v - 1][d] = div3((2.0 * c0 - c1 - c2) * sn + (-c0 + 2.0 * c1 - c2) * sij + (-c0 - c1 + 2.0 * c2) * sp1);
         }
       }
       double khn = rhog[ipl(0, k, lp)] * fac * Kh;

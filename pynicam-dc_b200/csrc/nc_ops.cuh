@@ -126,23 +126,21 @@ __device__ __forceinline__ double lap7(int i, int j, int k, int l, F scl) {
 // tangent-plane projection of one vector at an interior point
 // (kernels/horizontalizevec.py:51-54)
 __device__ __forceinline__ void horiz_reg(int i, int j, int l, double& vx, double& vy, double& vz) {
-  const double r = cC.rscale;
   double gx = P2(cG.GRD_x, 0, i, j, l), gy = P2(cG.GRD_x, 1, i, j, l), gz = P2(cG.GRD_x, 2, i, j, l);
-  double prd = (vx * gx + vy * gy + vz * gz) / r;
-  double nx = vx - prd * gx / r;
-  double ny = vy - prd * gy / r;
-  double nz = vz - prd * gz / r;
+  double prd = div_r(vx * gx + vy * gy + vz * gz);
+  double nx = vx - div_r(prd * gx);
+  double ny = vy - div_r(prd * gy);
+  double nz = vz - div_r(prd * gz);
   vx = nx; vy = ny; vz = nz;
 }
 // pole projection (kernels/horizontalizevec.py:67-71)
 __device__ __forceinline__ void horiz_pl(int g, int lp, double& vx, double& vy, double& vz) {
-  const double r = cC.rscale;
   const double* X = cG.GRD_x_pl;
   double gx = X[(g * cD.LP + lp) * 3 + 0], gy = X[(g * cD.LP + lp) * 3 + 1], gz = X[(g * cD.LP + lp) * 3 + 2];
-  double prd = vx * gx / r + vy * gy / r + vz * gz / r;
-  double nx = vx - prd * gx / r;
-  double ny = vy - prd * gy / r;
-  double nz = vz - prd * gz / r;
+  double prd = div_r(vx * gx) + div_r(vy * gy) + div_r(vz * gz);
+  double nx = vx - div_r(prd * gx);
+  double ny = vy - div_r(prd * gy);
+  double nz = vz - div_r(prd * gz);
   vx = nx; vy = ny; vz = nz;
 }
 

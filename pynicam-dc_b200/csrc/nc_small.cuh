@@ -91,8 +91,8 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(4)) k_dd3d_t(Four v, Th
       if (ii <= G - 2 && jj <= G - 2) {
         const int a = py * PX + px, b = a + 1, c = a + PX + 1, d = a + PX;
         auto C = [&](int dir, int pt, int t) { return P2c(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
-        const double wTI = ((rU[a] + rU[b] + rU[c]) - (rD[a] + rD[b] + rD[c])) / 3.0 * rdz;
-        const double wTJ = ((rU[a] + rU[c] + rU[d]) - (rD[a] + rD[c] + rD[d])) / 3.0 * rdz;
+        const double wTI = div3((rU[a] + rU[b] + rU[c]) - (rD[a] + rD[b] + rD[c])) * rdz;
+        const double wTJ = div3((rU[a] + rU[c] + rU[d]) - (rD[a] + rD[c] + rD[d])) * rdz;
         sTI = C(0, 0, 0) * s_vm[0][a] + C(0, 1, 0) * s_vm[0][b] + C(0, 2, 0) * s_vm[0][c] +
               C(1, 0, 0) * s_vm[1][a] + C(1, 1, 0) * s_vm[1][b] + C(1, 2, 0) * s_vm[1][c] +
               C(2, 0, 0) * s_vm[2][a] + C(2, 1, 0) * s_vm[2][b] + C(2, 2, 0) * s_vm[2][c] + wTI;
@@ -166,7 +166,7 @@ __global__ void k_dd3d_pl(Four v, Three out) {
   double sclt[5];
   for (int v_ = 1; v_ <= 5; ++v_) {
     int vp1 = (v_ == 5) ? 1 : v_ + 1;
-    double sw = ((rw(0, k + 1) + rw(v_, k + 1) + rw(vp1, k + 1)) - (rw(0, k) + rw(v_, k) + rw(vp1, k))) / 3.0 * cC.rdgz[k];
+    double sw = div3((rw(0, k + 1) + rw(v_, k + 1) + rw(vp1, k + 1)) - (rw(0, k) + rw(v_, k) + rw(vp1, k))) * cC.rdgz[k];
     const double* cI = cG.coef_intp_pl + (v_ * cD.LP + lp) * 9;
     sclt[v_ - 1] = cI[0] * vm[0][0] + cI[1] * vm[v_][0] + cI[2] * vm[vp1][0] + cI[3] * vm[0][1] + cI[4] * vm[v_][1] +
                    cI[5] * vm[vp1][1] + cI[6] * vm[0][2] + cI[7] * vm[v_][2] + cI[8] * vm[vp1][2] + sw;
@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) 
   const int tid = threadIdx.x, tx = tid % VP_DX, ty = tid / VP_DX;
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= gmax) && (j <= gmax);
-  const double ddc = cC.divdamp_coef, r = cC.rscale;
+  const double ddc = cC.divdamp_coef;
   const int n = cD.npti;
   const double* cz = cG.C2WGz;
   const double* const* P = a.P.v;
@@ -555,10 +555,10 @@ __global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) 
                        P2(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) +
                        P2(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI));
       {
-        const double prd = (dd[0] * gxyz[0] + dd[1] * gxyz[1] + dd[2] * gxyz[2]) / r;
-        dd[0] = dd[0] - prd * gxyz[0] / r;
-        dd[1] = dd[1] - prd * gxyz[1] / r;
-        dd[2] = dd[2] - prd * gxyz[2] / r;
+        const double prd = div_r(dd[0] * gxyz[0] + dd[1] * gxyz[1] + dd[2] * gxyz[2]);
+        dd[0] = dd[0] - div_r(prd * gxyz[0]);
+        dd[1] = dd[1] - div_r(prd * gxyz[1]);
+        dd[2] = dd[2] - div_r(prd * gxyz[2]);
       }
       // pressure gradient of pregd at level kk
       const int qkk = q0 + (int)kk * cD.planei, qk1 = qkk + cD.planei, qkm = qkk - cD.planei;
@@ -575,10 +575,10 @@ __global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) 
         pg[d] = g + (up - dn) * cC.rdgz[kk];
       }
       {
-        const double prd = (pg[0] * gxyz[0] + pg[1] * gxyz[1] + pg[2] * gxyz[2]) / r;
-        pg[0] = pg[0] - prd * gxyz[0] / r;
-        pg[1] = pg[1] - prd * gxyz[1] / r;
-        pg[2] = pg[2] - prd * gxyz[2] / r;
+        const double prd = div_r(pg[0] * gxyz[0] + pg[1] * gxyz[1] + pg[2] * gxyz[2]);
+        pg[0] = pg[0] - div_r(prd * gxyz[0]);
+        pg[1] = pg[1] - div_r(prd * gxyz[1]);
+        pg[2] = pg[2] - div_r(prd * gxyz[2]);
       }
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
@@ -821,7 +821,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_path1_l(Path1Args
   __syncthreads();
   const int i = i0 + tx, j = j0 + ty;
   if (i > gmax || j > gmax) return;
-  const double r = cC.rscale, ddc = cC.divdamp_coef, dt = a.dt, rweight = a.rweight;
+  const double ddc = cC.divdamp_coef, dt = a.dt, rweight = a.rweight;
   const int n = cD.npti;
   const double* cz = cG.C2WGz;
   const double gx = P2c(cG.GRD_x, 0, i, j, l), gy = P2c(cG.GRD_x, 1, i, j, l), gz = P2c(cG.GRD_x, 2, i, j, l);
@@ -840,10 +840,10 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_path1_l(Path1Args
                    P2c(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) + P2c(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
                    P2c(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) + P2c(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI));
   {
-    const double prd = (dd[0] * gx + dd[1] * gy + dd[2] * gz) / r;
-    dd[0] = dd[0] - prd * gx / r;
-    dd[1] = dd[1] - prd * gy / r;
-    dd[2] = dd[2] - prd * gz / r;
+    const double prd = div_r(dd[0] * gx + dd[1] * gy + dd[2] * gz);
+    dd[0] = dd[0] - div_r(prd * gx);
+    dd[1] = dd[1] - div_r(prd * gy);
+    dd[2] = dd[2] - div_r(prd * gz);
   }
   const int c0 = (ty + 1) * PX + (tx + 1);
   const double s7[7] = {s_p[c0], s_p[c0 + 1], s_p[c0 + PX + 1], s_p[c0 + PX], s_p[c0 - 1], s_p[c0 - PX - 1], s_p[c0 - PX]};
@@ -861,10 +861,10 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_path1_l(Path1Args
     pg[d] = g + (up - dn) * cC.rdgz[kk];
   }
   {
-    const double prd = (pg[0] * gx + pg[1] * gy + pg[2] * gz) / r;
-    pg[0] = pg[0] - prd * gx / r;
-    pg[1] = pg[1] - prd * gy / r;
-    pg[2] = pg[2] - prd * gz / r;
+    const double prd = div_r(pg[0] * gx + pg[1] * gy + pg[2] * gz);
+    pg[0] = pg[0] - div_r(prd * gx);
+    pg[1] = pg[1] - div_r(prd * gy);
+    pg[2] = pg[2] - div_r(prd * gz);
   }
   const int q = q0 + (int)k * cD.planei;
   double v[3];

@@ -32,8 +32,8 @@ _lib = None
 # every entry point declared in include/nicam_cuda.h
 EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_state_async", "nc_join_copies",
            "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",
-           "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_forcing_step", "nc_last_error",
-           "nc_destroy")
+           "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_forcing_step", "nc_divide_known",
+           "nc_last_error", "nc_destroy")
 
 
 def load_library(path: str = LIB_PATH):
@@ -71,6 +71,8 @@ def load_library(path: str = LIB_PATH):
     lib.nc_grid_spring.restype = ctypes.c_int
     lib.nc_forcing_step.argtypes = [vp]
     lib.nc_forcing_step.restype = ctypes.c_int
+    lib.nc_divide_known.argtypes = [dp, dp, i64, ctypes.c_double]
+    lib.nc_divide_known.restype = ctypes.c_int
     lib.nc_destroy.argtypes = [vp]
     lib.nc_destroy.restype = None
     for f in ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_state_async", "nc_join_copies",
@@ -99,6 +101,18 @@ def grid_spring(x, x_pl, have_sgp, plan, lam, dbar, dt, crit, max_iter):
     if rc != 0:
         raise NicamError(f"nc_grid_spring status {rc}: {lib.nc_last_error().decode(errors='replace')}")
     return x, x_pl, int(it.value)
+
+
+def divide_known(x, b: float) -> np.ndarray:
+    """x / b on the device with the kernels' known-divisor division
+    (nc_divide_known); the result should equal numpy's x / b bit for bit."""
+    lib = load_library()
+    x = np.ascontiguousarray(x, np.float64)
+    q = np.empty_like(x)
+    rc = lib.nc_divide_known(x.ctypes.data, q.ctypes.data, x.size, float(b))
+    if rc != 0:
+        raise NicamError(f"nc_divide_known status {rc}: {lib.nc_last_error().decode(errors='replace')}")
+    return q
 
 
 def _check(rc: int):
