@@ -183,15 +183,19 @@ int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* g
  * NC_ERR_STATE.  Asynchronous on the handle's stream, like nc_step. */
 int nc_forcing_step(nc_handle* h);
 
-/* Self-check of the known-divisor division the kernels use for x / rscale and
- * x / 3 (three fused multiply-adds and a multiply from RN(1/b) and its tail,
- * in place of a general division; the reference divides with numpy's IEEE
- * division, e.g. kernels/horizontalizevec.py:51-54, kernels/oprtdiffusion.py).
- * Copies n host doubles x to the device, writes q[i] = x[i] / b computed that
- * way, and copies q back (synchronous).  For finite x with a normal-range
- * quotient the bits equal the IEEE quotient; the tests compare them.
- * 0 <= n <= 2^28; b finite and nonzero, else NC_ERR_ARG. */
-int nc_divide_known(const double* x, double* q, int64_t n, double b);
+/* Self-check of the divisions the kernels use in place of a general division
+ * (the reference divides with numpy's IEEE division, e.g.
+ * kernels/horizontalizevec.py:51-54, kernels/oprtdiffusion.py,
+ * kernels/virhowsolver.py): a quotient formed from RN(1/b) and a tail with
+ * three fused multiply-adds and a multiply.  With y NULL every x[i] is divided
+ * by the constant b (reciprocal pair set on the host, as for rscale, 3 and
+ * CVdry); otherwise x[i] is divided by y[i] with the pair formed on the device
+ * from the correctly rounded reciprocal (as for the density that several
+ * diagnostics divide by).  Copies the n host doubles in, writes q, copies it
+ * back (synchronous).  For finite operands with a normal-range quotient the
+ * bits equal the IEEE quotient; the tests compare them.  0 <= n <= 2^28; with
+ * y NULL, b finite and nonzero; else NC_ERR_ARG. */
+int nc_divide_known(const double* x, const double* y, double* q, int64_t n, double b);
 
 const char* nc_last_error(void);
 

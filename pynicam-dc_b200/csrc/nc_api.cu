@@ -26,9 +26,10 @@ static void recip_pair(double b, double& h, double& l) {
   l = std::fma(-h, b, 1.0) / b;
 }
 
-__global__ void k_divide_known(const double* x, double* q, int n, double b, double bh, double bl) {
+__global__ void k_divide_known(const double* x, const double* y, double* q, int n, double b, double bh, double bl) {
   const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (t < n) q[t] = nc::div_by(x[t], b, bh, bl);
+  if (t >= n) return;
+  q[t] = y ? nc::div_by(x[t], nc::recip_of(y[t])) : nc::div_by(x[t], b, bh, bl);
 }
 
 static int fail(int code, const std::string& msg) {
@@ -1008,6 +1009,8 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   if (!(C.rscale != 0.0 && std::isfinite(C.rscale))) return fail(NC_ERR_ARG, "rscale must be finite and nonzero");
   recip_pair(C.rscale, C.rsc_h, C.rsc_l);
   recip_pair(3.0, C.third_h, C.third_l);
+  if (!(C.CVdry != 0.0 && std::isfinite(C.CVdry))) return fail(NC_ERR_ARG, "CVdry must be finite and nonzero");
+  recip_pair(C.CVdry, C.cvd_h, C.cvd_l);
   TRY(scalar(T, "dtl", h->dtl)); TRY(scalar(T, "dts", h->dts));
   {
     const nc_array* cvw = T.get("CVW");
@@ -1623,18 +1626,20 @@ int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* g
   return 0;
 }
 
-int nc_divide_known(const double* x, double* q, int64_t n, double b) {
+int nc_divide_known(const double* x, const double* y, double* q, int64_t n, double b) {
   if (!x || !q || n < 0 || n > (int64_t)1 << 28) return fail(NC_ERR_ARG, "nc_divide_known: bad argument");
-  if (!(b != 0.0 && std::isfinite(b))) return fail(NC_ERR_ARG, "nc_divide_known: divisor must be finite and nonzero");
+  if (!y && !(b != 0.0 && std::isfinite(b)))
+    return fail(NC_ERR_ARG, "nc_divide_known: divisor must be finite and nonzero");
   if (n == 0) return 0;
-  double bh, bl;
-  recip_pair(b, bh, bl);
+  double bh = 0.0, bl = 0.0;
+  if (!y) recip_pair(b, bh, bl);
   double* d = nullptr;
   const size_t bytes = (size_t)n * sizeof(double);
-  CU(cudaMalloc(&d, 2 * bytes));
+  CU(cudaMalloc(&d, 3 * bytes));
   cudaError_t e = cudaMemcpy(d, x, bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && y) e = cudaMemcpy(d + 2 * n, y, bytes, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
-    k_divide_known<<<(unsigned)((n + 255) / 256), 256>>>(d, d + n, (int)n, b, bh, bl);
+    k_divide_known<<<(unsigned)((n + 255) / 256), 256>>>(d, y ? d + 2 * n : nullptr, d + n, (int)n, b, bh, bl);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpy(q, d + n, bytes, cudaMemcpyDeviceToHost);

@@ -45,8 +45,8 @@ struct Consts {
   double Kh, divdamp_coef, hdiff_fact_rho, CVW0, PRE00;
   int gam_unit;   // RGAM, RGAMH and GAM2H are 1 everywhere (shallow atmosphere)
   // rounded reciprocals and their tails, RN(1/b) and RN(1/b - RN(1/b)), of the
-  // divisors rscale and 3 (see div_by)
-  double rsc_h, rsc_l, third_h, third_l;
+  // divisors rscale, 3 and CVdry (see div_by)
+  double rsc_h, rsc_l, third_h, third_l, cvd_h, cvd_l;
   double afact[NC_MAXK], bfact[NC_MAXK], cfact[NC_MAXK], dfact[NC_MAXK];
   double rdgz[NC_MAXK], rdgzh[NC_MAXK];
 };
@@ -120,9 +120,27 @@ __device__ __forceinline__ double div_by(double x, double b, double bh, double b
   const double q = __fma_rn(r, bh, q0);
   return (x == 0.0) ? __dmul_rn(x, bh) : q;
 }
-// x / rscale and x / 3.0
+// x / rscale, x / 3.0 and x / CVdry
 __device__ __forceinline__ double div_r(double x) { return div_by(x, cC.rscale, cC.rsc_h, cC.rsc_l); }
 __device__ __forceinline__ double div3(double x) { return div_by(x, 3.0, cC.third_h, cC.third_l); }
+__device__ __forceinline__ double div_cvd(double x) { return div_by(x, cC.CVdry, cC.cvd_h, cC.cvd_l); }
+
+// The same division for a divisor computed at run time that several quotients
+// share: bh = RN(1/b) from the correctly rounded reciprocal __drcp_rn, and the
+// tail RN((1 - b*bh) * bh) (1 - b*bh is exact), which is within a relative
+// 2^-52 of 1/b - bh, so RN(x*bh + x*bl) is still within one ulp of x/b and the
+// correction step rounds the quotient correctly.
+struct Recip {
+  double b, h, l;
+};
+__device__ __forceinline__ Recip recip_of(double b) {
+  Recip r;
+  r.b = b;
+  r.h = __drcp_rn(b);
+  r.l = __dmul_rn(__fma_rn(-r.h, b, 1.0), r.h);
+  return r;
+}
+__device__ __forceinline__ double div_by(double x, const Recip& r) { return div_by(x, r.b, r.h, r.l); }
 
 // ---- indexing -------------------------------------------------------------
 __device__ __forceinline__ int ix(int i, int j, int k, int l) {

@@ -134,12 +134,13 @@ __device__ void diag_column_fused(const Col c, const Met m, const DiagArgs& a, d
     int p = c.at(k);
     double RHOG = P[0][p];
     double rho = RHOG / m.GSGAM2[p];
-    const double vx = P[1][p] / RHOG, vy = P[2][p] / RHOG, vz = P[3][p] / RHOG;
+    const Recip rr = recip_of(RHOG);   // five quotients by RHOG
+    const double vx = div_by(P[1][p], rr), vy = div_by(P[2][p], rr), vz = div_by(P[3][p], rr);
     a.vx[p] = vx;
     a.vy[p] = vy;
     a.vz[p] = vz;
-    double ein = P[5][p] / RHOG;
-    double q0 = a.Pq0[p] / RHOG;
+    double ein = div_by(P[5][p], rr);
+    double q0 = div_by(a.Pq0[p], rr);
     double qd = 1.0 - q0;
     double cv = q0 * cC.CVW0 + qd * cC.CVdry;
     double tem = ein / cv;

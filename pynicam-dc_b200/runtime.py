@@ -71,7 +71,7 @@ def load_library(path: str = LIB_PATH):
     lib.nc_grid_spring.restype = ctypes.c_int
     lib.nc_forcing_step.argtypes = [vp]
     lib.nc_forcing_step.restype = ctypes.c_int
-    lib.nc_divide_known.argtypes = [dp, dp, i64, ctypes.c_double]
+    lib.nc_divide_known.argtypes = [dp, dp, dp, i64, ctypes.c_double]
     lib.nc_divide_known.restype = ctypes.c_int
     lib.nc_destroy.argtypes = [vp]
     lib.nc_destroy.restype = None
@@ -103,13 +103,21 @@ def grid_spring(x, x_pl, have_sgp, plan, lam, dbar, dt, crit, max_iter):
     return x, x_pl, int(it.value)
 
 
-def divide_known(x, b: float) -> np.ndarray:
-    """x / b on the device with the kernels' known-divisor division
-    (nc_divide_known); the result should equal numpy's x / b bit for bit."""
+def divide_known(x, b) -> np.ndarray:
+    """x / b on the device with the kernels' division by a known divisor
+    (nc_divide_known): b a float (constant divisor, reciprocal pair from the
+    host) or an array like x (per-element reciprocal formed on the device).
+    The result should equal numpy's x / b bit for bit."""
     lib = load_library()
     x = np.ascontiguousarray(x, np.float64)
     q = np.empty_like(x)
-    rc = lib.nc_divide_known(x.ctypes.data, q.ctypes.data, x.size, float(b))
+    if np.ndim(b) == 0:
+        rc = lib.nc_divide_known(x.ctypes.data, None, q.ctypes.data, x.size, float(b))
+    else:
+        y = np.ascontiguousarray(b, np.float64)
+        if y.shape != x.shape:
+            raise ValueError("divisor array must have the shape of x")
+        rc = lib.nc_divide_known(x.ctypes.data, y.ctypes.data, q.ctypes.data, x.size, 0.0)
     if rc != 0:
         raise NicamError(f"nc_divide_known status {rc}: {lib.nc_last_error().decode(errors='replace')}")
     return q

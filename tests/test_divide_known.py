@@ -7,7 +7,8 @@ result must carry the same bits as x / b.
 The CPU test restates the method with exact rational arithmetic for the fused
 multiply-adds and checks it on random and near-midpoint quotients (the cases
 where a faithful but not correctly rounded quotient would show); the GPU test
-runs the device routine (nc_divide_known) on ten million values."""
+runs the device routine (nc_divide_known) on ten million values per divisor,
+and on per-element divisors with the reciprocal formed on the device."""
 from __future__ import annotations
 
 import math
@@ -31,6 +32,13 @@ def _fma(a: float, b: float, c: float) -> float:
 def _recip_pair(b: float):
     h = 1.0 / b
     return h, float(Fraction(1) / Fraction(b) - Fraction(h))
+
+
+def _recip_runtime(b: float):
+    """the device form for a divisor known only at run time: RN(1/b) and the
+    tail RN((1 - b*RN(1/b)) * RN(1/b))"""
+    h = 1.0 / b
+    return h, _fma(-h, b, 1.0) * h
 
 
 def _div_by(x: float, b: float, bh: float, bl: float) -> float:
@@ -71,11 +79,20 @@ def test_method_random_divisors():
             assert _bits(_div_by(x, b, bh, bl)) == _bits(x / b), (x, b)
 
 
+def test_method_runtime_reciprocal():
+    rng = random.Random(9)
+    for _ in range(60):
+        b = rng.uniform(1.0, 2.0) * 2.0 ** rng.randint(-40, 40)
+        bh, bl = _recip_runtime(b)
+        for x in _cases(b, 300, rng):
+            assert _bits(_div_by(x, b, bh, bl)) == _bits(x / b), (x, b)
+
+
 def test_method_signed_zero():
     for b in (3.0, -3.0, RSCALE):
-        bh, bl = _recip_pair(b)
-        for x in (0.0, -0.0):
-            assert _bits(_div_by(x, b, bh, bl)) == _bits(x / b)
+        for bh, bl in (_recip_pair(b), _recip_runtime(b)):
+            for x in (0.0, -0.0):
+                assert _bits(_div_by(x, b, bh, bl)) == _bits(x / b)
 
 
 def _device_cases(b: float, n: int, seed: int) -> np.ndarray:
@@ -97,3 +114,20 @@ def test_device_division_matches_ieee(pkg, b):
     want = x / b
     diff = np.flatnonzero(q.view(np.uint64) != want.view(np.uint64))
     assert diff.size == 0, (x[diff[:5]], q[diff[:5]], want[diff[:5]])
+
+
+@pytest.mark.gpu
+def test_device_division_per_element_divisors(pkg):
+    rng = np.random.default_rng(11)
+    n = 2_000_000
+    y = rng.uniform(1.0, 2.0, n) * np.exp2(rng.integers(-30, 30, n)).astype(np.float64)
+    x = rng.uniform(-1.0, 1.0, n) * np.exp2(rng.integers(-200, 200, n)).astype(np.float64)
+    m = rng.uniform(1.0, 2.0, n) * np.exp2(rng.integers(-60, 60, n)).astype(np.float64)
+    half = (np.nextafter(m, np.inf) - m) / 2
+    near = ((m.astype(np.longdouble) + half.astype(np.longdouble)) * y.astype(np.longdouble)).astype(np.float64)
+    xs = np.concatenate([x, near, np.nextafter(near, np.inf), [0.0, -0.0]])
+    ys = np.concatenate([y, y, y, [3.0, 3.0]])
+    q = pkg.runtime.divide_known(xs, ys)
+    want = xs / ys
+    diff = np.flatnonzero(q.view(np.uint64) != want.view(np.uint64))
+    assert diff.size == 0, (xs[diff[:5]], ys[diff[:5]], q[diff[:5]], want[diff[:5]])
