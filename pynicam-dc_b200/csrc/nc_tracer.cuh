@@ -252,10 +252,10 @@ __global__ void k_trc_hflux(TrcHfluxArgs a) {
       else fl[3 + f] = 0.0;
     }
     if (i == 1 && j == 1) fl[5] *= (double)cG.pntmask[l * 2 + 0];
-    double rg = a.rhog_t[p];
+    const Recip rg = recip_of(a.rhog_t[p]);   // six quotients by rhog_t
     for (int f = 0; f < 6; ++f) {
       a.flx[f][p] = fl[f];
-      double chv = fl[f] / rg;
+      double chv = div_by(fl[f], rg);
       a.ch[f][p] = chv;
       a.cm[f][p] = 0.5 - copysign(0.5, chv - cC.EPS);
     }
