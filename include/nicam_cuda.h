@@ -183,6 +183,33 @@ int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* g
  * NC_ERR_STATE.  Asynchronous on the handle's stream, like nc_step. */
 int nc_forcing_step(nc_handle* h);
 
+/* Dyn.history_vars_step (pynicamdc/nhm/dynamics/mod_dynamics.py:737-772 ->
+ * Hvar.history_vars, pynicamdc/nhm/driver/mod_history_vars.py:30-186) on the
+ * state the handle holds: the derived history diagnostics, computed on the
+ * device and copied to host arrays in the reference's layout.  items[n] (n <
+ * nitems) are item ids, written to out[n]:
+ *   0 ml_u, 1 ml_v, 2 ml_w, 3 ml_th, 4 ml_thv, 5 ml_omg, 6 ml_pres, 7 ml_tem,
+ *   8 ml_rho, 9 ml_hgt, 10 ml_mse, 11 ml_rh, 12 ml_rha, 13 ml_rhi, 14 ml_du,
+ *   15 ml_dv, 16 ml_dw, 17 ml_dtem, 18 ml_dq, 19 ml_ucos, 20 ml_vcos,
+ *   21 ml_th_prime                      -> (gall_1d, gall_1d, kall, lall)
+ *   22 sl_ps, 23 sl_pw, 24 sl_lwp, 25 sl_iwp, then 26.. 41 sl_u850, sl_v850,
+ *   sl_w850, sl_t850, the same at 500, 250 and 100 hPa -> (gall_1d, gall_1d, lall)
+ * (the reference's I/O order, share/mod_io.py:251-260).  The tendencies ml_d*
+ * are stateful as in the reference: the first output of each is zero, later
+ * ones (previous - current) * 86400 / dt / (nstep - nstep of the last output
+ * that formed tendencies), dq in g/kg/day; nstep is the model step count
+ * (TIME_cstep), dt the large time step.  The half-level w at the boundary rows
+ * is the one the last nc_step left (zero before the first step).  Needs the
+ * setup entries HIST_hgt (GRD_vz Z, (gall_1d, gall_1d, kall, lall)),
+ * HIST_coslat, HIST_zsfc, HIST_area (cos GRD_LAT, GRD_zs ZSFC, GMTR_area at K0;
+ * (gall_1d, gall_1d, 1, lall)), HIST_IJ (GMTR_p IX, IY, IZ, JX, JY, JZ at K0;
+ * (gall_1d, gall_1d, 1, lall, 6)), HIST_dgz (kall), HIST_consts (LHV, UNDEF,
+ * PSAT0, RTEM00, CPovR_liq, CPovR_ice, LovR_liq, LovR_ice, SATURATION_LLIMIT_TEMP,
+ * SATURATION_ULIMIT_TEMP) and HIST_tracers (int64 I_QV, I_QC, I_QR, I_QI, I_QS,
+ * I_QG, -1 where absent), with PRE00; otherwise NC_ERR_STATE.  Synchronous. */
+int nc_history_vars(nc_handle* h, const int32_t* items, int32_t nitems, int64_t nstep, double dt,
+                    double* const* out);
+
 /* Self-check of the divisions the kernels use in place of a general division
  * (the reference divides with numpy's IEEE division, e.g.
  * kernels/horizontalizevec.py:51-54, kernels/oprtdiffusion.py,

@@ -1552,10 +1552,12 @@ def tracer_advection(g, rhogq, rhogq_pl, rhog_in, rhog_in_pl, PM, PM_pl, frhog, 
 # --------------------------------------------------------------------------
 # the large step
 # --------------------------------------------------------------------------
-def dynamics_step(g, prg, prg_pl):
+def dynamics_step(g, prg, prg_pl, keep=None):
     """mod_dynamics.py:1725-2741 numpy path: one RK3-HEVI large step.
     ``prg (i,j,k,l,6+nq)`` / ``prg_pl (g,k,l,6+nq)`` are not modified; the new
-    state is returned (after the final halo exchange)."""
+    state is returned (after the final halo exchange).  With a dict ``keep``,
+    ``keep["w"]`` receives the diagnostic w of the last RK stage (boundary rows
+    as BNDCND left them), the buffer the history diagnostics read."""
     PROG = prg[..., 0:6].copy()
     PROG_pl = prg_pl[..., 0:6].copy()
     PROGq = prg[..., 6:].copy()
@@ -1606,6 +1608,8 @@ def dynamics_step(g, prg, prg_pl):
     out = np.concatenate([PROG, PROGq], axis=-1)
     out_pl = np.concatenate([PROG_pl, PROGq_pl], axis=-1)
     comm(g, out, out_pl)
+    if keep is not None:
+        keep["w"] = DIAG[..., I_w].copy()
     return out, out_pl
 
 

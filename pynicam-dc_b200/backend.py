@@ -29,7 +29,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .runtime import NicamCuda
+from .runtime import HIST_ITEMS, NicamCuda
 
 
 def geo_from_msc(msc) -> dict:
@@ -88,7 +88,37 @@ def geo_from_msc(msc) -> dict:
     elif getattr(m.rcnf, "AF_TYPE", "NONE") == "HELD-SUAREZ":
         # the column latitudes the forcing reads (mod_dynamics.py: GRD_LAT[:, :, K0, :])
         g["GRD_LAT"] = np.ascontiguousarray(m.grd.GRD_LAT[:, :, m.adm.ADM_K0, :])
+    g.update(_history_setup(m))
     return {k: np.asarray(v) for k, v in g.items()}
+
+
+def _history_setup(m) -> dict:
+    """what the derived history diagnostics read (mod_history_vars.py:30-186,
+    nhm/share/mod_saturation.py): height, latitude, surface height, layer
+    thicknesses, the GMTR_p east/north vectors and cell areas at K0, the
+    saturation constants and the tracer indices; empty when the services do
+    not carry them (the handle then has no history diagnostics)"""
+    try:
+        K0 = m.adm.ADM_K0
+        grd, gm, cn, st, r = m.grd, m.gmtr, m.cnst, m.satr, m.rcnf
+        h = {"hist_hgt": np.ascontiguousarray(grd.GRD_vz[:, :, :, :, grd.GRD_Z]),
+             "hist_lat": np.ascontiguousarray(grd.GRD_LAT[:, :, K0, :]),
+             "hist_zsfc": np.ascontiguousarray(grd.GRD_zs[:, :, K0, :, grd.GRD_ZSFC]),
+             "hist_dgz": np.asarray(grd.GRD_dgz),
+             "hist_area": np.ascontiguousarray(gm.GMTR_area),
+             "hist_IJ": np.stack([gm.GMTR_p[:, :, K0, :, i] for i in (gm.GMTR_p_IX, gm.GMTR_p_IY, gm.GMTR_p_IZ,
+                                                                       gm.GMTR_p_JX, gm.GMTR_p_JY, gm.GMTR_p_JZ)],
+                                 axis=-1),
+             "hist_LHV": cn.CONST_LHV, "hist_UNDEF": cn.CONST_UNDEF, "hist_PSAT0": cn.CONST_PSAT0,
+             "hist_RTEM00": st.RTEM00, "hist_CPovR_liq": st.CPovR_liq, "hist_CPovR_ice": st.CPovR_ice,
+             "hist_LovR_liq": st.LovR_liq, "hist_LovR_ice": st.LovR_ice,
+             "hist_SAT_LLIMIT": st.SATURATION_LLIMIT_TEMP, "hist_SAT_ULIMIT": st.SATURATION_ULIMIT_TEMP,
+             "hist_I_QV": r.I_QV}
+        for k in ("I_QC", "I_QR", "I_QI", "I_QS", "I_QG"):
+            h["hist_" + k] = getattr(r, k, -1)
+    except AttributeError:
+        return {}
+    return h
 
 
 class CudaDyn:
@@ -155,6 +185,28 @@ class CudaDyn:
         self.core.forcing_step()
         self._host_stale = True
         return None
+
+    def history_vars_step(self, msc, write_3d=True, write_2d=True):
+        """Dyn.history_vars_step (mod_dynamics.py:737-772): the derived history
+        diagnostics of the current state, computed on the device
+        (nc_history_vars) and returned as host arrays; the names are the I/O
+        groups being written (``msc.io._diag_names`` / ``_diag_names_2d``), all
+        of them without an I/O object.  The tendencies keep their previous
+        output on the device, as the reference's ``Hvar`` keeps it."""
+        io = getattr(msc, "io", None)
+        active = None
+        if io is not None:
+            active = set()
+            if write_3d:
+                active |= set(getattr(io, "_diag_names", []))
+            if write_2d:
+                active |= set(getattr(io, "_diag_names_2d", []))
+        names = HIST_ITEMS if active is None else tuple(n for n in HIST_ITEMS if n in active)
+        if active is not None and active - set(HIST_ITEMS):
+            raise NotImplementedError(f"cuda backend: history diagnostics {sorted(active - set(HIST_ITEMS))} "
+                                      "are not built on the device")
+        self._ensure_device(msc)
+        return self.core.history_vars(names, nstep=msc.tim.TIME_cstep, dt=msc.tim.TIME_dtl)
 
     def sync_prgvar_to_host(self, prgv, msc=None):
         if not self._device_valid:

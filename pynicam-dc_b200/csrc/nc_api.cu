@@ -14,6 +14,7 @@
 #include "nc_forcing.cuh"
 #include "nc_tracer.cuh"
 #include "nc_grid.cuh"
+#include "nc_history.cuh"
 
 using namespace nc;
 
@@ -250,6 +251,18 @@ struct nc_handle {
   FieldPair flx_v, rhog_t, flx[6], xc[9], ch[6], cm[6], q, gq[3], qa[3], Qmin, Qmax;
   FieldPair vph[8];             // horizontal terms of vp0 (div1, div2, dd, dpg)
   const double* hs_lat = nullptr;   // Held-Suarez latitude planes (optional)
+  // derived history diagnostics (optional setup; nc_history_vars)
+  bool hist = false;
+  const double *hist_hgt = nullptr, *hist_coslat = nullptr, *hist_zsfc = nullptr, *hist_area = nullptr;
+  const double *hist_IJ = nullptr, *hist_dgz = nullptr;
+  double hist_c[10] = {};
+  int hist_trc[6] = {-1, -1, -1, -1, -1, -1};   // I_QV, I_QC, I_QR, I_QI, I_QS, I_QG
+  double* hist_out[H_N] = {};                    // device outputs, allocated on first request
+  double* hist_old[5] = {};                      // previous outputs of the tendency fields
+  bool hist_old_set[5] = {};
+  double* hist_thmean = nullptr;
+  bool hist_has_nstep = false;
+  long long hist_nstep = 0;
   // offline tracer advection (integ_type TRCADV, DCMIP2012 test 1-1 winds)
   bool trcadv = false;
   double* trc_time = nullptr;       // model time of the prescribed winds (device scalar)
@@ -1092,6 +1105,26 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
     TRY(scalar(T, "PRE00", C.PRE00));
     TRY(up_reg(h, T, "AF_hs_lat_terms", 1, 3, &h->hs_lat));
   }
+  if (T.get("HIST_hgt")) {   // derived history diagnostics configured (nc_history_vars)
+    if (!T.get("PRE00")) return fail(NC_ERR_ARG, "HIST_hgt given without PRE00");
+    TRY(scalar(T, "PRE00", C.PRE00));
+    TRY(up_reg(h, T, "HIST_hgt", D.KA, 1, &h->hist_hgt));
+    TRY(up_reg(h, T, "HIST_coslat", 1, 1, &h->hist_coslat));
+    TRY(up_reg(h, T, "HIST_zsfc", 1, 1, &h->hist_zsfc));
+    TRY(up_reg(h, T, "HIST_area", 1, 1, &h->hist_area));
+    TRY(up_reg(h, T, "HIST_IJ", 1, 6, &h->hist_IJ));
+    TRY(up_pl(h, T, "HIST_dgz", D.KA, &h->hist_dgz));
+    TRY(up_vec(T, "HIST_consts", 10, h->hist_c));
+    const nc_array* tr = T.get("HIST_tracers");
+    if (!tr || tr->dtype != NC_I64 || numel(tr) != 6) return fail(NC_ERR_ARG, "HIST_tracers: six int64 indices");
+    for (int n = 0; n < 6; ++n) {
+      const int64_t v = ((const int64_t*)tr->data)[n];
+      if (v < -1 || v >= D.nq) return fail(NC_ERR_ARG, "HIST_tracers: index outside the tracers");
+      h->hist_trc[n] = (int)v;
+    }
+    TRY(dev_alloc(h, &h->hist_thmean, (size_t)D.KA));
+    h->hist = true;
+  }
   const int64_t npl = D.npl;
   TRY(up_pl(h, T, "VMTR_GSGAM2_pl", npl, &Gm.GSGAM2_pl));
   TRY(up_pl(h, T, "VMTR_GSGAM2H_pl", npl, &Gm.GSGAM2H_pl));
@@ -1596,6 +1629,96 @@ int nc_grid_spring(int32_t lall, int32_t gall_1d, double* x, double* x_pl, const
   for (void* p : mem) cudaFree(p);
   if (st) cudaStreamDestroy(st);
   return rc;
+}
+
+int nc_history_vars(nc_handle* h, const int32_t* items, int32_t nitems, int64_t nstep, double dt,
+                    double* const* out) {
+  if (!h || (nitems > 0 && (!items || !out)) || nitems < 0 || nitems > H_N)
+    return fail(NC_ERR_ARG, "nc_history_vars: bad argument");
+  if (!h->hist)
+    return fail(NC_ERR_STATE, "nc_history_vars: the handle was created without the HIST_* setup entries");
+  if (!h->have_state) return fail(NC_ERR_STATE, "nc_history_vars: no state uploaded");
+  if (!(dt > 0.0)) return fail(NC_ERR_ARG, "nc_history_vars: dt must be positive");
+  bool want[H_N] = {};
+  for (int n = 0; n < nitems; ++n) {
+    if (items[n] < 0 || items[n] >= H_N) return fail(NC_ERR_ARG, "nc_history_vars: item id out of range");
+    if (want[items[n]]) return fail(NC_ERR_ARG, "nc_history_vars: item requested twice");
+    if (!out[n]) return fail(NC_ERR_ARG, "nc_history_vars: null output pointer");
+    want[items[n]] = true;
+  }
+  TRY(load_consts(h));
+  const Dims& D = h->D;
+  cudaStream_t s = h->stream;
+  HistArgs a;
+  for (int v = 0; v < 6; ++v) a.P[v] = h->P[v].r;
+  for (int v = 0; v < NC_MAXNQ; ++v) a.Pq[v] = v < D.nq ? h->Pq[v].r : nullptr;
+  a.iqv = h->hist_trc[0];
+  a.iql[0] = h->hist_trc[1]; a.iql[1] = h->hist_trc[2];
+  a.iqs[0] = h->hist_trc[3]; a.iqs[1] = h->hist_trc[4]; a.iqs[2] = h->hist_trc[5];
+  a.wdiag = h->w.r;
+  a.hgt = h->hist_hgt; a.coslat = h->hist_coslat; a.zsfc = h->hist_zsfc; a.IJ = h->hist_IJ;
+  a.dgz = h->hist_dgz;
+  a.thmean = h->hist_thmean;
+  for (int n = 0; n < H_N; ++n) {
+    a.out[n] = nullptr;
+    if (!want[n]) continue;
+    if (!h->hist_out[n]) TRY(dev_alloc(h, &h->hist_out[n], (size_t)(n < H_N3 ? D.npt : D.npt2)));
+    a.out[n] = h->hist_out[n];
+  }
+  // interval tendencies: the previous output of each tendency field and the
+  // step count of the last output that formed any (mod_history_vars.py:166-180)
+  bool need_tend = false;
+  for (int n = 0; n < 5; ++n) need_tend = need_tend || want[H_DU + n];
+  const long long dn = (need_tend && h->hist_has_nstep) ? (long long)nstep - h->hist_nstep : 0;
+  a.fac = 86400.0 / dt;
+  a.fac_q = a.fac * 1.0e3;
+  a.dn = (double)dn;
+  for (int n = 0; n < 5; ++n) {
+    a.old[n] = nullptr;
+    a.tform[n] = 0;
+    if (!want[H_DU + n]) continue;
+    if (!h->hist_old[n]) TRY(dev_alloc(h, &h->hist_old[n], (size_t)D.npt));
+    a.old[n] = h->hist_old[n];
+    a.tform[n] = (h->hist_old_set[n] && dn > 0) ? 1 : 0;
+  }
+  const double* c = h->hist_c;
+  a.LHV = c[0]; a.UNDEF = c[1]; a.PSAT0 = c[2]; a.RTEM00 = c[3]; a.CPovR_liq = c[4]; a.CPovR_ice = c[5];
+  a.LovR_liq = c[6]; a.LovR_ice = c[7]; a.SAT_LL = c[8]; a.SAT_UL = c[9];
+  // the state may still be arriving on the upload stream; the staging buffer
+  // reused below may still be leaving on the download stream
+  CU(cudaStreamWaitEvent(s, h->ev_in_ready, 0));
+  CU(cudaStreamWaitEvent(s, h->ev_out_done, 0));
+  if (want[H_TH_PRIME]) {
+    k_history_thmean<<<(unsigned)D.KA, 256, 0, s>>>(a, h->hist_area, h->hist_thmean);
+    TRY(check_launch(h, "history_thmean"));
+  }
+  k_history<<<(unsigned)((D.npt2 + 127) / 128), 128, 0, s>>>(a);
+  TRY(check_launch(h, "history"));
+  for (int n = 0; n < 5; ++n)
+    if (want[H_DU + n]) h->hist_old_set[n] = true;
+  if (need_tend) {
+    h->hist_nstep = nstep;
+    h->hist_has_nstep = true;
+  }
+  // each output to the host in the reference layout: (i, j, k, l) or (i, j, l)
+  for (int n = 0; n < nitems; ++n) {
+    const int it = items[n];
+    if (it < H_N3) {
+      VarPtrs vp{};
+      vp.v[0] = h->hist_out[it];
+      const dim3 gt((unsigned)((D.G + UI - 1) / UI), (unsigned)((D.L + UC - 1) / UC), (unsigned)(D.G * D.KA));
+      k_pack_t<<<gt, 256, 0, s>>>(h->stage_out, vp, 1);
+      TRY(check_launch(h, "history_pack"));
+      CU(cudaMemcpyAsync(out[n], h->stage_out, (size_t)D.npt * sizeof(double), cudaMemcpyDeviceToHost, s));
+    } else {
+      k_pack_plane<<<(unsigned)((D.npt2 + 255) / 256), 256, 0, s>>>(h->stage_out, h->hist_out[it]);
+      TRY(check_launch(h, "history_pack_plane"));
+      CU(cudaMemcpyAsync(out[n], h->stage_out, (size_t)D.npt2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    CU(cudaStreamSynchronize(s));
+  }
+  CU(cudaStreamSynchronize(s));
+  return 0;
 }
 
 int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* gsgam2, const double* volume,

@@ -32,7 +32,7 @@ _lib = None
 # every entry point declared in include/nicam_cuda.h
 EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_state_async", "nc_join_copies",
            "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",
-           "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_forcing_step", "nc_divide_known",
+           "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_forcing_step", "nc_history_vars", "nc_divide_known",
            "nc_last_error", "nc_destroy")
 
 
@@ -72,6 +72,8 @@ def load_library(path: str = LIB_PATH):
     lib.nc_forcing_step.argtypes = [vp]
     lib.nc_forcing_step.restype = ctypes.c_int
     lib.nc_divide_known.argtypes = [dp, dp, dp, i64, ctypes.c_double]
+    lib.nc_history_vars.argtypes = [vp, dp, i32, i64, ctypes.c_double, dp]
+    lib.nc_history_vars.restype = ctypes.c_int
     lib.nc_divide_known.restype = ctypes.c_int
     lib.nc_destroy.argtypes = [vp]
     lib.nc_destroy.restype = None
@@ -146,6 +148,19 @@ def _scalar(a):
     return np.asarray(a).reshape(-1)[0].item()
 
 
+# derived history diagnostics: item names in the order of nc_history_vars's ids
+# (the reference's I/O order, share/mod_io.py:251-260), the constants and the
+# tracer indices of its setup entries
+HIST_ITEMS = ('ml_u', 'ml_v', 'ml_w', 'ml_th', 'ml_thv', 'ml_omg', 'ml_pres', 'ml_tem', 'ml_rho', 'ml_hgt',
+              'ml_mse', 'ml_rh', 'ml_rha', 'ml_rhi', 'ml_du', 'ml_dv', 'ml_dw', 'ml_dtem', 'ml_dq', 'ml_ucos',
+              'ml_vcos', 'ml_th_prime', 'sl_ps', 'sl_pw', 'sl_lwp', 'sl_iwp') + tuple(
+    f'sl_{f}{lev}' for lev in ('850', '500', '250', '100') for f in ('u', 'v', 'w', 't'))
+HIST_N3 = 22
+HIST_CONSTS = ("LHV", "UNDEF", "PSAT0", "RTEM00", "CPovR_liq", "CPovR_ice", "LovR_liq", "LovR_ice", "SAT_LLIMIT",
+               "SAT_ULIMIT")
+HIST_TRACERS = ("I_QV", "I_QC", "I_QR", "I_QI", "I_QS", "I_QG")
+
+
 def setup_table(geo: dict) -> dict:
     """Host arrays handed to ``nc_create`` (names as in include/nicam_cuda.h).
 
@@ -191,6 +206,18 @@ def setup_table(geo: dict) -> dict:
         lat = lat.reshape(lat.shape[0], lat.shape[1], 1, lat.shape[-1])
         sinlat, coslat = np.abs(np.sin(lat)), np.abs(np.cos(lat))
         t["AF_hs_lat_terms"] = np.ascontiguousarray(np.stack([sinlat ** 2, coslat ** 2, coslat ** 4], axis=-1))
+        t["PRE00"] = np.asarray(float(_scalar(geo["PRE00"])), np.float64)
+    if "hist_hgt" in geo:   # derived history diagnostics (nc_history_vars)
+        G, L = int(_scalar(geo["gall_1d"])), int(_scalar(geo["lall"]))
+        plane = lambda x: np.ascontiguousarray(np.asarray(x, np.float64).reshape(G, G, 1, L))
+        t["HIST_hgt"] = np.ascontiguousarray(geo["hist_hgt"], np.float64)
+        t["HIST_coslat"] = plane(np.cos(np.asarray(geo["hist_lat"], np.float64)))
+        t["HIST_zsfc"] = plane(geo["hist_zsfc"])
+        t["HIST_area"] = plane(geo["hist_area"])
+        t["HIST_IJ"] = np.ascontiguousarray(np.asarray(geo["hist_IJ"], np.float64).reshape(G, G, 1, L, 6))
+        t["HIST_dgz"] = np.ascontiguousarray(geo["hist_dgz"], np.float64)
+        t["HIST_consts"] = np.ascontiguousarray([float(_scalar(geo["hist_" + k])) for k in HIST_CONSTS], np.float64)
+        t["HIST_tracers"] = np.ascontiguousarray([int(_scalar(geo["hist_" + k])) for k in HIST_TRACERS], np.int64)
         t["PRE00"] = np.asarray(float(_scalar(geo["PRE00"])), np.float64)
     t["pntmask"] = np.ascontiguousarray(geo["pntmask"], np.int32)
     t["have_sgp"] = np.ascontiguousarray(geo["have_sgp"], np.bool_)
@@ -270,6 +297,24 @@ class NicamCuda:
         """Dyn.forcing_step for AF_TYPE 'HELD-SUAREZ' (nc_forcing_step); the
         handle must have been built from a setup with GRD_LAT"""
         _check(self._lib.nc_forcing_step(self._h))
+
+    def history_vars(self, names, nstep: int, dt: float) -> dict:
+        """the derived history diagnostics ``names`` (from ``HIST_ITEMS``) of
+        the device state (nc_history_vars): {name: host array}, model-level
+        fields (gall_1d, gall_1d, kall, lall), slices and column integrals
+        (gall_1d, gall_1d, lall)"""
+        ids = []
+        for n in names:
+            if n not in HIST_ITEMS:
+                raise NotImplementedError(f"history diagnostic {n!r} is not built on the device")
+            ids.append(HIST_ITEMS.index(n))
+        G, K, L = self.shape[0], self.shape[2], self.shape[3]
+        res = {n: np.empty((G, G, K, L) if i < HIST_N3 else (G, G, L)) for n, i in zip(names, ids)}
+        idarr = np.ascontiguousarray(ids, np.int32)
+        ptrs = np.ascontiguousarray([res[n].ctypes.data for n in names], np.uint64)
+        _check(self._lib.nc_history_vars(self._h, idarr.ctypes.data if ids else None, len(ids), int(nstep),
+                                         float(dt), ptrs.ctypes.data if ids else None))
+        return res
 
     def run_phases(self, nphases: int):
         """debugging: run the first ``nphases`` phases of one step"""

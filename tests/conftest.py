@@ -48,3 +48,30 @@ def golden_trcadv():
     the prescribed winds read) and four states"""
     from make_golden import load
     return load(os.path.join(GOLDEN, "gl03_z10_trcadv.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_hist():
+    """the reference's own history diagnostics of the gl03_z10_trc run
+    (make_hist.py): the extra setup they read (keys without the geo. prefix:
+    GRD_Z, GRD_LAT, GRD_zsfc, GRD_dgz, GMTR_p_IJ, GMTR_area, constants, tracer
+    indices), the outputs after step 2 (seeded after step 1) and the step
+    counts and dt of the two calls"""
+    import numpy as np
+    z = np.load(os.path.join(GOLDEN, "gl03_z10_hist.npz"))
+    hg = {k[4:]: z[k] for k in z.files if k.startswith("geo.")}
+    out = {k[5:]: z[k] for k in z.files if k.startswith("hist.")}
+    return hg, out
+
+
+def hist_geo(geo: dict, hg: dict) -> dict:
+    """the setup dict of a handle with history diagnostics: the fixture's
+    arrays under the keys the backend's setup collects (``hist_*``)"""
+    g = dict(geo)
+    g.update(hist_hgt=hg["GRD_Z"], hist_lat=hg["GRD_LAT"], hist_zsfc=hg["GRD_zsfc"], hist_dgz=hg["GRD_dgz"],
+             hist_area=hg["GMTR_area"], hist_IJ=hg["GMTR_p_IJ"])
+    for k in ("LHV", "UNDEF", "PSAT0", "RTEM00", "CPovR_liq", "CPovR_ice", "LovR_liq", "LovR_ice",
+              "I_QV", "I_QC", "I_QR", "I_QI", "I_QS", "I_QG"):
+        g["hist_" + k] = hg[k]
+    g["hist_SAT_LLIMIT"], g["hist_SAT_ULIMIT"] = hg["SAT_LLIMIT"], hg["SAT_ULIMIT"]
+    return g

@@ -12,7 +12,7 @@ import numpy as np
 
 
 def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_type: str = "RK3",
-             coords: dict = None):
+             coords: dict = None, hist: dict = None, io_names=None):
     g = {k: np.asarray(v) for k, v in geo.items()}
     sc = lambda k: g[k].reshape(-1)[0].item()
     adm = NS(ADM_kall=int(sc("kall")), ADM_kmin=int(sc("kmin")), ADM_kmax=int(sc("kmax")),
@@ -21,6 +21,9 @@ def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_
     cnst = NS(CONST_GRAV=sc("GRAV"), CONST_Rdry=sc("Rdry"), CONST_CVdry=sc("CVdry"), CONST_CPdry=sc("CPdry"),
               CONST_Rvap=sc("Rvap"), CONST_OHM=sc("OHM"), CONST_RADIUS=sc("RADIUS"), CONST_EPS=sc("EPS"),
               CONST_HUGE=sc("HUGE"), CONST_PRE00=sc("PRE00"))
+    if hist is not None:
+        cnst.CONST_LHV, cnst.CONST_UNDEF, cnst.CONST_PSAT0 = (np.asarray(hist[k]).item()
+                                                            for k in ("LHV", "UNDEF", "PSAT0"))
     grd = NS(GRD_rscale=sc("rscale"))
     for k in ("GRD_x", "GRD_x_pl", "GRD_xr", "GRD_xr_pl", "GRD_afact", "GRD_bfact", "GRD_cfact", "GRD_dfact",
               "GRD_rdgz", "GRD_rdgzh"):
@@ -36,6 +39,19 @@ def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_
         grd.GRD_vz = np.stack([coords["GRD_Z"], coords["GRD_ZH"]], axis=-1)
         grd.GRD_vz_pl = np.stack([coords["GRD_Z_pl"], coords["GRD_ZH_pl"]], axis=-1)
     gmtr = NS(**{k: g[k] for k in ("GMTR_t", "GMTR_a", "GMTR_p", "GMTR_t_pl", "GMTR_a_pl", "GMTR_p_pl")})
+    satr = None
+    if hist is not None:   # what the history diagnostics read (make_hist.py's extra setup)
+        grd.GRD_Z, grd.GRD_ZSFC = 0, 0
+        grd.GRD_vz = np.asarray(hist["GRD_Z"])[..., None]
+        grd.GRD_LAT = np.asarray(hist["GRD_LAT"])[:, :, None, :]
+        grd.GRD_zs = np.asarray(hist["GRD_zsfc"])[:, :, None, :, None]
+        grd.GRD_dgz = np.asarray(hist["GRD_dgz"])
+        gmtr.GMTR_area = np.asarray(hist["GMTR_area"])
+        gmtr.GMTR_p_IX, gmtr.GMTR_p_IY, gmtr.GMTR_p_IZ, gmtr.GMTR_p_JX, gmtr.GMTR_p_JY, gmtr.GMTR_p_JZ = range(2, 8)
+        h = lambda k: np.asarray(hist[k]).item()
+        satr = NS(RTEM00=h("RTEM00"), CPovR_liq=h("CPovR_liq"), CPovR_ice=h("CPovR_ice"), LovR_liq=h("LovR_liq"),
+                  LovR_ice=h("LovR_ice"), SATURATION_LLIMIT_TEMP=h("SAT_LLIMIT"),
+                  SATURATION_ULIMIT_TEMP=h("SAT_ULIMIT"))
     oprt = NS(**{k: g[k] for k in g if k.startswith("OPRT_")})
     vmtr = NS(**{k: g[k] for k in g if k.startswith("VMTR_")})
     bsst = NS(**{k: g[k] for k in ("rho_bs", "pre_bs", "tem_bs", "rho_bs_pl", "pre_bs_pl", "tem_bs_pl")})
@@ -49,7 +65,10 @@ def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_
               THUBURN_LIM=True, DYN_DIV_NUM=1,
               DCTEST_type="Traceradvection" if integ_type == "TRCADV" else "",
               DCTEST_case="1-1" if integ_type == "TRCADV" else "")
-    tim = NS(TIME_dtl=sc("dtl"), TIME_dts=sc("dts"), TIME_integ_type=integ_type)
+    tim = NS(TIME_dtl=sc("dtl"), TIME_dts=sc("dts"), TIME_integ_type=integ_type, TIME_cstep=0)
+    if hist is not None:
+        for k in ("I_QV", "I_QC", "I_QR", "I_QI", "I_QS", "I_QG"):
+            setattr(rcnf, k, int(np.asarray(hist[k]).item()))
     n = int(sc("gall_1d")) ** 2 * int(sc("lall"))
     numf = NS(hdiff_fact_rho=sc("hdiff_fact_rho"), Kh_coef=np.full(n, sc("Kh_coef")),
               divdamp_coef=np.full(n, sc("divdamp_coef")), lap_order_hdiff=2, lap_order_divdamp=2,
@@ -59,5 +78,11 @@ def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_
     dyn = NS(num_of_iteration_lstep=len(sstep), num_of_iteration_sstep=np.concatenate([sstep, np.zeros(4, np.int64)]))
     ppm = NS(pntmask=g["pntmask"])
     prgv = NS(PRG_var=np.array(state, copy=True), PRG_var_pl=np.array(state_pl, copy=True))
-    return NS(adm=adm, cnst=cnst, grd=grd, gmtr=gmtr, oprt=oprt, vmtr=vmtr, bsst=bsst, comm=comm, rcnf=rcnf,
-              tim=tim, numf=numf, dyn=dyn, ppm=ppm, prgv=prgv)
+    m = NS(adm=adm, cnst=cnst, grd=grd, gmtr=gmtr, oprt=oprt, vmtr=vmtr, bsst=bsst, comm=comm, rcnf=rcnf,
+           tim=tim, numf=numf, dyn=dyn, ppm=ppm, prgv=prgv)
+    if satr is not None:
+        m.satr = satr
+    if io_names is not None:   # the I/O object's diagnostic groups (share/mod_io.py:248-265)
+        m.io = NS(_diag_names=[n for n in io_names if n.startswith("ml_")],
+                  _diag_names_2d=[n for n in io_names if n.startswith("sl_")])
+    return m

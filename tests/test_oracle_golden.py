@@ -58,3 +58,25 @@ def test_oracle_trcadv_matches_reference_three_steps(golden_trcadv):
     # four passive tracers were advected and the winds were reset every step
     assert np.abs(st["state3"][..., 7:11] - st["state0"][..., 7:11]).max() > 0.0
     assert np.abs(st["state2"][..., 1:5] - st["state1"][..., 1:5]).max() > 0.0
+
+
+def test_oracle_history_matches_reference(golden, golden_hist):
+    """the derived history diagnostics (oracle/nicam_history.py) against the
+    reference's own Dyn.history_vars_step after steps 1 and 2
+    (tests/golden/make_hist.py): all 42 fields bit-for-bit, the tendencies
+    over one step included"""
+    from oracle import nicam_history as OH
+    geo, st = golden
+    hg, ref = golden_hist
+    G = O.Geo(geo)
+    H = OH.History()
+    s, sp = st["state0"], st["state0_pl"]
+    for n in (1, 2):
+        keep = {}
+        s, sp = O.dynamics_step(G, s, sp, keep=keep)
+        out = H(G, hg, s, dt=float(ref["dtl"]), nstep=int(ref[f"nstep{n}"]), w_prev=keep["w"])
+    assert sorted(out) == sorted(OH.ML + OH.SL)
+    for k in OH.ML + OH.SL:
+        assert np.array_equal(out[k], ref[k]), k
+    for k in ("ml_du", "ml_dtem", "ml_dq", "sl_pw", "ml_th_prime", "sl_u850", "ml_rh"):
+        assert np.abs(ref[k]).max() > 0.0, k
