@@ -183,6 +183,31 @@ int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* g
  * NC_ERR_STATE.  Asynchronous on the handle's stream, like nc_step. */
 int nc_forcing_step(nc_handle* h);
 
+/* Restart files in the reference's fio format (input/output_io_mode
+ * "ADVANCED", nhm/share/mod_fio.py), read and written from the device state:
+ * every variable is stored as a big-endian float64 stream (region, k, ij) with
+ * ij = j*gall_1d + i, which is the device field layout byte-swapped, so the
+ * payloads move without a host transposition; the headers are the caller's.
+ * var: 0..5 RHOG, RHOGVX, RHOGVY, RHOGVZ, RHOGW, RHOGE; 6.. the tracers.
+ *
+ * nc_restart_pack: writes the regional payload of `var` (lall*kall*gall_1d^2
+ * doubles, file byte order) into `host` (Prgvar.restart_output,
+ * nhm/share/mod_prgvar.py:182-216, prognostic items).  Synchronous.
+ *
+ * nc_restart_unpack: loads the regional field `var` from such a payload,
+ * repairing non-finite values on the dummy levels as fio_read does
+ * (mod_fio.py:73-84).  Synchronous.
+ *
+ * nc_restart_finish: after every variable is loaded, COMM_var
+ * (share/mod_comm.py:2172-2300): each pole centre takes the value of its
+ * source cell (pole_src: nsrc rows of int64 [pole g, pole l, i, j, l], the
+ * p2r copies whose regional side is the region the pole belongs to), then the
+ * halo exchange of the whole state.  The state is then the handle's
+ * (Prgvar._read_prognostic_restart, mod_prgvar.py:266-306).  nsrc <= 64. */
+int nc_restart_pack(nc_handle* h, int32_t var, void* host);
+int nc_restart_unpack(nc_handle* h, int32_t var, const void* host);
+int nc_restart_finish(nc_handle* h, const int64_t* pole_src, int32_t nsrc);
+
 /* Dyn.history_vars_step (pynicamdc/nhm/dynamics/mod_dynamics.py:737-772 ->
  * Hvar.history_vars, pynicamdc/nhm/driver/mod_history_vars.py:30-186) on the
  * state the handle holds: the derived history diagnostics, computed on the

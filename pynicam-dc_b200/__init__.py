@@ -8,4 +8,4 @@ conventions and step API kept on the host side.
 """
 from .runtime import NicamCuda, NicamError, load_library, setup_table, LIB_PATH, EXPORTS  # noqa: F401
 from .backend import CudaDyn  # noqa: F401
-from . import halo  # noqa: F401
+from . import halo, restart  # noqa: F401

@@ -29,6 +29,7 @@ from __future__ import annotations
 
 import numpy as np
 
+from . import restart
 from .runtime import HIST_ITEMS, NicamCuda
 
 
@@ -90,6 +91,22 @@ def geo_from_msc(msc) -> dict:
         g["GRD_LAT"] = np.ascontiguousarray(m.grd.GRD_LAT[:, :, m.adm.ADM_K0, :])
     g.update(_history_setup(m))
     return {k: np.asarray(v) for k, v in g.items()}
+
+
+def pole_centre_sources(m):
+    """the p2r copies COMM_var reverses to fill the pole centres
+    (share/mod_comm.py:2249-2262): rows [pole g, pole l, i, j, l] of the copies
+    whose regional side belongs to the region the pole is assigned to"""
+    a, co = m.adm, m.comm
+    cl = co.Copy_list_p2r
+    rows = []
+    for ipos in range(int(co.Copy_info_p2r[co.I_size])):
+        l_reg = int(cl[co.I_l_to, ipos])
+        r = a.RGNMNG_lp2r[l_reg, co.Copy_info_p2r[co.I_prc_to]]
+        if r == a.RGNMNG_rgn4pl[a.I_NPL] or r == a.RGNMNG_rgn4pl[a.I_SPL]:
+            rows.append([int(cl[co.I_gridi_from, ipos]), int(cl[co.I_l_from, ipos]), int(cl[co.I_gridi_to, ipos]),
+                         int(cl[co.I_gridj_to, ipos]), l_reg])
+    return np.asarray(rows, np.int64).reshape(-1, 5)
 
 
 def _history_setup(m) -> dict:
@@ -207,6 +224,37 @@ class CudaDyn:
                                       "are not built on the device")
         self._ensure_device(msc)
         return self.core.history_vars(names, nstep=msc.tim.TIME_cstep, dt=msc.tim.TIME_dtl)
+
+    def restart_output(self, msc, basename: str, ctime: int = 0):
+        """Prgvar.restart_output (nhm/share/mod_prgvar.py:182-216) for
+        output_io_mode "ADVANCED" and the prognostic items, written from the
+        device state without a host copy of PRG_var: <basename>000000 (one
+        process holds every region)."""
+        prgv = msc.prgv
+        if prgv.output_io_mode != "ADVANCED" or getattr(prgv, "output_diagnostics", False):
+            raise NotImplementedError("cuda backend: restart output in the ADVANCED (fio) format with the "
+                                      "prognostic variables only")
+        items = [(name, desc, unit, slot) for (name, desc, unit, _src, slot) in
+                 prgv._restart_output_items(msc.rcnf)]
+        self._ensure_device(msc)
+        a = msc.adm
+        rgnid = [int(a.RGNMNG_lp2r[l, a.ADM_prc_me]) for l in range(a.ADM_lall)]
+        restart.write(self.core, basename + "0" * 6, items, prgv.layername, rgnid, a.ADM_glevel, a.ADM_rlevel,
+                      ctime)
+
+    def restart_input(self, msc):
+        """Prgvar.restart_input's prognostic read (nhm/share/mod_prgvar.py:266-330)
+        of <restart_input_basename>000000 in the ADVANCED (fio) format straight
+        into the device state (COMM_var included); the host PRG_var is then
+        stale."""
+        prgv, r = msc.prgv, msc.rcnf
+        if prgv.input_io_mode != "ADVANCED" or getattr(prgv, "input_diagnostics", False):
+            raise NotImplementedError("cuda backend: restart input in the ADVANCED (fio) format, prognostic read")
+        names = [r.PRG_name[v] for v in range(r.PRG_vmax0)] + ["rhog" + r.TRC_name[q] for q in range(r.TRC_vmax)]
+        restart.read(self.core, prgv.restart_input_basename + "0" * 6, names, pole_centre_sources(msc),
+                     allow_missingq=bool(getattr(prgv, "allow_missingq", False)))
+        self._device_valid = True
+        self._host_stale = True
 
     def sync_prgvar_to_host(self, prgv, msc=None):
         if not self._device_valid:

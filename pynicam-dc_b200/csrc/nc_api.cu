@@ -149,6 +149,42 @@ __global__ void __launch_bounds__(256) k_pack_t(double* st, VarPtrs reg, int nv)
   }
 }
 
+// restart payloads: 64-bit byte swap between the file's big-endian stream and a field
+__device__ __forceinline__ unsigned long long bswap64(unsigned long long x) {
+  const unsigned lo = __byte_perm((unsigned)x, 0u, 0x0123), hi = __byte_perm((unsigned)(x >> 32), 0u, 0x0123);
+  return ((unsigned long long)lo << 32) | hi;
+}
+__global__ void k_restart_swap(unsigned long long* dst, const unsigned long long* src, int n) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t < n) dst[t] = bswap64(src[t]);
+}
+// fio_read's repair of the dummy levels (nhm/share/mod_fio.py:73-84): a
+// non-finite value on the top dummy level takes the level below, then one on
+// the bottom dummy level takes the level above
+__global__ void k_restart_dummy(double* f) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.npt2i) return;
+  const int G = cD.G, KA = cD.KA;
+  const int i = t % G, j = (t / G) % G, l = t / (G * G);
+  const int pt = ix(i, j, KA - 1, l), pb = ix(i, j, 0, l);
+  if (!isfinite(f[pt])) f[pt] = f[pt - cD.planei];
+  if (!isfinite(f[pb])) f[pb] = f[pb + cD.planei];
+}
+// COMM_var's p2r-reverse copy (share/mod_comm.py:2249-2262): the pole centre
+// takes the value of the regional halo cell its designated region holds
+struct PoleSrc {
+  int n;
+  int e[64][5];   // pole g, pole l, regional i, j, l
+};
+__global__ void k_pole_centre(VarPtrs reg, VarPtrs pol, int nv, PoleSrc ps) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= ps.n * cD.KA) return;
+  const int e = t / cD.KA, k = t % cD.KA;
+  const int* r = ps.e[e];
+  const int qp = ipl(r[0], k, r[1]), qr = ix(r[2], r[3], k, r[4]);
+  for (int v = 0; v < nv; ++v) pol.v[v][qp] = reg.v[v][qr];
+}
+
 // the pole part of the layout conversion: (g, k, l, v) <-> fields [v][g][k][l]
 __global__ void k_unpack_pl(const double* st_pl, VarPtrs pol, int nv) {
   const int q = (int)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1629,6 +1665,82 @@ int nc_grid_spring(int32_t lall, int32_t gall_1d, double* x, double* x_pl, const
   for (void* p : mem) cudaFree(p);
   if (st) cudaStreamDestroy(st);
   return rc;
+}
+
+// ---- restart files (fio "ADVANCED": nhm/share/mod_fio.py) ------------------
+// A variable's payload in the file is the big-endian stream (region, k, ij),
+// ij = j*gall_1d + i: the device field layout [l][k][j][i], byte-swapped.
+static int restart_field(nc_handle* h, int32_t var, double** f) {
+  if (var < 0 || var >= 6 + h->D.nq) return fail(NC_ERR_ARG, "restart: variable index out of range");
+  *f = var < 6 ? h->P[var].r : h->Pq[var - 6].r;
+  return 0;
+}
+
+int nc_restart_pack(nc_handle* h, int32_t var, void* host) {
+  if (!h || !host) return fail(NC_ERR_ARG, "nc_restart_pack: null argument");
+  if (!h->have_state) return fail(NC_ERR_STATE, "nc_restart_pack: no state uploaded");
+  double* f;
+  TRY(restart_field(h, var, &f));
+  TRY(load_consts(h));
+  const Dims& D = h->D;
+  CU(cudaStreamWaitEvent(h->stream, h->ev_out_done, 0));   // the staging buffer is free
+  k_restart_swap<<<(unsigned)((D.npt + 255) / 256), 256, 0, h->stream>>>(
+      (unsigned long long*)h->stage_out, (const unsigned long long*)f, (int)D.npt);
+  TRY(check_launch(h, "restart_pack"));
+  CU(cudaMemcpyAsync(host, h->stage_out, (size_t)D.npt * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int nc_restart_unpack(nc_handle* h, int32_t var, const void* host) {
+  if (!h || !host) return fail(NC_ERR_ARG, "nc_restart_unpack: null argument");
+  double* f;
+  TRY(restart_field(h, var, &f));
+  TRY(load_consts(h));
+  const Dims& D = h->D;
+  // no upload may still be using the staging buffer
+  CU(cudaStreamSynchronize(h->s_h2d));
+  CU(cudaStreamSynchronize(h->stream));
+  CU(cudaMemcpyAsync(h->stage, host, (size_t)D.npt * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  k_restart_swap<<<(unsigned)((D.npt + 255) / 256), 256, 0, h->stream>>>(
+      (unsigned long long*)f, (const unsigned long long*)h->stage, (int)D.npt);
+  TRY(check_launch(h, "restart_unpack"));
+  if (D.KA >= 3) {
+    k_restart_dummy<<<(unsigned)((D.npt2 + 255) / 256), 256, 0, h->stream>>>(f);
+    TRY(check_launch(h, "restart_dummy"));
+  }
+  CU(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int nc_restart_finish(nc_handle* h, const int64_t* pole_src, int32_t nsrc) {
+  if (!h || (nsrc > 0 && !pole_src) || nsrc < 0 || nsrc > 64) return fail(NC_ERR_ARG, "nc_restart_finish: bad argument");
+  TRY(load_consts(h));
+  const Dims& D = h->D;
+  PoleSrc ps{};
+  ps.n = nsrc;
+  for (int e = 0; e < nsrc; ++e) {
+    const int64_t* r = pole_src + 5 * e;
+    if (r[0] < 0 || r[0] >= 6 || r[1] < 0 || r[1] >= D.LP || r[2] < 0 || r[2] >= D.G || r[3] < 0 ||
+        r[3] >= D.G || r[4] < 0 || r[4] >= D.L)
+      return fail(NC_ERR_ARG, "nc_restart_finish: pole source entry out of range");
+    for (int c = 0; c < 5; ++c) ps.e[e][c] = (int)r[c];
+  }
+  VarPtrs reg{}, pol{};
+  const int nv = 6 + D.nq;
+  for (int v = 0; v < nv; ++v) {
+    reg.v[v] = v < 6 ? h->P[v].r : h->Pq[v - 6].r;
+    pol.v[v] = v < 6 ? h->P[v].p : h->Pq[v - 6].p;
+  }
+  if (nsrc > 0) {
+    k_pole_centre<<<(unsigned)((nsrc * D.KA + 127) / 128), 128, 0, h->stream>>>(reg, pol, nv, ps);
+    TRY(check_launch(h, "restart_pole_centre"));
+  }
+  TRY(comm_prg(h));
+  TRY(join_pl(h));
+  CU(cudaStreamSynchronize(h->stream));
+  h->have_state = true;
+  return 0;
 }
 
 int nc_history_vars(nc_handle* h, const int32_t* items, int32_t nitems, int64_t nstep, double dt,

@@ -32,7 +32,8 @@ _lib = None
 # every entry point declared in include/nicam_cuda.h
 EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_state_async", "nc_join_copies",
            "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",
-           "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_forcing_step", "nc_history_vars", "nc_divide_known",
+           "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_forcing_step", "nc_history_vars", "nc_restart_pack",
+           "nc_restart_unpack", "nc_restart_finish", "nc_divide_known",
            "nc_last_error", "nc_destroy")
 
 
@@ -74,6 +75,11 @@ def load_library(path: str = LIB_PATH):
     lib.nc_divide_known.argtypes = [dp, dp, dp, i64, ctypes.c_double]
     lib.nc_history_vars.argtypes = [vp, dp, i32, i64, ctypes.c_double, dp]
     lib.nc_history_vars.restype = ctypes.c_int
+    for f in ("nc_restart_pack", "nc_restart_unpack"):
+        getattr(lib, f).argtypes = [vp, i32, vp]
+        getattr(lib, f).restype = ctypes.c_int
+    lib.nc_restart_finish.argtypes = [vp, dp, i32]
+    lib.nc_restart_finish.restype = ctypes.c_int
     lib.nc_divide_known.restype = ctypes.c_int
     lib.nc_destroy.argtypes = [vp]
     lib.nc_destroy.restype = None
@@ -315,6 +321,24 @@ class NicamCuda:
         _check(self._lib.nc_history_vars(self._h, idarr.ctypes.data if ids else None, len(ids), int(nstep),
                                          float(dt), ptrs.ctypes.data if ids else None))
         return res
+
+    # ---- restart payloads (fio "ADVANCED" byte order; see restart.py)
+    def restart_pack(self, var: int, buf: np.ndarray):
+        """the big-endian file payload of prognostic ``var`` into ``buf``
+        (lall*kall*gall_1d^2 float64 slots)"""
+        if buf.nbytes != 8 * self.shape[0] * self.shape[1] * self.shape[2] * self.shape[3]:
+            raise ValueError("restart payload buffer has the wrong size")
+        _check(self._lib.nc_restart_pack(self._h, int(var), buf.ctypes.data))
+
+    def restart_unpack(self, var: int, buf: np.ndarray):
+        if buf.nbytes != 8 * self.shape[0] * self.shape[1] * self.shape[2] * self.shape[3]:
+            raise ValueError("restart payload has the wrong size")
+        buf = np.ascontiguousarray(buf)
+        _check(self._lib.nc_restart_unpack(self._h, int(var), buf.ctypes.data))
+
+    def restart_finish(self, pole_src):
+        ps = np.ascontiguousarray(pole_src, np.int64).reshape(-1, 5)
+        _check(self._lib.nc_restart_finish(self._h, ps.ctypes.data if len(ps) else None, len(ps)))
 
     def run_phases(self, nphases: int):
         """debugging: run the first ``nphases`` phases of one step"""

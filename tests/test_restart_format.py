@@ -1,0 +1,80 @@
+"""Restart files (fio "ADVANCED") against files the reference wrote itself
+(tests/golden/make_restart.py), on the CPU: the header bytes this package
+writes, the payload layout the device swaps into, and the read semantics the
+device follows (fio_read's dummy-level repair, COMM_var's pole-centre fill,
+then the halo exchange) restated with numpy and the oracle's exchange."""
+import gzip
+import importlib
+import os
+
+import numpy as np
+import pytest
+
+from oracle import nicam_step as O
+
+R = importlib.import_module("pynicam-dc_b200.restart")
+
+
+@pytest.fixture(scope="module")
+def rs(tmp_path_factory):
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "gl03_z10_restart.npz"))
+    d = tmp_path_factory.mktemp("restart")
+    files = {}
+    for k in ("write", "read"):
+        p = str(d / f"{k}.pe000000")
+        with open(p, "wb") as f:
+            f.write(gzip.decompress(z[f"{k}_file_gz"].tobytes()))
+        files[k] = p
+    return z, files
+
+
+def test_headers_match_reference(rs, golden):
+    z, files = rs
+    meta, items = R.parse(files["write"])
+    assert meta["header"] == "INITIAL/RESTART_data_of_prognostic_variables"
+    assert [it["varname"] for it in items] == list(z["names"])
+    with open(files["write"], "rb") as f:
+        b = f.read()
+    head = R.file_header(meta["header"], "", 0, 2, 0, int(z["glevel"]), int(z["rlevel"]), z["rgnid"])
+    assert b.startswith(head + len(items).to_bytes(4, "big"))
+    K = golden[1]["state1"].shape[2]
+    for it, nm, lb, un in zip(items, z["names"], z["labels"], z["units"]):
+        ih = R.item_header(str(nm), str(lb), str(un), str(z["layername"]), it["datasize"], R.F8, K, 1,
+                           int(z["ctime"]), int(z["ctime"]))
+        assert b[it["offset"] - len(ih):it["offset"]] == ih, nm
+
+
+def test_payload_is_device_layout_big_endian(rs, golden):
+    """each variable's data: the (l, k, j, i) array, big-endian float64"""
+    z, files = rs
+    _, st = golden
+    _, items = R.parse(files["write"])
+    with open(files["write"], "rb") as f:
+        b = f.read()
+    for v, it in enumerate(items):
+        want = np.ascontiguousarray(st["state1"][..., v].transpose(3, 2, 1, 0)).astype(">f8").tobytes()
+        assert b[it["offset"]:it["offset"] + it["datasize"]] == want, it["varname"]
+
+
+def test_read_semantics_vs_reference(rs, golden):
+    z, files = rs
+    geo, st = golden
+    g = O.Geo(geo)
+    _, items = R.parse(files["read"])
+    G, K, L = st["state1"].shape[0], st["state1"].shape[2], st["state1"].shape[3]
+    var = np.zeros(st["state1"].shape)
+    for v, it in enumerate(items):
+        a = np.fromfile(files["read"], dtype=">f8", count=it["datasize"] // 8, offset=it["offset"])
+        a = a.reshape(L, K, G, G).astype(np.float64)
+        for kd, ks in ((K - 1, K - 2), (0, 1)):
+            bad = ~np.isfinite(a[:, kd])
+            a[:, kd][bad] = a[:, ks][bad]
+        var[..., v] = a.transpose(3, 2, 1, 0)
+    assert not np.all(np.isfinite(np.fromfile(files["read"], dtype=">f8", count=items[1]["datasize"] // 8,
+                                              offset=items[1]["offset"])))
+    var_pl = np.full(st["state1_pl"].shape, np.nan)
+    for pg, pl, i, j, l in z["pole_src"]:
+        var_pl[pg, :, pl, :] = var[i, j, :, l, :]
+    O.comm(g, var, var_pl)
+    assert np.array_equal(var, z["read_state"])
+    assert np.array_equal(var_pl, z["read_state_pl"])
