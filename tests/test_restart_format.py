@@ -78,3 +78,21 @@ def test_read_semantics_vs_reference(rs, golden):
     O.comm(g, var, var_pl)
     assert np.array_equal(var, z["read_state"])
     assert np.array_equal(var_pl, z["read_state_pl"])
+
+
+def test_pole_centre_sources(rs, golden):
+    """backend.pole_centre_sources on the reference's copy lists with the rl01
+    region table (region ids = local indices on one process; regions 2 and 21
+    are the first whose north / south vertex is a pole, RGNMNG_rgn4pl,
+    share/mod_adm.py:267-278): the rows the reference's COMM_var used"""
+    from types import SimpleNamespace as NS
+    B = importlib.import_module("pynicam-dc_b200.backend")
+    z, _ = rs
+    geo, _ = golden
+    cl = np.asarray(geo["copy_p2r"])
+    L = int(np.asarray(geo["lall"]))
+    adm = NS(RGNMNG_lp2r=np.arange(L).reshape(L, 1), RGNMNG_rgn4pl=np.array([2, 21]), I_NPL=0, I_SPL=1)
+    comm = NS(Copy_list_p2r=cl, Copy_info_p2r=np.array([cl.shape[1], 0, 0]), I_size=0, I_prc_to=2,
+              I_gridi_from=0, I_gridj_from=1, I_l_from=2, I_gridi_to=3, I_gridj_to=4, I_l_to=5)
+    got = B.pole_centre_sources(NS(adm=adm, comm=comm))
+    assert np.array_equal(got, z["pole_src"])
