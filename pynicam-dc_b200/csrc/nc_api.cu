@@ -830,8 +830,12 @@ static int run_step(nc_handle* h) {
   }
   PHASE();
   for (int iq = 0; iq < D.nq; ++iq) {
-    k_trc_grad<<<greg, kBlock, 0, s>>>(h->Pq[iq].r, h->rhog_t.r, h->q.r,
-                                                                             h->gq[0].r, h->gq[1].r, h->gq[2].r);
+    {
+      const dim3 gt((unsigned)D.KA, (unsigned)(((D.G - 2 + TG_DX - 1) / TG_DX) * ((D.G - 2 + TG_DY - 1) / TG_DY)),
+                    (unsigned)D.L);
+      k_trc_grad_t<<<gt, TG_DX * TG_DY, 0, s>>>(h->Pq[iq].r, h->rhog_t.r, h->q.r, h->gq[0].r, h->gq[1].r,
+                                                h->gq[2].r);
+    }
     TRY(check_launch(h, "trc_grad"));
     k_trc_grad_pl<<<1, plk, 0, ps>>>(h->Pq[iq].p, h->rhog_t.p, h->q.p, h->gq[0].p, h->gq[1].p, h->gq[2].p);
     TRY(check_launch(h, "trc_grad_pl"));

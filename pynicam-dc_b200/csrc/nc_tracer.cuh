@@ -67,68 +67,68 @@ struct TrcVadvArgs {
   double dtl;
 };
 
+// One upward sweep with the values of levels k-1, k, k+1 in registers: at
+// level k the cell's outflow bounds are formed, the face value qh[k] is
+// limited with the bounds of cells k-1 and k, and cell k-1, whose two faces
+// are then final, is updated.  The same expressions as the three-pass form
+// of the reference (q, qh and ck on every level, the limiter, the update),
+// in the same order, so the same results.
 __device__ void trc_vadv_column(const Col c, const TrcVadvArgs& a) {
   const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
   const double BIG = cC.HUGE_, EPS = cC.EPS;
-  double q[NC_MAXK], qh[NC_MAXK], ck0[NC_MAXK], ck1[NC_MAXK];
-  for (int k = 0; k < KA; ++k) {
-    int p = c.at(k);
-    q[k] = a.rhogq[p] / a.den[p];
-  }
-  for (int k = 0; k < KA; ++k) {
-    if (k >= kmin && k <= kmax + 1) qh[k] = cC.afact[k] * q[k] + cC.bfact[k] * q[k - 1];
-    else qh[k] = 0.0;
-    if (k >= kmin && k <= kmax) {
-      int p = c.at(k);
-      ck0[k] = -a.flx_v[p] / a.den[p] * cC.rdgz[k];
-      ck1[k] = a.flx_v[c.at(k + 1)] / a.den[p] * cC.rdgz[k];
-    } else {
-      ck0[k] = 0.0;
-      ck1[k] = 0.0;
-    }
-  }
-  double qmin_prev = 0.0, qmax_prev = 0.0;
+  auto finish = [&](int k, double x) {   // clamp and store of one updated level
+    if (a.clamp && x > -1.0e-10 && x < 0.0) x = 0.0;
+    if (a.clamp) x = x + a.dtl * 0.0;
+    a.rhogq[c.at(k)] = x;
+  };
+  // q at kmin-1 and kmin, den and flx_v at kmin (read before the ghost levels are zeroed)
+  const int p = c.at(kmin);
+  double rq_m = a.rhogq[c.at(kmin - 1)], rq_k = a.rhogq[p];
+  double q_m = rq_m / a.den[c.at(kmin - 1)], q_k = rq_k / a.den[p];
+  double den_k = a.den[p], flx_k = a.flx_v[p];
+  double qmin_prev = 0.0, qmax_prev = 0.0, qh_prev = 0.0, rq_prev = 0.0, flx_prev = 0.0;
   for (int k = kmin; k <= kmax; ++k) {
-    int p = c.at(k);
-    double inL = 0.5 - copysign(0.5, ck0[k]);
-    double inU = 0.5 + copysign(0.5, ck0[k + 1]);
-    double qc = q[k], qb = q[k - 1], qa = q[k + 1];
-    double QminL = (inL == 1.0) ? npmin(qc, qb) : BIG;
-    double QminU = (inU == 1.0) ? npmin(qc, qa) : BIG;
-    double QmaxL = (inL == 1.0) ? npmax(qc, qb) : -BIG;
-    double QmaxU = (inU == 1.0) ? npmax(qc, qa) : -BIG;
-    double qnmin = npmin(npmin(QminL, QminU), qc);
-    double qnmax = npmax(npmax(QmaxL, QmaxU), qc);
-    double c1 = ck0[k], c2 = ck1[k];
-    double Cin = inL * c1 + inU * c2;
-    double Cout = (1.0 - inL) * c1 + (1.0 - inU) * c2;
-    double CQmin = inL * c1 * QminL + inU * c2 * QminU;
-    double CQmax = inL * c1 * QmaxL + inU * c2 * QmaxU;
-    double zsw = 0.5 - copysign(0.5, fabs(Cout) - EPS);
-    double dk = a.bcoef * a.frhog[p] / a.den[p] * a.dt;
-    double qomin = ((qc - qnmax) + qnmax * (Cin + Cout - dk) - CQmax) / (Cout + zsw) * (1.0 - zsw) + qc * zsw;
-    double qomax = ((qc - qnmin) + qnmin * (Cin + Cout - dk) - CQmin) / (Cout + zsw) * (1.0 - zsw) + qc * zsw;
-    if (k > kmin) {
-      double h = qh[k];
-      qh[k] = inL * npmin(npmax(h, qmin_prev), qmax_prev) + (1.0 - inL) * npmin(npmax(h, qomin), qomax);
-    }
+    const int pp = c.at(k + 1);
+    const double rq_p = a.rhogq[pp], den_p = a.den[pp], flx_p = a.flx_v[pp];
+    const double q_p = rq_p / den_p;
+    const double ck0 = -flx_k / den_k * cC.rdgz[k];
+    const double ck1 = flx_p / den_k * cC.rdgz[k];
+    const double ck0_p = (k + 1 <= kmax) ? -flx_p / den_p * cC.rdgz[k + 1] : 0.0;
+    const double qh_raw = cC.afact[k] * q_k + cC.bfact[k] * q_m;
+    const double inL = 0.5 - copysign(0.5, ck0);
+    const double inU = 0.5 + copysign(0.5, ck0_p);
+    const double qc = q_k, qb = q_m, qa = q_p;
+    const double QminL = (inL == 1.0) ? npmin(qc, qb) : BIG;
+    const double QminU = (inU == 1.0) ? npmin(qc, qa) : BIG;
+    const double QmaxL = (inL == 1.0) ? npmax(qc, qb) : -BIG;
+    const double QmaxU = (inU == 1.0) ? npmax(qc, qa) : -BIG;
+    const double qnmin = npmin(npmin(QminL, QminU), qc);
+    const double qnmax = npmax(npmax(QmaxL, QmaxU), qc);
+    const double c1 = ck0, c2 = ck1;
+    const double Cin = inL * c1 + inU * c2;
+    const double Cout = (1.0 - inL) * c1 + (1.0 - inU) * c2;
+    const double CQmin = inL * c1 * QminL + inU * c2 * QminU;
+    const double CQmax = inL * c1 * QmaxL + inU * c2 * QmaxU;
+    const double zsw = 0.5 - copysign(0.5, fabs(Cout) - EPS);
+    const double dk = a.bcoef * a.frhog[c.at(k)] / den_k * a.dt;
+    const double qomin = ((qc - qnmax) + qnmax * (Cin + Cout - dk) - CQmax) / (Cout + zsw) * (1.0 - zsw) + qc * zsw;
+    const double qomax = ((qc - qnmin) + qnmin * (Cin + Cout - dk) - CQmin) / (Cout + zsw) * (1.0 - zsw) + qc * zsw;
+    double qh = 0.0;   // the face at kmin stays zero
+    if (k > kmin)
+      qh = inL * npmin(npmax(qh_raw, qmin_prev), qmax_prev) + (1.0 - inL) * npmin(npmax(qh_raw, qomin), qomax);
+    if (k > kmin) finish(k - 1, rq_prev - (flx_k * qh - flx_prev * qh_prev) * cC.rdgz[k - 1]);
     qmin_prev = qomin;
     qmax_prev = qomax;
+    qh_prev = qh;
+    rq_prev = rq_k;
+    flx_prev = flx_k;
+    q_m = q_k; q_k = q_p; rq_k = rq_p;
+    den_k = den_p; flx_k = flx_p;
   }
-  qh[kmin] = 0.0;
-  qh[kmax + 1] = 0.0;
-  for (int k = 0; k < KA; ++k) {
-    int p = c.at(k);
-    double x;
-    if (k >= kmin && k <= kmax) {
-      x = a.rhogq[p] - (a.flx_v[c.at(k + 1)] * qh[k + 1] - a.flx_v[p] * qh[k]) * cC.rdgz[k];
-      if (a.clamp && x > -1.0e-10 && x < 0.0) x = 0.0;
-    } else {
-      x = 0.0;
-    }
-    if (a.clamp) x = x + a.dtl * 0.0;
-    a.rhogq[p] = x;
-  }
+  // cell kmax: its upper face (kmax+1) is zero
+  finish(kmax, rq_prev - (flx_k * 0.0 - flx_prev * qh_prev) * cC.rdgz[kmax]);
+  for (int k = 0; k < kmin; ++k) finish(k, 0.0);
+  for (int k = kmax + 1; k < KA; ++k) finish(k, 0.0);
 }
 
 __global__ void k_trc_vadv(TrcVadvArgs a, int pole) {
@@ -309,19 +309,54 @@ __global__ void k_trc_hflux_pl(TrcHfluxPlArgs a) {
 // ---------------------------------------------------------------------------
 // per tracer: q and its gradient (mod_src_tracer.py:758-771, 1634-1640)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 8) k_trc_grad(const double* rhogq, const double* rhog_t, double* q, double* gq0, double* gq1,
-                           double* gq2) {
-  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
-  int i, j, l;
-  if (col_of(t, i, j, l)) {
-    const bool in = interior(i, j);
-    for (int k = 0; k < cD.KA; ++k) {
-      int p = ix(i, j, k, l);
-      q[p] = rhogq[p] / rhog_t[p];
-      double g[3] = {0.0, 0.0, 0.0};
-      if (in) grad7(i, j, k, l, [&](int ii, int jj, int kk) { int qq = ix(ii, jj, kk, l); return rhogq[qq] / rhog_t[qq]; }, g);
-      gq0[p] = g[0]; gq1[p] = g[1]; gq2[p] = g[2];
+// One block per (level, 32 x 8 tile of interior cells): q of the haloed tile
+// is formed once into shared memory (one division per cell instead of one per
+// stencil use), then each cell's gradient is read from there.  The region's
+// halo cells get q and a zero gradient from the tile that holds their nearest
+// interior cell, so every cell is written once, as by the column form.
+#define TG_DX 32
+#define TG_DY 8
+__global__ void __launch_bounds__(TG_DX * TG_DY) k_trc_grad_t(const double* rhogq, const double* rhog_t, double* q,
+                                                              double* gq0, double* gq1, double* gq2) {
+  constexpr int PX = TG_DX + 2, PY = TG_DY + 2;
+  __shared__ double s_q[PY * PX];
+  const TileLv tl = tile_level<TG_DX, TG_DY>(0);
+  const int k = tl.k, l = tl.l, i0 = tl.i0, j0 = tl.j0;
+  const int G = cD.G, gmax = cD.G - 2;
+  const int tid = threadIdx.x;
+  for (int p = tid; p < PX * PY; p += blockDim.x) {
+    const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
+    double v = 0.0;
+    if (ii < G && jj < G) {
+      const int qq = ix(ii, jj, k, l);
+      v = rhogq[qq] / rhog_t[qq];
+      if (!interior(ii, jj)) {
+        const int ci = min(max(ii, 1), gmax), cj = min(max(jj, 1), gmax);
+        if (ci >= i0 && ci < i0 + TG_DX && cj >= j0 && cj < j0 + TG_DY) {
+          q[qq] = v;
+          gq0[qq] = 0.0;
+          gq1[qq] = 0.0;
+          gq2[qq] = 0.0;
+        }
+      }
     }
+    s_q[p] = v;
+  }
+  __syncthreads();
+  const int tx = tid % TG_DX, ty = tid / TG_DX;
+  const int i = i0 + tx, j = j0 + ty;
+  if (i > gmax || j > gmax) return;
+  const int qq = ix(i, j, k, l);
+  const int c0 = (ty + 1) * PX + (tx + 1);
+  const double s7[7] = {s_q[c0], s_q[c0 + 1], s_q[c0 + PX + 1], s_q[c0 + PX], s_q[c0 - 1], s_q[c0 - PX - 1], s_q[c0 - PX]};
+  q[qq] = s7[0];
+  double* gq[3] = {gq0, gq1, gq2};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {   // grad7 (kernels/oprtgradient.py:45-70)
+    double a = P2c(cG.coef_grad, d * 7 + 0, i, j, l) * s7[0];
+#pragma unroll
+    for (int m = 1; m < 7; ++m) a = a + P2c(cG.coef_grad, d * 7 + m, i, j, l) * s7[m];
+    gq[d][qq] = a;
   }
 }
 
