@@ -60,11 +60,15 @@ struct CommFields {
 
 __global__ void k_comm(CommFields f, const long long* r_dst, const long long* r_src, int nr, const long long* p_dst,
                        const long long* p_src, int np) {
+  // consecutive threads take consecutive entries of one level: the entries are
+  // sorted by destination, so a region's halo rows are read and written in
+  // contiguous runs
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long ne = (long long)(nr + np) * cD.KA;
+  const int nent = nr + np;
+  long long ne = (long long)nent * cD.KA;
   if (t >= ne) return;
-  int k = (int)(t % cD.KA);
-  int e = (int)(t / cD.KA);
+  int k = (int)(t / nent);
+  int e = (int)(t % nent);
   const long long pl = cD.plane;
   if (e < nr) {
     long long d = r_dst[e];
@@ -820,7 +824,10 @@ static int run_step(nc_handle* h) {
     for (int f = 0; f < 6; ++f) { ha.flx[f] = h->flx[f].r; ha.ch[f] = h->ch[f].r; ha.cm[f] = h->cm[f].r; }
     for (int f = 0; f < 9; ++f) ha.xc[f] = h->xc[f].r;
     ha.dt = dt;
-    k_trc_hflux<<<greg, kBlock, 0, s>>>(ha);
+    {
+      const dim3 gt((unsigned)D.KA, (unsigned)(((D.G + TH_DX - 1) / TH_DX) * ((D.G + TH_DY - 1) / TH_DY)), (unsigned)D.L);
+      k_trc_hflux_t<<<gt, TH_DX * TH_DY, 0, s>>>(ha);
+    }
     TRY(check_launch(h, "trc_hflux"));
     TrcHfluxPlArgs hp;
     hp.rho = h->PM[0].p; hp.rvx = h->PM[1].p; hp.rvy = h->PM[2].p; hp.rvz = h->PM[3].p; hp.rhog_t = h->rhog_t.p;

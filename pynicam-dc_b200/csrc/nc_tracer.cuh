@@ -154,39 +154,6 @@ struct TrcHfluxArgs {
   double dt;
 };
 
-// rho/rho*v at the two triangle vertices of cell (ii,jj): TI and TJ (4 fields),
-// before the singular-point fix
-__device__ void trc_vertex_raw(const TrcHfluxArgs& a, int ii, int jj, int k, int l, double TI[4], double TJ[4]) {
-  int q0 = ix(ii, jj, k, l), qi = ix(ii + 1, jj, k, l), qd = ix(ii + 1, jj + 1, k, l), qj = ix(ii, jj + 1, k, l);
-  double w1i = P2c(cG.GMTR_t, 0, ii, jj, l), w2i = P2c(cG.GMTR_t, 1, ii, jj, l), w3i = P2c(cG.GMTR_t, 2, ii, jj, l);
-  double w1j = P2c(cG.GMTR_t, 3, ii, jj, l), w2j = P2c(cG.GMTR_t, 4, ii, jj, l), w3j = P2c(cG.GMTR_t, 5, ii, jj, l);
-  auto F = [&](int n, int q) -> double {
-    if (n == 0) return a.rho[q];
-    const double* r = (n == 1) ? a.rvx : ((n == 2) ? a.rvy : a.rvz);
-    return r[q] * cG.RGAM[q];
-  };
-  for (int n = 0; n < 4; ++n) {
-    double f0 = F(n, q0), fi = F(n, qi), fd = F(n, qd), fj = F(n, qj);
-    double ti = f0 * w1i + fi * w2i;
-    ti = ti + fd * w3i;
-    double tj = f0 * w1j;
-    tj = tj + (fd * w2j + fj * w3j);
-    TI[n] = ti;
-    TJ[n] = tj;
-  }
-}
-
-// vertex values with the singular-point fix at (0,0) (mod_src_tracer.py:1409-1412)
-__device__ void trc_vertex(const TrcHfluxArgs& a, int ii, int jj, int k, int l, double TI[4], double TJ[4]) {
-  trc_vertex_raw(a, ii, jj, k, l, TI, TJ);
-  if (ii == 0 && jj == 0) {
-    double TI1[4], TJ1[4];
-    trc_vertex_raw(a, 1, 0, k, l, TI1, TJ1);
-    double m0 = (double)cG.pntmask[l * 2 + 0], m1 = (double)cG.pntmask[l * 2 + 1];
-    for (int n = 0; n < 4; ++n) TI[n] = TI[n] * m0 + TJ1[n] * m1;
-  }
-}
-
 // flux and centroid of face f of cell (ii,jj) given the summed vertex values
 __device__ __forceinline__ double trc_face(const TrcHfluxArgs& a, int ii, int jj, int l, int f, const double s[4],
                                            double xc[3]) {
@@ -197,68 +164,124 @@ __device__ __forceinline__ double trc_face(const TrcHfluxArgs& a, int ii, int jj
   return flux;
 }
 
-// face f in {0,1,2} of cell (ii,jj): returns false if the reference leaves it zero
-__device__ bool trc_face_flux(const TrcHfluxArgs& a, int ii, int jj, int k, int l, int f, double& flux, double xc[3]) {
-  const int G = cD.G;
-  double s[4];
-  if (f == 0) {
-    if (!(ii >= 0 && ii <= G - 2 && jj >= 1 && jj <= G - 2)) return false;
-    double TIa[4], TJa[4], TIb[4], TJb[4];
-    trc_vertex(a, ii, jj - 1, k, l, TIb, TJb);
-    trc_vertex(a, ii, jj, k, l, TIa, TJa);
-    for (int n = 0; n < 4; ++n) s[n] = TJb[n] + TIa[n];
-  } else if (f == 1) {
-    if (!(ii >= 0 && ii <= G - 2 && jj >= 0 && jj <= G - 2)) return false;
-    double TIa[4], TJa[4];
-    trc_vertex(a, ii, jj, k, l, TIa, TJa);
-    for (int n = 0; n < 4; ++n) s[n] = TIa[n] + TJa[n];
-  } else {
-    if (!(ii >= 1 && ii <= G - 2 && jj >= 0 && jj <= G - 2)) return false;
-    double TIa[4], TJa[4], TIb[4], TJb[4];
-    trc_vertex(a, ii, jj, k, l, TIa, TJa);
-    trc_vertex(a, ii - 1, jj, k, l, TIb, TJb);
-    for (int n = 0; n < 4; ++n) s[n] = TJa[n] + TIb[n];
+// One block per level and 32 x 8 tile of cells, the halo ring included (every
+// cell gets its six faces; a face the reference leaves out is zero): rho and
+// rho*v*RGAM of the haloed tile staged in shared memory, the triangle values
+// TI/TJ of every vertex the tile's faces use formed once
+// (mod_src_tracer.py:1390-1412, the singular-point fix at the (0,0) vertex
+// after them), then each cell's faces 0..2 and its neighbours' faces 0..2
+// (its faces 3..5, opposite sign) from those, with the face coefficients of
+// the face's owner cell (mod_src_tracer.py:1414-1484).
+#define TH_DX 32
+#define TH_DY 8
+__global__ void __launch_bounds__(TH_DX * TH_DY) k_trc_hflux_t(TrcHfluxArgs a) {
+  constexpr int PX = TH_DX + 2, PY = TH_DY + 2, TX = TH_DX + 1, TY = TH_DY + 1;
+  __shared__ double s_f[4][PY * PX];
+  __shared__ double s_ti[4][TY * TX], s_tj[4][TY * TX];
+  const int G = cD.G, k = (int)blockIdx.x, l = (int)blockIdx.z;
+  const int ntx = (G + TH_DX - 1) / TH_DX;
+  const int i0 = ((int)blockIdx.y % ntx) * TH_DX, j0 = ((int)blockIdx.y / ntx) * TH_DY;
+  const int tid = threadIdx.x;
+  for (int p = tid; p < PX * PY; p += blockDim.x) {
+    const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
+    double f0 = 0.0, f1 = 0.0, f2 = 0.0, f3 = 0.0;
+    if (ii >= 0 && jj >= 0 && ii < G && jj < G) {
+      const int q = ix(ii, jj, k, l);
+      const double rg = cG.RGAM[q];
+      f0 = a.rho[q];
+      f1 = a.rvx[q] * rg;
+      f2 = a.rvy[q] * rg;
+      f3 = a.rvz[q] * rg;
+    }
+    s_f[0][p] = f0; s_f[1][p] = f1; s_f[2][p] = f2; s_f[3][p] = f3;
   }
-  flux = trc_face(a, ii, jj, l, f, s, xc);
-  return true;
-}
-
-__global__ void k_trc_hflux(TrcHfluxArgs a) {
-  int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
-  int i, j, l;
-  if (!col_of(t, i, j, l)) return;
+  __syncthreads();
+  for (int p = tid; p < TX * TY; p += blockDim.x) {   // vertex values of (i0-1.., j0-1..)
+    const int px = p % TX, py = p / TX;
+    const int vi = i0 - 1 + px, vj = j0 - 1 + py;
+    const bool ok = vi >= 0 && vj >= 0 && vi <= G - 2 && vj <= G - 2;
+    double w1i = 0.0, w2i = 0.0, w3i = 0.0, w1j = 0.0, w2j = 0.0, w3j = 0.0;
+    if (ok) {
+      w1i = P2c(cG.GMTR_t, 0, vi, vj, l); w2i = P2c(cG.GMTR_t, 1, vi, vj, l); w3i = P2c(cG.GMTR_t, 2, vi, vj, l);
+      w1j = P2c(cG.GMTR_t, 3, vi, vj, l); w2j = P2c(cG.GMTR_t, 4, vi, vj, l); w3j = P2c(cG.GMTR_t, 5, vi, vj, l);
+    }
+    const int ia = py * PX + px, ib = ia + 1, ic = ia + PX + 1, id = ia + PX;
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      double ti = 0.0, tj = 0.0;
+      if (ok) {
+        const double f0 = s_f[n][ia], fi = s_f[n][ib], fd = s_f[n][ic], fj = s_f[n][id];
+        ti = f0 * w1i + fi * w2i;
+        ti = ti + fd * w3i;
+        tj = f0 * w1j;
+        tj = tj + (fd * w2j + fj * w3j);
+      }
+      s_ti[n][p] = ti;
+      s_tj[n][p] = tj;
+    }
+  }
+  __syncthreads();
+  if (i0 == 0 && j0 == 0 && tid < 4) {   // singular-point fix of vertex (0,0) (mod_src_tracer.py:1409-1412)
+    const int v00 = 1 * TX + 1, v10 = 1 * TX + 2;
+    const double m0 = (double)cG.pntmask[l * 2 + 0], m1 = (double)cG.pntmask[l * 2 + 1];
+    s_ti[tid][v00] = s_ti[tid][v00] * m0 + s_tj[tid][v10] * m1;
+  }
+  __syncthreads();
+  const int i = i0 + tid % TH_DX, j = j0 + tid / TH_DX;
+  if (i >= G || j >= G) return;
+  const int p = ix(i, j, k, l);
   const double dt = a.dt;
   const double PR = P2c(cG.GMTR_p, 0, i, j, l);
-  for (int k = 0; k < cD.KA; ++k) {
-    int p = ix(i, j, k, l);
-    double fl[6];
-    double xc[3];
-    for (int f = 0; f < 3; ++f) {
-      double flux;
-      if (trc_face_flux(a, i, j, k, l, f, flux, xc)) {
-        fl[f] = flux * PR * dt;
-        for (int d = 0; d < 3; ++d) a.xc[f * 3 + d][p] = xc[d];
-      } else {
-        fl[f] = 0.0;
-        for (int d = 0; d < 3; ++d) a.xc[f * 3 + d][p] = 0.0;
-      }
+  const int vc = (j - j0 + 1) * TX + (i - i0 + 1);   // vertex (i, j); (i-1, j) is vc-1, (i, j-1) vc-TX
+  // face f of the cell (ci, cj) from vertex sums TA + TB (trc_face_flux's three cases)
+  auto face = [&](int ci, int cj, int f, int va, bool a_is_j, int vb, bool b_is_j, double xc[3]) {
+    double sv[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+      const double A = a_is_j ? s_tj[n][va] : s_ti[n][va];
+      const double B = b_is_j ? s_tj[n][vb] : s_ti[n][vb];
+      sv[n] = A + B;
     }
-    // edges 3..5 are the opposite sides of the neighbours' edges 0..2
-    const int nbI[3] = {-1, -1, 0}, nbJ[3] = {0, -1, -1};
-    for (int f = 0; f < 3; ++f) {
-      double flux;
-      double xcn[3];
-      if (trc_face_flux(a, i + nbI[f], j + nbJ[f], k, l, f, flux, xcn)) fl[3 + f] = -flux * PR * dt;
-      else fl[3 + f] = 0.0;
-    }
-    if (i == 1 && j == 1) fl[5] *= (double)cG.pntmask[l * 2 + 0];
-    const Recip rg = recip_of(a.rhog_t[p]);   // six quotients by rhog_t
-    for (int f = 0; f < 6; ++f) {
-      a.flx[f][p] = fl[f];
-      double chv = div_by(fl[f], rg);
-      a.ch[f][p] = chv;
-      a.cm[f][p] = 0.5 - copysign(0.5, chv - cC.EPS);
-    }
+    return trc_face(a, ci, cj, l, f, sv, xc);
+  };
+  double fl[6], xc[3];
+  // face 0: TJ(i, j-1) + TI(i, j)
+  if (i >= 0 && i <= G - 2 && j >= 1 && j <= G - 2) {
+    fl[0] = face(i, j, 0, vc - TX, true, vc, false, xc) * PR * dt;
+  } else {
+    fl[0] = 0.0; xc[0] = xc[1] = xc[2] = 0.0;
+  }
+  for (int d = 0; d < 3; ++d) a.xc[0 * 3 + d][p] = xc[d];
+  // face 1: TI(i, j) + TJ(i, j)
+  if (i >= 0 && i <= G - 2 && j >= 0 && j <= G - 2) {
+    fl[1] = face(i, j, 1, vc, false, vc, true, xc) * PR * dt;
+  } else {
+    fl[1] = 0.0; xc[0] = xc[1] = xc[2] = 0.0;
+  }
+  for (int d = 0; d < 3; ++d) a.xc[1 * 3 + d][p] = xc[d];
+  // face 2: TJ(i, j) + TI(i-1, j)
+  if (i >= 1 && i <= G - 2 && j >= 0 && j <= G - 2) {
+    fl[2] = face(i, j, 2, vc, true, vc - 1, false, xc) * PR * dt;
+  } else {
+    fl[2] = 0.0; xc[0] = xc[1] = xc[2] = 0.0;
+  }
+  for (int d = 0; d < 3; ++d) a.xc[2 * 3 + d][p] = xc[d];
+  // faces 3..5: the neighbours' faces 0..2, opposite sign
+  double xcn[3];
+  fl[3] = (i - 1 >= 0 && i - 1 <= G - 2 && j >= 1 && j <= G - 2)
+              ? -face(i - 1, j, 0, vc - 1 - TX, true, vc - 1, false, xcn) * PR * dt : 0.0;
+  fl[4] = (i - 1 >= 0 && i - 1 <= G - 2 && j - 1 >= 0 && j - 1 <= G - 2)
+              ? -face(i - 1, j - 1, 1, vc - 1 - TX, false, vc - 1 - TX, true, xcn) * PR * dt : 0.0;
+  fl[5] = (i >= 1 && i <= G - 2 && j - 1 >= 0 && j - 1 <= G - 2)
+              ? -face(i, j - 1, 2, vc - TX, true, vc - TX - 1, false, xcn) * PR * dt : 0.0;
+  if (i == 1 && j == 1) fl[5] *= (double)cG.pntmask[l * 2 + 0];
+  const Recip rg = recip_of(a.rhog_t[p]);   // six quotients by rhog_t
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    a.flx[f][p] = fl[f];
+    const double chv = div_by(fl[f], rg);
+    a.ch[f][p] = chv;
+    a.cm[f][p] = 0.5 - copysign(0.5, chv - cC.EPS);
   }
 }
 
