@@ -1301,7 +1301,14 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   h->mass_blocks = (int)((D.npt2 + D.LP + 255) / 256);
   TRY(dev_alloc(h, &h->mass_part, (size_t)h->mass_blocks * 2));
   CU(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-  CU(cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking));
+  {
+    // the pole stream at the highest priority: its one-block kernels are
+    // dispatched as soon as an SM has room instead of after the regional
+    // kernel's remaining blocks, so they finish under the regional work
+    int least = 0, greatest = 0;
+    CU(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    CU(cudaStreamCreateWithPriority(&h->stream2, cudaStreamNonBlocking, greatest));
+  }
   CU(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
   CU(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
   CU(cudaStreamCreateWithFlags(&h->s_h2d, cudaStreamNonBlocking));
@@ -1452,7 +1459,7 @@ int nc_step(nc_handle* h, int32_t nsteps) {
     }
     if (ec != cudaSuccess) return fail(NC_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
     h->graph = g;
-    CU(cudaGraphInstantiate(&h->gexec, h->graph, 0));
+    CU(cudaGraphInstantiate(&h->gexec, h->graph, cudaGraphInstantiateFlagUseNodePriority));
     h->launches = before;
     h->graph_kernels = 0;
     {
