@@ -1118,6 +1118,14 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   TRY(up_reg(h, T, "OPRT_coef_grad", 1, 21, &Gm.coef_grad));
   TRY(up_reg(h, T, "OPRT_coef_lap", 1, 7, &Gm.coef_lap));
   TRY(up_reg(h, T, "OPRT_coef_intp", 1, 18, &Gm.coef_intp));
+  {
+    double* w;
+    TRY(dev_alloc(h, &w, (size_t)18 * D.npt2));
+    k_intp_weights<<<(unsigned)((D.npt2 + 255) / 256), 256>>>(Gm.coef_intp, w, (int)D.npt2);
+    CU(cudaGetLastError());
+    CU(cudaDeviceSynchronize());
+    Gm.intp_w = w;
+  }
   TRY(up_reg(h, T, "OPRT_coef_diff", 1, 18, &Gm.coef_diff));
   TRY(up_reg(h, T, "GRD_x", 1, 3, &Gm.GRD_x));
   TRY(up_reg(h, T, "GRD_xr", 1, 9, &Gm.GRD_xr));

@@ -65,6 +65,7 @@ struct Geom {
   const double *coef_grad;  // 21 planes
   const double *coef_lap;   // 7
   const double *coef_intp;  // 18 planes ((d*3+p)*2+t)
+  const double *intp_w;     // 18 planes ((d*3+m)*2+t): the diffusion's vertex weights formed from coef_intp
   const double *coef_diff;  // 18 planes (d*6+m)
   const double *GRD_x;      // 3
   const double *GRD_xr;     // 9 (face*3+d)

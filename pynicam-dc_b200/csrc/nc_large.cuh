@@ -485,61 +485,22 @@ __global__ void k_hdiff1_pl(Six src, SixOut out) {
   }
 }
 
-// kh-weighted diffusion at one interior point (kernels/oprtdiffusion.py:59-134)
-// KH(ii,jj) returns the diffusion coefficient field at (ii,jj,k).
-template <class S, class KH>
-__device__ double diffusion_at(int i, int j, int k, int l, S scl, KH kh) {
-  // vertex values tTI/tTJ at (ii,jj) for the three directions
-  auto tvert = [&](int ii, int jj, double tti[3], double ttj[3]) {
-    double s0 = scl(ii, jj), sip = scl(ii + 1, jj), sd = scl(ii + 1, jj + 1), sjp = scl(ii, jj + 1);
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      double c1i = P2(cG.coef_intp, (d * 3 + 0) * 2 + 0, ii, jj, l);
-      double c2i = P2(cG.coef_intp, (d * 3 + 1) * 2 + 0, ii, jj, l);
-      double c3i = P2(cG.coef_intp, (d * 3 + 2) * 2 + 0, ii, jj, l);
-      double c1j = P2(cG.coef_intp, (d * 3 + 0) * 2 + 1, ii, jj, l);
-      double c2j = P2(cG.coef_intp, (d * 3 + 1) * 2 + 1, ii, jj, l);
-      double c3j = P2(cG.coef_intp, (d * 3 + 2) * 2 + 1, ii, jj, l);
-      tti[d] = div3((2.0 * c1i - c2i - c3i) * s0 + (-c1i + 2.0 * c2i - c3i) * sip + (-c1i - c2i + 2.0 * c3i) * sd);
-      ttj[d] = div3((2.0 * c1j - c2j - c3j) * s0 + (-c1j + 2.0 * c2j - c3j) * sd + (-c1j - c2j + 2.0 * c3j) * sjp);
+// The three vertex weights of each triangle of the Kh-weighted diffusion,
+// formed once from the interpolation coefficients with the reference's
+// expressions (kernels/oprtdiffusion.py:59-90): for direction d and triangle
+// t (i or j), 2*c1 - c2 - c3, -c1 + 2*c2 - c3 and -c1 - c2 + 2*c3 of
+// coef_intp[d][0..2][t].  Planes [((d*3+m)*2+t)][l][j][i].
+__global__ void k_intp_weights(const double* ci, double* w, int npt2) {
+  const int q = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (q >= npt2) return;
+  for (int d = 0; d < 3; ++d)
+    for (int t = 0; t < 2; ++t) {
+      const double c1 = ci[((d * 3 + 0) * 2 + t) * npt2 + q], c2 = ci[((d * 3 + 1) * 2 + t) * npt2 + q];
+      const double c3 = ci[((d * 3 + 2) * 2 + t) * npt2 + q];
+      w[((d * 3 + 0) * 2 + t) * npt2 + q] = 2.0 * c1 - c2 - c3;
+      w[((d * 3 + 1) * 2 + t) * npt2 + q] = -c1 + 2.0 * c2 - c3;
+      w[((d * 3 + 2) * 2 + t) * npt2 + q] = -c1 - c2 + 2.0 * c3;
     }
-    if (ii == 0 && jj == 0) {  // singular-point fix (kernels/oprtdiffusion.py:91-96)
-      double m0 = (double)cG.pntmask[l * 2 + 0], m1 = (double)cG.pntmask[l * 2 + 1];
-      double s0b = scl(1, 0), sipb = scl(2, 0), sdb = scl(2, 1), sjpb = scl(1, 1);
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        double c1j = P2(cG.coef_intp, (d * 3 + 0) * 2 + 1, 1, 0, l);
-        double c2j = P2(cG.coef_intp, (d * 3 + 1) * 2 + 1, 1, 0, l);
-        double c3j = P2(cG.coef_intp, (d * 3 + 2) * 2 + 1, 1, 0, l);
-        double tj10 = div3((2.0 * c1j - c2j - c3j) * s0b + (-c1j + 2.0 * c2j - c3j) * sdb + (-c1j - c2j + 2.0 * c3j) * sjpb);
-        (void)sipb;
-        tti[d] = tti[d] * m0 + tj10 * m1;
-      }
-    }
-  };
-  double aTI[3], aTJ[3], bTI[3], bTJ[3], cTI[3], cTJ[3], dTI[3], dTJ[3];
-  tvert(i, j, aTI, aTJ);
-  tvert(i - 1, j, bTI, bTJ);
-  tvert(i - 1, j - 1, cTI, cTJ);
-  tvert(i, j - 1, dTI, dTJ);
-  double kh0 = kh(i, j);
-  double kf1 = 0.5 * (kh0 + kh(i + 1, j + 1));
-  double kf2 = 0.5 * (kh0 + kh(i, j + 1));
-  double kf3 = 0.5 * (kh0 + kh(i - 1, j));
-  double kf4 = 0.5 * (kh0 + kh(i - 1, j - 1));
-  double kf5 = 0.5 * (kh0 + kh(i, j - 1));
-  double kf6 = 0.5 * (kh0 + kh(i + 1, j));
-  double inner = 0.0;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    double cd0 = P2(cG.coef_diff, d * 6 + 0, i, j, l), cd1 = P2(cG.coef_diff, d * 6 + 1, i, j, l),
-           cd2 = P2(cG.coef_diff, d * 6 + 2, i, j, l), cd3 = P2(cG.coef_diff, d * 6 + 3, i, j, l),
-           cd4 = P2(cG.coef_diff, d * 6 + 4, i, j, l), cd5 = P2(cG.coef_diff, d * 6 + 5, i, j, l);
-    double blk = kf1 * cd0 * (aTI[d] + aTJ[d]) + kf2 * cd1 * (aTJ[d] + bTI[d]) + kf3 * cd2 * (bTI[d] + cTJ[d]) +
-                 kf4 * cd3 * (cTJ[d] + cTI[d]) + kf5 * cd4 * (cTI[d] + dTJ[d]) + kf6 * cd5 * (dTJ[d] + aTI[d]);
-    inner = (d == 0) ? blk : inner + blk;
-  }
-  return inner;
 }
 
 // Second hyperdiffusion pass, one block per (level, HD_DX x HD_DY tile) of
@@ -589,14 +550,15 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, 4) k_hdiff2_l(Six vt, const dou
         for (int d = 0; d < 3; ++d) {
           double ti = 0.0, tj = 0.0;
           if (ok) {
-            const double c1i = P2(cG.coef_intp, (d * 3 + 0) * 2 + 0, ii, jj, l);
-            const double c2i = P2(cG.coef_intp, (d * 3 + 1) * 2 + 0, ii, jj, l);
-            const double c3i = P2(cG.coef_intp, (d * 3 + 2) * 2 + 0, ii, jj, l);
-            const double c1j = P2(cG.coef_intp, (d * 3 + 0) * 2 + 1, ii, jj, l);
-            const double c2j = P2(cG.coef_intp, (d * 3 + 1) * 2 + 1, ii, jj, l);
-            const double c3j = P2(cG.coef_intp, (d * 3 + 2) * 2 + 1, ii, jj, l);
-            ti = div3((2.0 * c1i - c2i - c3i) * s0 + (-c1i + 2.0 * c2i - c3i) * sip + (-c1i - c2i + 2.0 * c3i) * sd);
-            tj = div3((2.0 * c1j - c2j - c3j) * s0 + (-c1j + 2.0 * c2j - c3j) * sd + (-c1j - c2j + 2.0 * c3j) * sjp);
+            // weights 2c1-c2-c3, -c1+2c2-c3, -c1-c2+2c3 of the i and j triangles (k_intp_weights)
+            const double w1i = P2(cG.intp_w, (d * 3 + 0) * 2 + 0, ii, jj, l);
+            const double w2i = P2(cG.intp_w, (d * 3 + 1) * 2 + 0, ii, jj, l);
+            const double w3i = P2(cG.intp_w, (d * 3 + 2) * 2 + 0, ii, jj, l);
+            const double w1j = P2(cG.intp_w, (d * 3 + 0) * 2 + 1, ii, jj, l);
+            const double w2j = P2(cG.intp_w, (d * 3 + 1) * 2 + 1, ii, jj, l);
+            const double w3j = P2(cG.intp_w, (d * 3 + 2) * 2 + 1, ii, jj, l);
+            ti = div3(w1i * s0 + w2i * sip + w3i * sd);
+            tj = div3(w1j * s0 + w2j * sd + w3j * sjp);
           }
           s_t[f][d][p] = ti;
           s_t[f][3 + d][p] = tj;

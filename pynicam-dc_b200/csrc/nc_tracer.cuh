@@ -84,12 +84,12 @@ __device__ void trc_vadv_column(const Col c, const TrcVadvArgs& a) {
   // q at kmin-1 and kmin, den and flx_v at kmin (read before the ghost levels are zeroed)
   const int p = c.at(kmin);
   double rq_m = a.rhogq[c.at(kmin - 1)], rq_k = a.rhogq[p];
-  double q_m = rq_m / a.den[c.at(kmin - 1)], q_k = rq_k / a.den[p];
-  double den_k = a.den[p], flx_k = a.flx_v[p];
+  double q_m = rq_m / __ldg(&a.den[c.at(kmin - 1)]), q_k = rq_k / __ldg(&a.den[p]);
+  double den_k = __ldg(&a.den[p]), flx_k = __ldg(&a.flx_v[p]);
   double qmin_prev = 0.0, qmax_prev = 0.0, qh_prev = 0.0, rq_prev = 0.0, flx_prev = 0.0;
   for (int k = kmin; k <= kmax; ++k) {
     const int pp = c.at(k + 1);
-    const double rq_p = a.rhogq[pp], den_p = a.den[pp], flx_p = a.flx_v[pp];
+    const double rq_p = a.rhogq[pp], den_p = __ldg(&a.den[pp]), flx_p = __ldg(&a.flx_v[pp]);
     const double q_p = rq_p / den_p;
     const double ck0 = -flx_k / den_k * cC.rdgz[k];
     const double ck1 = flx_p / den_k * cC.rdgz[k];
@@ -110,7 +110,7 @@ __device__ void trc_vadv_column(const Col c, const TrcVadvArgs& a) {
     const double CQmin = inL * c1 * QminL + inU * c2 * QminU;
     const double CQmax = inL * c1 * QmaxL + inU * c2 * QmaxU;
     const double zsw = 0.5 - copysign(0.5, fabs(Cout) - EPS);
-    const double dk = a.bcoef * a.frhog[c.at(k)] / den_k * a.dt;
+    const double dk = a.bcoef * __ldg(&a.frhog[c.at(k)]) / den_k * a.dt;
     const double qomin = ((qc - qnmax) + qnmax * (Cin + Cout - dk) - CQmax) / (Cout + zsw) * (1.0 - zsw) + qc * zsw;
     const double qomax = ((qc - qnmin) + qnmin * (Cin + Cout - dk) - CQmin) / (Cout + zsw) * (1.0 - zsw) + qc * zsw;
     double qh = 0.0;   // the face at kmin stays zero
