@@ -4,8 +4,8 @@ against the oracle.
 
 The forcing's T_eq uses log and pow, which CUDA and numpy may round
 differently in the last bit, so these comparisons use a tolerance: relative
-L2 per prognostic <= 1e-12 after each forced step (the north star's one-step
-tolerance) and <= 1e-14 for the forcing alone."""
+L2 per prognostic <= 1e-12 after each forced step (the one-step
+parity tolerance) and <= 1e-14 for the forcing alone."""
 import numpy as np
 import pytest
 

@@ -9,7 +9,7 @@ bit.  The potential temperatures, the saturation ratios and the pressure-level
 slices go through pow, exp and log, which CUDA and numpy may round differently
 in the last bit, and the per-layer mean of th_prime and the column water sum
 add in another order: those are compared to a relative max-norm of 1e-12 (the
-north star's one-step tolerance)."""
+one-step parity tolerance of the step itself)."""
 import numpy as np
 import pytest
 
