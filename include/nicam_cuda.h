@@ -217,8 +217,9 @@ int nc_restart_finish(nc_handle* h, const int64_t* pole_src, int32_t nsrc);
  *   8 ml_rho, 9 ml_hgt, 10 ml_mse, 11 ml_rh, 12 ml_rha, 13 ml_rhi, 14 ml_du,
  *   15 ml_dv, 16 ml_dw, 17 ml_dtem, 18 ml_dq, 19 ml_ucos, 20 ml_vcos,
  *   21 ml_th_prime                      -> (gall_1d, gall_1d, kall, lall)
- *   22 sl_ps, 23 sl_pw, 24 sl_lwp, 25 sl_iwp, then 26.. 41 sl_u850, sl_v850,
- *   sl_w850, sl_t850, the same at 500, 250 and 100 hPa -> (gall_1d, gall_1d, lall)
+ *   22 sl_ps, 23 sl_pw, 24 sl_lwp, 25 sl_iwp, 26 sl_u850, 27 sl_v850,
+ *   28 sl_w850, 29 sl_t850, then ids 30-41 the same four at 500, 250 and
+ *   100 hPa                             -> (gall_1d, gall_1d, lall)
  * (the reference's I/O order, share/mod_io.py:251-260).  The tendencies ml_d*
  * are stateful as in the reference: the first output of each is zero, later
  * ones (previous - current) * 86400 / dt / (nstep - nstep of the last output

@@ -35,3 +35,16 @@ def test_create_without_gpu_fails_loudly(pkg, golden):
     geo, _ = golden
     with pytest.raises(pkg.NicamError):
         pkg.NicamCuda(geo)
+
+
+def test_history_item_ids_match_header(pkg):
+    """the binding's history item order is the id list nc_history_vars documents"""
+    import re
+    hdr = open(os.path.join(ROOT, "include", "nicam_cuda.h")).read()
+    doc = hdr[hdr.index("int nc_history_vars") - 2500:hdr.index("int nc_history_vars")]
+    ids = {int(n): name for n, name in re.findall(r"\b(\d+) ((?:ml|sl)_\w+)", doc)}
+    items = pkg.runtime.HIST_ITEMS
+    for n, name in ids.items():
+        assert items[n] == name, (n, name)
+    assert len(items) == 42 and items[26:30] == ("sl_u850", "sl_v850", "sl_w850", "sl_t850")
+    assert items[-4:] == ("sl_u100", "sl_v100", "sl_w100", "sl_t100")
