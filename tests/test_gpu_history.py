@@ -100,3 +100,14 @@ def test_history_step_api_through_backend(pkg, golden, golden_hist):
     msc.io._diag_names_2d = ["sl_cl"]
     with pytest.raises(NotImplementedError):
         dyn.history_vars_step(msc)
+
+
+def test_history_needs_its_setup(pkg, golden):
+    """a handle created without the HIST_* entries refuses, with a status"""
+    geo, st = golden
+    c = pkg.NicamCuda(geo)
+    c.upload(st["state0"], st["state0_pl"])
+    with pytest.raises(pkg.NicamError):
+        c.history_vars(("ml_u",), nstep=0, dt=1200.0)
+    with pytest.raises(NotImplementedError):
+        c.history_vars(("sl_cl",), nstep=0, dt=1200.0)

@@ -80,3 +80,17 @@ def test_missing_variable_is_an_error(pkg, golden, rs):
     pkg.restart.read(core, files["read"], names[:6] + ["rhogqx"], z["pole_src"], allow_missingq=True)
     got, _ = core.download()
     assert not np.any(got[..., 6])
+
+
+def test_restart_argument_checks(pkg, golden):
+    """no state to write, a variable index outside the state, a payload of the
+    wrong size: refused before any device work"""
+    geo, st = golden
+    core = pkg.NicamCuda(geo)
+    n = int(np.prod(st["state0"].shape[:4]))
+    with pytest.raises(pkg.NicamError):
+        core.restart_pack(0, np.empty(n, np.uint64))
+    with pytest.raises(pkg.NicamError):
+        core.restart_unpack(99, np.zeros(n, np.uint64))
+    with pytest.raises(ValueError):
+        core.restart_unpack(0, np.zeros(n - 1, np.uint64))
