@@ -238,13 +238,13 @@ int nc_history_vars(nc_handle* h, const int32_t* items, int32_t nitems, int64_t 
 
 /* Self-check of the divisions the kernels use in place of a general division
  * (the reference divides with numpy's IEEE division, e.g.
- * kernels/horizontalizevec.py:51-54, kernels/oprtdiffusion.py,
- * kernels/virhowsolver.py): a quotient formed from RN(1/b) and a tail with
- * three fused multiply-adds and a multiply.  With y NULL every x[i] is divided
- * by the constant b (reciprocal pair set on the host, as for rscale, 3 and
- * CVdry); otherwise x[i] is divided by y[i] with the pair formed on the device
- * from the correctly rounded reciprocal (as for the density that several
- * diagnostics divide by).  Copies the n host doubles in, writes q, copies it
+ * kernels/horizontalizevec.py:51-54, kernels/oprtdiffusion.py, kernels/diag.py,
+ * mod_src_tracer.py): a quotient formed from RN(1/b) and a tail with three
+ * fused multiply-adds and a multiply.  With y NULL every x[i] is divided by the
+ * constant b (reciprocal pair set on the host, as for rscale and 3); otherwise
+ * x[i] is divided by y[i] with the pair formed on the device from the
+ * correctly rounded reciprocal (as for the density that the diagnostics and
+ * the tracer Courant numbers divide by).  Copies the n host doubles in, writes q, copies it
  * back (synchronous).  For finite operands with a normal-range quotient the
  * bits equal the IEEE quotient; the tests compare them.  0 <= n <= 2^28; with
  * y NULL, b finite and nonzero; else NC_ERR_ARG. */

@@ -1069,8 +1069,6 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   if (!(C.rscale != 0.0 && std::isfinite(C.rscale))) return fail(NC_ERR_ARG, "rscale must be finite and nonzero");
   recip_pair(C.rscale, C.rsc_h, C.rsc_l);
   recip_pair(3.0, C.third_h, C.third_l);
-  if (!(C.CVdry != 0.0 && std::isfinite(C.CVdry))) return fail(NC_ERR_ARG, "CVdry must be finite and nonzero");
-  recip_pair(C.CVdry, C.cvd_h, C.cvd_l);
   TRY(scalar(T, "dtl", h->dtl)); TRY(scalar(T, "dts", h->dts));
   {
     const nc_array* cvw = T.get("CVW");

@@ -45,8 +45,8 @@ struct Consts {
   double Kh, divdamp_coef, hdiff_fact_rho, CVW0, PRE00;
   int gam_unit;   // RGAM, RGAMH and GAM2H are 1 everywhere (shallow atmosphere)
   // rounded reciprocals and their tails, RN(1/b) and RN(1/b - RN(1/b)), of the
-  // divisors rscale, 3 and CVdry (see div_by)
-  double rsc_h, rsc_l, third_h, third_l, cvd_h, cvd_l;
+  // divisors rscale and 3 (see div_by)
+  double rsc_h, rsc_l, third_h, third_l;
   double afact[NC_MAXK], bfact[NC_MAXK], cfact[NC_MAXK], dfact[NC_MAXK];
   double rdgz[NC_MAXK], rdgzh[NC_MAXK];
 };
@@ -121,10 +121,9 @@ __device__ __forceinline__ double div_by(double x, double b, double bh, double b
   const double q = __fma_rn(r, bh, q0);
   return (x == 0.0) ? __dmul_rn(x, bh) : q;
 }
-// x / rscale, x / 3.0 and x / CVdry
+// x / rscale and x / 3.0
 __device__ __forceinline__ double div_r(double x) { return div_by(x, cC.rscale, cC.rsc_h, cC.rsc_l); }
 __device__ __forceinline__ double div3(double x) { return div_by(x, 3.0, cC.third_h, cC.third_l); }
-__device__ __forceinline__ double div_cvd(double x) { return div_by(x, cC.CVdry, cC.cvd_h, cC.cvd_l); }
 
 // The same division for a divisor computed at run time that several quotients
 // share: bh = RN(1/b) from the correctly rounded reciprocal __drcp_rn, and the
@@ -154,14 +153,6 @@ __device__ __forceinline__ int ix2(int c, int i, int j, int l) {
 }
 // pole (g, k, l)
 __device__ __forceinline__ int ipl(int g, int k, int lp) { return (g * cD.KA + k) * cD.LP + lp; }
-// pole (g, k, l, c) with nc comps
-__device__ __forceinline__ int iplc(int g, int k, int lp, int c, int ncomp) {
-  return ((g * cD.KA + k) * cD.LP + lp) * ncomp + c;
-}
-// 3-D metric component c of a multi-component regional metric
-__device__ __forceinline__ double M3(const double* a, int c, int i, int j, int k, int l) {
-  return a[c * cD.npti + ix(i, j, k, l)];
-}
 __device__ __forceinline__ double P2(const double* a, int c, int i, int j, int l) { return a[ix2(c, i, j, l)]; }
 // the same through the read-only (non-coherent) path: the planes are constant
 // after set-up, and the compiler may batch these loads ahead of shared-memory
@@ -188,8 +179,5 @@ __device__ __forceinline__ bool col_of(int t, int& i, int& j, int& l) {
   l = (int)(r / cD.G);
   return true;
 }
-
-__device__ __forceinline__ double dmin(double a, double b) { return fmin(a, b); }
-__device__ __forceinline__ double dmax(double a, double b) { return fmax(a, b); }
 
 }  // namespace nc

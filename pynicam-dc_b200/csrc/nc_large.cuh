@@ -236,33 +236,6 @@ struct AdvMomArgs {
   double *gvx, *gvy, *gvz, *gw;               // out
 };
 
-// regional: flux convergence of the scaled fluxes rhogv*scl at level k
-template <class SCL>
-__device__ __forceinline__ double advconv_reg(int i, int j, int k, int l, const Col& c, const Met& m,
-                                              const double* rvx, const double* rvy, const double* rvz,
-                                              const double* rw, SCL scl) {
-  double div = 0.0;
-  if (interior(i, j)) {
-    div = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) -> double {
-      int q = ix(ii, jj, kk, l);
-      const double* rv = (d == 0) ? rvx : ((d == 1) ? rvy : rvz);
-      return (rv[q] * scl(q, kk)) * gam_at(cG.RGAM, q);
-    });
-  }
-  auto vmh = [&](int kk) -> double {
-    if (kk <= cD.kmin || kk > cD.kmax) return 0.0;
-    double h = vmh_horiz(c, m, kk, [&](int k2, int d) -> double {
-      int q = c.at(k2);
-      const double* rv = (d == 0) ? rvx : ((d == 1) ? rvy : rvz);
-      return rv[q] * scl(q, k2);
-    });
-    int q = c.at(kk);
-    double sw = rw[q] * (cC.afact[kk] * scl(q, kk) + cC.bfact[kk] * scl(c.at(kk - 1), kk - 1));
-    return h + 1.0 * sw * m.RGSQRTH[q];
-  };
-  return -div - (vmh(k + 1) - vmh(k)) * cC.rdgz[k];
-}
-
 // Tiled momentum advection for interior cells: one block per 32x8 tile of a
 // region, marching upward over kmin..kmax (the vertical-momentum tendency at k
 // needs the projection at k-1, and the half-level flux at k is reused from the
