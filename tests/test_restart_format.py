@@ -96,3 +96,45 @@ def test_pole_centre_sources(rs, golden):
               I_gridi_from=0, I_gridj_from=1, I_l_from=2, I_gridi_to=3, I_gridj_to=4, I_l_to=5)
     got = B.pole_centre_sources(NS(adm=adm, comm=comm))
     assert np.array_equal(got, z["pole_src"])
+
+
+class _FakeCore:
+    """records what restart.read hands to the device (host logic only)"""
+
+    def __init__(self, shape):
+        self.shape = shape
+        self.unpacked, self.finished = {}, None
+
+    def restart_unpack(self, var, buf):
+        self.unpacked[var] = np.array(buf, copy=True)
+
+    def restart_finish(self, pole_src):
+        self.finished = np.asarray(pole_src)
+
+
+def test_read_host_logic(rs, golden):
+    """restart.read without a device: each named variable's payload goes to its
+    device index unchanged (big-endian bytes, swapped on the device), a missing
+    tracer is zero only when allowed, and COMM_var gets the pole sources"""
+    z, files = rs
+    _, st = golden
+    names = [str(n) for n in z["names"]]
+    core = _FakeCore(st["state1"].shape)
+    R.read(core, files["write"], names, z["pole_src"])
+    _, items = R.parse(files["write"])
+    for v, it in enumerate(items):
+        raw = np.fromfile(files["write"], dtype=np.uint64, count=it["datasize"] // 8, offset=it["offset"])
+        assert np.array_equal(core.unpacked[v], raw), names[v]
+    assert np.array_equal(core.finished, z["pole_src"])
+    with pytest.raises(KeyError):
+        R.read(_FakeCore(st["state1"].shape), files["write"], names[:6] + ["rhogqx"], z["pole_src"])
+    c2 = _FakeCore(st["state1"].shape)
+    R.read(c2, files["write"], names[:6] + ["rhogqx"], z["pole_src"], allow_missingq=True)
+    assert not np.any(c2.unpacked[6])
+    with pytest.raises(KeyError):   # a missing prognostic is never zero-filled
+        R.read(_FakeCore(st["state1"].shape), files["write"], ["rhogx"] + names[1:], z["pole_src"],
+               allow_missingq=True)
+    bad = list(st["state1"].shape)
+    bad[2] += 1
+    with pytest.raises(ValueError):   # payload size does not match the device grid
+        R.read(_FakeCore(tuple(bad)), files["write"], names, z["pole_src"])
