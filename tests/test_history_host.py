@@ -1,0 +1,57 @@
+"""Host logic of CudaDyn.history_vars_step (mirror of the reference's
+Dyn.history_vars_step, pynicamdc/nhm/dynamics/mod_dynamics.py:737-772): which
+names are formed for the I/O groups being written, and what reaches the
+device call; a recording stand-in replaces the device core."""
+from types import SimpleNamespace as NS
+
+import pytest
+
+
+class _Core:
+    def __init__(self):
+        self.calls = []
+
+    def history_vars(self, names, nstep, dt):
+        self.calls.append((tuple(names), nstep, dt))
+        return {n: None for n in names}
+
+
+def _dyn(pkg):
+    d = object.__new__(pkg.backend.CudaDyn)
+    d.core, d._device_valid, d._host_stale, d._forced = _Core(), True, True, False
+    return d
+
+
+def _msc(io=None):
+    m = NS(tim=NS(TIME_cstep=7, TIME_dtl=150.0))
+    if io is not None:
+        m.io = io
+    return m
+
+
+def test_names_follow_the_io_groups(pkg):
+    d = _dyn(pkg)
+    io = NS(_diag_names=["ml_th", "ml_u"], _diag_names_2d=["sl_ps"])
+    assert sorted(d.history_vars_step(_msc(io))) == ["ml_th", "ml_u", "sl_ps"]
+    assert sorted(d.history_vars_step(_msc(io), write_2d=False)) == ["ml_th", "ml_u"]
+    assert sorted(d.history_vars_step(_msc(io), write_3d=False)) == ["sl_ps"]
+    names, nstep, dt = d.core.calls[0]
+    assert names == ("ml_u", "ml_th", "sl_ps") and nstep == 7 and dt == 150.0   # the device's id order
+
+
+def test_without_io_every_item(pkg):
+    d = _dyn(pkg)
+    out = d.history_vars_step(_msc())
+    assert tuple(out) == pkg.runtime.HIST_ITEMS
+
+
+def test_empty_groups_form_nothing(pkg):
+    d = _dyn(pkg)
+    assert d.history_vars_step(_msc(NS(_diag_names=[], _diag_names_2d=[]))) == {}
+
+
+def test_unknown_names_raise(pkg):
+    d = _dyn(pkg)
+    with pytest.raises(NotImplementedError):
+        d.history_vars_step(_msc(NS(_diag_names=["ml_u"], _diag_names_2d=["sl_cly"])))
+    assert d.core.calls == []
