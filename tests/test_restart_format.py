@@ -138,3 +138,42 @@ def test_read_host_logic(rs, golden):
     bad[2] += 1
     with pytest.raises(ValueError):   # payload size does not match the device grid
         R.read(_FakeCore(tuple(bad)), files["write"], names, z["pole_src"])
+
+
+class _PackCore:
+    """hands restart.write the payload the device's byte swap produces for a
+    state: (l, k, j, i) big-endian"""
+
+    def __init__(self, state):
+        self.shape = state.shape
+        self.state = state
+
+    def restart_pack(self, var, buf):
+        be = np.ascontiguousarray(self.state[..., var].transpose(3, 2, 1, 0)).astype(">f8")
+        buf[:] = be.reshape(-1).view(np.uint64)
+
+
+def test_writer_host_logic_matches_reference_file(rs, golden, tmp_path):
+    """restart.write with the device payload emulated: the whole file equals the
+    one the reference's restart_output wrote, byte for byte; and through
+    CudaDyn.restart_output with the reference's own item list"""
+    z, files = rs
+    _, st = golden
+    items = [(str(n), str(lb), str(u), v) for v, (n, lb, u) in enumerate(zip(z["names"], z["labels"], z["units"]))]
+    out = str(tmp_path / "w.pe000000")
+    R.write(_PackCore(st["state1"]), out, items, str(z["layername"]), z["rgnid"], int(z["glevel"]),
+            int(z["rlevel"]), int(z["ctime"]))
+    with open(out, "rb") as f, open(files["write"], "rb") as g:
+        assert f.read() == g.read()
+    from types import SimpleNamespace as NS
+    B = importlib.import_module("pynicam-dc_b200.backend")
+    d = object.__new__(B.CudaDyn)
+    d.core, d._device_valid, d._host_stale, d._forced = _PackCore(st["state1"]), True, True, False
+    L = len(z["rgnid"])
+    prgv = NS(output_io_mode="ADVANCED", output_diagnostics=False, layername=str(z["layername"]),
+              _restart_output_items=lambda rcnf: [(n, lb, u, None, v) for (n, lb, u, v) in items])
+    msc = NS(prgv=prgv, rcnf=None, adm=NS(RGNMNG_lp2r=np.asarray(z["rgnid"]).reshape(L, 1), ADM_prc_me=0,
+                                          ADM_lall=L, ADM_glevel=int(z["glevel"]), ADM_rlevel=int(z["rlevel"])))
+    d.restart_output(msc, str(tmp_path / "d.pe"), ctime=int(z["ctime"]))
+    with open(str(tmp_path / "d.pe000000"), "rb") as f, open(files["write"], "rb") as g:
+        assert f.read() == g.read()
