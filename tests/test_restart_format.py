@@ -177,3 +177,31 @@ def test_writer_host_logic_matches_reference_file(rs, golden, tmp_path):
     d.restart_output(msc, str(tmp_path / "d.pe"), ctime=int(z["ctime"]))
     with open(str(tmp_path / "d.pe000000"), "rb") as f, open(files["write"], "rb") as g:
         assert f.read() == g.read()
+
+
+def test_restart_input_host_logic(rs, golden):
+    """CudaDyn.restart_input: the reference's variable names (PRG_name, then
+    'rhog' + TRC_name), the <basename>000000 file, the pole-centre sources from
+    the copy lists; the device state is then the handle's and the host copy stale"""
+    from types import SimpleNamespace as NS
+    B = importlib.import_module("pynicam-dc_b200.backend")
+    z, files = rs
+    geo, st = golden
+    d = object.__new__(B.CudaDyn)
+    d.core, d._device_valid, d._host_stale, d._forced = _FakeCore(st["state1"].shape), False, False, False
+    cl = np.asarray(geo["copy_p2r"])
+    L = int(np.asarray(geo["lall"]))
+    names = [str(n) for n in z["names"]]
+    msc = NS(prgv=NS(input_io_mode="ADVANCED", input_diagnostics=False, allow_missingq=False,
+                     restart_input_basename=files["read"][:-6]),
+             rcnf=NS(PRG_name=names[:6], PRG_vmax0=6, TRC_name=["qv"], TRC_vmax=1),
+             adm=NS(RGNMNG_lp2r=np.arange(L).reshape(L, 1), RGNMNG_rgn4pl=np.array([2, 21]), I_NPL=0, I_SPL=1),
+             comm=NS(Copy_list_p2r=cl, Copy_info_p2r=np.array([cl.shape[1], 0, 0]), I_size=0, I_prc_to=2,
+                     I_gridi_from=0, I_gridj_from=1, I_l_from=2, I_gridi_to=3, I_gridj_to=4, I_l_to=5))
+    d.restart_input(msc)
+    assert sorted(d.core.unpacked) == list(range(7))
+    assert np.array_equal(d.core.finished, z["pole_src"])
+    assert d._device_valid and d._host_stale
+    msc.prgv.input_io_mode = "npz"
+    with pytest.raises(NotImplementedError):
+        d.restart_input(msc)
