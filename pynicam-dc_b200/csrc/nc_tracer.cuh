@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(TH_DX * TH_DY) k_trc_hflux_t(TrcHfluxArgs a) {
   const double dt = a.dt;
   const double PR = P2c(cG.GMTR_p, 0, i, j, l);
   const int vc = (j - j0 + 1) * TX + (i - i0 + 1);   // vertex (i, j); (i-1, j) is vc-1, (i, j-1) vc-TX
-  // face f of the cell (ci, cj) from vertex sums TA + TB (trc_face_flux's three cases)
+  // face f of the cell (ci, cj) from the vertex sums TA + TB (mod_src_tracer.py:1414-1484)
   auto face = [&](int ci, int cj, int f, int va, bool a_is_j, int vb, bool b_is_j, double xc[3]) {
     double sv[4];
 #pragma unroll
@@ -336,7 +336,7 @@ __global__ void k_trc_hflux_pl(TrcHfluxPlArgs a) {
 // is formed once into shared memory (one division per cell instead of one per
 // stencil use), then each cell's gradient is read from there.  The region's
 // halo cells get q and a zero gradient from the tile that holds their nearest
-// interior cell, so every cell is written once, as by the column form.
+// interior cell, so every cell is written exactly once.
 #define TG_DX 32
 #define TG_DY 8
 __global__ void __launch_bounds__(TG_DX * TG_DY) k_trc_grad_t(const double* rhogq, const double* rhog_t, double* q,
