@@ -55,3 +55,25 @@ def test_unknown_names_raise(pkg):
     with pytest.raises(NotImplementedError):
         d.history_vars_step(_msc(NS(_diag_names=["ml_u"], _diag_names_2d=["sl_cly"])))
     assert d.core.calls == []
+
+
+def test_setup_table_history_entries(pkg, golden, golden_hist):
+    """the HIST_* entries nc_create reads: shapes, cos(lat) with numpy's cos,
+    constants and tracer indices in the header's order, PRE00 alongside"""
+    import numpy as np
+    from conftest import hist_geo
+    geo, _ = golden
+    hg, _ = golden_hist
+    t = pkg.runtime.setup_table(hist_geo(geo, hg))
+    G, K, L = (int(np.asarray(geo[k])) for k in ("gall_1d", "kall", "lall"))
+    assert t["HIST_hgt"].shape == (G, G, K, L)
+    for k in ("HIST_coslat", "HIST_zsfc", "HIST_area"):
+        assert t[k].shape == (G, G, 1, L), k
+    assert t["HIST_IJ"].shape == (G, G, 1, L, 6)
+    assert np.array_equal(t["HIST_coslat"][:, :, 0, :], np.cos(hg["GRD_LAT"]))
+    assert t["HIST_consts"].tolist() == [float(hg[k]) for k in ("LHV", "UNDEF", "PSAT0", "RTEM00", "CPovR_liq",
+                                                                 "CPovR_ice", "LovR_liq", "LovR_ice",
+                                                                 "SAT_LLIMIT", "SAT_ULIMIT")]
+    assert t["HIST_tracers"].dtype == np.int64 and t["HIST_tracers"].tolist()[0] == int(hg["I_QV"])
+    assert float(t["PRE00"]) == float(np.asarray(geo["PRE00"]))
+    assert "HIST_hgt" not in pkg.runtime.setup_table(geo)
