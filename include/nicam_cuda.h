@@ -65,8 +65,32 @@ int nc_upload_state(nc_handle* h, const double* prg, const double* prg_pl);
 
 /* Marshal-out (Dyn.sync_prgvar_to_host, mod_dynamics.py:429-440) into host
  * memory in the same layout, after every step queued before the call;
- * returns when the host arrays hold the state. */
+ * returns when the host arrays hold the state.  The copy also checks every
+ * value: if the state holds a NaN or infinity the arrays are still filled and
+ * the call returns NC_ERR_NONFINITE, naming the lowest such variable index
+ * (the reference has no such check; its nearest is the opt-in device checksum
+ * of pynicamdc/api.py:878-900). */
 int nc_download_state(nc_handle* h, double* prg, double* prg_pl);
+
+/* Device-memory marshal for a PyTorch (or any CUDA) host: the same layouts as
+ * nc_upload_state / nc_download_state, but prg and prg_pl are device pointers
+ * (e.g. torch.float64 CUDA tensors of shapes (gall_1d, gall_1d, kall, lall,
+ * 6+nq) and (6, kall, 2, 6+nq), contiguous), and the work is ordered against
+ * the caller's `stream` (a cudaStream_t; NULL for the legacy default stream):
+ * it starts after what is queued on `stream` and what is queued on `stream`
+ * afterwards follows it.  Replaces the host drain of Dyn.sync_prgvar_to_host
+ * (mod_dynamics.py:429-440) and the marshal-in of mod_dynamics.py:1876-1880
+ * when the state lives in device tensors.  No finiteness status (use
+ * nc_check_finite). */
+int nc_upload_state_device(nc_handle* h, const double* prg, const double* prg_pl, void* stream);
+int nc_download_state_device(nc_handle* h, double* prg, double* prg_pl, void* stream);
+
+/* Finiteness of the device state (every prognostic and tracer, halo and
+ * ghost levels included): 0, or NC_ERR_NONFINITE naming the lowest variable
+ * index that holds a NaN or infinity.  Waits for the steps queued before it.
+ * The reference's counterpart is its opt-in device checksum
+ * (pynicamdc/api.py:878-900, PYNICAM_DEV_CHECKSUM). */
+int nc_check_finite(nc_handle* h);
 
 /* nc_download_state without the wait: the copy runs on the handle's download
  * stream, overlapping the steps queued after this call (into pinned host
@@ -146,8 +170,8 @@ int nc_grid_spring(int32_t lall, int32_t gall_1d, double* x, double* x_pl, const
 /* Allocation-free air or tracer mass sum.  No counterpart in the reference.
  * For callers that may not call cudaMalloc: code that runs inside another
  * framework's memory manager (a caching allocator that owns the device memory,
- * an XLA/JAX custom call) or on a stream that is being captured, where a new
- * allocation either fails, is forbidden or would break the capture.  Creating
+ * an XLA/JAX custom call), where a new allocation either fails or is
+ * forbidden.  Creating
  * a handle (nc_create) allocates, so this entry point takes no handle: the
  * caller passes its own device arrays in the library's device layout --
  * regional (lall, kall, gall_1d, gall_1d) C-order, pole (6, kall, 2) -- and a
@@ -156,6 +180,7 @@ int nc_grid_spring(int32_t lall, int32_t gall_1d, double* x, double* x_pl, const
  * interior cells and the two pole points, levels kmin..kmax, of
  * num / gsgam2 * volume with num = rhogq if given, else rhog: the same
  * compensated sum, in the same order, as nc_mass_sums.
+ * kall must be the leading level extent of the caller's arrays (4..128).
  * Limit: lall * gall_1d^2 + 2 <= 1,048,576 columns (grid level 8 at rlevel 1
  * uses 676,002); larger grids get NC_ERR_ARG.  The block partial sums live in
  * one fixed 64 KiB device array that every GPU loading the library keeps
@@ -163,9 +188,10 @@ int nc_grid_spring(int32_t lall, int32_t gall_1d, double* x, double* x_pl, const
  * state needs clearing between calls, but calls that run concurrently on the
  * GPU (different streams, overlapping) race on it and must be serialized by
  * the caller.  The first call on each device looks up that array's device
- * address (cudaGetSymbolAddress) with the device current; make that first
- * call before any stream capture.  Asynchronous: read out after the stream
- * is synchronized. */
+ * address (cudaGetSymbolAddress) with the device current and keeps it for
+ * the life of the process (the device's primary context must not be reset
+ * meanwhile); make that first call before any stream capture.  Asynchronous:
+ * read out after the stream is synchronized. */
 int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* gsgam2, const double* volume,
                         const double* rhog_pl, const double* rhogq_pl, const double* gsgam2_pl,
                         const double* volume_pl, int32_t gall_1d, int32_t lall, int32_t kall, int32_t kmin,

@@ -6,6 +6,6 @@ hand-written sm_100a CUDA kernels in ``libnicamcuda.so`` behind a C ABI
 (include/nicam_cuda.h), with the reference's prognostic layout, region/halo
 conventions and step API kept on the host side.
 """
-from .runtime import NicamCuda, NicamError, load_library, setup_table, LIB_PATH, EXPORTS  # noqa: F401
+from .runtime import NicamCuda, NicamError, NonFiniteStateError, load_library, setup_table, LIB_PATH, EXPORTS  # noqa: F401
 from .backend import CudaDyn  # noqa: F401
 from . import halo, restart  # noqa: F401

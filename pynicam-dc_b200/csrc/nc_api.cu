@@ -131,7 +131,15 @@ __global__ void __launch_bounds__(256) k_unpack_t(const double* st, VarPtrs reg,
   }
 }
 
-__global__ void __launch_bounds__(256) k_pack_t(double* st, VarPtrs reg, int nv) {
+// The pack also looks at every value it moves: the lowest variable index
+// holding a non-finite value goes to *bad (atomicMin; the caller presets it to
+// a value above every index), so a download reports a non-finite state
+// without another pass over the fields.
+__device__ __forceinline__ void note_nonfinite(int* bad, double x, int v) {
+  if (!isfinite(x)) atomicMin(bad, v);
+}
+
+__global__ void __launch_bounds__(256) k_pack_t(double* st, VarPtrs reg, int nv, int* bad) {
   __shared__ double tile[UI][UC + 1];
   const int G = cD.G, KA = cD.KA, L = cD.L;
   const int i0 = (int)blockIdx.x * UI, c0 = (int)blockIdx.y * UC;
@@ -142,7 +150,9 @@ __global__ void __launch_bounds__(256) k_pack_t(double* st, VarPtrs reg, int nv)
     const int i = i0 + ii, c = c0 + cc;
     if (i < G && c < ncl) {
       const int l = c / nv, v = c % nv;
-      tile[ii][cc] = reg.v[v][((l * KA + k) * G + j) * G + i];
+      const double x = reg.v[v][((l * KA + k) * G + j) * G + i];
+      note_nonfinite(bad, x, v);
+      tile[ii][cc] = x;
     }
   }
   __syncthreads();
@@ -195,10 +205,28 @@ __global__ void k_unpack_pl(const double* st_pl, VarPtrs pol, int nv) {
   if (q >= cD.npl) return;
   for (int v = 0; v < nv; ++v) pol.v[v][q] = st_pl[(long long)q * nv + v];
 }
-__global__ void k_pack_pl(double* st_pl, VarPtrs pol, int nv) {
+__global__ void k_pack_pl(double* st_pl, VarPtrs pol, int nv, int* bad) {
   const int q = (int)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= cD.npl) return;
-  for (int v = 0; v < nv; ++v) st_pl[(long long)q * nv + v] = pol.v[v][q];
+  for (int v = 0; v < nv; ++v) {
+    const double x = pol.v[v][q];
+    note_nonfinite(bad, x, v);
+    st_pl[(long long)q * nv + v] = x;
+  }
+}
+
+// finiteness of the prognostic state: the lowest variable index with a
+// non-finite value (regional fields with their halo and ghost levels, then the
+// pole fields) into *bad, preset to a value above every index
+__global__ void k_finite(VarPtrs reg, VarPtrs pol, int nv, int* bad) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int stride = (int)(gridDim.x * blockDim.x);
+  for (int v = 0; v < nv; ++v) {
+    bool ok = true;
+    for (int p = t; p < cD.npti; p += stride) ok = ok && isfinite(reg.v[v][p]);
+    for (int p = t; p < cD.npl; p += stride) ok = ok && isfinite(pol.v[v][p]);
+    if (!ok) atomicMin(bad, v);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -256,6 +284,9 @@ struct FieldPair {
   double* p = nullptr;
 };
 
+// "no non-finite value seen": every byte 0x7f, above any variable index
+#define NC_BAD_NONE 0x7f7f7f7f
+
 struct nc_handle {
   Dims D{};
   Consts C{};
@@ -277,6 +308,10 @@ struct nc_handle {
   double *stage = nullptr, *stage_pl = nullptr;
   double* mass_part = nullptr;
   int mass_blocks = 0;
+  // non-finite detection: device slot (lowest variable index seen, NC_BAD_NONE
+  // if none) and its pinned host copy, written by the downloads' pack kernels
+  int* bad = nullptr;
+  int* bad_host = nullptr;
   double* vol = nullptr;
   double* vol_pl = nullptr;
   long long launches = 0;
@@ -317,6 +352,7 @@ struct nc_handle {
   // download stages through its own buffer
   cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
   cudaEvent_t ev_in_ready = nullptr, ev_in_free = nullptr, ev_out_ready = nullptr, ev_out_done = nullptr;
+  cudaEvent_t ev_user = nullptr;   // ordering against a caller's stream (device-pointer marshal)
   double *stage_out = nullptr, *stage_out_pl = nullptr;
   // per-kernel timing (opt-in, eager launches only): an event after every
   // launch; a kernel's time is the gap to the previous event on the stream
@@ -973,7 +1009,10 @@ __global__ void k_mass_noalloc_fold(const double* part, int nblocks, double* out
   out[0] = S + Cc;
 }
 
-// device address of g_mass_scratch, looked up once per device
+// device address of g_mass_scratch, looked up once per device ordinal and kept
+// for the life of the process: this assumes the device's primary context is
+// never reset (cudaDeviceReset) while the library is loaded, since a reset
+// context would give the array a new address
 static std::mutex g_scratch_mu;
 static std::map<int, double*> g_scratch_addr;
 
@@ -1306,6 +1345,10 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   TRY(dev_alloc(h, &h->stage_out_pl, (size_t)D.npl * (6 + D.nq)));
   h->mass_blocks = (int)((D.npt2 + D.LP + 255) / 256);
   TRY(dev_alloc(h, &h->mass_part, (size_t)h->mass_blocks * 2));
+  CU(cudaMalloc((void**)&h->bad, sizeof(int)));
+  h->allocs.push_back(h->bad);
+  CU(cudaHostAlloc((void**)&h->bad_host, sizeof(int), cudaHostAllocDefault));
+  *h->bad_host = NC_BAD_NONE;
   CU(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   {
     // the pole stream at the highest priority: its one-block kernels are
@@ -1319,7 +1362,7 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   CU(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
   CU(cudaStreamCreateWithFlags(&h->s_h2d, cudaStreamNonBlocking));
   CU(cudaStreamCreateWithFlags(&h->s_d2h, cudaStreamNonBlocking));
-  for (cudaEvent_t* e : {&h->ev_in_ready, &h->ev_in_free, &h->ev_out_ready, &h->ev_out_done})
+  for (cudaEvent_t* e : {&h->ev_in_ready, &h->ev_in_free, &h->ev_out_ready, &h->ev_out_done, &h->ev_user})
     CU(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   return 0;
 }
@@ -1348,10 +1391,11 @@ void nc_destroy(nc_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   for (void* p : h->allocs) cudaFree(p);
+  if (h->bad_host) cudaFreeHost(h->bad_host);
   if (h->stream2) cudaStreamSynchronize(h->stream2);
   for (cudaStream_t st : {h->s_h2d, h->s_d2h})
     if (st) cudaStreamSynchronize(st);
-  for (cudaEvent_t e : {h->ev_in_ready, h->ev_in_free, h->ev_out_ready, h->ev_out_done})
+  for (cudaEvent_t e : {h->ev_in_ready, h->ev_in_free, h->ev_out_ready, h->ev_out_done, h->ev_user})
     if (e) cudaEventDestroy(e);
   for (cudaStream_t st : {h->s_h2d, h->s_d2h})
     if (st) cudaStreamDestroy(st);
@@ -1394,22 +1438,39 @@ int nc_upload_state(nc_handle* h, const double* prg, const double* prg_pl) {
 
 // pack the state into the download staging buffer on the library stream and
 // copy it out on the download stream
+static int reset_bad(nc_handle* h, cudaStream_t st) {
+  CU(cudaMemsetAsync(h->bad, 0x7f, sizeof(int), st));
+  return 0;
+}
+
 static int download_issue(nc_handle* h, double* prg, double* prg_pl) {
   const Dims& D = h->D;
   const int nv = 6 + D.nq;
   CU(cudaStreamWaitEvent(h->stream, h->ev_out_done, 0));   // the previous download has left the buffer
   const dim3 gt((unsigned)((D.G + UI - 1) / UI), (unsigned)((D.L * nv + UC - 1) / UC), (unsigned)(D.G * D.KA));
-  k_pack_t<<<gt, 256, 0, h->stream>>>(h->stage_out, state_ptrs(h, false), nv);
+  TRY(reset_bad(h, h->stream));
+  k_pack_t<<<gt, 256, 0, h->stream>>>(h->stage_out, state_ptrs(h, false), nv, h->bad);
   TRY(check_launch(h, "pack"));
-  k_pack_pl<<<(unsigned)((D.npl + 127) / 128), 128, 0, h->stream>>>(h->stage_out_pl, state_ptrs(h, true), nv);
+  k_pack_pl<<<(unsigned)((D.npl + 127) / 128), 128, 0, h->stream>>>(h->stage_out_pl, state_ptrs(h, true), nv,
+                                                                    h->bad);
   TRY(check_launch(h, "pack_pl"));
   CU(cudaEventRecord(h->ev_out_ready, h->stream));
   CU(cudaStreamWaitEvent(h->s_d2h, h->ev_out_ready, 0));
   CU(cudaMemcpyAsync(prg, h->stage_out, (size_t)D.npt * nv * sizeof(double), cudaMemcpyDeviceToHost, h->s_d2h));
   CU(cudaMemcpyAsync(prg_pl, h->stage_out_pl, (size_t)D.npl * nv * sizeof(double), cudaMemcpyDeviceToHost,
                      h->s_d2h));
+  CU(cudaMemcpyAsync(h->bad_host, h->bad, sizeof(int), cudaMemcpyDeviceToHost, h->s_d2h));
   CU(cudaEventRecord(h->ev_out_done, h->s_d2h));
   return 0;
+}
+
+// NC_ERR_NONFINITE naming the lowest variable index the last finiteness check
+// or download saw non-finite (the caller has synchronized with it)
+static int bad_status(nc_handle* h, const char* what) {
+  const int v = *h->bad_host;
+  if (v == NC_BAD_NONE) return 0;
+  return fail(NC_ERR_NONFINITE, std::string(what) + ": non-finite value in prognostic variable " + std::to_string(v) +
+                                    " (0-5 RHOG..RHOGE, 6.. tracers)");
 }
 
 int nc_download_state(nc_handle* h, double* prg, double* prg_pl) {
@@ -1418,7 +1479,66 @@ int nc_download_state(nc_handle* h, double* prg, double* prg_pl) {
   TRY(load_consts(h));
   TRY(download_issue(h, prg, prg_pl));
   CU(cudaEventSynchronize(h->ev_out_done));
+  return bad_status(h, "nc_download_state");
+}
+
+int nc_check_finite(nc_handle* h) {
+  if (!h) return fail(NC_ERR_ARG, "nc_check_finite: null handle");
+  if (!h->have_state) return fail(NC_ERR_STATE, "nc_check_finite: no state uploaded");
+  TRY(load_consts(h));
+  const int nv = 6 + h->D.nq;
+  TRY(reset_bad(h, h->stream));
+  k_finite<<<4 * 148, 256, 0, h->stream>>>(state_ptrs(h, false), state_ptrs(h, true), nv, h->bad);
+  TRY(check_launch(h, "finite"));
+  CU(cudaMemcpyAsync(h->bad_host, h->bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return bad_status(h, "nc_check_finite");
+}
+
+// the library stream waits for the work queued so far on the caller's stream
+// (cudaStream_t; NULL is the legacy default stream)
+static int after_caller(nc_handle* h, void* stream) {
+  CU(cudaEventRecord(h->ev_user, (cudaStream_t)stream));
+  CU(cudaStreamWaitEvent(h->stream, h->ev_user, 0));
   return 0;
+}
+// ... and the caller's stream waits for the library stream
+static int before_caller(nc_handle* h, void* stream) {
+  CU(cudaEventRecord(h->ev_user, h->stream));
+  CU(cudaStreamWaitEvent((cudaStream_t)stream, h->ev_user, 0));
+  return 0;
+}
+
+int nc_upload_state_device(nc_handle* h, const double* prg, const double* prg_pl, void* stream) {
+  if (!h || !prg || !prg_pl) return fail(NC_ERR_ARG, "nc_upload_state_device: null argument");
+  TRY(load_consts(h));
+  const Dims& D = h->D;
+  const int nv = 6 + D.nq;
+  TRY(after_caller(h, stream));
+  const dim3 gt((unsigned)((D.G + UI - 1) / UI), (unsigned)((D.L * nv + UC - 1) / UC), (unsigned)(D.G * D.KA));
+  k_unpack_t<<<gt, 256, 0, h->stream>>>(prg, state_ptrs(h, false), nv);
+  TRY(check_launch(h, "unpack"));
+  k_unpack_pl<<<(unsigned)((D.npl + 127) / 128), 128, 0, h->stream>>>(prg_pl, state_ptrs(h, true), nv);
+  TRY(check_launch(h, "unpack_pl"));
+  TRY(before_caller(h, stream));
+  h->have_state = true;
+  return 0;
+}
+
+int nc_download_state_device(nc_handle* h, double* prg, double* prg_pl, void* stream) {
+  if (!h || !prg || !prg_pl) return fail(NC_ERR_ARG, "nc_download_state_device: null argument");
+  if (!h->have_state) return fail(NC_ERR_STATE, "nc_download_state_device: no state uploaded");
+  TRY(load_consts(h));
+  const Dims& D = h->D;
+  const int nv = 6 + D.nq;
+  TRY(after_caller(h, stream));
+  TRY(reset_bad(h, h->stream));
+  const dim3 gt((unsigned)((D.G + UI - 1) / UI), (unsigned)((D.L * nv + UC - 1) / UC), (unsigned)(D.G * D.KA));
+  k_pack_t<<<gt, 256, 0, h->stream>>>(prg, state_ptrs(h, false), nv, h->bad);
+  TRY(check_launch(h, "pack"));
+  k_pack_pl<<<(unsigned)((D.npl + 127) / 128), 128, 0, h->stream>>>(prg_pl, state_ptrs(h, true), nv, h->bad);
+  TRY(check_launch(h, "pack_pl"));
+  return before_caller(h, stream);
 }
 
 int nc_download_state_async(nc_handle* h, double* prg, double* prg_pl) {
@@ -1843,7 +1963,7 @@ int nc_history_vars(nc_handle* h, const int32_t* items, int32_t nitems, int64_t 
       VarPtrs vp{};
       vp.v[0] = h->hist_out[it];
       const dim3 gt((unsigned)((D.G + UI - 1) / UI), (unsigned)((D.L + UC - 1) / UC), (unsigned)(D.G * D.KA));
-      k_pack_t<<<gt, 256, 0, s>>>(h->stage_out, vp, 1);
+      k_pack_t<<<gt, 256, 0, s>>>(h->stage_out, vp, 1, h->bad);   // the finiteness note is not read here
       TRY(check_launch(h, "history_pack"));
       CU(cudaMemcpyAsync(out[n], h->stage_out, (size_t)D.npt * sizeof(double), cudaMemcpyDeviceToHost, s));
     } else {
@@ -1865,8 +1985,9 @@ int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* g
     return fail(NC_ERR_ARG, "nc_mass_sum_noalloc: null pointer");
   if ((rhogq == nullptr) != (rhogq_pl == nullptr))
     return fail(NC_ERR_ARG, "nc_mass_sum_noalloc: rhogq and rhogq_pl must both be given or both be null");
-  if (gall_1d < 3 || lall < 1 || kmin < 0 || kmax < kmin || kmax >= kall)
-    return fail(NC_ERR_ARG, "nc_mass_sum_noalloc: bad sizes");
+  if (gall_1d < 4 || lall < 1 || kall < 4 || kall > NC_MAXK || kmin < 0 || kmax < kmin || kmax >= kall)
+    return fail(NC_ERR_ARG, "nc_mass_sum_noalloc: bad sizes (need gall_1d >= 4, lall >= 1, 4 <= kall <= 128, "
+                            "0 <= kmin <= kmax < kall)");
   const long long cols = (long long)lall * gall_1d * gall_1d + 2;
   const long long blocks = (cols + 255) / 256;
   if (blocks > NC_NOALLOC_MASS_MAX_BLOCKS)

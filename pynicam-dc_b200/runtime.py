@@ -31,6 +31,7 @@ _lib = None
 
 # every entry point declared in include/nicam_cuda.h
 EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_state_async", "nc_join_copies",
+           "nc_upload_state_device", "nc_download_state_device", "nc_check_finite",
            "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",
            "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_forcing_step", "nc_history_vars", "nc_restart_pack",
            "nc_restart_unpack", "nc_restart_finish", "nc_divide_known",
@@ -51,6 +52,9 @@ def load_library(path: str = LIB_PATH):
     lib.nc_download_state.argtypes = [vp, dp, dp]
     lib.nc_download_state_async.argtypes = [vp, dp, dp]
     lib.nc_join_copies.argtypes = [vp]
+    lib.nc_upload_state_device.argtypes = [vp, dp, dp, vp]
+    lib.nc_download_state_device.argtypes = [vp, dp, dp, vp]
+    lib.nc_check_finite.argtypes = [vp]
     lib.nc_step.argtypes = [vp, i32]
     lib.nc_set_graph.argtypes = [vp, i32]
     lib.nc_run_phases.argtypes = [vp, i32]
@@ -84,14 +88,26 @@ def load_library(path: str = LIB_PATH):
     lib.nc_destroy.argtypes = [vp]
     lib.nc_destroy.restype = None
     for f in ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_state_async", "nc_join_copies",
+              "nc_upload_state_device", "nc_download_state_device", "nc_check_finite",
               "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_stream", "nc_profile"):
         getattr(lib, f).restype = ctypes.c_int
     _lib = lib
     return lib
 
 
+NC_ERR_ARG, NC_ERR_CUDA, NC_ERR_STATE, NC_ERR_NONFINITE = 1, 2, 3, 4
+
+
 class NicamError(RuntimeError):
-    pass
+    """a non-zero status of the C ABI; ``status`` holds the code"""
+
+    def __init__(self, msg: str, status: int = 0):
+        super().__init__(msg)
+        self.status = status
+
+
+class NonFiniteStateError(NicamError):
+    """NC_ERR_NONFINITE: the device state holds a NaN or an infinity"""
 
 
 def grid_spring(x, x_pl, have_sgp, plan, lam, dbar, dt, crit, max_iter):
@@ -131,10 +147,11 @@ def divide_known(x, b) -> np.ndarray:
     return q
 
 
-def _check(rc: int):
+def _check(rc: int, lib=None):
     if rc != 0:
-        msg = _lib.nc_last_error().decode(errors="replace")
-        raise NicamError(f"libnicamcuda status {rc}: {msg}")
+        msg = (lib or _lib).nc_last_error().decode(errors="replace")
+        cls = NonFiniteStateError if rc == NC_ERR_NONFINITE else NicamError
+        raise cls(f"libnicamcuda status {rc}: {msg}", rc)
 
 
 def _dtype_code(a: np.ndarray) -> int:
@@ -286,6 +303,40 @@ class NicamCuda:
 
     def download_ptr(self, prg_ptr: int, prg_pl_ptr: int):
         _check(self._lib.nc_download_state(self._h, prg_ptr, prg_pl_ptr))
+
+    def upload_tensor(self, prg, prg_pl):
+        """marshal-in from CUDA tensors (torch.float64, contiguous, the
+        reference layout and shapes), ordered on torch's current stream"""
+        self._check_tensors(prg, prg_pl)
+        import torch
+        st = torch.cuda.current_stream(prg.device).cuda_stream
+        _check(self._lib.nc_upload_state_device(self._h, prg.data_ptr(), prg_pl.data_ptr(), st))
+
+    def download_tensor(self, prg=None, prg_pl=None):
+        """marshal-out into CUDA tensors (allocated when not given), ordered
+        on torch's current stream; returns (prg, prg_pl)"""
+        import torch
+        if prg is None:
+            prg = torch.empty(self.shape, dtype=torch.float64, device="cuda")
+        if prg_pl is None:
+            prg_pl = torch.empty(self.shape_pl, dtype=torch.float64, device=prg.device)
+        self._check_tensors(prg, prg_pl)
+        st = torch.cuda.current_stream(prg.device).cuda_stream
+        _check(self._lib.nc_download_state_device(self._h, prg.data_ptr(), prg_pl.data_ptr(), st))
+        return prg, prg_pl
+
+    def _check_tensors(self, prg, prg_pl):
+        import torch
+        for t, shp in ((prg, self.shape), (prg_pl, self.shape_pl)):
+            if (not t.is_cuda or t.dtype != torch.float64 or tuple(t.shape) != tuple(shp)
+                    or not t.is_contiguous()):
+                raise ValueError(f"expected a contiguous float64 CUDA tensor of shape {shp}, got "
+                                 f"{t.dtype} {tuple(t.shape)} on {t.device}")
+
+    def check_finite(self):
+        """raise NonFiniteStateError if the device state holds a NaN or an
+        infinity (nc_check_finite)"""
+        _check(self._lib.nc_check_finite(self._h))
 
     def download_ptr_async(self, prg_ptr: int, prg_pl_ptr: int):
         """download into raw (pinned) host pointers without waiting; the data

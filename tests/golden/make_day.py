@@ -25,9 +25,9 @@ Modes (all CPU):
   compare  compares the two runs and writes ``gl05_z40_day_pin.json``.
 
     python tests/golden/make_day.py --mode digest
-    python tests/golden/make_day.py --mode ref --work /tmp/day &
-    python tests/golden/make_day.py --mode oracle --work /tmp/day
-    python tests/golden/make_day.py --mode compare --work /tmp/day
+    python tests/golden/make_day.py --mode ref --ref <pyNICAM-DC checkout> --work <scratch dir> &
+    python tests/golden/make_day.py --mode oracle --ref <pyNICAM-DC checkout> --work <scratch dir>
+    python tests/golden/make_day.py --mode compare --ref <pyNICAM-DC checkout> --work <scratch dir>
 """
 from __future__ import annotations
 
@@ -239,7 +239,7 @@ def mode_compare(work: str, out_path: str):
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--mode", choices=("digest", "ref", "oracle", "compare"), default="digest")
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of a pyNICAM-DC checkout")
     ap.add_argument("--work", default=os.path.join(tempfile.gettempdir(), "nicam_day"))
     args = ap.parse_args()
     if args.mode == "digest":

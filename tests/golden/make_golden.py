@@ -3,7 +3,7 @@
 Run in a container where the reference tree is available (it is read-only and
 is copied nowhere; the prep tools write into a scratch case directory):
 
-    python tests/golden/make_golden.py --ref /root/reference --out tests/golden
+    python tests/golden/make_golden.py --ref <pyNICAM-DC checkout> --out tests/golden
 
 For each case this script
   1. builds the region table, the icosahedral grid (recursive division +
@@ -243,7 +243,7 @@ def load(path: str):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of a pyNICAM-DC checkout")
     ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
     ap.add_argument("--case", default="gl03_z10_trc")
     args = ap.parse_args()

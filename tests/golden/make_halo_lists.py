@@ -7,9 +7,10 @@ region topology; they are the index maps the device halo exchange must
 reproduce exactly.  Run once, next to a reference checkout, with an rl01
 single-process mnginfo file written by the reference's prep/mnginfo tool:
 
-    python make_halo_lists.py <reference root> <rl01 mnginfo toml>
+    python tests/golden/make_halo_lists.py <reference root> <rl01 mnginfo toml>
 
-Only this generator reads the reference; the package reads the .npz.
+It writes pynicam-dc_b200/data/halo_rl01.npz.  Only this generator reads the
+reference; the package reads the .npz.
 """
 import os
 import subprocess
@@ -67,7 +68,8 @@ def main(ref_root: str, mnginfo: str):
             for k in ("r2r", "p2r", "r2p", "sgp"):
                 out[f"gl{gl:02d}_{k}"] = z[k].astype(np.int16)
             out["have_sgp"] = z["have_sgp"].astype(np.bool_)
-    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "halo_rl01.npz")
+    here = os.path.dirname(os.path.abspath(__file__))
+    dst = os.path.join(here, "..", "..", "pynicam-dc_b200", "data", "halo_rl01.npz")
     np.savez_compressed(dst, **out)
     print("wrote", dst, os.path.getsize(dst))
 

@@ -11,7 +11,7 @@ second).  Stores the extra setup the diagnostics read (height, latitude,
 surface height, layer thicknesses, the saturation constants) and the second
 call's outputs; the states are those of gl03_z10_trc.npz (checked here).
 
-    python tests/golden/make_hist.py --ref /root/reference --out tests/golden
+    python tests/golden/make_hist.py --ref <pyNICAM-DC checkout> --out tests/golden
 """
 from __future__ import annotations
 
@@ -127,7 +127,7 @@ def run(ref: str, out_dir: str):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of a pyNICAM-DC checkout")
     ap.add_argument("--out", default=HERE)
     args = ap.parse_args()
     run(os.path.abspath(args.ref), os.path.abspath(args.out))

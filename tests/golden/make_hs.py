@@ -7,7 +7,7 @@ Dyn.dynamics_step followed by Dyn.forcing_step (pynicamdc/api.py:724-730).
 Stores the setup arrays, the column latitudes GRD_LAT[:, :, K0, :] the forcing
 reads, and the states before and after two forced steps.
 
-    python tests/golden/make_hs.py --ref /root/reference --out tests/golden
+    python tests/golden/make_hs.py --ref <pyNICAM-DC checkout> --out tests/golden
 """
 from __future__ import annotations
 
@@ -89,7 +89,7 @@ def run(ref: str, out_dir: str):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of a pyNICAM-DC checkout")
     ap.add_argument("--out", default=HERE)
     args = ap.parse_args()
     run(os.path.abspath(args.ref), os.path.abspath(args.out))

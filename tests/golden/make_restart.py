@@ -19,7 +19,7 @@ Stores both files (gzip), the state read back, and the metadata the writer
 takes from the run (variable names, labels, units, layer name, region ids,
 grid levels, the pole-centre source cells).
 
-    python tests/golden/make_restart.py --ref /root/reference --out tests/golden
+    python tests/golden/make_restart.py --ref <pyNICAM-DC checkout> --out tests/golden
 """
 from __future__ import annotations
 
@@ -149,7 +149,7 @@ def run(ref: str, out_dir: str):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of a pyNICAM-DC checkout")
     ap.add_argument("--out", default=HERE)
     args = ap.parse_args()
     run(os.path.abspath(args.ref), os.path.abspath(args.out))

@@ -11,7 +11,7 @@ forcing_update, nhm/forcing/mod_af_trcadv.py test11_velocity).  Grid level 3,
 Stores the setup arrays, the column lon/lat, the full- and half-level heights
 the wind formulas read, and the states before and after three steps.
 
-    python tests/golden/make_trcadv.py --ref /root/reference --out tests/golden
+    python tests/golden/make_trcadv.py --ref <pyNICAM-DC checkout> --out tests/golden
 """
 from __future__ import annotations
 
@@ -98,7 +98,7 @@ def run(ref: str, out_dir: str):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of a pyNICAM-DC checkout")
     ap.add_argument("--out", default=HERE)
     args = ap.parse_args()
     run(os.path.abspath(args.ref), os.path.abspath(args.out))

@@ -48,3 +48,24 @@ def test_history_item_ids_match_header(pkg):
         assert items[n] == name, (n, name)
     assert len(items) == 42 and items[26:30] == ("sl_u850", "sl_v850", "sl_w850", "sl_t850")
     assert items[-4:] == ("sl_u100", "sl_v100", "sl_w100", "sl_t100")
+
+
+def test_status_codes_map_to_exceptions(pkg):
+    """a non-zero status becomes NicamError with the library's message;
+    NC_ERR_NONFINITE (a NaN-seeded state found by nc_check_finite or a
+    download) becomes NonFiniteStateError (no GPU: a stand-in library)"""
+    class FakeLib:
+        def __init__(self, msg):
+            self.msg = msg
+
+        def nc_last_error(self):
+            return self.msg
+
+    rt = pkg.runtime
+    rt._check(0, FakeLib(b""))
+    with pytest.raises(pkg.NonFiniteStateError, match="variable 5") as ei:
+        rt._check(rt.NC_ERR_NONFINITE, FakeLib(b"nc_check_finite: non-finite value in prognostic variable 5"))
+    assert ei.value.status == rt.NC_ERR_NONFINITE
+    with pytest.raises(pkg.NicamError) as ei:
+        rt._check(rt.NC_ERR_STATE, FakeLib(b"nc_step: no state uploaded"))
+    assert not isinstance(ei.value, pkg.NonFiniteStateError) and ei.value.status == rt.NC_ERR_STATE

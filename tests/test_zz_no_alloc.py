@@ -1,8 +1,9 @@
 """nc_mass_sum_noalloc: the mass sum for callers that may not allocate device
-memory (a framework's caching allocator or custom-call context, or a stream
-under capture).  It takes the caller's device arrays and keeps its partial sums
-in a fixed device array of the library instead of allocating; its result must
-equal nc_mass_sums of a handle holding the same state, on consecutive calls.
+memory (a framework's caching allocator or custom-call context).  It takes the
+caller's device arrays and keeps its partial sums in a fixed device array of
+the library instead of allocating; it adds the same terms in the same order as
+nc_mass_sums, so its result must equal that of a handle holding the same state
+bit for bit, on consecutive calls.
 
 Kept in a file of its own that pytest collects last.
 """
@@ -12,9 +13,6 @@ import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
-
-REL_TOL = 1e-12          # the tolerance of the mass-sum test in test_gpu_parity
-
 
 def _dev(torch, a):
     return torch.from_numpy(np.ascontiguousarray(a, np.float64)).cuda()
@@ -52,8 +50,8 @@ def test_noalloc_mass_sum_matches_handle(pkg, golden):
     for _ in range(2):                       # two calls in a row of each kind
         air = call(None, None)
         trc = call(rhogq, rhogq_pl)
-        assert abs(air - want[0]) <= REL_TOL * abs(want[0])
-        assert abs(trc - want[1]) <= REL_TOL * abs(want[1])
+        assert air == want[0]
+        assert trc == want[1]
 
 
 def test_noalloc_mass_sum_rejects_oversize_grid(pkg):
@@ -64,3 +62,6 @@ def test_noalloc_mass_sum_rejects_oversize_grid(pkg):
     rc = lib.nc_mass_sum_noalloc(p, None, p, p, p, None, p, p, 1026, 1000, 42, 1, 40, p, None)
     assert rc != 0
     assert "scratch limit" in lib.nc_last_error().decode()
+    rc = lib.nc_mass_sum_noalloc(p, None, p, p, p, None, p, p, 34, 40, 200, 1, 40, p, None)
+    assert rc != 0                           # kall beyond the library's 128 levels
+    assert "bad sizes" in lib.nc_last_error().decode()
