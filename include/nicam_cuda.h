@@ -52,7 +52,21 @@ typedef struct nc_array {
 typedef struct nc_handle nc_handle;
 
 /* Replaces Dyn.dynamics_setup (mod_dynamics.py:164) for the device: uploads
- * geometry, metrics and the halo plan, allocates all device work arrays. */
+ * geometry, metrics and the halo plan, allocates all device work arrays.
+ *
+ * The optional scalar entry "precision" selects the arithmetic, as the
+ * reference's Backend.configure(name, precision) does
+ * (pynicamdc/share/mod_backend.py:175-185): 0 (default) float64, the
+ * reference's numpy arithmetic bit for bit; 1 the mixed form: float32 work
+ * fields, metrics and stencil / advection / hyperdiffusion / tracer
+ * arithmetic, with the tridiagonal (HEVI) elimination and its matrix, the
+ * pressure and density deviations from the reference state
+ * (mod_dynamics.py:1056-1057) and the mass sums in float64.  The host state
+ * and every marshal call stay float64 in both forms.  A mixed handle runs the
+ * dynamics step, the marshal calls, nc_mass_sums, nc_check_finite and
+ * nc_get_field; nc_forcing_step, nc_history_vars, the restart calls and
+ * nc_state_pointers return NC_ERR_STATE for it, and the TRCADV, Held-Suarez
+ * and history set-up entries are rejected (NC_ERR_ARG). */
 int nc_create(const nc_array* arrays, int32_t narrays, nc_handle** out);
 
 /* Marshal-in of the prognostic state (mod_dynamics.py:1876-1880) from host

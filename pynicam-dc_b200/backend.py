@@ -141,13 +141,16 @@ def _history_setup(m) -> dict:
 class CudaDyn:
     """Device-resident replacement of the reference's ``Dyn`` step API."""
 
-    def __init__(self, msc=None, geo: dict = None, graph: bool = True):
+    def __init__(self, msc=None, geo: dict = None, graph: bool = True, precision: str = "float64"):
+        """``precision``: "float64" or "mixed" (see ``NicamCuda``); the
+        reference selects its working precision with
+        ``Backend.configure(name, precision)`` (share/mod_backend.py:175)."""
         if geo is None:
             if msc is None:
                 raise ValueError("CudaDyn needs the reference services (msc) or a setup dict (geo)")
             self._check_config(msc)
             geo = geo_from_msc(msc)
-        self.core = NicamCuda(geo, graph=graph)
+        self.core = NicamCuda(geo, graph=graph, precision=precision)
         self._forced = "GRD_LAT" in geo and str(np.asarray(geo.get("integ_type", "RK3"))) != "TRCADV"
         self._host_stale = False
         self._device_valid = False

@@ -1,12 +1,14 @@
 // C ABI, device memory, halo exchange and the orchestration of one NICAM-DC
 // large step (RK3 HEVI, pynicamdc/nhm/dynamics/mod_dynamics.py:1725-2741).
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/nicam_cuda.h"
@@ -52,13 +54,15 @@ static int fail(int code, const std::string& msg) {
 // p2r, r2p and singular lists composed on the host, so the copy is a single
 // race-free pass: no source is also a destination).
 // ---------------------------------------------------------------------------
+template <class R>
 struct CommFields {
-  double* r[NC_MAXCOMM];
-  double* p[NC_MAXCOMM];
+  R* r[NC_MAXCOMM];
+  R* p[NC_MAXCOMM];
   int n;
 };
 
-__global__ void k_comm(CommFields f, const long long* r_dst, const long long* r_src, int nr, const long long* p_dst,
+template <class R>
+__global__ void k_comm(CommFields<R> f, const long long* r_dst, const long long* r_src, int nr, const long long* p_dst,
                        const long long* p_src, int np) {
   // consecutive threads take consecutive entries of one level: the entries are
   // sorted by destination, so a region's halo rows are read and written in
@@ -97,8 +101,9 @@ __global__ void k_comm(CommFields f, const long long* r_dst, const long long* r_
 // ---------------------------------------------------------------------------
 // marshal kernels: host layout (i,j,k,l,v) <-> per-variable [l][k][j][i]
 // ---------------------------------------------------------------------------
+template <class R>
 struct VarPtrs {
-  double* v[NC_MAXNQ + 6];
+  R* v[NC_MAXNQ + 6];
 };
 
 // Tiled layout conversion of the regional state between the reference layout
@@ -109,7 +114,8 @@ struct VarPtrs {
 // memory so that both sides are read and written in contiguous runs.
 #define UI 32
 #define UC 128
-__global__ void __launch_bounds__(256) k_unpack_t(const double* st, VarPtrs reg, int nv) {
+template <class R>
+__global__ void __launch_bounds__(256) k_unpack_t(const double* st, VarPtrs<R> reg, int nv) {
   __shared__ double tile[UI][UC + 1];
   const int G = cD.G, KA = cD.KA, L = cD.L;
   const int i0 = (int)blockIdx.x * UI, c0 = (int)blockIdx.y * UC;
@@ -126,7 +132,7 @@ __global__ void __launch_bounds__(256) k_unpack_t(const double* st, VarPtrs reg,
     const int i = i0 + ii, c = c0 + cc;
     if (i < G && c < ncl) {
       const int l = c / nv, v = c % nv;
-      reg.v[v][((l * KA + k) * G + j) * G + i] = tile[ii][cc];
+      reg.v[v][((l * KA + k) * G + j) * G + i] = (R)tile[ii][cc];
     }
   }
 }
@@ -139,7 +145,8 @@ __device__ __forceinline__ void note_nonfinite(int* bad, double x, int v) {
   if (!isfinite(x)) atomicMin(bad, v);
 }
 
-__global__ void __launch_bounds__(256) k_pack_t(double* st, VarPtrs reg, int nv, int* bad) {
+template <class R>
+__global__ void __launch_bounds__(256) k_pack_t(double* st, VarPtrs<R> reg, int nv, int* bad) {
   __shared__ double tile[UI][UC + 1];
   const int G = cD.G, KA = cD.KA, L = cD.L;
   const int i0 = (int)blockIdx.x * UI, c0 = (int)blockIdx.y * UC;
@@ -150,7 +157,7 @@ __global__ void __launch_bounds__(256) k_pack_t(double* st, VarPtrs reg, int nv,
     const int i = i0 + ii, c = c0 + cc;
     if (i < G && c < ncl) {
       const int l = c / nv, v = c % nv;
-      const double x = reg.v[v][((l * KA + k) * G + j) * G + i];
+      const double x = (double)reg.v[v][((l * KA + k) * G + j) * G + i];
       note_nonfinite(bad, x, v);
       tile[ii][cc] = x;
     }
@@ -190,7 +197,7 @@ struct PoleSrc {
   int n;
   int e[64][5];   // pole g, pole l, regional i, j, l
 };
-__global__ void k_pole_centre(VarPtrs reg, VarPtrs pol, int nv, PoleSrc ps) {
+__global__ void k_pole_centre(VarPtrs<double> reg, VarPtrs<double> pol, int nv, PoleSrc ps) {
   const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (t >= ps.n * cD.KA) return;
   const int e = t / cD.KA, k = t % cD.KA;
@@ -200,16 +207,18 @@ __global__ void k_pole_centre(VarPtrs reg, VarPtrs pol, int nv, PoleSrc ps) {
 }
 
 // the pole part of the layout conversion: (g, k, l, v) <-> fields [v][g][k][l]
-__global__ void k_unpack_pl(const double* st_pl, VarPtrs pol, int nv) {
+template <class R>
+__global__ void k_unpack_pl(const double* st_pl, VarPtrs<R> pol, int nv) {
   const int q = (int)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= cD.npl) return;
-  for (int v = 0; v < nv; ++v) pol.v[v][q] = st_pl[(long long)q * nv + v];
+  for (int v = 0; v < nv; ++v) pol.v[v][q] = (R)st_pl[(long long)q * nv + v];
 }
-__global__ void k_pack_pl(double* st_pl, VarPtrs pol, int nv, int* bad) {
+template <class R>
+__global__ void k_pack_pl(double* st_pl, VarPtrs<R> pol, int nv, int* bad) {
   const int q = (int)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= cD.npl) return;
   for (int v = 0; v < nv; ++v) {
-    const double x = pol.v[v][q];
+    const double x = (double)pol.v[v][q];
     note_nonfinite(bad, x, v);
     st_pl[(long long)q * nv + v] = x;
   }
@@ -218,7 +227,8 @@ __global__ void k_pack_pl(double* st_pl, VarPtrs pol, int nv, int* bad) {
 // finiteness of the prognostic state: the lowest variable index with a
 // non-finite value (regional fields with their halo and ghost levels, then the
 // pole fields) into *bad, preset to a value above every index
-__global__ void k_finite(VarPtrs reg, VarPtrs pol, int nv, int* bad) {
+template <class R>
+__global__ void k_finite(VarPtrs<R> reg, VarPtrs<R> pol, int nv, int* bad) {
   const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int stride = (int)(gridDim.x * blockDim.x);
   for (int v = 0; v < nv; ++v) {
@@ -239,27 +249,28 @@ __device__ __forceinline__ void neu_add(double& s, double& c, double x) {
   s = t;
 }
 
-__global__ void k_mass(const double* rhog, const double* rhogq, const double* vol, const double* rhog_pl,
-                       const double* rhogq_pl, const double* vol_pl, double* part) {
+template <class R>
+__global__ void k_mass(const R* rhog, const R* rhogq, const double* vol, const R* rhog_pl,
+                       const R* rhogq_pl, const double* vol_pl, double* part) {
   // part[block*2 + {0,1}] = (sum, compensation) of rho*VOLUME (rhogq given: rho*q*VOLUME)
   __shared__ double ss[256], sc[256];
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double s = 0.0, c = 0.0;
   int i, j, l;
-  const double* num = rhogq ? rhogq : rhog;
+  const R* num = rhogq ? rhogq : rhog;
   if (col_of(t, i, j, l)) {
     if (interior(i, j)) {
       for (int k = cD.kmin; k <= cD.kmax; ++k) {
         long long p = ix(i, j, k, l);
-        neu_add(s, c, num[p] / cG.GSGAM2[p] * vol[p]);
+        neu_add(s, c, (double)num[p] / cG.GSGAM2[p] * vol[p]);
       }
     }
   } else if (t - cD.npt2 < cD.LP) {
     int lp = (int)(t - cD.npt2);
-    const double* nump = rhogq_pl ? rhogq_pl : rhog_pl;
+    const R* nump = rhogq_pl ? rhogq_pl : rhog_pl;
     for (int k = cD.kmin; k <= cD.kmax; ++k) {
       int p = ipl(0, k, lp);
-      neu_add(s, c, nump[p] / cG.GSGAM2_pl[p] * vol_pl[p]);
+      neu_add(s, c, (double)nump[p] / cG.GSGAM2_pl[p] * vol_pl[p]);
     }
   }
   ss[threadIdx.x] = s;
@@ -279,10 +290,17 @@ __global__ void k_mass(const double* rhog, const double* rhogq, const double* vo
 // ---------------------------------------------------------------------------
 // handle
 // ---------------------------------------------------------------------------
+// One field: regional and pole arrays.  The pointers hold the device
+// addresses; the element type is float64, or float32 for the work fields of a
+// mixed-precision handle (RG/PL give the typed view).
 struct FieldPair {
   double* r = nullptr;
   double* p = nullptr;
 };
+template <class R>
+static inline R* RG(const FieldPair& f) { return reinterpret_cast<R*>(f.r); }
+template <class R>
+static inline R* PL(const FieldPair& f) { return reinterpret_cast<R*>(f.p); }
 
 // "no non-finite value seen": every byte 0x7f, above any variable index
 #define NC_BAD_NONE 0x7f7f7f7f
@@ -291,6 +309,12 @@ struct nc_handle {
   Dims D{};
   Consts C{};
   Geom Gm{};
+  // mixed precision: float32 work fields, geometry and constants (the
+  // deviations pregd/rhogd and the implicit matrix Mc/Mu/Ml stay float64)
+  bool mixed = false;
+  ConstsT<float> Cf{};
+  GeomT<float> Gmf{};
+  std::map<std::string, int> field_esize;   // bytes per element of each named field
   std::vector<void*> allocs;          // everything cudaMalloc'd
   std::map<std::string, FieldPair> fields;
   cudaStream_t stream = nullptr;
@@ -365,19 +389,26 @@ struct nc_handle {
 
 static nc_handle* g_current = nullptr;   // handle whose constants are loaded
 
-static int dev_alloc(nc_handle* h, double** p, size_t n) {
-  CU(cudaMalloc((void**)p, n * sizeof(double)));
+static int dev_alloc_bytes(nc_handle* h, void** p, size_t bytes) {
+  CU(cudaMalloc(p, bytes));
   h->allocs.push_back(*p);
-  CU(cudaMemset(*p, 0, n * sizeof(double)));
+  CU(cudaMemset(*p, 0, bytes));
   return 0;
 }
+static int dev_alloc(nc_handle* h, double** p, size_t n) {
+  return dev_alloc_bytes(h, (void**)p, n * sizeof(double));
+}
 
-static int field(nc_handle* h, FieldPair& f, const char* name) {
-  int rc = dev_alloc(h, &f.r, (size_t)h->D.npt);
+// a named field of npt regional and npl pole values: float32 in a mixed
+// handle unless f64 is set, else float64
+static int field(nc_handle* h, FieldPair& f, const char* name, bool f64 = false) {
+  const size_t es = (h->mixed && !f64) ? sizeof(float) : sizeof(double);
+  int rc = dev_alloc_bytes(h, (void**)&f.r, (size_t)h->D.npt * es);
   if (rc) return rc;
-  rc = dev_alloc(h, &f.p, (size_t)h->D.npl);
+  rc = dev_alloc_bytes(h, (void**)&f.p, (size_t)h->D.npl * es);
   if (rc) return rc;
   h->fields[name] = f;
+  h->field_esize[name] = (int)es;
   return 0;
 }
 
@@ -459,6 +490,10 @@ static int load_consts(nc_handle* h) {
   CU(cudaMemcpyToSymbol(cD, &h->D, sizeof(Dims)));
   CU(cudaMemcpyToSymbol(cC, &h->C, sizeof(Consts)));
   CU(cudaMemcpyToSymbol(cG, &h->Gm, sizeof(Geom)));
+  if (h->mixed) {
+    CU(cudaMemcpyToSymbol(cCf, &h->Cf, sizeof(ConstsT<float>)));
+    CU(cudaMemcpyToSymbol(cGf, &h->Gmf, sizeof(GeomT<float>)));
+  }
   g_current = h;
   return 0;
 }
@@ -534,12 +569,13 @@ static int join_pl(nc_handle* h) {
 }
 static cudaStream_t pole_stream(nc_handle* h) { return (h->prof || !h->stream2) ? h->stream : h->stream2; }
 
+template <class R>
 static int comm(nc_handle* h, std::initializer_list<FieldPair> fl) {
-  CommFields f{};
+  CommFields<R> f{};
   f.n = 0;
   for (const FieldPair& p : fl) {
-    f.r[f.n] = p.r;
-    f.p[f.n] = p.p;
+    f.r[f.n] = RG<R>(p);
+    f.p[f.n] = PL<R>(p);
     f.n++;
   }
   long long ne = (long long)(h->nr + h->np) * h->D.KA;
@@ -550,14 +586,16 @@ static int comm(nc_handle* h, std::initializer_list<FieldPair> fl) {
   return fork_pl(h);
 }
 
-static Prog prog_reg(nc_handle* h) {
-  Prog p;
-  for (int v = 0; v < 6; ++v) p.v[v] = h->P[v].r;
+template <class R>
+static Prog<R> prog_reg(nc_handle* h) {
+  Prog<R> p;
+  for (int v = 0; v < 6; ++v) p.v[v] = RG<R>(h->P[v]);
   return p;
 }
-static Prog prog_pl(nc_handle* h) {
-  Prog p;
-  for (int v = 0; v < 6; ++v) p.v[v] = h->P[v].p;
+template <class R>
+static Prog<R> prog_pl(nc_handle* h) {
+  Prog<R> p;
+  for (int v = 0; v < 6; ++v) p.v[v] = PL<R>(h->P[v]);
   return p;
 }
 
@@ -570,21 +608,23 @@ static Prog prog_pl(nc_handle* h) {
   } while (0)
 
 // halo exchange of the whole PRG_var: PROG and every tracer
+template <class R>
 static int comm_prg(nc_handle* h) {
   const Dims& D = h->D;
-  CommFields f{};
+  CommFields<R> f{};
   int n = 0;
-  for (int v = 0; v < 6; ++v) { f.r[n] = h->P[v].r; f.p[n] = h->P[v].p; n++; }
-  for (int iq = 0; iq < D.nq && n < NC_MAXCOMM; ++iq) { f.r[n] = h->Pq[iq].r; f.p[n] = h->Pq[iq].p; n++; }
+  for (int v = 0; v < 6; ++v) { f.r[n] = RG<R>(h->P[v]); f.p[n] = PL<R>(h->P[v]); n++; }
+  for (int iq = 0; iq < D.nq && n < NC_MAXCOMM; ++iq) { f.r[n] = RG<R>(h->Pq[iq]); f.p[n] = PL<R>(h->Pq[iq]); n++; }
   f.n = n;
   long long ne = (long long)(h->nr + h->np) * D.KA;
   TRY(join_pl(h));
   k_comm<<<(unsigned)((ne + 255) / 256), 256, 0, h->stream>>>(f, h->r_dst, h->r_src, h->nr, h->p_dst, h->p_src, h->np);
   TRY(check_launch(h, "comm_final"));
-  for (int iq = NC_MAXCOMM - 6; iq < D.nq; ++iq) TRY(comm(h, {h->Pq[iq]}));
+  for (int iq = NC_MAXCOMM - 6; iq < D.nq; ++iq) TRY(comm<R>(h, {h->Pq[iq]}));
   return 0;
 }
 
+template <class R>
 static int run_step(nc_handle* h) {
   cudaStream_t s = h->stream;
   const cudaStream_t ps = pole_stream(h);
@@ -602,8 +642,8 @@ static int run_step(nc_handle* h) {
                        (unsigned)(((D.G - 2 + VP_DX - 1) / VP_DX) * ((D.G - 2 + VP_DY - 1) / VP_DY)), (unsigned)D.L);
   // PROG0 = PROG at the start of the step (mod_dynamics.py:1939-1968)
   for (int v = 0; v < 6; ++v) {
-    CU(cudaMemcpyAsync(h->P0[v].r, h->P[v].r, D.npt * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    CU(cudaMemcpyAsync(h->P0[v].p, h->P[v].p, D.npl * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CU(cudaMemcpyAsync(RG<R>(h->P0[v]), RG<R>(h->P[v]), D.npt * sizeof(R), cudaMemcpyDeviceToDevice, s));
+    CU(cudaMemcpyAsync(PL<R>(h->P0[v]), PL<R>(h->P[v]), D.npl * sizeof(R), cudaMemcpyDeviceToDevice, s));
   }
   if (h->prof) TRY(mark(h, nullptr));
   TRY(fork_pl(h));
@@ -611,12 +651,13 @@ static int run_step(nc_handle* h) {
     const bool last = (nl == h->nstage - 1);
     // ---- Pre_Post
     auto diag_args = [&](bool pole) {
-      DiagArgs a;
-      a.P = pole ? prog_pl(h) : prog_reg(h);
-      a.Pq0 = pole ? h->Pq[0].p : h->Pq[0].r;
-      auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
+      DiagArgs<R> a;
+      a.P = pole ? prog_pl<R>(h) : prog_reg<R>(h);
+      a.Pq0 = pole ? PL<R>(h->Pq[0]) : RG<R>(h->Pq[0]);
+      auto F = [&](FieldPair& f) { return pole ? PL<R>(f) : RG<R>(f); };
+      auto F64 = [&](FieldPair& f) { return pole ? f.p : f.r; };
       a.pre = F(h->pre); a.tem = F(h->tem); a.vx = F(h->vx); a.vy = F(h->vy); a.vz = F(h->vz); a.w = F(h->w);
-      a.rho = F(h->rho); a.ein = F(h->ein); a.eth = F(h->eth); a.pregd = F(h->pregd); a.rhogd = F(h->rhogd);
+      a.rho = F(h->rho); a.ein = F(h->ein); a.eth = F(h->eth); a.pregd = F64(h->pregd); a.rhogd = F64(h->rhogd);
       a.vvx = F(h->vv[0]); a.vvy = F(h->vv[1]); a.vvz = F(h->vv[2]);
       return a;
     };
@@ -627,59 +668,59 @@ static int run_step(nc_handle* h) {
     TRY(check_launch(h, "diag_pl"));
     PHASE();
     // ---- momentum advection
-    AdvMomArgs am;
-    am.rg = h->P[0].r; am.rvx = h->P[1].r; am.rvy = h->P[2].r; am.rvz = h->P[3].r; am.rw = h->P[4].r;
-    am.vvx = h->vv[0].r; am.vvy = h->vv[1].r; am.vvz = h->vv[2].r;
-    am.gvx = h->gadv[0].r; am.gvy = h->gadv[1].r; am.gvz = h->gadv[2].r; am.gw = h->gadv[3].r;
+    AdvMomArgs<R> am;
+    am.rg = RG<R>(h->P[0]); am.rvx = RG<R>(h->P[1]); am.rvy = RG<R>(h->P[2]); am.rvz = RG<R>(h->P[3]); am.rw = RG<R>(h->P[4]);
+    am.vvx = RG<R>(h->vv[0]); am.vvy = RG<R>(h->vv[1]); am.vvz = RG<R>(h->vv[2]);
+    am.gvx = RG<R>(h->gadv[0]); am.gvy = RG<R>(h->gadv[1]); am.gvz = RG<R>(h->gadv[2]); am.gw = RG<R>(h->gadv[3]);
     {
       // interior cells, levels kmin..kmax (see k_advmom_t)
       const dim3 gt((unsigned)(((D.G - 2 + 31) / 32) * ((D.G - 2 + 7) / 8)), 1, (unsigned)D.L);
       k_advmom_t<<<gt, 256, 0, s>>>(am);
     }
     TRY(check_launch(h, "advmom"));
-    AdvMomArgs amp;
-    amp.rg = h->P[0].p; amp.rvx = h->P[1].p; amp.rvy = h->P[2].p; amp.rvz = h->P[3].p; amp.rw = h->P[4].p;
-    amp.vvx = h->vv[0].p; amp.vvy = h->vv[1].p; amp.vvz = h->vv[2].p;
-    amp.gvx = h->gadv[0].p; amp.gvy = h->gadv[1].p; amp.gvz = h->gadv[2].p; amp.gw = h->gadv[3].p;
+    AdvMomArgs<R> amp;
+    amp.rg = PL<R>(h->P[0]); amp.rvx = PL<R>(h->P[1]); amp.rvy = PL<R>(h->P[2]); amp.rvz = PL<R>(h->P[3]); amp.rw = PL<R>(h->P[4]);
+    amp.vvx = PL<R>(h->vv[0]); amp.vvy = PL<R>(h->vv[1]); amp.vvz = PL<R>(h->vv[2]);
+    amp.gvx = PL<R>(h->gadv[0]); amp.gvy = PL<R>(h->gadv[1]); amp.gvz = PL<R>(h->gadv[2]); amp.gw = PL<R>(h->gadv[3]);
     k_advmom_pl<<<1, 32, 0, ps>>>(amp);
     TRY(check_launch(h, "advmom_pl"));
     PHASE();
     // ---- hyperdiffusion
-    Six src, srcp;
-    SixOut o1, o1p;
+    Six<R> src, srcp;
+    SixOut<R> o1, o1p;
     const FieldPair* sf[6] = {&h->vx, &h->vy, &h->vz, &h->w, &h->tem, &h->rho};
     for (int n = 0; n < 6; ++n) {
-      src.f[n] = sf[n]->r; srcp.f[n] = sf[n]->p;
-      o1.f[n] = h->vt[n].r; o1p.f[n] = h->vt[n].p;
+      src.f[n] = RG<R>(*sf[n]); srcp.f[n] = PL<R>(*sf[n]);
+      o1.f[n] = RG<R>(h->vt[n]); o1p.f[n] = PL<R>(h->vt[n]);
     }
     k_hdiff1<<<greg, kBlock, 0, s>>>(src, o1);
     TRY(check_launch(h, "hdiff1"));
     k_hdiff1_pl<<<1, plk, 0, ps>>>(srcp, o1p);
     TRY(check_launch(h, "hdiff1_pl"));
-    TRY(comm(h, {h->vt[0], h->vt[1], h->vt[2], h->vt[3], h->vt[4], h->vt[5]}));
+    TRY(comm<R>(h, {h->vt[0], h->vt[1], h->vt[2], h->vt[3], h->vt[4], h->vt[5]}));
     PHASE();
-    Six vin, vinp;
-    SixOut o2, o2p;
+    Six<R> vin, vinp;
+    SixOut<R> o2, o2p;
     for (int n = 0; n < 6; ++n) {
-      vin.f[n] = h->vt[n].r; vinp.f[n] = h->vt[n].p;
-      o2.f[n] = h->vt2[n].r; o2p.f[n] = h->vt2[n].p;
+      vin.f[n] = RG<R>(h->vt[n]); vinp.f[n] = PL<R>(h->vt[n]);
+      o2.f[n] = RG<R>(h->vt2[n]); o2p.f[n] = PL<R>(h->vt2[n]);
     }
     {
       // interior cells; the exchange below fills the halo rows
       const dim3 gt((unsigned)((D.G - 2 + HD_DX - 1) / HD_DX), (unsigned)((D.G - 2 + HD_DY - 1) / HD_DY),
                     (unsigned)D.L);
       const dim3 gl2((unsigned)D.KA, gt.x * gt.y, gt.z);
-      k_hdiff2_l<<<gl2, HD_DX * HD_DY, 0, s>>>(vin, h->P[0].r, o2);
+      k_hdiff2_l<<<gl2, HD_DX * HD_DY, 0, s>>>(vin, RG<R>(h->P[0]), o2);
       TRY(check_launch(h, "hdiff2"));
     }
-    k_hdiff2_pl<<<1, plk, 0, ps>>>(vinp, h->P[0].p, o2p);
+    k_hdiff2_pl<<<1, plk, 0, ps>>>(vinp, PL<R>(h->P[0]), o2p);
     TRY(check_launch(h, "hdiff2_pl"));
-    TRY(comm(h, {h->vt2[0], h->vt2[1], h->vt2[2], h->vt2[3], h->vt2[4], h->vt2[5]}));
+    TRY(comm<R>(h, {h->vt2[0], h->vt2[1], h->vt2[2], h->vt2[3], h->vt2[4], h->vt2[5]}));
     PHASE();
     // ---- large-step tendency
     for (int pole = 0; pole < 2; ++pole) {
-      GtendArgs ga;
-      auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
+      GtendArgs<R> ga;
+      auto F = [&](FieldPair& f) { return pole ? PL<R>(f) : RG<R>(f); };
       for (int n = 0; n < 6; ++n) { ga.vt2.f[n] = F(h->vt2[n]); ga.gT0[n] = F(h->gT0[n]); }
       ga.rhog = F(h->P[0]); ga.gvx = F(h->gadv[0]); ga.gvy = F(h->gadv[1]); ga.gvz = F(h->gadv[2]);
       ga.gw = F(h->gadv[3]); ga.frhog = F(h->frhog);
@@ -689,21 +730,21 @@ static int run_step(nc_handle* h) {
     }
     PHASE();
     // ---- vi_small_step (mod_vi.py:104-1590)
-    k_split_init<<<npt_blocks, kBlock, 0, s>>>(h->P0[0].r, h->P0[1].r, h->P0[2].r, h->P0[3].r, h->P0[4].r,
-                                                h->P0[5].r, prog_reg(h), h->PSa[0].r, h->PSa[1].r, h->PSa[2].r,
-                                                h->PSa[3].r, h->PSa[4].r, h->PSa[5].r, h->PM[0].r, h->PM[1].r,
-                                                h->PM[2].r, h->PM[3].r, h->PM[4].r, D.npt, nl == 0);
+    k_split_init<<<npt_blocks, kBlock, 0, s>>>(RG<R>(h->P0[0]), RG<R>(h->P0[1]), RG<R>(h->P0[2]), RG<R>(h->P0[3]), RG<R>(h->P0[4]),
+                                                RG<R>(h->P0[5]), prog_reg<R>(h), RG<R>(h->PSa[0]), RG<R>(h->PSa[1]), RG<R>(h->PSa[2]),
+                                                RG<R>(h->PSa[3]), RG<R>(h->PSa[4]), RG<R>(h->PSa[5]), RG<R>(h->PM[0]), RG<R>(h->PM[1]),
+                                                RG<R>(h->PM[2]), RG<R>(h->PM[3]), RG<R>(h->PM[4]), D.npt, nl == 0);
     TRY(check_launch(h, "split_init"));
-    k_split_init<<<npl_blocks, kBlock, 0, ps>>>(h->P0[0].p, h->P0[1].p, h->P0[2].p, h->P0[3].p, h->P0[4].p,
-                                                h->P0[5].p, prog_pl(h), h->PSa[0].p, h->PSa[1].p, h->PSa[2].p,
-                                                h->PSa[3].p, h->PSa[4].p, h->PSa[5].p, h->PM[0].p, h->PM[1].p,
-                                                h->PM[2].p, h->PM[3].p, h->PM[4].p, D.npl, nl == 0);
+    k_split_init<<<npl_blocks, kBlock, 0, ps>>>(PL<R>(h->P0[0]), PL<R>(h->P0[1]), PL<R>(h->P0[2]), PL<R>(h->P0[3]), PL<R>(h->P0[4]),
+                                                PL<R>(h->P0[5]), prog_pl<R>(h), PL<R>(h->PSa[0]), PL<R>(h->PSa[1]), PL<R>(h->PSa[2]),
+                                                PL<R>(h->PSa[3]), PL<R>(h->PSa[4]), PL<R>(h->PSa[5]), PL<R>(h->PM[0]), PL<R>(h->PM[1]),
+                                                PL<R>(h->PM[2]), PL<R>(h->PM[3]), PL<R>(h->PM[4]), D.npl, nl == 0);
     TRY(check_launch(h, "split_init_pl"));
     auto dd3d = [&](FieldPair* v4) -> int {
-      Four v, vp;
-      Three o, op;
-      for (int n = 0; n < 4; ++n) { v.f[n] = v4[n].r; vp.f[n] = v4[n].p; }
-      for (int d = 0; d < 3; ++d) { o.f[d] = h->vtmp2[d].r; op.f[d] = h->vtmp2[d].p; }
+      Four<R> v, vp;
+      Three<R> o, op;
+      for (int n = 0; n < 4; ++n) { v.f[n] = RG<R>(v4[n]); vp.f[n] = PL<R>(v4[n]); }
+      for (int d = 0; d < 3; ++d) { o.f[d] = RG<R>(h->vtmp2[d]); op.f[d] = PL<R>(h->vtmp2[d]); }
       // interior cells only: halo rows are filled by the exchange below and the
       // boundary levels of vtmp2 stay zero from allocation
       const dim3 gt((unsigned)((D.G - 2 + DD_DX - 1) / DD_DX), (unsigned)((D.G - 2 + DD_DY - 1) / DD_DY), (unsigned)D.L);
@@ -711,7 +752,7 @@ static int run_step(nc_handle* h) {
       TRY(check_launch(h, "dd3d"));
       k_dd3d_pl<<<1, plk, 0, ps>>>(vp, op);
       TRY(check_launch(h, "dd3d_pl"));
-      return comm(h, {h->vtmp2[0], h->vtmp2[1], h->vtmp2[2]});
+      return comm<R>(h, {h->vtmp2[0], h->vtmp2[1], h->vtmp2[2]});
     };
     {
       FieldPair v4[4] = {h->P[1], h->P[2], h->P[3], h->P[4]};
@@ -719,18 +760,19 @@ static int run_step(nc_handle* h) {
     }
     PHASE();
     for (int pole = 0; pole < 2; ++pole) {
-      Vp0Args va;
-      auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
-      va.P = pole ? prog_pl(h) : prog_reg(h);
-      va.vx = F(h->vx); va.vy = F(h->vy); va.vz = F(h->vz); va.eth = F(h->eth); va.pregd = F(h->pregd);
-      va.rhogd = F(h->rhogd);
+      Vp0Args<R> va;
+      auto F = [&](FieldPair& f) { return pole ? PL<R>(f) : RG<R>(f); };
+      auto F64 = [&](FieldPair& f) { return pole ? f.p : f.r; };
+      va.P = pole ? prog_pl<R>(h) : prog_reg<R>(h);
+      va.vx = F(h->vx); va.vy = F(h->vy); va.vz = F(h->vz); va.eth = F(h->eth); va.pregd = F64(h->pregd);
+      va.rhogd = F64(h->rhogd);
       for (int d = 0; d < 3; ++d) va.vt.f[d] = F(h->vtmp2[d]);
       for (int n = 0; n < 6; ++n) { va.gT0[n] = F(h->gT0[n]); va.gT[n] = F(h->gT[n]); }
-      va.Mc = F(h->Mc); va.Mu = F(h->Mu); va.Ml = F(h->Ml); va.ethtot0 = F(h->ethtot0);
+      va.Mc = F64(h->Mc); va.Mu = F64(h->Mu); va.Ml = F64(h->Ml); va.ethtot0 = F(h->ethtot0);
       va.dt = h->dts;
       if (!pole) {
-        Vp0H vh;
-        for (int n = 0; n < 8; ++n) vh.out[n] = h->vph[n].r;
+        Vp0H<R> vh;
+        for (int n = 0; n < 8; ++n) vh.out[n] = RG<R>(h->vph[n]);
         k_vp0_hl<<<lvgrid_vp, VP_DX * VP_DY, 0, s>>>(va, vh);
         TRY(check_launch(h, "vp0_h"));
         k_vp0_cr<<<(unsigned)((D.npt2 + NC_VP0C_BLOCK - 1) / NC_VP0C_BLOCK), NC_VP0C_BLOCK, 0, s>>>(va, vh);
@@ -753,8 +795,8 @@ static int run_step(nc_handle* h) {
       }
       PHASE();
       for (int pole = 0; pole < 2; ++pole) {
-        Path1Args pa;
-        auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
+        Path1Args<R> pa;
+        auto F = [&](FieldPair& f) { return pole ? PL<R>(f) : RG<R>(f); };
         for (int n = 0; n < 6; ++n) { pa.PS[n] = F(PS[n]); pa.gT[n] = F(h->gT[n]); }
         pa.rhog = F(h->P[0]);
         for (int d = 0; d < 3; ++d) { pa.vt.f[d] = F(h->vtmp2[d]); pa.dvh[d] = F(PN[1 + d]); }
@@ -768,14 +810,15 @@ static int run_step(nc_handle* h) {
           TRY(check_launch(h, "path1_pl"));
         }
       }
-      TRY(comm(h, {PN[1], PN[2], PN[3]}));
+      TRY(comm<R>(h, {PN[1], PN[2], PN[3]}));
       PHASE();
       for (int pole = 0; pole < 2; ++pole) {
-        VimainArgs va;
-        auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
+        VimainArgs<R> va;
+        auto F = [&](FieldPair& f) { return pole ? PL<R>(f) : RG<R>(f); };
+      auto F64 = [&](FieldPair& f) { return pole ? f.p : f.r; };
         for (int n = 0; n < 6; ++n) { va.PS[n] = F(PS[n]); va.P[n] = F(h->P[n]); va.gT[n] = F(h->gT[n]); }
         va.eth = F(h->eth); va.ethtot0 = F(h->ethtot0); va.gT0e = F(h->gT0[5]);
-        va.Mc = F(h->Mc); va.Mu = F(h->Mu); va.Ml = F(h->Ml);
+        va.Mc = F64(h->Mc); va.Mu = F64(h->Mu); va.Ml = F64(h->Ml);
         for (int d = 0; d < 3; ++d) { va.dvh.f[d] = F(PN[1 + d]); va.hdiv[d] = F(h->hdiv[d]); }
         va.dwe[0] = F(PN[0]); va.dwe[1] = F(PN[4]); va.dwe[2] = F(PN[5]);
         va.PM0 = F(h->PM[0]); va.PM4 = F(h->PM[4]);
@@ -783,8 +826,8 @@ static int run_step(nc_handle* h) {
         if (!pole) {
           k_vimain_a_l<<<lvgrid, DD_DX * DD_DY, 0, s>>>(va);
           TRY(check_launch(h, "vimain_a"));
-          if (h->C.gam_unit) k_vi_solve<true><<<greg, kBlock, 0, s>>>(va);
-          else k_vi_solve<false><<<greg, kBlock, 0, s>>>(va);
+          if (h->C.gam_unit) k_vi_solve<R, true><<<greg, kBlock, 0, s>>>(va);
+          else k_vi_solve<R, false><<<greg, kBlock, 0, s>>>(va);
           TRY(check_launch(h, "vi_solve"));
           k_vi_energy_p<<<npt_blocks, kBlock, 0, s>>>(va);
           TRY(check_launch(h, "vi_energy"));
@@ -795,18 +838,18 @@ static int run_step(nc_handle* h) {
           TRY(check_launch(h, "vimain_b_pl"));
         }
       }
-      TRY(comm(h, {PN[0], PN[4], PN[5]}));
+      TRY(comm<R>(h, {PN[0], PN[4], PN[5]}));
       PHASE();
     }
     FieldPair* PSf = (nitr % 2 == 0) ? h->PSa : h->PSb;
-    k_post<<<greg, kBlock, 0, s>>>(prog_reg(h), PSf[0].r, PSf[1].r, PSf[2].r, PSf[3].r, PSf[4].r, PSf[5].r, 0);
+    k_post<<<greg, kBlock, 0, s>>>(prog_reg<R>(h), RG<R>(PSf[0]), RG<R>(PSf[1]), RG<R>(PSf[2]), RG<R>(PSf[3]), RG<R>(PSf[4]), RG<R>(PSf[5]), 0);
     TRY(check_launch(h, "post"));
-    k_post<<<1, 32, 0, ps>>>(prog_pl(h), PSf[0].p, PSf[1].p, PSf[2].p, PSf[3].p, PSf[4].p, PSf[5].p, 1);
+    k_post<<<1, 32, 0, ps>>>(prog_pl<R>(h), PL<R>(PSf[0]), PL<R>(PSf[1]), PL<R>(PSf[2]), PL<R>(PSf[3]), PL<R>(PSf[4]), PL<R>(PSf[5]), 1);
     TRY(check_launch(h, "post_pl"));
-    TRY(comm(h, {h->PM[0], h->PM[1], h->PM[2], h->PM[3], h->PM[4]}));
+    TRY(comm<R>(h, {h->PM[0], h->PM[1], h->PM[2], h->PM[3], h->PM[4]}));
     PHASE();
     if (!last) {
-      TRY(comm(h, {h->P[0], h->P[1], h->P[2], h->P[3], h->P[4], h->P[5]}));
+      TRY(comm<R>(h, {h->P[0], h->P[1], h->P[2], h->P[3], h->P[4], h->P[5]}));
       PHASE();
       continue;
     }
@@ -816,19 +859,19 @@ static int run_step(nc_handle* h) {
     // tracers move with the current PROG (as the mean state, rhog_in = PROG0) and
     // no density tendency
     for (int v = 0; v < 5; ++v) {
-      CU(cudaMemcpyAsync(h->PM[v].r, h->P[v].r, D.npt * sizeof(double), cudaMemcpyDeviceToDevice, s));
-      CU(cudaMemcpyAsync(h->PM[v].p, h->P[v].p, D.npl * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      CU(cudaMemcpyAsync(RG<R>(h->PM[v]), RG<R>(h->P[v]), D.npt * sizeof(R), cudaMemcpyDeviceToDevice, s));
+      CU(cudaMemcpyAsync(PL<R>(h->PM[v]), PL<R>(h->P[v]), D.npl * sizeof(R), cudaMemcpyDeviceToDevice, s));
     }
-    CU(cudaMemsetAsync(h->frhog.r, 0, D.npt * sizeof(double), s));
-    CU(cudaMemsetAsync(h->frhog.p, 0, D.npl * sizeof(double), s));
+    CU(cudaMemsetAsync(RG<R>(h->frhog), 0, D.npt * sizeof(R), s));
+    CU(cudaMemsetAsync(PL<R>(h->frhog), 0, D.npl * sizeof(R), s));
     TRY(join_pl(h));
     TRY(fork_pl(h));
   }
   // ---- tracer advection (mod_src_tracer.py:83-1228), after the last RK stage
   const double dt = h->dtl;
   for (int pole = 0; pole < 2; ++pole) {
-    TrcFluxArgs ta;
-    auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
+    TrcFluxArgs<R> ta;
+    auto F = [&](FieldPair& f) { return pole ? PL<R>(f) : RG<R>(f); };
     ta.rvx = F(h->PM[1]); ta.rvy = F(h->PM[2]); ta.rvz = F(h->PM[3]); ta.rw = F(h->PM[4]);
     ta.rhog_in = F(h->P0[0]); ta.frhog = F(h->frhog); ta.flx_v = F(h->flx_v); ta.rhog_t = F(h->rhog_t);
     ta.dt = dt;
@@ -838,8 +881,8 @@ static int run_step(nc_handle* h) {
   }
   auto vadv = [&](int iq, bool second) -> int {
     for (int pole = 0; pole < 2; ++pole) {
-      TrcVadvArgs va;
-      auto F = [&](FieldPair& f) { return pole ? f.p : f.r; };
+      TrcVadvArgs<R> va;
+      auto F = [&](FieldPair& f) { return pole ? PL<R>(f) : RG<R>(f); };
       va.rhogq = F(h->Pq[iq]);
       va.den = second ? F(h->rhog_t) : F(h->P0[0]);
       va.flx_v = F(h->flx_v); va.frhog = F(h->frhog);
@@ -855,19 +898,19 @@ static int run_step(nc_handle* h) {
   for (int iq = 0; iq < D.nq; ++iq) TRY(vadv(iq, false));
   PHASE();
   {
-    TrcHfluxArgs ha;
-    ha.rho = h->PM[0].r; ha.rvx = h->PM[1].r; ha.rvy = h->PM[2].r; ha.rvz = h->PM[3].r; ha.rhog_t = h->rhog_t.r;
-    for (int f = 0; f < 6; ++f) { ha.flx[f] = h->flx[f].r; ha.ch[f] = h->ch[f].r; ha.cm[f] = h->cm[f].r; }
-    for (int f = 0; f < 9; ++f) ha.xc[f] = h->xc[f].r;
+    TrcHfluxArgs<R> ha;
+    ha.rho = RG<R>(h->PM[0]); ha.rvx = RG<R>(h->PM[1]); ha.rvy = RG<R>(h->PM[2]); ha.rvz = RG<R>(h->PM[3]); ha.rhog_t = RG<R>(h->rhog_t);
+    for (int f = 0; f < 6; ++f) { ha.flx[f] = RG<R>(h->flx[f]); ha.ch[f] = RG<R>(h->ch[f]); ha.cm[f] = RG<R>(h->cm[f]); }
+    for (int f = 0; f < 9; ++f) ha.xc[f] = RG<R>(h->xc[f]);
     ha.dt = dt;
     {
       const dim3 gt((unsigned)D.KA, (unsigned)(((D.G + TH_DX - 1) / TH_DX) * ((D.G + TH_DY - 1) / TH_DY)), (unsigned)D.L);
       k_trc_hflux_t<<<gt, TH_DX * TH_DY, 0, s>>>(ha);
     }
     TRY(check_launch(h, "trc_hflux"));
-    TrcHfluxPlArgs hp;
-    hp.rho = h->PM[0].p; hp.rvx = h->PM[1].p; hp.rvy = h->PM[2].p; hp.rvz = h->PM[3].p; hp.rhog_t = h->rhog_t.p;
-    hp.flx = h->flx[0].p; hp.xc = h->xc[0].p; hp.ch = h->ch[0].p; hp.cm = h->cm[0].p; hp.dt = dt;
+    TrcHfluxPlArgs<R> hp;
+    hp.rho = PL<R>(h->PM[0]); hp.rvx = PL<R>(h->PM[1]); hp.rvy = PL<R>(h->PM[2]); hp.rvz = PL<R>(h->PM[3]); hp.rhog_t = PL<R>(h->rhog_t);
+    hp.flx = PL<R>(h->flx[0]); hp.xc = PL<R>(h->xc[0]); hp.ch = PL<R>(h->ch[0]); hp.cm = PL<R>(h->cm[0]); hp.dt = dt;
     k_trc_hflux_pl<<<1, plk, 0, ps>>>(hp);
     TRY(check_launch(h, "trc_hflux_pl"));
   }
@@ -876,40 +919,40 @@ static int run_step(nc_handle* h) {
     {
       const dim3 gt((unsigned)D.KA, (unsigned)(((D.G - 2 + TG_DX - 1) / TG_DX) * ((D.G - 2 + TG_DY - 1) / TG_DY)),
                     (unsigned)D.L);
-      k_trc_grad_t<<<gt, TG_DX * TG_DY, 0, s>>>(h->Pq[iq].r, h->rhog_t.r, h->q.r, h->gq[0].r, h->gq[1].r,
-                                                h->gq[2].r);
+      k_trc_grad_t<<<gt, TG_DX * TG_DY, 0, s>>>(RG<R>(h->Pq[iq]), RG<R>(h->rhog_t), RG<R>(h->q), RG<R>(h->gq[0]), RG<R>(h->gq[1]),
+                                                RG<R>(h->gq[2]));
     }
     TRY(check_launch(h, "trc_grad"));
-    k_trc_grad_pl<<<1, plk, 0, ps>>>(h->Pq[iq].p, h->rhog_t.p, h->q.p, h->gq[0].p, h->gq[1].p, h->gq[2].p);
+    k_trc_grad_pl<<<1, plk, 0, ps>>>(PL<R>(h->Pq[iq]), PL<R>(h->rhog_t), PL<R>(h->q), PL<R>(h->gq[0]), PL<R>(h->gq[1]), PL<R>(h->gq[2]));
     TRY(check_launch(h, "trc_grad_pl"));
-    TRY(comm(h, {h->gq[0], h->gq[1], h->gq[2]}));
-    TrcRemapArgs ra;
-    ra.q = h->q.r; ra.gq0 = h->gq[0].r; ra.gq1 = h->gq[1].r; ra.gq2 = h->gq[2].r;
-    for (int f = 0; f < 9; ++f) ra.xc[f] = h->xc[f].r;
-    for (int f = 0; f < 6; ++f) ra.cm[f] = h->cm[f].r;
-    for (int f = 0; f < 3; ++f) ra.qa[f] = h->qa[f].r;
+    TRY(comm<R>(h, {h->gq[0], h->gq[1], h->gq[2]}));
+    TrcRemapArgs<R> ra;
+    ra.q = RG<R>(h->q); ra.gq0 = RG<R>(h->gq[0]); ra.gq1 = RG<R>(h->gq[1]); ra.gq2 = RG<R>(h->gq[2]);
+    for (int f = 0; f < 9; ++f) ra.xc[f] = RG<R>(h->xc[f]);
+    for (int f = 0; f < 6; ++f) ra.cm[f] = RG<R>(h->cm[f]);
+    for (int f = 0; f < 3; ++f) ra.qa[f] = RG<R>(h->qa[f]);
     k_trc_remap<<<greg, kBlock, 0, s>>>(ra);
     TRY(check_launch(h, "trc_remap"));
-    TrcRemapPlArgs rp;
-    rp.q = h->q.p; rp.gq0 = h->gq[0].p; rp.gq1 = h->gq[1].p; rp.gq2 = h->gq[2].p; rp.xc = h->xc[0].p;
-    rp.cm = h->cm[0].p; rp.qa = h->qa[0].p;
+    TrcRemapPlArgs<R> rp;
+    rp.q = PL<R>(h->q); rp.gq0 = PL<R>(h->gq[0]); rp.gq1 = PL<R>(h->gq[1]); rp.gq2 = PL<R>(h->gq[2]); rp.xc = PL<R>(h->xc[0]);
+    rp.cm = PL<R>(h->cm[0]); rp.qa = PL<R>(h->qa[0]);
     k_trc_remap_pl<<<1, plk, 0, ps>>>(rp);
     TRY(check_launch(h, "trc_remap_pl"));
-    TrcLimArgs la;
-    la.q = h->q.r; la.rhog_t = h->rhog_t.r; la.frhog = h->frhog.r;
-    for (int f = 0; f < 6; ++f) { la.ch[f] = h->ch[f].r; la.cm[f] = h->cm[f].r; la.flx[f] = h->flx[f].r; }
-    for (int f = 0; f < 3; ++f) la.qa[f] = h->qa[f].r;
-    la.qout_min = h->Qmin.r; la.qout_max = h->Qmax.r; la.Qmin = h->Qmin.r; la.Qmax = h->Qmax.r;
-    la.rhogq = h->Pq[iq].r; la.dt = dt;
-    TrcLimPlArgs lp;
-    lp.q = h->q.p; lp.ch = h->ch[0].p; lp.cm = h->cm[0].p; lp.rhog_t = h->rhog_t.p; lp.frhog = h->frhog.p;
-    lp.qa = h->qa[0].p; lp.flx = h->flx[0].p; lp.Qmin = h->Qmin.p; lp.Qmax = h->Qmax.p;
-    lp.qout_min = h->Qmin.p; lp.qout_max = h->Qmax.p; lp.rhogq = h->Pq[iq].p; lp.dt = dt;
+    TrcLimArgs<R> la;
+    la.q = RG<R>(h->q); la.rhog_t = RG<R>(h->rhog_t); la.frhog = RG<R>(h->frhog);
+    for (int f = 0; f < 6; ++f) { la.ch[f] = RG<R>(h->ch[f]); la.cm[f] = RG<R>(h->cm[f]); la.flx[f] = RG<R>(h->flx[f]); }
+    for (int f = 0; f < 3; ++f) la.qa[f] = RG<R>(h->qa[f]);
+    la.qout_min = RG<R>(h->Qmin); la.qout_max = RG<R>(h->Qmax); la.Qmin = RG<R>(h->Qmin); la.Qmax = RG<R>(h->Qmax);
+    la.rhogq = RG<R>(h->Pq[iq]); la.dt = dt;
+    TrcLimPlArgs<R> lp;
+    lp.q = PL<R>(h->q); lp.ch = PL<R>(h->ch[0]); lp.cm = PL<R>(h->cm[0]); lp.rhog_t = PL<R>(h->rhog_t); lp.frhog = PL<R>(h->frhog);
+    lp.qa = PL<R>(h->qa[0]); lp.flx = PL<R>(h->flx[0]); lp.Qmin = PL<R>(h->Qmin); lp.Qmax = PL<R>(h->Qmax);
+    lp.qout_min = PL<R>(h->Qmin); lp.qout_max = PL<R>(h->Qmax); lp.rhogq = PL<R>(h->Pq[iq]); lp.dt = dt;
     k_trc_qout<<<greg, kBlock, 0, s>>>(la);
     TRY(check_launch(h, "trc_qout"));
     k_trc_qout_pl<<<1, plk, 0, ps>>>(lp);
     TRY(check_launch(h, "trc_qout_pl"));
-    TRY(comm(h, {h->Qmin, h->Qmax}));
+    TRY(comm<R>(h, {h->Qmin, h->Qmax}));
     k_trc_apply<<<greg, kBlock, 0, s>>>(la);
     TRY(check_launch(h, "trc_apply"));
     k_trc_apply_pl<<<1, plk, 0, ps>>>(lp);
@@ -917,30 +960,32 @@ static int run_step(nc_handle* h) {
   }
   PHASE();
   TRY(join_pl(h));
-  k_trc_rhog<<<gkl, kBlock, 0, s>>>(h->rhog_t.r, h->flx[0].r, h->flx[1].r, h->flx[2].r, h->flx[3].r, h->flx[4].r,
-                                     h->flx[5].r, h->frhog.r, dt, h->flx[0].p, h->rhog_t.p, h->frhog.p);
+  k_trc_rhog<<<gkl, kBlock, 0, s>>>(RG<R>(h->rhog_t), RG<R>(h->flx[0]), RG<R>(h->flx[1]), RG<R>(h->flx[2]), RG<R>(h->flx[3]), RG<R>(h->flx[4]),
+                                     RG<R>(h->flx[5]), RG<R>(h->frhog), (R)dt, PL<R>(h->flx[0]), PL<R>(h->rhog_t), PL<R>(h->frhog));
   TRY(check_launch(h, "trc_rhog"));
   TRY(fork_pl(h));
   for (int iq = 0; iq < D.nq; ++iq) TRY(vadv(iq, true));
   PHASE();
+  if constexpr (std::is_same<R, double>::value) {   // TRCADV is a float64 configuration (checked at set-up)
   if (h->trcadv) {
     // the prescribed winds of the next time (mod_forcing.py forcing_update)
     TRY(join_pl(h));
     k_trcadv_time<<<1, 1, 0, s>>>(h->trc_time, h->dtl);
     TRY(check_launch(h, "trcadv_time"));
     TrcWindArgs w;
-    for (int v = 0; v < 6; ++v) w.P.v[v] = h->P[v].r;
+    for (int v = 0; v < 6; ++v) w.P.v[v] = RG<double>(h->P[v]);
     w.lon = h->trc_lon; w.lat = h->trc_lat; w.zf = h->trc_zf; w.zh = h->trc_zh; w.time = h->trc_time;
     w.a = 6371220.0; w.Rd = 287.0; w.g = 9.80616; w.pi = 3.141592653589793238;
     k_trcadv_winds<<<npt_blocks, kBlock, 0, s>>>(w, 0);
     TRY(check_launch(h, "trcadv_winds"));
-    for (int v = 0; v < 6; ++v) w.P.v[v] = h->P[v].p;
+    for (int v = 0; v < 6; ++v) w.P.v[v] = PL<double>(h->P[v]);
     w.lon = h->trc_lon_pl; w.lat = h->trc_lat_pl; w.zf = h->trc_zf_pl; w.zh = h->trc_zh_pl;
     k_trcadv_winds<<<npl_blocks, kBlock, 0, s>>>(w, 1);
     TRY(check_launch(h, "trcadv_winds_pl"));
   }
+  }
   // marshal-out halo exchange of PRG_var (mod_dynamics.py:2726-2727)
-  TRY(comm_prg(h));
+  TRY(comm_prg<R>(h));
   TRY(join_pl(h));
   return 0;
 }
@@ -1032,6 +1077,55 @@ static int mass_scratch_ptr(double** out) {
   return 0;
 }
 
+template <class R>
+static VarPtrs<R> state_ptrs(nc_handle* h, bool pole) {
+  VarPtrs<R> v{};
+  for (int n = 0; n < 6; ++n) v.v[n] = pole ? PL<R>(h->P[n]) : RG<R>(h->P[n]);
+  for (int n = 0; n < h->D.nq; ++n) v.v[6 + n] = pole ? PL<R>(h->Pq[n]) : RG<R>(h->Pq[n]);
+  return v;
+}
+
+// the marshal kernels of one state (reference layout <-> fields of type R)
+template <class R>
+static int unpack_state(nc_handle* h, const double* st, const double* st_pl) {
+  const Dims& D = h->D;
+  const int nv = 6 + D.nq;
+  const dim3 gt((unsigned)((D.G + UI - 1) / UI), (unsigned)((D.L * nv + UC - 1) / UC), (unsigned)(D.G * D.KA));
+  k_unpack_t<<<gt, 256, 0, h->stream>>>(st, state_ptrs<R>(h, false), nv);
+  TRY(check_launch(h, "unpack"));
+  k_unpack_pl<<<(unsigned)((D.npl + 127) / 128), 128, 0, h->stream>>>(st_pl, state_ptrs<R>(h, true), nv);
+  return check_launch(h, "unpack_pl");
+}
+template <class R>
+static int pack_state(nc_handle* h, double* st, double* st_pl) {
+  const Dims& D = h->D;
+  const int nv = 6 + D.nq;
+  const dim3 gt((unsigned)((D.G + UI - 1) / UI), (unsigned)((D.L * nv + UC - 1) / UC), (unsigned)(D.G * D.KA));
+  k_pack_t<<<gt, 256, 0, h->stream>>>(st, state_ptrs<R>(h, false), nv, h->bad);
+  TRY(check_launch(h, "pack"));
+  k_pack_pl<<<(unsigned)((D.npl + 127) / 128), 128, 0, h->stream>>>(st_pl, state_ptrs<R>(h, true), nv, h->bad);
+  return check_launch(h, "pack_pl");
+}
+template <class R>
+static int finite_state(nc_handle* h) {
+  k_finite<<<4 * 148, 256, 0, h->stream>>>(state_ptrs<R>(h, false), state_ptrs<R>(h, true), 6 + h->D.nq, h->bad);
+  return check_launch(h, "finite");
+}
+template <class R>
+static int mass_sum(nc_handle* h, int n) {
+  const R* num = n == 0 ? nullptr : RG<R>(h->Pq[n - 1]);
+  const R* nump = n == 0 ? nullptr : PL<R>(h->Pq[n - 1]);
+  k_mass<<<h->mass_blocks, 256, 0, h->stream>>>(RG<R>(h->P[0]), num, h->vol, PL<R>(h->P[0]), nump, h->vol_pl,
+                                                h->mass_part);
+  return check_launch(h, "mass");
+}
+static int step_once(nc_handle* h) { return h->mixed ? run_step<float>(h) : run_step<double>(h); }
+// the entry points of the float64 form only
+static int f64_only(nc_handle* h, const char* what) {
+  if (h->mixed) return fail(NC_ERR_STATE, std::string(what) + ": not available for a mixed-precision handle");
+  return 0;
+}
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
@@ -1039,6 +1133,7 @@ extern "C" {
 
 int nc_forcing_step(nc_handle* h) {
   if (!h) return fail(NC_ERR_ARG, "nc_forcing_step: null handle");
+  TRY(f64_only(h, "nc_forcing_step"));
   if (!h->have_state) return fail(NC_ERR_STATE, "nc_forcing_step: no state uploaded");
   if (!h->hs_lat)
     return fail(NC_ERR_STATE, "nc_forcing_step: the handle was created without AF_hs_lat_terms "
@@ -1061,7 +1156,7 @@ int nc_forcing_step(nc_handle* h) {
   a.PRE00 = h->C.PRE00;
   k_forcing_hs<<<(unsigned)((D.npt2 + kBlock - 1) / kBlock), kBlock, 0, h->stream>>>(a);
   TRY(check_launch(h, "forcing_hs"));
-  TRY(comm_prg(h));
+  TRY(comm_prg<double>(h));
   TRY(join_pl(h));
   return 0;
 }
@@ -1069,6 +1164,81 @@ int nc_forcing_step(nc_handle* h) {
 const char* nc_last_error(void) { return g_err.c_str(); }
 
 int64_t nc_kernel_launches(nc_handle* h) { return h ? h->launches : 0; }
+
+// float32 copy of n float64 device values
+__global__ void k_to_f32(const double* src, float* dst, long long n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dst[t] = (float)src[t];
+}
+static int to_f32(nc_handle* h, const double* src, long long n, const float** dst) {
+  if (!src) {
+    *dst = nullptr;
+    return 0;
+  }
+  float* d = nullptr;
+  TRY(dev_alloc_bytes(h, (void**)&d, (size_t)n * sizeof(float)));
+  k_to_f32<<<(unsigned)((n + 255) / 256), 256>>>(src, d, n);
+  CU(cudaGetLastError());
+  *dst = d;
+  return 0;
+}
+
+// The mixed form's float32 geometry and constants, rounded from the float64
+// ones (which stay resident: the mass sums read GSGAM2 in float64).
+static int make_f32_geometry(nc_handle* h) {
+  const Dims& D = h->D;
+  const Geom& G = h->Gm;
+  GeomT<float>& F = h->Gmf;
+  const long long n3 = D.npt, n2 = D.npt2, np = D.npl, gl = 6LL * D.LP;
+  struct Item {
+    const double* src;
+    long long n;
+    const float** dst;
+  } items[] = {
+      {G.GSGAM2, n3, &F.GSGAM2}, {G.GSGAM2H, n3, &F.GSGAM2H}, {G.RGSGAM2, n3, &F.RGSGAM2},
+      {G.RGSGAM2H, n3, &F.RGSGAM2H}, {G.RGSQRTH, n3, &F.RGSQRTH}, {G.RGAM, n3, &F.RGAM}, {G.RGAMH, n3, &F.RGAMH},
+      {G.GAM2H, n3, &F.GAM2H}, {G.PHI, n3, &F.PHI}, {G.C2W, 2 * n3, &F.C2W}, {G.W2C, 2 * n3, &F.W2C},
+      {G.C2WGz, 6 * n3, &F.C2WGz}, {G.rho_bs, n3, &F.rho_bs}, {G.pre_bs, n3, &F.pre_bs}, {G.tem_bs, n3, &F.tem_bs},
+      {G.coef_div, 21 * n2, &F.coef_div}, {G.coef_grad, 21 * n2, &F.coef_grad}, {G.coef_lap, 7 * n2, &F.coef_lap},
+      {G.coef_intp, 18 * n2, &F.coef_intp}, {G.intp_w, 18 * n2, &F.intp_w}, {G.coef_diff, 18 * n2, &F.coef_diff},
+      {G.GRD_x, 3 * n2, &F.GRD_x}, {G.GRD_xr, 9 * n2, &F.GRD_xr}, {G.GMTR_t, 6 * n2, &F.GMTR_t},
+      {G.GMTR_a, 9 * n2, &F.GMTR_a}, {G.GMTR_p, n2, &F.GMTR_p},
+      {G.GSGAM2_pl, np, &F.GSGAM2_pl}, {G.GSGAM2H_pl, np, &F.GSGAM2H_pl}, {G.RGSGAM2_pl, np, &F.RGSGAM2_pl},
+      {G.RGSGAM2H_pl, np, &F.RGSGAM2H_pl}, {G.RGSQRTH_pl, np, &F.RGSQRTH_pl}, {G.RGAM_pl, np, &F.RGAM_pl},
+      {G.RGAMH_pl, np, &F.RGAMH_pl}, {G.GAM2H_pl, np, &F.GAM2H_pl}, {G.PHI_pl, np, &F.PHI_pl},
+      {G.C2W_pl, 2 * np, &F.C2W_pl}, {G.W2C_pl, 2 * np, &F.W2C_pl}, {G.C2WGz_pl, 6 * np, &F.C2WGz_pl},
+      {G.rho_bs_pl, np, &F.rho_bs_pl}, {G.pre_bs_pl, np, &F.pre_bs_pl}, {G.tem_bs_pl, np, &F.tem_bs_pl},
+      {G.coef_div_pl, gl * 3, &F.coef_div_pl}, {G.coef_grad_pl, gl * 3, &F.coef_grad_pl},
+      {G.coef_lap_pl, gl, &F.coef_lap_pl}, {G.coef_intp_pl, gl * 9, &F.coef_intp_pl},
+      {G.coef_diff_pl, gl * 3, &F.coef_diff_pl}, {G.GRD_x_pl, gl * 3, &F.GRD_x_pl}, {G.GRD_xr_pl, gl * 3, &F.GRD_xr_pl},
+      {G.GMTR_t_pl, gl * 5, &F.GMTR_t_pl}, {G.GMTR_a_pl, gl * 18, &F.GMTR_a_pl}, {G.GMTR_p_pl, gl * 8, &F.GMTR_p_pl},
+  };
+  for (const Item& it : items) TRY(to_f32(h, it.src, it.n, it.dst));
+  F.pntmask = G.pntmask;
+  F.have_sgp = G.have_sgp;
+  CU(cudaDeviceSynchronize());
+  const Consts& C = h->C;
+  ConstsT<float>& Cf = h->Cf;
+  Cf.GRAV = (float)C.GRAV; Cf.Rdry = (float)C.Rdry; Cf.CVdry = (float)C.CVdry; Cf.CPdry = (float)C.CPdry;
+  Cf.Rvap = (float)C.Rvap; Cf.OHM = (float)C.OHM;
+  // the reference's float32 constants (share/mod_const.py:170-172): EPS and HUGE are
+  // the working type's machine epsilon and largest value (the float64 HUGE would
+  // round to infinity, and 0 * HUGE in the limiters' masks would give NaN)
+  Cf.EPS = FLT_EPSILON;
+  Cf.HUGE_ = FLT_MAX;
+  Cf.rscale = (float)C.rscale; Cf.alpha = (float)C.alpha; Cf.Kh = (float)C.Kh; Cf.divdamp_coef = (float)C.divdamp_coef;
+  Cf.hdiff_fact_rho = (float)C.hdiff_fact_rho; Cf.CVW0 = (float)C.CVW0; Cf.PRE00 = (float)C.PRE00;
+  Cf.gam_unit = C.gam_unit;
+  Cf.rsc_h = (float)(1.0 / C.rscale);   // the float32 divisions multiply by the rounded reciprocal
+  Cf.rsc_l = 0.0f;
+  Cf.third_h = (float)(1.0 / 3.0);
+  Cf.third_l = 0.0f;
+  for (int k = 0; k < NC_MAXK; ++k) {
+    Cf.afact[k] = (float)C.afact[k]; Cf.bfact[k] = (float)C.bfact[k]; Cf.cfact[k] = (float)C.cfact[k];
+    Cf.dfact[k] = (float)C.dfact[k]; Cf.rdgz[k] = (float)C.rdgz[k]; Cf.rdgzh[k] = (float)C.rdgzh[k];
+  }
+  return 0;
+}
 
 static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   ArrTab T;
@@ -1106,6 +1276,12 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   TRY(scalar(T, "alpha", C.alpha)); TRY(scalar(T, "Kh_coef", C.Kh)); TRY(scalar(T, "divdamp_coef", C.divdamp_coef));
   TRY(scalar(T, "hdiff_fact_rho", C.hdiff_fact_rho));
   if (!(C.rscale != 0.0 && std::isfinite(C.rscale))) return fail(NC_ERR_ARG, "rscale must be finite and nonzero");
+  if (T.get("precision")) {   // 0: float64, 1: mixed (float32 bulk, float64 HEVI solve / deviations / sums)
+    double pr;
+    TRY(scalar(T, "precision", pr));
+    if (pr != 0.0 && pr != 1.0) return fail(NC_ERR_ARG, "precision must be 0 (float64) or 1 (mixed)");
+    h->mixed = (pr == 1.0);
+  }
   recip_pair(C.rscale, C.rsc_h, C.rsc_l);
   recip_pair(3.0, C.third_h, C.third_l);
   TRY(scalar(T, "dtl", h->dtl)); TRY(scalar(T, "dts", h->dts));
@@ -1293,6 +1469,12 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
       if (numel(src[n])) CU(cudaMemcpy(*dst[n], src[n]->data, numel(src[n]) * sizeof(long long), cudaMemcpyHostToDevice));
     }
   }
+  if (h->mixed) {
+    if (h->trcadv || h->hist || h->hs_lat)
+      return fail(NC_ERR_ARG, "the mixed-precision form runs the dynamics step only (no TRCADV, Held-Suarez "
+                              "forcing or history diagnostics set-up)");
+    TRY(make_f32_geometry(h));
+  }
   // state and work fields
   char nm[32];
   const char* pn[6] = {"RHOG", "RHOGVX", "RHOGVY", "RHOGVZ", "RHOGW", "RHOGE"};
@@ -1301,7 +1483,7 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   for (int v = 0; v < 6; ++v) { snprintf(nm, sizeof nm, "PROG0.%d", v); TRY(field(h, h->P0[v], nm)); }
   TRY(field(h, h->pre, "pre")); TRY(field(h, h->tem, "tem")); TRY(field(h, h->vx, "vx")); TRY(field(h, h->vy, "vy"));
   TRY(field(h, h->vz, "vz")); TRY(field(h, h->w, "w")); TRY(field(h, h->rho, "rho")); TRY(field(h, h->ein, "ein"));
-  TRY(field(h, h->eth, "eth")); TRY(field(h, h->pregd, "pregd")); TRY(field(h, h->rhogd, "rhogd"));
+  TRY(field(h, h->eth, "eth")); TRY(field(h, h->pregd, "pregd", true)); TRY(field(h, h->rhogd, "rhogd", true));
   for (int d = 0; d < 3; ++d) { snprintf(nm, sizeof nm, "vv.%d", d); TRY(field(h, h->vv[d], nm)); }
   for (int d = 0; d < 4; ++d) { snprintf(nm, sizeof nm, "gadv.%d", d); TRY(field(h, h->gadv[d], nm)); }
   for (int n = 0; n < 6; ++n) {
@@ -1320,7 +1502,7 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
     snprintf(nm, sizeof nm, "gq.%d", d); TRY(field(h, h->gq[d], nm));
     snprintf(nm, sizeof nm, "qa.%d", d); TRY(field(h, h->qa[d], nm));
   }
-  TRY(field(h, h->Mc, "Mc")); TRY(field(h, h->Mu, "Mu")); TRY(field(h, h->Ml, "Ml"));
+  TRY(field(h, h->Mc, "Mc", true)); TRY(field(h, h->Mu, "Mu", true)); TRY(field(h, h->Ml, "Ml", true));
   TRY(field(h, h->ethtot0, "ethtot0"));
   TRY(field(h, h->flx_v, "flx_v")); TRY(field(h, h->rhog_t, "rhog_t")); TRY(field(h, h->q, "q"));
   TRY(field(h, h->Qmin, "Qmin")); TRY(field(h, h->Qmax, "Qmax"));
@@ -1407,12 +1589,6 @@ void nc_destroy(nc_handle* h) {
   delete h;
 }
 
-static VarPtrs state_ptrs(nc_handle* h, bool pole) {
-  VarPtrs v{};
-  for (int n = 0; n < 6; ++n) v.v[n] = pole ? h->P[n].p : h->P[n].r;
-  for (int n = 0; n < h->D.nq; ++n) v.v[6 + n] = pole ? h->Pq[n].p : h->Pq[n].r;
-  return v;
-}
 
 int nc_upload_state(nc_handle* h, const double* prg, const double* prg_pl) {
   if (!h || !prg || !prg_pl) return fail(NC_ERR_ARG, "nc_upload_state: null argument");
@@ -1426,11 +1602,7 @@ int nc_upload_state(nc_handle* h, const double* prg, const double* prg_pl) {
   CU(cudaMemcpyAsync(h->stage_pl, prg_pl, (size_t)D.npl * nv * sizeof(double), cudaMemcpyHostToDevice, h->s_h2d));
   CU(cudaEventRecord(h->ev_in_ready, h->s_h2d));
   CU(cudaStreamWaitEvent(h->stream, h->ev_in_ready, 0));
-  const dim3 gt((unsigned)((D.G + UI - 1) / UI), (unsigned)((D.L * nv + UC - 1) / UC), (unsigned)(D.G * D.KA));
-  k_unpack_t<<<gt, 256, 0, h->stream>>>(h->stage, state_ptrs(h, false), nv);
-  TRY(check_launch(h, "unpack"));
-  k_unpack_pl<<<(unsigned)((D.npl + 127) / 128), 128, 0, h->stream>>>(h->stage_pl, state_ptrs(h, true), nv);
-  TRY(check_launch(h, "unpack_pl"));
+  TRY(h->mixed ? unpack_state<float>(h, h->stage, h->stage_pl) : unpack_state<double>(h, h->stage, h->stage_pl));
   CU(cudaEventRecord(h->ev_in_free, h->stream));
   h->have_state = true;
   return 0;
@@ -1449,11 +1621,8 @@ static int download_issue(nc_handle* h, double* prg, double* prg_pl) {
   CU(cudaStreamWaitEvent(h->stream, h->ev_out_done, 0));   // the previous download has left the buffer
   const dim3 gt((unsigned)((D.G + UI - 1) / UI), (unsigned)((D.L * nv + UC - 1) / UC), (unsigned)(D.G * D.KA));
   TRY(reset_bad(h, h->stream));
-  k_pack_t<<<gt, 256, 0, h->stream>>>(h->stage_out, state_ptrs(h, false), nv, h->bad);
-  TRY(check_launch(h, "pack"));
-  k_pack_pl<<<(unsigned)((D.npl + 127) / 128), 128, 0, h->stream>>>(h->stage_out_pl, state_ptrs(h, true), nv,
-                                                                    h->bad);
-  TRY(check_launch(h, "pack_pl"));
+  TRY(h->mixed ? pack_state<float>(h, h->stage_out, h->stage_out_pl)
+               : pack_state<double>(h, h->stage_out, h->stage_out_pl));
   CU(cudaEventRecord(h->ev_out_ready, h->stream));
   CU(cudaStreamWaitEvent(h->s_d2h, h->ev_out_ready, 0));
   CU(cudaMemcpyAsync(prg, h->stage_out, (size_t)D.npt * nv * sizeof(double), cudaMemcpyDeviceToHost, h->s_d2h));
@@ -1486,10 +1655,8 @@ int nc_check_finite(nc_handle* h) {
   if (!h) return fail(NC_ERR_ARG, "nc_check_finite: null handle");
   if (!h->have_state) return fail(NC_ERR_STATE, "nc_check_finite: no state uploaded");
   TRY(load_consts(h));
-  const int nv = 6 + h->D.nq;
   TRY(reset_bad(h, h->stream));
-  k_finite<<<4 * 148, 256, 0, h->stream>>>(state_ptrs(h, false), state_ptrs(h, true), nv, h->bad);
-  TRY(check_launch(h, "finite"));
+  TRY(h->mixed ? finite_state<float>(h) : finite_state<double>(h));
   CU(cudaMemcpyAsync(h->bad_host, h->bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->stream));
   return bad_status(h, "nc_check_finite");
@@ -1512,14 +1679,8 @@ static int before_caller(nc_handle* h, void* stream) {
 int nc_upload_state_device(nc_handle* h, const double* prg, const double* prg_pl, void* stream) {
   if (!h || !prg || !prg_pl) return fail(NC_ERR_ARG, "nc_upload_state_device: null argument");
   TRY(load_consts(h));
-  const Dims& D = h->D;
-  const int nv = 6 + D.nq;
   TRY(after_caller(h, stream));
-  const dim3 gt((unsigned)((D.G + UI - 1) / UI), (unsigned)((D.L * nv + UC - 1) / UC), (unsigned)(D.G * D.KA));
-  k_unpack_t<<<gt, 256, 0, h->stream>>>(prg, state_ptrs(h, false), nv);
-  TRY(check_launch(h, "unpack"));
-  k_unpack_pl<<<(unsigned)((D.npl + 127) / 128), 128, 0, h->stream>>>(prg_pl, state_ptrs(h, true), nv);
-  TRY(check_launch(h, "unpack_pl"));
+  TRY(h->mixed ? unpack_state<float>(h, prg, prg_pl) : unpack_state<double>(h, prg, prg_pl));
   TRY(before_caller(h, stream));
   h->have_state = true;
   return 0;
@@ -1529,15 +1690,9 @@ int nc_download_state_device(nc_handle* h, double* prg, double* prg_pl, void* st
   if (!h || !prg || !prg_pl) return fail(NC_ERR_ARG, "nc_download_state_device: null argument");
   if (!h->have_state) return fail(NC_ERR_STATE, "nc_download_state_device: no state uploaded");
   TRY(load_consts(h));
-  const Dims& D = h->D;
-  const int nv = 6 + D.nq;
   TRY(after_caller(h, stream));
   TRY(reset_bad(h, h->stream));
-  const dim3 gt((unsigned)((D.G + UI - 1) / UI), (unsigned)((D.L * nv + UC - 1) / UC), (unsigned)(D.G * D.KA));
-  k_pack_t<<<gt, 256, 0, h->stream>>>(prg, state_ptrs(h, false), nv, h->bad);
-  TRY(check_launch(h, "pack"));
-  k_pack_pl<<<(unsigned)((D.npl + 127) / 128), 128, 0, h->stream>>>(prg_pl, state_ptrs(h, true), nv, h->bad);
-  TRY(check_launch(h, "pack_pl"));
+  TRY(h->mixed ? pack_state<float>(h, prg, prg_pl) : pack_state<double>(h, prg, prg_pl));
   return before_caller(h, stream);
 }
 
@@ -1568,7 +1723,7 @@ int nc_step(nc_handle* h, int32_t nsteps) {
   if (!h->use_graph || h->prof) {
     for (int n = 0; n < nsteps; ++n) {
       if (h->prof) h->ev_used = 0;
-      TRY(run_step(h));
+      TRY(step_once(h));
       if (h->prof) TRY(collect_profile(h));
     }
     return 0;
@@ -1576,7 +1731,7 @@ int nc_step(nc_handle* h, int32_t nsteps) {
   if (!h->gexec) {
     long long before = h->launches;
     CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = run_step(h);
+    int rc = step_once(h);
     cudaGraph_t g = nullptr;
     cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
     if (rc) {
@@ -1612,7 +1767,7 @@ int nc_run_phases(nc_handle* h, int32_t nphases) {
   if (!h->have_state) return fail(NC_ERR_STATE, "nc_run_phases: no state uploaded");
   TRY(load_consts(h));
   h->stop_phase = nphases;
-  int rc = run_step(h);
+  int rc = step_once(h);
   h->stop_phase = 0;
   if (rc) return rc;
   CU(cudaStreamSynchronize(h->stream));
@@ -1633,10 +1788,7 @@ int nc_mass_sums(nc_handle* h, double* out, int32_t nout) {
   TRY(load_consts(h));
   std::vector<double> part((size_t)h->mass_blocks * 2);
   for (int n = 0; n < nout && n <= h->D.nq; ++n) {
-    const double* num = n == 0 ? nullptr : h->Pq[n - 1].r;
-    const double* nump = n == 0 ? nullptr : h->Pq[n - 1].p;
-    k_mass<<<h->mass_blocks, 256, 0, h->stream>>>(h->P[0].r, num, h->vol, h->P[0].p, nump, h->vol_pl, h->mass_part);
-    TRY(check_launch(h, "mass"));
+    TRY(h->mixed ? mass_sum<float>(h, n) : mass_sum<double>(h, n));
     CU(cudaMemcpyAsync(part.data(), h->mass_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
     double S = 0.0, Cc = 0.0;
@@ -1660,21 +1812,37 @@ int nc_get_field(nc_handle* h, const char* name, double* host_reg, double* host_
   TRY(load_consts(h));
   const Dims& D = h->D;
   CU(cudaStreamSynchronize(h->stream));
+  const bool f32 = h->field_esize[name] == (int)sizeof(float);
   if (host_reg) {
     std::vector<double> tmp((size_t)D.npt);
-    CU(cudaMemcpy(tmp.data(), it->second.r, D.npt * sizeof(double), cudaMemcpyDeviceToHost));
+    if (f32) {
+      std::vector<float> tf((size_t)D.npt);
+      CU(cudaMemcpy(tf.data(), it->second.r, D.npt * sizeof(float), cudaMemcpyDeviceToHost));
+      for (size_t n = 0; n < tf.size(); ++n) tmp[n] = tf[n];
+    } else {
+      CU(cudaMemcpy(tmp.data(), it->second.r, D.npt * sizeof(double), cudaMemcpyDeviceToHost));
+    }
     for (int l = 0; l < D.L; ++l)
       for (int k = 0; k < D.KA; ++k)
         for (int j = 0; j < D.G; ++j)
           for (int i = 0; i < D.G; ++i)
             host_reg[(((size_t)i * D.G + j) * D.KA + k) * D.L + l] = tmp[(((size_t)l * D.KA + k) * D.G + j) * D.G + i];
   }
-  if (host_pl) CU(cudaMemcpy(host_pl, it->second.p, D.npl * sizeof(double), cudaMemcpyDeviceToHost));
+  if (host_pl) {
+    if (f32) {
+      std::vector<float> tf((size_t)D.npl);
+      CU(cudaMemcpy(tf.data(), it->second.p, D.npl * sizeof(float), cudaMemcpyDeviceToHost));
+      for (int n = 0; n < D.npl; ++n) host_pl[n] = tf[n];
+    } else {
+      CU(cudaMemcpy(host_pl, it->second.p, D.npl * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+  }
   return 0;
 }
 
 int nc_state_pointers(nc_handle* h, int32_t v, double** reg, double** pl) {
   if (!h || v < 0 || v >= 6 + h->D.nq || !reg || !pl) return fail(NC_ERR_ARG, "nc_state_pointers: bad argument");
+  TRY(f64_only(h, "nc_state_pointers"));
   FieldPair f = v < 6 ? h->P[v] : h->Pq[v - 6];
   *reg = f.r;
   *pl = f.p;
@@ -1822,6 +1990,7 @@ static int restart_field(nc_handle* h, int32_t var, double** f) {
 
 int nc_restart_pack(nc_handle* h, int32_t var, void* host) {
   if (!h || !host) return fail(NC_ERR_ARG, "nc_restart_pack: null argument");
+  TRY(f64_only(h, "nc_restart_pack"));
   if (!h->have_state) return fail(NC_ERR_STATE, "nc_restart_pack: no state uploaded");
   double* f;
   TRY(restart_field(h, var, &f));
@@ -1838,6 +2007,7 @@ int nc_restart_pack(nc_handle* h, int32_t var, void* host) {
 
 int nc_restart_unpack(nc_handle* h, int32_t var, const void* host) {
   if (!h || !host) return fail(NC_ERR_ARG, "nc_restart_unpack: null argument");
+  TRY(f64_only(h, "nc_restart_unpack"));
   double* f;
   TRY(restart_field(h, var, &f));
   TRY(load_consts(h));
@@ -1859,6 +2029,7 @@ int nc_restart_unpack(nc_handle* h, int32_t var, const void* host) {
 
 int nc_restart_finish(nc_handle* h, const int64_t* pole_src, int32_t nsrc) {
   if (!h || (nsrc > 0 && !pole_src) || nsrc < 0 || nsrc > 64) return fail(NC_ERR_ARG, "nc_restart_finish: bad argument");
+  TRY(f64_only(h, "nc_restart_finish"));
   TRY(load_consts(h));
   const Dims& D = h->D;
   PoleSrc ps{};
@@ -1870,7 +2041,7 @@ int nc_restart_finish(nc_handle* h, const int64_t* pole_src, int32_t nsrc) {
       return fail(NC_ERR_ARG, "nc_restart_finish: pole source entry out of range");
     for (int c = 0; c < 5; ++c) ps.e[e][c] = (int)r[c];
   }
-  VarPtrs reg{}, pol{};
+  VarPtrs<double> reg{}, pol{};
   const int nv = 6 + D.nq;
   for (int v = 0; v < nv; ++v) {
     reg.v[v] = v < 6 ? h->P[v].r : h->Pq[v - 6].r;
@@ -1880,7 +2051,7 @@ int nc_restart_finish(nc_handle* h, const int64_t* pole_src, int32_t nsrc) {
     k_pole_centre<<<(unsigned)((nsrc * D.KA + 127) / 128), 128, 0, h->stream>>>(reg, pol, nv, ps);
     TRY(check_launch(h, "restart_pole_centre"));
   }
-  TRY(comm_prg(h));
+  TRY(comm_prg<double>(h));
   TRY(join_pl(h));
   CU(cudaStreamSynchronize(h->stream));
   h->have_state = true;
@@ -1891,6 +2062,7 @@ int nc_history_vars(nc_handle* h, const int32_t* items, int32_t nitems, int64_t 
                     double* const* out) {
   if (!h || (nitems > 0 && (!items || !out)) || nitems < 0 || nitems > H_N)
     return fail(NC_ERR_ARG, "nc_history_vars: bad argument");
+  TRY(f64_only(h, "nc_history_vars"));
   if (!h->hist)
     return fail(NC_ERR_STATE, "nc_history_vars: the handle was created without the HIST_* setup entries");
   if (!h->have_state) return fail(NC_ERR_STATE, "nc_history_vars: no state uploaded");
@@ -1960,7 +2132,7 @@ int nc_history_vars(nc_handle* h, const int32_t* items, int32_t nitems, int64_t 
   for (int n = 0; n < nitems; ++n) {
     const int it = items[n];
     if (it < H_N3) {
-      VarPtrs vp{};
+      VarPtrs<double> vp{};
       vp.v[0] = h->hist_out[it];
       const dim3 gt((unsigned)((D.G + UI - 1) / UI), (unsigned)((D.L + UC - 1) / UC), (unsigned)(D.G * D.KA));
       k_pack_t<<<gt, 256, 0, s>>>(h->stage_out, vp, 1, h->bad);   // the finiteness note is not read here

@@ -1,6 +1,6 @@
 // Device data model of the NICAM-DC dynamics step on one B200.
 //
-// Regional fields: one float64 array per variable, layout [l][k][j][i] with i
+// Regional fields: one array per variable, layout [l][k][j][i] with i
 // fastest (the Fortran/fio (gall, kall, lall) order, ij = j*gall_1d + i), so a
 // warp of threads on consecutive i issues coalesced 128-byte loads and the
 // 7-point hexagonal stencil touches rows j-1, j, j+1 of the same k-plane.
@@ -11,9 +11,13 @@
 // walks k, so k-independent coefficients are loaded once into registers and
 // the vertical recurrences (Thomas solve, limiter) stay in registers.
 //
-// All arithmetic follows the float64 numpy reference op-for-op (same
-// association order, no FMA contraction: the library is built -fmad=false),
-// which is what makes the CUDA step bit-identical to the reference.
+// Two forms of every kernel, selected per handle: float64 (R = double) and
+// the mixed form (R = float: float32 fields, metrics and arithmetic, with the
+// Thomas elimination, the pressure / density deviations and the mass sums in
+// float64).  The float64 arithmetic follows the numpy reference op-for-op
+// (same association order, no FMA contraction: the library is built
+// -fmad=false), which is what makes the float64 step bit-identical to the
+// reference.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -40,69 +44,100 @@ struct Dims {
 };
 
 // Physical / run constants (identical names to the reference's CONST_*).
-struct Consts {
-  double GRAV, Rdry, CVdry, CPdry, Rvap, OHM, EPS, HUGE_, rscale, alpha;
-  double Kh, divdamp_coef, hdiff_fact_rho, CVW0, PRE00;
+// R is the arithmetic type of the kernels that read them: the float64 form
+// uses ConstsT<double> (cC) throughout; the mixed form loads a float copy
+// (cCf) for its float32 kernels and keeps cC for its float64 parts.
+template <class R>
+struct ConstsT {
+  R GRAV, Rdry, CVdry, CPdry, Rvap, OHM, EPS, HUGE_, rscale, alpha;
+  R Kh, divdamp_coef, hdiff_fact_rho, CVW0, PRE00;
   int gam_unit;   // RGAM, RGAMH and GAM2H are 1 everywhere (shallow atmosphere)
   // rounded reciprocals and their tails, RN(1/b) and RN(1/b - RN(1/b)), of the
   // divisors rscale and 3 (see div_by)
-  double rsc_h, rsc_l, third_h, third_l;
-  double afact[NC_MAXK], bfact[NC_MAXK], cfact[NC_MAXK], dfact[NC_MAXK];
-  double rdgz[NC_MAXK], rdgzh[NC_MAXK];
+  R rsc_h, rsc_l, third_h, third_l;
+  R afact[NC_MAXK], bfact[NC_MAXK], cfact[NC_MAXK], dfact[NC_MAXK];
+  R rdgz[NC_MAXK], rdgzh[NC_MAXK];
 };
+using Consts = ConstsT<double>;
 
-// Geometry on the device (all float64).  Regional 3-D metrics [l][k][j][i];
-// 2-D coefficient planes [c][l][j][i].  Pole arrays in reference layout.
-struct Geom {
+// Geometry on the device.  Regional 3-D metrics [l][k][j][i]; 2-D coefficient
+// planes [c][l][j][i].  Pole arrays in reference layout.  GeomT<double> (cG)
+// holds the float64 arrays; the mixed form stores a float32 copy of every
+// array (GeomT<float>, cGf) and its kernels read that one.
+template <class R>
+struct GeomT {
   // 3-D vertical metrics
-  const double *GSGAM2, *GSGAM2H, *RGSGAM2, *RGSGAM2H, *RGSQRTH, *RGAM, *RGAMH, *GAM2H, *PHI;
-  const double *C2W;     // 2 comps
-  const double *W2C;     // 2 comps
-  const double *C2WGz;   // 6 comps
-  const double *rho_bs, *pre_bs, *tem_bs;
+  const R *GSGAM2, *GSGAM2H, *RGSGAM2, *RGSGAM2H, *RGSQRTH, *RGAM, *RGAMH, *GAM2H, *PHI;
+  const R *C2W;     // 2 comps
+  const R *W2C;     // 2 comps
+  const R *C2WGz;   // 6 comps
+  const R *rho_bs, *pre_bs, *tem_bs;
   // 2-D horizontal coefficients
-  const double *coef_div;   // 21 planes (d*7+m)
-  const double *coef_grad;  // 21 planes
-  const double *coef_lap;   // 7
-  const double *coef_intp;  // 18 planes ((d*3+p)*2+t)
-  const double *intp_w;     // 18 planes ((d*3+m)*2+t): the diffusion's vertex weights formed from coef_intp
-  const double *coef_diff;  // 18 planes (d*6+m)
-  const double *GRD_x;      // 3
-  const double *GRD_xr;     // 9 (face*3+d)
-  const double *GMTR_t;     // 6 (t*3 + (W-2))
-  const double *GMTR_a;     // 9 (face*3 + HN)
-  const double *GMTR_p;     // 1 (P_RAREA)
-  const int *pntmask;       // [l][2]
-  const int *have_sgp;      // [l]
+  const R *coef_div;   // 21 planes (d*7+m)
+  const R *coef_grad;  // 21 planes
+  const R *coef_lap;   // 7
+  const R *coef_intp;  // 18 planes ((d*3+p)*2+t)
+  const R *intp_w;     // 18 planes ((d*3+m)*2+t): the diffusion's vertex weights formed from coef_intp
+  const R *coef_diff;  // 18 planes (d*6+m)
+  const R *GRD_x;      // 3
+  const R *GRD_xr;     // 9 (face*3+d)
+  const R *GMTR_t;     // 6 (t*3 + (W-2))
+  const R *GMTR_a;     // 9 (face*3 + HN)
+  const R *GMTR_p;     // 1 (P_RAREA)
+  const int *pntmask;  // [l][2]
+  const int *have_sgp; // [l]
   // pole (reference layouts)
-  const double *GSGAM2_pl, *GSGAM2H_pl, *RGSGAM2_pl, *RGSGAM2H_pl, *RGSQRTH_pl, *RGAM_pl, *RGAMH_pl,
+  const R *GSGAM2_pl, *GSGAM2H_pl, *RGSGAM2_pl, *RGSGAM2H_pl, *RGSQRTH_pl, *RGAM_pl, *RGAMH_pl,
       *GAM2H_pl, *PHI_pl;
-  const double *C2W_pl, *W2C_pl, *C2WGz_pl;   // (g,k,l,c)
-  const double *rho_bs_pl, *pre_bs_pl, *tem_bs_pl;
-  const double *coef_div_pl;   // (g,l,3)
-  const double *coef_grad_pl;  // (g,l,3)
-  const double *coef_lap_pl;   // (g,l)
-  const double *coef_intp_pl;  // (g,l,3,3)
-  const double *coef_diff_pl;  // (g,l,3)
-  const double *GRD_x_pl;      // (g,l,3)
-  const double *GRD_xr_pl;     // (g,l,3)
-  const double *GMTR_t_pl;     // (g,l,5)
-  const double *GMTR_a_pl;     // (g,l,18)
-  const double *GMTR_p_pl;     // (g,l,8)
+  const R *C2W_pl, *W2C_pl, *C2WGz_pl;   // (g,k,l,c)
+  const R *rho_bs_pl, *pre_bs_pl, *tem_bs_pl;
+  const R *coef_div_pl;   // (g,l,3)
+  const R *coef_grad_pl;  // (g,l,3)
+  const R *coef_lap_pl;   // (g,l)
+  const R *coef_intp_pl;  // (g,l,3,3)
+  const R *coef_diff_pl;  // (g,l,3)
+  const R *GRD_x_pl;      // (g,l,3)
+  const R *GRD_xr_pl;     // (g,l,3)
+  const R *GMTR_t_pl;     // (g,l,5)
+  const R *GMTR_a_pl;     // (g,l,18)
+  const R *GMTR_p_pl;     // (g,l,8)
 };
+using Geom = GeomT<double>;
 
 // The library is one translation unit (nc_api.cu includes every kernel
 // header), so the constant-memory symbols are defined here.
 __constant__ Dims cD;
 __constant__ Consts cC;
 __constant__ Geom cG;
+__constant__ ConstsT<float> cCf;
+__constant__ GeomT<float> cGf;
+
+// a non-deduced context: a parameter of type Id<R>::type converts to R
+// instead of taking part in deducing R
+template <class T>
+struct Id {
+  using type = T;
+};
+
+// constants and geometry of arithmetic / storage type R
+template <class R> __device__ __forceinline__ const ConstsT<R>& consts();
+template <> __device__ __forceinline__ const ConstsT<double>& consts<double>() { return cC; }
+template <> __device__ __forceinline__ const ConstsT<float>& consts<float>() { return cCf; }
+template <class R> __device__ __forceinline__ const GeomT<R>& geom();
+template <> __device__ __forceinline__ const GeomT<double>& geom<double>() { return cG; }
+template <> __device__ __forceinline__ const GeomT<float>& geom<float>() { return cGf; }
+// inside a kernel templated on R
+#define CC (consts<R>())
+#define CG (geom<R>())
 
 // The gamma factors of the vertical metrics: RGAM, RGAMH, GAM2H (regional or
 // pole) at index p.  With a shallow atmosphere every value is exactly 1 (the
 // host checks each element at set-up and sets gam_unit); the factor is then
 // not loaded, and x * 1.0 == x leaves every product bit-for-bit unchanged.
-__device__ __forceinline__ double gam_at(const double* a, int p) { return cC.gam_unit ? 1.0 : a[p]; }
-__device__ __forceinline__ double gam_at_ldg(const double* a, int p) { return cC.gam_unit ? 1.0 : __ldg(a + p); }
+template <class R>
+__device__ __forceinline__ R gam_at(const R* a, int p) { return cC.gam_unit ? R(1) : a[p]; }
+template <class R>
+__device__ __forceinline__ R gam_at_ldg(const R* a, int p) { return cC.gam_unit ? R(1) : __ldg(a + p); }
 
 // x / b for a divisor fixed before the launch, with the same bits as the IEEE
 // division x / b for finite x whose quotient is in the normal range.  From
@@ -142,6 +177,17 @@ __device__ __forceinline__ Recip recip_of(double b) {
 }
 __device__ __forceinline__ double div_by(double x, const Recip& r) { return div_by(x, r.b, r.h, r.l); }
 
+// The float32 forms used by the mixed-precision kernels: a multiplication by
+// the rounded reciprocal (within 1.5 ulp of the quotient; the float32 kernels
+// are not bit-for-bit with anything, so the correction step is left out).
+__device__ __forceinline__ float div_r(float x) { return x * cCf.rsc_h; }
+__device__ __forceinline__ float div3(float x) { return x * cCf.third_h; }
+struct RecipF {
+  float h;
+};
+__device__ __forceinline__ RecipF recip_of(float b) { return RecipF{__frcp_rn(b)}; }
+__device__ __forceinline__ float div_by(float x, const RecipF& r) { return x * r.h; }
+
 // ---- indexing -------------------------------------------------------------
 __device__ __forceinline__ int ix(int i, int j, int k, int l) {
   return ((l * cD.KA + k) * cD.G + j) * cD.G + i;
@@ -153,13 +199,15 @@ __device__ __forceinline__ int ix2(int c, int i, int j, int l) {
 }
 // pole (g, k, l)
 __device__ __forceinline__ int ipl(int g, int k, int lp) { return (g * cD.KA + k) * cD.LP + lp; }
-__device__ __forceinline__ double P2(const double* a, int c, int i, int j, int l) { return a[ix2(c, i, j, l)]; }
+template <class R>
+__device__ __forceinline__ R P2(const R* a, int c, int i, int j, int l) { return a[ix2(c, i, j, l)]; }
 // the same through the read-only (non-coherent) path: the planes are constant
 // after set-up, and the compiler may batch these loads ahead of shared-memory
 // stores.  Used where that measured faster (path 1, 3-D divergence damping,
 // tracer horizontal flux); where it raised register pressure into spills
 // (momentum advection, vp0 horizontal terms) the plain load is kept.
-__device__ __forceinline__ double P2c(const double* a, int c, int i, int j, int l) { return __ldg(a + ix2(c, i, j, l)); }
+template <class R>
+__device__ __forceinline__ R P2c(const R* a, int c, int i, int j, int l) { return __ldg(a + ix2(c, i, j, l)); }
 
 // 7-point neighbour offsets in the reference's coefficient order:
 // (i,j) (i+1,j) (i+1,j+1) (i,j+1) (i-1,j) (i-1,j-1) (i,j-1)

@@ -7,7 +7,7 @@ namespace nc {
 
 // Held & Suarez (1994) dry-case parameters (nhm/forcing/mod_af_heldsuarez.py:19-36)
 struct HsArgs {
-  Prog P;                 // PROG, updated in place
+  Prog<double> P;         // PROG, updated in place
   const double* Pq0;      // first tracer (water vapour) for the diagnostics
   const double* lat3;     // planes |sin lat|^2, |cos lat|^2, |cos lat|^4 of each column
   double dt, RdCp;        // large time step; Rdry / CPdry
@@ -91,7 +91,7 @@ namespace nc {
 // can differ from numpy's in the last bits.
 // ---------------------------------------------------------------------------
 struct TrcWindArgs {
-  Prog P;                     // RHOGV{X,Y,Z}, RHOGW set to wind * RHOG
+  Prog<double> P;                    // RHOGV{X,Y,Z}, RHOGW set to wind * RHOG
   const double *lon, *lat;    // column longitude / latitude: regional [l][j][i], pole [g][l]
   const double *zf, *zh;      // full / half-level height: regional [l][k][j][i], pole [g][k][l]
   const double* time;         // model time of the winds (device scalar)

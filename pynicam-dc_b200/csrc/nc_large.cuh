@@ -6,7 +6,8 @@
 namespace nc {
 
 // Field bundles (device pointers, one array per variable)
-struct Prog { double* v[6]; };   // RHOG, RHOGVX, RHOGVY, RHOGVZ, RHOGW, RHOGE
+template <class R>
+struct Prog { R* v[6]; };   // RHOG, RHOGVX, RHOGVY, RHOGVZ, RHOGW, RHOGE
 
 // ---------------------------------------------------------------------------
 // Pre_Post: diagnostics (kernels/diag.py:53-143), BNDCND_all
@@ -15,16 +16,19 @@ struct Prog { double* v[6]; };   // RHOG, RHOGVX, RHOGVY, RHOGVZ, RHOGW, RHOGE
 // momentum advection (kernels/advconvmom.py:54-78).  One thread per column,
 // regional and pole columns alike.
 // ---------------------------------------------------------------------------
+template <class R>
 struct DiagArgs {
-  Prog P;               // in/out (ghost rows written)
-  const double* Pq0;    // first tracer (water vapour)
-  double *pre, *tem, *vx, *vy, *vz, *w, *rho, *ein, *eth, *pregd, *rhogd;
-  double *vvx, *vvy, *vvz;
+  Prog<R> P;            // in/out (ghost rows written)
+  const R* Pq0;         // first tracer (water vapour)
+  R *pre, *tem, *vx, *vy, *vz, *w, *rho, *ein, *eth;
+  double *pregd, *rhogd;   // float64 in both forms
+  R *vvx, *vvy, *vvz;
 };
 
-__device__ void diag_column(const Col c, const Met m, const DiagArgs& a, double gx, double gy, double gz) {
+template <class R>
+__device__ void diag_column(const Col c, const MetT<R> m, const DiagArgs<R>& a, double gx, double gy, double gz) {
   const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
-  double** P = const_cast<double**>(a.P.v);
+  R** P = const_cast<R**>(a.P.v);
   for (int k = 0; k < KA; ++k) {
     int p = c.at(k);
     double RHOG = P[0][p];
@@ -72,7 +76,7 @@ __device__ void diag_column(const Col c, const Met m, const DiagArgs& a, double 
     P[1 + d][pT] = vT[d];
     P[1 + d][pB] = vB[d];
   }
-  double* dv[3] = {a.vx, a.vy, a.vz};
+  R* dv[3] = {a.vx, a.vy, a.vz};
   for (int d = 0; d < 3; ++d) {
     dv[d][pT] = P[1 + d][pT] / P[0][pT];
     dv[d][pB] = P[1 + d][pB] / P[0][pB];
@@ -111,9 +115,10 @@ __device__ void diag_column(const Col c, const Met m, const DiagArgs& a, double 
 // values carried in registers.  The four levels next to and on the boundary
 // rows are finished after the boundary conditions, as in diag_column.  Same
 // expressions, same results.
-__device__ void diag_column_fused(const Col c, const Met m, const DiagArgs& a, double gx, double gy, double gz) {
+template <class R>
+__device__ void diag_column_fused(const Col c, const MetT<R> m, const DiagArgs<R>& a, double gx, double gy, double gz) {
   const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
-  double** P = const_cast<double**>(a.P.v);
+  R** P = const_cast<R**>(a.P.v);
   auto finish = [&](int k, int p, double pre, double rho, double ein, double vxk, double vyk, double vzk,
                     double wk, double wk1) {
     a.eth[p] = ein + pre / rho;
@@ -134,7 +139,7 @@ __device__ void diag_column_fused(const Col c, const Met m, const DiagArgs& a, d
     int p = c.at(k);
     double RHOG = P[0][p];
     double rho = RHOG / m.GSGAM2[p];
-    const Recip rr = recip_of(RHOG);   // five quotients by RHOG
+    const auto rr = recip_of(RHOG);   // five quotients by RHOG
     const double vx = div_by(P[1][p], rr), vy = div_by(P[2][p], rr), vz = div_by(P[3][p], rr);
     a.vx[p] = vx;
     a.vy[p] = vy;
@@ -184,7 +189,7 @@ __device__ void diag_column_fused(const Col c, const Met m, const DiagArgs& a, d
     P[1 + d][pT] = vT[d];
     P[1 + d][pB] = vB[d];
   }
-  double* dv[3] = {a.vx, a.vy, a.vz};
+  R* dv[3] = {a.vx, a.vy, a.vz};
   for (int d = 0; d < 3; ++d) {
     dv[d][pT] = P[1 + d][pT] / P[0][pT];
     dv[d][pB] = P[1 + d][pB] / P[0][pB];
@@ -211,17 +216,18 @@ __device__ void diag_column_fused(const Col c, const Met m, const DiagArgs& a, d
 
 // eight 128-thread blocks per SM (64 registers): measured faster than the
 // uncapped 84 registers
-__global__ void __launch_bounds__(128, 8) k_diag(DiagArgs a, int pole) {
+template <class R>
+__global__ void __launch_bounds__(128, 8) k_diag(DiagArgs<R> a, int pole) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
   if (!pole) {
-    diag_column_fused(col_reg(i, j, l), met_of(false), a, P2(cG.GRD_x, 0, i, j, l), P2(cG.GRD_x, 1, i, j, l),
-                      P2(cG.GRD_x, 2, i, j, l));
+    diag_column_fused(col_reg(i, j, l), met_of<R>(false), a, (double)P2(CG.GRD_x, 0, i, j, l),
+                      (double)P2(CG.GRD_x, 1, i, j, l), (double)P2(CG.GRD_x, 2, i, j, l));
   } else {
-    const double* X = cG.GRD_x_pl;
-    diag_column(col_pl(g, lp), met_of(true), a, X[(g * cD.LP + lp) * 3 + 0], X[(g * cD.LP + lp) * 3 + 1],
-                X[(g * cD.LP + lp) * 3 + 2]);
+    const R* X = CG.GRD_x_pl;
+    diag_column(col_pl(g, lp), met_of<R>(true), a, (double)X[(g * cD.LP + lp) * 3 + 0],
+                (double)X[(g * cD.LP + lp) * 3 + 1], (double)X[(g * cD.LP + lp) * 3 + 2]);
   }
 }
 
@@ -230,10 +236,11 @@ __global__ void __launch_bounds__(128, 8) k_diag(DiagArgs a, int pole) {
 // (mod_src.py:96-497, kernels/advconv.py:42-108, fluxconv.py:111-208,
 // advconvmom.py:111-194).  Outputs grhogv{x,y,z}, grhogw.
 // ---------------------------------------------------------------------------
+template <class R>
 struct AdvMomArgs {
-  const double *rg, *rvx, *rvy, *rvz, *rw;    // PROG (post BNDCND)
-  const double *vvx, *vvy, *vvz;              // merged velocity
-  double *gvx, *gvy, *gvz, *gw;               // out
+  const R *rg, *rvx, *rvy, *rvz, *rw;    // PROG (post BNDCND)
+  const R *vvx, *vvy, *vvz;              // merged velocity
+  R *gvx, *gvy, *gvz, *gw;               // out
 };
 
 // Tiled momentum advection for interior cells: one block per 32x8 tile of a
@@ -245,10 +252,11 @@ struct AdvMomArgs {
 // the large-step tendencies derived from them are replaced by the exchanges).
 // Arithmetic and association order are those of the reference's expressions
 // (kernels/advconv.py, kernels/advconvmom.py), as in the pole kernel.
-__global__ void __launch_bounds__(256, 2) k_advmom_t(AdvMomArgs a) {
+template <class R>
+__global__ void __launch_bounds__(256, 2) k_advmom_t(AdvMomArgs<R> a) {
   constexpr int TXD = 32, TYD = 8;
   constexpr int PX = TXD + 2, PY = TYD + 2;
-  __shared__ double s_rv[3][PY * PX], s_vv[3][PY * PX], s_rg[PY * PX];
+  __shared__ R s_rv[3][PY * PX], s_vv[3][PY * PX], s_rg[PY * PX];
   const int ntx = (cD.G - 2 + TXD - 1) / TXD;
   const int l = (int)blockIdx.z;
   const int i0 = 1 + ((int)blockIdx.x % ntx) * TXD, j0 = 1 + ((int)blockIdx.x / ntx) * TYD;
@@ -256,20 +264,20 @@ __global__ void __launch_bounds__(256, 2) k_advmom_t(AdvMomArgs a) {
   const int tid = threadIdx.x, tx = tid % TXD, ty = tid / TXD;
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= gmax) && (j <= gmax);
-  const double* rv[3] = {a.rvx, a.rvy, a.rvz};
-  const double* vv[3] = {a.vvx, a.vvy, a.vvz};
-  const double* cz = cG.C2WGz;
+  const R* rv[3] = {a.rvx, a.rvy, a.rvz};
+  const R* vv[3] = {a.vvx, a.vvy, a.vvz};
+  const R* cz = CG.C2WGz;
   const int n = cD.npti;
-  double gx = 0.0, gy = 0.0, gz = 0.0;
+  R gx = R(0.0), gy = R(0.0), gz = R(0.0);
   int q0 = 0;
   if (own) {
-    gx = div_r(P2(cG.GRD_x, 0, i, j, l));
-    gy = div_r(P2(cG.GRD_x, 1, i, j, l));
-    gz = div_r(P2(cG.GRD_x, 2, i, j, l));
+    gx = div_r(P2(CG.GRD_x, 0, i, j, l));
+    gy = div_r(P2(CG.GRD_x, 1, i, j, l));
+    gz = div_r(P2(CG.GRD_x, 2, i, j, l));
     q0 = ix(i, j, 0, l);
   }
-  double vmh_lo[3] = {0.0, 0.0, 0.0};
-  double gwc_prev = 0.0;
+  R vmh_lo[3] = {R(0.0), R(0.0), R(0.0)};
+  R gwc_prev = R(0.0);
   for (int k = kmin; k <= kmax; ++k) {
     for (int p = tid; p < PX * PY; p += blockDim.x) {
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
@@ -277,10 +285,10 @@ __global__ void __launch_bounds__(256, 2) k_advmom_t(AdvMomArgs a) {
       const int q = ok ? ix(ii, jj, k, l) : 0;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        s_rv[d][p] = ok ? rv[d][q] : 0.0;
-        s_vv[d][p] = ok ? vv[d][q] : 0.0;
+        s_rv[d][p] = ok ? rv[d][q] : R(0.0);
+        s_vv[d][p] = ok ? vv[d][q] : R(0.0);
       }
-      s_rg[p] = ok ? gam_at(cG.RGAM, q) : 0.0;
+      s_rg[p] = ok ? gam_at(CG.RGAM, q) : R(0.0);
     }
     __syncthreads();
     if (own) {
@@ -290,44 +298,44 @@ __global__ void __launch_bounds__(256, 2) k_advmom_t(AdvMomArgs a) {
       const int kk = k + 1;
       const bool hv = (kk > kmin && kk <= kmax);
       const int qh = p + cD.planei;   // level k+1 of the own column
-      double dv[3];
+      R dv[3];
 #pragma unroll
       for (int s = 0; s < 3; ++s) {
-        double acc[3];
+        R acc[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          double sm = 0.0;
+          R sm = R(0.0);
 #pragma unroll
           for (int m = 0; m < 7; ++m) {
-            const double v = (s_rv[d][nb[m]] * s_vv[s][nb[m]]) * s_rg[nb[m]];
-            const double t = P2(cG.coef_div, d * 7 + m, i, j, l) * v;
+            const R v = (s_rv[d][nb[m]] * s_vv[s][nb[m]]) * s_rg[nb[m]];
+            const R t = P2(CG.coef_div, d * 7 + m, i, j, l) * v;
             sm = (m == 0) ? t : sm + t;
           }
           acc[d] = sm;
         }
-        const double div = acc[0] + acc[1] + acc[2];
-        double vmh_hi = 0.0;
+        const R div = acc[0] + acc[1] + acc[2];
+        R vmh_hi = R(0.0);
         if (hv) {
-          const double sh = vv[s][qh], sl = s_vv[s][c0];
-          const double h = cz[qh] * (rv[0][qh] * sh) + cz[n + qh] * (s_rv[0][c0] * sl) +
+          const R sh = vv[s][qh], sl = s_vv[s][c0];
+          const R h = cz[qh] * (rv[0][qh] * sh) + cz[n + qh] * (s_rv[0][c0] * sl) +
                            cz[2 * n + qh] * (rv[1][qh] * sh) + cz[3 * n + qh] * (s_rv[1][c0] * sl) +
                            cz[4 * n + qh] * (rv[2][qh] * sh) + cz[5 * n + qh] * (s_rv[2][c0] * sl);
-          const double sw = a.rw[qh] * (cC.afact[kk] * sh + cC.bfact[kk] * sl);
-          vmh_hi = h * gam_at(cG.RGAMH, qh) + 1.0 * sw * cG.RGSQRTH[qh];
+          const R sw = a.rw[qh] * (CC.afact[kk] * sh + CC.bfact[kk] * sl);
+          vmh_hi = h * gam_at(CG.RGAMH, qh) + R(1.0) * sw * CG.RGSQRTH[qh];
         }
-        dv[s] = -div - (vmh_hi - vmh_lo[s]) * cC.rdgz[k];
+        dv[s] = -div - (vmh_hi - vmh_lo[s]) * CC.rdgz[k];
         vmh_lo[s] = vmh_hi;
       }
-      const double rh = a.rg[p];
-      const double dvx = dv[0] - (-2.0 * rh * (cC.OHM * s_vv[1][c0]));
-      const double dvy = dv[1] - (2.0 * rh * (cC.OHM * s_vv[0][c0]));
-      const double dvz = dv[2];
-      const double prd = dvx * gx + dvy * gy + dvz * gz;
+      const R rh = a.rg[p];
+      const R dvx = dv[0] - (-R(2.0) * rh * (CC.OHM * s_vv[1][c0]));
+      const R dvy = dv[1] - (R(2.0) * rh * (CC.OHM * s_vv[0][c0]));
+      const R dvz = dv[2];
+      const R prd = dvx * gx + dvy * gy + dvz * gz;
       a.gvx[p] = dvx - prd * gx;
       a.gvy[p] = dvy - prd * gy;
       a.gvz[p] = dvz - prd * gz;
-      const double gwc = prd * cC.alpha;
-      a.gw[p] = (k >= kmin + 1) ? (cG.C2W[p] * gwc + cG.C2W[n + p] * gwc_prev) : 0.0;
+      const R gwc = prd * CC.alpha;
+      a.gw[p] = (k >= kmin + 1) ? (CG.C2W[p] * gwc + CG.C2W[n + p] * gwc_prev) : R(0.0);
       gwc_prev = gwc;
     }
     __syncthreads();
@@ -335,66 +343,68 @@ __global__ void __launch_bounds__(256, 2) k_advmom_t(AdvMomArgs a) {
 }
 
 // pole part of the momentum advection (one thread per pole column (g, lp))
-__device__ double advconv_pl_at(int g, int lp, int k, const Col& c, const Met& m, const double* rvx,
-                                const double* rvy, const double* rvz, const double* rw, const double* scl) {
-  double div = 0.0;
+template <class R>
+__device__ R advconv_pl_at(int g, int lp, int k, const Col& c, const MetT<R>& m, const R* rvx,
+                                const R* rvy, const R* rvz, const R* rw, const R* scl) {
+  R div = R(0.0);
   if (g == 0) {
-    const double* cd = cG.coef_div_pl;
-    double row = 0.0;
+    const R* cd = CG.coef_div_pl;
+    R row = R(0.0);
     for (int v = 0; v < 6; ++v) {
       int q = ipl(v, k, lp);
-      double vx = (rvx[q] * scl[q]) * gam_at(cG.RGAM_pl, q);
-      double vy = (rvy[q] * scl[q]) * gam_at(cG.RGAM_pl, q);
-      double vz = (rvz[q] * scl[q]) * gam_at(cG.RGAM_pl, q);
-      double pv = cd[(v * cD.LP + lp) * 3 + 0] * vx + cd[(v * cD.LP + lp) * 3 + 1] * vy +
+      R vx = (rvx[q] * scl[q]) * gam_at(CG.RGAM_pl, q);
+      R vy = (rvy[q] * scl[q]) * gam_at(CG.RGAM_pl, q);
+      R vz = (rvz[q] * scl[q]) * gam_at(CG.RGAM_pl, q);
+      R pv = cd[(v * cD.LP + lp) * 3 + 0] * vx + cd[(v * cD.LP + lp) * 3 + 1] * vy +
                   cd[(v * cD.LP + lp) * 3 + 2] * vz;
       row = (v == 0) ? pv : row + pv;
     }
     div = row;
   }
-  auto vmh = [&](int kk) -> double {
-    if (kk <= cD.kmin || kk > cD.kmax) return 0.0;
-    double h = vmh_horiz(c, m, kk, [&](int k2, int d) -> double {
+  auto vmh = [&](int kk) -> R {
+    if (kk <= cD.kmin || kk > cD.kmax) return R(0.0);
+    R h = vmh_horiz(c, m, kk, [&](int k2, int d) -> R {
       int q = c.at(k2);
-      const double* rv = (d == 0) ? rvx : ((d == 1) ? rvy : rvz);
+      const R* rv = (d == 0) ? rvx : ((d == 1) ? rvy : rvz);
       return rv[q] * scl[q];
     });
     int q = c.at(kk);
-    double sw = rw[q] * (cC.afact[kk] * scl[q] + cC.bfact[kk] * scl[c.at(kk - 1)]);
-    return h + 1.0 * sw * m.RGSQRTH[q];
+    R sw = rw[q] * (CC.afact[kk] * scl[q] + CC.bfact[kk] * scl[c.at(kk - 1)]);
+    return h + R(1.0) * sw * m.RGSQRTH[q];
   };
-  return -div - (vmh(k + 1) - vmh(k)) * cC.rdgz[k];
+  return -div - (vmh(k + 1) - vmh(k)) * CC.rdgz[k];
 }
 
-__global__ void k_advmom_pl(AdvMomArgs a) {
+template <class R>
+__global__ void k_advmom_pl(AdvMomArgs<R> a) {
   int t = threadIdx.x;
   if (t >= 6 * cD.LP) return;
   int g = t / cD.LP, lp = t % cD.LP;
   const Col c = col_pl(g, lp);
-  const Met m = met_of(true);
-  const double* X = cG.GRD_x_pl;
-  const double gx = div_r(X[(g * cD.LP + lp) * 3 + 0]), gy = div_r(X[(g * cD.LP + lp) * 3 + 1]),
+  const MetT<R> m = met_of<R>(true);
+  const R* X = CG.GRD_x_pl;
+  const R gx = div_r(X[(g * cD.LP + lp) * 3 + 0]), gy = div_r(X[(g * cD.LP + lp) * 3 + 1]),
                gz = div_r(X[(g * cD.LP + lp) * 3 + 2]);
-  double gwc_prev = 0.0;
+  R gwc_prev = R(0.0);
   for (int k = 0; k < cD.KA; ++k) {
     int p = c.at(k);
     if (k < cD.kmin || k > cD.kmax) {
-      a.gvx[p] = 0.0; a.gvy[p] = 0.0; a.gvz[p] = 0.0; a.gw[p] = 0.0;
+      a.gvx[p] = R(0.0); a.gvy[p] = R(0.0); a.gvz[p] = R(0.0); a.gw[p] = R(0.0);
       continue;
     }
-    double dv[3];
-    const double* vv[3] = {a.vvx, a.vvy, a.vvz};
+    R dv[3];
+    const R* vv[3] = {a.vvx, a.vvy, a.vvz};
     for (int s = 0; s < 3; ++s) dv[s] = advconv_pl_at(g, lp, k, c, m, a.rvx, a.rvy, a.rvz, a.rw, vv[s]);
-    double rh = a.rg[p];
-    double dvx = dv[0] - (-2.0 * rh * (cC.OHM * a.vvy[p]));
-    double dvy = dv[1] - (2.0 * rh * (cC.OHM * a.vvx[p]));
-    double dvz = dv[2];
-    double prd = dvx * gx + dvy * gy + dvz * gz;
+    R rh = a.rg[p];
+    R dvx = dv[0] - (-R(2.0) * rh * (CC.OHM * a.vvy[p]));
+    R dvy = dv[1] - (R(2.0) * rh * (CC.OHM * a.vvx[p]));
+    R dvz = dv[2];
+    R prd = dvx * gx + dvy * gy + dvz * gz;
     a.gvx[p] = dvx - prd * gx;
     a.gvy[p] = dvy - prd * gy;
     a.gvz[p] = dvz - prd * gz;
-    double gwc = prd * cC.alpha;
-    a.gw[p] = (k >= cD.kmin + 1) ? (mc(m.C2W, c, 0, 2, k) * gwc + mc(m.C2W, c, 1, 2, k) * gwc_prev) : 0.0;
+    R gwc = prd * CC.alpha;
+    a.gw[p] = (k >= cD.kmin + 1) ? (mc(m.C2W, c, 0, 2, k) * gwc + mc(m.C2W, c, 1, 2, k) * gwc_prev) : R(0.0);
     gwc_prev = gwc;
   }
 }
@@ -404,26 +414,29 @@ __global__ void k_advmom_pl(AdvMomArgs a) {
 // Pass 1: vt = -lap(src), src = (vx, vy, vz, w, tem - tem_bs, rho - rho_bs).
 // Pass 2: vt2 = -(lap of comps 0..3, kh-weighted diffusion of comps 4, 5).
 // ---------------------------------------------------------------------------
-struct Six { const double* f[6]; };
-struct SixOut { double* f[6]; };
+template <class R>
+struct Six { const R* f[6]; };
+template <class R>
+struct SixOut { R* f[6]; };
 
-__global__ void k_hdiff1(Six src, SixOut out) {
+template <class R>
+__global__ void k_hdiff1(Six<R> src, SixOut<R> out) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
   const bool in = interior(i, j);
   // the column's seven laplacian coefficients, loaded once for all levels
-  double cl[7];
+  R cl[7];
 #pragma unroll
-  for (int m = 0; m < 7; ++m) cl[m] = in ? P2(cG.coef_lap, m, i, j, l) : 0.0;
+  for (int m = 0; m < 7; ++m) cl[m] = in ? P2(CG.coef_lap, m, i, j, l) : R(0.0);
   for (int k = 0; k < cD.KA; ++k) {
     int p = ix(i, j, k, l);
 #pragma unroll
     for (int n = 0; n < 6; ++n) {
-      double v = 0.0;
+      R v = R(0.0);
       if (in) {
-        const double* s = src.f[n];
-        const double* bs = (n == 4) ? cG.tem_bs : cG.rho_bs;
+        const R* s = src.f[n];
+        const R* bs = (n == 4) ? CG.tem_bs : CG.rho_bs;
         // lap7 (kernels/oprtlaplacian.py:41-55) with the reference-state
         // deviation for TEM and RHO
         auto scl = [&](int m) {
@@ -439,22 +452,23 @@ __global__ void k_hdiff1(Six src, SixOut out) {
   }
 }
 
-__global__ void k_hdiff1_pl(Six src, SixOut out) {
+template <class R>
+__global__ void k_hdiff1_pl(Six<R> src, SixOut<R> out) {
   int t = threadIdx.x;
   if (t >= cD.KA * cD.LP) return;
   int k = t / cD.LP, lp = t % cD.LP;
   for (int n = 0; n < 6; ++n) {
-    double row = 0.0;
+    R row = R(0.0);
     for (int v = 0; v < 6; ++v) {
       int q = ipl(v, k, lp);
-      double s = src.f[n][q];
-      if (n == 4) s = s - cG.tem_bs_pl[q];
-      if (n == 5) s = s - cG.rho_bs_pl[q];
-      double tv = cG.coef_lap_pl[v * cD.LP + lp] * s;
+      R s = src.f[n][q];
+      if (n == 4) s = s - CG.tem_bs_pl[q];
+      if (n == 5) s = s - CG.rho_bs_pl[q];
+      R tv = CG.coef_lap_pl[v * cD.LP + lp] * s;
       row = (v == 0) ? tv : row + tv;
     }
     out.f[n][ipl(0, k, lp)] = -row;
-    for (int g = 1; g < 6; ++g) out.f[n][ipl(g, k, lp)] = -0.0;
+    for (int g = 1; g < 6; ++g) out.f[n][ipl(g, k, lp)] = -R(0.0);
   }
 }
 
@@ -485,11 +499,12 @@ __global__ void k_intp_weights(const double* ci, double* w, int npt2) {
 // kernels/oprtdiffusion.py).  Halo cells are left to the exchange that follows.
 #define HD_DX 32
 #define HD_DY 8
-__global__ void __launch_bounds__(HD_DX * HD_DY, 4) k_hdiff2_l(Six vt, const double* rhog, SixOut out) {
+template <class R>
+__global__ void __launch_bounds__(HD_DX * HD_DY, 4) k_hdiff2_l(Six<R> vt, const R* rhog, SixOut<R> out) {
   constexpr int PX = HD_DX + 2, PY = HD_DY + 2, TX = HD_DX + 1, TY = HD_DY + 1;
-  __shared__ double s_f[6][PY * PX];
-  __shared__ double s_r[PY * PX];
-  __shared__ double s_t[2][6][TY * TX];   // field 4/5: tti x,y,z then ttj x,y,z
+  __shared__ R s_f[6][PY * PX];
+  __shared__ R s_r[PY * PX];
+  __shared__ R s_t[2][6][TY * TX];   // field 4/5: tti x,y,z then ttj x,y,z
   const int kb = (int)blockIdx.x, l = (int)blockIdx.z;
   const int ntx = (cD.G - 2 + HD_DX - 1) / HD_DX;
   const int i0 = 1 + ((int)blockIdx.y % ntx) * HD_DX, j0 = 1 + ((int)blockIdx.y / ntx) * HD_DY;
@@ -497,8 +512,8 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, 4) k_hdiff2_l(Six vt, const dou
   const int tid = threadIdx.x, tx = tid % HD_DX, ty = tid / HD_DX;
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= gmax) && (j <= gmax);
-  const double Kh = cC.Kh;
-  const double kfac[2] = {cC.CVdry, cC.hdiff_fact_rho};
+  const R Kh = CC.Kh;
+  const R kfac[2] = {CC.CVdry, CC.hdiff_fact_rho};
   {
     const int k = kb;
     for (int p = tid; p < PX * PY; p += blockDim.x) {
@@ -506,8 +521,8 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, 4) k_hdiff2_l(Six vt, const dou
       const bool ok = ii < G && jj < G;
       const int q = ok ? ix(ii, jj, k, l) : 0;
 #pragma unroll
-      for (int n = 0; n < 6; ++n) s_f[n][p] = ok ? vt.f[n][q] : 0.0;
-      s_r[p] = ok ? rhog[q] : 0.0;
+      for (int n = 0; n < 6; ++n) s_f[n][p] = ok ? vt.f[n][q] : R(0.0);
+      s_r[p] = ok ? rhog[q] : R(0.0);
     }
     __syncthreads();
     for (int p = tid; p < TX * TY; p += blockDim.x) {
@@ -517,19 +532,19 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, 4) k_hdiff2_l(Six vt, const dou
       const int ia = py * PX + px, ib = ia + 1, ic = ia + PX + 1, id = ia + PX;
 #pragma unroll
       for (int f = 0; f < 2; ++f) {
-        const double* s = s_f[4 + f];
-        const double s0 = s[ia], sip = s[ib], sd = s[ic], sjp = s[id];
+        const R* s = s_f[4 + f];
+        const R s0 = s[ia], sip = s[ib], sd = s[ic], sjp = s[id];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          double ti = 0.0, tj = 0.0;
+          R ti = R(0.0), tj = R(0.0);
           if (ok) {
             // weights 2c1-c2-c3, -c1+2c2-c3, -c1-c2+2c3 of the i and j triangles (k_intp_weights)
-            const double w1i = P2(cG.intp_w, (d * 3 + 0) * 2 + 0, ii, jj, l);
-            const double w2i = P2(cG.intp_w, (d * 3 + 1) * 2 + 0, ii, jj, l);
-            const double w3i = P2(cG.intp_w, (d * 3 + 2) * 2 + 0, ii, jj, l);
-            const double w1j = P2(cG.intp_w, (d * 3 + 0) * 2 + 1, ii, jj, l);
-            const double w2j = P2(cG.intp_w, (d * 3 + 1) * 2 + 1, ii, jj, l);
-            const double w3j = P2(cG.intp_w, (d * 3 + 2) * 2 + 1, ii, jj, l);
+            const R w1i = P2(CG.intp_w, (d * 3 + 0) * 2 + 0, ii, jj, l);
+            const R w2i = P2(CG.intp_w, (d * 3 + 1) * 2 + 0, ii, jj, l);
+            const R w3i = P2(CG.intp_w, (d * 3 + 2) * 2 + 0, ii, jj, l);
+            const R w1j = P2(CG.intp_w, (d * 3 + 0) * 2 + 1, ii, jj, l);
+            const R w2j = P2(CG.intp_w, (d * 3 + 1) * 2 + 1, ii, jj, l);
+            const R w3j = P2(CG.intp_w, (d * 3 + 2) * 2 + 1, ii, jj, l);
             ti = div3(w1i * s0 + w2i * sip + w3i * sd);
             tj = div3(w1j * s0 + w2j * sd + w3j * sjp);
           }
@@ -541,7 +556,7 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, 4) k_hdiff2_l(Six vt, const dou
     __syncthreads();
     if (i0 == 1 && j0 == 1 && tid < 6) {   // singular-point fix of the (0,0) triangle, fields 4 and 5
       const int f = tid / 3, d = tid % 3;
-      const double m0 = (double)cG.pntmask[l * 2 + 0], m1 = (double)cG.pntmask[l * 2 + 1];
+      const R m0 = (R)CG.pntmask[l * 2 + 0], m1 = (R)CG.pntmask[l * 2 + 1];
       s_t[f][d][0] = s_t[f][d][0] * m0 + s_t[f][3 + d][1] * m1;
     }
     __syncthreads();
@@ -551,27 +566,27 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, 4) k_hdiff2_l(Six vt, const dou
       const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
 #pragma unroll
       for (int n = 0; n < 4; ++n) {
-        double v = P2(cG.coef_lap, 0, i, j, l) * s_f[n][nb[0]];
+        R v = P2(CG.coef_lap, 0, i, j, l) * s_f[n][nb[0]];
 #pragma unroll
-        for (int m = 1; m < 7; ++m) v = v + P2(cG.coef_lap, m, i, j, l) * s_f[n][nb[m]];
+        for (int m = 1; m < 7; ++m) v = v + P2(CG.coef_lap, m, i, j, l) * s_f[n][nb[m]];
         out.f[n][q] = -v;
       }
       const int ta = (ty + 1) * TX + (tx + 1), tb = ta - 1, tc = ta - TX - 1, td = ta - TX;
 #pragma unroll
       for (int f = 0; f < 2; ++f) {
         auto kh = [&](int pt) { return s_r[pt] * kfac[f] * Kh; };
-        const double kh0 = kh(nb[0]);
-        const double kf1 = 0.5 * (kh0 + kh(nb[2])), kf2 = 0.5 * (kh0 + kh(nb[3])), kf3 = 0.5 * (kh0 + kh(nb[4]));
-        const double kf4 = 0.5 * (kh0 + kh(nb[5])), kf5 = 0.5 * (kh0 + kh(nb[6])), kf6 = 0.5 * (kh0 + kh(nb[1]));
-        double inner = 0.0;
+        const R kh0 = kh(nb[0]);
+        const R kf1 = R(0.5) * (kh0 + kh(nb[2])), kf2 = R(0.5) * (kh0 + kh(nb[3])), kf3 = R(0.5) * (kh0 + kh(nb[4]));
+        const R kf4 = R(0.5) * (kh0 + kh(nb[5])), kf5 = R(0.5) * (kh0 + kh(nb[6])), kf6 = R(0.5) * (kh0 + kh(nb[1]));
+        R inner = R(0.0);
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          const double aTI = s_t[f][d][ta], aTJ = s_t[f][3 + d][ta], bTI = s_t[f][d][tb];
-          const double cTI = s_t[f][d][tc], cTJ = s_t[f][3 + d][tc], dTJ = s_t[f][3 + d][td];
-          const double cd0 = P2(cG.coef_diff, d * 6 + 0, i, j, l), cd1 = P2(cG.coef_diff, d * 6 + 1, i, j, l),
-                       cd2 = P2(cG.coef_diff, d * 6 + 2, i, j, l), cd3 = P2(cG.coef_diff, d * 6 + 3, i, j, l),
-                       cd4 = P2(cG.coef_diff, d * 6 + 4, i, j, l), cd5 = P2(cG.coef_diff, d * 6 + 5, i, j, l);
-          const double blk = kf1 * cd0 * (aTI + aTJ) + kf2 * cd1 * (aTJ + bTI) + kf3 * cd2 * (bTI + cTJ) +
+          const R aTI = s_t[f][d][ta], aTJ = s_t[f][3 + d][ta], bTI = s_t[f][d][tb];
+          const R cTI = s_t[f][d][tc], cTJ = s_t[f][3 + d][tc], dTJ = s_t[f][3 + d][td];
+          const R cd0 = P2(CG.coef_diff, d * 6 + 0, i, j, l), cd1 = P2(CG.coef_diff, d * 6 + 1, i, j, l),
+                       cd2 = P2(CG.coef_diff, d * 6 + 2, i, j, l), cd3 = P2(CG.coef_diff, d * 6 + 3, i, j, l),
+                       cd4 = P2(CG.coef_diff, d * 6 + 4, i, j, l), cd5 = P2(CG.coef_diff, d * 6 + 5, i, j, l);
+          const R blk = kf1 * cd0 * (aTI + aTJ) + kf2 * cd1 * (aTJ + bTI) + kf3 * cd2 * (bTI + cTJ) +
                              kf4 * cd3 * (cTJ + cTI) + kf5 * cd4 * (cTI + dTJ) + kf6 * cd5 * (dTJ + aTI);
           inner = (d == 0) ? blk : inner + blk;
         }
@@ -582,50 +597,51 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, 4) k_hdiff2_l(Six vt, const dou
   }
 }
 
-__global__ void k_hdiff2_pl(Six vt, const double* rhog, SixOut out) {
+template <class R>
+__global__ void k_hdiff2_pl(Six<R> vt, const R* rhog, SixOut<R> out) {
   int t = threadIdx.x;
   if (t >= cD.KA * cD.LP) return;
   int k = t / cD.LP, lp = t % cD.LP;
-  const double Kh = cC.Kh;
+  const R Kh = CC.Kh;
   for (int n = 0; n < 6; ++n) {
-    const double* s = vt.f[n];
-    double row = 0.0;
+    const R* s = vt.f[n];
+    R row = R(0.0);
     if (n < 4) {
       for (int v = 0; v < 6; ++v) {
-        double tv = cG.coef_lap_pl[v * cD.LP + lp] * s[ipl(v, k, lp)];
+        R tv = CG.coef_lap_pl[v * cD.LP + lp] * s[ipl(v, k, lp)];
         row = (v == 0) ? tv : row + tv;
       }
     } else {
       // kernels/oprtdiffusion.py:137-177
-      const double fac = (n == 4) ? cC.CVdry : cC.hdiff_fact_rho;
-      double sn = s[ipl(0, k, lp)];
-      double vt_[5][3];
+      const R fac = (n == 4) ? CC.CVdry : CC.hdiff_fact_rho;
+      R sn = s[ipl(0, k, lp)];
+      R vt_[5][3];
       for (int v = 1; v <= 5; ++v) {
         int vp1 = (v == 5) ? 1 : v + 1;
-        double sij = s[ipl(v, k, lp)], sp1 = s[ipl(vp1, k, lp)];
+        R sij = s[ipl(v, k, lp)], sp1 = s[ipl(vp1, k, lp)];
         for (int d = 0; d < 3; ++d) {
-          const double* cI = cG.coef_intp_pl + ((v * cD.LP + lp) * 3 + d) * 3;
-          double c0 = cI[0], c1 = cI[1], c2 = cI[2];
-          vt_[v - 1][d] = div3((2.0 * c0 - c1 - c2) * sn + (-c0 + 2.0 * c1 - c2) * sij + (-c0 - c1 + 2.0 * c2) * sp1);
+          const R* cI = CG.coef_intp_pl + ((v * cD.LP + lp) * 3 + d) * 3;
+          R c0 = cI[0], c1 = cI[1], c2 = cI[2];
+          vt_[v - 1][d] = div3((R(2.0) * c0 - c1 - c2) * sn + (-c0 + R(2.0) * c1 - c2) * sij + (-c0 - c1 + R(2.0) * c2) * sp1);
         }
       }
-      double khn = rhog[ipl(0, k, lp)] * fac * Kh;
+      R khn = rhog[ipl(0, k, lp)] * fac * Kh;
       for (int v = 1; v <= 5; ++v) {
         int vm1 = (v == 1) ? 5 : v - 1;
-        double khv = rhog[ipl(v, k, lp)] * fac * Kh;
-        double kavg = 0.5 * (khn + khv);
-        double sd = 0.0;
+        R khv = rhog[ipl(v, k, lp)] * fac * Kh;
+        R kavg = R(0.5) * (khn + khv);
+        R sd = R(0.0);
         for (int d = 0; d < 3; ++d) {
-          double cdv = cG.coef_diff_pl[(v * cD.LP + lp) * 3 + d];
-          double tv = cdv * (vt_[vm1 - 1][d] + vt_[v - 1][d]);
+          R cdv = CG.coef_diff_pl[(v * cD.LP + lp) * 3 + d];
+          R tv = cdv * (vt_[vm1 - 1][d] + vt_[v - 1][d]);
           sd = (d == 0) ? tv : sd + tv;
         }
-        double contrib = kavg * sd;
+        R contrib = kavg * sd;
         row = (v == 1) ? contrib : row + contrib;
       }
     }
     out.f[n][ipl(0, k, lp)] = -row;
-    for (int g = 1; g < 6; ++g) out.f[n][ipl(g, k, lp)] = -0.0;
+    for (int g = 1; g < 6; ++g) out.f[n][ipl(g, k, lp)] = -R(0.0);
   }
 }
 
@@ -634,47 +650,50 @@ __global__ void k_hdiff2_pl(Six vt, const double* rhog, SixOut out) {
 // + horizontalize (mod_numfilter.py:1364-1369) + g_TEND = adv + f
 // (mod_dynamics.py:1340-1464).  All columns; projection on interior points.
 // ---------------------------------------------------------------------------
+template <class R>
 struct GtendArgs {
-  Six vt2;                       // post-COMM hyperdiffusion Laplacians
-  const double *rhog, *gvx, *gvy, *gvz, *gw;
-  double* gT0[6];
-  double* frhog;                 // f_TEND[RHOG] (tracer input)
+  Six<R> vt2;                       // post-COMM hyperdiffusion Laplacians
+  const R *rhog, *gvx, *gvy, *gvz, *gw;
+  R* gT0[6];
+  R* frhog;                 // f_TEND[RHOG] (tracer input)
 };
 
-__device__ void gtend_column(const Col c, const Met m, const GtendArgs& a, int i, int j, int l, int g, int lp) {
-  const double Kh = cC.Kh;
+template <class R>
+__device__ void gtend_column(const Col c, const MetT<R> m, const GtendArgs<R>& a, int i, int j, int l, int g, int lp) {
+  const R Kh = CC.Kh;
   for (int k = 0; k < cD.KA; ++k) {
     int p = c.at(k);
-    double rg = a.rhog[p];
-    double rgh = 0.0;
+    R rg = a.rhog[p];
+    R rgh = R(0.0);
     if (k >= cD.kmin) rgh = mc(m.C2W, c, 0, 2, k) * rg + mc(m.C2W, c, 1, 2, k) * a.rhog[c.at(k - 1)];
-    double fx = -(a.vt2.f[0][p] * Kh + 0.0) * rg;
-    double fy = -(a.vt2.f[1][p] * Kh + 0.0) * rg;
-    double fz = -(a.vt2.f[2][p] * Kh + 0.0) * rg;
-    double fw = -(a.vt2.f[3][p] * Kh + 0.0) * rgh;
-    double fe = -(a.vt2.f[4][p] + 0.0);
-    double fr = -(a.vt2.f[5][p] + 0.0);
+    R fx = -(a.vt2.f[0][p] * Kh + R(0.0)) * rg;
+    R fy = -(a.vt2.f[1][p] * Kh + R(0.0)) * rg;
+    R fz = -(a.vt2.f[2][p] * Kh + R(0.0)) * rg;
+    R fw = -(a.vt2.f[3][p] * Kh + R(0.0)) * rgh;
+    R fe = -(a.vt2.f[4][p] + R(0.0));
+    R fr = -(a.vt2.f[5][p] + R(0.0));
     if (!c.pole) {
       if (interior(i, j)) horiz_reg(i, j, l, fx, fy, fz);
     } else {
       horiz_pl(g, lp, fx, fy, fz);
     }
-    a.gT0[0][p] = 0.0 + fr;
+    a.gT0[0][p] = R(0.0) + fr;
     a.gT0[1][p] = a.gvx[p] + fx;
     a.gT0[2][p] = a.gvy[p] + fy;
     a.gT0[3][p] = a.gvz[p] + fz;
     a.gT0[4][p] = a.gw[p] + fw;
-    a.gT0[5][p] = 0.0 + fe;
+    a.gT0[5][p] = R(0.0) + fe;
     a.frhog[p] = fr;
   }
 }
 
-__global__ void k_gtend(GtendArgs a, int pole) {
+template <class R>
+__global__ void k_gtend(GtendArgs<R> a, int pole) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
-  if (!pole) gtend_column(col_reg(i, j, l), met_of(false), a, i, j, l, 0, 0);
-  else gtend_column(col_pl(g, lp), met_of(true), a, 0, 0, 0, g, lp);
+  if (!pole) gtend_column(col_reg(i, j, l), met_of<R>(false), a, i, j, l, 0, 0);
+  else gtend_column(col_pl(g, lp), met_of<R>(true), a, 0, 0, 0, g, lp);
 }
 
 }  // namespace nc

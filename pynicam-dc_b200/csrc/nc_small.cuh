@@ -9,17 +9,21 @@ namespace nc {
 // ---------------------------------------------------------------------------
 // 3-D divergence damping operator (kernels/oprt3ddivdamp.py:85-173)
 // ---------------------------------------------------------------------------
-struct Four { const double* f[4]; };   // rhogvx, rhogvy, rhogvz, rhogw
-struct Three { double* f[3]; };
-struct CThree { const double* f[3]; };
+template <class R>
+struct Four { const R* f[4]; };   // rhogvx, rhogvy, rhogvz, rhogw
+template <class R>
+struct Three { R* f[3]; };
+template <class R>
+struct CThree { const R* f[3]; };
 
 // the six-edge divergence-damping combination for direction d at (i,j)
 // (kernels/oprtdivdamp.py:110-120)
-__device__ __forceinline__ double ddivd(int i, int j, int l, int d, const double aTI, const double aTJ,
-                                        const double bTI, const double cTJ, const double cTI, const double dTJ) {
-  return P2(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) + P2(cG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
-         P2(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) + P2(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
-         P2(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) + P2(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI);
+template <class R>
+__device__ __forceinline__ R ddivd(int i, int j, int l, int d, const R aTI, const R aTJ,
+                                        const R bTI, const R cTJ, const R cTI, const R dTJ) {
+  return P2(CG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) + P2(CG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
+         P2(CG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) + P2(CG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
+         P2(CG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) + P2(CG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI);
 }
 
 // Tiled 3-D divergence damping: one block per DD_DX x DD_DY tile of output
@@ -40,12 +44,13 @@ __device__ __forceinline__ double ddivd(int i, int j, int l, int d, const double
 #endif
 // resident blocks per SM for a register budget of n blocks of 256 threads
 #define DD_MINB(n) ((n) * 256 / (DD_DX * DD_DY) > 0 ? (n) * 256 / (DD_DX * DD_DY) : 1)
-__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(4)) k_dd3d_t(Four v, Three out) {
+template <class R>
+__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(4)) k_dd3d_t(Four<R> v, Three<R> out) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2;   // points i0-1 .. i0+DX, j0-1 .. j0+DY
   constexpr int TX = DD_DX + 1, TY = DD_DY + 1;   // triangles i0-1 .. i0+DX-1, j0-1 .. j0+DY-1
-  __shared__ double s_vm[3][PY * PX];
-  __shared__ double s_rw[2][PY * PX];
-  __shared__ double s_ti[TY * TX], s_tj[TY * TX];
+  __shared__ R s_vm[3][PY * PX];
+  __shared__ R s_rw[2][PY * PX];
+  __shared__ R s_ti[TY * TX], s_tj[TY * TX];
   const int l = blockIdx.z;
   const int i0 = 1 + blockIdx.x * DD_DX, j0 = 1 + blockIdx.y * DD_DY;
   const int G = cD.G, gmax = cD.G - 2;
@@ -53,26 +58,26 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(4)) k_dd3d_t(Four v, Th
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= gmax) && (j <= gmax);
   const int n = cD.npti;
-  const double* cz = cG.C2WGz;
-  for (int p = tid; p < PX * PY; p += blockDim.x) s_rw[0][p] = 0.0;   // rwv(kmin) = 0
+  const R* cz = CG.C2WGz;
+  for (int p = tid; p < PX * PY; p += blockDim.x) s_rw[0][p] = R(0.0);   // rwv(kmin) = 0
   int cur = 0;
   for (int k = cD.kmin; k <= cD.kmax; ++k) {
     const bool up = (k + 1 <= cD.kmax);   // rwv(k+1) = 0 above kmax
     for (int p = tid; p < PX * PY; p += blockDim.x) {
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
-      double a = 0.0, b = 0.0, c = 0.0, r = 0.0;
+      R a = R(0.0), b = R(0.0), c = R(0.0), r = R(0.0);
       if (ii < G && jj < G) {
         const int q = ix(ii, jj, k, l);
-        const double f0 = v.f[0][q], f1 = v.f[1][q], f2 = v.f[2][q];
-        const double rg = gam_at(cG.RGAM, q);
+        const R f0 = v.f[0][q], f1 = v.f[1][q], f2 = v.f[2][q];
+        const R rg = gam_at(CG.RGAM, q);
         a = f0 * rg;
         b = f1 * rg;
         c = f2 * rg;
         if (up) {
           const int qp = q + cD.planei;   // level k+1
-          const double h = cz[qp] * v.f[0][qp] + cz[n + qp] * f0 + cz[2 * n + qp] * v.f[1][qp] +
+          const R h = cz[qp] * v.f[0][qp] + cz[n + qp] * f0 + cz[2 * n + qp] * v.f[1][qp] +
                            cz[3 * n + qp] * f1 + cz[4 * n + qp] * v.f[2][qp] + cz[5 * n + qp] * f2;
-          r = h * gam_at(cG.RGAMH, qp) + v.f[3][qp] * cG.RGSQRTH[qp];
+          r = h * gam_at(CG.RGAMH, qp) + v.f[3][qp] * CG.RGSQRTH[qp];
         }
       }
       s_vm[0][p] = a;
@@ -81,18 +86,18 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(4)) k_dd3d_t(Four v, Th
       s_rw[cur ^ 1][p] = r;
     }
     __syncthreads();
-    const double rdz = cC.rdgz[k];
-    const double* rU = s_rw[cur ^ 1];
-    const double* rD = s_rw[cur];
+    const R rdz = CC.rdgz[k];
+    const R* rU = s_rw[cur ^ 1];
+    const R* rD = s_rw[cur];
     for (int p = tid; p < TX * TY; p += blockDim.x) {
       const int px = p % TX, py = p / TX;
       const int ii = i0 - 1 + px, jj = j0 - 1 + py;
-      double sTI = 0.0, sTJ = 0.0;
+      R sTI = R(0.0), sTJ = R(0.0);
       if (ii <= G - 2 && jj <= G - 2) {
         const int a = py * PX + px, b = a + 1, c = a + PX + 1, d = a + PX;
-        auto C = [&](int dir, int pt, int t) { return P2c(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
-        const double wTI = div3((rU[a] + rU[b] + rU[c]) - (rD[a] + rD[b] + rD[c])) * rdz;
-        const double wTJ = div3((rU[a] + rU[c] + rU[d]) - (rD[a] + rD[c] + rD[d])) * rdz;
+        auto C = [&](int dir, int pt, int t) { return P2c(CG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
+        const R wTI = div3((rU[a] + rU[b] + rU[c]) - (rD[a] + rD[b] + rD[c])) * rdz;
+        const R wTJ = div3((rU[a] + rU[c] + rU[d]) - (rD[a] + rD[c] + rD[d])) * rdz;
         sTI = C(0, 0, 0) * s_vm[0][a] + C(0, 1, 0) * s_vm[0][b] + C(0, 2, 0) * s_vm[0][c] +
               C(1, 0, 0) * s_vm[1][a] + C(1, 1, 0) * s_vm[1][b] + C(1, 2, 0) * s_vm[1][c] +
               C(2, 0, 0) * s_vm[2][a] + C(2, 1, 0) * s_vm[2][b] + C(2, 2, 0) * s_vm[2][c] + wTI;
@@ -105,20 +110,20 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(4)) k_dd3d_t(Four v, Th
     }
     __syncthreads();
     if (tid == 0 && i0 == 1 && j0 == 1)   // singular-point fix at the (0,0) triangle
-      s_ti[0] = s_ti[0] * (double)cG.pntmask[l * 2 + 0] + s_tj[1] * (double)cG.pntmask[l * 2 + 1];
+      s_ti[0] = s_ti[0] * (R)CG.pntmask[l * 2 + 0] + s_tj[1] * (R)CG.pntmask[l * 2 + 1];
     __syncthreads();
     if (own) {
       const int ta = (ty + 1) * TX + (tx + 1);   // triangle (i, j)
-      const double aTI = s_ti[ta], aTJ = s_tj[ta];
-      const double bTI = s_ti[ta - 1];            // (i-1, j)
-      const double cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1];   // (i-1, j-1)
-      const double dTJ = s_tj[ta - TX];           // (i, j-1)
+      const R aTI = s_ti[ta], aTJ = s_tj[ta];
+      const R bTI = s_ti[ta - 1];            // (i-1, j)
+      const R cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1];   // (i-1, j-1)
+      const R dTJ = s_tj[ta - TX];           // (i, j-1)
       const int q = ix(i, j, k, l);
 #pragma unroll
       for (int d = 0; d < 3; ++d)
-        out.f[d][q] = P2c(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) + P2c(cG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
-                      P2c(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) + P2c(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
-                      P2c(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) + P2c(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI);
+        out.f[d][q] = P2c(CG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) + P2c(CG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
+                      P2c(CG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) + P2c(CG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
+                      P2c(CG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) + P2c(CG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI);
     }
     __syncthreads();
     cur ^= 1;
@@ -143,40 +148,41 @@ __device__ __forceinline__ TileLv tile_level(int kbase) {
 }
 
 // pole 3-D divergence damping (kernels/oprt3ddivdamp.py:176-237)
-__global__ void k_dd3d_pl(Four v, Three out) {
+template <class R>
+__global__ void k_dd3d_pl(Four<R> v, Three<R> out) {
   int t = threadIdx.x;
   if (t >= cD.KA * cD.LP) return;
   int k = t / cD.LP, lp = t % cD.LP;
   for (int g = 0; g < 6; ++g)
-    for (int d = 0; d < 3; ++d) out.f[d][ipl(g, k, lp)] = 0.0;
+    for (int d = 0; d < 3; ++d) out.f[d][ipl(g, k, lp)] = R(0.0);
   if (k < cD.kmin || k > cD.kmax) return;
-  auto rw = [&](int g, int kk) -> double {
-    if (kk <= cD.kmin || kk > cD.kmax) return 0.0;
+  auto rw = [&](int g, int kk) -> R {
+    if (kk <= cD.kmin || kk > cD.kmax) return R(0.0);
     int q = ipl(g, kk, lp), qm = ipl(g, kk - 1, lp);
-    const double* cz = cG.C2WGz_pl;
-    double h = cz[q * 6 + 0] * v.f[0][q] + cz[q * 6 + 1] * v.f[0][qm] + cz[q * 6 + 2] * v.f[1][q] +
+    const R* cz = CG.C2WGz_pl;
+    R h = cz[q * 6 + 0] * v.f[0][q] + cz[q * 6 + 1] * v.f[0][qm] + cz[q * 6 + 2] * v.f[1][q] +
                cz[q * 6 + 3] * v.f[1][qm] + cz[q * 6 + 4] * v.f[2][q] + cz[q * 6 + 5] * v.f[2][qm];
-    return h * gam_at(cG.RGAMH_pl, q) + v.f[3][q] * cG.RGSQRTH_pl[q];
+    return h * gam_at(CG.RGAMH_pl, q) + v.f[3][q] * CG.RGSQRTH_pl[q];
   };
-  double vm[6][3];
+  R vm[6][3];
   for (int g = 0; g < 6; ++g) {
     int q = ipl(g, k, lp);
-    for (int d = 0; d < 3; ++d) vm[g][d] = v.f[d][q] * gam_at(cG.RGAM_pl, q);
+    for (int d = 0; d < 3; ++d) vm[g][d] = v.f[d][q] * gam_at(CG.RGAM_pl, q);
   }
-  double sclt[5];
+  R sclt[5];
   for (int v_ = 1; v_ <= 5; ++v_) {
     int vp1 = (v_ == 5) ? 1 : v_ + 1;
-    double sw = div3((rw(0, k + 1) + rw(v_, k + 1) + rw(vp1, k + 1)) - (rw(0, k) + rw(v_, k) + rw(vp1, k))) * cC.rdgz[k];
-    const double* cI = cG.coef_intp_pl + (v_ * cD.LP + lp) * 9;
+    R sw = div3((rw(0, k + 1) + rw(v_, k + 1) + rw(vp1, k + 1)) - (rw(0, k) + rw(v_, k) + rw(vp1, k))) * CC.rdgz[k];
+    const R* cI = CG.coef_intp_pl + (v_ * cD.LP + lp) * 9;
     sclt[v_ - 1] = cI[0] * vm[0][0] + cI[1] * vm[v_][0] + cI[2] * vm[vp1][0] + cI[3] * vm[0][1] + cI[4] * vm[v_][1] +
                    cI[5] * vm[vp1][1] + cI[6] * vm[0][2] + cI[7] * vm[v_][2] + cI[8] * vm[vp1][2] + sw;
   }
   for (int d = 0; d < 3; ++d) {
-    double row = 0.0;
+    R row = R(0.0);
     for (int v_ = 1; v_ <= 5; ++v_) {
       int vm1 = (v_ == 1) ? 5 : v_ - 1;
-      double pair = sclt[vm1 - 1] + sclt[v_ - 1];
-      double tv = cG.coef_diff_pl[(v_ * cD.LP + lp) * 3 + d] * pair;
+      R pair = sclt[vm1 - 1] + sclt[v_ - 1];
+      R tv = CG.coef_diff_pl[(v_ * cD.LP + lp) * 3 + d] * pair;
       row = (v_ == 1) ? tv : row + tv;
     }
     out.f[d][ipl(0, k, lp)] = row;
@@ -187,60 +193,62 @@ __global__ void k_dd3d_pl(Four v, Three out) {
 // post-COMM 2-D divergence damping (kernels/divdamppostcomm.py:29-81):
 // gd = coef * OPRT_divdamp(-vtmp2), then horizontalize (interior).
 // ---------------------------------------------------------------------------
-__device__ void divdamp2d_at(const CThree& vt, int i, int j, int k, int l, double gd[3]) {
+template <class R>
+__device__ void divdamp2d_at(const CThree<R>& vt, int i, int j, int k, int l, R gd[3]) {
   if (!interior(i, j)) {
-    for (int d = 0; d < 3; ++d) gd[d] = cC.divdamp_coef * 0.0;
+    for (int d = 0; d < 3; ++d) gd[d] = CC.divdamp_coef * R(0.0);
     return;
   }
-  auto sc = [&](int ii, int jj, double& sTI, double& sTJ) {
+  auto sc = [&](int ii, int jj, R& sTI, R& sTJ) {
     int a = ix(ii, jj, k, l), b = ix(ii + 1, jj, k, l), c = ix(ii + 1, jj + 1, k, l), d = ix(ii, jj + 1, k, l);
-    auto C = [&](int dir, int p, int t) { return P2(cG.coef_intp, (dir * 3 + p) * 2 + t, ii, jj, l); };
-    double x0 = -vt.f[0][a], x1 = -vt.f[0][b], x2 = -vt.f[0][c], x3 = -vt.f[0][d];
-    double y0 = -vt.f[1][a], y1 = -vt.f[1][b], y2 = -vt.f[1][c], y3 = -vt.f[1][d];
-    double z0 = -vt.f[2][a], z1 = -vt.f[2][b], z2 = -vt.f[2][c], z3 = -vt.f[2][d];
+    auto C = [&](int dir, int p, int t) { return P2(CG.coef_intp, (dir * 3 + p) * 2 + t, ii, jj, l); };
+    R x0 = -vt.f[0][a], x1 = -vt.f[0][b], x2 = -vt.f[0][c], x3 = -vt.f[0][d];
+    R y0 = -vt.f[1][a], y1 = -vt.f[1][b], y2 = -vt.f[1][c], y3 = -vt.f[1][d];
+    R z0 = -vt.f[2][a], z1 = -vt.f[2][b], z2 = -vt.f[2][c], z3 = -vt.f[2][d];
     sTI = C(0, 0, 0) * x0 + C(0, 1, 0) * x1 + C(0, 2, 0) * x2 + C(1, 0, 0) * y0 + C(1, 1, 0) * y1 + C(1, 2, 0) * y2 +
           C(2, 0, 0) * z0 + C(2, 1, 0) * z1 + C(2, 2, 0) * z2;
     sTJ = C(0, 0, 1) * x0 + C(0, 1, 1) * x2 + C(0, 2, 1) * x3 + C(1, 0, 1) * y0 + C(1, 1, 1) * y2 + C(1, 2, 1) * y3 +
           C(2, 0, 1) * z0 + C(2, 1, 1) * z2 + C(2, 2, 1) * z3;
   };
-  double aTI, aTJ, bTI, bTJ, cTI, cTJ, dTI, dTJ;
+  R aTI, aTJ, bTI, bTJ, cTI, cTJ, dTI, dTJ;
   sc(i, j, aTI, aTJ);
   sc(i - 1, j, bTI, bTJ);
   sc(i - 1, j - 1, cTI, cTJ);
   sc(i, j - 1, dTI, dTJ);
-  double o[3];
-  for (int d = 0; d < 3; ++d) o[d] = cC.divdamp_coef * ddivd(i, j, l, d, aTI, aTJ, bTI, cTJ, cTI, dTJ);
+  R o[3];
+  for (int d = 0; d < 3; ++d) o[d] = CC.divdamp_coef * ddivd(i, j, l, d, aTI, aTJ, bTI, cTJ, cTI, dTJ);
   horiz_reg(i, j, l, o[0], o[1], o[2]);
   gd[0] = o[0]; gd[1] = o[1]; gd[2] = o[2];
 }
 
 // pole 2-D divergence damping of -vtmp2 at (g,k,lp) (kernels/oprtdivdamp.py:125-173
 // then horizontalize over all g)
-__device__ void divdamp2d_pl_at(const CThree& vt, int g, int k, int lp, double gd[3]) {
-  double o[3] = {0.0, 0.0, 0.0};
+template <class R>
+__device__ void divdamp2d_pl_at(const CThree<R>& vt, int g, int k, int lp, R gd[3]) {
+  R o[3] = {R(0.0), R(0.0), R(0.0)};
   if (g == 0) {
-    double vv[6][3];
+    R vv[6][3];
     for (int q = 0; q < 6; ++q)
       for (int d = 0; d < 3; ++d) vv[q][d] = -vt.f[d][ipl(q, k, lp)];
-    double sclt[5];
+    R sclt[5];
     for (int v_ = 1; v_ <= 5; ++v_) {
       int vp1 = (v_ == 5) ? 1 : v_ + 1;
-      const double* cI = cG.coef_intp_pl + (v_ * cD.LP + lp) * 9;
+      const R* cI = CG.coef_intp_pl + (v_ * cD.LP + lp) * 9;
       sclt[v_ - 1] = cI[0] * vv[0][0] + cI[1] * vv[v_][0] + cI[2] * vv[vp1][0] + cI[3] * vv[0][1] +
                      cI[4] * vv[v_][1] + cI[5] * vv[vp1][1] + cI[6] * vv[0][2] + cI[7] * vv[v_][2] +
                      cI[8] * vv[vp1][2];
     }
     for (int d = 0; d < 3; ++d) {
-      double row = 0.0;
+      R row = R(0.0);
       for (int v_ = 1; v_ <= 5; ++v_) {
         int vm1 = (v_ == 1) ? 5 : v_ - 1;
-        double tv = cG.coef_diff_pl[(v_ * cD.LP + lp) * 3 + d] * (sclt[vm1 - 1] + sclt[v_ - 1]);
+        R tv = CG.coef_diff_pl[(v_ * cD.LP + lp) * 3 + d] * (sclt[vm1 - 1] + sclt[v_ - 1]);
         row = (v_ == 1) ? tv : row + tv;
       }
       o[d] = row;
     }
   }
-  for (int d = 0; d < 3; ++d) o[d] = cC.divdamp_coef * o[d];
+  for (int d = 0; d < 3; ++d) o[d] = CC.divdamp_coef * o[d];
   horiz_pl(g, lp, o[0], o[1], o[2]);
   gd[0] = o[0]; gd[1] = o[1]; gd[2] = o[2];
 }
@@ -250,36 +258,36 @@ __device__ void divdamp2d_pl_at(const CThree& vt, int g, int k, int lp, double g
 // k with the first-layer remedy and the tangent-plane projection.
 // P(ii,jj,kk) gives the pressure; returns Pgrad (3 comps).
 // ---------------------------------------------------------------------------
-template <class PF>
-__device__ void presgrad_reg(int i, int j, int k, int l, const Col& c, const Met& m, PF P, double out[3]) {
+template <class R, class PF>
+__device__ void presgrad_reg(int i, int j, int k, int l, const Col& c, const MetT<R>& m, PF P, R out[3]) {
   const int kmin = cD.kmin, kmax = cD.kmax;
-  out[0] = out[1] = out[2] = 0.0;
+  out[0] = out[1] = out[2] = R(0.0);
   if (k >= kmin && k <= kmax) {
     const int kk = (k == kmin) ? kmin + 1 : k;
-    double gh[3] = {0.0, 0.0, 0.0};
-    if (interior(i, j)) grad7(i, j, kk, l, [&](int ii, int jj, int k2) { return P(ii, jj, k2) * gam_at(cG.RGAM, ix(ii, jj, k2, l)); }, gh);
+    R gh[3] = {R(0.0), R(0.0), R(0.0)};
+    if (interior(i, j)) grad7(i, j, kk, l, [&](int ii, int jj, int k2) { return P(ii, jj, k2) * gam_at(CG.RGAM, ix(ii, jj, k2, l)); }, gh);
     auto pvmh = [&](int k2, int d) {
       return (mc(m.C2WGz, c, 2 * d, 6, k2) * P(i, j, k2) + mc(m.C2WGz, c, 2 * d + 1, 6, k2) * P(i, j, k2 - 1)) *
              gam_at(m.RGAMH, c.at(k2));
     };
-    for (int d = 0; d < 3; ++d) out[d] = gh[d] + (pvmh(kk + 1, d) - pvmh(kk, d)) * cC.rdgz[kk];
+    for (int d = 0; d < 3; ++d) out[d] = gh[d] + (pvmh(kk + 1, d) - pvmh(kk, d)) * CC.rdgz[kk];
   }
   if (interior(i, j)) horiz_reg(i, j, l, out[0], out[1], out[2]);
 }
 
-template <class PF>
-__device__ void presgrad_pl(int g, int k, int lp, const Col& c, const Met& m, PF P, double out[3]) {
+template <class R, class PF>
+__device__ void presgrad_pl(int g, int k, int lp, const Col& c, const MetT<R>& m, PF P, R out[3]) {
   const int kmin = cD.kmin, kmax = cD.kmax;
-  out[0] = out[1] = out[2] = 0.0;
+  out[0] = out[1] = out[2] = R(0.0);
   if (k >= kmin && k <= kmax) {
     const int kk = (k == kmin) ? kmin + 1 : k;
-    double gh[3] = {0.0, 0.0, 0.0};
+    R gh[3] = {R(0.0), R(0.0), R(0.0)};
     if (g == 0) {
       for (int d = 0; d < 3; ++d) {
-        double row = 0.0;
+        R row = R(0.0);
         for (int v_ = 0; v_ < 6; ++v_) {
-          double pvm = P(v_, kk) * gam_at(cG.RGAM_pl, ipl(v_, kk, lp)) * 1.0;
-          double tv = cG.coef_grad_pl[(v_ * cD.LP + lp) * 3 + d] * pvm;
+          R pvm = P(v_, kk) * gam_at(CG.RGAM_pl, ipl(v_, kk, lp)) * R(1.0);
+          R tv = CG.coef_grad_pl[(v_ * cD.LP + lp) * 3 + d] * pvm;
           row = (v_ == 0) ? tv : row + tv;
         }
         gh[d] = row;
@@ -289,43 +297,44 @@ __device__ void presgrad_pl(int g, int k, int lp, const Col& c, const Met& m, PF
       return (mc(m.C2WGz, c, 2 * d, 6, k2) * P(g, k2) + mc(m.C2WGz, c, 2 * d + 1, 6, k2) * P(g, k2 - 1)) *
              gam_at(m.RGAMH, c.at(k2));
     };
-    for (int d = 0; d < 3; ++d) out[d] = gh[d] + (pvmh(kk + 1, d) - pvmh(kk, d)) * cC.rdgz[kk];
+    for (int d = 0; d < 3; ++d) out[d] = gh[d] + (pvmh(kk + 1, d) - pvmh(kk, d)) * CC.rdgz[kk];
   }
   horiz_pl(g, lp, out[0], out[1], out[2]);
 }
 
 // vertical pressure gradient (kernels/presgrad.py:196-204)
-template <class PF>
-__device__ __forceinline__ double presgradw(const Col& c, const Met& m, int k, PF Pk) {
-  if (k < cD.kmin + 1 || k > cD.kmax) return 0.0;
+template <class R, class PF>
+__device__ __forceinline__ R presgradw(const Col& c, const MetT<R>& m, int k, PF Pk) {
+  if (k < cD.kmin + 1 || k > cD.kmax) return R(0.0);
   int p = c.at(k), pm = c.at(k - 1);
-  return gam_at(m.GAM2H, p) * (Pk(k) * m.RGSGAM2[p] - Pk(k - 1) * m.RGSGAM2[pm]) * cC.rdgzh[k];
+  return gam_at(m.GAM2H, p) * (Pk(k) * m.RGSGAM2[p] - Pk(k - 1) * m.RGSGAM2[pm]) * CC.rdgzh[k];
 }
 
 // flux convergence at level k of a regional or pole column given the
 // horizontal divergence value (zero on the halo) and the flux accessors
 // (kernels/fluxconv.py:111-208, vflag 1 or 0)
-template <class FH, class FW>
-__device__ __forceinline__ double fluxconv_col(const Col& c, const Met& m, int k, double div, double vflag, FH fh, FW fw) {
-  if (k < cD.kmin || k > cD.kmax) return 0.0;
-  auto vmh = [&](int kk) -> double {
-    if (kk <= cD.kmin || kk > cD.kmax) return 0.0;
-    double h = vmh_horiz(c, m, kk, fh);
+template <class R, class FH, class FW>
+__device__ __forceinline__ R fluxconv_col(const Col& c, const MetT<R>& m, int k, typename Id<R>::type div,
+                                          typename Id<R>::type vflag, FH fh, FW fw) {
+  if (k < cD.kmin || k > cD.kmax) return R(0.0);
+  auto vmh = [&](int kk) -> R {
+    if (kk <= cD.kmin || kk > cD.kmax) return R(0.0);
+    R h = vmh_horiz(c, m, kk, fh);
     return h + vflag * fw(kk) * m.RGSQRTH[c.at(kk)];
   };
-  return -div - (vmh(k + 1) - vmh(k)) * cC.rdgz[k];
+  return -div - (vmh(k + 1) - vmh(k)) * CC.rdgz[k];
 }
 
 // pole divergence row of (fx,fy,fz)*RGAM at level k (kernels/fluxconv.py:81-108)
-template <class F>
-__device__ __forceinline__ double div_pl(int lp, int k, F f) {
-  double row = 0.0;
+template <class R, class F>
+__device__ __forceinline__ R div_pl(int lp, int k, F f) {
+  R row = R(0.0);
   for (int v_ = 0; v_ < 6; ++v_) {
     int q = ipl(v_, k, lp);
-    double rg = gam_at(cG.RGAM_pl, q);
-    double vx = f(q, 0) * rg, vy = f(q, 1) * rg, vz = f(q, 2) * rg;
-    const double* cd = cG.coef_div_pl + (v_ * cD.LP + lp) * 3;
-    double pv = cd[0] * vx + cd[1] * vy + cd[2] * vz;
+    R rg = gam_at(CG.RGAM_pl, q);
+    R vx = f(q, 0) * rg, vy = f(q, 1) * rg, vz = f(q, 2) * rg;
+    const R* cd = CG.coef_div_pl + (v_ * cD.LP + lp) * 3;
+    R pv = cd[0] * vx + cd[1] * vy + cd[2] * vz;
     row = (v_ == 0) ? pv : row + pv;
   }
   return row;
@@ -336,103 +345,117 @@ __device__ __forceinline__ double div_pl(int lp, int k, F f) {
 // implicit matrix and ethtot0 (mod_vi.py:295-878 numpy path,
 // kernels/vimatrix.py:67-136, kernels/vimain.py:195-239)
 // ---------------------------------------------------------------------------
+template <class R>
 struct Vp0Args {
-  Prog P;                       // PROG (post BNDCND)
-  const double *vx, *vy, *vz, *eth, *pregd, *rhogd;
-  CThree vt;                    // post-COMM 3-D divdamp of PROG
-  const double* gT0[6];         // large-step tendency
-  double* gT[6];                // out: small-step tendency
-  double *Mc, *Mu, *Ml, *ethtot0;
+  Prog<R> P;                    // PROG (post BNDCND)
+  const R *vx, *vy, *vz, *eth;
+  const double *pregd, *rhogd;  // float64 in both forms
+  CThree<R> vt;                 // post-COMM 3-D divdamp of PROG
+  const R* gT0[6];              // large-step tendency
+  R* gT[6];                     // out: small-step tendency
+  double *Mc, *Mu, *Ml;         // float64 in both forms
+  R* ethtot0;
   double dt;                    // small-step dt
 };
 
-template <bool POLE>
-__device__ void vp0_column(const Vp0Args& a, int i, int j, int l, int g, int lp) {
+// One pole column of vp0.  In the mixed form the horizontal operators run in
+// float32 (R) and the vertical part -- buoyancy and vertical pressure gradient
+// of the float64 deviations, gz, the implicit matrix and the vertical-momentum
+// tendency -- in float64, as in the regional column kernel k_vp0_cr.
+template <class R, bool POLE>
+__device__ void vp0_column(const Vp0Args<R>& a, int i, int j, int l, int g, int lp) {
   const Col c = POLE ? col_pl(g, lp) : col_reg(i, j, l);
-  const Met m = met_of(POLE);
+  const MetT<R> m = met_of<R>(POLE);
   const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
-  const double* const* P = a.P.v;
-  double dt = a.dt;
-  // column-local half-level values
+  const R* const* P = a.P.v;
+  const double dt = a.dt;
+  // column-local half-level values (float64)
   auto rhog_h = [&](int k) -> double {
     int kk = (k < kmin) ? kmin : k;
-    return mc(m.C2W, c, 0, 2, kk) * P[0][c.at(kk)] + mc(m.C2W, c, 1, 2, kk) * P[0][c.at(kk - 1)];
+    return (double)mc(m.C2W, c, 0, 2, kk) * (double)P[0][c.at(kk)] +
+           (double)mc(m.C2W, c, 1, 2, kk) * (double)P[0][c.at(kk - 1)];
   };
   auto eth_h = [&](int k) -> double {
     int kk = (k < kmin) ? kmin : k;
-    return cC.afact[kk] * a.eth[c.at(kk)] + cC.bfact[kk] * a.eth[c.at(kk - 1)];
+    return cC.afact[kk] * (double)a.eth[c.at(kk)] + cC.bfact[kk] * (double)a.eth[c.at(kk - 1)];
   };
   auto dbuo = [&](int k) -> double {
     if (k < kmin + 1 || k > kmax) return 0.0;
-    return -cC.GRAV * (mc(m.C2W, c, 0, 2, k) * a.rhogd[c.at(k)] + mc(m.C2W, c, 1, 2, k) * a.rhogd[c.at(k - 1)]);
+    return -cC.GRAV * ((double)mc(m.C2W, c, 0, 2, k) * a.rhogd[c.at(k)] +
+                       (double)mc(m.C2W, c, 1, 2, k) * a.rhogd[c.at(k - 1)]);
   };
-  auto dpgw = [&](int k) -> double { return presgradw(c, m, k, [&](int kk) { return a.pregd[c.at(kk)]; }); };
+  auto dpgw = [&](int k) -> double {
+    if (k < kmin + 1 || k > kmax) return 0.0;
+    const int p = c.at(k), pm = c.at(k - 1);
+    return (double)gam_at(m.GAM2H, p) *
+           (a.pregd[p] * (double)m.RGSGAM2[p] - a.pregd[pm] * (double)m.RGSGAM2[pm]) * cC.rdgzh[k];
+  };
   auto gz = [&](int k) -> double { return cC.GRAV - (dpgw(k) - dbuo(k)) / rhog_h(k); };
-  auto pwh = [&](int k) -> double { return -gz(k) * P[4][c.at(k)]; };
-  auto PF = [&](int k, int d) -> double { return P[1 + d][c.at(k)]; };
-  auto PEF = [&](int k, int d) -> double { return P[1 + d][c.at(k)] * a.eth[c.at(k)]; };
+  auto pwh = [&](int k) -> R { return R(-gz(k) * (double)P[4][c.at(k)]); };
+  auto PF = [&](int k, int d) -> R { return P[1 + d][c.at(k)]; };
+  auto PEF = [&](int k, int d) -> R { return P[1 + d][c.at(k)] * a.eth[c.at(k)]; };
   for (int k = 0; k < KA; ++k) {
     int p = c.at(k);
     // horizontal divergences
-    double div1 = 0.0, div2 = 0.0;
+    R div1 = R(0.0), div2 = R(0.0);
     if (!POLE) {
       if (interior(i, j)) {
-        div1 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
+        div1 = div7<R>(i, j, k, l, [&](int ii, int jj, int kk, int d) {
           int q = ix(ii, jj, kk, l);
-          return P[1 + d][q] * gam_at(cG.RGAM, q);
+          return P[1 + d][q] * gam_at(CG.RGAM, q);
         });
-        div2 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
+        div2 = div7<R>(i, j, k, l, [&](int ii, int jj, int kk, int d) {
           int q = ix(ii, jj, kk, l);
-          return (P[1 + d][q] * a.eth[q]) * gam_at(cG.RGAM, q);
+          return (P[1 + d][q] * a.eth[q]) * gam_at(CG.RGAM, q);
         });
       }
     } else if (g == 0) {
-      div1 = div_pl(lp, k, [&](int q, int d) { return P[1 + d][q]; });
-      div2 = div_pl(lp, k, [&](int q, int d) { return P[1 + d][q] * a.eth[q]; });
+      div1 = div_pl<R>(lp, k, [&](int q, int d) { return P[1 + d][q]; });
+      div2 = div_pl<R>(lp, k, [&](int q, int d) { return P[1 + d][q] * a.eth[q]; });
     }
-    double drhog = fluxconv_col(c, m, k, div1, 1.0, PF, [&](int kk) { return P[4][c.at(kk)]; });
-    double drhoge = fluxconv_col(c, m, k, div2, 1.0, PEF, [&](int kk) {
+    R drhog = fluxconv_col(c, m, k, div1, R(1.0), PF, [&](int kk) { return P[4][c.at(kk)]; });
+    R drhoge = fluxconv_col(c, m, k, div2, R(1.0), PEF, [&](int kk) {
       int q = c.at(kk);
-      return P[4][q] * (cC.afact[kk] * a.eth[q] + cC.bfact[kk] * a.eth[c.at(kk - 1)]);
+      return P[4][q] * (CC.afact[kk] * a.eth[q] + CC.bfact[kk] * a.eth[c.at(kk - 1)]);
     });
-    double dd[3], dpg[3];
+    R dd[3], dpg[3];
     if (!POLE) {
       divdamp2d_at(a.vt, i, j, k, l, dd);
-      presgrad_reg(i, j, k, l, c, m, [&](int ii, int jj, int kk) { return a.pregd[ix(ii, jj, kk, l)]; }, dpg);
+      presgrad_reg(i, j, k, l, c, m, [&](int ii, int jj, int kk) { return R(a.pregd[ix(ii, jj, kk, l)]); }, dpg);
     } else {
       divdamp2d_pl_at(a.vt, g, k, lp, dd);
-      presgrad_pl(g, k, lp, c, m, [&](int gg, int kk) { return a.pregd[ipl(gg, kk, lp)]; }, dpg);
+      presgrad_pl(g, k, lp, c, m, [&](int gg, int kk) { return R(a.pregd[ipl(gg, kk, lp)]); }, dpg);
     }
-    double pw = 0.0;
+    R pw = R(0.0);
     if (k >= kmin && k <= kmax)
       pw = a.vx[p] * dpg[0] + a.vy[p] * dpg[1] + a.vz[p] * dpg[2] + mc(m.W2C, c, 0, 2, k) * pwh(k + 1) +
            mc(m.W2C, c, 1, 2, k) * pwh(k);
     a.gT[0][p] = a.gT0[0][p] + drhog;
-    a.gT[1][p] = a.gT0[1][p] - dpg[0] + dd[0] + 0.0;
-    a.gT[2][p] = a.gT0[2][p] - dpg[1] + dd[1] + 0.0;
-    a.gT[3][p] = a.gT0[3][p] - dpg[2] + dd[2] + 0.0;
-    a.gT[4][p] = a.gT0[4][p] + 0.0 * cC.alpha - dpgw(k) + dbuo(k);
+    a.gT[1][p] = a.gT0[1][p] - dpg[0] + dd[0] + R(0.0);
+    a.gT[2][p] = a.gT0[2][p] - dpg[1] + dd[1] + R(0.0);
+    a.gT[3][p] = a.gT0[3][p] - dpg[2] + dd[2] + R(0.0);
+    a.gT[4][p] = R((double)a.gT0[4][p] + 0.0 * cC.alpha - dpgw(k) + dbuo(k));
     a.gT[5][p] = a.gT0[5][p] + drhoge + pw;
-    // vertical implicit matrix on k = kmin+1..kmax
+    // vertical implicit matrix on k = kmin+1..kmax (float64)
     if (k >= kmin + 1 && k <= kmax) {
       const double GCVovR = cC.GRAV * cC.CVdry / cC.Rdry;
       const double ACVovRt2 = cC.alpha * cC.CVdry / cC.Rdry / (dt * dt);
       int pm = c.at(k - 1), pp = c.at(k + 1);
       double rg = cC.rdgz[k], rgm = cC.rdgz[k - 1];
-      double Ca = (m.RGSGAM2[p] * rg + m.RGSGAM2[pm] * rgm) * gam_at(m.GAM2H, p);
+      double Ca = ((double)m.RGSGAM2[p] * rg + (double)m.RGSGAM2[pm] * rgm) * (double)gam_at(m.GAM2H, p);
       double Cb = cC.dfact[k] - cC.cfact[k - 1];
-      double Cu1 = m.RGSGAM2[p] * rg * gam_at(m.GAM2H, pp);
-      double rgh2 = gam_at(m.RGAMH, p) * gam_at(m.RGAMH, p);
-      double Cu2 = gam_at(m.GAM2H, pp) * rgh2 * GCVovR;
-      double Cl1 = m.RGSGAM2[p] * rg * gam_at(m.GAM2H, pm);
-      double Cl2 = gam_at(m.GAM2H, pm) * rgh2 * GCVovR;
+      double Cu1 = (double)m.RGSGAM2[p] * rg * (double)gam_at(m.GAM2H, pp);
+      double rgh2 = (double)gam_at(m.RGAMH, p) * (double)gam_at(m.RGAMH, p);
+      double Cu2 = (double)gam_at(m.GAM2H, pp) * rgh2 * GCVovR;
+      double Cl1 = (double)m.RGSGAM2[p] * rg * (double)gam_at(m.GAM2H, pm);
+      double Cl2 = (double)gam_at(m.GAM2H, pm) * rgh2 * GCVovR;
       double rgh = cC.rdgzh[k];
-      a.Mc[p] = ACVovRt2 / m.RGSQRTH[p] + rgh * (Ca * eth_h(k) - Cb * (gz(k) + GCVovR));
+      a.Mc[p] = ACVovRt2 / (double)m.RGSQRTH[p] + rgh * (Ca * eth_h(k) - Cb * (gz(k) + GCVovR));
       a.Mu[p] = -rgh * (Cu1 * eth_h(k + 1) + cC.cfact[k] * (gz(k + 1) + Cu2));
       a.Ml[p] = -rgh * (Cl1 * eth_h(k - 1) - cC.dfact[k - 1] * (gz(k - 1) + Cl2));
     }
     // total energy at the start of the small steps
-    double kin0 = rhogkin_at(c, m, k, [&](int kk, int comp) { return P[comp][c.at(kk)]; });
+    R kin0 = rhogkin_at(c, m, k, [&](int kk, int comp) { return P[comp][c.at(kk)]; });
     a.ethtot0[p] = a.eth[p] + kin0 / P[0][p] + m.PHI[p];
   }
 }
@@ -441,8 +464,9 @@ __device__ void vp0_column(const Vp0Args& a, int i, int j, int l, int g, int lp)
 // levels kmin..kmax, the divergences of RGAM*rhogv and RGAM*rhogv*eth
 // (div1, div2), the 2-D divergence damping of -vtmp2 (dd) and the pressure
 // gradient of pregd (dpg), written to eight work fields for the column kernel.
+template <class R>
 struct Vp0H {
-  double* out[8];               // div1, div2, dd x/y/z, dpg x/y/z
+  R* out[8];               // div1, div2, dd x/y/z, dpg x/y/z
 };
 
 // vp0 horizontal terms, one block per (level, tile).
@@ -450,28 +474,29 @@ struct Vp0H {
 // static shared memory at larger tiles
 #define VP_DX 32
 #define VP_DY 8
-__global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) {
+template <class R>
+__global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args<R> a, Vp0H<R> h) {
   constexpr int PX = VP_DX + 2, PY = VP_DY + 2, TX = VP_DX + 1, TY = VP_DY + 1;
-  __shared__ double s_m[3][PY * PX];    // RGAM * rhogv
-  __shared__ double s_e[3][PY * PX];    // RGAM * rhogv * eth
-  __shared__ double s_v[3][PY * PX];    // -vtmp2
-  __shared__ double s_p[PY * PX];       // RGAM * pregd at the gradient level
-  __shared__ double s_ti[TY * TX], s_tj[TY * TX];
+  __shared__ R s_m[3][PY * PX];    // RGAM * rhogv
+  __shared__ R s_e[3][PY * PX];    // RGAM * rhogv * eth
+  __shared__ R s_v[3][PY * PX];    // -vtmp2
+  __shared__ R s_p[PY * PX];       // RGAM * pregd at the gradient level
+  __shared__ R s_ti[TY * TX], s_tj[TY * TX];
   const TileLv tl = tile_level<VP_DX, VP_DY>(cD.kmin);
   const int l = tl.l, i0 = tl.i0, j0 = tl.j0;
   const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin;
   const int tid = threadIdx.x, tx = tid % VP_DX, ty = tid / VP_DX;
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= gmax) && (j <= gmax);
-  const double ddc = cC.divdamp_coef;
+  const R ddc = CC.divdamp_coef;
   const int n = cD.npti;
-  const double* cz = cG.C2WGz;
-  const double* const* P = a.P.v;
-  double gxyz[3] = {0.0, 0.0, 0.0};
+  const R* cz = CG.C2WGz;
+  const R* const* P = a.P.v;
+  R gxyz[3] = {R(0.0), R(0.0), R(0.0)};
   int q0 = 0;
   if (own) {
 #pragma unroll
-    for (int d = 0; d < 3; ++d) gxyz[d] = P2(cG.GRD_x, d, i, j, l);
+    for (int d = 0; d < 3; ++d) gxyz[d] = P2(CG.GRD_x, d, i, j, l);
     q0 = ix(i, j, 0, l);
   }
   {
@@ -479,19 +504,19 @@ __global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) 
     const int kk = (k == kmin) ? kmin + 1 : k;
     for (int p = tid; p < PX * PY; p += blockDim.x) {
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
-      double mv[3] = {0.0, 0.0, 0.0}, ev[3] = {0.0, 0.0, 0.0}, vv[3] = {0.0, 0.0, 0.0}, pp = 0.0;
+      R mv[3] = {R(0.0), R(0.0), R(0.0)}, ev[3] = {R(0.0), R(0.0), R(0.0)}, vv[3] = {R(0.0), R(0.0), R(0.0)}, pp = R(0.0);
       if (ii < G && jj < G) {
         const int q = ix(ii, jj, k, l);
-        const double rg = cG.RGAM[q], e = a.eth[q];
+        const R rg = CG.RGAM[q], e = a.eth[q];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          const double pv = P[1 + d][q];
+          const R pv = P[1 + d][q];
           mv[d] = pv * rg;
           ev[d] = (pv * e) * rg;
           vv[d] = -a.vt.f[d][q];
         }
         const int qk = ix(ii, jj, kk, l);
-        pp = a.pregd[qk] * cG.RGAM[qk];
+        pp = a.pregd[qk] * CG.RGAM[qk];
       }
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
@@ -505,10 +530,10 @@ __global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) 
     for (int p = tid; p < TX * TY; p += blockDim.x) {
       const int px = p % TX, py = p / TX;
       const int ii = i0 - 1 + px, jj = j0 - 1 + py;
-      double sTI = 0.0, sTJ = 0.0;
+      R sTI = R(0.0), sTJ = R(0.0);
       if (ii <= G - 2 && jj <= G - 2) {
         const int ia = py * PX + px, ib = ia + 1, ic = ia + PX + 1, id = ia + PX;
-        auto C = [&](int dir, int pt, int t) { return P2(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
+        auto C = [&](int dir, int pt, int t) { return P2(CG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
         sTI = C(0, 0, 0) * s_v[0][ia] + C(0, 1, 0) * s_v[0][ib] + C(0, 2, 0) * s_v[0][ic] +
               C(1, 0, 0) * s_v[1][ia] + C(1, 1, 0) * s_v[1][ib] + C(1, 2, 0) * s_v[1][ic] +
               C(2, 0, 0) * s_v[2][ia] + C(2, 1, 0) * s_v[2][ib] + C(2, 2, 0) * s_v[2][ic];
@@ -525,14 +550,14 @@ __global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) 
       const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
       const int q = q0 + (int)k * cD.planei;
       // divergences (div7: per direction left to right, then x + y + z)
-      double acc1[3], acc2[3];
+      R acc1[3], acc2[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        double s1 = 0.0, s2 = 0.0;
+        R s1 = R(0.0), s2 = R(0.0);
 #pragma unroll
         for (int m = 0; m < 7; ++m) {
-          const double cdv = P2(cG.coef_div, d * 7 + m, i, j, l);
-          const double t1 = cdv * s_m[d][nb[m]], t2 = cdv * s_e[d][nb[m]];
+          const R cdv = P2(CG.coef_div, d * 7 + m, i, j, l);
+          const R t1 = cdv * s_m[d][nb[m]], t2 = cdv * s_e[d][nb[m]];
           s1 = (m == 0) ? t1 : s1 + t1;
           s2 = (m == 0) ? t2 : s2 + t2;
         }
@@ -543,39 +568,39 @@ __global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) 
       h.out[1][q] = acc2[0] + acc2[1] + acc2[2];
       // 2-D divergence damping, projected
       const int ta = (ty + 1) * TX + (tx + 1);
-      const double aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
-      const double cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1], dTJ = s_tj[ta - TX];
-      double dd[3];
+      const R aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
+      const R cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1], dTJ = s_tj[ta - TX];
+      R dd[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d)
-        dd[d] = ddc * (P2(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) +
-                       P2(cG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
-                       P2(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) +
-                       P2(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
-                       P2(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) +
-                       P2(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI));
+        dd[d] = ddc * (P2(CG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) +
+                       P2(CG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
+                       P2(CG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) +
+                       P2(CG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
+                       P2(CG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) +
+                       P2(CG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI));
       {
-        const double prd = div_r(dd[0] * gxyz[0] + dd[1] * gxyz[1] + dd[2] * gxyz[2]);
+        const R prd = div_r(dd[0] * gxyz[0] + dd[1] * gxyz[1] + dd[2] * gxyz[2]);
         dd[0] = dd[0] - div_r(prd * gxyz[0]);
         dd[1] = dd[1] - div_r(prd * gxyz[1]);
         dd[2] = dd[2] - div_r(prd * gxyz[2]);
       }
       // pressure gradient of pregd at level kk
       const int qkk = q0 + (int)kk * cD.planei, qk1 = qkk + cD.planei, qkm = qkk - cD.planei;
-      const double P_k1 = a.pregd[qk1], P_k = a.pregd[qkk], P_km = a.pregd[qkm];
-      const double rgh1 = cG.RGAMH[qk1], rgh0 = cG.RGAMH[qkk];
-      double pg[3];
+      const R P_k1 = a.pregd[qk1], P_k = a.pregd[qkk], P_km = a.pregd[qkm];
+      const R rgh1 = CG.RGAMH[qk1], rgh0 = CG.RGAMH[qkk];
+      R pg[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        double g = P2(cG.coef_grad, d * 7 + 0, i, j, l) * s_p[nb[0]];
+        R g = P2(CG.coef_grad, d * 7 + 0, i, j, l) * s_p[nb[0]];
 #pragma unroll
-        for (int m = 1; m < 7; ++m) g = g + P2(cG.coef_grad, d * 7 + m, i, j, l) * s_p[nb[m]];
-        const double up = (cz[(2 * d) * n + qk1] * P_k1 + cz[(2 * d + 1) * n + qk1] * P_k) * rgh1;
-        const double dn = (cz[(2 * d) * n + qkk] * P_k + cz[(2 * d + 1) * n + qkk] * P_km) * rgh0;
-        pg[d] = g + (up - dn) * cC.rdgz[kk];
+        for (int m = 1; m < 7; ++m) g = g + P2(CG.coef_grad, d * 7 + m, i, j, l) * s_p[nb[m]];
+        const R up = (cz[(2 * d) * n + qk1] * P_k1 + cz[(2 * d + 1) * n + qk1] * P_k) * rgh1;
+        const R dn = (cz[(2 * d) * n + qkk] * P_k + cz[(2 * d + 1) * n + qkk] * P_km) * rgh0;
+        pg[d] = g + (up - dn) * CC.rdgz[kk];
       }
       {
-        const double prd = div_r(pg[0] * gxyz[0] + pg[1] * gxyz[1] + pg[2] * gxyz[2]);
+        const R prd = div_r(pg[0] * gxyz[0] + pg[1] * gxyz[1] + pg[2] * gxyz[2]);
         pg[0] = pg[0] - div_r(prd * gxyz[0]);
         pg[1] = pg[1] - div_r(prd * gxyz[1]);
         pg[2] = pg[2] - div_r(prd * gxyz[2]);
@@ -603,7 +628,8 @@ __global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args a, Vp0H h) 
 // 256-thread blocks capped at 64 registers (four per SM; measured faster
 // than three at 74 registers)
 #define NC_VP0C_BLOCK 256
-__global__ void __launch_bounds__(NC_VP0C_BLOCK, 4) k_vp0_cr(Vp0Args a, Vp0H h) {
+template <class R>
+__global__ void __launch_bounds__(NC_VP0C_BLOCK, 4) k_vp0_cr(Vp0Args<R> a, Vp0H<R> h) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
@@ -611,12 +637,12 @@ __global__ void __launch_bounds__(NC_VP0C_BLOCK, 4) k_vp0_cr(Vp0Args a, Vp0H h) 
   const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
   const int n = cD.npti;
   const bool in = interior(i, j);
-  const double* const* P = a.P.v;
+  const R* const* P = a.P.v;
   const double dt = a.dt;
   const double GRAV = cC.GRAV;
-  const double* cz = cG.C2WGz;
-  const double* c2w = cG.C2W;
-  const double* w2c = cG.W2C;
+  const R* cz = CG.C2WGz;
+  const R* c2w = CG.C2W;
+  const R* w2c = CG.W2C;
   const double GCVovR = cC.GRAV * cC.CVdry / cC.Rdry;
   const double ACVovRt2 = cC.alpha * cC.CVdry / cC.Rdry / (dt * dt);
   // values at level k (index 0) and k-1 (index m), carried upward
@@ -632,7 +658,7 @@ __global__ void __launch_bounds__(NC_VP0C_BLOCK, 4) k_vp0_cr(Vp0Args a, Vp0H h) 
     if (kn < KA) {
       const int q = c.at(kn), qm = c.at(kn - 1);
       if (kn > kmin && kn <= kmax) {
-        const double rgh = gam_at(cG.RGAMH, q), rsq = cG.RGSQRTH[q];
+        const double rgh = gam_at(CG.RGAMH, q), rsq = CG.RGSQRTH[q];
         const double z0 = cz[q], z1 = cz[n + q], z2 = cz[2 * n + q], z3 = cz[3 * n + q], z4 = cz[4 * n + q],
                      z5 = cz[5 * n + q];
         const double px = P[1][q], pxm = P[1][qm], py = P[2][q], pym = P[2][qm], pz = P[3][q], pzm = P[3][qm];
@@ -647,7 +673,7 @@ __global__ void __launch_bounds__(NC_VP0C_BLOCK, 4) k_vp0_cr(Vp0Args a, Vp0H h) 
         vint1 = 0.5 * (w * w) / den;
         // buoyancy and vertical pressure gradient
         dbuo1 = -GRAV * (c2w[q] * a.rhogd[q] + c2w[n + q] * a.rhogd[qm]);
-        dpgw1 = gam_at(cG.GAM2H, q) * (a.pregd[q] * cG.RGSGAM2[q] - a.pregd[qm] * cG.RGSGAM2[qm]) * cC.rdgzh[kn];
+        dpgw1 = gam_at(CG.GAM2H, q) * (a.pregd[q] * CG.RGSGAM2[q] - a.pregd[qm] * CG.RGSGAM2[qm]) * cC.rdgzh[kn];
       }
       if (kn >= kmin && kn <= kmax + 1) {
         const int kk = kn;   // kn >= kmin here, so the clamp of rhog_h / eth_h is inactive
@@ -681,15 +707,15 @@ __global__ void __launch_bounds__(NC_VP0C_BLOCK, 4) k_vp0_cr(Vp0Args a, Vp0H h) 
     if (k >= kmin + 1 && k <= kmax) {
       const int pm = c.at(k - 1), pp = c.at(k + 1);
       const double rg = cC.rdgz[k], rgm = cC.rdgz[k - 1];
-      const double Ca = (cG.RGSGAM2[p] * rg + cG.RGSGAM2[pm] * rgm) * gam_at(cG.GAM2H, p);
+      const double Ca = (CG.RGSGAM2[p] * rg + CG.RGSGAM2[pm] * rgm) * gam_at(CG.GAM2H, p);
       const double Cb = cC.dfact[k] - cC.cfact[k - 1];
-      const double Cu1 = cG.RGSGAM2[p] * rg * gam_at(cG.GAM2H, pp);
-      const double rgh2 = gam_at(cG.RGAMH, p) * gam_at(cG.RGAMH, p);
-      const double Cu2 = gam_at(cG.GAM2H, pp) * rgh2 * GCVovR;
-      const double Cl1 = cG.RGSGAM2[p] * rg * gam_at(cG.GAM2H, pm);
-      const double Cl2 = gam_at(cG.GAM2H, pm) * rgh2 * GCVovR;
+      const double Cu1 = CG.RGSGAM2[p] * rg * gam_at(CG.GAM2H, pp);
+      const double rgh2 = gam_at(CG.RGAMH, p) * gam_at(CG.RGAMH, p);
+      const double Cu2 = gam_at(CG.GAM2H, pp) * rgh2 * GCVovR;
+      const double Cl1 = CG.RGSGAM2[p] * rg * gam_at(CG.GAM2H, pm);
+      const double Cl2 = gam_at(CG.GAM2H, pm) * rgh2 * GCVovR;
       const double rgh = cC.rdgzh[k];
-      a.Mc[p] = ACVovRt2 / cG.RGSQRTH[p] + rgh * (Ca * eh0 - Cb * (gz0 + GCVovR));
+      a.Mc[p] = ACVovRt2 / CG.RGSQRTH[p] + rgh * (Ca * eh0 - Cb * (gz0 + GCVovR));
       a.Mu[p] = -rgh * (Cu1 * eh1 + cC.cfact[k] * (gz1 + Cu2));
       a.Ml[p] = -rgh * (Cl1 * ehm - cC.dfact[k - 1] * (gzm + Cl2));
     }
@@ -699,7 +725,7 @@ __global__ void __launch_bounds__(NC_VP0C_BLOCK, 4) k_vp0_cr(Vp0Args a, Vp0H h) 
       const double kh = 0.5 * (vx * vx + vy * vy + vz * vz) / rg;
       kin0 = kh + w2c[p] * vint1 + w2c[n + p] * vint0;
     }
-    a.ethtot0[p] = a.eth[p] + kin0 / P[0][p] + cG.PHI[p];
+    a.ethtot0[p] = a.eth[p] + kin0 / P[0][p] + CG.PHI[p];
     vA0 = vA1; vE0 = vE1;
     gzm = gz0; gz0 = gz1;
     ehm = eh0; eh0 = eh1;
@@ -707,43 +733,45 @@ __global__ void __launch_bounds__(NC_VP0C_BLOCK, 4) k_vp0_cr(Vp0Args a, Vp0H h) 
   }
 }
 
-__global__ void k_vp0(Vp0Args a, int pole) {
+template <class R>
+__global__ void k_vp0(Vp0Args<R> a, int pole) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
-  if (!pole) vp0_column<false>(a, i, j, l, 0, 0);
-  else vp0_column<true>(a, 0, 0, 0, g, lp);
+  if (!pole) vp0_column<R, false>(a, i, j, l, 0, 0);
+  else vp0_column<R, true>(a, 0, 0, 0, g, lp);
 }
 
 // ---------------------------------------------------------------------------
 // acoustic loop, path1 (kernels/vipath1.py:68-160): diff_vh with BNDCND and
 // the running mean of the horizontal momentum.
 // ---------------------------------------------------------------------------
+template <class R>
 struct Path1Args {
-  const double* PS[6];     // PROG_split (RHOGE boundary rows read clamped)
-  const double* rhog;      // PROG rhog
-  const double* gT[6];
-  CThree vt;               // post-COMM 3-D divdamp of PROG_split
-  double* dvh[3];          // out
-  double* PM[5];           // running mean (in/out)
-  double dt, rweight, RovCV;
+  const R* PS[6];     // PROG_split (RHOGE boundary rows read clamped)
+  const R* rhog;      // PROG rhog
+  const R* gT[6];
+  CThree<R> vt;               // post-COMM 3-D divdamp of PROG_split
+  R* dvh[3];          // out
+  R* PM[5];           // running mean (in/out)
+  R dt, rweight, RovCV;
 };
 
-template <bool POLE>
-__device__ void path1_column(const Path1Args& a, int i, int j, int l, int g, int lp) {
+template <class R, bool POLE>
+__device__ void path1_column(const Path1Args<R>& a, int i, int j, int l, int g, int lp) {
   const Col c = POLE ? col_pl(g, lp) : col_reg(i, j, l);
-  const Met m = met_of(POLE);
+  const MetT<R> m = met_of<R>(POLE);
   const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
-  const double dt = a.dt;
-  auto pregs = [&](int base_q, int kk) -> double {  // preg_prim_split with clamped boundary rows
+  const R dt = a.dt;
+  auto pregs = [&](int base_q, int kk) -> R {  // preg_prim_split with clamped boundary rows
     int k2 = kk < kmin ? kmin : (kk > kmax ? kmax : kk);
     return a.PS[5][base_q + (int)k2 * c.ks] * a.RovCV;
   };
-  double vals[3][2];  // values at kmin and kmax for the boundary rows
-  double* const* out = a.dvh;
+  R vals[3][2];  // values at kmin and kmax for the boundary rows
+  R* const* out = a.dvh;
   for (int k = 0; k < KA; ++k) {
     int p = c.at(k);
-    double dd[3], pg[3];
+    R dd[3], pg[3];
     if (!POLE) {
       divdamp2d_at(a.vt, i, j, k, l, dd);
       presgrad_reg(i, j, k, l, c, m, [&](int ii, int jj, int kk) { return pregs(ix(ii, jj, 0, l), kk); }, pg);
@@ -752,8 +780,8 @@ __device__ void path1_column(const Path1Args& a, int i, int j, int l, int g, int
       presgrad_pl(g, k, lp, c, m, [&](int gg, int kk) { return pregs((int)gg * cD.KA * cD.LP + lp, kk); }, pg);
     }
     for (int d = 0; d < 3; ++d) {
-      double drv = a.gT[1 + d][p] - pg[d] + dd[d] + 0.0;
-      double v = a.PS[1 + d][p] + drv * dt;
+      R drv = a.gT[1 + d][p] - pg[d] + dd[d] + R(0.0);
+      R v = a.PS[1 + d][p] + drv * dt;
       out[d][p] = v;
       if (k == kmin) vals[d][0] = v;
       if (k == kmax) vals[d][1] = v;
@@ -761,8 +789,8 @@ __device__ void path1_column(const Path1Args& a, int i, int j, int l, int g, int
   }
   const int pT = c.at(kmax + 1), pK = c.at(kmax), pB = c.at(kmin - 1), pN = c.at(kmin);
   for (int d = 0; d < 3; ++d) {
-    out[d][pT] = 1.0 * (vals[d][1] / a.rhog[pK]) * a.rhog[pT];
-    out[d][pB] = -1.0 * (vals[d][0] / a.rhog[pN]) * a.rhog[pB];
+    out[d][pT] = R(1.0) * (vals[d][1] / a.rhog[pK]) * a.rhog[pT];
+    out[d][pB] = -R(1.0) * (vals[d][0] / a.rhog[pN]) * a.rhog[pB];
   }
   for (int k = 0; k < KA; ++k) {
     int p = c.at(k);
@@ -773,27 +801,28 @@ __device__ void path1_column(const Path1Args& a, int i, int j, int l, int g, int
 // Regional path 1, one block per (level, tile): same stencils and
 // arithmetic as path1_column.  The blocks at kmin and kmax also write the
 // boundary rows kmin-1 and kmax+1 from the values they computed.
-__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_path1_l(Path1Args a) {
+template <class R>
+__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_path1_l(Path1Args<R> a) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
-  __shared__ double s_v[3][PY * PX];
-  __shared__ double s_p[PY * PX];
-  __shared__ double s_ti[TY * TX], s_tj[TY * TX];
+  __shared__ R s_v[3][PY * PX];
+  __shared__ R s_p[PY * PX];
+  __shared__ R s_ti[TY * TX], s_tj[TY * TX];
   const TileLv tl = tile_level<DD_DX, DD_DY>(cD.kmin);
   const int k = tl.k, l = tl.l, i0 = tl.i0, j0 = tl.j0;
   const int G = cD.G, gmax = cD.G - 2, kmin = cD.kmin, kmax = cD.kmax;
   const int kk = (k == kmin) ? kmin + 1 : k;
   const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
-  const double RovCV = a.RovCV;
+  const R RovCV = a.RovCV;
   for (int p = tid; p < PX * PY; p += blockDim.x) {
     const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
-    double x = 0.0, y = 0.0, z = 0.0, pp = 0.0;
+    R x = R(0.0), y = R(0.0), z = R(0.0), pp = R(0.0);
     if (ii < G && jj < G) {
       const int q = ix(ii, jj, k, l);
       x = -__ldg(&a.vt.f[0][q]);
       y = -__ldg(&a.vt.f[1][q]);
       z = -__ldg(&a.vt.f[2][q]);
       const int qk = ix(ii, jj, kk, l);
-      pp = __ldg(&a.PS[5][qk]) * RovCV * __ldg(&cG.RGAM[qk]);
+      pp = __ldg(&a.PS[5][qk]) * RovCV * __ldg(&CG.RGAM[qk]);
     }
     s_v[0][p] = x;
     s_v[1][p] = y;
@@ -804,10 +833,10 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_path1_l(Path1Args
   for (int p = tid; p < TX * TY; p += blockDim.x) {
     const int px = p % TX, py = p / TX;
     const int ii = i0 - 1 + px, jj = j0 - 1 + py;
-    double sTI = 0.0, sTJ = 0.0;
+    R sTI = R(0.0), sTJ = R(0.0);
     if (ii <= G - 2 && jj <= G - 2) {
       const int ia = py * PX + px, ib = ia + 1, ic = ia + PX + 1, id = ia + PX;
-      auto C = [&](int dir, int pt, int t) { return P2c(cG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
+      auto C = [&](int dir, int pt, int t) { return P2c(CG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
       sTI = C(0, 0, 0) * s_v[0][ia] + C(0, 1, 0) * s_v[0][ib] + C(0, 2, 0) * s_v[0][ic] +
             C(1, 0, 0) * s_v[1][ia] + C(1, 1, 0) * s_v[1][ib] + C(1, 2, 0) * s_v[1][ic] +
             C(2, 0, 0) * s_v[2][ia] + C(2, 1, 0) * s_v[2][ib] + C(2, 2, 0) * s_v[2][ic];
@@ -821,56 +850,56 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_path1_l(Path1Args
   __syncthreads();
   const int i = i0 + tx, j = j0 + ty;
   if (i > gmax || j > gmax) return;
-  const double ddc = cC.divdamp_coef, dt = a.dt, rweight = a.rweight;
+  const R ddc = CC.divdamp_coef, dt = a.dt, rweight = a.rweight;
   const int n = cD.npti;
-  const double* cz = cG.C2WGz;
-  const double gx = P2c(cG.GRD_x, 0, i, j, l), gy = P2c(cG.GRD_x, 1, i, j, l), gz = P2c(cG.GRD_x, 2, i, j, l);
+  const R* cz = CG.C2WGz;
+  const R gx = P2c(CG.GRD_x, 0, i, j, l), gy = P2c(CG.GRD_x, 1, i, j, l), gz = P2c(CG.GRD_x, 2, i, j, l);
   const int q0 = ix(i, j, 0, l);
   auto Pown = [&](int k2) {
     const int kc = k2 < kmin ? kmin : (k2 > kmax ? kmax : k2);
     return __ldg(&a.PS[5][q0 + (int)kc * cD.planei]) * RovCV;
   };
   const int ta = (ty + 1) * TX + (tx + 1);
-  const double aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
-  const double cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1], dTJ = s_tj[ta - TX];
-  double dd[3];
+  const R aTI = s_ti[ta], aTJ = s_tj[ta], bTI = s_ti[ta - 1];
+  const R cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1], dTJ = s_tj[ta - TX];
+  R dd[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d)
-    dd[d] = ddc * (P2c(cG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) + P2c(cG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
-                   P2c(cG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) + P2c(cG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
-                   P2c(cG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) + P2c(cG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI));
+    dd[d] = ddc * (P2c(CG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) + P2c(CG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
+                   P2c(CG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) + P2c(CG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
+                   P2c(CG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) + P2c(CG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI));
   {
-    const double prd = div_r(dd[0] * gx + dd[1] * gy + dd[2] * gz);
+    const R prd = div_r(dd[0] * gx + dd[1] * gy + dd[2] * gz);
     dd[0] = dd[0] - div_r(prd * gx);
     dd[1] = dd[1] - div_r(prd * gy);
     dd[2] = dd[2] - div_r(prd * gz);
   }
   const int c0 = (ty + 1) * PX + (tx + 1);
-  const double s7[7] = {s_p[c0], s_p[c0 + 1], s_p[c0 + PX + 1], s_p[c0 + PX], s_p[c0 - 1], s_p[c0 - PX - 1], s_p[c0 - PX]};
+  const R s7[7] = {s_p[c0], s_p[c0 + 1], s_p[c0 + PX + 1], s_p[c0 + PX], s_p[c0 - 1], s_p[c0 - PX - 1], s_p[c0 - PX]};
   const int qkk = q0 + (int)kk * cD.planei, qk1 = qkk + cD.planei;
-  const double P_k1 = Pown(kk + 1), P_k = Pown(kk), P_km = Pown(kk - 1);
-  const double rgh1 = __ldg(&cG.RGAMH[qk1]), rgh0 = __ldg(&cG.RGAMH[qkk]);
-  double pg[3];
+  const R P_k1 = Pown(kk + 1), P_k = Pown(kk), P_km = Pown(kk - 1);
+  const R rgh1 = __ldg(&CG.RGAMH[qk1]), rgh0 = __ldg(&CG.RGAMH[qkk]);
+  R pg[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    double g = P2c(cG.coef_grad, d * 7 + 0, i, j, l) * s7[0];
+    R g = P2c(CG.coef_grad, d * 7 + 0, i, j, l) * s7[0];
 #pragma unroll
-    for (int m = 1; m < 7; ++m) g = g + P2c(cG.coef_grad, d * 7 + m, i, j, l) * s7[m];
-    const double up = (__ldg(&cz[(2 * d) * n + qk1]) * P_k1 + __ldg(&cz[(2 * d + 1) * n + qk1]) * P_k) * rgh1;
-    const double dn = (__ldg(&cz[(2 * d) * n + qkk]) * P_k + __ldg(&cz[(2 * d + 1) * n + qkk]) * P_km) * rgh0;
-    pg[d] = g + (up - dn) * cC.rdgz[kk];
+    for (int m = 1; m < 7; ++m) g = g + P2c(CG.coef_grad, d * 7 + m, i, j, l) * s7[m];
+    const R up = (__ldg(&cz[(2 * d) * n + qk1]) * P_k1 + __ldg(&cz[(2 * d + 1) * n + qk1]) * P_k) * rgh1;
+    const R dn = (__ldg(&cz[(2 * d) * n + qkk]) * P_k + __ldg(&cz[(2 * d + 1) * n + qkk]) * P_km) * rgh0;
+    pg[d] = g + (up - dn) * CC.rdgz[kk];
   }
   {
-    const double prd = div_r(pg[0] * gx + pg[1] * gy + pg[2] * gz);
+    const R prd = div_r(pg[0] * gx + pg[1] * gy + pg[2] * gz);
     pg[0] = pg[0] - div_r(prd * gx);
     pg[1] = pg[1] - div_r(prd * gy);
     pg[2] = pg[2] - div_r(prd * gz);
   }
   const int q = q0 + (int)k * cD.planei;
-  double v[3];
+  R v[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    const double drv = __ldg(&a.gT[1 + d][q]) - pg[d] + dd[d] + 0.0;
+    const R drv = __ldg(&a.gT[1 + d][q]) - pg[d] + dd[d] + R(0.0);
     v[d] = __ldg(&a.PS[1 + d][q]) + drv * dt;
     a.dvh[d][q] = v[d];
     a.PM[1 + d][q] = a.PM[1 + d][q] + v[d] * rweight;
@@ -879,7 +908,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_path1_l(Path1Args
     const int pB = q - cD.planei;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const double vB = -1.0 * (v[d] / __ldg(&a.rhog[q])) * __ldg(&a.rhog[pB]);
+      const R vB = -R(1.0) * (v[d] / __ldg(&a.rhog[q])) * __ldg(&a.rhog[pB]);
       a.dvh[d][pB] = vB;
       a.PM[1 + d][pB] = a.PM[1 + d][pB] + vB * rweight;
     }
@@ -888,19 +917,20 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_path1_l(Path1Args
     const int pT = q + cD.planei;
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const double vT = 1.0 * (v[d] / __ldg(&a.rhog[q])) * __ldg(&a.rhog[pT]);
+      const R vT = R(1.0) * (v[d] / __ldg(&a.rhog[q])) * __ldg(&a.rhog[pT]);
       a.dvh[d][pT] = vT;
       a.PM[1 + d][pT] = a.PM[1 + d][pT] + vT * rweight;
     }
   }
 }
 
-__global__ void k_path1(Path1Args a, int pole) {
+template <class R>
+__global__ void k_path1(Path1Args<R> a, int pole) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
-  if (!pole) path1_column<false>(a, i, j, l, 0, 0);
-  else path1_column<true>(a, 0, 0, 0, g, lp);
+  if (!pole) path1_column<R, false>(a, i, j, l, 0, 0);
+  else path1_column<R, true>(a, 0, 0, 0, g, lp);
 }
 
 // ---------------------------------------------------------------------------
@@ -908,22 +938,24 @@ __global__ void k_path1(Path1Args a, int pole) {
 // then per column the flux convergences, the tridiagonal Thomas solve
 // (kernels/virhowsolver.py:42-120), kinetic energies and the energy update.
 // ---------------------------------------------------------------------------
+template <class R>
 struct VimainArgs {
-  const double* PS[6];
-  const double* P[6];          // PROG
-  const double *eth, *ethtot0;
-  const double* gT[6];         // small-step tendency
-  const double* gT0e;          // large-step tendency of RHOGE (grhogetot)
-  const double *Mc, *Mu, *Ml;
-  CThree dvh;                  // post-COMM diff_vh
-  double* hdiv[3];             // kernel A output
-  double* dwe[3];              // out: rhog_s1, rhogw_s1, rhoge_s1
-  double* PM0;                 // running mean of RHOG (in/out)
-  double* PM4;                 // running mean of RHOGW (in/out)
+  const R* PS[6];
+  const R* P[6];          // PROG
+  const R *eth, *ethtot0;
+  const R* gT[6];         // small-step tendency
+  const R* gT0e;          // large-step tendency of RHOGE (grhogetot)
+  const double *Mc, *Mu, *Ml;  // float64 in both forms
+  CThree<R> dvh;                  // post-COMM diff_vh
+  R* hdiv[3];             // kernel A output
+  R* dwe[3];              // out: rhog_s1, rhogw_s1, rhoge_s1
+  R* PM0;                 // running mean of RHOG (in/out)
+  R* PM4;                 // running mean of RHOGW (in/out)
   double dt, rweight, RovCV;
 };
 
-__global__ void k_vimain_a(VimainArgs a, int pole) {
+template <class R>
+__global__ void k_vimain_a(VimainArgs<R> a, int pole) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!pole) {
@@ -931,19 +963,19 @@ __global__ void k_vimain_a(VimainArgs a, int pole) {
     const bool in = interior(i, j);
     for (int k = 0; k < cD.KA; ++k) {
       int p = ix(i, j, k, l);
-      double h1 = 0.0, h2 = 0.0, h3 = 0.0;
+      R h1 = R(0.0), h2 = R(0.0), h3 = R(0.0);
       if (in && k >= cD.kmin && k <= cD.kmax) {
-        h1 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
+        h1 = div7<R>(i, j, k, l, [&](int ii, int jj, int kk, int d) {
           int q = ix(ii, jj, kk, l);
-          return a.dvh.f[d][q] * gam_at(cG.RGAM, q);
+          return a.dvh.f[d][q] * gam_at(CG.RGAM, q);
         });
-        h2 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
+        h2 = div7<R>(i, j, k, l, [&](int ii, int jj, int kk, int d) {
           int q = ix(ii, jj, kk, l);
-          return (a.dvh.f[d][q] * a.eth[q]) * gam_at(cG.RGAM, q);
+          return (a.dvh.f[d][q] * a.eth[q]) * gam_at(CG.RGAM, q);
         });
-        h3 = div7(i, j, k, l, [&](int ii, int jj, int kk, int d) {
+        h3 = div7<R>(i, j, k, l, [&](int ii, int jj, int kk, int d) {
           int q = ix(ii, jj, kk, l);
-          return ((a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q]) * gam_at(cG.RGAM, q);
+          return ((a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q]) * gam_at(CG.RGAM, q);
         });
       }
       a.hdiv[0][p] = h1; a.hdiv[1][p] = h2; a.hdiv[2][p] = h3;
@@ -954,11 +986,11 @@ __global__ void k_vimain_a(VimainArgs a, int pole) {
       int k = (int)(tp / cD.LP), lp = (int)(tp % cD.LP);
       for (int g = 0; g < 6; ++g) {
         int p = ipl(g, k, lp);
-        double h1 = 0.0, h2 = 0.0, h3 = 0.0;
+        R h1 = R(0.0), h2 = R(0.0), h3 = R(0.0);
         if (g == 0 && k >= cD.kmin && k <= cD.kmax) {
-          h1 = div_pl(lp, k, [&](int q, int d) { return a.dvh.f[d][q]; });
-          h2 = div_pl(lp, k, [&](int q, int d) { return a.dvh.f[d][q] * a.eth[q]; });
-          h3 = div_pl(lp, k, [&](int q, int d) { return (a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q]; });
+          h1 = div_pl<R>(lp, k, [&](int q, int d) { return a.dvh.f[d][q]; });
+          h2 = div_pl<R>(lp, k, [&](int q, int d) { return a.dvh.f[d][q] * a.eth[q]; });
+          h3 = div_pl<R>(lp, k, [&](int q, int d) { return (a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q]; });
         }
         a.hdiv[0][p] = h1; a.hdiv[1][p] = h2; a.hdiv[2][p] = h3;
       }
@@ -968,9 +1000,10 @@ __global__ void k_vimain_a(VimainArgs a, int pole) {
 
 // vi_main kernel A, one block per (level, tile): the horizontal divergences
 // of RGAM*diff_vh, RGAM*diff_vh*eth and RGAM*(rhogv + diff_vh)*ethtot0.
-__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_vimain_a_l(VimainArgs a) {
+template <class R>
+__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_vimain_a_l(VimainArgs<R> a) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2;
-  __shared__ double s_h[3][3][PY * PX];
+  __shared__ R s_h[3][3][PY * PX];
   const TileLv tl = tile_level<DD_DX, DD_DY>(cD.kmin);
   const int l = tl.l, i0 = tl.i0, j0 = tl.j0;
   const int G = cD.G, gmax = cD.G - 2;
@@ -983,10 +1016,10 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_vimain_a_l(Vimain
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
       if (ii < G && jj < G) {
         const int q = ix(ii, jj, k, l);
-        const double rg = gam_at_ldg(cG.RGAM, q), e = __ldg(&a.eth[q]), et = __ldg(&a.ethtot0[q]);
+        const R rg = gam_at_ldg(CG.RGAM, q), e = __ldg(&a.eth[q]), et = __ldg(&a.ethtot0[q]);
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          const double dv = __ldg(&a.dvh.f[d][q]);
+          const R dv = __ldg(&a.dvh.f[d][q]);
           s_h[0][d][p] = dv * rg;
           s_h[1][d][p] = (dv * e) * rg;
           s_h[2][d][p] = ((__ldg(&a.P[1 + d][q]) + dv) * et) * rg;
@@ -995,7 +1028,7 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_vimain_a_l(Vimain
 #pragma unroll
         for (int f = 0; f < 3; ++f)
 #pragma unroll
-          for (int d = 0; d < 3; ++d) s_h[f][d][p] = 0.0;
+          for (int d = 0; d < 3; ++d) s_h[f][d][p] = R(0.0);
       }
     }
     __syncthreads();
@@ -1003,16 +1036,16 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_vimain_a_l(Vimain
       const int c0 = (ty + 1) * PX + (tx + 1);
       const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
       const int q = ix(i, j, k, l);
-      double acc[3][3];
+      R acc[3][3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        double s[3] = {0.0, 0.0, 0.0};
+        R s[3] = {R(0.0), R(0.0), R(0.0)};
 #pragma unroll
         for (int m = 0; m < 7; ++m) {
-          const double cdv = P2c(cG.coef_div, d * 7 + m, i, j, l);
+          const R cdv = P2c(CG.coef_div, d * 7 + m, i, j, l);
 #pragma unroll
           for (int f = 0; f < 3; ++f) {
-            const double t = cdv * s_h[f][d][nb[m]];
+            const R t = cdv * s_h[f][d][nb[m]];
             s[f] = (m == 0) ? t : s[f] + t;
           }
         }
@@ -1026,50 +1059,56 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_vimain_a_l(Vimain
   }
 }
 
-template <bool POLE>
-__device__ void vimain_column(const VimainArgs& a, const Col c) {
-  const Met m = met_of(POLE);
+// One pole column of vi_main.  In the mixed form the flux convergences and
+// the energy update run in float32 (R) and the tridiagonal solve in float64,
+// as in the regional kernels k_vi_solve / k_vi_energy_p.
+template <class R, bool POLE>
+__device__ void vimain_column(const VimainArgs<R>& a, const Col c) {
+  const MetT<R> m = met_of<R>(POLE);
   const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
   const double dt = a.dt;
+  const R dtR = R(a.dt);
   const double Rdry = cC.Rdry, CVdry = cC.CVdry;
-  auto PSk = [&](int comp, int k) -> double {  // PROG_split with clamped RHOGE boundary rows
+  auto PSk = [&](int comp, int k) -> R {  // PROG_split with clamped RHOGE boundary rows
     if (comp == 5) k = k < kmin ? kmin : (k > kmax ? kmax : k);
     return a.PS[comp][c.at(k)];
   };
-  auto preg0 = [&](int k) -> double { return PSk(5, k) * a.RovCV; };
-  auto DV = [&](int k, int d) -> double { return a.dvh.f[d][c.at(k)]; };
-  auto DVE = [&](int k, int d) -> double { return a.dvh.f[d][c.at(k)] * a.eth[c.at(k)]; };
+  auto preg0 = [&](int k) -> double { return (double)PSk(5, k) * a.RovCV; };
+  auto DV = [&](int k, int d) -> R { return a.dvh.f[d][c.at(k)]; };
+  auto DVE = [&](int k, int d) -> R { return a.dvh.f[d][c.at(k)] * a.eth[c.at(k)]; };
   // grhog1 and gpre on every level
   double grhog1[NC_MAXK], gpre[NC_MAXK];
   for (int k = 0; k < KA; ++k) {
     int p = c.at(k);
-    double drhog = fluxconv_col(c, m, k, a.hdiv[0][p], 0.0, DV, [&](int kk) { return PSk(4, kk); });
-    double drhoge = fluxconv_col(c, m, k, a.hdiv[1][p], 0.0, DVE, [&](int kk) { return 0.0; });
-    grhog1[k] = a.gT[0][p] + drhog;
-    double grhoge1 = a.gT[5][p] + drhoge;
+    R drhog = fluxconv_col(c, m, k, a.hdiv[0][p], R(0.0), DV, [&](int kk) { return PSk(4, kk); });
+    R drhoge = fluxconv_col(c, m, k, a.hdiv[1][p], R(0.0), DVE, [&](int kk) { return R(0.0); });
+    grhog1[k] = (double)a.gT[0][p] + (double)drhog;
+    double grhoge1 = (double)a.gT[5][p] + (double)drhoge;
     gpre[k] = grhoge1 * Rdry / CVdry;
   }
-  // Thomas solve (kernels/virhowsolver.py:67-120)
+  // Thomas solve (kernels/virhowsolver.py:67-120), float64
   const int kT = kmax + 1;
-  double rw_top = -(mc(m.C2WGz, c, 0, 6, kT) * DV(kT, 0) + mc(m.C2WGz, c, 1, 6, kT) * DV(kmax, 0) +
-                    mc(m.C2WGz, c, 2, 6, kT) * DV(kT, 1) + mc(m.C2WGz, c, 3, 6, kT) * DV(kmax, 1) +
-                    mc(m.C2WGz, c, 4, 6, kT) * DV(kT, 2) + mc(m.C2WGz, c, 5, 6, kT) * DV(kmax, 2));
+  double rw_top = -((double)mc(m.C2WGz, c, 0, 6, kT) * DV(kT, 0) + (double)mc(m.C2WGz, c, 1, 6, kT) * DV(kmax, 0) +
+                    (double)mc(m.C2WGz, c, 2, 6, kT) * DV(kT, 1) + (double)mc(m.C2WGz, c, 3, 6, kT) * DV(kmax, 1) +
+                    (double)mc(m.C2WGz, c, 4, 6, kT) * DV(kT, 2) + (double)mc(m.C2WGz, c, 5, 6, kT) * DV(kmax, 2));
   const double CVovRt2 = CVdry / Rdry / (dt * dt);
-  const double rw_kmin = 0.0 * m.RGSGAM2H[c.at(kmin)];
-  const double rw_kmaxp1 = rw_top * m.RGSGAM2H[c.at(kT)];
+  const double rw_kmin = 0.0 * (double)m.RGSGAM2H[c.at(kmin)];
+  const double rw_kmaxp1 = rw_top * (double)m.RGSGAM2H[c.at(kT)];
   const int N = kmax - kmin;
   double u[NC_MAXK], gam[NC_MAXK];
   double beta = 0.0;
   for (int n = 0; n < N; ++n) {
     int k = kmin + 1 + n;
     int p = c.at(k), pm = c.at(k - 1);
-    double rg2 = gam_at(m.RGAMH, p) * gam_at(m.RGAMH, p);
-    double rgam2 = gam_at(m.RGAM, p) * gam_at(m.RGAM, p), rgam2m = gam_at(m.RGAM, pm) * gam_at(m.RGAM, pm);
-    double Sw = a.gT[4][p] + 0.0 * cC.alpha;
-    double S = ((PSk(4, k) * cC.alpha + dt * Sw) * rg2 -
-                ((preg0(k) + dt * gpre[k]) * m.RGSGAM2[p] - (preg0(k - 1) + dt * gpre[k - 1]) * m.RGSGAM2[pm]) * dt *
-                    cC.rdgzh[k] -
-                ((PSk(0, k) + dt * grhog1[k]) * rgam2 * cC.afact[k] + (PSk(0, k - 1) + dt * grhog1[k - 1]) * rgam2m * cC.bfact[k]) *
+    double rg2 = (double)gam_at(m.RGAMH, p) * (double)gam_at(m.RGAMH, p);
+    double rgam2 = (double)gam_at(m.RGAM, p) * (double)gam_at(m.RGAM, p);
+    double rgam2m = (double)gam_at(m.RGAM, pm) * (double)gam_at(m.RGAM, pm);
+    double Sw = (double)a.gT[4][p] + 0.0 * cC.alpha;
+    double S = (((double)PSk(4, k) * cC.alpha + dt * Sw) * rg2 -
+                ((preg0(k) + dt * gpre[k]) * (double)m.RGSGAM2[p] - (preg0(k - 1) + dt * gpre[k - 1]) * (double)m.RGSGAM2[pm]) *
+                    dt * cC.rdgzh[k] -
+                (((double)PSk(0, k) + dt * grhog1[k]) * rgam2 * cC.afact[k] +
+                 ((double)PSk(0, k - 1) + dt * grhog1[k - 1]) * rgam2m * cC.bfact[k]) *
                     dt * cC.GRAV) *
                CVovRt2;
     if (n == 0) S = S - a.Ml[c.at(kmin + 1)] * rw_kmin;
@@ -1085,55 +1124,55 @@ __device__ void vimain_column(const VimainArgs& a, const Col c) {
       gam[n] = gg;
     }
   }
-  double rws1[NC_MAXK];
-  for (int k = 0; k < KA; ++k) rws1[k] = 0.0;
+  R rws1[NC_MAXK];
+  for (int k = 0; k < KA; ++k) rws1[k] = R(0.0);
   {
     double x = u[N - 1];
-    rws1[kmin + N] = x * m.GSGAM2H[c.at(kmin + N)];
+    rws1[kmin + N] = R(x * (double)m.GSGAM2H[c.at(kmin + N)]);
     for (int n = N - 2; n >= 0; --n) {
       x = u[n] - gam[n + 1] * x;
-      rws1[kmin + 1 + n] = x * m.GSGAM2H[c.at(kmin + 1 + n)];
+      rws1[kmin + 1 + n] = R(x * (double)m.GSGAM2H[c.at(kmin + 1 + n)]);
     }
-    rws1[kmin] = rw_kmin * m.GSGAM2H[c.at(kmin)];
-    rws1[kT] = rw_kmaxp1 * m.GSGAM2H[c.at(kT)];
+    rws1[kmin] = R(rw_kmin * (double)m.GSGAM2H[c.at(kmin)]);
+    rws1[kT] = R(rw_kmaxp1 * (double)m.GSGAM2H[c.at(kT)]);
   }
   // rhog_split1, kinetic energies, total-energy advection, rhoge_split1
-  double rs1[NC_MAXK];
+  R rs1[NC_MAXK];
   for (int k = 0; k < KA; ++k) {
     int p = c.at(k);
-    double drhog2 = fluxconv_col(c, m, k, a.hdiv[0][p], 1.0, DV, [&](int kk) { return rws1[kk]; });
-    rs1[k] = PSk(0, k) + (a.gT[0][p] + drhog2) * dt;
+    R drhog2 = fluxconv_col(c, m, k, a.hdiv[0][p], R(1.0), DV, [&](int kk) { return rws1[kk]; });
+    rs1[k] = PSk(0, k) + (a.gT[0][p] + drhog2) * dtR;
   }
   for (int k = 0; k < KA; ++k) {
     int p = c.at(k);
-    auto st10 = [&](int kk, int comp) -> double {
+    auto st10 = [&](int kk, int comp) -> R {
       int q = c.at(kk);
       return a.P[comp][q] + PSk(comp, kk);
     };
-    auto st11 = [&](int kk, int comp) -> double {
+    auto st11 = [&](int kk, int comp) -> R {
       int q = c.at(kk);
       if (comp == 0) return a.P[0][q] + rs1[kk];
       if (comp == 4) return a.P[4][q] + rws1[kk];
       return a.P[comp][q] + a.dvh.f[comp - 1][q];
     };
-    double kin10 = rhogkin_at(c, m, k, st10);
-    double kin11 = rhogkin_at(c, m, k, st11);
-    double drhogetot = fluxconv_col(
-        c, m, k, a.hdiv[2][p], 1.0,
+    R kin10 = rhogkin_at(c, m, k, st10);
+    R kin11 = rhogkin_at(c, m, k, st11);
+    R drhogetot = fluxconv_col(
+        c, m, k, a.hdiv[2][p], R(1.0),
         [&](int kk, int d) {
           int q = c.at(kk);
           return (a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q];
         },
         [&](int kk) {
           int q = c.at(kk), qm = c.at(kk - 1);
-          return (a.P[4][q] + rws1[kk]) * (cC.afact[kk] * a.ethtot0[q] + cC.bfact[kk] * a.ethtot0[qm]);
+          return (a.P[4][q] + rws1[kk]) * (CC.afact[kk] * a.ethtot0[q] + CC.bfact[kk] * a.ethtot0[qm]);
         });
-    double re = PSk(5, k) + (a.gT0e[p] + drhogetot) * dt + (kin10 - kin11) + (PSk(0, k) - rs1[k]) * m.PHI[p];
+    R re = PSk(5, k) + (a.gT0e[p] + drhogetot) * dtR + (kin10 - kin11) + (PSk(0, k) - rs1[k]) * m.PHI[p];
     a.dwe[0][p] = rs1[k];
     a.dwe[1][p] = rws1[k];
     a.dwe[2][p] = re;
-    a.PM0[p] = a.PM0[p] + rs1[k] * a.rweight;
-    a.PM4[p] = a.PM4[p] + rws1[k] * a.rweight;
+    a.PM0[p] = a.PM0[p] + rs1[k] * R(a.rweight);
+    a.PM4[p] = a.PM4[p] + rws1[k] * R(a.rweight);
   }
 }
 
@@ -1145,18 +1184,18 @@ __device__ void vimain_column(const VimainArgs& a, const Col c) {
 // nine 128-thread blocks per SM (56 registers): the 655,360 interior columns
 // of gl08 fill 3.84 waves of the 148 SMs instead of 4.32 at eight
 // GU: the gamma factors are all 1 and are not loaded; the other instance loads them
-template <bool GU>
-__global__ void __launch_bounds__(128, 9) k_vi_solve(VimainArgs a) {
+template <class R, bool GU>
+__global__ void __launch_bounds__(128, 9) k_vi_solve(VimainArgs<R> a) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l) || !interior(i, j)) return;
   const Col c = col_reg(i, j, l);
-  const Met m = met_of(false);
+  const MetT<R> m = met_of<R>(false);
   const int kmin = cD.kmin, kmax = cD.kmax, kT = kmax + 1;
   const double dt = a.dt, Rdry = cC.Rdry, CVdry = cC.CVdry, RovCV = a.RovCV;
   const int n = cD.npti;
-  const double* cz = cG.C2WGz;
-  const double* const* DVp = a.dvh.f;
+  const R* cz = CG.C2WGz;
+  const R* const* DVp = a.dvh.f;
   auto preg0 = [&](int k) -> double {
     const int k2 = k < kmin ? kmin : (k > kmax ? kmax : k);
     return a.PS[5][c.at(k2)] * RovCV;
@@ -1261,7 +1300,8 @@ __global__ void __launch_bounds__(128, 9) k_vi_solve(VimainArgs a) {
 // energies, total-energy advection and rhoge_split1 from the rhog_s1 /
 // rhogw_s1 written by k_vi_solve (no vertical recurrence; neighbouring levels
 // are read through the cache).
-__global__ void __launch_bounds__(128) k_vi_energy_p(VimainArgs a) {
+template <class R>
+__global__ void __launch_bounds__(128) k_vi_energy_p(VimainArgs<R> a) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= cD.npti) return;
   const int G = cD.G, KA = cD.KA;
@@ -1269,74 +1309,77 @@ __global__ void __launch_bounds__(128) k_vi_energy_p(VimainArgs a) {
   const int l = (int)(t / ((int)G * G * KA));
   if (!interior(i, j)) return;
   const Col c = col_reg(i, j, l);
-  const Met m = met_of(false);
+  const MetT<R> m = met_of<R>(false);
   const int kmin = cD.kmin, kmax = cD.kmax;
-  const double* rs1 = a.dwe[0];
-  const double* rws1 = a.dwe[1];
-  auto PSk = [&](int comp, int kk) -> double {
+  const R* rs1 = a.dwe[0];
+  const R* rws1 = a.dwe[1];
+  auto PSk = [&](int comp, int kk) -> R {
     if (comp == 5) kk = kk < kmin ? kmin : (kk > kmax ? kmax : kk);
     return a.PS[comp][c.at(kk)];
   };
   const int p = c.at(k);
-  auto st10 = [&](int kk, int comp) -> double { return a.P[comp][c.at(kk)] + PSk(comp, kk); };
-  auto st11 = [&](int kk, int comp) -> double {
+  auto st10 = [&](int kk, int comp) -> R { return a.P[comp][c.at(kk)] + PSk(comp, kk); };
+  auto st11 = [&](int kk, int comp) -> R {
     const int q = c.at(kk);
     if (comp == 0) return a.P[0][q] + rs1[q];
     if (comp == 4) return a.P[4][q] + rws1[q];
     return a.P[comp][q] + a.dvh.f[comp - 1][q];
   };
-  const double kin10 = rhogkin_at(c, m, k, st10);
-  const double kin11 = rhogkin_at(c, m, k, st11);
-  const double drhogetot = fluxconv_col(
-      c, m, k, a.hdiv[2][p], 1.0,
+  const R kin10 = rhogkin_at(c, m, k, st10);
+  const R kin11 = rhogkin_at(c, m, k, st11);
+  const R drhogetot = fluxconv_col(
+      c, m, k, a.hdiv[2][p], R(1.0),
       [&](int kk, int d) {
         const int q = c.at(kk);
         return (a.P[1 + d][q] + a.dvh.f[d][q]) * a.ethtot0[q];
       },
       [&](int kk) {
         const int q = c.at(kk), qm = c.at(kk - 1);
-        return (a.P[4][q] + rws1[q]) * (cC.afact[kk] * a.ethtot0[q] + cC.bfact[kk] * a.ethtot0[qm]);
+        return (a.P[4][q] + rws1[q]) * (CC.afact[kk] * a.ethtot0[q] + CC.bfact[kk] * a.ethtot0[qm]);
       });
-  a.dwe[2][p] = PSk(5, k) + (a.gT0e[p] + drhogetot) * a.dt + (kin10 - kin11) + (PSk(0, k) - rs1[p]) * m.PHI[p];
+  a.dwe[2][p] = PSk(5, k) + (a.gT0e[p] + drhogetot) * R(a.dt) + (kin10 - kin11) + (PSk(0, k) - rs1[p]) * m.PHI[p];
 }
 
-__global__ void k_vimain_b(VimainArgs a, int pole) {
+template <class R>
+__global__ void k_vimain_b(VimainArgs<R> a, int pole) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
-  if (!pole) vimain_column<false>(a, col_reg(i, j, l));
-  else vimain_column<true>(a, col_pl(g, lp));
+  if (!pole) vimain_column<R, false>(a, col_reg(i, j, l));
+  else vimain_column<R, true>(a, col_pl(g, lp));
 }
 
 // ---------------------------------------------------------------------------
 // elementwise helpers of the small step
 // ---------------------------------------------------------------------------
 // PROG_split = 0 (first stage) or PROG0 - PROG; PROG_mean = PROG[0:5]
-__global__ void k_split_init(const double* P0a, const double* P0b, const double* P0c, const double* P0d,
-                             const double* P0e, const double* P0f, Prog P, double* PS0, double* PS1, double* PS2,
-                             double* PS3, double* PS4, double* PS5, double* PM0, double* PM1, double* PM2,
-                             double* PM3, double* PM4, int n, int first) {
+template <class R>
+__global__ void k_split_init(const R* P0a, const R* P0b, const R* P0c, const R* P0d,
+                             const R* P0e, const R* P0f, Prog<R> P, R* PS0, R* PS1, R* PS2,
+                             R* PS3, R* PS4, R* PS5, R* PM0, R* PM1, R* PM2,
+                             R* PM3, R* PM4, int n, int first) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  const double* P0[6] = {P0a, P0b, P0c, P0d, P0e, P0f};
-  double* PS[6] = {PS0, PS1, PS2, PS3, PS4, PS5};
-  double* PM[5] = {PM0, PM1, PM2, PM3, PM4};
-  for (int v = 0; v < 6; ++v) PS[v][t] = first ? 0.0 : (P0[v][t] - P.v[v][t]);
+  const R* P0[6] = {P0a, P0b, P0c, P0d, P0e, P0f};
+  R* PS[6] = {PS0, PS1, PS2, PS3, PS4, PS5};
+  R* PM[5] = {PM0, PM1, PM2, PM3, PM4};
+  for (int v = 0; v < 6; ++v) PS[v][t] = first ? R(0.0) : (P0[v][t] - P.v[v][t]);
   for (int v = 0; v < 5; ++v) PM[v][t] = P.v[v][t];
 }
 
 // PROG += PROG_split, then horizontalize the momentum (mod_vi.py:1572-1583)
-__global__ void k_post(Prog P, const double* PS0, const double* PS1, const double* PS2, const double* PS3,
-                       const double* PS4, const double* PS5, int pole) {
+template <class R>
+__global__ void k_post(Prog<R> P, const R* PS0, const R* PS1, const R* PS2, const R* PS3,
+                       const R* PS4, const R* PS5, int pole) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
-  const double* PS[6] = {PS0, PS1, PS2, PS3, PS4, PS5};
+  const R* PS[6] = {PS0, PS1, PS2, PS3, PS4, PS5};
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
   const Col c = pole ? col_pl(g, lp) : col_reg(i, j, l);
   const bool in = !pole && interior(i, j);
   for (int k = 0; k < cD.KA; ++k) {
     int p = c.at(k);
-    double v[6];
+    R v[6];
     for (int n = 0; n < 6; ++n) v[n] = P.v[n][p] + PS[n][p];
     if (pole) horiz_pl(g, lp, v[1], v[2], v[3]);
     else if (in) horiz_reg(i, j, l, v[1], v[2], v[3]);

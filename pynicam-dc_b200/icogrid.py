@@ -463,6 +463,7 @@ class Grid:
             vz_pl[:, 0, k, 1] = gzh[k] + zs_pl[:, 0] * np.sinh((htop - gzh[k]) / h_efold) / sh
         self.exch(vz, vz_pl)
         self.vz, self.vz_pl = vz, vz_pl
+        self.zs, self.zs_pl = zs, zs_pl
 
     @staticmethod
     def _jw_surface(lat):
@@ -1021,4 +1022,10 @@ class Grid:
         for k in ("rho_bs", "pre_bs", "tem_bs"):
             g[k] = np.zeros((G, G, K, L))
             g[k + "_pl"] = np.zeros((6, K, LP))
+        # heights of the surface-pressure diagnostic (not uploaded): the
+        # lowest full level and the surface, (G, G, L) and pole (6, 2)
+        g["sfc_zkmin"] = np.ascontiguousarray(np.moveaxis(self.vz[:, :, :, 1, 0], 0, 2))
+        g["sfc_zs"] = np.ascontiguousarray(np.moveaxis(self.zs, 0, 2))
+        g["sfc_zkmin_pl"] = np.ascontiguousarray(np.moveaxis(self.vz_pl[:, :, 1, 0], 0, 1))
+        g["sfc_zs_pl"] = np.ascontiguousarray(np.moveaxis(np.broadcast_to(self.zs_pl[:, :1], (LP, 6)), 0, 1))
         return {k: np.asarray(v) for k, v in g.items()}

@@ -251,13 +251,26 @@ def setup_table(geo: dict) -> dict:
     return t
 
 
-class NicamCuda:
-    """One device-resident NICAM-DC dynamical core (one C-ABI handle)."""
+PRECISIONS = ("float64", "mixed")
 
-    def __init__(self, geo: dict, graph: bool = True):
+
+class NicamCuda:
+    """One device-resident NICAM-DC dynamical core (one C-ABI handle).
+
+    ``precision`` is "float64" (the reference's numpy arithmetic, bit for
+    bit) or "mixed": float32 work fields, metrics and stencil / advection /
+    hyperdiffusion arithmetic, with the tridiagonal (HEVI) elimination and its
+    matrix, the pressure and density deviations from the reference state and
+    the mass sums in float64.  The host-side state stays float64 in both."""
+
+    def __init__(self, geo: dict, graph: bool = True, precision: str = "float64"):
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {PRECISIONS}, got {precision!r}")
         lib = load_library()
         self._lib = lib
+        self.precision = precision
         self._tab = setup_table(geo)
+        self._tab["precision"] = np.asarray(1.0 if precision == "mixed" else 0.0, np.float64)
         names, arrs = [], []
         entries = (NcArray * len(self._tab))()
         for n, (k, a) in enumerate(self._tab.items()):

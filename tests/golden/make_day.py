@@ -60,8 +60,10 @@ def state_sha(s, s_pl) -> str:
 
 
 def geo_sha(geo: dict) -> str:
+    """hash of the setup arrays (the surface-pressure diagnostic's heights,
+    keys sfc_*, are not part of the setup the step reads)"""
     h = hashlib.sha256()
-    for k in sorted(geo):
+    for k in sorted(k for k in geo if not k.startswith("sfc_")):
         h.update(k.encode())
         h.update(np.ascontiguousarray(np.asarray(geo[k])).tobytes())
     return h.hexdigest()
