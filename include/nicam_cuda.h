@@ -63,10 +63,11 @@ typedef struct nc_handle nc_handle;
  * pressure and density deviations from the reference state
  * (mod_dynamics.py:1056-1057) and the mass sums in float64.  The host state
  * and every marshal call stay float64 in both forms.  A mixed handle runs the
- * dynamics step, the marshal calls, nc_mass_sums, nc_check_finite and
- * nc_get_field; nc_forcing_step, nc_history_vars, the restart calls and
- * nc_state_pointers return NC_ERR_STATE for it, and the TRCADV, Held-Suarez
- * and history set-up entries are rejected (NC_ERR_ARG). */
+ * dynamics step (the offline tracer advection TRCADV included), the marshal
+ * calls, nc_mass_sums, nc_check_finite and nc_get_field; nc_forcing_step,
+ * nc_history_vars, the restart calls and nc_state_pointers return
+ * NC_ERR_STATE for it, and the Held-Suarez and history set-up entries are
+ * rejected (NC_ERR_ARG). */
 int nc_create(const nc_array* arrays, int32_t narrays, nc_handle** out);
 
 /* Marshal-in of the prognostic state (mod_dynamics.py:1876-1880) from host

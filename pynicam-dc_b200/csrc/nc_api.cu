@@ -966,23 +966,21 @@ static int run_step(nc_handle* h) {
   TRY(fork_pl(h));
   for (int iq = 0; iq < D.nq; ++iq) TRY(vadv(iq, true));
   PHASE();
-  if constexpr (std::is_same<R, double>::value) {   // TRCADV is a float64 configuration (checked at set-up)
   if (h->trcadv) {
     // the prescribed winds of the next time (mod_forcing.py forcing_update)
     TRY(join_pl(h));
     k_trcadv_time<<<1, 1, 0, s>>>(h->trc_time, h->dtl);
     TRY(check_launch(h, "trcadv_time"));
-    TrcWindArgs w;
-    for (int v = 0; v < 6; ++v) w.P.v[v] = RG<double>(h->P[v]);
+    TrcWindArgs<R> w;
+    for (int v = 0; v < 6; ++v) w.P.v[v] = RG<R>(h->P[v]);
     w.lon = h->trc_lon; w.lat = h->trc_lat; w.zf = h->trc_zf; w.zh = h->trc_zh; w.time = h->trc_time;
     w.a = 6371220.0; w.Rd = 287.0; w.g = 9.80616; w.pi = 3.141592653589793238;
     k_trcadv_winds<<<npt_blocks, kBlock, 0, s>>>(w, 0);
     TRY(check_launch(h, "trcadv_winds"));
-    for (int v = 0; v < 6; ++v) w.P.v[v] = PL<double>(h->P[v]);
+    for (int v = 0; v < 6; ++v) w.P.v[v] = PL<R>(h->P[v]);
     w.lon = h->trc_lon_pl; w.lat = h->trc_lat_pl; w.zf = h->trc_zf_pl; w.zh = h->trc_zh_pl;
     k_trcadv_winds<<<npl_blocks, kBlock, 0, s>>>(w, 1);
     TRY(check_launch(h, "trcadv_winds_pl"));
-  }
   }
   // marshal-out halo exchange of PRG_var (mod_dynamics.py:2726-2727)
   TRY(comm_prg<R>(h));
@@ -1470,9 +1468,9 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
     }
   }
   if (h->mixed) {
-    if (h->trcadv || h->hist || h->hs_lat)
-      return fail(NC_ERR_ARG, "the mixed-precision form runs the dynamics step only (no TRCADV, Held-Suarez "
-                              "forcing or history diagnostics set-up)");
+    if (h->hist || h->hs_lat)
+      return fail(NC_ERR_ARG, "the mixed-precision form runs the dynamics step and the offline tracer advection "
+                              "only (no Held-Suarez forcing or history diagnostics set-up)");
     TRY(make_f32_geometry(h));
   }
   // state and work fields

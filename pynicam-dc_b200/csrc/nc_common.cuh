@@ -130,6 +130,43 @@ template <> __device__ __forceinline__ const GeomT<float>& geom<float>() { retur
 #define CC (consts<R>())
 #define CG (geom<R>())
 
+// Resident-block targets of the launch bounds: the float64 instances keep the
+// values measured for them; the float32 instances need about half the
+// registers and take their own targets, from a sweep of 4-16 blocks per SM
+// at gl08 on B200 (per-kernel event times; the ones left at the float64
+// value were slower at every higher target).
+#define NC_MINB(R, f64, f32) (sizeof(R) == 8 ? (f64) : (f32))
+#ifndef NC_F32_DIAG
+#define NC_F32_DIAG 9
+#endif
+#ifndef NC_F32_ADVMOM
+#define NC_F32_ADVMOM 4
+#endif
+#ifndef NC_F32_HDIFF2
+#define NC_F32_HDIFF2 4
+#endif
+#ifndef NC_F32_DD3D
+#define NC_F32_DD3D 6
+#endif
+#ifndef NC_F32_VP0H
+#define NC_F32_VP0H 5
+#endif
+#ifndef NC_F32_VP0C
+#define NC_F32_VP0C 4
+#endif
+#ifndef NC_F32_PATH1
+#define NC_F32_PATH1 6
+#endif
+#ifndef NC_F32_VIMAINA
+#define NC_F32_VIMAINA 6
+#endif
+#ifndef NC_F32_VISOLVE
+#define NC_F32_VISOLVE 9
+#endif
+#ifndef NC_F32_VIENERGY
+#define NC_F32_VIENERGY 12
+#endif
+
 // The gamma factors of the vertical metrics: RGAM, RGAMH, GAM2H (regional or
 // pole) at index p.  With a shallow atmosphere every value is exactly 1 (the
 // host checks each element at set-up and sets gam_unit); the factor is then

@@ -90,8 +90,9 @@ namespace nc {
 // Sp_Unit_East / Sp_Unit_North).  exp, sin and cos are CUDA's, so the winds
 // can differ from numpy's in the last bits.
 // ---------------------------------------------------------------------------
+template <class R>
 struct TrcWindArgs {
-  Prog<double> P;                    // RHOGV{X,Y,Z}, RHOGW set to wind * RHOG
+  Prog<R> P;                  // RHOGV{X,Y,Z}, RHOGW set to wind * RHOG (float64 arithmetic in both forms)
   const double *lon, *lat;    // column longitude / latitude: regional [l][j][i], pole [g][l]
   const double *zf, *zh;      // full / half-level height: regional [l][k][j][i], pole [g][k][l]
   const double* time;         // model time of the winds (device scalar)
@@ -101,7 +102,8 @@ struct TrcWindArgs {
 __global__ void k_trcadv_time(double* time, double dt) { *time = *time + dt; }
 
 // one thread per point of the regional (pole == 0) or pole (pole != 0) grid
-__global__ void k_trcadv_winds(TrcWindArgs w, int pole) {
+template <class R>
+__global__ void k_trcadv_winds(TrcWindArgs<R> w, int pole) {
   const int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   const int KA = cD.KA;
   int p, c2;   // point index and column index of lon/lat
@@ -147,7 +149,7 @@ __global__ void k_trcadv_winds(TrcWindArgs w, int pole) {
   const double s = (1.0 + exp((ptop - p0) / (bs * ptop)) - exp((ph - p0) / (bs * ptop)) -
                     exp((ptop - ph) / (bs * ptop)));
   const double ww = -(w.Rd * T0) / (w.g * ph) * omega0 * sl * cl * cos(dlon) * s;
-  const double rg = w.P.v[0][p];
+  const double rg = (double)w.P.v[0][p];
   w.P.v[1][p] = vx * rg;
   w.P.v[2][p] = vy * rg;
   w.P.v[3][p] = vz * rg;

@@ -217,7 +217,7 @@ __device__ void diag_column_fused(const Col c, const MetT<R> m, const DiagArgs<R
 // eight 128-thread blocks per SM (64 registers): measured faster than the
 // uncapped 84 registers
 template <class R>
-__global__ void __launch_bounds__(128, 8) k_diag(DiagArgs<R> a, int pole) {
+__global__ void __launch_bounds__(128, NC_MINB(R, 8, NC_F32_DIAG)) k_diag(DiagArgs<R> a, int pole) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l, g, lp;
   if (!map_col(pole, t, i, j, l, g, lp)) return;
@@ -253,7 +253,7 @@ struct AdvMomArgs {
 // Arithmetic and association order are those of the reference's expressions
 // (kernels/advconv.py, kernels/advconvmom.py), as in the pole kernel.
 template <class R>
-__global__ void __launch_bounds__(256, 2) k_advmom_t(AdvMomArgs<R> a) {
+__global__ void __launch_bounds__(256, NC_MINB(R, 2, NC_F32_ADVMOM)) k_advmom_t(AdvMomArgs<R> a) {
   constexpr int TXD = 32, TYD = 8;
   constexpr int PX = TXD + 2, PY = TYD + 2;
   __shared__ R s_rv[3][PY * PX], s_vv[3][PY * PX], s_rg[PY * PX];
@@ -500,7 +500,8 @@ __global__ void k_intp_weights(const double* ci, double* w, int npt2) {
 #define HD_DX 32
 #define HD_DY 8
 template <class R>
-__global__ void __launch_bounds__(HD_DX * HD_DY, 4) k_hdiff2_l(Six<R> vt, const R* rhog, SixOut<R> out) {
+__global__ void __launch_bounds__(HD_DX * HD_DY, NC_MINB(R, 4, NC_F32_HDIFF2)) k_hdiff2_l(Six<R> vt, const R* rhog,
+                                                                                       SixOut<R> out) {
   constexpr int PX = HD_DX + 2, PY = HD_DY + 2, TX = HD_DX + 1, TY = HD_DY + 1;
   __shared__ R s_f[6][PY * PX];
   __shared__ R s_r[PY * PX];

@@ -45,7 +45,7 @@ __device__ __forceinline__ R ddivd(int i, int j, int l, int d, const R aTI, cons
 // resident blocks per SM for a register budget of n blocks of 256 threads
 #define DD_MINB(n) ((n) * 256 / (DD_DX * DD_DY) > 0 ? (n) * 256 / (DD_DX * DD_DY) : 1)
 template <class R>
-__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(4)) k_dd3d_t(Four<R> v, Three<R> out) {
+__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(NC_MINB(R, 4, NC_F32_DD3D))) k_dd3d_t(Four<R> v, Three<R> out) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2;   // points i0-1 .. i0+DX, j0-1 .. j0+DY
   constexpr int TX = DD_DX + 1, TY = DD_DY + 1;   // triangles i0-1 .. i0+DX-1, j0-1 .. j0+DY-1
   __shared__ R s_vm[3][PY * PX];
@@ -119,11 +119,11 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(4)) k_dd3d_t(Four<R> v,
       const R cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1];   // (i-1, j-1)
       const R dTJ = s_tj[ta - TX];           // (i, j-1)
       const int q = ix(i, j, k, l);
+      auto D = [&](int m) { return P2c(CG.coef_diff, m, i, j, l); };
 #pragma unroll
       for (int d = 0; d < 3; ++d)
-        out.f[d][q] = P2c(CG.coef_diff, d * 6 + 0, i, j, l) * (aTI + aTJ) + P2c(CG.coef_diff, d * 6 + 1, i, j, l) * (aTJ + bTI) +
-                      P2c(CG.coef_diff, d * 6 + 2, i, j, l) * (bTI + cTJ) + P2c(CG.coef_diff, d * 6 + 3, i, j, l) * (cTJ + cTI) +
-                      P2c(CG.coef_diff, d * 6 + 4, i, j, l) * (cTI + dTJ) + P2c(CG.coef_diff, d * 6 + 5, i, j, l) * (dTJ + aTI);
+        out.f[d][q] = D(d * 6 + 0) * (aTI + aTJ) + D(d * 6 + 1) * (aTJ + bTI) + D(d * 6 + 2) * (bTI + cTJ) +
+                      D(d * 6 + 3) * (cTJ + cTI) + D(d * 6 + 4) * (cTI + dTJ) + D(d * 6 + 5) * (dTJ + aTI);
     }
     __syncthreads();
     cur ^= 1;
@@ -475,7 +475,7 @@ struct Vp0H {
 #define VP_DX 32
 #define VP_DY 8
 template <class R>
-__global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args<R> a, Vp0H<R> h) {
+__global__ void __launch_bounds__(VP_DX * VP_DY, NC_MINB(R, 4, NC_F32_VP0H)) k_vp0_hl(Vp0Args<R> a, Vp0H<R> h) {
   constexpr int PX = VP_DX + 2, PY = VP_DY + 2, TX = VP_DX + 1, TY = VP_DY + 1;
   __shared__ R s_m[3][PY * PX];    // RGAM * rhogv
   __shared__ R s_e[3][PY * PX];    // RGAM * rhogv * eth
@@ -629,7 +629,7 @@ __global__ void __launch_bounds__(VP_DX * VP_DY, 4) k_vp0_hl(Vp0Args<R> a, Vp0H<
 // than three at 74 registers)
 #define NC_VP0C_BLOCK 256
 template <class R>
-__global__ void __launch_bounds__(NC_VP0C_BLOCK, 4) k_vp0_cr(Vp0Args<R> a, Vp0H<R> h) {
+__global__ void __launch_bounds__(NC_VP0C_BLOCK, NC_MINB(R, 4, NC_F32_VP0C)) k_vp0_cr(Vp0Args<R> a, Vp0H<R> h) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
@@ -802,7 +802,7 @@ __device__ void path1_column(const Path1Args<R>& a, int i, int j, int l, int g, 
 // arithmetic as path1_column.  The blocks at kmin and kmax also write the
 // boundary rows kmin-1 and kmax+1 from the values they computed.
 template <class R>
-__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_path1_l(Path1Args<R> a) {
+__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(NC_MINB(R, 6, NC_F32_PATH1))) k_path1_l(Path1Args<R> a) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2, TX = DD_DX + 1, TY = DD_DY + 1;
   __shared__ R s_v[3][PY * PX];
   __shared__ R s_p[PY * PX];
@@ -1001,7 +1001,7 @@ __global__ void k_vimain_a(VimainArgs<R> a, int pole) {
 // vi_main kernel A, one block per (level, tile): the horizontal divergences
 // of RGAM*diff_vh, RGAM*diff_vh*eth and RGAM*(rhogv + diff_vh)*ethtot0.
 template <class R>
-__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(6)) k_vimain_a_l(VimainArgs<R> a) {
+__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(NC_MINB(R, 6, NC_F32_VIMAINA))) k_vimain_a_l(VimainArgs<R> a) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2;
   __shared__ R s_h[3][3][PY * PX];
   const TileLv tl = tile_level<DD_DX, DD_DY>(cD.kmin);
@@ -1185,7 +1185,7 @@ __device__ void vimain_column(const VimainArgs<R>& a, const Col c) {
 // of gl08 fill 3.84 waves of the 148 SMs instead of 4.32 at eight
 // GU: the gamma factors are all 1 and are not loaded; the other instance loads them
 template <class R, bool GU>
-__global__ void __launch_bounds__(128, 9) k_vi_solve(VimainArgs<R> a) {
+__global__ void __launch_bounds__(128, NC_MINB(R, 9, NC_F32_VISOLVE)) k_vi_solve(VimainArgs<R> a) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l) || !interior(i, j)) return;
@@ -1301,7 +1301,7 @@ __global__ void __launch_bounds__(128, 9) k_vi_solve(VimainArgs<R> a) {
 // rhogw_s1 written by k_vi_solve (no vertical recurrence; neighbouring levels
 // are read through the cache).
 template <class R>
-__global__ void __launch_bounds__(128) k_vi_energy_p(VimainArgs<R> a) {
+__global__ void __launch_bounds__(128, NC_MINB(R, 1, NC_F32_VIENERGY)) k_vi_energy_p(VimainArgs<R> a) {
   int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= cD.npti) return;
   const int G = cD.G, KA = cD.KA;

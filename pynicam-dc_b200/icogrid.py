@@ -333,16 +333,24 @@ def gravcenter(x, x_pl, have_sgp, exch: Exchange):
 # ---------------------------------------------------------------------------
 # vertical grid
 # ---------------------------------------------------------------------------
-def vertical_levels(vlayer: int, ztop: float):
-    """ULLRICH14 stretched layers with one dummy level at each end: returns
-    (gz, gzh) of length vlayer + 2."""
+def vertical_levels(vlayer: int, ztop: float, layer: str = "ULLRICH14"):
+    """ULLRICH14 stretched or EVEN layers with one dummy level at each end
+    (prep/vgrid/mkvlayer.py: mk_layer_ullrich14, mk_layer_even,
+    generate_layers): returns (gz, gzh) of length vlayer + 2."""
     kall = vlayer + 2
     z_h = np.zeros(kall)
     z_c = np.zeros(kall)
-    mu = 15.0
-    for k in range(1, vlayer + 2):
-        fact = ((k + 1) / vlayer) ** 2
-        z_h[k] = ztop * (np.sqrt(mu * fact + 1.0) - 1.0) / (np.sqrt(mu + 1.0) - 1.0)
+    if layer == "ULLRICH14":
+        mu = 15.0
+        for k in range(1, vlayer + 2):
+            fact = ((k + 1) / vlayer) ** 2
+            z_h[k] = ztop * (np.sqrt(mu * fact + 1.0) - 1.0) / (np.sqrt(mu + 1.0) - 1.0)
+    elif layer == "EVEN":
+        dz = ztop / vlayer
+        for k in range(kall):
+            z_h[k] = dz * k
+    else:
+        raise ValueError(f"unknown layer type {layer!r}")
     z_h[0] = z_h[1] - (z_h[2] - z_h[1])
     for k in range(0, vlayer + 1):
         z_c[k] = z_h[k] + 0.5 * (z_h[k + 1] - z_h[k])
@@ -384,8 +392,12 @@ class Grid:
     """All setup arrays of one grid level in region-major layout."""
 
     def __init__(self, glevel: int, vlayer: int = 40, ztop: float = 30000.0, device: str = "cpu",
-                 h_efold: float = 40000.0, raw=None):
+                 h_efold: float = 40000.0, raw=None, layer: str = "ULLRICH14", topo: str = "JW"):
+        """``layer``: vertical layering, "ULLRICH14" (the JW cases) or "EVEN"
+        (the tracer-transport case); ``topo``: "JW" (the balanced jet's
+        surface height) or "NONE" (flat surface, DCMIP 1-1)."""
         self.glevel = glevel
+        self.layer, self.topo = layer, topo
         self.G = G = 2 ** (glevel - 1) + 2
         self.L = L = 40
         self.kall = vlayer + 2
@@ -443,15 +455,21 @@ class Grid:
         self.xr, self.xr_pl = xr, xr_pl
 
     def _vertical(self, vlayer, ztop, h_efold):
-        gz, gzh = vertical_levels(vlayer, ztop)
+        gz, gzh = vertical_levels(vlayer, ztop, self.layer)
         self.gz, self.gzh = gz, gzh
         self.vf = vertical_factors(gz, gzh)
         kall = len(gz)
         kmin, kmax = 1, kall - 2
         L, G = self.L, self.G
-        # JW surface height (geopotential of the balanced state at eta = 1)
-        zs = self._jw_surface(self.lat)
-        zs_pl = self._jw_surface(self.lat_pl)
+        # JW surface height (geopotential of the balanced state at eta = 1), or flat
+        if self.topo == "JW":
+            zs = self._jw_surface(self.lat)
+            zs_pl = self._jw_surface(self.lat_pl)
+        elif self.topo == "NONE":
+            zs = np.zeros_like(self.lat)
+            zs_pl = np.zeros_like(self.lat_pl)
+        else:
+            raise ValueError(f"unknown topography {self.topo!r}")
         htop = gzh[kmax + 1] - gzh[kmin]
         vz = np.zeros((L, G, G, kall, 2))
         vz_pl = np.zeros((LP, 6, kall, 2))
@@ -935,33 +953,24 @@ class Grid:
                                 zip(bounds[:-1], bounds[1:])))
         return tuple(np.concatenate([p[v] for p in parts], axis=0) for v in range(5))
 
-    def jw_state(self, nq: int = 1):
-        """JW balanced jet + perturbation as PRG_var (G, G, kall, L, 6+nq) and
-        PRG_var_pl (6, kall, 2, 6+nq) in the reference layout."""
-        kmin, kmax = 1, self.kall - 2
-        out = []
-        # the pole columns are evaluated like the region halo cells that carry
-        # the pole point, i.e. with the regional lat/lon convention
-        lat_p, lon_p = _latlon(self.x_pl)
-        for z3, lat, lon in ((self.vz, self.lat, self.lon), (self.vz_pl, lat_p, lon_p)):
-            z = np.zeros(z3.shape[:-1])
-            z[..., kmin - 1] = z3[..., kmin, 1]
-            z[..., kmin:kmax + 2] = z3[..., kmin:kmax + 2, 0]
-            out.append(self._jw_chunked(z, lat, lon))
-        diag = np.stack(out[0] + (np.zeros_like(out[0][0]),), axis=-1)        # (L,G,G,K,6) pre,tem,vx,vy,vz,w
-        diag_pl = np.stack(out[1] + (np.zeros_like(out[1][0]),), axis=-1)
-        self.exch(diag, diag_pl)
+    def _diag_to_prg(self, diag, diag_pl, q=None, q_pl=None):
+        """PRG_var / PRG_var_pl in the reference layout from the diagnostic
+        columns (pre, tem, vx, vy, vz, w) in region-major layout and optional
+        tracer mixing ratios (..., nq) (the reference's cnvvar diag -> prg for a
+        dry state: rho = p / (Rdry T), RHOG = rho GSGAM2, RHOGV = RHOG v,
+        RHOGE = RHOG cv T, RHOGW = rho_h w, RHOGQ = RHOG q)"""
         prg = []
-        for d, sfx in ((diag, ""), (diag_pl, "_pl")):
+        for d, qq, sfx in ((diag, q, ""), (diag_pl, q_pl, "_pl")):
             gs2 = self.vmtr["GSGAM2" + sfx]
             c2w = self.vmtr["C2Wfact" + sfx]
             pre, tem = d[..., 0], d[..., 1]
-            q = np.zeros(pre.shape)
-            cv = 0.0 + q * CVDRY
-            qd = 1.0 - q
+            qv = np.zeros(pre.shape)
+            cv = 0.0 + qv * CVDRY
+            qd = 1.0 - qv
             cv = cv + qd * CVDRY
-            rho = pre / ((qd * RDRY + q * RVAP) * tem)
+            rho = pre / ((qd * RDRY + qv * RVAP) * tem)
             ein = tem * cv
+            nq = 1 if qq is None else qq.shape[-1]
             P = np.zeros(pre.shape + (6 + nq,))
             P[..., 0] = rho * gs2
             P[..., 1] = P[..., 0] * d[..., 2]
@@ -972,13 +981,109 @@ class Grid:
             rh[..., 1:] = c2w[..., 1:, 0] * P[..., 1:, 0] + c2w[..., 1:, 1] * P[..., :-1, 0]
             rh[..., 0] = rh[..., 1]
             P[..., 4] = rh * d[..., 5]
+            if qq is not None:
+                P[..., 6:] = P[..., 0:1] * qq
             prg.append(P)
         return (np.ascontiguousarray(prg[0].transpose(1, 2, 3, 0, 4)),
                 np.ascontiguousarray(prg[1].transpose(1, 2, 0, 3)))
 
+    def _column_coords(self):
+        """per region-major grid (regional, pole): (z, lat, lon) of the state
+        evaluation -- full-level heights with the bottom dummy level at the
+        lowest half level, the column latitude / longitude (the pole columns
+        like the region halo cells that carry the pole point)"""
+        kmin, kmax = 1, self.kall - 2
+        lat_p, lon_p = _latlon(self.x_pl)
+        out = []
+        for z3, lat, lon in ((self.vz, self.lat, self.lon), (self.vz_pl, lat_p, lon_p)):
+            z = np.zeros(z3.shape[:-1])
+            z[..., kmin - 1] = z3[..., kmin, 1]
+            z[..., kmin:kmax + 2] = z3[..., kmin:kmax + 2, 0]
+            out.append((z, lat, lon))
+        return out
+
+    def jw_state(self, nq: int = 1):
+        """JW balanced jet + perturbation as PRG_var (G, G, kall, L, 6+nq) and
+        PRG_var_pl (6, kall, 2, 6+nq) in the reference layout."""
+        out = [self._jw_chunked(z, lat, lon) for z, lat, lon in self._column_coords()]
+        diag = np.stack(out[0] + (np.zeros_like(out[0][0]),), axis=-1)        # (L,G,G,K,6) pre,tem,vx,vy,vz,w
+        diag_pl = np.stack(out[1] + (np.zeros_like(out[1][0]),), axis=-1)
+        self.exch(diag, diag_pl)
+        s, s_pl = self._diag_to_prg(diag, diag_pl)
+        if nq != 1:
+            s = np.concatenate([s[..., :6], np.zeros(s.shape[:4] + (nq,))], axis=-1)
+            s_pl = np.concatenate([s_pl[..., :6], np.zeros(s_pl.shape[:3] + (nq,))], axis=-1)
+        return s, s_pl
+
+    @staticmethod
+    def dcmip11_fields(lon, lat, z):
+        """DCMIP2012 test 1-1 (3-D deformational flow) at time 0 on columns of
+        longitude / latitude and heights z (..., kall): pressure, temperature,
+        zonal / meridional / vertical wind, and the test's own four tracers
+        (restating nhm/share/mod_dcmip_ic.py test1_advection_deformation:
+        isothermal T0 = 300 K, p = p0 exp(-z / H), period 12 days)"""
+        a, Rd, g, p0, pi = 6371220.0, 287.0, 9.80616, 100000.0, 3.141592653589793238
+        tau = 12.0 * 86400.0
+        u0 = (2.0 * pi * a) / tau
+        k0 = (10.0 * a) / tau
+        omega0 = (23000.0 * pi) / tau
+        T0 = 300.0
+        H = Rd * T0 / g
+        lon = lon[..., None]
+        lat = lat[..., None]
+        p = p0 * np.exp(-z / H)
+        ptop = p0 * np.exp(-12000.0 / H)
+        bs = 0.2
+        sfac = (1.0 + np.exp((ptop - p0) / (bs * ptop)) - np.exp((p - p0) / (bs * ptop)) -
+                np.exp((ptop - p) / (bs * ptop)))
+        ud = (omega0 * a) / (bs * ptop) * np.cos(lon) * (np.cos(lat) ** 2) * (
+            -np.exp((p - p0) / (bs * ptop)) + np.exp((ptop - p) / (bs * ptop)))
+        u = k0 * np.sin(lon) * np.sin(lon) * np.sin(2.0 * lat) + u0 * np.cos(lat) + ud
+        v = k0 * np.sin(2.0 * lon) * np.cos(lat)
+        w = -((Rd * T0) / (g * p)) * omega0 * np.sin(lon) * np.cos(lat) * sfac
+        t = np.full_like(p, T0)
+        RR, ZZ, z0 = 0.5, 1000.0, 5000.0
+        lam0, lam1 = 5.0 * pi / 6.0, 7.0 * pi / 6.0
+        r = np.arccos(np.sin(lat) * 0.0 + np.cos(lat) * 1.0 * np.cos(lon - lam0))
+        r2 = np.arccos(np.sin(lat) * 0.0 + np.cos(lat) * 1.0 * np.cos(lon - lam1))
+        d1 = np.minimum(1.0, (r / RR) ** 2 + ((z - z0) / ZZ) ** 2)
+        d2 = np.minimum(1.0, (r2 / RR) ** 2 + ((z - z0) / ZZ) ** 2)
+        q1 = 0.5 * (1.0 + np.cos(pi * d1)) + 0.5 * (1.0 + np.cos(pi * d2))
+        q2 = 0.9 - 0.8 * q1 ** 2
+        q3 = np.where((d1 <= RR) | (d2 <= RR), 1.0, 0.1)
+        q3 = np.where((z > z0) & (np.abs(lat) < 0.125), 0.1, q3)
+        q4 = 1.0 - 0.3 * (q1 + q2 + q3)
+        shape = p.shape
+        u, v, w = (np.broadcast_to(x, shape) for x in (u, v, w))
+        return p, t, u, v, w, np.stack([np.broadcast_to(x, shape) for x in (q1, q2, q3, q4)], axis=-1)
+
+    def trcadv_state(self, tracers=None):
+        """The DCMIP 1-1 offline tracer-advection state (initial winds, the
+        isothermal atmosphere) as PRG_var / PRG_var_pl.  ``tracers``: a
+        function (lon, lat, z) -> mixing ratios (..., kall, nq) on the state's
+        columns; default the test's own four tracers."""
+        diag, qs = [], []
+        for z, lat, lon in self._column_coords():
+            p, t, u, v, w, q4 = self.dcmip11_fields(lon, lat, z)
+            lonk, latk = lon[..., None], lat[..., None]
+            ex, ey = -np.sin(lonk), np.cos(lonk)
+            nx, ny, nz = -np.sin(latk) * np.cos(lonk), -np.sin(latk) * np.sin(lonk), np.cos(latk)
+            d = np.stack([p, t, ex * u + nx * v, ey * u + ny * v, nz * v, w], axis=-1)
+            diag.append(d)
+            qs.append(q4 if tracers is None else tracers(lon, lat, z))
+        self.exch(diag[0], diag[1])
+        for n in range(qs[0].shape[-1]):
+            a, b = np.ascontiguousarray(qs[0][..., n]), np.ascontiguousarray(qs[1][..., n])
+            self.exch(a, b)
+            qs[0][..., n], qs[1][..., n] = a, b
+        return self._diag_to_prg(diag[0], diag[1], qs[0], qs[1])
+
     # -- the setup dict of NicamCuda ----------------------------------------
-    def setup(self, dtl: float, gamma: float, nq: int = 1) -> dict:
-        """Setup arrays in the reference's attribute names and layouts."""
+    def setup(self, dtl: float, gamma: float, nq: int = 1, trcadv: bool = False) -> dict:
+        """Setup arrays in the reference's attribute names and layouts;
+        ``trcadv``: the offline tracer-advection configuration (integ_type
+        TRCADV, no acoustic steps) with the coordinates its prescribed winds
+        are computed from."""
         L, G, K = self.L, self.G, self.kall
         # regional (L,G,G,K,...) -> (G,G,K,L,...)
         to3 = lambda a: np.ascontiguousarray(np.moveaxis(a, 0, 3))
@@ -1022,6 +1127,18 @@ class Grid:
         for k in ("rho_bs", "pre_bs", "tem_bs"):
             g[k] = np.zeros((G, G, K, L))
             g[k + "_pl"] = np.zeros((6, K, LP))
+        if trcadv:
+            g["integ_type"] = "TRCADV"
+            g["sstep"] = np.zeros(0, np.int64)
+            g["dts"] = float(dtl)
+            g["GRD_LON"] = np.ascontiguousarray(np.moveaxis(self.lon, 0, 2))
+            g["GRD_LAT"] = np.ascontiguousarray(np.moveaxis(self.lat, 0, 2))
+            g["GRD_LON_pl"] = np.ascontiguousarray(np.moveaxis(self.lon_pl, 0, 1))
+            g["GRD_LAT_pl"] = np.ascontiguousarray(np.moveaxis(self.lat_pl, 0, 1))
+            g["GRD_Z"] = to3(self.vz[..., 0])
+            g["GRD_ZH"] = to3(self.vz[..., 1])
+            g["GRD_Z_pl"] = pl3(self.vz_pl[..., 0])
+            g["GRD_ZH_pl"] = pl3(self.vz_pl[..., 1])
         # heights of the surface-pressure diagnostic (not uploaded): the
         # lowest full level and the surface, (G, G, L) and pole (6, 2)
         g["sfc_zkmin"] = np.ascontiguousarray(np.moveaxis(self.vz[:, :, :, 1, 0], 0, 2))

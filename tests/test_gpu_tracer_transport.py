@@ -1,0 +1,168 @@
+"""Tracer transport at the stated size: the DCMIP 2012 test 1-1 deformational
+flow (offline tracer advection, integ_type TRCADV, the reference's prescribed
+winds: period 12 days, u0 = 2 pi a / 12 d = 38.6 m/s, k0 = 10 a / 12 d, the
+deformation and the vertical overturning) on grid level 7 (163,842 cells)
+with 60 layers evenly spaced to 12 km, dt = 300 s for one full period (3456
+steps), carrying 16 passive tracers: 8 smooth 3-D Gaussian hills (amplitude 1,
+a quarter Earth radius wide, 1 km deep) and 8 sharp-edged shapes (4 compact
+cosine bells on a 0.1 background, 4 slotted cylinders), all centred at random
+points drawn from a seeded generator.  The case is built by the package's grid
+generator (checked against the reference's own TRCADV case in
+test_icogrid.py); the first tracer slot is the water-vapour slot, zero.
+
+Checked in both forms, the float64 one and the mixed one (float32 tracer
+arithmetic, float64 mass sums):
+
+* tracer mass conserved over the period: 1e-13 relative (float64), 1e-7
+  (mixed);
+* positivity and monotonicity: every mixing ratio stays within the initial
+  range of its tracer (the Thuburn limiters' guarantee), up to 1e-12 (float64)
+  and 1e-6 (mixed) of that range;
+* after one period the flow has brought the tracers back: the normalised l2
+  error of each tracer against its initial field is reported.
+
+The limiter branch choices are pinned separately: the first step (initial
+winds) of the same 16-tracer case at grid level 4 must equal the oracle's bit
+for bit, the second step to 1e-12 (the winds use exp / sin / cos).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+A = 6371220.0
+SEED = 2012
+
+
+def tracer_fields(seed=SEED):
+    """(lon, lat, z) -> mixing ratios (..., kall, 17): slot 0 water vapour
+    (zero), 1-8 Gaussian hills, 9-12 compact cosine bells, 13-16 slotted
+    cylinders"""
+    rng = np.random.default_rng(seed)
+    lon_c = rng.uniform(0.0, 2.0 * np.pi, 16)
+    lat_c = rng.uniform(-np.pi / 3.0, np.pi / 3.0, 16)
+    z_c = rng.uniform(3000.0, 9000.0, 16)
+
+    def f(lon, lat, z):
+        lon = lon[..., None]
+        lat = lat[..., None]
+        out = np.zeros(z.shape + (17,))
+        for n in range(16):
+            cosr = np.sin(lat) * np.sin(lat_c[n]) + np.cos(lat) * np.cos(lat_c[n]) * np.cos(lon - lon_c[n])
+            r = np.arccos(np.clip(cosr, -1.0, 1.0))            # great-circle angle
+            dz = (z - z_c[n]) / 1000.0
+            if n < 8:
+                q = np.exp(-(r / 0.25) ** 2 - dz ** 2)        # width a/4
+            else:
+                d = (r / 0.5) ** 2 + dz ** 2                   # compact support: r < a/2, |dz| < 1 km
+                if n < 12:
+                    q = np.where(d < 1.0, 0.1 + 0.9 * 0.5 * (1.0 + np.cos(np.pi * np.minimum(d, 1.0))), 0.1)
+                else:
+                    dlon = np.angle(np.exp(1j * (lon - lon_c[n])))
+                    slot = (np.abs(dlon) < 0.1) & (lat < lat_c[n] + 0.25)
+                    q = np.where((d < 1.0) & ~slot, 1.0, 0.1)
+            out[..., n + 1] = q
+        return out
+    return f
+
+
+def build(glevel, vlayer=60, dtl=300.0):
+    import importlib
+    ig = importlib.import_module("pynicam-dc_b200.icogrid")
+    g = ig.Grid(glevel, vlayer=vlayer, ztop=12000.0, device="cuda", layer="EVEN", topo="NONE")
+    gamma = {4: 9.6e16, 5: 1.2e16, 6: 1.5e15, 7: 2.0e14}[glevel]
+    geo = g.setup(dtl=dtl, gamma=gamma, nq=17, trcadv=True)
+    s, s_pl = g.trcadv_state(tracer_fields())
+    return geo, s, s_pl
+
+
+def _q(s, kmin, kmax):
+    """interior mixing ratios (i, j, k, l, tracer) of the 16 passive tracers"""
+    v = s[1:-1, 1:-1, kmin:kmax + 1]
+    return v[..., 7:] / v[..., 0:1]
+
+
+@pytest.fixture(scope="module")
+def period(pkg):
+    geo, s0, s0p = build(7)
+    nsteps = int(round(12 * 86400 / float(geo["dtl"])))
+    out = {"geo": geo, "s0": s0, "nsteps": nsteps}
+    for prec in ("float64", "mixed"):
+        c = pkg.NicamCuda(geo, graph=True, precision=prec)
+        try:
+            c.upload(s0, s0p)
+            m0 = c.mass_sums()
+            c.step(nsteps)
+            c.check_finite()
+            s, sp = c.download()
+            out[prec] = dict(mass0=m0, mass1=c.mass_sums(), s=s, sp=sp)
+        finally:
+            c.close()
+    return out
+
+
+@pytest.mark.parametrize("prec,tol", [("float64", 1e-13), ("mixed", 1e-7)])
+def test_tracer_mass_conserved_over_a_period(period, prec, tol):
+    r = period[prec]
+    drift = np.abs(r["mass1"][2:] - r["mass0"][2:]) / np.abs(r["mass0"][2:])
+    print(prec, "tracer mass drift over", period["nsteps"], "steps:", drift)
+    assert drift.max() <= tol, drift
+
+
+@pytest.mark.parametrize("prec,tol", [("float64", 1e-12), ("mixed", 1e-6)])
+def test_tracers_positive_and_monotone(period, prec, tol):
+    geo = period["geo"]
+    kmin, kmax = int(geo["kmin"]), int(geo["kmax"])
+    q0 = _q(period["s0"], kmin, kmax)
+    q1 = _q(period[prec]["s"], kmin, kmax)
+    lo0, hi0 = q0.min(axis=(0, 1, 2, 3)), q0.max(axis=(0, 1, 2, 3))
+    lo1, hi1 = q1.min(axis=(0, 1, 2, 3)), q1.max(axis=(0, 1, 2, 3))
+    span = hi0 - lo0
+    print(prec, "undershoot / span:", (lo0 - lo1) / span, "overshoot / span:", (hi1 - hi0) / span)
+    assert np.all(lo1 >= -tol * span), lo1           # positive (the initial minima are >= 0)
+    assert np.all(lo1 >= lo0 - tol * span), (lo0, lo1)
+    assert np.all(hi1 <= hi0 + tol * span), (hi0, hi1)
+
+
+def test_tracers_return_after_a_period(period):
+    """the deformational flow is periodic: report the normalised l2 error of
+    every tracer after one period (float64) and the mixed form's difference
+    from float64"""
+    geo = period["geo"]
+    kmin, kmax = int(geo["kmin"]), int(geo["kmax"])
+    q0 = _q(period["s0"], kmin, kmax)
+    q1 = _q(period["float64"]["s"], kmin, kmax)
+    qm = _q(period["mixed"]["s"], kmin, kmax)
+    l2 = np.sqrt(((q1 - q0) ** 2).sum(axis=(0, 1, 2, 3)) / (q0 ** 2).sum(axis=(0, 1, 2, 3)))
+    dm = np.sqrt(((qm - q1) ** 2).sum(axis=(0, 1, 2, 3)) / (q1 ** 2).sum(axis=(0, 1, 2, 3)))
+    print("l2 error after one period, hills / bells / cylinders:", l2[:8], l2[8:12], l2[12:])
+    print("mixed vs float64:", dm)
+    assert np.all(l2[:8] < 0.5) and np.all(dm < 1e-2), (l2, dm)
+
+
+def test_limiters_bit_exact_vs_oracle_first_steps(pkg):
+    """16-tracer case at grid level 4: step 1 (initial winds) bit for bit with
+    the oracle, step 2 (winds from exp / sin / cos) to 1e-12"""
+    from oracle import nicam_step as O
+    geo, s0, s0p = build(4, vlayer=60, dtl=600.0)
+    c = pkg.NicamCuda(geo, graph=False)
+    try:
+        c.upload(s0, s0p)
+        outs = []
+        for _ in range(2):
+            c.step(1)
+            outs.append(c.download())
+    finally:
+        c.close()
+    G = O.Geo(geo)
+    crd = [geo[k] for k in ("GRD_LON", "GRD_LAT", "GRD_Z", "GRD_ZH", "GRD_LON_pl", "GRD_LAT_pl", "GRD_Z_pl", "GRD_ZH_pl")]
+    s, sp = s0, s0p
+    dtl = float(geo["dtl"])
+    for n, (d, dp) in enumerate(outs, start=1):
+        s, sp = O.trcadv_step(G, s, sp, n * dtl, *crd)
+        if n == 1:
+            assert np.array_equal(d[..., 6:], s[..., 6:]) and np.array_equal(dp[..., 6:], sp[..., 6:])
+        else:
+            for v in range(6, s.shape[-1]):
+                den = np.sqrt(np.sum(s[..., v] ** 2))
+                assert np.sqrt(np.sum((d[..., v] - s[..., v]) ** 2)) <= 1e-12 * den, v

@@ -7,9 +7,12 @@ Everything is bit-for-bit except the operator coefficients (assembled in a
 different summation order: rounding level) and the terrain-slope metric
 C2WfactGz (gradient of a nearly flat height field through those coefficients).
 """
+import os
+
 import numpy as np
 import pytest
 
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 COEF_TOL = 2e-15          # relative, max-norm over the array
 SLOPE_TOL = 5e-12
 
@@ -70,3 +73,33 @@ def test_device_spring_matches_host(pkg):
         xd, xdp, idv = ig.spring(x, xpl, gl, ex, device="cuda")
         assert ih == iters and idv == iters
         assert np.abs(xd - xh).max() < 1e-12 and np.abs(xdp - xhp).max() < 1e-12
+
+
+def test_trcadv_case_matches_reference():
+    """the DCMIP 1-1 offline tracer-advection case (EVEN layers to 12 km, flat
+    surface, integ_type TRCADV) built by the package reproduces the
+    reference's own set-up and initial state (make_trcadv.py fixture): the
+    state bit for bit, the set-up arrays to round-off (the terrain-slope
+    metric of a flat surface is round-off noise of ~1e-16)"""
+    import importlib
+    from make_golden import load
+    ig = importlib.import_module("pynicam-dc_b200.icogrid")
+    geo_r, st = load(os.path.join(GOLDEN, "gl03_z10_trcadv.npz"))
+    g = ig.Grid(3, vlayer=10, ztop=12000.0, device="cpu", layer="EVEN", topo="NONE")
+    geo = g.setup(dtl=1200.0, gamma=7.68e17, nq=5, trcadv=True)
+
+    def trc(lon, lat, z):
+        q4 = g.dcmip11_fields(lon, lat, z)[-1]
+        return np.concatenate([np.zeros(q4.shape[:-1] + (1,)), q4], axis=-1)
+
+    s, s_pl = g.trcadv_state(trc)
+    assert np.array_equal(s, st["state0"]) and np.array_equal(s_pl, st["state0_pl"])
+    assert str(geo["integ_type"]) == "TRCADV" and geo["sstep"].size == 0
+    for k, v in geo_r.items():
+        a = np.asarray(v)
+        if a.dtype.kind != "f" or k not in geo or k == "CVW":
+            continue
+        b = np.asarray(geo[k], np.float64)
+        assert b.shape == a.shape, k
+        tol = 1e-17 if k.startswith("VMTR_C2WfactGz") else 1e-13 * max(np.abs(a).max(), 1e-300)
+        assert np.abs(b - a).max() <= tol, k
