@@ -12,7 +12,10 @@
  *
  * Every function returns 0 on success and a non-zero status otherwise;
  * nc_last_error() returns the message.  No function aborts the process.
- * A handle is not re-entrant: one host thread drives one handle.
+ * A handle is not re-entrant: one host thread drives one handle.  Several
+ * handles on one device run one after another: the run constants are
+ * device-global, so a call on a handle first waits for the work still queued
+ * by the handle used before it.
  */
 #ifndef NICAM_CUDA_H
 #define NICAM_CUDA_H

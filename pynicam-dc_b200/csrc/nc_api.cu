@@ -485,8 +485,23 @@ static int up_vec(const ArrTab& T, const char* name, int n, double* dst) {
   return 0;
 }
 
+// The run constants and geometry pointers are device-global (__constant__), so
+// a handle's kernels read whatever handle is current when they run.  Before
+// another handle's tables are loaded, the previously current handle's queued
+// work (steps, marshal kernels, copies) must have finished: its streams are
+// non-blocking, so nothing else orders them before the constant copy.
+static int drain(nc_handle* h) {
+  for (cudaStream_t st : {h->stream, h->stream2, h->s_h2d, h->s_d2h})
+    if (st) CU(cudaStreamSynchronize(st));
+  return 0;
+}
+
 static int load_consts(nc_handle* h) {
   if (g_current == h) return 0;
+  if (g_current) {
+    int rc = drain(g_current);
+    if (rc) return rc;
+  }
   CU(cudaMemcpyToSymbol(cD, &h->D, sizeof(Dims)));
   CU(cudaMemcpyToSymbol(cC, &h->C, sizeof(Consts)));
   CU(cudaMemcpyToSymbol(cG, &h->Gm, sizeof(Geom)));
