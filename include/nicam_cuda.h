@@ -127,6 +127,18 @@ int nc_step(nc_handle* h, int32_t nsteps);
 /* Capture one large step as a CUDA graph and replay it (default on). */
 int nc_set_graph(nc_handle* h, int32_t enable);
 
+/* Threads per block of one column / point kernel of the step, named as in
+ * nc_kernel_stats: "diag", "vi_solve", "vi_energy", "vp0_c", "gtend",
+ * "hdiff1", "post", "split_init", "trc_vflux", "trc_vadv", "trc_remap",
+ * "trc_qout", "trc_apply", "trc_rhog".  A multiple of 32 up to the kernel's
+ * launch bound (128 for diag, vi_solve and vi_energy, 256 for vp0_c, 1024 for
+ * the others); the default is 128 (256 for vp0_c).  Changing it drops the
+ * captured step graph.  The knobs of the project's autotuner
+ * (pynicam-dc_b200/autotune.py); no counterpart in the reference, whose
+ * jax backend leaves launch shapes to XLA. */
+int nc_set_block(nc_handle* h, const char* kernel, int32_t threads);
+int nc_get_block(nc_handle* h, const char* kernel, int32_t* threads);
+
 /* Debugging aid: run only the first nphases phases of one large step
  * (phase boundaries sit after each halo exchange / kernel group, in the order
  * of Dyn.dynamics_step), without graph capture, then synchronize. */

@@ -302,6 +302,18 @@ static inline R* RG(const FieldPair& f) { return reinterpret_cast<R*>(f.r); }
 template <class R>
 static inline R* PL(const FieldPair& f) { return reinterpret_cast<R*>(f.p); }
 
+// Threads per block of the column / point kernels: chosen at run time (the
+// autotuner, nc_set_block), within each kernel's launch bound.
+enum {
+  TB_DIAG, TB_VISOLVE, TB_VIENERGY, TB_VP0C, TB_GTEND, TB_HDIFF1, TB_POST, TB_SPLIT, TB_TRC_VFLUX, TB_TRC_VADV,
+  TB_TRC_REMAP, TB_TRC_QOUT, TB_TRC_APPLY, TB_TRC_RHOG, TB_N
+};
+static const char* const kTuneName[TB_N] = {"diag", "vi_solve", "vi_energy", "vp0_c", "gtend", "hdiff1", "post",
+                                            "split_init", "trc_vflux", "trc_vadv", "trc_remap", "trc_qout",
+                                            "trc_apply", "trc_rhog"};
+static const int kTuneMax[TB_N] = {128, 128, 128, NC_VP0C_BLOCK, 1024, 1024, 1024, 1024, 1024, 1024, 1024, 1024,
+                                   1024, 1024};
+
 // "no non-finite value seen": every byte 0x7f, above any variable index
 #define NC_BAD_NONE 0x7f7f7f7f
 
@@ -309,6 +321,7 @@ struct nc_handle {
   Dims D{};
   Consts C{};
   Geom Gm{};
+  int blk[TB_N] = {128, 128, 128, NC_VP0C_BLOCK, 128, 128, 128, 128, 128, 128, 128, 128, 128, 128};
   // mixed precision: float32 work fields, geometry and constants (the
   // deviations pregd/rhogd and the implicit matrix Mc/Mu/Ml stay float64)
   bool mixed = false;
@@ -646,8 +659,10 @@ static int run_step(nc_handle* h) {
   h->phase = 0;
   const Dims& D = h->D;
   const unsigned gkl = grid_cols_kl(h);
-  const unsigned greg = (unsigned)((D.npt2 + kBlock - 1) / kBlock);
-  const unsigned plk = (unsigned)(((D.KA * D.LP) + 31) / 32 * 32);
+  // pole kernels: one thread per pole column (6 * LP) or per pole level (kall * LP);
+  // LP = 2 per ensemble member
+  const unsigned pcb = (unsigned)((6 * D.LP + 31) / 32);
+  const unsigned pkb = (unsigned)((D.KA * D.LP + 127) / 128);
   const unsigned npt_blocks = (unsigned)((D.npt + kBlock - 1) / kBlock);
   const unsigned npl_blocks = (unsigned)((D.npl + kBlock - 1) / kBlock);
   // per-level tiled kernels: (levels kmin..kmax, tiles, regions)
@@ -677,9 +692,9 @@ static int run_step(nc_handle* h) {
       return a;
     };
     // regional and pole columns: same kernel, launched with the matching pointers
-    k_diag<<<greg, kBlock, 0, s>>>(diag_args(false), 0);
+    k_diag<<<(unsigned)((D.npt2 + h->blk[TB_DIAG] - 1) / h->blk[TB_DIAG]), h->blk[TB_DIAG], 0, s>>>(diag_args(false), 0);
     TRY(check_launch(h, "diag"));
-    k_diag<<<1, 32, 0, ps>>>(diag_args(true), 1);
+    k_diag<<<pcb, 32, 0, ps>>>(diag_args(true), 1);
     TRY(check_launch(h, "diag_pl"));
     PHASE();
     // ---- momentum advection
@@ -697,7 +712,7 @@ static int run_step(nc_handle* h) {
     amp.rg = PL<R>(h->P[0]); amp.rvx = PL<R>(h->P[1]); amp.rvy = PL<R>(h->P[2]); amp.rvz = PL<R>(h->P[3]); amp.rw = PL<R>(h->P[4]);
     amp.vvx = PL<R>(h->vv[0]); amp.vvy = PL<R>(h->vv[1]); amp.vvz = PL<R>(h->vv[2]);
     amp.gvx = PL<R>(h->gadv[0]); amp.gvy = PL<R>(h->gadv[1]); amp.gvz = PL<R>(h->gadv[2]); amp.gw = PL<R>(h->gadv[3]);
-    k_advmom_pl<<<1, 32, 0, ps>>>(amp);
+    k_advmom_pl<<<pcb, 32, 0, ps>>>(amp);
     TRY(check_launch(h, "advmom_pl"));
     PHASE();
     // ---- hyperdiffusion
@@ -708,9 +723,9 @@ static int run_step(nc_handle* h) {
       src.f[n] = RG<R>(*sf[n]); srcp.f[n] = PL<R>(*sf[n]);
       o1.f[n] = RG<R>(h->vt[n]); o1p.f[n] = PL<R>(h->vt[n]);
     }
-    k_hdiff1<<<greg, kBlock, 0, s>>>(src, o1);
+    k_hdiff1<<<(unsigned)((D.npt2 + h->blk[TB_HDIFF1] - 1) / h->blk[TB_HDIFF1]), h->blk[TB_HDIFF1], 0, s>>>(src, o1);
     TRY(check_launch(h, "hdiff1"));
-    k_hdiff1_pl<<<1, plk, 0, ps>>>(srcp, o1p);
+    k_hdiff1_pl<<<pkb, 128, 0, ps>>>(srcp, o1p);
     TRY(check_launch(h, "hdiff1_pl"));
     TRY(comm<R>(h, {h->vt[0], h->vt[1], h->vt[2], h->vt[3], h->vt[4], h->vt[5]}));
     PHASE();
@@ -728,7 +743,7 @@ static int run_step(nc_handle* h) {
       k_hdiff2_l<<<gl2, HD_DX * HD_DY, 0, s>>>(vin, RG<R>(h->P[0]), o2);
       TRY(check_launch(h, "hdiff2"));
     }
-    k_hdiff2_pl<<<1, plk, 0, ps>>>(vinp, PL<R>(h->P[0]), o2p);
+    k_hdiff2_pl<<<pkb, 128, 0, ps>>>(vinp, PL<R>(h->P[0]), o2p);
     TRY(check_launch(h, "hdiff2_pl"));
     TRY(comm<R>(h, {h->vt2[0], h->vt2[1], h->vt2[2], h->vt2[3], h->vt2[4], h->vt2[5]}));
     PHASE();
@@ -739,13 +754,13 @@ static int run_step(nc_handle* h) {
       for (int n = 0; n < 6; ++n) { ga.vt2.f[n] = F(h->vt2[n]); ga.gT0[n] = F(h->gT0[n]); }
       ga.rhog = F(h->P[0]); ga.gvx = F(h->gadv[0]); ga.gvy = F(h->gadv[1]); ga.gvz = F(h->gadv[2]);
       ga.gw = F(h->gadv[3]); ga.frhog = F(h->frhog);
-      if (!pole) k_gtend<<<greg, kBlock, 0, s>>>(ga, 0);
-      else k_gtend<<<1, 32, 0, ps>>>(ga, 1);
+      if (!pole) k_gtend<<<(unsigned)((D.npt2 + h->blk[TB_GTEND] - 1) / h->blk[TB_GTEND]), h->blk[TB_GTEND], 0, s>>>(ga, 0);
+      else k_gtend<<<pcb, 32, 0, ps>>>(ga, 1);
       TRY(check_launch(h, pole ? "gtend_pl" : "gtend"));
     }
     PHASE();
     // ---- vi_small_step (mod_vi.py:104-1590)
-    k_split_init<<<npt_blocks, kBlock, 0, s>>>(RG<R>(h->P0[0]), RG<R>(h->P0[1]), RG<R>(h->P0[2]), RG<R>(h->P0[3]), RG<R>(h->P0[4]),
+    k_split_init<<<(unsigned)((D.npt + h->blk[TB_SPLIT] - 1) / h->blk[TB_SPLIT]), h->blk[TB_SPLIT], 0, s>>>(RG<R>(h->P0[0]), RG<R>(h->P0[1]), RG<R>(h->P0[2]), RG<R>(h->P0[3]), RG<R>(h->P0[4]),
                                                 RG<R>(h->P0[5]), prog_reg<R>(h), RG<R>(h->PSa[0]), RG<R>(h->PSa[1]), RG<R>(h->PSa[2]),
                                                 RG<R>(h->PSa[3]), RG<R>(h->PSa[4]), RG<R>(h->PSa[5]), RG<R>(h->PM[0]), RG<R>(h->PM[1]),
                                                 RG<R>(h->PM[2]), RG<R>(h->PM[3]), RG<R>(h->PM[4]), D.npt, nl == 0);
@@ -765,7 +780,7 @@ static int run_step(nc_handle* h) {
       const dim3 gt((unsigned)((D.G - 2 + DD_DX - 1) / DD_DX), (unsigned)((D.G - 2 + DD_DY - 1) / DD_DY), (unsigned)D.L);
       k_dd3d_t<<<gt, DD_DX * DD_DY, 0, s>>>(v, o);
       TRY(check_launch(h, "dd3d"));
-      k_dd3d_pl<<<1, plk, 0, ps>>>(vp, op);
+      k_dd3d_pl<<<pkb, 128, 0, ps>>>(vp, op);
       TRY(check_launch(h, "dd3d_pl"));
       return comm<R>(h, {h->vtmp2[0], h->vtmp2[1], h->vtmp2[2]});
     };
@@ -790,10 +805,10 @@ static int run_step(nc_handle* h) {
         for (int n = 0; n < 8; ++n) vh.out[n] = RG<R>(h->vph[n]);
         k_vp0_hl<<<lvgrid_vp, VP_DX * VP_DY, 0, s>>>(va, vh);
         TRY(check_launch(h, "vp0_h"));
-        k_vp0_cr<<<(unsigned)((D.npt2 + NC_VP0C_BLOCK - 1) / NC_VP0C_BLOCK), NC_VP0C_BLOCK, 0, s>>>(va, vh);
+        k_vp0_cr<<<(unsigned)((D.npt2 + h->blk[TB_VP0C] - 1) / h->blk[TB_VP0C]), h->blk[TB_VP0C], 0, s>>>(va, vh);
         TRY(check_launch(h, "vp0_c"));
       } else {
-        k_vp0<<<1, 32, 0, ps>>>(va, 1);
+        k_vp0<<<pcb, 32, 0, ps>>>(va, 1);
         TRY(check_launch(h, "vp0_pl"));
       }
     }
@@ -821,7 +836,7 @@ static int run_step(nc_handle* h) {
           k_path1_l<<<lvgrid, DD_DX * DD_DY, 0, s>>>(pa);
           TRY(check_launch(h, "path1"));
         } else {
-          k_path1<<<1, 32, 0, ps>>>(pa, 1);
+          k_path1<<<pcb, 32, 0, ps>>>(pa, 1);
           TRY(check_launch(h, "path1_pl"));
         }
       }
@@ -841,15 +856,15 @@ static int run_step(nc_handle* h) {
         if (!pole) {
           k_vimain_a_l<<<lvgrid, DD_DX * DD_DY, 0, s>>>(va);
           TRY(check_launch(h, "vimain_a"));
-          if (h->C.gam_unit) k_vi_solve<R, true><<<greg, kBlock, 0, s>>>(va);
-          else k_vi_solve<R, false><<<greg, kBlock, 0, s>>>(va);
+          if (h->C.gam_unit) k_vi_solve<R, true><<<(unsigned)((D.npt2 + h->blk[TB_VISOLVE] - 1) / h->blk[TB_VISOLVE]), h->blk[TB_VISOLVE], 0, s>>>(va);
+          else k_vi_solve<R, false><<<(unsigned)((D.npt2 + h->blk[TB_VISOLVE] - 1) / h->blk[TB_VISOLVE]), h->blk[TB_VISOLVE], 0, s>>>(va);
           TRY(check_launch(h, "vi_solve"));
-          k_vi_energy_p<<<npt_blocks, kBlock, 0, s>>>(va);
+          k_vi_energy_p<<<(unsigned)((D.npt + h->blk[TB_VIENERGY] - 1) / h->blk[TB_VIENERGY]), h->blk[TB_VIENERGY], 0, s>>>(va);
           TRY(check_launch(h, "vi_energy"));
         } else {
-          k_vimain_a<<<1, plk, 0, ps>>>(va, 1);
+          k_vimain_a<<<pkb, 128, 0, ps>>>(va, 1);
           TRY(check_launch(h, "vimain_a_pl"));
-          k_vimain_b<<<1, 32, 0, ps>>>(va, 1);
+          k_vimain_b<<<pcb, 32, 0, ps>>>(va, 1);
           TRY(check_launch(h, "vimain_b_pl"));
         }
       }
@@ -857,9 +872,9 @@ static int run_step(nc_handle* h) {
       PHASE();
     }
     FieldPair* PSf = (nitr % 2 == 0) ? h->PSa : h->PSb;
-    k_post<<<greg, kBlock, 0, s>>>(prog_reg<R>(h), RG<R>(PSf[0]), RG<R>(PSf[1]), RG<R>(PSf[2]), RG<R>(PSf[3]), RG<R>(PSf[4]), RG<R>(PSf[5]), 0);
+    k_post<<<(unsigned)((D.npt2 + h->blk[TB_POST] - 1) / h->blk[TB_POST]), h->blk[TB_POST], 0, s>>>(prog_reg<R>(h), RG<R>(PSf[0]), RG<R>(PSf[1]), RG<R>(PSf[2]), RG<R>(PSf[3]), RG<R>(PSf[4]), RG<R>(PSf[5]), 0);
     TRY(check_launch(h, "post"));
-    k_post<<<1, 32, 0, ps>>>(prog_pl<R>(h), PL<R>(PSf[0]), PL<R>(PSf[1]), PL<R>(PSf[2]), PL<R>(PSf[3]), PL<R>(PSf[4]), PL<R>(PSf[5]), 1);
+    k_post<<<pcb, 32, 0, ps>>>(prog_pl<R>(h), PL<R>(PSf[0]), PL<R>(PSf[1]), PL<R>(PSf[2]), PL<R>(PSf[3]), PL<R>(PSf[4]), PL<R>(PSf[5]), 1);
     TRY(check_launch(h, "post_pl"));
     TRY(comm<R>(h, {h->PM[0], h->PM[1], h->PM[2], h->PM[3], h->PM[4]}));
     PHASE();
@@ -890,8 +905,8 @@ static int run_step(nc_handle* h) {
     ta.rvx = F(h->PM[1]); ta.rvy = F(h->PM[2]); ta.rvz = F(h->PM[3]); ta.rw = F(h->PM[4]);
     ta.rhog_in = F(h->P0[0]); ta.frhog = F(h->frhog); ta.flx_v = F(h->flx_v); ta.rhog_t = F(h->rhog_t);
     ta.dt = dt;
-    if (!pole) k_trc_vflux<<<greg, kBlock, 0, s>>>(ta, 0);
-    else k_trc_vflux<<<1, 32, 0, ps>>>(ta, 1);
+    if (!pole) k_trc_vflux<<<(unsigned)((D.npt2 + h->blk[TB_TRC_VFLUX] - 1) / h->blk[TB_TRC_VFLUX]), h->blk[TB_TRC_VFLUX], 0, s>>>(ta, 0);
+    else k_trc_vflux<<<pcb, 32, 0, ps>>>(ta, 1);
     TRY(check_launch(h, pole ? "trc_vflux_pl" : "trc_vflux"));
   }
   auto vadv = [&](int iq, bool second) -> int {
@@ -902,8 +917,8 @@ static int run_step(nc_handle* h) {
       va.den = second ? F(h->rhog_t) : F(h->P0[0]);
       va.flx_v = F(h->flx_v); va.frhog = F(h->frhog);
       va.dt = dt; va.bcoef = 0.0; va.clamp = second ? 1 : 0; va.dtl = dt;
-      if (!pole) k_trc_vadv<<<greg, kBlock, 0, s>>>(va, 0);
-      else k_trc_vadv<<<1, 32, 0, ps>>>(va, 1);
+      if (!pole) k_trc_vadv<<<(unsigned)((D.npt2 + h->blk[TB_TRC_VADV] - 1) / h->blk[TB_TRC_VADV]), h->blk[TB_TRC_VADV], 0, s>>>(va, 0);
+      else k_trc_vadv<<<pcb, 32, 0, ps>>>(va, 1);
       TRY(check_launch(h, pole ? "trc_vadv_pl" : "trc_vadv"));
     }
     return 0;
@@ -926,7 +941,7 @@ static int run_step(nc_handle* h) {
     TrcHfluxPlArgs<R> hp;
     hp.rho = PL<R>(h->PM[0]); hp.rvx = PL<R>(h->PM[1]); hp.rvy = PL<R>(h->PM[2]); hp.rvz = PL<R>(h->PM[3]); hp.rhog_t = PL<R>(h->rhog_t);
     hp.flx = PL<R>(h->flx[0]); hp.xc = PL<R>(h->xc[0]); hp.ch = PL<R>(h->ch[0]); hp.cm = PL<R>(h->cm[0]); hp.dt = dt;
-    k_trc_hflux_pl<<<1, plk, 0, ps>>>(hp);
+    k_trc_hflux_pl<<<pkb, 128, 0, ps>>>(hp);
     TRY(check_launch(h, "trc_hflux_pl"));
   }
   PHASE();
@@ -938,7 +953,7 @@ static int run_step(nc_handle* h) {
                                                 RG<R>(h->gq[2]));
     }
     TRY(check_launch(h, "trc_grad"));
-    k_trc_grad_pl<<<1, plk, 0, ps>>>(PL<R>(h->Pq[iq]), PL<R>(h->rhog_t), PL<R>(h->q), PL<R>(h->gq[0]), PL<R>(h->gq[1]), PL<R>(h->gq[2]));
+    k_trc_grad_pl<<<pkb, 128, 0, ps>>>(PL<R>(h->Pq[iq]), PL<R>(h->rhog_t), PL<R>(h->q), PL<R>(h->gq[0]), PL<R>(h->gq[1]), PL<R>(h->gq[2]));
     TRY(check_launch(h, "trc_grad_pl"));
     TRY(comm<R>(h, {h->gq[0], h->gq[1], h->gq[2]}));
     TrcRemapArgs<R> ra;
@@ -946,12 +961,12 @@ static int run_step(nc_handle* h) {
     for (int f = 0; f < 9; ++f) ra.xc[f] = RG<R>(h->xc[f]);
     for (int f = 0; f < 6; ++f) ra.cm[f] = RG<R>(h->cm[f]);
     for (int f = 0; f < 3; ++f) ra.qa[f] = RG<R>(h->qa[f]);
-    k_trc_remap<<<greg, kBlock, 0, s>>>(ra);
+    k_trc_remap<<<(unsigned)((D.npt2 + h->blk[TB_TRC_REMAP] - 1) / h->blk[TB_TRC_REMAP]), h->blk[TB_TRC_REMAP], 0, s>>>(ra);
     TRY(check_launch(h, "trc_remap"));
     TrcRemapPlArgs<R> rp;
     rp.q = PL<R>(h->q); rp.gq0 = PL<R>(h->gq[0]); rp.gq1 = PL<R>(h->gq[1]); rp.gq2 = PL<R>(h->gq[2]); rp.xc = PL<R>(h->xc[0]);
     rp.cm = PL<R>(h->cm[0]); rp.qa = PL<R>(h->qa[0]);
-    k_trc_remap_pl<<<1, plk, 0, ps>>>(rp);
+    k_trc_remap_pl<<<pkb, 128, 0, ps>>>(rp);
     TRY(check_launch(h, "trc_remap_pl"));
     TrcLimArgs<R> la;
     la.q = RG<R>(h->q); la.rhog_t = RG<R>(h->rhog_t); la.frhog = RG<R>(h->frhog);
@@ -963,19 +978,19 @@ static int run_step(nc_handle* h) {
     lp.q = PL<R>(h->q); lp.ch = PL<R>(h->ch[0]); lp.cm = PL<R>(h->cm[0]); lp.rhog_t = PL<R>(h->rhog_t); lp.frhog = PL<R>(h->frhog);
     lp.qa = PL<R>(h->qa[0]); lp.flx = PL<R>(h->flx[0]); lp.Qmin = PL<R>(h->Qmin); lp.Qmax = PL<R>(h->Qmax);
     lp.qout_min = PL<R>(h->Qmin); lp.qout_max = PL<R>(h->Qmax); lp.rhogq = PL<R>(h->Pq[iq]); lp.dt = dt;
-    k_trc_qout<<<greg, kBlock, 0, s>>>(la);
+    k_trc_qout<<<(unsigned)((D.npt2 + h->blk[TB_TRC_QOUT] - 1) / h->blk[TB_TRC_QOUT]), h->blk[TB_TRC_QOUT], 0, s>>>(la);
     TRY(check_launch(h, "trc_qout"));
-    k_trc_qout_pl<<<1, plk, 0, ps>>>(lp);
+    k_trc_qout_pl<<<pkb, 128, 0, ps>>>(lp);
     TRY(check_launch(h, "trc_qout_pl"));
     TRY(comm<R>(h, {h->Qmin, h->Qmax}));
-    k_trc_apply<<<greg, kBlock, 0, s>>>(la);
+    k_trc_apply<<<(unsigned)((D.npt2 + h->blk[TB_TRC_APPLY] - 1) / h->blk[TB_TRC_APPLY]), h->blk[TB_TRC_APPLY], 0, s>>>(la);
     TRY(check_launch(h, "trc_apply"));
-    k_trc_apply_pl<<<1, plk, 0, ps>>>(lp);
+    k_trc_apply_pl<<<pkb, 128, 0, ps>>>(lp);
     TRY(check_launch(h, "trc_apply_pl"));
   }
   PHASE();
   TRY(join_pl(h));
-  k_trc_rhog<<<gkl, kBlock, 0, s>>>(RG<R>(h->rhog_t), RG<R>(h->flx[0]), RG<R>(h->flx[1]), RG<R>(h->flx[2]), RG<R>(h->flx[3]), RG<R>(h->flx[4]),
+  k_trc_rhog<<<(unsigned)(((D.npt2 + (long long)D.KA * D.LP) + h->blk[TB_TRC_RHOG] - 1) / h->blk[TB_TRC_RHOG]), h->blk[TB_TRC_RHOG], 0, s>>>(RG<R>(h->rhog_t), RG<R>(h->flx[0]), RG<R>(h->flx[1]), RG<R>(h->flx[2]), RG<R>(h->flx[3]), RG<R>(h->flx[4]),
                                      RG<R>(h->flx[5]), RG<R>(h->frhog), (R)dt, PL<R>(h->flx[0]), PL<R>(h->rhog_t), PL<R>(h->frhog));
   TRY(check_launch(h, "trc_rhog"));
   TRY(fork_pl(h));
@@ -1133,6 +1148,15 @@ static int mass_sum(nc_handle* h, int n) {
   return check_launch(h, "mass");
 }
 static int step_once(nc_handle* h) { return h->mixed ? run_step<float>(h) : run_step<double>(h); }
+// forget the captured step (the next nc_step captures it again)
+static int drop_graph(nc_handle* h) {
+  if (h->gexec || h->graph) CU(cudaStreamSynchronize(h->stream));
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  h->gexec = nullptr;
+  h->graph = nullptr;
+  return 0;
+}
 // the entry points of the float64 form only
 static int f64_only(nc_handle* h, const char* what) {
   if (h->mixed) return fail(NC_ERR_STATE, std::string(what) + ": not available for a mixed-precision handle");
@@ -1270,6 +1294,12 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   TRY(scalar(T, "gmax", v)); D.gmax = (int)v;
   TRY(scalar(T, "nq", v)); D.nq = (int)v;
   D.LP = 2;
+  if (T.get("members")) {   // ensemble members stacked along the region axis (lall = 40 * members)
+    double mem;
+    TRY(scalar(T, "members", mem));
+    if (mem < 1 || mem > 4096) return fail(NC_ERR_ARG, "members must be 1..4096");
+    D.LP = 2 * (int)mem;
+  }
   if (D.G < 4 || D.KA < 4 || D.KA > NC_MAXK || D.L < 1 || D.kmin != 1 || D.kmax != D.KA - 2 || D.gmin != 1 ||
       D.gmax != D.G - 2 || D.nq < 1 || D.nq > NC_MAXNQ)
     return fail(NC_ERR_ARG, "unsupported grid dimensions (need kmin=1, kmax=kall-2, 1<=nq<=32, kall<=128)");
@@ -1721,6 +1751,32 @@ int nc_join_copies(nc_handle* h) {
   CU(cudaStreamWaitEvent(h->stream, h->ev_in_ready, 0));
   CU(cudaStreamWaitEvent(h->stream, h->ev_out_done, 0));
   return 0;
+}
+
+int nc_set_block(nc_handle* h, const char* kernel, int32_t threads) {
+  if (!h || !kernel) return fail(NC_ERR_ARG, "nc_set_block: null argument");
+  for (int n = 0; n < TB_N; ++n) {
+    if (std::strcmp(kernel, kTuneName[n]) != 0) continue;
+    if (threads < 32 || threads > kTuneMax[n] || threads % 32 != 0)
+      return fail(NC_ERR_ARG, std::string("nc_set_block: ") + kernel + " takes a multiple of 32 threads up to " +
+                                  std::to_string(kTuneMax[n]));
+    if (h->blk[n] != threads) {
+      h->blk[n] = threads;
+      TRY(drop_graph(h));
+    }
+    return 0;
+  }
+  return fail(NC_ERR_ARG, std::string("nc_set_block: no tunable kernel ") + kernel);
+}
+
+int nc_get_block(nc_handle* h, const char* kernel, int32_t* threads) {
+  if (!h || !kernel || !threads) return fail(NC_ERR_ARG, "nc_get_block: null argument");
+  for (int n = 0; n < TB_N; ++n)
+    if (std::strcmp(kernel, kTuneName[n]) == 0) {
+      *threads = h->blk[n];
+      return 0;
+    }
+  return fail(NC_ERR_ARG, std::string("nc_get_block: no tunable kernel ") + kernel);
 }
 
 int nc_set_graph(nc_handle* h, int32_t enable) {

@@ -377,7 +377,7 @@ __device__ R advconv_pl_at(int g, int lp, int k, const Col& c, const MetT<R>& m,
 
 template <class R>
 __global__ void k_advmom_pl(AdvMomArgs<R> a) {
-  int t = threadIdx.x;
+  int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (t >= 6 * cD.LP) return;
   int g = t / cD.LP, lp = t % cD.LP;
   const Col c = col_pl(g, lp);
@@ -454,7 +454,7 @@ __global__ void k_hdiff1(Six<R> src, SixOut<R> out) {
 
 template <class R>
 __global__ void k_hdiff1_pl(Six<R> src, SixOut<R> out) {
-  int t = threadIdx.x;
+  int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (t >= cD.KA * cD.LP) return;
   int k = t / cD.LP, lp = t % cD.LP;
   for (int n = 0; n < 6; ++n) {
@@ -600,7 +600,7 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, NC_MINB(R, 4, NC_F32_HDIFF2)) k
 
 template <class R>
 __global__ void k_hdiff2_pl(Six<R> vt, const R* rhog, SixOut<R> out) {
-  int t = threadIdx.x;
+  int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (t >= cD.KA * cD.LP) return;
   int k = t / cD.LP, lp = t % cD.LP;
   const R Kh = CC.Kh;

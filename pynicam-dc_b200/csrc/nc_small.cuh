@@ -150,7 +150,7 @@ __device__ __forceinline__ TileLv tile_level(int kbase) {
 // pole 3-D divergence damping (kernels/oprt3ddivdamp.py:176-237)
 template <class R>
 __global__ void k_dd3d_pl(Four<R> v, Three<R> out) {
-  int t = threadIdx.x;
+  int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (t >= cD.KA * cD.LP) return;
   int k = t / cD.LP, lp = t % cD.LP;
   for (int g = 0; g < 6; ++g)

@@ -304,7 +304,7 @@ struct TrcHfluxPlArgs {
 
 template <class R>
 __global__ void k_trc_hflux_pl(TrcHfluxPlArgs<R> a) {
-  int t = threadIdx.x;
+  int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (t >= cD.KA * cD.LP) return;
   int k = t / cD.LP, lp = t % cD.LP;
   const R* gt = CG.GMTR_t_pl;
@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(TG_DX * TG_DY) k_trc_grad_t(const R* rhogq, co
 template <class R>
 __global__ void k_trc_grad_pl(const R* rhogq, const R* rhog_t, R* q, R* gq0, R* gq1,
                               R* gq2) {
-  int t = threadIdx.x;
+  int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (t >= cD.KA * cD.LP) return;
   int k = t / cD.LP, lp = t % cD.LP;
   R qv[6];
@@ -471,7 +471,7 @@ struct TrcRemapPlArgs {
 
 template <class R>
 __global__ void k_trc_remap_pl(TrcRemapPlArgs<R> a) {
-  int t = threadIdx.x;
+  int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (t >= cD.KA * cD.LP) return;
   int k = t / cD.LP, lp = t % cD.LP;
   const R* X = CG.GRD_x_pl;
@@ -664,7 +664,7 @@ __device__ void trc_qin_pl(const TrcLimPlArgs<R>& a, int v, int k, int lp, R& in
 
 template <class R>
 __global__ void k_trc_qout_pl(TrcLimPlArgs<R> a) {
-  int t = threadIdx.x;
+  int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (t >= cD.KA * cD.LP) return;
   int k = t / cD.LP, lp = t % cD.LP;
   int p0 = ipl(0, k, lp);
@@ -695,7 +695,7 @@ __global__ void k_trc_qout_pl(TrcLimPlArgs<R> a) {
 
 template <class R>
 __global__ void k_trc_apply_pl(TrcLimPlArgs<R> a) {
-  int t = threadIdx.x;
+  int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (t >= cD.KA * cD.LP) return;
   int k = t / cD.LP, lp = t % cD.LP;
   int p0 = ipl(0, k, lp);

@@ -31,7 +31,7 @@ _lib = None
 
 # every entry point declared in include/nicam_cuda.h
 EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_state_async", "nc_join_copies",
-           "nc_upload_state_device", "nc_download_state_device", "nc_check_finite",
+           "nc_upload_state_device", "nc_download_state_device", "nc_check_finite", "nc_set_block", "nc_get_block",
            "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",
            "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_forcing_step", "nc_history_vars", "nc_restart_pack",
            "nc_restart_unpack", "nc_restart_finish", "nc_divide_known",
@@ -55,6 +55,8 @@ def load_library(path: str = LIB_PATH):
     lib.nc_upload_state_device.argtypes = [vp, dp, dp, vp]
     lib.nc_download_state_device.argtypes = [vp, dp, dp, vp]
     lib.nc_check_finite.argtypes = [vp]
+    lib.nc_set_block.argtypes = [vp, ctypes.c_char_p, i32]
+    lib.nc_get_block.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(i32)]
     lib.nc_step.argtypes = [vp, i32]
     lib.nc_set_graph.argtypes = [vp, i32]
     lib.nc_run_phases.argtypes = [vp, i32]
@@ -88,8 +90,8 @@ def load_library(path: str = LIB_PATH):
     lib.nc_destroy.argtypes = [vp]
     lib.nc_destroy.restype = None
     for f in ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_state_async", "nc_join_copies",
-              "nc_upload_state_device", "nc_download_state_device", "nc_check_finite",
-              "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_stream", "nc_profile"):
+              "nc_upload_state_device", "nc_download_state_device", "nc_check_finite", "nc_set_block",
+              "nc_get_block", "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_stream", "nc_profile"):
         getattr(lib, f).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -244,8 +246,13 @@ def setup_table(geo: dict) -> dict:
         t["PRE00"] = np.asarray(float(_scalar(geo["PRE00"])), np.float64)
     t["pntmask"] = np.ascontiguousarray(geo["pntmask"], np.int32)
     t["have_sgp"] = np.ascontiguousarray(geo["have_sgp"], np.bool_)
-    plan = halo.compose(geo["copy_r2r"], geo["copy_p2r"], geo["copy_r2p"], geo["copy_sgp"],
-                        int(_scalar(geo["gall_1d"])), int(_scalar(geo["lall"])))
+    if "halo_plan" in geo:   # composed elsewhere (ensemble.stack_setup: members stacked along the regions)
+        plan = geo["halo_plan"]
+    else:
+        plan = halo.compose(geo["copy_r2r"], geo["copy_p2r"], geo["copy_r2p"], geo["copy_sgp"],
+                            int(_scalar(geo["gall_1d"])), int(_scalar(geo["lall"])))
+    if "members" in geo:
+        t["members"] = np.asarray(int(_scalar(geo["members"])), np.int64)
     for k, v in zip(("halo_r_dst", "halo_r_src", "halo_p_dst", "halo_p_src"), plan):
         t[k] = np.ascontiguousarray(v, np.int64)
     return t
@@ -345,6 +352,15 @@ class NicamCuda:
                     or not t.is_contiguous()):
                 raise ValueError(f"expected a contiguous float64 CUDA tensor of shape {shp}, got "
                                  f"{t.dtype} {tuple(t.shape)} on {t.device}")
+
+    def set_block(self, kernel: str, threads: int):
+        """threads per block of a column / point kernel (nc_set_block)"""
+        _check(self._lib.nc_set_block(self._h, kernel.encode(), int(threads)))
+
+    def get_block(self, kernel: str) -> int:
+        t = ctypes.c_int32(0)
+        _check(self._lib.nc_get_block(self._h, kernel.encode(), ctypes.byref(t)))
+        return int(t.value)
 
     def check_finite(self):
         """raise NonFiniteStateError if the device state holds a NaN or an
