@@ -13,8 +13,14 @@ test_icogrid.py); the first tracer slot is the water-vapour slot, zero.
 Checked in both forms, the float64 one and the mixed one (float32 tracer
 arithmetic, float64 mass sums):
 
-* tracer mass conserved over the period: 1e-13 relative (float64), 1e-7
-  (mixed);
+* tracer mass conserved over the period.  The scheme's fluxes conserve mass
+  to round-off; the one exception is the reference's own clamp of tiny
+  negative rhogq values to zero at the end of the tracer step
+  (nhm/dynamics/mod_src_tracer.py:1186-1203), which adds mass.  Measured on
+  B200 with this case over the period in float64: every tracer within 1.4e-15
+  with the clamp compiled out (a probe copy, not this library); with it, 14
+  tracers within 2e-15 and the two deepest Gaussian hills +5.8e-14 and
+  +7.4e-13.  Bounds: float64 median 1e-14 and every tracer 1e-12; mixed 1e-7;
 * positivity and monotonicity: every mixing ratio stays within the initial
   range of its tracer (the Thuburn limiters' guarantee), up to 1e-12 (float64)
   and 1e-6 (mixed) of that range;
@@ -101,12 +107,12 @@ def period(pkg):
     return out
 
 
-@pytest.mark.parametrize("prec,tol", [("float64", 1e-13), ("mixed", 1e-7)])
-def test_tracer_mass_conserved_over_a_period(period, prec, tol):
+@pytest.mark.parametrize("prec,median_tol,tol", [("float64", 1e-14, 1e-12), ("mixed", 1e-7, 1e-7)])
+def test_tracer_mass_conserved_over_a_period(period, prec, median_tol, tol):
     r = period[prec]
     drift = np.abs(r["mass1"][2:] - r["mass0"][2:]) / np.abs(r["mass0"][2:])
     print(prec, "tracer mass drift over", period["nsteps"], "steps:", drift)
-    assert drift.max() <= tol, drift
+    assert np.median(drift) <= median_tol and drift.max() <= tol, drift
 
 
 @pytest.mark.parametrize("prec,tol", [("float64", 1e-12), ("mixed", 1e-6)])
