@@ -306,6 +306,88 @@ int nc_history_vars(nc_handle* h, const int32_t* items, int32_t nitems, int64_t 
  * y NULL, b finite and nonzero; else NC_ERR_ARG. */
 int nc_divide_known(const double* x, const double* y, double* q, int64_t n, double b);
 
+/* Tangent-linear and adjoint operators of the step, for differentiation
+ * (the reference differentiates its jax backend with jax.vjp; these are the
+ * hand-written counterparts of the operators named below).  They work on
+ * caller device buffers in the handle's device layout -- regional fields
+ * [l][k][j][i] of lall*kall*gall_1d^2 doubles, pole fields [g][k][lp] of
+ * 6*kall*2 doubles -- take the run constants, geometry and halo plan from
+ * the handle, are ordered after the work queued on the caller's `stream`
+ * (cudaStream_t, NULL the legacy default stream) and before what the caller
+ * queues there next.  Float64 handles with kall <= 64 only (NC_ERR_STATE for
+ * a mixed handle, NC_ERR_ARG above 64 levels).
+ *
+ * nc_vsolve: the HEVI vertical implicit system of kernels/virhowsolver.py:
+ * 67-122 per column (pole = 0: the regional columns, buffers regional;
+ * pole = 1: the pole columns, buffers pole): rows n = kmin+1..kmax of
+ * Ml[n] x[n-1] + Mc[n] x[n] + Mu[n] x[n+1] = b[n] solved by the Thomas
+ * algorithm, x zero on the other levels.  transpose = 1 solves with the
+ * transposed matrix (the adjoint: b is the cotangent of x, x receives the
+ * cotangent of b); with x_fwd (the forward solution) it also writes the
+ * matrix cotangents gMc[n] = -x[n] x_fwd[n], gMu[n] = -x[n] x_fwd[n+1],
+ * gMl[n] = -x[n] x_fwd[n-1] (zero outside the system).
+ *
+ * nc_vadv_lin: one vertical tracer advection step with the vertical Thuburn
+ * limiter (mod_src_tracer.py:389-533 and 1909-2074) at the tracer mass
+ * rhogq, for fixed density den, vertical mass flux flx_v, density tendency
+ * frhog (the limiter's d = bcoef * frhog / den * dt) and the clamp of tiny
+ * negatives (clamp != 0).  mode 0 writes the step's result F(rhogq) to out;
+ * mode 1 the tangent-linear dF(in); mode 2 the adjoint dF^T(in).  The
+ * limiter's branches are those taken at rhogq (the active-branch
+ * linearisation).  The halo and ghost levels of out are zero in modes 0/1.
+ *
+ * nc_laplacian: y = L(C(q)), the halo exchange C of the handle's plan
+ * followed by the hexagonal Laplacian of kernels/oprtlaplacian.py:41-70 on
+ * the interior cells and the pole points (other cells of y zero);
+ * transpose = 1 writes y = C^T L^T q, the adjoint, with the exchange's
+ * adjoint adding each halo value into its source cell (atomically: the
+ * order of those additions, and so the last bits, may vary between calls).
+ * q and y must not alias.  The forward form allocates one scratch copy of
+ * a field in the handle on its first call. */
+int nc_vsolve(nc_handle* h, int32_t pole, int32_t transpose, const double* Mc, const double* Mu, const double* Ml,
+              const double* b, double* x, const double* x_fwd, double* gMc, double* gMu, double* gMl,
+              void* stream);
+int nc_vadv_lin(nc_handle* h, int32_t pole, int32_t mode, const double* rhogq, const double* den,
+                const double* flx_v, const double* frhog, const double* in, double* out, double dt, double bcoef,
+                int32_t clamp, void* stream);
+int nc_laplacian(nc_handle* h, int32_t transpose, const double* q, const double* q_pl, double* y, double* y_pl,
+                 void* stream);
+
+/* nc_trc_step_lin: the tracer advection of one step (mod_src_tracer.py:
+ * 83-1228 as the step runs it: vertical step, horizontal step with the
+ * MIURA2004 face values and the horizontal Thuburn limiter of 2190-2605,
+ * the density update, vertical step with the clamp, then the closing halo
+ * exchange of PRG_var, mod_dynamics.py:2726) for one tracer mass x0 with the
+ * winds, densities and density tendency of the last step this handle ran
+ * (PROG_mean, PROG at the step's start and frhog as that step left them;
+ * NC_ERR_STATE if no step has run).  mode 0 writes the step's tracer mass
+ * T(x0) -- equal, bit for bit, to what the step made of that tracer; mode 1
+ * the tangent-linear dT(x0) in; mode 2 the adjoint dT(x0)^T in.  Every min /
+ * max of both limiters is linearised on the branch the forward takes at x0
+ * (the active-branch linearisation).  Device-layout buffers as above
+ * (regional x0, in, out; pole x0_pl, in_pl, out_pl).  The forward stages are
+ * recomputed in every call (they are not kept between calls); the first call
+ * allocates sixteen float64 work fields in the handle.  The adjoint
+ * accumulates with atomic additions, so its last bits may vary between
+ * calls. */
+int nc_trc_step_lin(nc_handle* h, int32_t mode, const double* x0, const double* x0_pl, const double* in,
+                    const double* in_pl, double* out, double* out_pl, void* stream);
+
+/* The model time of an offline-advection handle's prescribed winds
+ * (setup entry "trcadv"; it starts at 0 and every step adds dtl).  Re-running
+ * steps from stored states (as the tracer-transport adjoint does) needs the
+ * time of each state set back.  NC_ERR_STATE for a handle without
+ * prescribed winds; synchronous. */
+int nc_set_time(nc_handle* h, double time);
+
+/* For an offline-advection handle: puts the winds of the uploaded state on
+ * the handle as its step's tracer advection reads them (PROG_mean = PROG,
+ * PROG at the step's start = PROG, no density tendency; mod_dynamics.py:
+ * 2030-2085) without running the step, so that nc_trc_step_lin linearises
+ * the step from that state.  NC_ERR_STATE without prescribed winds or
+ * without a state. */
+int nc_trc_prepare(nc_handle* h);
+
 const char* nc_last_error(void);
 
 void nc_destroy(nc_handle* h);

@@ -1,0 +1,367 @@
+"""Differentiation of step operators through PyTorch autograd.
+
+Each operator is a ``torch.autograd.Function`` whose forward, tangent-linear
+(``jvp``, forward-mode AD) and adjoint (``backward``, reverse-mode AD) are the
+library's hand-written float64 kernels (``nc_vsolve``, ``nc_vadv_lin``,
+``nc_laplacian``), on CUDA tensors in the handle's device layout: regional
+fields of shape (lall, kall, gall_1d, gall_1d), pole fields (6, kall, 2).
+
+* ``VerticalSolve`` -- the HEVI tridiagonal system of
+  kernels/virhowsolver.py:67-122; the adjoint is the transposed solve plus
+  the matrix cotangents, differentiable in the matrix and the right-hand side.
+* ``VerticalAdvection`` -- one vertical tracer advection step with the
+  vertical Thuburn limiter (mod_src_tracer.py:389-533, 1909-2074),
+  differentiable in the tracer mass; the limiter's branches are those of the
+  forward evaluation (active-branch linearisation); density, vertical mass
+  flux and density tendency are held fixed (passing one that requires a
+  gradient is an error).
+* ``Laplacian`` -- halo exchange then the hexagonal Laplacian
+  (kernels/oprtlaplacian.py:41-70), linear; the adjoint runs the transposed
+  stencil and adds each halo value back into its exchange source.
+
+* ``TracerStep`` -- the whole tracer advection of a step
+  (mod_src_tracer.py:83-1228: vertical step, horizontal step with the
+  horizontal Thuburn limiter of 2190-2605, vertical step with the clamp, the
+  closing exchange) for the winds and densities of the handle's last step,
+  differentiable in the tracer mass (``nc_trc_step_lin``).
+
+``ColumnTransport`` chains the operators into a multi-step tracer model
+(vertical advection with the limiter, then horizontal diffusion by the
+Laplacian) whose steps can be checkpointed with ``torch.utils.checkpoint``.
+
+``TracerTransport`` differentiates a run of the handle's own steps with
+respect to the initial tracer masses of all tracers (the winds do not depend
+on the tracers: the offline advection, or passive tracers): the forward pass
+stores the full state every ``checkpoint_every`` steps; the backward pass
+re-runs each segment from its stored state, keeping the segment's per-step
+states, and walks back through it, re-running each step to put its winds and
+densities on the handle before applying the step's adjoint.
+
+The reference obtains gradients with jax.vjp of its jax backend; jax is not
+part of this build's environment, so the checks here are the dot-product
+test (tangent-linear against adjoint) and central finite differences.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+import torch.utils.checkpoint
+
+from .runtime import _scalar
+
+
+def to_device_layout(field, device="cuda"):
+    """(gall_1d, gall_1d, kall, lall) array -> (lall, kall, gall_1d, gall_1d) tensor"""
+    t = torch.as_tensor(np.asarray(field, np.float64) if not torch.is_tensor(field) else field)
+    return t.permute(3, 2, 1, 0).contiguous().to(device)
+
+
+def from_device_layout(t):
+    """inverse of ``to_device_layout`` (returns a numpy array)"""
+    return t.detach().permute(3, 2, 1, 0).contiguous().cpu().numpy()
+
+
+def _c(t):
+    return t.contiguous()
+
+
+def _fixed(name, *ts):
+    for t in ts:
+        if t is not None and t.requires_grad:
+            raise ValueError(f"{name}: density, fluxes and tendencies are held fixed; detach them")
+
+
+class VerticalSolve(torch.autograd.Function):
+    """x = M^-1 b per column, M tridiagonal (Mc, Mu, Ml)"""
+
+    @staticmethod
+    def forward(ctx, core, pole, Mc, Mu, Ml, b):
+        Mc, Mu, Ml, b = _c(Mc), _c(Mu), _c(Ml), _c(b)
+        x = torch.empty_like(b)
+        core.vsolve(Mc, Mu, Ml, b, x, pole=pole)
+        ctx.core, ctx.pole = core, pole
+        ctx.save_for_backward(Mc, Mu, Ml, x)
+        ctx.save_for_forward(Mc, Mu, Ml, x)
+        return x
+
+    @staticmethod
+    def backward(ctx, gx):
+        Mc, Mu, Ml, x = ctx.saved_tensors
+        gb = torch.empty_like(x)
+        gM = tuple(torch.empty_like(x) for _ in range(3))
+        ctx.core.vsolve(Mc, Mu, Ml, _c(gx), gb, pole=ctx.pole, transpose=True, x_fwd=x, gM=gM)
+        return None, None, gM[0], gM[1], gM[2], gb
+
+    @staticmethod
+    def jvp(ctx, _core, _pole, dMc, dMu, dMl, db):
+        # dx = M^-1 (db - dM x) on the system rows kmin+1..kmax
+        Mc, Mu, Ml, x = ctx.saved_tensors
+        k0, k1 = ctx.core.kmin + 1, ctx.core.kmax
+        r = torch.zeros_like(x) if db is None else db.clone()
+        rs = r[:, k0:k1 + 1]
+        if dMc is not None:
+            rs -= dMc[:, k0:k1 + 1] * x[:, k0:k1 + 1]
+        if dMu is not None:
+            rs[:, :-1] -= dMu[:, k0:k1] * x[:, k0 + 1:k1 + 1]
+        if dMl is not None:
+            rs[:, 1:] -= dMl[:, k0 + 1:k1 + 1] * x[:, k0:k1]
+        dx = torch.empty_like(x)
+        ctx.core.vsolve(Mc, Mu, Ml, _c(r), dx, pole=ctx.pole)
+        return dx
+
+
+class VerticalAdvection(torch.autograd.Function):
+    """one vertical tracer advection step of rhogq (den, flx_v, frhog fixed)"""
+
+    @staticmethod
+    def forward(ctx, core, pole, rhogq, den, flx_v, frhog, dt, bcoef, clamp):
+        _fixed("VerticalAdvection", den, flx_v, frhog)
+        rhogq, den, flx_v, frhog = _c(rhogq), _c(den), _c(flx_v), _c(frhog)
+        out = torch.empty_like(rhogq)
+        core.vadv_lin(0, rhogq, den, flx_v, frhog, None, out, dt, bcoef, clamp, pole)
+        ctx.core, ctx.args = core, (pole, dt, bcoef, clamp)
+        ctx.save_for_backward(rhogq, den, flx_v, frhog)
+        ctx.save_for_forward(rhogq, den, flx_v, frhog)
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        rhogq, den, flx_v, frhog = ctx.saved_tensors
+        pole, dt, bcoef, clamp = ctx.args
+        gq = torch.empty_like(rhogq)
+        ctx.core.vadv_lin(2, rhogq, den, flx_v, frhog, _c(g), gq, dt, bcoef, clamp, pole)
+        return None, None, gq, None, None, None, None, None, None
+
+    @staticmethod
+    def jvp(ctx, _core, _pole, drhogq, *_rest):
+        rhogq, den, flx_v, frhog = ctx.saved_tensors
+        pole, dt, bcoef, clamp = ctx.args
+        out = torch.empty_like(rhogq)
+        if drhogq is None:
+            return out.zero_()
+        ctx.core.vadv_lin(1, rhogq, den, flx_v, frhog, _c(drhogq), out, dt, bcoef, clamp, pole)
+        return out
+
+
+class Laplacian(torch.autograd.Function):
+    """(y, y_pl) = L(C(q, q_pl)): halo exchange then the hexagonal Laplacian"""
+
+    @staticmethod
+    def forward(ctx, core, q, q_pl):
+        y, y_pl = torch.empty_like(q), torch.empty_like(q_pl)
+        core.laplacian(_c(q), _c(q_pl), y, y_pl)
+        ctx.core = core
+        return y, y_pl
+
+    @staticmethod
+    def backward(ctx, gy, gy_pl):
+        core = ctx.core
+        gy = torch.zeros(core.field_shape, dtype=torch.float64, device="cuda") if gy is None else _c(gy)
+        gy_pl = torch.zeros(core.field_shape_pl, dtype=torch.float64, device=gy.device) if gy_pl is None else _c(gy_pl)
+        g, g_pl = torch.empty_like(gy), torch.empty_like(gy_pl)
+        core.laplacian(gy, gy_pl, g, g_pl, transpose=True)
+        return None, g, g_pl
+
+    @staticmethod
+    def jvp(ctx, _core, dq, dq_pl):
+        core = ctx.core
+        dq = torch.zeros(core.field_shape, dtype=torch.float64, device="cuda") if dq is None else _c(dq)
+        dq_pl = torch.zeros(core.field_shape_pl, dtype=torch.float64, device=dq.device) if dq_pl is None else _c(dq_pl)
+        y, y_pl = torch.empty_like(dq), torch.empty_like(dq_pl)
+        core.laplacian(dq, dq_pl, y, y_pl)
+        return y, y_pl
+
+
+class TracerStep(torch.autograd.Function):
+    """(y, y_pl) = T(x, x_pl): one tracer advection step with the winds and
+    densities of the handle's last step (they must still be the ones the
+    forward used when the backward runs)"""
+
+    @staticmethod
+    def forward(ctx, core, x, x_pl):
+        x, x_pl = _c(x), _c(x_pl)
+        y, y_pl = torch.empty_like(x), torch.empty_like(x_pl)
+        core.trc_step_lin(0, x, x_pl, None, None, y, y_pl)
+        ctx.core = core
+        ctx.save_for_backward(x, x_pl)
+        ctx.save_for_forward(x, x_pl)
+        return y, y_pl
+
+    @staticmethod
+    def backward(ctx, gy, gy_pl):
+        x, x_pl = ctx.saved_tensors
+        gy = torch.zeros_like(x) if gy is None else _c(gy)
+        gy_pl = torch.zeros_like(x_pl) if gy_pl is None else _c(gy_pl)
+        g, g_pl = torch.empty_like(x), torch.empty_like(x_pl)
+        ctx.core.trc_step_lin(2, x, x_pl, gy, gy_pl, g, g_pl)
+        return None, g, g_pl
+
+    @staticmethod
+    def jvp(ctx, _core, dx, dx_pl):
+        x, x_pl = ctx.saved_tensors
+        dx = torch.zeros_like(x) if dx is None else _c(dx)
+        dx_pl = torch.zeros_like(x_pl) if dx_pl is None else _c(dx_pl)
+        y, y_pl = torch.empty_like(x), torch.empty_like(x_pl)
+        ctx.core.trc_step_lin(1, x, x_pl, dx, dx_pl, y, y_pl)
+        return y, y_pl
+
+
+def tracer_step(core, x, x_pl):
+    return TracerStep.apply(core, x, x_pl)
+
+
+def _tracers(prg, prg_pl, nq):
+    """device-layout tracer masses (nq, lall, kall, g, g) / (nq, 6, kall, LP)
+    of a reference-layout state tensor"""
+    x = prg[..., 6:6 + nq].permute(4, 3, 2, 1, 0).contiguous()
+    x_pl = prg_pl[..., 6:6 + nq].permute(3, 0, 1, 2).contiguous()
+    return x, x_pl
+
+
+def _with_tracers(prg, prg_pl, x, x_pl):
+    s, sp = prg.clone(), prg_pl.clone()
+    nq = x.shape[0]
+    s[..., 6:6 + nq] = x.permute(4, 3, 2, 1, 0)
+    sp[..., 6:6 + nq] = x_pl.permute(1, 2, 3, 0)
+    return s.contiguous(), sp.contiguous()
+
+
+class _TracerRun(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, model, nsteps, x, x_pl):
+        core = model.core
+        s, sp = _with_tracers(model.prg, model.prg_pl, x.detach(), x_pl.detach())
+        model.clock(0)
+        core.upload_tensor(s, sp)
+        stored = {}
+        for n in range(nsteps):
+            if n % model.every == 0:
+                stored[n] = core.download_tensor()
+            core.step(1)
+        y, y_pl = _tracers(*core.download_tensor(), x.shape[0])
+        ctx.model, ctx.nsteps, ctx.stored = model, nsteps, stored
+        return y, y_pl
+
+    @staticmethod
+    def backward(ctx, gy, gy_pl):
+        model, core, nq = ctx.model, ctx.model.core, ctx.model.nq
+        g = torch.zeros((nq,) + core.field_shape, dtype=torch.float64, device="cuda") if gy is None else gy.clone()
+        g_pl = (torch.zeros((nq,) + core.field_shape_pl, dtype=torch.float64, device="cuda") if gy_pl is None
+                else gy_pl.clone())
+        out, out_pl = torch.empty_like(g[0]), torch.empty_like(g_pl[0])
+        starts = sorted(ctx.stored)
+        for seg, n0 in reversed(list(enumerate(starts))):
+            n1 = starts[seg + 1] if seg + 1 < len(starts) else ctx.nsteps
+            states = [ctx.stored[n0]]                      # the segment's per-step states, re-run
+            model.clock(n0)
+            core.upload_tensor(*states[0])
+            for _ in range(n0, n1 - 1):
+                core.step(1)
+                states.append(core.download_tensor())
+            for m, (s, sp) in reversed(list(enumerate(states))):
+                model.clock(n0 + m)
+                core.upload_tensor(s, sp)
+                model.coefficients()                       # the step's winds and densities onto the handle
+                x, x_pl = _tracers(s, sp, nq)
+                for iq in range(nq):
+                    core.trc_step_lin(2, x[iq], x_pl[iq], g[iq], g_pl[iq], out, out_pl)
+                    g[iq].copy_(out)
+                    g_pl[iq].copy_(out_pl)
+            del states
+        return None, None, g, g_pl
+
+
+class TracerTransport:
+    """Runs of the handle's own steps from the state (prg, prg_pl) (device
+    tensors, reference layout) as a differentiable function of the initial
+    tracer masses of its nq tracers: ``run(x, x_pl, nsteps)`` with x of shape
+    (nq, lall, kall, gall_1d, gall_1d) and x_pl (nq, 6, kall, LP) returns the
+    tracer masses after nsteps steps, the full state stored every
+    ``checkpoint_every`` steps for the backward pass"""
+
+    def __init__(self, core, prg, prg_pl, checkpoint_every: int = 1, time0: float = 0.0):
+        self.core, self.prg, self.prg_pl = core, prg, prg_pl
+        self.nq = prg.shape[-1] - 6
+        self.every = max(1, int(checkpoint_every))
+        self.time0 = float(time0)
+
+    def coefficients(self):
+        """the winds and densities of the step from the uploaded state onto
+        the handle: the offline advection reads them straight from the state
+        (nc_trc_prepare); otherwise the step is re-run"""
+        if self.core.trcadv:
+            self.core.trc_prepare()
+        else:
+            self.core.step(1)
+
+    def directional(self, x, x_pl, d, d_pl, nsteps: int):
+        """the run and its tangent-linear along (d, d_pl): the tracer masses
+        after nsteps steps and their derivative along the direction, each
+        step's tangent-linear applied while the step's winds are on the
+        handle"""
+        core = self.core
+        s, sp = _with_tracers(self.prg, self.prg_pl, x, x_pl)
+        self.clock(0)
+        core.upload_tensor(s, sp)
+        d, d_pl = d.clone(), d_pl.clone()
+        out, out_pl = torch.empty_like(d[0]), torch.empty_like(d_pl[0])
+        for _ in range(nsteps):
+            xs, xs_pl = _tracers(*core.download_tensor(), self.nq)
+            core.step(1)
+            for iq in range(self.nq):
+                core.trc_step_lin(1, xs[iq], xs_pl[iq], d[iq], d_pl[iq], out, out_pl)
+                d[iq].copy_(out)
+                d_pl[iq].copy_(out_pl)
+        y, y_pl = _tracers(*core.download_tensor(), self.nq)
+        return (y, y_pl), (d, d_pl)
+
+    def clock(self, n: int):
+        """an offline-advection handle's prescribed-wind time at step n"""
+        if self.core.trcadv:
+            self.core.set_time(self.time0 + n * float(_scalar(self.core._tab["dtl"])))
+
+    def initial_tracers(self):
+        return _tracers(self.prg, self.prg_pl, self.nq)
+
+    def run(self, x, x_pl, nsteps: int):
+        return _TracerRun.apply(self, nsteps, x, x_pl)
+
+
+def vertical_solve(core, Mc, Mu, Ml, b, pole=False):
+    return VerticalSolve.apply(core, pole, Mc, Mu, Ml, b)
+
+
+def vertical_advection(core, rhogq, den, flx_v, frhog, dt, bcoef=0.0, clamp=True, pole=False):
+    return VerticalAdvection.apply(core, pole, rhogq, den, flx_v, frhog, dt, bcoef, clamp)
+
+
+def laplacian(core, q, q_pl):
+    return Laplacian.apply(core, q, q_pl)
+
+
+class ColumnTransport:
+    """A tracer model built from the differentiable operators: each step is
+    one vertical advection step (limiter, clamp) of the regional and pole
+    columns, then horizontal diffusion rhogq += kappa * L(C(rhogq)).
+
+    ``fields``: dict of device-layout tensors den, flx_v, frhog and their
+    ``_pl`` pole counterparts (held fixed); ``dt`` the advection step."""
+
+    def __init__(self, core, fields: dict, dt: float, kappa: float, clamp: bool = True):
+        self.core, self.f, self.dt, self.kappa, self.clamp = core, fields, dt, kappa, clamp
+
+    def step(self, q, q_pl):
+        f, c = self.f, self.core
+        q = vertical_advection(c, q, f["den"], f["flx_v"], f["frhog"], self.dt, 0.0, self.clamp)
+        q_pl = vertical_advection(c, q_pl, f["den_pl"], f["flx_v_pl"], f["frhog_pl"], self.dt, 0.0, self.clamp,
+                                  pole=True)
+        y, y_pl = laplacian(c, q, q_pl)
+        return q + self.kappa * y, q_pl + self.kappa * y_pl
+
+    def run(self, q, q_pl, nsteps: int, checkpoint: bool = False):
+        for _ in range(nsteps):
+            if checkpoint:
+                q, q_pl = torch.utils.checkpoint.checkpoint(self.step, q, q_pl, use_reentrant=False)
+            else:
+                q, q_pl = self.step(q, q_pl)
+        return q, q_pl

@@ -1,0 +1,758 @@
+// Tangent-linear and adjoint kernels of step operators (float64), for the
+// differentiable path behind torch.autograd.Function (adjoint.py):
+//
+// * the HEVI vertical implicit solve (kernels/virhowsolver.py:67-122): per
+//   column the tridiagonal system Ml x[n-1] + Mc x[n] + Mu x[n+1] = b[n] on the
+//   levels kmin+1..kmax, solved by the Thomas algorithm; its adjoint is the
+//   solve with the transposed matrix (sub-diagonal Mu[n-1], super-diagonal
+//   Ml[n+1]);
+// * one vertical tracer advection step with the vertical Thuburn limiter
+//   (mod_src_tracer.py:389-533, 1909-2074; the forward arithmetic is that of
+//   trc_vadv_column): the tangent-linear and adjoint of the step at a given
+//   tracer state, with the limiter's branches (upwind side, min / max
+//   choices, the final clamp of tiny negatives) those of the forward
+//   evaluation -- the active-branch linearisation; the density, fluxes and
+//   Courant numbers are fixed inputs;
+// * the horizontal Laplacian (kernels/oprtlaplacian.py:41-55, the pole row
+//   :143-157) after the halo exchange: y = L(C(q)) on interior cells and the
+//   pole points; the adjoint C^T L^T, with the exchange's adjoint adding each
+//   halo value back into its source cell.
+#pragma once
+#include "nc_tracer.cuh"
+
+namespace nc {
+
+// levels held per thread by the column kernels below (local arrays); the
+// entry points refuse grids with more
+#define NC_ADJ_K 64
+
+// ---------------------------------------------------------------------------
+// tridiagonal solve and its transpose, one thread per regional column
+// ---------------------------------------------------------------------------
+struct TriArgs {
+  const double *Mc, *Mu, *Ml, *b;
+  double* x;
+  // with the transposed solve: the forward solution and the cotangents of the
+  // matrix entries (-lambda[n] x[n], -lambda[n] x[n+1], -lambda[n] x[n-1]),
+  // written when x_fwd is not null
+  const double* x_fwd;
+  double *gMc, *gMu, *gMl;
+  int transpose;
+};
+
+__device__ void tri_column(const Col c, const TriArgs& a) {
+  const int k0 = cD.kmin + 1, N = cD.kmax - cD.kmin, KA = cD.KA;
+  // row n: lo(n) x[n-1] + Mc[n] x[n] + up(n) x[n+1] = b[n]
+  auto lo = [&](int n) { return a.transpose ? a.Mu[c.at(k0 + n - 1)] : a.Ml[c.at(k0 + n)]; };
+  auto up = [&](int n) { return a.transpose ? a.Ml[c.at(k0 + n + 1)] : a.Mu[c.at(k0 + n)]; };
+  double u[NC_ADJ_K], gam[NC_ADJ_K];
+  double beta = a.Mc[c.at(k0)];
+  u[0] = a.b[c.at(k0)] / beta;
+  for (int n = 1; n < N; ++n) {
+    gam[n] = up(n - 1) / beta;
+    beta = a.Mc[c.at(k0 + n)] - lo(n) * gam[n];
+    u[n] = (a.b[c.at(k0 + n)] - lo(n) * u[n - 1]) / beta;
+  }
+  for (int n = N - 2; n >= 0; --n) u[n] = u[n] - gam[n + 1] * u[n + 1];
+  for (int k = 0; k < KA; ++k) a.x[c.at(k)] = (k >= k0 && k < k0 + N) ? u[k - k0] : 0.0;
+  if (!a.x_fwd) return;
+  for (int k = 0; k < KA; ++k) {
+    const int n = k - k0;
+    double gc = 0.0, gu = 0.0, gl = 0.0;
+    if (n >= 0 && n < N) {
+      gc = -u[n] * a.x_fwd[c.at(k)];
+      if (n + 1 < N) gu = -u[n] * a.x_fwd[c.at(k + 1)];
+      if (n > 0) gl = -u[n] * a.x_fwd[c.at(k - 1)];
+    }
+    a.gMc[c.at(k)] = gc;
+    a.gMu[c.at(k)] = gu;
+    a.gMl[c.at(k)] = gl;
+  }
+}
+
+__global__ void k_tri_solve(TriArgs a, int pole) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  int i, j, l, g, lp;
+  if (!map_col(pole, t, i, j, l, g, lp)) return;
+  tri_column(pole ? col_pl(g, lp) : col_reg(i, j, l), a);
+}
+
+// ---------------------------------------------------------------------------
+// vertical tracer advection step: forward, tangent-linear, adjoint
+// ---------------------------------------------------------------------------
+struct VadvLin {
+  const double *rhogq, *den, *flx_v, *frhog;   // linearisation point and the fixed inputs
+  const double* in;                            // TL: perturbation of rhogq; AD: adjoint of the output
+  double* out;                                 // forward: F(rhogq); TL: perturbation of F; AD: adjoint of rhogq
+  double dt, bcoef;
+  int clamp, mode;                             // mode 0 forward, 1 tangent-linear, 2 adjoint
+};
+
+// the argument npmin / npmax return (0 the first, 1 the second; on ties the
+// second, as they do): the linearisation follows the forward's choice
+__device__ __forceinline__ int amin2(double a, double b) { return (a < b) ? 0 : 1; }
+__device__ __forceinline__ int amax2(double a, double b) { return (a > b) ? 0 : 1; }
+
+__device__ void vadv_lin_column(const Col c, const VadvLin& a) {
+  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax;
+  const double BIG = cC.HUGE_, EPS = cC.EPS;
+  double q[NC_ADJ_K], raw[NC_ADJ_K], omin[NC_ADJ_K], omax[NC_ADJ_K];
+  double fk[NC_ADJ_K], zk[NC_ADJ_K], Ak[NC_ADJ_K], c1v[NC_ADJ_K], c2v[NC_ADJ_K];
+  // branch record per level: upwind sides; argument of the Q bounds (0 qc, 1 neighbour);
+  // qnmin / qnmax (0 QL, 1 QU, 2 qc); limited face (0 raw, 1 lower bound, 2 upper bound)
+  signed char inL[NC_ADJ_K], inU[NC_ADJ_K], sminL[NC_ADJ_K], sminU[NC_ADJ_K], smaxL[NC_ADJ_K], smaxU[NC_ADJ_K];
+  signed char snmin[NC_ADJ_K], snmax[NC_ADJ_K], sh[NC_ADJ_K];
+  bool clamped[NC_ADJ_K];
+  for (int k = 0; k < KA; ++k) q[k] = a.rhogq[c.at(k)] / a.den[c.at(k)];
+  for (int k = kmin; k <= kmax + 1; ++k) raw[k] = cC.afact[k] * q[k] + cC.bfact[k] * q[k - 1];
+  for (int k = kmin; k <= kmax; ++k) {
+    const int p = c.at(k);
+    const double denk = a.den[p];
+    const double ck0 = -a.flx_v[p] / denk * cC.rdgz[k];
+    const double ck1 = a.flx_v[c.at(k + 1)] / denk * cC.rdgz[k];
+    const double ck0p = (k + 1 <= kmax) ? -a.flx_v[c.at(k + 1)] / a.den[c.at(k + 1)] * cC.rdgz[k + 1] : 0.0;
+    const double L = 0.5 - copysign(0.5, ck0), U = 0.5 + copysign(0.5, ck0p);
+    inL[k] = (L == 1.0);
+    inU[k] = (U == 1.0);
+    const double qc = q[k], qb = q[k - 1], qa = q[k + 1];
+    sminL[k] = amin2(qc, qb); smaxL[k] = amax2(qc, qb);
+    sminU[k] = amin2(qc, qa); smaxU[k] = amax2(qc, qa);
+    const double QminL = inL[k] ? (sminL[k] ? qb : qc) : BIG, QmaxL = inL[k] ? (smaxL[k] ? qb : qc) : -BIG;
+    const double QminU = inU[k] ? (sminU[k] ? qa : qc) : BIG, QmaxU = inU[k] ? (smaxU[k] ? qa : qc) : -BIG;
+    const int s1 = amin2(QminL, QminU);
+    const double m1 = s1 ? QminU : QminL;
+    snmin[k] = amin2(m1, qc) ? 2 : s1;
+    const double qnmin = (snmin[k] == 2) ? qc : m1;
+    const int s2 = amax2(QmaxL, QmaxU);
+    const double x1 = s2 ? QmaxU : QmaxL;
+    snmax[k] = amax2(x1, qc) ? 2 : s2;
+    const double qnmax = (snmax[k] == 2) ? qc : x1;
+    const double Cin = L * ck0 + U * ck1, Cout = (1.0 - L) * ck0 + (1.0 - U) * ck1;
+    const double CQmin = L * ck0 * QminL + U * ck1 * QminU, CQmax = L * ck0 * QmaxL + U * ck1 * QmaxU;
+    const double zsw = 0.5 - copysign(0.5, fabs(Cout) - EPS);
+    const double dk = a.bcoef * a.frhog[p] / denk * a.dt;
+    const double A = Cin + Cout - dk;
+    omin[k] = ((qc - qnmax) + qnmax * A - CQmax) / (Cout + zsw) * (1.0 - zsw) + qc * zsw;
+    omax[k] = ((qc - qnmin) + qnmin * A - CQmin) / (Cout + zsw) * (1.0 - zsw) + qc * zsw;
+    fk[k] = (1.0 - zsw) / (Cout + zsw);
+    zk[k] = zsw;
+    Ak[k] = A;
+    c1v[k] = L * ck0;
+    c2v[k] = U * ck1;
+  }
+  // limited faces qh[k] on k = kmin+1..kmax, zero at kmin and kmax+1: the
+  // bounds of the upwind cell, k-1 when inflow comes from below (inL)
+  double qh[NC_ADJ_K];
+  for (int k = 0; k < KA; ++k) qh[k] = 0.0;
+  for (int k = kmin + 1; k <= kmax; ++k) {
+    const int jb = inL[k] ? k - 1 : k;
+    const double lo = omin[jb], hi = omax[jb];
+    const int s_lo = amax2(raw[k], lo);            // np.maximum(raw, lo)
+    const double mx = s_lo ? lo : raw[k];
+    const int s_hi = amin2(mx, hi);                // np.minimum(mx, hi)
+    sh[k] = s_hi ? 2 : (s_lo ? 1 : 0);
+    qh[k] = s_hi ? hi : mx;
+  }
+  for (int k = 0; k < KA; ++k) clamped[k] = false;
+  if (a.mode == 0) {
+    for (int k = 0; k < KA; ++k) a.out[c.at(k)] = 0.0;
+    for (int k = kmin; k <= kmax; ++k) {
+      double x = a.rhogq[c.at(k)] - (a.flx_v[c.at(k + 1)] * qh[k + 1] - a.flx_v[c.at(k)] * qh[k]) * cC.rdgz[k];
+      if (a.clamp && x > -1.0e-10 && x < 0.0) x = 0.0;
+      a.out[c.at(k)] = x;
+    }
+    return;
+  }
+  for (int k = kmin; k <= kmax; ++k) {
+    const double x = a.rhogq[c.at(k)] - (a.flx_v[c.at(k + 1)] * qh[k + 1] - a.flx_v[c.at(k)] * qh[k]) * cC.rdgz[k];
+    clamped[k] = a.clamp && x > -1.0e-10 && x < 0.0;
+  }
+  if (a.mode == 1) {
+    // tangent-linear: the same sequence on perturbations
+    double dq[NC_ADJ_K], draw[NC_ADJ_K], dmin[NC_ADJ_K], dmax[NC_ADJ_K], dqh[NC_ADJ_K];
+    for (int k = 0; k < KA; ++k) {
+      dq[k] = a.in[c.at(k)] / a.den[c.at(k)];
+      dqh[k] = 0.0;
+    }
+    for (int k = kmin; k <= kmax + 1; ++k) draw[k] = cC.afact[k] * dq[k] + cC.bfact[k] * dq[k - 1];
+    for (int k = kmin; k <= kmax; ++k) {
+      const double dc = dq[k];
+      const double dminL = inL[k] ? (sminL[k] ? dq[k - 1] : dc) : 0.0, dmaxL = inL[k] ? (smaxL[k] ? dq[k - 1] : dc) : 0.0;
+      const double dminU = inU[k] ? (sminU[k] ? dq[k + 1] : dc) : 0.0, dmaxU = inU[k] ? (smaxU[k] ? dq[k + 1] : dc) : 0.0;
+      const double dnmin = (snmin[k] == 2) ? dc : (snmin[k] == 1 ? dminU : dminL);
+      const double dnmax = (snmax[k] == 2) ? dc : (snmax[k] == 1 ? dmaxU : dmaxL);
+      const double dCQmin = c1v[k] * dminL + c2v[k] * dminU, dCQmax = c1v[k] * dmaxL + c2v[k] * dmaxU;
+      // qomin = f (qc - qnmax + A qnmax - CQmax) + zsw qc
+      dmin[k] = fk[k] * (dc + (Ak[k] - 1.0) * dnmax - dCQmax) + zk[k] * dc;
+      dmax[k] = fk[k] * (dc + (Ak[k] - 1.0) * dnmin - dCQmin) + zk[k] * dc;
+    }
+    for (int k = kmin + 1; k <= kmax; ++k) {
+      const int jb = inL[k] ? k - 1 : k;
+      dqh[k] = (sh[k] == 0) ? draw[k] : (sh[k] == 1 ? dmin[jb] : dmax[jb]);
+    }
+    for (int k = 0; k < KA; ++k) a.out[c.at(k)] = 0.0;
+    for (int k = kmin; k <= kmax; ++k) {
+      const double d = a.in[c.at(k)] - (a.flx_v[c.at(k + 1)] * dqh[k + 1] - a.flx_v[c.at(k)] * dqh[k]) * cC.rdgz[k];
+      a.out[c.at(k)] = clamped[k] ? 0.0 : d;
+    }
+    return;
+  }
+  // adjoint: the tangent-linear steps transposed, in reverse order
+  double gy[NC_ADJ_K], gqh[NC_ADJ_K], graw[NC_ADJ_K], gmin[NC_ADJ_K], gmax[NC_ADJ_K], gq[NC_ADJ_K], gr[NC_ADJ_K];
+  for (int k = 0; k < KA; ++k) {
+    gy[k] = (k >= kmin && k <= kmax && !clamped[k]) ? a.in[c.at(k)] : 0.0;
+    gqh[k] = graw[k] = gmin[k] = gmax[k] = gq[k] = gr[k] = 0.0;
+  }
+  for (int k = kmin; k <= kmax; ++k) {   // out_k = in_k - (flx_{k+1} qh_{k+1} - flx_k qh_k) rdgz_k
+    gr[k] += gy[k];
+    gqh[k + 1] -= a.flx_v[c.at(k + 1)] * cC.rdgz[k] * gy[k];
+    gqh[k] += a.flx_v[c.at(k)] * cC.rdgz[k] * gy[k];
+  }
+  for (int k = kmin + 1; k <= kmax; ++k) {
+    const int jb = inL[k] ? k - 1 : k;
+    if (sh[k] == 0) graw[k] += gqh[k];
+    else if (sh[k] == 1) gmin[jb] += gqh[k];
+    else gmax[jb] += gqh[k];
+  }
+  for (int k = kmin; k <= kmax; ++k) {
+    // dmin = (f + zsw) dc + f (A - 1) dnmax - f dCQmax, and the same for dmax with qnmin / CQmin
+    gq[k] += (fk[k] + zk[k]) * (gmin[k] + gmax[k]);
+    const double gnmax = fk[k] * (Ak[k] - 1.0) * gmin[k], gCQmax = -fk[k] * gmin[k];
+    const double gnmin = fk[k] * (Ak[k] - 1.0) * gmax[k], gCQmin = -fk[k] * gmax[k];
+    double gminL = c1v[k] * gCQmin, gminU = c2v[k] * gCQmin, gmaxL = c1v[k] * gCQmax, gmaxU = c2v[k] * gCQmax;
+    if (snmin[k] == 2) gq[k] += gnmin;
+    else if (snmin[k] == 1) gminU += gnmin;
+    else gminL += gnmin;
+    if (snmax[k] == 2) gq[k] += gnmax;
+    else if (snmax[k] == 1) gmaxU += gnmax;
+    else gmaxL += gnmax;
+    if (inL[k]) {
+      gq[sminL[k] ? k - 1 : k] += gminL;
+      gq[smaxL[k] ? k - 1 : k] += gmaxL;
+    }
+    if (inU[k]) {
+      gq[sminU[k] ? k + 1 : k] += gminU;
+      gq[smaxU[k] ? k + 1 : k] += gmaxU;
+    }
+  }
+  for (int k = kmin; k <= kmax + 1; ++k) {   // raw_k = afact_k q_k + bfact_k q_{k-1}
+    gq[k] += cC.afact[k] * graw[k];
+    gq[k - 1] += cC.bfact[k] * graw[k];
+  }
+  for (int k = 0; k < KA; ++k) a.out[c.at(k)] = gr[k] + gq[k] / a.den[c.at(k)];
+}
+
+__global__ void k_vadv_lin(VadvLin a, int pole) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  int i, j, l, g, lp;
+  if (!map_col(pole, t, i, j, l, g, lp)) return;
+  vadv_lin_column(pole ? col_pl(g, lp) : col_reg(i, j, l), a);
+}
+
+// ---------------------------------------------------------------------------
+// horizontal Laplacian and its adjoint (the exchange first / its adjoint last)
+// ---------------------------------------------------------------------------
+// y = L(q) on interior cells (halo cells 0); pole point row g = 0, neighbours 0
+__global__ void k_lap_fwd(const double* q, double* y) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.npti) return;
+  const int G = cD.G, KA = cD.KA;
+  const int i = t % G, j = (t / G) % G, k = (t / (G * G)) % KA, l = t / (G * G * KA);
+  double v = 0.0;
+  if (interior(i, j)) v = lap7<double>(i, j, k, l, [&](int ii, int jj, int kk) { return q[ix(ii, jj, kk, l)]; });
+  y[t] = v;
+}
+__global__ void k_lap_fwd_pl(const double* q, double* y) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.KA * cD.LP) return;
+  const int k = t / cD.LP, lp = t % cD.LP;
+  double row = 0.0;
+  for (int v = 0; v < 6; ++v) {
+    const double tv = cG.coef_lap_pl[v * cD.LP + lp] * q[ipl(v, k, lp)];
+    row = (v == 0) ? tv : row + tv;
+  }
+  y[ipl(0, k, lp)] = row;
+  for (int g = 1; g < 6; ++g) y[ipl(g, k, lp)] = 0.0;
+}
+// the transposed stencil: every cell gathers coef_lap[m](i) y(i) from the
+// interior cells i whose stencil point m it is
+__global__ void k_lap_adj(const double* y, double* g) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.npti) return;
+  const int G = cD.G, KA = cD.KA;
+  const int i = t % G, j = (t / G) % G, k = (t / (G * G)) % KA, l = t / (G * G * KA);
+  double s = 0.0;
+  for (int m = 0; m < 7; ++m) {
+    const int si = i - kNbI[m], sj = j - kNbJ[m];
+    if (si >= 0 && sj >= 0 && si < G && sj < G && interior(si, sj))
+      s += P2(cG.coef_lap, m, si, sj, l) * y[ix(si, sj, k, l)];
+  }
+  g[t] = s;
+}
+__global__ void k_lap_adj_pl(const double* y, double* g) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.KA * cD.LP) return;
+  const int k = t / cD.LP, lp = t % cD.LP;
+  const double y0 = y[ipl(0, k, lp)];
+  for (int v = 0; v < 6; ++v) g[ipl(v, k, lp)] = cG.coef_lap_pl[v * cD.LP + lp] * y0;
+}
+// adjoint of the halo exchange on one field: each destination's value is added
+// to its source (atomically: several destinations may share a source), then
+// the destinations are cleared by k_comm_adj_clear
+__global__ void k_comm_adj_add(double* r, double* p, const long long* r_dst, const long long* r_src, int nr,
+                               const long long* p_dst, const long long* p_src, int np) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nent = nr + np;
+  if (t >= (long long)nent * cD.KA) return;
+  const int k = (int)(t / nent), e = (int)(t % nent);
+  const long long pl = cD.plane;
+  auto reg_at = [&](long long cidx) { return ((cidx / pl) * cD.KA + k) * pl + cidx % pl; };
+  if (e < nr) {
+    const double v = r[reg_at(r_dst[e])];
+    const long long s = r_src[e];
+    if (s >= 0) atomicAdd(&r[reg_at(s)], v);
+    else {
+      const long long gp = -s - 1;
+      atomicAdd(&p[ipl((int)(gp / cD.LP), k, (int)(gp % cD.LP))], v);
+    }
+  } else {
+    const int ee = e - nr;
+    const long long gp = p_dst[ee];
+    const double v = p[ipl((int)(gp / cD.LP), k, (int)(gp % cD.LP))];
+    atomicAdd(&r[reg_at(p_src[ee])], v);
+  }
+}
+__global__ void k_comm_adj_clear(double* r, double* p, const long long* r_dst, int nr, const long long* p_dst,
+                                 int np) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nent = nr + np;
+  if (t >= (long long)nent * cD.KA) return;
+  const int k = (int)(t / nent), e = (int)(t % nent);
+  const long long pl = cD.plane;
+  if (e < nr) {
+    const long long d = r_dst[e];
+    r[((d / pl) * cD.KA + k) * pl + d % pl] = 0.0;
+  } else {
+    const long long gp = p_dst[e - nr];
+    p[ipl((int)(gp / cD.LP), k, (int)(gp % cD.LP))] = 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// horizontal tracer step (mod_src_tracer.py:758-916, 1634-1787, 2190-2605):
+// tangent-linear and adjoint at a forward evaluation.  The forward arrays q,
+// qa (face values), Qmin / Qmax (after their exchange) of that evaluation are
+// given; every min / max of the limiter is re-decided from them exactly as
+// the forward kernels decide it, and the linearised value follows the chosen
+// argument (a constant +-HUGE contributes nothing).
+// ---------------------------------------------------------------------------
+enum { SRC_NONE = 0, SRC_Q = 1, SRC_QA = 2, SRC_QMIN = 3, SRC_QMAX = 4 };
+struct Src {
+  int kind, idx, f;   // f: face of a SRC_QA source
+};
+
+struct HLin {
+  // forward evaluation
+  const double *q, *qa[3], *Qmin, *Qmax, *rhog_t, *frhog;
+  const double *ch[6], *cm[6], *flx[6], *xc[9];
+  // pole arrays: q, qa, Qmin / Qmax (g, k, lp); ch / cm / flx (g, k, lp); xc (g, k, lp, 3)
+  const double *q_pl, *qa_pl, *Qmin_pl, *Qmax_pl, *rhog_t_pl, *frhog_pl, *ch_pl, *cm_pl, *flx_pl, *xc_pl;
+  double dt;
+  // tangent-linear: inputs dq, dqa, dQmin / dQmax; outputs dQmin / dQmax (qout) or y (apply)
+  // adjoint: cotangents accumulated into gq, gqa, gQmin / gQmax
+  const double *dq, *dqa[3], *dQmin, *dQmax, *dq_pl, *dqa_pl, *dQmin_pl, *dQmax_pl;
+  double *oQmin, *oQmax, *oQmin_pl, *oQmax_pl;
+  const double *x, *x_pl;   // apply: the step's input perturbation (TL) / output cotangent (AD)
+  double *y, *y_pl;         // apply TL output
+  double *gq, *gqa[3], *gQmin, *gQmax, *gq_pl, *gqa_pl, *gQmin_pl, *gQmax_pl;
+  double *gg[3], *gg_pl[3];   // cotangents of the (exchanged) gradient
+  double *gx, *gx_pl;         // cotangent of the step's input, accumulated
+};
+
+// indices of the min / max over the stencil of edge f of cell (a, b)
+// (trc_face_minmax: npmin / npmax chains in the same order)
+__device__ void face_minmax_idx(const double* q, int a, int b, int k, int l, int f, int& imin, int& imax) {
+  auto I = [&](int ii, int jj) { return ix(ii, jj, k, l); };
+  const int i0 = I(a, b), i2 = I(a + 1, b), i3 = I(a + 1, b + 1), ij = I(a, b + 1);
+  int v[3];
+  if (f == 0) {
+    v[0] = (b > 0) ? I(a, b - 1) : I(0, 0); v[1] = i2; v[2] = i3;
+  } else if (f == 1) {
+    v[0] = i2; v[1] = i3; v[2] = ij;
+  } else {
+    v[0] = i3; v[1] = ij; v[2] = (a > 0) ? I(a - 1, b) : I(0, 0);
+  }
+  int m = i0, M = i0;
+  for (int n = 0; n < 3; ++n) {
+    if (!(q[m] < q[v[n]])) m = v[n];
+    if (!(q[M] > q[v[n]])) M = v[n];
+  }
+  imin = m;
+  imax = M;
+}
+
+// Qin of slot m of cell (i, j) (trc_qin): value and source of the min / max
+__device__ void qin_src(const HLin& a, int i, int j, int k, int l, int m, double& vmin, double& vmax, Src& smin,
+                        Src& smax) {
+  const double BIG = cC.HUGE_;
+  int ai = i, bj = j, f = m;
+  if (m >= 3) {
+    const int nbI[3] = {-1, -1, 0}, nbJ[3] = {0, -1, -1};
+    ai = i + nbI[m - 3];
+    bj = j + nbJ[m - 3];
+    f = m - 3;
+  }
+  const double cmv = a.cm[f][ix(ai, bj, k, l)];
+  int imin, imax;
+  if (cG.have_sgp[l] && ai == 0 && bj == 0 && f == 1) {
+    const int c4[4] = {ix(0, 0, k, l), ix(1, 1, k, l), ix(2, 1, k, l), ix(0, 1, k, l)};
+    imin = imax = c4[0];
+    for (int n = 1; n < 4; ++n) {
+      if (!(a.q[imin] < a.q[c4[n]])) imin = c4[n];
+      if (!(a.q[imax] > a.q[c4[n]])) imax = c4[n];
+    }
+  } else {
+    face_minmax_idx(a.q, ai, bj, k, l, f, imin, imax);
+  }
+  const bool use = (m < 3) ? (cmv == 1.0) : (cmv != 1.0);
+  if (use) {
+    vmin = a.q[imin]; vmax = a.q[imax];
+    smin = Src{SRC_Q, imin, 0}; smax = Src{SRC_Q, imax, 0};
+  } else {
+    vmin = BIG; vmax = -BIG;
+    smin = Src{SRC_NONE, 0, 0}; smax = Src{SRC_NONE, 0, 0};
+  }
+}
+
+// npmin(npmax(x, lo), hi) and npmax(npmin(x, hi), lo) with their sources
+__device__ __forceinline__ void clamp_minmax(double& x, Src& sx, double lo, Src slo, double hi, Src shi) {
+  if (!(x > lo)) { x = lo; sx = slo; }
+  if (!(x < hi)) { x = hi; sx = shi; }
+}
+__device__ __forceinline__ void clamp_maxmin(double& x, Src& sx, double lo, Src slo, double hi, Src shi) {
+  if (!(x < hi)) { x = hi; sx = shi; }
+  if (!(x > lo)) { x = lo; sx = slo; }
+}
+
+// source of the limited value of edge f of cell (ai, bj) (trc_limited_face)
+__device__ Src limited_face_src(const HLin& a, int ai, int bj, int k, int l, int f) {
+  const int mi[3] = {1, 1, 0}, mj[3] = {0, 1, 1};
+  const int ni = ai + mi[f], nj = bj + mj[f];
+  const int p = ix(ai, bj, k, l), pn = ix(ni, nj, k, l);
+  const bool c = a.cm[f][p] == 1.0;
+  double v = a.qa[f][p];
+  Src sv{SRC_QA, p, f};
+  double lo, hi;
+  Src slo, shi;
+  if (c) qin_src(a, ai, bj, k, l, f, lo, hi, slo, shi);
+  else qin_src(a, ni, nj, k, l, 3 + f, lo, hi, slo, shi);
+  clamp_minmax(v, sv, lo, slo, hi, shi);
+  const int pc = c ? pn : p;
+  clamp_maxmin(v, sv, a.Qmin[pc], Src{SRC_QMIN, pc, 0}, a.Qmax[pc], Src{SRC_QMAX, pc, 0});
+  return sv;
+}
+
+__device__ __forceinline__ double src_tl(const HLin& a, Src s) {
+  switch (s.kind) {
+    case SRC_Q: return a.dq[s.idx];
+    case SRC_QA: return a.dqa[s.f][s.idx];
+    case SRC_QMIN: return a.dQmin[s.idx];
+    case SRC_QMAX: return a.dQmax[s.idx];
+    default: return 0.0;
+  }
+}
+__device__ __forceinline__ void src_ad(const HLin& a, Src s, double v) {
+  switch (s.kind) {
+    case SRC_Q: atomicAdd(&a.gq[s.idx], v); break;
+    case SRC_QA: atomicAdd(&a.gqa[s.f][s.idx], v); break;
+    case SRC_QMIN: atomicAdd(&a.gQmin[s.idx], v); break;
+    case SRC_QMAX: atomicAdd(&a.gQmax[s.idx], v); break;
+    default: break;
+  }
+}
+
+// Qout of an interior cell as a linear form of q at the forward's branches
+// (k_trc_qout): Qmin = fz qc + sum wmin_n q[smin_n], the same for Qmax
+struct QoutLin {
+  double fz, B, f;
+  Src nmin, nmax, imin[6], imax[6];
+  double chm[6];
+};
+__device__ void qout_lin(const HLin& a, int i, int j, int k, int l, QoutLin& o) {
+  const int p = ix(i, j, k, l);
+  const double qc = a.q[p];
+  double qnmin = qc, qnmax = qc, Cin = 0.0, Cout = 0.0;
+  o.nmin = o.nmax = Src{SRC_Q, p, 0};
+  for (int m = 0; m < 6; ++m) {
+    double qi, qx;
+    qin_src(a, i, j, k, l, m, qi, qx, o.imin[m], o.imax[m]);
+    if (!(qnmin < qi)) { qnmin = qi; o.nmin = o.imin[m]; }
+    if (!(qnmax > qx)) { qnmax = qx; o.nmax = o.imax[m]; }
+    const double chv = a.ch[m][p];
+    const double chm = (chv < 0.0) ? chv : 0.0;
+    o.chm[m] = chm;
+    if (m == 0) { Cin = chm; Cout = chv - chm; }
+    else { Cin = Cin + chm; Cout = Cout + (chv - chm); }
+  }
+  const double zsw = 0.5 - copysign(0.5, fabs(Cout) - cC.EPS);
+  const double d = 1.0 * a.frhog[p] / a.rhog_t[p] * a.dt;
+  o.B = 1.0 - Cin - Cout + d;
+  o.f = (1.0 - zsw) / (Cout + zsw);
+  o.fz = o.f + zsw;
+}
+
+__global__ void k_hlin_qout(HLin a, int adjoint) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  int i, j, l;
+  if (!col_of(t, i, j, l)) return;
+  const bool in = interior(i, j);
+  for (int k = 0; k < cD.KA; ++k) {
+    const int p = ix(i, j, k, l);
+    if (!in) {   // Qmin = Qmax = q
+      if (adjoint) atomicAdd(&a.gq[p], a.gQmin[p] + a.gQmax[p]);
+      else { a.oQmin[p] = a.dq[p]; a.oQmax[p] = a.dq[p]; }
+      continue;
+    }
+    QoutLin o;
+    qout_lin(a, i, j, k, l, o);
+    if (!adjoint) {
+      double cqmin = 0.0, cqmax = 0.0;
+      for (int m = 0; m < 6; ++m) {
+        cqmin += o.chm[m] * src_tl(a, o.imin[m]);
+        cqmax += o.chm[m] * src_tl(a, o.imax[m]);
+      }
+      a.oQmin[p] = o.fz * a.dq[p] - o.f * cqmax - o.f * o.B * src_tl(a, o.nmax);
+      a.oQmax[p] = o.fz * a.dq[p] - o.f * cqmin - o.f * o.B * src_tl(a, o.nmin);
+    } else {
+      const double gn = a.gQmin[p], gx = a.gQmax[p];
+      atomicAdd(&a.gq[p], o.fz * (gn + gx));
+      for (int m = 0; m < 6; ++m) {
+        src_ad(a, o.imax[m], -o.f * o.chm[m] * gn);
+        src_ad(a, o.imin[m], -o.f * o.chm[m] * gx);
+      }
+      src_ad(a, o.nmax, -o.f * o.B * gn);
+      src_ad(a, o.nmin, -o.f * o.B * gx);
+    }
+  }
+}
+
+// the flux update of the interior cells (k_trc_apply): y = x - sum flx_f v_f
+__global__ void k_hlin_apply(HLin a, int adjoint) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  int i, j, l;
+  if (!col_of(t, i, j, l)) return;
+  const bool in = interior(i, j);
+  for (int k = 0; k < cD.KA; ++k) {
+    const int p = ix(i, j, k, l);
+    if (!in) {
+      if (!adjoint) a.y[p] = a.x[p];
+      continue;
+    }
+    const Src s[6] = {limited_face_src(a, i, j, k, l, 0),     limited_face_src(a, i, j, k, l, 1),
+                      limited_face_src(a, i, j, k, l, 2),     limited_face_src(a, i - 1, j, k, l, 0),
+                      limited_face_src(a, i - 1, j - 1, k, l, 1), limited_face_src(a, i, j - 1, k, l, 2)};
+    if (!adjoint) {
+      double upd = 0.0;
+      for (int f = 0; f < 6; ++f) upd += a.flx[f][p] * src_tl(a, s[f]);
+      a.y[p] = a.x[p] - upd;
+    } else {
+      const double g = a.x[p];
+      for (int f = 0; f < 6; ++f) src_ad(a, s[f], -a.flx[f][p] * g);
+    }
+  }
+}
+
+// MIURA2004 face values (k_trc_remap), adjoint: scatter into gq and the gradient cotangents
+__global__ void k_hlin_remap_ad(HLin a) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  int i, j, l;
+  if (!col_of(t, i, j, l)) return;
+  const int G = cD.G;
+  if (i > G - 2 || j > G - 2) return;
+  const int mi[3] = {1, 1, 0}, mj[3] = {0, 1, 1};
+  for (int k = 0; k < cD.KA; ++k) {
+    const int p = ix(i, j, k, l);
+    for (int f = 0; f < 3; ++f) {
+      const double g = a.gqa[f][p];
+      if (g == 0.0) continue;
+      const double c = a.cm[f][p];
+      const int ni = i + mi[f], nj = j + mj[f], pn = ix(ni, nj, k, l);
+      atomicAdd(&a.gq[p], (1.0 - c) * g);
+      atomicAdd(&a.gq[pn], c * g);
+      for (int d = 0; d < 3; ++d) {
+        const double xcv = a.xc[f * 3 + d][p];
+        atomicAdd(&a.gg[d][p], (1.0 - c) * g * (xcv - P2(cG.GRD_x, d, i, j, l)));
+        atomicAdd(&a.gg[d][pn], c * g * (xcv - P2(cG.GRD_x, d, ni, nj, l)));
+      }
+    }
+  }
+}
+
+// gradient (k_trc_grad_t) adjoint on the interior cells, then x-bar +=
+// q-bar / rhog_t on every regional cell
+__global__ void k_hlin_grad_ad(HLin a) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.npti) return;
+  const int G = cD.G, KA = cD.KA;
+  const int i = t % G, j = (t / G) % G, k = (t / (G * G)) % KA, l = t / (G * G * KA);
+  double s = 0.0;
+  for (int m = 0; m < 7; ++m) {   // every interior cell whose stencil point m is (i, j)
+    const int si = i - kNbI[m], sj = j - kNbJ[m];
+    if (si >= 1 && sj >= 1 && si <= G - 2 && sj <= G - 2) {
+      const int ps = ix(si, sj, k, l);
+      for (int d = 0; d < 3; ++d) s += P2(cG.coef_grad, d * 7 + m, si, sj, l) * a.gg[d][ps];
+    }
+  }
+  a.gx[t] += (a.gq[t] + s) / a.rhog_t[t];
+}
+
+// ---- pole point (g = 0) of each pole and level
+__device__ void qin_pl_src(const HLin& a, int v, int k, int lp, double& in0n, double& in1n, double& in0x,
+                           double& in1x, Src& sn, Src& sx, bool& c1) {
+  const double BIG = cC.HUGE_;
+  const int vp1 = (v + 1 > 5) ? 1 : v + 1, vm1 = (v - 1 < 1) ? 5 : v - 1;
+  const int c4[4] = {ipl(0, k, lp), ipl(v, k, lp), ipl(vm1, k, lp), ipl(vp1, k, lp)};
+  int imin = c4[0], imax = c4[0];
+  for (int n = 1; n < 4; ++n) {   // pymin / pymax: the later argument only when strictly beyond
+    if (a.q_pl[c4[n]] < a.q_pl[imin]) imin = c4[n];
+    if (a.q_pl[c4[n]] > a.q_pl[imax]) imax = c4[n];
+  }
+  c1 = a.cm_pl[ipl(v, k, lp)] == 1.0;
+  const double qn = a.q_pl[imin], qx = a.q_pl[imax];
+  in0n = c1 ? qn : BIG;
+  in1n = c1 ? BIG : qn;
+  in0x = c1 ? qx : -BIG;
+  in1x = c1 ? -BIG : qx;
+  sn = Src{SRC_Q, imin, 0};
+  sx = Src{SRC_Q, imax, 0};
+}
+
+__device__ __forceinline__ double src_tl_pl(const HLin& a, Src s) {
+  switch (s.kind) {
+    case SRC_Q: return a.dq_pl[s.idx];
+    case SRC_QA: return a.dqa_pl[s.idx];
+    case SRC_QMIN: return a.dQmin_pl[s.idx];
+    case SRC_QMAX: return a.dQmax_pl[s.idx];
+    default: return 0.0;
+  }
+}
+__device__ __forceinline__ void src_ad_pl(const HLin& a, Src s, double v) {
+  switch (s.kind) {
+    case SRC_Q: atomicAdd(&a.gq_pl[s.idx], v); break;
+    case SRC_QA: atomicAdd(&a.gqa_pl[s.idx], v); break;
+    case SRC_QMIN: atomicAdd(&a.gQmin_pl[s.idx], v); break;
+    case SRC_QMAX: atomicAdd(&a.gQmax_pl[s.idx], v); break;
+    default: break;
+  }
+}
+
+// pole Qout (k_trc_qout_pl) and flux update (k_trc_apply_pl): one thread per (k, lp)
+__global__ void k_hlin_pole(HLin a, int adjoint, int stage) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.KA * cD.LP) return;
+  const int k = t / cD.LP, lp = t % cD.LP;
+  const int p0 = ipl(0, k, lp);
+  if (stage == 0) {   // Qout at p0
+    double qnm = a.q_pl[p0], qnx = a.q_pl[p0];
+    Src snm{SRC_Q, p0, 0}, snx{SRC_Q, p0, 0}, sn[6], sx[6];
+    double chm[6], Ci = 0.0, Co = 0.0;
+    for (int v = 1; v <= 5; ++v) {
+      double in0n, in1n, in0x, in1x;
+      bool c1;
+      qin_pl_src(a, v, k, lp, in0n, in1n, in0x, in1x, sn[v], sx[v], c1);
+      if (!c1) sn[v] = sx[v] = Src{SRC_NONE, 0, 0};
+      if (in0n < qnm) { qnm = in0n; snm = sn[v]; }
+      if (in0x > qnx) { qnx = in0x; snx = sx[v]; }
+      const int pv = ipl(v, k, lp);
+      chm[v] = a.cm_pl[pv] * a.ch_pl[pv];
+      Ci = Ci + chm[v];
+      Co = Co + (a.ch_pl[pv] - chm[v]);
+    }
+    const double zs = 0.5 - copysign(0.5, fabs(Co) - cC.EPS);
+    const double f = (1.0 - zs) / (Co + zs), fz = f + zs;
+    const double B = 1.0 - Ci - Co + 1.0 * a.frhog_pl[p0] / a.rhog_t_pl[p0] * a.dt;
+    if (!adjoint) {
+      double cqn = 0.0, cqx = 0.0;
+      for (int v = 1; v <= 5; ++v) {
+        cqn += chm[v] * src_tl_pl(a, sn[v]);
+        cqx += chm[v] * src_tl_pl(a, sx[v]);
+      }
+      a.oQmin_pl[p0] = fz * a.dq_pl[p0] - f * cqx - f * B * src_tl_pl(a, snx);
+      a.oQmax_pl[p0] = fz * a.dq_pl[p0] - f * cqn - f * B * src_tl_pl(a, snm);
+    } else {
+      const double gn = a.gQmin_pl[p0], gx = a.gQmax_pl[p0];
+      atomicAdd(&a.gq_pl[p0], fz * (gn + gx));
+      for (int v = 1; v <= 5; ++v) {
+        src_ad_pl(a, sx[v], -f * chm[v] * gn);
+        src_ad_pl(a, sn[v], -f * chm[v] * gx);
+      }
+      src_ad_pl(a, snx, -f * B * gn);
+      src_ad_pl(a, snm, -f * B * gx);
+    }
+    return;
+  }
+  // stage 1: flux update of p0 from its five edges (the other pole points keep x)
+  double acc = 0.0;
+  const double g = adjoint ? a.x_pl[p0] : 0.0;
+  for (int v = 1; v <= 5; ++v) {
+    const int pv = ipl(v, k, lp);
+    double in0n, in1n, in0x, in1x;
+    Src sn, sx;
+    bool c1;
+    qin_pl_src(a, v, k, lp, in0n, in1n, in0x, in1x, sn, sx, c1);
+    const Src none{SRC_NONE, 0, 0};
+    double x = a.qa_pl[pv];
+    Src s{SRC_QA, pv, 0};
+    if (c1) clamp_minmax(x, s, in0n, sn, in0x, sx);        // a0, chosen by c = 1
+    else clamp_minmax(x, s, in1n, sn, in1x, sx);           // a1
+    (void)none;
+    const int pc = c1 ? pv : p0;
+    clamp_maxmin(x, s, a.Qmin_pl[pc], Src{SRC_QMIN, pc, 0}, a.Qmax_pl[pc], Src{SRC_QMAX, pc, 0});
+    if (!adjoint) acc += a.flx_pl[pv] * src_tl_pl(a, s);
+    else src_ad_pl(a, s, -a.flx_pl[pv] * g);
+  }
+  if (!adjoint) {
+    for (int v = 0; v < 6; ++v) a.y_pl[ipl(v, k, lp)] = a.x_pl[ipl(v, k, lp)];
+    a.y_pl[p0] = a.x_pl[p0] - acc;
+  }
+}
+
+// pole remap (k_trc_remap_pl) adjoint: one thread per (k, lp); before the
+// gradient cotangents' exchange adjoint
+__global__ void k_hlin_pole_remap_ad(HLin a) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.KA * cD.LP) return;
+  const int k = t / cD.LP, lp = t % cD.LP;
+  const int p0 = ipl(0, k, lp);
+  const double* X = cG.GRD_x_pl;
+  // qa[pv] = c am + (1 - c) ap, ap from p0, am from pv
+  for (int v = 1; v <= 5; ++v) {
+    const int pv = ipl(v, k, lp);
+    const double g = a.gqa_pl[pv], c = a.cm_pl[pv];
+    a.gq_pl[p0] += (1.0 - c) * g;
+    a.gq_pl[pv] += c * g;
+    for (int d = 0; d < 3; ++d) {
+      a.gg_pl[d][p0] += (1.0 - c) * g * (a.xc_pl[pv * 3 + d] - X[(0 * cD.LP + lp) * 3 + d]);
+      a.gg_pl[d][pv] += c * g * (a.xc_pl[pv * 3 + d] - X[(v * cD.LP + lp) * 3 + d]);
+    }
+  }
+}
+
+// pole gradient (k_trc_grad_pl) adjoint, then x-bar += q-bar / rhog_t on the
+// pole arrays: gq_d[p0] = sum_v coef_grad_pl(v, d) q[v], the other rows zero
+__global__ void k_hlin_pole_grad_ad(HLin a) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.KA * cD.LP) return;
+  const int k = t / cD.LP, lp = t % cD.LP;
+  const int p0 = ipl(0, k, lp);
+  for (int d = 0; d < 3; ++d) {
+    const double g = a.gg_pl[d][p0];
+    for (int v = 0; v < 6; ++v) a.gq_pl[ipl(v, k, lp)] += cG.coef_grad_pl[(v * cD.LP + lp) * 3 + d] * g;
+  }
+  for (int v = 0; v < 6; ++v) {
+    const int pv = ipl(v, k, lp);
+    a.gx_pl[pv] += a.gq_pl[pv] / a.rhog_t_pl[pv];
+  }
+}
+
+}  // namespace nc

@@ -17,6 +17,7 @@
 #include "nc_tracer.cuh"
 #include "nc_grid.cuh"
 #include "nc_history.cuh"
+#include "nc_adjoint.cuh"
 
 using namespace nc;
 
@@ -391,6 +392,12 @@ struct nc_handle {
   cudaEvent_t ev_in_ready = nullptr, ev_in_free = nullptr, ev_out_ready = nullptr, ev_out_done = nullptr;
   cudaEvent_t ev_user = nullptr;   // ordering against a caller's stream (device-pointer marshal)
   double *stage_out = nullptr, *stage_out_pl = nullptr;
+  double* adj_work = nullptr;   // exchanged copy of the Laplacian's input (allocated on first use)
+  // linearised tracer step (nc_trc_step_lin): work fields allocated on first use
+  FieldPair lin[20];
+  bool lin_ready = false;
+  bool stepped = false;   // a step has run: PM, P0 and frhog hold its winds and densities
+  bool single = false;    // pole kernels on the library stream (no second stream)
   // per-kernel timing (opt-in, eager launches only): an event after every
   // launch; a kernel's time is the gap to the previous event on the stream
   bool prof = false;
@@ -584,18 +591,20 @@ static int collect_profile(nc_handle* h) {
   } while (0)
 
 static int fork_pl(nc_handle* h) {
-  if (h->prof || !h->stream2) return 0;
+  if (h->prof || h->single || !h->stream2) return 0;
   CU(cudaEventRecord(h->ev_fork, h->stream));
   CU(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0));
   return 0;
 }
 static int join_pl(nc_handle* h) {
-  if (h->prof || !h->stream2) return 0;
+  if (h->prof || h->single || !h->stream2) return 0;
   CU(cudaEventRecord(h->ev_join, h->stream2));
   CU(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
   return 0;
 }
-static cudaStream_t pole_stream(nc_handle* h) { return (h->prof || !h->stream2) ? h->stream : h->stream2; }
+static cudaStream_t pole_stream(nc_handle* h) {
+  return (h->prof || h->single || !h->stream2) ? h->stream : h->stream2;
+}
 
 template <class R>
 static int comm(nc_handle* h, std::initializer_list<FieldPair> fl) {
@@ -649,6 +658,146 @@ static int comm_prg(nc_handle* h) {
   k_comm<<<(unsigned)((ne + 255) / 256), 256, 0, h->stream>>>(f, h->r_dst, h->r_src, h->nr, h->p_dst, h->p_src, h->np);
   TRY(check_launch(h, "comm_final"));
   for (int iq = NC_MAXCOMM - 6; iq < D.nq; ++iq) TRY(comm<R>(h, {h->Pq[iq]}));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// the tracer advection of a step (mod_src_tracer.py:83-1228) in its parts:
+// vertical mass fluxes and the density after the vertical half step, the
+// vertical advection of one tracer, the horizontal fluxes, Courant numbers and
+// face centroids, the horizontal advection with the Thuburn limiter of one
+// tracer, and the density after the horizontal step.  The winds are PM, the
+// density at the step's start P0[0], the density tendency frhog.
+// ---------------------------------------------------------------------------
+template <class R>
+static int trc_vflux(nc_handle* h) {
+  const Dims& D = h->D;
+  const cudaStream_t s = h->stream, ps = pole_stream(h);
+  const unsigned pcb = (unsigned)((6 * D.LP + 31) / 32);
+  const double dt = h->dtl;
+  for (int pole = 0; pole < 2; ++pole) {
+    TrcFluxArgs<R> ta;
+    auto F = [&](FieldPair& f) { return pole ? PL<R>(f) : RG<R>(f); };
+    ta.rvx = F(h->PM[1]); ta.rvy = F(h->PM[2]); ta.rvz = F(h->PM[3]); ta.rw = F(h->PM[4]);
+    ta.rhog_in = F(h->P0[0]); ta.frhog = F(h->frhog); ta.flx_v = F(h->flx_v); ta.rhog_t = F(h->rhog_t);
+    ta.dt = dt;
+    if (!pole) k_trc_vflux<<<(unsigned)((D.npt2 + h->blk[TB_TRC_VFLUX] - 1) / h->blk[TB_TRC_VFLUX]), h->blk[TB_TRC_VFLUX], 0, s>>>(ta, 0);
+    else k_trc_vflux<<<pcb, 32, 0, ps>>>(ta, 1);
+    TRY(check_launch(h, pole ? "trc_vflux_pl" : "trc_vflux"));
+  }
+  return 0;
+}
+
+// vertical advection of the tracer mass x in place: the first (second) step
+// of the tracer advection, density P0[0] (rhog_t), no clamp (clamp)
+template <class R>
+static int trc_vadv(nc_handle* h, FieldPair& x, bool second) {
+  const Dims& D = h->D;
+  const cudaStream_t s = h->stream, ps = pole_stream(h);
+  const unsigned pcb = (unsigned)((6 * D.LP + 31) / 32);
+  const double dt = h->dtl;
+  for (int pole = 0; pole < 2; ++pole) {
+    TrcVadvArgs<R> va;
+    auto F = [&](FieldPair& f) { return pole ? PL<R>(f) : RG<R>(f); };
+    va.rhogq = F(x);
+    va.den = second ? F(h->rhog_t) : F(h->P0[0]);
+    va.flx_v = F(h->flx_v); va.frhog = F(h->frhog);
+    va.dt = dt; va.bcoef = 0.0; va.clamp = second ? 1 : 0; va.dtl = dt;
+    if (!pole) k_trc_vadv<<<(unsigned)((D.npt2 + h->blk[TB_TRC_VADV] - 1) / h->blk[TB_TRC_VADV]), h->blk[TB_TRC_VADV], 0, s>>>(va, 0);
+    else k_trc_vadv<<<pcb, 32, 0, ps>>>(va, 1);
+    TRY(check_launch(h, pole ? "trc_vadv_pl" : "trc_vadv"));
+  }
+  return 0;
+}
+
+template <class R>
+static int trc_hflux(nc_handle* h) {
+  const Dims& D = h->D;
+  const cudaStream_t s = h->stream, ps = pole_stream(h);
+  const unsigned pkb = (unsigned)((D.KA * D.LP + 127) / 128);
+  const double dt = h->dtl;
+  {
+    TrcHfluxArgs<R> ha;
+    ha.rho = RG<R>(h->PM[0]); ha.rvx = RG<R>(h->PM[1]); ha.rvy = RG<R>(h->PM[2]); ha.rvz = RG<R>(h->PM[3]); ha.rhog_t = RG<R>(h->rhog_t);
+    for (int f = 0; f < 6; ++f) { ha.flx[f] = RG<R>(h->flx[f]); ha.ch[f] = RG<R>(h->ch[f]); ha.cm[f] = RG<R>(h->cm[f]); }
+    for (int f = 0; f < 9; ++f) ha.xc[f] = RG<R>(h->xc[f]);
+    ha.dt = dt;
+    {
+      const dim3 gt((unsigned)D.KA, (unsigned)(((D.G + TH_DX - 1) / TH_DX) * ((D.G + TH_DY - 1) / TH_DY)), (unsigned)D.L);
+      k_trc_hflux_t<<<gt, TH_DX * TH_DY, 0, s>>>(ha);
+    }
+    TRY(check_launch(h, "trc_hflux"));
+    TrcHfluxPlArgs<R> hp;
+    hp.rho = PL<R>(h->PM[0]); hp.rvx = PL<R>(h->PM[1]); hp.rvy = PL<R>(h->PM[2]); hp.rvz = PL<R>(h->PM[3]); hp.rhog_t = PL<R>(h->rhog_t);
+    hp.flx = PL<R>(h->flx[0]); hp.xc = PL<R>(h->xc[0]); hp.ch = PL<R>(h->ch[0]); hp.cm = PL<R>(h->cm[0]); hp.dt = dt;
+    k_trc_hflux_pl<<<pkb, 128, 0, ps>>>(hp);
+    TRY(check_launch(h, "trc_hflux_pl"));
+  }
+  return 0;
+}
+
+// horizontal advection of the tracer mass x in place (gradient, exchange, face
+// values, Qout, exchange, flux update); leaves q, gq, qa, Qmin / Qmax behind
+template <class R>
+static int trc_horizontal(nc_handle* h, FieldPair& x) {
+  const Dims& D = h->D;
+  const cudaStream_t s = h->stream, ps = pole_stream(h);
+  const unsigned pkb = (unsigned)((D.KA * D.LP + 127) / 128);
+  const double dt = h->dtl;
+  {
+    const dim3 gt((unsigned)D.KA, (unsigned)(((D.G - 2 + TG_DX - 1) / TG_DX) * ((D.G - 2 + TG_DY - 1) / TG_DY)),
+                  (unsigned)D.L);
+    k_trc_grad_t<<<gt, TG_DX * TG_DY, 0, s>>>(RG<R>(x), RG<R>(h->rhog_t), RG<R>(h->q), RG<R>(h->gq[0]), RG<R>(h->gq[1]),
+                                              RG<R>(h->gq[2]));
+  }
+  TRY(check_launch(h, "trc_grad"));
+  k_trc_grad_pl<<<pkb, 128, 0, ps>>>(PL<R>(x), PL<R>(h->rhog_t), PL<R>(h->q), PL<R>(h->gq[0]), PL<R>(h->gq[1]), PL<R>(h->gq[2]));
+  TRY(check_launch(h, "trc_grad_pl"));
+  TRY(comm<R>(h, {h->gq[0], h->gq[1], h->gq[2]}));
+  TrcRemapArgs<R> ra;
+  ra.q = RG<R>(h->q); ra.gq0 = RG<R>(h->gq[0]); ra.gq1 = RG<R>(h->gq[1]); ra.gq2 = RG<R>(h->gq[2]);
+  for (int f = 0; f < 9; ++f) ra.xc[f] = RG<R>(h->xc[f]);
+  for (int f = 0; f < 6; ++f) ra.cm[f] = RG<R>(h->cm[f]);
+  for (int f = 0; f < 3; ++f) ra.qa[f] = RG<R>(h->qa[f]);
+  k_trc_remap<<<(unsigned)((D.npt2 + h->blk[TB_TRC_REMAP] - 1) / h->blk[TB_TRC_REMAP]), h->blk[TB_TRC_REMAP], 0, s>>>(ra);
+  TRY(check_launch(h, "trc_remap"));
+  TrcRemapPlArgs<R> rp;
+  rp.q = PL<R>(h->q); rp.gq0 = PL<R>(h->gq[0]); rp.gq1 = PL<R>(h->gq[1]); rp.gq2 = PL<R>(h->gq[2]); rp.xc = PL<R>(h->xc[0]);
+  rp.cm = PL<R>(h->cm[0]); rp.qa = PL<R>(h->qa[0]);
+  k_trc_remap_pl<<<pkb, 128, 0, ps>>>(rp);
+  TRY(check_launch(h, "trc_remap_pl"));
+  TrcLimArgs<R> la;
+  la.q = RG<R>(h->q); la.rhog_t = RG<R>(h->rhog_t); la.frhog = RG<R>(h->frhog);
+  for (int f = 0; f < 6; ++f) { la.ch[f] = RG<R>(h->ch[f]); la.cm[f] = RG<R>(h->cm[f]); la.flx[f] = RG<R>(h->flx[f]); }
+  for (int f = 0; f < 3; ++f) la.qa[f] = RG<R>(h->qa[f]);
+  la.qout_min = RG<R>(h->Qmin); la.qout_max = RG<R>(h->Qmax); la.Qmin = RG<R>(h->Qmin); la.Qmax = RG<R>(h->Qmax);
+  la.rhogq = RG<R>(x); la.dt = dt;
+  TrcLimPlArgs<R> lp;
+  lp.q = PL<R>(h->q); lp.ch = PL<R>(h->ch[0]); lp.cm = PL<R>(h->cm[0]); lp.rhog_t = PL<R>(h->rhog_t); lp.frhog = PL<R>(h->frhog);
+  lp.qa = PL<R>(h->qa[0]); lp.flx = PL<R>(h->flx[0]); lp.Qmin = PL<R>(h->Qmin); lp.Qmax = PL<R>(h->Qmax);
+  lp.qout_min = PL<R>(h->Qmin); lp.qout_max = PL<R>(h->Qmax); lp.rhogq = PL<R>(x); lp.dt = dt;
+  k_trc_qout<<<(unsigned)((D.npt2 + h->blk[TB_TRC_QOUT] - 1) / h->blk[TB_TRC_QOUT]), h->blk[TB_TRC_QOUT], 0, s>>>(la);
+  TRY(check_launch(h, "trc_qout"));
+  k_trc_qout_pl<<<pkb, 128, 0, ps>>>(lp);
+  TRY(check_launch(h, "trc_qout_pl"));
+  TRY(comm<R>(h, {h->Qmin, h->Qmax}));
+  k_trc_apply<<<(unsigned)((D.npt2 + h->blk[TB_TRC_APPLY] - 1) / h->blk[TB_TRC_APPLY]), h->blk[TB_TRC_APPLY], 0, s>>>(la);
+  TRY(check_launch(h, "trc_apply"));
+  k_trc_apply_pl<<<pkb, 128, 0, ps>>>(lp);
+  TRY(check_launch(h, "trc_apply_pl"));
+  return 0;
+}
+
+template <class R>
+static int trc_rhog(nc_handle* h) {
+  const Dims& D = h->D;
+  const cudaStream_t s = h->stream;
+  const double dt = h->dtl;
+  TRY(join_pl(h));
+  k_trc_rhog<<<(unsigned)(((D.npt2 + (long long)D.KA * D.LP) + h->blk[TB_TRC_RHOG] - 1) / h->blk[TB_TRC_RHOG]), h->blk[TB_TRC_RHOG], 0, s>>>(RG<R>(h->rhog_t), RG<R>(h->flx[0]), RG<R>(h->flx[1]), RG<R>(h->flx[2]), RG<R>(h->flx[3]), RG<R>(h->flx[4]),
+                                     RG<R>(h->flx[5]), RG<R>(h->frhog), (R)dt, PL<R>(h->flx[0]), PL<R>(h->rhog_t), PL<R>(h->frhog));
+  TRY(check_launch(h, "trc_rhog"));
+  TRY(fork_pl(h));
   return 0;
 }
 
@@ -898,103 +1047,17 @@ static int run_step(nc_handle* h) {
     TRY(fork_pl(h));
   }
   // ---- tracer advection (mod_src_tracer.py:83-1228), after the last RK stage
-  const double dt = h->dtl;
-  for (int pole = 0; pole < 2; ++pole) {
-    TrcFluxArgs<R> ta;
-    auto F = [&](FieldPair& f) { return pole ? PL<R>(f) : RG<R>(f); };
-    ta.rvx = F(h->PM[1]); ta.rvy = F(h->PM[2]); ta.rvz = F(h->PM[3]); ta.rw = F(h->PM[4]);
-    ta.rhog_in = F(h->P0[0]); ta.frhog = F(h->frhog); ta.flx_v = F(h->flx_v); ta.rhog_t = F(h->rhog_t);
-    ta.dt = dt;
-    if (!pole) k_trc_vflux<<<(unsigned)((D.npt2 + h->blk[TB_TRC_VFLUX] - 1) / h->blk[TB_TRC_VFLUX]), h->blk[TB_TRC_VFLUX], 0, s>>>(ta, 0);
-    else k_trc_vflux<<<pcb, 32, 0, ps>>>(ta, 1);
-    TRY(check_launch(h, pole ? "trc_vflux_pl" : "trc_vflux"));
-  }
-  auto vadv = [&](int iq, bool second) -> int {
-    for (int pole = 0; pole < 2; ++pole) {
-      TrcVadvArgs<R> va;
-      auto F = [&](FieldPair& f) { return pole ? PL<R>(f) : RG<R>(f); };
-      va.rhogq = F(h->Pq[iq]);
-      va.den = second ? F(h->rhog_t) : F(h->P0[0]);
-      va.flx_v = F(h->flx_v); va.frhog = F(h->frhog);
-      va.dt = dt; va.bcoef = 0.0; va.clamp = second ? 1 : 0; va.dtl = dt;
-      if (!pole) k_trc_vadv<<<(unsigned)((D.npt2 + h->blk[TB_TRC_VADV] - 1) / h->blk[TB_TRC_VADV]), h->blk[TB_TRC_VADV], 0, s>>>(va, 0);
-      else k_trc_vadv<<<pcb, 32, 0, ps>>>(va, 1);
-      TRY(check_launch(h, pole ? "trc_vadv_pl" : "trc_vadv"));
-    }
-    return 0;
-  };
+  TRY(trc_vflux<R>(h));
   // first vertical step uses the density at the start of the step; the
   // Courant numbers of the first step are those of rhog_in
-  for (int iq = 0; iq < D.nq; ++iq) TRY(vadv(iq, false));
+  for (int iq = 0; iq < D.nq; ++iq) TRY(trc_vadv<R>(h, h->Pq[iq], false));
   PHASE();
-  {
-    TrcHfluxArgs<R> ha;
-    ha.rho = RG<R>(h->PM[0]); ha.rvx = RG<R>(h->PM[1]); ha.rvy = RG<R>(h->PM[2]); ha.rvz = RG<R>(h->PM[3]); ha.rhog_t = RG<R>(h->rhog_t);
-    for (int f = 0; f < 6; ++f) { ha.flx[f] = RG<R>(h->flx[f]); ha.ch[f] = RG<R>(h->ch[f]); ha.cm[f] = RG<R>(h->cm[f]); }
-    for (int f = 0; f < 9; ++f) ha.xc[f] = RG<R>(h->xc[f]);
-    ha.dt = dt;
-    {
-      const dim3 gt((unsigned)D.KA, (unsigned)(((D.G + TH_DX - 1) / TH_DX) * ((D.G + TH_DY - 1) / TH_DY)), (unsigned)D.L);
-      k_trc_hflux_t<<<gt, TH_DX * TH_DY, 0, s>>>(ha);
-    }
-    TRY(check_launch(h, "trc_hflux"));
-    TrcHfluxPlArgs<R> hp;
-    hp.rho = PL<R>(h->PM[0]); hp.rvx = PL<R>(h->PM[1]); hp.rvy = PL<R>(h->PM[2]); hp.rvz = PL<R>(h->PM[3]); hp.rhog_t = PL<R>(h->rhog_t);
-    hp.flx = PL<R>(h->flx[0]); hp.xc = PL<R>(h->xc[0]); hp.ch = PL<R>(h->ch[0]); hp.cm = PL<R>(h->cm[0]); hp.dt = dt;
-    k_trc_hflux_pl<<<pkb, 128, 0, ps>>>(hp);
-    TRY(check_launch(h, "trc_hflux_pl"));
-  }
+  TRY(trc_hflux<R>(h));
   PHASE();
-  for (int iq = 0; iq < D.nq; ++iq) {
-    {
-      const dim3 gt((unsigned)D.KA, (unsigned)(((D.G - 2 + TG_DX - 1) / TG_DX) * ((D.G - 2 + TG_DY - 1) / TG_DY)),
-                    (unsigned)D.L);
-      k_trc_grad_t<<<gt, TG_DX * TG_DY, 0, s>>>(RG<R>(h->Pq[iq]), RG<R>(h->rhog_t), RG<R>(h->q), RG<R>(h->gq[0]), RG<R>(h->gq[1]),
-                                                RG<R>(h->gq[2]));
-    }
-    TRY(check_launch(h, "trc_grad"));
-    k_trc_grad_pl<<<pkb, 128, 0, ps>>>(PL<R>(h->Pq[iq]), PL<R>(h->rhog_t), PL<R>(h->q), PL<R>(h->gq[0]), PL<R>(h->gq[1]), PL<R>(h->gq[2]));
-    TRY(check_launch(h, "trc_grad_pl"));
-    TRY(comm<R>(h, {h->gq[0], h->gq[1], h->gq[2]}));
-    TrcRemapArgs<R> ra;
-    ra.q = RG<R>(h->q); ra.gq0 = RG<R>(h->gq[0]); ra.gq1 = RG<R>(h->gq[1]); ra.gq2 = RG<R>(h->gq[2]);
-    for (int f = 0; f < 9; ++f) ra.xc[f] = RG<R>(h->xc[f]);
-    for (int f = 0; f < 6; ++f) ra.cm[f] = RG<R>(h->cm[f]);
-    for (int f = 0; f < 3; ++f) ra.qa[f] = RG<R>(h->qa[f]);
-    k_trc_remap<<<(unsigned)((D.npt2 + h->blk[TB_TRC_REMAP] - 1) / h->blk[TB_TRC_REMAP]), h->blk[TB_TRC_REMAP], 0, s>>>(ra);
-    TRY(check_launch(h, "trc_remap"));
-    TrcRemapPlArgs<R> rp;
-    rp.q = PL<R>(h->q); rp.gq0 = PL<R>(h->gq[0]); rp.gq1 = PL<R>(h->gq[1]); rp.gq2 = PL<R>(h->gq[2]); rp.xc = PL<R>(h->xc[0]);
-    rp.cm = PL<R>(h->cm[0]); rp.qa = PL<R>(h->qa[0]);
-    k_trc_remap_pl<<<pkb, 128, 0, ps>>>(rp);
-    TRY(check_launch(h, "trc_remap_pl"));
-    TrcLimArgs<R> la;
-    la.q = RG<R>(h->q); la.rhog_t = RG<R>(h->rhog_t); la.frhog = RG<R>(h->frhog);
-    for (int f = 0; f < 6; ++f) { la.ch[f] = RG<R>(h->ch[f]); la.cm[f] = RG<R>(h->cm[f]); la.flx[f] = RG<R>(h->flx[f]); }
-    for (int f = 0; f < 3; ++f) la.qa[f] = RG<R>(h->qa[f]);
-    la.qout_min = RG<R>(h->Qmin); la.qout_max = RG<R>(h->Qmax); la.Qmin = RG<R>(h->Qmin); la.Qmax = RG<R>(h->Qmax);
-    la.rhogq = RG<R>(h->Pq[iq]); la.dt = dt;
-    TrcLimPlArgs<R> lp;
-    lp.q = PL<R>(h->q); lp.ch = PL<R>(h->ch[0]); lp.cm = PL<R>(h->cm[0]); lp.rhog_t = PL<R>(h->rhog_t); lp.frhog = PL<R>(h->frhog);
-    lp.qa = PL<R>(h->qa[0]); lp.flx = PL<R>(h->flx[0]); lp.Qmin = PL<R>(h->Qmin); lp.Qmax = PL<R>(h->Qmax);
-    lp.qout_min = PL<R>(h->Qmin); lp.qout_max = PL<R>(h->Qmax); lp.rhogq = PL<R>(h->Pq[iq]); lp.dt = dt;
-    k_trc_qout<<<(unsigned)((D.npt2 + h->blk[TB_TRC_QOUT] - 1) / h->blk[TB_TRC_QOUT]), h->blk[TB_TRC_QOUT], 0, s>>>(la);
-    TRY(check_launch(h, "trc_qout"));
-    k_trc_qout_pl<<<pkb, 128, 0, ps>>>(lp);
-    TRY(check_launch(h, "trc_qout_pl"));
-    TRY(comm<R>(h, {h->Qmin, h->Qmax}));
-    k_trc_apply<<<(unsigned)((D.npt2 + h->blk[TB_TRC_APPLY] - 1) / h->blk[TB_TRC_APPLY]), h->blk[TB_TRC_APPLY], 0, s>>>(la);
-    TRY(check_launch(h, "trc_apply"));
-    k_trc_apply_pl<<<pkb, 128, 0, ps>>>(lp);
-    TRY(check_launch(h, "trc_apply_pl"));
-  }
+  for (int iq = 0; iq < D.nq; ++iq) TRY(trc_horizontal<R>(h, h->Pq[iq]));
   PHASE();
-  TRY(join_pl(h));
-  k_trc_rhog<<<(unsigned)(((D.npt2 + (long long)D.KA * D.LP) + h->blk[TB_TRC_RHOG] - 1) / h->blk[TB_TRC_RHOG]), h->blk[TB_TRC_RHOG], 0, s>>>(RG<R>(h->rhog_t), RG<R>(h->flx[0]), RG<R>(h->flx[1]), RG<R>(h->flx[2]), RG<R>(h->flx[3]), RG<R>(h->flx[4]),
-                                     RG<R>(h->flx[5]), RG<R>(h->frhog), (R)dt, PL<R>(h->flx[0]), PL<R>(h->rhog_t), PL<R>(h->frhog));
-  TRY(check_launch(h, "trc_rhog"));
-  TRY(fork_pl(h));
-  for (int iq = 0; iq < D.nq; ++iq) TRY(vadv(iq, true));
+  TRY(trc_rhog<R>(h));
+  for (int iq = 0; iq < D.nq; ++iq) TRY(trc_vadv<R>(h, h->Pq[iq], true));
   PHASE();
   if (h->trcadv) {
     // the prescribed winds of the next time (mod_forcing.py forcing_update)
@@ -1162,6 +1225,180 @@ static int f64_only(nc_handle* h, const char* what) {
   if (h->mixed) return fail(NC_ERR_STATE, std::string(what) + ": not available for a mixed-precision handle");
   return 0;
 }
+
+// ---------------------------------------------------------------------------
+// linearised tracer advection step (nc_trc_step_lin)
+// ---------------------------------------------------------------------------
+enum { LN_X0, LN_X1, LN_X2, LN_X3, LN_RHO, LN_T1, LN_T2, LN_DQ, LN_DG0, LN_DG1, LN_DG2, LN_DQA0, LN_DQA1,
+       LN_DQA2, LN_DQN, LN_DQX, LN_N };
+static int lin_buffers(nc_handle* h) {
+  if (h->lin_ready) return 0;
+  static const char* names[LN_N] = {"lin.x0", "lin.x1", "lin.x2", "lin.x3", "lin.rho", "lin.t1", "lin.t2", "lin.dq",
+                                    "lin.dg0", "lin.dg1", "lin.dg2", "lin.dqa0", "lin.dqa1", "lin.dqa2",
+                                    "lin.dqmin", "lin.dqmax"};
+  for (int n = 0; n < LN_N; ++n) TRY(field(h, h->lin[n], names[n], true));
+  h->lin_ready = true;
+  return 0;
+}
+static int copy_in(nc_handle* h, FieldPair& dst, const double* r, const double* p) {
+  CU(cudaMemcpyAsync(dst.r, r, h->D.npt * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CU(cudaMemcpyAsync(dst.p, p, h->D.npl * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  return 0;
+}
+static int copy_out(nc_handle* h, double* r, double* p, const FieldPair& src) {
+  CU(cudaMemcpyAsync(r, src.r, h->D.npt * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CU(cudaMemcpyAsync(p, src.p, h->D.npl * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  return 0;
+}
+static int zero_pair(nc_handle* h, FieldPair& f) {
+  CU(cudaMemsetAsync(f.r, 0, h->D.npt * sizeof(double), h->stream));
+  CU(cudaMemsetAsync(f.p, 0, h->D.npl * sizeof(double), h->stream));
+  return 0;
+}
+// the exchange adjoint on one field (k_comm_adj_add, then the destinations cleared)
+static int comm_adj(nc_handle* h, FieldPair& f) {
+  const long long ne = (long long)(h->nr + h->np) * h->D.KA;
+  if (ne == 0) return 0;
+  const unsigned g = (unsigned)((ne + 255) / 256);
+  k_comm_adj_add<<<g, 256, 0, h->stream>>>(f.r, f.p, h->r_dst, h->r_src, h->nr, h->p_dst, h->p_src, h->np);
+  TRY(check_launch(h, "comm_adj"));
+  k_comm_adj_clear<<<g, 256, 0, h->stream>>>(f.r, f.p, h->r_dst, h->nr, h->p_dst, h->np);
+  return check_launch(h, "comm_adj_clear");
+}
+static int vadv_lin_launch(nc_handle* h, int mode, const FieldPair& at, const FieldPair& den, const double* in_r,
+                           const double* in_p, double* out_r, double* out_p, bool second) {
+  for (int pole = 0; pole < 2; ++pole) {
+    VadvLin a{pole ? at.p : at.r, pole ? den.p : den.r, pole ? h->flx_v.p : h->flx_v.r,
+              pole ? h->frhog.p : h->frhog.r, pole ? in_p : in_r, pole ? out_p : out_r, h->dtl, 0.0,
+              second ? 1 : 0, mode};
+    const long long n = pole ? 6LL * h->D.LP : h->D.npt2;
+    k_vadv_lin<<<(unsigned)((n + 63) / 64), 64, 0, h->stream>>>(a, pole);
+    TRY(check_launch(h, "vadv_lin"));
+  }
+  return 0;
+}
+static HLin hlin_args(nc_handle* h) {
+  HLin a{};
+  FieldPair* L = h->lin;
+  a.q = h->q.r; a.Qmin = h->Qmin.r; a.Qmax = h->Qmax.r; a.rhog_t = L[LN_RHO].r; a.frhog = h->frhog.r;
+  for (int f = 0; f < 3; ++f) a.qa[f] = h->qa[f].r;
+  for (int f = 0; f < 6; ++f) { a.ch[f] = h->ch[f].r; a.cm[f] = h->cm[f].r; a.flx[f] = h->flx[f].r; }
+  for (int f = 0; f < 9; ++f) a.xc[f] = h->xc[f].r;
+  a.q_pl = h->q.p; a.qa_pl = h->qa[0].p; a.Qmin_pl = h->Qmin.p; a.Qmax_pl = h->Qmax.p; a.rhog_t_pl = L[LN_RHO].p;
+  a.frhog_pl = h->frhog.p; a.ch_pl = h->ch[0].p; a.cm_pl = h->cm[0].p; a.flx_pl = h->flx[0].p; a.xc_pl = h->xc[0].p;
+  a.dt = h->dtl;
+  a.dq = L[LN_DQ].r; a.dq_pl = L[LN_DQ].p;
+  for (int f = 0; f < 3; ++f) a.dqa[f] = L[LN_DQA0 + f].r;
+  a.dqa_pl = L[LN_DQA0].p;
+  a.dQmin = L[LN_DQN].r; a.dQmax = L[LN_DQX].r; a.dQmin_pl = L[LN_DQN].p; a.dQmax_pl = L[LN_DQX].p;
+  a.oQmin = L[LN_DQN].r; a.oQmax = L[LN_DQX].r; a.oQmin_pl = L[LN_DQN].p; a.oQmax_pl = L[LN_DQX].p;
+  a.gq = L[LN_DQ].r; a.gq_pl = L[LN_DQ].p;
+  for (int f = 0; f < 3; ++f) a.gqa[f] = L[LN_DQA0 + f].r;
+  a.gqa_pl = L[LN_DQA0].p;
+  a.gQmin = L[LN_DQN].r; a.gQmax = L[LN_DQX].r; a.gQmin_pl = L[LN_DQN].p; a.gQmax_pl = L[LN_DQX].p;
+  for (int d = 0; d < 3; ++d) { a.gg[d] = L[LN_DG0 + d].r; a.gg_pl[d] = L[LN_DG0 + d].p; }
+  return a;
+}
+
+// the forward tracer step of x0 with the fluxes of the handle's last step,
+// keeping its stages: X0 the input, X1 after the first vertical step, X2 after the
+// horizontal step (and H's q, qa, Qmin / Qmax), X3 after the second
+// vertical step; rhog_t before the horizontal update in LN_RHO
+static int trc_lin_forward(nc_handle* h, const double* x0, const double* x0_pl) {
+  FieldPair* L = h->lin;
+  TRY(trc_vflux<double>(h));
+  TRY(trc_hflux<double>(h));
+  TRY(copy_in(h, L[LN_RHO], h->rhog_t.r, h->rhog_t.p));
+  TRY(copy_in(h, L[LN_X0], x0, x0_pl));
+  TRY(copy_in(h, L[LN_X1], x0, x0_pl));
+  TRY(trc_vadv<double>(h, L[LN_X1], false));
+  TRY(copy_in(h, L[LN_X2], L[LN_X1].r, L[LN_X1].p));
+  TRY(trc_horizontal<double>(h, L[LN_X2]));
+  TRY(trc_rhog<double>(h));
+  TRY(copy_in(h, L[LN_X3], L[LN_X2].r, L[LN_X2].p));
+  return trc_vadv<double>(h, L[LN_X3], true);
+}
+
+// tangent-linear of the horizontal step at X1: T2 = H'(X1) T1
+static int hlin_tl(nc_handle* h) {
+  const Dims& D = h->D;
+  FieldPair* L = h->lin;
+  const cudaStream_t s = h->stream;
+  const unsigned pkb = (unsigned)((D.KA * D.LP + 127) / 128), cb = (unsigned)((D.npt2 + 127) / 128);
+  {
+    const dim3 gt((unsigned)D.KA, (unsigned)(((D.G - 2 + TG_DX - 1) / TG_DX) * ((D.G - 2 + TG_DY - 1) / TG_DY)),
+                  (unsigned)D.L);
+    k_trc_grad_t<<<gt, TG_DX * TG_DY, 0, s>>>(L[LN_T1].r, L[LN_RHO].r, L[LN_DQ].r, L[LN_DG0].r, L[LN_DG1].r,
+                                              L[LN_DG2].r);
+    TRY(check_launch(h, "lin_grad"));
+  }
+  k_trc_grad_pl<<<pkb, 128, 0, s>>>(L[LN_T1].p, L[LN_RHO].p, L[LN_DQ].p, L[LN_DG0].p, L[LN_DG1].p, L[LN_DG2].p);
+  TRY(check_launch(h, "lin_grad_pl"));
+  TRY(comm<double>(h, {L[LN_DG0], L[LN_DG1], L[LN_DG2]}));
+  TrcRemapArgs<double> ra;
+  ra.q = L[LN_DQ].r; ra.gq0 = L[LN_DG0].r; ra.gq1 = L[LN_DG1].r; ra.gq2 = L[LN_DG2].r;
+  for (int f = 0; f < 9; ++f) ra.xc[f] = h->xc[f].r;
+  for (int f = 0; f < 6; ++f) ra.cm[f] = h->cm[f].r;
+  for (int f = 0; f < 3; ++f) ra.qa[f] = L[LN_DQA0 + f].r;
+  k_trc_remap<<<cb, 128, 0, s>>>(ra);
+  TRY(check_launch(h, "lin_remap"));
+  TrcRemapPlArgs<double> rp;
+  rp.q = L[LN_DQ].p; rp.gq0 = L[LN_DG0].p; rp.gq1 = L[LN_DG1].p; rp.gq2 = L[LN_DG2].p; rp.xc = h->xc[0].p;
+  rp.cm = h->cm[0].p; rp.qa = L[LN_DQA0].p;
+  k_trc_remap_pl<<<pkb, 128, 0, s>>>(rp);
+  TRY(check_launch(h, "lin_remap_pl"));
+  HLin a = hlin_args(h);
+  k_hlin_qout<<<cb, 128, 0, s>>>(a, 0);
+  TRY(check_launch(h, "lin_qout"));
+  k_hlin_pole<<<pkb, 128, 0, s>>>(a, 0, 0);
+  TRY(check_launch(h, "lin_qout_pl"));
+  TRY(comm<double>(h, {L[LN_DQN], L[LN_DQX]}));
+  a.x = L[LN_T1].r; a.x_pl = L[LN_T1].p; a.y = L[LN_T2].r; a.y_pl = L[LN_T2].p;
+  k_hlin_apply<<<cb, 128, 0, s>>>(a, 0);
+  TRY(check_launch(h, "lin_apply"));
+  k_hlin_pole<<<pkb, 128, 0, s>>>(a, 0, 1);
+  return check_launch(h, "lin_apply_pl");
+}
+
+// adjoint of the horizontal step at X1: T2 = H'(X1)^T T1
+static int hlin_ad(nc_handle* h) {
+  const Dims& D = h->D;
+  FieldPair* L = h->lin;
+  const cudaStream_t s = h->stream;
+  const unsigned pkb = (unsigned)((D.KA * D.LP + 127) / 128), cb = (unsigned)((D.npt2 + 127) / 128);
+  for (int n : {LN_DQ, LN_DG0, LN_DG1, LN_DG2, LN_DQA0, LN_DQA1, LN_DQA2, LN_DQN, LN_DQX}) TRY(zero_pair(h, L[n]));
+  TRY(copy_in(h, L[LN_T2], L[LN_T1].r, L[LN_T1].p));   // y = x - ...: the direct part
+  HLin a = hlin_args(h);
+  a.x = L[LN_T1].r; a.x_pl = L[LN_T1].p;
+  a.gx = L[LN_T2].r; a.gx_pl = L[LN_T2].p;
+  k_hlin_apply<<<cb, 128, 0, s>>>(a, 1);
+  TRY(check_launch(h, "lin_apply_ad"));
+  k_hlin_pole<<<pkb, 128, 0, s>>>(a, 1, 1);
+  TRY(check_launch(h, "lin_apply_ad_pl"));
+  TRY(comm_adj(h, L[LN_DQN]));
+  TRY(comm_adj(h, L[LN_DQX]));
+  k_hlin_qout<<<cb, 128, 0, s>>>(a, 1);
+  TRY(check_launch(h, "lin_qout_ad"));
+  k_hlin_pole<<<pkb, 128, 0, s>>>(a, 1, 0);
+  TRY(check_launch(h, "lin_qout_ad_pl"));
+  k_hlin_remap_ad<<<cb, 128, 0, s>>>(a);
+  TRY(check_launch(h, "lin_remap_ad"));
+  k_hlin_pole_remap_ad<<<pkb, 128, 0, s>>>(a);
+  TRY(check_launch(h, "lin_remap_ad_pl"));
+  for (int d = 0; d < 3; ++d) TRY(comm_adj(h, L[LN_DG0 + d]));
+  k_hlin_grad_ad<<<(unsigned)((D.npt + 255) / 256), 256, 0, s>>>(a);
+  TRY(check_launch(h, "lin_grad_ad"));
+  k_hlin_pole_grad_ad<<<pkb, 128, 0, s>>>(a);
+  return check_launch(h, "lin_grad_ad_pl");
+}
+
+// lifts the pole kernels onto the library stream for the duration of a call
+struct SingleStream {
+  nc_handle* h;
+  explicit SingleStream(nc_handle* hh) : h(hh) { h->single = true; }
+  ~SingleStream() { h->single = false; }
+};
+
 
 // ---------------------------------------------------------------------------
 // C ABI
@@ -1790,6 +2027,7 @@ int nc_step(nc_handle* h, int32_t nsteps) {
   if (!h->have_state) return fail(NC_ERR_STATE, "nc_step: no state uploaded");
   TRY(load_consts(h));
   if (!h->use_graph || h->prof) {
+    h->stepped = h->stepped || nsteps > 0;
     for (int n = 0; n < nsteps; ++n) {
       if (h->prof) h->ev_used = 0;
       TRY(step_once(h));
@@ -1824,6 +2062,7 @@ int nc_step(nc_handle* h, int32_t nsteps) {
       }
     }
   }
+  h->stepped = h->stepped || nsteps > 0;
   for (int n = 0; n < nsteps; ++n) {
     CU(cudaGraphLaunch(h->gexec, h->stream));
     h->launches += h->graph_kernels;
@@ -2269,4 +2508,167 @@ int nc_divide_known(const double* x, const double* y, double* q, int64_t n, doub
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// tangent-linear and adjoint operators on caller device buffers (float64)
+// ---------------------------------------------------------------------------
+static int adj_ready(nc_handle* h, const char* what) {
+  if (!h) return fail(NC_ERR_ARG, std::string(what) + ": null handle");
+  TRY(f64_only(h, what));
+  if (h->D.KA > NC_ADJ_K)
+    return fail(NC_ERR_ARG, std::string(what) + ": kall " + std::to_string(h->D.KA) + " above the limit of " +
+                                std::to_string(NC_ADJ_K) + " levels");
+  if (h->D.kmin < 1 || h->D.kmax > h->D.KA - 2 || h->D.kmax <= h->D.kmin)
+    return fail(NC_ERR_ARG, std::string(what) + ": needs 1 <= kmin < kmax <= kall - 2");
+  return load_consts(h);
+}
+static unsigned col_blocks(const nc_handle* h, int pole, int tpb) {
+  const long long n = pole ? 6LL * h->D.LP : h->D.npt2;
+  return (unsigned)((n + tpb - 1) / tpb);
+}
+
+int nc_vsolve(nc_handle* h, int32_t pole, int32_t transpose, const double* Mc, const double* Mu, const double* Ml,
+              const double* b, double* x, const double* x_fwd, double* gMc, double* gMu, double* gMl,
+              void* stream) {
+  TRY(adj_ready(h, "nc_vsolve"));
+  if (!Mc || !Mu || !Ml || !b || !x) return fail(NC_ERR_ARG, "nc_vsolve: null pointer");
+  if (x_fwd && (!transpose || !gMc || !gMu || !gMl))
+    return fail(NC_ERR_ARG, "nc_vsolve: the matrix cotangents need transpose = 1 and gMc, gMu, gMl");
+  TriArgs a{Mc, Mu, Ml, b, x, x_fwd, gMc, gMu, gMl, transpose ? 1 : 0};
+  TRY(after_caller(h, stream));
+  k_tri_solve<<<col_blocks(h, pole, 128), 128, 0, h->stream>>>(a, pole ? 1 : 0);
+  TRY(check_launch(h, "vsolve"));
+  return before_caller(h, stream);
+}
+
+int nc_vadv_lin(nc_handle* h, int32_t pole, int32_t mode, const double* rhogq, const double* den,
+                const double* flx_v, const double* frhog, const double* in, double* out, double dt, double bcoef,
+                int32_t clamp, void* stream) {
+  TRY(adj_ready(h, "nc_vadv_lin"));
+  if (mode < 0 || mode > 2) return fail(NC_ERR_ARG, "nc_vadv_lin: mode must be 0, 1 or 2");
+  if (!rhogq || !den || !flx_v || !frhog || !out || (mode && !in)) return fail(NC_ERR_ARG, "nc_vadv_lin: null pointer");
+  VadvLin a{rhogq, den, flx_v, frhog, in, out, dt, bcoef, clamp ? 1 : 0, mode};
+  TRY(after_caller(h, stream));
+  k_vadv_lin<<<col_blocks(h, pole, 64), 64, 0, h->stream>>>(a, pole ? 1 : 0);
+  TRY(check_launch(h, "vadv_lin"));
+  return before_caller(h, stream);
+}
+
+int nc_laplacian(nc_handle* h, int32_t transpose, const double* q, const double* q_pl, double* y, double* y_pl,
+                 void* stream) {
+  TRY(adj_ready(h, "nc_laplacian"));
+  if (!q || !q_pl || !y || !y_pl) return fail(NC_ERR_ARG, "nc_laplacian: null pointer");
+  if (q == y || q_pl == y_pl) return fail(NC_ERR_ARG, "nc_laplacian: input and output must not alias");
+  const Dims& D = h->D;
+  const long long ne = (long long)(h->nr + h->np) * D.KA;
+  const unsigned gc = (unsigned)((ne + 255) / 256);
+  const unsigned gr = (unsigned)((D.npt + 255) / 256), gp = (unsigned)((D.KA * D.LP + 127) / 128);
+  TRY(after_caller(h, stream));
+  if (!transpose) {
+    if (!h->adj_work) TRY(dev_alloc(h, &h->adj_work, (size_t)D.npt + D.npl));
+    double* w = h->adj_work;
+    double* w_pl = h->adj_work + D.npt;
+    CU(cudaMemcpyAsync(w, q, (size_t)D.npt * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CU(cudaMemcpyAsync(w_pl, q_pl, (size_t)D.npl * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CommFields<double> f{};
+    f.r[0] = w;
+    f.p[0] = w_pl;
+    f.n = 1;
+    if (ne > 0) {
+      k_comm<<<gc, 256, 0, h->stream>>>(f, h->r_dst, h->r_src, h->nr, h->p_dst, h->p_src, h->np);
+      TRY(check_launch(h, "lap_comm"));
+    }
+    k_lap_fwd<<<gr, 256, 0, h->stream>>>(w, y);
+    TRY(check_launch(h, "lap"));
+    k_lap_fwd_pl<<<gp, 128, 0, h->stream>>>(w_pl, y_pl);
+    TRY(check_launch(h, "lap_pl"));
+  } else {
+    k_lap_adj<<<gr, 256, 0, h->stream>>>(q, y);
+    TRY(check_launch(h, "lap_adj"));
+    k_lap_adj_pl<<<gp, 128, 0, h->stream>>>(q_pl, y_pl);
+    TRY(check_launch(h, "lap_adj_pl"));
+    if (ne > 0) {
+      k_comm_adj_add<<<gc, 256, 0, h->stream>>>(y, y_pl, h->r_dst, h->r_src, h->nr, h->p_dst, h->p_src, h->np);
+      TRY(check_launch(h, "comm_adj"));
+      k_comm_adj_clear<<<gc, 256, 0, h->stream>>>(y, y_pl, h->r_dst, h->nr, h->p_dst, h->np);
+      TRY(check_launch(h, "comm_adj_clear"));
+    }
+  }
+  return before_caller(h, stream);
+}
+
+int nc_trc_step_lin(nc_handle* h, int32_t mode, const double* x0, const double* x0_pl, const double* in,
+                    const double* in_pl, double* out, double* out_pl, void* stream) {
+  TRY(adj_ready(h, "nc_trc_step_lin"));
+  if (mode < 0 || mode > 2) return fail(NC_ERR_ARG, "nc_trc_step_lin: mode must be 0, 1 or 2");
+  if (!x0 || !x0_pl || !out || !out_pl || (mode && (!in || !in_pl)))
+    return fail(NC_ERR_ARG, "nc_trc_step_lin: null pointer");
+  if (!h->stepped) return fail(NC_ERR_STATE, "nc_trc_step_lin: no step has run on this handle");
+  TRY(lin_buffers(h));
+  SingleStream one(h);
+  TRY(after_caller(h, stream));
+  FieldPair* L = h->lin;
+  TRY(trc_lin_forward(h, x0, x0_pl));
+  CommFields<double> cf{};
+  cf.n = 1;
+  const long long ne = (long long)(h->nr + h->np) * h->D.KA;
+  const unsigned gc = (unsigned)((ne + 255) / 256);
+  if (mode == 0) {
+    TRY(copy_out(h, out, out_pl, L[LN_X3]));
+  } else if (mode == 1) {
+    TRY(vadv_lin_launch(h, 1, L[LN_X0], h->P0[0], in, in_pl, L[LN_T1].r, L[LN_T1].p, false));
+    TRY(hlin_tl(h));
+    TRY(vadv_lin_launch(h, 1, L[LN_X2], h->rhog_t, L[LN_T2].r, L[LN_T2].p, out, out_pl, true));
+  } else {
+    TRY(copy_in(h, L[LN_T2], in, in_pl));
+    TRY(comm_adj(h, L[LN_T2]));
+    TRY(vadv_lin_launch(h, 2, L[LN_X2], h->rhog_t, L[LN_T2].r, L[LN_T2].p, L[LN_T1].r, L[LN_T1].p, true));
+    TRY(hlin_ad(h));
+    TRY(vadv_lin_launch(h, 2, L[LN_X0], h->P0[0], L[LN_T2].r, L[LN_T2].p, out, out_pl, false));
+  }
+  if (mode != 2 && ne > 0) {   // the closing exchange of PRG_var
+    cf.r[0] = out;
+    cf.p[0] = out_pl;
+    k_comm<<<gc, 256, 0, h->stream>>>(cf, h->r_dst, h->r_src, h->nr, h->p_dst, h->p_src, h->np);
+    TRY(check_launch(h, "lin_comm"));
+  }
+  return before_caller(h, stream);
+}
+
+int nc_set_time(nc_handle* h, double time) {
+  if (!h) return fail(NC_ERR_ARG, "nc_set_time: null handle");
+  if (!h->trcadv) return fail(NC_ERR_STATE, "nc_set_time: the handle has no prescribed winds (trcadv)");
+  TRY(load_consts(h));
+  CU(cudaMemcpyAsync(h->trc_time, &time, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int nc_trc_prepare(nc_handle* h) {
+  if (!h) return fail(NC_ERR_ARG, "nc_trc_prepare: null handle");
+  if (!h->trcadv) return fail(NC_ERR_STATE, "nc_trc_prepare: the handle has no prescribed winds (trcadv)");
+  if (!h->have_state) return fail(NC_ERR_STATE, "nc_trc_prepare: no state uploaded");
+  TRY(load_consts(h));
+  const Dims& D = h->D;
+  const size_t es = h->mixed ? sizeof(float) : sizeof(double);
+  const cudaStream_t s = h->stream;
+  // what a step of the offline advection does before its tracer advection:
+  // PROG0 = PROG, PROG_mean = PROG, no density tendency
+  for (int v = 0; v < 6; ++v) {
+    CU(cudaMemcpyAsync(h->P0[v].r, h->P[v].r, D.npt * es, cudaMemcpyDeviceToDevice, s));
+    CU(cudaMemcpyAsync(h->P0[v].p, h->P[v].p, D.npl * es, cudaMemcpyDeviceToDevice, s));
+  }
+  for (int v = 0; v < 5; ++v) {
+    CU(cudaMemcpyAsync(h->PM[v].r, h->P[v].r, D.npt * es, cudaMemcpyDeviceToDevice, s));
+    CU(cudaMemcpyAsync(h->PM[v].p, h->P[v].p, D.npl * es, cudaMemcpyDeviceToDevice, s));
+  }
+  CU(cudaMemsetAsync(h->frhog.r, 0, D.npt * es, s));
+  CU(cudaMemsetAsync(h->frhog.p, 0, D.npl * es, s));
+  h->stepped = true;
+  return 0;
+}
+
 }  // extern "C"
+
+
+
+

@@ -34,8 +34,8 @@ EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_sta
            "nc_upload_state_device", "nc_download_state_device", "nc_check_finite", "nc_set_block", "nc_get_block",
            "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",
            "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_forcing_step", "nc_history_vars", "nc_restart_pack",
-           "nc_restart_unpack", "nc_restart_finish", "nc_divide_known",
-           "nc_last_error", "nc_destroy")
+           "nc_restart_unpack", "nc_restart_finish", "nc_divide_known", "nc_vsolve", "nc_vadv_lin", "nc_laplacian",
+           "nc_trc_step_lin", "nc_set_time", "nc_trc_prepare", "nc_last_error", "nc_destroy")
 
 
 def load_library(path: str = LIB_PATH):
@@ -87,6 +87,14 @@ def load_library(path: str = LIB_PATH):
     lib.nc_restart_finish.argtypes = [vp, dp, i32]
     lib.nc_restart_finish.restype = ctypes.c_int
     lib.nc_divide_known.restype = ctypes.c_int
+    lib.nc_vsolve.argtypes = [vp, i32, i32] + [dp] * 9 + [vp]
+    lib.nc_vadv_lin.argtypes = [vp, i32, i32] + [dp] * 6 + [ctypes.c_double, ctypes.c_double, i32, vp]
+    lib.nc_laplacian.argtypes = [vp, i32, dp, dp, dp, dp, vp]
+    lib.nc_trc_step_lin.argtypes = [vp, i32] + [dp] * 6 + [vp]
+    lib.nc_set_time.argtypes = [vp, ctypes.c_double]
+    lib.nc_trc_prepare.argtypes = [vp]
+    for f in ("nc_vsolve", "nc_vadv_lin", "nc_laplacian", "nc_trc_step_lin", "nc_set_time", "nc_trc_prepare"):
+        getattr(lib, f).restype = ctypes.c_int
     lib.nc_destroy.argtypes = [vp]
     lib.nc_destroy.restype = None
     for f in ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_state_async", "nc_join_copies",
@@ -298,7 +306,9 @@ class NicamCuda:
         _check(lib.nc_set_graph(h, 1 if graph else 0))
         G, K, L, nq = (int(_scalar(self._tab[k])) for k in ("gall_1d", "kall", "lall", "nq"))
         self.shape = (G, G, K, L, 6 + nq)
-        self.shape_pl = (6, K, 2, 6 + nq)
+        LP = 2 * (int(_scalar(self._tab["members"])) if "members" in self._tab else 1)
+        self.shape_pl = (6, K, LP, 6 + nq)
+        self.kmin, self.kmax = int(_scalar(self._tab["kmin"])), int(_scalar(self._tab["kmax"]))
 
     # ---- state marshal (host arrays in the reference layout)
     def upload(self, prg: np.ndarray, prg_pl: np.ndarray):
@@ -352,6 +362,77 @@ class NicamCuda:
                     or not t.is_contiguous()):
                 raise ValueError(f"expected a contiguous float64 CUDA tensor of shape {shp}, got "
                                  f"{t.dtype} {tuple(t.shape)} on {t.device}")
+
+    # ---- tangent-linear / adjoint operators on device-layout tensors
+    # (regional [l][k][j][i] = shape (lall, kall, gall_1d, gall_1d), pole
+    # [g][k][lp] = shape (6, kall, 2); float64 handles only)
+    @property
+    def field_shape(self):
+        G, K, L = self.shape[0], self.shape[2], self.shape[3]
+        return (L, K, G, G)
+
+    @property
+    def field_shape_pl(self):
+        return (6, self.shape[2], self.shape_pl[2])
+
+    def _dev(self, t, pole: bool = False):
+        import torch
+        shp = self.field_shape_pl if pole else self.field_shape
+        if t is None:
+            return None
+        if not t.is_cuda or t.dtype != torch.float64 or tuple(t.shape) != shp or not t.is_contiguous():
+            raise ValueError(f"expected a contiguous float64 CUDA tensor of shape {shp}, got "
+                             f"{t.dtype} {tuple(t.shape)} on {t.device}")
+        return t.data_ptr()
+
+    def vsolve(self, Mc, Mu, Ml, b, x, pole: bool = False, transpose: bool = False, x_fwd=None, gM=None):
+        """nc_vsolve: x = M^-1 b (M^-T b with transpose); with x_fwd and
+        gM = (gMc, gMu, gMl) also the matrix cotangents"""
+        import torch
+        st = torch.cuda.current_stream(b.device).cuda_stream
+        g = gM if gM is not None else (None, None, None)
+        _check(self._lib.nc_vsolve(self._h, int(pole), int(transpose), *(self._dev(t, pole) for t in (Mc, Mu, Ml, b, x)),
+                                   self._dev(x_fwd, pole), *(self._dev(t, pole) for t in g), st))
+
+    def vadv_lin(self, mode: int, rhogq, den, flx_v, frhog, inp, out, dt: float, bcoef: float = 0.0,
+                 clamp: bool = True, pole: bool = False):
+        """nc_vadv_lin: mode 0 F(rhogq), 1 dF(inp), 2 dF^T(inp) into out"""
+        import torch
+        st = torch.cuda.current_stream(out.device).cuda_stream
+        _check(self._lib.nc_vadv_lin(self._h, int(pole), int(mode), *(self._dev(t, pole) for t in
+                                                                      (rhogq, den, flx_v, frhog, inp, out)),
+                                     float(dt), float(bcoef), int(bool(clamp)), st))
+
+    def laplacian(self, q, q_pl, y, y_pl, transpose: bool = False):
+        """nc_laplacian: y = L(C(q)), or C^T L^T q with transpose"""
+        import torch
+        st = torch.cuda.current_stream(q.device).cuda_stream
+        _check(self._lib.nc_laplacian(self._h, int(transpose), self._dev(q), self._dev(q_pl, True), self._dev(y),
+                                      self._dev(y_pl, True), st))
+
+    @property
+    def trcadv(self) -> bool:
+        return "trcadv" in self._tab and float(_scalar(self._tab["trcadv"])) != 0.0
+
+    def set_time(self, time: float):
+        """the model time of the prescribed winds of an offline-advection
+        (trcadv) handle (nc_set_time); it starts at 0 and each step adds dtl"""
+        _check(self._lib.nc_set_time(self._h, float(time)))
+
+    def trc_prepare(self):
+        """offline advection: the uploaded state's winds onto the handle as
+        its step's tracer advection reads them, without stepping
+        (nc_trc_prepare)"""
+        _check(self._lib.nc_trc_prepare(self._h))
+
+    def trc_step_lin(self, mode: int, x0, x0_pl, inp, inp_pl, out, out_pl):
+        """nc_trc_step_lin: the tracer advection of the handle's last step
+        applied to the tracer mass x0 (mode 0), its tangent-linear (1) or
+        adjoint (2) applied to inp, into out"""
+        import torch
+        st = torch.cuda.current_stream(out.device).cuda_stream
+        _check(self._lib.nc_trc_step_lin(self._h, int(mode), self._dev(x0), self._dev(x0_pl, True), self._dev(inp),
+                                         self._dev(inp_pl, True), self._dev(out), self._dev(out_pl, True), st))
 
     def set_block(self, kernel: str, threads: int):
         """threads per block of a column / point kernel (nc_set_block)"""
