@@ -888,8 +888,8 @@ static int run_step(nc_handle* h) {
       // interior cells; the exchange below fills the halo rows
       const dim3 gt((unsigned)((D.G - 2 + HD_DX - 1) / HD_DX), (unsigned)((D.G - 2 + HD_DY - 1) / HD_DY),
                     (unsigned)D.L);
-      const dim3 gl2((unsigned)D.KA, gt.x * gt.y, gt.z);
-      k_hdiff2_l<<<gl2, HD_DX * HD_DY, 0, s>>>(vin, RG<R>(h->P[0]), o2);
+      const dim3 gl2((unsigned)((D.KA + HD_NK - 1) / HD_NK), gt.x * gt.y, gt.z);
+      k_hdiff2_m<<<gl2, HD_DX * HD_DY, hdiff2_m_smem<R>(), s>>>(vin, RG<R>(h->P[0]), o2);
       TRY(check_launch(h, "hdiff2"));
     }
     k_hdiff2_pl<<<pkb, 128, 0, ps>>>(vinp, PL<R>(h->P[0]), o2p);
@@ -1515,6 +1515,10 @@ static int make_f32_geometry(nc_handle* h) {
 }
 
 static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
+  // the multi-level hyperdiffusion kernel takes more than the default 48 KB of
+  // dynamic shared memory in its float64 instance
+  CU(cudaFuncSetAttribute(k_hdiff2_m<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, hdiff2_m_smem<double>()));
+  CU(cudaFuncSetAttribute(k_hdiff2_m<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, hdiff2_m_smem<float>()));
   ArrTab T;
   for (int n = 0; n < narrays; ++n) {
     if (!arrays[n].name || !arrays[n].data) return fail(NC_ERR_ARG, "null array entry");

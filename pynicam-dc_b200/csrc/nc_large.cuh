@@ -598,6 +598,130 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, NC_MINB(R, 4, NC_F32_HDIFF2)) k
   }
 }
 
+// The same second hyperdiffusion pass with HD_NK levels per block: the
+// tile's k-independent triangle weights (intp_w, 18 planes) are staged in
+// shared memory and the cell's Laplacian and diffusion coefficients (coef_lap
+// 7, coef_diff 18) held in registers once for all of the block's levels,
+// instead of re-read from L2 at every level.  Same expressions in the same
+// order as k_hdiff2_l (same results).  Dynamic shared memory:
+// hdiff2_m_smem<R>() bytes (45 KB float, 90 KB double).
+#define HD_NK 6
+template <class R>
+constexpr int hdiff2_m_smem() {
+  return ((18 + 12) * (HD_DX + 1) * (HD_DY + 1) + 7 * (HD_DX + 2) * (HD_DY + 2)) * (int)sizeof(R);
+}
+template <class R>
+__global__ void __launch_bounds__(HD_DX * HD_DY, NC_MINB(R, 2, 4)) k_hdiff2_m(Six<R> vt, const R* rhog,
+                                                                            SixOut<R> out) {
+  constexpr int PX = HD_DX + 2, PY = HD_DY + 2, NP = PX * PY, TX = HD_DX + 1, TY = HD_DY + 1, NT = TX * TY;
+  extern __shared__ __align__(16) unsigned char hd_smem[];
+  R* s_w = reinterpret_cast<R*>(hd_smem);   // [18][NT] triangle weights
+  R* s_f = s_w + 18 * NT;                     // [6][NP] the six Laplacians
+  R* s_r = s_f + 6 * NP;                      // [NP] rhog
+  R* s_t = s_r + NP;                          // [2][6][NT] triangle values of fields 4 and 5
+  const int l = (int)blockIdx.z;
+  const int ntx = (cD.G - 2 + HD_DX - 1) / HD_DX;
+  const int i0 = 1 + ((int)blockIdx.y % ntx) * HD_DX, j0 = 1 + ((int)blockIdx.y / ntx) * HD_DY;
+  const int k0 = (int)blockIdx.x * HD_NK, k1 = min(k0 + HD_NK, cD.KA);
+  const int G = cD.G, gmax = cD.G - 2;
+  const int tid = threadIdx.x, tx = tid % HD_DX, ty = tid / HD_DX;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool own = (i <= gmax) && (j <= gmax);
+  const R Kh = CC.Kh;
+  const R kfac[2] = {CC.CVdry, CC.hdiff_fact_rho};
+  for (int p = tid; p < NT; p += blockDim.x) {
+    const int ii = i0 - 1 + p % TX, jj = j0 - 1 + p / TX;
+    const bool ok = ii <= G - 2 && jj <= G - 2;
+#pragma unroll
+    for (int m = 0; m < 18; ++m) s_w[m * NT + p] = ok ? P2(CG.intp_w, m, ii, jj, l) : R(0.0);
+  }
+  R cl[7], cd[18];
+  if (own) {
+#pragma unroll
+    for (int m = 0; m < 7; ++m) cl[m] = P2(CG.coef_lap, m, i, j, l);
+#pragma unroll
+    for (int m = 0; m < 18; ++m) cd[m] = P2(CG.coef_diff, m, i, j, l);
+  }
+  for (int k = k0; k < k1; ++k) {
+    for (int p = tid; p < NP; p += blockDim.x) {
+      const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
+      const bool ok = ii < G && jj < G;
+      const int q = ok ? ix(ii, jj, k, l) : 0;
+#pragma unroll
+      for (int n = 0; n < 6; ++n) s_f[n * NP + p] = ok ? vt.f[n][q] : R(0.0);
+      s_r[p] = ok ? rhog[q] : R(0.0);
+    }
+    __syncthreads();
+    for (int p = tid; p < NT; p += blockDim.x) {
+      const int px = p % TX, py = p / TX;
+      const int ii = i0 - 1 + px, jj = j0 - 1 + py;
+      const bool ok = ii <= G - 2 && jj <= G - 2;
+      const int ia = py * PX + px, ib = ia + 1, ic = ia + PX + 1, id = ia + PX;
+#pragma unroll
+      for (int f = 0; f < 2; ++f) {
+        const R* sf = s_f + (4 + f) * NP;
+        const R s0 = sf[ia], sip = sf[ib], sd = sf[ic], sjp = sf[id];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          R ti = R(0.0), tj = R(0.0);
+          if (ok) {
+            // weights 2c1-c2-c3, -c1+2c2-c3, -c1-c2+2c3 of the i and j triangles (k_intp_weights)
+            const R w1i = s_w[((d * 3 + 0) * 2 + 0) * NT + p], w2i = s_w[((d * 3 + 1) * 2 + 0) * NT + p];
+            const R w3i = s_w[((d * 3 + 2) * 2 + 0) * NT + p], w1j = s_w[((d * 3 + 0) * 2 + 1) * NT + p];
+            const R w2j = s_w[((d * 3 + 1) * 2 + 1) * NT + p], w3j = s_w[((d * 3 + 2) * 2 + 1) * NT + p];
+            ti = div3(w1i * s0 + w2i * sip + w3i * sd);
+            tj = div3(w1j * s0 + w2j * sd + w3j * sjp);
+          }
+          s_t[(f * 6 + d) * NT + p] = ti;
+          s_t[(f * 6 + 3 + d) * NT + p] = tj;
+        }
+      }
+    }
+    __syncthreads();
+    if (i0 == 1 && j0 == 1 && tid < 6) {   // singular-point fix of the (0,0) triangle, fields 4 and 5
+      const int f = tid / 3, d = tid % 3;
+      const R m0 = (R)CG.pntmask[l * 2 + 0], m1 = (R)CG.pntmask[l * 2 + 1];
+      s_t[(f * 6 + d) * NT] = s_t[(f * 6 + d) * NT] * m0 + s_t[(f * 6 + 3 + d) * NT + 1] * m1;
+    }
+    __syncthreads();
+    if (own) {
+      const int q = ix(i, j, k, l);
+      const int c0 = (ty + 1) * PX + (tx + 1);
+      const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        const R* sf = s_f + n * NP;
+        R v = cl[0] * sf[nb[0]];
+#pragma unroll
+        for (int m = 1; m < 7; ++m) v = v + cl[m] * sf[nb[m]];
+        out.f[n][q] = -v;
+      }
+      const int ta = (ty + 1) * TX + (tx + 1), tb = ta - 1, tc = ta - TX - 1, td = ta - TX;
+#pragma unroll
+      for (int f = 0; f < 2; ++f) {
+        auto kh = [&](int pt) { return s_r[pt] * kfac[f] * Kh; };
+        const R kh0 = kh(nb[0]);
+        const R kf1 = R(0.5) * (kh0 + kh(nb[2])), kf2 = R(0.5) * (kh0 + kh(nb[3])), kf3 = R(0.5) * (kh0 + kh(nb[4]));
+        const R kf4 = R(0.5) * (kh0 + kh(nb[5])), kf5 = R(0.5) * (kh0 + kh(nb[6])), kf6 = R(0.5) * (kh0 + kh(nb[1]));
+        R inner = R(0.0);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const R* ti = s_t + (f * 6 + d) * NT;
+          const R* tj = s_t + (f * 6 + 3 + d) * NT;
+          const R aTI = ti[ta], aTJ = tj[ta], bTI = ti[tb];
+          const R cTI = ti[tc], cTJ = tj[tc], dTJ = tj[td];
+          const R blk = kf1 * cd[d * 6 + 0] * (aTI + aTJ) + kf2 * cd[d * 6 + 1] * (aTJ + bTI) +
+                        kf3 * cd[d * 6 + 2] * (bTI + cTJ) + kf4 * cd[d * 6 + 3] * (cTJ + cTI) +
+                        kf5 * cd[d * 6 + 4] * (cTI + dTJ) + kf6 * cd[d * 6 + 5] * (dTJ + aTI);
+          inner = (d == 0) ? blk : inner + blk;
+        }
+        out.f[4 + f][q] = -inner;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 template <class R>
 __global__ void k_hdiff2_pl(Six<R> vt, const R* rhog, SixOut<R> out) {
   int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
