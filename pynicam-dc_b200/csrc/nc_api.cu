@@ -815,6 +815,8 @@ static int run_step(nc_handle* h) {
   const unsigned npt_blocks = (unsigned)((D.npt + kBlock - 1) / kBlock);
   const unsigned npl_blocks = (unsigned)((D.npl + kBlock - 1) / kBlock);
   // per-level tiled kernels: (levels kmin..kmax, tiles, regions)
+  const dim3 vagrid((unsigned)((D.kmax - D.kmin + VA_NK) / VA_NK),
+                    (unsigned)(((D.G - 2 + DD_DX - 1) / DD_DX) * ((D.G - 2 + DD_DY - 1) / DD_DY)), (unsigned)D.L);
   const dim3 lvgrid((unsigned)(D.kmax - D.kmin + 1),
                     (unsigned)(((D.G - 2 + DD_DX - 1) / DD_DX) * ((D.G - 2 + DD_DY - 1) / DD_DY)), (unsigned)D.L);
   const dim3 lvgrid_vp((unsigned)(D.kmax - D.kmin + 1),
@@ -1003,7 +1005,8 @@ static int run_step(nc_handle* h) {
         va.PM0 = F(h->PM[0]); va.PM4 = F(h->PM[4]);
         va.dt = h->dts; va.rweight = rweight; va.RovCV = RovCV;
         if (!pole) {
-          k_vimain_a_l<<<lvgrid, DD_DX * DD_DY, 0, s>>>(va);
+          if constexpr (std::is_same<R, float>::value) k_vimain_a_m<<<vagrid, DD_DX * DD_DY, 0, s>>>(va);
+          else k_vimain_a_l<<<lvgrid, DD_DX * DD_DY, 0, s>>>(va);
           TRY(check_launch(h, "vimain_a"));
           if (h->C.gam_unit) k_vi_solve<R, true><<<(unsigned)((D.npt2 + h->blk[TB_VISOLVE] - 1) / h->blk[TB_VISOLVE]), h->blk[TB_VISOLVE], 0, s>>>(va);
           else k_vi_solve<R, false><<<(unsigned)((D.npt2 + h->blk[TB_VISOLVE] - 1) / h->blk[TB_VISOLVE]), h->blk[TB_VISOLVE], 0, s>>>(va);

@@ -1059,6 +1059,77 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(NC_MINB(R, 6, NC_F32_VI
   }
 }
 
+// vi_main A with VA_NK levels per block: the cell's divergence coefficients
+// (coef_div, 21 planes) are held in registers once for all of the block's
+// levels instead of re-read from L2 at every level.  Same expressions in the
+// same order as k_vimain_a_l (same results).  Used by the float instance
+// (gl08: 6.0 -> 5.5 ms per step); the double one stays on k_vimain_a_l, which
+// is faster there (9.9 against 11.6 ms: 42 more registers cost residency).
+#define VA_NK 5
+template <class R>
+__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(NC_MINB(R, 4, 5))) k_vimain_a_m(VimainArgs<R> a) {
+  constexpr int PX = DD_DX + 2, PY = DD_DY + 2;
+  __shared__ R s_h[3][3][PY * PX];
+  const int ntx = (cD.G - 2 + DD_DX - 1) / DD_DX;
+  const int l = (int)blockIdx.z;
+  const int i0 = 1 + ((int)blockIdx.y % ntx) * DD_DX, j0 = 1 + ((int)blockIdx.y / ntx) * DD_DY;
+  const int ka = cD.kmin + (int)blockIdx.x * VA_NK, kb = min(ka + VA_NK - 1, cD.kmax);
+  const int G = cD.G, gmax = cD.G - 2;
+  const int tid = threadIdx.x, tx = tid % DD_DX, ty = tid / DD_DX;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool own = (i <= gmax) && (j <= gmax);
+  R cdv[21];
+  if (own) {
+#pragma unroll
+    for (int m = 0; m < 21; ++m) cdv[m] = P2c(CG.coef_div, m, i, j, l);
+  }
+  for (int k = ka; k <= kb; ++k) {
+    for (int p = tid; p < PX * PY; p += blockDim.x) {
+      const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
+      if (ii < G && jj < G) {
+        const int q = ix(ii, jj, k, l);
+        const R rg = gam_at_ldg(CG.RGAM, q), e = __ldg(&a.eth[q]), et = __ldg(&a.ethtot0[q]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const R dv = __ldg(&a.dvh.f[d][q]);
+          s_h[0][d][p] = dv * rg;
+          s_h[1][d][p] = (dv * e) * rg;
+          s_h[2][d][p] = ((__ldg(&a.P[1 + d][q]) + dv) * et) * rg;
+        }
+      } else {
+#pragma unroll
+        for (int f = 0; f < 3; ++f)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) s_h[f][d][p] = R(0.0);
+      }
+    }
+    __syncthreads();
+    if (own) {
+      const int c0 = (ty + 1) * PX + (tx + 1);
+      const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
+      const int q = ix(i, j, k, l);
+      R acc[3][3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        R sv[3] = {R(0.0), R(0.0), R(0.0)};
+#pragma unroll
+        for (int m = 0; m < 7; ++m) {
+#pragma unroll
+          for (int f = 0; f < 3; ++f) {
+            const R t = cdv[d * 7 + m] * s_h[f][d][nb[m]];
+            sv[f] = (m == 0) ? t : sv[f] + t;
+          }
+        }
+#pragma unroll
+        for (int f = 0; f < 3; ++f) acc[f][d] = sv[f];
+      }
+#pragma unroll
+      for (int f = 0; f < 3; ++f) a.hdiv[f][q] = acc[f][0] + acc[f][1] + acc[f][2];
+    }
+    __syncthreads();
+  }
+}
+
 // One pole column of vi_main.  In the mixed form the flux convergences and
 // the energy update run in float32 (R) and the tridiagonal solve in float64,
 // as in the regional kernels k_vi_solve / k_vi_energy_p.
