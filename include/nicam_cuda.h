@@ -353,6 +353,19 @@ int nc_vadv_lin(nc_handle* h, int32_t pole, int32_t mode, const double* rhogq, c
 int nc_laplacian(nc_handle* h, int32_t transpose, const double* q, const double* q_pl, double* y, double* y_pl,
                  void* stream);
 
+/* nc_divergence: y = D(C(v)), the halo exchange of the three components
+ * then the divergence of kernels/fluxconv.py:52-108 (OPRT_divergence) on the
+ * interior cells and the pole points (other cells of y zero); v holds the
+ * three components one after the other (3 x lall*kall*gall_1d^2 regional,
+ * 3 x 6*kall*2 pole values).  transpose = 1 reads y and writes v = C^T D^T y.
+ * nc_gradient: g = Grad(C(q)) (kernels/oprtgradient.py:45-88,
+ * OPRT_gradient), g the three components one after the other; transpose = 1
+ * reads g and writes q = C^T Grad^T g.  The buffer written must not alias the
+ * one read.  The forward forms allocate a scratch copy in the handle on their
+ * first call; the adjoints add with atomics (last bits may vary). */
+int nc_divergence(nc_handle* h, int32_t transpose, double* v, double* v_pl, double* y, double* y_pl, void* stream);
+int nc_gradient(nc_handle* h, int32_t transpose, double* q, double* q_pl, double* g, double* g_pl, void* stream);
+
 /* nc_trc_step_lin: the tracer advection of one step (mod_src_tracer.py:
  * 83-1228 as the step runs it: vertical step, horizontal step with the
  * MIURA2004 face values and the horizontal Thuburn limiter of 2190-2605,

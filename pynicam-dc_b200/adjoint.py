@@ -18,6 +18,10 @@ fields of shape (lall, kall, gall_1d, gall_1d), pole fields (6, kall, 2).
 * ``Laplacian`` -- halo exchange then the hexagonal Laplacian
   (kernels/oprtlaplacian.py:41-70), linear; the adjoint runs the transposed
   stencil and adds each halo value back into its exchange source.
+* ``Divergence`` / ``Gradient`` -- halo exchange then OPRT_divergence
+  (kernels/fluxconv.py:52-108) / OPRT_gradient (kernels/oprtgradient.py:
+  45-88), linear, adjoints as for the Laplacian (``nc_divergence``,
+  ``nc_gradient``).
 
 * ``TracerStep`` -- the whole tracer advection of a step
   (mod_src_tracer.py:83-1228: vertical step, horizontal step with the
@@ -170,6 +174,72 @@ class Laplacian(torch.autograd.Function):
         y, y_pl = torch.empty_like(dq), torch.empty_like(dq_pl)
         core.laplacian(dq, dq_pl, y, y_pl)
         return y, y_pl
+
+
+class Divergence(torch.autograd.Function):
+    """(y, y_pl) = D(C(v, v_pl)): halo exchange of the three components then
+    the divergence (kernels/fluxconv.py:52-108); v of shape (3, lall, kall,
+    g, g), v_pl (3, 6, kall, LP)"""
+
+    @staticmethod
+    def forward(ctx, core, v, v_pl):
+        v, v_pl = _c(v), _c(v_pl)
+        y = torch.empty(core.field_shape, dtype=torch.float64, device=v.device)
+        y_pl = torch.empty(core.field_shape_pl, dtype=torch.float64, device=v.device)
+        core.divergence(v, v_pl, y, y_pl)
+        ctx.core = core
+        return y, y_pl
+
+    @staticmethod
+    def backward(ctx, gy, gy_pl):
+        core = ctx.core
+        gy = torch.zeros(core.field_shape, dtype=torch.float64, device="cuda") if gy is None else _c(gy)
+        gy_pl = torch.zeros(core.field_shape_pl, dtype=torch.float64, device="cuda") if gy_pl is None else _c(gy_pl)
+        gv = torch.empty((3,) + core.field_shape, dtype=torch.float64, device=gy.device)
+        gv_pl = torch.empty((3,) + core.field_shape_pl, dtype=torch.float64, device=gy.device)
+        core.divergence(gv, gv_pl, gy, gy_pl, transpose=True)
+        return None, gv, gv_pl
+
+    @staticmethod
+    def jvp(ctx, _core, dv, dv_pl):
+        return Divergence.forward(ctx, ctx.core, dv, dv_pl)
+
+
+class Gradient(torch.autograd.Function):
+    """(g, g_pl) = Grad(C(q, q_pl)): halo exchange then the gradient
+    (kernels/oprtgradient.py:45-88); g of shape (3, lall, kall, g, g)"""
+
+    @staticmethod
+    def forward(ctx, core, q, q_pl):
+        q, q_pl = _c(q), _c(q_pl)
+        g = torch.empty((3,) + core.field_shape, dtype=torch.float64, device=q.device)
+        g_pl = torch.empty((3,) + core.field_shape_pl, dtype=torch.float64, device=q.device)
+        core.gradient(q, q_pl, g, g_pl)
+        ctx.core = core
+        return g, g_pl
+
+    @staticmethod
+    def backward(ctx, gg, gg_pl):
+        core = ctx.core
+        gg = torch.zeros((3,) + core.field_shape, dtype=torch.float64, device="cuda") if gg is None else _c(gg)
+        gg_pl = (torch.zeros((3,) + core.field_shape_pl, dtype=torch.float64, device="cuda") if gg_pl is None
+                 else _c(gg_pl))
+        gq = torch.empty(core.field_shape, dtype=torch.float64, device=gg.device)
+        gq_pl = torch.empty(core.field_shape_pl, dtype=torch.float64, device=gg.device)
+        core.gradient(gq, gq_pl, gg, gg_pl, transpose=True)
+        return None, gq, gq_pl
+
+    @staticmethod
+    def jvp(ctx, _core, dq, dq_pl):
+        return Gradient.forward(ctx, ctx.core, dq, dq_pl)
+
+
+def divergence(core, v, v_pl):
+    return Divergence.apply(core, v, v_pl)
+
+
+def gradient(core, q, q_pl):
+    return Gradient.apply(core, q, q_pl)
 
 
 class TracerStep(torch.autograd.Function):

@@ -755,4 +755,111 @@ __global__ void k_hlin_pole_grad_ad(HLin a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// divergence (kernels/fluxconv.py:52-108) and gradient
+// (kernels/oprtgradient.py:45-88) after the halo exchange, and their
+// adjoints.  Three-component fields are stored one component after the other
+// (3 x npt regional, 3 x npl pole values).
+// ---------------------------------------------------------------------------
+__global__ void k_div_fwd(const double* v, double* y) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.npti) return;
+  const int G = cD.G, KA = cD.KA, n = cD.npti;
+  const int i = t % G, j = (t / G) % G, k = (t / (G * G)) % KA, l = t / (G * G * KA);
+  double r = 0.0;
+  if (interior(i, j))
+    r = div7<double>(i, j, k, l, [&](int ii, int jj, int kk, int d) { return v[d * n + ix(ii, jj, kk, l)]; });
+  y[t] = r;
+}
+__global__ void k_div_fwd_pl(const double* v, double* y) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.KA * cD.LP) return;
+  const int k = t / cD.LP, lp = t % cD.LP, np = cD.npl;
+  double row = 0.0;
+  for (int g = 0; g < 6; ++g) {
+    const int q = ipl(g, k, lp);
+    const double* cd = cG.coef_div_pl + (g * cD.LP + lp) * 3;
+    const double pv = cd[0] * v[q] + cd[1] * v[np + q] + cd[2] * v[2 * np + q];
+    row = (g == 0) ? pv : row + pv;
+  }
+  y[ipl(0, k, lp)] = row;
+  for (int g = 1; g < 6; ++g) y[ipl(g, k, lp)] = 0.0;
+}
+// v-bar_d at every cell: the interior cells s whose stencil point m it is
+__global__ void k_div_adj(const double* y, double* v) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.npti) return;
+  const int G = cD.G, KA = cD.KA, n = cD.npti;
+  const int i = t % G, j = (t / G) % G, k = (t / (G * G)) % KA, l = t / (G * G * KA);
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int m = 0; m < 7; ++m) {
+    const int si = i - kNbI[m], sj = j - kNbJ[m];
+    if (si >= 1 && sj >= 1 && si <= G - 2 && sj <= G - 2) {
+      const double ys = y[ix(si, sj, k, l)];
+      for (int d = 0; d < 3; ++d) acc[d] += P2(cG.coef_div, d * 7 + m, si, sj, l) * ys;
+    }
+  }
+  for (int d = 0; d < 3; ++d) v[d * n + t] = acc[d];
+}
+__global__ void k_div_adj_pl(const double* y, double* v) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.KA * cD.LP) return;
+  const int k = t / cD.LP, lp = t % cD.LP, np = cD.npl;
+  const double y0 = y[ipl(0, k, lp)];
+  for (int g = 0; g < 6; ++g) {
+    const int q = ipl(g, k, lp);
+    const double* cd = cG.coef_div_pl + (g * cD.LP + lp) * 3;
+    for (int d = 0; d < 3; ++d) v[d * np + q] = cd[d] * y0;
+  }
+}
+__global__ void k_grad_fwd(const double* q, double* gr) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.npti) return;
+  const int G = cD.G, KA = cD.KA, n = cD.npti;
+  const int i = t % G, j = (t / G) % G, k = (t / (G * G)) % KA, l = t / (G * G * KA);
+  double o[3] = {0.0, 0.0, 0.0};
+  if (interior(i, j)) grad7<double>(i, j, k, l, [&](int ii, int jj, int kk) { return q[ix(ii, jj, kk, l)]; }, o);
+  for (int d = 0; d < 3; ++d) gr[d * n + t] = o[d];
+}
+__global__ void k_grad_fwd_pl(const double* q, double* gr) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.KA * cD.LP) return;
+  const int k = t / cD.LP, lp = t % cD.LP, np = cD.npl;
+  for (int d = 0; d < 3; ++d) {
+    double row = 0.0;
+    for (int g = 0; g < 6; ++g) {
+      const double tv = cG.coef_grad_pl[(g * cD.LP + lp) * 3 + d] * q[ipl(g, k, lp)];
+      row = (g == 0) ? tv : row + tv;
+    }
+    gr[d * np + ipl(0, k, lp)] = row;
+    for (int g = 1; g < 6; ++g) gr[d * np + ipl(g, k, lp)] = 0.0;
+  }
+}
+__global__ void k_grad_adj(const double* gr, double* q) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.npti) return;
+  const int G = cD.G, KA = cD.KA, n = cD.npti;
+  const int i = t % G, j = (t / G) % G, k = (t / (G * G)) % KA, l = t / (G * G * KA);
+  double acc = 0.0;
+  for (int m = 0; m < 7; ++m) {
+    const int si = i - kNbI[m], sj = j - kNbJ[m];
+    if (si >= 1 && sj >= 1 && si <= G - 2 && sj <= G - 2) {
+      const int ps = ix(si, sj, k, l);
+      for (int d = 0; d < 3; ++d) acc += P2(cG.coef_grad, d * 7 + m, si, sj, l) * gr[d * n + ps];
+    }
+  }
+  q[t] = acc;
+}
+__global__ void k_grad_adj_pl(const double* gr, double* q) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.KA * cD.LP) return;
+  const int k = t / cD.LP, lp = t % cD.LP, np = cD.npl;
+  const int p0 = ipl(0, k, lp);
+  for (int g = 0; g < 6; ++g) {
+    double acc = 0.0;
+    for (int d = 0; d < 3; ++d) acc += cG.coef_grad_pl[(g * cD.LP + lp) * 3 + d] * gr[d * np + p0];
+    q[ipl(g, k, lp)] = acc;
+  }
+}
+
 }  // namespace nc

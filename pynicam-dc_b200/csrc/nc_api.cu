@@ -393,6 +393,7 @@ struct nc_handle {
   cudaEvent_t ev_user = nullptr;   // ordering against a caller's stream (device-pointer marshal)
   double *stage_out = nullptr, *stage_out_pl = nullptr;
   double* adj_work = nullptr;   // exchanged copy of the Laplacian's input (allocated on first use)
+  double* adj_work3 = nullptr;  // exchanged copy of the divergence's three components (first use)
   // linearised tracer step (nc_trc_step_lin): work fields allocated on first use
   FieldPair lin[20];
   bool lin_ready = false;
@@ -2674,7 +2675,88 @@ int nc_trc_prepare(nc_handle* h) {
   return 0;
 }
 
+// the exchange (forward) or its adjoint on nf fields stored one after the other
+static int comm_fields(nc_handle* h, double* r, double* p, int nf, bool adjoint) {
+  const Dims& D = h->D;
+  const long long ne = (long long)(h->nr + h->np) * D.KA;
+  if (ne == 0) return 0;
+  const unsigned gc = (unsigned)((ne + 255) / 256);
+  for (int f = 0; f < nf; ++f) {
+    double* rf = r + (size_t)f * D.npt;
+    double* pf = p + (size_t)f * D.npl;
+    if (!adjoint) {
+      CommFields<double> cf{};
+      cf.r[0] = rf;
+      cf.p[0] = pf;
+      cf.n = 1;
+      k_comm<<<gc, 256, 0, h->stream>>>(cf, h->r_dst, h->r_src, h->nr, h->p_dst, h->p_src, h->np);
+      TRY(check_launch(h, "op_comm"));
+    } else {
+      k_comm_adj_add<<<gc, 256, 0, h->stream>>>(rf, pf, h->r_dst, h->r_src, h->nr, h->p_dst, h->p_src, h->np);
+      TRY(check_launch(h, "op_comm_adj"));
+      k_comm_adj_clear<<<gc, 256, 0, h->stream>>>(rf, pf, h->r_dst, h->nr, h->p_dst, h->np);
+      TRY(check_launch(h, "op_comm_adj_clear"));
+    }
+  }
+  return 0;
+}
+
+int nc_divergence(nc_handle* h, int32_t transpose, double* v, double* v_pl, double* y, double* y_pl, void* stream) {
+  TRY(adj_ready(h, "nc_divergence"));
+  if (!v || !v_pl || !y || !y_pl) return fail(NC_ERR_ARG, "nc_divergence: null pointer");
+  const Dims& D = h->D;
+  const unsigned gr = (unsigned)((D.npt + 255) / 256), gp = (unsigned)((D.KA * D.LP + 127) / 128);
+  TRY(after_caller(h, stream));
+  if (!transpose) {
+    if (!h->adj_work3) TRY(dev_alloc(h, &h->adj_work3, 3 * ((size_t)D.npt + D.npl)));
+    double* w = h->adj_work3;
+    double* w_pl = w + 3 * (size_t)D.npt;
+    CU(cudaMemcpyAsync(w, v, 3 * D.npt * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CU(cudaMemcpyAsync(w_pl, v_pl, 3 * (size_t)D.npl * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    TRY(comm_fields(h, w, w_pl, 3, false));
+    k_div_fwd<<<gr, 256, 0, h->stream>>>(w, y);
+    TRY(check_launch(h, "div"));
+    k_div_fwd_pl<<<gp, 128, 0, h->stream>>>(w_pl, y_pl);
+    TRY(check_launch(h, "div_pl"));
+  } else {
+    k_div_adj<<<gr, 256, 0, h->stream>>>(y, v);
+    TRY(check_launch(h, "div_adj"));
+    k_div_adj_pl<<<gp, 128, 0, h->stream>>>(y_pl, v_pl);
+    TRY(check_launch(h, "div_adj_pl"));
+    TRY(comm_fields(h, v, v_pl, 3, true));
+  }
+  return before_caller(h, stream);
+}
+
+int nc_gradient(nc_handle* h, int32_t transpose, double* q, double* q_pl, double* g, double* g_pl, void* stream) {
+  TRY(adj_ready(h, "nc_gradient"));
+  if (!q || !q_pl || !g || !g_pl) return fail(NC_ERR_ARG, "nc_gradient: null pointer");
+  const Dims& D = h->D;
+  const unsigned gr = (unsigned)((D.npt + 255) / 256), gp = (unsigned)((D.KA * D.LP + 127) / 128);
+  TRY(after_caller(h, stream));
+  if (!transpose) {
+    if (!h->adj_work) TRY(dev_alloc(h, &h->adj_work, (size_t)D.npt + D.npl));
+    double* w = h->adj_work;
+    double* w_pl = w + D.npt;
+    CU(cudaMemcpyAsync(w, q, D.npt * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CU(cudaMemcpyAsync(w_pl, q_pl, (size_t)D.npl * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    TRY(comm_fields(h, w, w_pl, 1, false));
+    k_grad_fwd<<<gr, 256, 0, h->stream>>>(w, g);
+    TRY(check_launch(h, "grad"));
+    k_grad_fwd_pl<<<gp, 128, 0, h->stream>>>(w_pl, g_pl);
+    TRY(check_launch(h, "grad_pl"));
+  } else {
+    k_grad_adj<<<gr, 256, 0, h->stream>>>(g, q);
+    TRY(check_launch(h, "grad_adj"));
+    k_grad_adj_pl<<<gp, 128, 0, h->stream>>>(g_pl, q_pl);
+    TRY(check_launch(h, "grad_adj_pl"));
+    TRY(comm_fields(h, q, q_pl, 1, true));
+  }
+  return before_caller(h, stream);
+}
+
 }  // extern "C"
+
 
 
 

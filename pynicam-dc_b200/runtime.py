@@ -35,7 +35,7 @@ EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_sta
            "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",
            "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_forcing_step", "nc_history_vars", "nc_restart_pack",
            "nc_restart_unpack", "nc_restart_finish", "nc_divide_known", "nc_vsolve", "nc_vadv_lin", "nc_laplacian",
-           "nc_trc_step_lin", "nc_set_time", "nc_trc_prepare", "nc_last_error", "nc_destroy")
+           "nc_trc_step_lin", "nc_set_time", "nc_trc_prepare", "nc_divergence", "nc_gradient", "nc_last_error", "nc_destroy")
 
 
 def load_library(path: str = LIB_PATH):
@@ -93,7 +93,10 @@ def load_library(path: str = LIB_PATH):
     lib.nc_trc_step_lin.argtypes = [vp, i32] + [dp] * 6 + [vp]
     lib.nc_set_time.argtypes = [vp, ctypes.c_double]
     lib.nc_trc_prepare.argtypes = [vp]
-    for f in ("nc_vsolve", "nc_vadv_lin", "nc_laplacian", "nc_trc_step_lin", "nc_set_time", "nc_trc_prepare"):
+    lib.nc_divergence.argtypes = [vp, i32, dp, dp, dp, dp, vp]
+    lib.nc_gradient.argtypes = [vp, i32, dp, dp, dp, dp, vp]
+    for f in ("nc_vsolve", "nc_vadv_lin", "nc_laplacian", "nc_trc_step_lin", "nc_set_time", "nc_trc_prepare",
+              "nc_divergence", "nc_gradient"):
         getattr(lib, f).restype = ctypes.c_int
     lib.nc_destroy.argtypes = [vp]
     lib.nc_destroy.restype = None
@@ -375,9 +378,11 @@ class NicamCuda:
     def field_shape_pl(self):
         return (6, self.shape[2], self.shape_pl[2])
 
-    def _dev(self, t, pole: bool = False):
+    def _dev(self, t, pole: bool = False, comps: int = 0):
         import torch
         shp = self.field_shape_pl if pole else self.field_shape
+        if comps:
+            shp = (comps,) + shp
         if t is None:
             return None
         if not t.is_cuda or t.dtype != torch.float64 or tuple(t.shape) != shp or not t.is_contiguous():
@@ -418,6 +423,22 @@ class NicamCuda:
         """the model time of the prescribed winds of an offline-advection
         (trcadv) handle (nc_set_time); it starts at 0 and each step adds dtl"""
         _check(self._lib.nc_set_time(self._h, float(time)))
+
+    def divergence(self, v, v_pl, y, y_pl, transpose: bool = False):
+        """nc_divergence: y = D(C(v)) (v of shape (3,) + field shape), or
+        v = C^T D^T y with transpose"""
+        import torch
+        st = torch.cuda.current_stream(y.device).cuda_stream
+        _check(self._lib.nc_divergence(self._h, int(transpose), self._dev(v, comps=3), self._dev(v_pl, True, 3),
+                                       self._dev(y), self._dev(y_pl, True), st))
+
+    def gradient(self, q, q_pl, g, g_pl, transpose: bool = False):
+        """nc_gradient: g = Grad(C(q)) (g of shape (3,) + field shape), or
+        q = C^T Grad^T g with transpose"""
+        import torch
+        st = torch.cuda.current_stream(q.device).cuda_stream
+        _check(self._lib.nc_gradient(self._h, int(transpose), self._dev(q), self._dev(q_pl, True),
+                                     self._dev(g, comps=3), self._dev(g_pl, True, 3), st))
 
     def trc_prepare(self):
         """offline advection: the uploaded state's winds onto the handle as

@@ -1,5 +1,5 @@
 """Tangent-linear and adjoint operators (adjoint.py, nc_vsolve / nc_vadv_lin /
-nc_laplacian) on the device, float64.
+nc_laplacian / nc_divergence / nc_gradient) on the device, float64.
 
 The operators' inputs come from a real step: the balanced-jet case at grid
 level 4 with 40 layers is stepped once and the handle's implicit matrix
@@ -11,7 +11,8 @@ positive field with seeded noise (no ties for the limiter's min / max).
 
 * forward parity: the vertical advection step equals the oracle's
   (mod_src_tracer.py:389-533 with the limiter of 1909-2074) bit for bit, the
-  exchange + Laplacian equals the oracle's comm + laplacian bit for bit, and
+  exchange + Laplacian / divergence / gradient equal the oracle's comm +
+  laplacian / divergence / gradient bit for bit, and
   the tridiagonal solve equals a banded solve to 1e-12;
 * dot-product tests <TL x, y> = <x, AD y> to 1e-12 (relative to the
   magnitudes of the products) for every operator, regional and pole;
@@ -187,6 +188,42 @@ def test_vertical_solve_equals_banded_solve(gl04):
         assert np.all(xx[i, j, :kmin + 1, l] == 0) and np.all(xx[i, j, kmax + 1:, l] == 0)
 
 
+def _three(f, seed):
+    import torch
+    v = torch.stack([f["rhogq"] * (1.0 + 0.1 * n) + 1e-4 * _rand_like(f["rhogq"], seed + n) for n in range(3)])
+    v_pl = torch.stack([f["rhogq_pl"] * (1.0 + 0.1 * n) for n in range(3)])
+    return v.contiguous(), v_pl.contiguous()
+
+
+def test_divergence_and_gradient_equal_oracle(gl04):
+    from oracle import nicam_step as O
+    import torch
+    _, adj = _mods()
+    geo, core, f = gl04
+    G = O.Geo(geo)
+    v, v_pl = _three(f, 30)
+    y = torch.empty(core.field_shape, dtype=torch.float64, device="cuda")
+    y_pl = torch.empty(core.field_shape_pl, dtype=torch.float64, device="cuda")
+    core.divergence(v, v_pl, y, y_pl)
+    comps = []
+    for n in range(3):
+        a, a_pl = adj.from_device_layout(v[n]), v_pl[n].cpu().numpy()
+        O.comm1(G, a, a_pl)
+        comps.append((a, a_pl))
+    assert np.array_equal(adj.from_device_layout(y), O.divergence(G, *[c[0] for c in comps]))
+    assert np.array_equal(y_pl.cpu().numpy(), O.divergence_pl(G, *[c[1] for c in comps]))
+    q, q_pl = f["rhogq"], f["rhogq_pl"]
+    g = torch.empty((3,) + core.field_shape, dtype=torch.float64, device="cuda")
+    g_pl = torch.empty((3,) + core.field_shape_pl, dtype=torch.float64, device="cuda")
+    core.gradient(q, q_pl, g, g_pl)
+    a, a_pl = adj.from_device_layout(q), q_pl.cpu().numpy()
+    O.comm1(G, a, a_pl)
+    want, want_pl = O.gradient(G, a), O.gradient_pl(G, a_pl)
+    for d in range(3):
+        assert np.array_equal(adj.from_device_layout(g[d]), want[..., d]), d
+        assert np.array_equal(g_pl[d].cpu().numpy(), want_pl[..., d]), d
+
+
 # ---------------------------------------------------------------- dot-product tests
 @pytest.mark.parametrize("pole", [False, True])
 def test_dot_product_vertical_advection(gl04, pole):
@@ -217,6 +254,31 @@ def test_dot_product_laplacian(gl04):
     rhs = _dot(x, ad) + _dot(x_pl, ad_pl)
     scale = float((tl * y).abs().sum() + (tl_pl * y_pl).abs().sum())
     assert _dot_rel(lhs, rhs, scale) <= 1e-12, (lhs, rhs)
+
+
+def test_dot_product_divergence_and_gradient(gl04):
+    """through autograd: forward-mode (the forward stencil on the tangent)
+    against reverse-mode (the transposed stencil and the exchange's adjoint)"""
+    import torch
+    import torch.autograd.forward_ad as fwAD
+    _, adj = _mods()
+    _, core, f = gl04
+    v, v_pl = _three(f, 31)
+    dv, dv_pl = _rand_like(v, 32), _rand_like(v_pl, 33)
+    q, q_pl = f["rhogq"], f["rhogq_pl"]
+    dq, dq_pl = _rand_like(q, 34), _rand_like(q_pl, 35)
+    for op, x, x_pl, d, d_pl in ((adj.divergence, v, v_pl, dv, dv_pl), (adj.gradient, q, q_pl, dq, dq_pl)):
+        with fwAD.dual_level():
+            y, y_pl = op(core, fwAD.make_dual(x, d), fwAD.make_dual(x_pl, d_pl))
+            tl, tl_pl = fwAD.unpack_dual(y).tangent, fwAD.unpack_dual(y_pl).tangent
+        xs, xs_pl = x.clone().requires_grad_(True), x_pl.clone().requires_grad_(True)
+        y, y_pl = op(core, xs, xs_pl)
+        w, w_pl = _rand_like(y, 36), _rand_like(y_pl, 37)
+        gx, gx_pl = torch.autograd.grad((y, y_pl), (xs, xs_pl), (w, w_pl))
+        lhs = _dot(tl, w) + _dot(tl_pl, w_pl)
+        rhs = _dot(d, gx) + _dot(d_pl, gx_pl)
+        scale = float((tl * w).abs().sum() + (tl_pl * w_pl).abs().sum())
+        assert _dot_rel(lhs, rhs, scale) <= 1e-12, (op.__name__, lhs, rhs)
 
 
 @pytest.mark.parametrize("pole", [False, True])
