@@ -139,10 +139,6 @@ int nc_set_graph(nc_handle* h, int32_t enable);
 int nc_set_block(nc_handle* h, const char* kernel, int32_t threads);
 int nc_get_block(nc_handle* h, const char* kernel, int32_t* threads);
 
-/* Debugging aid: run only the first nphases phases of one large step
- * (phase boundaries sit after each halo exchange / kernel group, in the order
- * of Dyn.dynamics_step), without graph capture, then synchronize. */
-int nc_run_phases(nc_handle* h, int32_t nphases);
 
 /* Wait for the handle's streams (steps, uploads and downloads). */
 int nc_sync(nc_handle* h);
@@ -153,12 +149,6 @@ int nc_sync(nc_handle* h);
  * Float64 with compensated (Neumaier) summation on the device. */
 int nc_mass_sums(nc_handle* h, double* out, int32_t nout);
 
-/* Copy a named device work field to host in the reference layout
- * (regional (i,j,k,l), pole (g,k,l)).  Names are those registered by
- * nc_create: the state ("RHOG", "RHOGVX", .., "RHOGQ.<n>") and the work
- * fields of the step (e.g. "rho", "pre", "eth", "gT0.<n>", "Mc").  Returns
- * NC_ERR_ARG for an unknown name.  Debugging and parity tests only. */
-int nc_get_field(nc_handle* h, const char* name, double* host_reg, double* host_pl);
 
 /* Device pointers of the resident state, for callers that keep the state in
  * their own device memory pipeline: field v (0..5 PROG, 6.. tracers) regional
@@ -292,19 +282,6 @@ int nc_restart_finish(nc_handle* h, const int64_t* pole_src, int32_t nsrc);
 int nc_history_vars(nc_handle* h, const int32_t* items, int32_t nitems, int64_t nstep, double dt,
                     double* const* out);
 
-/* Self-check of the divisions the kernels use in place of a general division
- * (the reference divides with numpy's IEEE division, e.g.
- * kernels/horizontalizevec.py:51-54, kernels/oprtdiffusion.py, kernels/diag.py,
- * mod_src_tracer.py): a quotient formed from RN(1/b) and a tail with three
- * fused multiply-adds and a multiply.  With y NULL every x[i] is divided by the
- * constant b (reciprocal pair set on the host, as for rscale and 3); otherwise
- * x[i] is divided by y[i] with the pair formed on the device from the
- * correctly rounded reciprocal (as for the density that the diagnostics and
- * the tracer Courant numbers divide by).  Copies the n host doubles in, writes q, copies it
- * back (synchronous).  For finite operands with a normal-range quotient the
- * bits equal the IEEE quotient; the tests compare them.  0 <= n <= 2^28; with
- * y NULL, b finite and nonzero; else NC_ERR_ARG. */
-int nc_divide_known(const double* x, const double* y, double* q, int64_t n, double b);
 
 /* Tangent-linear and adjoint operators of the step, for differentiation
  * (the reference differentiates its jax backend with jax.vjp; these are the
@@ -408,5 +385,8 @@ void nc_destroy(nc_handle* h);
 #ifdef __cplusplus
 }
 #endif
+
+/* Test and debugging hooks (nc_run_phases, nc_get_field, nc_divide_known)
+ * are declared in nicam_cuda_debug.h. */
 
 #endif /* NICAM_CUDA_H */

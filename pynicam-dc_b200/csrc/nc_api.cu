@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/nicam_cuda.h"
+#include "../../include/nicam_cuda_debug.h"
 
 #include "nc_forcing.cuh"
 #include "nc_tracer.cuh"

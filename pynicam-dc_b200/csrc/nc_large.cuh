@@ -605,7 +605,9 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, NC_MINB(R, 4, NC_F32_HDIFF2)) k
 // instead of re-read from L2 at every level.  Same expressions in the same
 // order as k_hdiff2_l (same results).  Dynamic shared memory:
 // hdiff2_m_smem<R>() bytes (45 KB float, 90 KB double).
+#ifndef HD_NK
 #define HD_NK 6
+#endif
 template <class R>
 constexpr int hdiff2_m_smem() {
   return ((18 + 12) * (HD_DX + 1) * (HD_DY + 1) + 7 * (HD_DX + 2) * (HD_DY + 2)) * (int)sizeof(R);

@@ -1065,7 +1065,9 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(NC_MINB(R, 6, NC_F32_VI
 // same order as k_vimain_a_l (same results).  Used by the float instance
 // (gl08: 6.0 -> 5.5 ms per step); the double one stays on k_vimain_a_l, which
 // is faster there (9.9 against 11.6 ms: 42 more registers cost residency).
+#ifndef VA_NK
 #define VA_NK 5
+#endif
 template <class R>
 __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(NC_MINB(R, 4, 5))) k_vimain_a_m(VimainArgs<R> a) {
   constexpr int PX = DD_DX + 2, PY = DD_DY + 2;

@@ -29,7 +29,7 @@ class NcArray(ctypes.Structure):
 
 _lib = None
 
-# every entry point declared in include/nicam_cuda.h
+# every entry point declared in include/nicam_cuda.h and include/nicam_cuda_debug.h
 EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_state_async", "nc_join_copies",
            "nc_upload_state_device", "nc_download_state_device", "nc_check_finite", "nc_set_block", "nc_get_block",
            "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",

@@ -1,5 +1,6 @@
 """The C-ABI library: builds for sm_100a, loads, exports every entry point
-declared in include/nicam_cuda.h (no compute call without a GPU)."""
+declared in include/*.h (the drop-in surface nicam_cuda.h and the test hooks
+of nicam_cuda_debug.h; no compute call without a GPU)."""
 import ctypes
 import os
 import re
@@ -10,7 +11,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_functions():
-    src = open(os.path.join(ROOT, "include", "nicam_cuda.h")).read()
+    import glob
+    src = "".join(open(f).read() for f in sorted(glob.glob(os.path.join(ROOT, "include", "*.h"))))
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b(nc_[a-z_]+)\s*\(", src)))
 
