@@ -18,6 +18,10 @@ fields of shape (lall, kall, gall_1d, gall_1d), pole fields (6, kall, 2).
 * ``Laplacian`` -- halo exchange then the hexagonal Laplacian
   (kernels/oprtlaplacian.py:41-70), linear; the adjoint runs the transposed
   stencil and adds each halo value back into its exchange source.
+* ``hevi_matrix`` / ``hevi_solve`` -- the HEVI vertical implicit step
+  (kernels/vimatrix.py:67-164, kernels/virhowsolver.py:42-172): the matrix
+  and source assembly as torch expressions in the reference's operation
+  order around ``VerticalSolve``, differentiable in every field.
 * ``Divergence`` / ``Gradient`` -- halo exchange then OPRT_divergence
   (kernels/fluxconv.py:52-108) / OPRT_gradient (kernels/oprtgradient.py:
   45-88), linear, adjoints as for the Laplacian (``nc_divergence``,
@@ -399,6 +403,98 @@ class TracerTransport:
 
 def vertical_solve(core, Mc, Mu, Ml, b, pole=False):
     return VerticalSolve.apply(core, pole, Mc, Mu, Ml, b)
+
+
+# ---------------------------------------------------------------------------
+# the HEVI vertical implicit step: the matrix of kernels/vimatrix.py:67-164 and
+# the source assembly + solve of kernels/virhowsolver.py:42-172, as torch
+# expressions in the reference's operation order around the hand-written
+# tridiagonal solve (VerticalSolve); differentiable in every field argument.
+# Fields in device layout: the level axis is axis 1 for regional and pole
+# tensors alike.
+# ---------------------------------------------------------------------------
+def hevi_metrics(geo: dict, device="cuda") -> dict:
+    """device tensors of the metrics and vertical factors the HEVI matrix and
+    solve read (VMTR_* regional and pole, GRD_* 1-D), and the constants"""
+    m = {}
+    for k in ("RGSGAM2", "GAM2H", "RGAMH", "RGSQRTH", "RGAM", "RGSGAM2H", "GSGAM2H"):
+        m[k] = to_device_layout(geo["VMTR_" + k], device)
+        m[k + "_pl"] = torch.as_tensor(np.ascontiguousarray(geo["VMTR_" + k + "_pl"], np.float64)).to(device)
+    for k in ("rdgz", "rdgzh", "afact", "bfact", "cfact", "dfact"):
+        m[k] = torch.as_tensor(np.asarray(geo["GRD_" + k], np.float64)).to(device)
+    for k in ("GRAV", "CVdry", "Rdry", "alpha"):
+        m[k] = float(_scalar(geo[k]))
+    m["kmin"], m["kmax"] = int(_scalar(geo["kmin"])), int(_scalar(geo["kmax"]))
+    return m
+
+
+def _lev(v, sl, nd):
+    """a 1-D level vector sliced and shaped to broadcast along axis 1"""
+    shape = [1] * nd
+    shape[1] = -1
+    return v[sl].view(shape)
+
+
+def _pad_levels(x, kmin, kmax, kall):
+    """interior rows kmin+1..kmax -> all kall levels, zero elsewhere"""
+    lo = x.new_zeros(x.shape[:1] + (kmin + 1,) + x.shape[2:])
+    hi = x.new_zeros(x.shape[:1] + (kall - kmax - 1,) + x.shape[2:])
+    return torch.cat([lo, x, hi], dim=1)
+
+
+def hevi_matrix(m: dict, eth_h, gz, dt: float, pole: bool = False):
+    """(Mc, Mu, Ml) on all levels (rows kmin+1..kmax, zero elsewhere) from the
+    half-level enthalpy eth_h and gz (kernels/vimatrix.py:67-164)"""
+    sfx = "_pl" if pole else ""
+    kmin, kmax, nd, kall = m["kmin"], m["kmax"], eth_h.dim(), eth_h.shape[1]
+    ks, ksp, ksm = slice(kmin + 1, kmax + 1), slice(kmin + 2, kmax + 2), slice(kmin, kmax)
+    K = lambda a, sl: a[:, sl]
+    RGSGAM2, GAM2H, RGAMH, RGSQRTH = (m[k + sfx] for k in ("RGSGAM2", "GAM2H", "RGAMH", "RGSQRTH"))
+    GCVovR = m["GRAV"] * m["CVdry"] / m["Rdry"]
+    ACVovRt2 = m["alpha"] * m["CVdry"] / m["Rdry"] / (dt * dt)
+    rg, rgm = _lev(m["rdgz"], ks, nd), _lev(m["rdgz"], ksm, nd)
+    Ca = (K(RGSGAM2, ks) * rg + K(RGSGAM2, ksm) * rgm) * K(GAM2H, ks)
+    Cb = (m["dfact"][ks] - m["cfact"][ksm]).view([1, -1] + [1] * (nd - 2))
+    Cu1 = K(RGSGAM2, ks) * rg * K(GAM2H, ksp)
+    Cu2 = K(GAM2H, ksp) * K(RGAMH, ks) ** 2 * GCVovR
+    Cl1 = K(RGSGAM2, ks) * rg * K(GAM2H, ksm)
+    Cl2 = K(GAM2H, ksm) * K(RGAMH, ks) ** 2 * GCVovR
+    rgh, cf, dfm = _lev(m["rdgzh"], ks, nd), _lev(m["cfact"], ks, nd), _lev(m["dfact"], ksm, nd)
+    Mc = ACVovRt2 / K(RGSQRTH, ks) + rgh * (Ca * K(eth_h, ks) - Cb * (K(gz, ks) + GCVovR))
+    Mu = -rgh * (Cu1 * K(eth_h, ksp) + cf * (K(gz, ksp) + Cu2))
+    Ml = -rgh * (Cl1 * K(eth_h, ksm) - dfm * (K(gz, ksm) + Cl2))
+    return tuple(_pad_levels(x, kmin, kmax, kall).contiguous() for x in (Mc, Mu, Ml))
+
+
+def hevi_solve(core, m: dict, rhogw, rhogw0, preg0, rhog0, Srho, Sw, Spre, Mc, Mu, Ml, dt: float,
+               pole: bool = False):
+    """the new rhogw of the vertical implicit step (kernels/virhowsolver.py:
+    42-172): source assembly on rows kmin+1..kmax, the boundary rows of rhogw
+    (kmin, kmax+1) moved into the sources, the tridiagonal solve, the result
+    scaled by GSGAM2H; levels outside kmin..kmax+1 keep rhogw"""
+    sfx = "_pl" if pole else ""
+    kmin, kmax, nd, kall = m["kmin"], m["kmax"], rhogw.dim(), rhogw.shape[1]
+    ks, ksm = slice(kmin + 1, kmax + 1), slice(kmin, kmax)
+    K = lambda a, sl: a[:, sl]
+    RGAMH, RGSGAM2, RGAM, RGSGAM2H, GSGAM2H = (m[k + sfx] for k in ("RGAMH", "RGSGAM2", "RGAM", "RGSGAM2H",
+                                                                      "GSGAM2H"))
+    CVovRt2 = m["CVdry"] / m["Rdry"] / (dt * dt)
+    rgh, af, bf = _lev(m["rdgzh"], ks, nd), _lev(m["afact"], ks, nd), _lev(m["bfact"], ks, nd)
+    Sall = ((K(rhogw0, ks) * m["alpha"] + dt * K(Sw, ks)) * K(RGAMH, ks) ** 2
+            - ((K(preg0, ks) + dt * K(Spre, ks)) * K(RGSGAM2, ks)
+               - (K(preg0, ksm) + dt * K(Spre, ksm)) * K(RGSGAM2, ksm)) * dt * rgh
+            - ((K(rhog0, ks) + dt * K(Srho, ks)) * K(RGAM, ks) ** 2 * af
+               + (K(rhog0, ksm) + dt * K(Srho, ksm)) * K(RGAM, ksm) ** 2 * bf) * dt * m["GRAV"]
+            ) * CVovRt2
+    rw_kmin = rhogw[:, kmin] * RGSGAM2H[:, kmin]
+    rw_kmaxp1 = rhogw[:, kmax + 1] * RGSGAM2H[:, kmax + 1]
+    rows = list(Sall.unbind(1))
+    rows[0] = rows[0] - Ml[:, kmin + 1] * rw_kmin
+    rows[-1] = rows[-1] - Mu[:, kmax] * rw_kmaxp1
+    b = _pad_levels(torch.stack(rows, 1), kmin, kmax, kall).contiguous()
+    x = VerticalSolve.apply(core, pole, Mc, Mu, Ml, b)
+    return torch.cat([rhogw[:, :kmin], (rw_kmin * GSGAM2H[:, kmin]).unsqueeze(1), K(x, ks) * K(GSGAM2H, ks),
+                      (rw_kmaxp1 * GSGAM2H[:, kmax + 1]).unsqueeze(1), rhogw[:, kmax + 2:]], dim=1)
 
 
 def vertical_advection(core, rhogq, den, flx_v, frhog, dt, bcoef=0.0, clamp=True, pole=False):

@@ -16,6 +16,9 @@ positive field with seeded noise (no ties for the limiter's min / max).
   the tridiagonal solve equals a banded solve to 1e-12;
 * dot-product tests <TL x, y> = <x, AD y> to 1e-12 (relative to the
   magnitudes of the products) for every operator, regional and pole;
+* the HEVI vertical implicit step (adjoint.hevi_matrix / hevi_solve around
+  the hand-written solve) equals the oracle's rhow_matrix / rhow_solver bit
+  for bit and passes the dot-product test in all nine field arguments;
 * central finite differences along seeded random directions against the
   tangent-linear, to 1e-6 relative (relative steps of 1e-9 / 1e-8; the
   errors at 1e-6 are reported: the limiter is piecewise linear);
@@ -222,6 +225,94 @@ def test_divergence_and_gradient_equal_oracle(gl04):
     for d in range(3):
         assert np.array_equal(adj.from_device_layout(g[d]), want[..., d]), d
         assert np.array_equal(g_pl[d].cpu().numpy(), want_pl[..., d]), d
+
+
+def _hevi_case(geo, seed):
+    """the HEVI matrix and solve inputs at gl04: metrics with their unused
+    halo corners set to one (a zero there would divide), half-level enthalpy
+    and gz near their atmospheric values, prognostic deviations and tendencies
+    of plausible sizes, regional (reference layout) and pole"""
+    g = dict(geo)
+    for k in ("RGSGAM2", "GAM2H", "RGAMH", "RGSQRTH", "RGAM", "RGSGAM2H", "GSGAM2H"):
+        for sfx in ("", "_pl"):
+            a = np.array(geo["VMTR_" + k + sfx], np.float64)
+            a[a == 0] = 1.0
+            g["VMTR_" + k + sfx] = a
+    rng = np.random.default_rng(seed)
+    z = np.asarray(geo["GRD_gzh"], np.float64)
+    out = {}
+    for sfx, shp in (("", np.shape(geo["VMTR_RGAMH"])), ("_pl", np.shape(geo["VMTR_RGAMH_pl"]))):
+        kax = 2 if sfx == "" else 1
+        zz = z.reshape([-1 if d == kax else 1 for d in range(len(shp))])
+        r = lambda scale: scale * (1.0 + 0.1 * rng.standard_normal(shp))
+        out["eth_h" + sfx] = 3.0e5 * (1.0 + 0.01 * rng.standard_normal(shp))
+        out["gz" + sfx] = 9.80616 * zz * (1.0 + 1e-3 * rng.standard_normal(shp))
+        for k, sc in (("rhogw", 1e-2), ("rhogw0", 1e-2), ("preg0", 1e3), ("rhog0", 1.0), ("Srho", 1e-5),
+                      ("Sw", 1e-3), ("Spre", 1.0)):
+            out[k + sfx] = r(sc)
+    return g, out
+
+
+HEVI_ARGS = ("rhogw", "rhogw0", "preg0", "rhog0", "Srho", "Sw", "Spre")
+
+
+def _hevi_dev(x, pole):
+    import torch
+    _, adj = _mods()
+    return torch.as_tensor(np.ascontiguousarray(x)).cuda() if pole else adj.to_device_layout(x)
+
+
+def test_hevi_matrix_and_solve_equal_oracle(gl04):
+    from oracle import nicam_step as O
+    _, adj = _mods()
+    geo, core, _ = gl04
+    g, a = _hevi_case(geo, 40)
+    G, m = O.Geo(g), adj.hevi_metrics(g)
+    dt = float(geo["dts"])
+    kmin, kmax = int(geo["kmin"]), int(geo["kmax"])
+    ks = slice(kmin + 1, kmax + 1)
+    for pole in (False, True):
+        sfx = "_pl" if pole else ""
+        back = (lambda t: t.cpu().numpy()) if pole else adj.from_device_layout
+        want = O.rhow_matrix(G, a["eth_h" + sfx], a["gz" + sfx], dt, pole)
+        got = adj.hevi_matrix(m, _hevi_dev(a["eth_h" + sfx], pole), _hevi_dev(a["gz" + sfx], pole), dt, pole)
+        for w, t in zip(want, got):
+            x = back(t)
+            assert np.array_equal(x[:, ks] if pole else x[:, :, ks], w), pole
+        want_x = O.rhow_solver(G, *(a[k + sfx] for k in HEVI_ARGS), *want, dt, pole)
+        got_x = adj.hevi_solve(core, m, *(_hevi_dev(a[k + sfx], pole) for k in HEVI_ARGS), *got, dt, pole)
+        assert np.array_equal(back(got_x), want_x), (pole, np.abs(back(got_x) - want_x).max())
+
+
+def test_dot_product_hevi(gl04):
+    """forward-mode against reverse-mode through the matrix assembly, the
+    source assembly and the tridiagonal solve, in every field argument"""
+    import torch
+    import torch.autograd.forward_ad as fwAD
+    _, adj = _mods()
+    geo, core, _ = gl04
+    g, a = _hevi_case(geo, 41)
+    m = adj.hevi_metrics(g)
+    dt = float(geo["dts"])
+    names = ("eth_h", "gz") + HEVI_ARGS
+    for pole in (False, True):
+        sfx = "_pl" if pole else ""
+        xs = [_hevi_dev(a[k + sfx], pole) for k in names]
+        ds = [_rand_like(x, 50 + n) * x * 1e-3 for n, x in enumerate(xs)]
+
+        def f(*v):
+            M = adj.hevi_matrix(m, v[0], v[1], dt, pole)
+            return adj.hevi_solve(core, m, *v[2:], *M, dt, pole)
+        with fwAD.dual_level():
+            tl = fwAD.unpack_dual(f(*[fwAD.make_dual(x, d) for x, d in zip(xs, ds)])).tangent
+        leaves = [x.clone().requires_grad_(True) for x in xs]
+        y = f(*leaves)
+        w = _rand_like(y, 60)
+        grads = torch.autograd.grad(y, leaves, w)
+        lhs = _dot(tl, w)
+        rhs = sum(_dot(d, gr) for d, gr in zip(ds, grads))
+        scale = float((tl * w).abs().sum())
+        assert _dot_rel(lhs, rhs, scale) <= 1e-12, (pole, lhs, rhs)
 
 
 # ---------------------------------------------------------------- dot-product tests
