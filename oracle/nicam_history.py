@@ -82,8 +82,9 @@ class History:
         rho = RHOG / g.VMTR_GSGAM2
         vx, vy, vz = P[..., 1] / RHOG, P[..., 2] / RHOG, P[..., 3] / RHOG
         ein = P[..., 5] / RHOG
-        qd = 1.0 - np.sum(q[..., 0:1], axis=4)
-        cv = np.sum(q[..., 0:1] * g.CVW[0:1], axis=4) + qd * g.CVdry
+        nw = getattr(g, "nqw", 1)
+        qd = 1.0 - np.sum(q[..., 0:nw], axis=4)
+        cv = np.sum(q[..., 0:nw] * g.CVW[0:nw], axis=4) + qd * g.CVdry
         tem = ein / cv
         pre = rho * tem * (qd * g.Rdry + q[..., 0] * g.Rvap)
         w = np.zeros_like(tem) if w_prev is None else np.array(w_prev, np.float64, copy=True)

@@ -58,6 +58,8 @@ class Geo:
             setattr(self, k, float(c(k)))
         self.sstep = [int(x) for x in np.asarray(d["sstep"])]
         self.CVW = np.asarray(d["CVW"], np.float64)
+        # water tracers 0..NQW_END (mod_runconf.py RUNCONF_tracer_setup: NQW_STR = I_QV = 0)
+        self.nqw = int(c("NQW_END")) + 1 if "NQW_END" in d else 1
 
     def __getattr__(self, k):
         d = self.__dict__.get("d")
@@ -113,8 +115,10 @@ def diagnostics(g, PROG, PROGq, DIAG, PROG_pl, PROGq_pl, DIAG_pl):
         D[..., I_vz] = P[..., I_RHOGVZ] / RHOG
         ein = P[..., I_RHOGE] / RHOG
         q = Pq / RHOG[..., None]
-        qd = 1.0 - q[..., 0]
-        cv = q[..., 0] * g.CVW[0] + qd * g.CVdry
+        # kernels/diag.py:97-115: cv and qd over the water range, sums in index order
+        qw = q[..., 0:g.nqw]
+        qd = 1.0 - np.sum(qw, axis=-1)
+        cv = np.sum(qw * g.CVW[0:g.nqw], axis=-1) + qd * g.CVdry
         tem = ein / cv
         D[..., I_tem] = tem
         D[..., I_pre] = rho * tem * (qd * g.Rdry + q[..., 0] * g.Rvap)

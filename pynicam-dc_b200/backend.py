@@ -53,6 +53,7 @@ def geo_from_msc(msc) -> dict:
     g["Kh_coef"], g["divdamp_coef"] = float(Kh.flat[0]), float(dd.flat[0])
     g["sstep"] = np.asarray(m.dyn.num_of_iteration_sstep[:m.dyn.num_of_iteration_lstep])
     g["CVW"] = np.asarray(m.rcnf.CVW)
+    g["NQW_END"] = int(m.rcnf.NQW_END)
     co = m.comm
     g["copy_r2r"] = co.Copy_list_r2r[:, :int(co.Copy_info_r2r[co.I_size])].astype(np.int64)
     g["copy_p2r"] = co.Copy_list_p2r[:, :int(co.Copy_info_p2r[co.I_size])].astype(np.int64)
@@ -173,6 +174,9 @@ class CudaDyn:
                                       "2-D/vertical divdamp, lap1 or nonlinear diffusion")
         if r.DYN_DIV_NUM != 1:
             raise NotImplementedError("cuda backend: DYN_DIV_NUM = 1 only")
+        if int(getattr(r, "NQW_STR", 0)) != 0 or int(getattr(r, "I_QV", 0)) != 0 or \
+                int(getattr(r, "NQW_END", 0)) >= 6:
+            raise NotImplementedError("cuda backend: water tracers must come first (NQW_STR = I_QV = 0), at most six")
         if getattr(r, "AF_TYPE", "NONE") not in ("NONE", "HELD-SUAREZ"):
             raise NotImplementedError("cuda backend: artificial forcing NONE or HELD-SUAREZ only")
 

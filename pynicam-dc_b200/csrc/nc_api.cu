@@ -836,7 +836,7 @@ static int run_step(nc_handle* h) {
     auto diag_args = [&](bool pole) {
       DiagArgs<R> a;
       a.P = pole ? prog_pl<R>(h) : prog_reg<R>(h);
-      a.Pq0 = pole ? PL<R>(h->Pq[0]) : RG<R>(h->Pq[0]);
+      for (int n = 0; n < h->C.nqw; ++n) a.Pqw[n] = pole ? PL<R>(h->Pq[n]) : RG<R>(h->Pq[n]);
       auto F = [&](FieldPair& f) { return pole ? PL<R>(f) : RG<R>(f); };
       auto F64 = [&](FieldPair& f) { return pole ? f.p : f.r; };
       a.pre = F(h->pre); a.tem = F(h->tem); a.vx = F(h->vx); a.vy = F(h->vy); a.vz = F(h->vz); a.w = F(h->w);
@@ -1248,7 +1248,7 @@ static int lin_buffers(nc_handle* h) {
 static int copy_in(nc_handle* h, FieldPair& dst, const double* r, const double* p) {
   CU(cudaMemcpyAsync(dst.r, r, h->D.npt * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
   CU(cudaMemcpyAsync(dst.p, p, h->D.npl * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-  return 0;
+  return h->prof ? mark(h, "lin_copy") : 0;
 }
 static int copy_out(nc_handle* h, double* r, double* p, const FieldPair& src) {
   CU(cudaMemcpyAsync(r, src.r, h->D.npt * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
@@ -1258,7 +1258,7 @@ static int copy_out(nc_handle* h, double* r, double* p, const FieldPair& src) {
 static int zero_pair(nc_handle* h, FieldPair& f) {
   CU(cudaMemsetAsync(f.r, 0, h->D.npt * sizeof(double), h->stream));
   CU(cudaMemsetAsync(f.p, 0, h->D.npl * sizeof(double), h->stream));
-  return 0;
+  return h->prof ? mark(h, "lin_zero") : 0;
 }
 // the exchange adjoint on one field (k_comm_adj_add, then the destinations cleared)
 static int comm_adj(nc_handle* h, FieldPair& f) {
@@ -1278,7 +1278,7 @@ static int vadv_lin_launch(nc_handle* h, int mode, const FieldPair& at, const Fi
               second ? 1 : 0, mode};
     const long long n = pole ? 6LL * h->D.LP : h->D.npt2;
     k_vadv_lin<<<(unsigned)((n + 63) / 64), 64, 0, h->stream>>>(a, pole);
-    TRY(check_launch(h, "vadv_lin"));
+    TRY(check_launch(h, mode == 1 ? "vadv_tl" : "vadv_ad"));
   }
   return 0;
 }
@@ -1421,7 +1421,7 @@ int nc_forcing_step(nc_handle* h) {
   const Dims& D = h->D;
   HsArgs a;
   for (int v = 0; v < 6; ++v) a.P.v[v] = h->P[v].r;
-  a.Pq0 = h->Pq[0].r;
+  for (int n = 0; n < h->C.nqw; ++n) a.Pqw[n] = h->Pq[n].r;
   a.lat3 = h->hs_lat;
   a.dt = h->dtl;
   a.RdCp = h->C.Rdry / h->C.CPdry;
@@ -1507,6 +1507,8 @@ static int make_f32_geometry(nc_handle* h) {
   Cf.HUGE_ = FLT_MAX;
   Cf.rscale = (float)C.rscale; Cf.alpha = (float)C.alpha; Cf.Kh = (float)C.Kh; Cf.divdamp_coef = (float)C.divdamp_coef;
   Cf.hdiff_fact_rho = (float)C.hdiff_fact_rho; Cf.CVW0 = (float)C.CVW0; Cf.PRE00 = (float)C.PRE00;
+  for (int n = 0; n < NC_MAXQW; ++n) Cf.CVW[n] = (float)C.CVW[n];
+  Cf.nqw = C.nqw;
   Cf.gam_unit = C.gam_unit;
   Cf.rsc_h = (float)(1.0 / C.rscale);   // the float32 divisions multiply by the rounded reciprocal
   Cf.rsc_l = 0.0f;
@@ -1578,6 +1580,17 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
     const nc_array* cvw = T.get("CVW");
     if (!cvw || cvw->dtype != NC_F64 || numel(cvw) < 1) return fail(NC_ERR_ARG, "missing CVW");
     C.CVW0 = ((const double*)cvw->data)[0];
+    // water tracers 0..NQW_END (optional entry; one, the vapour, when absent)
+    C.nqw = 1;
+    if (T.get("NQW_END")) {
+      double f;
+      TRY(scalar(T, "NQW_END", f));
+      C.nqw = (int)f + 1;
+    }
+    if (C.nqw < 1 || C.nqw > NC_MAXQW || C.nqw > numel(cvw) || C.nqw > D.nq)
+      return fail(NC_ERR_ARG, "NQW_END must give 1.." + std::to_string(NC_MAXQW) +
+                                  " water tracers among the nq tracers, with CVW for each");
+    for (int n = 0; n < NC_MAXQW; ++n) C.CVW[n] = n < C.nqw ? ((const double*)cvw->data)[n] : 0.0;
     if (T.get("trcadv")) {
       double f;
       TRY(scalar(T, "trcadv", f));
@@ -2615,6 +2628,10 @@ int nc_trc_step_lin(nc_handle* h, int32_t mode, const double* x0, const double* 
   TRY(lin_buffers(h));
   SingleStream one(h);
   TRY(after_caller(h, stream));
+  if (h->prof) {   // per-kernel times of this call (nc_profile / nc_kernel_stats)
+    h->ev_used = 0;
+    TRY(mark(h, nullptr));
+  }
   FieldPair* L = h->lin;
   TRY(trc_lin_forward(h, x0, x0_pl));
   CommFields<double> cf{};
@@ -2640,6 +2657,7 @@ int nc_trc_step_lin(nc_handle* h, int32_t mode, const double* x0, const double* 
     k_comm<<<gc, 256, 0, h->stream>>>(cf, h->r_dst, h->r_src, h->nr, h->p_dst, h->p_src, h->np);
     TRY(check_launch(h, "lin_comm"));
   }
+  if (h->prof) TRY(collect_profile(h));
   return before_caller(h, stream);
 }
 

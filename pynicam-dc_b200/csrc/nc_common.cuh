@@ -24,6 +24,7 @@
 
 #define NC_MAXK 128
 #define NC_MAXNQ 32
+#define NC_MAXQW 6   // water tracers (RAIN_TYPE COLD: vapour, cloud, rain, ice, snow, graupel)
 
 namespace nc {
 
@@ -51,6 +52,8 @@ template <class R>
 struct ConstsT {
   R GRAV, Rdry, CVdry, CPdry, Rvap, OHM, EPS, HUGE_, rscale, alpha;
   R Kh, divdamp_coef, hdiff_fact_rho, CVW0, PRE00;
+  R CVW[NC_MAXQW];   // specific heats of the water tracers 0..nqw-1
+  int nqw;           // water tracers (NQW_END + 1; NQW_STR = I_QV = 0)
   int gam_unit;   // RGAM, RGAMH and GAM2H are 1 everywhere (shallow atmosphere)
   // rounded reciprocals and their tails, RN(1/b) and RN(1/b - RN(1/b)), of the
   // divisors rscale and 3 (see div_by)
@@ -253,6 +256,21 @@ __device__ __constant__ static const int kNbJ[7] = {0, 0, 1, 1, 0, -1, -1};
 
 __device__ __forceinline__ bool interior(int i, int j) {
   return i >= 1 && i <= cD.G - 2 && j >= 1 && j <= cD.G - 2;
+}
+
+// qd and cv from the water mixing ratios q0 = q(0), q(1) .. q(nqw-1)
+// (kernels/diag.py:97-115: both sums in index order; with one water tracer
+// qd = 1 - q0 and cv = q0 CVW0 + qd CVdry)
+template <class F>
+__device__ __forceinline__ void moist_qd_cv(F q, double q0, double& qd, double& cv) {
+  double sq = q0, sc = q0 * (double)cC.CVW[0];
+  for (int n = 1; n < cC.nqw; ++n) {
+    const double x = q(n);
+    sq = sq + x;
+    sc = sc + x * (double)cC.CVW[n];
+  }
+  qd = 1.0 - sq;
+  cv = sc + qd * cC.CVdry;
 }
 
 // Column thread mapping: thread -> (i, j, l).  Returns false for surplus threads.

@@ -8,7 +8,7 @@ namespace nc {
 // Held & Suarez (1994) dry-case parameters (nhm/forcing/mod_af_heldsuarez.py:19-36)
 struct HsArgs {
   Prog<double> P;         // PROG, updated in place
-  const double* Pq0;      // first tracer (water vapour) for the diagnostics
+  const double* Pqw[NC_MAXQW];   // the water tracers (0: vapour) for the diagnostics
   const double* lat3;     // planes |sin lat|^2, |cos lat|^2, |cos lat|^4 of each column
   double dt, RdCp;        // large time step; Rdry / CPdry
   double sigma_b, Kf, Dth_z, Ka, Ks, T_eq0, DT_y, PRE00;
@@ -40,9 +40,9 @@ __global__ void k_forcing_hs(HsArgs a) {
     vy = P[2][p] / RHOG;
     vz = P[3][p] / RHOG;
     const double ein = P[5][p] / RHOG;
-    const double q0 = a.Pq0[p] / RHOG;
-    const double qd = 1.0 - q0;
-    const double cv = q0 * cC.CVW0 + qd * cC.CVdry;
+    const double q0 = a.Pqw[0][p] / RHOG;
+    double qd, cv;
+    moist_qd_cv([&](int n) { return a.Pqw[n][p] / RHOG; }, q0, qd, cv);
     tem = ein / cv;
     pre = rho * tem * (qd * cC.Rdry + q0 * cC.Rvap);
   };

@@ -55,8 +55,8 @@ __device__ __forceinline__ DiagPt hist_diag(const HistArgs& a, int p) {
   d.vz = div_by(a.P[3][p], rr);
   const double ein = div_by(a.P[5][p], rr);
   const double q0 = div_by(a.Pq[0][p], rr);
-  const double qd = 1.0 - q0;
-  const double cv = q0 * cC.CVW0 + qd * cC.CVdry;
+  double qd, cv;
+  moist_qd_cv([&](int n) { return div_by(a.Pq[n][p], rr); }, q0, qd, cv);
   d.tem = ein / cv;
   d.pre = d.rho * d.tem * (qd * cC.Rdry + q0 * cC.Rvap);
   d.qv = (a.iqv >= 0) ? div_by(a.Pq[a.iqv][p], rr) : 0.0;

@@ -19,7 +19,7 @@ struct Prog { R* v[6]; };   // RHOG, RHOGVX, RHOGVY, RHOGVZ, RHOGW, RHOGE
 template <class R>
 struct DiagArgs {
   Prog<R> P;            // in/out (ghost rows written)
-  const R* Pq0;         // first tracer (water vapour)
+  const R* Pqw[NC_MAXQW];   // the water tracers (0: vapour)
   R *pre, *tem, *vx, *vy, *vz, *w, *rho, *ein, *eth;
   double *pregd, *rhogd;   // float64 in both forms
   R *vvx, *vvy, *vvz;
@@ -37,9 +37,9 @@ __device__ void diag_column(const Col c, const MetT<R> m, const DiagArgs<R>& a, 
     a.vy[p] = P[2][p] / RHOG;
     a.vz[p] = P[3][p] / RHOG;
     double ein = P[5][p] / RHOG;
-    double q0 = a.Pq0[p] / RHOG;
-    double qd = 1.0 - q0;
-    double cv = q0 * cC.CVW0 + qd * cC.CVdry;
+    double q0 = a.Pqw[0][p] / RHOG;
+    double qd, cv;
+    moist_qd_cv([&](int n) { return (double)a.Pqw[n][p] / RHOG; }, q0, qd, cv);
     double tem = ein / cv;
     a.tem[p] = tem;
     a.pre[p] = rho * tem * (qd * cC.Rdry + q0 * cC.Rvap);
@@ -145,9 +145,9 @@ __device__ void diag_column_fused(const Col c, const MetT<R> m, const DiagArgs<R
     a.vy[p] = vy;
     a.vz[p] = vz;
     double ein = div_by(P[5][p], rr);
-    double q0 = div_by(a.Pq0[p], rr);
-    double qd = 1.0 - q0;
-    double cv = q0 * cC.CVW0 + qd * cC.CVdry;
+    double q0 = div_by(a.Pqw[0][p], rr);
+    double qd, cv;
+    moist_qd_cv([&](int n) { return div_by(a.Pqw[n][p], rr); }, q0, qd, cv);
     double tem = ein / cv;
     const double pre = rho * tem * (qd * cC.Rdry + q0 * cC.Rvap);
     a.tem[p] = tem;

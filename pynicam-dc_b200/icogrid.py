@@ -1100,7 +1100,7 @@ class Grid:
                  GRAV=GRAV, Rdry=RDRY, CVdry=CVDRY, CPdry=CPDRY, Rvap=RVAP, OHM=OHM, RADIUS=RADIUS, EPS=EPS,
                  HUGE=HUGE, PRE00=PRE00, rscale=self.rscale, alpha=1.0, dtl=float(dtl), dts=float(dtl) / 6.0,
                  Kh_coef=float(gamma), divdamp_coef=float(gamma), hdiff_fact_rho=1.0e-2,
-                 sstep=np.array([2, 3, 6]), CVW=np.array([CVDRY] * nq))
+                 sstep=np.array([2, 3, 6]), CVW=np.array([CVDRY] * nq), NQW_END=np.asarray(0))
         for k, v in self.exch.lists.items():
             g["copy_" + k] = v
         g["GRD_gz"], g["GRD_gzh"] = self.gz, self.gzh

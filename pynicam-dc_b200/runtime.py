@@ -212,6 +212,8 @@ def setup_table(geo: dict) -> dict:
               "Kh_coef", "divdamp_coef", "hdiff_fact_rho"):
         t[k] = np.asarray(float(_scalar(geo[k])), np.float64)
     t["CVW"] = np.ascontiguousarray(geo["CVW"], np.float64)
+    if "NQW_END" in geo:   # water tracers 0..NQW_END (RAIN_TYPE); the vapour alone when absent
+        t["NQW_END"] = np.asarray(float(_scalar(geo["NQW_END"])), np.float64)
     t["sstep"] = np.ascontiguousarray(geo["sstep"], np.int64)
     for k in ("GRD_afact", "GRD_bfact", "GRD_cfact", "GRD_dfact", "GRD_rdgz", "GRD_rdgzh"):
         t[k] = np.ascontiguousarray(geo[k], np.float64)

@@ -29,6 +29,15 @@ def golden():
 
 
 @pytest.fixture(scope="session")
+def golden_warm():
+    """gl03 z10 with RAIN_TYPE WARM (vapour, cloud and rain tracers in the
+    thermodynamics), two steps of the reference (make_golden.py --case
+    gl03_z10_warm)"""
+    from make_golden import load
+    return load(os.path.join(GOLDEN, "gl03_z10_warm.npz"))
+
+
+@pytest.fixture(scope="session")
 def golden_hs():
     """gl03 z10 with the reference's Held-Suarez forcing (make_hs.py): setup
     arrays (plus GRD_LAT at K0), the column latitudes and three states"""

@@ -61,7 +61,7 @@ def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_
         setattr(comm, "Copy_info_" + name, np.array([g[key].shape[1]]))
     comm.Singular_list = g["copy_sgp"]
     comm.Singular_info = np.array([g["copy_sgp"].shape[1]])
-    rcnf = NS(NON_HYDRO_ALPHA=sc("alpha"), CVW=g["CVW"], AF_TYPE=af_type, TRC_ADV_TYPE="MIURA2004",
+    rcnf = NS(NON_HYDRO_ALPHA=sc("alpha"), CVW=g["CVW"], NQW_STR=0, I_QV=0, NQW_END=int(np.asarray(g.get("NQW_END", 0))), AF_TYPE=af_type, TRC_ADV_TYPE="MIURA2004",
               THUBURN_LIM=True, DYN_DIV_NUM=1,
               DCTEST_type="Traceradvection" if integ_type == "TRCADV" else "",
               DCTEST_case="1-1" if integ_type == "TRCADV" else "")

@@ -34,7 +34,12 @@ import numpy as np
 CASES = {
     # name: glevel, vlayer, ztop [m], dtl [s], gamma_h = alpha_d, nsteps, tracer
     "gl03_z10_trc": (3, 10, 30000.0, 1200.0, 7.68e17, 2, True),
+    # RAIN_TYPE WARM: three water tracers (vapour, cloud, rain) in the
+    # thermodynamics of the step (cv and qd over the water range)
+    "gl03_z10_warm": (3, 10, 30000.0, 1200.0, 7.68e17, 2, True),
 }
+RAIN = {"gl03_z10_warm": "WARM"}
+WATER_SCALE = (1.0, 0.05, 0.02)   # vapour, cloud, rain: multiples of the tracer field
 
 MKRAWGRID_TOML = """[admparam]
 glevel  = {gl}
@@ -106,7 +111,7 @@ def prep(ref: str, case_dir: str, gl: int, vl: int, ztop: float, layer_type: str
 NHM_TOML = os.path.join("tutorial", "case", "config", "nhm_jw.toml")
 
 
-def model_toml(ref: str, gl: int, vl: int, dtl: float, gamma: float, nsteps: int) -> str:
+def model_toml(ref: str, gl: int, vl: int, dtl: float, gamma: float, nsteps: int, rain: str = "") -> str:
     """the reference's JW tutorial config, pointed at the scratch case"""
     import toml
     c = toml.load(os.path.join(ref, NHM_TOML))
@@ -120,6 +125,8 @@ def model_toml(ref: str, gl: int, vl: int, dtl: float, gamma: float, nsteps: int
     c["restartparam"]["input_io_mode"] = "IDEAL"
     c["dycoretestparam"].update(init_type="Jablonowski", test_case="1")
     c["runconfparam"]["THUBURN_LIM"] = True
+    if rain:
+        c["runconfparam"]["RAIN_TYPE"] = rain
     c.setdefault("embudgetparam", {})["MNT_ON"] = False
     c["ioparam"]["PRGout_interval"] = 10 ** 9
     return toml.dumps(c)
@@ -154,6 +161,7 @@ def geo_from_msc(m, nq: int) -> dict:
     assert np.all(m.numf.divdamp_coef == float(m.numf.alpha_d))
     g["sstep"] = np.asarray(m.dyn.num_of_iteration_sstep[:m.dyn.num_of_iteration_lstep])
     g["CVW"] = np.asarray(m.rcnf.CVW)
+    g["NQW_END"] = int(m.rcnf.NQW_END)   # water tracers 0..NQW_END (NQW_STR = I_QV = 0)
     co = m.comm
     g["copy_r2r"] = co.Copy_list_r2r[:, :int(co.Copy_info_r2r[co.I_size])].astype(np.int64)
     g["copy_p2r"] = co.Copy_list_p2r[:, :int(co.Copy_info_p2r[co.I_size])].astype(np.int64)
@@ -182,7 +190,7 @@ def run_case(ref: str, name: str, out_dir: str, scratch: str):
     case_dir = os.path.join(scratch, name)
     prep(ref, case_dir, gl, vl, ztop)
     with open(os.path.join(case_dir, "case", "config", "nhm_jw.toml"), "w") as f:
-        f.write(model_toml(ref, gl, vl, dtl, gamma, nsteps))
+        f.write(model_toml(ref, gl, vl, dtl, gamma, nsteps, RAIN.get(name, "")))
     with open(os.path.join(case_dir, "drv.toml"), "w") as f:
         f.write('[driver]\nbackend="numpy"\nprecision="float64"\ncomm="serial"\n'
                 'nhm_driver_cnf="./case/config/nhm_jw.toml"\n')
@@ -217,12 +225,15 @@ def run_case(ref: str, name: str, out_dir: str, scratch: str):
         kk = pv.shape[2]
         lat, lon = m.grd.GRD_LAT[:, :, 0, :], m.grd.GRD_LON[:, :, 0, :]
         latp, lonp = m.grd.GRD_LAT_pl[:, 0, :], m.grd.GRD_LON_pl[:, 0, :]
-        pv[..., 6] = pv[..., 0] * np.moveaxis(tracer_field(lat, lon, kk), -1, 2)
-        pvp[..., 6] = pvp[..., 0] * np.moveaxis(tracer_field(latp, lonp, kk), -1, 1)
-        pv[:, :, 0, :, 6] = 0.0
-        pv[:, :, -1, :, 6] = 0.0
-        pvp[:, 0, :, 6] = 0.0
-        pvp[:, -1, :, 6] = 0.0
+        nw = int(m.rcnf.NQW_END) + 1 if name in RAIN else 1
+        for n in range(nw):
+            sc = WATER_SCALE[n]
+            pv[..., 6 + n] = pv[..., 0] * sc * np.moveaxis(tracer_field(lat, lon, kk), -1, 2)
+            pvp[..., 6 + n] = pvp[..., 0] * sc * np.moveaxis(tracer_field(latp, lonp, kk), -1, 1)
+            pv[:, :, 0, :, 6 + n] = 0.0
+            pv[:, :, -1, :, 6 + n] = 0.0
+            pvp[:, 0, :, 6 + n] = 0.0
+            pvp[:, -1, :, 6 + n] = 0.0
     out = {"geo." + k: v for k, v in geo_from_msc(m, pv.shape[-1] - 6).items()}
     out["state0"], out["state0_pl"] = pv.copy(), pvp.copy()
     for s in range(nsteps):

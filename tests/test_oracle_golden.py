@@ -14,6 +14,17 @@ def test_oracle_matches_reference_two_steps(golden):
         assert np.array_equal(out_pl, st[f"state{s + 1}_pl"]), f"step {s + 1} pole"
 
 
+def test_oracle_matches_reference_warm_rain(golden_warm):
+    """three water tracers (RAIN_TYPE WARM): cv and qd over the water range"""
+    geo, st = golden_warm
+    G = O.Geo(geo)
+    assert G.nqw == 3
+    for s in (0, 1):
+        out, out_pl = O.dynamics_step(G, st[f"state{s}"], st[f"state{s}_pl"])
+        assert np.array_equal(out, st[f"state{s + 1}"]), f"step {s + 1} regional"
+        assert np.array_equal(out_pl, st[f"state{s + 1}_pl"]), f"step {s + 1} pole"
+
+
 def test_golden_tracer_is_nontrivial(golden):
     _, st = golden
     q = st["state0"][..., 6]
