@@ -226,8 +226,26 @@ int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* g
  * reference's host path.  Needs the handle to have been created with the
  * setup entries "AF_hs_lat_terms" ((gall_1d, gall_1d, 1, lall, 3): |sin lat|^2,
  * |cos lat|^2, |cos lat|^4 of GRD_LAT[:, :, K0, :]) and "PRE00"; otherwise
- * NC_ERR_STATE.  Asynchronous on the handle's stream, like nc_step. */
+ * NC_ERR_STATE.  Asynchronous on the handle's stream, like nc_step.
+ *
+ * For AF_TYPE 'DCMIP' with Kessler warm-rain microphysics only (forcing_dcmip
+ * USE_Kessler, the scheme set of DCMIP2016 case 1-3; nhm/forcing/
+ * mod_forcing.py:207-321, mod_af_dcmip.py:129-230, kessler.py): the handle is
+ * created with "AF_dcmip_kessler_zf" (GRD_vz[..., GRD_Z], (gall_1d, gall_1d,
+ * kall, lall)), "PRE00", RAIN_TYPE WARM ("NQW_END" = 2: vapour, cloud, rain)
+ * and optionally "AF_negative_fixer" / "AF_update_tot_dens" (the reference's
+ * forcing_param, defaults 0 / 1).  Every regional column: diagnostics, dry
+ * mixing ratios, the microphysics with its sedimentation sub-cycles, the
+ * water and energy tendencies applied to the tracers, RHOGE and (with
+ * update_tot_dens) RHOG, then the exchange.  exp and pow are CUDA's, so
+ * results can differ from numpy's in the last bits.  The precipitation rate
+ * of the step per column is read with nc_forcing_precip. */
 int nc_forcing_step(nc_handle* h);
+
+/* The precipitation rate [m/s] of the last DCMIP Kessler forcing step per
+ * column, into host memory (gall_1d, gall_1d, lall) (the reference's
+ * frc.precip); synchronous.  NC_ERR_STATE without Kessler forcing. */
+int nc_forcing_precip(nc_handle* h, double* host);
 
 /* Restart files in the reference's fio format (input/output_io_mode
  * "ADVANCED", nhm/share/mod_fio.py), read and written from the device state:

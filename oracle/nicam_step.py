@@ -1688,6 +1688,141 @@ def forcing_step_hs(g, prg, prg_pl, lat):
 
 
 # --------------------------------------------------------------------------
+# DCMIP forcing with Kessler warm-rain microphysics only (AF_TYPE 'DCMIP',
+# USE_Kessler; the scheme set of DCMIP2016 case 1-3)
+# --------------------------------------------------------------------------
+def kessler(theta, qv, qc, qr, rho, pk, dt, z):
+    """nhm/forcing/kessler.py:9-179 on (ncol, nz) columns ordered surface to
+    top: potential temperature, dry mixing ratios, dry density, Exner
+    function, heights.  Returns the updated theta, qv, qc, qr and the
+    precipitation rate per column.  Rain sedimentation is sub-cycled per
+    column (CFL 0.8); columns with fewer sub-cycles are left unchanged in the
+    later ones."""
+    f2x = 17.27
+    f5 = 237.3 * f2x * 2500000.0 / 1003.0
+    xk = 0.2875
+    psl = 1000.0
+    rhoqr = 1000.0
+    theta, qv, qc, qr = theta.copy(), qv.copy(), qc.copy(), qr.copy()
+    r = 0.001 * rho
+    rhalf = np.sqrt(rho[:, 0:1] / rho)
+    pc = 3.8 / (pk ** (1.0 / xk) * psl)
+    velqr = 36.34 * (qr * r) ** 0.1364 * rhalf
+    dz = z[:, 1:] - z[:, :-1]
+    vk = velqr[:, :-1]
+    vk_safe = np.where(vk != 0.0, vk, 1.0)
+    cfl = np.where(vk != 0.0, 0.8 * dz / vk_safe, dt)
+    dt_max = np.minimum(dt, cfl.min(axis=1))
+    rainsplit = np.ceil(dt / dt_max).astype(np.int32)
+    dt0 = dt / rainsplit.astype(np.float64)
+    dt0c = dt0[:, None]
+    precl = np.zeros(theta.shape[0])
+    for nt in range(1, int(rainsplit.max()) + 1):
+        active = nt <= rainsplit
+        am = active[:, None]
+        precl = precl + np.where(active, rho[:, 0] * qr[:, 0] * velqr[:, 0] / rhoqr, 0.0)
+        num = r[:, 1:] * qr[:, 1:] * velqr[:, 1:] - r[:, :-1] * qr[:, :-1] * velqr[:, :-1]
+        sed_int = dt0c * num / (r[:, :-1] * dz)
+        sed_top = -dt0 * qr[:, -1] * velqr[:, -1] / (0.5 * (z[:, -1] - z[:, -2]))
+        sed = np.concatenate([sed_int, sed_top[:, None]], axis=1)
+        qc0, qr0, qv0, th0 = qc, qr, qv, theta
+        qrprod = qc0 - (qc0 - dt0c * np.maximum(0.001 * (qc0 - 0.001), 0.0)) / (1.0 + dt0c * 2.2 * qr0 ** 0.875)
+        qc1 = np.maximum(qc0 - qrprod, 0.0)
+        qr1 = np.maximum(qr0 + qrprod + sed, 0.0)
+        pkt = pk * th0
+        qvs = pc * np.exp(f2x * (pkt - 273.0) / (pkt - 36.0))
+        prod = (qv0 - qvs) / (1.0 + qvs * f5 / (pkt - 36.0) ** 2)
+        rqr = r * qr1
+        ern = np.minimum(np.minimum(
+            dt0c * (((1.6 + 124.9 * rqr ** 0.2046) * rqr ** 0.525) / (2550000.0 * pc / (3.8 * qvs) + 540000.0))
+            * (np.maximum(qvs - qv0, 0.0) / (r * qvs)),
+            np.maximum(-prod - qc1, 0.0)), qr1)
+        mpc = np.maximum(prod, -qc1)
+        th_new = th0 + 2500000.0 / (1003.0 * pk) * (mpc - ern)
+        qv_new = np.maximum(qv0 - mpc + ern, 0.0)
+        qc_new = qc1 + mpc
+        qr_new = qr1 - ern
+        theta = np.where(am, th_new, th0)
+        qv = np.where(am, qv_new, qv0)
+        qc = np.where(am, qc_new, qc0)
+        qr = np.where(am, qr_new, qr0)
+        velqr = np.where((nt < rainsplit)[:, None], 36.34 * (qr * r) ** 0.1364 * rhalf, velqr)
+    return theta, qv, qc, qr, precl / rainsplit.astype(np.float64)
+
+
+def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_dens=True):
+    """Dyn.forcing_step for AF_TYPE 'DCMIP' with Kessler microphysics only
+    (nhm/dynamics/mod_dynamics.py:597-735 -> nhm/forcing/mod_forcing.py:207-321
+    forcing_step -> mod_af_dcmip.py:129-230 AF_dcmip, Kessler branch):
+    diagnostics of the regional prognostic (water tracers 0, 1, 2 = vapour,
+    cloud, rain), dry mixing ratios and density, Exner function and
+    potential temperature on kmin..kmax, the microphysics, the tracer and
+    energy tendencies (the energy one from increments), applied as
+    PROG + dt * f * rho * GSGAM2 with the water tendencies also added to
+    RHOG (update_tot_dens), then the halo exchange of PRG_var.  ``zf`` is
+    GRD_vz[..., GRD_Z] (i, j, k, l).  Returns (prg, prg_pl, precip (i, j, l))."""
+    out = prg.copy()
+    out_pl = prg_pl.copy()
+    PROG = out[..., 0:6]
+    PROGq = out[..., 6:]
+    DIAG = np.zeros(PROG.shape)
+    rho, ein, q, _, _, _ = diagnostics(g, PROG, PROGq, DIAG, prg_pl[..., 0:6].copy(), prg_pl[..., 6:].copy(),
+                                       np.zeros(prg_pl[..., 0:6].shape))
+    pre, tem = DIAG[..., I_pre], DIAG[..., I_tem]
+    if negative_fixer:
+        q = np.maximum(q, 0.0)
+    kmin, kmax = g.kmin, g.kmax
+    I, J, K, L = rho.shape
+    sl = slice(kmin, kmax + 1)
+    dt = g.dtl
+    col = lambda a: a.transpose(0, 1, 3, 2).reshape(I * J * L, K)[:, sl]      # (ncol, levels kmin..kmax)
+    qv_m, qc_m, qr_m = col(q[..., 0]), col(q[..., 1]), col(q[..., 2])
+    qd = 1.0 - qv_m - qc_m - qr_m
+    qvk, qck, qrk = qv_m / qd, qc_m / qd, qr_m / qd
+    rhod = col(rho) * qd
+    pk = (col(pre) / g.PRE00) ** (g.Rdry / g.CPdry)
+    theta_k = col(tem) / pk
+    theta_k, qvk, qck, qrk, precl = kessler(theta_k, qvk, qck, qrk, rhod, pk, dt, col(zf))
+    qd2 = 1.0 / (1.0 + qvk + qck + qrk)
+    qvk, qck, qrk = qvk * qd2, qck * qd2, qrk * qd2
+    cvk = qd2 * g.CVdry + qvk * g.CVW[0] + qck * g.CVW[1] + qrk * g.CVW[2]
+    tem_new = theta_k * pk
+    tem_old = col(tem)
+    cv_old = col(ein) / tem_old
+    dtem = tem_new - tem_old
+    dcv = cvk - cv_old
+
+    def grid(c):   # (ncol, levels kmin..kmax) -> (i, j, k, l), zero outside kmin..kmax
+        full = np.zeros((I * J * L, K))
+        full[:, sl] = c
+        return full.reshape(I, J, L, K).transpose(0, 1, 3, 2)
+    fe = grid((cv_old * dtem + tem_old * dcv + dcv * dtem) / dt)
+    fq = [grid((qvk - qv_m) / dt), grid((qck - qc_m) / dt), grid((qrk - qr_m) / dt)]
+    GS = g.VMTR_GSGAM2
+    zero = np.zeros_like(fe)
+    new = PROG.copy()
+    for v in (I_RHOGVX, I_RHOGVY, I_RHOGVZ):
+        new[..., v] = PROG[..., v] + dt * zero * rho * GS
+    new[..., I_RHOGE] = PROG[..., I_RHOGE] + dt * fe * rho * GS
+    rhog = PROG[..., I_RHOG]
+    for n in range(PROGq.shape[-1]):
+        f = fq[n] if n < 3 else zero
+        frhogq = f * rho * GS
+        if negative_fixer:
+            tmp = np.maximum(PROGq[..., n] + dt * frhogq, 0.0)
+            frhogq = (tmp - PROGq[..., n]) / dt
+            PROGq[..., n] = tmp
+        else:
+            PROGq[..., n] = PROGq[..., n] + dt * frhogq
+        if update_tot_dens and n < g.nqw:
+            rhog = rhog + dt * frhogq
+    new[..., I_RHOG] = rhog
+    out[..., 0:6] = new
+    comm(g, out, out_pl)
+    return out, out_pl, precl.reshape(I, J, L)
+
+
+# --------------------------------------------------------------------------
 # offline tracer advection  (integ_type TRCADV, DCMIP2012 test 1-1)
 # --------------------------------------------------------------------------
 TRC_A, TRC_RD, TRC_G, TRC_PI = 6371220.0, 287.0, 9.80616, 3.141592653589793238   # mod_af_trcadv.py:14-19

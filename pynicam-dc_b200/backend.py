@@ -33,6 +33,19 @@ from . import restart
 from .runtime import HIST_ITEMS, NicamCuda
 
 
+def _dcmip_flags(msc) -> dict:
+    """the DCMIP scheme flags the reference resolved (mod_af_dcmip.py
+    AF_dcmip_init): from ``msc.afdcmip`` when the services carry it, else the
+    reference module's instance"""
+    obj = getattr(msc, "afdcmip", None)
+    if obj is None:
+        import sys
+        mod = sys.modules.get("pynicamdc.nhm.forcing.mod_af_dcmip")
+        obj = getattr(mod, "afdcmip", None) if mod is not None else None
+    keys = ("USE_Kessler", "USE_SimpleMicrophys", "USE_ToyChemistry", "USE_HeldSuarez")
+    return {k: bool(getattr(obj, k, False)) for k in keys}
+
+
 def geo_from_msc(msc) -> dict:
     """Collect the setup arrays of the reference's services into the flat
     dict that ``NicamCuda`` uploads (attribute names kept)."""
@@ -87,6 +100,14 @@ def geo_from_msc(msc) -> dict:
         g["GRD_ZH"] = np.ascontiguousarray(grd.GRD_vz[:, :, :, :, grd.GRD_ZH])
         g["GRD_Z_pl"] = np.ascontiguousarray(grd.GRD_vz_pl[:, :, :, grd.GRD_Z])
         g["GRD_ZH_pl"] = np.ascontiguousarray(grd.GRD_vz_pl[:, :, :, grd.GRD_ZH])
+    elif getattr(m.rcnf, "AF_TYPE", "NONE") == "DCMIP":
+        # Kessler microphysics only (checked by CudaDyn._check_config): the
+        # full-level heights it reads and the forcing's flags (mod_forcing.py:44-71)
+        g["AF_dcmip_kessler"] = 1
+        g["GRD_Z"] = np.ascontiguousarray(m.grd.GRD_vz[:, :, :, :, m.grd.GRD_Z])
+        frc = getattr(m, "frc", None)
+        g["AF_negative_fixer"] = int(bool(getattr(frc, "NEGATIVE_FIXER", False)))
+        g["AF_update_tot_dens"] = int(bool(getattr(frc, "UPDATE_TOT_DENS", True)))
     elif getattr(m.rcnf, "AF_TYPE", "NONE") == "HELD-SUAREZ":
         # the column latitudes the forcing reads (mod_dynamics.py: GRD_LAT[:, :, K0, :])
         g["GRD_LAT"] = np.ascontiguousarray(m.grd.GRD_LAT[:, :, m.adm.ADM_K0, :])
@@ -152,7 +173,9 @@ class CudaDyn:
             self._check_config(msc)
             geo = geo_from_msc(msc)
         self.core = NicamCuda(geo, graph=graph, precision=precision)
-        self._forced = "GRD_LAT" in geo and str(np.asarray(geo.get("integ_type", "RK3"))) != "TRCADV"
+        self._forced = ("GRD_LAT" in geo and str(np.asarray(geo.get("integ_type", "RK3"))) != "TRCADV") or \
+            bool(int(np.asarray(geo.get("AF_dcmip_kessler", 0))))
+        self._kessler = bool(int(np.asarray(geo.get("AF_dcmip_kessler", 0))))
         self._host_stale = False
         self._device_valid = False
 
@@ -177,7 +200,14 @@ class CudaDyn:
         if int(getattr(r, "NQW_STR", 0)) != 0 or int(getattr(r, "I_QV", 0)) != 0 or \
                 int(getattr(r, "NQW_END", 0)) >= 6:
             raise NotImplementedError("cuda backend: water tracers must come first (NQW_STR = I_QV = 0), at most six")
-        if getattr(r, "AF_TYPE", "NONE") not in ("NONE", "HELD-SUAREZ"):
+        if getattr(r, "AF_TYPE", "NONE") == "DCMIP":
+            flags = _dcmip_flags(msc)
+            if not (flags.get("USE_Kessler") and not flags.get("USE_SimpleMicrophys")
+                    and not flags.get("USE_ToyChemistry") and not flags.get("USE_HeldSuarez")) \
+                    or getattr(r, "RAIN_TYPE", "DRY") != "WARM":
+                raise NotImplementedError("cuda backend: DCMIP forcing with Kessler microphysics only "
+                                          "(RAIN_TYPE WARM, no simple physics, toy chemistry or Held-Suarez)")
+        elif getattr(r, "AF_TYPE", "NONE") not in ("NONE", "HELD-SUAREZ"):
             raise NotImplementedError("cuda backend: artificial forcing NONE or HELD-SUAREZ only")
 
     # -- the reference's step API -------------------------------------------
@@ -203,11 +233,13 @@ class CudaDyn:
         af = getattr(msc.rcnf, "AF_TYPE", "NONE")
         if af in ("NONE", None):
             return None
-        if af != "HELD-SUAREZ" or not self._forced:
+        if af not in ("HELD-SUAREZ", "DCMIP") or not self._forced or (af == "DCMIP") != self._kessler:
             raise NotImplementedError(f"cuda backend: artificial forcing {af!r} is not configured on the device")
         self._ensure_device(msc)
         self.core.forcing_step()
         self._host_stale = True
+        if self._kessler:   # the reference's forcing_step returns the precipitation for DCMIP
+            return self.core.forcing_precip()
         return None
 
     def history_vars_step(self, msc, write_3d=True, write_2d=True):

@@ -365,6 +365,11 @@ struct nc_handle {
   FieldPair flx_v, rhog_t, flx[6], xc[9], ch[6], cm[6], q, gq[3], qa[3], Qmin, Qmax;
   FieldPair vph[8];             // horizontal terms of vp0 (div1, div2, dd, dpg)
   const double* hs_lat = nullptr;   // Held-Suarez latitude planes (optional)
+  // DCMIP forcing with Kessler microphysics (optional): full-level heights,
+  // the precipitation rate of the last forcing step, the forcing's flags
+  const double* kess_zf = nullptr;
+  double* kess_precip = nullptr;
+  int kess_negative_fixer = 0, kess_update_tot_dens = 1;
   // derived history diagnostics (optional setup; nc_history_vars)
   bool hist = false;
   const double *hist_hgt = nullptr, *hist_coslat = nullptr, *hist_zsfc = nullptr, *hist_area = nullptr;
@@ -1414,11 +1419,29 @@ int nc_forcing_step(nc_handle* h) {
   if (!h) return fail(NC_ERR_ARG, "nc_forcing_step: null handle");
   TRY(f64_only(h, "nc_forcing_step"));
   if (!h->have_state) return fail(NC_ERR_STATE, "nc_forcing_step: no state uploaded");
-  if (!h->hs_lat)
-    return fail(NC_ERR_STATE, "nc_forcing_step: the handle was created without AF_hs_lat_terms "
-                              "(Held-Suarez forcing not configured)");
+  if (!h->hs_lat && !h->kess_zf)
+    return fail(NC_ERR_STATE, "nc_forcing_step: the handle was created without AF_hs_lat_terms or "
+                              "AF_dcmip_kessler_zf (no forcing configured)");
   TRY(load_consts(h));
   const Dims& D = h->D;
+  if (h->kess_zf) {
+    KesslerArgs a;
+    for (int v = 0; v < 6; ++v) a.P.v[v] = h->P[v].r;
+    for (int n = 0; n < D.nq; ++n) a.Pq[n] = h->Pq[n].r;
+    a.nq = D.nq;
+    a.zf = h->kess_zf;
+    a.precip = h->kess_precip;
+    a.dt = h->dtl;
+    a.RdCp = h->C.Rdry / h->C.CPdry;
+    a.PRE00 = h->C.PRE00;
+    a.negative_fixer = h->kess_negative_fixer;
+    a.update_tot_dens = h->kess_update_tot_dens;
+    k_forcing_kessler<<<(unsigned)((D.npt2 + 63) / 64), 64, 0, h->stream>>>(a);
+    TRY(check_launch(h, "forcing_kessler"));
+    TRY(comm_prg<double>(h));
+    TRY(join_pl(h));
+    return 0;
+  }
   HsArgs a;
   for (int v = 0; v < 6; ++v) a.P.v[v] = h->P[v].r;
   for (int n = 0; n < h->C.nqw; ++n) a.Pqw[n] = h->Pq[n].r;
@@ -1437,6 +1460,20 @@ int nc_forcing_step(nc_handle* h) {
   TRY(check_launch(h, "forcing_hs"));
   TRY(comm_prg<double>(h));
   TRY(join_pl(h));
+  return 0;
+}
+
+int nc_forcing_precip(nc_handle* h, double* host) {
+  if (!h || !host) return fail(NC_ERR_ARG, "nc_forcing_precip: null argument");
+  if (!h->kess_precip) return fail(NC_ERR_STATE, "nc_forcing_precip: no Kessler forcing configured");
+  TRY(load_consts(h));
+  const Dims& D = h->D;
+  CU(cudaStreamSynchronize(h->stream));
+  std::vector<double> tmp((size_t)D.L * D.G * D.G);
+  CU(cudaMemcpy(tmp.data(), h->kess_precip, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int l = 0; l < D.L; ++l)
+    for (int j = 0; j < D.G; ++j)
+      for (int i = 0; i < D.G; ++i) host[((size_t)i * D.G + j) * D.L + l] = tmp[((size_t)l * D.G + j) * D.G + i];
   return 0;
 }
 
@@ -1670,6 +1707,25 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
     TRY(dev_alloc(h, &h->trc_time, 1));
     CU(cudaMemset(h->trc_time, 0, sizeof(double)));
   }
+  if (T.get("AF_dcmip_kessler_zf")) {   // DCMIP forcing with Kessler microphysics (nc_forcing_step)
+    if (T.get("AF_hs_lat_terms")) return fail(NC_ERR_ARG, "Held-Suarez and DCMIP forcing set-ups both given");
+    if (!T.get("PRE00")) return fail(NC_ERR_ARG, "AF_dcmip_kessler_zf given without PRE00");
+    if (C.nqw != 3) return fail(NC_ERR_ARG, "Kessler microphysics needs RAIN_TYPE WARM (NQW_END = 2: vapour, cloud, rain)");
+    if (D.kmax - D.kmin + 1 > NC_KESS_K || D.kmax - D.kmin < 1)
+      return fail(NC_ERR_ARG, "Kessler microphysics: 2.." + std::to_string(NC_KESS_K) + " model levels");
+    TRY(scalar(T, "PRE00", C.PRE00));
+    TRY(up_reg(h, T, "AF_dcmip_kessler_zf", D.KA, 1, &h->kess_zf));
+    double f;
+    if (T.get("AF_negative_fixer")) {
+      TRY(scalar(T, "AF_negative_fixer", f));
+      h->kess_negative_fixer = f != 0.0;
+    }
+    if (T.get("AF_update_tot_dens")) {
+      TRY(scalar(T, "AF_update_tot_dens", f));
+      h->kess_update_tot_dens = f != 0.0;
+    }
+    TRY(dev_alloc(h, &h->kess_precip, (size_t)D.L * D.G * D.G));
+  }
   if (T.get("AF_hs_lat_terms")) {   // Held-Suarez forcing configured (nc_forcing_step)
     if (!T.get("PRE00")) return fail(NC_ERR_ARG, "AF_hs_lat_terms given without PRE00");
     TRY(scalar(T, "PRE00", C.PRE00));
@@ -1772,7 +1828,7 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
     }
   }
   if (h->mixed) {
-    if (h->hist || h->hs_lat)
+    if (h->hist || h->hs_lat || h->kess_zf)
       return fail(NC_ERR_ARG, "the mixed-precision form runs the dynamics step and the offline tracer advection "
                               "only (no Held-Suarez forcing or history diagnostics set-up)");
     TRY(make_f32_geometry(h));

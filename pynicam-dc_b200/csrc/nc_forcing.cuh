@@ -79,6 +79,194 @@ __global__ void k_forcing_hs(HsArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// DCMIP forcing with Kessler warm-rain microphysics only (AF_TYPE 'DCMIP',
+// USE_Kessler: nhm/forcing/mod_forcing.py:207-321 forcing_step ->
+// mod_af_dcmip.py:129-230 AF_dcmip, Kessler branch -> kessler.py:9-179).
+// One thread per regional column (every column of the tile, as the
+// reference forces all of them before the exchange): the diagnostics with the
+// water tracers vapour, cloud, rain (0, 1, 2), dry mixing ratios, dry
+// density, Exner function and potential temperature on kmin..kmax, the
+// microphysics with its per-column sedimentation sub-cycles, the water and
+// energy tendencies (the energy one from increments), applied as
+// PROG + dt * f * rho * GSGAM2 on every level (f zero outside kmin..kmax;
+// the water tendencies also added to RHOG), and the column's precipitation
+// rate.  Same association order as the reference; exp, pow and sqrt are
+// CUDA's (sqrt correctly rounded, exp and pow within their documented ulp
+// bounds), so results can differ from numpy's in the last bits.
+// ---------------------------------------------------------------------------
+#define NC_KESS_K 64
+struct KesslerArgs {
+  Prog<double> P;                 // PROG, updated in place
+  double* Pq[NC_MAXNQ];           // tracer masses, updated in place
+  int nq;
+  const double* zf;               // full-level heights [l][k][j][i]
+  double* precip;                 // precipitation rate per column [l][j][i]
+  double dt, RdCp, PRE00;
+  int negative_fixer, update_tot_dens;
+};
+
+__global__ void k_forcing_kessler(KesslerArgs a) {
+  const int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, l;
+  if (!col_of(t, i, j, l)) return;
+  const Col c = col_reg(i, j, l);
+  const int KA = cD.KA, kmin = cD.kmin, kmax = cD.kmax, nz = kmax - kmin + 1;
+  double* const* P = a.P.v;
+  const double dt = a.dt;
+  // diagnostics at level k (kernels/diag.py:53-143) with the water mixing ratios
+  auto diag = [&](int k, double& rho, double& pre, double& tem, double& ein, double q[3]) {
+    const int p = c.at(k);
+    const double RHOG = P[0][p];
+    rho = RHOG / cG.GSGAM2[p];
+    ein = P[5][p] / RHOG;
+    for (int n = 0; n < 3; ++n) q[n] = a.Pq[n][p] / RHOG;
+    double qd, cv;
+    moist_qd_cv([&](int n) { return a.Pq[n][p] / RHOG; }, q[0], qd, cv);
+    tem = ein / cv;
+    pre = rho * tem * (qd * cC.Rdry + q[0] * cC.Rvap);
+    if (a.negative_fixer)
+      for (int n = 0; n < 3; ++n) q[n] = fmax(q[n], 0.0);
+  };
+  double th[NC_KESS_K], qv[NC_KESS_K], qc[NC_KESS_K], qr[NC_KESS_K], r[NC_KESS_K], rh[NC_KESS_K];
+  double pc[NC_KESS_K], vq[NC_KESS_K], pk[NC_KESS_K], z[NC_KESS_K];
+  // dry mixing ratios, dry density (in rh for now), Exner function, theta
+  for (int m = 0; m < nz; ++m) {
+    double rho, pre, tem, ein, q[3];
+    diag(kmin + m, rho, pre, tem, ein, q);
+    const double qd = 1.0 - q[0] - q[1] - q[2];
+    qv[m] = q[0] / qd;
+    qc[m] = q[1] / qd;
+    qr[m] = q[2] / qd;
+    rh[m] = rho * qd;
+    pk[m] = pow(pre / a.PRE00, a.RdCp);
+    th[m] = tem / pk[m];
+    z[m] = a.zf[c.at(kmin + m)];
+  }
+  // kessler.py: constants, local arrays, CFL and sub-cycles
+  const double f2x = 17.27, f5 = 237.3 * f2x * 2500000.0 / 1003.0, xk = 0.2875, psl = 1000.0, rhoqr = 1000.0;
+  const double rho0 = rh[0];
+  for (int m = 0; m < nz; ++m) {
+    r[m] = 0.001 * rh[m];
+    rh[m] = sqrt(rho0 / rh[m]);
+    pc[m] = 3.8 / (pow(pk[m], 1.0 / xk) * psl);
+    vq[m] = 36.34 * pow(qr[m] * r[m], 0.1364) * rh[m];
+  }
+  double cflmin = 0.0;
+  for (int m = 0; m < nz - 1; ++m) {
+    const double cfl = (vq[m] != 0.0) ? 0.8 * (z[m + 1] - z[m]) / vq[m] : dt;
+    cflmin = (m == 0 || cfl < cflmin) ? cfl : cflmin;
+  }
+  const double dt_max = fmin(dt, cflmin);
+  const int rainsplit = (int)ceil(dt / dt_max);
+  const double dt0 = dt / (double)rainsplit;
+  double precl = 0.0;
+  for (int nt = 1; nt <= rainsplit; ++nt) {
+    precl = precl + rho0 * qr[0] * vq[0] / rhoqr;
+    // sedimentation from the start-of-sub-cycle rain (upstream), then the
+    // level updates; sed of level m reads level m+1, so form it first
+    double sed_next = 0.0;
+    for (int m = 0; m < nz; ++m) {
+      double sed;
+      if (m < nz - 1) {
+        const double num = r[m + 1] * qr[m + 1] * vq[m + 1] - r[m] * qr[m] * vq[m];
+        sed = dt0 * num / (r[m] * (z[m + 1] - z[m]));
+      } else {
+        sed = -dt0 * qr[m] * vq[m] / (0.5 * (z[m] - z[m - 1]));
+      }
+      // level m - 1 is updated once level m's sedimentation (which reads its old rain) is formed
+      if (m > 0) {
+        const int u = m - 1;
+        const double qc0 = qc[u], qr0 = qr[u], qv0 = qv[u], th0 = th[u];
+        const double qrprod = qc0 - (qc0 - dt0 * fmax(0.001 * (qc0 - 0.001), 0.0)) / (1.0 + dt0 * 2.2 * pow(qr0, 0.875));
+        const double qc1 = fmax(qc0 - qrprod, 0.0);
+        const double qr1 = fmax(qr0 + qrprod + sed_next, 0.0);
+        const double pkt = pk[u] * th0;
+        const double qvs = pc[u] * exp(f2x * (pkt - 273.0) / (pkt - 36.0));
+        const double prod = (qv0 - qvs) / (1.0 + qvs * f5 / ((pkt - 36.0) * (pkt - 36.0)));
+        const double rqr = r[u] * qr1;
+        const double ern =
+            fmin(fmin(dt0 * (((1.6 + 124.9 * pow(rqr, 0.2046)) * pow(rqr, 0.525)) /
+                             (2550000.0 * pc[u] / (3.8 * qvs) + 540000.0)) *
+                          (fmax(qvs - qv0, 0.0) / (r[u] * qvs)),
+                      fmax(-prod - qc1, 0.0)),
+                 qr1);
+        const double mpc = fmax(prod, -qc1);
+        th[u] = th0 + 2500000.0 / (1003.0 * pk[u]) * (mpc - ern);
+        qv[u] = fmax(qv0 - mpc + ern, 0.0);
+        qc[u] = qc1 + mpc;
+        qr[u] = qr1 - ern;
+      }
+      sed_next = sed;
+    }
+    {   // the top level
+      const int u = nz - 1;
+      const double qc0 = qc[u], qr0 = qr[u], qv0 = qv[u], th0 = th[u];
+      const double qrprod = qc0 - (qc0 - dt0 * fmax(0.001 * (qc0 - 0.001), 0.0)) / (1.0 + dt0 * 2.2 * pow(qr0, 0.875));
+      const double qc1 = fmax(qc0 - qrprod, 0.0);
+      const double qr1 = fmax(qr0 + qrprod + sed_next, 0.0);
+      const double pkt = pk[u] * th0;
+      const double qvs = pc[u] * exp(f2x * (pkt - 273.0) / (pkt - 36.0));
+      const double prod = (qv0 - qvs) / (1.0 + qvs * f5 / ((pkt - 36.0) * (pkt - 36.0)));
+      const double rqr = r[u] * qr1;
+      const double ern =
+          fmin(fmin(dt0 * (((1.6 + 124.9 * pow(rqr, 0.2046)) * pow(rqr, 0.525)) /
+                           (2550000.0 * pc[u] / (3.8 * qvs) + 540000.0)) *
+                        (fmax(qvs - qv0, 0.0) / (r[u] * qvs)),
+                    fmax(-prod - qc1, 0.0)),
+               qr1);
+      const double mpc = fmax(prod, -qc1);
+      th[u] = th0 + 2500000.0 / (1003.0 * pk[u]) * (mpc - ern);
+      qv[u] = fmax(qv0 - mpc + ern, 0.0);
+      qc[u] = qc1 + mpc;
+      qr[u] = qr1 - ern;
+    }
+    if (nt < rainsplit)
+      for (int m = 0; m < nz; ++m) vq[m] = 36.34 * pow(qr[m] * r[m], 0.1364) * rh[m];
+  }
+  a.precip[(l * cD.G + j) * cD.G + i] = precl / (double)rainsplit;
+  // back to wet mixing ratios, the tendencies, and their application on every level
+  for (int k = 0; k < KA; ++k) {
+    const int p = c.at(k);
+    double rho, pre, tem, ein, q[3];
+    diag(k, rho, pre, tem, ein, q);
+    double fe = 0.0, fq[3] = {0.0, 0.0, 0.0};
+    if (k >= kmin && k <= kmax) {
+      const int m = k - kmin;
+      const double qd2 = 1.0 / (1.0 + qv[m] + qc[m] + qr[m]);
+      const double qvk = qv[m] * qd2, qck = qc[m] * qd2, qrk = qr[m] * qd2;
+      const double cvk = qd2 * cC.CVdry + qvk * cC.CVW[0] + qck * cC.CVW[1] + qrk * cC.CVW[2];
+      fq[0] = (qvk - q[0]) / dt;
+      fq[1] = (qck - q[1]) / dt;
+      fq[2] = (qrk - q[2]) / dt;
+      const double tem_new = th[m] * pk[m];
+      const double cv_old = ein / tem;
+      const double dtem = tem_new - tem;
+      const double dcv = cvk - cv_old;
+      fe = (cv_old * dtem + tem * dcv + dcv * dtem) / dt;
+    }
+    const double gs = cG.GSGAM2[p];
+    P[1][p] = P[1][p] + dt * 0.0 * rho * gs;
+    P[2][p] = P[2][p] + dt * 0.0 * rho * gs;
+    P[3][p] = P[3][p] + dt * 0.0 * rho * gs;
+    P[5][p] = P[5][p] + dt * fe * rho * gs;
+    double rhog = P[0][p];
+    for (int n = 0; n < a.nq; ++n) {
+      double frhogq = (n < 3 ? fq[n] : 0.0) * rho * gs;
+      double* Q = a.Pq[n];
+      if (a.negative_fixer) {
+        const double tmp = fmax(Q[p] + dt * frhogq, 0.0);
+        frhogq = (tmp - Q[p]) / dt;
+        Q[p] = tmp;
+      } else {
+        Q[p] = Q[p] + dt * frhogq;
+      }
+      if (a.update_tot_dens && n < cC.nqw) rhog = rhog + dt * frhogq;
+    }
+    P[0][p] = rhog;
+  }
+}
+
 }  // namespace nc
 
 namespace nc {

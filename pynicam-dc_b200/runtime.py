@@ -35,7 +35,7 @@ EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_sta
            "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",
            "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_forcing_step", "nc_history_vars", "nc_restart_pack",
            "nc_restart_unpack", "nc_restart_finish", "nc_divide_known", "nc_vsolve", "nc_vadv_lin", "nc_laplacian",
-           "nc_trc_step_lin", "nc_set_time", "nc_trc_prepare", "nc_divergence", "nc_gradient", "nc_last_error", "nc_destroy")
+           "nc_trc_step_lin", "nc_set_time", "nc_trc_prepare", "nc_divergence", "nc_gradient", "nc_forcing_precip", "nc_last_error", "nc_destroy")
 
 
 def load_library(path: str = LIB_PATH):
@@ -94,6 +94,8 @@ def load_library(path: str = LIB_PATH):
     lib.nc_set_time.argtypes = [vp, ctypes.c_double]
     lib.nc_trc_prepare.argtypes = [vp]
     lib.nc_divergence.argtypes = [vp, i32, dp, dp, dp, dp, vp]
+    lib.nc_forcing_precip.argtypes = [vp, dp]
+    lib.nc_forcing_precip.restype = ctypes.c_int
     lib.nc_gradient.argtypes = [vp, i32, dp, dp, dp, dp, vp]
     for f in ("nc_vsolve", "nc_vadv_lin", "nc_laplacian", "nc_trc_step_lin", "nc_set_time", "nc_trc_prepare",
               "nc_divergence", "nc_gradient"):
@@ -245,6 +247,12 @@ def setup_table(geo: dict) -> dict:
         sinlat, coslat = np.abs(np.sin(lat)), np.abs(np.cos(lat))
         t["AF_hs_lat_terms"] = np.ascontiguousarray(np.stack([sinlat ** 2, coslat ** 2, coslat ** 4], axis=-1))
         t["PRE00"] = np.asarray(float(_scalar(geo["PRE00"])), np.float64)
+    if int(np.asarray(geo.get("AF_dcmip_kessler", 0))):   # DCMIP forcing, Kessler microphysics only
+        t["AF_dcmip_kessler_zf"] = np.ascontiguousarray(geo["GRD_Z"], np.float64)
+        t["PRE00"] = np.asarray(float(_scalar(geo["PRE00"])), np.float64)
+        for k in ("AF_negative_fixer", "AF_update_tot_dens"):
+            if k in geo:
+                t[k] = np.asarray(float(_scalar(geo[k])), np.float64)
     if "hist_hgt" in geo:   # derived history diagnostics (nc_history_vars)
         G, L = int(_scalar(geo["gall_1d"])), int(_scalar(geo["lall"]))
         plane = lambda x: np.ascontiguousarray(np.asarray(x, np.float64).reshape(G, G, 1, L))
@@ -487,6 +495,13 @@ class NicamCuda:
         """Dyn.forcing_step for AF_TYPE 'HELD-SUAREZ' (nc_forcing_step); the
         handle must have been built from a setup with GRD_LAT"""
         _check(self._lib.nc_forcing_step(self._h))
+
+    def forcing_precip(self) -> np.ndarray:
+        """the precipitation rate of the last DCMIP Kessler forcing step,
+        (gall_1d, gall_1d, lall) (nc_forcing_precip)"""
+        out = np.empty((self.shape[0], self.shape[1], self.shape[3]))
+        _check(self._lib.nc_forcing_precip(self._h, out.ctypes.data))
+        return out
 
     def history_vars(self, names, nstep: int, dt: float) -> dict:
         """the derived history diagnostics ``names`` (from ``HIST_ITEMS``) of

@@ -38,6 +38,19 @@ def golden_warm():
 
 
 @pytest.fixture(scope="session")
+def golden_kessler():
+    """gl03 z10 RAIN_TYPE WARM with the reference's DCMIP forcing, Kessler
+    microphysics only (make_kessler.py): setup arrays (GRD_Z the full-level
+    heights), three states and the precipitation rate after each step"""
+    import numpy as np
+    from make_golden import load
+    path = os.path.join(GOLDEN, "gl03_z10_kessler.npz")
+    geo, st = load(path)
+    d = np.load(path)
+    return geo, st, {k: d[k] for k in d.files if k.startswith("precip")}
+
+
+@pytest.fixture(scope="session")
 def golden_hs():
     """gl03 z10 with the reference's Held-Suarez forcing (make_hs.py): setup
     arrays (plus GRD_LAT at K0), the column latitudes and three states"""

@@ -1,6 +1,7 @@
-"""Held-Suarez forcing step on the device (nc_forcing_step) against the
+"""Forcing steps on the device (nc_forcing_step): Held-Suarez against the
 reference run with AF_TYPE 'HELD-SUAREZ' (tests/golden/make_hs.py) and
-against the oracle.
+against the oracle; DCMIP forcing with Kessler microphysics against the
+reference run with AF_TYPE 'DCMIP' (tests/golden/make_kessler.py).
 
 The forcing's T_eq uses log and pow, which CUDA and numpy may round
 differently in the last bit, so these comparisons use a tolerance: relative
@@ -67,7 +68,33 @@ def test_forcing_needs_its_setup(pkg, golden):
     c = pkg.NicamCuda(geo, graph=False)
     try:
         c.upload(st["state0"], st["state0_pl"])
-        with pytest.raises(pkg.NicamError, match="Held-Suarez"):
+        with pytest.raises(pkg.NicamError, match="no forcing configured"):
             c.forcing_step()
+    finally:
+        c.close()
+
+
+def test_kessler_forcing_vs_reference(pkg, golden_kessler):
+    """dynamics step + DCMIP forcing with Kessler microphysics (RAIN_TYPE
+    WARM) on the device against the reference's two steps: the microphysics
+    calls exp and pow, which are CUDA's, so the states and the precipitation
+    agree to relative L2 <= 1e-12 per prognostic rather than bit for bit"""
+    geo, st, pr = golden_kessler
+    g = dict(geo)
+    g["AF_dcmip_kessler"] = 1
+    c = pkg.NicamCuda(g, graph=False)
+    try:
+        c.upload(st["state0"], st["state0_pl"])
+        for n in (1, 2):
+            c.step(1)
+            c.forcing_step()
+            s, sp = c.download()
+            precip = c.forcing_precip()
+            for v in range(s.shape[-1]):
+                for a, b in ((s[..., v], st[f"state{n}"][..., v]), (sp[..., v], st[f"state{n}_pl"][..., v])):
+                    den = np.sqrt(np.sum(b * b))
+                    assert np.sqrt(np.sum((a - b) ** 2)) <= 1e-12 * max(den, 1e-300), (n, v)
+            want = pr[f"precip{n}"]
+            assert np.sqrt(np.sum((precip - want) ** 2)) <= 1e-12 * np.sqrt(np.sum(want * want)), n
     finally:
         c.close()

@@ -25,6 +25,30 @@ def test_oracle_matches_reference_warm_rain(golden_warm):
         assert np.array_equal(out_pl, st[f"state{s + 1}_pl"]), f"step {s + 1} pole"
 
 
+def test_oracle_kessler_forcing_matches_reference(golden_kessler):
+    """dynamics step + DCMIP forcing with Kessler microphysics, against the
+    reference run (tests/golden/make_kessler.py): states and precipitation"""
+    geo, st, pr = golden_kessler
+    G = O.Geo(geo)
+    s, sp = st["state0"], st["state0_pl"]
+    for n in (1, 2):
+        s, sp = O.dynamics_step(G, s, sp)
+        s, sp, precip = O.forcing_step_kessler(G, s, sp, geo["GRD_Z"])
+        assert np.array_equal(s, st[f"state{n}"]) and np.array_equal(sp, st[f"state{n}_pl"]), n
+        assert np.array_equal(precip, pr[f"precip{n}"]), n
+
+
+def test_kessler_fixture_is_active(golden_warm, golden_kessler):
+    """the microphysics changed the water and energy against the unforced
+    WARM run of the same case, and it rained somewhere"""
+    _, st0 = golden_warm
+    _, st, pr = golden_kessler
+    assert np.array_equal(st["state0"], st0["state0"])
+    assert np.abs(st["state1"][..., 5] - st0["state1"][..., 5]).max() > 1.0
+    assert np.abs(st["state1"][..., 8] - st0["state1"][..., 8]).max() > 1e-4
+    assert pr["precip1"].max() > 0.0
+
+
 def test_golden_tracer_is_nontrivial(golden):
     _, st = golden
     q = st["state0"][..., 6]
