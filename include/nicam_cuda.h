@@ -239,7 +239,14 @@ int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* g
  * water and energy tendencies applied to the tracers, RHOGE and (with
  * update_tot_dens) RHOG, then the exchange.  exp and pow are CUDA's, so
  * results can differ from numpy's in the last bits.  The precipitation rate
- * of the step per column is read with nc_forcing_precip. */
+ * of the step per column is read with nc_forcing_precip.  With the DCMIP
+ * terminator toy chemistry as well (USE_ToyChemistry, CHEM_TYPE PASSIVE;
+ * mod_af_dcmip.py:171-187, terminator.py:20-70), the handle is also created
+ * with "AF_dcmip_chem" (int64 [NCHEM_STR, NCHEM_END], the Cl and Cl2 tracer
+ * indices, both outside the water range) and "AF_dcmip_lat" / "AF_dcmip_lon"
+ * (GRD_LAT / GRD_LON[:, :, K0, :] in radians, (gall_1d, gall_1d, 1, lall));
+ * the Cl / Cl2 tendencies (per dry air, analytic over dt; sin, cos, exp and
+ * sqrt are CUDA's) join the tracer tendencies on kmin..kmax. */
 int nc_forcing_step(nc_handle* h);
 
 /* The precipitation rate [m/s] of the last DCMIP Kessler forcing step per

@@ -1750,7 +1750,28 @@ def kessler(theta, qv, qc, qr, rho, pk, dt, z):
     return theta, qv, qc, qr, precl / rainsplit.astype(np.float64)
 
 
-def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_dens=True):
+def terminator_tendency(lat_deg, lon_deg, cl, cl2, dt):
+    """nhm/forcing/terminator.py:20-70 tendency_terminator: the Cl / Cl2
+    photolysis-recombination rates (k1 from the solar zenith projection
+    toward 20 N, 300 E, k2 = 1) integrated analytically over dt; returns
+    (cl_f, cl2_f) per second, cl2_f = -cl_f / 2"""
+    d2r = np.pi / 180.0
+    lat_c, lon_c = 20.0 * d2r, 300.0 * d2r
+    la, lo = lat_deg * d2r, lon_deg * d2r
+    k1 = np.maximum(0.0, np.sin(la) * np.sin(lat_c) + np.cos(la) * np.cos(lat_c) * np.cos(lo - lon_c))
+    k2 = 1.0
+    r = k1 / (4.0 * k2)
+    cly = cl + 2.0 * cl2
+    det = np.sqrt(r * r + 2.0 * r * cly)
+    expdt = np.exp(-4.0 * k2 * det * dt)
+    mask = np.abs(det * k2 * dt) > 1.0e-16
+    det_safe = np.where(mask, det, np.ones_like(det))
+    el = np.where(mask, (1.0 - expdt) / det_safe / dt, np.full_like(det, 4.0 * k2))
+    cl_f = -el * (cl - det + r) * (cl + det + r) / (1.0 + expdt + dt * el * (cl + r))
+    return cl_f, -cl_f / 2.0
+
+
+def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_dens=True, chem=None):
     """Dyn.forcing_step for AF_TYPE 'DCMIP' with Kessler microphysics only
     (nhm/dynamics/mod_dynamics.py:597-735 -> nhm/forcing/mod_forcing.py:207-321
     forcing_step -> mod_af_dcmip.py:129-230 AF_dcmip, Kessler branch):
@@ -1760,7 +1781,10 @@ def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_de
     energy tendencies (the energy one from increments), applied as
     PROG + dt * f * rho * GSGAM2 with the water tendencies also added to
     RHOG (update_tot_dens), then the halo exchange of PRG_var.  ``zf`` is
-    GRD_vz[..., GRD_Z] (i, j, k, l).  Returns (prg, prg_pl, precip (i, j, l))."""
+    GRD_vz[..., GRD_Z] (i, j, k, l).  ``chem`` = (lat, lon, nchem_str,
+    nchem_end) adds the terminator toy chemistry (mod_af_dcmip.py:171-187;
+    lat, lon of the columns in radians (i, j, l)) on the Cl / Cl2 tracers.
+    Returns (prg, prg_pl, precip (i, j, l))."""
     out = prg.copy()
     out_pl = prg_pl.copy()
     PROG = out[..., 0:6]
@@ -1798,6 +1822,16 @@ def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_de
         return full.reshape(I, J, L, K).transpose(0, 1, 3, 2)
     fe = grid((cv_old * dtem + tem_old * dcv + dcv * dtem) / dt)
     fq = [grid((qvk - qv_m) / dt), grid((qck - qc_m) / dt), grid((qrk - qr_m) / dt)]
+    fq += [None] * (PROGq.shape[-1] - 3)
+    if chem is not None:
+        lat, lon, n_cl, n_cl2 = chem
+        d2r = np.pi / 180.0
+        lat_deg = (lat.reshape(I * J * L) / d2r)[:, None]
+        lon_deg = (lon.reshape(I * J * L) / d2r)[:, None]
+        qvd = 1.0 - qv_m
+        cl_f, cl2_f = terminator_tendency(lat_deg, lon_deg, col(q[..., n_cl]) / qvd, col(q[..., n_cl2]) / qvd, dt)
+        fq[n_cl] = grid(cl_f * qvd)
+        fq[n_cl2] = grid(cl2_f * qvd)
     GS = g.VMTR_GSGAM2
     zero = np.zeros_like(fe)
     new = PROG.copy()
@@ -1806,7 +1840,7 @@ def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_de
     new[..., I_RHOGE] = PROG[..., I_RHOGE] + dt * fe * rho * GS
     rhog = PROG[..., I_RHOG]
     for n in range(PROGq.shape[-1]):
-        f = fq[n] if n < 3 else zero
+        f = fq[n] if fq[n] is not None else zero
         frhogq = f * rho * GS
         if negative_fixer:
             tmp = np.maximum(PROGq[..., n] + dt * frhogq, 0.0)

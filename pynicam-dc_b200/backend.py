@@ -108,6 +108,11 @@ def geo_from_msc(msc) -> dict:
         frc = getattr(m, "frc", None)
         g["AF_negative_fixer"] = int(bool(getattr(frc, "NEGATIVE_FIXER", False)))
         g["AF_update_tot_dens"] = int(bool(getattr(frc, "UPDATE_TOT_DENS", True)))
+        if _dcmip_flags(msc)["USE_ToyChemistry"]:   # terminator chemistry on the Cl / Cl2 tracers
+            g["AF_dcmip_chem"] = np.asarray([m.rcnf.NCHEM_STR, m.rcnf.NCHEM_END], np.int64)
+            K0 = m.adm.ADM_K0
+            g["AF_dcmip_lat"] = np.ascontiguousarray(m.grd.GRD_LAT[:, :, K0, :])
+            g["AF_dcmip_lon"] = np.ascontiguousarray(m.grd.GRD_LON[:, :, K0, :])
     elif getattr(m.rcnf, "AF_TYPE", "NONE") == "HELD-SUAREZ":
         # the column latitudes the forcing reads (mod_dynamics.py: GRD_LAT[:, :, K0, :])
         g["GRD_LAT"] = np.ascontiguousarray(m.grd.GRD_LAT[:, :, m.adm.ADM_K0, :])
@@ -203,10 +208,11 @@ class CudaDyn:
         if getattr(r, "AF_TYPE", "NONE") == "DCMIP":
             flags = _dcmip_flags(msc)
             if not (flags.get("USE_Kessler") and not flags.get("USE_SimpleMicrophys")
-                    and not flags.get("USE_ToyChemistry") and not flags.get("USE_HeldSuarez")) \
-                    or getattr(r, "RAIN_TYPE", "DRY") != "WARM":
-                raise NotImplementedError("cuda backend: DCMIP forcing with Kessler microphysics only "
-                                          "(RAIN_TYPE WARM, no simple physics, toy chemistry or Held-Suarez)")
+                    and not flags.get("USE_HeldSuarez")) or getattr(r, "RAIN_TYPE", "DRY") != "WARM" or \
+                    (flags.get("USE_ToyChemistry") and int(getattr(r, "NCHEM_END", -1)) - int(getattr(r, "NCHEM_STR", -1)) != 1):
+                raise NotImplementedError("cuda backend: DCMIP forcing with Kessler microphysics and optionally the "
+                                          "terminator chemistry (RAIN_TYPE WARM, two chemistry tracers; no simple "
+                                          "physics or Held-Suarez)")
         elif getattr(r, "AF_TYPE", "NONE") not in ("NONE", "HELD-SUAREZ"):
             raise NotImplementedError("cuda backend: artificial forcing NONE or HELD-SUAREZ only")
 

@@ -370,6 +370,8 @@ struct nc_handle {
   const double* kess_zf = nullptr;
   double* kess_precip = nullptr;
   int kess_negative_fixer = 0, kess_update_tot_dens = 1;
+  int kess_n_cl = -1, kess_n_cl2 = -1;      // terminator toy chemistry tracers (optional)
+  const double *kess_lat = nullptr, *kess_lon = nullptr;
   // derived history diagnostics (optional setup; nc_history_vars)
   bool hist = false;
   const double *hist_hgt = nullptr, *hist_coslat = nullptr, *hist_zsfc = nullptr, *hist_area = nullptr;
@@ -1436,6 +1438,10 @@ int nc_forcing_step(nc_handle* h) {
     a.PRE00 = h->C.PRE00;
     a.negative_fixer = h->kess_negative_fixer;
     a.update_tot_dens = h->kess_update_tot_dens;
+    a.n_cl = h->kess_n_cl;
+    a.n_cl2 = h->kess_n_cl2;
+    a.lat = h->kess_lat;
+    a.lon = h->kess_lon;
     k_forcing_kessler<<<(unsigned)((D.npt2 + 63) / 64), 64, 0, h->stream>>>(a);
     TRY(check_launch(h, "forcing_kessler"));
     TRY(comm_prg<double>(h));
@@ -1725,6 +1731,17 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
       h->kess_update_tot_dens = f != 0.0;
     }
     TRY(dev_alloc(h, &h->kess_precip, (size_t)D.L * D.G * D.G));
+    if (T.get("AF_dcmip_chem")) {   // the terminator toy chemistry on tracers (Cl, Cl2)
+      const nc_array* ch = T.get("AF_dcmip_chem");
+      if (ch->dtype != NC_I64 || numel(ch) != 2) return fail(NC_ERR_ARG, "AF_dcmip_chem: two int64 tracer indices");
+      const long long* ix2 = (const long long*)ch->data;
+      if (ix2[0] < C.nqw || ix2[1] < C.nqw || ix2[0] >= D.nq || ix2[1] >= D.nq || ix2[0] == ix2[1])
+        return fail(NC_ERR_ARG, "AF_dcmip_chem: indices of two distinct non-water tracers");
+      h->kess_n_cl = (int)ix2[0];
+      h->kess_n_cl2 = (int)ix2[1];
+      TRY(up_reg(h, T, "AF_dcmip_lat", 1, 1, &h->kess_lat));
+      TRY(up_reg(h, T, "AF_dcmip_lon", 1, 1, &h->kess_lon));
+    }
   }
   if (T.get("AF_hs_lat_terms")) {   // Held-Suarez forcing configured (nc_forcing_step)
     if (!T.get("PRE00")) return fail(NC_ERR_ARG, "AF_hs_lat_terms given without PRE00");

@@ -104,7 +104,28 @@ struct KesslerArgs {
   double* precip;                 // precipitation rate per column [l][j][i]
   double dt, RdCp, PRE00;
   int negative_fixer, update_tot_dens;
+  // terminator toy chemistry (optional): the Cl and Cl2 tracer indices, the
+  // column latitude and longitude [l][j][i] in radians
+  int n_cl, n_cl2;
+  const double *lat, *lon;
 };
+
+// nhm/forcing/terminator.py:20-70 tendency_terminator at one level: the Cl
+// tendency (Cl2's is minus half of it); sin, cos, exp and sqrt are CUDA's
+__device__ __forceinline__ double terminator_cl_f(double lat_deg, double lon_deg, double cl, double cl2, double dt) {
+  const double d2r = 3.141592653589793 / 180.0;
+  const double lat_c = 20.0 * d2r, lon_c = 300.0 * d2r;
+  const double la = lat_deg * d2r, lo = lon_deg * d2r;
+  const double k1 = fmax(0.0, sin(la) * sin(lat_c) + cos(la) * cos(lat_c) * cos(lo - lon_c));
+  const double k2 = 1.0;
+  const double r = k1 / (4.0 * k2);
+  const double cly = cl + 2.0 * cl2;
+  const double det = sqrt(r * r + 2.0 * r * cly);
+  const double expdt = exp(-4.0 * k2 * det * dt);
+  const bool mask = fabs(det * k2 * dt) > 1.0e-16;
+  const double el = mask ? (1.0 - expdt) / det / dt : 4.0 * k2;
+  return -el * (cl - det + r) * (cl + det + r) / (1.0 + expdt + dt * el * (cl + r));
+}
 
 __global__ void k_forcing_kessler(KesslerArgs a) {
   const int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
@@ -230,7 +251,22 @@ __global__ void k_forcing_kessler(KesslerArgs a) {
     const int p = c.at(k);
     double rho, pre, tem, ein, q[3];
     diag(k, rho, pre, tem, ein, q);
-    double fe = 0.0, fq[3] = {0.0, 0.0, 0.0};
+    double fe = 0.0, fq[3] = {0.0, 0.0, 0.0}, fcl = 0.0, fcl2 = 0.0;
+    if (k >= kmin && k <= kmax && a.n_cl >= 0) {   // mod_af_dcmip.py:171-187
+      const double d2r = 3.141592653589793 / 180.0;
+      const int cidx = (l * cD.G + j) * cD.G + i;
+      const double lat_deg = a.lat[cidx] / d2r, lon_deg = a.lon[cidx] / d2r;
+      const double RHOG = P[0][p];
+      double qcl = a.Pq[a.n_cl][p] / RHOG, qcl2 = a.Pq[a.n_cl2][p] / RHOG;
+      if (a.negative_fixer) {
+        qcl = fmax(qcl, 0.0);
+        qcl2 = fmax(qcl2, 0.0);
+      }
+      const double qvd = 1.0 - q[0];
+      const double cl_f = terminator_cl_f(lat_deg, lon_deg, qcl / qvd, qcl2 / qvd, dt);
+      fcl = cl_f * qvd;
+      fcl2 = (-cl_f / 2.0) * qvd;
+    }
     if (k >= kmin && k <= kmax) {
       const int m = k - kmin;
       const double qd2 = 1.0 / (1.0 + qv[m] + qc[m] + qr[m]);
@@ -252,7 +288,8 @@ __global__ void k_forcing_kessler(KesslerArgs a) {
     P[5][p] = P[5][p] + dt * fe * rho * gs;
     double rhog = P[0][p];
     for (int n = 0; n < a.nq; ++n) {
-      double frhogq = (n < 3 ? fq[n] : 0.0) * rho * gs;
+      const double f = n < 3 ? fq[n] : (n == a.n_cl ? fcl : (n == a.n_cl2 ? fcl2 : 0.0));
+      double frhogq = f * rho * gs;
       double* Q = a.Pq[n];
       if (a.negative_fixer) {
         const double tmp = fmax(Q[p] + dt * frhogq, 0.0);

@@ -253,6 +253,11 @@ def setup_table(geo: dict) -> dict:
         for k in ("AF_negative_fixer", "AF_update_tot_dens"):
             if k in geo:
                 t[k] = np.asarray(float(_scalar(geo[k])), np.float64)
+        if "AF_dcmip_chem" in geo:   # terminator toy chemistry: (Cl, Cl2) tracer indices, column lat / lon
+            G, L = int(_scalar(geo["gall_1d"])), int(_scalar(geo["lall"]))
+            t["AF_dcmip_chem"] = np.ascontiguousarray(np.asarray(geo["AF_dcmip_chem"]).reshape(2), np.int64)
+            for k in ("AF_dcmip_lat", "AF_dcmip_lon"):
+                t[k] = np.ascontiguousarray(np.asarray(geo[k], np.float64).reshape(G, G, 1, L))
     if "hist_hgt" in geo:   # derived history diagnostics (nc_history_vars)
         G, L = int(_scalar(geo["gall_1d"])), int(_scalar(geo["lall"]))
         plane = lambda x: np.ascontiguousarray(np.asarray(x, np.float64).reshape(G, G, 1, L))

@@ -51,6 +51,21 @@ def golden_kessler():
 
 
 @pytest.fixture(scope="session")
+def golden_kessler_chem():
+    """the Kessler case with the reference's terminator toy chemistry as well
+    (make_kessler.py --chem): Cl and Cl2 in tracers 3 and 4 (NCHEM_STR,
+    NCHEM_END) away from their equilibrium, the column latitudes and
+    longitudes (GRD_LAT, GRD_LON at K0, radians), three states and the
+    precipitation after each step"""
+    import numpy as np
+    from make_golden import load
+    path = os.path.join(GOLDEN, "gl03_z10_kessler_chem.npz")
+    geo, st = load(path)
+    d = np.load(path)
+    return geo, st, {k: d[k] for k in d.files if k.startswith("precip")}
+
+
+@pytest.fixture(scope="session")
 def golden_hs():
     """gl03 z10 with the reference's Held-Suarez forcing (make_hs.py): setup
     arrays (plus GRD_LAT at K0), the column latitudes and three states"""

@@ -12,7 +12,7 @@ import numpy as np
 
 
 def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_type: str = "RK3",
-             coords: dict = None, hist: dict = None, io_names=None):
+             coords: dict = None, hist: dict = None, io_names=None, dcmip: dict = None):
     g = {k: np.asarray(v) for k, v in geo.items()}
     sc = lambda k: g[k].reshape(-1)[0].item()
     adm = NS(ADM_kall=int(sc("kall")), ADM_kmin=int(sc("kmin")), ADM_kmax=int(sc("kmax")),
@@ -82,6 +82,17 @@ def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_
            tim=tim, numf=numf, dyn=dyn, ppm=ppm, prgv=prgv)
     if satr is not None:
         m.satr = satr
+    if dcmip is not None:   # DCMIP forcing: Kessler (and the terminator chemistry when lat / lon are given)
+        chem = "GRD_LAT" in dcmip
+        grd.GRD_Z = 0
+        grd.GRD_vz = np.asarray(dcmip["GRD_Z"])[..., None]
+        if chem:
+            grd.GRD_LAT = np.asarray(dcmip["GRD_LAT"])[:, :, None, :]
+            grd.GRD_LON = np.asarray(dcmip["GRD_LON"])[:, :, None, :]
+            rcnf.NCHEM_STR, rcnf.NCHEM_END = int(dcmip["NCHEM_STR"]), int(dcmip["NCHEM_END"])
+        rcnf.RAIN_TYPE = "WARM"
+        m.afdcmip = NS(USE_Kessler=True, USE_SimpleMicrophys=False, USE_ToyChemistry=chem, USE_HeldSuarez=False)
+        m.frc = NS(NEGATIVE_FIXER=False, UPDATE_TOT_DENS=True)
     if io_names is not None:   # the I/O object's diagnostic groups (share/mod_io.py:248-265)
         m.io = NS(_diag_names=[n for n in io_names if n.startswith("ml_")],
                   _diag_names_2d=[n for n in io_names if n.startswith("sl_")])

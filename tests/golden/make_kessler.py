@@ -1,4 +1,4 @@
-"""Generate the DCMIP Kessler forcing fixture by running the reference itself.
+"""Generate the DCMIP forcing fixtures by running the reference itself.
 
 The gl03 z10 RAIN_TYPE WARM case of make_golden.py (reference prep tools, JW
 balanced jet, seeded vapour / cloud / rain fields) with the reference's DCMIP
@@ -7,9 +7,14 @@ artificial forcing switched on with Kessler warm-rain microphysics only
 scheme set of DCMIP2016 case 1-3): every large step is Dyn.dynamics_step
 followed by Dyn.forcing_step (pynicamdc/api.py:724-730).  Stores the setup
 arrays, the full-level heights GRD_vz[..., GRD_Z] the microphysics reads, and
-the states before and after two forced steps.
+the states before and after two forced steps.  With --chem the run also
+carries the two chemistry tracers Cl and Cl2 (CHEM_TYPE PASSIVE,
+CHEM_TRC_vmax 2) with the DCMIP terminator toy chemistry on
+(USE_ToyChemistry), started at half and one and a half times the reaction's
+equilibrium so that it acts, and the column latitudes and longitudes the
+chemistry reads are stored too.
 
-    python tests/golden/make_kessler.py --ref <pyNICAM-DC checkout> --out tests/golden
+    python tests/golden/make_kessler.py --ref <pyNICAM-DC checkout> --out tests/golden [--chem]
 """
 from __future__ import annotations
 
@@ -29,7 +34,7 @@ import make_golden as MG  # noqa: E402
 GL, VL, ZTOP, DTL, GAMMA, NSTEPS = 3, 10, 30000.0, 1200.0, 7.68e17, 2
 
 
-def run(ref: str, out_dir: str):
+def run(ref: str, out_dir: str, chem: bool = False):
     import toml
     with tempfile.TemporaryDirectory() as tmp:
         case_dir = os.path.join(tmp, "kessler")
@@ -37,6 +42,10 @@ def run(ref: str, out_dir: str):
         c = toml.loads(MG.model_toml(ref, GL, VL, DTL, GAMMA, NSTEPS, "WARM"))
         c["runconfparam"]["AF_TYPE"] = "DCMIP"
         c["forcing_dcmip_param"] = {"USE_Kessler": True}
+        if chem:
+            c["runconfparam"]["CHEM_TYPE"] = "PASSIVE"
+            c["chemvarparam"] = {"CHEM_TRC_vmax": 2}
+            c["forcing_dcmip_param"]["USE_ToyChemistry"] = True
         with open(os.path.join(case_dir, "case", "config", "nhm_jw.toml"), "w") as f:
             f.write(toml.dumps(c))
         with open(os.path.join(case_dir, "drv.toml"), "w") as f:
@@ -70,7 +79,7 @@ def run(ref: str, out_dir: str):
         nic.initialize()
         m = nic.msc
         assert m.rcnf.AF_TYPE == "DCMIP" and afdcmip.USE_Kessler and not afdcmip.USE_SimpleMicrophys
-        assert not afdcmip.USE_ToyChemistry and not afdcmip.USE_HeldSuarez
+        assert afdcmip.USE_ToyChemistry == chem and not afdcmip.USE_HeldSuarez
         assert m.rcnf.NQW_END == 2 and (m.rcnf.I_QV, m.rcnf.I_QC, m.rcnf.I_QR) == (0, 1, 2)
         assert not m.frc.NEGATIVE_FIXER and m.frc.UPDATE_TOT_DENS
         pv, pvp = m.prgv.PRG_var, m.prgv.PRG_var_pl
@@ -85,7 +94,21 @@ def run(ref: str, out_dir: str):
             pv[:, :, -1, :, 6 + n] = 0.0
             pvp[:, 0, :, 6 + n] = 0.0
             pvp[:, -1, :, 6 + n] = 0.0
+        if chem:
+            from pynicamdc.nhm.forcing import terminator
+            assert (m.rcnf.NCHEM_STR, m.rcnf.NCHEM_END) == (3, 4)
+            r2d = 180.0 / np.pi
+            for arr, la, lo in ((pv, lat, lon), (pvp, latp, lonp)):
+                cl, cl2 = terminator.initial_value_terminator(la * r2d, lo * r2d, np.float64)
+                kax = 2 if arr is pv else 1
+                q0 = arr[..., 6] / arr[..., 0]
+                arr[..., 9] = arr[..., 0] * 0.5 * np.expand_dims(cl, kax) * (1.0 - q0)
+                arr[..., 10] = arr[..., 0] * 1.5 * np.expand_dims(cl2, kax) * (1.0 - q0)
         out = {"geo." + k: v for k, v in MG.geo_from_msc(m, pv.shape[-1] - 6).items()}
+        if chem:
+            out["geo.GRD_LAT"] = np.ascontiguousarray(m.grd.GRD_LAT[:, :, m.adm.ADM_K0, :])
+            out["geo.GRD_LON"] = np.ascontiguousarray(m.grd.GRD_LON[:, :, m.adm.ADM_K0, :])
+            out["geo.NCHEM_STR"], out["geo.NCHEM_END"] = np.asarray(3), np.asarray(4)
         out["geo.GRD_Z"] = np.ascontiguousarray(m.grd.GRD_vz[:, :, :, :, m.grd.GRD_Z])
         out["geo.PRE00"] = np.asarray(m.cnst.CONST_PRE00)
         out["state0"], out["state0_pl"] = pv.copy(), pvp.copy()
@@ -93,7 +116,7 @@ def run(ref: str, out_dir: str):
             nic.run(1)
             out[f"state{s + 1}"], out[f"state{s + 1}_pl"] = m.prgv.PRG_var.copy(), m.prgv.PRG_var_pl.copy()
             out[f"precip{s + 1}"] = np.asarray(m.frc.precip).copy()
-    path = os.path.join(out_dir, "gl03_z10_kessler.npz")
+    path = os.path.join(out_dir, "gl03_z10_kessler_chem.npz" if chem else "gl03_z10_kessler.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path))
 
@@ -102,5 +125,6 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", required=True, help="root of a pyNICAM-DC checkout")
     ap.add_argument("--out", default=HERE)
+    ap.add_argument("--chem", action="store_true", help="with the terminator toy chemistry")
     args = ap.parse_args()
-    run(os.path.abspath(args.ref), os.path.abspath(args.out))
+    run(os.path.abspath(args.ref), os.path.abspath(args.out), args.chem)

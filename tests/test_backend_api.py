@@ -34,6 +34,57 @@ def test_unsupported_configurations_raise(pkg, golden):
         backend.CudaDyn._check_config(msc)
 
 
+def _dcmip_msc(geo, st, chem):
+    g = {k: v for k, v in geo.items() if k not in ("GRD_Z", "GRD_LAT", "GRD_LON", "NCHEM_STR", "NCHEM_END")}
+    extra = {k: geo[k] for k in ("GRD_Z", "GRD_LAT", "GRD_LON", "NCHEM_STR", "NCHEM_END") if k in geo}
+    return fake_msc(g, st["state0"], st["state0_pl"], af_type="DCMIP", dcmip=extra)
+
+
+def test_dcmip_setup_from_services(pkg, golden_kessler_chem):
+    """Kessler with the terminator chemistry passes the configuration check
+    and yields the chemistry's set-up (tracer indices, column lat / lon);
+    simple physics, Held-Suarez on top, or a third chemistry tracer do not"""
+    backend = __import__(pkg.__name__ + ".backend", fromlist=["geo_from_msc"])
+    geo, st, _ = golden_kessler_chem
+    msc = _dcmip_msc(geo, st, True)
+    backend.CudaDyn._check_config(msc)
+    got = backend.geo_from_msc(msc)
+    assert got["AF_dcmip_kessler"] == 1 and list(got["AF_dcmip_chem"]) == [3, 4]
+    assert np.array_equal(got["AF_dcmip_lat"], geo["GRD_LAT"]) and np.array_equal(got["AF_dcmip_lon"], geo["GRD_LON"])
+    assert np.array_equal(got["GRD_Z"], geo["GRD_Z"])
+    for attr in ("USE_SimpleMicrophys", "USE_HeldSuarez"):
+        msc = _dcmip_msc(geo, st, True)
+        setattr(msc.afdcmip, attr, True)
+        with pytest.raises(NotImplementedError):
+            backend.CudaDyn._check_config(msc)
+    msc = _dcmip_msc(geo, st, True)
+    msc.rcnf.NCHEM_END = 5
+    with pytest.raises(NotImplementedError):
+        backend.CudaDyn._check_config(msc)
+
+
+@pytest.mark.gpu
+def test_cudadyn_dcmip_kessler_with_chemistry(pkg, golden_kessler_chem):
+    """the reference-facing step API with DCMIP forcing (Kessler + terminator
+    chemistry): forcing_step returns the precipitation; states within the
+    1e-12 relative L2 of the device forcing test"""
+    geo, st, pr = golden_kessler_chem
+    msc = _dcmip_msc(geo, st, True)
+    dyn = pkg.CudaDyn(msc=msc)
+    try:
+        for n in (1, 2):
+            dyn.dynamics_step(msc)
+            precip = dyn.forcing_step(msc)
+            dyn.sync_prgvar_to_host(msc.prgv, msc)
+            ref = st[f"state{n}"]
+            err = np.sqrt(np.sum((msc.prgv.PRG_var - ref) ** 2)) / np.sqrt(np.sum(ref ** 2))
+            assert err <= 1e-12, (n, err)
+            want = pr[f"precip{n}"]
+            assert np.sqrt(np.sum((np.asarray(precip) - want) ** 2)) <= 1e-12 * np.sqrt(np.sum(want ** 2)), n
+    finally:
+        dyn.core.close()
+
+
 @pytest.mark.gpu
 def test_cudadyn_steps_through_the_reference_api(pkg, golden):
     geo, st = golden

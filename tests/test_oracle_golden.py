@@ -38,6 +38,34 @@ def test_oracle_kessler_forcing_matches_reference(golden_kessler):
         assert np.array_equal(precip, pr[f"precip{n}"]), n
 
 
+def test_oracle_terminator_chemistry_matches_reference(golden_kessler_chem):
+    """dynamics step + DCMIP forcing with Kessler microphysics and the
+    terminator toy chemistry on Cl / Cl2, against the reference run
+    (tests/golden/make_kessler.py --chem): states and precipitation"""
+    geo, st, pr = golden_kessler_chem
+    G = O.Geo(geo)
+    chem = (geo["GRD_LAT"], geo["GRD_LON"], int(geo["NCHEM_STR"]), int(geo["NCHEM_END"]))
+    s, sp = st["state0"], st["state0_pl"]
+    for n in (1, 2):
+        s, sp = O.dynamics_step(G, s, sp)
+        s, sp, precip = O.forcing_step_kessler(G, s, sp, geo["GRD_Z"], chem=chem)
+        assert np.array_equal(s, st[f"state{n}"]) and np.array_equal(sp, st[f"state{n}_pl"]), n
+        assert np.array_equal(precip, pr[f"precip{n}"]), n
+
+
+def test_terminator_fixture_is_active(golden_kessler_chem):
+    """the chemistry changed Cl and Cl2 against the same step without it,
+    and conserved the total chlorine Cl + 2 Cl2 of every cell"""
+    geo, st, _ = golden_kessler_chem
+    G = O.Geo(geo)
+    s, sp = O.dynamics_step(G, st["state0"], st["state0_pl"])
+    s, _, _ = O.forcing_step_kessler(G, s, sp, geo["GRD_Z"])
+    d_cl = st["state1"][..., 9] - s[..., 9]
+    assert np.abs(d_cl).max() > 1e-3 * np.abs(s[..., 9]).max()
+    cly, cly0 = st["state1"][..., 9] + 2.0 * st["state1"][..., 10], s[..., 9] + 2.0 * s[..., 10]
+    assert np.abs(cly - cly0).max() <= 1e-12 * np.abs(cly0).max()
+
+
 def test_kessler_fixture_is_active(golden_warm, golden_kessler):
     """the microphysics changed the water and energy against the unforced
     WARM run of the same case, and it rained somewhere"""
