@@ -70,7 +70,18 @@ typedef struct nc_handle nc_handle;
  * calls, nc_mass_sums, nc_check_finite and nc_get_field; nc_forcing_step,
  * nc_history_vars, the restart calls and nc_state_pointers return
  * NC_ERR_STATE for it, and the Held-Suarez and history set-up entries are
- * rejected (NC_ERR_ARG). */
+ * rejected (NC_ERR_ARG).
+ *
+ * Numerical filter options beyond the DIRECT hyperdiffusion (uniform
+ * "Kh_coef"): the NONLINEAR1 hyperdiffusion (mod_numfilter.py:1153-1206)
+ * with the entries "hdiff_nl_kh_max" (kall: the per-level upper bound,
+ * (1 - height_factor) Kh_coef_maxlim + height_factor Kh_coef_minlim),
+ * "hdiff_nl_minlim", "hdiff_nl_area" (AREA_ave) and "hdiff_nl_c1"
+ * (2 AREA_ave^2 / dtl): Kh per cell and level from the first Laplacian
+ * pass's temperature deviation, its half-level average for w; and the
+ * Rayleigh sponge (mod_numfilter.py:219-271) with "rayleigh_coef" and
+ * "rayleigh_coef_h" (kall: alpha_r times the height factor on full and
+ * half levels) and optionally "rayleigh_only_w". */
 int nc_create(const nc_array* arrays, int32_t narrays, nc_handle** out);
 
 /* Marshal-in of the prognostic state (mod_dynamics.py:1876-1880) from host

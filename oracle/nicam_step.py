@@ -719,6 +719,8 @@ def hdiffusion(g, rhog, rho, DIAG, rhog_pl, rho_pl, DIAG_pl):
                     DIAG_pl[..., I_tem] - g.tem_bs_pl, rho_pl - g.rho_bs_pl], axis=-1)
     KhA = np.full(rhog.shape, Kh)
     KhA_pl = np.full(rhog_pl.shape, Kh)
+    KhH, KhH_pl = KhA, KhA_pl
+    nonlinear = "hdiff_nl_kh_max" in g.d
     for p in range(2):
         v2 = np.zeros_like(vt)
         v2p = np.zeros_like(vtp)
@@ -726,6 +728,9 @@ def hdiffusion(g, rhog, rho, DIAG, rhog_pl, rho_pl, DIAG_pl):
             v2[..., n] = laplacian(g, vt[..., n])
             v2p[..., n] = laplacian_pl(g, vtp[..., n])
         if p == 1:
+            if nonlinear:
+                KhA, KhA_pl = hdiff_nonlinear_coef(g, vt[..., 4], vtp[..., 4])
+                KhH, KhH_pl = hdiff_nonlinear_coef_h(g, KhA), hdiff_nonlinear_coef_h(g, KhA_pl, pole=True)
             wk = rhog * g.CVdry * KhA
             wkp = rhog_pl * g.CVdry * KhA_pl
             v2[..., 4] = diffusion(g, vt[..., 4], wk)
@@ -745,11 +750,11 @@ def hdiffusion(g, rhog, rho, DIAG, rhog_pl, rho_pl, DIAG_pl):
     f = np.zeros(rhog.shape + (6,))
     fp = np.zeros(rhog_pl.shape + (6,))
     zero = 0.0 * 0.0
-    for (F, V, RG, RGH, KA) in ((f, vt, rhog, rhog_h, KhA), (fp, vtp, rhog_pl, rhog_h_pl, KhA_pl)):
+    for (F, V, RG, RGH, KA, KH) in ((f, vt, rhog, rhog_h, KhA, KhH), (fp, vtp, rhog_pl, rhog_h_pl, KhA_pl, KhH_pl)):
         F[..., I_RHOGVX] = -(V[..., 0] * KA + zero) * RG
         F[..., I_RHOGVY] = -(V[..., 1] * KA + zero) * RG
         F[..., I_RHOGVZ] = -(V[..., 2] * KA + zero) * RG
-        F[..., I_RHOGW] = -(V[..., 3] * KA + zero) * RGH
+        F[..., I_RHOGW] = -(V[..., 3] * KH + zero) * RGH
         F[..., I_RHOGE] = -(V[..., 4] + zero)
         F[..., I_RHOG] = -(V[..., 5] + zero)
     a, b, c = f[..., I_RHOGVX].copy(), f[..., I_RHOGVY].copy(), f[..., I_RHOGVZ].copy()
@@ -759,6 +764,54 @@ def hdiffusion(g, rhog, rho, DIAG, rhog_pl, rho_pl, DIAG_pl):
     horizontalize_pl(g, a, b, c)
     fp[..., I_RHOGVX], fp[..., I_RHOGVY], fp[..., I_RHOGVZ] = a, b, c
     return f, fp
+
+
+def hdiff_nonlinear_coef(g, lapT, lapT_pl):
+    """mod_numfilter.py:1153-1184 (hdiff_type NONLINEAR1): Kh from the
+    temperature-deviation Laplacian after the first Laplacian pass,
+    cfact AREA^2 / dt * |lapT| / T0 * AREA with cfact 2, T0 300 K, clipped to
+    [Kh_coef_minlim, kh_max(k)] (kh_max from height_factor, mod_numfilter.py:
+    832-843, 920-922).  Returns Kh (i,j,k,l) and pole."""
+    A, lo, hi = float(g.hdiff_nl_area), float(g.hdiff_nl_minlim), np.asarray(g.hdiff_nl_kh_max)
+    c1 = 2.0 * (A ** 2) / g.dtl
+    kh = np.clip(c1 * (np.abs(lapT) / 300.0 * A), lo, hi[None, None, :, None])
+    kh_pl = np.clip(c1 * (np.abs(lapT_pl) / 300.0 * A), lo, hi[None, :, None])
+    return kh, kh_pl
+
+
+def hdiff_nonlinear_coef_h(g, kh, pole=False):
+    """mod_numfilter.py:1186-1206: the half-level average of the nonlinear Kh
+    on kmin+1..kmax, zero at kmin-1, kmin and kmax+1"""
+    kmin, kmax = g.kmin, g.kmax
+    out = np.zeros_like(kh)
+    if pole:
+        out[:, kmin + 1:kmax + 1] = 0.5 * (kh[:, kmin + 1:kmax + 1] + kh[:, kmin:kmax])
+    else:
+        out[:, :, kmin + 1:kmax + 1] = 0.5 * (kh[:, :, kmin + 1:kmax + 1] + kh[:, :, kmin:kmax])
+    return out
+
+
+def rayleigh_damping(g, f, fp, rhog, rhog_pl, DIAG, DIAG_pl):
+    """mod_numfilter.py:240-271 numfilter_rayleigh_damping on the
+    hyperdiffusion tendency (in place): the momentum tendencies lose
+    rayleigh_coef(k) rhog v (unless only w is damped), the w tendency
+    rayleigh_coef_h(k) w (C2Wa rhog(k) + C2Wb rhog(k-1)), rhog(-1) = 0."""
+    rc, rch = np.asarray(g.rayleigh_coef), np.asarray(g.rayleigh_coef_h)
+    if not int(g.rayleigh_only_w):
+        coef = rc[None, None, :, None] * rhog
+        for n, v in ((I_RHOGVX, I_vx), (I_RHOGVY, I_vy), (I_RHOGVZ, I_vz)):
+            f[..., n] -= coef * DIAG[..., v]
+        coef_pl = rc[None, :, None] * rhog_pl
+        for n, v in ((I_RHOGVX, I_vx), (I_RHOGVY, I_vy), (I_RHOGVZ, I_vz)):
+            fp[..., n] -= coef_pl * DIAG_pl[..., v]
+    km1 = np.zeros_like(rhog)
+    km1[:, :, 1:] = rhog[:, :, :-1]
+    f[..., I_RHOGW] -= rch[None, None, :, None] * DIAG[..., I_w] * (
+        g.VMTR_C2Wfact[..., 0] * rhog + g.VMTR_C2Wfact[..., 1] * km1)
+    km1p = np.zeros_like(rhog_pl)
+    km1p[:, 1:] = rhog_pl[:, :-1]
+    fp[..., I_RHOGW] -= rch[None, :, None] * DIAG_pl[..., I_w] * (
+        g.VMTR_C2Wfact_pl[..., 0] * rhog_pl + g.VMTR_C2Wfact_pl[..., 1] * km1p)
 
 
 def numfilter_divdamp(g, rvx, rvy, rvz, rw, rvx_pl, rvy_pl, rvz_pl, rw_pl):
@@ -1591,6 +1644,8 @@ def dynamics_step(g, prg, prg_pl, keep=None):
             g_TEND[..., iv] = adv[n]
             g_TEND_pl[..., iv] = adv_pl[n]
         f_TEND, f_TEND_pl = hdiffusion(g, PROG[..., I_RHOG], rho, DIAG, PROG_pl[..., I_RHOG], rho_pl, DIAG_pl)
+        if "rayleigh_coef" in g.d:
+            rayleigh_damping(g, f_TEND, f_TEND_pl, PROG[..., I_RHOG], PROG_pl[..., I_RHOG], DIAG, DIAG_pl)
         g_TEND = g_TEND + f_TEND
         g_TEND_pl = g_TEND_pl + f_TEND_pl
         if nl == 0:

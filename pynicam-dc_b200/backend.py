@@ -60,10 +60,30 @@ def geo_from_msc(msc) -> dict:
              OHM=c.CONST_OHM, RADIUS=c.CONST_RADIUS, EPS=c.CONST_EPS, HUGE=c.CONST_HUGE, PRE00=c.CONST_PRE00)
     g.update(rscale=m.grd.GRD_rscale, alpha=float(m.rcnf.NON_HYDRO_ALPHA), dtl=m.tim.TIME_dtl,
              dts=m.tim.TIME_dts, hdiff_fact_rho=m.numf.hdiff_fact_rho)
-    Kh, dd = np.asarray(m.numf.Kh_coef), np.asarray(m.numf.divdamp_coef)
-    if not (np.all(Kh == Kh.flat[0]) and np.all(dd == dd.flat[0])):
-        raise NotImplementedError("cuda backend: only spatially uniform (DIRECT) diffusion coefficients")
-    g["Kh_coef"], g["divdamp_coef"] = float(Kh.flat[0]), float(dd.flat[0])
+    nf = m.numf
+    Kh, dd = np.asarray(nf.Kh_coef), np.asarray(nf.divdamp_coef)
+    nonlinear = bool(getattr(nf, "hdiff_nonlinear", False))
+    if not ((nonlinear or np.all(Kh == Kh.flat[0])) and np.all(dd == dd.flat[0])):
+        raise NotImplementedError("cuda backend: only spatially uniform (DIRECT) diffusion coefficients "
+                                  "or the NONLINEAR1 hyperdiffusion")
+    g["Kh_coef"], g["divdamp_coef"] = (0.0 if nonlinear else float(Kh.flat[0])), float(dd.flat[0])
+    if nonlinear:
+        # NONLINEAR1: the device forms Kh every large step from the temperature
+        # Laplacian; its per-level upper bound (height_factor, mod_numfilter.py:
+        # 832-843, 920-922), lower bound and the mean cell area
+        z, htop, zd = np.asarray(m.grd.GRD_gz), m.grd.GRD_htop, nf.ZD_hdiff_nl
+        pi = getattr(m.cnst, "CONST_PI", np.pi)
+        fact = np.zeros(len(z))
+        for k in range(len(z)):
+            sw = 0.5 + np.sign(z[k] - zd) * 0.5
+            fact[k] = sw * 0.5 * (1.0 - np.cos(pi * (z[k] - zd) / (htop - zd)))
+        g["hdiff_nl_kh_max"] = (1.0 - fact) * nf.Kh_coef_maxlim + fact * nf.Kh_coef_minlim
+        g["hdiff_nl_minlim"] = float(nf.Kh_coef_minlim)
+        g["hdiff_nl_area"] = float(nf.AREA_ave)
+    if getattr(nf, "NUMFILTER_DOrayleigh", False):   # the sponge coefficients (mod_numfilter.py:225-233)
+        g["rayleigh_coef"] = np.asarray(nf.rayleigh_coef, np.float64)
+        g["rayleigh_coef_h"] = np.asarray(nf.rayleigh_coef_h, np.float64)
+        g["rayleigh_only_w"] = int(bool(getattr(nf, "rayleigh_damp_only_w", False)))
     g["sstep"] = np.asarray(m.dyn.num_of_iteration_sstep[:m.dyn.num_of_iteration_lstep])
     g["CVW"] = np.asarray(m.rcnf.CVW)
     g["NQW_END"] = int(m.rcnf.NQW_END)
@@ -195,11 +215,10 @@ class CudaDyn:
         if r.TRC_ADV_TYPE != "MIURA2004" or not r.THUBURN_LIM:
             raise NotImplementedError("cuda backend: MIURA2004 tracer advection with Thuburn limiters only")
         nf = msc.numf
-        if nf.lap_order_hdiff != 2 or nf.lap_order_divdamp != 2 or nf.NUMFILTER_DOrayleigh or \
-                nf.NUMFILTER_DOdivdamp_2d or nf.NUMFILTER_DOdivdamp_v or nf.NUMFILTER_DOhorizontaldiff_lap1 \
-                or nf.hdiff_nonlinear:
-            raise NotImplementedError("cuda backend: lap_order 2 hyperdiffusion/divdamp without Rayleigh, "
-                                      "2-D/vertical divdamp, lap1 or nonlinear diffusion")
+        if nf.lap_order_hdiff != 2 or nf.lap_order_divdamp != 2 or \
+                nf.NUMFILTER_DOdivdamp_2d or nf.NUMFILTER_DOdivdamp_v or nf.NUMFILTER_DOhorizontaldiff_lap1:
+            raise NotImplementedError("cuda backend: lap_order 2 hyperdiffusion (DIRECT or NONLINEAR1) and 3-D "
+                                      "divdamp, optionally the Rayleigh sponge; no 2-D/vertical divdamp or lap1")
         if r.DYN_DIV_NUM != 1:
             raise NotImplementedError("cuda backend: DYN_DIV_NUM = 1 only")
         if int(getattr(r, "NQW_STR", 0)) != 0 or int(getattr(r, "I_QV", 0)) != 0 or \

@@ -912,6 +912,8 @@ static int run_step(nc_handle* h) {
       GtendArgs<R> ga;
       auto F = [&](FieldPair& f) { return pole ? PL<R>(f) : RG<R>(f); };
       for (int n = 0; n < 6; ++n) { ga.vt2.f[n] = F(h->vt2[n]); ga.gT0[n] = F(h->gT0[n]); }
+      ga.lapT = F(h->vt[4]);
+      ga.vx = F(h->vx); ga.vy = F(h->vy); ga.vz = F(h->vz); ga.w = F(h->w);
       ga.rhog = F(h->P[0]); ga.gvx = F(h->gadv[0]); ga.gvy = F(h->gadv[1]); ga.gvz = F(h->gadv[2]);
       ga.gw = F(h->gadv[3]); ga.frhog = F(h->frhog);
       if (!pole) k_gtend<<<(unsigned)((D.npt2 + h->blk[TB_GTEND] - 1) / h->blk[TB_GTEND]), h->blk[TB_GTEND], 0, s>>>(ga, 0);
@@ -1552,6 +1554,8 @@ static int make_f32_geometry(nc_handle* h) {
   Cf.hdiff_fact_rho = (float)C.hdiff_fact_rho; Cf.CVW0 = (float)C.CVW0; Cf.PRE00 = (float)C.PRE00;
   for (int n = 0; n < NC_MAXQW; ++n) Cf.CVW[n] = (float)C.CVW[n];
   Cf.nqw = C.nqw;
+  Cf.hdiff_nl = C.hdiff_nl; Cf.nl_c1 = (float)C.nl_c1; Cf.nl_area = (float)C.nl_area; Cf.nl_min = (float)C.nl_min;
+  Cf.rayleigh = C.rayleigh; Cf.rayleigh_only_w = C.rayleigh_only_w;
   Cf.gam_unit = C.gam_unit;
   Cf.rsc_h = (float)(1.0 / C.rscale);   // the float32 divisions multiply by the rounded reciprocal
   Cf.rsc_l = 0.0f;
@@ -1560,6 +1564,7 @@ static int make_f32_geometry(nc_handle* h) {
   for (int k = 0; k < NC_MAXK; ++k) {
     Cf.afact[k] = (float)C.afact[k]; Cf.bfact[k] = (float)C.bfact[k]; Cf.cfact[k] = (float)C.cfact[k];
     Cf.dfact[k] = (float)C.dfact[k]; Cf.rdgz[k] = (float)C.rdgz[k]; Cf.rdgzh[k] = (float)C.rdgzh[k];
+    Cf.nl_khmax[k] = (float)C.nl_khmax[k]; Cf.ray_c[k] = (float)C.ray_c[k]; Cf.ray_ch[k] = (float)C.ray_ch[k];
   }
   return 0;
 }
@@ -1650,6 +1655,23 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   TRY(up_vec(T, "GRD_afact", D.KA, C.afact)); TRY(up_vec(T, "GRD_bfact", D.KA, C.bfact));
   TRY(up_vec(T, "GRD_cfact", D.KA, C.cfact)); TRY(up_vec(T, "GRD_dfact", D.KA, C.dfact));
   TRY(up_vec(T, "GRD_rdgz", D.KA, C.rdgz)); TRY(up_vec(T, "GRD_rdgzh", D.KA, C.rdgzh));
+  if (T.get("hdiff_nl_kh_max")) {   // hyperdiffusion NONLINEAR1 (mod_numfilter.py:1153-1206)
+    C.hdiff_nl = 1;
+    TRY(up_vec(T, "hdiff_nl_kh_max", D.KA, C.nl_khmax));
+    TRY(scalar(T, "hdiff_nl_c1", C.nl_c1));
+    TRY(scalar(T, "hdiff_nl_area", C.nl_area));
+    TRY(scalar(T, "hdiff_nl_minlim", C.nl_min));
+  }
+  if (T.get("rayleigh_coef")) {   // Rayleigh sponge (mod_numfilter.py:219-271)
+    C.rayleigh = 1;
+    TRY(up_vec(T, "rayleigh_coef", D.KA, C.ray_c));
+    TRY(up_vec(T, "rayleigh_coef_h", D.KA, C.ray_ch));
+    if (T.get("rayleigh_only_w")) {
+      double f;
+      TRY(scalar(T, "rayleigh_only_w", f));
+      C.rayleigh_only_w = (f != 0.0);
+    }
+  }
   Geom& Gm = h->Gm;
   const int KA = D.KA;
   TRY(up_reg(h, T, "VMTR_GSGAM2", KA, 1, &Gm.GSGAM2));

@@ -60,6 +60,14 @@ struct ConstsT {
   R rsc_h, rsc_l, third_h, third_l;
   R afact[NC_MAXK], bfact[NC_MAXK], cfact[NC_MAXK], dfact[NC_MAXK];
   R rdgz[NC_MAXK], rdgzh[NC_MAXK];
+  // hyperdiffusion NONLINEAR1 (hdiff_nl): Kh = clip(nl_c1 |lapT| / 300 nl_area,
+  // nl_min, nl_khmax[k]), nl_c1 = 2 AREA_ave^2 / dtl
+  int hdiff_nl;
+  R nl_c1, nl_area, nl_min;
+  R nl_khmax[NC_MAXK];
+  // Rayleigh sponge (rayleigh): coefficients on full and half levels
+  int rayleigh, rayleigh_only_w;
+  R ray_c[NC_MAXK], ray_ch[NC_MAXK];
 };
 using Consts = ConstsT<double>;
 

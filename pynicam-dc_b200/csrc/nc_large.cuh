@@ -490,121 +490,33 @@ __global__ void k_intp_weights(const double* ci, double* w, int npt2) {
     }
 }
 
-// Second hyperdiffusion pass, one block per (level, HD_DX x HD_DY tile) of
-// interior cells: the haloed tile of the six Laplacians and of rhog is staged
-// in shared memory, the triangle gradients of the temperature and density
-// Laplacians are formed once (with the singular-point fix at the (0,0)
-// vertex), then each thread writes its cell's four Laplacians and two
-// Kh-weighted diffusions (kernels/oprtlaplacian.py:41-55,
-// kernels/oprtdiffusion.py).  Halo cells are left to the exchange that follows.
 #define HD_DX 32
 #define HD_DY 8
+
+// Kh of the hyperdiffusion at level k: the uniform DIRECT coefficient, or for
+// NONLINEAR1 (mod_numfilter.py:1153-1184) the coefficient from the
+// temperature-deviation Laplacian lapT of the first pass,
+// clip(2 AREA^2 / dtl * (|lapT| / 300 * AREA), Kh_coef_minlim, kh_max(k))
 template <class R>
-__global__ void __launch_bounds__(HD_DX * HD_DY, NC_MINB(R, 4, NC_F32_HDIFF2)) k_hdiff2_l(Six<R> vt, const R* rhog,
-                                                                                       SixOut<R> out) {
-  constexpr int PX = HD_DX + 2, PY = HD_DY + 2, TX = HD_DX + 1, TY = HD_DY + 1;
-  __shared__ R s_f[6][PY * PX];
-  __shared__ R s_r[PY * PX];
-  __shared__ R s_t[2][6][TY * TX];   // field 4/5: tti x,y,z then ttj x,y,z
-  const int kb = (int)blockIdx.x, l = (int)blockIdx.z;
-  const int ntx = (cD.G - 2 + HD_DX - 1) / HD_DX;
-  const int i0 = 1 + ((int)blockIdx.y % ntx) * HD_DX, j0 = 1 + ((int)blockIdx.y / ntx) * HD_DY;
-  const int G = cD.G, gmax = cD.G - 2;
-  const int tid = threadIdx.x, tx = tid % HD_DX, ty = tid / HD_DX;
-  const int i = i0 + tx, j = j0 + ty;
-  const bool own = (i <= gmax) && (j <= gmax);
-  const R Kh = CC.Kh;
-  const R kfac[2] = {CC.CVdry, CC.hdiff_fact_rho};
-  {
-    const int k = kb;
-    for (int p = tid; p < PX * PY; p += blockDim.x) {
-      const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
-      const bool ok = ii < G && jj < G;
-      const int q = ok ? ix(ii, jj, k, l) : 0;
-#pragma unroll
-      for (int n = 0; n < 6; ++n) s_f[n][p] = ok ? vt.f[n][q] : R(0.0);
-      s_r[p] = ok ? rhog[q] : R(0.0);
-    }
-    __syncthreads();
-    for (int p = tid; p < TX * TY; p += blockDim.x) {
-      const int px = p % TX, py = p / TX;
-      const int ii = i0 - 1 + px, jj = j0 - 1 + py;
-      const bool ok = ii <= G - 2 && jj <= G - 2;
-      const int ia = py * PX + px, ib = ia + 1, ic = ia + PX + 1, id = ia + PX;
-#pragma unroll
-      for (int f = 0; f < 2; ++f) {
-        const R* s = s_f[4 + f];
-        const R s0 = s[ia], sip = s[ib], sd = s[ic], sjp = s[id];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          R ti = R(0.0), tj = R(0.0);
-          if (ok) {
-            // weights 2c1-c2-c3, -c1+2c2-c3, -c1-c2+2c3 of the i and j triangles (k_intp_weights)
-            const R w1i = P2(CG.intp_w, (d * 3 + 0) * 2 + 0, ii, jj, l);
-            const R w2i = P2(CG.intp_w, (d * 3 + 1) * 2 + 0, ii, jj, l);
-            const R w3i = P2(CG.intp_w, (d * 3 + 2) * 2 + 0, ii, jj, l);
-            const R w1j = P2(CG.intp_w, (d * 3 + 0) * 2 + 1, ii, jj, l);
-            const R w2j = P2(CG.intp_w, (d * 3 + 1) * 2 + 1, ii, jj, l);
-            const R w3j = P2(CG.intp_w, (d * 3 + 2) * 2 + 1, ii, jj, l);
-            ti = div3(w1i * s0 + w2i * sip + w3i * sd);
-            tj = div3(w1j * s0 + w2j * sd + w3j * sjp);
-          }
-          s_t[f][d][p] = ti;
-          s_t[f][3 + d][p] = tj;
-        }
-      }
-    }
-    __syncthreads();
-    if (i0 == 1 && j0 == 1 && tid < 6) {   // singular-point fix of the (0,0) triangle, fields 4 and 5
-      const int f = tid / 3, d = tid % 3;
-      const R m0 = (R)CG.pntmask[l * 2 + 0], m1 = (R)CG.pntmask[l * 2 + 1];
-      s_t[f][d][0] = s_t[f][d][0] * m0 + s_t[f][3 + d][1] * m1;
-    }
-    __syncthreads();
-    if (own) {
-      const int q = ix(i, j, k, l);
-      const int c0 = (ty + 1) * PX + (tx + 1);
-      const int nb[7] = {c0, c0 + 1, c0 + PX + 1, c0 + PX, c0 - 1, c0 - PX - 1, c0 - PX};
-#pragma unroll
-      for (int n = 0; n < 4; ++n) {
-        R v = P2(CG.coef_lap, 0, i, j, l) * s_f[n][nb[0]];
-#pragma unroll
-        for (int m = 1; m < 7; ++m) v = v + P2(CG.coef_lap, m, i, j, l) * s_f[n][nb[m]];
-        out.f[n][q] = -v;
-      }
-      const int ta = (ty + 1) * TX + (tx + 1), tb = ta - 1, tc = ta - TX - 1, td = ta - TX;
-#pragma unroll
-      for (int f = 0; f < 2; ++f) {
-        auto kh = [&](int pt) { return s_r[pt] * kfac[f] * Kh; };
-        const R kh0 = kh(nb[0]);
-        const R kf1 = R(0.5) * (kh0 + kh(nb[2])), kf2 = R(0.5) * (kh0 + kh(nb[3])), kf3 = R(0.5) * (kh0 + kh(nb[4]));
-        const R kf4 = R(0.5) * (kh0 + kh(nb[5])), kf5 = R(0.5) * (kh0 + kh(nb[6])), kf6 = R(0.5) * (kh0 + kh(nb[1]));
-        R inner = R(0.0);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const R aTI = s_t[f][d][ta], aTJ = s_t[f][3 + d][ta], bTI = s_t[f][d][tb];
-          const R cTI = s_t[f][d][tc], cTJ = s_t[f][3 + d][tc], dTJ = s_t[f][3 + d][td];
-          const R cd0 = P2(CG.coef_diff, d * 6 + 0, i, j, l), cd1 = P2(CG.coef_diff, d * 6 + 1, i, j, l),
-                       cd2 = P2(CG.coef_diff, d * 6 + 2, i, j, l), cd3 = P2(CG.coef_diff, d * 6 + 3, i, j, l),
-                       cd4 = P2(CG.coef_diff, d * 6 + 4, i, j, l), cd5 = P2(CG.coef_diff, d * 6 + 5, i, j, l);
-          const R blk = kf1 * cd0 * (aTI + aTJ) + kf2 * cd1 * (aTJ + bTI) + kf3 * cd2 * (bTI + cTJ) +
-                             kf4 * cd3 * (cTJ + cTI) + kf5 * cd4 * (cTI + dTJ) + kf6 * cd5 * (dTJ + aTI);
-          inner = (d == 0) ? blk : inner + blk;
-        }
-        out.f[4 + f][q] = -inner;
-      }
-    }
-    __syncthreads();
-  }
+__device__ __forceinline__ R hdiff_kh(R lapT, int k) {
+  if (!CC.hdiff_nl) return CC.Kh;
+  const R c = CC.nl_c1 * (fabs(lapT) / R(300.0) * CC.nl_area);
+  return fmin(fmax(c, CC.nl_min), CC.nl_khmax[k]);
 }
 
-// The same second hyperdiffusion pass with HD_NK levels per block: the
-// tile's k-independent triangle weights (intp_w, 18 planes) are staged in
-// shared memory and the cell's Laplacian and diffusion coefficients (coef_lap
-// 7, coef_diff 18) held in registers once for all of the block's levels,
-// instead of re-read from L2 at every level.  Same expressions in the same
-// order as k_hdiff2_l (same results).  Dynamic shared memory:
-// hdiff2_m_smem<R>() bytes (45 KB float, 90 KB double).
+// Second hyperdiffusion pass, one block per (HD_NK levels, HD_DX x HD_DY tile)
+// of interior cells: the haloed tile of the six Laplacians and of rhog is
+// staged in shared memory per level, the triangle gradients of the
+// temperature and density Laplacians are formed once (with the singular-point
+// fix at the (0,0) vertex), then each thread writes its cell's four
+// Laplacians and two Kh-weighted diffusions (kernels/oprtlaplacian.py:41-55,
+// kernels/oprtdiffusion.py).  Halo cells are left to the exchange that
+// follows.  The tile's k-independent triangle weights (intp_w, 18 planes) are
+// staged in shared memory and the cell's Laplacian and diffusion coefficients
+// (coef_lap 7, coef_diff 18) held in registers once for all of the block's
+// levels, instead of re-read from L2 at every level.  Dynamic shared memory:
+// hdiff2_m_smem<R>() bytes (45 KB float, 90 KB double).  Kh per cell from
+// hdiff_kh (the first pass's temperature Laplacian is the staged field 4).
 #ifndef HD_NK
 #define HD_NK 6
 #endif
@@ -629,7 +541,6 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, NC_MINB(R, 2, 4)) k_hdiff2_m(Si
   const int tid = threadIdx.x, tx = tid % HD_DX, ty = tid / HD_DX;
   const int i = i0 + tx, j = j0 + ty;
   const bool own = (i <= gmax) && (j <= gmax);
-  const R Kh = CC.Kh;
   const R kfac[2] = {CC.CVdry, CC.hdiff_fact_rho};
   for (int p = tid; p < NT; p += blockDim.x) {
     const int ii = i0 - 1 + p % TX, jj = j0 - 1 + p / TX;
@@ -701,7 +612,7 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, NC_MINB(R, 2, 4)) k_hdiff2_m(Si
       const int ta = (ty + 1) * TX + (tx + 1), tb = ta - 1, tc = ta - TX - 1, td = ta - TX;
 #pragma unroll
       for (int f = 0; f < 2; ++f) {
-        auto kh = [&](int pt) { return s_r[pt] * kfac[f] * Kh; };
+        auto kh = [&](int pt) { return s_r[pt] * kfac[f] * hdiff_kh<R>(s_f[4 * NP + pt], k); };
         const R kh0 = kh(nb[0]);
         const R kf1 = R(0.5) * (kh0 + kh(nb[2])), kf2 = R(0.5) * (kh0 + kh(nb[3])), kf3 = R(0.5) * (kh0 + kh(nb[4]));
         const R kf4 = R(0.5) * (kh0 + kh(nb[5])), kf5 = R(0.5) * (kh0 + kh(nb[6])), kf6 = R(0.5) * (kh0 + kh(nb[1]));
@@ -729,7 +640,6 @@ __global__ void k_hdiff2_pl(Six<R> vt, const R* rhog, SixOut<R> out) {
   int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (t >= cD.KA * cD.LP) return;
   int k = t / cD.LP, lp = t % cD.LP;
-  const R Kh = CC.Kh;
   for (int n = 0; n < 6; ++n) {
     const R* s = vt.f[n];
     R row = R(0.0);
@@ -752,10 +662,10 @@ __global__ void k_hdiff2_pl(Six<R> vt, const R* rhog, SixOut<R> out) {
           vt_[v - 1][d] = div3((R(2.0) * c0 - c1 - c2) * sn + (-c0 + R(2.0) * c1 - c2) * sij + (-c0 - c1 + R(2.0) * c2) * sp1);
         }
       }
-      R khn = rhog[ipl(0, k, lp)] * fac * Kh;
+      R khn = rhog[ipl(0, k, lp)] * fac * hdiff_kh<R>(vt.f[4][ipl(0, k, lp)], k);
       for (int v = 1; v <= 5; ++v) {
         int vm1 = (v == 1) ? 5 : v - 1;
-        R khv = rhog[ipl(v, k, lp)] * fac * Kh;
+        R khv = rhog[ipl(v, k, lp)] * fac * hdiff_kh<R>(vt.f[4][ipl(v, k, lp)], k);
         R kavg = R(0.5) * (khn + khv);
         R sd = R(0.0);
         for (int d = 0; d < 3; ++d) {
@@ -780,6 +690,8 @@ __global__ void k_hdiff2_pl(Six<R> vt, const R* rhog, SixOut<R> out) {
 template <class R>
 struct GtendArgs {
   Six<R> vt2;                       // post-COMM hyperdiffusion Laplacians
+  const R* lapT;                    // the first pass's temperature Laplacian (NONLINEAR1 Kh)
+  const R *vx, *vy, *vz, *w;        // diagnosed velocities (Rayleigh sponge)
   const R *rhog, *gvx, *gvy, *gvz, *gw;
   R* gT0[6];
   R* frhog;                 // f_TEND[RHOG] (tracer input)
@@ -787,22 +699,37 @@ struct GtendArgs {
 
 template <class R>
 __device__ void gtend_column(const Col c, const MetT<R> m, const GtendArgs<R>& a, int i, int j, int l, int g, int lp) {
-  const R Kh = CC.Kh;
   for (int k = 0; k < cD.KA; ++k) {
     int p = c.at(k);
     R rg = a.rhog[p];
     R rgh = R(0.0);
     if (k >= cD.kmin) rgh = mc(m.C2W, c, 0, 2, k) * rg + mc(m.C2W, c, 1, 2, k) * a.rhog[c.at(k - 1)];
+    const R Kh = hdiff_kh<R>(CC.hdiff_nl ? a.lapT[p] : R(0.0), k);
+    // the coefficient of w: Kh itself (DIRECT), or for NONLINEAR1 the average of
+    // levels k and k-1 on kmin+1..kmax and zero elsewhere (mod_numfilter.py:1186-1206)
+    R Khh = Kh;
+    if (CC.hdiff_nl)
+      Khh = (k > cD.kmin && k <= cD.kmax) ? R(0.5) * (Kh + hdiff_kh<R>(a.lapT[c.at(k - 1)], k - 1)) : R(0.0);
     R fx = -(a.vt2.f[0][p] * Kh + R(0.0)) * rg;
     R fy = -(a.vt2.f[1][p] * Kh + R(0.0)) * rg;
     R fz = -(a.vt2.f[2][p] * Kh + R(0.0)) * rg;
-    R fw = -(a.vt2.f[3][p] * Kh + R(0.0)) * rgh;
+    R fw = -(a.vt2.f[3][p] * Khh + R(0.0)) * rgh;
     R fe = -(a.vt2.f[4][p] + R(0.0));
     R fr = -(a.vt2.f[5][p] + R(0.0));
     if (!c.pole) {
       if (interior(i, j)) horiz_reg(i, j, l, fx, fy, fz);
     } else {
       horiz_pl(g, lp, fx, fy, fz);
+    }
+    if (CC.rayleigh) {   // the sponge on the hyperdiffusion tendency (mod_numfilter.py:240-271)
+      if (!CC.rayleigh_only_w) {
+        const R coef = CC.ray_c[k] * rg;
+        fx = fx - coef * a.vx[p];
+        fy = fy - coef * a.vy[p];
+        fz = fz - coef * a.vz[p];
+      }
+      const R rgm1 = k > 0 ? a.rhog[c.at(k - 1)] : R(0.0);
+      fw = fw - CC.ray_ch[k] * a.w[p] * (mc(m.C2W, c, 0, 2, k) * rg + mc(m.C2W, c, 1, 2, k) * rgm1);
     }
     a.gT0[0][p] = R(0.0) + fr;
     a.gT0[1][p] = a.gvx[p] + fx;

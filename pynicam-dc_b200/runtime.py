@@ -217,6 +217,16 @@ def setup_table(geo: dict) -> dict:
     if "NQW_END" in geo:   # water tracers 0..NQW_END (RAIN_TYPE); the vapour alone when absent
         t["NQW_END"] = np.asarray(float(_scalar(geo["NQW_END"])), np.float64)
     t["sstep"] = np.ascontiguousarray(geo["sstep"], np.int64)
+    if "hdiff_nl_kh_max" in geo:   # hyperdiffusion NONLINEAR1: the Kh bounds and 2 AREA_ave^2 / dtl
+        area = float(_scalar(geo["hdiff_nl_area"]))
+        t["hdiff_nl_kh_max"] = np.ascontiguousarray(geo["hdiff_nl_kh_max"], np.float64)
+        t["hdiff_nl_area"] = np.asarray(area, np.float64)
+        t["hdiff_nl_minlim"] = np.asarray(float(_scalar(geo["hdiff_nl_minlim"])), np.float64)
+        t["hdiff_nl_c1"] = np.asarray(2.0 * (area ** 2) / float(_scalar(geo["dtl"])), np.float64)
+    if "rayleigh_coef" in geo:   # Rayleigh sponge on the full and half levels
+        t["rayleigh_coef"] = np.ascontiguousarray(geo["rayleigh_coef"], np.float64)
+        t["rayleigh_coef_h"] = np.ascontiguousarray(geo["rayleigh_coef_h"], np.float64)
+        t["rayleigh_only_w"] = np.asarray(float(_scalar(geo.get("rayleigh_only_w", 0))), np.float64)
     for k in ("GRD_afact", "GRD_bfact", "GRD_cfact", "GRD_dfact", "GRD_rdgz", "GRD_rdgzh"):
         t[k] = np.ascontiguousarray(geo[k], np.float64)
     for k in ("VMTR_GSGAM2", "VMTR_GSGAM2H", "VMTR_RGSGAM2", "VMTR_RGSGAM2H", "VMTR_RGSQRTH", "VMTR_RGAM",

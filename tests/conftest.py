@@ -38,6 +38,25 @@ def golden_warm():
 
 
 @pytest.fixture(scope="session")
+def golden_nlhdiff():
+    """gl03 z10 with the NONLINEAR1 hyperdiffusion (Kh from the temperature
+    Laplacian, clipped per level), two steps of the reference (make_golden.py
+    --case gl03_z10_nlhdiff); the set-up carries hdiff_nl_kh_max,
+    hdiff_nl_minlim and hdiff_nl_area"""
+    from make_golden import load
+    return load(os.path.join(GOLDEN, "gl03_z10_nlhdiff.npz"))
+
+
+@pytest.fixture(scope="session")
+def golden_rayleigh():
+    """gl03 z10 with the Rayleigh sponge above 15 km, two steps of the
+    reference (make_golden.py --case gl03_z10_rayleigh); the set-up carries
+    rayleigh_coef, rayleigh_coef_h and rayleigh_only_w"""
+    from make_golden import load
+    return load(os.path.join(GOLDEN, "gl03_z10_rayleigh.npz"))
+
+
+@pytest.fixture(scope="session")
 def golden_kessler():
     """gl03 z10 RAIN_TYPE WARM with the reference's DCMIP forcing, Kessler
     microphysics only (make_kessler.py): setup arrays (GRD_Z the full-level

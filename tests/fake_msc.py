@@ -12,7 +12,8 @@ import numpy as np
 
 
 def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_type: str = "RK3",
-             coords: dict = None, hist: dict = None, io_names=None, dcmip: dict = None):
+             coords: dict = None, hist: dict = None, io_names=None, dcmip: dict = None,
+             numf_opts: dict = None):
     g = {k: np.asarray(v) for k, v in geo.items()}
     sc = lambda k: g[k].reshape(-1)[0].item()
     adm = NS(ADM_kall=int(sc("kall")), ADM_kmin=int(sc("kmin")), ADM_kmax=int(sc("kmax")),
@@ -74,6 +75,12 @@ def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_
               divdamp_coef=np.full(n, sc("divdamp_coef")), lap_order_hdiff=2, lap_order_divdamp=2,
               NUMFILTER_DOrayleigh=False, NUMFILTER_DOdivdamp_2d=False, NUMFILTER_DOdivdamp_v=False,
               NUMFILTER_DOhorizontaldiff_lap1=False, hdiff_nonlinear=False)
+    if numf_opts:   # numfilter options (NONLINEAR1 bounds and mean cell area, Rayleigh coefficients)
+        for k, v in numf_opts.items():
+            setattr(numf, k, v)
+    if "GRD_gz" in g:   # the level heights and model-top height the NONLINEAR1 bounds read
+        grd.GRD_gz = g["GRD_gz"]
+        grd.GRD_htop = g["GRD_gzh"][int(sc("kmax")) + 1] - g["GRD_gzh"][int(sc("kmin"))]
     sstep = g["sstep"].astype(np.int64)
     dyn = NS(num_of_iteration_lstep=len(sstep), num_of_iteration_sstep=np.concatenate([sstep, np.zeros(4, np.int64)]))
     ppm = NS(pntmask=g["pntmask"])

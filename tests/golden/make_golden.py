@@ -39,6 +39,15 @@ CASES = {
     "gl03_z10_warm": (3, 10, 30000.0, 1200.0, 7.68e17, 2, True),
 }
 RAIN = {"gl03_z10_warm": "WARM"}
+# numfilter options beyond DIRECT hyperdiffusion: NONLINEAR1 (the temperature-
+# Laplacian-dependent Kh, mod_numfilter.py:1153-1207, as in the DCMIP2016
+# tutorial cases) and the Rayleigh sponge (mod_numfilter.py:219-271, as in the
+# mountain-wave cases), scaled to gl03 / dtl 1200 s
+CASES["gl03_z10_nlhdiff"] = CASES["gl03_z10_trc"]
+CASES["gl03_z10_rayleigh"] = CASES["gl03_z10_trc"]
+NUMF = {"gl03_z10_nlhdiff": dict(hdiff_type="NONLINEAR1", Kh_coef_maxlim=7.68e18, Kh_coef_minlim=7.68e17,
+                                 ZD_hdiff_nl=20000.0),
+        "gl03_z10_rayleigh": dict(alpha_r=2.0e-4, ZD=15000.0)}
 WATER_SCALE = (1.0, 0.05, 0.02)   # vapour, cloud, rain: multiples of the tracer field
 
 MKRAWGRID_TOML = """[admparam]
@@ -111,7 +120,8 @@ def prep(ref: str, case_dir: str, gl: int, vl: int, ztop: float, layer_type: str
 NHM_TOML = os.path.join("tutorial", "case", "config", "nhm_jw.toml")
 
 
-def model_toml(ref: str, gl: int, vl: int, dtl: float, gamma: float, nsteps: int, rain: str = "") -> str:
+def model_toml(ref: str, gl: int, vl: int, dtl: float, gamma: float, nsteps: int, rain: str = "",
+               numf: dict = None) -> str:
     """the reference's JW tutorial config, pointed at the scratch case"""
     import toml
     c = toml.load(os.path.join(ref, NHM_TOML))
@@ -122,6 +132,8 @@ def model_toml(ref: str, gl: int, vl: int, dtl: float, gamma: float, nsteps: int
     c["timeparam"].update(integ_type="RK3", dtl=dtl, lstep_max=max(nsteps, 1))
     c["numfilterparam"].update(hdiff_type="DIRECT", lap_order_hdiff=2, gamma_h=gamma, divdamp_type="DIRECT",
                                lap_order_divdamp=2, alpha_d=gamma)
+    if numf:
+        c["numfilterparam"].update(numf)
     c["restartparam"]["input_io_mode"] = "IDEAL"
     c["dycoretestparam"].update(init_type="Jablonowski", test_case="1")
     c["runconfparam"]["THUBURN_LIM"] = True
@@ -154,11 +166,23 @@ def geo_from_msc(m, nq: int) -> dict:
     c = m.cnst
     g.update(GRAV=c.CONST_GRAV, Rdry=c.CONST_Rdry, CVdry=c.CONST_CVdry, CPdry=c.CONST_CPdry, Rvap=c.CONST_Rvap,
              OHM=c.CONST_OHM, RADIUS=c.CONST_RADIUS, EPS=c.CONST_EPS, HUGE=c.CONST_HUGE, PRE00=c.CONST_PRE00)
+    nf = m.numf
     g.update(rscale=m.grd.GRD_rscale, alpha=float(m.rcnf.NON_HYDRO_ALPHA), dtl=m.tim.TIME_dtl,
-             dts=m.tim.TIME_dts, hdiff_fact_rho=m.numf.hdiff_fact_rho, Kh_coef=float(m.numf.gamma_h),
-             divdamp_coef=float(m.numf.alpha_d))
-    assert np.all(m.numf.Kh_coef == float(m.numf.gamma_h))
-    assert np.all(m.numf.divdamp_coef == float(m.numf.alpha_d))
+             dts=m.tim.TIME_dts, hdiff_fact_rho=nf.hdiff_fact_rho, Kh_coef=float(nf.gamma_h),
+             divdamp_coef=float(nf.alpha_d))
+    if nf.hdiff_nonlinear:   # NONLINEAR1: per-level upper bound, lower bound, mean cell area
+        fact = np.zeros(a.ADM_kall)
+        nf.height_factor(a.ADM_kall, m.grd.GRD_gz, m.grd.GRD_htop, nf.ZD_hdiff_nl, fact, m.cnst, np.float64)
+        g["hdiff_nl_kh_max"] = (1.0 - fact) * nf.Kh_coef_maxlim + fact * nf.Kh_coef_minlim
+        g["hdiff_nl_minlim"] = float(nf.Kh_coef_minlim)
+        g["hdiff_nl_area"] = float(nf.AREA_ave)
+    else:
+        assert np.all(nf.Kh_coef == float(nf.gamma_h))
+    assert np.all(nf.divdamp_coef == float(nf.alpha_d))
+    if nf.NUMFILTER_DOrayleigh:   # the sponge coefficients per full and half level
+        g["rayleigh_coef"] = np.asarray(nf.rayleigh_coef)
+        g["rayleigh_coef_h"] = np.asarray(nf.rayleigh_coef_h)
+        g["rayleigh_only_w"] = int(bool(nf.rayleigh_damp_only_w))
     g["sstep"] = np.asarray(m.dyn.num_of_iteration_sstep[:m.dyn.num_of_iteration_lstep])
     g["CVW"] = np.asarray(m.rcnf.CVW)
     g["NQW_END"] = int(m.rcnf.NQW_END)   # water tracers 0..NQW_END (NQW_STR = I_QV = 0)
@@ -190,7 +214,7 @@ def run_case(ref: str, name: str, out_dir: str, scratch: str):
     case_dir = os.path.join(scratch, name)
     prep(ref, case_dir, gl, vl, ztop)
     with open(os.path.join(case_dir, "case", "config", "nhm_jw.toml"), "w") as f:
-        f.write(model_toml(ref, gl, vl, dtl, gamma, nsteps, RAIN.get(name, "")))
+        f.write(model_toml(ref, gl, vl, dtl, gamma, nsteps, RAIN.get(name, ""), NUMF.get(name)))
     with open(os.path.join(case_dir, "drv.toml"), "w") as f:
         f.write('[driver]\nbackend="numpy"\nprecision="float64"\ncomm="serial"\n'
                 'nhm_driver_cnf="./case/config/nhm_jw.toml"\n')

@@ -63,6 +63,62 @@ def test_dcmip_setup_from_services(pkg, golden_kessler_chem):
         backend.CudaDyn._check_config(msc)
 
 
+def _numf_msc(geo, st, case):
+    """services for the NONLINEAR1 or Rayleigh fixture: the reference's numfilter
+    attributes (make_golden.NUMF) and the arrays it set up"""
+    from make_golden import NUMF
+    skip = ("hdiff_nl_kh_max", "hdiff_nl_minlim", "hdiff_nl_area", "rayleigh_coef", "rayleigh_coef_h",
+            "rayleigh_only_w")
+    g = {k: v for k, v in geo.items() if k not in skip}
+    if case == "nlhdiff":
+        o = NUMF["gl03_z10_nlhdiff"]
+        opts = dict(hdiff_nonlinear=True, Kh_coef=np.full(np.asarray(geo["VMTR_GSGAM2"]).shape, -999.0),
+                    Kh_coef_maxlim=o["Kh_coef_maxlim"], Kh_coef_minlim=o["Kh_coef_minlim"],
+                    ZD_hdiff_nl=o["ZD_hdiff_nl"], AREA_ave=float(geo["hdiff_nl_area"]))
+    else:
+        opts = dict(NUMFILTER_DOrayleigh=True, rayleigh_coef=geo["rayleigh_coef"],
+                    rayleigh_coef_h=geo["rayleigh_coef_h"], rayleigh_damp_only_w=False)
+    return fake_msc(g, st["state0"], st["state0_pl"], numf_opts=opts)
+
+
+@pytest.mark.parametrize("case", ["nlhdiff", "rayleigh"])
+def test_numfilter_setup_from_services(pkg, case, request):
+    """backend.geo_from_msc hands the NONLINEAR1 bounds (the per-level upper
+    bound restated from the reference's height_factor, equal to the one the
+    reference computed) and the Rayleigh coefficients to the device set-up,
+    and the configuration check accepts them"""
+    backend = __import__(pkg.__name__ + ".backend", fromlist=["geo_from_msc"])
+    geo, st = request.getfixturevalue("golden_" + case)
+    msc = _numf_msc(geo, st, case)
+    backend.CudaDyn._check_config(msc)
+    got = backend.geo_from_msc(msc)
+    keys = ("hdiff_nl_kh_max", "hdiff_nl_minlim", "hdiff_nl_area") if case == "nlhdiff" else \
+        ("rayleigh_coef", "rayleigh_coef_h", "rayleigh_only_w")
+    for k in keys:
+        assert np.array_equal(np.asarray(got[k]), np.asarray(geo[k])), k
+    msc.numf.NUMFILTER_DOdivdamp_2d = True
+    with pytest.raises(NotImplementedError):
+        backend.CudaDyn._check_config(msc)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["nlhdiff", "rayleigh"])
+def test_cudadyn_numfilter_options(pkg, case, request):
+    """the reference-facing step API with NONLINEAR1 or the Rayleigh sponge:
+    two steps bit for bit with the reference's"""
+    geo, st = request.getfixturevalue("golden_" + case)
+    msc = _numf_msc(geo, st, case)
+    dyn = pkg.CudaDyn(msc=msc)
+    try:
+        for n in (1, 2):
+            dyn.dynamics_step(msc)
+            dyn.sync_prgvar_to_host(msc.prgv, msc)
+            assert np.array_equal(msc.prgv.PRG_var, st[f"state{n}"]), n
+            assert np.array_equal(msc.prgv.PRG_var_pl, st[f"state{n}_pl"]), n
+    finally:
+        dyn.core.close()
+
+
 @pytest.mark.gpu
 def test_cudadyn_dcmip_kessler_with_chemistry(pkg, golden_kessler_chem):
     """the reference-facing step API with DCMIP forcing (Kessler + terminator

@@ -57,6 +57,29 @@ def test_warm_rain_two_steps_bit_exact_vs_reference(pkg, golden_warm):
                     assert np.sqrt(np.sum((out[..., v] - ref) ** 2)) <= 2e-3 * den, (s, v)
 
 
+@pytest.mark.parametrize("case", ["golden_nlhdiff", "golden_rayleigh"])
+def test_numfilter_options_two_steps_bit_exact_vs_reference(pkg, case, request):
+    """the NONLINEAR1 hyperdiffusion (per-cell Kh from the first pass's
+    temperature Laplacian, its half-level average for w) and the Rayleigh
+    sponge: bit for bit with the reference's two steps in float64, graph
+    replayed; the mixed form within 2e-3 (relative L2 per prognostic)"""
+    geo, st = request.getfixturevalue(case)
+    for prec in ("float64", "mixed"):
+        c = pkg.NicamCuda(geo, graph=True, precision=prec)
+        try:
+            outs = _steps(c, st, 2)
+        finally:
+            c.close()
+        for s, (out, out_pl) in enumerate(outs, start=1):
+            if prec == "float64":
+                assert np.array_equal(out, st[f"state{s}"]) and np.array_equal(out_pl, st[f"state{s}_pl"]), s
+            else:
+                for v in range(out.shape[-1]):
+                    ref = st[f"state{s}"][..., v]
+                    den = np.sqrt(np.sum(ref * ref))
+                    assert np.sqrt(np.sum((out[..., v] - ref) ** 2)) <= 2e-3 * den, (s, v)
+
+
 def test_graph_replay_equals_eager(pkg, golden):
     geo, st = golden
     c = pkg.NicamCuda(geo, graph=True)

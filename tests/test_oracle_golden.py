@@ -1,6 +1,7 @@
 """The CPU oracle against the golden states written by the reference itself
 (tests/golden/make_golden.py): bit-for-bit on two consecutive large steps."""
 import numpy as np
+import pytest
 
 from oracle import nicam_step as O
 
@@ -23,6 +24,47 @@ def test_oracle_matches_reference_warm_rain(golden_warm):
         out, out_pl = O.dynamics_step(G, st[f"state{s}"], st[f"state{s}_pl"])
         assert np.array_equal(out, st[f"state{s + 1}"]), f"step {s + 1} regional"
         assert np.array_equal(out_pl, st[f"state{s + 1}_pl"]), f"step {s + 1} pole"
+
+
+@pytest.mark.parametrize("case", ["golden_nlhdiff", "golden_rayleigh"])
+def test_oracle_numfilter_options_match_reference(case, request):
+    """the NONLINEAR1 hyperdiffusion and the Rayleigh sponge: two steps of
+    the oracle equal the reference's bit for bit"""
+    geo, st = request.getfixturevalue(case)
+    G = O.Geo(geo)
+    s, sp = st["state0"], st["state0_pl"]
+    for n in (1, 2):
+        s, sp = O.dynamics_step(G, s, sp)
+        assert np.array_equal(s, st[f"state{n}"]) and np.array_equal(sp, st[f"state{n}_pl"]), n
+
+
+def test_nonlinear_kh_takes_every_branch(golden_nlhdiff, monkeypatch):
+    """in the NONLINEAR1 fixture's first step Kh sits at its lower bound, at
+    the per-level upper bound and strictly between them, each for a sizeable
+    share of the cells, so the clip is tested both ways"""
+    geo, st = golden_nlhdiff
+    seen = []
+    orig = O.hdiff_nonlinear_coef
+
+    def spy(g, a, b):
+        kh, kh_pl = orig(g, a, b)
+        lo, hi = float(g.hdiff_nl_minlim), np.asarray(g.hdiff_nl_kh_max)[None, None, :, None]
+        seen.append(((kh == lo).mean(), (kh == hi).mean(), ((kh > lo) & (kh < hi)).mean()))
+        return kh, kh_pl
+    monkeypatch.setattr(O, "hdiff_nonlinear_coef", spy)
+    O.dynamics_step(O.Geo(geo), st["state0"], st["state0_pl"])
+    assert len(seen) == 3 and all(min(f) > 0.05 for f in seen), seen
+
+
+def test_rayleigh_fixture_is_active(golden, golden_rayleigh):
+    """the sponge changed the momentum against the undamped run from the same
+    state, and its coefficient is zero below 15 km"""
+    _, st0 = golden
+    geo, st = golden_rayleigh
+    assert np.array_equal(st["state0"], st0["state0"])
+    assert np.abs(st["state1"][..., 1] - st0["state1"][..., 1]).max() > 1e-3
+    rc = np.asarray(geo["rayleigh_coef"])
+    assert np.all(rc[np.asarray(geo["GRD_gz"]) < 15000.0] == 0.0) and rc.max() > 0.0
 
 
 def test_oracle_kessler_forcing_matches_reference(golden_kessler):
