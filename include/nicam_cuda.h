@@ -257,7 +257,18 @@ int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* g
  * indices, both outside the water range) and "AF_dcmip_lat" / "AF_dcmip_lon"
  * (GRD_LAT / GRD_LON[:, :, K0, :] in radians, (gall_1d, gall_1d, 1, lall));
  * the Cl / Cl2 tendencies (per dry air, analytic over dt; sin, cos, exp and
- * sqrt are CUDA's) join the tracer tendencies on kmin..kmax. */
+ * sqrt are CUDA's) join the tracer tendencies on kmin..kmax.  The optional
+ * "AF_dcmip_schemes" (int64 [Kessler, simple physics, large-scale
+ * condensation], default [1, 0, 0]) adds the DCMIP simple physics
+ * (USE_SimpleMicrophys, nhm/forcing/simple_physics.py with the RJ2012
+ * boundary layer; mod_af_dcmip.py:230-317) or runs it alone: its surface
+ * fluxes, implicit boundary-layer diffusion of u, v, potential temperature
+ * and vapour, and optional large-scale condensation, from the same state as
+ * Kessler, with momentum, vapour and energy tendencies and precipitation
+ * added to Kessler's.  It reads "AF_dcmip_zh" (GRD_vz[..., GRD_ZH], (gall_1d,
+ * gall_1d, kall, lall)), "AF_dcmip_zsfc" (GRD_zs at K0), "AF_dcmip_tsurf" (the
+ * sea-surface temperature per column) and "AF_dcmip_ij" (GMTR_p IX, IY, IZ,
+ * JX, JY, JZ at K0), all (gall_1d, gall_1d, 1, lall[, 6]). */
 int nc_forcing_step(nc_handle* h);
 
 /* The precipitation rate [m/s] of the last DCMIP Kessler forcing step per

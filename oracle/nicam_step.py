@@ -1826,7 +1826,104 @@ def terminator_tendency(lat_deg, lon_deg, cl, cl2, dt):
     return cl_f, -cl_f / 2.0
 
 
-def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_dens=True, chem=None):
+# DCMIP simple physics (nhm/forcing/simple_physics.py; DCMIP2016 v6 scheme):
+# constants of simple_physics.py:25-46 (use_HS off)
+SP_RAIR, SP_RH2O, SP_GRAV, SP_CPAIR, SP_LATVAP = 287.0, 461.5, 9.80616, 1.0045e3, 2.5e6
+SP_EPSILO, SP_ZVIR = SP_RAIR / SP_RH2O, (SP_RH2O / SP_RAIR) - 1.0
+SP_C, SP_T0, SP_E0, SP_RHOW = 0.0011, 273.16, 610.78, 1000.0
+SP_CD0, SP_CD1, SP_CM, SP_V20 = 0.0007, 0.000065, 0.002, 20.0
+SP_P0, SP_PBLTOP, SP_PBLCONST = 100000.0, 85000.0, 10000.0
+
+
+def dcmip_sst(lat, latdepend):
+    """simple_physics.py:152-197 _sst_tsurf without Held-Suarez: the
+    latitude-dependent sea-surface temperature of the moist baroclinic wave
+    (test 1) or the constant 302.15 K of the tropical cyclone (test 0)"""
+    if not latdepend:
+        return np.full_like(lat, 302.15)
+    import math
+    pi = math.pi
+    T00, u0, a, omega, q0, eta0 = 288.0, 35.0, 6371220.0, 7.29212e-5, 0.021, 0.252
+    etav, latw = (1.0 - eta0) * 0.5 * pi, 2.0 * pi / 9.0
+    sinl, cosl = np.sin(lat), np.cos(lat)
+    termA = (-2.0 * sinl ** 6 * (cosl ** 2 + 1.0 / 3.0) + 10.0 / 63.0) * u0 * (math.cos(etav)) ** 1.5
+    termB = (8.0 / 5.0 * cosl ** 3 * (sinl ** 2 + 2.0 / 3.0) - pi / 4.0) * a * omega * 0.5
+    pref = pi * u0 / SP_RAIR * 1.5 * math.sin(etav) * (math.cos(etav)) ** 0.5
+    return (T00 + pref * (termA + termB)) / (1.0 + SP_ZVIR * q0 * np.exp(-(lat / latw) ** 4))
+
+
+def simple_physics(t, q, u, v, pmid, pint, pdel, rpdel, ps, tsurf, dtime, lsc):
+    """simple_physics.py:310-366 (RJ2012 boundary layer, no Held-Suarez) on
+    (ncol, nz) columns ordered top to bottom: the lowest full level's
+    hydrostatic height, the large-scale condensation (lsc, :48-91), the
+    drag / diffusivities from the lowest-level wind (:118-149), the implicit
+    bulk surface fluxes of the lowest level (:200-225) and the implicit
+    boundary-layer diffusion of u, v, potential temperature and q
+    (:228-307).  Returns t, q, u, v and the condensation's precipitation."""
+    ncol, nz = t.shape
+    dlnpint = np.log(ps) - np.log(pint[:, nz - 1])
+    za = SP_RAIR / SP_GRAV * t[:, -1] * (1.0 + SP_ZVIR * q[:, -1]) * 0.5 * dlnpint
+    if lsc:
+        qsat = SP_EPSILO * SP_E0 / pmid * np.exp(-SP_LATVAP / SP_RH2O * ((1.0 / t) - 1.0 / SP_T0))
+        denom = 1.0 + (SP_LATVAP / SP_CPAIR) * (SP_EPSILO * SP_LATVAP * qsat / (SP_RAIR * t * t))
+        cond = np.where(q > qsat, (1.0 / dtime) * (q - qsat) / denom, 0.0)
+        t = t + (SP_LATVAP / SP_CPAIR) * cond * dtime
+        q = q - cond * dtime
+        precl = np.sum(cond * pdel / (SP_GRAV * SP_RHOW), axis=1)
+    else:
+        precl = np.zeros(ncol)
+    wind = np.sqrt(u[:, -1] ** 2 + v[:, -1] ** 2)
+    Cd = np.where(wind < SP_V20, SP_CD0 + SP_CD1 * wind, SP_CM)
+    decay = np.where(pint[:, 0:nz] >= SP_PBLTOP, 1.0, np.exp(-(SP_PBLTOP - pint[:, 0:nz]) ** 2 / SP_PBLCONST ** 2))
+    Km = (Cd * wind * za)[:, None] * decay
+    Ke = (SP_C * wind * za)[:, None] * decay
+    # surface fluxes, lowest level only
+    qsats = SP_EPSILO * SP_E0 / ps * np.exp(-SP_LATVAP / SP_RH2O * ((1.0 / tsurf) - 1.0 / SP_T0))
+    dm = 1.0 + Cd * wind * dtime / za
+    dh = 1.0 + SP_C * wind * dtime / za
+    u, v, t, q = u.copy(), v.copy(), t.copy(), q.copy()
+    u[:, -1] = u[:, -1] / dm
+    v[:, -1] = v[:, -1] / dm
+    t[:, -1] = (t[:, -1] + SP_C * wind * tsurf * dtime / za) / dh
+    q[:, -1] = (q[:, -1] + SP_C * wind * qsats * dtime / za) / dh
+    # implicit vertical diffusion: coefficients at the interfaces between levels c and c+1
+    kap = SP_RAIR / SP_CPAIR
+    g2dt = dtime * SP_GRAV * SP_GRAV
+    rho = pint[:, 1:nz] / (SP_RAIR * (t[:, 1:nz] * (1.0 + SP_ZVIR * q[:, 1:nz])
+                                      + t[:, 0:nz - 1] * (1.0 + SP_ZVIR * q[:, 0:nz - 1])) / 2.0)
+    dpm = pmid[:, 1:nz] - pmid[:, 0:nz - 1]
+    fm = g2dt * Km[:, 1:nz] * rho * rho / dpm
+    fe = g2dt * Ke[:, 1:nz] * rho * rho / dpm
+    CAm, CCm, CA, CC = (np.zeros((ncol, nz)) for _ in range(4))
+    CAm[:, 0:nz - 1] = rpdel[:, 0:nz - 1] * fm
+    CCm[:, 1:nz] = rpdel[:, 1:nz] * fm
+    CA[:, 0:nz - 1] = rpdel[:, 0:nz - 1] * fe
+    CC[:, 1:nz] = rpdel[:, 1:nz] * fe
+    CE, CEm, CFu, CFv, CFt, CFq = (np.zeros((ncol, nz)) for _ in range(6))
+    ce = cem = cfu = cfv = cft = cfq = np.zeros(ncol)
+    for c in range(nz - 1, -1, -1):   # upward elimination
+        de = 1.0 + CA[:, c] + CC[:, c] - CA[:, c] * ce
+        dmm = 1.0 + CAm[:, c] + CCm[:, c] - CAm[:, c] * cem
+        ce, cem = CC[:, c] / de, CCm[:, c] / dmm
+        cfu = (u[:, c] + CAm[:, c] * cfu) / dmm
+        cfv = (v[:, c] + CAm[:, c] * cfv) / dmm
+        cft = ((SP_P0 / pmid[:, c]) ** kap * t[:, c] + CA[:, c] * cft) / de
+        cfq = (q[:, c] + CA[:, c] * cfq) / de
+        CE[:, c], CEm[:, c], CFu[:, c], CFv[:, c], CFt[:, c], CFq[:, c] = ce, cem, cfu, cfv, cft, cfq
+    uo, vo, to, qo = (np.zeros((ncol, nz)) for _ in range(4))
+    uo[:, 0], vo[:, 0] = CFu[:, 0], CFv[:, 0]
+    to[:, 0] = CFt[:, 0] * (pmid[:, 0] / SP_P0) ** kap
+    qo[:, 0] = CFq[:, 0]
+    for c in range(1, nz):            # downward substitution
+        uo[:, c] = CEm[:, c] * uo[:, c - 1] + CFu[:, c]
+        vo[:, c] = CEm[:, c] * vo[:, c - 1] + CFv[:, c]
+        to[:, c] = (CE[:, c] * to[:, c - 1] * (SP_P0 / pmid[:, c - 1]) ** kap + CFt[:, c]) * (pmid[:, c] / SP_P0) ** kap
+        qo[:, c] = CE[:, c] * qo[:, c - 1] + CFq[:, c]
+    return to, qo, uo, vo, precl
+
+
+def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_dens=True, chem=None,
+                         kessler_on=True, sm=None):
     """Dyn.forcing_step for AF_TYPE 'DCMIP' with Kessler microphysics only
     (nhm/dynamics/mod_dynamics.py:597-735 -> nhm/forcing/mod_forcing.py:207-321
     forcing_step -> mod_af_dcmip.py:129-230 AF_dcmip, Kessler branch):
@@ -1839,7 +1936,13 @@ def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_de
     GRD_vz[..., GRD_Z] (i, j, k, l).  ``chem`` = (lat, lon, nchem_str,
     nchem_end) adds the terminator toy chemistry (mod_af_dcmip.py:171-187;
     lat, lon of the columns in radians (i, j, l)) on the Cl / Cl2 tracers.
-    Returns (prg, prg_pl, precip (i, j, l))."""
+    ``sm`` = dict(zh, zsfc, lat, ij, latdepend, lsc) adds the simple physics
+    (mod_af_dcmip.py:230-317) from the same (old) state: half-level heights
+    GRD_vz[..., GRD_ZH], the surface height and latitude (i, j, l), the
+    column unit vectors GMTR_p IX..JZ (i, j, l, 6), the sea-surface
+    temperature form and the large-scale condensation switch; its momentum,
+    vapour and energy tendencies add to Kessler's (``kessler_on`` False
+    leaves the simple physics alone).  Returns (prg, prg_pl, precip (i, j, l))."""
     out = prg.copy()
     out_pl = prg_pl.copy()
     PROG = out[..., 0:6]
@@ -1856,28 +1959,65 @@ def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_de
     dt = g.dtl
     col = lambda a: a.transpose(0, 1, 3, 2).reshape(I * J * L, K)[:, sl]      # (ncol, levels kmin..kmax)
     qv_m, qc_m, qr_m = col(q[..., 0]), col(q[..., 1]), col(q[..., 2])
-    qd = 1.0 - qv_m - qc_m - qr_m
-    qvk, qck, qrk = qv_m / qd, qc_m / qd, qr_m / qd
-    rhod = col(rho) * qd
-    pk = (col(pre) / g.PRE00) ** (g.Rdry / g.CPdry)
-    theta_k = col(tem) / pk
-    theta_k, qvk, qck, qrk, precl = kessler(theta_k, qvk, qck, qrk, rhod, pk, dt, col(zf))
-    qd2 = 1.0 / (1.0 + qvk + qck + qrk)
-    qvk, qck, qrk = qvk * qd2, qck * qd2, qrk * qd2
-    cvk = qd2 * g.CVdry + qvk * g.CVW[0] + qck * g.CVW[1] + qrk * g.CVW[2]
-    tem_new = theta_k * pk
-    tem_old = col(tem)
-    cv_old = col(ein) / tem_old
-    dtem = tem_new - tem_old
-    dcv = cvk - cv_old
 
     def grid(c):   # (ncol, levels kmin..kmax) -> (i, j, k, l), zero outside kmin..kmax
         full = np.zeros((I * J * L, K))
         full[:, sl] = c
         return full.reshape(I, J, L, K).transpose(0, 1, 3, 2)
-    fe = grid((cv_old * dtem + tem_old * dcv + dcv * dtem) / dt)
-    fq = [grid((qvk - qv_m) / dt), grid((qck - qc_m) / dt), grid((qrk - qr_m) / dt)]
-    fq += [None] * (PROGq.shape[-1] - 3)
+    zero = np.zeros(rho.shape)
+    fe, fv = zero, [zero, zero, zero]
+    fq = [zero, zero, zero] + [None] * (PROGq.shape[-1] - 3)
+    precl = np.zeros(I * J * L)
+    if kessler_on:
+        qd = 1.0 - qv_m - qc_m - qr_m
+        qvk, qck, qrk = qv_m / qd, qc_m / qd, qr_m / qd
+        rhod = col(rho) * qd
+        pk = (col(pre) / g.PRE00) ** (g.Rdry / g.CPdry)
+        theta_k = col(tem) / pk
+        theta_k, qvk, qck, qrk, prk = kessler(theta_k, qvk, qck, qrk, rhod, pk, dt, col(zf))
+        qd2 = 1.0 / (1.0 + qvk + qck + qrk)
+        qvk, qck, qrk = qvk * qd2, qck * qd2, qrk * qd2
+        cvk = qd2 * g.CVdry + qvk * g.CVW[0] + qck * g.CVW[1] + qrk * g.CVW[2]
+        tem_new = theta_k * pk
+        tem_old = col(tem)
+        cv_old = col(ein) / tem_old
+        dtem = tem_new - tem_old
+        dcv = cvk - cv_old
+        fe = fe + grid((cv_old * dtem + tem_old * dcv + dcv * dtem) / dt)
+        fq = [fq[0] + grid((qvk - qv_m) / dt), fq[1] + grid((qck - qc_m) / dt),
+              fq[2] + grid((qrk - qr_m) / dt)] + fq[3:]
+        precl = precl + prk
+    if sm is not None:
+        td = lambda a: col(a)[:, ::-1]            # levels kmax..kmin (top down)
+        flat = lambda a: a.reshape(I * J * L)
+        ij = [flat(sm["ij"][..., n]) for n in range(6)]
+        tem_td, pre_td, alt_td, alth_td = td(tem), td(pre), td(zf), td(sm["zh"])
+        vx_td, vy_td, vz_td, ein_td = td(DIAG[..., I_vx]), td(DIAG[..., I_vy]), td(DIAG[..., I_vz]), td(ein)
+        qv_old = td(q[..., 0])
+        u = vx_td * ij[0][:, None] + vy_td * ij[1][:, None] + vz_td * ij[2][:, None]
+        v = vx_td * ij[3][:, None] + vy_td * ij[4][:, None] + vz_td * ij[5][:, None]
+        nz = kmax - kmin + 1
+        pre_sfc = flat(pre[:, :, kmin, :] + rho[:, :, kmin, :] * g.GRAV * (zf[:, :, kmin, :] - sm["zsfc"]))
+        pint = np.zeros((I * J * L, nz + 1))
+        pint[:, 1:nz] = pre_td[:, 1:nz] * np.exp(np.log(pre_td[:, 0:nz - 1] / pre_td[:, 1:nz])
+                                                 * (alth_td[:, 0:nz - 1] - alt_td[:, 1:nz])
+                                                 / (alt_td[:, 0:nz - 1] - alt_td[:, 1:nz]))
+        pint[:, nz] = pre_sfc
+        pdel = pint[:, 1:nz + 1] - pint[:, 0:nz]
+        tsurf = dcmip_sst(flat(sm["lat"]), sm["latdepend"])
+        t_n, qv_n, u_n, v_n, pr2 = simple_physics(tem_td, qv_old, u, v, pre_td, pint, pdel, 1.0 / pdel, pre_sfc,
+                                                  tsurf, dt, sm["lsc"])
+        for d, (a, b, vd) in enumerate(((0, 3, vx_td), (1, 4, vy_td), (2, 5, vz_td))):
+            fv[d] = grid(((u_n * ij[a][:, None] + v_n * ij[b][:, None] - vd) / dt)[:, ::-1])
+        qc, qr = td(q[..., 1]), td(q[..., 2])
+        qd = 1.0 - qv_n - qc - qr
+        cv = qd * g.CVdry + qv_n * g.CVW[0] + qc * g.CVW[1] + qr * g.CVW[2]
+        cv_old = ein_td / tem_td
+        dtem = t_n - tem_td
+        dcv = cv - cv_old
+        fq[0] = fq[0] + grid(((qv_n - qv_old) / dt)[:, ::-1])
+        fe = fe + grid(((cv_old * dtem + tem_td * dcv + dcv * dtem) / dt)[:, ::-1])
+        precl = precl + pr2
     if chem is not None:
         lat, lon, n_cl, n_cl2 = chem
         d2r = np.pi / 180.0
@@ -1888,10 +2028,9 @@ def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_de
         fq[n_cl] = grid(cl_f * qvd)
         fq[n_cl2] = grid(cl2_f * qvd)
     GS = g.VMTR_GSGAM2
-    zero = np.zeros_like(fe)
     new = PROG.copy()
-    for v in (I_RHOGVX, I_RHOGVY, I_RHOGVZ):
-        new[..., v] = PROG[..., v] + dt * zero * rho * GS
+    for d, v in enumerate((I_RHOGVX, I_RHOGVY, I_RHOGVZ)):
+        new[..., v] = PROG[..., v] + dt * fv[d] * rho * GS
     new[..., I_RHOGE] = PROG[..., I_RHOGE] + dt * fe * rho * GS
     rhog = PROG[..., I_RHOG]
     for n in range(PROGq.shape[-1]):

@@ -42,7 +42,8 @@ def _dcmip_flags(msc) -> dict:
         import sys
         mod = sys.modules.get("pynicamdc.nhm.forcing.mod_af_dcmip")
         obj = getattr(mod, "afdcmip", None) if mod is not None else None
-    keys = ("USE_Kessler", "USE_SimpleMicrophys", "USE_ToyChemistry", "USE_HeldSuarez")
+    keys = ("USE_Kessler", "USE_SimpleMicrophys", "USE_ToyChemistry", "USE_HeldSuarez", "SM_Latdepend_SST",
+            "SM_LargeScaleCond", "SM_PBL_Bryan")
     return {k: bool(getattr(obj, k, False)) for k in keys}
 
 
@@ -128,11 +129,22 @@ def geo_from_msc(msc) -> dict:
         frc = getattr(m, "frc", None)
         g["AF_negative_fixer"] = int(bool(getattr(frc, "NEGATIVE_FIXER", False)))
         g["AF_update_tot_dens"] = int(bool(getattr(frc, "UPDATE_TOT_DENS", True)))
-        if _dcmip_flags(msc)["USE_ToyChemistry"]:   # terminator chemistry on the Cl / Cl2 tracers
-            g["AF_dcmip_chem"] = np.asarray([m.rcnf.NCHEM_STR, m.rcnf.NCHEM_END], np.int64)
-            K0 = m.adm.ADM_K0
+        fl = _dcmip_flags(msc)
+        K0 = m.adm.ADM_K0
+        g["AF_dcmip_schemes"] = np.asarray([fl["USE_Kessler"], fl["USE_SimpleMicrophys"], fl["SM_Latdepend_SST"],
+                                            fl["SM_LargeScaleCond"]], np.int64)
+        if fl["USE_ToyChemistry"] or fl["USE_SimpleMicrophys"]:
             g["AF_dcmip_lat"] = np.ascontiguousarray(m.grd.GRD_LAT[:, :, K0, :])
+        if fl["USE_ToyChemistry"]:   # terminator chemistry on the Cl / Cl2 tracers
+            g["AF_dcmip_chem"] = np.asarray([m.rcnf.NCHEM_STR, m.rcnf.NCHEM_END], np.int64)
             g["AF_dcmip_lon"] = np.ascontiguousarray(m.grd.GRD_LON[:, :, K0, :])
+        if fl["USE_SimpleMicrophys"]:   # the simple physics' geometry (mod_forcing.py:236-247)
+            gm = m.gmtr
+            g["AF_dcmip_zh"] = np.ascontiguousarray(m.grd.GRD_vz[:, :, :, :, m.grd.GRD_ZH])
+            g["AF_dcmip_zsfc"] = np.ascontiguousarray(m.grd.GRD_zs[:, :, K0, :, m.grd.GRD_ZSFC])
+            g["AF_dcmip_ij"] = np.ascontiguousarray(np.stack(
+                [gm.GMTR_p[:, :, K0, :, n] for n in (gm.GMTR_p_IX, gm.GMTR_p_IY, gm.GMTR_p_IZ, gm.GMTR_p_JX,
+                                                     gm.GMTR_p_JY, gm.GMTR_p_JZ)], axis=-1))
     elif getattr(m.rcnf, "AF_TYPE", "NONE") == "HELD-SUAREZ":
         # the column latitudes the forcing reads (mod_dynamics.py: GRD_LAT[:, :, K0, :])
         g["GRD_LAT"] = np.ascontiguousarray(m.grd.GRD_LAT[:, :, m.adm.ADM_K0, :])
@@ -226,12 +238,13 @@ class CudaDyn:
             raise NotImplementedError("cuda backend: water tracers must come first (NQW_STR = I_QV = 0), at most six")
         if getattr(r, "AF_TYPE", "NONE") == "DCMIP":
             flags = _dcmip_flags(msc)
-            if not (flags.get("USE_Kessler") and not flags.get("USE_SimpleMicrophys")
-                    and not flags.get("USE_HeldSuarez")) or getattr(r, "RAIN_TYPE", "DRY") != "WARM" or \
+            if not (flags.get("USE_Kessler") or flags.get("USE_SimpleMicrophys")) or flags.get("USE_HeldSuarez") \
+                    or flags.get("SM_PBL_Bryan") or getattr(r, "RAIN_TYPE", "DRY") != "WARM" or \
                     (flags.get("USE_ToyChemistry") and int(getattr(r, "NCHEM_END", -1)) - int(getattr(r, "NCHEM_STR", -1)) != 1):
-                raise NotImplementedError("cuda backend: DCMIP forcing with Kessler microphysics and optionally the "
-                                          "terminator chemistry (RAIN_TYPE WARM, two chemistry tracers; no simple "
-                                          "physics or Held-Suarez)")
+                raise NotImplementedError("cuda backend: DCMIP forcing with Kessler microphysics and / or the simple "
+                                          "physics (RJ2012 boundary layer), optionally the terminator chemistry "
+                                          "(RAIN_TYPE WARM, two chemistry tracers; no Bryan boundary layer or "
+                                          "moist Held-Suarez)")
         elif getattr(r, "AF_TYPE", "NONE") not in ("NONE", "HELD-SUAREZ"):
             raise NotImplementedError("cuda backend: artificial forcing NONE or HELD-SUAREZ only")
 

@@ -372,6 +372,8 @@ struct nc_handle {
   int kess_negative_fixer = 0, kess_update_tot_dens = 1;
   int kess_n_cl = -1, kess_n_cl2 = -1;      // terminator toy chemistry tracers (optional)
   const double *kess_lat = nullptr, *kess_lon = nullptr;
+  int kess_on = 1, sm_on = 0, sm_lsc = 0;   // DCMIP schemes: Kessler, simple physics, its condensation
+  const double *sm_zh = nullptr, *sm_zsfc = nullptr, *sm_tsurf = nullptr, *sm_ij = nullptr;
   // derived history diagnostics (optional setup; nc_history_vars)
   bool hist = false;
   const double *hist_hgt = nullptr, *hist_coslat = nullptr, *hist_zsfc = nullptr, *hist_area = nullptr;
@@ -1429,7 +1431,7 @@ int nc_forcing_step(nc_handle* h) {
   TRY(load_consts(h));
   const Dims& D = h->D;
   if (h->kess_zf) {
-    KesslerArgs a;
+    DcmipArgs a;
     for (int v = 0; v < 6; ++v) a.P.v[v] = h->P[v].r;
     for (int n = 0; n < D.nq; ++n) a.Pq[n] = h->Pq[n].r;
     a.nq = D.nq;
@@ -1444,8 +1446,15 @@ int nc_forcing_step(nc_handle* h) {
     a.n_cl2 = h->kess_n_cl2;
     a.lat = h->kess_lat;
     a.lon = h->kess_lon;
-    k_forcing_kessler<<<(unsigned)((D.npt2 + 63) / 64), 64, 0, h->stream>>>(a);
-    TRY(check_launch(h, "forcing_kessler"));
+    a.kessler = h->kess_on;
+    a.sm = h->sm_on;
+    a.sm_lsc = h->sm_lsc;
+    a.zh = h->sm_zh;
+    a.zsfc = h->sm_zsfc;
+    a.tsurf = h->sm_tsurf;
+    a.ij = h->sm_ij;
+    k_forcing_dcmip<<<(unsigned)((D.npt2 + 63) / 64), 64, 0, h->stream>>>(a);
+    TRY(check_launch(h, "forcing_dcmip"));
     TRY(comm_prg<double>(h));
     TRY(join_pl(h));
     return 0;
@@ -1735,12 +1744,26 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
     TRY(dev_alloc(h, &h->trc_time, 1));
     CU(cudaMemset(h->trc_time, 0, sizeof(double)));
   }
-  if (T.get("AF_dcmip_kessler_zf")) {   // DCMIP forcing with Kessler microphysics (nc_forcing_step)
+  if (T.get("AF_dcmip_kessler_zf")) {   // DCMIP forcing (nc_forcing_step): Kessler and / or simple physics
     if (T.get("AF_hs_lat_terms")) return fail(NC_ERR_ARG, "Held-Suarez and DCMIP forcing set-ups both given");
     if (!T.get("PRE00")) return fail(NC_ERR_ARG, "AF_dcmip_kessler_zf given without PRE00");
-    if (C.nqw != 3) return fail(NC_ERR_ARG, "Kessler microphysics needs RAIN_TYPE WARM (NQW_END = 2: vapour, cloud, rain)");
+    if (C.nqw != 3) return fail(NC_ERR_ARG, "DCMIP forcing needs RAIN_TYPE WARM (NQW_END = 2: vapour, cloud, rain)");
     if (D.kmax - D.kmin + 1 > NC_KESS_K || D.kmax - D.kmin < 1)
-      return fail(NC_ERR_ARG, "Kessler microphysics: 2.." + std::to_string(NC_KESS_K) + " model levels");
+      return fail(NC_ERR_ARG, "DCMIP forcing: 2.." + std::to_string(NC_KESS_K) + " model levels");
+    if (const nc_array* sc = T.get("AF_dcmip_schemes")) {   // [Kessler, simple physics, large-scale condensation]
+      if (sc->dtype != NC_I64 || numel(sc) != 3) return fail(NC_ERR_ARG, "AF_dcmip_schemes: three int64 switches");
+      const long long* f3 = (const long long*)sc->data;
+      h->kess_on = f3[0] != 0;
+      h->sm_on = f3[1] != 0;
+      h->sm_lsc = h->sm_on && f3[2] != 0;
+      if (!h->kess_on && !h->sm_on) return fail(NC_ERR_ARG, "AF_dcmip_schemes: neither Kessler nor simple physics");
+    }
+    if (h->sm_on) {   // what the simple physics reads besides the state (mod_forcing.py:236-250)
+      TRY(up_reg(h, T, "AF_dcmip_zh", D.KA, 1, &h->sm_zh));
+      TRY(up_reg(h, T, "AF_dcmip_zsfc", 1, 1, &h->sm_zsfc));
+      TRY(up_reg(h, T, "AF_dcmip_tsurf", 1, 1, &h->sm_tsurf));
+      TRY(up_reg(h, T, "AF_dcmip_ij", 1, 6, &h->sm_ij));
+    }
     TRY(scalar(T, "PRE00", C.PRE00));
     TRY(up_reg(h, T, "AF_dcmip_kessler_zf", D.KA, 1, &h->kess_zf));
     double f;

@@ -96,7 +96,7 @@ __global__ void k_forcing_hs(HsArgs a) {
 // bounds), so results can differ from numpy's in the last bits.
 // ---------------------------------------------------------------------------
 #define NC_KESS_K 64
-struct KesslerArgs {
+struct DcmipArgs {
   Prog<double> P;                 // PROG, updated in place
   double* Pq[NC_MAXNQ];           // tracer masses, updated in place
   int nq;
@@ -104,11 +104,124 @@ struct KesslerArgs {
   double* precip;                 // precipitation rate per column [l][j][i]
   double dt, RdCp, PRE00;
   int negative_fixer, update_tot_dens;
+  int kessler;                    // Kessler warm-rain microphysics on
   // terminator toy chemistry (optional): the Cl and Cl2 tracer indices, the
   // column latitude and longitude [l][j][i] in radians
   int n_cl, n_cl2;
   const double *lat, *lon;
+  // simple physics (optional): large-scale condensation switch, half-level
+  // heights [l][k][j][i], surface height, sea-surface temperature [l][j][i],
+  // the column unit vectors IX, IY, IZ, JX, JY, JZ [6][l][j][i]
+  int sm, sm_lsc;
+  const double *zh, *zsfc, *tsurf, *ij;
 };
+
+// numpy's sum of a contiguous row (pairwise: eight running partial sums
+// combined as ((0+1)+(2+3))+((4+5)+(6+7)), then the remainder in order;
+// rows below eight summed in order from 0), for n <= 128
+__device__ __forceinline__ double np_rowsum(const double* x, int n) {
+  if (n < 8) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s = s + x[i];
+    return s;
+  }
+  double r[8];
+  for (int m = 0; m < 8; ++m) r[m] = x[m];
+  int i = 8;
+  for (; i < n - (n % 8); i += 8)
+    for (int m = 0; m < 8; ++m) r[m] = r[m] + x[i + m];
+  double s = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+  for (; i < n; ++i) s = s + x[i];
+  return s;
+}
+
+// DCMIP simple physics (nhm/forcing/simple_physics.py:310-366, the DCMIP2016
+// v6 scheme with the RJ2012 boundary layer, no Held-Suarez) on one column of
+// nz levels ordered top to bottom: t, q, u, v updated in place; pm the full-
+// level pressure, pint the nz + 1 interface pressures (pint[nz] = ps);
+// CE..CFq work arrays of nz.  Returns the large-scale condensation's
+// precipitation rate (0 without lsc).  log, exp, pow are CUDA's.
+__device__ double simple_physics_col(int nz, double* t, double* q, double* u, double* v, const double* pm,
+                                     const double* pint, double ps, double tsurf, double dt, int lsc, double* CE,
+                                     double* CEm, double* CFu, double* CFv, double* CFt, double* CFq) {
+  const double rair = 287.0, rh2o = 461.5, grav = 9.80616, cpair = 1.0045e3, latvap = 2.5e6;
+  const double epsilo = rair / rh2o, zvir = (rh2o / rair) - 1.0;
+  const double Cv = 0.0011, T0 = 273.16, e0 = 610.78, rhow = 1000.0;
+  const double Cd0 = 0.0007, Cd1 = 0.000065, Cm = 0.002, v20 = 20.0;
+  const double p0 = 100000.0, pbltop = 85000.0, pblconst2 = 10000.0 * 10000.0;
+  const int b = nz - 1;
+  // height of the lowest full level from the initial state (:73-96)
+  const double za = rair / grav * t[b] * (1.0 + zvir * q[b]) * 0.5 * (log(ps) - log(pint[b]));
+  double precl = 0.0;
+  if (lsc) {   // large-scale condensation (:48-91); the rates into CE for the column sum
+    for (int c = 0; c < nz; ++c) {
+      const double qsat = epsilo * e0 / pm[c] * exp(-latvap / rh2o * ((1.0 / t[c]) - 1.0 / T0));
+      const double denom = 1.0 + (latvap / cpair) * (epsilo * latvap * qsat / (rair * t[c] * t[c]));
+      const double cond = (q[c] > qsat) ? (1.0 / dt) * (q[c] - qsat) / denom : 0.0;
+      t[c] = t[c] + (latvap / cpair) * cond * dt;
+      q[c] = q[c] - cond * dt;
+      CE[c] = cond * (pint[c + 1] - pint[c]) / (grav * rhow);
+    }
+    precl = np_rowsum(CE, nz);
+  }
+  // drag and diffusivities from the lowest-level wind (:118-149)
+  const double wind = sqrt(u[b] * u[b] + v[b] * v[b]);
+  const double Cd = (wind < v20) ? Cd0 + Cd1 * wind : Cm;
+  const double KmC = Cd * wind * za, KeC = Cv * wind * za;
+  auto decay = [&](int c) {
+    const double x = pbltop - pint[c];
+    return (pint[c] >= pbltop) ? 1.0 : exp(-(x * x) / pblconst2);
+  };
+  // implicit bulk surface fluxes of the lowest level (:200-225)
+  const double qsats = epsilo * e0 / ps * exp(-latvap / rh2o * ((1.0 / tsurf) - 1.0 / T0));
+  const double dm = 1.0 + Cd * wind * dt / za, dh = 1.0 + Cv * wind * dt / za;
+  u[b] = u[b] / dm;
+  v[b] = v[b] / dm;
+  t[b] = (t[b] + Cv * wind * tsurf * dt / za) / dh;
+  q[b] = (q[b] + Cv * wind * qsats * dt / za) / dh;
+  // implicit boundary-layer diffusion (:228-307): the interface between c and
+  // c + 1 couples them through fm (momentum) and fe (heat, moisture)
+  const double kap = rair / cpair, g2dt = dt * grav * grav;
+  auto iface = [&](int c, double& fm, double& fe) {
+    const double tvp = t[c + 1] * (1.0 + zvir * q[c + 1]), tv = t[c] * (1.0 + zvir * q[c]);
+    const double rho = pint[c + 1] / (rair * (tvp + tv) / 2.0);
+    const double dpm = pm[c + 1] - pm[c];
+    const double dc = decay(c + 1);
+    fm = g2dt * (KmC * dc) * rho * rho / dpm;
+    fe = g2dt * (KeC * dc) * rho * rho / dpm;
+  };
+  double ce = 0.0, cem = 0.0, cfu = 0.0, cfv = 0.0, cft = 0.0, cfq = 0.0;
+  double fm_lo = 0.0, fe_lo = 0.0;   // the interface below level c
+  for (int c = nz - 1; c >= 0; --c) {
+    const double rp = 1.0 / (pint[c + 1] - pint[c]);
+    double fm_up = 0.0, fe_up = 0.0;
+    if (c > 0) iface(c - 1, fm_up, fe_up);
+    // CAm / CCm, CA / CC of the reference: couplings to the level below / above
+    const double am = (c < nz - 1) ? rp * fm_lo : 0.0, ae = (c < nz - 1) ? rp * fe_lo : 0.0;
+    const double bm = (c > 0) ? rp * fm_up : 0.0, be = (c > 0) ? rp * fe_up : 0.0;
+    const double de = 1.0 + ae + be - ae * ce, dmm = 1.0 + am + bm - am * cem;
+    ce = be / de;
+    cem = bm / dmm;
+    cfu = (u[c] + am * cfu) / dmm;
+    cfv = (v[c] + am * cfv) / dmm;
+    cft = (pow(p0 / pm[c], kap) * t[c] + ae * cft) / de;
+    cfq = (q[c] + ae * cfq) / de;
+    CE[c] = ce; CEm[c] = cem; CFu[c] = cfu; CFv[c] = cfv; CFt[c] = cft; CFq[c] = cfq;
+    fm_lo = fm_up;
+    fe_lo = fe_up;
+  }
+  u[0] = CFu[0];
+  v[0] = CFv[0];
+  t[0] = CFt[0] * pow(pm[0] / p0, kap);
+  q[0] = CFq[0];
+  for (int c = 1; c < nz; ++c) {
+    u[c] = CEm[c] * u[c - 1] + CFu[c];
+    v[c] = CEm[c] * v[c - 1] + CFv[c];
+    t[c] = (CE[c] * t[c - 1] * pow(p0 / pm[c - 1], kap) + CFt[c]) * pow(pm[c] / p0, kap);
+    q[c] = CE[c] * q[c - 1] + CFq[c];
+  }
+  return precl;
+}
 
 // nhm/forcing/terminator.py:20-70 tendency_terminator at one level: the Cl
 // tendency (Cl2's is minus half of it); sin, cos, exp and sqrt are CUDA's
@@ -127,7 +240,7 @@ __device__ __forceinline__ double terminator_cl_f(double lat_deg, double lon_deg
   return -el * (cl - det + r) * (cl + det + r) / (1.0 + expdt + dt * el * (cl + r));
 }
 
-__global__ void k_forcing_kessler(KesslerArgs a) {
+__global__ void k_forcing_dcmip(DcmipArgs a) {
   const int t = (int)blockIdx.x * blockDim.x + threadIdx.x;
   int i, j, l;
   if (!col_of(t, i, j, l)) return;
@@ -149,8 +262,10 @@ __global__ void k_forcing_kessler(KesslerArgs a) {
     if (a.negative_fixer)
       for (int n = 0; n < 3; ++n) q[n] = fmax(q[n], 0.0);
   };
-  double th[NC_KESS_K], qv[NC_KESS_K], qc[NC_KESS_K], qr[NC_KESS_K], r[NC_KESS_K], rh[NC_KESS_K];
-  double pc[NC_KESS_K], vq[NC_KESS_K], pk[NC_KESS_K], z[NC_KESS_K];
+  double th[NC_KESS_K], qv[NC_KESS_K], qc[NC_KESS_K], qr[NC_KESS_K], pk[NC_KESS_K];
+  double prec = 0.0;
+  if (a.kessler) {
+  double r[NC_KESS_K], rh[NC_KESS_K], pc[NC_KESS_K], vq[NC_KESS_K], z[NC_KESS_K];
   // dry mixing ratios, dry density (in rh for now), Exner function, theta
   for (int m = 0; m < nz; ++m) {
     double rho, pre, tem, ein, q[3];
@@ -245,16 +360,54 @@ __global__ void k_forcing_kessler(KesslerArgs a) {
     if (nt < rainsplit)
       for (int m = 0; m < nz; ++m) vq[m] = 36.34 * pow(qr[m] * r[m], 0.1364) * rh[m];
   }
-  a.precip[(l * cD.G + j) * cD.G + i] = precl / (double)rainsplit;
+  prec = prec + precl / (double)rainsplit;
+  }   // Kessler
+  // simple physics from the same state, top down (mod_af_dcmip.py:230-317)
+  double st[NC_KESS_K], sq[NC_KESS_K], su[NC_KESS_K], sv[NC_KESS_K];
+  const int cidx = (l * cD.G + j) * cD.G + i;
+  const int npl = cD.L * cD.G * cD.G;
+  if (a.sm) {
+    double pm[NC_KESS_K], pint[NC_KESS_K + 1];
+    double w1[NC_KESS_K], w2[NC_KESS_K], w3[NC_KESS_K], w4[NC_KESS_K], w5[NC_KESS_K], w6[NC_KESS_K];
+    const double* IJ = a.ij;
+    double alt_up = 0.0, alth_up = 0.0;
+    for (int cc = 0; cc < nz; ++cc) {
+      const int k = kmax - cc, p = c.at(k);
+      double rho, pre, tem, ein, q[3];
+      diag(k, rho, pre, tem, ein, q);
+      const double RHOG = P[0][p];
+      const double vx = P[1][p] / RHOG, vy = P[2][p] / RHOG, vz = P[3][p] / RHOG;
+      st[cc] = tem;
+      sq[cc] = q[0];
+      su[cc] = vx * IJ[cidx] + vy * IJ[npl + cidx] + vz * IJ[2 * npl + cidx];
+      sv[cc] = vx * IJ[3 * npl + cidx] + vy * IJ[4 * npl + cidx] + vz * IJ[5 * npl + cidx];
+      pm[cc] = pre;
+      const double alt = a.zf[p], alth = a.zh[p];
+      if (cc > 0)   // log-interpolated interface pressure (mod_af_dcmip.py:254-259)
+        pint[cc] = pm[cc] * exp(log(pm[cc - 1] / pm[cc]) * (alth_up - alt) / (alt_up - alt));
+      alt_up = alt;
+      alth_up = alth;
+    }
+    double ps;
+    {   // single-layer hydrostatic surface pressure (mod_forcing.py:250)
+      double rho, pre, tem, ein, q[3];
+      diag(kmin, rho, pre, tem, ein, q);
+      ps = pre + rho * cC.GRAV * (a.zf[c.at(kmin)] - a.zsfc[cidx]);
+    }
+    pint[0] = 0.0;
+    pint[nz] = ps;
+    prec = prec + simple_physics_col(nz, st, sq, su, sv, pm, pint, ps, a.tsurf[cidx], dt, a.sm_lsc, w1, w2, w3, w4,
+                                     w5, w6);
+  }
+  a.precip[cidx] = prec;
   // back to wet mixing ratios, the tendencies, and their application on every level
   for (int k = 0; k < KA; ++k) {
     const int p = c.at(k);
     double rho, pre, tem, ein, q[3];
     diag(k, rho, pre, tem, ein, q);
-    double fe = 0.0, fq[3] = {0.0, 0.0, 0.0}, fcl = 0.0, fcl2 = 0.0;
+    double fe = 0.0, fq[3] = {0.0, 0.0, 0.0}, fv[3] = {0.0, 0.0, 0.0}, fcl = 0.0, fcl2 = 0.0;
     if (k >= kmin && k <= kmax && a.n_cl >= 0) {   // mod_af_dcmip.py:171-187
       const double d2r = 3.141592653589793 / 180.0;
-      const int cidx = (l * cD.G + j) * cD.G + i;
       const double lat_deg = a.lat[cidx] / d2r, lon_deg = a.lon[cidx] / d2r;
       const double RHOG = P[0][p];
       double qcl = a.Pq[a.n_cl][p] / RHOG, qcl2 = a.Pq[a.n_cl2][p] / RHOG;
@@ -267,24 +420,39 @@ __global__ void k_forcing_kessler(KesslerArgs a) {
       fcl = cl_f * qvd;
       fcl2 = (-cl_f / 2.0) * qvd;
     }
-    if (k >= kmin && k <= kmax) {
+    if (k >= kmin && k <= kmax && a.kessler) {
       const int m = k - kmin;
       const double qd2 = 1.0 / (1.0 + qv[m] + qc[m] + qr[m]);
       const double qvk = qv[m] * qd2, qck = qc[m] * qd2, qrk = qr[m] * qd2;
       const double cvk = qd2 * cC.CVdry + qvk * cC.CVW[0] + qck * cC.CVW[1] + qrk * cC.CVW[2];
-      fq[0] = (qvk - q[0]) / dt;
-      fq[1] = (qck - q[1]) / dt;
-      fq[2] = (qrk - q[2]) / dt;
+      fq[0] = fq[0] + (qvk - q[0]) / dt;
+      fq[1] = fq[1] + (qck - q[1]) / dt;
+      fq[2] = fq[2] + (qrk - q[2]) / dt;
       const double tem_new = th[m] * pk[m];
       const double cv_old = ein / tem;
       const double dtem = tem_new - tem;
       const double dcv = cvk - cv_old;
-      fe = (cv_old * dtem + tem * dcv + dcv * dtem) / dt;
+      fe = fe + (cv_old * dtem + tem * dcv + dcv * dtem) / dt;
+    }
+    if (k >= kmin && k <= kmax && a.sm) {   // mod_af_dcmip.py:472-511 (WARM)
+      const int cc = kmax - k;
+      const double RHOG = P[0][p];
+      const double vel[3] = {P[1][p] / RHOG, P[2][p] / RHOG, P[3][p] / RHOG};
+      for (int d = 0; d < 3; ++d)
+        fv[d] = (su[cc] * a.ij[d * npl + cidx] + sv[cc] * a.ij[(3 + d) * npl + cidx] - vel[d]) / dt;
+      const double qvn = sq[cc];
+      const double qd = 1.0 - qvn - q[1] - q[2];
+      const double cv = qd * cC.CVdry + qvn * cC.CVW[0] + q[1] * cC.CVW[1] + q[2] * cC.CVW[2];
+      fq[0] = fq[0] + (qvn - q[0]) / dt;
+      const double cv_old = ein / tem;
+      const double dtem = st[cc] - tem;
+      const double dcv = cv - cv_old;
+      fe = fe + (cv_old * dtem + tem * dcv + dcv * dtem) / dt;
     }
     const double gs = cG.GSGAM2[p];
-    P[1][p] = P[1][p] + dt * 0.0 * rho * gs;
-    P[2][p] = P[2][p] + dt * 0.0 * rho * gs;
-    P[3][p] = P[3][p] + dt * 0.0 * rho * gs;
+    P[1][p] = P[1][p] + dt * fv[0] * rho * gs;
+    P[2][p] = P[2][p] + dt * fv[1] * rho * gs;
+    P[3][p] = P[3][p] + dt * fv[2] * rho * gs;
     P[5][p] = P[5][p] + dt * fe * rho * gs;
     double rhog = P[0][p];
     for (int n = 0; n < a.nq; ++n) {

@@ -199,6 +199,25 @@ HIST_CONSTS = ("LHV", "UNDEF", "PSAT0", "RTEM00", "CPovR_liq", "CPovR_ice", "Lov
 HIST_TRACERS = ("I_QV", "I_QC", "I_QR", "I_QI", "I_QS", "I_QG")
 
 
+def dcmip_sst(lat, latdepend: bool):
+    """the sea-surface temperature of the DCMIP simple physics per column
+    (nhm/forcing/simple_physics.py:152-197 _sst_tsurf, no Held-Suarez): the
+    moist baroclinic wave's latitude profile, or 302.15 K everywhere; the
+    reference's numpy expressions, so the device reads the reference's values"""
+    import math
+    if not latdepend:
+        return np.full_like(lat, 302.15)
+    pi = math.pi
+    T00, u0, a, omega, q0, eta0, rair, rh2o = 288.0, 35.0, 6371220.0, 7.29212e-5, 0.021, 0.252, 287.0, 461.5
+    zvir = (rh2o / rair) - 1.0
+    etav, latw = (1.0 - eta0) * 0.5 * pi, 2.0 * pi / 9.0
+    sinl, cosl = np.sin(lat), np.cos(lat)
+    termA = (-2.0 * sinl ** 6 * (cosl ** 2 + 1.0 / 3.0) + 10.0 / 63.0) * u0 * (math.cos(etav)) ** 1.5
+    termB = (8.0 / 5.0 * cosl ** 3 * (sinl ** 2 + 2.0 / 3.0) - pi / 4.0) * a * omega * 0.5
+    pref = pi * u0 / rair * 1.5 * math.sin(etav) * (math.cos(etav)) ** 0.5
+    return (T00 + pref * (termA + termB)) / (1.0 + zvir * q0 * np.exp(-(lat / latw) ** 4))
+
+
 def setup_table(geo: dict) -> dict:
     """Host arrays handed to ``nc_create`` (names as in include/nicam_cuda.h).
 
@@ -263,6 +282,16 @@ def setup_table(geo: dict) -> dict:
         for k in ("AF_negative_fixer", "AF_update_tot_dens"):
             if k in geo:
                 t[k] = np.asarray(float(_scalar(geo[k])), np.float64)
+        if "AF_dcmip_schemes" in geo:   # [Kessler, simple physics, latitude-dependent SST, condensation]
+            kes, sm, latdep, lsc = (int(x) for x in np.asarray(geo["AF_dcmip_schemes"]).reshape(4))
+            t["AF_dcmip_schemes"] = np.asarray([kes, sm, lsc], np.int64)
+            if sm:
+                G, L = int(_scalar(geo["gall_1d"])), int(_scalar(geo["lall"]))
+                t["AF_dcmip_zh"] = np.ascontiguousarray(geo["AF_dcmip_zh"], np.float64)
+                t["AF_dcmip_zsfc"] = np.ascontiguousarray(np.asarray(geo["AF_dcmip_zsfc"], np.float64).reshape(G, G, 1, L))
+                t["AF_dcmip_ij"] = np.ascontiguousarray(np.asarray(geo["AF_dcmip_ij"], np.float64).reshape(G, G, 1, L, 6))
+                lat = np.asarray(geo["AF_dcmip_lat"], np.float64).reshape(G, G, 1, L)
+                t["AF_dcmip_tsurf"] = np.ascontiguousarray(dcmip_sst(lat, bool(latdep)))
         if "AF_dcmip_chem" in geo:   # terminator toy chemistry: (Cl, Cl2) tracer indices, column lat / lon
             G, L = int(_scalar(geo["gall_1d"])), int(_scalar(geo["lall"]))
             t["AF_dcmip_chem"] = np.ascontiguousarray(np.asarray(geo["AF_dcmip_chem"]).reshape(2), np.int64)

@@ -84,6 +84,60 @@ def golden_kessler_chem():
     return geo, st, {k: d[k] for k in d.files if k.startswith("precip")}
 
 
+def _dcmip_fixture(name):
+    import numpy as np
+    from make_golden import load
+    path = os.path.join(GOLDEN, f"gl03_z10_{name}.npz")
+    geo, st = load(path)
+    d = np.load(path)
+    return geo, st, {k: d[k] for k in d.files if k.startswith("precip")}
+
+
+@pytest.fixture(scope="session")
+def golden_dcmip11():
+    """the DCMIP2016 case 1-1 scheme set run by the reference
+    (make_kessler.py --case dcmip11): Kessler, the simple physics with the
+    latitude-dependent sea-surface temperature and no large-scale
+    condensation, the terminator chemistry; set-up arrays with the
+    half-level heights, surface height, column lat / lon and unit vectors"""
+    return _dcmip_fixture("dcmip11")
+
+
+@pytest.fixture(scope="session")
+def golden_smlsc():
+    """the simple physics alone with its large-scale condensation and the
+    constant sea-surface temperature, run by the reference
+    (make_kessler.py --case smlsc)"""
+    return _dcmip_fixture("smlsc")
+
+
+def dcmip_oracle_args(geo):
+    """the oracle's forcing_step_kessler keywords for a DCMIP fixture"""
+    fl = [int(x) for x in geo["dcmip_flags"]]
+    chem = (geo["GRD_LAT"], geo["GRD_LON"], int(geo["NCHEM_STR"]), int(geo["NCHEM_END"])) \
+        if "NCHEM_STR" in geo else None
+    sm = dict(zh=geo["GRD_ZH"], zsfc=geo["GRD_zsfc"], lat=geo["GRD_LAT"], ij=geo["GMTR_p_IJ"],
+              latdepend=bool(fl[2]), lsc=bool(fl[3])) if fl[1] else None
+    return dict(chem=chem, kessler_on=bool(fl[0]), sm=sm)
+
+
+def dcmip_device_setup(geo):
+    """the fixture's set-up with the DCMIP entries the device reads (GRD_LAT
+    itself would be taken for the Held-Suarez latitudes)"""
+    import numpy as np
+    g = {k: v for k, v in geo.items() if k not in ("GRD_LAT", "GRD_LON", "GRD_ZH", "GRD_zsfc", "GMTR_p_IJ")}
+    g["AF_dcmip_kessler"] = 1
+    g["AF_dcmip_schemes"] = np.asarray(geo["dcmip_flags"], np.int64)
+    if "NCHEM_STR" in geo:
+        g["AF_dcmip_chem"] = np.asarray([int(geo["NCHEM_STR"]), int(geo["NCHEM_END"])], np.int64)
+        g["AF_dcmip_lon"] = geo["GRD_LON"]
+    if "GRD_LAT" in geo:
+        g["AF_dcmip_lat"] = geo["GRD_LAT"]
+    if "GRD_ZH" in geo:
+        g["AF_dcmip_zh"], g["AF_dcmip_zsfc"], g["AF_dcmip_ij"] = geo["GRD_ZH"], geo["GRD_zsfc"], geo["GMTR_p_IJ"]
+    return g
+
+
 @pytest.fixture(scope="session")
 def golden_hs():
     """gl03 z10 with the reference's Held-Suarez forcing (make_hs.py): setup

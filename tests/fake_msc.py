@@ -89,16 +89,25 @@ def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_
            tim=tim, numf=numf, dyn=dyn, ppm=ppm, prgv=prgv)
     if satr is not None:
         m.satr = satr
-    if dcmip is not None:   # DCMIP forcing: Kessler (and the terminator chemistry when lat / lon are given)
-        chem = "GRD_LAT" in dcmip
-        grd.GRD_Z = 0
-        grd.GRD_vz = np.asarray(dcmip["GRD_Z"])[..., None]
-        if chem:
+    if dcmip is not None:   # DCMIP forcing: the schemes of dcmip_flags (Kessler only when absent)
+        chem = "NCHEM_STR" in dcmip
+        fl = [int(x) for x in dcmip.get("dcmip_flags", (1, 0, 0, 0))]
+        grd.GRD_Z, grd.GRD_ZH, grd.GRD_ZSFC = 0, 1, 0
+        zh = dcmip.get("GRD_ZH", dcmip["GRD_Z"])
+        grd.GRD_vz = np.stack([np.asarray(dcmip["GRD_Z"]), np.asarray(zh)], axis=-1)
+        if "GRD_LAT" in dcmip:
             grd.GRD_LAT = np.asarray(dcmip["GRD_LAT"])[:, :, None, :]
             grd.GRD_LON = np.asarray(dcmip["GRD_LON"])[:, :, None, :]
+        if chem:
             rcnf.NCHEM_STR, rcnf.NCHEM_END = int(dcmip["NCHEM_STR"]), int(dcmip["NCHEM_END"])
+        if fl[1]:   # the simple physics' surface height; its unit vectors are GMTR_p columns 2..7
+            grd.GRD_zs = np.asarray(dcmip["GRD_zsfc"])[:, :, None, :, None]
+            gmtr.GMTR_p_IX, gmtr.GMTR_p_IY, gmtr.GMTR_p_IZ, gmtr.GMTR_p_JX, gmtr.GMTR_p_JY, gmtr.GMTR_p_JZ = range(2, 8)
+            assert np.array_equal(gmtr.GMTR_p[:, :, 0, :, 2:8], dcmip["GMTR_p_IJ"])
         rcnf.RAIN_TYPE = "WARM"
-        m.afdcmip = NS(USE_Kessler=True, USE_SimpleMicrophys=False, USE_ToyChemistry=chem, USE_HeldSuarez=False)
+        m.afdcmip = NS(USE_Kessler=bool(fl[0]), USE_SimpleMicrophys=bool(fl[1]), SM_Latdepend_SST=bool(fl[2]),
+                       SM_LargeScaleCond=bool(fl[3]), SM_PBL_Bryan=False, USE_ToyChemistry=chem,
+                       USE_HeldSuarez=False)
         m.frc = NS(NEGATIVE_FIXER=False, UPDATE_TOT_DENS=True)
     if io_names is not None:   # the I/O object's diagnostic groups (share/mod_io.py:248-265)
         m.io = NS(_diag_names=[n for n in io_names if n.startswith("ml_")],

@@ -12,9 +12,15 @@ carries the two chemistry tracers Cl and Cl2 (CHEM_TYPE PASSIVE,
 CHEM_TRC_vmax 2) with the DCMIP terminator toy chemistry on
 (USE_ToyChemistry), started at half and one and a half times the reaction's
 equilibrium so that it acts, and the column latitudes and longitudes the
-chemistry reads are stored too.
+chemistry reads are stored too.  --case dcmip11 adds the DCMIP simple physics
+(USE_SimpleMicrophys with the latitude-dependent sea-surface temperature, no
+large-scale condensation: the scheme set of DCMIP2016 case 1-1) to Kessler
+and the chemistry; --case smlsc runs the simple physics alone with its
+large-scale condensation and the constant sea-surface temperature.  Both
+also store the half-level heights, the surface height and the column unit
+vectors the simple physics reads.
 
-    python tests/golden/make_kessler.py --ref <pyNICAM-DC checkout> --out tests/golden [--chem]
+    python tests/golden/make_kessler.py --ref <pyNICAM-DC checkout> --out tests/golden [--chem | --case NAME]
 """
 from __future__ import annotations
 
@@ -34,14 +40,27 @@ import make_golden as MG  # noqa: E402
 GL, VL, ZTOP, DTL, GAMMA, NSTEPS = 3, 10, 30000.0, 1200.0, 7.68e17, 2
 
 
-def run(ref: str, out_dir: str, chem: bool = False):
+# case name: (forcing_dcmip_param, terminator chemistry)
+CASES = {
+    "kessler": ({"USE_Kessler": True}, False),
+    "kessler_chem": ({"USE_Kessler": True}, True),
+    "dcmip11": ({"USE_Kessler": True, "USE_SimpleMicrophys": True, "SM_Latdepend_SST": True,
+                 "SM_LargeScaleCond": False}, True),
+    "smlsc": ({"USE_Kessler": False, "USE_SimpleMicrophys": True, "SM_Latdepend_SST": False,
+               "SM_LargeScaleCond": True}, False),
+}
+
+
+def run(ref: str, out_dir: str, case: str = "kessler"):
     import toml
+    flags, chem = CASES[case]
+    sm = bool(flags.get("USE_SimpleMicrophys", False))
     with tempfile.TemporaryDirectory() as tmp:
         case_dir = os.path.join(tmp, "kessler")
         MG.prep(ref, case_dir, GL, VL, ZTOP)
         c = toml.loads(MG.model_toml(ref, GL, VL, DTL, GAMMA, NSTEPS, "WARM"))
         c["runconfparam"]["AF_TYPE"] = "DCMIP"
-        c["forcing_dcmip_param"] = {"USE_Kessler": True}
+        c["forcing_dcmip_param"] = dict(flags)
         if chem:
             c["runconfparam"]["CHEM_TYPE"] = "PASSIVE"
             c["chemvarparam"] = {"CHEM_TRC_vmax": 2}
@@ -78,8 +97,10 @@ def run(ref: str, out_dir: str, chem: bool = False):
         mio.Io = _NoIo
         nic.initialize()
         m = nic.msc
-        assert m.rcnf.AF_TYPE == "DCMIP" and afdcmip.USE_Kessler and not afdcmip.USE_SimpleMicrophys
-        assert afdcmip.USE_ToyChemistry == chem and not afdcmip.USE_HeldSuarez
+        assert m.rcnf.AF_TYPE == "DCMIP" and afdcmip.USE_SimpleMicrophys == sm
+        for k, v in flags.items():
+            assert getattr(afdcmip, k) == v, k
+        assert afdcmip.USE_ToyChemistry == chem and not afdcmip.USE_HeldSuarez and not afdcmip.SM_PBL_Bryan
         assert m.rcnf.NQW_END == 2 and (m.rcnf.I_QV, m.rcnf.I_QC, m.rcnf.I_QR) == (0, 1, 2)
         assert not m.frc.NEGATIVE_FIXER and m.frc.UPDATE_TOT_DENS
         pv, pvp = m.prgv.PRG_var, m.prgv.PRG_var_pl
@@ -105,10 +126,20 @@ def run(ref: str, out_dir: str, chem: bool = False):
                 arr[..., 9] = arr[..., 0] * 0.5 * np.expand_dims(cl, kax) * (1.0 - q0)
                 arr[..., 10] = arr[..., 0] * 1.5 * np.expand_dims(cl2, kax) * (1.0 - q0)
         out = {"geo." + k: v for k, v in MG.geo_from_msc(m, pv.shape[-1] - 6).items()}
+        K0 = m.adm.ADM_K0
+        if chem or sm:
+            out["geo.GRD_LAT"] = np.ascontiguousarray(m.grd.GRD_LAT[:, :, K0, :])
+            out["geo.GRD_LON"] = np.ascontiguousarray(m.grd.GRD_LON[:, :, K0, :])
         if chem:
-            out["geo.GRD_LAT"] = np.ascontiguousarray(m.grd.GRD_LAT[:, :, m.adm.ADM_K0, :])
-            out["geo.GRD_LON"] = np.ascontiguousarray(m.grd.GRD_LON[:, :, m.adm.ADM_K0, :])
             out["geo.NCHEM_STR"], out["geo.NCHEM_END"] = np.asarray(3), np.asarray(4)
+        if sm:   # what the simple physics reads besides the state (mod_forcing.py:236-247)
+            gm = m.gmtr
+            idx = [gm.GMTR_p_IX, gm.GMTR_p_IY, gm.GMTR_p_IZ, gm.GMTR_p_JX, gm.GMTR_p_JY, gm.GMTR_p_JZ]
+            out["geo.GMTR_p_IJ"] = np.ascontiguousarray(np.stack([gm.GMTR_p[:, :, K0, :, n] for n in idx], -1))
+            out["geo.GRD_ZH"] = np.ascontiguousarray(m.grd.GRD_vz[:, :, :, :, m.grd.GRD_ZH])
+            out["geo.GRD_zsfc"] = np.ascontiguousarray(m.grd.GRD_zs[:, :, K0, :, m.grd.GRD_ZSFC])
+        out["geo.dcmip_flags"] = np.asarray([int(afdcmip.USE_Kessler), int(afdcmip.USE_SimpleMicrophys),
+                                             int(afdcmip.SM_Latdepend_SST), int(afdcmip.SM_LargeScaleCond)])
         out["geo.GRD_Z"] = np.ascontiguousarray(m.grd.GRD_vz[:, :, :, :, m.grd.GRD_Z])
         out["geo.PRE00"] = np.asarray(m.cnst.CONST_PRE00)
         out["state0"], out["state0_pl"] = pv.copy(), pvp.copy()
@@ -116,7 +147,7 @@ def run(ref: str, out_dir: str, chem: bool = False):
             nic.run(1)
             out[f"state{s + 1}"], out[f"state{s + 1}_pl"] = m.prgv.PRG_var.copy(), m.prgv.PRG_var_pl.copy()
             out[f"precip{s + 1}"] = np.asarray(m.frc.precip).copy()
-    path = os.path.join(out_dir, "gl03_z10_kessler_chem.npz" if chem else "gl03_z10_kessler.npz")
+    path = os.path.join(out_dir, f"gl03_z10_{case}.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path))
 
@@ -125,6 +156,7 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", required=True, help="root of a pyNICAM-DC checkout")
     ap.add_argument("--out", default=HERE)
-    ap.add_argument("--chem", action="store_true", help="with the terminator toy chemistry")
+    ap.add_argument("--chem", action="store_true", help="the Kessler case with the terminator toy chemistry")
+    ap.add_argument("--case", choices=sorted(CASES), default=None)
     args = ap.parse_args()
-    run(os.path.abspath(args.ref), os.path.abspath(args.out), args.chem)
+    run(os.path.abspath(args.ref), os.path.abspath(args.out), args.case or ("kessler_chem" if args.chem else "kessler"))

@@ -34,16 +34,65 @@ def test_unsupported_configurations_raise(pkg, golden):
         backend.CudaDyn._check_config(msc)
 
 
-def _dcmip_msc(geo, st, chem):
-    g = {k: v for k, v in geo.items() if k not in ("GRD_Z", "GRD_LAT", "GRD_LON", "NCHEM_STR", "NCHEM_END")}
-    extra = {k: geo[k] for k in ("GRD_Z", "GRD_LAT", "GRD_LON", "NCHEM_STR", "NCHEM_END") if k in geo}
+_DCMIP_KEYS = ("GRD_Z", "GRD_ZH", "GRD_zsfc", "GMTR_p_IJ", "GRD_LAT", "GRD_LON", "NCHEM_STR", "NCHEM_END",
+               "dcmip_flags")
+
+
+def _dcmip_msc(geo, st, chem=True):
+    g = {k: v for k, v in geo.items() if k not in _DCMIP_KEYS}
+    extra = {k: geo[k] for k in _DCMIP_KEYS if k in geo}
     return fake_msc(g, st["state0"], st["state0_pl"], af_type="DCMIP", dcmip=extra)
+
+
+@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_smlsc"])
+def test_dcmip_simple_physics_setup_from_services(pkg, case, request):
+    """the simple physics passes the configuration check (with or without
+    Kessler) and geo_from_msc hands the device its switches, half-level
+    heights, surface height, latitude and unit vectors; the Bryan boundary
+    layer and moist Held-Suarez are refused"""
+    backend = __import__(pkg.__name__ + ".backend", fromlist=["geo_from_msc"])
+    geo, st, _ = request.getfixturevalue(case)
+    msc = _dcmip_msc(geo, st)
+    backend.CudaDyn._check_config(msc)
+    got = backend.geo_from_msc(msc)
+    assert list(got["AF_dcmip_schemes"]) == [int(x) for x in geo["dcmip_flags"]]
+    for k, w in (("AF_dcmip_zh", "GRD_ZH"), ("AF_dcmip_zsfc", "GRD_zsfc"), ("AF_dcmip_ij", "GMTR_p_IJ"),
+                 ("AF_dcmip_lat", "GRD_LAT")):
+        assert np.array_equal(got[k], geo[w]), k
+    for attr in ("SM_PBL_Bryan", "USE_HeldSuarez"):
+        msc = _dcmip_msc(geo, st)
+        setattr(msc.afdcmip, attr, True)
+        with pytest.raises(NotImplementedError):
+            backend.CudaDyn._check_config(msc)
+
+
+@pytest.mark.gpu
+def test_cudadyn_dcmip_simple_physics(pkg, golden_dcmip11):
+    """the reference-facing step API with the DCMIP2016 case 1-1 scheme set
+    (Kessler, simple physics, chemistry): 1e-12 relative L2 over the state
+    and the precipitation"""
+    geo, st, pr = golden_dcmip11
+    msc = _dcmip_msc(geo, st)
+    dyn = pkg.CudaDyn(msc=msc)
+    try:
+        for n in (1, 2):
+            dyn.dynamics_step(msc)
+            precip = dyn.forcing_step(msc)
+            dyn.sync_prgvar_to_host(msc.prgv, msc)
+            ref = st[f"state{n}"]
+            err = np.sqrt(np.sum((msc.prgv.PRG_var - ref) ** 2)) / np.sqrt(np.sum(ref ** 2))
+            assert err <= 1e-12, (n, err)
+            want = pr[f"precip{n}"]
+            assert np.sqrt(np.sum((np.asarray(precip) - want) ** 2)) <= 1e-12 * np.sqrt(np.sum(want ** 2)), n
+    finally:
+        dyn.core.close()
 
 
 def test_dcmip_setup_from_services(pkg, golden_kessler_chem):
     """Kessler with the terminator chemistry passes the configuration check
-    and yields the chemistry's set-up (tracer indices, column lat / lon);
-    simple physics, Held-Suarez on top, or a third chemistry tracer do not"""
+    and yields the chemistry's set-up (tracer indices, column lat / lon); the
+    Bryan boundary layer, Held-Suarez on top, or a third chemistry tracer do
+    not"""
     backend = __import__(pkg.__name__ + ".backend", fromlist=["geo_from_msc"])
     geo, st, _ = golden_kessler_chem
     msc = _dcmip_msc(geo, st, True)
@@ -52,7 +101,7 @@ def test_dcmip_setup_from_services(pkg, golden_kessler_chem):
     assert got["AF_dcmip_kessler"] == 1 and list(got["AF_dcmip_chem"]) == [3, 4]
     assert np.array_equal(got["AF_dcmip_lat"], geo["GRD_LAT"]) and np.array_equal(got["AF_dcmip_lon"], geo["GRD_LON"])
     assert np.array_equal(got["GRD_Z"], geo["GRD_Z"])
-    for attr in ("USE_SimpleMicrophys", "USE_HeldSuarez"):
+    for attr in ("SM_PBL_Bryan", "USE_HeldSuarez"):
         msc = _dcmip_msc(geo, st, True)
         setattr(msc.afdcmip, attr, True)
         with pytest.raises(NotImplementedError):

@@ -150,3 +150,34 @@ def test_terminator_chemistry_setup_is_checked(pkg, golden_kessler_chem):
         g = _chem_setup(geo, bad)
         with pytest.raises(pkg.NicamError, match="AF_dcmip_chem"):
             pkg.NicamCuda(g, graph=False).close()
+
+
+@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_smlsc"])
+def test_simple_physics_vs_reference(pkg, case, request):
+    """DCMIP forcing with the simple physics on the device against the
+    reference's two steps (with Kessler and the chemistry as in DCMIP2016 case
+    1-1; alone with the large-scale condensation): log, exp, pow, sin and cos
+    are CUDA's, so relative L2 <= 1e-12 per prognostic and for the
+    precipitation, 1e-11 for Cl / Cl2"""
+    from conftest import dcmip_device_setup
+    geo, st, pr = request.getfixturevalue(case)
+    c = pkg.NicamCuda(dcmip_device_setup(geo), graph=False)
+    chem = (6 + int(geo["NCHEM_STR"]), 6 + int(geo["NCHEM_END"])) if "NCHEM_STR" in geo else ()
+    try:
+        c.upload(st["state0"], st["state0_pl"])
+        for n in (1, 2):
+            c.step(1)
+            c.forcing_step()
+            s, sp = c.download()
+            precip = c.forcing_precip()
+            errs = {}
+            for v in range(s.shape[-1]):
+                for a, b in ((s[..., v], st[f"state{n}"][..., v]), (sp[..., v], st[f"state{n}_pl"][..., v])):
+                    errs[v] = max(errs.get(v, 0.0), np.sqrt(np.sum((a - b) ** 2)) / max(np.sqrt(np.sum(b * b)), 1e-300))
+            want = pr[f"precip{n}"]
+            errs["precip"] = np.sqrt(np.sum((precip - want) ** 2)) / np.sqrt(np.sum(want * want))
+            print(case, "step", n, "relative L2:", errs)
+            for v, e in errs.items():
+                assert e <= (1e-11 if v in chem else 1e-12), (n, v, e)
+    finally:
+        c.close()

@@ -95,6 +95,45 @@ def test_oracle_terminator_chemistry_matches_reference(golden_kessler_chem):
         assert np.array_equal(precip, pr[f"precip{n}"]), n
 
 
+@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_smlsc"])
+def test_oracle_simple_physics_matches_reference(case, request):
+    """dynamics step + DCMIP forcing with the simple physics (with Kessler and
+    the chemistry as in DCMIP2016 case 1-1; alone with the large-scale
+    condensation and constant SST), against the reference run: states and
+    precipitation bit for bit"""
+    from conftest import dcmip_oracle_args
+    geo, st, pr = request.getfixturevalue(case)
+    G = O.Geo(geo)
+    kw = dcmip_oracle_args(geo)
+    s, sp = st["state0"], st["state0_pl"]
+    for n in (1, 2):
+        s, sp = O.dynamics_step(G, s, sp)
+        s, sp, precip = O.forcing_step_kessler(G, s, sp, geo["GRD_Z"], **kw)
+        assert np.array_equal(s, st[f"state{n}"]) and np.array_equal(sp, st[f"state{n}_pl"]), n
+        assert np.array_equal(precip, pr[f"precip{n}"]), n
+
+
+def test_simple_physics_fixtures_are_active(golden_kessler_chem, golden_dcmip11, golden_smlsc):
+    """the simple physics moved momentum, energy and vapour against the same
+    run without it, and its condensation rained in a fifth of the columns"""
+    _, a, _ = golden_kessler_chem
+    _, b, _ = golden_dcmip11
+    assert np.array_equal(a["state0"], b["state0"])
+    for v, lim in ((1, 0.1), (5, 10.0), (6, 1e-5)):
+        assert np.abs(a["state1"][..., v] - b["state1"][..., v]).max() > lim, v
+    _, _, pr = golden_smlsc
+    assert (pr["precip1"] > 0).mean() > 0.2
+
+
+def test_sst_of_the_device_setup_equals_the_oracle(pkg, golden_dcmip11):
+    """the sea-surface temperature runtime.setup_table hands the device is the
+    oracle's (pinned to the reference by the fixture), in both forms"""
+    geo, _, _ = golden_dcmip11
+    lat = geo["GRD_LAT"]
+    for latdep in (True, False):
+        assert np.array_equal(pkg.runtime.dcmip_sst(lat, latdep), O.dcmip_sst(lat, latdep))
+
+
 def test_terminator_fixture_is_active(golden_kessler_chem):
     """the chemistry changed Cl and Cl2 against the same step without it,
     and conserved the total chlorine Cl + 2 Cl2 of every cell"""
