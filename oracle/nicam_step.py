@@ -1692,9 +1692,12 @@ def hs_latitude_terms(lat):
     return sinlat ** 2, coslat ** 2, coslat ** 4
 
 
-def held_suarez(g, lat, pre, tem, vx, vy, vz):
+def held_suarez(g, lat, pre, tem, vx, vy, vz, moist=False):
     """forcing/mod_af_heldsuarez.py:38-88 AF_heldsuarez: tendencies
-    (fvx, fvy, fvz, fe) on regional (i,j,k,l) fields, zero outside kmin..kmax."""
+    (fvx, fvy, fvz, fe) on regional (i,j,k,l) fields, zero outside kmin..kmax;
+    ``moist`` takes the moist case's equilibrium profile (T_eq0 294 K,
+    DT_y 65 K; AF_heldsuarez_init :31-39)."""
+    T_eq0, DT_y = (294.0, 65.0) if moist else (HS_T_EQ0, HS_DT_Y)
     kmin, kmax = g.kmin, g.kmax
     sin2, cos2, cos4 = (t[:, :, None, :] for t in hs_latitude_terms(lat))
     psref = (0.5 * (pre[:, :, kmin, :] + pre[:, :, kmin - 1, :]))[:, :, None, :]
@@ -1705,7 +1708,7 @@ def held_suarez(g, lat, pre, tem, vx, vy, vz):
     fvz = -HS_KF * factor * vz
     ap0 = np.abs(pre / g.PRE00)
     Kt = HS_KA + (HS_KS - HS_KA) * factor * cos4
-    T_eq = np.maximum(200.0, (HS_T_EQ0 - HS_DT_Y * sin2
+    T_eq = np.maximum(200.0, (T_eq0 - DT_y * sin2
                               - HS_DTH_Z * np.log(np.maximum(ap0, 1e-30)) * cos2) * ap0 ** (g.Rdry / g.CPdry))
     fe = -Kt * (tem - T_eq) * g.CVdry
     kk = np.arange(pre.shape[2]).reshape(1, 1, -1, 1)
@@ -1835,14 +1838,20 @@ SP_CD0, SP_CD1, SP_CM, SP_V20 = 0.0007, 0.000065, 0.002, 20.0
 SP_P0, SP_PBLTOP, SP_PBLCONST = 100000.0, 85000.0, 10000.0
 
 
-def dcmip_sst(lat, latdepend):
-    """simple_physics.py:152-197 _sst_tsurf without Held-Suarez: the
-    latitude-dependent sea-surface temperature of the moist baroclinic wave
-    (test 1) or the constant 302.15 K of the tropical cyclone (test 0)"""
-    if not latdepend:
-        return np.full_like(lat, 302.15)
+def dcmip_sst(lat, latdepend, held_suarez=False, mitc_type=1):
+    """simple_physics.py:152-197 _sst_tsurf: for moist Held-Suarez the
+    Gaussian-in-latitude SST of MITC type 1-3; otherwise the latitude-dependent
+    sea-surface temperature of the moist baroclinic wave (test 1) or the
+    constant 302.15 K of the tropical cyclone (test 0)"""
     import math
     pi = math.pi
+    if held_suarez:
+        if mitc_type == 1:
+            return 29.0 * np.exp(-0.5 * lat * lat / (26.0 / 180.0 * pi) ** 2) + 271.0
+        amp, w, c0 = (29.0, 20.0, 17.0) if mitc_type == 2 else (32.0, 23.0, 12.0)
+        return amp * np.exp(-0.5 * np.maximum(np.abs(lat) - (c0 / 180.0 * pi), 0.0) ** 2 / (w / 180.0 * pi) ** 2) + 271.0
+    if not latdepend:
+        return np.full_like(lat, 302.15)
     T00, u0, a, omega, q0, eta0 = 288.0, 35.0, 6371220.0, 7.29212e-5, 0.021, 0.252
     etav, latw = (1.0 - eta0) * 0.5 * pi, 2.0 * pi / 9.0
     sinl, cosl = np.sin(lat), np.cos(lat)
@@ -1852,14 +1861,16 @@ def dcmip_sst(lat, latdepend):
     return (T00 + pref * (termA + termB)) / (1.0 + SP_ZVIR * q0 * np.exp(-(lat / latw) ** 4))
 
 
-def simple_physics(t, q, u, v, pmid, pint, pdel, rpdel, ps, tsurf, dtime, lsc):
+def simple_physics(t, q, u, v, pmid, pint, pdel, rpdel, ps, tsurf, dtime, lsc, Cexch=SP_C):
     """simple_physics.py:310-366 (RJ2012 boundary layer, no Held-Suarez) on
     (ncol, nz) columns ordered top to bottom: the lowest full level's
     hydrostatic height, the large-scale condensation (lsc, :48-91), the
     drag / diffusivities from the lowest-level wind (:118-149), the implicit
     bulk surface fluxes of the lowest level (:200-225) and the implicit
     boundary-layer diffusion of u, v, potential temperature and q
-    (:228-307).  Returns t, q, u, v and the condensation's precipitation."""
+    (:228-307).  ``Cexch`` is the heat / moisture exchange coefficient
+    (four times 0.0011 for moist Held-Suarez).  Returns t, q, u, v and the
+    condensation's precipitation."""
     ncol, nz = t.shape
     dlnpint = np.log(ps) - np.log(pint[:, nz - 1])
     za = SP_RAIR / SP_GRAV * t[:, -1] * (1.0 + SP_ZVIR * q[:, -1]) * 0.5 * dlnpint
@@ -1876,16 +1887,16 @@ def simple_physics(t, q, u, v, pmid, pint, pdel, rpdel, ps, tsurf, dtime, lsc):
     Cd = np.where(wind < SP_V20, SP_CD0 + SP_CD1 * wind, SP_CM)
     decay = np.where(pint[:, 0:nz] >= SP_PBLTOP, 1.0, np.exp(-(SP_PBLTOP - pint[:, 0:nz]) ** 2 / SP_PBLCONST ** 2))
     Km = (Cd * wind * za)[:, None] * decay
-    Ke = (SP_C * wind * za)[:, None] * decay
+    Ke = (Cexch * wind * za)[:, None] * decay
     # surface fluxes, lowest level only
     qsats = SP_EPSILO * SP_E0 / ps * np.exp(-SP_LATVAP / SP_RH2O * ((1.0 / tsurf) - 1.0 / SP_T0))
     dm = 1.0 + Cd * wind * dtime / za
-    dh = 1.0 + SP_C * wind * dtime / za
+    dh = 1.0 + Cexch * wind * dtime / za
     u, v, t, q = u.copy(), v.copy(), t.copy(), q.copy()
     u[:, -1] = u[:, -1] / dm
     v[:, -1] = v[:, -1] / dm
-    t[:, -1] = (t[:, -1] + SP_C * wind * tsurf * dtime / za) / dh
-    q[:, -1] = (q[:, -1] + SP_C * wind * qsats * dtime / za) / dh
+    t[:, -1] = (t[:, -1] + Cexch * wind * tsurf * dtime / za) / dh
+    q[:, -1] = (q[:, -1] + Cexch * wind * qsats * dtime / za) / dh
     # implicit vertical diffusion: coefficients at the interfaces between levels c and c+1
     kap = SP_RAIR / SP_CPAIR
     g2dt = dtime * SP_GRAV * SP_GRAV
@@ -1942,7 +1953,12 @@ def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_de
     column unit vectors GMTR_p IX..JZ (i, j, l, 6), the sea-surface
     temperature form and the large-scale condensation switch; its momentum,
     vapour and energy tendencies add to Kessler's (``kessler_on`` False
-    leaves the simple physics alone).  Returns (prg, prg_pl, precip (i, j, l))."""
+    leaves the simple physics alone).  With sm["held_suarez"] (and
+    sm["mitc"], the SST type) the moist Held-Suarez case: the simple physics
+    with the exchange coefficient x4 and the Held-Suarez SST, and the
+    Held-Suarez relaxation on top, its momentum tendency replacing the
+    others', its energy tendency added (mod_forcing.py:278-287).  Returns
+    (prg, prg_pl, precip (i, j, l))."""
     out = prg.copy()
     out_pl = prg_pl.copy()
     PROG = out[..., 0:6]
@@ -2004,9 +2020,10 @@ def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_de
                                                  / (alt_td[:, 0:nz - 1] - alt_td[:, 1:nz]))
         pint[:, nz] = pre_sfc
         pdel = pint[:, 1:nz + 1] - pint[:, 0:nz]
-        tsurf = dcmip_sst(flat(sm["lat"]), sm["latdepend"])
+        hs = bool(sm.get("held_suarez", False))
+        tsurf = dcmip_sst(flat(sm["lat"]), sm["latdepend"], hs, sm.get("mitc", 1))
         t_n, qv_n, u_n, v_n, pr2 = simple_physics(tem_td, qv_old, u, v, pre_td, pint, pdel, 1.0 / pdel, pre_sfc,
-                                                  tsurf, dt, sm["lsc"])
+                                                  tsurf, dt, sm["lsc"], SP_C * (4.0 if hs else 1.0))
         for d, (a, b, vd) in enumerate(((0, 3, vx_td), (1, 4, vy_td), (2, 5, vz_td))):
             fv[d] = grid(((u_n * ij[a][:, None] + v_n * ij[b][:, None] - vd) / dt)[:, ::-1])
         qc, qr = td(q[..., 1]), td(q[..., 2])
@@ -2018,6 +2035,11 @@ def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_de
         fq[0] = fq[0] + grid(((qv_n - qv_old) / dt)[:, ::-1])
         fe = fe + grid(((cv_old * dtem + tem_td * dcv + dcv * dtem) / dt)[:, ::-1])
         precl = precl + pr2
+        if hs:
+            hfvx, hfvy, hfvz, hfe = held_suarez(g, sm["lat"], pre, tem, DIAG[..., I_vx], DIAG[..., I_vy],
+                                                DIAG[..., I_vz], moist=True)
+            fv = [hfvx, hfvy, hfvz]
+            fe = fe + hfe
     if chem is not None:
         lat, lon, n_cl, n_cl2 = chem
         d2r = np.pi / 180.0

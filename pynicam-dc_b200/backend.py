@@ -44,7 +44,9 @@ def _dcmip_flags(msc) -> dict:
         obj = getattr(mod, "afdcmip", None) if mod is not None else None
     keys = ("USE_Kessler", "USE_SimpleMicrophys", "USE_ToyChemistry", "USE_HeldSuarez", "SM_Latdepend_SST",
             "SM_LargeScaleCond", "SM_PBL_Bryan")
-    return {k: bool(getattr(obj, k, False)) for k in keys}
+    out = {k: bool(getattr(obj, k, False)) for k in keys}
+    out["SM_MITC_SST_TYPE"] = int(getattr(obj, "SM_MITC_SST_TYPE", 1))
+    return out
 
 
 def geo_from_msc(msc) -> dict:
@@ -132,8 +134,9 @@ def geo_from_msc(msc) -> dict:
         fl = _dcmip_flags(msc)
         K0 = m.adm.ADM_K0
         g["AF_dcmip_schemes"] = np.asarray([fl["USE_Kessler"], fl["USE_SimpleMicrophys"], fl["SM_Latdepend_SST"],
-                                            fl["SM_LargeScaleCond"]], np.int64)
-        if fl["USE_ToyChemistry"] or fl["USE_SimpleMicrophys"]:
+                                            fl["SM_LargeScaleCond"], fl["USE_HeldSuarez"], fl["SM_MITC_SST_TYPE"]],
+                                           np.int64)
+        if fl["USE_ToyChemistry"] or fl["USE_SimpleMicrophys"] or fl["USE_HeldSuarez"]:
             g["AF_dcmip_lat"] = np.ascontiguousarray(m.grd.GRD_LAT[:, :, K0, :])
         if fl["USE_ToyChemistry"]:   # terminator chemistry on the Cl / Cl2 tracers
             g["AF_dcmip_chem"] = np.asarray([m.rcnf.NCHEM_STR, m.rcnf.NCHEM_END], np.int64)
@@ -238,13 +241,13 @@ class CudaDyn:
             raise NotImplementedError("cuda backend: water tracers must come first (NQW_STR = I_QV = 0), at most six")
         if getattr(r, "AF_TYPE", "NONE") == "DCMIP":
             flags = _dcmip_flags(msc)
-            if not (flags.get("USE_Kessler") or flags.get("USE_SimpleMicrophys")) or flags.get("USE_HeldSuarez") \
+            if not (flags.get("USE_Kessler") or flags.get("USE_SimpleMicrophys")) \
                     or flags.get("SM_PBL_Bryan") or getattr(r, "RAIN_TYPE", "DRY") != "WARM" or \
                     (flags.get("USE_ToyChemistry") and int(getattr(r, "NCHEM_END", -1)) - int(getattr(r, "NCHEM_STR", -1)) != 1):
                 raise NotImplementedError("cuda backend: DCMIP forcing with Kessler microphysics and / or the simple "
                                           "physics (RJ2012 boundary layer), optionally the terminator chemistry "
-                                          "(RAIN_TYPE WARM, two chemistry tracers; no Bryan boundary layer or "
-                                          "moist Held-Suarez)")
+                                          "and moist Held-Suarez (RAIN_TYPE WARM, two chemistry tracers; no Bryan "
+                                          "boundary layer)")
         elif getattr(r, "AF_TYPE", "NONE") not in ("NONE", "HELD-SUAREZ"):
             raise NotImplementedError("cuda backend: artificial forcing NONE or HELD-SUAREZ only")
 

@@ -373,6 +373,8 @@ struct nc_handle {
   int kess_n_cl = -1, kess_n_cl2 = -1;      // terminator toy chemistry tracers (optional)
   const double *kess_lat = nullptr, *kess_lon = nullptr;
   int kess_on = 1, sm_on = 0, sm_lsc = 0;   // DCMIP schemes: Kessler, simple physics, its condensation
+  int dcmip_hs = 0;                         // moist Held-Suarez on top of the DCMIP schemes
+  const double* dcmip_hs_lat = nullptr;
   const double *sm_zh = nullptr, *sm_zsfc = nullptr, *sm_tsurf = nullptr, *sm_ij = nullptr;
   // derived history diagnostics (optional setup; nc_history_vars)
   bool hist = false;
@@ -1419,6 +1421,22 @@ struct SingleStream {
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
+// the Held & Suarez (1994) parameters (nhm/forcing/mod_af_heldsuarez.py:19-39),
+// with the moist case's equilibrium profile for DCMIP2016 case 2-1
+static HsParams hs_params(const nc_handle* h, bool moist = false) {
+  HsParams hp;
+  hp.RdCp = h->C.Rdry / h->C.CPdry;
+  hp.sigma_b = 0.7;
+  hp.Kf = 1.0 / (1.0 * 86400.0);
+  hp.Dth_z = 10.0;
+  hp.Ka = 1.0 / (40.0 * 86400.0);
+  hp.Ks = 1.0 / (4.0 * 86400.0);
+  hp.T_eq0 = moist ? 294.0 : 315.0;
+  hp.DT_y = moist ? 65.0 : 60.0;
+  hp.PRE00 = h->C.PRE00;
+  return hp;
+}
+
 extern "C" {
 
 int nc_forcing_step(nc_handle* h) {
@@ -1453,6 +1471,10 @@ int nc_forcing_step(nc_handle* h) {
     a.zsfc = h->sm_zsfc;
     a.tsurf = h->sm_tsurf;
     a.ij = h->sm_ij;
+    a.hs = h->dcmip_hs;
+    a.sm_C = h->dcmip_hs ? 0.0011 * 4.0 : 0.0011;   // simple_physics.py:25-46
+    a.hs_lat3 = h->dcmip_hs_lat;
+    a.hp = hs_params(h, true);
     k_forcing_dcmip<<<(unsigned)((D.npt2 + 63) / 64), 64, 0, h->stream>>>(a);
     TRY(check_launch(h, "forcing_dcmip"));
     TRY(comm_prg<double>(h));
@@ -1464,15 +1486,7 @@ int nc_forcing_step(nc_handle* h) {
   for (int n = 0; n < h->C.nqw; ++n) a.Pqw[n] = h->Pq[n].r;
   a.lat3 = h->hs_lat;
   a.dt = h->dtl;
-  a.RdCp = h->C.Rdry / h->C.CPdry;
-  a.sigma_b = 0.7;
-  a.Kf = 1.0 / (1.0 * 86400.0);
-  a.Dth_z = 10.0;
-  a.Ka = 1.0 / (40.0 * 86400.0);
-  a.Ks = 1.0 / (4.0 * 86400.0);
-  a.T_eq0 = 315.0;
-  a.DT_y = 60.0;
-  a.PRE00 = h->C.PRE00;
+  a.hp = hs_params(h);
   k_forcing_hs<<<(unsigned)((D.npt2 + kBlock - 1) / kBlock), kBlock, 0, h->stream>>>(a);
   TRY(check_launch(h, "forcing_hs"));
   TRY(comm_prg<double>(h));
@@ -1750,14 +1764,17 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
     if (C.nqw != 3) return fail(NC_ERR_ARG, "DCMIP forcing needs RAIN_TYPE WARM (NQW_END = 2: vapour, cloud, rain)");
     if (D.kmax - D.kmin + 1 > NC_KESS_K || D.kmax - D.kmin < 1)
       return fail(NC_ERR_ARG, "DCMIP forcing: 2.." + std::to_string(NC_KESS_K) + " model levels");
-    if (const nc_array* sc = T.get("AF_dcmip_schemes")) {   // [Kessler, simple physics, large-scale condensation]
-      if (sc->dtype != NC_I64 || numel(sc) != 3) return fail(NC_ERR_ARG, "AF_dcmip_schemes: three int64 switches");
+    if (const nc_array* sc = T.get("AF_dcmip_schemes")) {   // [Kessler, simple physics, condensation(, Held-Suarez)]
+      if (sc->dtype != NC_I64 || (numel(sc) != 3 && numel(sc) != 4))
+        return fail(NC_ERR_ARG, "AF_dcmip_schemes: three or four int64 switches");
       const long long* f3 = (const long long*)sc->data;
       h->kess_on = f3[0] != 0;
       h->sm_on = f3[1] != 0;
       h->sm_lsc = h->sm_on && f3[2] != 0;
+      h->dcmip_hs = numel(sc) == 4 && f3[3] != 0;
       if (!h->kess_on && !h->sm_on) return fail(NC_ERR_ARG, "AF_dcmip_schemes: neither Kessler nor simple physics");
     }
+    if (h->dcmip_hs) TRY(up_reg(h, T, "AF_dcmip_hs_lat_terms", 1, 3, &h->dcmip_hs_lat));
     if (h->sm_on) {   // what the simple physics reads besides the state (mod_forcing.py:236-250)
       TRY(up_reg(h, T, "AF_dcmip_zh", D.KA, 1, &h->sm_zh));
       TRY(up_reg(h, T, "AF_dcmip_zsfc", 1, 1, &h->sm_zsfc));

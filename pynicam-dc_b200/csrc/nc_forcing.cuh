@@ -6,13 +6,35 @@
 namespace nc {
 
 // Held & Suarez (1994) dry-case parameters (nhm/forcing/mod_af_heldsuarez.py:19-36)
+struct HsParams {
+  double RdCp;            // Rdry / CPdry
+  double sigma_b, Kf, Dth_z, Ka, Ks, T_eq0, DT_y, PRE00;
+};
 struct HsArgs {
   Prog<double> P;         // PROG, updated in place
   const double* Pqw[NC_MAXQW];   // the water tracers (0: vapour) for the diagnostics
   const double* lat3;     // planes |sin lat|^2, |cos lat|^2, |cos lat|^4 of each column
-  double dt, RdCp;        // large time step; Rdry / CPdry
-  double sigma_b, Kf, Dth_z, Ka, Ks, T_eq0, DT_y, PRE00;
+  double dt;              // large time step
+  HsParams hp;
 };
+
+// the Held-Suarez tendencies at one level (mod_af_heldsuarez.py:38-88):
+// Rayleigh friction below sigma_b and Newtonian relaxation of temperature to
+// the radiative-equilibrium profile; psref = (pre(kmin) + pre(kmin-1)) / 2
+__device__ __forceinline__ void hs_tendency(const HsParams& a, double sin2, double cos2, double cos4, double psref,
+                                            double pre, double tem, double vx, double vy, double vz, double& fvx,
+                                            double& fvy, double& fvz, double& fe) {
+  const double sigma = pre / psref;
+  const double factor = npmax((sigma - a.sigma_b) / (1.0 - a.sigma_b), 0.0);
+  fvx = -a.Kf * factor * vx;
+  fvy = -a.Kf * factor * vy;
+  fvz = -a.Kf * factor * vz;
+  const double ap0 = fabs(pre / a.PRE00);
+  const double Kt = a.Ka + (a.Ks - a.Ka) * factor * cos4;
+  const double T_eq = npmax(200.0, (a.T_eq0 - a.DT_y * sin2 - a.Dth_z * log(npmax(ap0, 1e-30)) * cos2) *
+                                       pow(ap0, a.RdCp));
+  fe = -Kt * (tem - T_eq) * cC.CVdry;
+}
 
 // One thread per interior regional column: the diagnostics of the prognostic
 // (kernels/diag.py, no boundary conditions), the Held-Suarez tendencies
@@ -59,16 +81,8 @@ __global__ void k_forcing_hs(HsArgs a) {
       continue;
     }
     diag(k, rho, pre, tem, vx, vy, vz);
-    const double sigma = pre / psref;
-    const double factor = npmax((sigma - a.sigma_b) / (1.0 - a.sigma_b), 0.0);
-    const double fvx = -a.Kf * factor * vx;
-    const double fvy = -a.Kf * factor * vy;
-    const double fvz = -a.Kf * factor * vz;
-    const double ap0 = fabs(pre / a.PRE00);
-    const double Kt = a.Ka + (a.Ks - a.Ka) * factor * cos4;
-    const double T_eq = npmax(200.0, (a.T_eq0 - a.DT_y * sin2 - a.Dth_z * log(npmax(ap0, 1e-30)) * cos2) *
-                                         pow(ap0, a.RdCp));
-    const double fe = -Kt * (tem - T_eq) * cC.CVdry;
+    double fvx, fvy, fvz, fe;
+    hs_tendency(a.hp, sin2, cos2, cos4, psref, pre, tem, vx, vy, vz, fvx, fvy, fvz, fe);
     const double gs = cG.GSGAM2[p];
     P[0][p] = P[0][p] + 0.0;
     P[1][p] = P[1][p] + a.dt * fvx * rho * gs;
@@ -80,20 +94,21 @@ __global__ void k_forcing_hs(HsArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// DCMIP forcing with Kessler warm-rain microphysics only (AF_TYPE 'DCMIP',
-// USE_Kessler: nhm/forcing/mod_forcing.py:207-321 forcing_step ->
-// mod_af_dcmip.py:129-230 AF_dcmip, Kessler branch -> kessler.py:9-179).
-// One thread per regional column (every column of the tile, as the
-// reference forces all of them before the exchange): the diagnostics with the
-// water tracers vapour, cloud, rain (0, 1, 2), dry mixing ratios, dry
-// density, Exner function and potential temperature on kmin..kmax, the
-// microphysics with its per-column sedimentation sub-cycles, the water and
-// energy tendencies (the energy one from increments), applied as
-// PROG + dt * f * rho * GSGAM2 on every level (f zero outside kmin..kmax;
-// the water tendencies also added to RHOG), and the column's precipitation
-// rate.  Same association order as the reference; exp, pow and sqrt are
-// CUDA's (sqrt correctly rounded, exp and pow within their documented ulp
-// bounds), so results can differ from numpy's in the last bits.
+// DCMIP forcing (AF_TYPE 'DCMIP': nhm/forcing/mod_forcing.py:207-321
+// forcing_step -> mod_af_dcmip.py:129-317 AF_dcmip): Kessler warm-rain
+// microphysics (kessler.py:9-179), the simple physics (simple_physics.py) and
+// the terminator toy chemistry, each optional, all from the same state, with
+// the Held-Suarez relaxation on top for the moist Held-Suarez case (its
+// momentum tendency replaces the others', its energy tendency adds).  One
+// thread per regional column (every column of the tile, as the reference
+// forces all of them before the exchange): the diagnostics with the water
+// tracers vapour, cloud, rain (0, 1, 2), the schemes, the water, momentum and
+// energy tendencies (the energy ones from increments), applied as
+// PROG + dt * f * rho * GSGAM2 on every level (f zero outside kmin..kmax; the
+// water tendencies also added to RHOG), and the column's precipitation rate.
+// Same association order as the reference; exp, log, pow, sin, cos are
+// CUDA's (sqrt correctly rounded), so results can differ from numpy's in the
+// last bits.
 // ---------------------------------------------------------------------------
 #define NC_KESS_K 64
 struct DcmipArgs {
@@ -114,6 +129,11 @@ struct DcmipArgs {
   // the column unit vectors IX, IY, IZ, JX, JY, JZ [6][l][j][i]
   int sm, sm_lsc;
   const double *zh, *zsfc, *tsurf, *ij;
+  double sm_C;                    // the heat / moisture exchange coefficient (x4 for moist Held-Suarez)
+  // moist Held-Suarez (optional): |sin lat|^2, |cos lat|^2, |cos lat|^4 planes
+  int hs;
+  const double* hs_lat3;
+  HsParams hp;
 };
 
 // numpy's sum of a contiguous row (pairwise: eight running partial sums
@@ -136,17 +156,18 @@ __device__ __forceinline__ double np_rowsum(const double* x, int n) {
 }
 
 // DCMIP simple physics (nhm/forcing/simple_physics.py:310-366, the DCMIP2016
-// v6 scheme with the RJ2012 boundary layer, no Held-Suarez) on one column of
+// v6 scheme with the RJ2012 boundary layer; Cv the exchange coefficient of
+// heat and moisture, 0.0011, four times that for moist Held-Suarez) on one column of
 // nz levels ordered top to bottom: t, q, u, v updated in place; pm the full-
 // level pressure, pint the nz + 1 interface pressures (pint[nz] = ps);
 // CE..CFq work arrays of nz.  Returns the large-scale condensation's
 // precipitation rate (0 without lsc).  log, exp, pow are CUDA's.
 __device__ double simple_physics_col(int nz, double* t, double* q, double* u, double* v, const double* pm,
-                                     const double* pint, double ps, double tsurf, double dt, int lsc, double* CE,
-                                     double* CEm, double* CFu, double* CFv, double* CFt, double* CFq) {
+                                     const double* pint, double ps, double tsurf, double dt, int lsc, double Cv,
+                                     double* CE, double* CEm, double* CFu, double* CFv, double* CFt, double* CFq) {
   const double rair = 287.0, rh2o = 461.5, grav = 9.80616, cpair = 1.0045e3, latvap = 2.5e6;
   const double epsilo = rair / rh2o, zvir = (rh2o / rair) - 1.0;
-  const double Cv = 0.0011, T0 = 273.16, e0 = 610.78, rhow = 1000.0;
+  const double T0 = 273.16, e0 = 610.78, rhow = 1000.0;
   const double Cd0 = 0.0007, Cd1 = 0.000065, Cm = 0.002, v20 = 20.0;
   const double p0 = 100000.0, pbltop = 85000.0, pblconst2 = 10000.0 * 10000.0;
   const int b = nz - 1;
@@ -396,8 +417,19 @@ __global__ void k_forcing_dcmip(DcmipArgs a) {
     }
     pint[0] = 0.0;
     pint[nz] = ps;
-    prec = prec + simple_physics_col(nz, st, sq, su, sv, pm, pint, ps, a.tsurf[cidx], dt, a.sm_lsc, w1, w2, w3, w4,
-                                     w5, w6);
+    prec = prec + simple_physics_col(nz, st, sq, su, sv, pm, pint, ps, a.tsurf[cidx], dt, a.sm_lsc, a.sm_C, w1, w2,
+                                     w3, w4, w5, w6);
+  }
+  double hs_psref = 0.0, sin2 = 0.0, cos2 = 0.0, cos4 = 0.0;
+  if (a.hs) {   // moist Held-Suarez: the reference surface pressure of the column
+    double rho, pre, tem, ein, q[3];
+    diag(kmin, rho, pre, tem, ein, q);
+    const double pre_kmin = pre;
+    diag(kmin - 1, rho, pre, tem, ein, q);
+    hs_psref = 0.5 * (pre_kmin + pre);
+    sin2 = a.hs_lat3[cidx];
+    cos2 = a.hs_lat3[npl + cidx];
+    cos4 = a.hs_lat3[2 * npl + cidx];
   }
   a.precip[cidx] = prec;
   // back to wet mixing ratios, the tendencies, and their application on every level
@@ -448,6 +480,13 @@ __global__ void k_forcing_dcmip(DcmipArgs a) {
       const double dtem = st[cc] - tem;
       const double dcv = cv - cv_old;
       fe = fe + (cv_old * dtem + tem * dcv + dcv * dtem) / dt;
+    }
+    if (k >= kmin && k <= kmax && a.hs) {   // mod_forcing.py:278-287: HS momentum replaces, HS energy adds
+      const double RHOG = P[0][p];
+      double hfe;
+      hs_tendency(a.hp, sin2, cos2, cos4, hs_psref, pre, tem, P[1][p] / RHOG, P[2][p] / RHOG, P[3][p] / RHOG, fv[0],
+                  fv[1], fv[2], hfe);
+      fe = fe + hfe;
     }
     const double gs = cG.GSGAM2[p];
     P[1][p] = P[1][p] + dt * fv[0] * rho * gs;

@@ -199,15 +199,24 @@ HIST_CONSTS = ("LHV", "UNDEF", "PSAT0", "RTEM00", "CPovR_liq", "CPovR_ice", "Lov
 HIST_TRACERS = ("I_QV", "I_QC", "I_QR", "I_QI", "I_QS", "I_QG")
 
 
-def dcmip_sst(lat, latdepend: bool):
+def dcmip_sst(lat, latdepend: bool, held_suarez: bool = False, mitc_type: int = 1):
     """the sea-surface temperature of the DCMIP simple physics per column
-    (nhm/forcing/simple_physics.py:152-197 _sst_tsurf, no Held-Suarez): the
-    moist baroclinic wave's latitude profile, or 302.15 K everywhere; the
+    (nhm/forcing/simple_physics.py:152-197 _sst_tsurf): for moist Held-Suarez
+    the Gaussian-in-latitude profile of MITC type 1, 2 or 3, else the moist
+    baroclinic wave's latitude profile, or 302.15 K everywhere; the
     reference's numpy expressions, so the device reads the reference's values"""
     import math
+    pi = math.pi
+    if held_suarez:
+        if mitc_type == 1:
+            return 29.0 * np.exp(-0.5 * lat * lat / (26.0 / 180.0 * pi) ** 2) + 271.0
+        if mitc_type in (2, 3):
+            amp, w, c0 = (29.0, 20.0, 17.0) if mitc_type == 2 else (32.0, 23.0, 12.0)
+            dphi2, dphi0 = (w / 180.0 * pi) ** 2, (c0 / 180.0 * pi)
+            return amp * np.exp(-0.5 * np.maximum(np.abs(lat) - dphi0, 0.0) ** 2 / dphi2) + 271.0
+        raise ValueError(f"MITC_TYPE out of range: {mitc_type}")
     if not latdepend:
         return np.full_like(lat, 302.15)
-    pi = math.pi
     T00, u0, a, omega, q0, eta0, rair, rh2o = 288.0, 35.0, 6371220.0, 7.29212e-5, 0.021, 0.252, 287.0, 461.5
     zvir = (rh2o / rair) - 1.0
     etav, latw = (1.0 - eta0) * 0.5 * pi, 2.0 * pi / 9.0
@@ -282,16 +291,23 @@ def setup_table(geo: dict) -> dict:
         for k in ("AF_negative_fixer", "AF_update_tot_dens"):
             if k in geo:
                 t[k] = np.asarray(float(_scalar(geo[k])), np.float64)
-        if "AF_dcmip_schemes" in geo:   # [Kessler, simple physics, latitude-dependent SST, condensation]
-            kes, sm, latdep, lsc = (int(x) for x in np.asarray(geo["AF_dcmip_schemes"]).reshape(4))
-            t["AF_dcmip_schemes"] = np.asarray([kes, sm, lsc], np.int64)
+        if "AF_dcmip_schemes" in geo:
+            # [Kessler, simple physics, latitude-dependent SST, condensation(, moist Held-Suarez, MITC SST type)]
+            fl = [int(x) for x in np.asarray(geo["AF_dcmip_schemes"]).reshape(-1)]
+            kes, sm, latdep, lsc = fl[:4]
+            hs, mitc = (fl[4], fl[5]) if len(fl) >= 6 else (0, 1)
+            t["AF_dcmip_schemes"] = np.asarray([kes, sm, lsc] + ([hs] if hs else []), np.int64)
+            G, L = int(_scalar(geo["gall_1d"])), int(_scalar(geo["lall"]))
+            if sm or hs:
+                lat = np.asarray(geo["AF_dcmip_lat"], np.float64).reshape(G, G, 1, L)
             if sm:
-                G, L = int(_scalar(geo["gall_1d"])), int(_scalar(geo["lall"]))
                 t["AF_dcmip_zh"] = np.ascontiguousarray(geo["AF_dcmip_zh"], np.float64)
                 t["AF_dcmip_zsfc"] = np.ascontiguousarray(np.asarray(geo["AF_dcmip_zsfc"], np.float64).reshape(G, G, 1, L))
                 t["AF_dcmip_ij"] = np.ascontiguousarray(np.asarray(geo["AF_dcmip_ij"], np.float64).reshape(G, G, 1, L, 6))
-                lat = np.asarray(geo["AF_dcmip_lat"], np.float64).reshape(G, G, 1, L)
-                t["AF_dcmip_tsurf"] = np.ascontiguousarray(dcmip_sst(lat, bool(latdep)))
+                t["AF_dcmip_tsurf"] = np.ascontiguousarray(dcmip_sst(lat, bool(latdep), bool(hs), mitc))
+            if hs:   # the Held-Suarez latitude terms, as for AF_TYPE 'HELD-SUAREZ'
+                sinlat, coslat = np.abs(np.sin(lat)), np.abs(np.cos(lat))
+                t["AF_dcmip_hs_lat_terms"] = np.ascontiguousarray(np.stack([sinlat ** 2, coslat ** 2, coslat ** 4], -1))
         if "AF_dcmip_chem" in geo:   # terminator toy chemistry: (Cl, Cl2) tracer indices, column lat / lon
             G, L = int(_scalar(geo["gall_1d"])), int(_scalar(geo["lall"]))
             t["AF_dcmip_chem"] = np.ascontiguousarray(np.asarray(geo["AF_dcmip_chem"]).reshape(2), np.int64)

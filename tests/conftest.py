@@ -104,6 +104,15 @@ def golden_dcmip11():
 
 
 @pytest.fixture(scope="session")
+def golden_dcmip21():
+    """the DCMIP2016 case 2-1 scheme set (moist Held-Suarez: Kessler, the
+    simple physics with the Held-Suarez SST and exchange coefficient, the
+    Held-Suarez relaxation on top) run by the reference
+    (make_kessler.py --case dcmip21)"""
+    return _dcmip_fixture("dcmip21")
+
+
+@pytest.fixture(scope="session")
 def golden_smlsc():
     """the simple physics alone with its large-scale condensation and the
     constant sea-surface temperature, run by the reference
@@ -117,7 +126,7 @@ def dcmip_oracle_args(geo):
     chem = (geo["GRD_LAT"], geo["GRD_LON"], int(geo["NCHEM_STR"]), int(geo["NCHEM_END"])) \
         if "NCHEM_STR" in geo else None
     sm = dict(zh=geo["GRD_ZH"], zsfc=geo["GRD_zsfc"], lat=geo["GRD_LAT"], ij=geo["GMTR_p_IJ"],
-              latdepend=bool(fl[2]), lsc=bool(fl[3])) if fl[1] else None
+              latdepend=bool(fl[2]), lsc=bool(fl[3]), held_suarez=bool(fl[4]), mitc=fl[5]) if fl[1] else None
     return dict(chem=chem, kessler_on=bool(fl[0]), sm=sm)
 
 

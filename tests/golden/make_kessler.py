@@ -16,7 +16,8 @@ chemistry reads are stored too.  --case dcmip11 adds the DCMIP simple physics
 (USE_SimpleMicrophys with the latitude-dependent sea-surface temperature, no
 large-scale condensation: the scheme set of DCMIP2016 case 1-1) to Kessler
 and the chemistry; --case smlsc runs the simple physics alone with its
-large-scale condensation and the constant sea-surface temperature.  Both
+large-scale condensation and the constant sea-surface temperature; --case dcmip21 the moist
+Held-Suarez scheme set of DCMIP2016 case 2-1.  They
 also store the half-level heights, the surface height and the column unit
 vectors the simple physics reads.
 
@@ -48,6 +49,9 @@ CASES = {
                  "SM_LargeScaleCond": False}, True),
     "smlsc": ({"USE_Kessler": False, "USE_SimpleMicrophys": True, "SM_Latdepend_SST": False,
                "SM_LargeScaleCond": True}, False),
+    # DCMIP2016 case 2-1, moist Held-Suarez (the SET_DCMIP2016_21 scheme set)
+    "dcmip21": ({"USE_Kessler": True, "USE_SimpleMicrophys": True, "SM_Latdepend_SST": False,
+                 "SM_LargeScaleCond": False, "USE_HeldSuarez": True}, False),
 }
 
 
@@ -100,7 +104,7 @@ def run(ref: str, out_dir: str, case: str = "kessler"):
         assert m.rcnf.AF_TYPE == "DCMIP" and afdcmip.USE_SimpleMicrophys == sm
         for k, v in flags.items():
             assert getattr(afdcmip, k) == v, k
-        assert afdcmip.USE_ToyChemistry == chem and not afdcmip.USE_HeldSuarez and not afdcmip.SM_PBL_Bryan
+        assert afdcmip.USE_ToyChemistry == chem and not afdcmip.SM_PBL_Bryan and afdcmip.SM_MITC_SST_TYPE == 1
         assert m.rcnf.NQW_END == 2 and (m.rcnf.I_QV, m.rcnf.I_QC, m.rcnf.I_QR) == (0, 1, 2)
         assert not m.frc.NEGATIVE_FIXER and m.frc.UPDATE_TOT_DENS
         pv, pvp = m.prgv.PRG_var, m.prgv.PRG_var_pl
@@ -139,7 +143,8 @@ def run(ref: str, out_dir: str, case: str = "kessler"):
             out["geo.GRD_ZH"] = np.ascontiguousarray(m.grd.GRD_vz[:, :, :, :, m.grd.GRD_ZH])
             out["geo.GRD_zsfc"] = np.ascontiguousarray(m.grd.GRD_zs[:, :, K0, :, m.grd.GRD_ZSFC])
         out["geo.dcmip_flags"] = np.asarray([int(afdcmip.USE_Kessler), int(afdcmip.USE_SimpleMicrophys),
-                                             int(afdcmip.SM_Latdepend_SST), int(afdcmip.SM_LargeScaleCond)])
+                                             int(afdcmip.SM_Latdepend_SST), int(afdcmip.SM_LargeScaleCond),
+                                             int(afdcmip.USE_HeldSuarez), int(afdcmip.SM_MITC_SST_TYPE)])
         out["geo.GRD_Z"] = np.ascontiguousarray(m.grd.GRD_vz[:, :, :, :, m.grd.GRD_Z])
         out["geo.PRE00"] = np.asarray(m.cnst.CONST_PRE00)
         out["state0"], out["state0_pl"] = pv.copy(), pvp.copy()

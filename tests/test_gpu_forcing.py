@@ -152,11 +152,12 @@ def test_terminator_chemistry_setup_is_checked(pkg, golden_kessler_chem):
             pkg.NicamCuda(g, graph=False).close()
 
 
-@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_smlsc"])
+@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_smlsc", "golden_dcmip21"])
 def test_simple_physics_vs_reference(pkg, case, request):
     """DCMIP forcing with the simple physics on the device against the
     reference's two steps (with Kessler and the chemistry as in DCMIP2016 case
-    1-1; alone with the large-scale condensation): log, exp, pow, sin and cos
+    1-1; alone with the large-scale condensation; moist Held-Suarez as in case
+    2-1): log, exp, pow, sin and cos
     are CUDA's, so relative L2 <= 1e-12 per prognostic and for the
     precipitation, 1e-11 for Cl / Cl2"""
     from conftest import dcmip_device_setup

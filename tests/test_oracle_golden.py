@@ -95,7 +95,7 @@ def test_oracle_terminator_chemistry_matches_reference(golden_kessler_chem):
         assert np.array_equal(precip, pr[f"precip{n}"]), n
 
 
-@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_smlsc"])
+@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_smlsc", "golden_dcmip21"])
 def test_oracle_simple_physics_matches_reference(case, request):
     """dynamics step + DCMIP forcing with the simple physics (with Kessler and
     the chemistry as in DCMIP2016 case 1-1; alone with the large-scale
@@ -111,6 +111,15 @@ def test_oracle_simple_physics_matches_reference(case, request):
         s, sp, precip = O.forcing_step_kessler(G, s, sp, geo["GRD_Z"], **kw)
         assert np.array_equal(s, st[f"state{n}"]) and np.array_equal(sp, st[f"state{n}_pl"]), n
         assert np.array_equal(precip, pr[f"precip{n}"]), n
+
+
+def test_moist_held_suarez_fixture_is_active(golden_kessler, golden_dcmip21):
+    """the Held-Suarez relaxation replaced the momentum tendency: the moist
+    Held-Suarez run moved the momentum away from the Kessler-only run"""
+    _, a, _ = golden_kessler
+    _, b, _ = golden_dcmip21
+    assert np.array_equal(a["state0"], b["state0"])
+    assert np.abs(a["state1"][..., 1] - b["state1"][..., 1]).max() > 0.1
 
 
 def test_simple_physics_fixtures_are_active(golden_kessler_chem, golden_dcmip11, golden_smlsc):
@@ -132,6 +141,8 @@ def test_sst_of_the_device_setup_equals_the_oracle(pkg, golden_dcmip11):
     lat = geo["GRD_LAT"]
     for latdep in (True, False):
         assert np.array_equal(pkg.runtime.dcmip_sst(lat, latdep), O.dcmip_sst(lat, latdep))
+    for mitc in (1, 2, 3):
+        assert np.array_equal(pkg.runtime.dcmip_sst(lat, False, True, mitc), O.dcmip_sst(lat, False, True, mitc))
 
 
 def test_terminator_fixture_is_active(golden_kessler_chem):
