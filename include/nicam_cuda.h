@@ -259,7 +259,7 @@ int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* g
  * the Cl / Cl2 tendencies (per dry air, analytic over dt; sin, cos, exp and
  * sqrt are CUDA's) join the tracer tendencies on kmin..kmax.  The optional
  * "AF_dcmip_schemes" (int64 [Kessler, simple physics, large-scale
- * condensation], default [1, 0, 0]) adds the DCMIP simple physics
+ * condensation(, moist Held-Suarez)], default [1, 0, 0]) adds the DCMIP simple physics
  * (USE_SimpleMicrophys, nhm/forcing/simple_physics.py with the RJ2012
  * boundary layer; mod_af_dcmip.py:230-317) or runs it alone: its surface
  * fluxes, implicit boundary-layer diffusion of u, v, potential temperature
@@ -268,7 +268,13 @@ int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* g
  * added to Kessler's.  It reads "AF_dcmip_zh" (GRD_vz[..., GRD_ZH], (gall_1d,
  * gall_1d, kall, lall)), "AF_dcmip_zsfc" (GRD_zs at K0), "AF_dcmip_tsurf" (the
  * sea-surface temperature per column) and "AF_dcmip_ij" (GMTR_p IX, IY, IZ,
- * JX, JY, JZ at K0), all (gall_1d, gall_1d, 1, lall[, 6]). */
+ * JX, JY, JZ at K0), all (gall_1d, gall_1d, 1, lall[, 6]).  The fourth
+ * switch (DCMIP2016 case 2-1, moist Held-Suarez) applies the Held-Suarez
+ * relaxation with the moist equilibrium profile (T_eq0 294 K, DT_y 65 K) on
+ * top: its momentum tendency replaces the others', its energy tendency adds
+ * (mod_forcing.py:278-287); it reads "AF_dcmip_hs_lat_terms" (as
+ * "AF_hs_lat_terms"), and the simple physics then takes the Held-Suarez
+ * sea-surface temperature and four times the exchange coefficient. */
 int nc_forcing_step(nc_handle* h);
 
 /* The precipitation rate [m/s] of the last DCMIP Kessler forcing step per
