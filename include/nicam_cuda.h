@@ -318,8 +318,9 @@ int nc_restart_finish(nc_handle* h, const int64_t* pole_src, int32_t nsrc);
  *   21 ml_th_prime                      -> (gall_1d, gall_1d, kall, lall)
  *   22 sl_ps, 23 sl_pw, 24 sl_lwp, 25 sl_iwp, 26 sl_u850, 27 sl_v850,
  *   28 sl_w850, 29 sl_t850, then ids 30-41 the same four at 500, 250 and
- *   100 hPa                             -> (gall_1d, gall_1d, lall)
- * (the reference's I/O order, share/mod_io.py:251-260).  The tendencies ml_d*
+ *   100 hPa, 42 sl_cl, 43 sl_cl2, 44 sl_cly (the terminator chemistry's
+ *   column means; AF_TYPE 'DCMIP' only)   -> (gall_1d, gall_1d, lall)
+ * (the reference's I/O order, share/mod_io.py:251-261).  The tendencies ml_d*
  * are stateful as in the reference: the first output of each is zero, later
  * ones (previous - current) * 86400 / dt / (nstep - nstep of the last output
  * that formed tendencies), dq in g/kg/day; nstep is the model step count
@@ -331,7 +332,8 @@ int nc_restart_finish(nc_handle* h, const int64_t* pole_src, int32_t nsrc);
  * (gall_1d, gall_1d, 1, lall, 6)), HIST_dgz (kall), HIST_consts (LHV, UNDEF,
  * PSAT0, RTEM00, CPovR_liq, CPovR_ice, LovR_liq, LovR_ice, SATURATION_LLIMIT_TEMP,
  * SATURATION_ULIMIT_TEMP) and HIST_tracers (int64 I_QV, I_QC, I_QR, I_QI, I_QS,
- * I_QG, -1 where absent), with PRE00; otherwise NC_ERR_STATE.  Synchronous. */
+ * I_QG, -1 where absent), with PRE00; otherwise NC_ERR_STATE.  Ids 42-44 also
+ * need HIST_chem (int64 NCHEM_STR, NCHEM_END), else NC_ERR_ARG.  Synchronous. */
 int nc_history_vars(nc_handle* h, const int32_t* items, int32_t nitems, int64_t nstep, double dt,
                     double* const* out);
 

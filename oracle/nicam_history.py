@@ -97,7 +97,7 @@ class History:
         ntrc = q.shape[-1]
         qv = q[..., iqv] if ntrc > 0 else None
         need_slices = want is None or bool(want & set(SL[4:]))
-        need_paths = W('sl_pw', 'sl_lwp', 'sl_iwp')
+        need_paths = W('sl_pw', 'sl_lwp', 'sl_iwp', 'sl_cl', 'sl_cl2', 'sl_cly')
         need_tend = dt is not None and W(*TEND)
         res = {'ml_rho': rho, 'ml_tem': tem, 'ml_pres': pre}
         hgt = np.asarray(hg["GRD_Z"])
@@ -180,6 +180,14 @@ class History:
                 res['sl_lwp'] = colint(sum_tracers((int(sc("I_QC")), int(sc("I_QR")))))
             if W('sl_iwp'):
                 res['sl_iwp'] = colint(sum_tracers((int(sc("I_QI")), int(sc("I_QS")), int(sc("I_QG")))))
+            # the terminator chemistry's column means (mod_history_vars.py:149-156), with
+            # hg["NCHEM"] = (NCHEM_STR, NCHEM_END) for AF_TYPE 'DCMIP' with the chemistry
+            if "NCHEM" in hg and W('sl_cl', 'sl_cl2', 'sl_cly'):
+                ns, ne = (int(x) for x in np.asarray(hg["NCHEM"]))
+                rhodz = colint(np.ones_like(tem))
+                res['sl_cl'] = colint(q[..., ns]) / rhodz
+                res['sl_cl2'] = colint(q[..., ne]) / rhodz
+                res['sl_cly'] = colint(q[..., ns] + 2.0 * q[..., ne]) / rhodz
         if need_tend:
             dday = 86400.0 / dt
             prev_n = self.tend_nstep

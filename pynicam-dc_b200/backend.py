@@ -30,7 +30,7 @@ from __future__ import annotations
 import numpy as np
 
 from . import restart
-from .runtime import HIST_ITEMS, NicamCuda
+from .runtime import HIST_CHEM, HIST_ITEMS, NicamCuda
 
 
 def _dcmip_flags(msc) -> dict:
@@ -195,6 +195,8 @@ def _history_setup(m) -> dict:
              "hist_I_QV": r.I_QV}
         for k in ("I_QC", "I_QR", "I_QI", "I_QS", "I_QG"):
             h["hist_" + k] = getattr(r, k, -1)
+        if getattr(r, "AF_TYPE", "") == "DCMIP" and getattr(r, "NCHEM_STR", -1) >= 0:   # mod_io.py:259-261
+            h["hist_NCHEM"] = np.asarray([r.NCHEM_STR, r.NCHEM_END], np.int64)
     except AttributeError:
         return {}
     return h
@@ -216,6 +218,7 @@ class CudaDyn:
         self._forced = ("GRD_LAT" in geo and str(np.asarray(geo.get("integ_type", "RK3"))) != "TRCADV") or \
             bool(int(np.asarray(geo.get("AF_dcmip_kessler", 0))))
         self._kessler = bool(int(np.asarray(geo.get("AF_dcmip_kessler", 0))))
+        self._hist_chem = "hist_NCHEM" in geo
         self._host_stale = False
         self._device_valid = False
 
@@ -298,7 +301,11 @@ class CudaDyn:
                 active |= set(getattr(io, "_diag_names", []))
             if write_2d:
                 active |= set(getattr(io, "_diag_names_2d", []))
-        names = HIST_ITEMS if active is None else tuple(n for n in HIST_ITEMS if n in active)
+        every = HIST_ITEMS if self._hist_chem else tuple(n for n in HIST_ITEMS if n not in HIST_CHEM)
+        names = every if active is None else tuple(n for n in every if n in active)
+        if active is not None and active & set(HIST_CHEM) and not self._hist_chem:
+            raise NotImplementedError("cuda backend: the chemistry's history columns need AF_TYPE 'DCMIP' "
+                                      "with the terminator chemistry")
         if active is not None and active - set(HIST_ITEMS):
             raise NotImplementedError(f"cuda backend: history diagnostics {sorted(active - set(HIST_ITEMS))} "
                                       "are not built on the device")

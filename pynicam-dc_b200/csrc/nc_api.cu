@@ -382,6 +382,7 @@ struct nc_handle {
   const double *hist_IJ = nullptr, *hist_dgz = nullptr;
   double hist_c[10] = {};
   int hist_trc[6] = {-1, -1, -1, -1, -1, -1};   // I_QV, I_QC, I_QR, I_QI, I_QS, I_QG
+  int hist_chem[2] = {-1, -1};                   // NCHEM_STR, NCHEM_END (the chemistry's columns)
   double* hist_out[H_N] = {};                    // device outputs, allocated on first request
   double* hist_old[5] = {};                      // previous outputs of the tendency fields
   bool hist_old_set[5] = {};
@@ -1827,6 +1828,14 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
       if (v < -1 || v >= D.nq) return fail(NC_ERR_ARG, "HIST_tracers: index outside the tracers");
       h->hist_trc[n] = (int)v;
     }
+    if (const nc_array* ch = T.get("HIST_chem")) {   // AF_TYPE 'DCMIP' with the terminator chemistry
+      if (ch->dtype != NC_I64 || numel(ch) != 2) return fail(NC_ERR_ARG, "HIST_chem: two int64 tracer indices");
+      for (int n = 0; n < 2; ++n) {
+        const int64_t v = ((const int64_t*)ch->data)[n];
+        if (v < 0 || v >= D.nq) return fail(NC_ERR_ARG, "HIST_chem: index outside the tracers");
+        h->hist_chem[n] = (int)v;
+      }
+    }
     TRY(dev_alloc(h, &h->hist_thmean, (size_t)D.KA));
     h->hist = true;
   }
@@ -2537,6 +2546,8 @@ int nc_history_vars(nc_handle* h, const int32_t* items, int32_t nitems, int64_t 
     if (items[n] < 0 || items[n] >= H_N) return fail(NC_ERR_ARG, "nc_history_vars: item id out of range");
     if (want[items[n]]) return fail(NC_ERR_ARG, "nc_history_vars: item requested twice");
     if (!out[n]) return fail(NC_ERR_ARG, "nc_history_vars: null output pointer");
+    if (items[n] >= H_CL && h->hist_chem[0] < 0)
+      return fail(NC_ERR_ARG, "nc_history_vars: the chemistry's columns need the HIST_chem setup entry");
     want[items[n]] = true;
   }
   TRY(load_consts(h));
@@ -2548,6 +2559,7 @@ int nc_history_vars(nc_handle* h, const int32_t* items, int32_t nitems, int64_t 
   a.iqv = h->hist_trc[0];
   a.iql[0] = h->hist_trc[1]; a.iql[1] = h->hist_trc[2];
   a.iqs[0] = h->hist_trc[3]; a.iqs[1] = h->hist_trc[4]; a.iqs[2] = h->hist_trc[5];
+  a.icl = h->hist_chem[0]; a.icl2 = h->hist_chem[1];
   a.wdiag = h->w.r;
   a.hgt = h->hist_hgt; a.coslat = h->hist_coslat; a.zsfc = h->hist_zsfc; a.IJ = h->hist_IJ;
   a.dgz = h->hist_dgz;

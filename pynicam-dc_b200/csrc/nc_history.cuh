@@ -21,7 +21,9 @@ enum HistItem {
   H_DU, H_DV, H_DW, H_DTEM, H_DQ, H_UCOS, H_VCOS, H_TH_PRIME,
   H_PS, H_PW, H_LWP, H_IWP,
   H_SL0,                 // then for 850, 500, 250, 100 hPa: u, v, w, t
-  H_N = H_SL0 + 16
+  H_CL = H_SL0 + 16,     // the terminator chemistry's column means (AF_TYPE 'DCMIP' only): Cl, Cl2, Cly
+  H_CL2, H_CLY,
+  H_N
 };
 constexpr int H_N3 = H_PS;   // ids below are (i, j, k, l) fields, the rest (i, j, l)
 
@@ -30,6 +32,7 @@ struct HistArgs {
   const double* Pq[NC_MAXNQ];
   int iqv;                  // water-vapour tracer (-1: none)
   int iql[2], iqs[3];       // liquid (QC, QR) and solid (QI, QS, QG) tracers (-1: absent)
+  int icl, icl2;            // the chemistry's Cl and Cl2 tracers (-1: none)
   const double* wdiag;      // diagnostic w of the last step [l][k][j][i]
   const double *hgt, *coslat, *zsfc, *IJ;   // GRD_Z [l][k][j][i]; planes [l][j][i]; IJ [6][l][j][i]
   const double* dgz;        // GRD_dgz (kall)
@@ -112,7 +115,7 @@ __global__ void __launch_bounds__(128) k_history(HistArgs a) {
   const double IX = a.IJ[c2], IY = a.IJ[np2 + c2], IZ = a.IJ[2 * np2 + c2];
   const double JX = a.IJ[3 * np2 + c2], JY = a.IJ[4 * np2 + c2], JZ = a.IJ[5 * np2 + c2];
   const double cosl = a.coslat ? a.coslat[c2] : 1.0;
-  double pw = 0.0, lwp = 0.0, iwp = 0.0;
+  double pw = 0.0, lwp = 0.0, iwp = 0.0, rdz = 0.0, ccl = 0.0, ccl2 = 0.0, ccly = 0.0;
   double pre_col[NC_MAXK];
   for (int k = 0; k < KA; ++k) {
     const int p = q0 + k * ks;
@@ -172,12 +175,24 @@ __global__ void __launch_bounds__(128) k_history(HistArgs a) {
       pw = (k == kmin) ? xv : pw + xv;
       lwp = (k == kmin) ? xl : lwp + xl;
       iwp = (k == kmin) ? xs : iwp + xs;
+      if (a.icl >= 0) {   // mod_history_vars.py:149-156
+        const double q1 = a.Pq[a.icl][p] / RHOG, q2 = a.Pq[a.icl2][p] / RHOG;
+        const double xo = d.rho * 1.0 * wcol, x1 = d.rho * q1 * wcol, x2 = d.rho * q2 * wcol;
+        const double x3 = d.rho * (q1 + 2.0 * q2) * wcol;
+        rdz = (k == kmin) ? xo : rdz + xo;
+        ccl = (k == kmin) ? x1 : ccl + x1;
+        ccl2 = (k == kmin) ? x2 : ccl2 + x2;
+        ccly = (k == kmin) ? x3 : ccly + x3;
+      }
     }
     if (k == kmin && a.out[H_PS]) a.out[H_PS][c2] = d.pre + d.rho * GRAV * (hgt - a.zsfc[c2]);
   }
   if (a.out[H_PW]) a.out[H_PW][c2] = pw;
   if (a.out[H_LWP]) a.out[H_LWP][c2] = lwp;
   if (a.out[H_IWP]) a.out[H_IWP][c2] = iwp;
+  if (a.out[H_CL]) a.out[H_CL][c2] = ccl / rdz;
+  if (a.out[H_CL2]) a.out[H_CL2][c2] = ccl2 / rdz;
+  if (a.out[H_CLY]) a.out[H_CLY][c2] = ccly / rdz;
   // pressure-level slices, log-p linear between the bracketing levels
   // (mod_history_vars.py:188-209)
   const double plevs[4] = {850.0e2, 500.0e2, 250.0e2, 100.0e2};

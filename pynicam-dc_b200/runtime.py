@@ -192,7 +192,9 @@ def _scalar(a):
 HIST_ITEMS = ('ml_u', 'ml_v', 'ml_w', 'ml_th', 'ml_thv', 'ml_omg', 'ml_pres', 'ml_tem', 'ml_rho', 'ml_hgt',
               'ml_mse', 'ml_rh', 'ml_rha', 'ml_rhi', 'ml_du', 'ml_dv', 'ml_dw', 'ml_dtem', 'ml_dq', 'ml_ucos',
               'ml_vcos', 'ml_th_prime', 'sl_ps', 'sl_pw', 'sl_lwp', 'sl_iwp') + tuple(
-    f'sl_{f}{lev}' for lev in ('850', '500', '250', '100') for f in ('u', 'v', 'w', 't'))
+    f'sl_{f}{lev}' for lev in ('850', '500', '250', '100') for f in ('u', 'v', 'w', 't')) + (
+    'sl_cl', 'sl_cl2', 'sl_cly')
+HIST_CHEM = ('sl_cl', 'sl_cl2', 'sl_cly')   # AF_TYPE 'DCMIP' with the terminator chemistry only
 HIST_N3 = 22
 HIST_CONSTS = ("LHV", "UNDEF", "PSAT0", "RTEM00", "CPovR_liq", "CPovR_ice", "LovR_liq", "LovR_ice", "SAT_LLIMIT",
                "SAT_ULIMIT")
@@ -324,6 +326,8 @@ def setup_table(geo: dict) -> dict:
         t["HIST_dgz"] = np.ascontiguousarray(geo["hist_dgz"], np.float64)
         t["HIST_consts"] = np.ascontiguousarray([float(_scalar(geo["hist_" + k])) for k in HIST_CONSTS], np.float64)
         t["HIST_tracers"] = np.ascontiguousarray([int(_scalar(geo["hist_" + k])) for k in HIST_TRACERS], np.int64)
+        if "hist_NCHEM" in geo:   # the terminator chemistry's tracers (NCHEM_STR, NCHEM_END)
+            t["HIST_chem"] = np.ascontiguousarray(np.asarray(geo["hist_NCHEM"]).reshape(2), np.int64)
         t["PRE00"] = np.asarray(float(_scalar(geo["PRE00"])), np.float64)
     t["pntmask"] = np.ascontiguousarray(geo["pntmask"], np.int32)
     t["have_sgp"] = np.ascontiguousarray(geo["have_sgp"], np.bool_)

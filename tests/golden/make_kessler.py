@@ -12,7 +12,9 @@ carries the two chemistry tracers Cl and Cl2 (CHEM_TYPE PASSIVE,
 CHEM_TRC_vmax 2) with the DCMIP terminator toy chemistry on
 (USE_ToyChemistry), started at half and one and a half times the reaction's
 equilibrium so that it acts, and the column latitudes and longitudes the
-chemistry reads are stored too.  --case dcmip11 adds the DCMIP simple physics
+chemistry reads are stored too, with the reference's history columns of the
+chemistry (sl_cl, sl_cl2, sl_cly) of the last state and the set-up arrays the
+history diagnostics read (hgeo.*).  --case dcmip11 adds the DCMIP simple physics
 (USE_SimpleMicrophys with the latitude-dependent sea-surface temperature, no
 large-scale condensation: the scheme set of DCMIP2016 case 1-1) to Kessler
 and the chemistry; --case smlsc runs the simple physics alone with its
@@ -152,6 +154,25 @@ def run(ref: str, out_dir: str, case: str = "kessler"):
             nic.run(1)
             out[f"state{s + 1}"], out[f"state{s + 1}_pl"] = m.prgv.PRG_var.copy(), m.prgv.PRG_var_pl.copy()
             out[f"precip{s + 1}"] = np.asarray(m.frc.precip).copy()
+        if chem:   # the chemistry's history columns of the last state and what the diagnostics read
+            m.io._diag_names, m.io._diag_names_2d = [], ["sl_cl", "sl_cl2", "sl_cly"]
+            h = m.dyn.history_vars_step(m)
+            assert sorted(h) == ["sl_cl", "sl_cl2", "sl_cly"]
+            for k, v in h.items():
+                out["hist." + k] = np.asarray(v)
+            g, gm, cn, st = m.grd, m.gmtr, m.cnst, m.satr
+            hg = dict(GRD_Z=g.GRD_vz[:, :, :, :, g.GRD_Z], GRD_LAT=g.GRD_LAT[:, :, K0, :],
+                      GRD_zsfc=g.GRD_zs[:, :, K0, :, g.GRD_ZSFC], GRD_dgz=g.GRD_dgz, GMTR_area=gm.GMTR_area,
+                      GMTR_p_IJ=np.stack([gm.GMTR_p[:, :, K0, :, i] for i in (
+                          gm.GMTR_p_IX, gm.GMTR_p_IY, gm.GMTR_p_IZ, gm.GMTR_p_JX, gm.GMTR_p_JY, gm.GMTR_p_JZ)], -1),
+                      LHV=cn.CONST_LHV, UNDEF=cn.CONST_UNDEF, PSAT0=cn.CONST_PSAT0, RTEM00=st.RTEM00,
+                      CPovR_liq=st.CPovR_liq, CPovR_ice=st.CPovR_ice, LovR_liq=st.LovR_liq, LovR_ice=st.LovR_ice,
+                      SAT_ULIMIT=st.SATURATION_ULIMIT_TEMP, SAT_LLIMIT=st.SATURATION_LLIMIT_TEMP,
+                      NCHEM=np.asarray([m.rcnf.NCHEM_STR, m.rcnf.NCHEM_END]))
+            for k in ("I_QV", "I_QC", "I_QR", "I_QI", "I_QS", "I_QG"):
+                hg[k] = getattr(m.rcnf, k, -1)
+            for k, v in hg.items():
+                out["hgeo." + k] = np.ascontiguousarray(np.asarray(v))
     path = os.path.join(out_dir, f"gl03_z10_{case}.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path))

@@ -48,8 +48,9 @@ def test_history_item_ids_match_header(pkg):
     items = pkg.runtime.HIST_ITEMS
     for n, name in ids.items():
         assert items[n] == name, (n, name)
-    assert len(items) == 42 and items[26:30] == ("sl_u850", "sl_v850", "sl_w850", "sl_t850")
-    assert items[-4:] == ("sl_u100", "sl_v100", "sl_w100", "sl_t100")
+    assert len(items) == 45 and items[26:30] == ("sl_u850", "sl_v850", "sl_w850", "sl_t850")
+    assert items[38:42] == ("sl_u100", "sl_v100", "sl_w100", "sl_t100")
+    assert items[42:] == pkg.runtime.HIST_CHEM == ("sl_cl", "sl_cl2", "sl_cly")
 
 
 def test_status_codes_map_to_exceptions(pkg):

@@ -10,6 +10,8 @@ slices go through pow, exp and log, which CUDA and numpy may round differently
 in the last bit, and the per-layer mean of th_prime and the column water sum
 add in another order: those are compared to a relative max-norm of 1e-12 (the
 one-step parity tolerance of the step itself)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -45,10 +47,11 @@ def _core(pkg, golden, golden_hist):
 
 
 def test_history_two_steps_vs_reference(pkg, golden, golden_hist):
-    """seeded after step 1 (tendencies zero), then all 42 fields after step 2"""
+    """seeded after step 1 (tendencies zero), then all 42 fields after step 2
+    (the chemistry's columns have their own test)"""
     _, st = golden
     _, ref = golden_hist
-    names = pkg.runtime.HIST_ITEMS
+    names = tuple(n for n in pkg.runtime.HIST_ITEMS if n not in pkg.runtime.HIST_CHEM)
     assert sorted(names) == sorted(OH.ML + OH.SL)
     c = _core(pkg, golden, golden_hist)
     c.upload(st["state0"], st["state0_pl"])
@@ -98,7 +101,7 @@ def test_history_step_api_through_backend(pkg, golden, golden_hist):
     assert sorted(h3) == ["ml_dtem", "ml_th", "ml_u"]
     _check(h3, ref, h3)
     msc.io._diag_names_2d = ["sl_cl"]
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(NotImplementedError):   # no terminator chemistry on this handle
         dyn.history_vars_step(msc)
 
 
@@ -110,4 +113,35 @@ def test_history_needs_its_setup(pkg, golden):
     with pytest.raises(pkg.NicamError):
         c.history_vars(("ml_u",), nstep=0, dt=1200.0)
     with pytest.raises(NotImplementedError):
-        c.history_vars(("sl_cl",), nstep=0, dt=1200.0)
+        c.history_vars(("sl_foo",), nstep=0, dt=1200.0)
+
+
+def test_chemistry_columns_vs_reference(pkg, golden_kessler_chem):
+    """sl_cl, sl_cl2 and sl_cly (the terminator chemistry's column means,
+    mod_history_vars.py:149-156) of the DCMIP chemistry run's last state
+    against the reference's: bit for bit (sums in the reference's order, no
+    transcendental functions); a handle without HIST_chem refuses them"""
+    import numpy as np
+    from conftest import GOLDEN, hist_geo
+    geo, st, _ = golden_kessler_chem
+    d = np.load(os.path.join(GOLDEN, "gl03_z10_kessler_chem.npz"))
+    hg = {k[5:]: d[k] for k in d.files if k.startswith("hgeo.")}
+    g = hist_geo({k: v for k, v in geo.items() if k not in ("GRD_LAT", "GRD_LON")}, hg)
+    names = ("sl_cl", "sl_cl2", "sl_cly")
+    c = pkg.NicamCuda(g, graph=False)
+    try:
+        c.upload(st["state2"], st["state2_pl"])
+        with pytest.raises(pkg.NicamError):
+            c.history_vars(names, nstep=2, dt=float(geo["dtl"]))
+    finally:
+        c.close()
+    g["hist_NCHEM"] = hg["NCHEM"]
+    c = pkg.NicamCuda(g, graph=False)
+    try:
+        c.upload(st["state2"], st["state2_pl"])
+        out = c.history_vars(names, nstep=2, dt=float(geo["dtl"]))
+    finally:
+        c.close()
+    for n in names:
+        print(n, "max relative difference", _rel(out[n], d["hist." + n]))
+        assert np.array_equal(out[n], d["hist." + n]), n

@@ -16,9 +16,10 @@ class _Core:
         return {n: None for n in names}
 
 
-def _dyn(pkg):
+def _dyn(pkg, chem=False):
     d = object.__new__(pkg.backend.CudaDyn)
     d.core, d._device_valid, d._host_stale, d._forced = _Core(), True, True, False
+    d._hist_chem = chem
     return d
 
 
@@ -40,8 +41,11 @@ def test_names_follow_the_io_groups(pkg):
 
 
 def test_without_io_every_item(pkg):
-    d = _dyn(pkg)
-    out = d.history_vars_step(_msc())
+    """every item, the chemistry's columns only with the chemistry configured
+    (the reference forms them for AF_TYPE 'DCMIP' with NCHEM_STR >= 0)"""
+    out = _dyn(pkg).history_vars_step(_msc())
+    assert tuple(out) == tuple(n for n in pkg.runtime.HIST_ITEMS if n not in pkg.runtime.HIST_CHEM)
+    out = _dyn(pkg, chem=True).history_vars_step(_msc())
     assert tuple(out) == pkg.runtime.HIST_ITEMS
 
 
@@ -51,10 +55,15 @@ def test_empty_groups_form_nothing(pkg):
 
 
 def test_unknown_names_raise(pkg):
+    """names the device does not form, and the chemistry's columns without
+    the chemistry, raise before any device call"""
     d = _dyn(pkg)
-    with pytest.raises(NotImplementedError):
-        d.history_vars_step(_msc(NS(_diag_names=["ml_u"], _diag_names_2d=["sl_cly"])))
+    for names in (["sl_foo"], ["sl_cly"]):
+        with pytest.raises(NotImplementedError):
+            d.history_vars_step(_msc(NS(_diag_names=["ml_u"], _diag_names_2d=names)))
     assert d.core.calls == []
+    d = _dyn(pkg, chem=True)
+    assert sorted(d.history_vars_step(_msc(NS(_diag_names=[], _diag_names_2d=["sl_cly"])))) == ["sl_cly"]
 
 
 def test_setup_table_history_entries(pkg, golden, golden_hist):

@@ -113,6 +113,22 @@ def test_oracle_simple_physics_matches_reference(case, request):
         assert np.array_equal(precip, pr[f"precip{n}"]), n
 
 
+def test_oracle_chemistry_history_columns_match_reference(golden_kessler_chem):
+    """sl_cl, sl_cl2, sl_cly of the chemistry run's last state: the oracle's
+    history equals the reference's Dyn.history_vars_step bit for bit"""
+    import os
+    from conftest import GOLDEN
+    from oracle import nicam_history as OH
+    geo, st, _ = golden_kessler_chem
+    d = np.load(os.path.join(GOLDEN, "gl03_z10_kessler_chem.npz"))
+    hg = {k[5:]: d[k] for k in d.files if k.startswith("hgeo.")}
+    names = ("sl_cl", "sl_cl2", "sl_cly")
+    got = OH.History()(O.Geo(geo), hg, st["state2"], items=names)
+    for n in names:
+        assert np.array_equal(got[n], d["hist." + n]), n
+    assert 1e-6 < d["hist.sl_cly"].min() and d["hist.sl_cly"].max() < 1e-5   # mixing ratios of order 4e-6
+
+
 def test_moist_held_suarez_fixture_is_active(golden_kessler, golden_dcmip21):
     """the Held-Suarez relaxation replaced the momentum tendency: the moist
     Held-Suarez run moved the momentum away from the Kessler-only run"""
