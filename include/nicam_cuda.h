@@ -259,9 +259,10 @@ int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* g
  * the Cl / Cl2 tendencies (per dry air, analytic over dt; sin, cos, exp and
  * sqrt are CUDA's) join the tracer tendencies on kmin..kmax.  The optional
  * "AF_dcmip_schemes" (int64 [Kessler, simple physics, large-scale
- * condensation(, moist Held-Suarez)], default [1, 0, 0]) adds the DCMIP simple physics
- * (USE_SimpleMicrophys, nhm/forcing/simple_physics.py with the RJ2012
- * boundary layer; mod_af_dcmip.py:230-317) or runs it alone: its surface
+ * condensation(, moist Held-Suarez(, Bryan boundary layer))], default
+ * [1, 0, 0]) adds the DCMIP simple physics (USE_SimpleMicrophys,
+ * nhm/forcing/simple_physics.py with the RJ2012 boundary layer, or the Bryan
+ * one, SM_PBL_Bryan; mod_af_dcmip.py:230-317) or runs it alone: its surface
  * fluxes, implicit boundary-layer diffusion of u, v, potential temperature
  * and vapour, and optional large-scale condensation, from the same state as
  * Kessler, with momentum, vapour and energy tendencies and precipitation

@@ -1861,7 +1861,7 @@ def dcmip_sst(lat, latdepend, held_suarez=False, mitc_type=1):
     return (T00 + pref * (termA + termB)) / (1.0 + SP_ZVIR * q0 * np.exp(-(lat / latw) ** 4))
 
 
-def simple_physics(t, q, u, v, pmid, pint, pdel, rpdel, ps, tsurf, dtime, lsc, Cexch=SP_C):
+def simple_physics(t, q, u, v, pmid, pint, pdel, rpdel, ps, tsurf, dtime, lsc, Cexch=SP_C, bryan=False):
     """simple_physics.py:310-366 (RJ2012 boundary layer, no Held-Suarez) on
     (ncol, nz) columns ordered top to bottom: the lowest full level's
     hydrostatic height, the large-scale condensation (lsc, :48-91), the
@@ -1869,8 +1869,9 @@ def simple_physics(t, q, u, v, pmid, pint, pdel, rpdel, ps, tsurf, dtime, lsc, C
     bulk surface fluxes of the lowest level (:200-225) and the implicit
     boundary-layer diffusion of u, v, potential temperature and q
     (:228-307).  ``Cexch`` is the heat / moisture exchange coefficient
-    (four times 0.0011 for moist Held-Suarez).  Returns t, q, u, v and the
-    condensation's precipitation."""
+    (four times 0.0011 for moist Held-Suarez); ``bryan`` takes the
+    height-based boundary layer of the tropical-cyclone test (TC_PBL_mod).
+    Returns t, q, u, v and the condensation's precipitation."""
     ncol, nz = t.shape
     dlnpint = np.log(ps) - np.log(pint[:, nz - 1])
     za = SP_RAIR / SP_GRAV * t[:, -1] * (1.0 + SP_ZVIR * q[:, -1]) * 0.5 * dlnpint
@@ -1885,9 +1886,22 @@ def simple_physics(t, q, u, v, pmid, pint, pdel, rpdel, ps, tsurf, dtime, lsc, C
         precl = np.zeros(ncol)
     wind = np.sqrt(u[:, -1] ** 2 + v[:, -1] ** 2)
     Cd = np.where(wind < SP_V20, SP_CD0 + SP_CD1 * wind, SP_CM)
-    decay = np.where(pint[:, 0:nz] >= SP_PBLTOP, 1.0, np.exp(-(SP_PBLTOP - pint[:, 0:nz]) ** 2 / SP_PBLCONST ** 2))
-    Km = (Cd * wind * za)[:, None] * decay
-    Ke = (Cexch * wind * za)[:, None] * decay
+    if bryan:   # :128-141, the height-based boundary layer of the tropical-cyclone test
+        Km, Ke = np.zeros((ncol, nz)), np.zeros((ncol, nz))
+        zi = np.zeros(ncol)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            for c in range(nz - 1, -1, -1):
+                dlnpint = np.log(pint[:, c + 1]) - np.log(pint[:, c])
+                zi = zi + SP_RAIR / SP_GRAV * t[:, c] * (1.0 + SP_ZVIR * q[:, c]) * dlnpint
+                below = zi <= 1000.0
+                fac = 1.0 - zi / 1000.0
+                base = wind * zi * fac * fac
+                Km[:, c] = np.where(below, 0.4 * np.sqrt(Cd) * base, 0.0)
+                Ke[:, c] = np.where(below, 0.4 * np.sqrt(Cexch) * base, 0.0)
+    else:
+        decay = np.where(pint[:, 0:nz] >= SP_PBLTOP, 1.0, np.exp(-(SP_PBLTOP - pint[:, 0:nz]) ** 2 / SP_PBLCONST ** 2))
+        Km = (Cd * wind * za)[:, None] * decay
+        Ke = (Cexch * wind * za)[:, None] * decay
     # surface fluxes, lowest level only
     qsats = SP_EPSILO * SP_E0 / ps * np.exp(-SP_LATVAP / SP_RH2O * ((1.0 / tsurf) - 1.0 / SP_T0))
     dm = 1.0 + Cd * wind * dtime / za
@@ -2023,7 +2037,8 @@ def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_de
         hs = bool(sm.get("held_suarez", False))
         tsurf = dcmip_sst(flat(sm["lat"]), sm["latdepend"], hs, sm.get("mitc", 1))
         t_n, qv_n, u_n, v_n, pr2 = simple_physics(tem_td, qv_old, u, v, pre_td, pint, pdel, 1.0 / pdel, pre_sfc,
-                                                  tsurf, dt, sm["lsc"], SP_C * (4.0 if hs else 1.0))
+                                                  tsurf, dt, sm["lsc"], SP_C * (4.0 if hs else 1.0),
+                                                  bryan=bool(sm.get("bryan", False)))
         for d, (a, b, vd) in enumerate(((0, 3, vx_td), (1, 4, vy_td), (2, 5, vz_td))):
             fv[d] = grid(((u_n * ij[a][:, None] + v_n * ij[b][:, None] - vd) / dt)[:, ::-1])
         qc, qr = td(q[..., 1]), td(q[..., 2])

@@ -134,8 +134,8 @@ def geo_from_msc(msc) -> dict:
         fl = _dcmip_flags(msc)
         K0 = m.adm.ADM_K0
         g["AF_dcmip_schemes"] = np.asarray([fl["USE_Kessler"], fl["USE_SimpleMicrophys"], fl["SM_Latdepend_SST"],
-                                            fl["SM_LargeScaleCond"], fl["USE_HeldSuarez"], fl["SM_MITC_SST_TYPE"]],
-                                           np.int64)
+                                            fl["SM_LargeScaleCond"], fl["USE_HeldSuarez"], fl["SM_MITC_SST_TYPE"],
+                                            fl["SM_PBL_Bryan"]], np.int64)
         if fl["USE_ToyChemistry"] or fl["USE_SimpleMicrophys"] or fl["USE_HeldSuarez"]:
             g["AF_dcmip_lat"] = np.ascontiguousarray(m.grd.GRD_LAT[:, :, K0, :])
         if fl["USE_ToyChemistry"]:   # terminator chemistry on the Cl / Cl2 tracers
@@ -245,12 +245,11 @@ class CudaDyn:
         if getattr(r, "AF_TYPE", "NONE") == "DCMIP":
             flags = _dcmip_flags(msc)
             if not (flags.get("USE_Kessler") or flags.get("USE_SimpleMicrophys")) \
-                    or flags.get("SM_PBL_Bryan") or getattr(r, "RAIN_TYPE", "DRY") != "WARM" or \
+                    or getattr(r, "RAIN_TYPE", "DRY") != "WARM" or \
                     (flags.get("USE_ToyChemistry") and int(getattr(r, "NCHEM_END", -1)) - int(getattr(r, "NCHEM_STR", -1)) != 1):
                 raise NotImplementedError("cuda backend: DCMIP forcing with Kessler microphysics and / or the simple "
-                                          "physics (RJ2012 boundary layer), optionally the terminator chemistry "
-                                          "and moist Held-Suarez (RAIN_TYPE WARM, two chemistry tracers; no Bryan "
-                                          "boundary layer)")
+                                          "physics, optionally the terminator chemistry and moist Held-Suarez "
+                                          "(RAIN_TYPE WARM, two chemistry tracers)")
         elif getattr(r, "AF_TYPE", "NONE") not in ("NONE", "HELD-SUAREZ"):
             raise NotImplementedError("cuda backend: artificial forcing NONE or HELD-SUAREZ only")
 

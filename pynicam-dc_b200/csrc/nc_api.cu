@@ -373,6 +373,7 @@ struct nc_handle {
   int kess_n_cl = -1, kess_n_cl2 = -1;      // terminator toy chemistry tracers (optional)
   const double *kess_lat = nullptr, *kess_lon = nullptr;
   int kess_on = 1, sm_on = 0, sm_lsc = 0;   // DCMIP schemes: Kessler, simple physics, its condensation
+  int sm_bryan = 0;                         // the simple physics with the Bryan boundary layer
   int dcmip_hs = 0;                         // moist Held-Suarez on top of the DCMIP schemes
   const double* dcmip_hs_lat = nullptr;
   const double *sm_zh = nullptr, *sm_zsfc = nullptr, *sm_tsurf = nullptr, *sm_ij = nullptr;
@@ -945,7 +946,7 @@ static int run_step(nc_handle* h) {
       // interior cells only: halo rows are filled by the exchange below and the
       // boundary levels of vtmp2 stay zero from allocation
       const dim3 gt((unsigned)((D.G - 2 + DD_DX - 1) / DD_DX), (unsigned)((D.G - 2 + DD_DY - 1) / DD_DY), (unsigned)D.L);
-      k_dd3d_t<<<gt, DD_DX * DD_DY, 0, s>>>(v, o);
+      k_dd3d_m<R, true><<<gt, DD_DX * DD_DY, dd3d_m_smem<R>(), s>>>(v, o);
       TRY(check_launch(h, "dd3d"));
       k_dd3d_pl<<<pkb, 128, 0, ps>>>(vp, op);
       TRY(check_launch(h, "dd3d_pl"));
@@ -1468,6 +1469,7 @@ int nc_forcing_step(nc_handle* h) {
     a.kessler = h->kess_on;
     a.sm = h->sm_on;
     a.sm_lsc = h->sm_lsc;
+    a.sm_bryan = h->sm_bryan;
     a.zh = h->sm_zh;
     a.zsfc = h->sm_zsfc;
     a.tsurf = h->sm_tsurf;
@@ -1598,6 +1600,8 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   // dynamic shared memory in its float64 instance
   CU(cudaFuncSetAttribute(k_hdiff2_m<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, hdiff2_m_smem<double>()));
   CU(cudaFuncSetAttribute(k_hdiff2_m<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, hdiff2_m_smem<float>()));
+  CU(cudaFuncSetAttribute(k_dd3d_m<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dd3d_m_smem<double>()));
+  CU(cudaFuncSetAttribute(k_dd3d_m<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dd3d_m_smem<float>()));
   ArrTab T;
   for (int n = 0; n < narrays; ++n) {
     if (!arrays[n].name || !arrays[n].data) return fail(NC_ERR_ARG, "null array entry");
@@ -1765,14 +1769,16 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
     if (C.nqw != 3) return fail(NC_ERR_ARG, "DCMIP forcing needs RAIN_TYPE WARM (NQW_END = 2: vapour, cloud, rain)");
     if (D.kmax - D.kmin + 1 > NC_KESS_K || D.kmax - D.kmin < 1)
       return fail(NC_ERR_ARG, "DCMIP forcing: 2.." + std::to_string(NC_KESS_K) + " model levels");
-    if (const nc_array* sc = T.get("AF_dcmip_schemes")) {   // [Kessler, simple physics, condensation(, Held-Suarez)]
-      if (sc->dtype != NC_I64 || (numel(sc) != 3 && numel(sc) != 4))
-        return fail(NC_ERR_ARG, "AF_dcmip_schemes: three or four int64 switches");
+    if (const nc_array* sc = T.get("AF_dcmip_schemes")) {
+      // [Kessler, simple physics, condensation(, Held-Suarez(, Bryan boundary layer))]
+      if (sc->dtype != NC_I64 || numel(sc) < 3 || numel(sc) > 5)
+        return fail(NC_ERR_ARG, "AF_dcmip_schemes: three to five int64 switches");
       const long long* f3 = (const long long*)sc->data;
       h->kess_on = f3[0] != 0;
       h->sm_on = f3[1] != 0;
       h->sm_lsc = h->sm_on && f3[2] != 0;
-      h->dcmip_hs = numel(sc) == 4 && f3[3] != 0;
+      h->dcmip_hs = numel(sc) >= 4 && f3[3] != 0;
+      h->sm_bryan = h->sm_on && numel(sc) >= 5 && f3[4] != 0;
       if (!h->kess_on && !h->sm_on) return fail(NC_ERR_ARG, "AF_dcmip_schemes: neither Kessler nor simple physics");
     }
     if (h->dcmip_hs) TRY(up_reg(h, T, "AF_dcmip_hs_lat_terms", 1, 3, &h->dcmip_hs_lat));

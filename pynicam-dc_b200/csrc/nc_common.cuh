@@ -156,9 +156,6 @@ template <> __device__ __forceinline__ const GeomT<float>& geom<float>() { retur
 #ifndef NC_F32_HDIFF2
 #define NC_F32_HDIFF2 4
 #endif
-#ifndef NC_F32_DD3D
-#define NC_F32_DD3D 6
-#endif
 #ifndef NC_F32_VP0H
 #define NC_F32_VP0H 5
 #endif

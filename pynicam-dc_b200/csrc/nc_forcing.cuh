@@ -127,7 +127,7 @@ struct DcmipArgs {
   // simple physics (optional): large-scale condensation switch, half-level
   // heights [l][k][j][i], surface height, sea-surface temperature [l][j][i],
   // the column unit vectors IX, IY, IZ, JX, JY, JZ [6][l][j][i]
-  int sm, sm_lsc;
+  int sm, sm_lsc, sm_bryan;        // simple physics, its condensation, the Bryan boundary layer
   const double *zh, *zsfc, *tsurf, *ij;
   double sm_C;                    // the heat / moisture exchange coefficient (x4 for moist Held-Suarez)
   // moist Held-Suarez (optional): |sin lat|^2, |cos lat|^2, |cos lat|^4 planes
@@ -156,7 +156,7 @@ __device__ __forceinline__ double np_rowsum(const double* x, int n) {
 }
 
 // DCMIP simple physics (nhm/forcing/simple_physics.py:310-366, the DCMIP2016
-// v6 scheme with the RJ2012 boundary layer; Cv the exchange coefficient of
+// v6 scheme with the RJ2012 boundary layer, or Bryan's with bryan; Cv the exchange coefficient of
 // heat and moisture, 0.0011, four times that for moist Held-Suarez) on one column of
 // nz levels ordered top to bottom: t, q, u, v updated in place; pm the full-
 // level pressure, pint the nz + 1 interface pressures (pint[nz] = ps);
@@ -164,7 +164,8 @@ __device__ __forceinline__ double np_rowsum(const double* x, int n) {
 // precipitation rate (0 without lsc).  log, exp, pow are CUDA's.
 __device__ double simple_physics_col(int nz, double* t, double* q, double* u, double* v, const double* pm,
                                      const double* pint, double ps, double tsurf, double dt, int lsc, double Cv,
-                                     double* CE, double* CEm, double* CFu, double* CFv, double* CFt, double* CFq) {
+                                     int bryan, double* CE, double* CEm, double* CFu, double* CFv, double* CFt,
+                                     double* CFq) {
   const double rair = 287.0, rh2o = 461.5, grav = 9.80616, cpair = 1.0045e3, latvap = 2.5e6;
   const double epsilo = rair / rh2o, zvir = (rh2o / rair) - 1.0;
   const double T0 = 273.16, e0 = 610.78, rhow = 1000.0;
@@ -193,6 +194,20 @@ __device__ double simple_physics_col(int nz, double* t, double* q, double* u, do
     const double x = pbltop - pint[c];
     return (pint[c] >= pbltop) ? 1.0 : exp(-(x * x) / pblconst2);
   };
+  // the Bryan boundary layer (TC_PBL_mod, :128-141): diffusivities from the
+  // interface heights below 1 km, integrated upward from the surface
+  double kmB[NC_KESS_K], keB[NC_KESS_K];
+  if (bryan) {
+    double zi = 0.0;
+    for (int c = nz - 1; c >= 0; --c) {
+      const double dlnpint = log(pint[c + 1]) - log(pint[c]);
+      zi = zi + rair / grav * t[c] * (1.0 + zvir * q[c]) * dlnpint;
+      const double fac = 1.0 - zi / 1000.0;
+      const double base = wind * zi * fac * fac;
+      kmB[c] = (zi <= 1000.0) ? 0.4 * sqrt(Cd) * base : 0.0;
+      keB[c] = (zi <= 1000.0) ? 0.4 * sqrt(Cv) * base : 0.0;
+    }
+  }
   // implicit bulk surface fluxes of the lowest level (:200-225)
   const double qsats = epsilo * e0 / ps * exp(-latvap / rh2o * ((1.0 / tsurf) - 1.0 / T0));
   const double dm = 1.0 + Cd * wind * dt / za, dh = 1.0 + Cv * wind * dt / za;
@@ -207,9 +222,9 @@ __device__ double simple_physics_col(int nz, double* t, double* q, double* u, do
     const double tvp = t[c + 1] * (1.0 + zvir * q[c + 1]), tv = t[c] * (1.0 + zvir * q[c]);
     const double rho = pint[c + 1] / (rair * (tvp + tv) / 2.0);
     const double dpm = pm[c + 1] - pm[c];
-    const double dc = decay(c + 1);
-    fm = g2dt * (KmC * dc) * rho * rho / dpm;
-    fe = g2dt * (KeC * dc) * rho * rho / dpm;
+    const double dc = bryan ? 0.0 : decay(c + 1);
+    fm = g2dt * (bryan ? kmB[c + 1] : KmC * dc) * rho * rho / dpm;
+    fe = g2dt * (bryan ? keB[c + 1] : KeC * dc) * rho * rho / dpm;
   };
   double ce = 0.0, cem = 0.0, cfu = 0.0, cfv = 0.0, cft = 0.0, cfq = 0.0;
   double fm_lo = 0.0, fe_lo = 0.0;   // the interface below level c
@@ -417,8 +432,8 @@ __global__ void k_forcing_dcmip(DcmipArgs a) {
     }
     pint[0] = 0.0;
     pint[nz] = ps;
-    prec = prec + simple_physics_col(nz, st, sq, su, sv, pm, pint, ps, a.tsurf[cidx], dt, a.sm_lsc, a.sm_C, w1, w2,
-                                     w3, w4, w5, w6);
+    prec = prec + simple_physics_col(nz, st, sq, su, sv, pm, pint, ps, a.tsurf[cidx], dt, a.sm_lsc, a.sm_C,
+                                     a.sm_bryan, w1, w2, w3, w4, w5, w6);
   }
   double hs_psref = 0.0, sin2 = 0.0, cos2 = 0.0, cos4 = 0.0;
   if (a.hs) {   // moist Held-Suarez: the reference surface pressure of the column

@@ -44,13 +44,35 @@ __device__ __forceinline__ R ddivd(int i, int j, int l, int d, const R aTI, cons
 #endif
 // resident blocks per SM for a register budget of n blocks of 256 threads
 #define DD_MINB(n) ((n) * 256 / (DD_DX * DD_DY) > 0 ? (n) * 256 / (DD_DX * DD_DY) : 1)
+// The tile's k-invariant coefficients are read once per block instead of
+// once per level: the triangle weights coef_intp (18 planes) staged in shared
+// memory, the cell's coef_diff (18) held in registers (CDR) or read per
+// level.  Dynamic shared memory dd3d_m_smem<R>().
 template <class R>
-__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(NC_MINB(R, 4, NC_F32_DD3D))) k_dd3d_t(Four<R> v, Three<R> out) {
-  constexpr int PX = DD_DX + 2, PY = DD_DY + 2;   // points i0-1 .. i0+DX, j0-1 .. j0+DY
-  constexpr int TX = DD_DX + 1, TY = DD_DY + 1;   // triangles i0-1 .. i0+DX-1, j0-1 .. j0+DY-1
-  __shared__ R s_vm[3][PY * PX];
-  __shared__ R s_rw[2][PY * PX];
-  __shared__ R s_ti[TY * TX], s_tj[TY * TX];
+constexpr int dd3d_m_smem() {
+  return (18 * (DD_DX + 1) * (DD_DY + 1) + 5 * (DD_DX + 2) * (DD_DY + 2) + 2 * (DD_DX + 1) * (DD_DY + 1)) *
+         (int)sizeof(R);
+}
+#ifndef DD_M_MINB
+#define DD_M_MINB 2
+#endif
+// The next level's staging writes s_vm and the rwv buffer of the level below,
+// which only this level's triangle pass reads (done before its second
+// barrier), and the next level's triangle pass writes s_ti / s_tj only after
+// the next first barrier, which every thread reaches after its cell pass: no
+// barrier is needed at the end of a level, and the corner tile alone waits
+// for its singular-point fix.
+
+template <class R, bool CDR>
+__global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(NC_MINB(R, DD_M_MINB, 4))) k_dd3d_m(Four<R> v, Three<R> out) {
+  constexpr int PX = DD_DX + 2, PY = DD_DY + 2, NP = PX * PY;
+  constexpr int TX = DD_DX + 1, TY = DD_DY + 1, NT = TX * TY;
+  extern __shared__ __align__(16) unsigned char dd_smem[];
+  R* s_ci = reinterpret_cast<R*>(dd_smem);   // [18][NT] coef_intp of each triangle
+  R* s_vm = s_ci + 18 * NT;                    // [3][NP]
+  R* s_rw = s_vm + 3 * NP;                     // [2][NP]
+  R* s_ti = s_rw + 2 * NP;                     // [NT]
+  R* s_tj = s_ti + NT;                         // [NT]
   const int l = blockIdx.z;
   const int i0 = 1 + blockIdx.x * DD_DX, j0 = 1 + blockIdx.y * DD_DY;
   const int G = cD.G, gmax = cD.G - 2;
@@ -59,11 +81,22 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(NC_MINB(R, 4, NC_F32_DD
   const bool own = (i <= gmax) && (j <= gmax);
   const int n = cD.npti;
   const R* cz = CG.C2WGz;
-  for (int p = tid; p < PX * PY; p += blockDim.x) s_rw[0][p] = R(0.0);   // rwv(kmin) = 0
+  for (int p = tid; p < NT; p += blockDim.x) {
+    const int ii = i0 - 1 + p % TX, jj = j0 - 1 + p / TX;
+    const bool ok = ii <= G - 2 && jj <= G - 2;
+#pragma unroll
+    for (int m = 0; m < 18; ++m) s_ci[m * NT + p] = ok ? P2c(CG.coef_intp, m, ii, jj, l) : R(0.0);
+  }
+  R cd[CDR ? 18 : 1];
+  if (CDR && own) {
+#pragma unroll
+    for (int m = 0; m < (CDR ? 18 : 1); ++m) cd[m] = P2c(CG.coef_diff, m, i, j, l);
+  }
+  for (int p = tid; p < NP; p += blockDim.x) s_rw[p] = R(0.0);   // rwv(kmin) = 0
   int cur = 0;
   for (int k = cD.kmin; k <= cD.kmax; ++k) {
     const bool up = (k + 1 <= cD.kmax);   // rwv(k+1) = 0 above kmax
-    for (int p = tid; p < PX * PY; p += blockDim.x) {
+    for (int p = tid; p < NP; p += blockDim.x) {
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
       R a = R(0.0), b = R(0.0), c = R(0.0), r = R(0.0);
       if (ii < G && jj < G) {
@@ -76,42 +109,44 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(NC_MINB(R, 4, NC_F32_DD
         if (up) {
           const int qp = q + cD.planei;   // level k+1
           const R h = cz[qp] * v.f[0][qp] + cz[n + qp] * f0 + cz[2 * n + qp] * v.f[1][qp] +
-                           cz[3 * n + qp] * f1 + cz[4 * n + qp] * v.f[2][qp] + cz[5 * n + qp] * f2;
+                      cz[3 * n + qp] * f1 + cz[4 * n + qp] * v.f[2][qp] + cz[5 * n + qp] * f2;
           r = h * gam_at(CG.RGAMH, qp) + v.f[3][qp] * CG.RGSQRTH[qp];
         }
       }
-      s_vm[0][p] = a;
-      s_vm[1][p] = b;
-      s_vm[2][p] = c;
-      s_rw[cur ^ 1][p] = r;
+      s_vm[p] = a;
+      s_vm[NP + p] = b;
+      s_vm[2 * NP + p] = c;
+      s_rw[(cur ^ 1) * NP + p] = r;
     }
     __syncthreads();
     const R rdz = CC.rdgz[k];
-    const R* rU = s_rw[cur ^ 1];
-    const R* rD = s_rw[cur];
-    for (int p = tid; p < TX * TY; p += blockDim.x) {
+    const R* rU = s_rw + (cur ^ 1) * NP;
+    const R* rD = s_rw + cur * NP;
+    for (int p = tid; p < NT; p += blockDim.x) {
       const int px = p % TX, py = p / TX;
+      const int a = py * PX + px, b = a + 1, c = a + PX + 1, d = a + PX;
+      auto C = [&](int dir, int pt, int t) { return s_ci[((dir * 3 + pt) * 2 + t) * NT + p]; };
+      const R wTI = div3((rU[a] + rU[b] + rU[c]) - (rD[a] + rD[b] + rD[c])) * rdz;
+      const R wTJ = div3((rU[a] + rU[c] + rU[d]) - (rD[a] + rD[c] + rD[d])) * rdz;
+      const R* v0 = s_vm;
+      const R* v1 = s_vm + NP;
+      const R* v2 = s_vm + 2 * NP;
+      R sTI = C(0, 0, 0) * v0[a] + C(0, 1, 0) * v0[b] + C(0, 2, 0) * v0[c] + C(1, 0, 0) * v1[a] +
+              C(1, 1, 0) * v1[b] + C(1, 2, 0) * v1[c] + C(2, 0, 0) * v2[a] + C(2, 1, 0) * v2[b] +
+              C(2, 2, 0) * v2[c] + wTI;
+      R sTJ = C(0, 0, 1) * v0[a] + C(0, 1, 1) * v0[c] + C(0, 2, 1) * v0[d] + C(1, 0, 1) * v1[a] +
+              C(1, 1, 1) * v1[c] + C(1, 2, 1) * v1[d] + C(2, 0, 1) * v2[a] + C(2, 1, 1) * v2[c] +
+              C(2, 2, 1) * v2[d] + wTJ;
       const int ii = i0 - 1 + px, jj = j0 - 1 + py;
-      R sTI = R(0.0), sTJ = R(0.0);
-      if (ii <= G - 2 && jj <= G - 2) {
-        const int a = py * PX + px, b = a + 1, c = a + PX + 1, d = a + PX;
-        auto C = [&](int dir, int pt, int t) { return P2c(CG.coef_intp, (dir * 3 + pt) * 2 + t, ii, jj, l); };
-        const R wTI = div3((rU[a] + rU[b] + rU[c]) - (rD[a] + rD[b] + rD[c])) * rdz;
-        const R wTJ = div3((rU[a] + rU[c] + rU[d]) - (rD[a] + rD[c] + rD[d])) * rdz;
-        sTI = C(0, 0, 0) * s_vm[0][a] + C(0, 1, 0) * s_vm[0][b] + C(0, 2, 0) * s_vm[0][c] +
-              C(1, 0, 0) * s_vm[1][a] + C(1, 1, 0) * s_vm[1][b] + C(1, 2, 0) * s_vm[1][c] +
-              C(2, 0, 0) * s_vm[2][a] + C(2, 1, 0) * s_vm[2][b] + C(2, 2, 0) * s_vm[2][c] + wTI;
-        sTJ = C(0, 0, 1) * s_vm[0][a] + C(0, 1, 1) * s_vm[0][c] + C(0, 2, 1) * s_vm[0][d] +
-              C(1, 0, 1) * s_vm[1][a] + C(1, 1, 1) * s_vm[1][c] + C(1, 2, 1) * s_vm[1][d] +
-              C(2, 0, 1) * s_vm[2][a] + C(2, 1, 1) * s_vm[2][c] + C(2, 2, 1) * s_vm[2][d] + wTJ;
-      }
+      if (!(ii <= G - 2 && jj <= G - 2)) sTI = sTJ = R(0.0);
       s_ti[p] = sTI;
       s_tj[p] = sTJ;
     }
     __syncthreads();
-    if (tid == 0 && i0 == 1 && j0 == 1)   // singular-point fix at the (0,0) triangle
-      s_ti[0] = s_ti[0] * (R)CG.pntmask[l * 2 + 0] + s_tj[1] * (R)CG.pntmask[l * 2 + 1];
-    __syncthreads();
+    if (i0 == 1 && j0 == 1) {   // singular-point fix at the (0,0) triangle (block-uniform branch)
+      if (tid == 0) s_ti[0] = s_ti[0] * (R)CG.pntmask[l * 2 + 0] + s_tj[1] * (R)CG.pntmask[l * 2 + 1];
+      __syncthreads();
+    }
     if (own) {
       const int ta = (ty + 1) * TX + (tx + 1);   // triangle (i, j)
       const R aTI = s_ti[ta], aTJ = s_tj[ta];
@@ -119,13 +154,12 @@ __global__ void __launch_bounds__(DD_DX * DD_DY, DD_MINB(NC_MINB(R, 4, NC_F32_DD
       const R cTI = s_ti[ta - TX - 1], cTJ = s_tj[ta - TX - 1];   // (i-1, j-1)
       const R dTJ = s_tj[ta - TX];           // (i, j-1)
       const int q = ix(i, j, k, l);
-      auto D = [&](int m) { return P2c(CG.coef_diff, m, i, j, l); };
+      auto D = [&](int m) { return CDR ? cd[CDR ? m : 0] : P2c(CG.coef_diff, m, i, j, l); };
 #pragma unroll
       for (int d = 0; d < 3; ++d)
         out.f[d][q] = D(d * 6 + 0) * (aTI + aTJ) + D(d * 6 + 1) * (aTJ + bTI) + D(d * 6 + 2) * (bTI + cTJ) +
                       D(d * 6 + 3) * (cTJ + cTI) + D(d * 6 + 4) * (cTI + dTJ) + D(d * 6 + 5) * (dTJ + aTI);
     }
-    __syncthreads();
     cur ^= 1;
   }
 }

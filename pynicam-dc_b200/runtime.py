@@ -294,11 +294,13 @@ def setup_table(geo: dict) -> dict:
             if k in geo:
                 t[k] = np.asarray(float(_scalar(geo[k])), np.float64)
         if "AF_dcmip_schemes" in geo:
-            # [Kessler, simple physics, latitude-dependent SST, condensation(, moist Held-Suarez, MITC SST type)]
+            # [Kessler, simple physics, latitude-dependent SST, condensation(, moist Held-Suarez, MITC SST
+            # type(, Bryan boundary layer))]
             fl = [int(x) for x in np.asarray(geo["AF_dcmip_schemes"]).reshape(-1)]
             kes, sm, latdep, lsc = fl[:4]
             hs, mitc = (fl[4], fl[5]) if len(fl) >= 6 else (0, 1)
-            t["AF_dcmip_schemes"] = np.asarray([kes, sm, lsc] + ([hs] if hs else []), np.int64)
+            bryan = fl[6] if len(fl) >= 7 else 0
+            t["AF_dcmip_schemes"] = np.asarray([kes, sm, lsc, hs, bryan], np.int64)
             G, L = int(_scalar(geo["gall_1d"])), int(_scalar(geo["lall"]))
             if sm or hs:
                 lat = np.asarray(geo["AF_dcmip_lat"], np.float64).reshape(G, G, 1, L)

@@ -84,10 +84,10 @@ def golden_kessler_chem():
     return geo, st, {k: d[k] for k in d.files if k.startswith("precip")}
 
 
-def _dcmip_fixture(name):
+def _dcmip_fixture(name, vl=10):
     import numpy as np
     from make_golden import load
-    path = os.path.join(GOLDEN, f"gl03_z10_{name}.npz")
+    path = os.path.join(GOLDEN, f"gl03_z{vl}_{name}.npz")
     geo, st = load(path)
     d = np.load(path)
     return geo, st, {k: d[k] for k in d.files if k.startswith("precip")}
@@ -113,6 +113,13 @@ def golden_dcmip21():
 
 
 @pytest.fixture(scope="session")
+def golden_dcmip12bryan():
+    """the DCMIP2016 case 1-2 (tropical cyclone) scheme set with the Bryan
+    boundary layer run by the reference (make_kessler.py --case dcmip12bryan)"""
+    return _dcmip_fixture("dcmip12bryan", 30)
+
+
+@pytest.fixture(scope="session")
 def golden_smlsc():
     """the simple physics alone with its large-scale condensation and the
     constant sea-surface temperature, run by the reference
@@ -126,7 +133,8 @@ def dcmip_oracle_args(geo):
     chem = (geo["GRD_LAT"], geo["GRD_LON"], int(geo["NCHEM_STR"]), int(geo["NCHEM_END"])) \
         if "NCHEM_STR" in geo else None
     sm = dict(zh=geo["GRD_ZH"], zsfc=geo["GRD_zsfc"], lat=geo["GRD_LAT"], ij=geo["GMTR_p_IJ"],
-              latdepend=bool(fl[2]), lsc=bool(fl[3]), held_suarez=bool(fl[4]), mitc=fl[5]) if fl[1] else None
+              latdepend=bool(fl[2]), lsc=bool(fl[3]), held_suarez=bool(fl[4]), mitc=fl[5],
+              bryan=bool(fl[6])) if fl[1] else None
     return dict(chem=chem, kessler_on=bool(fl[0]), sm=sm)
 
 

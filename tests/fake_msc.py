@@ -91,7 +91,7 @@ def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_
         m.satr = satr
     if dcmip is not None:   # DCMIP forcing: the schemes of dcmip_flags (Kessler only when absent)
         chem = "NCHEM_STR" in dcmip
-        fl = [int(x) for x in dcmip.get("dcmip_flags", (1, 0, 0, 0, 0, 1))]
+        fl = [int(x) for x in dcmip.get("dcmip_flags", (1, 0, 0, 0, 0, 1, 0))]
         grd.GRD_Z, grd.GRD_ZH, grd.GRD_ZSFC = 0, 1, 0
         zh = dcmip.get("GRD_ZH", dcmip["GRD_Z"])
         grd.GRD_vz = np.stack([np.asarray(dcmip["GRD_Z"]), np.asarray(zh)], axis=-1)
@@ -106,7 +106,7 @@ def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_
             assert np.array_equal(gmtr.GMTR_p[:, :, 0, :, 2:8], dcmip["GMTR_p_IJ"])
         rcnf.RAIN_TYPE = "WARM"
         m.afdcmip = NS(USE_Kessler=bool(fl[0]), USE_SimpleMicrophys=bool(fl[1]), SM_Latdepend_SST=bool(fl[2]),
-                       SM_LargeScaleCond=bool(fl[3]), SM_PBL_Bryan=False, USE_ToyChemistry=chem,
+                       SM_LargeScaleCond=bool(fl[3]), SM_PBL_Bryan=bool(fl[6]), USE_ToyChemistry=chem,
                        USE_HeldSuarez=bool(fl[4]), SM_MITC_SST_TYPE=fl[5])
         m.frc = NS(NEGATIVE_FIXER=False, UPDATE_TOT_DENS=True)
     if io_names is not None:   # the I/O object's diagnostic groups (share/mod_io.py:248-265)

@@ -19,7 +19,8 @@ history diagnostics read (hgeo.*).  --case dcmip11 adds the DCMIP simple physics
 large-scale condensation: the scheme set of DCMIP2016 case 1-1) to Kessler
 and the chemistry; --case smlsc runs the simple physics alone with its
 large-scale condensation and the constant sea-surface temperature; --case dcmip21 the moist
-Held-Suarez scheme set of DCMIP2016 case 2-1.  They
+Held-Suarez scheme set of DCMIP2016 case 2-1; --case dcmip12bryan the
+tropical-cyclone scheme set with the Bryan boundary layer.  They
 also store the half-level heights, the surface height and the column unit
 vectors the simple physics reads.
 
@@ -51,10 +52,17 @@ CASES = {
                  "SM_LargeScaleCond": False}, True),
     "smlsc": ({"USE_Kessler": False, "USE_SimpleMicrophys": True, "SM_Latdepend_SST": False,
                "SM_LargeScaleCond": True}, False),
+    # the DCMIP2016 case 1-2 (tropical cyclone) scheme set with the Bryan boundary layer
+    "dcmip12bryan": ({"USE_Kessler": True, "USE_SimpleMicrophys": True, "SM_Latdepend_SST": False,
+                      "SM_LargeScaleCond": False, "SM_PBL_Bryan": True}, False),
     # DCMIP2016 case 2-1, moist Held-Suarez (the SET_DCMIP2016_21 scheme set)
     "dcmip21": ({"USE_Kessler": True, "USE_SimpleMicrophys": True, "SM_Latdepend_SST": False,
                  "SM_LargeScaleCond": False, "USE_HeldSuarez": True}, False),
 }
+
+
+# the Bryan boundary layer mixes below 1 km: 30 layers put the lowest ones there
+VLAYERS = {"dcmip12bryan": 30}
 
 
 def run(ref: str, out_dir: str, case: str = "kessler"):
@@ -63,8 +71,9 @@ def run(ref: str, out_dir: str, case: str = "kessler"):
     sm = bool(flags.get("USE_SimpleMicrophys", False))
     with tempfile.TemporaryDirectory() as tmp:
         case_dir = os.path.join(tmp, "kessler")
-        MG.prep(ref, case_dir, GL, VL, ZTOP)
-        c = toml.loads(MG.model_toml(ref, GL, VL, DTL, GAMMA, NSTEPS, "WARM"))
+        vl = VLAYERS.get(case, VL)
+        MG.prep(ref, case_dir, GL, vl, ZTOP)
+        c = toml.loads(MG.model_toml(ref, GL, vl, DTL, GAMMA, NSTEPS, "WARM"))
         c["runconfparam"]["AF_TYPE"] = "DCMIP"
         c["forcing_dcmip_param"] = dict(flags)
         if chem:
@@ -106,7 +115,7 @@ def run(ref: str, out_dir: str, case: str = "kessler"):
         assert m.rcnf.AF_TYPE == "DCMIP" and afdcmip.USE_SimpleMicrophys == sm
         for k, v in flags.items():
             assert getattr(afdcmip, k) == v, k
-        assert afdcmip.USE_ToyChemistry == chem and not afdcmip.SM_PBL_Bryan and afdcmip.SM_MITC_SST_TYPE == 1
+        assert afdcmip.USE_ToyChemistry == chem and afdcmip.SM_MITC_SST_TYPE == 1
         assert m.rcnf.NQW_END == 2 and (m.rcnf.I_QV, m.rcnf.I_QC, m.rcnf.I_QR) == (0, 1, 2)
         assert not m.frc.NEGATIVE_FIXER and m.frc.UPDATE_TOT_DENS
         pv, pvp = m.prgv.PRG_var, m.prgv.PRG_var_pl
@@ -146,7 +155,8 @@ def run(ref: str, out_dir: str, case: str = "kessler"):
             out["geo.GRD_zsfc"] = np.ascontiguousarray(m.grd.GRD_zs[:, :, K0, :, m.grd.GRD_ZSFC])
         out["geo.dcmip_flags"] = np.asarray([int(afdcmip.USE_Kessler), int(afdcmip.USE_SimpleMicrophys),
                                              int(afdcmip.SM_Latdepend_SST), int(afdcmip.SM_LargeScaleCond),
-                                             int(afdcmip.USE_HeldSuarez), int(afdcmip.SM_MITC_SST_TYPE)])
+                                             int(afdcmip.USE_HeldSuarez), int(afdcmip.SM_MITC_SST_TYPE),
+                                             int(afdcmip.SM_PBL_Bryan)])
         out["geo.GRD_Z"] = np.ascontiguousarray(m.grd.GRD_vz[:, :, :, :, m.grd.GRD_Z])
         out["geo.PRE00"] = np.asarray(m.cnst.CONST_PRE00)
         out["state0"], out["state0_pl"] = pv.copy(), pvp.copy()
@@ -173,7 +183,7 @@ def run(ref: str, out_dir: str, case: str = "kessler"):
                 hg[k] = getattr(m.rcnf, k, -1)
             for k, v in hg.items():
                 out["hgeo." + k] = np.ascontiguousarray(np.asarray(v))
-    path = os.path.join(out_dir, f"gl03_z10_{case}.npz")
+    path = os.path.join(out_dir, f"gl03_z{VLAYERS.get(case, VL)}_{case}.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path))
 

@@ -44,12 +44,12 @@ def _dcmip_msc(geo, st, chem=True):
     return fake_msc(g, st["state0"], st["state0_pl"], af_type="DCMIP", dcmip=extra)
 
 
-@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_smlsc", "golden_dcmip21"])
+@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_smlsc", "golden_dcmip21", "golden_dcmip12bryan"])
 def test_dcmip_simple_physics_setup_from_services(pkg, case, request):
     """the simple physics passes the configuration check (with or without
-    Kessler, with moist Held-Suarez) and geo_from_msc hands the device its
-    switches, half-level heights, surface height, latitude and unit vectors;
-    the Bryan boundary layer is refused"""
+    Kessler, with moist Held-Suarez, with the Bryan boundary layer) and
+    geo_from_msc hands the device its switches, half-level heights, surface
+    height, latitude and unit vectors; RAIN_TYPE other than WARM is refused"""
     backend = __import__(pkg.__name__ + ".backend", fromlist=["geo_from_msc"])
     geo, st, _ = request.getfixturevalue(case)
     msc = _dcmip_msc(geo, st)
@@ -60,13 +60,13 @@ def test_dcmip_simple_physics_setup_from_services(pkg, case, request):
                  ("AF_dcmip_lat", "GRD_LAT")):
         assert np.array_equal(got[k], geo[w]), k
     msc = _dcmip_msc(geo, st)
-    msc.afdcmip.SM_PBL_Bryan = True
+    msc.rcnf.RAIN_TYPE = "COLD"
     with pytest.raises(NotImplementedError):
         backend.CudaDyn._check_config(msc)
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_dcmip21"])
+@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_dcmip21", "golden_dcmip12bryan"])
 def test_cudadyn_dcmip_simple_physics(pkg, case, request):
     """the reference-facing step API with the DCMIP2016 case 1-1 (Kessler,
     simple physics, chemistry) and case 2-1 (moist Held-Suarez) scheme sets:
@@ -90,8 +90,8 @@ def test_cudadyn_dcmip_simple_physics(pkg, case, request):
 
 def test_dcmip_setup_from_services(pkg, golden_kessler_chem):
     """Kessler with the terminator chemistry passes the configuration check
-    and yields the chemistry's set-up (tracer indices, column lat / lon); the
-    Bryan boundary layer or a third chemistry tracer do not"""
+    and yields the chemistry's set-up (tracer indices, column lat / lon); a
+    third chemistry tracer does not"""
     backend = __import__(pkg.__name__ + ".backend", fromlist=["geo_from_msc"])
     geo, st, _ = golden_kessler_chem
     msc = _dcmip_msc(geo, st, True)
@@ -100,11 +100,7 @@ def test_dcmip_setup_from_services(pkg, golden_kessler_chem):
     assert got["AF_dcmip_kessler"] == 1 and list(got["AF_dcmip_chem"]) == [3, 4]
     assert np.array_equal(got["AF_dcmip_lat"], geo["GRD_LAT"]) and np.array_equal(got["AF_dcmip_lon"], geo["GRD_LON"])
     assert np.array_equal(got["GRD_Z"], geo["GRD_Z"])
-    for attr in ("SM_PBL_Bryan",):
-        msc = _dcmip_msc(geo, st, True)
-        setattr(msc.afdcmip, attr, True)
-        with pytest.raises(NotImplementedError):
-            backend.CudaDyn._check_config(msc)
+
     msc = _dcmip_msc(geo, st, True)
     msc.rcnf.NCHEM_END = 5
     with pytest.raises(NotImplementedError):
