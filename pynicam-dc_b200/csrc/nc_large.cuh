@@ -521,15 +521,8 @@ __device__ __forceinline__ R hdiff_kh(R lapT, int k) {
 #define HD_NK 6
 #endif
 template <class R>
-// With HD_DBUF the staged Laplacians and rhog are double-buffered by level:
-// the next level's staging then cannot overwrite what this level's cell pass
-// still reads, so a level needs no closing barrier, and only the corner tile
-// waits for its singular-point fix.
-#ifndef HD_DBUF
-#define HD_DBUF 0
-#endif
 constexpr int hdiff2_m_smem() {
-  return ((18 + 12) * (HD_DX + 1) * (HD_DY + 1) + (HD_DBUF ? 14 : 7) * (HD_DX + 2) * (HD_DY + 2)) * (int)sizeof(R);
+  return ((18 + 12) * (HD_DX + 1) * (HD_DY + 1) + 7 * (HD_DX + 2) * (HD_DY + 2)) * (int)sizeof(R);
 }
 template <class R>
 __global__ void __launch_bounds__(HD_DX * HD_DY, NC_MINB(R, 2, 4)) k_hdiff2_m(Six<R> vt, const R* rhog,
@@ -537,8 +530,9 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, NC_MINB(R, 2, 4)) k_hdiff2_m(Si
   constexpr int PX = HD_DX + 2, PY = HD_DY + 2, NP = PX * PY, TX = HD_DX + 1, TY = HD_DY + 1, NT = TX * TY;
   extern __shared__ __align__(16) unsigned char hd_smem[];
   R* s_w = reinterpret_cast<R*>(hd_smem);   // [18][NT] triangle weights
-  R* s_t = s_w + 18 * NT;                     // [2][6][NT] triangle values of fields 4 and 5
-  R* s_fr0 = s_t + 12 * NT;                   // [(HD_DBUF ? 2 : 1)][7][NP]: the six Laplacians, then rhog
+  R* s_f = s_w + 18 * NT;                     // [6][NP] the six Laplacians
+  R* s_r = s_f + 6 * NP;                      // [NP] rhog
+  R* s_t = s_r + NP;                          // [2][6][NT] triangle values of fields 4 and 5
   const int l = (int)blockIdx.z;
   const int ntx = (cD.G - 2 + HD_DX - 1) / HD_DX;
   const int i0 = 1 + ((int)blockIdx.y % ntx) * HD_DX, j0 = 1 + ((int)blockIdx.y / ntx) * HD_DY;
@@ -562,8 +556,6 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, NC_MINB(R, 2, 4)) k_hdiff2_m(Si
     for (int m = 0; m < 18; ++m) cd[m] = P2(CG.coef_diff, m, i, j, l);
   }
   for (int k = k0; k < k1; ++k) {
-    R* s_f = s_fr0 + (HD_DBUF ? ((k - k0) & 1) * 7 * NP : 0);
-    R* s_r = s_f + 6 * NP;
     for (int p = tid; p < NP; p += blockDim.x) {
       const int ii = i0 - 1 + p % PX, jj = j0 - 1 + p / PX;
       const bool ok = ii < G && jj < G;
@@ -599,14 +591,12 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, NC_MINB(R, 2, 4)) k_hdiff2_m(Si
       }
     }
     __syncthreads();
-    if (i0 == 1 && j0 == 1) {   // singular-point fix of the (0,0) triangle, fields 4 and 5 (block-uniform)
-      if (tid < 6) {
-        const int f = tid / 3, d = tid % 3;
-        const R m0 = (R)CG.pntmask[l * 2 + 0], m1 = (R)CG.pntmask[l * 2 + 1];
-        s_t[(f * 6 + d) * NT] = s_t[(f * 6 + d) * NT] * m0 + s_t[(f * 6 + 3 + d) * NT + 1] * m1;
-      }
-      __syncthreads();
+    if (i0 == 1 && j0 == 1 && tid < 6) {   // singular-point fix of the (0,0) triangle, fields 4 and 5
+      const int f = tid / 3, d = tid % 3;
+      const R m0 = (R)CG.pntmask[l * 2 + 0], m1 = (R)CG.pntmask[l * 2 + 1];
+      s_t[(f * 6 + d) * NT] = s_t[(f * 6 + d) * NT] * m0 + s_t[(f * 6 + 3 + d) * NT + 1] * m1;
     }
+    __syncthreads();
     if (own) {
       const int q = ix(i, j, k, l);
       const int c0 = (ty + 1) * PX + (tx + 1);
@@ -641,7 +631,7 @@ __global__ void __launch_bounds__(HD_DX * HD_DY, NC_MINB(R, 2, 4)) k_hdiff2_m(Si
         out.f[4 + f][q] = -inner;
       }
     }
-    if (!HD_DBUF) __syncthreads();
+    __syncthreads();
   }
 }
 

@@ -61,9 +61,12 @@ def state_sha(s, s_pl) -> str:
 
 def geo_sha(geo: dict) -> str:
     """hash of the setup arrays (the surface-pressure diagnostic's heights,
-    keys sfc_*, are not part of the setup the step reads)"""
+    keys sfc_*, are not part of the setup the step reads; NQW_END = 0, the
+    vapour as the only water tracer, is the default the step assumes without
+    the key)"""
     h = hashlib.sha256()
-    for k in sorted(k for k in geo if not k.startswith("sfc_")):
+    default = lambda k: k == "NQW_END" and int(np.asarray(geo[k])) == 0
+    for k in sorted(k for k in geo if not k.startswith("sfc_") and not default(k)):
         h.update(k.encode())
         h.update(np.ascontiguousarray(np.asarray(geo[k])).tobytes())
     return h.hexdigest()
