@@ -243,7 +243,8 @@ int nc_mass_sum_noalloc(const double* rhog, const double* rhogq, const double* g
  * USE_Kessler, the scheme set of DCMIP2016 case 1-3; nhm/forcing/
  * mod_forcing.py:207-321, mod_af_dcmip.py:129-230, kessler.py): the handle is
  * created with "AF_dcmip_kessler_zf" (GRD_vz[..., GRD_Z], (gall_1d, gall_1d,
- * kall, lall)), "PRE00", RAIN_TYPE WARM ("NQW_END" = 2: vapour, cloud, rain)
+ * kall, lall)), "PRE00", RAIN_TYPE WARM ("NQW_END" = 2: vapour, cloud, rain; the
+ * simple physics alone also runs with RAIN_TYPE DRY, "NQW_END" = 0)
  * and optionally "AF_negative_fixer" / "AF_update_tot_dens" (the reference's
  * forcing_param, defaults 0 / 1).  Every regional column: diagnostics, dry
  * mixing ratios, the microphysics with its sedimentation sub-cycles, the

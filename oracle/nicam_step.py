@@ -1988,7 +1988,10 @@ def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_de
     sl = slice(kmin, kmax + 1)
     dt = g.dtl
     col = lambda a: a.transpose(0, 1, 3, 2).reshape(I * J * L, K)[:, sl]      # (ncol, levels kmin..kmax)
-    qv_m, qc_m, qr_m = col(q[..., 0]), col(q[..., 1]), col(q[..., 2])
+    warm = g.nqw == 3   # RAIN_TYPE WARM (vapour, cloud, rain) or DRY (vapour only)
+    qv_m = col(q[..., 0])
+    if warm:
+        qc_m, qr_m = col(q[..., 1]), col(q[..., 2])
 
     def grid(c):   # (ncol, levels kmin..kmax) -> (i, j, k, l), zero outside kmin..kmax
         full = np.zeros((I * J * L, K))
@@ -1996,7 +1999,8 @@ def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_de
         return full.reshape(I, J, L, K).transpose(0, 1, 3, 2)
     zero = np.zeros(rho.shape)
     fe, fv = zero, [zero, zero, zero]
-    fq = [zero, zero, zero] + [None] * (PROGq.shape[-1] - 3)
+    nwq = 3 if warm else 1
+    fq = [zero] * nwq + [None] * (PROGq.shape[-1] - nwq)
     precl = np.zeros(I * J * L)
     if kessler_on:
         qd = 1.0 - qv_m - qc_m - qr_m
@@ -2041,9 +2045,13 @@ def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_de
                                                   bryan=bool(sm.get("bryan", False)))
         for d, (a, b, vd) in enumerate(((0, 3, vx_td), (1, 4, vy_td), (2, 5, vz_td))):
             fv[d] = grid(((u_n * ij[a][:, None] + v_n * ij[b][:, None] - vd) / dt)[:, ::-1])
-        qc, qr = td(q[..., 1]), td(q[..., 2])
-        qd = 1.0 - qv_n - qc - qr
-        cv = qd * g.CVdry + qv_n * g.CVW[0] + qc * g.CVW[1] + qr * g.CVW[2]
+        if warm:   # mod_af_dcmip.py:486-499
+            qc, qr = td(q[..., 1]), td(q[..., 2])
+            qd = 1.0 - qv_n - qc - qr
+            cv = qd * g.CVdry + qv_n * g.CVW[0] + qc * g.CVW[1] + qr * g.CVW[2]
+        else:
+            qd = 1.0 - qv_n
+            cv = qd * g.CVdry + qv_n * g.CVW[0]
         cv_old = ein_td / tem_td
         dtem = t_n - tem_td
         dcv = cv - cv_old

@@ -244,12 +244,13 @@ class CudaDyn:
             raise NotImplementedError("cuda backend: water tracers must come first (NQW_STR = I_QV = 0), at most six")
         if getattr(r, "AF_TYPE", "NONE") == "DCMIP":
             flags = _dcmip_flags(msc)
+            rain = getattr(r, "RAIN_TYPE", "DRY")
             if not (flags.get("USE_Kessler") or flags.get("USE_SimpleMicrophys")) \
-                    or getattr(r, "RAIN_TYPE", "DRY") != "WARM" or \
+                    or rain not in ("WARM", "DRY") or (flags.get("USE_Kessler") and rain != "WARM") or \
                     (flags.get("USE_ToyChemistry") and int(getattr(r, "NCHEM_END", -1)) - int(getattr(r, "NCHEM_STR", -1)) != 1):
-                raise NotImplementedError("cuda backend: DCMIP forcing with Kessler microphysics and / or the simple "
-                                          "physics, optionally the terminator chemistry and moist Held-Suarez "
-                                          "(RAIN_TYPE WARM, two chemistry tracers)")
+                raise NotImplementedError("cuda backend: DCMIP forcing with Kessler microphysics (RAIN_TYPE WARM) "
+                                          "and / or the simple physics (WARM or DRY), optionally the terminator "
+                                          "chemistry (two tracers) and moist Held-Suarez")
         elif getattr(r, "AF_TYPE", "NONE") not in ("NONE", "HELD-SUAREZ"):
             raise NotImplementedError("cuda backend: artificial forcing NONE or HELD-SUAREZ only")
 

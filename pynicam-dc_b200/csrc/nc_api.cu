@@ -1766,7 +1766,8 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
   if (T.get("AF_dcmip_kessler_zf")) {   // DCMIP forcing (nc_forcing_step): Kessler and / or simple physics
     if (T.get("AF_hs_lat_terms")) return fail(NC_ERR_ARG, "Held-Suarez and DCMIP forcing set-ups both given");
     if (!T.get("PRE00")) return fail(NC_ERR_ARG, "AF_dcmip_kessler_zf given without PRE00");
-    if (C.nqw != 3) return fail(NC_ERR_ARG, "DCMIP forcing needs RAIN_TYPE WARM (NQW_END = 2: vapour, cloud, rain)");
+    if (C.nqw != 3 && C.nqw != 1)
+      return fail(NC_ERR_ARG, "DCMIP forcing needs RAIN_TYPE WARM (NQW_END = 2: vapour, cloud, rain) or DRY");
     if (D.kmax - D.kmin + 1 > NC_KESS_K || D.kmax - D.kmin < 1)
       return fail(NC_ERR_ARG, "DCMIP forcing: 2.." + std::to_string(NC_KESS_K) + " model levels");
     if (const nc_array* sc = T.get("AF_dcmip_schemes")) {
@@ -1781,6 +1782,7 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
       h->sm_bryan = h->sm_on && numel(sc) >= 5 && f3[4] != 0;
       if (!h->kess_on && !h->sm_on) return fail(NC_ERR_ARG, "AF_dcmip_schemes: neither Kessler nor simple physics");
     }
+    if (h->kess_on && C.nqw != 3) return fail(NC_ERR_ARG, "Kessler microphysics needs RAIN_TYPE WARM");
     if (h->dcmip_hs) TRY(up_reg(h, T, "AF_dcmip_hs_lat_terms", 1, 3, &h->dcmip_hs_lat));
     if (h->sm_on) {   // what the simple physics reads besides the state (mod_forcing.py:236-250)
       TRY(up_reg(h, T, "AF_dcmip_zh", D.KA, 1, &h->sm_zh));

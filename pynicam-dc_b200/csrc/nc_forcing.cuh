@@ -290,7 +290,7 @@ __global__ void k_forcing_dcmip(DcmipArgs a) {
     const double RHOG = P[0][p];
     rho = RHOG / cG.GSGAM2[p];
     ein = P[5][p] / RHOG;
-    for (int n = 0; n < 3; ++n) q[n] = a.Pq[n][p] / RHOG;
+    for (int n = 0; n < 3; ++n) q[n] = n < cC.nqw ? a.Pq[n][p] / RHOG : 0.0;   // DRY: vapour only
     double qd, cv;
     moist_qd_cv([&](int n) { return a.Pq[n][p] / RHOG; }, q[0], qd, cv);
     tem = ein / cv;
@@ -481,15 +481,21 @@ __global__ void k_forcing_dcmip(DcmipArgs a) {
       const double dcv = cvk - cv_old;
       fe = fe + (cv_old * dtem + tem * dcv + dcv * dtem) / dt;
     }
-    if (k >= kmin && k <= kmax && a.sm) {   // mod_af_dcmip.py:472-511 (WARM)
+    if (k >= kmin && k <= kmax && a.sm) {   // mod_af_dcmip.py:472-511 (DRY or WARM)
       const int cc = kmax - k;
       const double RHOG = P[0][p];
       const double vel[3] = {P[1][p] / RHOG, P[2][p] / RHOG, P[3][p] / RHOG};
       for (int d = 0; d < 3; ++d)
         fv[d] = (su[cc] * a.ij[d * npl + cidx] + sv[cc] * a.ij[(3 + d) * npl + cidx] - vel[d]) / dt;
       const double qvn = sq[cc];
-      const double qd = 1.0 - qvn - q[1] - q[2];
-      const double cv = qd * cC.CVdry + qvn * cC.CVW[0] + q[1] * cC.CVW[1] + q[2] * cC.CVW[2];
+      double cv;
+      if (cC.nqw == 3) {
+        const double qd = 1.0 - qvn - q[1] - q[2];
+        cv = qd * cC.CVdry + qvn * cC.CVW[0] + q[1] * cC.CVW[1] + q[2] * cC.CVW[2];
+      } else {   // RAIN_TYPE DRY
+        const double qd = 1.0 - qvn;
+        cv = qd * cC.CVdry + qvn * cC.CVW[0];
+      }
       fq[0] = fq[0] + (qvn - q[0]) / dt;
       const double cv_old = ein / tem;
       const double dtem = st[cc] - tem;
@@ -510,7 +516,7 @@ __global__ void k_forcing_dcmip(DcmipArgs a) {
     P[5][p] = P[5][p] + dt * fe * rho * gs;
     double rhog = P[0][p];
     for (int n = 0; n < a.nq; ++n) {
-      const double f = n < 3 ? fq[n] : (n == a.n_cl ? fcl : (n == a.n_cl2 ? fcl2 : 0.0));
+      const double f = n < cC.nqw ? fq[n] : (n == a.n_cl ? fcl : (n == a.n_cl2 ? fcl2 : 0.0));
       double frhogq = f * rho * gs;
       double* Q = a.Pq[n];
       if (a.negative_fixer) {

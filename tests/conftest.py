@@ -120,6 +120,13 @@ def golden_dcmip12bryan():
 
 
 @pytest.fixture(scope="session")
+def golden_smdry():
+    """the simple physics with RAIN_TYPE DRY (vapour the only water tracer) run
+    by the reference (make_kessler.py --case smdry)"""
+    return _dcmip_fixture("smdry")
+
+
+@pytest.fixture(scope="session")
 def golden_smlsc():
     """the simple physics alone with its large-scale condensation and the
     constant sea-surface temperature, run by the reference

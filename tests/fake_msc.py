@@ -104,7 +104,7 @@ def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_
             grd.GRD_zs = np.asarray(dcmip["GRD_zsfc"])[:, :, None, :, None]
             gmtr.GMTR_p_IX, gmtr.GMTR_p_IY, gmtr.GMTR_p_IZ, gmtr.GMTR_p_JX, gmtr.GMTR_p_JY, gmtr.GMTR_p_JZ = range(2, 8)
             assert np.array_equal(gmtr.GMTR_p[:, :, 0, :, 2:8], dcmip["GMTR_p_IJ"])
-        rcnf.RAIN_TYPE = "WARM"
+        rcnf.RAIN_TYPE = "WARM" if int(np.asarray(g.get("NQW_END", 0))) == 2 else "DRY"
         m.afdcmip = NS(USE_Kessler=bool(fl[0]), USE_SimpleMicrophys=bool(fl[1]), SM_Latdepend_SST=bool(fl[2]),
                        SM_LargeScaleCond=bool(fl[3]), SM_PBL_Bryan=bool(fl[6]), USE_ToyChemistry=chem,
                        USE_HeldSuarez=bool(fl[4]), SM_MITC_SST_TYPE=fl[5])

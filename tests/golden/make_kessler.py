@@ -20,7 +20,8 @@ large-scale condensation: the scheme set of DCMIP2016 case 1-1) to Kessler
 and the chemistry; --case smlsc runs the simple physics alone with its
 large-scale condensation and the constant sea-surface temperature; --case dcmip21 the moist
 Held-Suarez scheme set of DCMIP2016 case 2-1; --case dcmip12bryan the
-tropical-cyclone scheme set with the Bryan boundary layer.  They
+tropical-cyclone scheme set with the Bryan boundary layer; --case smdry the
+simple physics with RAIN_TYPE DRY (vapour the only water tracer).  They
 also store the half-level heights, the surface height and the column unit
 vectors the simple physics reads.
 
@@ -55,12 +56,17 @@ CASES = {
     # the DCMIP2016 case 1-2 (tropical cyclone) scheme set with the Bryan boundary layer
     "dcmip12bryan": ({"USE_Kessler": True, "USE_SimpleMicrophys": True, "SM_Latdepend_SST": False,
                       "SM_LargeScaleCond": False, "SM_PBL_Bryan": True}, False),
+    # the simple physics with RAIN_TYPE DRY (vapour the only water tracer; the DCMIP2016 DRY presets)
+    "smdry": ({"USE_Kessler": False, "USE_SimpleMicrophys": True, "SM_Latdepend_SST": True,
+               "SM_LargeScaleCond": True}, False),
     # DCMIP2016 case 2-1, moist Held-Suarez (the SET_DCMIP2016_21 scheme set)
     "dcmip21": ({"USE_Kessler": True, "USE_SimpleMicrophys": True, "SM_Latdepend_SST": False,
                  "SM_LargeScaleCond": False, "USE_HeldSuarez": True}, False),
 }
 
 
+# RAIN_TYPE of a case (WARM where absent): the simple physics alone also runs dry
+RAIN = {"smdry": "DRY"}
 # the Bryan boundary layer mixes below 1 km: 30 layers put the lowest ones there
 VLAYERS = {"dcmip12bryan": 30}
 
@@ -73,7 +79,8 @@ def run(ref: str, out_dir: str, case: str = "kessler"):
         case_dir = os.path.join(tmp, "kessler")
         vl = VLAYERS.get(case, VL)
         MG.prep(ref, case_dir, GL, vl, ZTOP)
-        c = toml.loads(MG.model_toml(ref, GL, vl, DTL, GAMMA, NSTEPS, "WARM"))
+        rain = RAIN.get(case, "WARM")
+        c = toml.loads(MG.model_toml(ref, GL, vl, DTL, GAMMA, NSTEPS, rain))
         c["runconfparam"]["AF_TYPE"] = "DCMIP"
         c["forcing_dcmip_param"] = dict(flags)
         if chem:
@@ -116,13 +123,14 @@ def run(ref: str, out_dir: str, case: str = "kessler"):
         for k, v in flags.items():
             assert getattr(afdcmip, k) == v, k
         assert afdcmip.USE_ToyChemistry == chem and afdcmip.SM_MITC_SST_TYPE == 1
-        assert m.rcnf.NQW_END == 2 and (m.rcnf.I_QV, m.rcnf.I_QC, m.rcnf.I_QR) == (0, 1, 2)
+        nw = 3 if rain == "WARM" else 1   # vapour, cloud, rain / vapour only
+        assert m.rcnf.NQW_END == nw - 1 and m.rcnf.I_QV == 0
         assert not m.frc.NEGATIVE_FIXER and m.frc.UPDATE_TOT_DENS
         pv, pvp = m.prgv.PRG_var, m.prgv.PRG_var_pl
         kk = pv.shape[2]
         lat, lon = m.grd.GRD_LAT[:, :, 0, :], m.grd.GRD_LON[:, :, 0, :]
         latp, lonp = m.grd.GRD_LAT_pl[:, 0, :], m.grd.GRD_LON_pl[:, 0, :]
-        for n in range(3):
+        for n in range(nw):
             sc = MG.WATER_SCALE[n]
             pv[..., 6 + n] = pv[..., 0] * sc * np.moveaxis(MG.tracer_field(lat, lon, kk), -1, 2)
             pvp[..., 6 + n] = pvp[..., 0] * sc * np.moveaxis(MG.tracer_field(latp, lonp, kk), -1, 1)

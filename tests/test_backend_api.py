@@ -44,7 +44,8 @@ def _dcmip_msc(geo, st, chem=True):
     return fake_msc(g, st["state0"], st["state0_pl"], af_type="DCMIP", dcmip=extra)
 
 
-@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_smlsc", "golden_dcmip21", "golden_dcmip12bryan"])
+@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_smlsc", "golden_dcmip21", "golden_dcmip12bryan",
+                                  "golden_smdry"])
 def test_dcmip_simple_physics_setup_from_services(pkg, case, request):
     """the simple physics passes the configuration check (with or without
     Kessler, with moist Held-Suarez, with the Bryan boundary layer) and
@@ -66,7 +67,8 @@ def test_dcmip_simple_physics_setup_from_services(pkg, case, request):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_dcmip21", "golden_dcmip12bryan"])
+@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_dcmip21", "golden_dcmip12bryan",
+                                  "golden_smdry"])
 def test_cudadyn_dcmip_simple_physics(pkg, case, request):
     """the reference-facing step API with the DCMIP2016 case 1-1 (Kessler,
     simple physics, chemistry) and case 2-1 (moist Held-Suarez) scheme sets:

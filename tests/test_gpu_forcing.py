@@ -152,7 +152,8 @@ def test_terminator_chemistry_setup_is_checked(pkg, golden_kessler_chem):
             pkg.NicamCuda(g, graph=False).close()
 
 
-@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_smlsc", "golden_dcmip21", "golden_dcmip12bryan"])
+@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_smlsc", "golden_dcmip21", "golden_dcmip12bryan",
+                                  "golden_smdry"])
 def test_simple_physics_vs_reference(pkg, case, request):
     """DCMIP forcing with the simple physics on the device against the
     reference's two steps (with Kessler and the chemistry as in DCMIP2016 case

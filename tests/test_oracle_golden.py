@@ -95,7 +95,8 @@ def test_oracle_terminator_chemistry_matches_reference(golden_kessler_chem):
         assert np.array_equal(precip, pr[f"precip{n}"]), n
 
 
-@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_smlsc", "golden_dcmip21", "golden_dcmip12bryan"])
+@pytest.mark.parametrize("case", ["golden_dcmip11", "golden_smlsc", "golden_dcmip21", "golden_dcmip12bryan",
+                                  "golden_smdry"])
 def test_oracle_simple_physics_matches_reference(case, request):
     """dynamics step + DCMIP forcing with the simple physics (with Kessler and
     the chemistry as in DCMIP2016 case 1-1; alone with the large-scale
