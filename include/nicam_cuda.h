@@ -421,7 +421,9 @@ int nc_trc_step_lin(nc_handle* h, int32_t mode, const double* x0, const double* 
                     const double* in_pl, double* out, double* out_pl, void* stream);
 
 /* The model time of an offline-advection handle's prescribed winds
- * (setup entry "trcadv"; it starts at 0 and every step adds dtl).  Re-running
+ * (setup entry "trcadv": 1 for the DCMIP 1-1 deformational flow, 2 for the
+ * DCMIP 1-2 Hadley-like circulation, mod_af_trcadv.py:22-149; the time
+ * starts at 0 and every step adds dtl).  Re-running
  * steps from stored states (as the tracer-transport adjoint does) needs the
  * time of each state set back.  NC_ERR_STATE for a handle without
  * prescribed winds; synchronous. */

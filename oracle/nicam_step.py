@@ -2101,11 +2101,36 @@ def forcing_step_kessler(g, prg, prg_pl, zf, negative_fixer=False, update_tot_de
 TRC_A, TRC_RD, TRC_G, TRC_PI = 6371220.0, 287.0, 9.80616, 3.141592653589793238   # mod_af_trcadv.py:14-19
 
 
-def trcadv_winds(time, lon, lat, zf, zh):
+def trcadv_winds12(time, lon, lat, zf, zh):
+    """nhm/forcing/mod_af_trcadv.py:100-149 test12_velocity (DCMIP2012 test
+    1-2, Hadley-like meridional circulation) with Sp_Unit_East /
+    Sp_Unit_North: winds (vx, vy, vz) at full levels and w at half levels"""
+    tau, u0, w0, T0 = 1.0 * 86400.0, 40.0, 0.15, 300.0
+    H = TRC_RD * T0 / TRC_G
+    K, ztop, p0, pi = 5.0, 12.0e3, 1000.e2, TRC_PI
+    rho0 = p0 / (TRC_RD * T0)
+    rho = p0 * np.exp(-zf / H) / (TRC_RD * T0)
+    u = u0 * np.cos(lat)
+    v = (-(rho0 / rho) * TRC_A * w0 * pi / (K * ztop) * np.cos(lat) * np.sin(K * lat)
+         * np.cos(pi * zf / ztop) * np.cos(pi * time / tau))
+    e0, e1, e2 = -np.sin(lon), np.cos(lon), np.zeros_like(lon)
+    n0, n1, n2 = -np.sin(lat) * np.cos(lon), -np.sin(lat) * np.sin(lon), np.cos(lat)
+    vx = e0 * u + n0 * v
+    vy = e1 * u + n1 * v
+    vz = e2 * u + n2 * v
+    rho = p0 * np.exp(-zh / H) / (TRC_RD * T0)
+    w = ((rho0 / rho) * (w0 / K) * (-2.0 * np.sin(K * lat) * np.sin(lat) + K * np.cos(lat) * np.cos(K * lat))
+         * np.sin(pi * zh / ztop) * np.cos(pi * time / tau))
+    return vx, vy, vz, w
+
+
+def trcadv_winds(time, lon, lat, zf, zh, case="1-1"):
     """nhm/forcing/mod_af_trcadv.py:22-97 test11_velocity with
     Sp_Unit_East / Sp_Unit_North (:151-171): winds (vx, vy, vz) at full levels
     and w at half levels at model time ``time``; ``lon``/``lat`` broadcast
-    against the heights."""
+    against the heights.  ``case`` "1-2" takes test12_velocity instead."""
+    if case == "1-2":
+        return trcadv_winds12(time, lon, lat, zf, zh)
     tau = 12.0 * 86400.0
     u0 = 2.0 * TRC_PI * TRC_A / tau
     k0 = 10.0 * TRC_A / tau
@@ -2133,7 +2158,7 @@ def trcadv_winds(time, lon, lat, zf, zh):
     return vx, vy, vz, w
 
 
-def trcadv_step(g, prg, prg_pl, time, lon, lat, zf, zh, lon_pl, lat_pl, zf_pl, zh_pl):
+def trcadv_step(g, prg, prg_pl, time, lon, lat, zf, zh, lon_pl, lat_pl, zf_pl, zh_pl, case="1-1"):
     """Dyn.dynamics_step for integ_type TRCADV (mod_dynamics.py:2030-2085 and
     the marshal-out :2690-2727): the tracers are advected with the current
     PROG as the mean state (rhog_in = PROG0 rhog, no density tendency), then
@@ -2152,7 +2177,7 @@ def trcadv_step(g, prg, prg_pl, time, lon, lat, zf, zh, lon_pl, lat_pl, zf_pl, z
                      np.zeros_like(rhog_in), np.zeros_like(rhog_in_pl), g.dtl)
     for P, lo, la, z, zhh in ((PROG, lon[:, :, None, :], lat[:, :, None, :], zf, zh),
                               (PROG_pl, lon_pl[:, None, :], lat_pl[:, None, :], zf_pl, zh_pl)):
-        vx, vy, vz, w = trcadv_winds(time, lo, la, z, zhh)
+        vx, vy, vz, w = trcadv_winds(time, lo, la, z, zhh, case)
         P[..., I_RHOGVX] = vx * P[..., I_RHOG]
         P[..., I_RHOGVY] = vy * P[..., I_RHOG]
         P[..., I_RHOGVZ] = vz * P[..., I_RHOG]

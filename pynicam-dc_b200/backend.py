@@ -115,6 +115,8 @@ def geo_from_msc(msc) -> dict:
         K0 = m.adm.ADM_K0
         grd = m.grd
         g["integ_type"] = "TRCADV"
+        if getattr(m.rcnf, "DCTEST_case", "1-1") == "1-2":   # the Hadley-like circulation's winds
+            g["trcadv_case"] = "1-2"
         g["GRD_LON"] = np.ascontiguousarray(grd.GRD_LON[:, :, K0, :])
         g["GRD_LAT"] = np.ascontiguousarray(grd.GRD_LAT[:, :, K0, :])
         g["GRD_LON_pl"] = np.ascontiguousarray(grd.GRD_LON_pl[:, K0, :])
@@ -226,8 +228,8 @@ class CudaDyn:
     def _check_config(msc):
         r = msc.rcnf
         if msc.tim.TIME_integ_type == "TRCADV":
-            if (getattr(r, "DCTEST_type", "") != "Traceradvection" or getattr(r, "DCTEST_case", "") != "1-1"):
-                raise NotImplementedError("cuda backend: offline tracer advection with the DCMIP 1-1 winds only")
+            if (getattr(r, "DCTEST_type", "") != "Traceradvection" or getattr(r, "DCTEST_case", "") not in ("1-1", "1-2")):
+                raise NotImplementedError("cuda backend: offline tracer advection with the DCMIP 1-1 or 1-2 winds")
         elif msc.tim.TIME_integ_type != "RK3":
             raise NotImplementedError("cuda backend: RK3 time integration or TRCADV only")
         if r.TRC_ADV_TYPE != "MIURA2004" or not r.THUBURN_LIM:

@@ -392,6 +392,7 @@ struct nc_handle {
   long long hist_nstep = 0;
   // offline tracer advection (integ_type TRCADV, DCMIP2012 test 1-1 winds)
   bool trcadv = false;
+  bool trcadv_hadley = false;   // the DCMIP 1-2 winds instead of 1-1
   double* trc_time = nullptr;       // model time of the prescribed winds (device scalar)
   const double *trc_lon = nullptr, *trc_lat = nullptr, *trc_zf = nullptr, *trc_zh = nullptr;
   const double *trc_lon_pl = nullptr, *trc_lat_pl = nullptr, *trc_zf_pl = nullptr, *trc_zh_pl = nullptr;
@@ -1088,6 +1089,7 @@ static int run_step(nc_handle* h) {
     for (int v = 0; v < 6; ++v) w.P.v[v] = RG<R>(h->P[v]);
     w.lon = h->trc_lon; w.lat = h->trc_lat; w.zf = h->trc_zf; w.zh = h->trc_zh; w.time = h->trc_time;
     w.a = 6371220.0; w.Rd = 287.0; w.g = 9.80616; w.pi = 3.141592653589793238;
+    w.hadley = h->trcadv_hadley;
     k_trcadv_winds<<<npt_blocks, kBlock, 0, s>>>(w, 0);
     TRY(check_launch(h, "trcadv_winds"));
     for (int v = 0; v < 6; ++v) w.P.v[v] = PL<R>(h->P[v]);
@@ -1669,8 +1671,10 @@ static int create_impl(const nc_array* arrays, int32_t narrays, nc_handle* h) {
     for (int n = 0; n < NC_MAXQW; ++n) C.CVW[n] = n < C.nqw ? ((const double*)cvw->data)[n] : 0.0;
     if (T.get("trcadv")) {
       double f;
-      TRY(scalar(T, "trcadv", f));
+      TRY(scalar(T, "trcadv", f));   // 1: DCMIP 1-1 winds, 2: DCMIP 1-2 winds
+      if (f != 0.0 && f != 1.0 && f != 2.0) return fail(NC_ERR_ARG, "trcadv must be 0, 1 (DCMIP 1-1) or 2 (1-2)");
       h->trcadv = (f != 0.0);
+      h->trcadv_hadley = (f == 2.0);
     }
     const nc_array* ss = T.get("sstep");
     if (!ss || numel(ss) > 4 || (numel(ss) < 1 && !h->trcadv)) return fail(NC_ERR_ARG, "missing sstep");

@@ -550,7 +550,25 @@ struct TrcWindArgs {
   const double *zf, *zh;      // full / half-level height: regional [l][k][j][i], pole [g][k][l]
   const double* time;         // model time of the winds (device scalar)
   double a, Rd, g, pi;        // the test's constants (mod_af_trcadv.py:14-19)
+  int hadley;                 // DCMIP 1-2 (test12_velocity) instead of 1-1
 };
+
+// DCMIP2012 test 1-2, Hadley-like meridional circulation (nhm/forcing/
+// mod_af_trcadv.py:100-149 test12_velocity): the full-level winds (u, v) and
+// the half-level w at one point
+__device__ __forceinline__ void trcadv12(double time, double lat, double zf, double zh, double a, double Rd, double g,
+                                         double pi, double& u, double& v, double& ww) {
+  const double tau = 1.0 * 86400.0, u0 = 40.0, w0 = 0.15, T0 = 300.0;
+  const double H = Rd * T0 / g;
+  const double K = 5.0, ztop = 12.0e3, p0 = 1000.e2;
+  const double rho0 = p0 / (Rd * T0);
+  double rho = p0 * exp(-zf / H) / (Rd * T0);
+  u = u0 * cos(lat);
+  v = -(rho0 / rho) * a * w0 * pi / (K * ztop) * cos(lat) * sin(K * lat) * cos(pi * zf / ztop) * cos(pi * time / tau);
+  rho = p0 * exp(-zh / H) / (Rd * T0);
+  ww = (rho0 / rho) * (w0 / K) * (-2.0 * sin(K * lat) * sin(lat) + K * cos(lat) * cos(K * lat)) *
+       sin(pi * zh / ztop) * cos(pi * time / tau);
+}
 
 __global__ void k_trcadv_time(double* time, double dt) { *time = *time + dt; }
 
@@ -574,6 +592,20 @@ __global__ void k_trcadv_winds(TrcWindArgs<R> w, int pole) {
   }
   const double time = *w.time;
   const double a = w.a, pi = w.pi;
+  if (w.hadley) {
+    const double lon = w.lon[c2], lat = w.lat[c2];
+    double u, v, ww;
+    trcadv12(time, lat, w.zf[p], w.zh[p], a, w.Rd, w.g, pi, u, v, ww);
+    const double e0 = -sin(lon), e1 = cos(lon), e2 = 0.0;
+    const double n0 = -sin(lat) * cos(lon), n1 = -sin(lat) * sin(lon), n2 = cos(lat);
+    const double vx = e0 * u + n0 * v, vy = e1 * u + n1 * v, vz = e2 * u + n2 * v;
+    const double rg = (double)w.P.v[0][p];
+    w.P.v[1][p] = vx * rg;
+    w.P.v[2][p] = vy * rg;
+    w.P.v[3][p] = vz * rg;
+    w.P.v[4][p] = ww * rg;
+    return;
+  }
   const double tau = 12.0 * 86400.0;
   const double u0 = 2.0 * pi * a / tau;
   const double k0 = 10.0 * a / tau;

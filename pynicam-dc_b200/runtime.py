@@ -275,7 +275,8 @@ def setup_table(geo: dict) -> dict:
     t["GMTR_p_RAREA"] = np.ascontiguousarray(np.asarray(geo["GMTR_p"])[..., 1:2], np.float64)
     trcadv = str(np.asarray(geo.get("integ_type", "RK3"))) == "TRCADV"
     if trcadv:   # offline tracer advection: the coordinates the prescribed winds are computed from
-        t["trcadv"] = np.asarray(1.0, np.float64)
+        # 1: the DCMIP 1-1 winds, 2: the DCMIP 1-2 winds (Hadley-like circulation)
+        t["trcadv"] = np.asarray(2.0 if str(np.asarray(geo.get("trcadv_case", "1-1"))) == "1-2" else 1.0, np.float64)
         G, L = int(_scalar(geo["gall_1d"])), int(_scalar(geo["lall"]))
         for k in ("GRD_LON", "GRD_LAT"):
             t[k] = np.ascontiguousarray(np.asarray(geo[k], np.float64).reshape(G, G, 1, L))

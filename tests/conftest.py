@@ -185,6 +185,14 @@ def golden_trcadv():
 
 
 @pytest.fixture(scope="session")
+def golden_trcadv12():
+    """the same for DCMIP 1-2 (Hadley-like circulation; make_trcadv.py --case
+    1-2): the setup also carries the key trcadv_case"""
+    from make_golden import load
+    return load(os.path.join(GOLDEN, "gl03_z10_trcadv12.npz"))
+
+
+@pytest.fixture(scope="session")
 def golden_hist():
     """the reference's own history diagnostics of the gl03_z10_trc run
     (make_hist.py): the extra setup they read (keys without the geo. prefix:

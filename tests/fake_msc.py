@@ -13,7 +13,7 @@ import numpy as np
 
 def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_type: str = "RK3",
              coords: dict = None, hist: dict = None, io_names=None, dcmip: dict = None,
-             numf_opts: dict = None):
+             numf_opts: dict = None, dctest_case: str = "1-1"):
     g = {k: np.asarray(v) for k, v in geo.items()}
     sc = lambda k: g[k].reshape(-1)[0].item()
     adm = NS(ADM_kall=int(sc("kall")), ADM_kmin=int(sc("kmin")), ADM_kmax=int(sc("kmax")),
@@ -65,7 +65,7 @@ def fake_msc(geo: dict, state, state_pl, af_type: str = "NONE", lat=None, integ_
     rcnf = NS(NON_HYDRO_ALPHA=sc("alpha"), CVW=g["CVW"], NQW_STR=0, I_QV=0, NQW_END=int(np.asarray(g.get("NQW_END", 0))), AF_TYPE=af_type, TRC_ADV_TYPE="MIURA2004",
               THUBURN_LIM=True, DYN_DIV_NUM=1,
               DCTEST_type="Traceradvection" if integ_type == "TRCADV" else "",
-              DCTEST_case="1-1" if integ_type == "TRCADV" else "")
+              DCTEST_case=dctest_case if integ_type == "TRCADV" else "")
     tim = NS(TIME_dtl=sc("dtl"), TIME_dts=sc("dts"), TIME_integ_type=integ_type, TIME_cstep=0)
     if hist is not None:
         for k in ("I_QV", "I_QC", "I_QR", "I_QI", "I_QS", "I_QG"):

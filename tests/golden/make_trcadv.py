@@ -9,7 +9,9 @@ winds of the next time (mod_dynamics.py:2030-2085, nhm/forcing/mod_forcing.py
 forcing_update, nhm/forcing/mod_af_trcadv.py test11_velocity).  Grid level 3,
 10 EVEN layers to 12 km (the tracer case's vertical grid type), dtl 1200 s.
 Stores the setup arrays, the column lon/lat, the full- and half-level heights
-the wind formulas read, and the states before and after three steps.
+the wind formulas read, and the states before and after three steps.  With
+--case 1-2 the same for test 1-2 (Hadley-like meridional circulation, one
+tracer layer; test12_velocity), written to gl03_z10_trcadv12.npz.
 
     python tests/golden/make_trcadv.py --ref <pyNICAM-DC checkout> --out tests/golden
 """
@@ -31,7 +33,7 @@ import make_golden as MG  # noqa: E402
 GL, VL, ZTOP, DTL, GAMMA, NSTEPS = 3, 10, 12000.0, 1200.0, 7.68e17, 3
 
 
-def run(ref: str, out_dir: str):
+def run(ref: str, out_dir: str, case: str = "1-1"):
     import toml
     with tempfile.TemporaryDirectory() as tmp:
         case_dir = os.path.join(tmp, "tr")
@@ -39,8 +41,8 @@ def run(ref: str, out_dir: str):
         c = toml.loads(MG.model_toml(ref, GL, VL, DTL, GAMMA, NSTEPS))
         c["timeparam"]["integ_type"] = "TRCADV"
         c["grdparam"]["topo_io_mode"] = "NONE"
-        c["runconfparam"].update(CHEM_TYPE="PASSIVE", DCTEST_type="Traceradvection", DCTEST_case="1-1")
-        c["dycoretestparam"].update(init_type="Traceradvection", test_case="1-1")
+        c["runconfparam"].update(CHEM_TYPE="PASSIVE", DCTEST_type="Traceradvection", DCTEST_case=case)
+        c["dycoretestparam"].update(init_type="Traceradvection", test_case=case)
         c["chemvarparam"] = {"CHEM_TRC_vmax": 4}
         with open(os.path.join(case_dir, "case", "config", "nhm_jw.toml"), "w") as f:
             f.write(toml.dumps(c))
@@ -87,11 +89,13 @@ def run(ref: str, out_dir: str):
         out["geo.GRD_Z_pl"] = np.ascontiguousarray(g.GRD_vz_pl[:, :, :, g.GRD_Z])
         out["geo.GRD_ZH_pl"] = np.ascontiguousarray(g.GRD_vz_pl[:, :, :, g.GRD_ZH])
         out["geo.integ_type"] = np.array("TRCADV")
+        if case != "1-1":
+            out["geo.trcadv_case"] = np.array(case)
         out["state0"], out["state0_pl"] = pv.copy(), pvp.copy()
         for s in range(NSTEPS):
             nic.run(1)
             out[f"state{s + 1}"], out[f"state{s + 1}_pl"] = m.prgv.PRG_var.copy(), m.prgv.PRG_var_pl.copy()
-    path = os.path.join(out_dir, "gl03_z10_trcadv.npz")
+    path = os.path.join(out_dir, "gl03_z10_trcadv.npz" if case == "1-1" else "gl03_z10_trcadv12.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path))
 
@@ -100,5 +104,7 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", required=True, help="root of a pyNICAM-DC checkout")
     ap.add_argument("--out", default=HERE)
+    ap.add_argument("--case", default="1-1", choices=["1-1", "1-2"],
+                    help="DCMIP2012 test: 1-1 deformational flow, 1-2 Hadley-like circulation")
     args = ap.parse_args()
-    run(os.path.abspath(args.ref), os.path.abspath(args.out))
+    run(os.path.abspath(args.ref), os.path.abspath(args.out), args.case)

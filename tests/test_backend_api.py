@@ -226,13 +226,17 @@ def test_cudadyn_held_suarez_forcing(pkg, golden_hs):
 
 
 @pytest.mark.gpu
-def test_cudadyn_offline_tracer_advection(pkg, golden_trcadv):
+@pytest.mark.parametrize("case", ["golden_trcadv", "golden_trcadv12"])
+def test_cudadyn_offline_tracer_advection(pkg, case, request):
+    """three offline-advection steps through the step API, with the DCMIP 1-1
+    and the 1-2 winds"""
     from conftest import TRC_COORDS
-    geo, st = golden_trcadv
+    geo, st = request.getfixturevalue(case)
     geo = dict(geo)
     coords = {k: geo.pop(k) for k in TRC_COORDS}
     geo.pop("integ_type")
-    msc = fake_msc(geo, st["state0"], st["state0_pl"], integ_type="TRCADV", coords=coords)
+    dcase = str(geo.pop("trcadv_case", "1-1"))
+    msc = fake_msc(geo, st["state0"], st["state0_pl"], integ_type="TRCADV", coords=coords, dctest_case=dcase)
     dyn = pkg.CudaDyn(msc=msc)
     try:
         dyn.run_timeloop_chunk(msc, 3)

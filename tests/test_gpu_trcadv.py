@@ -47,6 +47,21 @@ def test_trcadv_three_steps_vs_reference(pkg, golden_trcadv):
         assert np.array_equal(s[..., 0], st["state0"][..., 0])
 
 
+def test_trcadv12_three_steps_vs_reference(pkg, golden_trcadv12):
+    """the DCMIP 1-2 winds (Hadley-like circulation, test12_velocity; exp, sin
+    and cos are CUDA's): the first step's tracers bit for bit (they move with
+    the initial winds), every state within 1e-12 relative L2 per prognostic,
+    graph replay equal to eager launches"""
+    geo, st = golden_trcadv12
+    outs = _run(pkg, geo, st, graph=False)
+    assert np.array_equal(outs[0][0][..., 6:], st["state1"][..., 6:]), "step 1 tracers (initial winds)"
+    for n, (s, sp) in enumerate(outs, start=1):
+        assert max(_rel_l2(s, st[f"state{n}"])) <= 1e-12, (n, _rel_l2(s, st[f"state{n}"]))
+        assert max(_rel_l2(sp, st[f"state{n}_pl"])) <= 1e-12, (n, _rel_l2(sp, st[f"state{n}_pl"]))
+    for (x, xp), (y, yp) in zip(outs, _run(pkg, geo, st, graph=True)):
+        assert np.array_equal(x, y) and np.array_equal(xp, yp)
+
+
 def test_trcadv_graph_equals_eager(pkg, golden_trcadv):
     geo, st = golden_trcadv
     a = _run(pkg, geo, st, graph=False)

@@ -213,6 +213,24 @@ def test_held_suarez_fixture_is_forced(golden, golden_hs):
     assert d > 0.0
 
 
+def test_oracle_trcadv12_matches_reference_three_steps(golden_trcadv12):
+    """offline tracer advection with the DCMIP 1-2 winds (Hadley-like
+    circulation, test12_velocity) against the reference's own run"""
+    from conftest import TRC_COORDS
+    geo, st = golden_trcadv12
+    geo = dict(geo)
+    co = [geo.pop(k) for k in TRC_COORDS]
+    assert str(geo.pop("integ_type")) == "TRCADV" and str(geo.pop("trcadv_case")) == "1-2"
+    G = O.Geo(geo)
+    s, sp = st["state0"], st["state0_pl"]
+    for n in (1, 2, 3):
+        s, sp = O.trcadv_step(G, s, sp, n * G.dtl, *co, case="1-2")
+        assert np.array_equal(s, st[f"state{n}"]), f"step {n} regional"
+        assert np.array_equal(sp, st[f"state{n}_pl"]), f"step {n} pole"
+    assert np.abs(st["state3"][..., 7] - st["state0"][..., 7]).max() > 1e-3   # the tracer layer moved
+    assert np.abs(st["state2"][..., 4] - st["state1"][..., 4]).max() > 0.0    # w is time-dependent
+
+
 def test_oracle_trcadv_matches_reference_three_steps(golden_trcadv):
     """offline tracer advection (integ_type TRCADV, DCMIP 1-1 winds) against
     the reference's own run (tests/golden/make_trcadv.py)"""
