@@ -400,6 +400,19 @@ int nc_laplacian(nc_handle* h, int32_t transpose, const double* q, const double*
 int nc_divergence(nc_handle* h, int32_t transpose, double* v, double* v_pl, double* y, double* y_pl, void* stream);
 int nc_gradient(nc_handle* h, int32_t transpose, double* q, double* q_pl, double* g, double* g_pl, void* stream);
 
+/* The Kh-weighted horizontal diffusion of the hyperdiffusion's scalar pass
+ * (kernels/oprtdiffusion.py, OPRT_diffusion; mod_numfilter.py:1219-1240)
+ * after the halo exchange, and its adjoint, float64, on device buffers in the
+ * library's field layout ordered on the caller's stream: y = Dk(C(s)) on
+ * interior cells and the pole point (other cells zero) for the coefficient
+ * field kh (rhog x CVdry x Kh or rhog x hdiff_fact_rho x Kh in the step; given
+ * for every point and pole point, held fixed); transpose = 1 reads y and
+ * writes s = C^T Dk^T y.  The buffer written must not alias the one read; the
+ * forward allocates a scratch copy in the handle on its first call, the
+ * adjoint a six-field scratch and adds with atomics in its exchange. */
+int nc_diffusion(nc_handle* h, int32_t transpose, const double* kh, const double* kh_pl, double* s, double* s_pl,
+                 double* y, double* y_pl, void* stream);
+
 /* nc_trc_step_lin: the tracer advection of one step (mod_src_tracer.py:
  * 83-1228 as the step runs it: vertical step, horizontal step with the
  * MIURA2004 face values and the horizontal Thuburn limiter of 2190-2605,

@@ -238,6 +238,94 @@ class Gradient(torch.autograd.Function):
         return Gradient.forward(ctx, ctx.core, dq, dq_pl)
 
 
+class Diffusion(torch.autograd.Function):
+    """(y, y_pl) = Dk(C(s, s_pl)): halo exchange then the kh-weighted
+    diffusion of the hyperdiffusion's scalar pass (kernels/oprtdiffusion.py);
+    linear in s, with the coefficient field (kh, kh_pl) held fixed (no
+    cotangent for it)"""
+
+    @staticmethod
+    def forward(ctx, core, s, s_pl, kh, kh_pl):
+        kh, kh_pl = _c(kh.detach()), _c(kh_pl.detach())
+        y, y_pl = torch.empty_like(s), torch.empty_like(s_pl)
+        core.diffusion(kh, kh_pl, _c(s), _c(s_pl), y, y_pl)
+        ctx.core = core
+        ctx.save_for_backward(kh, kh_pl)
+        return y, y_pl
+
+    @staticmethod
+    def backward(ctx, gy, gy_pl):
+        core = ctx.core
+        kh, kh_pl = ctx.saved_tensors
+        gy = torch.zeros_like(kh) if gy is None else _c(gy)
+        gy_pl = torch.zeros_like(kh_pl) if gy_pl is None else _c(gy_pl)
+        g, g_pl = torch.empty_like(gy), torch.empty_like(gy_pl)
+        core.diffusion(kh, kh_pl, g, g_pl, gy, gy_pl, transpose=True)
+        return None, g, g_pl, None, None
+
+
+def diffusion(core, s, s_pl, kh, kh_pl):
+    return Diffusion.apply(core, s, s_pl, kh, kh_pl)
+
+
+def hdiff_setup(geo: dict, device="cuda") -> dict:
+    """the fixed inputs of ``hyperdiffusion`` from a setup dict (DIRECT Kh):
+    Kh, CVdry, hdiff_fact_rho, the C2W weights (device layout, two
+    components) and the unit-radius position vectors GRD_x / rscale of the
+    regional points and pole points"""
+    sc = lambda k: float(np.asarray(geo[k]).reshape(-1)[0])
+    c2w = np.asarray(geo["VMTR_C2Wfact"], np.float64)
+    c2w_pl = np.asarray(geo["VMTR_C2Wfact_pl"], np.float64)
+    gx = np.asarray(geo["GRD_x"], np.float64)[:, :, 0, :, :]               # (i, j, l, 3)
+    gx_pl = np.asarray(geo["GRD_x_pl"], np.float64)[:, 0, :, :]            # (g, l, 3)
+    f = {"Kh": sc("Kh_coef"), "CVdry": sc("CVdry"), "hfr": sc("hdiff_fact_rho"), "rscale": sc("rscale"),
+         "kmin": int(sc("kmin"))}
+    f["c2w"] = torch.stack([to_device_layout(c2w[..., c], device) for c in range(2)])
+    f["c2w_pl"] = torch.as_tensor(np.ascontiguousarray(np.moveaxis(c2w_pl, -1, 0))).to(device)
+    f["gx"] = torch.as_tensor(np.ascontiguousarray(np.moveaxis(gx, (2, 1, 0, 3), (1, 2, 3, 0))))[:, :, None].to(device)
+    f["gx_pl"] = torch.as_tensor(np.ascontiguousarray(np.moveaxis(gx_pl, -1, 0)))[:, :, None, :].to(device)
+    return f
+
+
+def hyperdiffusion(core, x, x_pl, rhog, rhog_pl, fixed: dict):
+    """The hyperdiffusion tendency of the large step (mod_numfilter.py:845-1469,
+    DIRECT Kh, lap_order 2; _hdiff_tendency_host :1519-1578 and the final
+    horizontalize) as a differentiable function of the six fields
+    x = (vx, vy, vz, w, tem - tem_bs, rho - rho_bs) (6, lall, kall, g, g) and
+    x_pl (6, 6, kall, LP), at a fixed density (rhog, rhog_pl): two
+    Laplacian passes (the second a kh-weighted diffusion for the two scalars),
+    the tendencies scaled by Kh and rhog (rhog at half levels for w), the
+    momentum made horizontal.  Returns (f, f_pl) in prognostic order (RHOG,
+    RHOGVX, RHOGVY, RHOGVZ, RHOGW, RHOGE) on interior cells and the pole
+    point; the adjoint follows from the operators' hand-written transposes."""
+    Kh, r = fixed["Kh"], fixed["rscale"]
+    rhog, rhog_pl = rhog.detach(), rhog_pl.detach()
+    v1 = [laplacian(core, x[n], x_pl[n]) for n in range(6)]
+    v1 = [(-a, -b) for a, b in v1]
+    v2 = [laplacian(core, *v1[n]) for n in range(4)]
+    v2.append(diffusion(core, *v1[4], rhog * fixed["CVdry"] * Kh, rhog_pl * fixed["CVdry"] * Kh))
+    v2.append(diffusion(core, *v1[5], rhog * fixed["hfr"] * Kh, rhog_pl * fixed["hfr"] * Kh))
+    v2 = [(-a, -b) for a, b in v2]
+    kmin = fixed["kmin"]
+    out = []
+    for pole in (0, 1):
+        rg = rhog_pl if pole else rhog
+        c2w = fixed["c2w_pl"] if pole else fixed["c2w"]
+        kax = 1   # the level axis of (lall, kall, g, g) and of (6, kall, LP)
+        below = torch.zeros_like(rg)
+        below.narrow(kax, 1, rg.shape[kax] - 1).copy_(rg.narrow(kax, 0, rg.shape[kax] - 1))
+        rgh = c2w[0] * rg + c2w[1] * below
+        rgh.narrow(kax, 0, kmin).zero_()
+        v = [t[pole] for t in v2]
+        fx, fy, fz = (-(v[n] * Kh) * rg for n in range(3))
+        fw = -(v[3] * Kh) * rgh
+        gx = fixed["gx_pl"] if pole else fixed["gx"]
+        prd = (fx * gx[0] + fy * gx[1] + fz * gx[2]) / r
+        fx, fy, fz = fx - prd * gx[0] / r, fy - prd * gx[1] / r, fz - prd * gx[2] / r
+        out.append(torch.stack([-v[5], fx, fy, fz, fw, -v[4]]))
+    return out[0], out[1]
+
+
 def divergence(core, v, v_pl):
     return Divergence.apply(core, v, v_pl)
 

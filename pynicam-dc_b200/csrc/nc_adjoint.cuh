@@ -862,4 +862,198 @@ __global__ void k_grad_adj_pl(const double* gr, double* q) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Kh-weighted horizontal diffusion (kernels/oprtdiffusion.py, the scalar pass
+// of the hyperdiffusion: OPRT_diffusion of s with the coefficient field kh)
+// after the halo exchange, and its adjoint.  y = D(C(s)) on interior cells and
+// the pole point; linear in s for a given kh.  The triangle values of the
+// forward are
+//   TI(i,j) = (wI1 s(i,j) + wI2 s(i+1,j) + wI3 s(i+1,j+1)) / 3,
+//   TJ(i,j) = (wJ1 s(i,j) + wJ2 s(i+1,j+1) + wJ3 s(i,j+1)) / 3
+// per direction d (weights intp_w), with the singular-point fix at (0,0),
+// TI(0,0) <- TI(0,0) m0 + TJ(1,0) m1; the cell sums the six edge terms
+// kf_e cd_e (T + T') (kf_e the mean of kh at the cell and its e-th
+// neighbour).  The adjoint gathers, for every triangle, the edge weights of
+// the (up to three) cells that use it, undoes the fix, then gathers for
+// every point the weights of the triangles that hold it.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool tri_ok(int ii, int jj) { return ii >= 0 && jj >= 0 && ii <= cD.G - 2 && jj <= cD.G - 2; }
+
+// raw triangle value (before the singular-point fix), direction d, t = 0: TI, 1: TJ
+__device__ __forceinline__ double diff_tri(const double* s, int ii, int jj, int k, int l, int d, int t) {
+  if (!tri_ok(ii, jj)) return 0.0;
+  const double w1 = P2(cG.intp_w, (d * 3 + 0) * 2 + t, ii, jj, l);
+  const double w2 = P2(cG.intp_w, (d * 3 + 1) * 2 + t, ii, jj, l);
+  const double w3 = P2(cG.intp_w, (d * 3 + 2) * 2 + t, ii, jj, l);
+  const double s0 = s[ix(ii, jj, k, l)], sd = s[ix(ii + 1, jj + 1, k, l)];
+  return t == 0 ? div3(w1 * s0 + w2 * s[ix(ii + 1, jj, k, l)] + w3 * sd)
+                : div3(w1 * s0 + w2 * sd + w3 * s[ix(ii, jj + 1, k, l)]);
+}
+__device__ __forceinline__ double diff_tri_fixed(const double* s, int ii, int jj, int k, int l, int d, int t) {
+  double v = diff_tri(s, ii, jj, k, l, d, t);
+  if (t == 0 && ii == 0 && jj == 0)
+    v = v * (double)cG.pntmask[l * 2 + 0] + diff_tri(s, 1, 0, k, l, d, 1) * (double)cG.pntmask[l * 2 + 1];
+  return v;
+}
+// the six edge weights kf_e (e = 1..6 at index e - 1) of interior cell (i, j)
+__device__ __forceinline__ void diff_kf(const double* kh, int i, int j, int k, int l, double kf[6]) {
+  const double k0 = kh[ix(i, j, k, l)];
+  kf[0] = 0.5 * (k0 + kh[ix(i + 1, j + 1, k, l)]);
+  kf[1] = 0.5 * (k0 + kh[ix(i, j + 1, k, l)]);
+  kf[2] = 0.5 * (k0 + kh[ix(i - 1, j, k, l)]);
+  kf[3] = 0.5 * (k0 + kh[ix(i - 1, j - 1, k, l)]);
+  kf[4] = 0.5 * (k0 + kh[ix(i, j - 1, k, l)]);
+  kf[5] = 0.5 * (k0 + kh[ix(i + 1, j, k, l)]);
+}
+
+__global__ void k_diff_fwd(const double* kh, const double* s, double* y) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.npti) return;
+  const int G = cD.G, KA = cD.KA;
+  const int i = t % G, j = (t / G) % G, k = (t / (G * G)) % KA, l = t / (G * G * KA);
+  double inner = 0.0;
+  if (interior(i, j)) {
+    double kf[6];
+    diff_kf(kh, i, j, k, l, kf);
+    for (int d = 0; d < 3; ++d) {
+      const double aTI = diff_tri_fixed(s, i, j, k, l, d, 0), aTJ = diff_tri_fixed(s, i, j, k, l, d, 1);
+      const double bTI = diff_tri_fixed(s, i - 1, j, k, l, d, 0);
+      const double cTI = diff_tri_fixed(s, i - 1, j - 1, k, l, d, 0), cTJ = diff_tri_fixed(s, i - 1, j - 1, k, l, d, 1);
+      const double dTJ = diff_tri_fixed(s, i, j - 1, k, l, d, 1);
+      auto cd = [&](int e) { return P2(cG.coef_diff, d * 6 + e, i, j, l); };
+      const double blk = kf[0] * cd(0) * (aTI + aTJ) + kf[1] * cd(1) * (aTJ + bTI) + kf[2] * cd(2) * (bTI + cTJ) +
+                         kf[3] * cd(3) * (cTJ + cTI) + kf[4] * cd(4) * (cTI + dTJ) + kf[5] * cd(5) * (dTJ + aTI);
+      inner = (d == 0) ? blk : inner + blk;
+    }
+  }
+  y[t] = inner;
+}
+
+// the pole row (kernels/oprtdiffusion.py:137-177): the pole point from the
+// five ring triangles; the ring rows are zero
+__global__ void k_diff_fwd_pl(const double* kh, const double* s, double* y) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.KA * cD.LP) return;
+  const int k = t / cD.LP, lp = t % cD.LP;
+  const double sn = s[ipl(0, k, lp)];
+  double vt[5][3];
+  for (int v = 1; v <= 5; ++v) {
+    const int vp1 = (v == 5) ? 1 : v + 1;
+    const double sij = s[ipl(v, k, lp)], sp1 = s[ipl(vp1, k, lp)];
+    for (int d = 0; d < 3; ++d) {
+      const double* cI = cG.coef_intp_pl + ((v * cD.LP + lp) * 3 + d) * 3;
+      const double c0 = cI[0], c1 = cI[1], c2 = cI[2];
+      vt[v - 1][d] = div3((2.0 * c0 - c1 - c2) * sn + (-c0 + 2.0 * c1 - c2) * sij + (-c0 - c1 + 2.0 * c2) * sp1);
+    }
+  }
+  const double khn = kh[ipl(0, k, lp)];
+  double row = 0.0;
+  for (int v = 1; v <= 5; ++v) {
+    const int vm1 = (v == 1) ? 5 : v - 1;
+    const double kavg = 0.5 * (khn + kh[ipl(v, k, lp)]);
+    double sd = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const double tv = cG.coef_diff_pl[(v * cD.LP + lp) * 3 + d] * (vt[vm1 - 1][d] + vt[v - 1][d]);
+      sd = (d == 0) ? tv : sd + tv;
+    }
+    const double contrib = kavg * sd;
+    row = (v == 1) ? contrib : row + contrib;
+  }
+  y[ipl(0, k, lp)] = row;
+  for (int g = 1; g < 6; ++g) y[ipl(g, k, lp)] = 0.0;
+}
+
+// cotangent of the raw (unfixed) triangle value from the cells that use it
+__device__ double diff_tbar_gathered(const double* kh, const double* y, int ii, int jj, int k, int l, int d, int t) {
+  double acc = 0.0;
+  double kf[6];
+  auto cd = [&](int e, int ci, int cj) { return P2(cG.coef_diff, d * 6 + e, ci, cj, l); };
+  // TI(ii,jj): cell (ii,jj) edges 1, 6; cell (ii+1,jj) edges 2, 3; cell (ii+1,jj+1) edges 4, 5
+  // TJ(ii,jj): cell (ii,jj) edges 1, 2; cell (ii+1,jj+1) edges 3, 4; cell (ii,jj+1) edges 5, 6
+  const int ci[3] = {ii, ii + 1, t == 0 ? ii + 1 : ii};
+  const int cj[3] = {jj, t == 0 ? jj : jj + 1, jj + 1};
+  const int e0[3] = {0, t == 0 ? 1 : 2, t == 0 ? 3 : 4};
+  const int e1[3] = {t == 0 ? 5 : 1, t == 0 ? 2 : 3, t == 0 ? 4 : 5};
+  for (int c = 0; c < 3; ++c) {
+    const int i = ci[c], j = cj[c];
+    if (i < 1 || j < 1 || i > cD.G - 2 || j > cD.G - 2) continue;
+    diff_kf(kh, i, j, k, l, kf);
+    acc += y[ix(i, j, k, l)] * (kf[e0[c]] * cd(e0[c], i, j) + kf[e1[c]] * cd(e1[c], i, j));
+  }
+  return acc;
+}
+
+// per triangle point: the cotangents of its two raw triangle values, three
+// directions each (tb[(t * 3 + d) * npt + point]), the singular-point fix undone
+__global__ void k_diff_adj_tri(const double* kh, const double* y, double* tb) {
+  const int p = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (p >= cD.npti) return;
+  const int G = cD.G, KA = cD.KA, n = cD.npti;
+  const int ii = p % G, jj = (p / G) % G, k = (p / (G * G)) % KA, l = p / (G * G * KA);
+  for (int t = 0; t < 2; ++t)
+    for (int d = 0; d < 3; ++d) {
+      double v = 0.0;
+      if (tri_ok(ii, jj)) {
+        v = diff_tbar_gathered(kh, y, ii, jj, k, l, d, t);
+        if (t == 0 && ii == 0 && jj == 0) v = v * (double)cG.pntmask[l * 2 + 0];
+        if (t == 1 && ii == 1 && jj == 0)
+          v = v + diff_tbar_gathered(kh, y, 0, 0, k, l, d, 0) * (double)cG.pntmask[l * 2 + 1];
+      }
+      tb[(t * 3 + d) * n + p] = v;
+    }
+}
+
+// per point: the cotangent of s from the triangles that hold it
+__global__ void k_diff_adj_pt(const double* tb, double* g) {
+  const int p = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (p >= cD.npti) return;
+  const int G = cD.G, KA = cD.KA, n = cD.npti;
+  const int i = p % G, j = (p / G) % G, k = (p / (G * G)) % KA, l = p / (G * G * KA);
+  // (triangle offset, kind t, vertex m): s(i,j) is vertex 1 of TI / TJ (i,j), vertex 2 of TI (i-1,j),
+  // vertex 3 of TI (i-1,j-1), vertex 2 of TJ (i-1,j-1), vertex 3 of TJ (i,j-1)
+  const int oi[6] = {0, 0, -1, -1, -1, 0}, oj[6] = {0, 0, 0, -1, -1, -1};
+  const int tt[6] = {0, 1, 0, 0, 1, 1}, mm[6] = {0, 0, 1, 2, 1, 2};
+  double acc = 0.0;
+  for (int c = 0; c < 6; ++c) {
+    const int ii = i + oi[c], jj = j + oj[c];
+    if (!tri_ok(ii, jj)) continue;
+    const int q = ix(ii, jj, k, l);
+    for (int d = 0; d < 3; ++d)
+      acc += P2(cG.intp_w, (d * 3 + mm[c]) * 2 + tt[c], ii, jj, l) * div3(tb[(tt[c] * 3 + d) * n + q]);
+  }
+  g[p] = acc;
+}
+
+// the pole row's adjoint: the pole point and its five ring points
+__global__ void k_diff_adj_pl(const double* kh, const double* y, double* g) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.KA * cD.LP) return;
+  const int k = t / cD.LP, lp = t % cD.LP;
+  const double y0 = y[ipl(0, k, lp)];
+  const double khn = kh[ipl(0, k, lp)];
+  double vtb[5][3] = {};
+  for (int v = 1; v <= 5; ++v) {
+    const int vm1 = (v == 1) ? 5 : v - 1;
+    const double kavg = 0.5 * (khn + kh[ipl(v, k, lp)]);
+    for (int d = 0; d < 3; ++d) {
+      const double w = y0 * kavg * cG.coef_diff_pl[(v * cD.LP + lp) * 3 + d];
+      vtb[vm1 - 1][d] += w;
+      vtb[v - 1][d] += w;
+    }
+  }
+  double gs[6] = {};
+  for (int v = 1; v <= 5; ++v) {
+    const int vp1 = (v == 5) ? 1 : v + 1;
+    for (int d = 0; d < 3; ++d) {
+      const double* cI = cG.coef_intp_pl + ((v * cD.LP + lp) * 3 + d) * 3;
+      const double c0 = cI[0], c1 = cI[1], c2 = cI[2];
+      const double b = div3(vtb[v - 1][d]);
+      gs[0] += (2.0 * c0 - c1 - c2) * b;
+      gs[v] += (-c0 + 2.0 * c1 - c2) * b;
+      gs[vp1] += (-c0 - c1 + 2.0 * c2) * b;
+    }
+  }
+  for (int g_ = 0; g_ < 6; ++g_) g[ipl(g_, k, lp)] = gs[g_];
+}
+
 }  // namespace nc

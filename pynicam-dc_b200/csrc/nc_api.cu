@@ -408,6 +408,7 @@ struct nc_handle {
   cudaEvent_t ev_user = nullptr;   // ordering against a caller's stream (device-pointer marshal)
   double *stage_out = nullptr, *stage_out_pl = nullptr;
   double* adj_work = nullptr;   // exchanged copy of the Laplacian's input (allocated on first use)
+  double* adj_work6 = nullptr;   // the diffusion adjoint's triangle cotangents (6 fields)
   double* adj_work3 = nullptr;  // exchanged copy of the divergence's three components (first use)
   // linearised tracer step (nc_trc_step_lin): work fields allocated on first use
   FieldPair lin[20];
@@ -2902,6 +2903,38 @@ int nc_divergence(nc_handle* h, int32_t transpose, double* v, double* v_pl, doub
     k_div_adj_pl<<<gp, 128, 0, h->stream>>>(y_pl, v_pl);
     TRY(check_launch(h, "div_adj_pl"));
     TRY(comm_fields(h, v, v_pl, 3, true));
+  }
+  return before_caller(h, stream);
+}
+
+int nc_diffusion(nc_handle* h, int32_t transpose, const double* kh, const double* kh_pl, double* s, double* s_pl,
+                 double* y, double* y_pl, void* stream) {
+  TRY(adj_ready(h, "nc_diffusion"));
+  if (!kh || !kh_pl || !s || !s_pl || !y || !y_pl) return fail(NC_ERR_ARG, "nc_diffusion: null pointer");
+  if (s == y || s_pl == y_pl) return fail(NC_ERR_ARG, "nc_diffusion: input and output must not alias");
+  const Dims& D = h->D;
+  const unsigned gr = (unsigned)((D.npt + 255) / 256), gp = (unsigned)((D.KA * D.LP + 127) / 128);
+  TRY(after_caller(h, stream));
+  if (!transpose) {
+    if (!h->adj_work) TRY(dev_alloc(h, &h->adj_work, (size_t)D.npt + D.npl));
+    double* w = h->adj_work;
+    double* w_pl = w + D.npt;
+    CU(cudaMemcpyAsync(w, s, D.npt * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CU(cudaMemcpyAsync(w_pl, s_pl, (size_t)D.npl * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    TRY(comm_fields(h, w, w_pl, 1, false));
+    k_diff_fwd<<<gr, 256, 0, h->stream>>>(kh, w, y);
+    TRY(check_launch(h, "diff"));
+    k_diff_fwd_pl<<<gp, 128, 0, h->stream>>>(kh_pl, w_pl, y_pl);
+    TRY(check_launch(h, "diff_pl"));
+  } else {
+    if (!h->adj_work6) TRY(dev_alloc(h, &h->adj_work6, 6 * (size_t)D.npt));
+    k_diff_adj_tri<<<gr, 256, 0, h->stream>>>(kh, y, h->adj_work6);
+    TRY(check_launch(h, "diff_adj_tri"));
+    k_diff_adj_pt<<<gr, 256, 0, h->stream>>>(h->adj_work6, s);
+    TRY(check_launch(h, "diff_adj_pt"));
+    k_diff_adj_pl<<<gp, 128, 0, h->stream>>>(kh_pl, y_pl, s_pl);
+    TRY(check_launch(h, "diff_adj_pl"));
+    TRY(comm_fields(h, s, s_pl, 1, true));
   }
   return before_caller(h, stream);
 }

@@ -1,5 +1,6 @@
 """Tangent-linear and adjoint operators (adjoint.py, nc_vsolve / nc_vadv_lin /
-nc_laplacian / nc_divergence / nc_gradient) on the device, float64.
+nc_laplacian / nc_divergence / nc_gradient / nc_diffusion) on the device,
+float64.
 
 The operators' inputs come from a real step: the balanced-jet case at grid
 level 4 with 40 layers is stepped once and the handle's implicit matrix
@@ -16,6 +17,10 @@ positive field with seeded noise (no ties for the limiter's min / max).
   the tridiagonal solve equals a banded solve to 1e-12;
 * dot-product tests <TL x, y> = <x, AD y> to 1e-12 (relative to the
   magnitudes of the products) for every operator, regional and pole;
+* the exchange + Kh-weighted diffusion equals the oracle's comm + diffusion
+  bit for bit, and the hyperdiffusion tendency composed from the Laplacian
+  and diffusion operators (adjoint.hyperdiffusion, at the case's state) equals
+  the oracle's hdiffusion to 1e-12 and passes the dot-product test;
 * the HEVI vertical implicit step (adjoint.hevi_matrix / hevi_solve around
   the hand-written solve) equals the oracle's rhow_matrix / rhow_solver bit
   for bit and passes the dot-product test in all nine field arguments;
@@ -102,6 +107,7 @@ def _case(pkg, glevel, vlayer=40):
     q = 1e-3 * (1.2 + 0.5 * np.sin(np.arange(rho.size).reshape(rho.shape) * 0.37)) * (1 + 0.1 * rng.random(rho.shape))
     f["rhogq"] = adj.to_device_layout(rho * q)
     f["rhogq_pl"] = torch.as_tensor(sp[..., 0] * 1.3e-3 * (1 + 0.1 * rng.random(sp.shape[:3]))).cuda()
+    f["state"], f["state_pl"] = s, sp
     return geo, core, f
 
 
@@ -345,6 +351,112 @@ def test_dot_product_laplacian(gl04):
     rhs = _dot(x, ad) + _dot(x_pl, ad_pl)
     scale = float((tl * y).abs().sum() + (tl_pl * y_pl).abs().sum())
     assert _dot_rel(lhs, rhs, scale) <= 1e-12, (lhs, rhs)
+
+
+def _kh(f, seed):
+    """a positive coefficient field of the size the step uses (rhog x CVdry x Kh)"""
+    import torch
+    rg, rg_pl = f["den"], f["den_pl"]
+    return (rg * 717.5 * 9.6e16 * (1.0 + 0.1 * _rand_like(rg, seed).abs()),
+            rg_pl * 717.5 * 9.6e16 * (1.0 + 0.1 * _rand_like(rg_pl, seed + 1).abs()))
+
+
+def test_diffusion_equals_oracle(gl04):
+    """exchange + kh-weighted diffusion against the oracle's comm + diffusion
+    (the hyperdiffusion's scalar pass, same expressions: bit for bit)"""
+    from oracle import nicam_step as O
+    import torch
+    _, adj = _mods()
+    geo, core, f = gl04
+    G = O.Geo(geo)
+    q, q_pl = f["rhogq"], f["rhogq_pl"]
+    kh, kh_pl = _kh(f, 21)
+    y, y_pl = torch.empty_like(q), torch.empty_like(q_pl)
+    core.diffusion(kh, kh_pl, q, q_pl, y, y_pl)
+    a, a_pl = adj.from_device_layout(q), q_pl.cpu().numpy()
+    O.comm1(G, a, a_pl)
+    want = O.diffusion(G, a, adj.from_device_layout(kh))
+    want_pl = O.diffusion_pl(G, a_pl, kh_pl.cpu().numpy())
+    got, got_pl = adj.from_device_layout(y), y_pl.cpu().numpy()
+    ins = (slice(1, -1), slice(1, -1))
+    assert np.array_equal(got[ins], want[ins]) and np.array_equal(got_pl[0], want_pl[0])
+
+
+def test_dot_product_diffusion(gl04):
+    import torch
+    _, core, f = gl04
+    kh, kh_pl = _kh(f, 31)
+    x, x_pl = _rand_like(f["rhogq"], 32), _rand_like(f["rhogq_pl"], 33)
+    y, y_pl = _rand_like(f["rhogq"], 34), _rand_like(f["rhogq_pl"], 35)
+    tl, tl_pl = torch.empty_like(x), torch.empty_like(x_pl)
+    ad, ad_pl = torch.empty_like(x), torch.empty_like(x_pl)
+    core.diffusion(kh, kh_pl, x, x_pl, tl, tl_pl)
+    core.diffusion(kh, kh_pl, ad, ad_pl, y, y_pl, transpose=True)
+    lhs = _dot(tl, y) + _dot(tl_pl, y_pl)
+    rhs = _dot(x, ad) + _dot(x_pl, ad_pl)
+    scale = float((tl * y).abs().sum() + (tl_pl * y_pl).abs().sum())
+    assert _dot_rel(lhs, rhs, scale) <= 1e-12, (lhs, rhs)
+
+
+def _hdiff_inputs(geo, f):
+    """the six fields of the hyperdiffusion (vx, vy, vz, w, tem - tem_bs,
+    rho - rho_bs) of the case's state from the oracle's diagnostics, in the
+    device layout, with rhog"""
+    from oracle import nicam_step as O
+    import torch
+    _, adj = _mods()
+    G = O.Geo(geo)
+    s, sp = f["state"].copy(), f["state_pl"].copy()
+    O.comm(G, s, sp)
+    P, Pq, P_pl, Pq_pl = s[..., :6].copy(), s[..., 6:].copy(), sp[..., :6].copy(), sp[..., 6:].copy()
+    D, D_pl = np.zeros(P.shape), np.zeros(P_pl.shape)
+    rho, _, _, rho_pl, _, _ = O.diagnostics(G, P, Pq, D, P_pl, Pq_pl, D_pl)
+    fields = [D[..., O.I_vx], D[..., O.I_vy], D[..., O.I_vz], D[..., O.I_w], D[..., O.I_tem] - G.tem_bs,
+              rho - G.rho_bs]
+    fields_pl = [D_pl[..., O.I_vx], D_pl[..., O.I_vy], D_pl[..., O.I_vz], D_pl[..., O.I_w],
+                 D_pl[..., O.I_tem] - G.tem_bs_pl, rho_pl - G.rho_bs_pl]
+    x = torch.stack([adj.to_device_layout(a) for a in fields])
+    x_pl = torch.stack([torch.as_tensor(np.ascontiguousarray(a)) for a in fields_pl]).cuda()
+    oracle_args = (P[..., 0], rho, D, P_pl[..., 0], rho_pl, D_pl)
+    return x, x_pl, adj.to_device_layout(P[..., 0]), torch.as_tensor(np.ascontiguousarray(P_pl[..., 0])).cuda(), \
+        oracle_args
+
+
+def test_hyperdiffusion_equals_oracle(gl04):
+    """the hyperdiffusion tendency composed from the differentiable
+    operators against the oracle's hdiffusion (mod_numfilter.py:845-1578) on
+    interior cells and the pole point: relative max difference <= 1e-12"""
+    from oracle import nicam_step as O
+    _, adj = _mods()
+    geo, core, f = gl04
+    x, x_pl, rg, rg_pl, oargs = _hdiff_inputs(geo, f)
+    got, got_pl = adj.hyperdiffusion(core, x, x_pl, rg, rg_pl, adj.hdiff_setup(geo))
+    want, want_pl = O.hdiffusion(O.Geo(geo), *oargs)
+    for v in range(6):
+        a = adj.from_device_layout(got[v])[1:-1, 1:-1]
+        b = want[1:-1, 1:-1, :, :, v]
+        assert np.abs(a - b).max() <= 1e-12 * max(np.abs(b).max(), 1e-300), v
+        ap, bp = got_pl[v][0].cpu().numpy(), want_pl[0, :, :, v]
+        assert np.abs(ap - bp).max() <= 1e-12 * max(np.abs(b).max(), 1e-300), v
+
+
+def test_dot_product_hyperdiffusion(gl04):
+    """<H dx, dy> = <dx, H^T dy> for the hyperdiffusion tendency at a fixed
+    density, H^T through torch.autograd and the operators' adjoint kernels"""
+    import torch
+    _, adj = _mods()
+    geo, core, f = gl04
+    x, x_pl, rg, rg_pl, _ = _hdiff_inputs(geo, f)
+    fixed = adj.hdiff_setup(geo)
+    dx = (_rand_like(x, 41) * x.abs().mean(dim=(1, 2, 3, 4), keepdim=True)).requires_grad_(True)
+    dx_pl = (_rand_like(x_pl, 42) * x_pl.abs().mean(dim=(1, 2, 3), keepdim=True)).requires_grad_(True)
+    y, y_pl = adj.hyperdiffusion(core, dx, dx_pl, rg, rg_pl, fixed)
+    wy, wy_pl = _rand_like(y, 43), _rand_like(y_pl, 44)
+    lhs = float((y * wy).sum() + (y_pl * wy_pl).sum())
+    gx, gx_pl = torch.autograd.grad((y * wy).sum() + (y_pl * wy_pl).sum(), (dx, dx_pl))
+    rhs = float((dx * gx).sum() + (dx_pl * gx_pl).sum())
+    scale = float((y * wy).abs().sum() + (y_pl * wy_pl).abs().sum())
+    assert abs(lhs - rhs) <= 1e-12 * scale, (lhs, rhs)
 
 
 def test_dot_product_divergence_and_gradient(gl04):
