@@ -413,6 +413,21 @@ int nc_gradient(nc_handle* h, int32_t transpose, double* q, double* q_pl, double
 int nc_diffusion(nc_handle* h, int32_t transpose, const double* kh, const double* kh_pl, double* s, double* s_pl,
                  double* y, double* y_pl, void* stream);
 
+/* The divergence damping's two operators (mod_numfilter.py:2032-2268) after
+ * the halo exchange of their inputs, and their adjoints, float64, device
+ * buffers in the library's field layout, components one after the other,
+ * ordered on the caller's stream.  nc_divdamp3d: y = D3(C(v)), v the four
+ * momenta (rhogvx, rhogvy, rhogvz, rhogw), y three components on interior
+ * cells and the pole point, levels kmin..kmax (kernels/oprt3ddivdamp.py:
+ * 50-237, the singular-point fix included).  nc_divdamp2d: y = D2(C(v)), v
+ * and y three components, every level (kernels/oprtdivdamp.py:54-173).
+ * transpose = 1 reads y and writes v = C^T D^T y.  The buffer written must
+ * not alias the one read; the forward forms allocate a scratch copy in the
+ * handle on their first call, the adjoints a scratch of six fields and add
+ * with atomics in the exchange's adjoint. */
+int nc_divdamp3d(nc_handle* h, int32_t transpose, double* v, double* v_pl, double* y, double* y_pl, void* stream);
+int nc_divdamp2d(nc_handle* h, int32_t transpose, double* v, double* v_pl, double* y, double* y_pl, void* stream);
+
 /* nc_trc_step_lin: the tracer advection of one step (mod_src_tracer.py:
  * 83-1228 as the step runs it: vertical step, horizontal step with the
  * MIURA2004 face values and the horizontal Thuburn limiter of 2190-2605,

@@ -268,18 +268,80 @@ def diffusion(core, s, s_pl, kh, kh_pl):
     return Diffusion.apply(core, s, s_pl, kh, kh_pl)
 
 
+class _DivDamp(torch.autograd.Function):
+    """(y, y_pl) = D(C(v, v_pl)): halo exchange then one of the divergence
+    damping's operators (three = True: the 3-D OPRT3D_divdamp of the four
+    momenta, kernels/oprt3ddivdamp.py; else the 2-D OPRT_divdamp of three
+    components, kernels/oprtdivdamp.py); linear in v"""
+
+    @staticmethod
+    def forward(ctx, core, three, v, v_pl):
+        op = core.divdamp3d if three else core.divdamp2d
+        y = torch.empty((3,) + tuple(v.shape[1:]), dtype=v.dtype, device=v.device)
+        y_pl = torch.empty((3,) + tuple(v_pl.shape[1:]), dtype=v_pl.dtype, device=v_pl.device)
+        op(_c(v), _c(v_pl), y, y_pl)
+        ctx.core, ctx.three, ctx.shapes = core, three, (tuple(v.shape), tuple(v_pl.shape))
+        return y, y_pl
+
+    @staticmethod
+    def backward(ctx, gy, gy_pl):
+        op = ctx.core.divdamp3d if ctx.three else ctx.core.divdamp2d
+        sv, sv_pl = ctx.shapes
+        dev = (gy if gy is not None else gy_pl).device
+        z = lambda shp: torch.zeros(shp, dtype=torch.float64, device=dev)
+        gy = z((3,) + sv[1:]) if gy is None else _c(gy)
+        gy_pl = z((3,) + sv_pl[1:]) if gy_pl is None else _c(gy_pl)
+        g, g_pl = z(sv), z(sv_pl)
+        op(g, g_pl, gy, gy_pl, transpose=True)
+        return None, None, g, g_pl
+
+
+def divdamp3d(core, v, v_pl):
+    """the 3-D divergence damping operator of the four momenta (4, ...) -> (3, ...)"""
+    return _DivDamp.apply(core, True, v, v_pl)
+
+
+def divdamp2d(core, v, v_pl):
+    """the 2-D divergence damping operator of three components (3, ...) -> (3, ...)"""
+    return _DivDamp.apply(core, False, v, v_pl)
+
+
+def divergence_damping(core, v, v_pl, fixed: dict):
+    """The divergence damping tendency of the large step (mod_numfilter.py:
+    2032-2268, lap_order 2): the 3-D operator on the four momenta
+    v = (rhogvx, rhogvy, rhogvz, rhogw) (4, lall, kall, g, g) and v_pl
+    (4, 6, kall, LP), the exchange, the 2-D operator on its negation, the
+    coefficient, the result made horizontal (kernels/horizontalizevec.py;
+    the pole rows with the per-term division of its pole form).  Returns
+    (gd, gd_pl) of shape (3, ...), differentiable through the operators'
+    hand-written transposes."""
+    r, coef = fixed["rscale"], fixed["divdamp_coef"]
+    d, d_pl = divdamp3d(core, v, v_pl)
+    o, o_pl = divdamp2d(core, -d, -d_pl)
+    out = []
+    for pole, t in ((0, o), (1, o_pl)):
+        fx, fy, fz = coef * t[0], coef * t[1], coef * t[2]
+        gx = fixed["gx_pl"] if pole else fixed["gx"]
+        if pole:
+            prd = fx * gx[0] / r + fy * gx[1] / r + fz * gx[2] / r
+        else:
+            prd = (fx * gx[0] + fy * gx[1] + fz * gx[2]) / r
+        out.append(torch.stack([fx - prd * gx[0] / r, fy - prd * gx[1] / r, fz - prd * gx[2] / r]))
+    return out[0], out[1]
+
+
 def hdiff_setup(geo: dict, device="cuda") -> dict:
-    """the fixed inputs of ``hyperdiffusion`` from a setup dict (DIRECT Kh):
-    Kh, CVdry, hdiff_fact_rho, the C2W weights (device layout, two
-    components) and the unit-radius position vectors GRD_x / rscale of the
-    regional points and pole points"""
+    """the fixed inputs of ``hyperdiffusion`` and ``divergence_damping`` from a
+    setup dict (DIRECT Kh): Kh, divdamp_coef, CVdry, hdiff_fact_rho, the C2W
+    weights (device layout, two components) and the unit-radius position
+    vectors GRD_x / rscale of the regional points and pole points"""
     sc = lambda k: float(np.asarray(geo[k]).reshape(-1)[0])
     c2w = np.asarray(geo["VMTR_C2Wfact"], np.float64)
     c2w_pl = np.asarray(geo["VMTR_C2Wfact_pl"], np.float64)
     gx = np.asarray(geo["GRD_x"], np.float64)[:, :, 0, :, :]               # (i, j, l, 3)
     gx_pl = np.asarray(geo["GRD_x_pl"], np.float64)[:, 0, :, :]            # (g, l, 3)
-    f = {"Kh": sc("Kh_coef"), "CVdry": sc("CVdry"), "hfr": sc("hdiff_fact_rho"), "rscale": sc("rscale"),
-         "kmin": int(sc("kmin"))}
+    f = {"Kh": sc("Kh_coef"), "divdamp_coef": sc("divdamp_coef"), "CVdry": sc("CVdry"),
+         "hfr": sc("hdiff_fact_rho"), "rscale": sc("rscale"), "kmin": int(sc("kmin"))}
     f["c2w"] = torch.stack([to_device_layout(c2w[..., c], device) for c in range(2)])
     f["c2w_pl"] = torch.as_tensor(np.ascontiguousarray(np.moveaxis(c2w_pl, -1, 0))).to(device)
     f["gx"] = torch.as_tensor(np.ascontiguousarray(np.moveaxis(gx, (2, 1, 0, 3), (1, 2, 3, 0))))[:, :, None].to(device)

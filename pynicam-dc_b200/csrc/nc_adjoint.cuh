@@ -1056,4 +1056,289 @@ __global__ void k_diff_adj_pl(const double* kh, const double* y, double* g) {
   for (int g_ = 0; g_ < 6; ++g_) g[ipl(g_, k, lp)] = gs[g_];
 }
 
+// ---------------------------------------------------------------------------
+// Divergence damping (mod_numfilter.py:2032-2268): the 3-D operator
+// OPRT3D_divdamp (kernels/oprt3ddivdamp.py:50-237) of the four momenta
+// (rhogvx, rhogvy, rhogvz, rhogw) and the 2-D OPRT_divdamp
+// (kernels/oprtdivdamp.py:54-173) of three components, each after the halo
+// exchange of its inputs, and their adjoints.  Per triangle the scalar
+//   T = sum over directions and vertices of coef_intp x v  (+ the vertical
+//       flux difference ((rwv(k+1) at the vertices) - (rwv(k))) / 3 rdgz(k)
+//       in 3-D, rwv the half-level mass flux of fluxconv's rhogw_vmh),
+// the 3-D operator with the singular-point fix at (0,0); each cell sums
+// coef_diff x (T + T') over its six edges per direction.  The 3-D outputs
+// live on kmin..kmax, the 2-D on every level.  The adjoint gathers for every
+// triangle the edge weights of the cells that use it, then for every point
+// the weights of the triangles that hold it (and, in 3-D, the vertical flux's
+// weights at levels k and k + 1).
+// ---------------------------------------------------------------------------
+// the half-level vertical mass flux at point q, level k (zero outside kmin+1..kmax)
+__device__ __forceinline__ double dd_rwv(const double* v, int q, int k) {
+  if (k < cD.kmin + 1 || k > cD.kmax) return 0.0;
+  const int n = cD.npti, qm = q - cD.planei;
+  const double* cz = cG.C2WGz;
+  const double h = cz[q] * v[q] + cz[n + q] * v[qm] + cz[2 * n + q] * v[n + q] + cz[3 * n + q] * v[n + qm] +
+                   cz[4 * n + q] * v[2 * n + q] + cz[5 * n + q] * v[2 * n + qm];
+  return h * gam_at(cG.RGAMH, q) + v[3 * n + q] * cG.RGSQRTH[q];
+}
+// raw triangle value (kind t: 0 TI, 1 TJ) at level k; 3-D with the vertical term and RGAM
+__device__ double dd_tri(const double* v, int ii, int jj, int k, int l, int t, bool three) {
+  if (!tri_ok(ii, jj)) return 0.0;
+  const int n = cD.npti;
+  const int qa = ix(ii, jj, k, l), qc = ix(ii + 1, jj + 1, k, l);
+  const int qb = (t == 0) ? ix(ii + 1, jj, k, l) : qc;
+  const int q3 = (t == 0) ? qc : ix(ii, jj + 1, k, l);
+  double sum = 0.0;
+  for (int dir = 0; dir < 3; ++dir) {
+    const double* f = v + dir * n;
+    const double va = three ? f[qa] * gam_at(cG.RGAM, qa) : f[qa];
+    const double vb = three ? f[qb] * gam_at(cG.RGAM, qb) : f[qb];
+    const double v3 = three ? f[q3] * gam_at(cG.RGAM, q3) : f[q3];
+    const double a = P2(cG.coef_intp, (dir * 3 + 0) * 2 + t, ii, jj, l) * va;
+    const double b = P2(cG.coef_intp, (dir * 3 + 1) * 2 + t, ii, jj, l) * vb;
+    const double c = P2(cG.coef_intp, (dir * 3 + 2) * 2 + t, ii, jj, l) * v3;
+    sum = (dir == 0) ? (a + b) + c : ((sum + a) + b) + c;
+  }
+  if (three) {
+    const double up = (dd_rwv(v, qa + cD.planei, k + 1) + dd_rwv(v, qb + cD.planei, k + 1)) +
+                      dd_rwv(v, q3 + cD.planei, k + 1);
+    const double dn = (dd_rwv(v, qa, k) + dd_rwv(v, qb, k)) + dd_rwv(v, q3, k);
+    sum = sum + div3(up - dn) * cC.rdgz[k];
+  }
+  return sum;
+}
+__device__ __forceinline__ double dd_tri_fixed(const double* v, int ii, int jj, int k, int l, int t, bool three) {
+  double x = dd_tri(v, ii, jj, k, l, t, three);
+  if (three && t == 0 && ii == 0 && jj == 0)
+    x = x * (double)cG.pntmask[l * 2 + 0] + dd_tri(v, 1, 0, k, l, 1, three) * (double)cG.pntmask[l * 2 + 1];
+  return x;
+}
+// three: v holds four components (rhogvx, rhogvy, rhogvz, rhogw), else three
+__global__ void k_ddamp_fwd(const double* v, double* y, int three) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.npti) return;
+  const int G = cD.G, KA = cD.KA, n = cD.npti;
+  const int i = t % G, j = (t / G) % G, k = (t / (G * G)) % KA, l = t / (G * G * KA);
+  const bool on = interior(i, j) && (!three || (k >= cD.kmin && k <= cD.kmax));
+  double aTI = 0.0, aTJ = 0.0, bTI = 0.0, cTI = 0.0, cTJ = 0.0, dTJ = 0.0;
+  if (on) {
+    aTI = dd_tri_fixed(v, i, j, k, l, 0, three);
+    aTJ = dd_tri_fixed(v, i, j, k, l, 1, three);
+    bTI = dd_tri_fixed(v, i - 1, j, k, l, 0, three);
+    cTI = dd_tri_fixed(v, i - 1, j - 1, k, l, 0, three);
+    cTJ = dd_tri_fixed(v, i - 1, j - 1, k, l, 1, three);
+    dTJ = dd_tri_fixed(v, i, j - 1, k, l, 1, three);
+  }
+  for (int d = 0; d < 3; ++d) {
+    double o = 0.0;
+    if (on) {
+      auto cd = [&](int e) { return P2(cG.coef_diff, d * 6 + e, i, j, l); };
+      o = cd(0) * (aTI + aTJ) + cd(1) * (aTJ + bTI) + cd(2) * (bTI + cTJ) + cd(3) * (cTJ + cTI) +
+          cd(4) * (cTI + dTJ) + cd(5) * (dTJ + aTI);
+    }
+    y[d * n + t] = o;
+  }
+}
+
+// pole rows: the pole point from its five triangles; ring rows zero
+__device__ __forceinline__ double dd_rwv_pl(const double* v, int g, int k, int lp) {
+  if (k < cD.kmin + 1 || k > cD.kmax) return 0.0;
+  const int np = cD.npl, q = ipl(g, k, lp), qm = ipl(g, k - 1, lp);
+  const double* cz = cG.C2WGz_pl + q * 6;
+  const double h = cz[0] * v[q] + cz[1] * v[qm] + cz[2] * v[np + q] + cz[3] * v[np + qm] + cz[4] * v[2 * np + q] +
+                   cz[5] * v[2 * np + qm];
+  return h * gam_at(cG.RGAMH_pl, q) + v[3 * np + q] * cG.RGSQRTH_pl[q];
+}
+__global__ void k_ddamp_fwd_pl(const double* v, double* y, int three) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.KA * cD.LP) return;
+  const int k = t / cD.LP, lp = t % cD.LP, np = cD.npl;
+  for (int g = 0; g < 6; ++g)
+    for (int d = 0; d < 3; ++d) y[d * np + ipl(g, k, lp)] = 0.0;
+  if (three && (k < cD.kmin || k > cD.kmax)) return;
+  double vm[6][3];
+  for (int g = 0; g < 6; ++g) {
+    const int q = ipl(g, k, lp);
+    for (int d = 0; d < 3; ++d) vm[g][d] = three ? v[d * np + q] * gam_at(cG.RGAM_pl, q) : v[d * np + q];
+  }
+  double sclt[5];
+  for (int vv = 1; vv <= 5; ++vv) {
+    const int vp1 = (vv == 5) ? 1 : vv + 1;
+    const double* cI = cG.coef_intp_pl + (vv * cD.LP + lp) * 9;
+    double x = cI[0] * vm[0][0] + cI[1] * vm[vv][0] + cI[2] * vm[vp1][0] + cI[3] * vm[0][1] + cI[4] * vm[vv][1] +
+               cI[5] * vm[vp1][1] + cI[6] * vm[0][2] + cI[7] * vm[vv][2] + cI[8] * vm[vp1][2];
+    if (three) {
+      const double up = (dd_rwv_pl(v, 0, k + 1, lp) + dd_rwv_pl(v, vv, k + 1, lp)) + dd_rwv_pl(v, vp1, k + 1, lp);
+      const double dn = (dd_rwv_pl(v, 0, k, lp) + dd_rwv_pl(v, vv, k, lp)) + dd_rwv_pl(v, vp1, k, lp);
+      x = x + div3(up - dn) * cC.rdgz[k];
+    }
+    sclt[vv - 1] = x;
+  }
+  for (int d = 0; d < 3; ++d) {
+    double row = 0.0;
+    for (int vv = 1; vv <= 5; ++vv) {
+      const int vm1 = (vv == 1) ? 5 : vv - 1;
+      const double tv = cG.coef_diff_pl[(vv * cD.LP + lp) * 3 + d] * (sclt[vm1 - 1] + sclt[vv - 1]);
+      row = (vv == 1) ? tv : row + tv;
+    }
+    y[d * np + ipl(0, k, lp)] = row;
+  }
+}
+
+// cotangent of a raw triangle value from the cells that use it (three directions)
+__device__ double dd_tbar_gathered(const double* y, int ii, int jj, int k, int l, int t) {
+  const int n = cD.npti;
+  const int ci[3] = {ii, ii + 1, t == 0 ? ii + 1 : ii};
+  const int cj[3] = {jj, t == 0 ? jj : jj + 1, jj + 1};
+  const int e0[3] = {0, t == 0 ? 1 : 2, t == 0 ? 3 : 4};
+  const int e1[3] = {t == 0 ? 5 : 1, t == 0 ? 2 : 3, t == 0 ? 4 : 5};
+  double acc = 0.0;
+  for (int c = 0; c < 3; ++c) {
+    const int i = ci[c], j = cj[c];
+    if (i < 1 || j < 1 || i > cD.G - 2 || j > cD.G - 2) continue;
+    const int q = ix(i, j, k, l);
+    for (int d = 0; d < 3; ++d)
+      acc += y[d * n + q] * (P2(cG.coef_diff, d * 6 + e0[c], i, j, l) + P2(cG.coef_diff, d * 6 + e1[c], i, j, l));
+  }
+  return acc;
+}
+// per triangle point and level: the cotangents of its two raw triangle values
+// (tb[t * npt + point]); zero outside the levels the operator writes
+__global__ void k_ddamp_adj_tri(const double* y, double* tb, int three) {
+  const int p = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (p >= cD.npti) return;
+  const int G = cD.G, KA = cD.KA, n = cD.npti;
+  const int ii = p % G, jj = (p / G) % G, k = (p / (G * G)) % KA, l = p / (G * G * KA);
+  const bool lev = !three || (k >= cD.kmin && k <= cD.kmax);
+  for (int t = 0; t < 2; ++t) {
+    double v = 0.0;
+    if (lev && tri_ok(ii, jj)) {
+      v = dd_tbar_gathered(y, ii, jj, k, l, t);
+      if (three && t == 0 && ii == 0 && jj == 0) v = v * (double)cG.pntmask[l * 2 + 0];
+      if (three && t == 1 && ii == 1 && jj == 0)
+        v = v + dd_tbar_gathered(y, 0, 0, k, l, 0) * (double)cG.pntmask[l * 2 + 1];
+    }
+    tb[t * n + p] = v;
+  }
+}
+// sum over the triangles holding point (i, j) at level k of weight(t, vertex, ii, jj) x tb
+template <class W>
+__device__ __forceinline__ double dd_gather_pt(const double* tb, int i, int j, int k, int l, W w) {
+  const int oi[6] = {0, 0, -1, -1, -1, 0}, oj[6] = {0, 0, 0, -1, -1, -1};
+  const int tt[6] = {0, 1, 0, 0, 1, 1}, mm[6] = {0, 0, 1, 2, 1, 2};
+  double acc = 0.0;
+  for (int c = 0; c < 6; ++c) {
+    const int ii = i + oi[c], jj = j + oj[c];
+    if (!tri_ok(ii, jj)) continue;
+    acc += w(tt[c], mm[c], ii, jj) * tb[tt[c] * cD.npti + ix(ii, jj, k, l)];
+  }
+  return acc;
+}
+// the 3-D vertical flux's cotangent at point (i, j), half level kp
+__device__ double dd_rwvbar(const double* tb, int i, int j, int kp, int l) {
+  if (kp < cD.kmin + 1 || kp > cD.kmax) return 0.0;
+  auto one = [](int, int, int, int) { return 1.0; };
+  const double up = dd_gather_pt(tb, i, j, kp - 1, l, one) * cC.rdgz[kp - 1] / 3.0;
+  const double dn = dd_gather_pt(tb, i, j, kp, l, one) * cC.rdgz[kp] / 3.0;
+  return up - dn;
+}
+// per point: the inputs' cotangents (three components, and rhogw in 3-D)
+__global__ void k_ddamp_adj_pt(const double* tb, double* g, int three) {
+  const int p = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (p >= cD.npti) return;
+  const int G = cD.G, KA = cD.KA, n = cD.npti;
+  const int i = p % G, j = (p / G) % G, k = (p / (G * G)) % KA, l = p / (G * G * KA);
+  const bool lev = !three || (k >= cD.kmin && k <= cD.kmax);
+  double r0 = 0.0, r1 = 0.0;
+  if (three) {
+    r0 = dd_rwvbar(tb, i, j, k, l);
+    r1 = (k + 1 < KA) ? dd_rwvbar(tb, i, j, k + 1, l) : 0.0;
+  }
+  for (int dir = 0; dir < 3; ++dir) {
+    double acc = 0.0;
+    if (lev) {
+      acc = dd_gather_pt(tb, i, j, k, l, [&](int t, int m, int ii, int jj) {
+        return P2(cG.coef_intp, (dir * 3 + m) * 2 + t, ii, jj, l);
+      });
+      if (three) acc = acc * gam_at(cG.RGAM, p);
+    }
+    if (three) {
+      const int n6 = cD.npti;
+      if (r0 != 0.0) acc += r0 * gam_at(cG.RGAMH, p) * cG.C2WGz[(2 * dir) * n6 + p];
+      if (r1 != 0.0) {
+        const int pu = p + cD.planei;
+        acc += r1 * gam_at(cG.RGAMH, pu) * cG.C2WGz[(2 * dir + 1) * n6 + pu];
+      }
+    }
+    g[dir * n + p] = acc;
+  }
+  if (three) g[3 * n + p] = r0 * cG.RGSQRTH[p];
+}
+// the pole rows' adjoint (one thread per level and pole)
+__global__ void k_ddamp_adj_pl(const double* y, double* g, int three) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.KA * cD.LP) return;
+  const int k = t / cD.LP, lp = t % cD.LP, np = cD.npl, KA = cD.KA;
+  const int nc = three ? 4 : 3;
+  // the triangles' cotangents at level kk (zero where the operator writes nothing)
+  auto sbar = [&](int kk, double out[5]) {
+    for (int vv = 0; vv < 5; ++vv) out[vv] = 0.0;
+    if (kk < 0 || kk >= KA || (three && (kk < cD.kmin || kk > cD.kmax))) return;
+    for (int vv = 1; vv <= 5; ++vv) {
+      const int vp1 = (vv == 5) ? 1 : vv + 1;
+      double acc = 0.0;
+      for (int d = 0; d < 3; ++d)
+        acc += y[d * np + ipl(0, kk, lp)] *
+               (cG.coef_diff_pl[(vv * cD.LP + lp) * 3 + d] + cG.coef_diff_pl[(vp1 * cD.LP + lp) * 3 + d]);
+      out[vv - 1] = acc;
+    }
+  };
+  double sb[5];
+  sbar(k, sb);
+  double gv[6][4] = {};
+  for (int vv = 1; vv <= 5; ++vv) {
+    const int vp1 = (vv == 5) ? 1 : vv + 1;
+    const double* cI = cG.coef_intp_pl + (vv * cD.LP + lp) * 9;
+    for (int d = 0; d < 3; ++d) {
+      gv[0][d] += cI[d * 3 + 0] * sb[vv - 1];
+      gv[vv][d] += cI[d * 3 + 1] * sb[vv - 1];
+      gv[vp1][d] += cI[d * 3 + 2] * sb[vv - 1];
+    }
+  }
+  if (three) {
+    for (int g_ = 0; g_ < 6; ++g_)
+      for (int d = 0; d < 3; ++d) gv[g_][d] = gv[g_][d] * gam_at(cG.RGAM_pl, ipl(g_, k, lp));
+    // the vertical flux's cotangent at pole point g_, half level kp: the triangles holding g_
+    auto rbar = [&](int g_, int kp) {
+      if (kp < cD.kmin + 1 || kp > cD.kmax) return 0.0;
+      double su[5], sd[5];
+      sbar(kp - 1, su);
+      sbar(kp, sd);
+      double up = 0.0, dn = 0.0;
+      for (int vv = 1; vv <= 5; ++vv) {
+        const int vp1 = (vv == 5) ? 1 : vv + 1;
+        if (g_ == 0 || g_ == vv || g_ == vp1) {
+          up += su[vv - 1];
+          dn += sd[vv - 1];
+        }
+      }
+      return up * cC.rdgz[kp - 1] / 3.0 - dn * cC.rdgz[kp] / 3.0;
+    };
+    for (int g_ = 0; g_ < 6; ++g_) {
+      const double r0 = rbar(g_, k), r1 = (k + 1 < KA) ? rbar(g_, k + 1) : 0.0;
+      const int q = ipl(g_, k, lp);
+      for (int d = 0; d < 3; ++d) {
+        if (r0 != 0.0) gv[g_][d] += r0 * gam_at(cG.RGAMH_pl, q) * cG.C2WGz_pl[q * 6 + 2 * d];
+        if (r1 != 0.0) {
+          const int qu = ipl(g_, k + 1, lp);
+          gv[g_][d] += r1 * gam_at(cG.RGAMH_pl, qu) * cG.C2WGz_pl[qu * 6 + 2 * d + 1];
+        }
+      }
+      gv[g_][3] = r0 * cG.RGSQRTH_pl[q];
+    }
+  }
+  for (int g_ = 0; g_ < 6; ++g_)
+    for (int c = 0; c < nc; ++c) g[c * np + ipl(g_, k, lp)] = gv[g_][c];
+}
+
 }  // namespace nc

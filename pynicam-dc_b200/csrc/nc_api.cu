@@ -408,7 +408,8 @@ struct nc_handle {
   cudaEvent_t ev_user = nullptr;   // ordering against a caller's stream (device-pointer marshal)
   double *stage_out = nullptr, *stage_out_pl = nullptr;
   double* adj_work = nullptr;   // exchanged copy of the Laplacian's input (allocated on first use)
-  double* adj_work6 = nullptr;   // the diffusion adjoint's triangle cotangents (6 fields)
+  double* adj_work6 = nullptr;   // the diffusion / divergence-damping adjoints' triangle cotangents (6 fields)
+  double* adj_work4 = nullptr;   // exchanged copy of the 3-D divergence damping's four momenta (first use)
   double* adj_work3 = nullptr;  // exchanged copy of the divergence's three components (first use)
   // linearised tracer step (nc_trc_step_lin): work fields allocated on first use
   FieldPair lin[20];
@@ -2937,6 +2938,50 @@ int nc_diffusion(nc_handle* h, int32_t transpose, const double* kh, const double
     TRY(comm_fields(h, s, s_pl, 1, true));
   }
   return before_caller(h, stream);
+}
+
+// the 3-D (three = 1: four input components) or 2-D (three input components)
+// divergence damping after the exchange of its inputs, or its adjoint
+static int ddamp(nc_handle* h, int three, int32_t transpose, double* v, double* v_pl, double* y, double* y_pl,
+                 void* stream, const char* name) {
+  TRY(adj_ready(h, name));
+  if (!v || !v_pl || !y || !y_pl) return fail(NC_ERR_ARG, std::string(name) + ": null pointer");
+  if (v == y || v_pl == y_pl) return fail(NC_ERR_ARG, std::string(name) + ": input and output must not alias");
+  const Dims& D = h->D;
+  const int nc = three ? 4 : 3;
+  const unsigned gr = (unsigned)((D.npt + 255) / 256), gp = (unsigned)((D.KA * D.LP + 127) / 128);
+  TRY(after_caller(h, stream));
+  if (!transpose) {
+    double** wp = three ? &h->adj_work4 : &h->adj_work3;
+    if (!*wp) TRY(dev_alloc(h, wp, (size_t)nc * ((size_t)D.npt + D.npl)));
+    double* w = *wp;
+    double* w_pl = w + (size_t)nc * D.npt;
+    CU(cudaMemcpyAsync(w, v, (size_t)nc * D.npt * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CU(cudaMemcpyAsync(w_pl, v_pl, (size_t)nc * D.npl * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    TRY(comm_fields(h, w, w_pl, nc, false));
+    k_ddamp_fwd<<<gr, 256, 0, h->stream>>>(w, y, three);
+    TRY(check_launch(h, "ddamp"));
+    k_ddamp_fwd_pl<<<gp, 128, 0, h->stream>>>(w_pl, y_pl, three);
+    TRY(check_launch(h, "ddamp_pl"));
+  } else {
+    if (!h->adj_work6) TRY(dev_alloc(h, &h->adj_work6, 6 * (size_t)D.npt));
+    k_ddamp_adj_tri<<<gr, 256, 0, h->stream>>>(y, h->adj_work6, three);
+    TRY(check_launch(h, "ddamp_adj_tri"));
+    k_ddamp_adj_pt<<<gr, 256, 0, h->stream>>>(h->adj_work6, v, three);
+    TRY(check_launch(h, "ddamp_adj_pt"));
+    k_ddamp_adj_pl<<<gp, 128, 0, h->stream>>>(y_pl, v_pl, three);
+    TRY(check_launch(h, "ddamp_adj_pl"));
+    TRY(comm_fields(h, v, v_pl, nc, true));
+  }
+  return before_caller(h, stream);
+}
+
+int nc_divdamp3d(nc_handle* h, int32_t transpose, double* v, double* v_pl, double* y, double* y_pl, void* stream) {
+  return ddamp(h, 1, transpose, v, v_pl, y, y_pl, stream, "nc_divdamp3d");
+}
+
+int nc_divdamp2d(nc_handle* h, int32_t transpose, double* v, double* v_pl, double* y, double* y_pl, void* stream) {
+  return ddamp(h, 0, transpose, v, v_pl, y, y_pl, stream, "nc_divdamp2d");
 }
 
 int nc_gradient(nc_handle* h, int32_t transpose, double* q, double* q_pl, double* g, double* g_pl, void* stream) {

@@ -35,7 +35,7 @@ EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_sta
            "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",
            "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_forcing_step", "nc_history_vars", "nc_restart_pack",
            "nc_restart_unpack", "nc_restart_finish", "nc_divide_known", "nc_vsolve", "nc_vadv_lin", "nc_laplacian",
-           "nc_trc_step_lin", "nc_set_time", "nc_trc_prepare", "nc_divergence", "nc_gradient", "nc_diffusion", "nc_forcing_precip", "nc_last_error", "nc_destroy")
+           "nc_trc_step_lin", "nc_set_time", "nc_trc_prepare", "nc_divergence", "nc_gradient", "nc_diffusion", "nc_divdamp3d", "nc_divdamp2d", "nc_forcing_precip", "nc_last_error", "nc_destroy")
 
 
 def load_library(path: str = LIB_PATH):
@@ -98,8 +98,10 @@ def load_library(path: str = LIB_PATH):
     lib.nc_forcing_precip.restype = ctypes.c_int
     lib.nc_gradient.argtypes = [vp, i32, dp, dp, dp, dp, vp]
     lib.nc_diffusion.argtypes = [vp, i32, dp, dp, dp, dp, dp, dp, vp]
+    lib.nc_divdamp3d.argtypes = [vp, i32, dp, dp, dp, dp, vp]
+    lib.nc_divdamp2d.argtypes = [vp, i32, dp, dp, dp, dp, vp]
     for f in ("nc_vsolve", "nc_vadv_lin", "nc_laplacian", "nc_trc_step_lin", "nc_set_time", "nc_trc_prepare",
-              "nc_divergence", "nc_gradient", "nc_diffusion"):
+              "nc_divergence", "nc_gradient", "nc_diffusion", "nc_divdamp3d", "nc_divdamp2d"):
         getattr(lib, f).restype = ctypes.c_int
     lib.nc_destroy.argtypes = [vp]
     lib.nc_destroy.restype = None
@@ -525,6 +527,22 @@ class NicamCuda:
         st = torch.cuda.current_stream(s.device).cuda_stream
         _check(self._lib.nc_diffusion(self._h, int(transpose), self._dev(kh), self._dev(kh_pl, True), self._dev(s),
                                       self._dev(s_pl, True), self._dev(y), self._dev(y_pl, True), st))
+
+    def divdamp3d(self, v, v_pl, y, y_pl, transpose: bool = False):
+        """nc_divdamp3d: y = D3(C(v)) (v of shape (4,) + field shape: the four
+        momenta; y (3,) + field shape), or v = C^T D3^T y with transpose"""
+        import torch
+        st = torch.cuda.current_stream(y.device).cuda_stream
+        _check(self._lib.nc_divdamp3d(self._h, int(transpose), self._dev(v, comps=4), self._dev(v_pl, True, 4),
+                                      self._dev(y, comps=3), self._dev(y_pl, True, 3), st))
+
+    def divdamp2d(self, v, v_pl, y, y_pl, transpose: bool = False):
+        """nc_divdamp2d: y = D2(C(v)) (v and y of shape (3,) + field shape), or
+        v = C^T D2^T y with transpose"""
+        import torch
+        st = torch.cuda.current_stream(y.device).cuda_stream
+        _check(self._lib.nc_divdamp2d(self._h, int(transpose), self._dev(v, comps=3), self._dev(v_pl, True, 3),
+                                      self._dev(y, comps=3), self._dev(y_pl, True, 3), st))
 
     def trc_prepare(self):
         """offline advection: the uploaded state's winds onto the handle as

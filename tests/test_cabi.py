@@ -14,7 +14,7 @@ def declared_functions():
     import glob
     src = "".join(open(f).read() for f in sorted(glob.glob(os.path.join(ROOT, "include", "*.h"))))
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(nc_[a-z_]+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(nc_[a-z0-9_]+)\s*\(", src)))
 
 
 def test_header_and_binding_agree(pkg):

@@ -452,7 +452,100 @@ def test_dot_product_hyperdiffusion(gl04):
     dx_pl = (_rand_like(x_pl, 42) * x_pl.abs().mean(dim=(1, 2, 3), keepdim=True)).requires_grad_(True)
     y, y_pl = adj.hyperdiffusion(core, dx, dx_pl, rg, rg_pl, fixed)
     wy, wy_pl = _rand_like(y, 43), _rand_like(y_pl, 44)
-    lhs = float((y * wy).sum() + (y_pl * wy_pl).sum())
+    lhs = float((y * wy).sum().detach() + (y_pl * wy_pl).sum().detach())
+    gx, gx_pl = torch.autograd.grad((y * wy).sum() + (y_pl * wy_pl).sum(), (dx, dx_pl))
+    rhs = float((dx * gx).sum() + (dx_pl * gx_pl).sum())
+    scale = float((y * wy).abs().sum() + (y_pl * wy_pl).abs().sum())
+    assert abs(lhs - rhs) <= 1e-12 * scale, (lhs, rhs)
+
+
+def _momenta(geo, f):
+    """the four momenta (rhogvx, rhogvy, rhogvz, rhogw) of the case's state,
+    exchanged, in the reference layout and the device layout"""
+    from oracle import nicam_step as O
+    import torch
+    _, adj = _mods()
+    G = O.Geo(geo)
+    s, sp = f["state"].copy(), f["state_pl"].copy()
+    O.comm(G, s, sp)
+    ref = [s[..., n] for n in range(1, 5)], [sp[..., n] for n in range(1, 5)]
+    v = torch.stack([adj.to_device_layout(a) for a in ref[0]])
+    v_pl = torch.stack([torch.as_tensor(np.ascontiguousarray(a)) for a in ref[1]]).cuda()
+    return G, ref, v, v_pl
+
+
+def test_divdamp_operators_equal_oracle(gl04):
+    """exchange + the 3-D divergence damping operator of the four momenta, and
+    exchange + the 2-D operator of three components, against the oracle's
+    comm + divdamp3d / divdamp (same expressions: bit for bit)"""
+    from oracle import nicam_step as O
+    import torch
+    _, adj = _mods()
+    geo, core, f = gl04
+    G, (r, r_pl), v, v_pl = _momenta(geo, f)
+    y, y_pl = torch.empty_like(v[:3]), torch.empty_like(v_pl[:3])
+    core.divdamp3d(v, v_pl, y, y_pl)
+    want, want_pl = O.divdamp3d(G, *r), O.divdamp3d_pl(G, *r_pl)
+    for d in range(3):
+        assert np.array_equal(adj.from_device_layout(y[d]), want[d]), d
+        assert np.array_equal(y_pl[d].cpu().numpy(), want_pl[d]), d
+    w, w_pl = _three(f, 51)
+    core.divdamp2d(w, w_pl, y, y_pl)
+    a = np.stack([adj.from_device_layout(t) for t in w], -1)
+    a_pl = np.ascontiguousarray(np.moveaxis(w_pl.cpu().numpy(), 0, -1))
+    O.comm(G, a, a_pl)
+    want = O.divdamp(G, a[..., 0], a[..., 1], a[..., 2])
+    want_pl = O.divdamp_pl(G, a_pl[..., 0], a_pl[..., 1], a_pl[..., 2])
+    for d in range(3):
+        assert np.array_equal(adj.from_device_layout(y[d]), want[d]), d
+        assert np.array_equal(y_pl[d].cpu().numpy(), want_pl[d]), d
+
+
+def test_divergence_damping_equals_oracle(gl04):
+    """the divergence damping tendency composed from the differentiable
+    operators against the oracle's numfilter_divdamp (mod_numfilter.py:
+    2032-2268) on interior cells and the pole point: relative max difference
+    <= 1e-12"""
+    from oracle import nicam_step as O
+    _, adj = _mods()
+    geo, core, f = gl04
+    G, (r, r_pl), v, v_pl = _momenta(geo, f)
+    got, got_pl = adj.divergence_damping(core, v, v_pl, adj.hdiff_setup(geo))
+    want, want_pl = O.numfilter_divdamp(G, *r, *r_pl)
+    for d in range(3):
+        a, b = adj.from_device_layout(got[d])[1:-1, 1:-1], want[d][1:-1, 1:-1]
+        tol = 1e-12 * max(np.abs(b).max(), 1e-300)
+        assert np.abs(a - b).max() <= tol, d
+        assert np.abs(got_pl[d][0].cpu().numpy() - want_pl[d][0]).max() <= tol, d
+
+
+def test_dot_product_divdamp(gl04):
+    """<D dx, dy> = <dx, D^T dy> for both operators (their transposes with
+    the exchange's adjoint) and for the whole tendency through autograd"""
+    import torch
+    _, adj = _mods()
+    geo, core, f = gl04
+    _, _, v, v_pl = _momenta(geo, f)
+    sc = v.abs().mean(dim=(1, 2, 3, 4), keepdim=True)
+    sc_pl = v_pl.abs().mean(dim=(1, 2, 3), keepdim=True)
+    for three in (True, False):
+        nc = 4 if three else 3
+        op = core.divdamp3d if three else core.divdamp2d
+        x, x_pl = _rand_like(v[:nc], 61) * sc[:nc], _rand_like(v_pl[:nc], 62) * sc_pl[:nc]
+        y, y_pl = _rand_like(v[:3], 63), _rand_like(v_pl[:3], 64)
+        tl, tl_pl = torch.empty_like(y), torch.empty_like(y_pl)
+        ad, ad_pl = torch.empty_like(x), torch.empty_like(x_pl)
+        op(x, x_pl, tl, tl_pl)
+        op(ad, ad_pl, y, y_pl, transpose=True)
+        lhs = _dot(tl, y) + _dot(tl_pl, y_pl)
+        rhs = _dot(x, ad) + _dot(x_pl, ad_pl)
+        scale = float((tl * y).abs().sum() + (tl_pl * y_pl).abs().sum())
+        assert _dot_rel(lhs, rhs, scale) <= 1e-12, (three, lhs, rhs)
+    dx = (_rand_like(v, 65) * sc).requires_grad_(True)
+    dx_pl = (_rand_like(v_pl, 66) * sc_pl).requires_grad_(True)
+    y, y_pl = adj.divergence_damping(core, dx, dx_pl, adj.hdiff_setup(geo))
+    wy, wy_pl = _rand_like(y, 67), _rand_like(y_pl, 68)
+    lhs = float((y * wy).sum().detach() + (y_pl * wy_pl).sum().detach())
     gx, gx_pl = torch.autograd.grad((y * wy).sum() + (y_pl * wy_pl).sum(), (dx, dx_pl))
     rhs = float((dx * gx).sum() + (dx_pl * gx_pl).sum())
     scale = float((y * wy).abs().sum() + (y_pl * wy_pl).abs().sum())
