@@ -413,6 +413,20 @@ int nc_gradient(nc_handle* h, int32_t transpose, double* q, double* q_pl, double
 int nc_diffusion(nc_handle* h, int32_t transpose, const double* kh, const double* kh_pl, double* s, double* s_pl,
                  double* y, double* y_pl, void* stream);
 
+/* The Kh-weighted diffusion's coefficient cotangent: gkh = the derivative of
+ * <y, Dk(C(s))> with respect to kh (the diffusion is bilinear in s and kh;
+ * kernels/oprtdiffusion.py), every regional point and pole row written, s
+ * exchanged in a scratch copy; float64 device buffers, caller's stream. */
+int nc_diffusion_kh(nc_handle* h, double* s, double* s_pl, const double* y, const double* y_pl, double* gkh,
+                    double* gkh_pl, void* stream);
+
+/* The halo exchange (share/mod_comm.py:1563-1644: region edges, pole rows,
+ * singular points) of nf float64 fields in place, device buffers in the
+ * library's field layout, fields one after the other, ordered on the
+ * caller's stream; transpose = 1 applies its adjoint in place (each halo
+ * value added into its source, the halo values then zeroed). */
+int nc_exchange(nc_handle* h, int32_t transpose, double* x, double* x_pl, int32_t nf, void* stream);
+
 /* The divergence damping's two operators (mod_numfilter.py:2032-2268) after
  * the halo exchange of their inputs, and their adjoints, float64, device
  * buffers in the library's field layout, components one after the other,

@@ -241,27 +241,80 @@ class Gradient(torch.autograd.Function):
 class Diffusion(torch.autograd.Function):
     """(y, y_pl) = Dk(C(s, s_pl)): halo exchange then the kh-weighted
     diffusion of the hyperdiffusion's scalar pass (kernels/oprtdiffusion.py);
-    linear in s, with the coefficient field (kh, kh_pl) held fixed (no
-    cotangent for it)"""
+    bilinear in s and the coefficient field (kh, kh_pl): the s cotangent is
+    the transposed operator, the kh cotangent ``nc_diffusion_kh``"""
 
     @staticmethod
     def forward(ctx, core, s, s_pl, kh, kh_pl):
-        kh, kh_pl = _c(kh.detach()), _c(kh_pl.detach())
+        s, s_pl, kh, kh_pl = _c(s), _c(s_pl), _c(kh), _c(kh_pl)
         y, y_pl = torch.empty_like(s), torch.empty_like(s_pl)
-        core.diffusion(kh, kh_pl, _c(s), _c(s_pl), y, y_pl)
+        core.diffusion(kh, kh_pl, s, s_pl, y, y_pl)
         ctx.core = core
-        ctx.save_for_backward(kh, kh_pl)
+        ctx.save_for_backward(s, s_pl, kh, kh_pl)
+        ctx.save_for_forward(s, s_pl, kh, kh_pl)
         return y, y_pl
 
     @staticmethod
     def backward(ctx, gy, gy_pl):
         core = ctx.core
-        kh, kh_pl = ctx.saved_tensors
+        s, s_pl, kh, kh_pl = ctx.saved_tensors
         gy = torch.zeros_like(kh) if gy is None else _c(gy)
         gy_pl = torch.zeros_like(kh_pl) if gy_pl is None else _c(gy_pl)
-        g, g_pl = torch.empty_like(gy), torch.empty_like(gy_pl)
-        core.diffusion(kh, kh_pl, g, g_pl, gy, gy_pl, transpose=True)
-        return None, g, g_pl, None, None
+        g = g_pl = gk = gk_pl = None
+        if ctx.needs_input_grad[1] or ctx.needs_input_grad[2]:
+            g, g_pl = torch.empty_like(gy), torch.empty_like(gy_pl)
+            core.diffusion(kh, kh_pl, g, g_pl, gy, gy_pl, transpose=True)
+        if ctx.needs_input_grad[3] or ctx.needs_input_grad[4]:
+            gk, gk_pl = torch.empty_like(gy), torch.empty_like(gy_pl)
+            core.diffusion_kh(s, s_pl, gy, gy_pl, gk, gk_pl)
+        return None, g, g_pl, gk, gk_pl
+
+    @staticmethod
+    def jvp(ctx, _core, ds, ds_pl, dkh, dkh_pl):
+        core = ctx.core
+        s, s_pl, kh, kh_pl = ctx.saved_tensors
+        y, y_pl = torch.zeros_like(s), torch.zeros_like(s_pl)
+        t, t_pl = torch.empty_like(s), torch.empty_like(s_pl)
+        if ds is not None or ds_pl is not None:
+            ds = torch.zeros_like(s) if ds is None else _c(ds)
+            ds_pl = torch.zeros_like(s_pl) if ds_pl is None else _c(ds_pl)
+            core.diffusion(kh, kh_pl, ds, ds_pl, t, t_pl)
+            y, y_pl = y + t, y_pl + t_pl
+        if dkh is not None or dkh_pl is not None:
+            dkh = torch.zeros_like(kh) if dkh is None else _c(dkh)
+            dkh_pl = torch.zeros_like(kh_pl) if dkh_pl is None else _c(dkh_pl)
+            core.diffusion(dkh, dkh_pl, s, s_pl, t, t_pl)
+            y, y_pl = y + t, y_pl + t_pl
+        return y, y_pl
+
+
+class Exchange(torch.autograd.Function):
+    """(y, y_pl) = C(x, x_pl): the halo exchange (share/mod_comm.py:1563-1644)
+    of one field or of (nf,) stacked fields, out of place; linear"""
+
+    @staticmethod
+    def forward(ctx, core, x, x_pl):
+        y, y_pl = x.detach().clone(memory_format=torch.contiguous_format), \
+            x_pl.detach().clone(memory_format=torch.contiguous_format)
+        core.exchange(y, y_pl)
+        ctx.core = core
+        return y, y_pl
+
+    @staticmethod
+    def backward(ctx, gy, gy_pl):
+        g, g_pl = gy.clone(memory_format=torch.contiguous_format), gy_pl.clone(memory_format=torch.contiguous_format)
+        ctx.core.exchange(g, g_pl, transpose=True)
+        return None, g, g_pl
+
+    @staticmethod
+    def jvp(ctx, _core, dx, dx_pl):
+        y, y_pl = dx.clone(memory_format=torch.contiguous_format), dx_pl.clone(memory_format=torch.contiguous_format)
+        ctx.core.exchange(y, y_pl)
+        return y, y_pl
+
+
+def exchange(core, x, x_pl):
+    return Exchange.apply(core, x, x_pl)
 
 
 def diffusion(core, s, s_pl, kh, kh_pl):
@@ -294,6 +347,10 @@ class _DivDamp(torch.autograd.Function):
         g, g_pl = z(sv), z(sv_pl)
         op(g, g_pl, gy, gy_pl, transpose=True)
         return None, None, g, g_pl
+
+    @staticmethod
+    def jvp(ctx, _core, _three, dv, dv_pl):
+        return _DivDamp.forward(ctx, ctx.core, ctx.three, dv, dv_pl)
 
 
 def divdamp3d(core, v, v_pl):

@@ -1341,4 +1341,71 @@ __global__ void k_ddamp_adj_pl(const double* y, double* g, int three) {
     for (int c = 0; c < nc; ++c) g[c * np + ipl(g_, k, lp)] = gv[g_][c];
 }
 
+// ---------------------------------------------------------------------------
+// The Kh-weighted diffusion's dependence on its coefficient field: y is
+// bilinear in (s, kh) through the edge weights kf_e = (kh(cell) + kh(edge
+// neighbour e)) / 2, so d<ybar, y>/d kh gathers, for every point, half of
+// ybar x E_e at the cells whose weight kf_e it enters (as the cell itself, or
+// as the neighbour across edge e), E_e = sum over directions of coef_diff x
+// the edge's pair of (fixed) triangle values of the exchanged s.
+// ---------------------------------------------------------------------------
+__device__ void diff_edge_sums(const double* s, int i, int j, int k, int l, double E[6]) {
+  for (int e = 0; e < 6; ++e) E[e] = 0.0;
+  for (int d = 0; d < 3; ++d) {
+    const double aTI = diff_tri_fixed(s, i, j, k, l, d, 0), aTJ = diff_tri_fixed(s, i, j, k, l, d, 1);
+    const double bTI = diff_tri_fixed(s, i - 1, j, k, l, d, 0);
+    const double cTI = diff_tri_fixed(s, i - 1, j - 1, k, l, d, 0), cTJ = diff_tri_fixed(s, i - 1, j - 1, k, l, d, 1);
+    const double dTJ = diff_tri_fixed(s, i, j - 1, k, l, d, 1);
+    const double pr[6] = {aTI + aTJ, aTJ + bTI, bTI + cTJ, cTJ + cTI, cTI + dTJ, dTJ + aTI};
+    for (int e = 0; e < 6; ++e) E[e] += P2(cG.coef_diff, d * 6 + e, i, j, l) * pr[e];
+  }
+}
+__global__ void k_diff_khbar(const double* s, const double* y, double* gkh) {
+  const int p = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (p >= cD.npti) return;
+  const int G = cD.G, KA = cD.KA;
+  const int i = p % G, j = (p / G) % G, k = (p / (G * G)) % KA, l = p / (G * G * KA);
+  // the edge-e neighbour of cell (i, j) is (i + oi[e], j + oj[e]) (the order of diff_kf)
+  const int oi[6] = {1, 0, -1, -1, 0, 1}, oj[6] = {1, 1, 0, -1, -1, 0};
+  double E[6], acc = 0.0;
+  if (interior(i, j)) {
+    diff_edge_sums(s, i, j, k, l, E);
+    const double yp = y[ix(i, j, k, l)];
+    for (int e = 0; e < 6; ++e) acc += 0.5 * yp * E[e];
+  }
+  for (int e = 0; e < 6; ++e) {
+    const int ci = i - oi[e], cj = j - oj[e];
+    if (ci < 1 || cj < 1 || ci > G - 2 || cj > G - 2) continue;
+    diff_edge_sums(s, ci, cj, k, l, E);
+    acc += 0.5 * y[ix(ci, cj, k, l)] * E[e];
+  }
+  gkh[p] = acc;
+}
+__global__ void k_diff_khbar_pl(const double* s, const double* y, double* gkh) {
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= cD.KA * cD.LP) return;
+  const int k = t / cD.LP, lp = t % cD.LP;
+  const double sn = s[ipl(0, k, lp)], y0 = y[ipl(0, k, lp)];
+  double vt[5][3];
+  for (int v = 1; v <= 5; ++v) {
+    const int vp1 = (v == 5) ? 1 : v + 1;
+    const double sij = s[ipl(v, k, lp)], sp1 = s[ipl(vp1, k, lp)];
+    for (int d = 0; d < 3; ++d) {
+      const double* cI = cG.coef_intp_pl + ((v * cD.LP + lp) * 3 + d) * 3;
+      const double c0 = cI[0], c1 = cI[1], c2 = cI[2];
+      vt[v - 1][d] = div3((2.0 * c0 - c1 - c2) * sn + (-c0 + 2.0 * c1 - c2) * sij + (-c0 - c1 + 2.0 * c2) * sp1);
+    }
+  }
+  double g0 = 0.0;
+  gkh[ipl(0, k, lp)] = 0.0;
+  for (int v = 1; v <= 5; ++v) {
+    const int vm1 = (v == 1) ? 5 : v - 1;
+    double sd = 0.0;
+    for (int d = 0; d < 3; ++d) sd += cG.coef_diff_pl[(v * cD.LP + lp) * 3 + d] * (vt[vm1 - 1][d] + vt[v - 1][d]);
+    g0 += 0.5 * y0 * sd;
+    gkh[ipl(v, k, lp)] = 0.5 * y0 * sd;
+  }
+  gkh[ipl(0, k, lp)] = g0;
+}
+
 }  // namespace nc

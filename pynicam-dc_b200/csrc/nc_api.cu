@@ -2881,6 +2881,15 @@ static int comm_fields(nc_handle* h, double* r, double* p, int nf, bool adjoint)
   return 0;
 }
 
+int nc_exchange(nc_handle* h, int32_t transpose, double* x, double* x_pl, int32_t nf, void* stream) {
+  TRY(adj_ready(h, "nc_exchange"));
+  if (!x || !x_pl) return fail(NC_ERR_ARG, "nc_exchange: null pointer");
+  if (nf < 1) return fail(NC_ERR_ARG, "nc_exchange: nf must be positive");
+  TRY(after_caller(h, stream));
+  TRY(comm_fields(h, x, x_pl, nf, transpose != 0));
+  return before_caller(h, stream);
+}
+
 int nc_divergence(nc_handle* h, int32_t transpose, double* v, double* v_pl, double* y, double* y_pl, void* stream) {
   TRY(adj_ready(h, "nc_divergence"));
   if (!v || !v_pl || !y || !y_pl) return fail(NC_ERR_ARG, "nc_divergence: null pointer");
@@ -2937,6 +2946,26 @@ int nc_diffusion(nc_handle* h, int32_t transpose, const double* kh, const double
     TRY(check_launch(h, "diff_adj_pl"));
     TRY(comm_fields(h, s, s_pl, 1, true));
   }
+  return before_caller(h, stream);
+}
+
+int nc_diffusion_kh(nc_handle* h, double* s, double* s_pl, const double* y, const double* y_pl, double* gkh,
+                    double* gkh_pl, void* stream) {
+  TRY(adj_ready(h, "nc_diffusion_kh"));
+  if (!s || !s_pl || !y || !y_pl || !gkh || !gkh_pl) return fail(NC_ERR_ARG, "nc_diffusion_kh: null pointer");
+  const Dims& D = h->D;
+  const unsigned gr = (unsigned)((D.npt + 255) / 256), gp = (unsigned)((D.KA * D.LP + 127) / 128);
+  TRY(after_caller(h, stream));
+  if (!h->adj_work) TRY(dev_alloc(h, &h->adj_work, (size_t)D.npt + D.npl));
+  double* w = h->adj_work;
+  double* w_pl = h->adj_work + D.npt;
+  CU(cudaMemcpyAsync(w, s, D.npt * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CU(cudaMemcpyAsync(w_pl, s_pl, (size_t)D.npl * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  TRY(comm_fields(h, w, w_pl, 1, false));
+  k_diff_khbar<<<gr, 256, 0, h->stream>>>(w, y, gkh);
+  TRY(check_launch(h, "diff_khbar"));
+  k_diff_khbar_pl<<<gp, 128, 0, h->stream>>>(w_pl, y_pl, gkh_pl);
+  TRY(check_launch(h, "diff_khbar_pl"));
   return before_caller(h, stream);
 }
 

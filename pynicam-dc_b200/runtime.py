@@ -35,7 +35,7 @@ EXPORTS = ("nc_create", "nc_upload_state", "nc_download_state", "nc_download_sta
            "nc_step", "nc_set_graph", "nc_run_phases", "nc_sync", "nc_mass_sums", "nc_get_field", "nc_state_pointers", "nc_kernel_launches", "nc_stream", "nc_profile",
            "nc_kernel_stats", "nc_grid_spring", "nc_mass_sum_noalloc", "nc_forcing_step", "nc_history_vars", "nc_restart_pack",
            "nc_restart_unpack", "nc_restart_finish", "nc_divide_known", "nc_vsolve", "nc_vadv_lin", "nc_laplacian",
-           "nc_trc_step_lin", "nc_set_time", "nc_trc_prepare", "nc_divergence", "nc_gradient", "nc_diffusion", "nc_divdamp3d", "nc_divdamp2d", "nc_forcing_precip", "nc_last_error", "nc_destroy")
+           "nc_trc_step_lin", "nc_set_time", "nc_trc_prepare", "nc_divergence", "nc_gradient", "nc_diffusion", "nc_divdamp3d", "nc_divdamp2d", "nc_exchange", "nc_diffusion_kh", "nc_forcing_precip", "nc_last_error", "nc_destroy")
 
 
 def load_library(path: str = LIB_PATH):
@@ -100,8 +100,10 @@ def load_library(path: str = LIB_PATH):
     lib.nc_diffusion.argtypes = [vp, i32, dp, dp, dp, dp, dp, dp, vp]
     lib.nc_divdamp3d.argtypes = [vp, i32, dp, dp, dp, dp, vp]
     lib.nc_divdamp2d.argtypes = [vp, i32, dp, dp, dp, dp, vp]
+    lib.nc_exchange.argtypes = [vp, i32, dp, dp, i32, vp]
+    lib.nc_diffusion_kh.argtypes = [vp, dp, dp, dp, dp, dp, dp, vp]
     for f in ("nc_vsolve", "nc_vadv_lin", "nc_laplacian", "nc_trc_step_lin", "nc_set_time", "nc_trc_prepare",
-              "nc_divergence", "nc_gradient", "nc_diffusion", "nc_divdamp3d", "nc_divdamp2d"):
+              "nc_divergence", "nc_gradient", "nc_diffusion", "nc_divdamp3d", "nc_divdamp2d", "nc_exchange", "nc_diffusion_kh"):
         getattr(lib, f).restype = ctypes.c_int
     lib.nc_destroy.argtypes = [vp]
     lib.nc_destroy.restype = None
@@ -527,6 +529,22 @@ class NicamCuda:
         st = torch.cuda.current_stream(s.device).cuda_stream
         _check(self._lib.nc_diffusion(self._h, int(transpose), self._dev(kh), self._dev(kh_pl, True), self._dev(s),
                                       self._dev(s_pl, True), self._dev(y), self._dev(y_pl, True), st))
+
+    def diffusion_kh(self, s, s_pl, y, y_pl, gkh, gkh_pl):
+        """nc_diffusion_kh: gkh = d<y, Dk(C(s))>/dkh"""
+        import torch
+        st = torch.cuda.current_stream(s.device).cuda_stream
+        _check(self._lib.nc_diffusion_kh(self._h, self._dev(s), self._dev(s_pl, True), self._dev(y),
+                                         self._dev(y_pl, True), self._dev(gkh), self._dev(gkh_pl, True), st))
+
+    def exchange(self, x, x_pl, transpose: bool = False):
+        """nc_exchange: the halo exchange of x (nf,) + field shape (or one
+        field) in place, or its adjoint with transpose"""
+        import torch
+        nf = x.shape[0] if x.dim() == len(self.field_shape) + 1 else 0
+        st = torch.cuda.current_stream(x.device).cuda_stream
+        _check(self._lib.nc_exchange(self._h, int(transpose), self._dev(x, comps=nf), self._dev(x_pl, True, nf),
+                                     max(nf, 1), st))
 
     def divdamp3d(self, v, v_pl, y, y_pl, transpose: bool = False):
         """nc_divdamp3d: y = D3(C(v)) (v of shape (4,) + field shape: the four

@@ -398,6 +398,24 @@ def test_dot_product_diffusion(gl04):
     assert _dot_rel(lhs, rhs, scale) <= 1e-12, (lhs, rhs)
 
 
+def test_dot_product_diffusion_kh(gl04):
+    """<Dk'(C(s)) y> for a coefficient direction dk (the forward operator with
+    kh = dk) against <dk, nc_diffusion_kh(s, y)>: the coefficient cotangent"""
+    import torch
+    _, core, f = gl04
+    s, s_pl = _rand_like(f["rhogq"], 81), _rand_like(f["rhogq_pl"], 82)
+    dk, dk_pl = _kh(f, 83)
+    y, y_pl = _rand_like(f["rhogq"], 84), _rand_like(f["rhogq_pl"], 85)
+    tl, tl_pl = torch.empty_like(s), torch.empty_like(s_pl)
+    gk, gk_pl = torch.empty_like(s), torch.empty_like(s_pl)
+    core.diffusion(dk, dk_pl, s, s_pl, tl, tl_pl)
+    core.diffusion_kh(s, s_pl, y, y_pl, gk, gk_pl)
+    lhs = _dot(tl, y) + _dot(tl_pl, y_pl)
+    rhs = _dot(dk, gk) + _dot(dk_pl, gk_pl)
+    scale = float((tl * y).abs().sum() + (tl_pl * y_pl).abs().sum())
+    assert _dot_rel(lhs, rhs, scale) <= 1e-12, (lhs, rhs)
+
+
 def _hdiff_inputs(geo, f):
     """the six fields of the hyperdiffusion (vx, vy, vz, w, tem - tem_bs,
     rho - rho_bs) of the case's state from the oracle's diagnostics, in the
