@@ -482,7 +482,7 @@ def vi_small_step(m, core, PROG, D, eth, rhogd, pregd, gT0, PS, nitr, dt):
     return out
 
 
-def _check_config(m, geo):
+def _check_config(geo):
     for key, what in (("hdiff_nl_kh_max", "NONLINEAR1 hyperdiffusion"), ("rayleigh_coef", "the Rayleigh sponge")):
         if key in geo:
             raise NotImplementedError(f"dynstep: {what} is not part of the differentiable step")
@@ -524,7 +524,7 @@ class DynamicsStep:
 
     def __init__(self, core, geo: dict, device="cuda"):
         self.core, self.m = core, Metrics(geo, device)
-        _check_config(self.m, geo)
+        _check_config(geo)
 
     def step(self, x, x_pl, tracers=None, tracers_pl=None):
         Q = [] if tracers is None else [F(tracers[n], tracers_pl[n]) for n in range(tracers.shape[0])]
