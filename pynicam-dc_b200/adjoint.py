@@ -27,6 +27,19 @@ fields of shape (lall, kall, gall_1d, gall_1d), pole fields (6, kall, 2).
   45-88), linear, adjoints as for the Laplacian (``nc_divergence``,
   ``nc_gradient``).
 
+* ``Diffusion`` -- halo exchange then the Kh-weighted diffusion of the
+  hyperdiffusion's scalar pass (kernels/oprtdiffusion.py), bilinear in the
+  field and the coefficient field: adjoints ``nc_diffusion`` (transposed)
+  and ``nc_diffusion_kh`` (the coefficient's cotangent).
+* ``divdamp3d`` / ``divdamp2d`` -- halo exchange then the divergence
+  damping's 3-D / 2-D operator (kernels/oprt3ddivdamp.py, oprtdivdamp.py),
+  linear (``nc_divdamp3d``, ``nc_divdamp2d``); ``hyperdiffusion`` and
+  ``divergence_damping`` compose the two filters' tendencies.
+* ``Exchange`` -- the halo exchange alone (share/mod_comm.py:1563-1644),
+  linear (``nc_exchange``).
+
+The whole dynamics step built from these operators is ``dynstep.DynamicsStep``.
+
 * ``TracerStep`` -- the whole tracer advection of a step
   (mod_src_tracer.py:83-1228: vertical step, horizontal step with the
   horizontal Thuburn limiter of 2190-2605, vertical step with the clamp, the
