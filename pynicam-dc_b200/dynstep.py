@@ -2,7 +2,7 @@
 
 One RK3-HEVI large step (mod_dynamics.py:1725-2741 with the numpy-path
 operators: Pre_Post diagnostics and boundary conditions, momentum advection,
-hyperdiffusion, the HEVI small steps of mod_vi.py:104-1590 with the 3-D and
+hyperdiffusion (DIRECT or NONLINEAR1 Kh), the Rayleigh sponge, the HEVI small steps of mod_vi.py:104-1590 with the 3-D and
 2-D divergence damping, path 1 and vi_main) restated as torch expressions in
 the reference's operation order, on CUDA tensors in the library's device
 layout (regional (lall, kall, g, g), pole (6, kall, 2): the level axis is
@@ -119,6 +119,15 @@ class Metrics(dict):
         self["kmin"], self["kmax"] = int(_scalar(geo["kmin"])), int(_scalar(geo["kmax"]))
         self["sstep"] = [int(x) for x in np.asarray(geo["sstep"]).reshape(-1)]
         self["hevi"] = A.hevi_metrics(geo, device)
+        vec = lambda k: torch.as_tensor(np.asarray(geo[k], np.float64).reshape(-1)).to(device)
+        self["nl"] = "hdiff_nl_kh_max" in geo           # NONLINEAR1 hyperdiffusion
+        if self["nl"]:
+            self["nl_khmax"] = vec("hdiff_nl_kh_max")
+            self["nl_minlim"], self["nl_area"] = sc("hdiff_nl_minlim"), sc("hdiff_nl_area")
+        self["ray"] = "rayleigh_coef" in geo            # the Rayleigh sponge
+        if self["ray"]:
+            self["ray_c"], self["ray_ch"] = vec("rayleigh_coef"), vec("rayleigh_coef_h")
+            self["ray_only_w"] = bool(int(_scalar(geo["rayleigh_only_w"])))
 
     def lv(self, name, sl):
         """a 1-D level vector sliced and shaped to broadcast along axis 1"""
@@ -333,27 +342,60 @@ def advection_momentum(m, core, D, P):
 # ---------------------------------------------------------------------------
 # numerical filters (mod_numfilter.py)
 # ---------------------------------------------------------------------------
+def hdiff_nonlinear_coef(m, lapT):
+    """mod_numfilter.py:1153-1206 (NONLINEAR1): Kh from the temperature
+    Laplacian of the first pass, 2 AREA^2 / dtl * (|lapT| / 300 * AREA)
+    clipped to [Kh_coef_minlim, kh_max(k)], and its half-level average on
+    kmin+1..kmax (zero elsewhere)"""
+    kmin, kmax, A_ = m["kmin"], m["kmax"], m["nl_area"]
+    c1 = 2.0 * (A_ ** 2) / m["dtl"]
+    hi = m.lv("nl_khmax", slice(None))
+    raw = c1 * (F(lapT.r.abs(), lapT.p.abs()) / 300.0 * A_)
+    kh = F(torch.minimum(torch.clamp(raw.r, min=m["nl_minlim"]), hi.r),
+           torch.minimum(torch.clamp(raw.p, min=m["nl_minlim"]), hi.p))
+    ks, km = slice(kmin + 1, kmax + 1), slice(kmin, kmax)
+    return kh, kh.zeros().setk(ks, 0.5 * (kh.k(ks) + kh.k(km)))
+
+
+def rayleigh_damping(m, f, rhog, D):
+    """mod_numfilter.py:240-271: the momentum tendencies lose
+    rayleigh_coef(k) rhog v (unless only w is damped), the w tendency
+    rayleigh_coef_h(k) w (C2Wa rhog(k) + C2Wb rhog(k-1)), rhog(-1) = 0"""
+    f = list(f)
+    if not m["ray_only_w"]:
+        coef = m.lv("ray_c", slice(None)) * rhog
+        for n, name in ((I_RHOGVX, "vx"), (I_RHOGVY, "vy"), (I_RHOGVZ, "vz")):
+            f[n] = f[n] - coef * D[name]
+    km1 = rhog.zeros().setk(slice(1, None), rhog.k(slice(0, -1)))
+    c = m["C2Wfact"]
+    f[I_RHOGW] = f[I_RHOGW] - m.lv("ray_ch", slice(None)) * D["w"] * (c[0] * rhog + c[1] * km1)
+    return f
+
+
 def hdiffusion(m, core, rhog, D):
-    """mod_numfilter.py:845-1578 (DIRECT Kh, lap_order 2): f_TEND in
-    prognostic order, differentiable in the density through the Kh rhog
-    weights of the scalar pass as well"""
+    """mod_numfilter.py:845-1578 (DIRECT or NONLINEAR1 Kh, lap_order 2):
+    f_TEND in prognostic order, differentiable in the density through the
+    Kh rhog weights of the scalar pass as well"""
     kmin, kmax, Kh = m["kmin"], m["kmax"], m["Kh_coef"]
     c = m["C2Wfact"]
     kk, kd = slice(kmin, kmax + 2), slice(kmin - 1, kmax + 1)
     rhog_h = rhog.zeros().setk(kk, c[0].k(kk) * rhog.k(kk) + c[1].k(kk) * rhog.k(kd))
     vt = [D["vx"], D["vy"], D["vz"], D["w"], D["tem"] - m["tem_bs"], D["rho"] - m["rho_bs"]]
+    KhA = KhH = Kh
     for p in range(2):
         v2 = [lap(core, vt[n]) for n in range(4)]
         if p == 1:
+            if m["nl"]:
+                KhA, KhH = hdiff_nonlinear_coef(m, vt[4])
             for s, fac in ((vt[4], m["CVdry"]), (vt[5], m["hdiff_fact_rho"])):
-                kh = rhog * fac * Kh
+                kh = rhog * fac * KhA
                 v2.append(F(*A.diffusion(core, s.r, s.p, kh.r, kh.p)))
         else:
             v2 += [lap(core, vt[4]), lap(core, vt[5])]
         vt = xch(core, [-a for a in v2])
     f = [None] * 6
-    f[I_RHOGVX], f[I_RHOGVY], f[I_RHOGVZ] = horizontalize(m, *[-(vt[n] * Kh) * rhog for n in range(3)])
-    f[I_RHOGW] = -(vt[3] * Kh) * rhog_h
+    f[I_RHOGVX], f[I_RHOGVY], f[I_RHOGVZ] = horizontalize(m, *[-(vt[n] * KhA) * rhog for n in range(3)])
+    f[I_RHOGW] = -(vt[3] * KhH) * rhog_h
     f[I_RHOGE] = -vt[4]
     f[I_RHOG] = -vt[5]
     return f
@@ -482,12 +524,6 @@ def vi_small_step(m, core, PROG, D, eth, rhogd, pregd, gT0, PS, nitr, dt):
     return out
 
 
-def _check_config(geo):
-    for key, what in (("hdiff_nl_kh_max", "NONLINEAR1 hyperdiffusion"), ("rayleigh_coef", "the Rayleigh sponge")):
-        if key in geo:
-            raise NotImplementedError(f"dynstep: {what} is not part of the differentiable step")
-
-
 def dynamics_step(m, core, prog, tracers=()):
     """one RK3-HEVI large step (mod_dynamics.py:1725-2741) of the six
     prognostic fields ``prog`` (list of ``F``), tracer masses held fixed;
@@ -504,6 +540,8 @@ def dynamics_step(m, core, prog, tracers=()):
         rhogd = (D["rho"] - m["rho_bs"]) * m["GSGAM2"]
         adv = advection_momentum(m, core, D, PROG)
         f = hdiffusion(m, core, PROG[I_RHOG], D)
+        if m["ray"]:
+            f = rayleigh_damping(m, f, PROG[I_RHOG], D)
         gT = [f[I_RHOG], adv[0] + f[I_RHOGVX], adv[1] + f[I_RHOGVY], adv[2] + f[I_RHOGVZ], adv[3] + f[I_RHOGW],
               f[I_RHOGE]]
         PS = [a.zeros() for a in PROG] if nl == 0 else [a - b for a, b in zip(PROG0, PROG)]
@@ -524,7 +562,6 @@ class DynamicsStep:
 
     def __init__(self, core, geo: dict, device="cuda"):
         self.core, self.m = core, Metrics(geo, device)
-        _check_config(geo)
 
     def step(self, x, x_pl, tracers=None, tracers_pl=None):
         Q = [] if tracers is None else [F(tracers[n], tracers_pl[n]) for n in range(tracers.shape[0])]

@@ -116,12 +116,14 @@ class OracleOps:
         x[:, k0:k1 + 1] = torch.stack(xs, 1)
 
 
-def test_step_equals_oracle(golden):
+@pytest.mark.parametrize("case", ["golden", "golden_nlhdiff", "golden_rayleigh"])
+def test_step_equals_oracle(case, request):
     """one large step of the torch composition against the oracle's
-    dynamics_step: relative max difference <= 1e-12 per prognostic"""
+    dynamics_step (DIRECT and NONLINEAR1 hyperdiffusion, the Rayleigh
+    sponge): relative max difference <= 1e-12 per prognostic"""
     from oracle import nicam_step as O
     ds, adj = _mods()
-    geo, st = golden
+    geo, st = request.getfixturevalue(case)
     ops = OracleOps(geo)
     stepper = ds.DynamicsStep(ops, geo, device="cpu")
     s, sp = st["state0"], st["state0_pl"]
