@@ -50,14 +50,6 @@ def _ref_state(x, x_pl, q, q_pl):
     return s, sp
 
 
-@pytest.fixture(scope="module")
-def gl03(pkg, golden):
-    geo, st = golden
-    core = pkg.NicamCuda(geo, graph=False)
-    yield geo, st, core
-    core.close()
-
-
 def _rel_check(y, y_pl, want, want_pl, tol=1e-12):
     _, adj = _mods()
     for n in range(6):
@@ -67,21 +59,27 @@ def _rel_check(y, y_pl, want, want_pl, tol=1e-12):
         assert np.abs(y_pl[n][0].detach().cpu().numpy() - want_pl[0, :, :, n]).max() <= t, n
 
 
-def test_step_equals_oracle_and_handle(gl03):
+@pytest.mark.parametrize("case", ["golden", "golden_nlhdiff", "golden_rayleigh"])
+def test_step_equals_oracle_and_handle(pkg, case, request):
+    """DIRECT and NONLINEAR1 hyperdiffusion, the Rayleigh sponge"""
     from oracle import nicam_step as O
     import torch
     ds, _ = _mods()
-    geo, st, core = gl03
-    s, sp = st["state0"], st["state0_pl"]
-    stepper = ds.DynamicsStep(core, geo)
-    with torch.no_grad():
-        y, y_pl = stepper.step(*_dev_state(s, sp))
-    want, want_pl = O.dynamics_step(O.Geo(geo), s, sp)
-    _rel_check(y, y_pl, want, want_pl)
-    core.upload(s, sp)
-    core.step(1)
-    got, got_pl = core.download()
-    _rel_check(y, y_pl, got, got_pl)
+    geo, st = request.getfixturevalue(case)
+    core = pkg.NicamCuda(geo, graph=False)
+    try:
+        s, sp = st["state0"], st["state0_pl"]
+        stepper = ds.DynamicsStep(core, geo)
+        with torch.no_grad():
+            y, y_pl = stepper.step(*_dev_state(s, sp))
+        want, want_pl = O.dynamics_step(O.Geo(geo), s, sp)
+        _rel_check(y, y_pl, want, want_pl)
+        core.upload(s, sp)
+        core.step(1)
+        got, got_pl = core.download()
+        _rel_check(y, y_pl, got, got_pl)
+    finally:
+        core.close()
 
 
 def _rand_like(t, seed):
@@ -96,12 +94,14 @@ def _scaled(x, x_pl, seed):
     return _rand_like(x, seed) * sc, _rand_like(x_pl, seed + 1) * sc.view(6, 1, 1, 1)
 
 
-def test_dot_product_step(gl03):
+@pytest.mark.parametrize("case", ["golden", "golden_nlhdiff"])
+def test_dot_product_step(pkg, case, request):
     """<J dx, w> = <dx, J^T w> for one large step"""
     import torch
     import torch.autograd.forward_ad as fwAD
     ds, _ = _mods()
-    geo, st, core = gl03
+    geo, st = request.getfixturevalue(case)
+    core = pkg.NicamCuda(geo, graph=False)
     x, x_pl, q, q_pl = _dev_state(st["state0"], st["state0_pl"])
     stepper = ds.DynamicsStep(core, geo)
     dx, dx_pl = _scaled(x, x_pl, 71)
@@ -115,6 +115,7 @@ def test_dot_product_step(gl03):
     lhs = float((ty * w).sum() + (ty_pl * w_pl).sum())
     rhs = float((dx * g).sum() + (dx_pl * g_pl).sum())
     scale = float((ty * w).abs().sum() + (ty_pl * w_pl).abs().sum())
+    core.close()
     assert abs(lhs - rhs) <= 1e-12 * scale, (lhs, rhs, scale)
 
 
