@@ -14,6 +14,7 @@ the Thomas solve ``VerticalSolve``), whose adjoints are hand-written
 transposed kernels; the pointwise and per-column algebra between them is
 differentiated by torch.  The reverse pass of a step is therefore the
 discrete adjoint of the step, and ``run`` checkpoints every large step.
+The Held-Suarez forcing step (``held_suarez``) can follow each step.
 
 The tracer masses are carried through unchanged: the tracer advection of the
 step's last stage (mod_src_tracer.py) is not part of this restatement, and
@@ -111,7 +112,7 @@ class Metrics(dict):
         self["GRD_x"] = [F(dl(gx[:, :, 0:1, :, d]), pl(gxp[:, 0:1, :, d])) for d in range(3)]
         for k in ("rdgz", "rdgzh", "afact", "bfact", "cfact", "dfact"):
             self[k] = torch.as_tensor(np.asarray(geo["GRD_" + k], np.float64)).to(device)
-        for k in ("GRAV", "Rdry", "CVdry", "CPdry", "Rvap", "OHM", "rscale", "alpha", "dtl", "dts", "Kh_coef",
+        for k in ("GRAV", "Rdry", "CVdry", "CPdry", "Rvap", "OHM", "PRE00", "rscale", "alpha", "dtl", "dts", "Kh_coef",
                   "divdamp_coef", "hdiff_fact_rho"):
             self[k] = sc(k)
         self["CVW"] = [float(x) for x in np.asarray(geo["CVW"], np.float64).reshape(-1)]
@@ -552,6 +553,43 @@ def dynamics_step(m, core, prog, tracers=()):
     return xch(core, PROG)
 
 
+# ---------------------------------------------------------------------------
+# Held-Suarez forcing (forcing/mod_af_heldsuarez.py:38-88 applied as in
+# mod_forcing.py:14-28, 323-349): the regional columns only
+# ---------------------------------------------------------------------------
+HS_SIGMA_B, HS_KF, HS_KA, HS_KS, HS_DTH_Z = 0.7, 1.0 / 86400.0, 1.0 / (40.0 * 86400.0), 1.0 / (4.0 * 86400.0), 10.0
+
+
+def held_suarez(m, core, prog, lat, tracers=(), moist=False):
+    """one forcing step: the diagnostics of the regional prognostics, the
+    Held-Suarez tendencies (Rayleigh friction below sigma 0.7, Newtonian
+    relaxation to the equilibrium temperature) applied as
+    PROG + dtl f rho GSGAM2 to the momenta and RHOGE on kmin..kmax, then
+    the halo exchange; ``lat`` the column latitudes (lall, 1, g, g);
+    ``moist`` the moist case's profile (T_eq0 294 K, DT_y 65 K)"""
+    T_eq0, DT_y = (294.0, 65.0) if moist else (315.0, 60.0)
+    kmin, kmax = m["kmin"], m["kmax"]
+    D = diagnostics(m, list(prog), list(tracers), prog[I_RHOGW].zeros())
+    pre, tem = D["pre"].r, D["tem"].r
+    sin2, cos2, cos4 = torch.sin(lat).abs() ** 2, torch.cos(lat).abs() ** 2, torch.cos(lat).abs() ** 4
+    psref = 0.5 * (pre[:, kmin:kmin + 1] + pre[:, kmin - 1:kmin])
+    factor = torch.clamp((pre / psref - HS_SIGMA_B) / (1.0 - HS_SIGMA_B), min=0.0)
+    ap0 = (pre / m["PRE00"]).abs()
+    Kt = HS_KA + (HS_KS - HS_KA) * factor * cos4
+    T_eq = torch.clamp((T_eq0 - DT_y * sin2 - HS_DTH_Z * torch.log(torch.clamp(ap0, min=1e-30)) * cos2)
+                       * ap0 ** (m["Rdry"] / m["CPdry"]), min=200.0)
+    valid = torch.zeros_like(pre)
+    valid[:, kmin:kmax + 1] = 1.0
+    scale = m["dtl"]
+    out = list(prog)
+    for iv, name in ((I_RHOGVX, "vx"), (I_RHOGVY, "vy"), (I_RHOGVZ, "vz")):
+        f = torch.where(valid > 0, -HS_KF * factor * D[name].r, torch.zeros_like(pre))
+        out[iv] = F(prog[iv].r + scale * f * D["rho"].r * m["GSGAM2"].r, prog[iv].p)
+    fe = torch.where(valid > 0, -Kt * (tem - T_eq) * m["CVdry"], torch.zeros_like(pre))
+    out[I_RHOGE] = F(prog[I_RHOGE].r + scale * fe * D["rho"].r * m["GSGAM2"].r, prog[I_RHOGE].p)
+    return xch(core, out)
+
+
 class DynamicsStep:
     """the differentiable dynamics step of one grid.
 
@@ -560,12 +598,20 @@ class DynamicsStep:
     pair (x, x_pl) of tensors (6, lall, kall, g, g) / (6, 6, kall, 2) in
     prognostic order (RHOG, RHOGVX, RHOGVY, RHOGVZ, RHOGW, RHOGE)."""
 
-    def __init__(self, core, geo: dict, device="cuda"):
+    def __init__(self, core, geo: dict, device="cuda", hs_lat=None, hs_moist: bool = False):
+        """``hs_lat``: the column latitudes (gall_1d, gall_1d, lall) of a
+        Held-Suarez run; each step is then followed by its forcing step"""
         self.core, self.m = core, Metrics(geo, device)
+        self.hs_lat, self.hs_moist = None, hs_moist
+        if hs_lat is not None:
+            self.hs_lat = torch.as_tensor(np.ascontiguousarray(np.transpose(np.asarray(hs_lat, np.float64),
+                                                                            (2, 1, 0)))[:, None]).to(device)
 
     def step(self, x, x_pl, tracers=None, tracers_pl=None):
         Q = [] if tracers is None else [F(tracers[n], tracers_pl[n]) for n in range(tracers.shape[0])]
         out = dynamics_step(self.m, self.core, unstack(x, x_pl), Q)
+        if self.hs_lat is not None:
+            out = held_suarez(self.m, self.core, out, self.hs_lat, Q, self.hs_moist)
         return stack(out)
 
     def run(self, x, x_pl, nsteps: int, checkpoint: bool = True, tracers=None, tracers_pl=None):

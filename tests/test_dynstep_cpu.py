@@ -140,3 +140,30 @@ def test_step_equals_oracle(case, request):
         tol = 1e-12 * np.abs(b).max()
         assert np.abs(a - b).max() <= tol, (n, np.abs(a - b).max() / np.abs(b).max())
         assert np.abs(y_pl[n][0].numpy() - want_pl[0, :, :, n]).max() <= tol, n
+
+
+def test_held_suarez_equals_oracle(golden_hs):
+    """the Held-Suarez forcing step (diagnostics, tendencies, update,
+    exchange) from the fixture's states against the oracle's
+    forcing_step_hs: relative max difference <= 1e-12 per prognostic"""
+    from oracle import nicam_step as O
+    ds, adj = _mods()
+    geo, lat, st = golden_hs
+    ops = OracleOps(geo)
+    m = ds.Metrics(geo, device="cpu")
+    latt = torch.as_tensor(np.ascontiguousarray(np.transpose(np.asarray(lat, np.float64), (2, 1, 0)))[:, None])
+    G = O.Geo(geo)
+    for name in ("state0", "state1"):
+        s, sp = st[name], st[name + "_pl"]
+        x = torch.stack([adj.to_device_layout(s[..., n], "cpu") for n in range(6)])
+        x_pl = torch.as_tensor(np.ascontiguousarray(np.moveaxis(sp[..., :6], -1, 0)))
+        Q = [ds.F(adj.to_device_layout(s[..., 6 + n], "cpu"), torch.as_tensor(np.ascontiguousarray(sp[..., 6 + n])))
+             for n in range(s.shape[-1] - 6)]
+        with torch.no_grad():
+            y, y_pl = ds.stack(ds.held_suarez(m, ops, ds.unstack(x, x_pl), latt, Q))
+        want, want_pl = O.forcing_step_hs(G, s, sp, lat)
+        for n in range(6):
+            a, b = adj.from_device_layout(y[n])[1:-1, 1:-1], want[1:-1, 1:-1, :, :, n]
+            tol = 1e-12 * np.abs(b).max()
+            assert np.abs(a - b).max() <= tol, (name, n, np.abs(a - b).max() / np.abs(b).max())
+            assert np.abs(y_pl[n][0].numpy() - want_pl[0, :, :, n]).max() <= tol, (name, n)
