@@ -119,6 +119,42 @@ def test_dot_product_step(pkg, case, request):
     assert abs(lhs - rhs) <= 1e-12 * scale, (lhs, rhs, scale)
 
 
+def test_held_suarez_step(pkg, golden_hs):
+    """the Held-Suarez forcing step on the device against the oracle's
+    forcing_step_hs (1e-12), and the dot-product test of a large step
+    followed by it (1e-12)"""
+    from oracle import nicam_step as O
+    import torch
+    import torch.autograd.forward_ad as fwAD
+    ds, adj = _mods()
+    geo, lat, st = golden_hs
+    core = pkg.NicamCuda(geo, graph=False)
+    try:
+        s, sp = st["state1"], st["state1_pl"]
+        x, x_pl, q, q_pl = _dev_state(s, sp)
+        m = ds.Metrics(geo)
+        latt = torch.as_tensor(np.ascontiguousarray(np.transpose(np.asarray(lat, np.float64), (2, 1, 0)))[:, None]).cuda()
+        Q = [ds.F(q[n], q_pl[n]) for n in range(q.shape[0])]
+        with torch.no_grad():
+            y, y_pl = ds.stack(ds.held_suarez(m, core, ds.unstack(x, x_pl), latt, Q))
+        _rel_check(y, y_pl, *O.forcing_step_hs(O.Geo(geo), s, sp, lat))
+        stepper = ds.DynamicsStep(core, geo, hs_lat=lat)
+        dx, dx_pl = _scaled(x, x_pl, 91)
+        with fwAD.dual_level():
+            y, y_pl = stepper.step(fwAD.make_dual(x, dx), fwAD.make_dual(x_pl, dx_pl), q, q_pl)
+            ty, ty_pl = fwAD.unpack_dual(y).tangent, fwAD.unpack_dual(y_pl).tangent
+        w, w_pl = _rand_like(ty, 93), _rand_like(ty_pl, 94)
+        xr, xr_pl = x.clone().requires_grad_(True), x_pl.clone().requires_grad_(True)
+        y, y_pl = stepper.step(xr, xr_pl, q, q_pl)
+        g, g_pl = torch.autograd.grad((y * w).sum() + (y_pl * w_pl).sum(), (xr, xr_pl))
+        lhs = float((ty * w).sum() + (ty_pl * w_pl).sum())
+        rhs = float((dx * g).sum() + (dx_pl * g_pl).sum())
+        scale = float((ty * w).abs().sum() + (ty_pl * w_pl).abs().sum())
+        assert abs(lhs - rhs) <= 1e-12 * scale, (lhs, rhs, scale)
+    finally:
+        core.close()
+
+
 def _report(key, rep):
     out_dir = os.environ.get("NC_REPORT_DIR")
     if not out_dir:
