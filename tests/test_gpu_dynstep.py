@@ -2,10 +2,13 @@
 
 * one large step of the torch composition over the library's operators
   against the oracle's dynamics_step and against the handle's own step
-  (gl03 z10 fixture): relative max difference <= 1e-12;
+  (gl03 z10 fixtures: DIRECT and NONLINEAR1 hyperdiffusion, the Rayleigh
+  sponge): relative max difference <= 1e-12;
 * dot-product test of one step, the tangent-linear by forward-mode AD (the
   operators' forward kernels on the tangent) against the adjoint by
   reverse-mode AD (their transposed kernels): 1e-12;
+* the Held-Suarez forcing step against the oracle's, and the dot-product
+  test of a step followed by it;
 * the adjoint configuration: grid level 6, 40 layers, the balanced jet plus
   seeded Gaussian temperature noise (0.1 K), 36 steps of 300 s, loss the sum
   over a 20 x 20 degree box of the squared deviation of the surface pressure
